@@ -1,0 +1,418 @@
+// CPU oracle: the time model of the `retime` effect and the extern "C" surface the tests, the
+// smoke check and the CPU baseline leg of the benchmark load through ctypes. TEST
+// INFRASTRUCTURE ONLY; the product library never links it.
+//
+// Time model restated from plugins/retime-engine/src/timeline.rs (Rates :106-131,
+// frame_positions :136-142, RemapTimeMap::src_pos :266-331, frame_time :336-344, select :451-469,
+// exact_position :429-439), the parameter reads of frontend.rs:184-244 and the frame loop of
+// crates/fx-cli/src/temporal.rs:183-250 (current_time = n * time_step, missing frames blank:
+// host.rs:338-352).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "oracle_core.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+using namespace orc;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int rc, const std::string& e) {
+    g_err = e;
+    return rc;
+}
+
+struct Key {
+    long long time;
+    double value;
+    bool ease;
+};
+
+// crates/fx-core/src/curves.rs:348-375 and :537-544: a float curve (constant when no key)
+struct Curve {
+    double constant = 0.0;
+    std::vector<Key> keys;
+    double at(long long time) const {
+        if (keys.empty()) return constant;
+        size_t last = keys.size() - 1;
+        if (time <= keys[0].time) return keys[0].value;
+        if (time >= keys[last].time) return keys[last].value;
+        size_t i = 0;
+        while (i + 1 < keys.size() && keys[i + 1].time <= time) i++;
+        const Key &a = keys[i], &b = keys[i + 1];
+        double u = (double)(time - a.time) / (double)(b.time - a.time);
+        double f;
+        if (!a.ease && !b.ease) f = u;
+        else if (a.ease && b.ease) f = u * u * (3.0 - 2.0 * u);
+        else if (a.ease) f = u * u * (2.0 - u);
+        else f = u * (1.0 + u * (1.0 - u));
+        return a.value + (b.value - a.value) * f;
+    }
+};
+
+// crates/fx-core/src/fixed.rs:8-10
+int32_t float_to_fixed(double f) {
+    double v = f * 65536.0 + (f < 0.0 ? -0.5 : 0.5);
+    if (std::isnan(v)) return 0;
+    if (v >= 2147483647.0) return INT32_MAX;
+    if (v <= -2147483648.0) return INT32_MIN;
+    return (int32_t)v;
+}
+// frontend.rs:131-133
+float fixed_reader(int32_t fixed, float scale) { return (float)((double)fixed * (1.0 / 65536.0)) * scale; }
+
+int32_t cvtt_i32_d(double x) {  // timeline.rs:43-49
+    if (x > -2147483649.0 && x < 2147483648.0) return (int32_t)x;
+    return INT32_MIN;
+}
+int32_t cvtt_i32_f(float x) {  // timeline.rs:52-58
+    if (x > -2147483904.0f && x < 2147483648.0f) return (int32_t)x;
+    return INT32_MIN;
+}
+
+struct TimeMap {
+    Curve speed;
+    double in_fps = 30.0, out_fps = 30.0;
+    float dur = 100.0f;
+    int lts = 100;
+    int base = 0;
+    // timeline.rs:266-331 (Speed mode; Src Time Offset 0)
+    float src_pos(float t) {
+        float lts_f = (float)lts;
+        float out = 0.0f;
+        int time0 = cvtt_i32_d((double)(lts_f * t) + 0.05);
+        (void)time0;
+        base = 0;  // -trunc(0 * 2^-16)
+        int n2 = cvtt_i32_f(t * 2.0f);
+        float k = 1.0f;
+        while ((float)n2 >= k) {
+            int time = cvtt_i32_d((double)((lts_f * k) / 2.0f) + 0.05);
+            float sp = (float)((double)float_to_fixed(speed.at(time)) / 6553600.0);
+            out = (sp / 2.0f) + out;
+            k += 1.0f;
+        }
+        float tt = t * 2.0f;
+        float rem = tt - (k + -1.0f);
+        if ((double)rem > 0.0001) {
+            int time = cvtt_i32_d((double)((tt * lts_f) / 2.0f) + 0.05);
+            float sp = (float)((double)float_to_fixed(speed.at(time)) / 6553600.0);
+            out = ((rem * sp) / 2.0f) + out;
+        }
+        return (float)((in_fps / out_fps) * (double)out);
+    }
+    int frame_time(float f) const {  // timeline.rs:336-344
+        float d = f - (float)base;
+        if (std::fabs(in_fps - out_fps) < 0.05) return cvtt_i32_d((double)d * (double)dur + 0.5);
+        return cvtt_i32_d((double)(d * dur) + (double)dur * 0.05);
+    }
+};
+
+bool exact_position(float s0, float s1, float blur) {  // timeline.rs:429-439
+    bool exact = true;
+    float frac = s0 - std::floor(s0);
+    if ((double)std::fabs(frac) > 0.005 && (double)std::fabs((float)((double)frac - 1.0)) > 0.005) exact = false;
+    if ((double)std::fabs(s0 - s1) > 1e-6 && (double)blur > 0.005) exact = false;
+    return exact;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Parameters of one `retime` render, as the effect reads them (plugins/retime/src/lib.rs:59-99).
+// Popups carry their raw 1-based values. The speed curve is constant (`nkeys == 0`) or keyed at
+// frame numbers with an optional ease flag per key.
+struct or_retime_params {
+    int fps_num, fps_den;      // --fps
+    int quality_high;          // --quality (1 high, 0 draft)
+    double speed_percent;      // constant Speed %
+    int nkeys;                 // keyed Speed % (0: constant)
+    const double* key_frames;  // frame numbers of the keys
+    const double* key_values;
+    const int* key_ease;
+    int vectors;               // popup 1..5 (5 Best)
+    int frame_interp;          // popup 1..3 (2 Blend)
+    int smart_blend;
+    double sensitivity;        // slider, percent
+    double blur_compensation;  // slider
+    // The two orders the reference changed after its parity grid was recorded (docs/parity.md,
+    // "The rewrite" table): 1, 1 is the reference's current code (plugins/retime/src/glue.rs:39-40,
+    // flow/conv.rs:598-615); 0, 0 reproduces parity/retime-flow/results/base.grid.tsv.
+    int rows_reversed;         // motion path on bottom-up rows
+    int taps_above_first;      // vertical border rows of the solver's filters
+};
+
+const char* or_last_error(void) { return g_err.c_str(); }
+
+int or_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void or_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+// ---- single functions, for the parity tests ---------------------------------------------------
+
+int or_from_frame(const void* wire, int w, int h, int fmt, void* engine) {
+    Image img = from_frame(wire, w, h, (Fmt)fmt);
+    std::memcpy(engine, img.data(), img.bytes());
+    return 0;
+}
+
+int or_to_frame(const void* engine, int w, int h, int fmt, void* wire) {
+    Image img(w, h, (Fmt)fmt);
+    std::memcpy(img.data(), engine, img.bytes());
+    to_frame(img, wire);
+    return 0;
+}
+
+int or_gaussian_kernel(float r, float* out, int cap) {
+    std::vector<float> k = gaussian_kernel(r);
+    int n = (int)k.size();
+    for (int i = 0; i < n && i < cap; i++) out[i] = k[i];
+    return n;
+}
+
+void or_start_level(float sensitivity, int levels, int* start, float* damp) { start_level(sensitivity, levels, start, damp); }
+
+float or_block_cost(const float* b, int w, int h, const float* p9, float x2, float y2, int* some) {
+    bool s;
+    float c = block_cost(nullptr, b, w, h, p9, x2, y2, &s);
+    *some = s ? 1 : 0;
+    return c;
+}
+
+void or_convolve(float* data, int w, int h, int c, const float* k, int n, int above_first) {
+    convolve(data, w, h, c, k, n, above_first != 0);
+}
+void or_calc_grad(const float* img, int w, int h, float* g) {
+    auto v = calc_grad(img, w, h);
+    std::memcpy(g, v.data(), v.size() * 4);
+}
+void or_new_disp(float* flow, const float* a, const float* b, long npx) { new_disp(flow, a, b, (size_t)npx); }
+void or_upsample_flow(const float* src, int sw, int sh, int dw, int dh, float* dst) {
+    auto v = upsample_flow(src, sw, sh, dw, dh);
+    std::memcpy(dst, v.data(), v.size() * 4);
+}
+void or_block_match(const float* a, const float* b, float* flow, int w, int h) { block_match(a, b, flow, w, h); }
+int or_all_out_of_range(const float* flow, int w, int h) { return all_flow_out_of_range(flow, w, h) ? 1 : 0; }
+
+// Flow geometry: returns the level count and writes (w, h) per level into sizes (2 * cap ints).
+int or_geometry(int quality, int hiq, int w, int h, int* reduction, int* sizes, int cap) {
+    FlowSettings s;
+    s.quality = quality;
+    s.hiq = hiq != 0;
+    Geometry g;
+    std::string e;
+    if (!geometry(s, w, h, &g, &e)) return fail(-1, e);
+    *reduction = g.reduction;
+    for (int i = 0; i < g.levels && i < cap; i++) { sizes[2 * i] = g.sizes[i].first; sizes[2 * i + 1] = g.sizes[i].second; }
+    return g.levels;
+}
+
+// The band pass levels of one engine image, concatenated finest first.
+int or_build_pyramid(const void* engine, int w, int h, int fmt, int quality, int hiq, float sensitivity, int above_first,
+                     float* levels_out) {
+    Image img(w, h, (Fmt)fmt);
+    std::memcpy(img.data(), engine, img.bytes());
+    FlowSettings s;
+    s.taps_above_first = above_first != 0;
+    s.quality = quality;
+    s.hiq = hiq != 0;
+    s.sensitivity = sensitivity;
+    Pyramid p;
+    std::string e;
+    if (!build_pyramid(img, s, &p, &e)) return fail(-1, e);
+    size_t off = 0;
+    for (auto& l : p.levels) { std::memcpy(levels_out + off, l.d.data(), l.d.size() * 4); off += l.d.size(); }
+    return p.geo.levels;
+}
+
+// flow::solve_pair on two engine images; f_ab and f_ba receive the working size fields.
+int or_solve_pair(const void* a_eng, const void* b_eng, int w, int h, int fmt, int quality, int hiq, float sensitivity,
+                  int skip_refine, int above_first, float* f_ab, float* f_ba) {
+    Image a(w, h, (Fmt)fmt), b(w, h, (Fmt)fmt);
+    std::memcpy(a.data(), a_eng, a.bytes());
+    std::memcpy(b.data(), b_eng, b.bytes());
+    FlowSettings s;
+    s.quality = quality;
+    s.hiq = hiq != 0;
+    s.sensitivity = sensitivity;
+    s.skip_refine = skip_refine != 0;
+    s.taps_above_first = above_first != 0;
+    FlowField fab, fba;
+    std::string e;
+    if (!solve_pair(a, b, s, &fab, &fba, &e)) return fail(-1, e);
+    std::memcpy(f_ab, fab.d.data(), fab.d.size() * 4);
+    std::memcpy(f_ba, fba.d.data(), fba.d.size() * 4);
+    return 0;
+}
+
+// warp::inv_warp / inv_warp_coverage on engine images (hold, mode 1, no 360). cov may be null.
+int or_inv_warp(void* out_eng, const void* src_eng, int w, int h, int fmt, const float* flow, int fw, int fh, float amount,
+                int hold, uint8_t* cov) {
+    Image src(w, h, (Fmt)fmt), out(w, h, (Fmt)fmt);
+    std::memcpy(src.data(), src_eng, src.bytes());
+    std::memcpy(out.data(), out_eng, out.bytes());
+    FlowField f(fw, fh);
+    std::memcpy(f.d.data(), flow, f.d.size() * 4);
+    WarpOpts o;
+    o.hold = hold != 0;
+    Coverage c;
+    std::string e;
+    int rc = inv_warp(out, src, f, amount, o, cov ? &c : nullptr, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(out_eng, out.data(), out.bytes());
+    if (cov) std::memcpy(cov, c.d.data(), c.d.size());
+    return 0;
+}
+
+int or_blend(void* out_eng, const void* a_eng, const void* b_eng, int w, int h, int fmt, float wt) {
+    Image a(w, h, (Fmt)fmt), b(w, h, (Fmt)fmt), out(w, h, (Fmt)fmt);
+    std::memcpy(a.data(), a_eng, a.bytes());
+    std::memcpy(b.data(), b_eng, b.bytes());
+    blend(out, a, b, wt);
+    std::memcpy(out_eng, out.data(), out.bytes());
+    return 0;
+}
+
+// compose::compose_vectors (warping code 0) on engine images with given flows.
+int or_compose_vectors(const void* a_eng, const void* b_eng, int w, int h, int fmt, const float* f_ab, const float* f_ba,
+                       int fw, int fh, float wa, int interp, void* out_eng) {
+    Image a(w, h, (Fmt)fmt), b(w, h, (Fmt)fmt), out;
+    std::memcpy(a.data(), a_eng, a.bytes());
+    std::memcpy(b.data(), b_eng, b.bytes());
+    FlowField fab(fw, fh), fba(fw, fh);
+    if (f_ab) std::memcpy(fab.d.data(), f_ab, fab.d.size() * 4);
+    if (f_ba) std::memcpy(fba.d.data(), f_ba, fba.d.size() * 4);
+    ComposeSettings cs;
+    Selection sel;
+    sel.wa = wa;
+    sel.interp = interp;
+    std::string e;
+    int rc = compose_vectors(cs, sel, a, b, f_ab ? &fab : nullptr, f_ba ? &fba : nullptr, &out, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(out_eng, out.data(), out.bytes());
+    return 0;
+}
+
+// ---- the whole effect ---------------------------------------------------------------------------
+
+// One output frame's selection (timeline.rs:451-469) for output frame index n of a clip.
+int or_select(const or_retime_params* p, int n, int w, int h, float* s0, float* s1, int* a, float* wa, int* exact,
+              int* vq, int* interp) {
+    bool integer = p->fps_den == 1;
+    int time_step = integer ? 100 : p->fps_den;
+    TimeMap map;
+    map.lts = time_step;
+    map.in_fps = 30.0;  // In FPS is Out FPS (default on): both rates 30 (timeline.rs:117-120)
+    map.out_fps = 30.0;
+    map.dur = (float)(((double)time_step * 30.0) / 30.0);
+    map.speed.constant = p->speed_percent;
+    for (int i = 0; i < p->nkeys; i++) {
+        long long t = (long long)std::llround(p->key_frames[i] * (double)time_step);
+        map.speed.keys.push_back({t, p->key_values[i], p->key_ease && p->key_ease[i] != 0});
+    }
+    int cur = n * time_step;
+    float t0 = (float)cur / (float)time_step;
+    float t1 = ((float)time_step + (float)cur) / (float)time_step;
+    *s0 = map.src_pos(t0);
+    *s1 = map.src_pos(t1);
+    float blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
+    *a = cvtt_i32_f(*s0);
+    float frac = *s0 - (float)*a;
+    *wa = 1.0f - frac;
+    *exact = exact_position(*s0, *s1, blur) ? 1 : 0;
+    int vqr = p->vectors - 1;
+    *vq = (w >= 2 && h >= 2) ? vqr : 0;  // prep.rs:111-117
+    *interp = p->frame_interp - 1;
+    return 0;
+}
+
+// Renders `nout` output frames of the `retime` effect over a raw clip of `nframes` wire frames.
+// Returns 0, or a nonzero status with or_last_error() naming what is not restated.
+int or_retime_clip(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int nout,
+                   void* out) {
+    Fmt f = (Fmt)fmt;
+    size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
+    size_t frame_bytes = (size_t)w * h * 4 * es;
+    bool integer = p->fps_den == 1;
+    int time_step = integer ? 100 : p->fps_den;
+    if (p->smart_blend) return fail(2, "smart blend is not restated in the clip runner");
+    float sensitivity = fixed_reader(float_to_fixed(p->sensitivity), 1.0f) / 100.0f;
+    for (int n = 0; n < nout; n++) {
+        float s0, s1, wa;
+        int a, exact, vq, interp;
+        or_select(p, n, w, h, &s0, &s1, &a, &wa, &exact, &vq, &interp);
+        auto fetch = [&](int pos) -> Image {
+            // main_frame(position): frame_time (dur == lts, equal rates), then the clip frame of that tick
+            double d = (double)(float)pos;
+            int time = cvtt_i32_d(d * (double)time_step + 0.5);
+            long long idx = time >= 0 ? time / time_step : -(((long long)-time + time_step - 1) / time_step);
+            if (idx < 0 || idx >= nframes) return Image(w, h, f);
+            return from_frame((const uint8_t*)frames + (size_t)idx * frame_bytes, w, h, f);
+        };
+        Image A = fetch(a), B = fetch(a + 1), result;
+        Selection sel;
+        sel.s0 = s0; sel.s1 = s1; sel.a = a; sel.b = a + 1; sel.wa = wa; sel.exact = exact != 0;
+        sel.vectors_quality = vq; sel.interp = interp;
+        std::string e;
+        if (vq != 0 && !exact) {
+            if (interp < 0 || interp > 1) return fail(2, "weighted blend on the vector path is not restated");
+            // plugin 01 runs the motion path on bottom-up rows (plugins/retime/src/glue.rs:39-40,
+            // compose/vector.rs:303-314)
+            Image ar = p->rows_reversed ? rows_reversed(A) : A, br = p->rows_reversed ? rows_reversed(B) : B;
+            FlowSettings fs;
+            fs.quality = vq;
+            fs.hiq = p->quality_high != 0;
+            fs.sensitivity = sensitivity;
+            fs.taps_above_first = p->taps_above_first != 0;
+            FlowField fab, fba;
+            bool have_ab = false, have_ba = false;
+            if (interp == 0) {
+                ComposeSettings cs0;
+                if (nearest_uses_f_ab(wa, cs0.warp_mode)) {
+                    if (!solve(ar, br, fs, &fab, &e)) return fail(1, e);
+                    have_ab = true;
+                } else {
+                    if (!solve(br, ar, fs, &fba, &e)) return fail(1, e);
+                    have_ba = true;
+                }
+            } else {
+                if (!solve_pair(ar, br, fs, &fab, &fba, &e)) return fail(1, e);
+                have_ab = have_ba = true;
+            }
+            ComposeSettings cs;
+            cs.quality_high = fs.hiq;
+            cs.blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
+            Image o;
+            int rc = compose_vectors(cs, sel, ar, br, have_ab ? &fab : nullptr, have_ba ? &fba : nullptr, &o, &e);
+            if (rc) return fail(rc, e);
+            result = p->rows_reversed ? rows_reversed(o) : o;
+        } else {
+            int rc = interpolate(sel, A, B, &result, &e);
+            if (rc) return fail(rc, e);
+        }
+        to_frame(result, (uint8_t*)out + (size_t)n * frame_bytes);
+    }
+    return 0;
+}
+
+}  // extern "C"

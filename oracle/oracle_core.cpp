@@ -1,0 +1,1123 @@
+// CPU oracle, core functions. TEST INFRASTRUCTURE ONLY (see oracle_core.h). Each function cites
+// the reference file:line (crate plugins/retime-engine/src/) whose arithmetic it restates.
+#include "oracle_core.h"
+
+#include <algorithm>
+#include <cstdio>
+
+#ifdef _OPENMP
+#include <omp.h>
+#define OMP_FOR _Pragma("omp parallel for schedule(static)")
+#else
+#define OMP_FOR
+#endif
+
+namespace orc {
+
+// =============================================================================================
+// image boundary
+
+static const float INV_255 = bits_f(0x3b808081u);            // image.rs:261
+static const float PREMUL_16_COLOR = bits_f(0x387fff00u);    // image.rs:263
+static const float PREMUL_16_ALPHA = bits_f(0x3fffff00u);    // image.rs:265
+static const float UNPREMUL_16_ALPHA = bits_f(0x3f000080u);  // image.rs:267
+
+static inline uint16_t u16_to_q15(uint16_t v) { return (uint16_t)(((uint32_t)v * 32768u + 32767u) / 65535u); }
+static inline uint16_t q15_to_u16(uint16_t v) {
+    uint32_t m = v < 32768 ? v : 32768;
+    return (uint16_t)((m * 65535u + 16384u) / 32768u);
+}
+
+// image.rs:276-280
+static inline void premultiply_u8(const uint8_t p[4], uint8_t o[4]) {
+    float a = (float)p[0] * INV_255;
+    o[0] = p[0];
+    for (int c = 1; c < 4; c++) o[c] = (uint8_t)q((float)p[c] * a);
+}
+// image.rs:283-291
+static inline void premultiply_u16(const uint16_t p[4], uint16_t o[4]) {
+    float a = (float)p[0] * PREMUL_16_COLOR;
+    o[0] = (uint16_t)q((float)p[0] * PREMUL_16_ALPHA);
+    for (int c = 1; c < 4; c++) o[c] = (uint16_t)q((float)p[c] * a);
+}
+// image.rs:294-303
+static inline void premultiply_f32(const float p[4], float o[4]) {
+    float r[4] = {p[0], p[0] * p[1], p[0] * p[2], p[0] * p[3]};
+    if (std::isnan(r[1]) || std::isnan(r[2]) || std::isnan(r[3]) || std::isnan(r[0])) {
+        r[1] = nr::mul(p[0], p[1]);
+        r[2] = nr::mul(p[0], p[2]);
+        r[3] = nr::mul(p[0], p[3]);
+    }
+    for (int c = 0; c < 4; c++) o[c] = r[c];
+}
+// image.rs:306-320
+static inline void unpremultiply_u8(const uint8_t p[4], uint8_t o[4]) {
+    if (p[0] == 0) { for (int c = 0; c < 4; c++) o[c] = p[c]; return; }
+    float s = 255.0f / (float)p[0];
+    o[0] = p[0];
+    for (int c = 1; c < 4; c++) {
+        float v = (float)p[c] * s;
+        if (v > 255.0f) v = 255.0f;
+        o[c] = (uint8_t)q(v);
+    }
+}
+// image.rs:325-332
+static inline void unpremultiply_u16(const uint16_t p[4], uint16_t o[4]) {
+    if (p[0] == 0) { for (int c = 0; c < 4; c++) o[c] = p[c]; return; }
+    float a = (float)p[0];
+    float s = 32768.0f / a;
+    o[0] = (uint16_t)q(a * UNPREMUL_16_ALPHA);
+    for (int c = 1; c < 4; c++) o[c] = (uint16_t)q((float)p[c] * s);
+}
+// image.rs:339-351
+static inline void unpremultiply_f32(const float p[4], float o[4]) {
+    if ((double)p[0] < 1e-12) { for (int c = 0; c < 4; c++) o[c] = 0.0f; return; }
+    float inv = 1.0f / p[0];
+    float r[4] = {p[0], p[1] * inv, p[2] * inv, p[3] * inv};
+    if (std::isnan(r[0]) || std::isnan(r[1]) || std::isnan(r[2]) || std::isnan(r[3])) {
+        r[1] = nr::mul(p[1], inv);
+        r[2] = nr::mul(p[2], inv);
+        r[3] = nr::mul(p[3], inv);
+    }
+    for (int c = 0; c < 4; c++) o[c] = r[c];
+}
+
+Image from_frame(const void* wire, int w, int h, Fmt fmt) {
+    Image img(w, h, fmt);
+    size_t n = (size_t)w * h;
+    if (fmt == U8) {
+        const uint8_t* px = (const uint8_t*)wire;
+        OMP_FOR
+        for (long i = 0; i < (long)n; i++) {
+            uint8_t p[4] = {px[i * 4 + 3], px[i * 4 + 0], px[i * 4 + 1], px[i * 4 + 2]};
+            premultiply_u8(p, &img.u8[i * 4]);
+        }
+    } else if (fmt == U16) {
+        const uint16_t* px = (const uint16_t*)wire;  // little endian host
+        OMP_FOR
+        for (long i = 0; i < (long)n; i++) {
+            uint16_t p[4] = {u16_to_q15(px[i * 4 + 3]), u16_to_q15(px[i * 4 + 0]), u16_to_q15(px[i * 4 + 1]),
+                             u16_to_q15(px[i * 4 + 2])};
+            premultiply_u16(p, &img.u16[i * 4]);
+        }
+    } else {
+        const float* pl = (const float*)wire;  // planes G, B, R, A
+        OMP_FOR
+        for (long i = 0; i < (long)n; i++) {
+            float p[4] = {pl[3 * n + i], pl[2 * n + i], pl[0 * n + i], pl[1 * n + i]};
+            premultiply_f32(p, &img.f32[i * 4]);
+        }
+    }
+    return img;
+}
+
+void to_frame(const Image& img, void* wire) {
+    size_t n = (size_t)img.w * img.h;
+    if (img.fmt == U8) {
+        uint8_t* out = (uint8_t*)wire;
+        OMP_FOR
+        for (long i = 0; i < (long)n; i++) {
+            uint8_t o[4];
+            unpremultiply_u8(&img.u8[i * 4], o);
+            out[i * 4 + 0] = o[1]; out[i * 4 + 1] = o[2]; out[i * 4 + 2] = o[3]; out[i * 4 + 3] = o[0];
+        }
+    } else if (img.fmt == U16) {
+        uint16_t* out = (uint16_t*)wire;
+        OMP_FOR
+        for (long i = 0; i < (long)n; i++) {
+            uint16_t o[4];
+            unpremultiply_u16(&img.u16[i * 4], o);
+            out[i * 4 + 0] = q15_to_u16(o[1]); out[i * 4 + 1] = q15_to_u16(o[2]);
+            out[i * 4 + 2] = q15_to_u16(o[3]); out[i * 4 + 3] = q15_to_u16(o[0]);
+        }
+    } else {
+        float* pl = (float*)wire;
+        OMP_FOR
+        for (long i = 0; i < (long)n; i++) {
+            float o[4];
+            unpremultiply_f32(&img.f32[i * 4], o);
+            // pixel [r, g, b, a] -> planes in the channel order 1, 2, 0, 3 = G, B, R, A
+            pl[0 * n + i] = o[2]; pl[1 * n + i] = o[3]; pl[2 * n + i] = o[1]; pl[3 * n + i] = o[0];
+        }
+    }
+}
+
+Image rows_reversed(const Image& img) {
+    Image out(img.w, img.h, img.fmt);
+    size_t es = img.fmt == U8 ? 1 : img.fmt == U16 ? 2 : 4;
+    size_t row = (size_t)img.w * 4 * es;
+    const uint8_t* s = (const uint8_t*)img.data();
+    uint8_t* o = (uint8_t*)out.data();
+    for (int y = 0; y < img.h; y++) std::memcpy(o + (size_t)y * row, s + (size_t)(img.h - 1 - y) * row, row);
+    return out;
+}
+
+// =============================================================================================
+// geometry (prep.rs:63-146, flow.rs:129-197)
+
+void flow_resolution(int qv, bool hiq, int w, int h, int* r_out, int* w0, int* h0) {
+    int r = (qv <= 2) ? 3 : (qv == 3) ? 2 : (qv == 4) ? 1 : 0;
+    if (!hiq) r = (r == 0) ? 1 : (r == 1) ? 2 : (r == 2) ? 3 : r;
+    while (r > 0 && ((w >> r) < 2 || (h >> r) < 2)) r -= 1;
+    int ww = w, hh = h;
+    for (int i = 0; i < r; i++) { ww /= 2; hh /= 2; }
+    *r_out = r; *w0 = ww; *h0 = hh;
+}
+
+int level_count(int w0, int h0, int min_size) {
+    int levels = 1, w = w0, h = h0;
+    for (;;) {
+        w /= 2;
+        if (w < min_size) break;
+        h /= 2;
+        if (h < min_size) break;
+        if (w > 2 && h > 2 && !(w == 2 && h == 2)) levels += 1;
+        else break;
+    }
+    return levels;
+}
+
+bool geometry(const FlowSettings& s, int w, int h, Geometry* g, std::string* err) {
+    if (s.quality == 0 || s.quality > 5) { *err = "flow quality outside 1..=5"; return false; }
+    if (!(s.sensitivity >= 0.0f) || !std::isfinite(s.sensitivity)) { *err = "bad sensitivity"; return false; }
+    flow_resolution(s.quality, s.hiq, w, h, &g->reduction, &g->w, &g->h);
+    if (g->w < 2 || g->h < 2) { *err = "working size below 2x2"; return false; }
+    g->levels = level_count(g->w, g->h, 2);
+    g->sizes.clear();
+    int lw = g->w, lh = g->h;
+    for (int i = 0; i < g->levels; i++) {
+        g->sizes.push_back({lw, lh});
+        lw = std::max(lw / 2, 2);
+        lh = std::max(lh / 2, 2);
+    }
+    return true;
+}
+
+// flow.rs:179-197
+void start_level(float sensitivity, int levels, int* start, float* damp) {
+    float p = (float)std::pow((double)sensitivity, 2.0);
+    float l1 = (float)std::log((double)p);
+    float l2 = (float)std::log(2.0);
+    float lv = (float)levels;
+    float x = l1 / l2 + lv;
+    if (0.0f <= x || std::isnan(x)) {
+        if (x < lv || std::isnan(x)) {
+            float f = std::floor(x);
+            int s = cvtt32(f);
+            int su = s < 0 ? 0 : s;
+            *start = std::min(su, levels - 1);
+            *damp = x - (float)su;
+        } else {
+            *start = levels - 1;
+            *damp = 1.0f;
+        }
+    } else {
+        *start = 0;
+        *damp = 0.0f;
+    }
+}
+
+// =============================================================================================
+// separable convolution (flow/conv.rs)
+
+std::vector<float> gaussian_kernel(float r) {  // conv.rs:64-86
+    int ri = std::isnan(r) ? 0 : (r >= 2147483648.0f ? INT32_MAX : (r < -2147483648.0f ? INT32_MIN : (int)r));
+    long nn = (long)ri + 1;
+    int n = nn < 0 ? 0 : (int)nn;
+    float s3 = r / 3.0f;
+    float d = s3 * s3;
+    std::vector<float> k;
+    float sum = 0.0f;
+    for (int i = 0; i < n; i++) {
+        float fi = (float)i;
+        float t = fi * fi;
+        float e = -(t / d);
+        float v = (float)std::pow(2.0, (double)e);
+        k.push_back(v);
+        sum += v;
+    }
+    if (n == 0) return k;
+    float den = sum * 2.0f - k[0];
+    for (auto& v : k) v /= den;
+    return k;
+}
+
+// conv.rs:101-137, border element; element t of the line at line[t * stride]
+template <int C, bool LEFT_FIRST>
+static inline float border_value(const float* line, long stride, int len, int i, const float* k, int n) {
+    float centre = (i >= 0 && i < len) ? line[(long)i * stride] : 0.0f;
+    float num = k[0] * centre;
+    float den = k[0];
+    for (int j = n - 1; j >= 1; j--) {
+        float kj = k[j];
+        for (int side = 0; side < 2; side++) {
+            bool right = (side == 0) != LEFT_FIRST;
+            int t = right ? i + j : i - j;
+            bool inside = t >= 0 && t < len;
+            float xv, w;
+            if (C == 1) {
+                if (inside) { xv = line[(long)t * stride]; w = kj; }
+                else { xv = 0.0f; w = 0.0f; }
+            } else {
+                float v = inside ? line[(long)t * stride] : -1.0f;
+                float mask = (v != -1.0f) ? 1.0f : 0.0f;
+                xv = v;
+                w = mask * kj;
+            }
+            den = den + w;
+            num = num + xv * w;
+        }
+    }
+    return num / den;
+}
+
+// conv.rs:141-190: one row of the horizontal pass
+template <int C>
+static void hrow(const float* x, float* out, int len, const float* k, int n) {
+    int head = std::min(n, len);
+    int interior = std::max(len - 2 * n, 0);
+    for (int c = 0; c < C; c++) {
+        for (int i = 0; i < head; i++) out[i * C + c] = border_value<C, false>(x + c, C, len, i, k, n);
+        for (int i = head + interior; i < len; i++) out[i * C + c] = border_value<C, false>(x + c, C, len, i, k, n);
+    }
+    if (interior > 0) {
+        int a = head * C, b = (head + interior) * C;
+        float k0 = k[0];
+        for (int t = a; t < b; t++) out[t] = x[t] * k0;
+        for (int j = n - 1; j >= 1; j--) {
+            int off = j * C;
+            float kj = k[j];
+            for (int t = a; t < b; t++) out[t] = out[t] + (x[t + off] + x[t - off]) * kj;
+        }
+    }
+}
+
+// conv.rs:268-301 (vrow_ordered); ABOVE_FIRST is the solver's order
+template <int C, bool ABOVE_FIRST>
+static void vrow_ordered(const float* src, float* out, int y, int w, int h, const float* k, int n) {
+    long row = (long)w * C;
+    int head = std::min(n, h);
+    int interior = std::max(h - 2 * n, 0);
+    if (y >= head && y < head + interior) {
+        float k0 = k[0];
+        const float* s0 = src + (long)y * row;
+        for (long t = 0; t < row; t++) out[t] = s0[t] * k0;
+        for (int j = n - 1; j >= 1; j--) {
+            const float* below = src + (long)(y + j) * row;
+            const float* above = src + (long)(y - j) * row;
+            float kj = k[j];
+            for (long t = 0; t < row; t++) out[t] = out[t] + (below[t] + above[t]) * kj;
+        }
+    } else {
+        for (int xc = 0; xc < w; xc++)
+            for (int c = 0; c < C; c++)
+                out[xc * C + c] = border_value<C, ABOVE_FIRST>(src + (long)xc * C + c, row, h, y, k, n);
+    }
+}
+
+template <int C, bool ABOVE_FIRST>
+static void convolve_c(float* data, int w, int h, const float* k, int n) {
+    if ((long)w * h == 0 || n == 0) return;
+    std::vector<float> tmp((size_t)w * h * C);
+    long row = (long)w * C;
+    OMP_FOR
+    for (int y = 0; y < h; y++) hrow<C>(data + y * row, tmp.data() + y * row, w, k, n);
+    OMP_FOR
+    for (int y = 0; y < h; y++) vrow_ordered<C, ABOVE_FIRST>(tmp.data(), data + y * row, y, w, h, k, n);
+}
+
+// conv.rs:598-615 (convolve_above_first) and conv.rs:306-318 (convolve, tap below first)
+void convolve(float* data, int w, int h, int c, const float* k, int n, bool above_first) {
+    if (above_first) {
+        if (c == 1) convolve_c<1, true>(data, w, h, k, n);
+        else if (c == 2) convolve_c<2, true>(data, w, h, k, n);
+        else convolve_c<3, true>(data, w, h, k, n);
+    } else {
+        if (c == 1) convolve_c<1, false>(data, w, h, k, n);
+        else if (c == 2) convolve_c<2, false>(data, w, h, k, n);
+        else convolve_c<3, false>(data, w, h, k, n);
+    }
+}
+
+void blur_gaussian(float* data, int w, int h, int c, float r, bool above_first) {  // conv.rs:618-624
+    if ((double)r < 0.001) return;
+    std::vector<float> k = gaussian_kernel(r);
+    convolve(data, w, h, c, k.data(), (int)k.size(), above_first);
+}
+
+static const float BINOMIAL5[3] = {0.375f, 0.25f, 0.0625f};  // conv.rs:48
+void blur5(float* data, int w, int h, bool above_first) { convolve(data, w, h, 1, BINOMIAL5, 3, above_first); }
+
+// =============================================================================================
+// samplers (flow/sample.rs)
+
+static inline void cell(float x, int len, int* io, float* fo) {  // sample.rs:31-41
+    int i = cvtt32(x);
+    float f = x - (float)i;
+    int last = len - 1;
+    if (i >= last) { i = last - 1; f = 1.0f; }
+    int iu = i < 0 ? 0 : i;
+    int lim = len >= 2 ? len - 2 : 0;
+    *io = std::min(iu, lim);
+    *fo = f;
+}
+
+float bilinear1(const float* img, int w, int h, float x, float y) {  // sample.rs:47-64
+    int ix, iy; float fx, fy;
+    cell(x, w, &ix, &fx);
+    cell(y, h, &iy, &fy);
+    long i = (long)iy * w + ix;
+    float p00 = img[i], p10 = img[i + 1], p01 = img[i + w], p11 = img[i + w + 1];
+    float top = (p10 - p00) * fx + p00;
+    float bot = (p11 - p01) * fx + p01;
+    return (bot - top) * fy + top;
+}
+
+void bilinear2(const float* img, int w, int h, float x, float y, float out[2]) {  // sample.rs:69-86
+    int ix, iy; float fx, fy;
+    cell(x, w, &ix, &fx);
+    cell(y, h, &iy, &fy);
+    long i = ((long)iy * w + ix) * 2;
+    long r = (long)w * 2;
+    for (int c = 0; c < 2; c++) {
+        float p00 = img[i + c], p10 = img[i + 2 + c], p01 = img[i + r + c], p11 = img[i + r + 2 + c];
+        float top = (p10 - p00) * fx + p00;
+        float bot = (p11 - p01) * fx + p01;
+        out[c] = (bot - top) * fy + top;
+    }
+}
+
+Plane resample1(const Plane& src, int dw, int dh) {  // sample.rs:91-112
+    Plane dst(dw, dh);
+    float sx = ((float)src.w - 1.0f) / (float)(dw - 1);
+    float sy = ((float)src.h - 1.0f) / (float)(dh - 1);
+    if (dw == 0 || dh == 0) return dst;
+    OMP_FOR
+    for (int y = 0; y < dh; y++) {
+        float fy = (float)y * sy;
+        for (int x = 0; x < dw; x++) dst.d[(size_t)y * dw + x] = bilinear1(src.d.data(), src.w, src.h, (float)x * sx, fy);
+    }
+    return dst;
+}
+
+// =============================================================================================
+// prep (prep.rs:168-259) and the pyramid (flow.rs:242-275)
+
+Plane luma(const Image& img, bool track_alpha, bool video_range) {
+    Plane out(img.w, img.h);
+    const float W30F = 0.3f, W59F = 0.59f, W11F = 0.11f;
+    const double W30D = 0.3, W59D = 0.59, W11D = 0.11;
+    long n = (long)img.w * img.h;
+    if (img.fmt == U8) {
+        OMP_FOR
+        for (long i = 0; i < n; i++) {
+            const uint8_t* px = &img.u8[i * 4];
+            float a = (float)px[0], r = (float)px[1], g = (float)px[2], b = (float)px[3];
+            float v;
+            if (video_range) v = ((r - 16.0f) * 255.0f) / 219.0f;
+            else {
+                float sum = (r * W30F + g * W59F) + b * W11F;
+                v = track_alpha ? (float)((double)sum + (double)a * W30D) : sum;
+            }
+            out.d[i] = v;
+        }
+    } else if (img.fmt == U16) {
+        OMP_FOR
+        for (long i = 0; i < n; i++) {
+            const uint16_t* px = &img.u16[i * 4];
+            double a = px[0], r = px[1], g = px[2], b = px[3];
+            float v;
+            if (video_range) v = (((float)px[1] / 257.0f - 16.0f) * 255.0f) / 219.0f;
+            else {
+                double sum = (g * W59D + r * W30D) + b * W11D;
+                if (track_alpha) sum += a * W30D;
+                v = (float)(sum / 257.0);
+            }
+            out.d[i] = v;
+        }
+    } else {
+        OMP_FOR
+        for (long i = 0; i < n; i++) {
+            const float* px = &img.f32[i * 4];
+            double a = px[0], r = px[1], g = px[2], b = px[3];
+            float v;
+            if (video_range) v = ((px[1] * 255.0f - 16.0f) * 255.0f) / 219.0f;
+            else {
+                double sum = (g * W59D + r * W30D) + b * W11D;
+                if (track_alpha) sum += a * W30D;
+                v = (float)(sum * 255.0);
+            }
+            out.d[i] = v;
+        }
+    }
+    return out;
+}
+
+Plane reduce(Plane t, int r, bool above_first) {  // prep.rs:252-259
+    for (int i = 0; i < r; i++) {
+        blur5(t.d.data(), t.w, t.h, above_first);
+        int nw = t.w / 2, nh = t.h / 2;
+        t = resample1(t, nw, nh);
+    }
+    return t;
+}
+
+bool build_pyramid(const Image& img, const FlowSettings& s, Pyramid* out, std::string* err) {
+    if (!geometry(s, img.w, img.h, &out->geo, err)) return false;
+    if (s.video_range_luma && s.track_alpha) { *err = "video range luma with track alpha"; return false; }
+    if (s.prep_delinearize || s.prep_contrast_edge) { *err = "prep transforms are not restated"; return false; }
+    Plane orig = reduce(luma(img, s.track_alpha, s.video_range_luma), out->geo.reduction, s.taps_above_first);
+    int n = out->geo.levels;
+    out->levels.clear();
+    for (int i = 0; i < n; i++) {
+        Plane tmp = orig;
+        blur5(tmp.d.data(), tmp.w, tmp.h, s.taps_above_first);
+        Plane next;
+        bool has_next = i + 1 < n;
+        if (has_next) next = resample1(tmp, out->geo.sizes[i + 1].first, out->geo.sizes[i + 1].second);
+        Plane band = orig;
+        for (size_t k = 0; k < band.d.size(); k++) band.d[k] = band.d[k] - tmp.d[k];
+        out->levels.push_back(std::move(band));
+        if (!has_next) break;
+        orig = std::move(next);
+    }
+    return true;
+}
+
+// =============================================================================================
+// solver kernels (flow.rs:277-442)
+
+std::vector<float> calc_grad(const float* img, int w, int h) {  // flow.rs:283-316
+    std::vector<float> g((size_t)w * h * 2, 0.0f);
+    if (w == 0 || h == 0) return g;
+    OMP_FOR
+    for (int y = 0; y < h; y++) {
+        for (int x = 0; x < w; x++) {
+            float c = img[(long)y * w + x];
+            float nx = 0.0f, dx = 0.0f, ny = 0.0f, dy = 0.0f;
+            if (x >= 1) { nx = (c - img[(long)y * w + x - 1]) + 0.0f; dx = 1.0f; }
+            if (y >= 1) { ny = (c - img[(long)(y - 1) * w + x]) + 0.0f; dy = 1.0f; }
+            if (x + 1 <= w - 1) { nx = nx + (img[(long)y * w + x + 1] - c); dx = dx + 1.0f; }
+            if (y + 1 <= h - 1) { ny = ny + (img[(long)(y + 1) * w + x] - c); dy = dy + 1.0f; }
+            g[((long)y * w + x) * 2] = nx / dx;
+            g[((long)y * w + x) * 2 + 1] = ny / dy;
+        }
+    }
+    return g;
+}
+
+std::vector<float> calc_a(const std::vector<float>& grad, int w, int h) {  // flow.rs:319-328
+    std::vector<float> a((size_t)w * h * 3);
+    long n = (long)w * h;
+    OMP_FOR
+    for (long i = 0; i < n; i++) {
+        float gx = grad[i * 2], gy = grad[i * 2 + 1];
+        a[i * 3] = gx * gx;
+        a[i * 3 + 1] = gx * gy;
+        a[i * 3 + 2] = gy * gy;
+    }
+    return a;
+}
+
+std::vector<float> calc_b(const float* i1, const float* i0, const float* grad, const float* flow, int w,
+                          int h) {  // flow.rs:334-357
+    std::vector<float> b((size_t)w * h * 2, 0.0f);
+    float fw = (float)w, fh = (float)h;
+    OMP_FOR
+    for (int y = 0; y < h; y++) {
+        float fy = (float)y;
+        for (int x = 0; x < w; x++) {
+            float fx = (float)x;
+            long i = (long)y * w + x;
+            float sx = fx - flow[i * 2];
+            float sy = fy - flow[i * 2 + 1];
+            if (sx < 0.0f || fw - 1.0f < sx || sy < 0.0f || fh - 1.0f < sy) {
+                b[i * 2] = 0.0f;
+                b[i * 2 + 1] = 0.0f;
+            } else {
+                float s = bilinear1(i0, w, h, sx, sy);
+                float r = s - i1[i];
+                b[i * 2] = r * grad[i * 2];
+                b[i * 2 + 1] = r * grad[i * 2 + 1];
+            }
+        }
+    }
+    return b;
+}
+
+void new_disp(float* flow, const float* a, const float* b, size_t npx) {  // flow.rs:361-371
+    OMP_FOR
+    for (long i = 0; i < (long)npx; i++) {
+        float aa = a[i * 3], ab = a[i * 3 + 1], ad = a[i * 3 + 2];
+        float bx = b[i * 2], by = b[i * 2 + 1];
+        float t = ab * ab - ad * aa;
+        if (std::fabs(t) > 40.0f) {
+            flow[i * 2] = (ab * by - ad * bx) / t + flow[i * 2];
+            flow[i * 2 + 1] = (ab * bx - aa * by) / t + flow[i * 2 + 1];
+        }
+    }
+}
+
+std::vector<float> upsample_flow(const float* src, int sw, int sh, int dw, int dh) {  // flow.rs:376-391
+    float sx = ((float)dw - 1.0f) / (float)(sw - 1);
+    float sy = ((float)dh - 1.0f) / (float)(sh - 1);
+    float rx = (float)(1.0 / (double)sx);
+    float ry = (float)(1.0 / (double)sy);
+    std::vector<float> dst((size_t)dw * dh * 2, 0.0f);
+    OMP_FOR
+    for (int y = 0; y < dh; y++) {
+        float fy = (float)y * ry;
+        for (int x = 0; x < dw; x++) {
+            float v[2];
+            bilinear2(src, sw, sh, (float)x * rx, fy, v);
+            dst[((long)y * dw + x) * 2] = v[0] * sx;
+            dst[((long)y * dw + x) * 2 + 1] = v[1] * sy;
+        }
+    }
+    return dst;
+}
+
+void scale_values(float* d, size_t n, float f) {  // flow.rs:422-427
+    if (f == 1.0f) return;
+    for (size_t i = 0; i < n; i++) d[i] = f * d[i];
+}
+
+bool all_flow_out_of_range(const float* flow, int w, int h) {  // flow.rs:430-442
+    float fw = (float)(w - 1), fh = (float)(h - 1);
+    for (int y = 0; y < h; y++) {
+        float fy = (float)y;
+        for (int x = 0; x < w; x++) {
+            float px = (float)x + flow[((long)y * w + x) * 2];
+            float py = fy + flow[((long)y * w + x) * 2 + 1];
+            if (0.0f <= px && px <= fw && 0.0f <= py && py <= fh) return false;
+        }
+    }
+    return true;
+}
+
+// flow.rs:474-523 (Block::cost)
+float block_cost(const float* a, const float* b, int w, int h, const float p[9], float x2, float y2, bool* some) {
+    (void)a;
+    float wm2 = (float)(w - 2), hm2 = (float)(h - 2);
+    *some = false;
+    if (x2 > wm2 || y2 > hm2) return 0.0f;
+    int ix, iy; float fx, fy;
+    if (x2 == wm2) { ix = cvtt32(wm2 - 1.0f); fx = 1.0f; }
+    else { ix = cvtt32(x2); fx = x2 - (float)ix; }
+    if (y2 == hm2) { iy = cvtt32(hm2 - 1.0f); fy = 1.0f; }
+    else { iy = cvtt32(y2); fy = y2 - (float)iy; }
+    if (ix < 1 || iy < 1) return 0.0f;
+    float w11 = fy * fx;
+    float w10 = fx - w11;
+    float w01 = fy - w11;
+    float w00 = ((1.0f - fx) - fy) + w11;
+    const float* base = b + (long)(iy - 1) * w + ix - 1;
+    float sq[9];
+    int n = 0;
+    for (int bb = 0; bb < 3; bb++) {
+        for (int aa = 0; aa < 3; aa++) {
+            const float* t = base + (long)bb * w + aa;
+            float qv = ((w00 * t[0] + w10 * t[1]) + w01 * t[w]) + w11 * t[w + 1];
+            float d = p[n] - qv;
+            sq[n] = d * d;
+            n++;
+        }
+    }
+    float s = sq[0] + sq[1];
+    for (int k = 2; k < 8; k++) s = s + sq[k];
+    *some = true;
+    return sq[8] + s;
+}
+
+// flow.rs:529-546 (Block::step); returns true when the neighbour replaces the vector
+static inline bool bm_step(const float* a, const float* b, int w, int h, int x, int y, const float cur[2],
+                           const float nb[2]) {
+    float tx = (float)x - cur[0];
+    float ty = (float)y - cur[1];
+    float w1 = (float)(w - 1), h1 = (float)(h - 1);
+    if (0.0f <= tx && tx <= w1 && 0.0f <= ty && ty <= h1) {
+        float p[9];
+        const float* pa = a + (long)(y - 1) * w + x - 1;
+        p[0] = pa[0]; p[1] = pa[1]; p[2] = pa[2];
+        p[3] = pa[w]; p[4] = pa[w + 1]; p[5] = pa[w + 2];
+        p[6] = pa[2 * w]; p[7] = pa[2 * w + 1]; p[8] = pa[2 * w + 2];
+        bool s0, s1;
+        float c0 = block_cost(a, b, w, h, p, tx, ty, &s0);
+        if (s0) {
+            float c1 = block_cost(a, b, w, h, p, (float)x - nb[0], (float)y - nb[1], &s1);
+            if (s1 && c1 < c0) return true;
+        }
+    }
+    return false;
+}
+
+void block_match(const float* a, const float* b, float* flow, int w, int h) {  // flow.rs:551-622
+    if (w < 3 || h < 3) return;
+    OMP_FOR
+    for (int y = 1; y <= h - 2; y++) {
+        float* row = flow + (long)y * w * 2;
+        for (int x = 1; x <= w - 2; x++) {
+            float cur[2] = {row[x * 2], row[x * 2 + 1]};
+            float nb[2] = {row[(x - 1) * 2], row[(x - 1) * 2 + 1]};
+            if (bm_step(a, b, w, h, x, y, cur, nb)) { row[x * 2] = nb[0]; row[x * 2 + 1] = nb[1]; }
+        }
+    }
+    OMP_FOR
+    for (int y = 1; y <= h - 2; y++) {
+        float* row = flow + (long)y * w * 2;
+        for (int x = w - 2; x >= 1; x--) {
+            float cur[2] = {row[x * 2], row[x * 2 + 1]};
+            float nb[2] = {row[(x + 1) * 2], row[(x + 1) * 2 + 1]};
+            if (bm_step(a, b, w, h, x, y, cur, nb)) { row[x * 2] = nb[0]; row[x * 2 + 1] = nb[1]; }
+        }
+    }
+    // the column sweeps run in place on the field; the reference transposes for contiguity only
+    OMP_FOR
+    for (int x = 1; x <= w - 2; x++) {
+        for (int y = 1; y <= h - 2; y++) {
+            float* c = flow + ((long)y * w + x) * 2;
+            float* p = flow + ((long)(y - 1) * w + x) * 2;
+            float cur[2] = {c[0], c[1]};
+            float nb[2] = {p[0], p[1]};
+            if (bm_step(a, b, w, h, x, y, cur, nb)) { c[0] = nb[0]; c[1] = nb[1]; }
+        }
+    }
+    OMP_FOR
+    for (int x = 1; x <= w - 2; x++) {
+        for (int y = h - 2; y >= 1; y--) {
+            float* c = flow + ((long)y * w + x) * 2;
+            float* p = flow + ((long)(y + 1) * w + x) * 2;
+            float cur[2] = {c[0], c[1]};
+            float nb[2] = {p[0], p[1]};
+            if (bm_step(a, b, w, h, x, y, cur, nb)) { c[0] = nb[0]; c[1] = nb[1]; }
+        }
+    }
+}
+
+// flow.rs:1258-1307
+FlowField solve_pyramids(const Pyramid& x, const Pyramid& y, const FlowSettings& s) {
+    const Geometry& geo = x.geo;
+    int levels = geo.levels;
+    int start; float damp;
+    start_level(s.sensitivity, levels, &start, &damp);
+    int sw0 = geo.sizes[start].first, sh0 = geo.sizes[start].second;
+    std::vector<float> flow((size_t)sw0 * sh0 * 2, 0.0f);
+    bool check = true;
+    for (int l = start; l >= 0; l--) {
+        int w = geo.sizes[l].first, h = geo.sizes[l].second;
+        const float* img_a = x.levels[l].d.data();
+        const float* img_b = y.levels[l].d.data();
+        std::vector<float> grad = calc_grad(img_a, w, h);
+        std::vector<float> a = calc_a(grad, w, h);
+        blur_gaussian(a.data(), w, h, 3, 7.0f, s.taps_above_first);
+        for (int it = 0; it < 3; it++) {
+            std::vector<float> b = calc_b(img_a, img_b, grad.data(), flow.data(), w, h);
+            blur_gaussian(b.data(), w, h, 2, 7.0f, s.taps_above_first);
+            new_disp(flow.data(), a.data(), b.data(), (size_t)w * h);
+            blur_gaussian(flow.data(), w, h, 2, 5.0f, s.taps_above_first);
+            if (it == 1 && l == 0 && !s.skip_refine) block_match(img_a, img_b, flow.data(), w, h);
+        }
+        if (l != 0 && !s.skip_refine) block_match(img_a, img_b, flow.data(), w, h);
+        if (check) {
+            if (all_flow_out_of_range(flow.data(), w, h)) std::fill(flow.begin(), flow.end(), 0.0f);
+            else check = false;
+        }
+        if (l == start && std::fabs((double)damp - 1.0) >= 1e-6) scale_values(flow.data(), flow.size(), damp);
+        if (l > 0) {
+            int nw = geo.sizes[l - 1].first, nh = geo.sizes[l - 1].second;
+            flow = upsample_flow(flow.data(), w, h, nw, nh);
+        }
+    }
+    scale_values(flow.data(), flow.size(), -1.0f);
+    FlowField out;
+    out.w = geo.w;
+    out.h = geo.h;
+    out.d = std::move(flow);
+    return out;
+}
+
+bool solve(const Image& x, const Image& y, const FlowSettings& s, FlowField* out, std::string* err) {
+    if (x.w != y.w || x.h != y.h || x.fmt != y.fmt) { *err = "incompatible inputs"; return false; }
+    Pyramid px, py;
+    if (!build_pyramid(x, s, &px, err) || !build_pyramid(y, s, &py, err)) return false;
+    *out = solve_pyramids(px, py, s);
+    return true;
+}
+
+bool solve_pair(const Image& a, const Image& b, const FlowSettings& s, FlowField* f_ab, FlowField* f_ba,
+                std::string* err) {  // flow.rs:1347-1353
+    if (a.w != b.w || a.h != b.h || a.fmt != b.fmt) { *err = "incompatible inputs"; return false; }
+    Pyramid pa, pb;
+    if (!build_pyramid(a, s, &pa, err) || !build_pyramid(b, s, &pb, err)) return false;
+    *f_ba = solve_pyramids(pb, pa, s);
+    *f_ab = solve_pyramids(pa, pb, s);
+    return true;
+}
+
+// =============================================================================================
+// inverse warp (warp.rs)
+
+uint8_t sat_u8(float v) {  // warp.rs:129-135
+    int32_t i = cvtt32(v + 0.5f);
+    int32_t t = (int32_t)((uint32_t)i + (uint32_t)(-128));
+    int32_t wv = std::min(std::max(t, -32768), 32767);
+    int32_t bv = std::min(std::max(wv, -128), 127);
+    return (uint8_t)(bv + 128);
+}
+uint16_t sat_u16(float v) {  // warp.rs:141-146
+    int32_t i = cvtt32(v + 0.5f);
+    int32_t t = (int32_t)((uint32_t)i + (uint32_t)(-32768));
+    int32_t wv = std::min(std::max(t, -32768), 32767);
+    return (uint16_t)(wv + 32768);
+}
+static inline uint8_t scale_u8(uint8_t b, float f) {  // warp.rs:152-155
+    float v = (float)b * f;
+    return (uint8_t)cvtt64d((double)v + 0.5);
+}
+static inline uint16_t scale_u16(uint16_t b, float f) {  // warp.rs:159-162
+    float v = (float)b * f;
+    return (uint16_t)cvtt64d((double)v + 0.5);
+}
+
+bool clip_to_rect(float x, float y, float* ix, float* iy, float w1, float h1) {  // warp.rs:178-215
+    for (int it = 0; it < 4096; it++) {
+        if (*ix < 0.0f) {
+            float dy = y - *iy, dxs = x - *ix, num = x - 0.0f;
+            *ix = 0.0f;
+            *iy = y - (num / dxs) * dy;
+            continue;
+        }
+        if (*ix > w1) {
+            float dy = y - *iy, dxs = x - *ix, num = x - w1;
+            *ix = w1;
+            *iy = y - (num / dxs) * dy;
+            continue;
+        }
+        if (*iy < 0.0f) {
+            float dyy = y - *iy, num = y - 0.0f, dx = x - *ix;
+            *ix = x - (num / dyy) * dx;
+            *iy = 0.0f;
+            continue;
+        }
+        if (*iy > h1) {
+            float dyy = y - *iy, num = y - h1, dx = x - *ix;
+            *ix = x - (num / dyy) * dx;
+            *iy = h1;
+            continue;
+        }
+        return true;
+    }
+    return false;
+}
+
+template <typename P> struct PixT;
+template <> struct PixT<uint8_t> {
+    static float f(uint8_t v) { return (float)v; }
+    static uint8_t store(float v) { return sat_u8(v); }
+    static uint8_t faded(float v, float f) { return scale_u8(sat_u8(v), f); }
+};
+template <> struct PixT<uint16_t> {
+    static float f(uint16_t v) { return (float)v; }
+    static uint16_t store(float v) { return sat_u16(v); }
+    static uint16_t faded(float v, float f) { return scale_u16(sat_u16(v), f); }
+};
+template <> struct PixT<float> {
+    static float f(float v) { return v; }
+    static float store(float v) { return v; }
+    static float faded(float v, float f) { return v * f; }
+};
+
+// warp.rs:290-360 (bilerp4 + mix4 with the NaN rule repeat)
+template <typename P>
+static inline void bilerp4(const P* src, int w, int w1, int h1, float x, float y, float out[4]) {
+    int ix = cvtt32(x), iy = cvtt32(y);
+    float fx = x - (float)ix, fy = y - (float)iy;
+    if (ix >= w1) { ix = w1 - 1; fx = 1.0f; }
+    if (iy >= h1) { iy = h1 - 1; fy = 1.0f; }
+    long i00 = ((long)iy * w + ix) * 4;
+    long i01 = i00 + (long)w * 4;
+    bool any = false;
+    for (int k = 0; k < 4; k++) {
+        float p00 = PixT<P>::f(src[i00 + k]), p10 = PixT<P>::f(src[i00 + 4 + k]);
+        float p01 = PixT<P>::f(src[i01 + k]), p11 = PixT<P>::f(src[i01 + 4 + k]);
+        float top = p00 + (p10 - p00) * fx;
+        float bot = p01 + (p11 - p01) * fx;
+        out[k] = top + (bot - top) * fy;
+        any = any || std::isnan(out[k]);
+    }
+    if (any) {
+        for (int k = 0; k < 4; k++) {
+            float p00 = PixT<P>::f(src[i00 + k]), p10 = PixT<P>::f(src[i00 + 4 + k]);
+            float p01 = PixT<P>::f(src[i01 + k]), p11 = PixT<P>::f(src[i01 + 4 + k]);
+            float top = nr::add(p00, nr::mul(nr::sub(p10, p00), fx));
+            float bot = nr::add(p01, nr::mul(nr::sub(p11, p01), fx));
+            out[k] = nr::add(top, nr::mul(nr::sub(bot, top), fy));
+        }
+    }
+}
+
+// warp.rs:415-442 (Flow::bilerp)
+static inline void flow_bilerp(const float* d, int fw, int fw1, int fh1, float x, float y, float out[2]) {
+    int ix = cvtt32(x), iy = cvtt32(y);
+    float fx = x - (float)ix, fy = y - (float)iy;
+    if (ix >= fw1) { ix = fw1 - 1; fx = 1.0f; }
+    if (iy >= fh1) { iy = fh1 - 1; fy = 1.0f; }
+    long i00 = ((long)iy * fw + ix) * 2;
+    long i01 = i00 + (long)fw * 2;
+    for (int k = 0; k < 2; k++) {
+        float p00 = d[i00 + k], p10 = d[i00 + 2 + k], p01 = d[i01 + k], p11 = d[i01 + 2 + k];
+        float top = (p10 - p00) * fx + p00;
+        float bot = (p11 - p01) * fx + p01;
+        out[k] = (bot - top) * fy + top;
+    }
+}
+
+template <typename P>
+static bool warp_run(P* out, uint8_t* cov, const P* src, const FlowField& flow, float amount, WarpOpts o, int width,
+                     int height) {  // warp.rs:446-651
+    int w1i = width - 1, h1i = height - 1;
+    float rx = (float)(flow.w - 1) / (float)w1i;
+    float ry = (float)(flow.h - 1) / (float)h1i;
+    float sx = amount / rx, sy = amount / ry;
+    float wf = (float)width, hf = (float)height, w1 = (float)w1i, h1 = (float)h1i;
+    int fw1 = flow.w - 1, fh1 = flow.h - 1;
+    bool bad = false;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) reduction(|| : bad)
+#endif
+    for (int y = 0; y < height; y++) {
+        float yf = (float)y;
+        float fy = yf * ry;
+        for (int x = 0; x < width; x++) {
+            float xf = (float)x;
+            float dd[2];
+            flow_bilerp(flow.d.data(), flow.w, fw1, fh1, xf * rx, fy, dd);
+            float ix = dd[0] * sx + xf;
+            float iy = dd[1] * sy + yf;
+            P* px = out + ((long)y * width + x) * 4;
+            if (o.hold) {
+                if (!clip_to_rect(xf, yf, &ix, &iy, w1, h1) || std::isnan(ix) || std::isnan(iy)) {
+                    bad = true;
+                    for (int k = 0; k < 4; k++) px[k] = P(0);
+                    continue;
+                }
+                float s[4];
+                bilerp4(src, width, w1i, h1i, ix, iy, s);
+                for (int k = 0; k < 4; k++) px[k] = PixT<P>::store(s[k]);
+            } else {
+                uint8_t c;
+                if (!(ix > -1.0f && ix < wf && iy > -1.0f && iy < hf)) {
+                    for (int k = 0; k < 4; k++) px[k] = P(0);
+                    c = 0;
+                } else if (ix >= 0.0f && ix <= w1 && iy >= 0.0f && iy <= h1) {
+                    float s[4];
+                    bilerp4(src, width, w1i, h1i, ix, iy, s);
+                    for (int k = 0; k < 4; k++) px[k] = PixT<P>::store(s[k]);
+                    c = 255;
+                } else {
+                    float f = ix < 0.0f ? ix + 1.0f : (ix <= w1 ? 1.0f : wf - ix);
+                    if (iy < 0.0f) f *= iy + 1.0f;
+                    else if (iy > h1) f *= hf - iy;
+                    if (!clip_to_rect(xf, yf, &ix, &iy, w1, h1) || std::isnan(ix) || std::isnan(iy)) {
+                        bad = true;
+                        for (int k = 0; k < 4; k++) px[k] = P(0);
+                        c = 0;
+                    } else {
+                        float s[4];
+                        bilerp4(src, width, w1i, h1i, ix, iy, s);
+                        for (int k = 0; k < 4; k++) px[k] = PixT<P>::faded(s[k], f);
+                        float cc = f * 255.0f + 0.5f;
+                        c = cc <= 255.0f ? (uint8_t)cvtt64d((double)cc) : 255;
+                    }
+                }
+                if (cov) cov[(long)y * width + x] = c;
+            }
+        }
+    }
+    return !bad;
+}
+
+int inv_warp(Image& out, const Image& src, const FlowField& flow, float amount, WarpOpts o, Coverage* cov,
+             std::string* err) {  // warp.rs:693-786
+    if (out.w != src.w || out.h != src.h || out.fmt != src.fmt) { *err = "inverse warp: shape mismatch"; return 1; }
+    if (out.w < 2 || out.h < 2 || flow.w < 2 || flow.h < 2) { *err = "inverse warp: below 2x2"; return 1; }
+    if (cov) { cov->w = out.w; cov->h = out.h; cov->d.assign((size_t)out.w * out.h, 0xff); }
+    int width = out.w, height = out.h;
+    float a = amount < 0.0f ? -amount : amount;
+    bool copy_only = 0.005 > (double)a;
+    if (!copy_only) {
+        float r = (float)(flow.w - 1) / (float)(width - 1);
+        float qq = (float)((double)amount / (double)r);
+        if (qq < 0.0f) qq = -qq;
+        copy_only = 0.0001 > (double)qq;
+    }
+    if (copy_only) { copy_image(out, src); return 0; }
+    if (o.mode != 1) { *err = "inverse warp: mip map sampling"; return 2; }
+    if (o.is360) { *err = "inverse warp: 360 mode is not restated"; return 2; }
+    uint8_t* c = cov ? cov->d.data() : nullptr;
+    bool ok;
+    if (out.fmt == U8) ok = warp_run<uint8_t>(out.u8.data(), c, src.u8.data(), flow, amount, o, width, height);
+    else if (out.fmt == U16) ok = warp_run<uint16_t>(out.u16.data(), c, src.u16.data(), flow, amount, o, width, height);
+    else ok = warp_run<float>(out.f32.data(), c, src.f32.data(), flow, amount, o, width, height);
+    if (!ok) { *err = "inverse warp: a sample coordinate is NaN or never converges"; return 2; }
+    return 0;
+}
+
+// =============================================================================================
+// blend (blend.rs)
+
+void copy_image(Image& out, const Image& src) {  // blend.rs:117-125
+    std::memcpy(out.data(), src.data(), src.bytes());
+}
+
+template <typename T>
+static inline void lerp_pixel_int(T* f, const T* s, float w, float scale) {  // blend.rs:214-249
+    auto diff = [&](int i) { return (float)((int32_t)f[i] - (int32_t)s[i]); };
+    auto sf = [&](int i) { return (float)(int32_t)s[i]; };
+    auto store = [](float v) { return (T)cvtt64f(v); };
+    float a = diff(0) * w + sf(0);
+    float n = a / scale;
+    if (!(n > 0.0f)) { T z = store(0.0f); for (int i = 0; i < 4; i++) f[i] = z; return; }
+    float r = diff(1) * w + sf(1), g = diff(2) * w + sf(2), b = diff(3) * w + sf(3);
+    if (n > 1.0f) { r = r / n; g = g / n; b = b / n; a = scale; }
+    auto clamp = [&](float c) { return c > a ? a : (0.0f > c ? 0.0f : c); };
+    r = clamp(r); g = clamp(g); b = clamp(b);
+    f[1] = store(r + 0.5f);
+    f[2] = store(g + 0.5f);
+    f[3] = store(b + 0.5f);
+    f[0] = store(a + 0.5f);
+}
+
+static inline void lerp_pixel_f32(float* f, const float* s, float w) {  // blend.rs:182-211
+    bool rule = false;
+    for (int i = 0; i < 4; i++) rule = rule || std::isnan(f[i]) || std::isnan(s[i]);
+    if (!rule) {
+        float a = (f[0] - s[0]) * w + s[0];
+        if (!(a > 0.0f)) { for (int i = 0; i < 4; i++) f[i] = 0.0f; return; }
+        float r = (f[1] - s[1]) * w + s[1], g = (f[2] - s[2]) * w + s[2], b = (f[3] - s[3]) * w + s[3];
+        if (a > 1.0f) { r = r / a; g = g / a; b = b / a; a = 1.0f; }
+        f[1] = r + 0.0f; f[2] = g + 0.0f; f[3] = b + 0.0f; f[0] = a + 0.0f;
+    } else {
+        auto L = [](float a, float b, float w) { return nr::add(nr::mul(nr::sub(b, a), w), a); };
+        float a = L(s[0], f[0], w);
+        if (!(a > 0.0f)) { for (int i = 0; i < 4; i++) f[i] = 0.0f; return; }
+        float r = L(s[1], f[1], w), g = L(s[2], f[2], w), b = L(s[3], f[3], w);
+        if (a > 1.0f) { r = nr::div(r, a); g = nr::div(g, a); b = nr::div(b, a); a = 1.0f; }
+        f[1] = nr::add(r, 0.0f); f[2] = nr::add(g, 0.0f); f[3] = nr::add(b, 0.0f); f[0] = nr::add(a, 0.0f);
+    }
+}
+
+void lerp(Image& first, const Image& second, float w) {  // blend.rs:144-179
+    if (w == 1.0f) return;
+    if (w == 0.0f) { copy_image(first, second); return; }
+    long n = (long)first.w * first.h;
+    if (first.fmt == U8) {
+        OMP_FOR
+        for (long i = 0; i < n; i++) lerp_pixel_int<uint8_t>(&first.u8[i * 4], &second.u8[i * 4], w, 255.0f);
+    } else if (first.fmt == U16) {
+        OMP_FOR
+        for (long i = 0; i < n; i++) lerp_pixel_int<uint16_t>(&first.u16[i * 4], &second.u16[i * 4], w, 65535.0f);
+    } else {
+        OMP_FOR
+        for (long i = 0; i < n; i++) lerp_pixel_f32(&first.f32[i * 4], &second.f32[i * 4], w);
+    }
+}
+
+void blend(Image& out, const Image& a, const Image& b, float w) {  // blend.rs:55-114
+    const double SNAP = 0.005;
+    if (SNAP > (double)std::fabs(w)) { copy_image(out, a); return; }
+    if (SNAP > std::fabs((double)w - 1.0)) { copy_image(out, b); return; }
+    if (w < 0.0f || w > 1.0f) {
+        copy_image(out, a);
+        lerp(out, b, (float)(1.0 - (double)w));
+        return;
+    }
+    long n = (long)out.w * out.h * 4;
+    if (out.fmt == U8) {
+        OMP_FOR
+        for (long i = 0; i < n; i++) {
+            float af = (float)a.u8[i], bf = (float)b.u8[i];
+            out.u8[i] = (uint8_t)cvtt64f((bf - af) * w + af + 0.5f);
+        }
+    } else if (out.fmt == U16) {
+        OMP_FOR
+        for (long i = 0; i < n; i++) {
+            float af = (float)a.u16[i], bf = (float)b.u16[i];
+            out.u16[i] = (uint16_t)cvtt64f((bf - af) * w + af + 0.5f);
+        }
+    } else {
+        long row = (long)out.w * 4;
+        OMP_FOR
+        for (int y = 0; y < out.h; y++) {
+            bool any = false;
+            for (long i = y * row; i < (y + 1) * row; i++) {
+                out.f32[i] = (b.f32[i] - a.f32[i]) * w + a.f32[i] + 0.0f;
+                any = any || std::isnan(out.f32[i]);
+            }
+            if (any)
+                for (long i = y * row; i < (y + 1) * row; i++)
+                    out.f32[i] = nr::add(nr::add(nr::mul(nr::sub(b.f32[i], a.f32[i]), w), a.f32[i]), 0.0f);
+        }
+    }
+}
+
+// =============================================================================================
+// composition (compose/vector.rs:209-284, compose.rs:218-231)
+
+bool nearest_uses_f_ab(float wa, int code) {  // compose/vector.rs:61-64
+    unsigned c = (unsigned)code;
+    return (wa < 0.5f && c < 2) || (0.5f <= wa && c > 1);
+}
+
+int compose_vectors(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b,
+                    const FlowField* f_ab, const FlowField* f_ba, Image* out, std::string* err) {
+    if (cs.warp_mode != 0) { *err = "compose: only warping code 0 is restated here"; return 2; }
+    if (cs.blur > 0.005f && std::fabs(sel.s0 - sel.s1) > 1e-6f) { *err = "blur compensation is not restated"; return 2; }
+    float wa = sel.wa;
+    float frac = 1.0f - wa;
+    WarpOpts o;
+    *out = Image(a.w, a.h, a.fmt);
+    if (sel.interp == 0) {
+        const FlowField* flow = nearest_uses_f_ab(wa, cs.warp_mode) ? f_ab : f_ba;
+        if (!flow) { *err = "missing flow"; return 1; }
+        if (0.5f <= wa) return inv_warp(*out, a, *flow, frac, o, nullptr, err);
+        return inv_warp(*out, b, *flow, wa, o, nullptr, err);
+    }
+    if (sel.interp == 1) {
+        if (!f_ab || !f_ba) { *err = "missing flow"; return 1; }
+        Image ta(a.w, a.h, a.fmt), tb(b.w, b.h, b.fmt);
+        int rc = inv_warp(ta, a, *f_ba, frac, o, nullptr, err);
+        if (rc) return rc;
+        rc = inv_warp(tb, b, *f_ab, wa, o, nullptr, err);
+        if (rc) return rc;
+        blend(*out, ta, tb, frac);
+        return 0;
+    }
+    *err = "compose: interpolation mode not restated";
+    return 2;
+}
+
+int interpolate(const Selection& sel, const Image& a, const Image& b, Image* out, std::string* err) {
+    *out = Image(a.w, a.h, a.fmt);
+    if (sel.interp == 0) { copy_image(*out, sel.wa >= 0.5f ? a : b); return 0; }
+    if (sel.interp == 1) { blend(*out, a, b, (float)(1.0 - (double)sel.wa)); return 0; }
+    if (sel.interp == 2) {
+        // blend.rs:281-302: Weighted Blend without flows equals the plain Blend with weight 1 - wa
+        // for 8 and 16 bpc, and for float data whose samples are finite and at most 1e30
+        if (a.fmt == F32) {
+            for (float v : a.f32) if (!(std::fabs(v) <= 1.0e30f)) { *err = "weighted blend of unsound floats"; return 2; }
+            for (float v : b.f32) if (!(std::fabs(v) <= 1.0e30f)) { *err = "weighted blend of unsound floats"; return 2; }
+            Image a1 = a, b1 = b;
+            for (auto& v : a1.f32) v = v + 0.0f;
+            for (auto& v : b1.f32) v = v + 0.0f;
+            blend(*out, a1, b1, 1.0f - sel.wa);
+            return 0;
+        }
+        blend(*out, a, b, 1.0f - sel.wa);
+        return 0;
+    }
+    *err = "bad interpolation mode";
+    return 1;
+}
+
+}  // namespace orc

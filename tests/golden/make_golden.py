@@ -1,0 +1,105 @@
+"""Builds the committed golden fixtures of the parity tests from the reference tree.
+
+Run in a container that has the reference mounted (default /root/reference):
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+Writes, next to this script:
+
+* ``retime_flow_grid.npz`` - the cases of the reference's parity grid
+  ``parity/retime-flow`` that the hot path serves (warping code 0, Nearest or Blend, no prep, no
+  360 video, no smart blend, no blur compensation), their raw input clips as
+  ``parity/retime-flow/gen.py`` regenerates them (numpy, fixed seeds), and the sha256 of the
+  output clip that ``parity/retime-flow/results/base.grid.tsv`` records for each. That table was
+  recorded by the reference revision whose motion path ran on top-down rows with the vertical
+  border taps below first; the tests run the oracle and the CUDA path in that variant
+  (``rows_reversed=False, taps_above_first=False``) for these cases.
+* ``warp_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/warp_cases.hex``
+  (the reference's bit-exact numpy model of the inverse warp; format in its ``gen_warp.py``).
+
+Nothing under ``tests/`` reads the reference tree at test time; only this script does.
+"""
+import argparse
+import gzip
+import hashlib
+import importlib.util
+import io
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+SERVED = {"vectors", "frame_interp", "sensitivity", "blur_compensation", "smart_blend"}
+
+
+def load_gen(ref):
+    path = os.path.join(ref, "parity", "retime-flow", "gen.py")
+    spec = importlib.util.spec_from_file_location("rf_gen", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def served(case):
+    params = dict(p.split("=", 1) for p in case["params"])
+    params.pop("speed_percent")
+    if any(k not in SERVED for k in params):
+        return False
+    if params.get("smart_blend", "0") != "0":
+        return False
+    if params.get("frame_interp", "2") not in ("1", "2"):
+        # Weighted Blend (3) is served on the fast path only, which the case's own frames decide;
+        # keep those cases out of the fixture set
+        return False
+    if float(params.get("blur_compensation", "0")) > 0.005:
+        return False
+    return True
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    ref = args.reference
+    gen = load_gen(ref)
+    with tempfile.TemporaryDirectory() as tmp:
+        builder = gen.Builder()
+        gen.build_grid(builder)
+        table = {}
+        for line in open(os.path.join(ref, "parity", "retime-flow", "results", "base.grid.tsv")):
+            parts = line.rstrip("\n").split("\t")
+            if parts[0] != "id":
+                table[parts[0]] = (parts[1], parts[3])
+        cases, inputs = [], {}
+        for c in builder.cases:
+            if not served(c) or table[c["id"]][0] != "0":
+                continue
+            inp = builder.inputs[c["input"]]
+            key = c["input"]
+            if key not in inputs:
+                frames = [gen.frame_raw(inp["source"], inp["width"], inp["height"], t, inp["depth"])
+                          for t in range(inp["frames"])]
+                inputs[key] = np.frombuffer(b"".join(frames), np.uint8)
+            cases.append(dict(id=c["id"], params=c["params"], depth=c["depth"], width=c["width"],
+                              height=c["height"], frames=c["frames"], fps=c["fps"], input=key,
+                              sha256=table[c["id"]][1]))
+        keys = sorted(inputs)
+        arrays = {f"input_{i}": inputs[k] for i, k in enumerate(keys)}
+        meta = dict(inputs=keys, cases=cases)
+        arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), np.uint8)
+        np.savez_compressed(os.path.join(HERE, "retime_flow_grid.npz"), **arrays)
+        print(f"retime_flow_grid.npz: {len(cases)} cases, {len(keys)} input clips")
+
+    txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "warp_cases.hex")).read()
+    blob = bytes.fromhex("".join(txt.split()))
+    with gzip.open(os.path.join(HERE, "warp_cases.bin.gz"), "wb") as f:
+        f.write(blob)
+    print(f"warp_cases.bin.gz: {len(blob)} bytes, sha256 {hashlib.sha256(blob).hexdigest()}")
+
+
+if __name__ == "__main__":
+    sys.exit(main())

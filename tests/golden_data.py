@@ -1,0 +1,80 @@
+"""Readers of the committed golden fixtures (see tests/golden/make_golden.py)."""
+import gzip
+import json
+import os
+import struct
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+DT = {0: np.uint8, 1: np.uint16, 2: np.float32}
+FMT_OF_DEPTH = {8: 0, 16: 1, 32: 2}
+
+
+def grid():
+    """(meta cases, {input name: raw bytes as uint8})."""
+    z = np.load(os.path.join(GOLDEN, "retime_flow_grid.npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    inputs = {name: z[f"input_{i}"] for i, name in enumerate(meta["inputs"])}
+    return meta["cases"], inputs
+
+
+def case_params(case):
+    """Keyword arguments of oracle_lib.retime_params for a grid case (grid variant of the orders)."""
+    params = dict(p.split("=", 1) for p in case["params"])
+    sp = params.pop("speed_percent")
+    keys, speed = None, 100.0
+    if "@" in sp:
+        keys = []
+        for k in sp.split(";"):
+            v, f = k.split("@")
+            keys.append((float(f.rstrip("e")), float(v), f.endswith("e")))
+    else:
+        speed = float(sp)
+    fps = case["fps"]
+    fpsp = tuple(int(x) for x in fps.split("/")) if "/" in fps else (int(fps), 1)
+    return dict(fps=fpsp, speed=speed, keys=keys, vectors=int(params.get("vectors", 5)),
+                frame_interp=int(params.get("frame_interp", 2)), sensitivity=float(params.get("sensitivity", 70)),
+                blur=float(params.get("blur_compensation", 0)), rows_reversed=False, taps_above_first=False)
+
+
+def warp_cases():
+    """The reference's inverse warp fixtures: list of dicts (src, flow, expected out and coverage)."""
+    blob = gzip.open(os.path.join(GOLDEN, "warp_cases.bin.gz")).read()
+    assert blob[:4] == b"WRP1"
+    p = 4
+
+    def u32():
+        nonlocal p
+        v = struct.unpack_from("<I", blob, p)[0]
+        p += 4
+        return v
+
+    def f32():
+        nonlocal p
+        v = struct.unpack_from("<f", blob, p)[0]
+        p += 4
+        return np.float32(v)
+
+    def take(n):
+        nonlocal p
+        v = blob[p:p + n]
+        p += n
+        return v
+
+    out = []
+    for _ in range(u32()):
+        depth = u32()
+        w, h, fw, fh = u32(), u32(), u32(), u32()
+        amount = f32()
+        flags = u32()
+        dt = DT[depth]
+        es = np.dtype(dt).itemsize
+        src = np.frombuffer(take(w * h * 4 * es), dt).copy()
+        flow = np.frombuffer(take(fw * fh * 8), np.float32).copy()
+        exp = np.frombuffer(take(w * h * 4 * es), dt).copy()
+        cov = np.frombuffer(take(w * h), np.uint8).copy() if flags & 4 else None
+        out.append(dict(fmt=depth, w=w, h=h, fw=fw, fh=fh, amount=amount, hold=bool(flags & 1),
+                        is360=bool(flags & 2), want_cov=bool(flags & 4), src=src, flow=flow, out=exp, cov=cov))
+    assert p == len(blob)
+    return out

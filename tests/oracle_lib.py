@@ -1,0 +1,195 @@
+"""ctypes bindings of the CPU oracle (oracle/liboracle.so).
+
+The oracle is the checker of the parity tests: a C++ restatement of the reference CPU engine
+(baairon/twixtor, plugins/retime-engine). It is test infrastructure; the product library never
+links or calls it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+
+FMT = {"u8": 0, "u16": 1, "f32": 2}
+DTYPE = {0: np.uint8, 1: np.uint16, 2: np.float32}
+
+
+class RetimeParams(ctypes.Structure):
+    _fields_ = [
+        ("fps_num", ctypes.c_int),
+        ("fps_den", ctypes.c_int),
+        ("quality_high", ctypes.c_int),
+        ("speed_percent", ctypes.c_double),
+        ("nkeys", ctypes.c_int),
+        ("key_frames", ctypes.POINTER(ctypes.c_double)),
+        ("key_values", ctypes.POINTER(ctypes.c_double)),
+        ("key_ease", ctypes.POINTER(ctypes.c_int)),
+        ("vectors", ctypes.c_int),
+        ("frame_interp", ctypes.c_int),
+        ("smart_blend", ctypes.c_int),
+        ("sensitivity", ctypes.c_double),
+        ("blur_compensation", ctypes.c_double),
+        ("rows_reversed", ctypes.c_int),
+        ("taps_above_first", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def build():
+    """Compiles the oracle with its Makefile (g++ from PATH; no fast math, no FMA contraction)."""
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True, env=env)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = ctypes.CDLL(ORACLE_SO)
+        P = ctypes.c_void_p
+        i, f = ctypes.c_int, ctypes.c_float
+        L.or_last_error.restype = ctypes.c_char_p
+        L.or_gaussian_kernel.argtypes = [f, P, i]
+        L.or_start_level.argtypes = [f, i, P, P]
+        L.or_block_cost.argtypes = [P, i, i, P, f, f, P]
+        L.or_block_cost.restype = f
+        L.or_convolve.argtypes = [P, i, i, i, P, i, i]
+        L.or_calc_grad.argtypes = [P, i, i, P]
+        L.or_new_disp.argtypes = [P, P, P, ctypes.c_long]
+        L.or_upsample_flow.argtypes = [P, i, i, i, i, P]
+        L.or_block_match.argtypes = [P, P, P, i, i]
+        L.or_all_out_of_range.argtypes = [P, i, i]
+        L.or_geometry.argtypes = [i, i, i, i, P, P, i]
+        L.or_build_pyramid.argtypes = [P, i, i, i, i, i, f, i, P]
+        L.or_solve_pair.argtypes = [P, P, i, i, i, i, i, f, i, i, P, P]
+        L.or_inv_warp.argtypes = [P, P, i, i, i, P, i, i, f, i, P]
+        L.or_blend.argtypes = [P, P, P, i, i, i, f]
+        L.or_compose_vectors.argtypes = [P, P, i, i, i, P, P, i, i, f, i, P]
+        L.or_from_frame.argtypes = [P, i, i, i, P]
+        L.or_to_frame.argtypes = [P, i, i, i, P]
+        L.or_select.argtypes = [ctypes.POINTER(RetimeParams), i, i, i, P, P, P, P, P, P, P]
+        L.or_retime_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
+        L.or_set_threads.argtypes = [i]
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def err():
+    return lib().or_last_error().decode()
+
+
+def geometry(quality, hiq, w, h):
+    red = ctypes.c_int()
+    sizes = np.zeros(64, np.int32)
+    n = lib().or_geometry(quality, int(hiq), w, h, ctypes.byref(red), ptr(sizes), 32)
+    if n < 0:
+        raise ValueError(err())
+    return red.value, [(int(sizes[2 * i]), int(sizes[2 * i + 1])) for i in range(n)]
+
+
+def from_frame(wire, w, h, fmt):
+    out = np.zeros(w * h * 4, DTYPE[fmt])
+    lib().or_from_frame(ptr(wire), w, h, fmt, ptr(out))
+    return out
+
+
+def to_frame(engine, w, h, fmt):
+    out = np.zeros(w * h * 4, DTYPE[fmt])
+    lib().or_to_frame(ptr(engine), w, h, fmt, ptr(out))
+    return out
+
+
+def build_pyramid(engine, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, above_first=True):
+    _, sizes = geometry(quality, hiq, w, h)
+    total = sum(a * b for a, b in sizes)
+    out = np.zeros(total, np.float32)
+    n = lib().or_build_pyramid(ptr(engine), w, h, fmt, quality, int(hiq), sensitivity, int(above_first), ptr(out))
+    if n < 0:
+        raise ValueError(err())
+    levels, off = [], 0
+    for lw, lh in sizes:
+        levels.append(out[off:off + lw * lh].reshape(lh, lw))
+        off += lw * lh
+    return levels
+
+
+def solve_pair(a, b, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, skip_refine=False, above_first=True):
+    _, sizes = geometry(quality, hiq, w, h)
+    fw, fh = sizes[0]
+    f_ab = np.zeros(fw * fh * 2, np.float32)
+    f_ba = np.zeros(fw * fh * 2, np.float32)
+    rc = lib().or_solve_pair(ptr(a), ptr(b), w, h, fmt, quality, int(hiq), sensitivity, int(skip_refine),
+                             int(above_first), ptr(f_ab), ptr(f_ba))
+    if rc:
+        raise ValueError(err())
+    return f_ab, f_ba, (fw, fh)
+
+
+def inv_warp(src, w, h, fmt, flow, fw, fh, amount, hold=True, coverage=False, out=None):
+    o = np.zeros_like(src) if out is None else out.copy()
+    cov = np.zeros(w * h, np.uint8) if coverage else None
+    rc = lib().or_inv_warp(ptr(o), ptr(src), w, h, fmt, ptr(flow), fw, fh, amount, int(hold), ptr(cov))
+    if rc:
+        raise ValueError(err())
+    return (o, cov) if coverage else o
+
+
+def compose_vectors(a, b, w, h, fmt, f_ab, f_ba, fw, fh, wa, interp=1):
+    out = np.zeros_like(a)
+    rc = lib().or_compose_vectors(ptr(a), ptr(b), w, h, fmt, ptr(f_ab), ptr(f_ba), fw, fh, wa, interp, ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out
+
+
+def retime_params(fps=(24, 1), quality_high=True, speed=100.0, keys=None, vectors=5, frame_interp=2, smart_blend=0,
+                  sensitivity=70.0, blur=0.0, rows_reversed=True, taps_above_first=True):
+    """The `retime` parameters of one render. rows_reversed / taps_above_first at their defaults
+    are the reference's current code; both False is the revision the parity grid records."""
+    p = RetimeParams()
+    p.rows_reversed, p.taps_above_first = int(rows_reversed), int(taps_above_first)
+    p.fps_num, p.fps_den = fps
+    p.quality_high = int(quality_high)
+    p.speed_percent = speed
+    p.vectors, p.frame_interp, p.smart_blend = vectors, frame_interp, smart_blend
+    p.sensitivity, p.blur_compensation = sensitivity, blur
+    p.nkeys = 0
+    if keys:
+        fr = (ctypes.c_double * len(keys))(*[k[0] for k in keys])
+        va = (ctypes.c_double * len(keys))(*[k[1] for k in keys])
+        ea = (ctypes.c_int * len(keys))(*[int(k[2]) for k in keys])
+        p.nkeys = len(keys)
+        p.key_frames = ctypes.cast(fr, ctypes.POINTER(ctypes.c_double))
+        p.key_values = ctypes.cast(va, ctypes.POINTER(ctypes.c_double))
+        p.key_ease = ctypes.cast(ea, ctypes.POINTER(ctypes.c_int))
+        p._keep = (fr, va, ea)
+    return p
+
+
+def select(params, n, w, h):
+    s0, s1, wa = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+    a, ex, vq, it = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    lib().or_select(ctypes.byref(params), n, w, h, ctypes.byref(s0), ctypes.byref(s1), ctypes.byref(a),
+                    ctypes.byref(wa), ctypes.byref(ex), ctypes.byref(vq), ctypes.byref(it))
+    return dict(s0=s0.value, s1=s1.value, a=a.value, wa=wa.value, exact=bool(ex.value), vq=vq.value,
+                interp=it.value)
+
+
+def retime_clip(frames, nframes, w, h, fmt, params, nout):
+    out = np.zeros(nout * w * h * 4, DTYPE[fmt])
+    rc = lib().or_retime_clip(ptr(frames), nframes, w, h, fmt, ctypes.byref(params), nout, ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out
