@@ -1,0 +1,219 @@
+/*
+ * twixtor_b200: the retime hot path of baairon/twixtor (plugins/retime-engine) as sm_100a CUDA
+ * behind a C ABI.
+ *
+ * Conventions
+ *   - Images are engine images: 4 channels interleaved in the order A, R, G, B, colour
+ *     PREMULTIPLIED by alpha, rows tightly packed, top row first; 8 bpc (uint8), 16 bpc (uint16,
+ *     full range 0..65535) or 32 bpc (float, white 1.0). This is `image::Image`
+ *     (plugins/retime-engine/src/image.rs:17-73).
+ *   - Wire frames are the host's frames (crates/fx-core/src/frame.rs:79-131): 8 bpc RGBA
+ *     interleaved, 16 bpc RGBA little endian interleaved (range 0..65535), 32 bpc planar in the
+ *     plane order G, B, R, A.
+ *   - Flows are `flow::FlowField` (flow.rs:37-76): width * height * 2 floats, (dx, dy) interleaved,
+ *     at the working resolution of the estimator.
+ *   - The caller owns every host buffer it passes; the library owns the device memory and the
+ *     CUDA context state. Every call is synchronous at the ABI. One tw_ctx may be used from one
+ *     thread at a time (the reference's device backend serialises its queue behind a mutex,
+ *     device/exec/backend.rs:121-181; tw_ctx holds a mutex too).
+ *   - Every call returns a tw_status; TW_OK is 0. tw_last_error() names the cause of the last
+ *     failure on the context. Nothing is ever computed on the CPU: a stage the device cannot
+ *     serve returns TW_ERR_UNSUPPORTED and the caller decides (the reference's executor reruns
+ *     the CPU stage, device/exec/mod.rs:332-369).
+ *
+ * Strict mode: every kernel repeats the reference CPU engine's single precision operation order
+ * with no FMA contraction, IEEE division, x86 truncating conversions and the reference's double
+ * precision steps, so flows and output frames are bit identical to the CPU path on identical
+ * inputs (finite inputs; a NaN anywhere in a solved flow returns TW_ERR_NAN_OUTPUT, as the
+ * reference device path's download does, device/solver/mod.rs:575).
+ */
+#ifndef TWIXTOR_B200_H
+#define TWIXTOR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; map 1:1 onto the reference's `StageError` (device/image.rs:14-23): Cl -> TW_ERR_CUDA,
+ * NanOutput -> TW_ERR_NAN_OUTPUT, Unsupported -> TW_ERR_UNSUPPORTED; TW_ERR_MISMATCH and
+ * TW_ERR_BAD_PARAM are the CPU functions' FxError::Mismatch and FxError::BadParam. */
+typedef enum tw_status {
+    TW_OK = 0,
+    TW_ERR_CUDA = 1,
+    TW_ERR_NAN_OUTPUT = 2,
+    TW_ERR_UNSUPPORTED = 3,
+    TW_ERR_MISMATCH = 4,
+    TW_ERR_BAD_PARAM = 5,
+    TW_ERR_DEVICE_BOUND = 6 /* a data-dependent device loop reached its bound (never for finite data) */
+} tw_status;
+
+typedef enum tw_fmt { TW_U8 = 0, TW_U16 = 1, TW_F32 = 2 } tw_fmt;
+
+typedef struct tw_ctx tw_ctx;
+
+/* An engine image (image.rs:66-71). `data` holds width * height * 4 samples of `fmt`. */
+typedef struct tw_image {
+    int32_t width, height, fmt;
+    const void* data;
+} tw_image;
+
+typedef struct tw_image_mut {
+    int32_t width, height, fmt;
+    void* data;
+} tw_image_mut;
+
+/* flow::FlowField (flow.rs:37-76). */
+typedef struct tw_flow {
+    int32_t width, height;
+    float* data;
+} tw_flow;
+
+/* flow::FlowSettings (flow.rs:83-123), plus the vertical tap order of the solver's separable
+ * filters: 1 = the tap above first (flow/conv.rs:598-615, the reference's order); 0 = below
+ * first (the order of the reference revision its parity grid records). */
+typedef struct tw_flow_settings {
+    int32_t quality;          /* 1..5 */
+    int32_t hiq;              /* high quality render */
+    float sensitivity;        /* slider / 100 */
+    int32_t prep_contrast_edge;
+    int32_t prep_delinearize;
+    int32_t track_alpha;
+    int32_t video_range_luma;
+    int32_t skip_refine;
+    int32_t wrap;             /* 360 solve: TW_ERR_UNSUPPORTED */
+    int32_t taps_above_first;
+} tw_flow_settings;
+
+/* timeline::Selection (timeline.rs:391-414). */
+typedef struct tw_selection {
+    float s0, s1;
+    int32_t a, b;
+    float wa;
+    int32_t exact;
+    int32_t vectors_quality;
+    int32_t interp;           /* 0 Nearest, 1 Blend, 2 Weighted Blend */
+} tw_selection;
+
+/* The part of host::EngineSettings (host.rs:20-100) that compose_vectors reads. */
+typedef struct tw_engine_settings {
+    int32_t warp_mode;        /* 0 inverse, 1 Smart Blend, 2 forward + fill, 3 forward */
+    int32_t video_360;        /* "360 Video" checkbox */
+    int32_t wrap_360;         /* engine wrap-around flag */
+    int32_t quality_high;
+    float blur;               /* Blur Compensation slider */
+    int32_t taps_above_first; /* Stages::vertical_taps() of the stage set (stages.rs:66-70) */
+} tw_engine_settings;
+
+/* Everything one output frame of the `retime` effect needs beyond its selection: the flow
+ * settings, the compose settings and the row order of the motion path
+ * (EngineSettings::motion_rows_reversed, host.rs; plugin 01 sets it, plugins/retime/src/glue.rs:39-40). */
+typedef struct tw_retime_settings {
+    tw_flow_settings flow;
+    tw_engine_settings compose;
+    int32_t motion_rows_reversed;
+} tw_retime_settings;
+
+/* ---- context ------------------------------------------------------------------------------ */
+
+/* Opens device `device` (the reference's `--device gpu=N` open, device/exec/open.rs:72-116).
+ * Runs a small self check of the strict conversions on the device before returning. */
+int tw_open(int device, tw_ctx** out);
+void tw_close(tw_ctx* ctx);
+/* Copies the message of the last failure into buf (NUL terminated); returns its full length. */
+size_t tw_last_error(const tw_ctx* ctx, char* buf, size_t cap);
+/* Per-stage counters: launches of the library's kernels since open, and device bytes held. */
+int tw_stats(const tw_ctx* ctx, uint64_t* kernel_launches, uint64_t* device_bytes);
+
+/* ---- the Stages / Backend seam (stages.rs:33-71, device/exec/backend.rs:27-46) --------------- */
+
+/* Working geometry of a solve (FlowSettings::geometry, flow.rs:129-151): the flow size and the
+ * level count; sizes receives (w, h) per level, finest first, up to cap levels. */
+int tw_flow_geometry(const tw_flow_settings* s, int32_t width, int32_t height, int32_t* flow_w, int32_t* flow_h,
+                     int32_t* levels, int32_t* sizes, int32_t cap);
+
+/* flow::solve (flow.rs:1328-1332): X(p) ~ Y(p + out(p)); `out` has the working size. Replaces
+ * Backend::solve (device/exec/backend.rs:29). */
+int tw_solve(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_flow_settings* s, tw_flow* out);
+
+/* flow::solve_pair (flow.rs:1347-1353): f_ab = solve(A, B), f_ba = solve(B, A), the pyramids built
+ * once. Replaces Backend::solve_pair (device/exec/backend.rs:31). */
+int tw_solve_pair(tw_ctx* ctx, const tw_image* a, const tw_image* b, const tw_flow_settings* s, tw_flow* f_ab,
+                  tw_flow* f_ba);
+
+/* compose::compose_vectors (compose/vector.rs:209-284): the warps, the composition and the blur
+ * compensation tail of one vector frame. f_ab / f_ba may be NULL where the interpolation mode
+ * does not read them. Replaces Backend::compose_vectors (device/exec/backend.rs:39). */
+int tw_compose_vectors(tw_ctx* ctx, const tw_engine_settings* settings, const tw_selection* sel, const tw_image* a,
+                       const tw_image* b, const tw_flow* f_ab, const tw_flow* f_ba, tw_image_mut* out);
+
+/* ---- single stages, for callers that drive the engine step by step ------------------------ */
+
+/* flow::build_pyramid (flow.rs:242-275): the band pass levels, concatenated finest first
+ * (sum of w*h floats over the levels). */
+int tw_build_pyramid(tw_ctx* ctx, const tw_image* img, const tw_flow_settings* s, float* levels_out);
+
+/* flow::block_match (flow.rs:551-622): the four in-place sweeps over a level; a and b are the
+ * band pass planes of X and Y (w*h floats), flow is interleaved (w*h*2 floats), updated in place. */
+int tw_block_match(tw_ctx* ctx, const float* a, const float* b, float* flow, int32_t width, int32_t height);
+
+/* warp::inv_warp / inv_warp_coverage (warp.rs:693-786) with mode 1 and is360 off; cov may be NULL
+ * (no coverage image) or width*height bytes. */
+int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_flow* flow, float amount, int32_t hold,
+                uint8_t* cov);
+
+/* blend::blend (blend.rs:55-114). */
+int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* b, float w);
+
+/* image::Image::from_frame / to_frame (image.rs:178-245): wire frame <-> engine image. */
+int tw_from_frame(tw_ctx* ctx, const void* wire, int32_t width, int32_t height, int32_t fmt, void* engine_out);
+int tw_to_frame(tw_ctx* ctx, const void* engine, int32_t width, int32_t height, int32_t fmt, void* wire_out);
+
+/* ---- the time model of the `retime` effect (host scalars) ---------------------------------- */
+
+/* The parameters the Speed time map and the frame selection read (plugins/retime/src/lib.rs:59-99
+ * as frontend::read_settings reads them, frontend.rs:184-244). Popups carry their raw 1-based
+ * values. The speed curve is constant (nkeys == 0) or keyed at frame numbers, linear between keys
+ * or eased where a key's ease flag is set (crates/fx-core/src/curves.rs:348-375, :537-544).
+ * "In FPS is Out FPS" and Src Time Offset are at their defaults (on, 0). */
+typedef struct tw_time_params {
+    int32_t fps_num, fps_den;  /* the host's frame rate; integer rates get 100 ticks a frame */
+    double speed_percent;
+    int32_t nkeys;
+    const double* key_frames;
+    const double* key_values;
+    const int32_t* key_ease;
+    int32_t vectors;           /* Motion Vectors popup 1..5 */
+    int32_t frame_interp;      /* Frame Interp popup 1..3 */
+    double blur_compensation;
+} tw_time_params;
+
+/* The selection of output frame n of a clip of width x height (timeline::select, timeline.rs:
+ * 451-469, with RemapTimeMap::src_pos :266-331 and the tiny-frame rule prep.rs:111-117). */
+int tw_select(const tw_time_params* p, int32_t n, int32_t width, int32_t height, tw_selection* out);
+
+/* ---- whole output frames ------------------------------------------------------------------ */
+
+/* One output frame of the `retime` effect's core (compose.rs:93-101 with vector_path,
+ * compose/vector.rs:289-321, then the finish, frontend.rs:273-276): wire frames A and B of the
+ * selection in, the output wire frame out. Runs the vector path when sel->vectors_quality != 0
+ * and !sel->exact, else the fast path (compose.rs:218-231). A and B are the frames the host
+ * fetched for sel->a and sel->b (a blank frame for one outside the clip). */
+int tw_retime_frame(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection* sel, const void* wire_a,
+                    const void* wire_b, int32_t width, int32_t height, int32_t fmt, void* wire_out);
+
+/* The same over a clip resident in device memory: `frames` holds nframes wire frames back to
+ * back, `sels` nout selections; output frame k goes to out + k * frame_bytes. Source frames
+ * outside the clip are blank. All pointers are device pointers; the call enqueues on the
+ * context's stream and returns after it completes. */
+int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
+                          const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt,
+                          void* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TWIXTOR_B200_H */

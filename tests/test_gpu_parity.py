@@ -1,0 +1,241 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle, bit for bit.
+
+Every comparison is on bytes: flows as float bits, frames as samples. Inputs are seeded; the
+oracle is the pinned CPU restatement of the reference (tests/test_oracle_pins.py). The end to end
+cases of the reference's parity grid are checked against its recorded sha256 directly.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+import golden_data
+import oracle_lib as O
+import twixtor_b200 as tw
+from twixtor_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    tw.build()
+    d = tw.Device(0)
+    yield d
+    d.close()
+
+
+def same(a, b):
+    return np.asarray(a).view(np.uint8).tobytes() == np.asarray(b).view(np.uint8).tobytes()
+
+
+def rand_engine(rng, w, h, fmt):
+    """A random premultiplied engine image through the oracle's own from_frame."""
+    if fmt == 0:
+        wire = rng.randint(0, 256, w * h * 4).astype(np.uint8)
+    elif fmt == 1:
+        wire = rng.randint(0, 65536, w * h * 4).astype(np.uint16)
+    else:
+        wire = rng.random_sample(w * h * 4).astype(np.float32)
+    return O.from_frame(wire, w, h, fmt), wire
+
+
+# ---- image boundary ------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+def test_from_and_to_frame(dev, fmt):
+    rng = np.random.RandomState(11 + fmt)
+    w, h = 37, 23
+    eng, wire = rand_engine(rng, w, h, fmt)
+    assert same(dev.from_frame(wire, w, h, fmt), eng)
+    # to_frame of arbitrary engine samples (alpha 0 and above-alpha colours included)
+    if fmt == 2:
+        e = (rng.random_sample(w * h * 4) * 1.5 - 0.1).astype(np.float32)
+    else:
+        e = rng.randint(0, 256 if fmt == 0 else 65536, w * h * 4).astype(tw.DTYPES[fmt])
+        e[::16] = 0
+    assert same(dev.to_frame(e, w, h, fmt), O.to_frame(e, w, h, fmt))
+
+
+# ---- warps and blends ------------------------------------------------------------------------------
+
+WARP = golden_data.warp_cases()
+
+
+@pytest.mark.parametrize("i", [i for i, c in enumerate(WARP) if not c["is360"]])
+def test_inverse_warp_reference_fixtures(dev, i):
+    c = WARP[i]
+    r = dev.inv_warp(c["src"], c["w"], c["h"], c["fmt"], c["flow"], (c["fw"], c["fh"]), c["amount"], hold=c["hold"],
+                     coverage=c["want_cov"])
+    out, cov = r if c["want_cov"] else (r, None)
+    assert same(out, c["out"])
+    if c["want_cov"]:
+        assert (cov == c["cov"]).all()
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("w", [0.0, 0.003, 0.25, 0.5, 0.9971, 1.0, -0.4, 1.3])
+def test_blend_all_branches(dev, fmt, w):
+    rng = np.random.RandomState(5)
+    W, H = 19, 13
+    a, _ = rand_engine(rng, W, H, fmt)
+    b, _ = rand_engine(rng, W, H, fmt)
+    want = np.zeros_like(a)
+    O.lib().or_blend(O.ptr(want), O.ptr(a), O.ptr(b), W, H, fmt, np.float32(w))
+    assert same(dev.blend(a, b, W, H, fmt, w), want)
+
+
+# ---- pyramid and solver ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("size", [(160, 96), (33, 31), (7, 9), (2, 2), (3, 3), (64, 48), (241, 17)])
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("above_first", [True, False])
+def test_pyramid_levels(dev, size, fmt, above_first):
+    w, h = size
+    rng = np.random.RandomState(w * 31 + h + fmt)
+    eng, _ = rand_engine(rng, w, h, fmt)
+    for q, hiq in ((4, True), (5, True), (3, False)):
+        s = tw.FlowSettings(quality=q, hiq=hiq, taps_above_first=above_first)
+        got = dev.build_pyramid(eng, w, h, fmt, s)
+        want = O.build_pyramid(eng, w, h, fmt, quality=q, hiq=hiq, above_first=above_first)
+        assert len(got) == len(want)
+        for g, o in zip(got, want):
+            assert same(g, o)
+
+
+@pytest.mark.parametrize("size", [(12, 10), (40, 30), (97, 61), (3, 3), (5, 200), (960, 540)])
+@pytest.mark.parametrize("kind", ["noise", "smooth", "constant"])
+def test_block_match_sweeps(dev, size, kind):
+    """Random fields make long accepted runs and many run starts; the sweep is a loop-carried
+    recurrence, so this checks the parallel run decomposition against the sequential oracle."""
+    w, h = size
+    rng = np.random.RandomState(w + 7 * h)
+    a = (rng.random_sample((h, w)) * 50).astype(np.float32)
+    b = np.roll(a, 1, axis=1) + (rng.random_sample((h, w)) * 2).astype(np.float32)
+    if kind == "noise":
+        flow = ((rng.random_sample(w * h * 2) - 0.5) * 6).astype(np.float32)
+    elif kind == "smooth":
+        yy, xx = np.mgrid[0:h, 0:w]
+        flow = np.stack([np.sin(xx / 7.0) * 2 - 1, np.cos(yy / 5.0) * 1.5], -1).astype(np.float32).reshape(-1)
+        flow += (rng.random_sample(flow.size) * 0.2).astype(np.float32)
+    else:
+        flow = np.full(w * h * 2, -1.0, np.float32)
+        flow[::7] = 0.5
+    want = flow.copy()
+    O.lib().or_block_match(O.ptr(a), O.ptr(b), O.ptr(want), w, h)
+    got = dev.block_match(a, b, flow, w, h)
+    assert same(got, want)
+
+
+def clip_pair(w, h, fmt, seed, t=3):
+    depth = {0: 8, 1: 16, 2: 32}[fmt]
+    frames = synth.moving_clip(w, h, t + 2, depth=depth, seed=seed)
+    n = w * h * 4
+    wa, wb = frames[t * n:(t + 1) * n], frames[(t + 1) * n:(t + 2) * n]
+    return O.from_frame(wa, w, h, fmt), O.from_frame(wb, w, h, fmt), wa, wb
+
+
+@pytest.mark.parametrize("size,fmt", [((160, 96), 0), ((160, 96), 1), ((160, 96), 2), ((97, 61), 0), ((64, 48), 2),
+                                      ((6, 5), 0), ((320, 180), 0)])
+@pytest.mark.parametrize("sens,quality,hiq", [(0.7, 4, True), (1.0, 5, True), (0.33, 4, True), (0.7, 3, False)])
+@pytest.mark.parametrize("above_first", [True, False])
+def test_solve_pair_bit_exact(dev, size, fmt, sens, quality, hiq, above_first):
+    w, h = size
+    a, b, _, _ = clip_pair(w, h, fmt, seed=0x74570001 + w)
+    s = tw.FlowSettings(quality=quality, hiq=hiq, sensitivity=np.float32(sens), taps_above_first=above_first)
+    f_ab, f_ba, fs = dev.solve_pair(a, b, w, h, fmt, s)
+    o_ab, o_ba, ofs = O.solve_pair(a, b, w, h, fmt, quality=quality, hiq=hiq, sensitivity=np.float32(sens),
+                                   above_first=above_first)
+    assert fs == ofs
+    assert same(f_ab, o_ab)
+    assert same(f_ba, o_ba)
+    if w >= 64 and sens > 0.5:
+        assert np.abs(f_ab).max() > 0  # the solve moved
+
+
+def test_solve_skip_refine(dev):
+    w, h = 160, 96
+    a, b, _, _ = clip_pair(w, h, 0, seed=3)
+    s = tw.FlowSettings(skip_refine=True)
+    f_ab, f_ba, _ = dev.solve_pair(a, b, w, h, 0, s)
+    o_ab, o_ba, _ = O.solve_pair(a, b, w, h, 0, skip_refine=True)
+    assert same(f_ab, o_ab) and same(f_ba, o_ba)
+
+
+# ---- composition ------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("wa,interp", [(0.5, 1), (0.75, 1), (0.2, 1), (0.999, 1), (1.0, 1), (1.5, 1), (0.6, 0),
+                                       (0.3, 0)])
+def test_compose_vectors(dev, fmt, wa, interp):
+    w, h = 96, 64
+    a, b, _, _ = clip_pair(w, h, fmt, seed=9)
+    o_ab, o_ba, (fw, fh) = O.solve_pair(a, b, w, h, fmt)
+    sel = tw.Selection(wa=np.float32(wa), interp=interp)
+    got = dev.compose_vectors(tw.EngineSettings(), sel, a, b, w, h, fmt, o_ab, o_ba, (fw, fh))
+    want = O.compose_vectors(a, b, w, h, fmt, o_ab, o_ba, fw, fh, np.float32(wa), interp)
+    assert same(got, want)
+
+
+# ---- whole output frames -----------------------------------------------------------------------------
+
+CASES, INPUTS = golden_data.grid()
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["id"] for c in CASES])
+def test_retime_flow_grid_sha256(dev, case):
+    """The reference's recorded output of every served grid case, rendered by the CUDA path."""
+    fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
+    raw = INPUTS[case["input"]].view(tw.DTYPES[fmt])
+    kw = golden_data.case_params(case)
+    tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], keys=kw["keys"], vectors=kw["vectors"],
+                       frame_interp=kw["frame_interp"], blur_compensation=kw["blur"])
+    settings = tw.RetimeSettings(
+        flow=tw.FlowSettings(hiq=True, sensitivity=np.float32(np.float32(kw["sensitivity"]) / np.float32(100.0)),
+                             taps_above_first=False),
+        compose=tw.EngineSettings(taps_above_first=False), motion_rows_reversed=False)
+    out = tw.retime_clip(dev, raw, case["frames"], case["width"], case["height"], fmt, tp, case["frames"], settings)
+    assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
+
+
+def test_retime_config1_clip_matches_oracle(dev):
+    """160x96 8 bpc, 48 frames to 95 output frames at speed 50 %, the reference's current orders."""
+    w, h, n = 160, 96, 48
+    frames = synth.moving_clip(w, h, n, depth=8)
+    tp = tw.TimeParams(speed_percent=50.0)
+    out = tw.retime_clip(dev, frames, n, w, h, 0, tp, 95)
+    want = O.retime_clip(frames, n, w, h, 0, O.retime_params(speed=50.0), 95)
+    assert same(out, want)
+
+
+@pytest.mark.parametrize("fmt", [0, 1])
+def test_1080p_frame_matches_oracle(dev, fmt):
+    """One full size in-between frame (1920x1080, solve at 960x540, 8 levels)."""
+    w, h = 1920, 1080
+    depth = {0: 8, 1: 16}[fmt]
+    frames = synth.moving_clip(w, h, 2, depth=depth, seed=0x74570002, bg_velocity=(6.0, -3.0),
+                               square=240, square_start=(600.0, 400.0), square_velocity=(9.0, 4.0))
+    tp = tw.TimeParams(speed_percent=40.0)
+    sel = tw.select(tp, 1, w, h)  # s0 = 0.4
+    n = w * h * 4
+    out = dev.retime_frame(tw.RetimeSettings(), sel, frames[:n], frames[n:2 * n], w, h, fmt)
+    want = O.retime_clip(frames, 2, w, h, fmt, O.retime_params(speed=40.0), 2)[n:2 * n]
+    assert same(out, want)
+
+
+def test_frames_outside_the_clip_are_blank(dev):
+    w, h, n = 48, 32, 4
+    frames = synth.moving_clip(w, h, n, depth=8, seed=77)
+    tp = tw.TimeParams(speed_percent=150.0)
+    out = tw.retime_clip(dev, frames, n, w, h, 0, tp, 6)
+    want = O.retime_clip(frames, n, w, h, 0, O.retime_params(speed=150.0), 6)
+    assert same(out, want)
+
+
+def test_unsupported_settings_fail_loudly(dev):
+    w, h = 32, 24
+    a, b, _, _ = clip_pair(w, h, 0, seed=1)
+    with pytest.raises(tw.Unsupported):
+        dev.solve_pair(a, b, w, h, 0, tw.FlowSettings(prep_contrast_edge=True))
+    with pytest.raises(tw.BadParam):
+        dev.solve_pair(a, b, w, h, 0, tw.FlowSettings(quality=0))

@@ -1,0 +1,456 @@
+"""twixtor_b200: the retime hot path of baairon/twixtor on B200 (sm_100a CUDA behind a C ABI).
+
+This module is the Python face of the library ``libtwixtor_b200.so`` (declared in
+``include/twixtor_b200.h``). It mirrors the reference's stage seam
+(``plugins/retime-engine/src/stages.rs:33-71``, trait ``Stages``; its device side is
+``device/exec/backend.rs:27-46``, trait ``Backend``): ``solve``, ``solve_pair`` and
+``compose_vectors`` take the same arguments (engine images, ``FlowSettings``, a ``Selection``) and
+return what the CPU functions return. Every computation runs in the library's CUDA kernels; when
+the library is missing, importing a ``Device`` raises instead of falling back to anything else.
+
+Images are numpy arrays of ``width * height * 4`` samples (uint8, uint16 or float32) in the engine
+layout (A, R, G, B premultiplied, top row first); flows are float32 arrays of
+``width * height * 2`` values, (dx, dy) interleaved.
+"""
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtwixtor_b200.so")
+
+U8, U16, F32 = 0, 1, 2
+DTYPES = {U8: np.uint8, U16: np.uint16, F32: np.float32}
+FMT_OF_DTYPE = {np.dtype(np.uint8): U8, np.dtype(np.uint16): U16, np.dtype(np.float32): F32}
+
+OK, ERR_CUDA, ERR_NAN_OUTPUT, ERR_UNSUPPORTED, ERR_MISMATCH, ERR_BAD_PARAM, ERR_DEVICE_BOUND = range(7)
+
+
+class StageError(RuntimeError):
+    """A stage the device did not serve (the reference's ``device::image::StageError``)."""
+
+    def __init__(self, code, message):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+        self.message = message
+
+
+class Unsupported(StageError):
+    pass
+
+
+class NanOutput(StageError):
+    pass
+
+
+class Mismatch(StageError):
+    pass
+
+
+class BadParam(StageError):
+    pass
+
+
+_ERRORS = {ERR_UNSUPPORTED: Unsupported, ERR_NAN_OUTPUT: NanOutput, ERR_MISMATCH: Mismatch, ERR_BAD_PARAM: BadParam,
+           ERR_DEVICE_BOUND: Unsupported}
+
+
+# ---- C ABI structs (include/twixtor_b200.h) --------------------------------------------------------
+
+class _Image(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("fmt", ctypes.c_int32),
+                ("data", ctypes.c_void_p)]
+
+
+class _Flow(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("data", ctypes.c_void_p)]
+
+
+class _FlowSettings(ctypes.Structure):
+    _fields_ = [("quality", ctypes.c_int32), ("hiq", ctypes.c_int32), ("sensitivity", ctypes.c_float),
+                ("prep_contrast_edge", ctypes.c_int32), ("prep_delinearize", ctypes.c_int32),
+                ("track_alpha", ctypes.c_int32), ("video_range_luma", ctypes.c_int32),
+                ("skip_refine", ctypes.c_int32), ("wrap", ctypes.c_int32), ("taps_above_first", ctypes.c_int32)]
+
+
+class _Selection(ctypes.Structure):
+    _fields_ = [("s0", ctypes.c_float), ("s1", ctypes.c_float), ("a", ctypes.c_int32), ("b", ctypes.c_int32),
+                ("wa", ctypes.c_float), ("exact", ctypes.c_int32), ("vectors_quality", ctypes.c_int32),
+                ("interp", ctypes.c_int32)]
+
+
+class _EngineSettings(ctypes.Structure):
+    _fields_ = [("warp_mode", ctypes.c_int32), ("video_360", ctypes.c_int32), ("wrap_360", ctypes.c_int32),
+                ("quality_high", ctypes.c_int32), ("blur", ctypes.c_float), ("taps_above_first", ctypes.c_int32)]
+
+
+class _RetimeSettings(ctypes.Structure):
+    _fields_ = [("flow", _FlowSettings), ("compose", _EngineSettings), ("motion_rows_reversed", ctypes.c_int32)]
+
+
+class _TimeParams(ctypes.Structure):
+    _fields_ = [("fps_num", ctypes.c_int32), ("fps_den", ctypes.c_int32), ("speed_percent", ctypes.c_double),
+                ("nkeys", ctypes.c_int32), ("key_frames", ctypes.POINTER(ctypes.c_double)),
+                ("key_values", ctypes.POINTER(ctypes.c_double)), ("key_ease", ctypes.POINTER(ctypes.c_int32)),
+                ("vectors", ctypes.c_int32), ("frame_interp", ctypes.c_int32),
+                ("blur_compensation", ctypes.c_double)]
+
+
+# ---- the Python mirrors of the reference types -----------------------------------------------------
+
+@dataclass
+class FlowSettings:
+    """``flow::FlowSettings`` (flow.rs:83-123). ``taps_above_first`` is the vertical tap order of the
+    solver's filters: True is the reference's order; False the order of the revision its parity grid
+    records."""
+    quality: int = 4
+    hiq: bool = True
+    sensitivity: float = 0.7
+    prep_contrast_edge: bool = False
+    prep_delinearize: bool = False
+    track_alpha: bool = False
+    video_range_luma: bool = False
+    skip_refine: bool = False
+    wrap: bool = False
+    taps_above_first: bool = True
+
+    def _c(self):
+        return _FlowSettings(self.quality, int(self.hiq), np.float32(self.sensitivity), int(self.prep_contrast_edge),
+                             int(self.prep_delinearize), int(self.track_alpha), int(self.video_range_luma),
+                             int(self.skip_refine), int(self.wrap), int(self.taps_above_first))
+
+
+@dataclass
+class Selection:
+    """``timeline::Selection`` (timeline.rs:391-414)."""
+    s0: float = 0.0
+    s1: float = 0.0
+    a: int = 0
+    b: int = 1
+    wa: float = 1.0
+    exact: bool = True
+    vectors_quality: int = 4
+    interp: int = 1
+
+    def _c(self):
+        return _Selection(self.s0, self.s1, self.a, self.b, self.wa, int(self.exact), self.vectors_quality,
+                          self.interp)
+
+    @staticmethod
+    def _from_c(c):
+        return Selection(c.s0, c.s1, c.a, c.b, c.wa, bool(c.exact), c.vectors_quality, c.interp)
+
+
+@dataclass
+class EngineSettings:
+    """The fields of ``host::EngineSettings`` (host.rs:20-100) that ``compose_vectors`` reads."""
+    warp_mode: int = 0
+    video_360: bool = False
+    wrap_360: bool = False
+    quality_high: bool = True
+    blur: float = 0.0
+    taps_above_first: bool = True
+
+    def _c(self):
+        return _EngineSettings(self.warp_mode, int(self.video_360), int(self.wrap_360), int(self.quality_high),
+                               self.blur, int(self.taps_above_first))
+
+
+@dataclass
+class RetimeSettings:
+    """One output frame's settings of the ``retime`` effect beyond its selection."""
+    flow: FlowSettings = field(default_factory=FlowSettings)
+    compose: EngineSettings = field(default_factory=EngineSettings)
+    motion_rows_reversed: bool = True
+
+    def _c(self):
+        return _RetimeSettings(self.flow._c(), self.compose._c(), int(self.motion_rows_reversed))
+
+
+@dataclass
+class TimeParams:
+    """The parameters the Speed time map reads (plugins/retime/src/lib.rs:59-99). Popups carry
+    their 1-based values; ``keys`` is a list of (frame, value, ease) of a keyed Speed %."""
+    fps: Tuple[int, int] = (24, 1)
+    speed_percent: float = 100.0
+    keys: Optional[Sequence[Tuple[float, float, bool]]] = None
+    vectors: int = 5
+    frame_interp: int = 2
+    blur_compensation: float = 0.0
+
+    def _c(self):
+        p = _TimeParams()
+        p.fps_num, p.fps_den = self.fps
+        p.speed_percent = self.speed_percent
+        p.vectors, p.frame_interp = self.vectors, self.frame_interp
+        p.blur_compensation = self.blur_compensation
+        p.nkeys = 0
+        if self.keys:
+            n = len(self.keys)
+            fr = (ctypes.c_double * n)(*[k[0] for k in self.keys])
+            va = (ctypes.c_double * n)(*[k[1] for k in self.keys])
+            ea = (ctypes.c_int32 * n)(*[int(k[2]) for k in self.keys])
+            p.nkeys = n
+            p.key_frames = ctypes.cast(fr, ctypes.POINTER(ctypes.c_double))
+            p.key_values = ctypes.cast(va, ctypes.POINTER(ctypes.c_double))
+            p.key_ease = ctypes.cast(ea, ctypes.POINTER(ctypes.c_int32))
+            p._keep = (fr, va, ea)
+        return p
+
+
+# ---- library loading ----------------------------------------------------------------------------
+
+_lib = None
+
+
+def build(force=False):
+    """Compiles the library in tree (nvcc, sm_100a)."""
+    from . import buildlib
+    return buildlib.build(force=force)
+
+
+def library():
+    """The loaded library; raises when it is not built (there is no other implementation)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built: run `python -c 'import twixtor_b200; twixtor_b200.build()'`")
+    L = ctypes.CDLL(LIB_PATH)
+    P, i32 = ctypes.c_void_p, ctypes.c_int32
+    pimg, pflow = ctypes.POINTER(_Image), ctypes.POINTER(_Flow)
+    L.tw_open.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.tw_close.argtypes = [P]
+    L.tw_close.restype = None
+    L.tw_last_error.argtypes = [P, ctypes.c_char_p, ctypes.c_size_t]
+    L.tw_last_error.restype = ctypes.c_size_t
+    L.tw_stats.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    L.tw_flow_geometry.argtypes = [ctypes.POINTER(_FlowSettings), i32, i32, P, P, P, P, i32]
+    L.tw_solve.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), pflow]
+    L.tw_solve_pair.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), pflow, pflow]
+    L.tw_compose_vectors.argtypes = [P, ctypes.POINTER(_EngineSettings), ctypes.POINTER(_Selection), pimg, pimg,
+                                     pflow, pflow, pimg]
+    L.tw_build_pyramid.argtypes = [P, pimg, ctypes.POINTER(_FlowSettings), P]
+    L.tw_inv_warp.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, P]
+    L.tw_block_match.argtypes = [P, P, P, P, i32, i32]
+    L.tw_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float]
+    L.tw_from_frame.argtypes = [P, P, i32, i32, i32, P]
+    L.tw_to_frame.argtypes = [P, P, i32, i32, i32, P]
+    L.tw_select.argtypes = [ctypes.POINTER(_TimeParams), i32, i32, i32, ctypes.POINTER(_Selection)]
+    L.tw_retime_frame.argtypes = [P, ctypes.POINTER(_RetimeSettings), ctypes.POINTER(_Selection), P, P, i32, i32,
+                                  i32, P]
+    L.tw_retime_clip_device.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, ctypes.POINTER(_Selection), i32,
+                                        i32, i32, i32, P]
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _img(a, w, h, fmt):
+    a = np.ascontiguousarray(a)
+    assert a.dtype == DTYPES[fmt] and a.size == w * h * 4, "engine image of the wrong size or depth"
+    return _Image(w, h, fmt, a.ctypes.data), a
+
+
+def select(params: TimeParams, n: int, width: int, height: int) -> Selection:
+    """``timeline::select`` of output frame ``n`` (the Speed map, host scalars in the library)."""
+    out = _Selection()
+    rc = library().tw_select(ctypes.byref(params._c()), n, width, height, ctypes.byref(out))
+    if rc:
+        raise BadParam(rc, "tw_select")
+    return Selection._from_c(out)
+
+
+def flow_geometry(settings: FlowSettings, width: int, height: int):
+    """(flow width, flow height, [(w, h) per level]) of a solve (FlowSettings::geometry)."""
+    fw, fh, nl = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    sizes = np.zeros(64, np.int32)
+    rc = library().tw_flow_geometry(ctypes.byref(settings._c()), width, height, ctypes.byref(fw), ctypes.byref(fh),
+                                    ctypes.byref(nl), _ptr(sizes), 32)
+    if rc:
+        raise (_ERRORS.get(rc, StageError))(rc, "flow geometry")
+    return fw.value, fh.value, [(int(sizes[2 * i]), int(sizes[2 * i + 1])) for i in range(nl.value)]
+
+
+class Device:
+    """One CUDA device with the library's context (the reference's ``exec::open``,
+    device/exec/open.rs:72-116). Implements the ``Stages`` methods."""
+
+    def __init__(self, device: int = 0):
+        L = library()
+        h = ctypes.c_void_p()
+        rc = L.tw_open(device, ctypes.byref(h))
+        if rc:
+            raise StageError(rc, f"tw_open({device}) failed")
+        self._h = h
+        self._L = L
+
+    def close(self):
+        if self._h:
+            self._L.tw_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, rc):
+        if rc:
+            n = self._L.tw_last_error(self._h, None, 0)
+            buf = ctypes.create_string_buffer(n + 1)
+            self._L.tw_last_error(self._h, buf, n + 1)
+            raise (_ERRORS.get(rc, StageError))(rc, buf.value.decode())
+
+    def stats(self):
+        k, b = ctypes.c_uint64(), ctypes.c_uint64()
+        self._L.tw_stats(self._h, ctypes.byref(k), ctypes.byref(b))
+        return {"kernel_launches": k.value, "device_bytes": b.value}
+
+    # ---- Stages ---------------------------------------------------------------------------------
+
+    def solve(self, x, y, width, height, fmt, settings: FlowSettings):
+        """``flow::solve``: X(p) ~ Y(p + out(p)) at the working resolution."""
+        fw, fh, _ = flow_geometry(settings, width, height)
+        out = np.zeros(fw * fh * 2, np.float32)
+        xi, xa = _img(x, width, height, fmt)
+        yi, ya = _img(y, width, height, fmt)
+        fo = _Flow(fw, fh, out.ctypes.data)
+        self._check(self._L.tw_solve(self._h, ctypes.byref(xi), ctypes.byref(yi), ctypes.byref(settings._c()),
+                                     ctypes.byref(fo)))
+        return out, (fw, fh)
+
+    def solve_pair(self, a, b, width, height, fmt, settings: FlowSettings):
+        """``flow::solve_pair``: (f_ab, f_ba, (flow width, flow height))."""
+        fw, fh, _ = flow_geometry(settings, width, height)
+        f_ab = np.zeros(fw * fh * 2, np.float32)
+        f_ba = np.zeros(fw * fh * 2, np.float32)
+        ai, aa = _img(a, width, height, fmt)
+        bi, ba = _img(b, width, height, fmt)
+        fa, fb = _Flow(fw, fh, f_ab.ctypes.data), _Flow(fw, fh, f_ba.ctypes.data)
+        self._check(self._L.tw_solve_pair(self._h, ctypes.byref(ai), ctypes.byref(bi), ctypes.byref(settings._c()),
+                                          ctypes.byref(fa), ctypes.byref(fb)))
+        return f_ab, f_ba, (fw, fh)
+
+    def compose_vectors(self, settings: EngineSettings, sel: Selection, a, b, width, height, fmt, f_ab, f_ba,
+                        flow_size):
+        """``compose::compose_vectors`` (warping code 0): the engine image of the output frame."""
+        fw, fh = flow_size
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        ai, aa = _img(a, width, height, fmt)
+        bi, ba = _img(b, width, height, fmt)
+        oi = _Image(width, height, fmt, out.ctypes.data)
+        fab = _Flow(fw, fh, f_ab.ctypes.data) if f_ab is not None else None
+        fba = _Flow(fw, fh, f_ba.ctypes.data) if f_ba is not None else None
+        self._check(self._L.tw_compose_vectors(self._h, ctypes.byref(settings._c()), ctypes.byref(sel._c()),
+                                               ctypes.byref(ai), ctypes.byref(bi),
+                                               ctypes.byref(fab) if fab else None, ctypes.byref(fba) if fba else None,
+                                               ctypes.byref(oi)))
+        return out
+
+    # ---- single stages ----------------------------------------------------------------------------
+
+    def build_pyramid(self, img, width, height, fmt, settings: FlowSettings):
+        _, _, sizes = flow_geometry(settings, width, height)
+        out = np.zeros(sum(w * h for w, h in sizes), np.float32)
+        ii, ia = _img(img, width, height, fmt)
+        self._check(self._L.tw_build_pyramid(self._h, ctypes.byref(ii), ctypes.byref(settings._c()), _ptr(out)))
+        levels, off = [], 0
+        for w, h in sizes:
+            levels.append(out[off:off + w * h].reshape(h, w))
+            off += w * h
+        return levels
+
+    def block_match(self, a, b, flow, width, height):
+        """``flow::block_match`` on one level: returns the refined flow (interleaved)."""
+        a = np.ascontiguousarray(a, np.float32).reshape(-1)
+        b = np.ascontiguousarray(b, np.float32).reshape(-1)
+        f = np.array(flow, np.float32).reshape(-1)
+        self._check(self._L.tw_block_match(self._h, _ptr(a), _ptr(b), _ptr(f), width, height))
+        return f
+
+    def inv_warp(self, src, width, height, fmt, flow, flow_size, amount, hold=True, coverage=False):
+        fw, fh = flow_size
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        si, sa = _img(src, width, height, fmt)
+        oi = _Image(width, height, fmt, out.ctypes.data)
+        flow = np.ascontiguousarray(flow, np.float32)
+        fl = _Flow(fw, fh, flow.ctypes.data)
+        cov = np.zeros(width * height, np.uint8) if coverage else None
+        self._check(self._L.tw_inv_warp(self._h, ctypes.byref(oi), ctypes.byref(si), ctypes.byref(fl),
+                                        np.float32(amount), int(hold), _ptr(cov)))
+        return (out, cov) if coverage else out
+
+    def blend(self, a, b, width, height, fmt, w):
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        ai, aa = _img(a, width, height, fmt)
+        bi, ba = _img(b, width, height, fmt)
+        oi = _Image(width, height, fmt, out.ctypes.data)
+        self._check(self._L.tw_blend(self._h, ctypes.byref(oi), ctypes.byref(ai), ctypes.byref(bi), np.float32(w)))
+        return out
+
+    def from_frame(self, wire, width, height, fmt):
+        wire = np.ascontiguousarray(wire)
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        self._check(self._L.tw_from_frame(self._h, _ptr(wire), width, height, fmt, _ptr(out)))
+        return out
+
+    def to_frame(self, engine, width, height, fmt):
+        engine = np.ascontiguousarray(engine)
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        self._check(self._L.tw_to_frame(self._h, _ptr(engine), width, height, fmt, _ptr(out)))
+        return out
+
+    # ---- whole frames -------------------------------------------------------------------------------
+
+    def retime_frame(self, settings: RetimeSettings, sel: Selection, wire_a, wire_b, width, height, fmt, out=None):
+        """One output wire frame of the ``retime`` core; ``wire_a`` / ``wire_b`` None are blank frames."""
+        if out is None:
+            out = np.zeros(width * height * 4, DTYPES[fmt])
+        self._check(self._L.tw_retime_frame(self._h, ctypes.byref(settings._c()), ctypes.byref(sel._c()),
+                                            _ptr(wire_a), _ptr(wire_b), width, height, fmt, _ptr(out)))
+        return out
+
+    def retime_clip_device(self, settings: RetimeSettings, frames_ptr: int, nframes: int, sels, width, height, fmt,
+                           out_ptr: int):
+        """A clip resident in device memory (raw device pointers, e.g. ``tensor.data_ptr()``)."""
+        arr = (_Selection * len(sels))(*[s._c() for s in sels])
+        self._check(self._L.tw_retime_clip_device(self._h, ctypes.byref(settings._c()), ctypes.c_void_p(frames_ptr),
+                                                  nframes, arr, len(sels), width, height, fmt,
+                                                  ctypes.c_void_p(out_ptr)))
+
+
+def retime_clip(dev: Device, frames, nframes, width, height, fmt, params: TimeParams, nout,
+                settings: Optional[RetimeSettings] = None):
+    """Renders ``nout`` output frames of the ``retime`` effect over a raw clip (wire frames back to
+    back in one array), frame by frame through the library: the host part of the reference's
+    ``vfx apply retime`` loop (crates/fx-cli/src/temporal.rs:183-250) around ``tw_retime_frame``."""
+    settings = settings or RetimeSettings()
+    frame_samples = width * height * 4
+    frames = np.ascontiguousarray(frames).reshape(-1)
+    out = np.zeros(nout * frame_samples, DTYPES[fmt])
+    for n in range(nout):
+        sel = select(params, n, width, height)
+        sel_flow = FlowSettings(**{**settings.flow.__dict__})
+        fa = frames[sel.a * frame_samples:(sel.a + 1) * frame_samples] if 0 <= sel.a < nframes else None
+        fb = frames[sel.b * frame_samples:(sel.b + 1) * frame_samples] if 0 <= sel.b < nframes else None
+        s = RetimeSettings(sel_flow, settings.compose, settings.motion_rows_reversed)
+        dev.retime_frame(s, sel, fa, fb, width, height, fmt, out=out[n * frame_samples:(n + 1) * frame_samples])
+    return out

@@ -1,0 +1,550 @@
+// Image boundary, luma, inverse warps and blends, strict mode. Each kernel cites the reference
+// function (plugins/retime-engine/src/...) whose per-element arithmetic it repeats.
+#include "kernels.cuh"
+
+namespace tw {
+
+__device__ __forceinline__ float inv_255() { return __uint_as_float(0x3b808081u); }            // image.rs:261
+__device__ __forceinline__ float premul16_color() { return __uint_as_float(0x387fff00u); }     // image.rs:263
+__device__ __forceinline__ float premul16_alpha() { return __uint_as_float(0x3fffff00u); }     // image.rs:265
+__device__ __forceinline__ float unpremul16_alpha() { return __uint_as_float(0x3f000080u); }   // image.rs:267
+
+__device__ __forceinline__ uint16_t u16_to_q15(uint16_t v) { return (uint16_t)(((uint32_t)v * 32768u + 32767u) / 65535u); }
+__device__ __forceinline__ uint16_t q15_to_u16(uint16_t v) {
+    uint32_t m = v < 32768 ? v : 32768;
+    return (uint16_t)((m * 65535u + 16384u) / 32768u);
+}
+
+// ---- wire -> engine (image.rs:178-206, premultiply :276-303) ----------------------------------------
+
+__global__ void k_from_frame_u8(const uint8_t* __restrict__ wire, uint8_t* __restrict__ eng, int w, int h, bool flip) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long n = (long)w * h;
+    if (i >= n) return;
+    int y = (int)(i / w), x = (int)(i - (long)y * w);
+    long si = (long)(flip ? h - 1 - y : y) * w + x;
+    uchar4 p = reinterpret_cast<const uchar4*>(wire)[si];  // r, g, b, a
+    float a = (float)p.w * inv_255();
+    uchar4 o;
+    o.x = p.w;
+    o.y = (uint8_t)qround((float)p.x * a);
+    o.z = (uint8_t)qround((float)p.y * a);
+    o.w = (uint8_t)qround((float)p.z * a);
+    reinterpret_cast<uchar4*>(eng)[i] = o;
+}
+
+__global__ void k_from_frame_u16(const uint16_t* __restrict__ wire, uint16_t* __restrict__ eng, int w, int h, bool flip) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long n = (long)w * h;
+    if (i >= n) return;
+    int y = (int)(i / w), x = (int)(i - (long)y * w);
+    long si = (long)(flip ? h - 1 - y : y) * w + x;
+    ushort4 p = reinterpret_cast<const ushort4*>(wire)[si];
+    uint16_t A = u16_to_q15(p.w), R = u16_to_q15(p.x), G = u16_to_q15(p.y), Bc = u16_to_q15(p.z);
+    float a = (float)A * premul16_color();
+    ushort4 o;
+    o.x = (uint16_t)qround((float)A * premul16_alpha());
+    o.y = (uint16_t)qround((float)R * a);
+    o.z = (uint16_t)qround((float)G * a);
+    o.w = (uint16_t)qround((float)Bc * a);
+    reinterpret_cast<ushort4*>(eng)[i] = o;
+}
+
+__global__ void k_from_frame_f32(const float* __restrict__ wire, float* __restrict__ eng, int w, int h, bool flip) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long n = (long)w * h;
+    if (i >= n) return;
+    int y = (int)(i / w), x = (int)(i - (long)y * w);
+    long si = (long)(flip ? h - 1 - y : y) * w + x;
+    // planes G, B, R, A
+    float g = wire[si], b = wire[n + si], r = wire[2 * n + si], a = wire[3 * n + si];
+    float o1 = a * r, o2 = a * g, o3 = a * b;
+    if (isnan(o1) || isnan(o2) || isnan(o3) || isnan(a)) {
+        o1 = nr::mul(a, r);
+        o2 = nr::mul(a, g);
+        o3 = nr::mul(a, b);
+    }
+    reinterpret_cast<float4*>(eng)[i] = make_float4(a, o1, o2, o3);
+}
+
+// ---- engine -> wire (image.rs:213-245, unpremultiply :306-351) --------------------------------------
+
+__device__ __forceinline__ uchar4 unpremul_u8(uchar4 p) {  // -> r, g, b, a
+    if (p.x == 0) return make_uchar4(p.y, p.z, p.w, p.x);
+    float s = 255.0f / (float)p.x;
+    auto f = [&](uint8_t c) {
+        float v = (float)c * s;
+        if (v > 255.0f) v = 255.0f;
+        return (uint8_t)qround(v);
+    };
+    return make_uchar4(f(p.y), f(p.z), f(p.w), p.x);
+}
+
+__device__ __forceinline__ ushort4 unpremul_u16(ushort4 p) {  // -> wire r, g, b, a
+    ushort4 o;
+    if (p.x == 0) {
+        o = make_ushort4(p.y, p.z, p.w, p.x);
+    } else {
+        float a = (float)p.x;
+        float s = 32768.0f / a;
+        o = make_ushort4((uint16_t)qround((float)p.y * s), (uint16_t)qround((float)p.z * s),
+                         (uint16_t)qround((float)p.w * s), (uint16_t)qround(a * unpremul16_alpha()));
+    }
+    return make_ushort4(q15_to_u16(o.x), q15_to_u16(o.y), q15_to_u16(o.z), q15_to_u16(o.w));
+}
+
+__device__ __forceinline__ float4 unpremul_f32(float4 p) {  // -> a, r, g, b (engine order)
+    if ((double)p.x < 1e-12) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    // `1.0 / a` keeps a NaN alpha's payload as the x86 divide does (the quieted NaN operand)
+    float inv = nr::div(1.0f, p.x);
+    float r = p.y * inv, g = p.z * inv, b = p.w * inv;
+    if (isnan(r) || isnan(g) || isnan(b) || isnan(p.x)) {
+        r = nr::mul(p.y, inv);
+        g = nr::mul(p.z, inv);
+        b = nr::mul(p.w, inv);
+    }
+    return make_float4(p.x, r, g, b);
+}
+
+__global__ void k_to_frame_u8(const uint8_t* __restrict__ eng, uint8_t* __restrict__ wire, int w, int h, bool flip) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long n = (long)w * h;
+    if (i >= n) return;
+    int y = (int)(i / w), x = (int)(i - (long)y * w);
+    long si = (long)(flip ? h - 1 - y : y) * w + x;
+    reinterpret_cast<uchar4*>(wire)[i] = unpremul_u8(reinterpret_cast<const uchar4*>(eng)[si]);
+}
+
+__global__ void k_to_frame_u16(const uint16_t* __restrict__ eng, uint16_t* __restrict__ wire, int w, int h, bool flip) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long n = (long)w * h;
+    if (i >= n) return;
+    int y = (int)(i / w), x = (int)(i - (long)y * w);
+    long si = (long)(flip ? h - 1 - y : y) * w + x;
+    reinterpret_cast<ushort4*>(wire)[i] = unpremul_u16(reinterpret_cast<const ushort4*>(eng)[si]);
+}
+
+__global__ void k_to_frame_f32(const float* __restrict__ eng, float* __restrict__ wire, int w, int h, bool flip) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long n = (long)w * h;
+    if (i >= n) return;
+    int y = (int)(i / w), x = (int)(i - (long)y * w);
+    long si = (long)(flip ? h - 1 - y : y) * w + x;
+    float4 o = unpremul_f32(reinterpret_cast<const float4*>(eng)[si]);
+    wire[i] = o.z;          // G
+    wire[n + i] = o.w;      // B
+    wire[2 * n + i] = o.y;  // R
+    wire[3 * n + i] = o.x;  // A
+}
+
+// ---- luma (prep.rs:168-235) ------------------------------------------------------------------------
+
+__global__ void k_luma(const void* __restrict__ eng, int fmt, float* __restrict__ out, int w, int h, bool track_alpha,
+                       bool video_range) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long n = (long)w * h;
+    if (i >= n) return;
+    float v;
+    if (fmt == 0) {
+        uchar4 p = reinterpret_cast<const uchar4*>(eng)[i];
+        float a = (float)p.x, r = (float)p.y, g = (float)p.z, b = (float)p.w;
+        if (video_range) v = ((r - 16.0f) * 255.0f) / 219.0f;
+        else {
+            float sum = (r * 0.3f + g * 0.59f) + b * 0.11f;
+            v = track_alpha ? (float)((double)sum + (double)a * 0.3) : sum;
+        }
+    } else if (fmt == 1) {
+        ushort4 p = reinterpret_cast<const ushort4*>(eng)[i];
+        if (video_range) v = (((float)p.y / 257.0f - 16.0f) * 255.0f) / 219.0f;
+        else {
+            double sum = ((double)p.z * 0.59 + (double)p.y * 0.3) + (double)p.w * 0.11;
+            if (track_alpha) sum += (double)p.x * 0.3;
+            v = (float)(sum / 257.0);
+        }
+    } else {
+        float4 p = reinterpret_cast<const float4*>(eng)[i];
+        if (video_range) v = ((p.y * 255.0f - 16.0f) * 255.0f) / 219.0f;
+        else {
+            double sum = ((double)p.z * 0.59 + (double)p.y * 0.3) + (double)p.w * 0.11;
+            if (track_alpha) sum += (double)p.x * 0.3;
+            v = (float)(sum * 255.0);
+        }
+    }
+    out[i] = v;
+}
+
+// ---- inverse warp (warp.rs) -------------------------------------------------------------------------
+
+template <typename P> struct Pix;
+template <> struct Pix<uint8_t> {
+    __device__ static float f(uint8_t v) { return (float)v; }
+    __device__ static uint8_t store(float v) { return sat_u8(v); }
+    // warp.rs:152-155: the stored sample scaled by the fade, the add in double
+    __device__ static uint8_t faded(float v, float f) { return (uint8_t)cvtt64d((double)((float)sat_u8(v) * f) + 0.5); }
+};
+template <> struct Pix<uint16_t> {
+    __device__ static float f(uint16_t v) { return (float)v; }
+    __device__ static uint16_t store(float v) { return sat_u16(v); }
+    __device__ static uint16_t faded(float v, float f) { return (uint16_t)cvtt64d((double)((float)sat_u16(v) * f) + 0.5); }
+};
+template <> struct Pix<float> {
+    __device__ static float f(float v) { return v; }
+    __device__ static float store(float v) { return v; }
+    // a NaN sample keeps its payload through the fade product, as on x86
+    __device__ static float faded(float v, float f) { return nr::mul(v, f); }
+};
+
+// warp.rs:178-215 (clip_to_rect), bounded like the reference
+__device__ __forceinline__ bool clip_to_rect(float x, float y, float& ix, float& iy, float w1, float h1) {
+#pragma unroll 1
+    for (int it = 0; it < 4096; it++) {
+        if (ix < 0.0f) {
+            float dy = y - iy, dxs = x - ix, num = x - 0.0f;
+            ix = 0.0f;
+            iy = y - (num / dxs) * dy;
+            continue;
+        }
+        if (ix > w1) {
+            float dy = y - iy, dxs = x - ix, num = x - w1;
+            ix = w1;
+            iy = y - (num / dxs) * dy;
+            continue;
+        }
+        if (iy < 0.0f) {
+            float dyy = y - iy, num = y - 0.0f, dx = x - ix;
+            ix = x - (num / dyy) * dx;
+            iy = 0.0f;
+            continue;
+        }
+        if (iy > h1) {
+            float dyy = y - iy, num = y - h1, dx = x - ix;
+            ix = x - (num / dyy) * dx;
+            iy = h1;
+            continue;
+        }
+        return true;
+    }
+    return false;
+}
+
+// warp.rs:290-360 (bilerp4 + mix4 with the NaN rule repeat of the float depth)
+template <typename P>
+__device__ __forceinline__ void bilerp4(const P* __restrict__ src, int w, int w1, int h1, float x, float y, float o[4]) {
+    int ix = cvtt32(x), iy = cvtt32(y);
+    float fx = x - (float)ix, fy = y - (float)iy;
+    if (ix >= w1) { ix = w1 - 1; fx = 1.0f; }
+    if (iy >= h1) { iy = h1 - 1; fy = 1.0f; }
+    long i00 = ((long)iy * w + ix) * 4;
+    long i01 = i00 + (long)w * 4;
+    P a[4], b[4], c[4], d[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        a[k] = src[i00 + k];
+        b[k] = src[i00 + 4 + k];
+        c[k] = src[i01 + k];
+        d[k] = src[i01 + 4 + k];
+    }
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float p00 = Pix<P>::f(a[k]), p10 = Pix<P>::f(b[k]), p01 = Pix<P>::f(c[k]), p11 = Pix<P>::f(d[k]);
+        float top = p00 + (p10 - p00) * fx;
+        float bot = p01 + (p11 - p01) * fx;
+        o[k] = top + (bot - top) * fy;
+        any = any || isnan(o[k]);
+    }
+    if (any) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            float p00 = Pix<P>::f(a[k]), p10 = Pix<P>::f(b[k]), p01 = Pix<P>::f(c[k]), p11 = Pix<P>::f(d[k]);
+            float top = nr::add(p00, nr::mul(nr::sub(p10, p00), fx));
+            float bot = nr::add(p01, nr::mul(nr::sub(p11, p01), fx));
+            o[k] = nr::add(top, nr::mul(nr::sub(bot, top), fy));
+        }
+    }
+}
+
+// warp.rs:415-442 (Flow::bilerp) on a strided field
+__device__ __forceinline__ void flow_bilerp(const WarpParams& p, float x, float y, float& du, float& dv) {
+    int fw1 = p.fw - 1, fh1 = p.fh - 1;
+    int ix = cvtt32(x), iy = cvtt32(y);
+    float fx = x - (float)ix, fy = y - (float)iy;
+    if (ix >= fw1) { ix = fw1 - 1; fx = 1.0f; }
+    if (iy >= fh1) { iy = fh1 - 1; fy = 1.0f; }
+    long i00 = ((long)iy * p.fw + ix) * p.fstride;
+    long i01 = i00 + (long)p.fw * p.fstride;
+    long s = p.fstride;
+    const float* planes[2] = {p.fu, p.fv};
+    float r[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const float* d = planes[k];
+        float p00 = __ldg(d + i00), p10 = __ldg(d + i00 + s), p01 = __ldg(d + i01), p11 = __ldg(d + i01 + s);
+        float top = (p10 - p00) * fx + p00;
+        float bot = (p11 - p01) * fx + p01;
+        r[k] = (bot - top) * fy + top;
+    }
+    du = r[0];
+    dv = r[1];
+}
+
+// One output pixel of the inverse warp (warp.rs:466-561, Kernel::row / pixel_hold / pixel_fade).
+// Returns the coverage byte; sets bad for a coordinate the reference refuses.
+template <typename P>
+__device__ __forceinline__ uint8_t warp_pixel(const WarpParams& p, int x, int y, int w, int h, P o[4], bool& bad) {
+    const P* src = (const P*)p.src;
+    if (p.copy_only) {
+        const P* s = src + ((long)y * w + x) * 4;
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = s[k];
+        return 255;
+    }
+    int w1i = w - 1, h1i = h - 1;
+    float rx = (float)(p.fw - 1) / (float)w1i;
+    float ry = (float)(p.fh - 1) / (float)h1i;
+    float sx = p.amount / rx, sy = p.amount / ry;
+    float wf = (float)w, hf = (float)h, w1 = (float)w1i, h1 = (float)h1i;
+    float xf = (float)x, yf = (float)y;
+    float du, dv;
+    flow_bilerp(p, xf * rx, yf * ry, du, dv);
+    float ix = du * sx + xf;
+    float iy = dv * sy + yf;
+    float s[4];
+    if (p.hold) {
+        if (!clip_to_rect(xf, yf, ix, iy, w1, h1) || isnan(ix) || isnan(iy)) {
+            bad = true;
+#pragma unroll
+            for (int k = 0; k < 4; k++) o[k] = P(0);
+            return 255;
+        }
+        bilerp4<P>(src, w, w1i, h1i, ix, iy, s);
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = Pix<P>::store(s[k]);
+        return 255;
+    }
+    if (!(ix > -1.0f && ix < wf && iy > -1.0f && iy < hf)) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = P(0);
+        return 0;
+    }
+    if (ix >= 0.0f && ix <= w1 && iy >= 0.0f && iy <= h1) {
+        bilerp4<P>(src, w, w1i, h1i, ix, iy, s);
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = Pix<P>::store(s[k]);
+        return 255;
+    }
+    float f = ix < 0.0f ? ix + 1.0f : (ix <= w1 ? 1.0f : wf - ix);
+    if (iy < 0.0f) f *= iy + 1.0f;
+    else if (iy > h1) f *= hf - iy;
+    if (!clip_to_rect(xf, yf, ix, iy, w1, h1) || isnan(ix) || isnan(iy)) {
+        bad = true;
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = P(0);
+        return 0;
+    }
+    bilerp4<P>(src, w, w1i, h1i, ix, iy, s);
+#pragma unroll
+    for (int k = 0; k < 4; k++) o[k] = Pix<P>::faded(s[k], f);
+    float c = f * 255.0f + 0.5f;
+    return c <= 255.0f ? (uint8_t)cvtt64d((double)c) : (uint8_t)255;
+}
+
+template <typename P>
+__device__ __forceinline__ void inv_warp_px(const WarpParams& p, void* out, uint8_t* cov, int w, int h, int* bad) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    P o[4];
+    bool b = false;
+    uint8_t c = warp_pixel<P>(p, x, y, w, h, o, b);
+    P* dst = (P*)out + ((long)y * w + x) * 4;
+#pragma unroll
+    for (int k = 0; k < 4; k++) dst[k] = o[k];
+    if (cov) cov[(long)y * w + x] = c;
+    if (b) atomicOr(bad, 1);
+}
+
+__global__ void k_inv_warp(WarpParams p, int fmt, void* __restrict__ out, uint8_t* __restrict__ cov, int w, int h,
+                           int* __restrict__ bad) {
+    if (fmt == 0) inv_warp_px<uint8_t>(p, out, cov, w, h, bad);
+    else if (fmt == 1) inv_warp_px<uint16_t>(p, out, cov, w, h, bad);
+    else inv_warp_px<float>(p, out, cov, w, h, bad);
+}
+
+// ---- blend and lerp (blend.rs) -----------------------------------------------------------------------
+
+// blend.rs:81-114, the common branch of one sample
+template <typename P> __device__ __forceinline__ P blend_sample(P a, P b, float w);
+template <> __device__ __forceinline__ uint8_t blend_sample<uint8_t>(uint8_t a, uint8_t b, float w) {
+    float af = (float)a, bf = (float)b;
+    return (uint8_t)cvtt64f((bf - af) * w + af + 0.5f);
+}
+template <> __device__ __forceinline__ uint16_t blend_sample<uint16_t>(uint16_t a, uint16_t b, float w) {
+    float af = (float)a, bf = (float)b;
+    return (uint16_t)cvtt64f((bf - af) * w + af + 0.5f);
+}
+template <> __device__ __forceinline__ float blend_sample<float>(float a, float b, float w) {
+    float r = (b - a) * w + a + 0.0f;
+    if (isnan(r)) r = nr::add(nr::add(nr::mul(nr::sub(b, a), w), a), 0.0f);
+    return r;
+}
+
+// blend.rs:214-249 (lerp_pixel_int) and :182-211 (lerp_pixel_f32): first = second + (first - second) * w
+template <typename P> __device__ __forceinline__ void lerp_px(P f[4], const P s[4], float w);
+template <typename T>
+__device__ __forceinline__ void lerp_px_int(T f[4], const T s[4], float w, float scale) {
+    auto diff = [&](int i) { return (float)((int32_t)f[i] - (int32_t)s[i]); };
+    auto sf = [&](int i) { return (float)(int32_t)s[i]; };
+    float a = diff(0) * w + sf(0);
+    float n = a / scale;
+    if (!(n > 0.0f)) {
+        T z = (T)cvtt64f(0.0f);
+#pragma unroll
+        for (int i = 0; i < 4; i++) f[i] = z;
+        return;
+    }
+    float r = diff(1) * w + sf(1), g = diff(2) * w + sf(2), b = diff(3) * w + sf(3);
+    if (n > 1.0f) { r = r / n; g = g / n; b = b / n; a = scale; }
+    auto clamp = [&](float c) { return c > a ? a : (0.0f > c ? 0.0f : c); };
+    r = clamp(r); g = clamp(g); b = clamp(b);
+    f[1] = (T)cvtt64f(r + 0.5f);
+    f[2] = (T)cvtt64f(g + 0.5f);
+    f[3] = (T)cvtt64f(b + 0.5f);
+    f[0] = (T)cvtt64f(a + 0.5f);
+}
+template <> __device__ __forceinline__ void lerp_px<uint8_t>(uint8_t f[4], const uint8_t s[4], float w) {
+    lerp_px_int<uint8_t>(f, s, w, 255.0f);
+}
+template <> __device__ __forceinline__ void lerp_px<uint16_t>(uint16_t f[4], const uint16_t s[4], float w) {
+    lerp_px_int<uint16_t>(f, s, w, 65535.0f);
+}
+template <> __device__ __forceinline__ void lerp_px<float>(float f[4], const float s[4], float w) {
+    bool rule = false;
+#pragma unroll
+    for (int i = 0; i < 4; i++) rule = rule || isnan(f[i]) || isnan(s[i]);
+    if (!rule) {
+        float a = (f[0] - s[0]) * w + s[0];
+        if (!(a > 0.0f)) { for (int i = 0; i < 4; i++) f[i] = 0.0f; return; }
+        float r = (f[1] - s[1]) * w + s[1], g = (f[2] - s[2]) * w + s[2], b = (f[3] - s[3]) * w + s[3];
+        if (a > 1.0f) { r = r / a; g = g / a; b = b / a; a = 1.0f; }
+        f[1] = r + 0.0f; f[2] = g + 0.0f; f[3] = b + 0.0f; f[0] = a + 0.0f;
+    } else {
+        auto L = [](float a, float b, float w) { return nr::add(nr::mul(nr::sub(b, a), w), a); };
+        float a = L(s[0], f[0], w);
+        if (!(a > 0.0f)) { for (int i = 0; i < 4; i++) f[i] = 0.0f; return; }
+        float r = L(s[1], f[1], w), g = L(s[2], f[2], w), b = L(s[3], f[3], w);
+        if (a > 1.0f) { r = nr::div(r, a); g = nr::div(g, a); b = nr::div(b, a); a = 1.0f; }
+        f[1] = nr::add(r, 0.0f); f[2] = nr::add(g, 0.0f); f[3] = nr::add(b, 0.0f); f[0] = nr::add(a, 0.0f);
+    }
+}
+
+// blend.rs:55-78 (blend with its branches) on one pixel: mode 0 common, 1 copy a, 2 copy b,
+// 3 copy a then lerp(out, b, wl) with its w == 1 / w == 0 early outs
+template <typename P>
+__device__ __forceinline__ void blend_px(const P a[4], const P b[4], float w, float wl, int mode, P o[4]) {
+    if (mode == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = blend_sample<P>(a[k], b[k], w);
+    } else if (mode == 1) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = a[k];
+    } else if (mode == 2) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = b[k];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = a[k];
+        if (wl == 1.0f) return;
+        if (wl == 0.0f) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) o[k] = b[k];
+            return;
+        }
+        lerp_px<P>(o, b, wl);
+    }
+}
+
+__global__ void k_blend(const void* __restrict__ a, const void* __restrict__ b, void* __restrict__ out, int fmt,
+                        long nsamples, float w) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsamples) return;
+    if (fmt == 0) ((uint8_t*)out)[i] = blend_sample<uint8_t>(((const uint8_t*)a)[i], ((const uint8_t*)b)[i], w);
+    else if (fmt == 1) ((uint16_t*)out)[i] = blend_sample<uint16_t>(((const uint16_t*)a)[i], ((const uint16_t*)b)[i], w);
+    else ((float*)out)[i] = blend_sample<float>(((const float*)a)[i], ((const float*)b)[i], w);
+}
+
+template <typename P>
+__device__ __forceinline__ void lerp_one(void* first, const void* second, long i, float w) {
+    P f[4], s[4];
+    P* fp = (P*)first + i * 4;
+    const P* sp = (const P*)second + i * 4;
+#pragma unroll
+    for (int k = 0; k < 4; k++) { f[k] = fp[k]; s[k] = sp[k]; }
+    lerp_px<P>(f, s, w);
+#pragma unroll
+    for (int k = 0; k < 4; k++) fp[k] = f[k];
+}
+
+__global__ void k_lerp(void* __restrict__ first, const void* __restrict__ second, int fmt, long npx, float w) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npx) return;
+    if (fmt == 0) lerp_one<uint8_t>(first, second, i, w);
+    else if (fmt == 1) lerp_one<uint16_t>(first, second, i, w);
+    else lerp_one<float>(first, second, i, w);
+}
+
+// ---- the fused Blend composition of warping code 0 ---------------------------------------------------
+
+template <typename P>
+__device__ __forceinline__ void store_px(const P o[4], void* out, long i, bool to_wire, long npx);
+template <>
+__device__ __forceinline__ void store_px<uint8_t>(const uint8_t o[4], void* out, long i, bool to_wire, long npx) {
+    uchar4 e = make_uchar4(o[0], o[1], o[2], o[3]);
+    reinterpret_cast<uchar4*>(out)[i] = to_wire ? unpremul_u8(e) : e;
+}
+template <>
+__device__ __forceinline__ void store_px<uint16_t>(const uint16_t o[4], void* out, long i, bool to_wire, long npx) {
+    ushort4 e = make_ushort4(o[0], o[1], o[2], o[3]);
+    reinterpret_cast<ushort4*>(out)[i] = to_wire ? unpremul_u16(e) : e;
+}
+template <>
+__device__ __forceinline__ void store_px<float>(const float o[4], void* out, long i, bool to_wire, long npx) {
+    float4 e = make_float4(o[0], o[1], o[2], o[3]);
+    if (!to_wire) {
+        reinterpret_cast<float4*>(out)[i] = e;
+        return;
+    }
+    float4 u = unpremul_f32(e);
+    float* wire = (float*)out;
+    wire[i] = u.z;
+    wire[npx + i] = u.w;
+    wire[2 * npx + i] = u.y;
+    wire[3 * npx + i] = u.x;
+}
+
+template <typename P>
+__device__ __forceinline__ void compose_blend_px(const WarpParams& pa, const WarpParams& pb, float wblend, int mode,
+                                                 void* out, int w, int h, bool to_wire, bool flip_out, int* bad) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    // the output pixel (x, y) of the engine image lands on wire row h-1-y when flip_out
+    P ta[4], tb[4], o[4];
+    bool b = false;
+    if (mode != 2) warp_pixel<P>(pa, x, y, w, h, ta, b);
+    if (mode != 1) warp_pixel<P>(pb, x, y, w, h, tb, b);
+    float wl = (float)(1.0 - (double)wblend);
+    blend_px<P>(ta, tb, wblend, wl, mode, o);
+    int oy = flip_out ? h - 1 - y : y;
+    store_px<P>(o, out, (long)oy * w + x, to_wire, (long)w * h);
+    if (b) atomicOr(bad, 1);
+}
+
+__global__ void k_compose_blend(WarpParams pa, WarpParams pb, int fmt, float wblend, int blend_mode, void* __restrict__ out,
+                                int w, int h, bool to_wire, bool flip_out, int* __restrict__ bad) {
+    if (fmt == 0) compose_blend_px<uint8_t>(pa, pb, wblend, blend_mode, out, w, h, to_wire, flip_out, bad);
+    else if (fmt == 1) compose_blend_px<uint16_t>(pa, pb, wblend, blend_mode, out, w, h, to_wire, flip_out, bad);
+    else compose_blend_px<float>(pa, pb, wblend, blend_mode, out, w, h, to_wire, flip_out, bad);
+}
+
+}  // namespace tw

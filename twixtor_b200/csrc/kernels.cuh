@@ -1,0 +1,103 @@
+// Declarations of the library's sm_100a kernels (strict mode) and their small device helpers.
+//
+// Layout in HBM: every multi channel buffer of the solver is PLANAR (one float plane per channel,
+// row major, pitch = width), so each pass streams coalesced lanes and the separable filter runs
+// the same code on each plane. The reference's interleaved layout only changes where samples
+// live, never the arithmetic of an element, so results are bit identical. Engine images keep the
+// reference's interleaved A, R, G, B samples (one 32-bit word per 8 bpc pixel).
+#pragma once
+#include <cstdint>
+
+#include "strict.cuh"
+
+namespace tw {
+
+constexpr int MAX_TAPS = 8;  // Gaussian r=7 has 8 half taps (flow/conv.rs:64-86)
+
+struct Taps {
+    float k[MAX_TAPS];
+    int n;
+};
+
+// ---- image boundary and luma (image.rs, prep.rs) -------------------------------------------------
+// wire -> engine, optionally reading the wire rows bottom up (the motion path's row order)
+__global__ void k_from_frame_u8(const uint8_t* __restrict__ wire, uint8_t* __restrict__ eng, int w, int h, bool flip);
+__global__ void k_from_frame_u16(const uint16_t* __restrict__ wire, uint16_t* __restrict__ eng, int w, int h, bool flip);
+__global__ void k_from_frame_f32(const float* __restrict__ wire, float* __restrict__ eng, int w, int h, bool flip);
+// engine -> wire, optionally reading the engine rows bottom up
+__global__ void k_to_frame_u8(const uint8_t* __restrict__ eng, uint8_t* __restrict__ wire, int w, int h, bool flip);
+__global__ void k_to_frame_u16(const uint16_t* __restrict__ eng, uint16_t* __restrict__ wire, int w, int h, bool flip);
+__global__ void k_to_frame_f32(const float* __restrict__ eng, float* __restrict__ wire, int w, int h, bool flip);
+__global__ void k_luma(const void* __restrict__ eng, int fmt, float* __restrict__ out, int w, int h, bool track_alpha,
+                       bool video_range);
+
+// ---- separable filters and resampling (flow/conv.rs, flow/sample.rs) -------------------------------
+__global__ void k_conv_h(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t, bool multi);
+// vertical pass; when band != nullptr it also writes band = orig - result (flow.rs:266-267)
+__global__ void k_conv_v(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t, bool multi,
+                         bool above_first, const float* __restrict__ orig, float* __restrict__ band);
+__global__ void k_resample(const float* __restrict__ src, int sw, int sh, float* __restrict__ dst, int dw, int dh);
+
+// ---- solver (flow.rs:277-442) ------------------------------------------------------------------------
+// gradient (2 planes) and structure tensor (3 planes)
+__global__ void k_grad_tensor(const float* __restrict__ img, int w, int h, float* __restrict__ gx,
+                              float* __restrict__ gy, float* __restrict__ a0, float* __restrict__ a1,
+                              float* __restrict__ a2);
+__global__ void k_calc_b(const float* __restrict__ i1, const float* __restrict__ i0, const float* __restrict__ gx,
+                         const float* __restrict__ gy, const float* __restrict__ fu, const float* __restrict__ fv,
+                         int w, int h, float* __restrict__ bx, float* __restrict__ by);
+__global__ void k_new_disp(float* __restrict__ fu, float* __restrict__ fv, const float* __restrict__ a0,
+                           const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ bx,
+                           const float* __restrict__ by, long n);
+// sets *any_in_range when some pixel's x + u, y + v lies inside the level (flow.rs:430-442)
+__global__ void k_range_any(const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,
+                            int* __restrict__ any_in_range);
+// the range reset while the check is live, then the damping of the start level (flow.rs:1292-1300)
+__global__ void k_range_apply(float* __restrict__ fu, float* __restrict__ fv, long n, int* __restrict__ state,
+                              bool damp_now, float damp);
+__global__ void k_range_init(int* __restrict__ state);
+__global__ void k_range_next(int* __restrict__ state);
+__global__ void k_upsample_flow(const float* __restrict__ su, const float* __restrict__ sv, int sw, int sh,
+                                float* __restrict__ du, float* __restrict__ dv, int dw, int dh);
+// the final negation (flow.rs:1305) into the interleaved FlowField layout
+__global__ void k_negate_interleave(const float* __restrict__ fu, const float* __restrict__ fv, long n,
+                                    float* __restrict__ out, int* __restrict__ nan_flag);
+__global__ void k_fill(float* __restrict__ p, long n, float v);
+__global__ void k_deinterleave(const float* __restrict__ in, long n, float* __restrict__ fu, float* __restrict__ fv);
+__global__ void k_interleave(const float* __restrict__ fu, const float* __restrict__ fv, long n, float* __restrict__ out);
+
+// block matching (flow.rs:447-622): the four in-place sweeps; one CTA per row or column
+__global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
+                          float* __restrict__ fv, int w, int h, bool reverse);
+__global__ void k_bm_cols(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
+                          float* __restrict__ fv, int w, int h, bool reverse);
+size_t bm_smem_bytes(int len);
+
+// ---- warps and blends (warp.rs, blend.rs) ------------------------------------------------------------
+struct WarpParams {
+    const void* src;     // engine image
+    const float* fu;     // flow u (element stride fstride)
+    const float* fv;
+    int fstride;
+    int fw, fh;
+    float amount;
+    bool copy_only;      // the |amount| early outs of inv_warp (warp.rs:751-764)
+    bool hold;
+};
+// out = inv_warp(src, flow, amount); optional coverage
+__global__ void k_inv_warp(WarpParams p, int fmt, void* __restrict__ out, uint8_t* __restrict__ cov, int w, int h,
+                           int* __restrict__ bad);
+// out = blend(a, b, w) for the common branch (blend.rs:81-114); the snap / extrapolation branches
+// are decided on the host
+__global__ void k_blend(const void* __restrict__ a, const void* __restrict__ b, void* __restrict__ out, int fmt,
+                        long nsamples, float w);
+// lerp(first, second, w) in place (blend.rs:144-258)
+__global__ void k_lerp(void* __restrict__ first, const void* __restrict__ second, int fmt, long npx, float w);
+
+// The fused Blend composition of warping code 0 (compose/vector.rs:262-276): both inverse warps,
+// the blend and (to_wire) the unpremultiply + wire store of the finish, rows optionally read
+// bottom up on the way out. `blend_mode`: 0 common branch, 1 copy of tA, 2 copy of tB.
+__global__ void k_compose_blend(WarpParams pa, WarpParams pb, int fmt, float wblend, int blend_mode, void* __restrict__ out,
+                                int w, int h, bool to_wire, bool flip_out, int* __restrict__ bad);
+
+}  // namespace tw

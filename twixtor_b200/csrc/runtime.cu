@@ -1,0 +1,957 @@
+// Host runtime of the library: the device context, its buffers, the solve and compose pipelines
+// and the extern "C" entry points declared in include/twixtor_b200.h.
+//
+// Host scalars that the reference computes with the C runtime's libm (the start level, flow.rs:
+// 179-197, and the Gaussian taps, flow/conv.rs:58-86) are computed here with the same glibc
+// pow/log, exactly as the reference does on its host; every per-element operation runs in the
+// kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/twixtor_b200.h"
+#include "kernels.cuh"
+
+using namespace tw;
+
+namespace {
+
+// ---- host geometry (prep.rs:63-146, flow.rs:129-197) ---------------------------------------------
+
+struct Geo {
+    int reduction = 0, w = 0, h = 0, levels = 0;
+    int sizes[32][2];
+};
+
+void flow_resolution(int q, bool hiq, int w, int h, int* r_out, int* w0, int* h0) {
+    int r = (q <= 2) ? 3 : (q == 3) ? 2 : (q == 4) ? 1 : 0;
+    if (!hiq) r = (r == 0) ? 1 : (r == 1) ? 2 : (r == 2) ? 3 : r;
+    while (r > 0 && ((w >> r) < 2 || (h >> r) < 2)) r -= 1;
+    int ww = w, hh = h;
+    for (int i = 0; i < r; i++) { ww /= 2; hh /= 2; }
+    *r_out = r; *w0 = ww; *h0 = hh;
+}
+
+int level_count(int w0, int h0, int min_size) {
+    int levels = 1, w = w0, h = h0;
+    for (;;) {
+        w /= 2;
+        if (w < min_size) break;
+        h /= 2;
+        if (h < min_size) break;
+        if (w > 2 && h > 2 && !(w == 2 && h == 2)) levels += 1;
+        else break;
+    }
+    return levels;
+}
+
+int geometry(const tw_flow_settings& s, int w, int h, Geo* g, std::string* err) {
+    if (s.quality <= 0 || s.quality > 5) { *err = "flow quality is outside 1..=5 (0 disables the estimator)"; return TW_ERR_BAD_PARAM; }
+    if (!(s.sensitivity >= 0.0f) || !std::isfinite(s.sensitivity)) { *err = "sensitivity must be finite and not negative"; return TW_ERR_BAD_PARAM; }
+    flow_resolution(s.quality, s.hiq != 0, w, h, &g->reduction, &g->w, &g->h);
+    if (g->w < 2 || g->h < 2) { *err = "optical flow: working size below 2x2 is not supported"; return TW_ERR_UNSUPPORTED; }
+    g->levels = std::min(level_count(g->w, g->h, 2), 32);
+    int lw = g->w, lh = g->h;
+    for (int i = 0; i < g->levels; i++) {
+        g->sizes[i][0] = lw;
+        g->sizes[i][1] = lh;
+        lw = std::max(lw / 2, 2);
+        lh = std::max(lh / 2, 2);
+    }
+    return TW_OK;
+}
+
+void start_level(float sensitivity, int levels, int* start, float* damp) {  // flow.rs:179-197
+    float p = (float)std::pow((double)sensitivity, 2.0);
+    float l1 = (float)std::log((double)p);
+    float l2 = (float)std::log(2.0);
+    float lv = (float)levels;
+    float x = l1 / l2 + lv;
+    if (0.0f <= x || std::isnan(x)) {
+        if (x < lv || std::isnan(x)) {
+            float f = std::floor(x);
+            int s = (std::isnan(f) || f >= 2147483648.0f || f < -2147483648.0f) ? INT32_MIN : (int)f;
+            int su = s < 0 ? 0 : s;
+            *start = std::min(su, levels - 1);
+            *damp = x - (float)su;
+        } else {
+            *start = levels - 1;
+            *damp = 1.0f;
+        }
+    } else {
+        *start = 0;
+        *damp = 0.0f;
+    }
+}
+
+Taps gaussian_taps(float r) {  // flow/conv.rs:64-86
+    Taps t{};
+    int ri = std::isnan(r) ? 0 : (int)r;
+    int n = std::max(ri + 1, 0);
+    n = std::min(n, MAX_TAPS);
+    float s3 = r / 3.0f;
+    float d = s3 * s3;
+    float sum = 0.0f;
+    for (int i = 0; i < n; i++) {
+        float fi = (float)i;
+        float tt = fi * fi;
+        float e = -(tt / d);
+        float v = (float)std::pow(2.0, (double)e);
+        t.k[i] = v;
+        sum += v;
+    }
+    t.n = n;
+    if (n == 0) return t;
+    float den = sum * 2.0f - t.k[0];
+    for (int i = 0; i < n; i++) t.k[i] /= den;
+    return t;
+}
+
+Taps binomial5() {  // flow/conv.rs:48
+    Taps t{};
+    t.k[0] = 0.375f;
+    t.k[1] = 0.25f;
+    t.k[2] = 0.0625f;
+    t.n = 3;
+    return t;
+}
+
+size_t sample_bytes(int fmt) { return fmt == TW_U8 ? 1 : fmt == TW_U16 ? 2 : 4; }
+
+// ---- device buffers --------------------------------------------------------------------------------
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n, size_t* held) {
+        if (n <= cap) return cudaSuccess;
+        if (p) { cudaFree(p); *held -= cap; p = nullptr; cap = 0; }
+        size_t want = std::max(n, (size_t)256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) { cap = want; *held += want; }
+        return e;
+    }
+    void release(size_t* held) {
+        if (p) { cudaFree(p); *held -= cap; }
+        p = nullptr;
+        cap = 0;
+    }
+    template <typename T> T* as() const { return (T*)p; }
+};
+
+}  // namespace
+
+struct tw_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string err;
+    uint64_t launches = 0;
+    size_t held = 0;
+    Taps g7{}, g5{}, b5{};
+    // engine images, wire staging, pyramids, solve work, flows
+    DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags;
+    DevBuf host_stage;  // unused placeholder for pinned staging
+
+    int fail(int code, const char* fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        err = buf;
+        return code;
+    }
+    int cuda(cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return TW_OK;
+        return fail(TW_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    }
+    int ensure(DevBuf& b, size_t n, const char* what) { return cuda(b.ensure(n, &held), what); }
+};
+
+namespace {
+
+#define LAUNCH(ctx, kernel, grid, block, smem, ...)                                \
+    do {                                                                           \
+        kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);           \
+        (ctx)->launches++;                                                         \
+    } while (0)
+
+#define CHECK(expr)                 \
+    do {                            \
+        int _rc = (expr);           \
+        if (_rc != TW_OK) return _rc; \
+    } while (0)
+
+constexpr int TB = 256;
+
+dim3 grid2(int w, int h) { return dim3((unsigned)((w + TB - 1) / TB), (unsigned)h); }
+unsigned grid1(long n) { return (unsigned)((n + TB - 1) / TB); }
+
+// ---- separable convolution of `c` planes in place (flow/conv.rs: convolve_above_first) --------------
+void conv_planes(tw_ctx* ctx, float* const* planes, int c, int w, int h, const Taps& t, bool above_first, float* tmp) {
+    bool multi = c > 1;
+    for (int i = 0; i < c; i++) {
+        LAUNCH(ctx, k_conv_h, grid2(w, h), TB, 0, planes[i], tmp, w, h, t, multi);
+        LAUNCH(ctx, k_conv_v, grid2(w, h), TB, 0, tmp, planes[i], w, h, t, multi, above_first, (const float*)nullptr,
+               (float*)nullptr);
+    }
+}
+
+// ---- the pyramid of one engine image (flow.rs:242-275) ----------------------------------------------
+// Builds the band pass levels into `out` (levels concatenated, finest first). Scratch: plane[0..3].
+int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, const tw_flow_settings& s, const Geo& g,
+                      float* out) {
+    if (s.prep_contrast_edge || s.prep_delinearize)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "image prep (Contrast/Edge Enhance, Delinearize) is not on the device");
+    if (s.video_range_luma && s.track_alpha)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "optical flow luma: video range conversion together with Track RGB+A is not supported");
+    size_t full = (size_t)W * H * sizeof(float);
+    for (int i = 0; i < 3; i++) CHECK(ctx->ensure(ctx->plane[i], full, "pyramid scratch"));
+    float* cur = ctx->plane[0].as<float>();
+    float* tmp = ctx->plane[1].as<float>();
+    float* nxt = ctx->plane[2].as<float>();
+    long n = (long)W * H;
+    LAUNCH(ctx, k_luma, grid1(n), TB, 0, eng_dev, fmt, cur, W, H, s.track_alpha != 0, s.video_range_luma != 0);
+    int cw = W, ch = H;
+    bool af = s.taps_above_first != 0;
+    for (int r = 0; r < g.reduction; r++) {  // prep.rs:252-259
+        LAUNCH(ctx, k_conv_h, grid2(cw, ch), TB, 0, cur, tmp, cw, ch, ctx->b5, false);
+        LAUNCH(ctx, k_conv_v, grid2(cw, ch), TB, 0, tmp, cur, cw, ch, ctx->b5, false, af, (const float*)nullptr, (float*)nullptr);
+        int nw = cw / 2, nh = ch / 2;
+        LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, cur, cw, ch, nxt, nw, nh);
+        std::swap(cur, nxt);
+        cw = nw;
+        ch = nh;
+    }
+    size_t off = 0;
+    for (int i = 0; i < g.levels; i++) {
+        int lw = g.sizes[i][0], lh = g.sizes[i][1];
+        float* band = out + off;
+        LAUNCH(ctx, k_conv_h, grid2(lw, lh), TB, 0, cur, tmp, lw, lh, ctx->b5, false);
+        LAUNCH(ctx, k_conv_v, grid2(lw, lh), TB, 0, tmp, nxt, lw, lh, ctx->b5, false, af, (const float*)cur, band);
+        if (i + 1 < g.levels) {
+            int nw = g.sizes[i + 1][0], nh = g.sizes[i + 1][1];
+            LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, nxt, lw, lh, cur, nw, nh);
+        }
+        off += (size_t)lw * lh;
+    }
+    return TW_OK;
+}
+
+size_t pyramid_floats(const Geo& g) {
+    size_t n = 0;
+    for (int i = 0; i < g.levels; i++) n += (size_t)g.sizes[i][0] * g.sizes[i][1];
+    return n;
+}
+
+// ---- block matching (flow.rs:551-622) -----------------------------------------------------------------
+void block_match(tw_ctx* ctx, const float* A, const float* B, float* fu, float* fv, int w, int h) {
+    if (w < 3 || h < 3) return;
+    LAUNCH(ctx, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, false);
+    LAUNCH(ctx, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, true);
+    LAUNCH(ctx, k_bm_cols, w - 2, TB, bm_smem_bytes(h), A, B, fu, fv, w, h, false);
+    LAUNCH(ctx, k_bm_cols, w - 2, TB, bm_smem_bytes(h), A, B, fu, fv, w, h, true);
+}
+
+// ---- one solve over two resident pyramids (flow.rs:1258-1307) ------------------------------------------
+// x, y: band pass levels of X and Y; work: scratch for this solve; out: interleaved flow at level 0
+// size (device). nan_flag: set when the result holds a NaN.
+int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const Geo& g, const tw_flow_settings& s,
+                       DevBuf& work, float* out, int* state, int* nan_flag) {
+    size_t np0 = (size_t)g.w * g.h;
+    // planes: gx gy a0 a1 a2 bx by fu fv uu uv tmp
+    const int NP = 12;
+    CHECK(ctx->ensure(work, np0 * NP * sizeof(float), "solve scratch"));
+    float* base = work.as<float>();
+    float *gx = base, *gy = base + np0, *a0 = base + 2 * np0, *a1 = base + 3 * np0, *a2 = base + 4 * np0;
+    float *bx = base + 5 * np0, *by = base + 6 * np0, *fu = base + 7 * np0, *fv = base + 8 * np0;
+    float *uu = base + 9 * np0, *uv = base + 10 * np0, *tmp = base + 11 * np0;
+    int start;
+    float damp;
+    start_level(s.sensitivity, g.levels, &start, &damp);
+    size_t offs[32];
+    size_t off = 0;
+    for (int i = 0; i < g.levels; i++) { offs[i] = off; off += (size_t)g.sizes[i][0] * g.sizes[i][1]; }
+    long ns = (long)g.sizes[start][0] * g.sizes[start][1];
+    LAUNCH(ctx, k_fill, grid1(ns), TB, 0, fu, ns, 0.0f);
+    LAUNCH(ctx, k_fill, grid1(ns), TB, 0, fv, ns, 0.0f);
+    LAUNCH(ctx, k_range_init, 1, 32, 0, state);
+    bool af = s.taps_above_first != 0;
+    bool damp_now_any = std::fabs((double)damp - 1.0) >= 1e-6;
+    for (int l = start; l >= 0; l--) {
+        int w = g.sizes[l][0], h = g.sizes[l][1];
+        long n = (long)w * h;
+        const float* A = x + offs[l];
+        const float* B = y + offs[l];
+        LAUNCH(ctx, k_grad_tensor, grid2(w, h), TB, 0, A, w, h, gx, gy, a0, a1, a2);
+        float* ap[3] = {a0, a1, a2};
+        conv_planes(ctx, ap, 3, w, h, ctx->g7, af, tmp);
+        for (int it = 0; it < 3; it++) {
+            LAUNCH(ctx, k_calc_b, grid2(w, h), TB, 0, A, B, gx, gy, fu, fv, w, h, bx, by);
+            float* bp[2] = {bx, by};
+            conv_planes(ctx, bp, 2, w, h, ctx->g7, af, tmp);
+            LAUNCH(ctx, k_new_disp, grid1(n), TB, 0, fu, fv, a0, a1, a2, bx, by, n);
+            float* fp[2] = {fu, fv};
+            conv_planes(ctx, fp, 2, w, h, ctx->g5, af, tmp);
+            if (it == 1 && l == 0 && !s.skip_refine) block_match(ctx, A, B, fu, fv, w, h);
+        }
+        if (l != 0 && !s.skip_refine) block_match(ctx, A, B, fu, fv, w, h);
+        LAUNCH(ctx, k_range_any, grid2(w, h), TB, 0, fu, fv, w, h, state + 1);
+        LAUNCH(ctx, k_range_apply, grid1(n), TB, 0, fu, fv, n, state, l == start && damp_now_any, damp);
+        LAUNCH(ctx, k_range_next, 1, 32, 0, state);
+        if (l > 0) {
+            int nw = g.sizes[l - 1][0], nh = g.sizes[l - 1][1];
+            LAUNCH(ctx, k_upsample_flow, grid2(nw, nh), TB, 0, fu, fv, w, h, uu, uv, nw, nh);
+            std::swap(fu, uu);
+            std::swap(fv, uv);
+        }
+    }
+    LAUNCH(ctx, k_negate_interleave, grid1((long)np0), TB, 0, fu, fv, (long)np0, out, nan_flag);
+    return TW_OK;
+}
+
+bool same_shape(const tw_image* a, const tw_image* b) {
+    return a->width == b->width && a->height == b->height && a->fmt == b->fmt;
+}
+
+int check_image(tw_ctx* ctx, const tw_image* im, const char* what) {
+    if (!im || !im->data) return ctx->fail(TW_ERR_MISMATCH, "%s: no image", what);
+    if (im->fmt < 0 || im->fmt > 2) return ctx->fail(TW_ERR_BAD_PARAM, "%s: format %d is not 0..2", what, im->fmt);
+    if (im->width <= 0 || im->height <= 0) return ctx->fail(TW_ERR_MISMATCH, "%s: empty image", what);
+    return TW_OK;
+}
+
+// blend.rs:55-78: which branch blend(out, a, b, w) takes
+int blend_mode(float w) {
+    if (0.005 > (double)std::fabs(w)) return 1;
+    if (0.005 > std::fabs((double)w - 1.0)) return 2;
+    if (w < 0.0f || w > 1.0f) return 3;
+    return 0;
+}
+
+// warp.rs:751-764: the |amount| early outs of inv_warp (a plain copy)
+bool warp_copy_only(float amount, int fw, int width) {
+    float a = amount < 0.0f ? -amount : amount;
+    if (0.005 > (double)a) return true;
+    float r = (float)(fw - 1) / (float)(width - 1);
+    float q = (float)((double)amount / (double)r);
+    if (q < 0.0f) q = -q;
+    return 0.0001 > (double)q;
+}
+
+WarpParams warp_params(const void* src, const float* flow_interleaved, int fw, int fh, float amount, int width, bool hold) {
+    WarpParams p{};
+    p.src = src;
+    p.fu = flow_interleaved;
+    p.fv = flow_interleaved ? flow_interleaved + 1 : nullptr;
+    p.fstride = 2;
+    p.fw = fw;
+    p.fh = fh;
+    p.amount = amount;
+    p.hold = hold;
+    p.copy_only = flow_interleaved ? warp_copy_only(amount, fw, width) : true;
+    return p;
+}
+
+// compose_vectors for warping code 0 (compose/vector.rs:209-284) plus the fast path blends
+// (compose.rs:218-231), all as one fused kernel launch. eng_a/eng_b/f_ab/f_ba are device pointers.
+int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& sel, const void* eng_a,
+                const void* eng_b, const float* f_ab, const float* f_ba, int fw, int fh, int W, int H, int fmt,
+                void* out, bool to_wire, bool flip_out, int* bad) {
+    if (cs.warp_mode != 0)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "warping code %d (Smart Blend / forward warp) is not on the device yet", cs.warp_mode);
+    if (cs.wrap_360) return ctx->fail(TW_ERR_UNSUPPORTED, "the 360 inverse warp is not on the device");
+    if (W < 2 || H < 2 || fw < 2 || fh < 2)
+        return ctx->fail(TW_ERR_MISMATCH, "inverse warp needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W, H, fw, fh);
+    // blur compensation (warp/blurcomp.rs:33-40): runs only when |s0 - s1| > 1e-6 and blur > 0.005
+    float d = std::fabs(sel.s0 - sel.s1);
+    if ((double)d > 1e-6 && (double)cs.blur > 0.005)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "blur compensation is not on the device yet");
+    float wa = sel.wa;
+    float frac = 1.0f - wa;
+    WarpParams pa{}, pb{};
+    float wb = 0.0f;
+    int mode;
+    if (sel.interp == 0) {
+        bool use_ab = (wa < 0.5f && (unsigned)cs.warp_mode < 2) || (0.5f <= wa && (unsigned)cs.warp_mode > 1);
+        const float* flow = use_ab ? f_ab : f_ba;
+        if (!flow) return ctx->fail(TW_ERR_MISMATCH, "the composition needs the flow %s but it was not computed", use_ab ? "F_AB" : "F_BA");
+        if (0.5f <= wa) pa = warp_params(eng_a, flow, fw, fh, frac, W, true);
+        else pa = warp_params(eng_b, flow, fw, fh, wa, W, true);
+        pb = pa;
+        mode = 1;
+    } else if (sel.interp == 1) {
+        if (!f_ab || !f_ba) return ctx->fail(TW_ERR_MISMATCH, "the composition needs both flows");
+        pa = warp_params(eng_a, f_ba, fw, fh, frac, W, true);
+        pb = warp_params(eng_b, f_ab, fw, fh, wa, W, true);
+        wb = frac;
+        mode = blend_mode(frac);
+    } else if (sel.interp == 2) {
+        return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend on the vector path is not on the device yet");
+    } else {
+        return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
+    }
+    LAUNCH(ctx, k_compose_blend, grid2(W, H), TB, 0, pa, pb, fmt, wb, mode, out, W, H, to_wire, flip_out, bad);
+    return TW_OK;
+}
+
+// compose.rs:218-231 (interpolate): the fast path without flows
+int interpolate_dev(tw_ctx* ctx, const tw_selection& sel, const void* eng_a, const void* eng_b, int W, int H, int fmt,
+                    void* out, bool to_wire, int* bad) {
+    WarpParams pa = warp_params(eng_a, nullptr, 0, 0, 0.0f, W, true);
+    WarpParams pb = warp_params(eng_b, nullptr, 0, 0, 0.0f, W, true);
+    int mode;
+    float wb = 0.0f;
+    if (sel.interp == 0) {
+        mode = sel.wa >= 0.5f ? 1 : 2;
+    } else if (sel.interp == 1) {
+        wb = (float)(1.0 - (double)sel.wa);
+        mode = blend_mode(wb);
+    } else if (sel.interp == 2) {
+        // blend.rs:281-302: equals blend(a, b, 1 - wa) for 8 and 16 bpc
+        if (fmt == TW_F32)
+            return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend without flows of float frames is not on the device yet");
+        wb = 1.0f - sel.wa;
+        mode = blend_mode(wb);
+    } else {
+        return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
+    }
+    LAUNCH(ctx, k_compose_blend, grid2(W, H), TB, 0, pa, pb, fmt, wb, mode, out, W, H, to_wire, false, bad);
+    return TW_OK;
+}
+
+__global__ void k_selfcheck(int* out) {
+    // the x86 truncation rules the strict kernels rely on
+    float vals[6] = {-2.5f, 2.5f, 2147483648.0f, -2147483904.0f, __int_as_float(0x7fc00000), -0.0f};
+    int want[6] = {-2, 2, INT32_MIN, INT32_MIN, INT32_MIN, 0};
+    int ok = 1;
+    for (int i = 0; i < 6; i++) ok &= cvtt32(vals[i]) == want[i];
+    ok &= sat_u8(300.0f) == 255 && sat_u8(-3.0f) == 0 && sat_u8(__int_as_float(0x7fc00000)) == 255;
+    ok &= qround(254.5f) == 255;
+    out[0] = ok;
+}
+
+}  // namespace
+
+// =======================================================================================================
+// extern "C"
+
+extern "C" {
+
+int tw_open(int device, tw_ctx** out) {
+    if (!out) return TW_ERR_BAD_PARAM;
+    *out = nullptr;
+    tw_ctx* ctx = new tw_ctx();
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { delete ctx; return TW_ERR_CUDA; }
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete ctx; return TW_ERR_CUDA; }
+    ctx->g7 = gaussian_taps(7.0f);
+    ctx->g5 = gaussian_taps(5.0f);
+    ctx->b5 = binomial5();
+    // block matching keeps one line of the field in shared memory (up to 8192 elements)
+    cudaFuncSetAttribute(k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(8192));
+    cudaFuncSetAttribute(k_bm_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(8192));
+    if (ctx->ensure(ctx->flags, 64, "flags") != TW_OK) { tw_close(ctx); return TW_ERR_CUDA; }
+    k_selfcheck<<<1, 1, 0, ctx->stream>>>(ctx->flags.as<int>());
+    ctx->launches++;
+    int ok = 0;
+    e = cudaMemcpyAsync(&ok, ctx->flags.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess || ok != 1) { tw_close(ctx); return e != cudaSuccess ? TW_ERR_CUDA : TW_ERR_UNSUPPORTED; }
+    *out = ctx;
+    return TW_OK;
+}
+
+void tw_close(tw_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    for (auto* b : {&ctx->flags, &ctx->host_stage})
+        b->release(&ctx->held);
+    for (int i = 0; i < 3; i++) { ctx->eng[i].release(&ctx->held); ctx->wire[i].release(&ctx->held); }
+    for (int i = 0; i < 2; i++) { ctx->pyr[i].release(&ctx->held); ctx->work[i].release(&ctx->held); ctx->flow[i].release(&ctx->held); }
+    for (int i = 0; i < 4; i++) ctx->plane[i].release(&ctx->held);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+size_t tw_last_error(const tw_ctx* ctx, char* buf, size_t cap) {
+    if (!ctx) return 0;
+    size_t n = ctx->err.size();
+    if (buf && cap) {
+        size_t m = std::min(n, cap - 1);
+        std::memcpy(buf, ctx->err.data(), m);
+        buf[m] = 0;
+    }
+    return n;
+}
+
+int tw_stats(const tw_ctx* ctx, uint64_t* kernel_launches, uint64_t* device_bytes) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    if (kernel_launches) *kernel_launches = ctx->launches;
+    if (device_bytes) *device_bytes = ctx->held;
+    return TW_OK;
+}
+
+int tw_flow_geometry(const tw_flow_settings* s, int32_t width, int32_t height, int32_t* flow_w, int32_t* flow_h,
+                     int32_t* levels, int32_t* sizes, int32_t cap) {
+    if (!s) return TW_ERR_BAD_PARAM;
+    Geo g;
+    std::string e;
+    int rc = geometry(*s, width, height, &g, &e);
+    if (rc) return rc;
+    if (flow_w) *flow_w = g.w;
+    if (flow_h) *flow_h = g.h;
+    if (levels) *levels = g.levels;
+    if (sizes)
+        for (int i = 0; i < g.levels && i < cap; i++) { sizes[2 * i] = g.sizes[i][0]; sizes[2 * i + 1] = g.sizes[i][1]; }
+    return TW_OK;
+}
+
+static int upload_image(tw_ctx* ctx, DevBuf& b, const tw_image* im) {
+    size_t bytes = (size_t)im->width * im->height * 4 * sample_bytes(im->fmt);
+    CHECK(ctx->ensure(b, bytes, "image upload"));
+    return ctx->cuda(cudaMemcpyAsync(b.p, im->data, bytes, cudaMemcpyHostToDevice, ctx->stream), "image upload");
+}
+
+static int finish(tw_ctx* ctx, int* flags_host, int n) {
+    cudaError_t e = cudaMemcpyAsync(flags_host, ctx->flags.p, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return ctx->cuda(e, "kernel execution");
+}
+
+// flags layout (ints): [0..1] solve state of solve 0, [2..3] of solve 1, [4] NaN flag, [5] warp refused
+static int solve_common(tw_ctx* ctx, const tw_image* a, const tw_image* b, const tw_flow_settings* s, tw_flow* f_ab,
+                        tw_flow* f_ba, bool pair) {
+    CHECK(check_image(ctx, a, "solve"));
+    CHECK(check_image(ctx, b, "solve"));
+    if (!s) return ctx->fail(TW_ERR_BAD_PARAM, "no flow settings");
+    if (!same_shape(a, b))
+        return ctx->fail(TW_ERR_MISMATCH, "optical flow: incompatible inputs (%dx%d fmt %d against %dx%d fmt %d)", a->width,
+                         a->height, a->fmt, b->width, b->height, b->fmt);
+    if (s->wrap) return ctx->fail(TW_ERR_UNSUPPORTED, "the wrap-around (360) solve is not on the device");
+    Geo g;
+    CHECK(geometry(*s, a->width, a->height, &g, &ctx->err));
+    if (f_ab && (f_ab->width != g.w || f_ab->height != g.h || !f_ab->data))
+        return ctx->fail(TW_ERR_MISMATCH, "flow buffer is not %dx%d", g.w, g.h);
+    if (f_ba && (f_ba->width != g.w || f_ba->height != g.h || !f_ba->data))
+        return ctx->fail(TW_ERR_MISMATCH, "flow buffer is not %dx%d", g.w, g.h);
+    CHECK(upload_image(ctx, ctx->eng[0], a));
+    CHECK(upload_image(ctx, ctx->eng[1], b));
+    size_t pf = pyramid_floats(g);
+    CHECK(ctx->ensure(ctx->pyr[0], pf * 4, "pyramid"));
+    CHECK(ctx->ensure(ctx->pyr[1], pf * 4, "pyramid"));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, a->width, a->height, a->fmt, *s, g, ctx->pyr[0].as<float>()));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, b->width, b->height, b->fmt, *s, g, ctx->pyr[1].as<float>()));
+    size_t fb = (size_t)g.w * g.h * 2 * sizeof(float);
+    CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
+    CHECK(ctx->ensure(ctx->flow[1], fb, "flow"));
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, 64, ctx->stream), "flags"));
+    // f_ab = solve(X = A, Y = B); f_ba = solve(X = B, Y = A)
+    if (f_ab)
+        CHECK(solve_pyramids_dev(ctx, ctx->pyr[0].as<float>(), ctx->pyr[1].as<float>(), g, *s, ctx->work[0],
+                                 ctx->flow[0].as<float>(), flags + 0, flags + 4));
+    if (pair && f_ba)
+        CHECK(solve_pyramids_dev(ctx, ctx->pyr[1].as<float>(), ctx->pyr[0].as<float>(), g, *s, ctx->work[1],
+                                 ctx->flow[1].as<float>(), flags + 2, flags + 4));
+    if (f_ab) CHECK(ctx->cuda(cudaMemcpyAsync(f_ab->data, ctx->flow[0].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
+    if (pair && f_ba) CHECK(ctx->cuda(cudaMemcpyAsync(f_ba->data, ctx->flow[1].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
+    int hf[8];
+    CHECK(finish(ctx, hf, 8));
+    if (hf[4]) return ctx->fail(TW_ERR_NAN_OUTPUT, "the solved flow holds a NaN");
+    return TW_OK;
+}
+
+int tw_solve(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_flow_settings* s, tw_flow* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!out) return ctx->fail(TW_ERR_BAD_PARAM, "no output flow");
+    return solve_common(ctx, x, y, s, out, nullptr, false);
+}
+
+int tw_solve_pair(tw_ctx* ctx, const tw_image* a, const tw_image* b, const tw_flow_settings* s, tw_flow* f_ab,
+                  tw_flow* f_ba) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!f_ab || !f_ba) return ctx->fail(TW_ERR_BAD_PARAM, "no output flow");
+    return solve_common(ctx, a, b, s, f_ab, f_ba, true);
+}
+
+int tw_build_pyramid(tw_ctx* ctx, const tw_image* img, const tw_flow_settings* s, float* levels_out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CHECK(check_image(ctx, img, "build_pyramid"));
+    if (!s || !levels_out) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    Geo g;
+    CHECK(geometry(*s, img->width, img->height, &g, &ctx->err));
+    CHECK(upload_image(ctx, ctx->eng[0], img));
+    size_t pf = pyramid_floats(g);
+    CHECK(ctx->ensure(ctx->pyr[0], pf * 4, "pyramid"));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, img->width, img->height, img->fmt, *s, g, ctx->pyr[0].as<float>()));
+    CHECK(ctx->cuda(cudaMemcpyAsync(levels_out, ctx->pyr[0].p, pf * 4, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[1];
+    return finish(ctx, hf, 1);
+}
+
+int tw_compose_vectors(tw_ctx* ctx, const tw_engine_settings* settings, const tw_selection* sel, const tw_image* a,
+                       const tw_image* b, const tw_flow* f_ab, const tw_flow* f_ba, tw_image_mut* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!settings || !sel || !out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_image(ctx, a, "compose"));
+    CHECK(check_image(ctx, b, "compose"));
+    if (!same_shape(a, b) || out->width != a->width || out->height != a->height || out->fmt != a->fmt)
+        return ctx->fail(TW_ERR_MISMATCH, "compose: images of different shapes");
+    const tw_flow* f = f_ab ? f_ab : f_ba;
+    if (!f) return ctx->fail(TW_ERR_MISMATCH, "compose: no flow");
+    if (f_ab && f_ba && (f_ab->width != f_ba->width || f_ab->height != f_ba->height))
+        return ctx->fail(TW_ERR_MISMATCH, "compose: flows of different sizes");
+    int fw = f->width, fh = f->height;
+    CHECK(upload_image(ctx, ctx->eng[0], a));
+    CHECK(upload_image(ctx, ctx->eng[1], b));
+    size_t fb = (size_t)fw * fh * 2 * sizeof(float);
+    if (f_ab) {
+        CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
+        CHECK(ctx->cuda(cudaMemcpyAsync(ctx->flow[0].p, f_ab->data, fb, cudaMemcpyHostToDevice, ctx->stream), "flow upload"));
+    }
+    if (f_ba) {
+        CHECK(ctx->ensure(ctx->flow[1], fb, "flow"));
+        CHECK(ctx->cuda(cudaMemcpyAsync(ctx->flow[1].p, f_ba->data, fb, cudaMemcpyHostToDevice, ctx->stream), "flow upload"));
+    }
+    size_t ob = (size_t)a->width * a->height * 4 * sample_bytes(a->fmt);
+    CHECK(ctx->ensure(ctx->eng[2], ob, "compose output"));
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, 64, ctx->stream), "flags"));
+    CHECK(compose_dev(ctx, *settings, *sel, ctx->eng[0].p, ctx->eng[1].p, f_ab ? ctx->flow[0].as<float>() : nullptr,
+                      f_ba ? ctx->flow[1].as<float>() : nullptr, fw, fh, a->width, a->height, a->fmt, ctx->eng[2].p,
+                      false, false, flags + 5));
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[8];
+    CHECK(finish(ctx, hf, 8));
+    if (hf[5]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    return TW_OK;
+}
+
+int tw_block_match(tw_ctx* ctx, const float* a, const float* b, float* flow, int32_t width, int32_t height) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!a || !b || !flow || width <= 0 || height <= 0) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    size_t n = (size_t)width * height;
+    CHECK(ctx->ensure(ctx->plane[0], n * 4, "plane A"));
+    CHECK(ctx->ensure(ctx->plane[1], n * 4, "plane B"));
+    CHECK(ctx->ensure(ctx->plane[2], n * 8, "flow"));
+    CHECK(ctx->ensure(ctx->work[0], n * 8, "flow planes"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->plane[0].p, a, n * 4, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->plane[1].p, b, n * 4, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->plane[2].p, flow, n * 8, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    float* fu = ctx->work[0].as<float>();
+    float* fv = fu + n;
+    LAUNCH(ctx, k_deinterleave, grid1((long)n), TB, 0, ctx->plane[2].as<float>(), (long)n, fu, fv);
+    block_match(ctx, ctx->plane[0].as<float>(), ctx->plane[1].as<float>(), fu, fv, width, height);
+    LAUNCH(ctx, k_interleave, grid1((long)n), TB, 0, fu, fv, (long)n, ctx->plane[2].as<float>());
+    CHECK(ctx->cuda(cudaMemcpyAsync(flow, ctx->plane[2].p, n * 8, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[1];
+    return finish(ctx, hf, 1);
+}
+
+int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_flow* flow, float amount, int32_t hold,
+                uint8_t* cov) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CHECK(check_image(ctx, src, "inv_warp"));
+    if (!out || !out->data || !flow || !flow->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    if (out->width != src->width || out->height != src->height || out->fmt != src->fmt)
+        return ctx->fail(TW_ERR_MISMATCH, "inverse warp: destination and source differ");
+    int W = src->width, H = src->height;
+    if (W < 2 || H < 2 || flow->width < 2 || flow->height < 2)
+        return ctx->fail(TW_ERR_MISMATCH, "inverse warp needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W, H,
+                         flow->width, flow->height);
+    CHECK(upload_image(ctx, ctx->eng[0], src));
+    size_t fb = (size_t)flow->width * flow->height * 2 * sizeof(float);
+    CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->flow[0].p, flow->data, fb, cudaMemcpyHostToDevice, ctx->stream), "flow upload"));
+    size_t ob = (size_t)W * H * 4 * sample_bytes(src->fmt);
+    CHECK(ctx->ensure(ctx->eng[2], ob, "warp output"));
+    CHECK(ctx->ensure(ctx->plane[3], (size_t)W * H, "coverage"));
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, 64, ctx->stream), "flags"));
+    WarpParams p = warp_params(ctx->eng[0].p, ctx->flow[0].as<float>(), flow->width, flow->height, amount, W, hold != 0);
+    uint8_t* dcov = cov ? ctx->plane[3].as<uint8_t>() : nullptr;
+    LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, p, src->fmt, ctx->eng[2].p, dcov, W, H, flags + 5);
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    if (cov) CHECK(ctx->cuda(cudaMemcpyAsync(cov, dcov, (size_t)W * H, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[8];
+    CHECK(finish(ctx, hf, 8));
+    if (hf[5]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    return TW_OK;
+}
+
+int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* b, float w) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CHECK(check_image(ctx, a, "blend"));
+    CHECK(check_image(ctx, b, "blend"));
+    if (!out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    if (!same_shape(a, b) || out->width != a->width || out->height != a->height || out->fmt != a->fmt)
+        return ctx->fail(TW_ERR_MISMATCH, "image primitives need equal size and format");
+    int W = a->width, H = a->height;
+    CHECK(upload_image(ctx, ctx->eng[0], a));
+    CHECK(upload_image(ctx, ctx->eng[1], b));
+    size_t ob = (size_t)W * H * 4 * sample_bytes(a->fmt);
+    CHECK(ctx->ensure(ctx->eng[2], ob, "blend output"));
+    WarpParams pa = warp_params(ctx->eng[0].p, nullptr, 0, 0, 0.0f, W, true);
+    WarpParams pb = warp_params(ctx->eng[1].p, nullptr, 0, 0, 0.0f, W, true);
+    int* flags = ctx->flags.as<int>();
+    LAUNCH(ctx, k_compose_blend, grid2(W, H), TB, 0, pa, pb, a->fmt, w, blend_mode(w), ctx->eng[2].p, W, H, false, false,
+           flags + 5);
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[1];
+    return finish(ctx, hf, 1);
+}
+
+int tw_from_frame(tw_ctx* ctx, const void* wire, int32_t width, int32_t height, int32_t fmt, void* engine_out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!wire || !engine_out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
+    CHECK(ctx->ensure(ctx->wire[0], bytes, "wire"));
+    CHECK(ctx->ensure(ctx->eng[0], bytes, "engine"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->wire[0].p, wire, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    long n = (long)width * height;
+    if (fmt == TW_U8) LAUNCH(ctx, k_from_frame_u8, grid1(n), TB, 0, ctx->wire[0].as<uint8_t>(), ctx->eng[0].as<uint8_t>(), width, height, false);
+    else if (fmt == TW_U16) LAUNCH(ctx, k_from_frame_u16, grid1(n), TB, 0, ctx->wire[0].as<uint16_t>(), ctx->eng[0].as<uint16_t>(), width, height, false);
+    else LAUNCH(ctx, k_from_frame_f32, grid1(n), TB, 0, ctx->wire[0].as<float>(), ctx->eng[0].as<float>(), width, height, false);
+    CHECK(ctx->cuda(cudaMemcpyAsync(engine_out, ctx->eng[0].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[1];
+    return finish(ctx, hf, 1);
+}
+
+int tw_to_frame(tw_ctx* ctx, const void* engine, int32_t width, int32_t height, int32_t fmt, void* wire_out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!engine || !wire_out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
+    CHECK(ctx->ensure(ctx->wire[0], bytes, "wire"));
+    CHECK(ctx->ensure(ctx->eng[0], bytes, "engine"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->eng[0].p, engine, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    long n = (long)width * height;
+    if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, ctx->eng[0].as<uint8_t>(), ctx->wire[0].as<uint8_t>(), width, height, false);
+    else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, ctx->eng[0].as<uint16_t>(), ctx->wire[0].as<uint16_t>(), width, height, false);
+    else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, ctx->eng[0].as<float>(), ctx->wire[0].as<float>(), width, height, false);
+    CHECK(ctx->cuda(cudaMemcpyAsync(wire_out, ctx->wire[0].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[1];
+    return finish(ctx, hf, 1);
+}
+
+// ---- whole output frames ---------------------------------------------------------------------------
+
+static void from_frame_dev(tw_ctx* ctx, const void* wire, void* eng, int W, int H, int fmt, bool flip) {
+    long n = (long)W * H;
+    if (fmt == TW_U8) LAUNCH(ctx, k_from_frame_u8, grid1(n), TB, 0, (const uint8_t*)wire, (uint8_t*)eng, W, H, flip);
+    else if (fmt == TW_U16) LAUNCH(ctx, k_from_frame_u16, grid1(n), TB, 0, (const uint16_t*)wire, (uint16_t*)eng, W, H, flip);
+    else LAUNCH(ctx, k_from_frame_f32, grid1(n), TB, 0, (const float*)wire, (float*)eng, W, H, flip);
+}
+
+// One output frame from two device-resident wire frames (nullptr = a blank frame outside the clip).
+// Writes the output wire frame to out_wire (device). Flags: the caller resets them.
+static int retime_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel, const void* wa,
+                            const void* wb, int W, int H, int fmt, void* out_wire) {
+    size_t bytes = (size_t)W * H * 4 * sample_bytes(fmt);
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->ensure(ctx->eng[0], bytes, "engine A"));
+    CHECK(ctx->ensure(ctx->eng[1], bytes, "engine B"));
+    bool vector = sel.vectors_quality != 0 && !sel.exact;
+    bool flip = vector && s.motion_rows_reversed != 0;
+    // a frame outside the clip is blank (host.rs:338-352); blank images are all zero in every depth
+    if (wa) from_frame_dev(ctx, wa, ctx->eng[0].p, W, H, fmt, flip);
+    else CHECK(ctx->cuda(cudaMemsetAsync(ctx->eng[0].p, 0, bytes, ctx->stream), "blank"));
+    if (wb) from_frame_dev(ctx, wb, ctx->eng[1].p, W, H, fmt, flip);
+    else CHECK(ctx->cuda(cudaMemsetAsync(ctx->eng[1].p, 0, bytes, ctx->stream), "blank"));
+    if (!vector) return interpolate_dev(ctx, sel, ctx->eng[0].p, ctx->eng[1].p, W, H, fmt, out_wire, true, flags + 5);
+
+    // the vector path (compose/vector.rs:163-178 solve_flows, then compose_vectors)
+    tw_flow_settings fs = s.flow;
+    fs.quality = sel.vectors_quality;
+    if (fs.wrap) return ctx->fail(TW_ERR_UNSUPPORTED, "the wrap-around (360) solve is not on the device");
+    Geo g;
+    CHECK(geometry(fs, W, H, &g, &ctx->err));
+    size_t pf = pyramid_floats(g);
+    CHECK(ctx->ensure(ctx->pyr[0], pf * 4, "pyramid"));
+    CHECK(ctx->ensure(ctx->pyr[1], pf * 4, "pyramid"));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, W, H, fmt, fs, g, ctx->pyr[0].as<float>()));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, W, H, fmt, fs, g, ctx->pyr[1].as<float>()));
+    size_t fb = (size_t)g.w * g.h * 2 * sizeof(float);
+    CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
+    CHECK(ctx->ensure(ctx->flow[1], fb, "flow"));
+    bool need_ab = true, need_ba = true;
+    if (sel.interp == 0) {
+        bool use_ab = (sel.wa < 0.5f && (unsigned)s.compose.warp_mode < 2) || (0.5f <= sel.wa && (unsigned)s.compose.warp_mode > 1);
+        need_ab = use_ab;
+        need_ba = !use_ab;
+    } else if (sel.interp != 1 && sel.interp != 2) {
+        return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
+    }
+    if (need_ab)
+        CHECK(solve_pyramids_dev(ctx, ctx->pyr[0].as<float>(), ctx->pyr[1].as<float>(), g, fs, ctx->work[0],
+                                 ctx->flow[0].as<float>(), flags + 0, flags + 4));
+    if (need_ba)
+        CHECK(solve_pyramids_dev(ctx, ctx->pyr[1].as<float>(), ctx->pyr[0].as<float>(), g, fs, ctx->work[1],
+                                 ctx->flow[1].as<float>(), flags + 2, flags + 4));
+    return compose_dev(ctx, s.compose, sel, ctx->eng[0].p, ctx->eng[1].p, need_ab ? ctx->flow[0].as<float>() : nullptr,
+                       need_ba ? ctx->flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, out_wire, true, flip,
+                       flags + 5);
+}
+
+static int check_flags(tw_ctx* ctx) {
+    int hf[8];
+    CHECK(finish(ctx, hf, 8));
+    if (hf[4]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
+    if (hf[5]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    return TW_OK;
+}
+
+int tw_retime_frame(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection* sel, const void* wire_a,
+                    const void* wire_b, int32_t width, int32_t height, int32_t fmt, void* wire_out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!s || !sel || !wire_out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0)
+        return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
+    CHECK(ctx->ensure(ctx->wire[0], bytes, "wire A"));
+    CHECK(ctx->ensure(ctx->wire[1], bytes, "wire B"));
+    CHECK(ctx->ensure(ctx->wire[2], bytes, "wire out"));
+    if (wire_a) CHECK(ctx->cuda(cudaMemcpyAsync(ctx->wire[0].p, wire_a, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    if (wire_b) CHECK(ctx->cuda(cudaMemcpyAsync(ctx->wire[1].p, wire_b, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    CHECK(ctx->cuda(cudaMemsetAsync(ctx->flags.p, 0, 64, ctx->stream), "flags"));
+    CHECK(retime_frame_dev(ctx, *s, *sel, wire_a ? ctx->wire[0].p : nullptr, wire_b ? ctx->wire[1].p : nullptr, width,
+                           height, fmt, ctx->wire[2].p));
+    CHECK(ctx->cuda(cudaMemcpyAsync(wire_out, ctx->wire[2].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    return check_flags(ctx);
+}
+
+int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
+                          const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!s || !sels || !frames || !out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
+        return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
+    CHECK(ctx->cuda(cudaMemsetAsync(ctx->flags.p, 0, 64, ctx->stream), "flags"));
+    for (int k = 0; k < nout; k++) {
+        const tw_selection& sel = sels[k];
+        const uint8_t* base = (const uint8_t*)frames;
+        const void* fa = (sel.a >= 0 && sel.a < nframes) ? base + (size_t)sel.a * bytes : nullptr;
+        const void* fb = (sel.b >= 0 && sel.b < nframes) ? base + (size_t)sel.b * bytes : nullptr;
+        CHECK(retime_frame_dev(ctx, *s, sel, fa, fb, width, height, fmt, (uint8_t*)out + (size_t)k * bytes));
+    }
+    return check_flags(ctx);
+}
+
+}  // extern "C"
+
+// =======================================================================================================
+// The time model (timeline.rs) of the Speed map, host scalars
+
+namespace {
+
+int32_t cvtt_i32_d(double x) {  // timeline.rs:43-49
+    if (x > -2147483649.0 && x < 2147483648.0) return (int32_t)x;
+    return INT32_MIN;
+}
+int32_t cvtt_i32_f(float x) {  // timeline.rs:52-58
+    if (x > -2147483904.0f && x < 2147483648.0f) return (int32_t)x;
+    return INT32_MIN;
+}
+int32_t float_to_fixed(double f) {  // crates/fx-core/src/fixed.rs:8-10 (Rust `as i32` saturates)
+    double v = f * 65536.0 + (f < 0.0 ? -0.5 : 0.5);
+    if (std::isnan(v)) return 0;
+    if (v >= 2147483647.0) return INT32_MAX;
+    if (v <= -2147483648.0) return INT32_MIN;
+    return (int32_t)v;
+}
+float fixed_reader(int32_t fixed, float scale) { return (float)((double)fixed * (1.0 / 65536.0)) * scale; }
+
+struct SpeedCurve {  // crates/fx-core/src/curves.rs:348-375, :537-544
+    const tw_time_params* p;
+    long long key_time(int i, int step) const { return (long long)std::llround(p->key_frames[i] * (double)step); }
+    double at(long long t, int step) const {
+        if (p->nkeys <= 0) return p->speed_percent;
+        int last = p->nkeys - 1;
+        if (t <= key_time(0, step)) return p->key_values[0];
+        if (t >= key_time(last, step)) return p->key_values[last];
+        int i = 0;
+        while (i + 1 < p->nkeys && key_time(i + 1, step) <= t) i++;
+        long long ta = key_time(i, step), tb = key_time(i + 1, step);
+        bool ea = p->key_ease && p->key_ease[i], eb = p->key_ease && p->key_ease[i + 1];
+        double u = (double)(t - ta) / (double)(tb - ta);
+        double f = (!ea && !eb) ? u : (ea && eb) ? u * u * (3.0 - 2.0 * u) : ea ? u * u * (2.0 - u) : u * (1.0 + u * (1.0 - u));
+        return p->key_values[i] + (p->key_values[i + 1] - p->key_values[i]) * f;
+    }
+};
+
+// timeline.rs:266-331 (Speed mode, Src Time Offset 0, equal rates after "In FPS is Out FPS")
+float src_pos(const SpeedCurve& c, int lts, float t, bool* unsupported) {
+    float lts_f = (float)lts;
+    float out = 0.0f;
+    int n2 = cvtt_i32_f(t * 2.0f);
+    if (n2 >= (1 << 24)) { *unsupported = true; return 0.0f; }
+    float k = 1.0f;
+    while ((float)n2 >= k) {
+        int time = cvtt_i32_d((double)((lts_f * k) / 2.0f) + 0.05);
+        float sp = (float)((double)float_to_fixed(c.at(time, lts)) / 6553600.0);
+        out = (sp / 2.0f) + out;
+        k += 1.0f;
+    }
+    float tt = t * 2.0f;
+    float rem = tt - (k + -1.0f);
+    if ((double)rem > 0.0001) {
+        int time = cvtt_i32_d((double)((tt * lts_f) / 2.0f) + 0.05);
+        float sp = (float)((double)float_to_fixed(c.at(time, lts)) / 6553600.0);
+        out = ((rem * sp) / 2.0f) + out;
+    }
+    return (float)((30.0 / 30.0) * (double)out);
+}
+
+}  // namespace
+
+extern "C" int tw_select(const tw_time_params* p, int32_t n, int32_t width, int32_t height, tw_selection* out) {
+    if (!p || !out || p->fps_num <= 0 || p->fps_den <= 0) return TW_ERR_BAD_PARAM;
+    if (p->nkeys > 0 && (!p->key_frames || !p->key_values)) return TW_ERR_BAD_PARAM;
+    int lts = p->fps_den == 1 ? 100 : p->fps_den;  // crates/fx-core/src/time.rs:92-99
+    SpeedCurve c{p};
+    int cur = n * lts;
+    float t0 = (float)cur / (float)lts;                  // timeline.rs:136-142
+    float t1 = ((float)lts + (float)cur) / (float)lts;
+    bool bad = false;
+    float s0 = src_pos(c, lts, t0, &bad);
+    float s1 = src_pos(c, lts, t1, &bad);
+    if (bad) return TW_ERR_UNSUPPORTED;
+    float blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
+    int a = cvtt_i32_f(s0);
+    float frac = s0 - (float)a;
+    out->s0 = s0;
+    out->s1 = s1;
+    out->a = a;
+    out->b = (int32_t)((uint32_t)a + 1u);
+    out->wa = 1.0f - frac;
+    bool exact = true;  // timeline.rs:429-439
+    float fr = s0 - std::floor(s0);
+    if ((double)std::fabs(fr) > 0.005 && (double)std::fabs((float)((double)fr - 1.0)) > 0.005) exact = false;
+    if ((double)std::fabs(s0 - s1) > 1e-6 && (double)blur > 0.005) exact = false;
+    out->exact = exact ? 1 : 0;
+    int vq = p->vectors - 1;
+    out->vectors_quality = (width >= 2 && height >= 2) ? vq : 0;
+    out->interp = p->frame_interp - 1;
+    return TW_OK;
+}

@@ -1,0 +1,487 @@
+// Pyramid filters and the optical flow solver, strict mode. Each kernel cites the reference
+// function (plugins/retime-engine/src/...) whose per-element arithmetic it repeats.
+#include "kernels.cuh"
+
+namespace tw {
+
+// flow/conv.rs:101-137 (border_value_ordered): one border element of a line whose element t is
+// line[t * stride]. `multi` selects the 2- and 3-channel rule (the -1.0 sentinel decides whether a
+// tap exists, so a real sample of exactly -1.0 is dropped too); LEFT_FIRST adds the tap at i - j
+// before the tap at i + j.
+template <bool LEFT_FIRST>
+__device__ __forceinline__ float border_value(const float* __restrict__ line, long stride, int len, int i,
+                                              const Taps& t, bool multi) {
+    float centre = (i >= 0 && i < len) ? line[(long)i * stride] : 0.0f;
+    float num = t.k[0] * centre;
+    float den = t.k[0];
+#pragma unroll 1
+    for (int j = t.n - 1; j >= 1; j--) {
+        float kj = t.k[j];
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            bool right = (side == 0) != LEFT_FIRST;
+            int tt = right ? i + j : i - j;
+            bool inside = tt >= 0 && tt < len;
+            float xv, wv;
+            if (!multi) {
+                xv = inside ? line[(long)tt * stride] : 0.0f;
+                wv = inside ? kj : 0.0f;
+            } else {
+                float v = inside ? line[(long)tt * stride] : -1.0f;
+                float mask = (v != -1.0f) ? 1.0f : 0.0f;
+                xv = v;
+                wv = mask * kj;
+            }
+            den = den + wv;
+            num = num + xv * wv;
+        }
+    }
+    return num / den;
+}
+
+// conv.rs:141-190 (hrow + interior_run), one output sample per thread
+__global__ void k_conv_h(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t, bool multi) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const float* row = src + (long)y * w;
+    int n = t.n;
+    int head = min(n, w);
+    int interior = max(w - 2 * n, 0);
+    float r;
+    if (x >= head && x < head + interior) {
+        r = row[x] * t.k[0];
+#pragma unroll 1
+        for (int j = n - 1; j >= 1; j--) r = r + (row[x + j] + row[x - j]) * t.k[j];
+    } else {
+        r = border_value<false>(row, 1, w, x, t, multi);
+    }
+    dst[(long)y * w + x] = r;
+}
+
+// conv.rs:268-301 (vrow_ordered); the optional band output is flow.rs:266-267 (band = orig - blur)
+__global__ void k_conv_v(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t, bool multi,
+                         bool above_first, const float* __restrict__ orig, float* __restrict__ band) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    int n = t.n;
+    int head = min(n, h);
+    int interior = max(h - 2 * n, 0);
+    float r;
+    if (y >= head && y < head + interior) {
+        r = src[(long)y * w + x] * t.k[0];
+#pragma unroll 1
+        for (int j = n - 1; j >= 1; j--) r = r + (src[(long)(y + j) * w + x] + src[(long)(y - j) * w + x]) * t.k[j];
+    } else if (above_first) {
+        r = border_value<true>(src + x, w, h, y, t, multi);
+    } else {
+        r = border_value<false>(src + x, w, h, y, t, multi);
+    }
+    long i = (long)y * w + x;
+    dst[i] = r;
+    if (band) band[i] = orig[i] - r;
+}
+
+// flow/sample.rs:91-112 (resample1): corner aligned bilinear
+__global__ void k_resample(const float* __restrict__ src, int sw, int sh, float* __restrict__ dst, int dw, int dh) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= dw || y >= dh) return;
+    float sx = ((float)sw - 1.0f) / (float)(dw - 1);
+    float sy = ((float)sh - 1.0f) / (float)(dh - 1);
+    dst[(long)y * dw + x] = bilinear1(src, sw, sh, (float)x * sx, (float)y * sy);
+}
+
+// flow.rs:283-328 (calc_grad, calc_a)
+__global__ void k_grad_tensor(const float* __restrict__ img, int w, int h, float* __restrict__ gxo,
+                              float* __restrict__ gyo, float* __restrict__ a0, float* __restrict__ a1,
+                              float* __restrict__ a2) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    long i = (long)y * w + x;
+    float c = img[i];
+    float nx = 0.0f, dx = 0.0f, ny = 0.0f, dy = 0.0f;
+    if (x >= 1) { nx = (c - img[i - 1]) + 0.0f; dx = 1.0f; }
+    if (y >= 1) { ny = (c - img[i - w]) + 0.0f; dy = 1.0f; }
+    if (x + 1 <= w - 1) { nx = nx + (img[i + 1] - c); dx = dx + 1.0f; }
+    if (y + 1 <= h - 1) { ny = ny + (img[i + w] - c); dy = dy + 1.0f; }
+    float gx = nx / dx, gy = ny / dy;
+    gxo[i] = gx;
+    gyo[i] = gy;
+    a0[i] = gx * gx;
+    a1[i] = gx * gy;
+    a2[i] = gy * gy;
+}
+
+// flow.rs:334-357 (calc_b): i1 = imgA, i0 = imgB
+__global__ void k_calc_b(const float* __restrict__ i1, const float* __restrict__ i0, const float* __restrict__ gx,
+                         const float* __restrict__ gy, const float* __restrict__ fu, const float* __restrict__ fv,
+                         int w, int h, float* __restrict__ bx, float* __restrict__ by) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    long i = (long)y * w + x;
+    float fw = (float)w, fh = (float)h;
+    float sx = (float)x - fu[i];
+    float sy = (float)y - fv[i];
+    if (sx < 0.0f || fw - 1.0f < sx || sy < 0.0f || fh - 1.0f < sy) {
+        bx[i] = 0.0f;
+        by[i] = 0.0f;
+    } else {
+        float s = bilinear1(i0, w, h, sx, sy);
+        float r = s - i1[i];
+        bx[i] = r * gx[i];
+        by[i] = r * gy[i];
+    }
+}
+
+// flow.rs:361-371 (new_disp)
+__global__ void k_new_disp(float* __restrict__ fu, float* __restrict__ fv, const float* __restrict__ a0,
+                           const float* __restrict__ a1, const float* __restrict__ a2, const float* __restrict__ bx,
+                           const float* __restrict__ by, long n) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float aa = a0[i], ab = a1[i], ad = a2[i];
+    float b0 = bx[i], b1 = by[i];
+    float t = ab * ab - ad * aa;
+    if (fabsf(t) > 40.0f) {
+        fu[i] = (ab * b1 - ad * b0) / t + fu[i];
+        fv[i] = (ab * b0 - aa * b1) / t + fv[i];
+    }
+}
+
+// flow.rs:430-442 (all_flow_out_of_range), as "some pixel is in range"
+__global__ void k_range_any(const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,
+                            int* __restrict__ any_in_range) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    bool in = false;
+    if (x < w && y < h) {
+        long i = (long)y * w + x;
+        float px = (float)x + fu[i];
+        float py = (float)y + fv[i];
+        float fw = (float)(w - 1), fh = (float)(h - 1);
+        in = 0.0f <= px && px <= fw && 0.0f <= py && py <= fh;
+    }
+    if (__syncthreads_or(in) && threadIdx.x == 0) atomicOr(any_in_range, 1);
+}
+
+// flow.rs:1292-1300: state[0] = check (still live), state[1] = some pixel in range at this level
+__global__ void k_range_apply(float* __restrict__ fu, float* __restrict__ fv, long n, int* __restrict__ state,
+                              bool damp_now, float damp) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    bool zero = state[0] != 0 && state[1] == 0;
+    float u = zero ? 0.0f : fu[i];
+    float v = zero ? 0.0f : fv[i];
+    if (damp_now) {  // scale_values (flow.rs:422-427): f * p, untouched for f == 1
+        u = damp * u;
+        v = damp * v;
+    }
+    fu[i] = u;
+    fv[i] = v;
+}
+
+// the check state of a solve: check live, nothing in range yet (flow.rs:1270)
+__global__ void k_range_init(int* __restrict__ state) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        state[0] = 1;
+        state[1] = 0;
+    }
+}
+
+// the check state after a level: check = check && nothing was in range; clears the flag for the next level
+__global__ void k_range_next(int* __restrict__ state) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        state[0] = (state[0] != 0 && state[1] == 0) ? 1 : 0;
+        state[1] = 0;
+    }
+}
+
+// flow.rs:376-391 (upsample_flow) with sample.rs:69-86 (bilinear2) on the planar field
+__global__ void k_upsample_flow(const float* __restrict__ su, const float* __restrict__ sv, int sw, int sh,
+                                float* __restrict__ du, float* __restrict__ dv, int dw, int dh) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= dw || y >= dh) return;
+    float sx = ((float)dw - 1.0f) / (float)(sw - 1);
+    float sy = ((float)dh - 1.0f) / (float)(sh - 1);
+    float rx = (float)(1.0 / (double)sx);
+    float ry = (float)(1.0 / (double)sy);
+    int ix, iy;
+    float fx, fy;
+    cell((float)x * rx, sw, ix, fx);
+    cell((float)y * ry, sh, iy, fy);
+    long i = (long)iy * sw + ix;
+    float r[2];
+    const float* planes[2] = {su, sv};
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        const float* p = planes[c];
+        float p00 = p[i], p10 = p[i + 1], p01 = p[i + sw], p11 = p[i + sw + 1];
+        float top = (p10 - p00) * fx + p00;
+        float bot = (p11 - p01) * fx + p01;
+        r[c] = (bot - top) * fy + top;
+    }
+    long o = (long)y * dw + x;
+    du[o] = r[0] * sx;
+    dv[o] = r[1] * sy;
+}
+
+// flow.rs:1305: scale_values(flow, -1.0), written interleaved; flags a NaN
+__global__ void k_negate_interleave(const float* __restrict__ fu, const float* __restrict__ fv, long n,
+                                    float* __restrict__ out, int* __restrict__ nan_flag) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float u = -1.0f * fu[i], v = -1.0f * fv[i];
+    out[2 * i] = u;
+    out[2 * i + 1] = v;
+    if (isnan(u) || isnan(v)) atomicOr(nan_flag, 1);
+}
+
+__global__ void k_deinterleave(const float* __restrict__ in, long n, float* __restrict__ fu, float* __restrict__ fv) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    fu[i] = in[2 * i];
+    fv[i] = in[2 * i + 1];
+}
+
+__global__ void k_interleave(const float* __restrict__ fu, const float* __restrict__ fv, long n, float* __restrict__ out) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[2 * i] = fu[i];
+    out[2 * i + 1] = fv[i];
+}
+
+__global__ void k_fill(float* __restrict__ p, long n, float v) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// =====================================================================================================
+// Block matching (flow.rs:447-622).
+//
+// A sweep is an in-place, loop-carried recurrence along a row (or a column): with v the vectors
+// before the sweep, v'[x] = accept(x, v'[x-1]) ? v'[x-1] : v[x], where accept(x, n) holds when the
+// target of v[x] lies in the level, its block cost c0 exists, the cost c1 at the target of n
+// exists and c1 < c0 (Block::step, flow.rs:529-546). Every v'[x] is therefore the ORIGINAL vector
+// of the start s <= x of its run, and a run started at j continues while accept(x, v[j]) holds.
+// The kernel evaluates that exactly, in parallel:
+//   1. c0[x] and the validity of v[x] for every x of the line;
+//   2. end[j] = the first x past j where accept(x, v[j]) fails, for every candidate start j;
+//   3. the run starts: 0, end[0], end[end[0]], ... (a chain walked in shared memory);
+//   4. v'[x] = v[start of x's run].
+// Each cost evaluation is Block::cost bit for bit, so the result equals the sequential sweep.
+
+// flow.rs:474-523 (Block::cost)
+__device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int h, const float p[9], float x2,
+                                        float y2, float& out) {
+    float wm2 = (float)(w - 2), hm2 = (float)(h - 2);
+    if (x2 > wm2 || y2 > hm2) return false;
+    int ix, iy;
+    float fx, fy;
+    if (x2 == wm2) { ix = cvtt32(wm2 - 1.0f); fx = 1.0f; }
+    else { ix = cvtt32(x2); fx = x2 - (float)ix; }
+    if (y2 == hm2) { iy = cvtt32(hm2 - 1.0f); fy = 1.0f; }
+    else { iy = cvtt32(y2); fy = y2 - (float)iy; }
+    if (ix < 1 || iy < 1) return false;
+    float w11 = fy * fx;
+    float w10 = fx - w11;
+    float w01 = fy - w11;
+    float w00 = ((1.0f - fx) - fy) + w11;
+    const float* base = B + (long)(iy - 1) * w + ix - 1;
+    float t[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) t[r][c] = __ldg(base + (long)r * w + c);
+    float sq[9];
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            float q = ((w00 * t[b][a] + w10 * t[b][a + 1]) + w01 * t[b + 1][a]) + w11 * t[b + 1][a + 1];
+            float d = p[b * 3 + a] - q;
+            sq[b * 3 + a] = d * d;
+        }
+    }
+    float s = sq[0] + sq[1];
+#pragma unroll
+    for (int k = 2; k < 8; k++) s = s + sq[k];
+    out = sq[8] + s;
+    return true;
+}
+
+__device__ __forceinline__ void bm_patch(const float* __restrict__ A, int w, int x, int y, float p[9]) {
+    const float* pa = A + (long)(y - 1) * w + x - 1;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) p[r * 3 + c] = __ldg(pa + (long)r * w + c);
+}
+
+// shared memory of one line of length len (u, v, c0, end, start flag) plus one int per thread
+size_t bm_smem_bytes(int len) { return (size_t)len * (4 * 5) + 1024 * 4; }
+
+constexpr int BM_SCAN = 64;  // parallel scan length of a run; longer runs continue in the walk
+
+// accept(i, n) of the sweep at line position i (Block::step, flow.rs:529-546), given c0 = the cost
+// of the current vector (NaN when the step cannot happen at i: no target or no cost)
+template <bool COLS>
+__device__ __forceinline__ bool bm_accept(const float* __restrict__ A, const float* __restrict__ B, int w, int h,
+                                          int fixed, int i, float nu, float nv, float ci) {
+    if (isnan(ci)) return false;  // None, or a NaN cost that nothing compares below
+    int x = COLS ? fixed : i, y = COLS ? i : fixed;
+    float p[9];
+    bm_patch(A, w, x, y, p);
+    float c1;
+    if (!bm_cost(B, w, h, p, (float)x - nu, (float)y - nv, c1)) return false;
+    return c1 < ci;
+}
+
+// One sweep over a line. The line is the row y (COLS false: pixel (i, y)) or the column x
+// (COLS true: pixel (x, i)); len is its length. Forward sweeps run i = 1..len-2 with the
+// neighbour i - 1, reverse sweeps i = len-2..1 with the neighbour i + 1.
+template <bool COLS>
+__device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
+                        float* __restrict__ fv, int w, int h, int fixed, bool reverse) {
+    extern __shared__ float sm[];
+    int len = COLS ? h : w;
+    float* su = sm;
+    float* sv = su + len;
+    float* c0 = sv + len;
+    int* endj = (int*)(c0 + len);
+    int* own = endj + len;
+    int* summ = own + len;  // one int per thread
+    const float w1 = (float)(w - 1), h1 = (float)(h - 1);
+    auto gidx = [&](int i) -> long { return COLS ? (long)i * w + fixed : (long)fixed * w + i; };
+
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        su[i] = fu[gidx(i)];
+        sv[i] = fv[gidx(i)];
+        own[i] = 0;
+    }
+    __syncthreads();
+    // 1. c0: the cost of the current vector, NaN where no step can happen
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        float c = __int_as_float(0x7fc00000);
+        if (i >= 1 && i <= len - 2) {
+            int x = COLS ? fixed : i, y = COLS ? i : fixed;
+            float tx = (float)x - su[i];
+            float ty = (float)y - sv[i];
+            if (0.0f <= tx && tx <= w1 && 0.0f <= ty && ty <= h1) {
+                float p[9];
+                bm_patch(A, w, x, y, p);
+                float cc;
+                if (bm_cost(B, w, h, p, tx, ty, cc)) c = cc;
+            }
+        }
+        c0[i] = c;
+    }
+    __syncthreads();
+    // 2. run ends, scanned for at most BM_SCAN positions: endj[j] >= 0 is the first position
+    //    past j where the run of v[j] stops (len-1 / 0 when it reaches the end of the sweep);
+    //    endj[j] = -(r + 1) when the scan stopped unfinished at position r.
+    for (int j = threadIdx.x; j < len; j += blockDim.x) {
+        float nu = su[j], nv = sv[j];
+        int e;
+        if (!reverse) {
+            e = len - 1;
+            int lim = min(len - 2, j + BM_SCAN);
+            int i = j + 1;
+            for (; i <= lim; i++)
+                if (!bm_accept<COLS>(A, B, w, h, fixed, i, nu, nv, c0[i])) { e = i; break; }
+            if (i > lim && lim < len - 2) e = -(i + 1);
+        } else {
+            e = 0;
+            int lim = max(1, j - BM_SCAN);
+            int i = j - 1;
+            for (; i >= lim; i--)
+                if (!bm_accept<COLS>(A, B, w, h, fixed, i, nu, nv, c0[i])) { e = i; break; }
+            if (i < lim && lim > 1) e = -(i + 1);
+        }
+        endj[j] = e;
+    }
+    __syncthreads();
+    // 3. walk the run starts from the sweep's first element; an unfinished run continues its scan here
+    if (threadIdx.x == 0) {
+        if (!reverse) {
+            int s = 0;
+            while (s < len - 1) {
+                own[s] = 1;
+                int e = endj[s];
+                if (e < 0) {
+                    int i = -e - 1;
+                    e = len - 1;
+                    for (; i <= len - 2; i++)
+                        if (!bm_accept<COLS>(A, B, w, h, fixed, i, su[s], sv[s], c0[i])) { e = i; break; }
+                }
+                s = e;
+            }
+        } else {
+            int s = len - 1;
+            while (s > 0) {
+                own[s] = 1;
+                int e = endj[s];
+                if (e < 0) {
+                    int i = -e - 1;
+                    e = 0;
+                    for (; i >= 1; i--)
+                        if (!bm_accept<COLS>(A, B, w, h, fixed, i, su[s], sv[s], c0[i])) { e = i; break; }
+                }
+                s = e;
+            }
+        }
+    }
+    __syncthreads();
+    // 4. every interior element takes the vector of its run's start. Each thread owns a contiguous
+    //    chunk; the start owning the chunk's first element comes from the neighbouring chunks.
+    int nt = blockDim.x;
+    int chunk = (len + nt - 1) / nt;
+    int lo = threadIdx.x * chunk, hi = min(lo + chunk, len);
+    int mark = -1;
+    if (!reverse) { for (int i = lo; i < hi; i++) if (own[i]) mark = i; }
+    else { for (int i = hi - 1; i >= lo; i--) if (own[i]) mark = i; }
+    summ[threadIdx.x] = mark;
+    __syncthreads();
+    if (lo < hi) {
+        int cur = -1;
+        if (!reverse) {
+            for (int t = (int)threadIdx.x - 1; t >= 0 && cur < 0; t--) cur = summ[t];
+            for (int i = lo; i < hi; i++) {
+                if (own[i]) cur = i;
+                if (i >= 1 && i <= len - 2 && cur >= 0 && cur != i) {
+                    fu[gidx(i)] = su[cur];
+                    fv[gidx(i)] = sv[cur];
+                }
+            }
+        } else {
+            for (int t = (int)threadIdx.x + 1; t < nt && cur < 0; t++) cur = summ[t];
+            for (int i = hi - 1; i >= lo; i--) {
+                if (own[i]) cur = i;
+                if (i >= 1 && i <= len - 2 && cur >= 0 && cur != i) {
+                    fu[gidx(i)] = su[cur];
+                    fv[gidx(i)] = sv[cur];
+                }
+            }
+        }
+    }
+}
+
+__global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
+                          float* __restrict__ fv, int w, int h, bool reverse) {
+    int y = blockIdx.x + 1;  // rows 1..h-2
+    if (y > h - 2) return;
+    bm_line<false>(A, B, fu, fv, w, h, y, reverse);
+}
+
+__global__ void k_bm_cols(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
+                          float* __restrict__ fv, int w, int h, bool reverse) {
+    int x = blockIdx.x + 1;  // columns 1..w-2
+    if (x > w - 2) return;
+    bm_line<true>(A, B, fu, fv, w, h, x, reverse);
+}
+
+}  // namespace tw

@@ -1,0 +1,98 @@
+// Strict-mode arithmetic helpers for the retime kernels (sm_100a).
+//
+// Every translation unit of the library is compiled with -fmad=false -prec-div=true
+// -prec-sqrt=true -ftz=false: single precision adds, multiplies and divides round on their own
+// exactly as the reference CPU engine's SSE code does, so the kernels can repeat its operation
+// order bit for bit. These helpers give the x86 truncating conversions the reference relies on
+// (cvttss2si / cvttsd2si: NaN or out of range gives the integer indefinite INT_MIN), which the
+// CUDA cvt.rzi instructions do not (they saturate), and the depth store rules.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tw {
+
+// flow/sample.rs:17-24, warp.rs:104-110: f32 -> i32 truncation, NaN / out of range -> INT_MIN
+__device__ __forceinline__ int32_t cvtt32(float x) {
+    if (!(x >= -2147483648.0f && x < 2147483648.0f)) return INT32_MIN;
+    return __float2int_rz(x);
+}
+// warp.rs:113-120, image.rs:246-252: f64 -> i64 truncation
+__device__ __forceinline__ int64_t cvtt64d(double x) {
+    if (!(x >= -9.223372036854775808e18 && x < 9.223372036854775808e18)) return INT64_MIN;
+    return __double2ll_rz(x);
+}
+// blend.rs:18-25: f32 -> i64 truncation
+__device__ __forceinline__ int64_t cvtt64f(float x) {
+    if (!(x >= -9223372036854775808.0f && x < 9223372036854775808.0f)) return INT64_MIN;
+    return __float2ll_rz(x);
+}
+// image.rs:255-258: q(x) = trunc((f64)x + 0.5); callers keep the low byte / word
+__device__ __forceinline__ int64_t qround(float x) { return cvtt64d((double)x + 0.5); }
+
+// warp.rs:129-135: clamp(trunc(v + 0.5), 0, 255) through the -128 bias and two saturations
+__device__ __forceinline__ uint8_t sat_u8(float v) {
+    int32_t i = cvtt32(v + 0.5f);
+    int32_t t = (int32_t)((uint32_t)i + (uint32_t)(-128));
+    int32_t w = min(max(t, -32768), 32767);
+    int32_t b = min(max(w, -128), 127);
+    return (uint8_t)(b + 128);
+}
+// warp.rs:141-146
+__device__ __forceinline__ uint16_t sat_u16(float v) {
+    int32_t i = cvtt32(v + 0.5f);
+    int32_t t = (int32_t)((uint32_t)i + (uint32_t)(-32768));
+    int32_t w = min(max(t, -32768), 32767);
+    return (uint16_t)(w + 32768);
+}
+
+// nanrule.rs:44-124 (the crate's default `emulator-nan` selection). Numbers are unchanged; only a
+// NaN result takes the rule's payload. Used where the reference repeats an f32 kernel with the rule.
+namespace nr {
+__device__ __forceinline__ float quiet(float x) { return __uint_as_float(__float_as_uint(x) | 0x00400000u); }
+__device__ __forceinline__ float pick(float a, float b) {
+    uint32_t ba = __float_as_uint(a), bb = __float_as_uint(b);
+    bool sa = (ba & 0x00400000u) == 0, sb = (bb & 0x00400000u) == 0;
+    uint32_t fa = ba & 0x007fffffu, fb = bb & 0x007fffffu;
+    bool a_larger = fa > fb || (fa == fb && (ba >> 31) < (bb >> 31));
+    bool take_b = (sa == sb) ? !a_larger : sa;
+    return quiet(take_b ? b : a);
+}
+__device__ __forceinline__ float fix(float r, float a, float b) {
+    if (!isnan(r)) return r;
+    if (isnan(a)) return isnan(b) ? pick(a, b) : quiet(a);
+    if (isnan(b)) return quiet(b);
+    return __uint_as_float(0xffc00000u);
+}
+__device__ __forceinline__ float add(float a, float b) { return fix(a + b, a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return fix(a - b, a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return fix(a * b, a, b); }
+__device__ __forceinline__ float div(float a, float b) { return fix(a / b, a, b); }
+}  // namespace nr
+
+// sample.rs:31-41: index and fraction of one coordinate, clamped into 0..=len-2
+__device__ __forceinline__ void cell(float x, int len, int& io, float& fo) {
+    int i = cvtt32(x);
+    float f = x - (float)i;
+    int last = len - 1;
+    if (i >= last) { i = last - 1; f = 1.0f; }
+    int iu = i < 0 ? 0 : i;
+    int lim = len >= 2 ? len - 2 : 0;
+    io = min(iu, lim);
+    fo = f;
+}
+
+// sample.rs:47-64: (b - a) * f + a chains
+__device__ __forceinline__ float bilinear1(const float* __restrict__ img, int w, int h, float x, float y) {
+    int ix, iy;
+    float fx, fy;
+    cell(x, w, ix, fx);
+    cell(y, h, iy, fy);
+    long i = (long)iy * w + ix;
+    float p00 = __ldg(img + i), p10 = __ldg(img + i + 1), p01 = __ldg(img + i + w), p11 = __ldg(img + i + w + 1);
+    float top = (p10 - p00) * fx + p00;
+    float bot = (p11 - p01) * fx + p01;
+    return (bot - top) * fy + top;
+}
+
+}  // namespace tw

@@ -1,0 +1,90 @@
+"""Seeded synthetic clips standing in for the reference's `testsrc2` footage (which needs ffmpeg).
+
+The clips have the shapes and motion of the benchmark configurations: a band limited value noise
+background (lattice noise on three octaves, smoothly interpolated, rescaled to mean 128 / sd 40 on
+an 8 bit scale) translated by a constant velocity, plus a checker textured square moving on its
+own. Frames come out as wire frames (8 bpc RGBA interleaved, 16 bpc RGBA, or 32 bpc planar
+G, B, R, A), ready for ``tw_retime_frame`` or the oracle.
+"""
+import numpy as np
+
+
+def _lattice_noise(rng, w, h, cell):
+    gw, gh = w // cell + 4, h // cell + 4
+    return rng.standard_normal((gh, gw)).astype(np.float64), cell
+
+
+def _sample(lat, cell, X, Y):
+    # smooth (cubic Hermite) interpolation of the lattice at pixel coordinates; periodic lattice
+    gh, gw = lat.shape
+    fx, fy = X / cell, Y / cell
+    ix, iy = np.floor(fx).astype(np.int64), np.floor(fy).astype(np.int64)
+    tx, ty = fx - ix, fy - iy
+    sx, sy = tx * tx * (3 - 2 * tx), ty * ty * (3 - 2 * ty)
+    ix0, iy0 = ix % gw, iy % gh
+    ix1, iy1 = (ix + 1) % gw, (iy + 1) % gh
+    a = lat[iy0, ix0] * (1 - sx) + lat[iy0, ix1] * sx
+    b = lat[iy1, ix0] * (1 - sx) + lat[iy1, ix1] * sx
+    return a * (1 - sy) + b * sy
+
+
+class NoiseField:
+    """Three octaves of value noise; ``at(X, Y)`` gives values with mean 128, sd 40 (8 bit scale)."""
+
+    def __init__(self, seed, w, h):
+        rng = np.random.RandomState(seed)
+        self.octaves = [(_lattice_noise(rng, w, h, c), a) for c, a in ((24, 1.0), (10, 0.55), (4, 0.3))]
+        X, Y = np.meshgrid(np.arange(w, dtype=np.float64), np.arange(h, dtype=np.float64))
+        v = self._raw(X, Y)
+        self.mu, self.sd = float(v.mean()), float(v.std() or 1.0)
+
+    def _raw(self, X, Y):
+        v = 0.0
+        for (lat, cell), amp in self.octaves:
+            v = v + amp * _sample(lat, cell, X, Y)
+        return v
+
+    def at(self, X, Y):
+        return 128.0 + 40.0 * (self._raw(X, Y) - self.mu) / self.sd
+
+
+def _to_wire(rgb, alpha, depth):
+    """rgb: (H, W, 3) floats on the 8 bit scale; alpha (H, W) in [0, 1]."""
+    h, w = rgb.shape[:2]
+    if depth == 8:
+        px = np.empty((h, w, 4), np.uint8)
+        px[..., :3] = np.clip(np.rint(rgb), 0, 255)
+        px[..., 3] = np.clip(np.rint(alpha * 255.0), 0, 255)
+        return px.reshape(-1)
+    if depth == 16:
+        px = np.empty((h, w, 4), np.uint16)
+        px[..., :3] = np.clip(np.rint(rgb * 257.0), 0, 65535)
+        px[..., 3] = np.clip(np.rint(alpha * 65535.0), 0, 65535)
+        return px.reshape(-1)
+    f = np.empty((4, h, w), np.float32)  # planes G, B, R, A
+    f[0], f[1], f[2] = rgb[..., 1] / 255.0, rgb[..., 2] / 255.0, rgb[..., 0] / 255.0
+    f[3] = alpha
+    return f.reshape(-1)
+
+
+def moving_clip(width, height, frames, depth=8, seed=0x74570001, bg_velocity=(1.5, -0.75), square=32,
+                square_start=(20.0, 30.0), square_velocity=(2.0, 1.0), alpha=None):
+    """A clip of ``frames`` wire frames back to back (one flat array): the noise background
+    translated by ``bg_velocity`` px/frame and a ``square`` x ``square`` checker (8 px cells,
+    values 40 / 215) moving by ``square_velocity``. ``alpha`` (optional callable (X, Y, t) -> [0,1])
+    makes a straight alpha channel; opaque by default."""
+    noise = NoiseField(seed, width, height)
+    X, Y = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64))
+    out = []
+    for t in range(frames):
+        bx, by = bg_velocity[0] * t, bg_velocity[1] * t
+        g = noise.at(X - bx, Y - by)
+        rgb = np.stack([g, 0.85 * g + 20.0, 1.1 * g - 12.0], -1)
+        sx, sy = square_start[0] + square_velocity[0] * t, square_start[1] + square_velocity[1] * t
+        inside = (X >= sx) & (X < sx + square) & (Y >= sy) & (Y < sy + square)
+        chk = ((np.floor((X - sx) / 8) + np.floor((Y - sy) / 8)) % 2 == 0)
+        val = np.where(chk, 40.0, 215.0)
+        rgb = np.where(inside[..., None], val[..., None], rgb)
+        a = np.ones((height, width)) if alpha is None else alpha(X, Y, t)
+        out.append(_to_wire(rgb, a, depth))
+    return np.concatenate(out)
