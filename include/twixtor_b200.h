@@ -127,6 +127,19 @@ size_t tw_last_error(const tw_ctx* ctx, char* buf, size_t cap);
 /* Per-stage counters: launches of the library's kernels since open, and device bytes held. */
 int tw_stats(const tw_ctx* ctx, uint64_t* kernel_launches, uint64_t* device_bytes);
 
+/* Makes the context enqueue on `stream` (a cudaStream_t; NULL is the legacy default stream)
+ * instead of its own, so a caller can order the library's work with its own and time it with its
+ * own events. */
+int tw_set_stream(tw_ctx* ctx, void* stream);
+
+/* Live timing of one kernel by name (for example "k_conv_v"): between begin and end, every launch
+ * of that kernel is bracketed with CUDA events on the context's stream; end returns the summed
+ * device time, the launch count and the algorithmic bytes those launches move (each input plane
+ * read once, each output written once). Replaces the reference's VFX_DEVICE_REPORT counters
+ * (device/exec/mod.rs:141-322). */
+int tw_profile_begin(tw_ctx* ctx, const char* kernel);
+int tw_profile_end(tw_ctx* ctx, double* total_ms, uint64_t* launches, double* bytes);
+
 /* ---- the Stages / Backend seam (stages.rs:33-71, device/exec/backend.rs:27-46) --------------- */
 
 /* Working geometry of a solve (FlowSettings::geometry, flow.rs:129-151): the flow size and the

@@ -346,10 +346,10 @@ int or_select(const or_retime_params* p, int n, int w, int h, float* s0, float* 
     return 0;
 }
 
-// Renders `nout` output frames of the `retime` effect over a raw clip of `nframes` wire frames.
-// Returns 0, or a nonzero status with or_last_error() naming what is not restated.
-int or_retime_clip(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int nout,
-                   void* out) {
+// Renders output frame n of the `retime` effect over a raw clip of `nframes` wire frames into
+// `out` (one wire frame). Returns 0, or a nonzero status with or_last_error() naming what is not
+// restated.
+int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int n, void* out) {
     Fmt f = (Fmt)fmt;
     size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
     size_t frame_bytes = (size_t)w * h * 4 * es;
@@ -357,60 +357,71 @@ int or_retime_clip(const void* frames, int nframes, int w, int h, int fmt, const
     int time_step = integer ? 100 : p->fps_den;
     if (p->smart_blend) return fail(2, "smart blend is not restated in the clip runner");
     float sensitivity = fixed_reader(float_to_fixed(p->sensitivity), 1.0f) / 100.0f;
-    for (int n = 0; n < nout; n++) {
-        float s0, s1, wa;
-        int a, exact, vq, interp;
-        or_select(p, n, w, h, &s0, &s1, &a, &wa, &exact, &vq, &interp);
-        auto fetch = [&](int pos) -> Image {
-            // main_frame(position): frame_time (dur == lts, equal rates), then the clip frame of that tick
-            double d = (double)(float)pos;
-            int time = cvtt_i32_d(d * (double)time_step + 0.5);
-            long long idx = time >= 0 ? time / time_step : -(((long long)-time + time_step - 1) / time_step);
-            if (idx < 0 || idx >= nframes) return Image(w, h, f);
-            return from_frame((const uint8_t*)frames + (size_t)idx * frame_bytes, w, h, f);
-        };
-        Image A = fetch(a), B = fetch(a + 1), result;
-        Selection sel;
-        sel.s0 = s0; sel.s1 = s1; sel.a = a; sel.b = a + 1; sel.wa = wa; sel.exact = exact != 0;
-        sel.vectors_quality = vq; sel.interp = interp;
-        std::string e;
-        if (vq != 0 && !exact) {
-            if (interp < 0 || interp > 1) return fail(2, "weighted blend on the vector path is not restated");
-            // plugin 01 runs the motion path on bottom-up rows (plugins/retime/src/glue.rs:39-40,
-            // compose/vector.rs:303-314)
-            Image ar = p->rows_reversed ? rows_reversed(A) : A, br = p->rows_reversed ? rows_reversed(B) : B;
-            FlowSettings fs;
-            fs.quality = vq;
-            fs.hiq = p->quality_high != 0;
-            fs.sensitivity = sensitivity;
-            fs.taps_above_first = p->taps_above_first != 0;
-            FlowField fab, fba;
-            bool have_ab = false, have_ba = false;
-            if (interp == 0) {
-                ComposeSettings cs0;
-                if (nearest_uses_f_ab(wa, cs0.warp_mode)) {
-                    if (!solve(ar, br, fs, &fab, &e)) return fail(1, e);
-                    have_ab = true;
-                } else {
-                    if (!solve(br, ar, fs, &fba, &e)) return fail(1, e);
-                    have_ba = true;
-                }
+    float s0, s1, wa;
+    int a, exact, vq, interp;
+    or_select(p, n, w, h, &s0, &s1, &a, &wa, &exact, &vq, &interp);
+    auto fetch = [&](int pos) -> Image {
+        // main_frame(position): frame_time (dur == lts, equal rates), then the clip frame of that tick
+        double d = (double)(float)pos;
+        int time = cvtt_i32_d(d * (double)time_step + 0.5);
+        long long idx = time >= 0 ? time / time_step : -(((long long)-time + time_step - 1) / time_step);
+        if (idx < 0 || idx >= nframes) return Image(w, h, f);
+        return from_frame((const uint8_t*)frames + (size_t)idx * frame_bytes, w, h, f);
+    };
+    Image A = fetch(a), B = fetch(a + 1), result;
+    Selection sel;
+    sel.s0 = s0; sel.s1 = s1; sel.a = a; sel.b = a + 1; sel.wa = wa; sel.exact = exact != 0;
+    sel.vectors_quality = vq; sel.interp = interp;
+    std::string e;
+    if (vq != 0 && !exact) {
+        if (interp < 0 || interp > 1) return fail(2, "weighted blend on the vector path is not restated");
+        // plugin 01 runs the motion path on bottom-up rows (plugins/retime/src/glue.rs:39-40,
+        // compose/vector.rs:303-314)
+        Image ar = p->rows_reversed ? rows_reversed(A) : A, br = p->rows_reversed ? rows_reversed(B) : B;
+        FlowSettings fs;
+        fs.quality = vq;
+        fs.hiq = p->quality_high != 0;
+        fs.sensitivity = sensitivity;
+        fs.taps_above_first = p->taps_above_first != 0;
+        FlowField fab, fba;
+        bool have_ab = false, have_ba = false;
+        if (interp == 0) {
+            ComposeSettings cs0;
+            if (nearest_uses_f_ab(wa, cs0.warp_mode)) {
+                if (!solve(ar, br, fs, &fab, &e)) return fail(1, e);
+                have_ab = true;
             } else {
-                if (!solve_pair(ar, br, fs, &fab, &fba, &e)) return fail(1, e);
-                have_ab = have_ba = true;
+                if (!solve(br, ar, fs, &fba, &e)) return fail(1, e);
+                have_ba = true;
             }
-            ComposeSettings cs;
-            cs.quality_high = fs.hiq;
-            cs.blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
-            Image o;
-            int rc = compose_vectors(cs, sel, ar, br, have_ab ? &fab : nullptr, have_ba ? &fba : nullptr, &o, &e);
-            if (rc) return fail(rc, e);
-            result = p->rows_reversed ? rows_reversed(o) : o;
         } else {
-            int rc = interpolate(sel, A, B, &result, &e);
-            if (rc) return fail(rc, e);
+            if (!solve_pair(ar, br, fs, &fab, &fba, &e)) return fail(1, e);
+            have_ab = have_ba = true;
         }
-        to_frame(result, (uint8_t*)out + (size_t)n * frame_bytes);
+        ComposeSettings cs;
+        cs.quality_high = fs.hiq;
+        cs.blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
+        Image o;
+        int rc = compose_vectors(cs, sel, ar, br, have_ab ? &fab : nullptr, have_ba ? &fba : nullptr, &o, &e);
+        if (rc) return fail(rc, e);
+        result = p->rows_reversed ? rows_reversed(o) : o;
+    } else {
+        int rc = interpolate(sel, A, B, &result, &e);
+        if (rc) return fail(rc, e);
+    }
+    to_frame(result, out);
+    return 0;
+}
+
+// Renders `nout` output frames of the `retime` effect over a raw clip of `nframes` wire frames.
+int or_retime_clip(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int nout,
+                   void* out) {
+    Fmt f = (Fmt)fmt;
+    size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
+    size_t frame_bytes = (size_t)w * h * 4 * es;
+    for (int n = 0; n < nout; n++) {
+        int rc = or_retime_one(frames, nframes, w, h, fmt, p, n, (uint8_t*)out + (size_t)n * frame_bytes);
+        if (rc) return rc;
     }
     return 0;
 }

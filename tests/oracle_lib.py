@@ -77,6 +77,7 @@ def lib():
         L.or_to_frame.argtypes = [P, i, i, i, P]
         L.or_select.argtypes = [ctypes.POINTER(RetimeParams), i, i, i, P, P, P, P, P, P, P]
         L.or_retime_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
+        L.or_retime_one.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_set_threads.argtypes = [i]
         _lib = L
     return _lib
@@ -185,6 +186,15 @@ def select(params, n, w, h):
                     ctypes.byref(wa), ctypes.byref(ex), ctypes.byref(vq), ctypes.byref(it))
     return dict(s0=s0.value, s1=s1.value, a=a.value, wa=wa.value, exact=bool(ex.value), vq=vq.value,
                 interp=it.value)
+
+
+def retime_one(frames, nframes, w, h, fmt, params, n):
+    """Output frame n alone (the oracle's renderer is stateless per output frame)."""
+    out = np.zeros(w * h * 4, DTYPE[fmt])
+    rc = lib().or_retime_one(ptr(frames), nframes, w, h, fmt, ctypes.byref(params), n, ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out
 
 
 def retime_clip(frames, nframes, w, h, fmt, params, nout):

@@ -228,6 +228,10 @@ def library():
     L.tw_last_error.argtypes = [P, ctypes.c_char_p, ctypes.c_size_t]
     L.tw_last_error.restype = ctypes.c_size_t
     L.tw_stats.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    L.tw_set_stream.argtypes = [P, P]
+    L.tw_profile_begin.argtypes = [P, ctypes.c_char_p]
+    L.tw_profile_end.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64),
+                                 ctypes.POINTER(ctypes.c_double)]
     L.tw_flow_geometry.argtypes = [ctypes.POINTER(_FlowSettings), i32, i32, P, P, P, P, i32]
     L.tw_solve.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), pflow]
     L.tw_solve_pair.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), pflow, pflow]
@@ -318,6 +322,19 @@ class Device:
             buf = ctypes.create_string_buffer(n + 1)
             self._L.tw_last_error(self._h, buf, n + 1)
             raise (_ERRORS.get(rc, StageError))(rc, buf.value.decode())
+
+    def set_stream(self, stream_handle: int):
+        """Enqueue on a caller's CUDA stream (e.g. ``torch.cuda.current_stream().cuda_stream``)."""
+        self._check(self._L.tw_set_stream(self._h, ctypes.c_void_p(stream_handle)))
+
+    def profile_begin(self, kernel: str):
+        self._check(self._L.tw_profile_begin(self._h, kernel.encode()))
+
+    def profile_end(self):
+        """(device ms, launches, algorithmic bytes) of the profiled kernel since profile_begin."""
+        ms, n, b = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_double()
+        self._check(self._L.tw_profile_end(self._h, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(b)))
+        return ms.value, n.value, b.value
 
     def stats(self):
         k, b = ctypes.c_uint64(), ctypes.c_uint64()

@@ -148,9 +148,22 @@ struct DevBuf {
 
 }  // namespace
 
+// Live per-kernel timing for the benchmark: CUDA events around every launch of one named kernel on
+// the context's stream, with the algorithmic bytes each launch moves.
+struct KernelProfile {
+    bool on = false;
+    std::string name;
+    std::vector<cudaEvent_t> ev;  // start, stop pairs
+    double bytes = 0.0;
+    uint64_t launches = 0;
+};
+
 struct tw_ctx {
     int device = 0;
+    KernelProfile prof;
     cudaStream_t stream = nullptr;
+    cudaStream_t own = nullptr;  // the stream the context created
+    bool own_stream = true;
     std::mutex mu;
     std::string err;
     uint64_t launches = 0;
@@ -178,11 +191,29 @@ struct tw_ctx {
 
 namespace {
 
-#define LAUNCH(ctx, kernel, grid, block, smem, ...)                                \
+// Every kernel launch of the library goes through LAUNCHB (LAUNCH passes no byte count): it counts
+// the launch and, when the kernel is the one being profiled, brackets it with events.
+bool prof_match(tw_ctx* ctx, const char* kernel) { return ctx->prof.on && ctx->prof.name == kernel; }
+void prof_mark(tw_ctx* ctx) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, ctx->stream);
+    ctx->prof.ev.push_back(e);
+}
+
+#define LAUNCHB(ctx, nbytes_, kernel, grid, block, smem, ...)                        \
     do {                                                                           \
+        bool _p = prof_match((ctx), #kernel);                                      \
+        if (_p) prof_mark(ctx);                                                    \
         kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);           \
         (ctx)->launches++;                                                         \
+        if (_p) {                                                                  \
+            prof_mark(ctx);                                                        \
+            (ctx)->prof.bytes += (double)(nbytes_);                                \
+            (ctx)->prof.launches++;                                                \
+        }                                                                          \
     } while (0)
+#define LAUNCH(ctx, kernel, grid, block, smem, ...) LAUNCHB(ctx, 0, kernel, grid, block, smem, __VA_ARGS__)
 
 #define CHECK(expr)                 \
     do {                            \
@@ -199,9 +230,10 @@ unsigned grid1(long n) { return (unsigned)((n + TB - 1) / TB); }
 void conv_planes(tw_ctx* ctx, float* const* planes, int c, int w, int h, const Taps& t, bool above_first, float* tmp) {
     bool multi = c > 1;
     for (int i = 0; i < c; i++) {
-        LAUNCH(ctx, k_conv_h, grid2(w, h), TB, 0, planes[i], tmp, w, h, t, multi);
-        LAUNCH(ctx, k_conv_v, grid2(w, h), TB, 0, tmp, planes[i], w, h, t, multi, above_first, (const float*)nullptr,
-               (float*)nullptr);
+        double b = 8.0 * w * h;  // one plane read, one written
+        LAUNCHB(ctx, b, k_conv_h, grid2(w, h), TB, 0, planes[i], tmp, w, h, t, multi);
+        LAUNCHB(ctx, b, k_conv_v, grid2(w, h), TB, 0, tmp, planes[i], w, h, t, multi, above_first, (const float*)nullptr,
+                (float*)nullptr);
     }
 }
 
@@ -255,10 +287,11 @@ size_t pyramid_floats(const Geo& g) {
 // ---- block matching (flow.rs:551-622) -----------------------------------------------------------------
 void block_match(tw_ctx* ctx, const float* A, const float* B, float* fu, float* fv, int w, int h) {
     if (w < 3 || h < 3) return;
-    LAUNCH(ctx, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, false);
-    LAUNCH(ctx, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, true);
-    LAUNCH(ctx, k_bm_cols, w - 2, TB, bm_smem_bytes(h), A, B, fu, fv, w, h, false);
-    LAUNCH(ctx, k_bm_cols, w - 2, TB, bm_smem_bytes(h), A, B, fu, fv, w, h, true);
+    double b = 24.0 * w * h;  // per sweep: the field read and written (8 + 8), A and B read once (4 + 4)
+    LAUNCHB(ctx, b, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, false);
+    LAUNCHB(ctx, b, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, true);
+    LAUNCHB(ctx, b, k_bm_cols, w - 2, TB, bm_smem_bytes(h), A, B, fu, fv, w, h, false);
+    LAUNCHB(ctx, b, k_bm_cols, w - 2, TB, bm_smem_bytes(h), A, B, fu, fv, w, h, true);
 }
 
 // ---- one solve over two resident pyramids (flow.rs:1258-1307) ------------------------------------------
@@ -399,7 +432,10 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
     } else {
         return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
     }
-    LAUNCH(ctx, k_compose_blend, grid2(W, H), TB, 0, pa, pb, fmt, wb, mode, out, W, H, to_wire, flip_out, bad);
+    // A and B read, the output written, the two flows read (at their own resolution)
+    double px = (double)W * H * 4 * sample_bytes(fmt);
+    LAUNCHB(ctx, 3.0 * px + 16.0 * fw * fh, k_compose_blend, grid2(W, H), TB, 0, pa, pb, fmt, wb, mode, out, W, H,
+            to_wire, flip_out, bad);
     return TW_OK;
 }
 
@@ -453,8 +489,9 @@ int tw_open(int device, tw_ctx** out) {
     ctx->device = device;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) { delete ctx; return TW_ERR_CUDA; }
-    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete ctx; return TW_ERR_CUDA; }
+    ctx->stream = ctx->own;
     ctx->g7 = gaussian_taps(7.0f);
     ctx->g5 = gaussian_taps(5.0f);
     ctx->b5 = binomial5();
@@ -480,7 +517,8 @@ void tw_close(tw_ctx* ctx) {
     for (int i = 0; i < 3; i++) { ctx->eng[i].release(&ctx->held); ctx->wire[i].release(&ctx->held); }
     for (int i = 0; i < 2; i++) { ctx->pyr[i].release(&ctx->held); ctx->work[i].release(&ctx->held); ctx->flow[i].release(&ctx->held); }
     for (int i = 0; i < 4; i++) ctx->plane[i].release(&ctx->held);
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    for (auto e : ctx->prof.ev) cudaEventDestroy(e);
     delete ctx;
 }
 
@@ -499,6 +537,42 @@ int tw_stats(const tw_ctx* ctx, uint64_t* kernel_launches, uint64_t* device_byte
     if (!ctx) return TW_ERR_BAD_PARAM;
     if (kernel_launches) *kernel_launches = ctx->launches;
     if (device_bytes) *device_bytes = ctx->held;
+    return TW_OK;
+}
+
+int tw_profile_begin(tw_ctx* ctx, const char* kernel) {
+    if (!ctx || !kernel) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    for (auto e : ctx->prof.ev) cudaEventDestroy(e);
+    ctx->prof = KernelProfile();
+    ctx->prof.on = true;
+    ctx->prof.name = kernel;
+    return TW_OK;
+}
+
+int tw_profile_end(tw_ctx* ctx, double* total_ms, uint64_t* launches, double* bytes) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "profile sync"));
+    double ms = 0.0;
+    for (size_t i = 0; i + 1 < ctx->prof.ev.size(); i += 2) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, ctx->prof.ev[i], ctx->prof.ev[i + 1]);
+        ms += t;
+    }
+    if (total_ms) *total_ms = ms;
+    if (launches) *launches = ctx->prof.launches;
+    if (bytes) *bytes = ctx->prof.bytes;
+    for (auto e : ctx->prof.ev) cudaEventDestroy(e);
+    ctx->prof = KernelProfile();
+    return TW_OK;
+}
+
+int tw_set_stream(tw_ctx* ctx, void* stream) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->stream = (cudaStream_t)stream;
+    ctx->own_stream = false;
     return TW_OK;
 }
 

@@ -72,13 +72,31 @@ def moving_clip(width, height, frames, depth=8, seed=0x74570001, bg_velocity=(1.
     """A clip of ``frames`` wire frames back to back (one flat array): the noise background
     translated by ``bg_velocity`` px/frame and a ``square`` x ``square`` checker (8 px cells,
     values 40 / 215) moving by ``square_velocity``. ``alpha`` (optional callable (X, Y, t) -> [0,1])
-    makes a straight alpha channel; opaque by default."""
+    makes a straight alpha channel; opaque by default.
+
+    The background is evaluated once over the area every frame's translation covers and each
+    frame resamples it bilinearly at its sub-pixel offset."""
     noise = NoiseField(seed, width, height)
+    vx, vy = bg_velocity
+    span_x = abs(vx) * max(frames - 1, 0)
+    span_y = abs(vy) * max(frames - 1, 0)
+    ox = -(span_x if vx > 0 else 0.0) - 1.0
+    oy = -(span_y if vy > 0 else 0.0) - 1.0
+    bw, bh = int(np.ceil(width + span_x)) + 3, int(np.ceil(height + span_y)) + 3
+    BX, BY = np.meshgrid(np.arange(bw, dtype=np.float64) + ox, np.arange(bh, dtype=np.float64) + oy)
+    base = noise.at(BX, BY)
     X, Y = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64))
     out = []
     for t in range(frames):
-        bx, by = bg_velocity[0] * t, bg_velocity[1] * t
-        g = noise.at(X - bx, Y - by)
+        # background value at (X - vx t, Y - vy t): position inside the base grid
+        px, py = -vx * t - ox, -vy * t - oy
+        ix, iy = int(np.floor(px)), int(np.floor(py))
+        fx, fy = px - ix, py - iy
+        b00 = base[iy:iy + height, ix:ix + width]
+        b10 = base[iy:iy + height, ix + 1:ix + 1 + width]
+        b01 = base[iy + 1:iy + 1 + height, ix:ix + width]
+        b11 = base[iy + 1:iy + 1 + height, ix + 1:ix + 1 + width]
+        g = (b00 * (1 - fx) + b10 * fx) * (1 - fy) + (b01 * (1 - fx) + b11 * fx) * fy
         rgb = np.stack([g, 0.85 * g + 20.0, 1.1 * g - 12.0], -1)
         sx, sy = square_start[0] + square_velocity[0] * t, square_start[1] + square_velocity[1] * t
         inside = (X >= sx) & (X < sx + square) & (Y >= sy) & (Y < sy + square)
