@@ -47,7 +47,8 @@ typedef enum tw_status {
     TW_ERR_UNSUPPORTED = 3,
     TW_ERR_MISMATCH = 4,
     TW_ERR_BAD_PARAM = 5,
-    TW_ERR_DEVICE_BOUND = 6 /* a data-dependent device loop reached its bound (never for finite data) */
+    TW_ERR_DEVICE_BOUND = 6, /* a data-dependent device loop reached its bound (never for finite data) */
+    TW_ERR_TOO_LARGE = 7     /* tw_block_match_noalloc: width * height above TW_NOALLOC_MAX_PIXELS */
 } tw_status;
 
 typedef enum tw_fmt { TW_U8 = 0, TW_U16 = 1, TW_F32 = 2 } tw_fmt;
@@ -171,6 +172,25 @@ int tw_build_pyramid(tw_ctx* ctx, const tw_image* img, const tw_flow_settings* s
 /* flow::block_match (flow.rs:551-622): the four in-place sweeps over a level; a and b are the
  * band pass planes of X and Y (w*h floats), flow is interleaved (w*h*2 floats), updated in place. */
 int tw_block_match(tw_ctx* ctx, const float* a, const float* b, float* flow, int32_t width, int32_t height);
+
+/* Block matching for callers that cannot allocate device memory. No counterpart in the reference.
+ *
+ * Some hosts cannot call cudaMalloc: a plugin inside an application that owns the device memory
+ * pool and hands out only its own frame buffers, or a real-time render thread where a driver
+ * allocation can stall or is not allowed. This is tw_block_match with DEVICE pointers: a and b
+ * (width * height floats each) and flow (width * height * 2 floats, interleaved, updated in place)
+ * are the caller's device buffers, and the call allocates nothing (no cudaMalloc or cudaFree, no
+ * context). Its scratch is a fixed device array inside the library, 2 * TW_NOALLOC_MAX_PIXELS
+ * floats (4 MiB), which every GPU that loads the library holds until the process exits; frames
+ * above TW_NOALLOC_MAX_PIXELS pixels (e.g. anything above a 960 x 540 working size plus a
+ * little), or a side above 8192, return TW_ERR_TOO_LARGE. The work runs on `stream` (a
+ * cudaStream_t, NULL for the default stream) of the current device and the call returns when it
+ * is done. The first call on a device looks up the array's device address and sets the kernels'
+ * shared memory limit (no allocation either), so make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (from several host threads or
+ * streams at once) race on it and must be serialised by the caller. */
+#define TW_NOALLOC_MAX_PIXELS (1L << 19)
+int tw_block_match_noalloc(const float* a, const float* b, float* flow, int32_t width, int32_t height, void* stream);
 
 /* warp::inv_warp / inv_warp_coverage (warp.rs:693-786) with mode 1 and is360 off; cov may be NULL
  * (no coverage image) or width*height bytes. */

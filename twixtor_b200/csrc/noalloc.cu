@@ -1,0 +1,78 @@
+// Block matching for callers that cannot allocate device memory.
+//
+// Some hosts cannot call cudaMalloc at all: a plugin running inside an application that owns the
+// device memory pool (a video host that hands out only its own frame buffers), or code on a
+// real-time render thread where a driver allocation can stall or is forbidden. They can still pass
+// their own device buffers for the inputs and the output. This entry point runs the four block
+// matching sweeps (flow.rs:551-622) on such buffers without allocating anything: its only scratch,
+// the field split into two float planes, lives in the file-scope device array below, which every
+// GPU that loads the library holds until the process exits.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "../../include/twixtor_b200.h"
+#include "kernels.cuh"
+
+namespace {
+
+// Scratch of the allocation-free block matching: the u and v planes of the field.
+constexpr long NOALLOC_MAX_PIXELS = TW_NOALLOC_MAX_PIXELS;
+static __device__ __align__(256) float g_noalloc_planes[2 * NOALLOC_MAX_PIXELS];
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_setup_mu;
+float* g_planes_addr[MAX_DEVICES] = {};  // device address of g_noalloc_planes, per device
+
+// Once per device, with that device current: the device address of the scratch array (the host
+// side name g_noalloc_planes is only a stand-in, not a device pointer) and the shared memory limit
+// of the sweep kernels. Neither allocates.
+int setup(int device, float** planes) {
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    if (device < 0 || device >= MAX_DEVICES) return TW_ERR_UNSUPPORTED;
+    if (!g_planes_addr[device]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_planes) != cudaSuccess || !p) return TW_ERR_CUDA;
+        if (cudaFuncSetAttribute(tw::k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tw::bm_smem_bytes(8192)) != cudaSuccess)
+            return TW_ERR_CUDA;
+        if (cudaFuncSetAttribute(tw::k_bm_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tw::bm_smem_bytes(8192)) != cudaSuccess)
+            return TW_ERR_CUDA;
+        g_planes_addr[device] = (float*)p;
+    }
+    *planes = g_planes_addr[device];
+    return TW_OK;
+}
+
+}  // namespace
+
+extern "C" int tw_block_match_noalloc(const float* a, const float* b, float* flow, int32_t width, int32_t height,
+                                      void* stream) {
+    if (!a || !b || !flow || width <= 0 || height <= 0) return TW_ERR_BAD_PARAM;
+    if ((long)width * height > NOALLOC_MAX_PIXELS || width > 8192 || height > 8192) return TW_ERR_TOO_LARGE;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return TW_ERR_CUDA;
+    float* planes = nullptr;
+    int rc = setup(device, &planes);
+    if (rc != TW_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    long n = (long)width * height;
+    float* fu = planes;
+    float* fv = planes + n;
+    const int tb = 256;
+    unsigned g1 = (unsigned)((n + tb - 1) / tb);
+    // every element of the two planes this call reads is written first, so the previous call's
+    // contents never reach the result
+    tw::k_deinterleave<<<g1, tb, 0, s>>>(flow, n, fu, fv);
+    if (width >= 3 && height >= 3) {
+        tw::k_bm_rows<<<height - 2, tb, tw::bm_smem_bytes(width), s>>>(a, b, fu, fv, width, height, false);
+        tw::k_bm_rows<<<height - 2, tb, tw::bm_smem_bytes(width), s>>>(a, b, fu, fv, width, height, true);
+        tw::k_bm_cols<<<width - 2, tb, tw::bm_smem_bytes(height), s>>>(a, b, fu, fv, width, height, false);
+        tw::k_bm_cols<<<width - 2, tb, tw::bm_smem_bytes(height), s>>>(a, b, fu, fv, width, height, true);
+    }
+    tw::k_interleave<<<g1, tb, 0, s>>>(fu, fv, n, flow);
+    if (cudaGetLastError() != cudaSuccess) return TW_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return TW_ERR_CUDA;
+    return TW_OK;
+}
