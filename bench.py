@@ -307,6 +307,10 @@ def main():
         peak, which = peaks()
         achieved = (kbytes / (kms / 1e3)) / 1e9 if kms > 0 else None
         tr = traffic_of(ROOFLINE_KERNEL)
+        if isinstance(tr, dict):
+            # DRAM bytes of the captured launch scaled to the average launch of the timed region by
+            # the algorithmic bytes each moves (traffic grows in proportion to the units processed)
+            tr = tr["dram_bytes"] / tr["algorithmic_bytes"] * (kbytes / max(klaunch, 1))
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
