@@ -100,4 +100,25 @@ __global__ void k_lerp(void* __restrict__ first, const void* __restrict__ second
 __global__ void k_compose_blend(WarpParams pa, WarpParams pb, int fmt, float wblend, int blend_mode, void* __restrict__ out,
                                 int w, int h, bool to_wire, bool flip_out, int* __restrict__ bad);
 
+// ---- fused, shared-memory tiled kernels (fused.cu) -----------------------------------------------------
+constexpr int FUSED_TILE_X = 32, FUSED_TILE_Y = 32, FUSED_THREADS = 256;
+__global__ void k_blur5_band(const float* __restrict__ orig, const void* __restrict__ luma_src, int fmt, int w, int h,
+                             bool above_first, float* __restrict__ tmp_out, float* __restrict__ band_out);
+__global__ void k_level_init(const float* __restrict__ img, int w, int h, Taps g7, bool above_first,
+                             float* __restrict__ gxo, float* __restrict__ gyo, float* __restrict__ a0o,
+                             float* __restrict__ a1o, float* __restrict__ a2o);
+size_t level_init_smem();
+__global__ void k_level_iter(const float* __restrict__ i1, const float* __restrict__ i0, const float* __restrict__ gx,
+                             const float* __restrict__ gy, const float* __restrict__ a0, const float* __restrict__ a1,
+                             const float* __restrict__ a2, const float* __restrict__ fu, const float* __restrict__ fv,
+                             int w, int h, Taps g7, Taps g5, bool above_first, float* __restrict__ fu_out,
+                             float* __restrict__ fv_out);
+size_t level_iter_smem();
+__global__ void k_apply_upsample(const float* __restrict__ su, const float* __restrict__ sv, int sw, int sh,
+                                 const int* __restrict__ any, int l, int start, bool damp_now, float damp,
+                                 float* __restrict__ du, float* __restrict__ dv, int dw, int dh);
+__global__ void k_apply_negate(const float* __restrict__ fu, const float* __restrict__ fv, long n,
+                               const int* __restrict__ any, int start, bool damp_now, float damp,
+                               float* __restrict__ out, int* __restrict__ nan_flag);
+
 }  // namespace tw

@@ -222,6 +222,10 @@ void prof_mark(tw_ctx* ctx) {
     } while (0)
 
 constexpr int TB = 256;
+// device flags (ints): [0..31] per-level range flags of solve 0, [32..63] of solve 1, [64] NaN in a
+// flow, [65] a warp refused a sample coordinate
+constexpr int FL_ANY0 = 0, FL_ANY1 = 32, FL_NAN = 64, FL_BAD = 65;
+constexpr size_t FLAGS_BYTES = 128 * sizeof(int);
 
 dim3 grid2(int w, int h) { return dim3((unsigned)((w + TB - 1) / TB), (unsigned)h); }
 unsigned grid1(long n) { return (unsigned)((n + TB - 1) / TB); }
@@ -238,27 +242,36 @@ void conv_planes(tw_ctx* ctx, float* const* planes, int c, int w, int h, const T
 }
 
 // ---- the pyramid of one engine image (flow.rs:242-275) ----------------------------------------------
-// Builds the band pass levels into `out` (levels concatenated, finest first). Scratch: plane[0..3].
+// Builds the band pass levels into `out` (levels concatenated, finest first). Scratch: plane[0..2].
+// Luma, the reduction steps (prep.rs:252-259) and each level's blur5 + band run as tiled kernels
+// (k_blur5_band), each followed by the corner aligned resample to the next size.
+dim3 tiles(int w, int h) { return dim3((unsigned)((w + FUSED_TILE_X - 1) / FUSED_TILE_X), (unsigned)((h + FUSED_TILE_Y - 1) / FUSED_TILE_Y)); }
+
 int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, const tw_flow_settings& s, const Geo& g,
                       float* out) {
     if (s.prep_contrast_edge || s.prep_delinearize)
         return ctx->fail(TW_ERR_UNSUPPORTED, "image prep (Contrast/Edge Enhance, Delinearize) is not on the device");
     if (s.video_range_luma && s.track_alpha)
         return ctx->fail(TW_ERR_UNSUPPORTED, "optical flow luma: video range conversion together with Track RGB+A is not supported");
+    if (s.video_range_luma || s.track_alpha)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "video range luma and Track RGB+A are not on the device");
     size_t full = (size_t)W * H * sizeof(float);
     for (int i = 0; i < 3; i++) CHECK(ctx->ensure(ctx->plane[i], full, "pyramid scratch"));
     float* cur = ctx->plane[0].as<float>();
     float* tmp = ctx->plane[1].as<float>();
     float* nxt = ctx->plane[2].as<float>();
-    long n = (long)W * H;
-    LAUNCH(ctx, k_luma, grid1(n), TB, 0, eng_dev, fmt, cur, W, H, s.track_alpha != 0, s.video_range_luma != 0);
-    int cw = W, ch = H;
     bool af = s.taps_above_first != 0;
-    for (int r = 0; r < g.reduction; r++) {  // prep.rs:252-259
-        LAUNCH(ctx, k_conv_h, grid2(cw, ch), TB, 0, cur, tmp, cw, ch, ctx->b5, false);
-        LAUNCH(ctx, k_conv_v, grid2(cw, ch), TB, 0, tmp, cur, cw, ch, ctx->b5, false, af, (const float*)nullptr, (float*)nullptr);
+    int cw = W, ch = H;
+    if (g.reduction == 0) {
+        long n = (long)W * H;
+        LAUNCH(ctx, k_luma, grid1(n), TB, 0, eng_dev, fmt, cur, W, H, false, false);
+    }
+    for (int r = 0; r < g.reduction; r++) {  // prep.rs:252-259; the first step reads the luma on the fly
+        LAUNCHB(ctx, (r == 0 ? 4.0 * sample_bytes(fmt) : 4.0) * cw * ch + 4.0 * cw * ch, k_blur5_band, tiles(cw, ch),
+                FUSED_THREADS, 0, r == 0 ? (const float*)nullptr : cur, r == 0 ? eng_dev : nullptr, fmt, cw, ch, af, tmp,
+                (float*)nullptr);
         int nw = cw / 2, nh = ch / 2;
-        LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, cur, cw, ch, nxt, nw, nh);
+        LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, tmp, cw, ch, nxt, nw, nh);
         std::swap(cur, nxt);
         cw = nw;
         ch = nh;
@@ -266,12 +279,11 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
     size_t off = 0;
     for (int i = 0; i < g.levels; i++) {
         int lw = g.sizes[i][0], lh = g.sizes[i][1];
-        float* band = out + off;
-        LAUNCH(ctx, k_conv_h, grid2(lw, lh), TB, 0, cur, tmp, lw, lh, ctx->b5, false);
-        LAUNCH(ctx, k_conv_v, grid2(lw, lh), TB, 0, tmp, nxt, lw, lh, ctx->b5, false, af, (const float*)cur, band);
+        LAUNCHB(ctx, 12.0 * lw * lh, k_blur5_band, tiles(lw, lh), FUSED_THREADS, 0, cur, (const void*)nullptr, fmt, lw, lh,
+                af, tmp, out + off);
         if (i + 1 < g.levels) {
             int nw = g.sizes[i + 1][0], nh = g.sizes[i + 1][1];
-            LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, nxt, lw, lh, cur, nw, nh);
+            LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, tmp, lw, lh, cur, nw, nh);
         }
         off += (size_t)lw * lh;
     }
@@ -296,17 +308,19 @@ void block_match(tw_ctx* ctx, const float* A, const float* B, float* fu, float* 
 
 // ---- one solve over two resident pyramids (flow.rs:1258-1307) ------------------------------------------
 // x, y: band pass levels of X and Y; work: scratch for this solve; out: interleaved flow at level 0
-// size (device). nan_flag: set when the result holds a NaN.
+// size (device). any: 32 ints of per-level "some pixel in range" flags; nan_flag: set when the
+// result holds a NaN. Per level: one tiled kernel for the gradient and the blurred tensor, one per
+// iteration (calc_b, blur7, new_disp, blur5 in shared memory, the flow ping-ponged), the block
+// matching sweeps, the range check, and the reset / damping fused into the upsample.
 int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const Geo& g, const tw_flow_settings& s,
-                       DevBuf& work, float* out, int* state, int* nan_flag) {
+                       DevBuf& work, float* out, int* any, int* nan_flag) {
     size_t np0 = (size_t)g.w * g.h;
-    // planes: gx gy a0 a1 a2 bx by fu fv uu uv tmp
-    const int NP = 12;
+    // planes: gx gy a0 a1 a2 u0 v0 u1 v1
+    const int NP = 9;
     CHECK(ctx->ensure(work, np0 * NP * sizeof(float), "solve scratch"));
     float* base = work.as<float>();
     float *gx = base, *gy = base + np0, *a0 = base + 2 * np0, *a1 = base + 3 * np0, *a2 = base + 4 * np0;
-    float *bx = base + 5 * np0, *by = base + 6 * np0, *fu = base + 7 * np0, *fv = base + 8 * np0;
-    float *uu = base + 9 * np0, *uv = base + 10 * np0, *tmp = base + 11 * np0;
+    float *fu = base + 5 * np0, *fv = base + 6 * np0, *nu = base + 7 * np0, *nv = base + 8 * np0;
     int start;
     float damp;
     start_level(s.sensitivity, g.levels, &start, &damp);
@@ -314,40 +328,38 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const Geo& g
     size_t off = 0;
     for (int i = 0; i < g.levels; i++) { offs[i] = off; off += (size_t)g.sizes[i][0] * g.sizes[i][1]; }
     long ns = (long)g.sizes[start][0] * g.sizes[start][1];
-    LAUNCH(ctx, k_fill, grid1(ns), TB, 0, fu, ns, 0.0f);
-    LAUNCH(ctx, k_fill, grid1(ns), TB, 0, fv, ns, 0.0f);
-    LAUNCH(ctx, k_range_init, 1, 32, 0, state);
+    CHECK(ctx->cuda(cudaMemsetAsync(fu, 0, ns * sizeof(float), ctx->stream), "flow init"));
+    CHECK(ctx->cuda(cudaMemsetAsync(fv, 0, ns * sizeof(float), ctx->stream), "flow init"));
+    CHECK(ctx->cuda(cudaMemsetAsync(any, 0, 32 * sizeof(int), ctx->stream), "range flags"));
     bool af = s.taps_above_first != 0;
-    bool damp_now_any = std::fabs((double)damp - 1.0) >= 1e-6;
+    bool damp_any = std::fabs((double)damp - 1.0) >= 1e-6;
     for (int l = start; l >= 0; l--) {
         int w = g.sizes[l][0], h = g.sizes[l][1];
-        long n = (long)w * h;
         const float* A = x + offs[l];
         const float* B = y + offs[l];
-        LAUNCH(ctx, k_grad_tensor, grid2(w, h), TB, 0, A, w, h, gx, gy, a0, a1, a2);
-        float* ap[3] = {a0, a1, a2};
-        conv_planes(ctx, ap, 3, w, h, ctx->g7, af, tmp);
+        double px = (double)w * h;
+        LAUNCHB(ctx, 24.0 * px, k_level_init, tiles(w, h), FUSED_THREADS, level_init_smem(), A, w, h, ctx->g7, af, gx, gy,
+                a0, a1, a2);
         for (int it = 0; it < 3; it++) {
-            LAUNCH(ctx, k_calc_b, grid2(w, h), TB, 0, A, B, gx, gy, fu, fv, w, h, bx, by);
-            float* bp[2] = {bx, by};
-            conv_planes(ctx, bp, 2, w, h, ctx->g7, af, tmp);
-            LAUNCH(ctx, k_new_disp, grid1(n), TB, 0, fu, fv, a0, a1, a2, bx, by, n);
-            float* fp[2] = {fu, fv};
-            conv_planes(ctx, fp, 2, w, h, ctx->g5, af, tmp);
+            // I1, I0 (gather), grad, tensor, flow in; flow out
+            LAUNCHB(ctx, 4.0 * px * 12, k_level_iter, tiles(w, h), FUSED_THREADS, level_iter_smem(), A, B, gx, gy, a0, a1,
+                    a2, fu, fv, w, h, ctx->g7, ctx->g5, af, nu, nv);
+            std::swap(fu, nu);
+            std::swap(fv, nv);
             if (it == 1 && l == 0 && !s.skip_refine) block_match(ctx, A, B, fu, fv, w, h);
         }
         if (l != 0 && !s.skip_refine) block_match(ctx, A, B, fu, fv, w, h);
-        LAUNCH(ctx, k_range_any, grid2(w, h), TB, 0, fu, fv, w, h, state + 1);
-        LAUNCH(ctx, k_range_apply, grid1(n), TB, 0, fu, fv, n, state, l == start && damp_now_any, damp);
-        LAUNCH(ctx, k_range_next, 1, 32, 0, state);
+        LAUNCH(ctx, k_range_any, grid2(w, h), TB, 0, fu, fv, w, h, any + l);
+        bool damp_now = l == start && damp_any;
         if (l > 0) {
-            int nw = g.sizes[l - 1][0], nh = g.sizes[l - 1][1];
-            LAUNCH(ctx, k_upsample_flow, grid2(nw, nh), TB, 0, fu, fv, w, h, uu, uv, nw, nh);
-            std::swap(fu, uu);
-            std::swap(fv, uv);
+            int dw = g.sizes[l - 1][0], dh = g.sizes[l - 1][1];
+            LAUNCH(ctx, k_apply_upsample, grid2(dw, dh), TB, 0, fu, fv, w, h, any, l, start, damp_now, damp, nu, nv, dw, dh);
+            std::swap(fu, nu);
+            std::swap(fv, nv);
+        } else {
+            LAUNCH(ctx, k_apply_negate, grid1((long)np0), TB, 0, fu, fv, (long)np0, any, start, damp_now, damp, out, nan_flag);
         }
     }
-    LAUNCH(ctx, k_negate_interleave, grid1((long)np0), TB, 0, fu, fv, (long)np0, out, nan_flag);
     return TW_OK;
 }
 
@@ -498,7 +510,9 @@ int tw_open(int device, tw_ctx** out) {
     // block matching keeps one line of the field in shared memory (up to 8192 elements)
     cudaFuncSetAttribute(k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(8192));
     cudaFuncSetAttribute(k_bm_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(8192));
-    if (ctx->ensure(ctx->flags, 64, "flags") != TW_OK) { tw_close(ctx); return TW_ERR_CUDA; }
+    cudaFuncSetAttribute(k_level_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)level_init_smem());
+    cudaFuncSetAttribute(k_level_iter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)level_iter_smem());
+    if (ctx->ensure(ctx->flags, FLAGS_BYTES, "flags") != TW_OK) { tw_close(ctx); return TW_ERR_CUDA; }
     k_selfcheck<<<1, 1, 0, ctx->stream>>>(ctx->flags.as<int>());
     ctx->launches++;
     int ok = 0;
@@ -598,7 +612,7 @@ static int upload_image(tw_ctx* ctx, DevBuf& b, const tw_image* im) {
 }
 
 static int finish(tw_ctx* ctx, int* flags_host, int n) {
-    cudaError_t e = cudaMemcpyAsync(flags_host, ctx->flags.p, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e = cudaMemcpyAsync(flags_host, (int*)ctx->flags.p + FL_NAN, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess) e = cudaGetLastError();
     return ctx->cuda(e, "kernel execution");
@@ -631,19 +645,19 @@ static int solve_common(tw_ctx* ctx, const tw_image* a, const tw_image* b, const
     CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
     CHECK(ctx->ensure(ctx->flow[1], fb, "flow"));
     int* flags = ctx->flags.as<int>();
-    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, 64, ctx->stream), "flags"));
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
     // f_ab = solve(X = A, Y = B); f_ba = solve(X = B, Y = A)
     if (f_ab)
         CHECK(solve_pyramids_dev(ctx, ctx->pyr[0].as<float>(), ctx->pyr[1].as<float>(), g, *s, ctx->work[0],
-                                 ctx->flow[0].as<float>(), flags + 0, flags + 4));
+                                 ctx->flow[0].as<float>(), flags + FL_ANY0, flags + FL_NAN));
     if (pair && f_ba)
         CHECK(solve_pyramids_dev(ctx, ctx->pyr[1].as<float>(), ctx->pyr[0].as<float>(), g, *s, ctx->work[1],
-                                 ctx->flow[1].as<float>(), flags + 2, flags + 4));
+                                 ctx->flow[1].as<float>(), flags + FL_ANY1, flags + FL_NAN));
     if (f_ab) CHECK(ctx->cuda(cudaMemcpyAsync(f_ab->data, ctx->flow[0].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
     if (pair && f_ba) CHECK(ctx->cuda(cudaMemcpyAsync(f_ba->data, ctx->flow[1].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
-    int hf[8];
-    CHECK(finish(ctx, hf, 8));
-    if (hf[4]) return ctx->fail(TW_ERR_NAN_OUTPUT, "the solved flow holds a NaN");
+    int hf[2];
+    CHECK(finish(ctx, hf, 2));
+    if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "the solved flow holds a NaN");
     return TW_OK;
 }
 
@@ -706,14 +720,14 @@ int tw_compose_vectors(tw_ctx* ctx, const tw_engine_settings* settings, const tw
     size_t ob = (size_t)a->width * a->height * 4 * sample_bytes(a->fmt);
     CHECK(ctx->ensure(ctx->eng[2], ob, "compose output"));
     int* flags = ctx->flags.as<int>();
-    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, 64, ctx->stream), "flags"));
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
     CHECK(compose_dev(ctx, *settings, *sel, ctx->eng[0].p, ctx->eng[1].p, f_ab ? ctx->flow[0].as<float>() : nullptr,
                       f_ba ? ctx->flow[1].as<float>() : nullptr, fw, fh, a->width, a->height, a->fmt, ctx->eng[2].p,
-                      false, false, flags + 5));
+                      false, false, flags + FL_BAD));
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
-    int hf[8];
-    CHECK(finish(ctx, hf, 8));
-    if (hf[5]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    int hf[2];
+    CHECK(finish(ctx, hf, 2));
+    if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
     return TW_OK;
 }
 
@@ -759,15 +773,15 @@ int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_fl
     CHECK(ctx->ensure(ctx->eng[2], ob, "warp output"));
     CHECK(ctx->ensure(ctx->plane[3], (size_t)W * H, "coverage"));
     int* flags = ctx->flags.as<int>();
-    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, 64, ctx->stream), "flags"));
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
     WarpParams p = warp_params(ctx->eng[0].p, ctx->flow[0].as<float>(), flow->width, flow->height, amount, W, hold != 0);
     uint8_t* dcov = cov ? ctx->plane[3].as<uint8_t>() : nullptr;
-    LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, p, src->fmt, ctx->eng[2].p, dcov, W, H, flags + 5);
+    LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, p, src->fmt, ctx->eng[2].p, dcov, W, H, flags + FL_BAD);
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     if (cov) CHECK(ctx->cuda(cudaMemcpyAsync(cov, dcov, (size_t)W * H, cudaMemcpyDeviceToHost, ctx->stream), "download"));
-    int hf[8];
-    CHECK(finish(ctx, hf, 8));
-    if (hf[5]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    int hf[2];
+    CHECK(finish(ctx, hf, 2));
+    if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
     return TW_OK;
 }
 
@@ -788,7 +802,7 @@ int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* 
     WarpParams pb = warp_params(ctx->eng[1].p, nullptr, 0, 0, 0.0f, W, true);
     int* flags = ctx->flags.as<int>();
     LAUNCH(ctx, k_compose_blend, grid2(W, H), TB, 0, pa, pb, a->fmt, w, blend_mode(w), ctx->eng[2].p, W, H, false, false,
-           flags + 5);
+           flags + FL_BAD);
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     int hf[1];
     return finish(ctx, hf, 1);
@@ -852,7 +866,7 @@ static int retime_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_s
     else CHECK(ctx->cuda(cudaMemsetAsync(ctx->eng[0].p, 0, bytes, ctx->stream), "blank"));
     if (wb) from_frame_dev(ctx, wb, ctx->eng[1].p, W, H, fmt, flip);
     else CHECK(ctx->cuda(cudaMemsetAsync(ctx->eng[1].p, 0, bytes, ctx->stream), "blank"));
-    if (!vector) return interpolate_dev(ctx, sel, ctx->eng[0].p, ctx->eng[1].p, W, H, fmt, out_wire, true, flags + 5);
+    if (!vector) return interpolate_dev(ctx, sel, ctx->eng[0].p, ctx->eng[1].p, W, H, fmt, out_wire, true, flags + FL_BAD);
 
     // the vector path (compose/vector.rs:163-178 solve_flows, then compose_vectors)
     tw_flow_settings fs = s.flow;
@@ -878,20 +892,20 @@ static int retime_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_s
     }
     if (need_ab)
         CHECK(solve_pyramids_dev(ctx, ctx->pyr[0].as<float>(), ctx->pyr[1].as<float>(), g, fs, ctx->work[0],
-                                 ctx->flow[0].as<float>(), flags + 0, flags + 4));
+                                 ctx->flow[0].as<float>(), flags + FL_ANY0, flags + FL_NAN));
     if (need_ba)
         CHECK(solve_pyramids_dev(ctx, ctx->pyr[1].as<float>(), ctx->pyr[0].as<float>(), g, fs, ctx->work[1],
-                                 ctx->flow[1].as<float>(), flags + 2, flags + 4));
+                                 ctx->flow[1].as<float>(), flags + FL_ANY1, flags + FL_NAN));
     return compose_dev(ctx, s.compose, sel, ctx->eng[0].p, ctx->eng[1].p, need_ab ? ctx->flow[0].as<float>() : nullptr,
                        need_ba ? ctx->flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, out_wire, true, flip,
-                       flags + 5);
+                       flags + FL_BAD);
 }
 
 static int check_flags(tw_ctx* ctx) {
-    int hf[8];
-    CHECK(finish(ctx, hf, 8));
-    if (hf[4]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
-    if (hf[5]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    int hf[2];
+    CHECK(finish(ctx, hf, 2));
+    if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
+    if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
     return TW_OK;
 }
 
@@ -907,7 +921,7 @@ int tw_retime_frame(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection
     CHECK(ctx->ensure(ctx->wire[2], bytes, "wire out"));
     if (wire_a) CHECK(ctx->cuda(cudaMemcpyAsync(ctx->wire[0].p, wire_a, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload"));
     if (wire_b) CHECK(ctx->cuda(cudaMemcpyAsync(ctx->wire[1].p, wire_b, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload"));
-    CHECK(ctx->cuda(cudaMemsetAsync(ctx->flags.p, 0, 64, ctx->stream), "flags"));
+    CHECK(ctx->cuda(cudaMemsetAsync(ctx->flags.p, 0, FLAGS_BYTES, ctx->stream), "flags"));
     CHECK(retime_frame_dev(ctx, *s, *sel, wire_a ? ctx->wire[0].p : nullptr, wire_b ? ctx->wire[1].p : nullptr, width,
                            height, fmt, ctx->wire[2].p));
     CHECK(ctx->cuda(cudaMemcpyAsync(wire_out, ctx->wire[2].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
@@ -921,7 +935,7 @@ int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* 
     if (!s || !sels || !frames || !out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
         return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
     size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
-    CHECK(ctx->cuda(cudaMemsetAsync(ctx->flags.p, 0, 64, ctx->stream), "flags"));
+    CHECK(ctx->cuda(cudaMemsetAsync(ctx->flags.p, 0, FLAGS_BYTES, ctx->stream), "flags"));
     for (int k = 0; k < nout; k++) {
         const tw_selection& sel = sels[k];
         const uint8_t* base = (const uint8_t*)frames;
