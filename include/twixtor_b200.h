@@ -183,7 +183,7 @@ int tw_block_match(tw_ctx* ctx, const float* a, const float* b, float* flow, int
  * context). Its scratch is a fixed device array inside the library, 2 * TW_NOALLOC_MAX_PIXELS
  * floats (4 MiB), which every GPU that loads the library holds until the process exits; frames
  * above TW_NOALLOC_MAX_PIXELS pixels (e.g. anything above a 960 x 540 working size plus a
- * little), or a side above 8192, return TW_ERR_TOO_LARGE. The work runs on `stream` (a
+ * little), or a side above 6144, return TW_ERR_TOO_LARGE. The work runs on `stream` (a
  * cudaStream_t, NULL for the default stream) of the current device and the call returns when it
  * is done. The first call on a device looks up the array's device address and sets the kernels'
  * shared memory limit (no allocation either), so make that first call before any stream capture.

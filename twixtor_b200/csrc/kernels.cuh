@@ -72,6 +72,8 @@ __global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__
 __global__ void k_bm_cols(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
                           float* __restrict__ fv, int w, int h, bool reverse);
 size_t bm_smem_bytes(int len);
+// longest row or column block matching keeps in shared memory (9 arrays of 4-byte values per element)
+constexpr int BM_MAX_LINE = 6144;
 
 // ---- warps and blends (warp.rs, blend.rs) ------------------------------------------------------------
 struct WarpParams {

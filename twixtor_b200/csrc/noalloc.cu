@@ -34,10 +34,10 @@ int setup(int device, float** planes) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_planes) != cudaSuccess || !p) return TW_ERR_CUDA;
         if (cudaFuncSetAttribute(tw::k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tw::bm_smem_bytes(8192)) != cudaSuccess)
+                                 (int)tw::bm_smem_bytes(tw::BM_MAX_LINE)) != cudaSuccess)
             return TW_ERR_CUDA;
         if (cudaFuncSetAttribute(tw::k_bm_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tw::bm_smem_bytes(8192)) != cudaSuccess)
+                                 (int)tw::bm_smem_bytes(tw::BM_MAX_LINE)) != cudaSuccess)
             return TW_ERR_CUDA;
         g_planes_addr[device] = (float*)p;
     }
@@ -50,7 +50,8 @@ int setup(int device, float** planes) {
 extern "C" int tw_block_match_noalloc(const float* a, const float* b, float* flow, int32_t width, int32_t height,
                                       void* stream) {
     if (!a || !b || !flow || width <= 0 || height <= 0) return TW_ERR_BAD_PARAM;
-    if ((long)width * height > NOALLOC_MAX_PIXELS || width > 8192 || height > 8192) return TW_ERR_TOO_LARGE;
+    if ((long)width * height > NOALLOC_MAX_PIXELS || width > tw::BM_MAX_LINE || height > tw::BM_MAX_LINE)
+        return TW_ERR_TOO_LARGE;
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) return TW_ERR_CUDA;
     float* planes = nullptr;

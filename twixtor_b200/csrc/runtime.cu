@@ -57,6 +57,7 @@ int geometry(const tw_flow_settings& s, int w, int h, Geo* g, std::string* err) 
     if (!(s.sensitivity >= 0.0f) || !std::isfinite(s.sensitivity)) { *err = "sensitivity must be finite and not negative"; return TW_ERR_BAD_PARAM; }
     flow_resolution(s.quality, s.hiq != 0, w, h, &g->reduction, &g->w, &g->h);
     if (g->w < 2 || g->h < 2) { *err = "optical flow: working size below 2x2 is not supported"; return TW_ERR_UNSUPPORTED; }
+    if (g->w > BM_MAX_LINE || g->h > BM_MAX_LINE) { *err = "optical flow: a working size side above 6144 is not on the device"; return TW_ERR_UNSUPPORTED; }
     g->levels = std::min(level_count(g->w, g->h, 2), 32);
     int lw = g->w, lh = g->h;
     for (int i = 0; i < g->levels; i++) {
@@ -298,7 +299,7 @@ size_t pyramid_floats(const Geo& g) {
 
 // ---- block matching (flow.rs:551-622) -----------------------------------------------------------------
 void block_match(tw_ctx* ctx, const float* A, const float* B, float* fu, float* fv, int w, int h) {
-    if (w < 3 || h < 3) return;
+    if (w < 3 || h < 3) return;  // callers refuse lines above BM_MAX_LINE before any launch
     double b = 24.0 * w * h;  // per sweep: the field read and written (8 + 8), A and B read once (4 + 4)
     LAUNCHB(ctx, b, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, false);
     LAUNCHB(ctx, b, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, true);
@@ -507,11 +508,15 @@ int tw_open(int device, tw_ctx** out) {
     ctx->g7 = gaussian_taps(7.0f);
     ctx->g5 = gaussian_taps(5.0f);
     ctx->b5 = binomial5();
-    // block matching keeps one line of the field in shared memory (up to 8192 elements)
-    cudaFuncSetAttribute(k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(8192));
-    cudaFuncSetAttribute(k_bm_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(8192));
-    cudaFuncSetAttribute(k_level_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)level_init_smem());
-    cudaFuncSetAttribute(k_level_iter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)level_iter_smem());
+    // block matching keeps one line of the field in shared memory (up to BM_MAX_LINE elements)
+    e = cudaFuncSetAttribute(k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(BM_MAX_LINE));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_bm_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(BM_MAX_LINE));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_level_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)level_init_smem());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_level_iter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)level_iter_smem());
+    if (e != cudaSuccess) { tw_close(ctx); return TW_ERR_CUDA; }
     if (ctx->ensure(ctx->flags, FLAGS_BYTES, "flags") != TW_OK) { tw_close(ctx); return TW_ERR_CUDA; }
     k_selfcheck<<<1, 1, 0, ctx->stream>>>(ctx->flags.as<int>());
     ctx->launches++;
@@ -735,6 +740,7 @@ int tw_block_match(tw_ctx* ctx, const float* a, const float* b, float* flow, int
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
     if (!a || !b || !flow || width <= 0 || height <= 0) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    if (width > BM_MAX_LINE || height > BM_MAX_LINE) return ctx->fail(TW_ERR_UNSUPPORTED, "block matching: a side above 6144");
     size_t n = (size_t)width * height;
     CHECK(ctx->ensure(ctx->plane[0], n * 4, "plane A"));
     CHECK(ctx->ensure(ctx->plane[1], n * 4, "plane B"));

@@ -322,20 +322,27 @@ __device__ __forceinline__ void bm_patch(const float* __restrict__ A, int w, int
         for (int c = 0; c < 3; c++) p[r * 3 + c] = __ldg(pa + (long)r * w + c);
 }
 
-// shared memory of one line of length len (u, v, c0, end, start flag) plus one int per thread
-size_t bm_smem_bytes(int len) { return (size_t)len * (4 * 5) + 1024 * 4; }
+// Shared memory of one line of length len: u, v, c0 (floats), the three rows of A along the line
+// (floats), next / jump / on (ints), plus one int per warp for the block scan.
+size_t bm_smem_bytes(int len) { return (size_t)len * 4 * (3 + 3 + 3) + 64 * 4; }
 
-constexpr int BM_SCAN = 64;  // parallel scan length of a run; longer runs continue in the walk
+constexpr int BM_WINDOW = 4;  // accept tests a candidate run start evaluates at once (independent loads)
 
-// accept(i, n) of the sweep at line position i (Block::step, flow.rs:529-546), given c0 = the cost
-// of the current vector (NaN when the step cannot happen at i: no target or no cost)
+// accept(i, n) of the sweep at line position i (Block::step, flow.rs:529-546): the patch of A
+// around the pixel comes from shared memory (three rows of A along the line), c0 is the cost of
+// the current vector (NaN when the step cannot happen at i: no target or no cost).
 template <bool COLS>
-__device__ __forceinline__ bool bm_accept(const float* __restrict__ A, const float* __restrict__ B, int w, int h,
+__device__ __forceinline__ bool bm_accept(const float* s_a, int len, const float* __restrict__ B, int w, int h,
                                           int fixed, int i, float nu, float nv, float ci) {
     if (isnan(ci)) return false;  // None, or a NaN cost that nothing compares below
     int x = COLS ? fixed : i, y = COLS ? i : fixed;
     float p[9];
-    bm_patch(A, w, x, y, p);
+    // s_a holds A at offsets -1, 0, +1 across the line (rows y-1..y+1 for a row sweep, columns
+    // x-1..x+1 for a column sweep), each a line of len values
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) p[r * 3 + c] = COLS ? s_a[c * len + (i - 1 + r)] : s_a[r * len + (i - 1 + c)];
     float c1;
     if (!bm_cost(B, w, h, p, (float)x - nu, (float)y - nv, c1)) return false;
     return c1 < ci;
@@ -343,28 +350,36 @@ __device__ __forceinline__ bool bm_accept(const float* __restrict__ A, const flo
 
 // One sweep over a line. The line is the row y (COLS false: pixel (i, y)) or the column x
 // (COLS true: pixel (x, i)); len is its length. Forward sweeps run i = 1..len-2 with the
-// neighbour i - 1, reverse sweeps i = len-2..1 with the neighbour i + 1.
+// neighbour i - 1, reverse sweeps i = len-2..1 with the neighbour i + 1. In "sweep order"
+// position q (q = i forward, q = len-1-i reverse) both are the same forward recurrence.
 template <bool COLS>
 __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
                         float* __restrict__ fv, int w, int h, int fixed, bool reverse) {
     extern __shared__ float sm[];
-    int len = COLS ? h : w;
+    const int len = COLS ? h : w;
     float* su = sm;
     float* sv = su + len;
     float* c0 = sv + len;
-    int* endj = (int*)(c0 + len);
-    int* own = endj + len;
-    int* summ = own + len;  // one int per thread
+    float* s_a = c0 + len;        // 3 * len
+    int* jmp = (int*)(s_a + 3 * len);  // next^(2^r), ping-ponged with jmp2
+    int* jmp2 = jmp + len;
+    int* on = jmp2 + len;
+    int* wscan = on + len;        // one int per warp
     const float w1 = (float)(w - 1), h1 = (float)(h - 1);
     auto gidx = [&](int i) -> long { return COLS ? (long)i * w + fixed : (long)fixed * w + i; };
+    auto line_of = [&](int q) -> int { return reverse ? len - 1 - q : q; };  // sweep position -> line index
 
     for (int i = threadIdx.x; i < len; i += blockDim.x) {
-        su[i] = fu[gidx(i)];
-        sv[i] = fv[gidx(i)];
-        own[i] = 0;
+        long g = gidx(i);
+        su[i] = fu[g];
+        sv[i] = fv[g];
+        on[i] = 0;
+#pragma unroll
+        for (int o = 0; o < 3; o++)  // A at offset o-1 across the line
+            s_a[o * len + i] = COLS ? __ldg(A + (long)i * w + fixed - 1 + o) : __ldg(A + (long)(fixed - 1 + o) * w + i);
     }
     __syncthreads();
-    // 1. c0: the cost of the current vector, NaN where no step can happen
+    // 1. c0: the cost of the current vector at every interior position, NaN where no step can happen
     for (int i = threadIdx.x; i < len; i += blockDim.x) {
         float c = __int_as_float(0x7fc00000);
         if (i >= 1 && i <= len - 2) {
@@ -373,99 +388,83 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
             float ty = (float)y - sv[i];
             if (0.0f <= tx && tx <= w1 && 0.0f <= ty && ty <= h1) {
                 float p[9];
-                bm_patch(A, w, x, y, p);
-                float cc;
-                if (bm_cost(B, w, h, p, tx, ty, cc)) c = cc;
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+#pragma unroll
+                    for (int cc = 0; cc < 3; cc++) p[r * 3 + cc] = COLS ? s_a[cc * len + (i - 1 + r)] : s_a[r * len + (i - 1 + cc)];
+                float cost;
+                if (bm_cost(B, w, h, p, tx, ty, cost)) c = cost;
             }
         }
         c0[i] = c;
     }
     __syncthreads();
-    // 2. run ends, scanned for at most BM_SCAN positions: endj[j] >= 0 is the first position
-    //    past j where the run of v[j] stops (len-1 / 0 when it reaches the end of the sweep);
-    //    endj[j] = -(r + 1) when the scan stopped unfinished at position r.
-    for (int j = threadIdx.x; j < len; j += blockDim.x) {
+    // 2. next[q]: the sweep position where the run started at q ends (the first q' > q whose
+    //    accept of v[q] fails; len - 1 when the run reaches the end). BM_WINDOW tests at once;
+    //    longer runs continue one window at a time (bounded by the line).
+    for (int q = threadIdx.x; q < len; q += blockDim.x) {
+        int j = line_of(q);
         float nu = su[j], nv = sv[j];
-        int e;
-        if (!reverse) {
-            e = len - 1;
-            int lim = min(len - 2, j + BM_SCAN);
-            int i = j + 1;
-            for (; i <= lim; i++)
-                if (!bm_accept<COLS>(A, B, w, h, fixed, i, nu, nv, c0[i])) { e = i; break; }
-            if (i > lim && lim < len - 2) e = -(i + 1);
-        } else {
-            e = 0;
-            int lim = max(1, j - BM_SCAN);
-            int i = j - 1;
-            for (; i >= lim; i--)
-                if (!bm_accept<COLS>(A, B, w, h, fixed, i, nu, nv, c0[i])) { e = i; break; }
-            if (i < lim && lim > 1) e = -(i + 1);
+        int e = len - 1;
+        for (int q0 = q + 1; q0 <= len - 2; q0 += BM_WINDOW) {
+            bool acc[BM_WINDOW];
+#pragma unroll
+            for (int d = 0; d < BM_WINDOW; d++) {
+                int qq = q0 + d;
+                acc[d] = qq <= len - 2 && bm_accept<COLS>(s_a, len, B, w, h, fixed, line_of(qq), nu, nv, c0[line_of(qq)]);
+            }
+            int stop = -1;
+#pragma unroll
+            for (int d = BM_WINDOW - 1; d >= 0; d--)
+                if (!acc[d] && q0 + d <= len - 2) stop = q0 + d;
+            if (stop >= 0) { e = stop; break; }
         }
-        endj[j] = e;
+        jmp[q] = e;
     }
     __syncthreads();
-    // 3. walk the run starts from the sweep's first element; an unfinished run continues its scan here
-    if (threadIdx.x == 0) {
-        if (!reverse) {
-            int s = 0;
-            while (s < len - 1) {
-                own[s] = 1;
-                int e = endj[s];
-                if (e < 0) {
-                    int i = -e - 1;
-                    e = len - 1;
-                    for (; i <= len - 2; i++)
-                        if (!bm_accept<COLS>(A, B, w, h, fixed, i, su[s], sv[s], c0[i])) { e = i; break; }
-                }
-                s = e;
-            }
-        } else {
-            int s = len - 1;
-            while (s > 0) {
-                own[s] = 1;
-                int e = endj[s];
-                if (e < 0) {
-                    int i = -e - 1;
-                    e = 0;
-                    for (; i >= 1; i--)
-                        if (!bm_accept<COLS>(A, B, w, h, fixed, i, su[s], sv[s], c0[i])) { e = i; break; }
-                }
-                s = e;
-            }
-        }
-    }
+    // 3. the chain of run starts from sweep position 0, by pointer jumping: after round r every
+    //    start within 2^(r+1) hops of position 0 is marked (jmp holds next^(2^r))
+    if (threadIdx.x == 0) on[0] = 1;
     __syncthreads();
-    // 4. every interior element takes the vector of its run's start. Each thread owns a contiguous
-    //    chunk; the start owning the chunk's first element comes from the neighbouring chunks.
+    for (int span = 1; span < 2 * len; span *= 2) {
+        for (int q = threadIdx.x; q < len; q += blockDim.x)
+            if (on[q] && jmp[q] < len - 1) on[jmp[q]] = 1;
+        for (int q = threadIdx.x; q < len; q += blockDim.x) jmp2[q] = jmp[q] < len - 1 ? jmp[jmp[q]] : jmp[q];
+        __syncthreads();
+        int* t = jmp;
+        jmp = jmp2;
+        jmp2 = t;
+    }
+    // 4. owner of each position: the last marked start at or before it (a block-wide max scan over
+    //    contiguous chunks), then the scatter of v[owner]
     int nt = blockDim.x;
     int chunk = (len + nt - 1) / nt;
     int lo = threadIdx.x * chunk, hi = min(lo + chunk, len);
     int mark = -1;
-    if (!reverse) { for (int i = lo; i < hi; i++) if (own[i]) mark = i; }
-    else { for (int i = hi - 1; i >= lo; i--) if (own[i]) mark = i; }
-    summ[threadIdx.x] = mark;
+    for (int q = lo; q < hi; q++)
+        if (on[q]) mark = q;
+    // inclusive max scan of `mark` over the threads
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int v = mark;
+#pragma unroll
+    for (int o = 1; o < 32; o *= 2) {
+        int t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v = max(v, t);
+    }
+    if (lane == 31) wscan[warp] = v;
     __syncthreads();
-    if (lo < hi) {
-        int cur = -1;
-        if (!reverse) {
-            for (int t = (int)threadIdx.x - 1; t >= 0 && cur < 0; t--) cur = summ[t];
-            for (int i = lo; i < hi; i++) {
-                if (own[i]) cur = i;
-                if (i >= 1 && i <= len - 2 && cur >= 0 && cur != i) {
-                    fu[gidx(i)] = su[cur];
-                    fv[gidx(i)] = sv[cur];
-                }
-            }
-        } else {
-            for (int t = (int)threadIdx.x + 1; t < nt && cur < 0; t++) cur = summ[t];
-            for (int i = hi - 1; i >= lo; i--) {
-                if (own[i]) cur = i;
-                if (i >= 1 && i <= len - 2 && cur >= 0 && cur != i) {
-                    fu[gidx(i)] = su[cur];
-                    fv[gidx(i)] = sv[cur];
-                }
-            }
+    int before = -1;  // the max over all previous warps
+    for (int k = 0; k < warp; k++) before = max(before, wscan[k]);
+    int excl = __shfl_up_sync(0xffffffffu, v, 1);
+    if (lane == 0) excl = -1;
+    int cur = max(before, excl);  // the last start before this thread's chunk
+    for (int q = lo; q < hi; q++) {
+        if (on[q]) cur = q;
+        int i = line_of(q);
+        if (i >= 1 && i <= len - 2 && cur >= 0 && cur != q) {
+            int o = line_of(cur);
+            fu[gidx(i)] = su[o];
+            fv[gidx(i)] = sv[o];
         }
     }
 }
