@@ -204,6 +204,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--breakdown", action="store_true",
+                    help="after the timed region, time one more step with every kernel bracketed by events and "
+                         "print the per-kernel table to stderr (not part of the reported numbers)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -269,6 +272,11 @@ def main():
             times.append(e0.elapsed_time(e1))
     kms, klaunch, kbytes = dev.profile_end()
     launches = dev.stats()["kernel_launches"] - l0
+    if args.breakdown:
+        dev.profile_begin("*")
+        step_device(args.warmup)
+        print(dev.profile_report(), file=sys.stderr)
+        dev.profile_end()
     barrier()
     total_ms = max_over_ranks(sum(times))
     clocks = clk.summary()

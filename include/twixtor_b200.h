@@ -140,6 +140,10 @@ int tw_set_stream(tw_ctx* ctx, void* stream);
  * (device/exec/mod.rs:141-322). */
 int tw_profile_begin(tw_ctx* ctx, const char* kernel);
 int tw_profile_end(tw_ctx* ctx, double* total_ms, uint64_t* launches, double* bytes);
+/* With tw_profile_begin(ctx, "*") every kernel is timed: a text table per kernel (launches, device
+ * ms, us per launch, share, algorithmic GB/s) of the launches since begin, written into buf; returns
+ * its full length. Call it before tw_profile_end. */
+size_t tw_profile_report(tw_ctx* ctx, char* buf, size_t cap);
 
 /* ---- the Stages / Backend seam (stages.rs:33-71, device/exec/backend.rs:27-46) --------------- */
 
@@ -180,8 +184,8 @@ int tw_block_match(tw_ctx* ctx, const float* a, const float* b, float* flow, int
  * allocation can stall or is not allowed. This is tw_block_match with DEVICE pointers: a and b
  * (width * height floats each) and flow (width * height * 2 floats, interleaved, updated in place)
  * are the caller's device buffers, and the call allocates nothing (no cudaMalloc or cudaFree, no
- * context). Its scratch is a fixed device array inside the library, 2 * TW_NOALLOC_MAX_PIXELS
- * floats (4 MiB), which every GPU that loads the library holds until the process exits; frames
+ * context). Its scratch is a fixed device array inside the library, 6 * TW_NOALLOC_MAX_PIXELS
+ * floats (12 MiB), which every GPU that loads the library holds until the process exits; frames
  * above TW_NOALLOC_MAX_PIXELS pixels (e.g. anything above a 960 x 540 working size plus a
  * little), or a side above 6144, return TW_ERR_TOO_LARGE. The work runs on `stream` (a
  * cudaStream_t, NULL for the default stream) of the current device and the call returns when it

@@ -232,6 +232,8 @@ def library():
     L.tw_profile_begin.argtypes = [P, ctypes.c_char_p]
     L.tw_profile_end.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64),
                                  ctypes.POINTER(ctypes.c_double)]
+    L.tw_profile_report.argtypes = [P, ctypes.c_char_p, ctypes.c_size_t]
+    L.tw_profile_report.restype = ctypes.c_size_t
     L.tw_flow_geometry.argtypes = [ctypes.POINTER(_FlowSettings), i32, i32, P, P, P, P, i32]
     L.tw_solve.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), pflow]
     L.tw_solve_pair.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), pflow, pflow]
@@ -329,6 +331,13 @@ class Device:
 
     def profile_begin(self, kernel: str):
         self._check(self._L.tw_profile_begin(self._h, kernel.encode()))
+
+    def profile_report(self) -> str:
+        """Per-kernel table of the launches since ``profile_begin("*")``."""
+        n = self._L.tw_profile_report(self._h, None, 0)
+        buf = ctypes.create_string_buffer(n + 1)
+        self._L.tw_profile_report(self._h, buf, n + 1)
+        return buf.value.decode()
 
     def profile_end(self):
         """(device ms, launches, algorithmic bytes) of the profiled kernel since profile_begin."""

@@ -112,11 +112,13 @@ __device__ __forceinline__ float luma_of(const void* eng, int fmt, long i) {
 
 __global__ void __launch_bounds__(FT_THREADS) k_blur5_band(const float* __restrict__ orig, const void* __restrict__ luma_src,
                                                            int fmt, int w, int h, bool above_first,
-                                                           float* __restrict__ tmp_out, float* __restrict__ band_out) {
+                                                           float* __restrict__ tmp_out, float* __restrict__ band_out,
+                                                           float* __restrict__ band_t_out) {
     constexpr int N = 3, HALO = N - 1;
     constexpr int RW = FT_X + 2 * HALO, RH = FT_Y + 2 * HALO;
     __shared__ float s_in[RH * RW];
     __shared__ float s_h[RH * FT_X];
+    __shared__ float s_t[FT_Y][FT_X + 1];  // the band tile, for the transposed copy
     const float k[3] = {0.375f, 0.25f, 0.0625f};  // flow/conv.rs:48
     int X0 = blockIdx.x * FT_X, Y0 = blockIdx.y * FT_Y;
     int gx0 = X0 - HALO, gy0 = Y0 - HALO;
@@ -142,7 +144,19 @@ __global__ void __launch_bounds__(FT_THREADS) k_blur5_band(const float* __restri
                               : pass_elem<N, false, false>(line, gy0, FT_X, h, Y, k);
         long i = (long)Y * w + X;
         tmp_out[i] = v;
-        if (band_out) band_out[i] = s_in[(Y - gy0) * RW + (X - gx0)] - v;
+        if (band_out) {
+            float bv = s_in[(Y - gy0) * RW + (X - gx0)] - v;
+            band_out[i] = bv;
+            s_t[r][c] = bv;
+        }
+    }
+    if (band_t_out) {  // the band transposed (element (x, y) at [x * h + y]) for the column sweeps
+        __syncthreads();
+        for (int e = threadIdx.x; e < FT_X * FT_Y; e += blockDim.x) {
+            int c = e / FT_Y, r = e - c * FT_Y;
+            int X = X0 + c, Y = Y0 + r;
+            if (X < w && Y < h) band_t_out[(long)X * h + Y] = s_t[r][c];
+        }
     }
 }
 

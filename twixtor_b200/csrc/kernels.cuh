@@ -66,11 +66,15 @@ __global__ void k_fill(float* __restrict__ p, long n, float v);
 __global__ void k_deinterleave(const float* __restrict__ in, long n, float* __restrict__ fu, float* __restrict__ fv);
 __global__ void k_interleave(const float* __restrict__ fu, const float* __restrict__ fv, long n, float* __restrict__ out);
 
-// block matching (flow.rs:447-622): the four in-place sweeps; one CTA per row or column
+// block matching (flow.rs:447-622): the four in-place sweeps; one CTA per row or column. The column
+// sweeps take the transposes of A, B and the field (element (x, y) at [x * h + y]).
 __global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
                           float* __restrict__ fv, int w, int h, bool reverse);
-__global__ void k_bm_cols(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
-                          float* __restrict__ fv, int w, int h, bool reverse);
+__global__ void k_bm_cols(const float* __restrict__ AT, const float* __restrict__ BT, float* __restrict__ fuT,
+                          float* __restrict__ fvT, int w, int h, bool reverse);
+// two w x h planes into their h x w transposes; block (32, 8), grid (ceil(w/32), ceil(h/32))
+__global__ void k_transpose2(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ at,
+                             float* __restrict__ bt, int w, int h);
 size_t bm_smem_bytes(int len);
 // longest row or column block matching keeps in shared memory (9 arrays of 4-byte values per element)
 constexpr int BM_MAX_LINE = 6144;
@@ -105,7 +109,8 @@ __global__ void k_compose_blend(WarpParams pa, WarpParams pb, int fmt, float wbl
 // ---- fused, shared-memory tiled kernels (fused.cu) -----------------------------------------------------
 constexpr int FUSED_TILE_X = 32, FUSED_TILE_Y = 32, FUSED_THREADS = 256;
 __global__ void k_blur5_band(const float* __restrict__ orig, const void* __restrict__ luma_src, int fmt, int w, int h,
-                             bool above_first, float* __restrict__ tmp_out, float* __restrict__ band_out);
+                             bool above_first, float* __restrict__ tmp_out, float* __restrict__ band_out,
+                             float* __restrict__ band_t_out);
 __global__ void k_level_init(const float* __restrict__ img, int w, int h, Taps g7, bool above_first,
                              float* __restrict__ gxo, float* __restrict__ gyo, float* __restrict__ a0o,
                              float* __restrict__ a1o, float* __restrict__ a2o);

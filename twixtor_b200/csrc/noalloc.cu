@@ -4,9 +4,10 @@
 // device memory pool (a video host that hands out only its own frame buffers), or code on a
 // real-time render thread where a driver allocation can stall or is forbidden. They can still pass
 // their own device buffers for the inputs and the output. This entry point runs the four block
-// matching sweeps (flow.rs:551-622) on such buffers without allocating anything: its only scratch,
-// the field split into two float planes, lives in the file-scope device array below, which every
-// GPU that loads the library holds until the process exits.
+// matching sweeps (flow.rs:551-622) on such buffers without allocating anything: its only scratch
+// (the field split into two float planes, the transposes of the two images and of the field for
+// the column sweeps) lives in the file-scope device array below, which every GPU that loads the
+// library holds until the process exits.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -16,9 +17,10 @@
 
 namespace {
 
-// Scratch of the allocation-free block matching: the u and v planes of the field.
+// Scratch of the allocation-free block matching: the u and v planes of the field, the transposes
+// of A and B, and the transposed field of the column sweeps (6 planes).
 constexpr long NOALLOC_MAX_PIXELS = TW_NOALLOC_MAX_PIXELS;
-static __device__ __align__(256) float g_noalloc_planes[2 * NOALLOC_MAX_PIXELS];
+static __device__ __align__(256) float g_noalloc_planes[6 * NOALLOC_MAX_PIXELS];
 
 constexpr int MAX_DEVICES = 64;
 std::mutex g_setup_mu;
@@ -60,17 +62,22 @@ extern "C" int tw_block_match_noalloc(const float* a, const float* b, float* flo
     cudaStream_t s = (cudaStream_t)stream;
     long n = (long)width * height;
     float* fu = planes;
-    float* fv = planes + n;
+    float* fv = fu + n;
+    float *at = fv + n, *bt = at + n, *ut = bt + n, *vt = ut + n;
     const int tb = 256;
     unsigned g1 = (unsigned)((n + tb - 1) / tb);
-    // every element of the two planes this call reads is written first, so the previous call's
+    dim3 tt(32, 8), ga((width + 31) / 32, (height + 31) / 32), gb((height + 31) / 32, (width + 31) / 32);
+    // every element of the planes this call reads is written first, so the previous call's
     // contents never reach the result
     tw::k_deinterleave<<<g1, tb, 0, s>>>(flow, n, fu, fv);
     if (width >= 3 && height >= 3) {
         tw::k_bm_rows<<<height - 2, tb, tw::bm_smem_bytes(width), s>>>(a, b, fu, fv, width, height, false);
         tw::k_bm_rows<<<height - 2, tb, tw::bm_smem_bytes(width), s>>>(a, b, fu, fv, width, height, true);
-        tw::k_bm_cols<<<width - 2, tb, tw::bm_smem_bytes(height), s>>>(a, b, fu, fv, width, height, false);
-        tw::k_bm_cols<<<width - 2, tb, tw::bm_smem_bytes(height), s>>>(a, b, fu, fv, width, height, true);
+        tw::k_transpose2<<<ga, tt, 0, s>>>(a, b, at, bt, width, height);
+        tw::k_transpose2<<<ga, tt, 0, s>>>(fu, fv, ut, vt, width, height);
+        tw::k_bm_cols<<<width - 2, tb, tw::bm_smem_bytes(height), s>>>(at, bt, ut, vt, width, height, false);
+        tw::k_bm_cols<<<width - 2, tb, tw::bm_smem_bytes(height), s>>>(at, bt, ut, vt, width, height, true);
+        tw::k_transpose2<<<gb, tt, 0, s>>>(ut, vt, fu, fv, height, width);
     }
     tw::k_interleave<<<g1, tb, 0, s>>>(fu, fv, n, flow);
     if (cudaGetLastError() != cudaSuccess) return TW_ERR_CUDA;

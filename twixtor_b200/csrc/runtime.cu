@@ -153,8 +153,10 @@ struct DevBuf {
 // the context's stream, with the algorithmic bytes each launch moves.
 struct KernelProfile {
     bool on = false;
-    std::string name;
+    std::string name;             // one kernel, or "*" for every kernel
     std::vector<cudaEvent_t> ev;  // start, stop pairs
+    std::vector<std::string> who; // the kernel of each pair
+    std::vector<double> nbytes;   // the algorithmic bytes of each pair
     double bytes = 0.0;
     uint64_t launches = 0;
 };
@@ -194,7 +196,9 @@ namespace {
 
 // Every kernel launch of the library goes through LAUNCHB (LAUNCH passes no byte count): it counts
 // the launch and, when the kernel is the one being profiled, brackets it with events.
-bool prof_match(tw_ctx* ctx, const char* kernel) { return ctx->prof.on && ctx->prof.name == kernel; }
+bool prof_match(tw_ctx* ctx, const char* kernel) {
+    return ctx->prof.on && (ctx->prof.name == kernel || ctx->prof.name == "*");
+}
 void prof_mark(tw_ctx* ctx) {
     cudaEvent_t e;
     cudaEventCreate(&e);
@@ -212,6 +216,8 @@ void prof_mark(tw_ctx* ctx) {
             prof_mark(ctx);                                                        \
             (ctx)->prof.bytes += (double)(nbytes_);                                \
             (ctx)->prof.launches++;                                                \
+            (ctx)->prof.who.push_back(#kernel);                                    \
+            (ctx)->prof.nbytes.push_back((double)(nbytes_));                       \
         }                                                                          \
     } while (0)
 #define LAUNCH(ctx, kernel, grid, block, smem, ...) LAUNCHB(ctx, 0, kernel, grid, block, smem, __VA_ARGS__)
@@ -248,8 +254,10 @@ void conv_planes(tw_ctx* ctx, float* const* planes, int c, int w, int h, const T
 // (k_blur5_band), each followed by the corner aligned resample to the next size.
 dim3 tiles(int w, int h) { return dim3((unsigned)((w + FUSED_TILE_X - 1) / FUSED_TILE_X), (unsigned)((h + FUSED_TILE_Y - 1) / FUSED_TILE_Y)); }
 
+size_t pyramid_floats(const Geo& g);
+
 int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, const tw_flow_settings& s, const Geo& g,
-                      float* out) {
+                      float* out, float* out_t = nullptr) {
     if (s.prep_contrast_edge || s.prep_delinearize)
         return ctx->fail(TW_ERR_UNSUPPORTED, "image prep (Contrast/Edge Enhance, Delinearize) is not on the device");
     if (s.video_range_luma && s.track_alpha)
@@ -270,7 +278,7 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
     for (int r = 0; r < g.reduction; r++) {  // prep.rs:252-259; the first step reads the luma on the fly
         LAUNCHB(ctx, (r == 0 ? 4.0 * sample_bytes(fmt) : 4.0) * cw * ch + 4.0 * cw * ch, k_blur5_band, tiles(cw, ch),
                 FUSED_THREADS, 0, r == 0 ? (const float*)nullptr : cur, r == 0 ? eng_dev : nullptr, fmt, cw, ch, af, tmp,
-                (float*)nullptr);
+                (float*)nullptr, (float*)nullptr);
         int nw = cw / 2, nh = ch / 2;
         LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, tmp, cw, ch, nxt, nw, nh);
         std::swap(cur, nxt);
@@ -278,16 +286,18 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
         ch = nh;
     }
     size_t off = 0;
+    size_t pf = pyramid_floats(g);
     for (int i = 0; i < g.levels; i++) {
         int lw = g.sizes[i][0], lh = g.sizes[i][1];
-        LAUNCHB(ctx, 12.0 * lw * lh, k_blur5_band, tiles(lw, lh), FUSED_THREADS, 0, cur, (const void*)nullptr, fmt, lw, lh,
-                af, tmp, out + off);
+        LAUNCHB(ctx, 16.0 * lw * lh, k_blur5_band, tiles(lw, lh), FUSED_THREADS, 0, cur, (const void*)nullptr, fmt, lw, lh,
+                af, tmp, out + off, out_t ? out_t + off : (float*)nullptr);
         if (i + 1 < g.levels) {
             int nw = g.sizes[i + 1][0], nh = g.sizes[i + 1][1];
             LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, tmp, lw, lh, cur, nw, nh);
         }
         off += (size_t)lw * lh;
     }
+    (void)pf;
     return TW_OK;
 }
 
@@ -298,13 +308,20 @@ size_t pyramid_floats(const Geo& g) {
 }
 
 // ---- block matching (flow.rs:551-622) -----------------------------------------------------------------
-void block_match(tw_ctx* ctx, const float* A, const float* B, float* fu, float* fv, int w, int h) {
+// Rows on the row-major planes; then the field is transposed, the column sweeps run on the
+// transposed planes (AT, BT: the level's bands stored column by column), and the field goes back.
+// uT, vT: scratch for the transposed field (w * h floats each).
+void block_match(tw_ctx* ctx, const float* A, const float* B, const float* AT, const float* BT, float* fu, float* fv,
+                 float* uT, float* vT, int w, int h) {
     if (w < 3 || h < 3) return;  // callers refuse lines above BM_MAX_LINE before any launch
     double b = 24.0 * w * h;  // per sweep: the field read and written (8 + 8), A and B read once (4 + 4)
     LAUNCHB(ctx, b, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, false);
     LAUNCHB(ctx, b, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, true);
-    LAUNCHB(ctx, b, k_bm_cols, w - 2, TB, bm_smem_bytes(h), A, B, fu, fv, w, h, false);
-    LAUNCHB(ctx, b, k_bm_cols, w - 2, TB, bm_smem_bytes(h), A, B, fu, fv, w, h, true);
+    dim3 tb(32, 8);
+    LAUNCHB(ctx, 16.0 * w * h, k_transpose2, dim3((w + 31) / 32, (h + 31) / 32), tb, 0, fu, fv, uT, vT, w, h);
+    LAUNCHB(ctx, b, k_bm_cols, w - 2, TB, bm_smem_bytes(h), AT, BT, uT, vT, w, h, false);
+    LAUNCHB(ctx, b, k_bm_cols, w - 2, TB, bm_smem_bytes(h), AT, BT, uT, vT, w, h, true);
+    LAUNCHB(ctx, 16.0 * w * h, k_transpose2, dim3((h + 31) / 32, (w + 31) / 32), tb, 0, uT, vT, fu, fv, h, w);
 }
 
 // ---- one solve over two resident pyramids (flow.rs:1258-1307) ------------------------------------------
@@ -313,15 +330,16 @@ void block_match(tw_ctx* ctx, const float* A, const float* B, float* fu, float* 
 // result holds a NaN. Per level: one tiled kernel for the gradient and the blurred tensor, one per
 // iteration (calc_b, blur7, new_disp, blur5 in shared memory, the flow ping-ponged), the block
 // matching sweeps, the range check, and the reset / damping fused into the upsample.
-int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const Geo& g, const tw_flow_settings& s,
-                       DevBuf& work, float* out, int* any, int* nan_flag) {
+int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float* xt, const float* yt, const Geo& g,
+                       const tw_flow_settings& s, DevBuf& work, float* out, int* any, int* nan_flag) {
     size_t np0 = (size_t)g.w * g.h;
-    // planes: gx gy a0 a1 a2 u0 v0 u1 v1
-    const int NP = 9;
+    // planes: gx gy a0 a1 a2 u0 v0 u1 v1 uT vT
+    const int NP = 11;
     CHECK(ctx->ensure(work, np0 * NP * sizeof(float), "solve scratch"));
     float* base = work.as<float>();
     float *gx = base, *gy = base + np0, *a0 = base + 2 * np0, *a1 = base + 3 * np0, *a2 = base + 4 * np0;
     float *fu = base + 5 * np0, *fv = base + 6 * np0, *nu = base + 7 * np0, *nv = base + 8 * np0;
+    float *ut = base + 9 * np0, *vt = base + 10 * np0;
     int start;
     float damp;
     start_level(s.sensitivity, g.levels, &start, &damp);
@@ -338,6 +356,8 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const Geo& g
         int w = g.sizes[l][0], h = g.sizes[l][1];
         const float* A = x + offs[l];
         const float* B = y + offs[l];
+        const float* AT = xt + offs[l];
+        const float* BT = yt + offs[l];
         double px = (double)w * h;
         LAUNCHB(ctx, 24.0 * px, k_level_init, tiles(w, h), FUSED_THREADS, level_init_smem(), A, w, h, ctx->g7, af, gx, gy,
                 a0, a1, a2);
@@ -347,9 +367,9 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const Geo& g
                     a2, fu, fv, w, h, ctx->g7, ctx->g5, af, nu, nv);
             std::swap(fu, nu);
             std::swap(fv, nv);
-            if (it == 1 && l == 0 && !s.skip_refine) block_match(ctx, A, B, fu, fv, w, h);
+            if (it == 1 && l == 0 && !s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h);
         }
-        if (l != 0 && !s.skip_refine) block_match(ctx, A, B, fu, fv, w, h);
+        if (l != 0 && !s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h);
         LAUNCH(ctx, k_range_any, grid2(w, h), TB, 0, fu, fv, w, h, any + l);
         bool damp_now = l == start && damp_any;
         if (l > 0) {
@@ -587,6 +607,43 @@ int tw_profile_end(tw_ctx* ctx, double* total_ms, uint64_t* launches, double* by
     return TW_OK;
 }
 
+size_t tw_profile_report(tw_ctx* ctx, char* buf, size_t cap) {
+    if (!ctx) return 0;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return 0;
+    struct Row { double ms = 0.0, bytes = 0.0; uint64_t n = 0; };
+    std::vector<std::pair<std::string, Row>> rows;
+    double total = 0.0;
+    for (size_t i = 0; i + 1 < ctx->prof.ev.size(); i += 2) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, ctx->prof.ev[i], ctx->prof.ev[i + 1]);
+        const std::string& k = ctx->prof.who[i / 2];
+        auto it = std::find_if(rows.begin(), rows.end(), [&](const std::pair<std::string, Row>& r) { return r.first == k; });
+        if (it == rows.end()) { rows.push_back({k, Row()}); it = rows.end() - 1; }
+        it->second.ms += t;
+        it->second.bytes += ctx->prof.nbytes[i / 2];
+        it->second.n++;
+        total += t;
+    }
+    std::sort(rows.begin(), rows.end(), [](const auto& a, const auto& b) { return a.second.ms > b.second.ms; });
+    std::string out;
+    char line[256];
+    snprintf(line, sizeof line, "%-20s %8s %10s %8s %7s %10s\n", "kernel", "launches", "ms", "us/launch", "share", "alg GB/s");
+    out += line;
+    for (auto& r : rows) {
+        snprintf(line, sizeof line, "%-20s %8llu %10.3f %8.2f %6.1f%% %10.1f\n", r.first.c_str(),
+                 (unsigned long long)r.second.n, r.second.ms, 1e3 * r.second.ms / std::max<uint64_t>(r.second.n, 1),
+                 100.0 * r.second.ms / std::max(total, 1e-9), r.second.ms > 0 ? r.second.bytes / (r.second.ms * 1e6) : 0.0);
+        out += line;
+    }
+    if (buf && cap) {
+        size_t m = std::min(out.size(), cap - 1);
+        std::memcpy(buf, out.data(), m);
+        buf[m] = 0;
+    }
+    return out.size();
+}
+
 int tw_set_stream(tw_ctx* ctx, void* stream) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -642,10 +699,12 @@ static int solve_common(tw_ctx* ctx, const tw_image* a, const tw_image* b, const
     CHECK(upload_image(ctx, ctx->eng[0], a));
     CHECK(upload_image(ctx, ctx->eng[1], b));
     size_t pf = pyramid_floats(g);
-    CHECK(ctx->ensure(ctx->pyr[0], pf * 4, "pyramid"));
-    CHECK(ctx->ensure(ctx->pyr[1], pf * 4, "pyramid"));
-    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, a->width, a->height, a->fmt, *s, g, ctx->pyr[0].as<float>()));
-    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, b->width, b->height, b->fmt, *s, g, ctx->pyr[1].as<float>()));
+    CHECK(ctx->ensure(ctx->pyr[0], 2 * pf * 4, "pyramid"));
+    CHECK(ctx->ensure(ctx->pyr[1], 2 * pf * 4, "pyramid"));
+    float* px_ = ctx->pyr[0].as<float>();
+    float* py_ = ctx->pyr[1].as<float>();
+    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, a->width, a->height, a->fmt, *s, g, px_, px_ + pf));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, b->width, b->height, b->fmt, *s, g, py_, py_ + pf));
     size_t fb = (size_t)g.w * g.h * 2 * sizeof(float);
     CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
     CHECK(ctx->ensure(ctx->flow[1], fb, "flow"));
@@ -653,11 +712,11 @@ static int solve_common(tw_ctx* ctx, const tw_image* a, const tw_image* b, const
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
     // f_ab = solve(X = A, Y = B); f_ba = solve(X = B, Y = A)
     if (f_ab)
-        CHECK(solve_pyramids_dev(ctx, ctx->pyr[0].as<float>(), ctx->pyr[1].as<float>(), g, *s, ctx->work[0],
-                                 ctx->flow[0].as<float>(), flags + FL_ANY0, flags + FL_NAN));
+        CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, *s, ctx->work[0], ctx->flow[0].as<float>(),
+                                 flags + FL_ANY0, flags + FL_NAN));
     if (pair && f_ba)
-        CHECK(solve_pyramids_dev(ctx, ctx->pyr[1].as<float>(), ctx->pyr[0].as<float>(), g, *s, ctx->work[1],
-                                 ctx->flow[1].as<float>(), flags + FL_ANY1, flags + FL_NAN));
+        CHECK(solve_pyramids_dev(ctx, py_, px_, py_ + pf, px_ + pf, g, *s, ctx->work[1], ctx->flow[1].as<float>(),
+                                 flags + FL_ANY1, flags + FL_NAN));
     if (f_ab) CHECK(ctx->cuda(cudaMemcpyAsync(f_ab->data, ctx->flow[0].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
     if (pair && f_ba) CHECK(ctx->cuda(cudaMemcpyAsync(f_ba->data, ctx->flow[1].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
     int hf[2];
@@ -690,8 +749,9 @@ int tw_build_pyramid(tw_ctx* ctx, const tw_image* img, const tw_flow_settings* s
     CHECK(geometry(*s, img->width, img->height, &g, &ctx->err));
     CHECK(upload_image(ctx, ctx->eng[0], img));
     size_t pf = pyramid_floats(g);
-    CHECK(ctx->ensure(ctx->pyr[0], pf * 4, "pyramid"));
-    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, img->width, img->height, img->fmt, *s, g, ctx->pyr[0].as<float>()));
+    CHECK(ctx->ensure(ctx->pyr[0], 2 * pf * 4, "pyramid"));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, img->width, img->height, img->fmt, *s, g, ctx->pyr[0].as<float>(),
+                            ctx->pyr[0].as<float>() + pf));
     CHECK(ctx->cuda(cudaMemcpyAsync(levels_out, ctx->pyr[0].p, pf * 4, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     int hf[1];
     return finish(ctx, hf, 1);
@@ -745,14 +805,17 @@ int tw_block_match(tw_ctx* ctx, const float* a, const float* b, float* flow, int
     CHECK(ctx->ensure(ctx->plane[0], n * 4, "plane A"));
     CHECK(ctx->ensure(ctx->plane[1], n * 4, "plane B"));
     CHECK(ctx->ensure(ctx->plane[2], n * 8, "flow"));
-    CHECK(ctx->ensure(ctx->work[0], n * 8, "flow planes"));
+    CHECK(ctx->ensure(ctx->work[0], n * 4 * 6, "flow planes"));
     CHECK(ctx->cuda(cudaMemcpyAsync(ctx->plane[0].p, a, n * 4, cudaMemcpyHostToDevice, ctx->stream), "upload"));
     CHECK(ctx->cuda(cudaMemcpyAsync(ctx->plane[1].p, b, n * 4, cudaMemcpyHostToDevice, ctx->stream), "upload"));
     CHECK(ctx->cuda(cudaMemcpyAsync(ctx->plane[2].p, flow, n * 8, cudaMemcpyHostToDevice, ctx->stream), "upload"));
     float* fu = ctx->work[0].as<float>();
     float* fv = fu + n;
+    float *at = fv + n, *bt = at + n, *ut = bt + n, *vt = ut + n;
     LAUNCH(ctx, k_deinterleave, grid1((long)n), TB, 0, ctx->plane[2].as<float>(), (long)n, fu, fv);
-    block_match(ctx, ctx->plane[0].as<float>(), ctx->plane[1].as<float>(), fu, fv, width, height);
+    LAUNCH(ctx, k_transpose2, dim3((width + 31) / 32, (height + 31) / 32), dim3(32, 8), 0, ctx->plane[0].as<float>(),
+           ctx->plane[1].as<float>(), at, bt, width, height);
+    block_match(ctx, ctx->plane[0].as<float>(), ctx->plane[1].as<float>(), at, bt, fu, fv, ut, vt, width, height);
     LAUNCH(ctx, k_interleave, grid1((long)n), TB, 0, fu, fv, (long)n, ctx->plane[2].as<float>());
     CHECK(ctx->cuda(cudaMemcpyAsync(flow, ctx->plane[2].p, n * 8, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     int hf[1];
@@ -881,10 +944,12 @@ static int retime_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_s
     Geo g;
     CHECK(geometry(fs, W, H, &g, &ctx->err));
     size_t pf = pyramid_floats(g);
-    CHECK(ctx->ensure(ctx->pyr[0], pf * 4, "pyramid"));
-    CHECK(ctx->ensure(ctx->pyr[1], pf * 4, "pyramid"));
-    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, W, H, fmt, fs, g, ctx->pyr[0].as<float>()));
-    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, W, H, fmt, fs, g, ctx->pyr[1].as<float>()));
+    CHECK(ctx->ensure(ctx->pyr[0], 2 * pf * 4, "pyramid"));
+    CHECK(ctx->ensure(ctx->pyr[1], 2 * pf * 4, "pyramid"));
+    float* px_ = ctx->pyr[0].as<float>();
+    float* py_ = ctx->pyr[1].as<float>();
+    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, W, H, fmt, fs, g, px_, px_ + pf));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, W, H, fmt, fs, g, py_, py_ + pf));
     size_t fb = (size_t)g.w * g.h * 2 * sizeof(float);
     CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
     CHECK(ctx->ensure(ctx->flow[1], fb, "flow"));
@@ -897,11 +962,11 @@ static int retime_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_s
         return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
     }
     if (need_ab)
-        CHECK(solve_pyramids_dev(ctx, ctx->pyr[0].as<float>(), ctx->pyr[1].as<float>(), g, fs, ctx->work[0],
-                                 ctx->flow[0].as<float>(), flags + FL_ANY0, flags + FL_NAN));
+        CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, fs, ctx->work[0], ctx->flow[0].as<float>(),
+                                 flags + FL_ANY0, flags + FL_NAN));
     if (need_ba)
-        CHECK(solve_pyramids_dev(ctx, ctx->pyr[1].as<float>(), ctx->pyr[0].as<float>(), g, fs, ctx->work[1],
-                                 ctx->flow[1].as<float>(), flags + FL_ANY1, flags + FL_NAN));
+        CHECK(solve_pyramids_dev(ctx, py_, px_, py_ + pf, px_ + pf, g, fs, ctx->work[1], ctx->flow[1].as<float>(),
+                                 flags + FL_ANY1, flags + FL_NAN));
     return compose_dev(ctx, s.compose, sel, ctx->eng[0].p, ctx->eng[1].p, need_ab ? ctx->flow[0].as<float>() : nullptr,
                        need_ba ? ctx->flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, out_wire, true, flip,
                        flags + FL_BAD);

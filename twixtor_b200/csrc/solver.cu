@@ -275,9 +275,10 @@ __global__ void k_fill(float* __restrict__ p, long n, float v) {
 //   4. v'[x] = v[start of x's run].
 // Each cost evaluation is Block::cost bit for bit, so the result equals the sequential sweep.
 
-// flow.rs:474-523 (Block::cost)
-__device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int h, const float p[9], float x2,
-                                        float y2, float& out) {
+// flow.rs:474-523 (Block::cost). B(X, Y) is read at B[X * xs + Y * ys]: (1, w) for a row-major
+// plane, (h, 1) for its transpose; the arithmetic does not depend on the layout.
+__device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int h, long xs, long ys, const float p[9],
+                                        float x2, float y2, float& out) {
     float wm2 = (float)(w - 2), hm2 = (float)(h - 2);
     if (x2 > wm2 || y2 > hm2) return false;
     int ix, iy;
@@ -291,12 +292,12 @@ __device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int 
     float w10 = fx - w11;
     float w01 = fy - w11;
     float w00 = ((1.0f - fx) - fy) + w11;
-    const float* base = B + (long)(iy - 1) * w + ix - 1;
+    const float* base = B + (long)(iy - 1) * ys + (long)(ix - 1) * xs;
     float t[4][4];
 #pragma unroll
     for (int r = 0; r < 4; r++)
 #pragma unroll
-        for (int c = 0; c < 4; c++) t[r][c] = __ldg(base + (long)r * w + c);
+        for (int c = 0; c < 4; c++) t[r][c] = __ldg(base + (long)r * ys + (long)c * xs);
     float sq[9];
 #pragma unroll
     for (int b = 0; b < 3; b++) {
@@ -312,14 +313,6 @@ __device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int 
     for (int k = 2; k < 8; k++) s = s + sq[k];
     out = sq[8] + s;
     return true;
-}
-
-__device__ __forceinline__ void bm_patch(const float* __restrict__ A, int w, int x, int y, float p[9]) {
-    const float* pa = A + (long)(y - 1) * w + x - 1;
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) p[r * 3 + c] = __ldg(pa + (long)r * w + c);
 }
 
 // Shared memory of one line of length len: u, v, c0 (floats), the three rows of A along the line
@@ -344,7 +337,7 @@ __device__ __forceinline__ bool bm_accept(const float* s_a, int len, const float
 #pragma unroll
         for (int c = 0; c < 3; c++) p[r * 3 + c] = COLS ? s_a[c * len + (i - 1 + r)] : s_a[r * len + (i - 1 + c)];
     float c1;
-    if (!bm_cost(B, w, h, p, (float)x - nu, (float)y - nv, c1)) return false;
+    if (!bm_cost(B, w, h, COLS ? (long)h : 1L, COLS ? 1L : (long)w, p, (float)x - nu, (float)y - nv, c1)) return false;
     return c1 < ci;
 }
 
@@ -352,6 +345,9 @@ __device__ __forceinline__ bool bm_accept(const float* s_a, int len, const float
 // (COLS true: pixel (x, i)); len is its length. Forward sweeps run i = 1..len-2 with the
 // neighbour i - 1, reverse sweeps i = len-2..1 with the neighbour i + 1. In "sweep order"
 // position q (q = i forward, q = len-1-i reverse) both are the same forward recurrence.
+// Column sweeps take TRANSPOSED planes (A, B and the field stored column by column, element
+// (x, y) at [x * h + y]) so that a warp's lanes, which walk down one column, read contiguous memory;
+// the reference transposes its field for the same sweeps (flow.rs:583-621).
 template <bool COLS>
 __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
                         float* __restrict__ fv, int w, int h, int fixed, bool reverse) {
@@ -366,7 +362,8 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
     int* on = jmp2 + len;
     int* wscan = on + len;        // one int per warp
     const float w1 = (float)(w - 1), h1 = (float)(h - 1);
-    auto gidx = [&](int i) -> long { return COLS ? (long)i * w + fixed : (long)fixed * w + i; };
+    // both layouts keep the line contiguous: row y of a row-major plane, column x of a transposed one
+    auto gidx = [&](int i) -> long { return (long)fixed * len + i; };
     auto line_of = [&](int q) -> int { return reverse ? len - 1 - q : q; };  // sweep position -> line index
 
     for (int i = threadIdx.x; i < len; i += blockDim.x) {
@@ -375,8 +372,8 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
         sv[i] = fv[g];
         on[i] = 0;
 #pragma unroll
-        for (int o = 0; o < 3; o++)  // A at offset o-1 across the line
-            s_a[o * len + i] = COLS ? __ldg(A + (long)i * w + fixed - 1 + o) : __ldg(A + (long)(fixed - 1 + o) * w + i);
+        for (int o = 0; o < 3; o++)  // A at offset o-1 across the line: rows y-1..y+1, or columns x-1..x+1
+            s_a[o * len + i] = __ldg(A + (long)(fixed - 1 + o) * len + i);
     }
     __syncthreads();
     // 1. c0: the cost of the current vector at every interior position, NaN where no step can happen
@@ -393,7 +390,7 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
 #pragma unroll
                     for (int cc = 0; cc < 3; cc++) p[r * 3 + cc] = COLS ? s_a[cc * len + (i - 1 + r)] : s_a[r * len + (i - 1 + cc)];
                 float cost;
-                if (bm_cost(B, w, h, p, tx, ty, cost)) c = cost;
+                if (bm_cost(B, w, h, COLS ? (long)h : 1L, COLS ? 1L : (long)w, p, tx, ty, cost)) c = cost;
             }
         }
         c0[i] = c;
@@ -465,6 +462,28 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
             int o = line_of(cur);
             fu[gidx(i)] = su[o];
             fv[gidx(i)] = sv[o];
+        }
+    }
+}
+
+// Two planes of w x h (row major) into their transposes (h x w), through a padded shared tile.
+__global__ void k_transpose2(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ at,
+                             float* __restrict__ bt, int w, int h) {
+    __shared__ float ta[32][33], tb[32][33];
+    int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int x = x0 + threadIdx.x, y = y0 + r;
+        if (x < w && y < h) {
+            ta[r][threadIdx.x] = a[(long)y * w + x];
+            tb[r][threadIdx.x] = b[(long)y * w + x];
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int y = y0 + threadIdx.x, x = x0 + r;
+        if (x < w && y < h) {
+            at[(long)x * h + y] = ta[threadIdx.x][r];
+            bt[(long)x * h + y] = tb[threadIdx.x][r];
         }
     }
 }
