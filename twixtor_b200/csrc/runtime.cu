@@ -161,9 +161,25 @@ struct KernelProfile {
     uint64_t launches = 0;
 };
 
+// One set of buffers for one output frame in flight, with two streams: the two pyramids and the
+// two solves of a pair run concurrently (stream 0: A's pyramid, solve(A, B), the composition;
+// stream 1: B's pyramid, solve(B, A)). Several lanes keep several output frames in flight.
+struct Lane {
+    cudaStream_t s[2] = {nullptr, nullptr};
+    cudaEvent_t ev_pyr[2] = {nullptr, nullptr};  // pyramid of A / B done
+    cudaEvent_t ev_solve1 = nullptr;             // solve on stream 1 done
+    cudaEvent_t ev_done = nullptr;               // the frame's composition done (stream 0)
+    bool used = false;
+    DevBuf eng[2], pyr[2], work[2], flow[2], scratch[2][3], flags;
+};
+constexpr int MAX_LANES = 4;
+
 struct tw_ctx {
     int device = 0;
     KernelProfile prof;
+    cudaStream_t cur = nullptr;  // the stream every launch goes to
+    Lane lanes[MAX_LANES];
+    cudaEvent_t ev_start = nullptr;
     cudaStream_t stream = nullptr;
     cudaStream_t own = nullptr;  // the stream the context created
     bool own_stream = true;
@@ -202,7 +218,7 @@ bool prof_match(tw_ctx* ctx, const char* kernel) {
 void prof_mark(tw_ctx* ctx) {
     cudaEvent_t e;
     cudaEventCreate(&e);
-    cudaEventRecord(e, ctx->stream);
+    cudaEventRecord(e, ctx->cur);
     ctx->prof.ev.push_back(e);
 }
 
@@ -210,7 +226,7 @@ void prof_mark(tw_ctx* ctx) {
     do {                                                                           \
         bool _p = prof_match((ctx), #kernel);                                      \
         if (_p) prof_mark(ctx);                                                    \
-        kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);           \
+        kernel<<<(grid), (block), (smem), (ctx)->cur>>>(__VA_ARGS__);              \
         (ctx)->launches++;                                                         \
         if (_p) {                                                                  \
             prof_mark(ctx);                                                        \
@@ -257,7 +273,7 @@ dim3 tiles(int w, int h) { return dim3((unsigned)((w + FUSED_TILE_X - 1) / FUSED
 size_t pyramid_floats(const Geo& g);
 
 int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, const tw_flow_settings& s, const Geo& g,
-                      float* out, float* out_t = nullptr) {
+                      float* out, float* out_t, DevBuf* scratch) {
     if (s.prep_contrast_edge || s.prep_delinearize)
         return ctx->fail(TW_ERR_UNSUPPORTED, "image prep (Contrast/Edge Enhance, Delinearize) is not on the device");
     if (s.video_range_luma && s.track_alpha)
@@ -265,10 +281,10 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
     if (s.video_range_luma || s.track_alpha)
         return ctx->fail(TW_ERR_UNSUPPORTED, "video range luma and Track RGB+A are not on the device");
     size_t full = (size_t)W * H * sizeof(float);
-    for (int i = 0; i < 3; i++) CHECK(ctx->ensure(ctx->plane[i], full, "pyramid scratch"));
-    float* cur = ctx->plane[0].as<float>();
-    float* tmp = ctx->plane[1].as<float>();
-    float* nxt = ctx->plane[2].as<float>();
+    for (int i = 0; i < 3; i++) CHECK(ctx->ensure(scratch[i], full, "pyramid scratch"));
+    float* cur = scratch[0].as<float>();
+    float* tmp = scratch[1].as<float>();
+    float* nxt = scratch[2].as<float>();
     bool af = s.taps_above_first != 0;
     int cw = W, ch = H;
     if (g.reduction == 0) {
@@ -347,9 +363,9 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
     size_t off = 0;
     for (int i = 0; i < g.levels; i++) { offs[i] = off; off += (size_t)g.sizes[i][0] * g.sizes[i][1]; }
     long ns = (long)g.sizes[start][0] * g.sizes[start][1];
-    CHECK(ctx->cuda(cudaMemsetAsync(fu, 0, ns * sizeof(float), ctx->stream), "flow init"));
-    CHECK(ctx->cuda(cudaMemsetAsync(fv, 0, ns * sizeof(float), ctx->stream), "flow init"));
-    CHECK(ctx->cuda(cudaMemsetAsync(any, 0, 32 * sizeof(int), ctx->stream), "range flags"));
+    CHECK(ctx->cuda(cudaMemsetAsync(fu, 0, ns * sizeof(float), ctx->cur), "flow init"));
+    CHECK(ctx->cuda(cudaMemsetAsync(fv, 0, ns * sizeof(float), ctx->cur), "flow init"));
+    CHECK(ctx->cuda(cudaMemsetAsync(any, 0, 32 * sizeof(int), ctx->cur), "range flags"));
     bool af = s.taps_above_first != 0;
     bool damp_any = std::fabs((double)damp - 1.0) >= 1e-6;
     for (int l = start; l >= 0; l--) {
@@ -525,6 +541,8 @@ int tw_open(int device, tw_ctx** out) {
     e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete ctx; return TW_ERR_CUDA; }
     ctx->stream = ctx->own;
+    ctx->cur = ctx->stream;
+    if (cudaEventCreateWithFlags(&ctx->ev_start, cudaEventDisableTiming) != cudaSuccess) { tw_close(ctx); return TW_ERR_CUDA; }
     ctx->g7 = gaussian_taps(7.0f);
     ctx->g5 = gaussian_taps(5.0f);
     ctx->b5 = binomial5();
@@ -556,6 +574,19 @@ void tw_close(tw_ctx* ctx) {
     for (int i = 0; i < 3; i++) { ctx->eng[i].release(&ctx->held); ctx->wire[i].release(&ctx->held); }
     for (int i = 0; i < 2; i++) { ctx->pyr[i].release(&ctx->held); ctx->work[i].release(&ctx->held); ctx->flow[i].release(&ctx->held); }
     for (int i = 0; i < 4; i++) ctx->plane[i].release(&ctx->held);
+    for (auto& L : ctx->lanes) {
+        for (int i = 0; i < 2; i++) {
+            L.eng[i].release(&ctx->held); L.pyr[i].release(&ctx->held); L.work[i].release(&ctx->held);
+            L.flow[i].release(&ctx->held);
+            for (int j = 0; j < 3; j++) L.scratch[i][j].release(&ctx->held);
+            if (L.s[i]) cudaStreamDestroy(L.s[i]);
+            if (L.ev_pyr[i]) cudaEventDestroy(L.ev_pyr[i]);
+        }
+        L.flags.release(&ctx->held);
+        if (L.ev_solve1) cudaEventDestroy(L.ev_solve1);
+        if (L.ev_done) cudaEventDestroy(L.ev_done);
+    }
+    if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     for (auto e : ctx->prof.ev) cudaEventDestroy(e);
     delete ctx;
@@ -582,6 +613,7 @@ int tw_stats(const tw_ctx* ctx, uint64_t* kernel_launches, uint64_t* device_byte
 int tw_profile_begin(tw_ctx* ctx, const char* kernel) {
     if (!ctx || !kernel) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     for (auto e : ctx->prof.ev) cudaEventDestroy(e);
     ctx->prof = KernelProfile();
     ctx->prof.on = true;
@@ -592,6 +624,7 @@ int tw_profile_begin(tw_ctx* ctx, const char* kernel) {
 int tw_profile_end(tw_ctx* ctx, double* total_ms, uint64_t* launches, double* bytes) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "profile sync"));
     double ms = 0.0;
     for (size_t i = 0; i + 1 < ctx->prof.ev.size(); i += 2) {
@@ -610,6 +643,7 @@ int tw_profile_end(tw_ctx* ctx, double* total_ms, uint64_t* launches, double* by
 size_t tw_profile_report(tw_ctx* ctx, char* buf, size_t cap) {
     if (!ctx) return 0;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return 0;
     struct Row { double ms = 0.0, bytes = 0.0; uint64_t n = 0; };
     std::vector<std::pair<std::string, Row>> rows;
@@ -647,7 +681,9 @@ size_t tw_profile_report(tw_ctx* ctx, char* buf, size_t cap) {
 int tw_set_stream(tw_ctx* ctx, void* stream) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     ctx->stream = (cudaStream_t)stream;
+    ctx->cur = ctx->stream;
     ctx->own_stream = false;
     return TW_OK;
 }
@@ -703,8 +739,8 @@ static int solve_common(tw_ctx* ctx, const tw_image* a, const tw_image* b, const
     CHECK(ctx->ensure(ctx->pyr[1], 2 * pf * 4, "pyramid"));
     float* px_ = ctx->pyr[0].as<float>();
     float* py_ = ctx->pyr[1].as<float>();
-    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, a->width, a->height, a->fmt, *s, g, px_, px_ + pf));
-    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, b->width, b->height, b->fmt, *s, g, py_, py_ + pf));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, a->width, a->height, a->fmt, *s, g, px_, px_ + pf, ctx->plane));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, b->width, b->height, b->fmt, *s, g, py_, py_ + pf, ctx->plane));
     size_t fb = (size_t)g.w * g.h * 2 * sizeof(float);
     CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
     CHECK(ctx->ensure(ctx->flow[1], fb, "flow"));
@@ -728,6 +764,7 @@ static int solve_common(tw_ctx* ctx, const tw_image* a, const tw_image* b, const
 int tw_solve(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_flow_settings* s, tw_flow* out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     if (!out) return ctx->fail(TW_ERR_BAD_PARAM, "no output flow");
     return solve_common(ctx, x, y, s, out, nullptr, false);
 }
@@ -736,6 +773,7 @@ int tw_solve_pair(tw_ctx* ctx, const tw_image* a, const tw_image* b, const tw_fl
                   tw_flow* f_ba) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     if (!f_ab || !f_ba) return ctx->fail(TW_ERR_BAD_PARAM, "no output flow");
     return solve_common(ctx, a, b, s, f_ab, f_ba, true);
 }
@@ -743,6 +781,7 @@ int tw_solve_pair(tw_ctx* ctx, const tw_image* a, const tw_image* b, const tw_fl
 int tw_build_pyramid(tw_ctx* ctx, const tw_image* img, const tw_flow_settings* s, float* levels_out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     CHECK(check_image(ctx, img, "build_pyramid"));
     if (!s || !levels_out) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
     Geo g;
@@ -751,7 +790,7 @@ int tw_build_pyramid(tw_ctx* ctx, const tw_image* img, const tw_flow_settings* s
     size_t pf = pyramid_floats(g);
     CHECK(ctx->ensure(ctx->pyr[0], 2 * pf * 4, "pyramid"));
     CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, img->width, img->height, img->fmt, *s, g, ctx->pyr[0].as<float>(),
-                            ctx->pyr[0].as<float>() + pf));
+                            ctx->pyr[0].as<float>() + pf, ctx->plane));
     CHECK(ctx->cuda(cudaMemcpyAsync(levels_out, ctx->pyr[0].p, pf * 4, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     int hf[1];
     return finish(ctx, hf, 1);
@@ -761,6 +800,7 @@ int tw_compose_vectors(tw_ctx* ctx, const tw_engine_settings* settings, const tw
                        const tw_image* b, const tw_flow* f_ab, const tw_flow* f_ba, tw_image_mut* out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     if (!settings || !sel || !out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
     CHECK(check_image(ctx, a, "compose"));
     CHECK(check_image(ctx, b, "compose"));
@@ -799,6 +839,7 @@ int tw_compose_vectors(tw_ctx* ctx, const tw_engine_settings* settings, const tw
 int tw_block_match(tw_ctx* ctx, const float* a, const float* b, float* flow, int32_t width, int32_t height) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     if (!a || !b || !flow || width <= 0 || height <= 0) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
     if (width > BM_MAX_LINE || height > BM_MAX_LINE) return ctx->fail(TW_ERR_UNSUPPORTED, "block matching: a side above 6144");
     size_t n = (size_t)width * height;
@@ -826,6 +867,7 @@ int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_fl
                 uint8_t* cov) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     CHECK(check_image(ctx, src, "inv_warp"));
     if (!out || !out->data || !flow || !flow->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
     if (out->width != src->width || out->height != src->height || out->fmt != src->fmt)
@@ -857,6 +899,7 @@ int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_fl
 int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* b, float w) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     CHECK(check_image(ctx, a, "blend"));
     CHECK(check_image(ctx, b, "blend"));
     if (!out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
@@ -880,6 +923,7 @@ int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* 
 int tw_from_frame(tw_ctx* ctx, const void* wire, int32_t width, int32_t height, int32_t fmt, void* engine_out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     if (!wire || !engine_out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
     size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
     CHECK(ctx->ensure(ctx->wire[0], bytes, "wire"));
@@ -897,6 +941,7 @@ int tw_from_frame(tw_ctx* ctx, const void* wire, int32_t width, int32_t height, 
 int tw_to_frame(tw_ctx* ctx, const void* engine, int32_t width, int32_t height, int32_t fmt, void* wire_out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     if (!engine || !wire_out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
     size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
     CHECK(ctx->ensure(ctx->wire[0], bytes, "wire"));
@@ -920,23 +965,47 @@ static void from_frame_dev(tw_ctx* ctx, const void* wire, void* eng, int W, int 
     else LAUNCH(ctx, k_from_frame_f32, grid1(n), TB, 0, (const float*)wire, (float*)eng, W, H, flip);
 }
 
-// One output frame from two device-resident wire frames (nullptr = a blank frame outside the clip).
-// Writes the output wire frame to out_wire (device). Flags: the caller resets them.
-static int retime_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel, const void* wa,
-                            const void* wb, int W, int H, int fmt, void* out_wire) {
+static int lane_ready(tw_ctx* ctx, Lane& L) {
+    if (L.s[0]) return TW_OK;
+    for (int i = 0; i < 2; i++) {
+        CHECK(ctx->cuda(cudaStreamCreateWithFlags(&L.s[i], cudaStreamNonBlocking), "lane stream"));
+        CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_pyr[i], cudaEventDisableTiming), "lane event"));
+    }
+    CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_solve1, cudaEventDisableTiming), "lane event"));
+    CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming), "lane event"));
+    CHECK(ctx->ensure(L.flags, FLAGS_BYTES, "lane flags"));
+    return TW_OK;
+}
+
+// One output frame on lane L from two device-resident wire frames (nullptr = a blank frame outside
+// the clip); writes the output wire frame to out_wire (device). Both lane streams must already be
+// ordered after the caller's work (ctx->ev_start); the frame's end is L.ev_done on stream 0.
+static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, const tw_selection& sel, const void* wa,
+                             const void* wb, int W, int H, int fmt, void* out_wire) {
     size_t bytes = (size_t)W * H * 4 * sample_bytes(fmt);
-    int* flags = ctx->flags.as<int>();
-    CHECK(ctx->ensure(ctx->eng[0], bytes, "engine A"));
-    CHECK(ctx->ensure(ctx->eng[1], bytes, "engine B"));
+    int* flags = L.flags.as<int>();
+    CHECK(ctx->ensure(L.eng[0], bytes, "engine A"));
+    CHECK(ctx->ensure(L.eng[1], bytes, "engine B"));
     bool vector = sel.vectors_quality != 0 && !sel.exact;
     bool flip = vector && s.motion_rows_reversed != 0;
+    // stream 1 reuses this lane's buffers: it waits for the lane's previous frame
+    if (L.used) CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[1], L.ev_done, 0), "lane order"));
+    L.used = true;
     // a frame outside the clip is blank (host.rs:338-352); blank images are all zero in every depth
-    if (wa) from_frame_dev(ctx, wa, ctx->eng[0].p, W, H, fmt, flip);
-    else CHECK(ctx->cuda(cudaMemsetAsync(ctx->eng[0].p, 0, bytes, ctx->stream), "blank"));
-    if (wb) from_frame_dev(ctx, wb, ctx->eng[1].p, W, H, fmt, flip);
-    else CHECK(ctx->cuda(cudaMemsetAsync(ctx->eng[1].p, 0, bytes, ctx->stream), "blank"));
-    if (!vector) return interpolate_dev(ctx, sel, ctx->eng[0].p, ctx->eng[1].p, W, H, fmt, out_wire, true, flags + FL_BAD);
-
+    ctx->cur = L.s[0];
+    if (wa) from_frame_dev(ctx, wa, L.eng[0].p, W, H, fmt, flip);
+    else CHECK(ctx->cuda(cudaMemsetAsync(L.eng[0].p, 0, bytes, ctx->cur), "blank"));
+    ctx->cur = L.s[1];
+    if (wb) from_frame_dev(ctx, wb, L.eng[1].p, W, H, fmt, flip);
+    else CHECK(ctx->cuda(cudaMemsetAsync(L.eng[1].p, 0, bytes, ctx->cur), "blank"));
+    if (!vector) {
+        CHECK(ctx->cuda(cudaEventRecord(L.ev_pyr[1], L.s[1]), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_pyr[1], 0), "event"));
+        ctx->cur = L.s[0];
+        CHECK(interpolate_dev(ctx, sel, L.eng[0].p, L.eng[1].p, W, H, fmt, out_wire, true, flags + FL_BAD));
+        CHECK(ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event"));
+        return TW_OK;
+    }
     // the vector path (compose/vector.rs:163-178 solve_flows, then compose_vectors)
     tw_flow_settings fs = s.flow;
     fs.quality = sel.vectors_quality;
@@ -944,15 +1013,21 @@ static int retime_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_s
     Geo g;
     CHECK(geometry(fs, W, H, &g, &ctx->err));
     size_t pf = pyramid_floats(g);
-    CHECK(ctx->ensure(ctx->pyr[0], 2 * pf * 4, "pyramid"));
-    CHECK(ctx->ensure(ctx->pyr[1], 2 * pf * 4, "pyramid"));
-    float* px_ = ctx->pyr[0].as<float>();
-    float* py_ = ctx->pyr[1].as<float>();
-    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, W, H, fmt, fs, g, px_, px_ + pf));
-    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, W, H, fmt, fs, g, py_, py_ + pf));
+    CHECK(ctx->ensure(L.pyr[0], 2 * pf * 4, "pyramid"));
+    CHECK(ctx->ensure(L.pyr[1], 2 * pf * 4, "pyramid"));
+    float* px_ = L.pyr[0].as<float>();
+    float* py_ = L.pyr[1].as<float>();
     size_t fb = (size_t)g.w * g.h * 2 * sizeof(float);
-    CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
-    CHECK(ctx->ensure(ctx->flow[1], fb, "flow"));
+    CHECK(ctx->ensure(L.flow[0], fb, "flow"));
+    CHECK(ctx->ensure(L.flow[1], fb, "flow"));
+    ctx->cur = L.s[0];
+    CHECK(build_pyramid_dev(ctx, L.eng[0].p, W, H, fmt, fs, g, px_, px_ + pf, L.scratch[0]));
+    CHECK(ctx->cuda(cudaEventRecord(L.ev_pyr[0], L.s[0]), "event"));
+    ctx->cur = L.s[1];
+    CHECK(build_pyramid_dev(ctx, L.eng[1].p, W, H, fmt, fs, g, py_, py_ + pf, L.scratch[1]));
+    CHECK(ctx->cuda(cudaEventRecord(L.ev_pyr[1], L.s[1]), "event"));
+    CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_pyr[1], 0), "event"));
+    CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[1], L.ev_pyr[0], 0), "event"));
     bool need_ab = true, need_ba = true;
     if (sel.interp == 0) {
         bool use_ab = (sel.wa < 0.5f && (unsigned)s.compose.warp_mode < 2) || (0.5f <= sel.wa && (unsigned)s.compose.warp_mode > 1);
@@ -961,20 +1036,61 @@ static int retime_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_s
     } else if (sel.interp != 1 && sel.interp != 2) {
         return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
     }
-    if (need_ab)
-        CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, fs, ctx->work[0], ctx->flow[0].as<float>(),
+    if (need_ab) {
+        ctx->cur = L.s[0];
+        CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, fs, L.work[0], L.flow[0].as<float>(),
                                  flags + FL_ANY0, flags + FL_NAN));
-    if (need_ba)
-        CHECK(solve_pyramids_dev(ctx, py_, px_, py_ + pf, px_ + pf, g, fs, ctx->work[1], ctx->flow[1].as<float>(),
+    }
+    if (need_ba) {
+        ctx->cur = L.s[1];
+        CHECK(solve_pyramids_dev(ctx, py_, px_, py_ + pf, px_ + pf, g, fs, L.work[1], L.flow[1].as<float>(),
                                  flags + FL_ANY1, flags + FL_NAN));
-    return compose_dev(ctx, s.compose, sel, ctx->eng[0].p, ctx->eng[1].p, need_ab ? ctx->flow[0].as<float>() : nullptr,
-                       need_ba ? ctx->flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, out_wire, true, flip,
-                       flags + FL_BAD);
+    }
+    CHECK(ctx->cuda(cudaEventRecord(L.ev_solve1, L.s[1]), "event"));
+    CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_solve1, 0), "event"));
+    ctx->cur = L.s[0];
+    CHECK(compose_dev(ctx, s.compose, sel, L.eng[0].p, L.eng[1].p, need_ab ? L.flow[0].as<float>() : nullptr,
+                      need_ba ? L.flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, out_wire, true, flip,
+                      flags + FL_BAD));
+    CHECK(ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event"));
+    return TW_OK;
 }
 
-static int check_flags(tw_ctx* ctx) {
-    int hf[2];
-    CHECK(finish(ctx, hf, 2));
+// Orders the first `nl` lanes' streams after the caller's work on ctx->stream (flags cleared first).
+static int lanes_begin(tw_ctx* ctx, int nl) {
+    for (int i = 0; i < nl; i++) {
+        Lane& L = ctx->lanes[i];
+        CHECK(lane_ready(ctx, L));
+        CHECK(ctx->cuda(cudaMemsetAsync(L.flags.p, 0, FLAGS_BYTES, ctx->stream), "flags"));
+    }
+    CHECK(ctx->cuda(cudaEventRecord(ctx->ev_start, ctx->stream), "event"));
+    for (int i = 0; i < nl; i++)
+        for (int k = 0; k < 2; k++) CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->lanes[i].s[k], ctx->ev_start, 0), "event"));
+    return TW_OK;
+}
+
+// The caller's stream waits for the lanes; then their flags are checked (this synchronises).
+static int lanes_end(tw_ctx* ctx, int nl) {
+    for (int i = 0; i < nl; i++) {
+        Lane& L = ctx->lanes[i];
+        if (!L.used) continue;
+        CHECK(ctx->cuda(cudaEventRecord(L.ev_solve1, L.s[1]), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, L.ev_solve1, 0), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, L.ev_done, 0), "event"));
+    }
+    ctx->cur = ctx->stream;
+    int hf[2] = {0, 0};
+    for (int i = 0; i < nl; i++) {
+        Lane& L = ctx->lanes[i];
+        if (!L.used) continue;
+        int f[2];
+        CHECK(ctx->cuda(cudaMemcpyAsync(f, (int*)L.flags.p + FL_NAN, sizeof f, cudaMemcpyDeviceToHost, ctx->stream), "flags"));
+        CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution"));
+        hf[0] |= f[0];
+        hf[1] |= f[1];
+        L.used = false;
+    }
+    CHECK(ctx->cuda(cudaGetLastError(), "kernel execution"));
     if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
     if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
     return TW_OK;
@@ -984,6 +1100,7 @@ int tw_retime_frame(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection
                     const void* wire_b, int32_t width, int32_t height, int32_t fmt, void* wire_out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     if (!s || !sel || !wire_out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0)
         return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
     size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
@@ -992,29 +1109,36 @@ int tw_retime_frame(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection
     CHECK(ctx->ensure(ctx->wire[2], bytes, "wire out"));
     if (wire_a) CHECK(ctx->cuda(cudaMemcpyAsync(ctx->wire[0].p, wire_a, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload"));
     if (wire_b) CHECK(ctx->cuda(cudaMemcpyAsync(ctx->wire[1].p, wire_b, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload"));
-    CHECK(ctx->cuda(cudaMemsetAsync(ctx->flags.p, 0, FLAGS_BYTES, ctx->stream), "flags"));
-    CHECK(retime_frame_dev(ctx, *s, *sel, wire_a ? ctx->wire[0].p : nullptr, wire_b ? ctx->wire[1].p : nullptr, width,
-                           height, fmt, ctx->wire[2].p));
+    CHECK(lanes_begin(ctx, 1));
+    int rc = retime_frame_lane(ctx, ctx->lanes[0], *s, *sel, wire_a ? ctx->wire[0].p : nullptr,
+                               wire_b ? ctx->wire[1].p : nullptr, width, height, fmt, ctx->wire[2].p);
+    int rc2 = lanes_end(ctx, 1);
+    if (rc) return rc;
+    if (rc2) return rc2;
     CHECK(ctx->cuda(cudaMemcpyAsync(wire_out, ctx->wire[2].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
-    return check_flags(ctx);
+    return ctx->cuda(cudaStreamSynchronize(ctx->stream), "download");
 }
 
 int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
                           const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
     if (!s || !sels || !frames || !out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
         return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
     size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
-    CHECK(ctx->cuda(cudaMemsetAsync(ctx->flags.p, 0, FLAGS_BYTES, ctx->stream), "flags"));
-    for (int k = 0; k < nout; k++) {
+    const int nl = std::min(MAX_LANES, 3);
+    CHECK(lanes_begin(ctx, nl));
+    int rc = TW_OK;
+    for (int k = 0; k < nout && rc == TW_OK; k++) {
         const tw_selection& sel = sels[k];
         const uint8_t* base = (const uint8_t*)frames;
         const void* fa = (sel.a >= 0 && sel.a < nframes) ? base + (size_t)sel.a * bytes : nullptr;
         const void* fb = (sel.b >= 0 && sel.b < nframes) ? base + (size_t)sel.b * bytes : nullptr;
-        CHECK(retime_frame_dev(ctx, *s, sel, fa, fb, width, height, fmt, (uint8_t*)out + (size_t)k * bytes));
+        rc = retime_frame_lane(ctx, ctx->lanes[k % nl], *s, sel, fa, fb, width, height, fmt, (uint8_t*)out + (size_t)k * bytes);
     }
-    return check_flags(ctx);
+    int rc2 = lanes_end(ctx, nl);
+    return rc ? rc : rc2;
 }
 
 }  // extern "C"
