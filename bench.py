@@ -9,9 +9,9 @@ the reference CPU path.
 
 * ``value``: output frames/s with the source clip resident in HBM (tw_retime_clip_device), timed
   with CUDA events on the library's stream, L2 flushed between steps, max over ranks.
-* ``e2e``: the same frames through the reference-facing C ABI call with host buffers
-  (tw_retime_frame: both source frames uploaded from pinned host memory and the output frame read
-  back, for every output frame).
+* ``e2e``: the same frames through the C ABI's host-buffer clip call (tw_retime_clip): every
+  source frame the step references is uploaded from pinned host memory and every output frame is
+  read back into pinned host memory inside the timed region.
 * ``roofline``: the dominant kernel's algorithmic bytes / its event-timed device time.
 * ``cpu_baseline``: the CPU oracle (the reference CPU path restated in C++, OpenMP over all host
   cores) on a bounded sample of the same workload.
@@ -288,10 +288,10 @@ def main():
     out_host = torch.empty(FRAMES_PER_STEP * fs, dtype=torch.uint8).pin_memory().numpy()
 
     def step_host(k):
-        for j, sel in enumerate(sels[k * FRAMES_PER_STEP:(k + 1) * FRAMES_PER_STEP]):
-            fa = pin_np[sel.a * fs:(sel.a + 1) * fs] if 0 <= sel.a < nframes else None
-            fb = pin_np[sel.b * fs:(sel.b + 1) * fs] if 0 <= sel.b < nframes else None
-            dev.retime_frame(settings, sel, fa, fb, W, H, 0, out=out_host[j * fs:(j + 1) * fs])
+        # the step's source frames (the ones its selections reference) are uploaded from pinned host
+        # memory inside the call, and every output frame is copied back into pinned host memory
+        s = sels[k * FRAMES_PER_STEP:(k + 1) * FRAMES_PER_STEP]
+        dev.retime_clip(settings, pin_np, nframes, s, W, H, 0, out=out_host)
 
     for k in range(args.warmup):
         step_host(k)
@@ -308,7 +308,7 @@ def main():
     barrier()
     e2e_ms = max_over_ranks(sum(etimes))
     e2e_value = ws * args.steps * FRAMES_PER_STEP / (e2e_ms / 1e3)
-    h2d = sum(fs * ((0 <= s.a < nframes) + (0 <= s.b < nframes)) for s in sels[:FRAMES_PER_STEP])
+    h2d = fs * len({f for s in sels[:FRAMES_PER_STEP] for f in (s.a, s.b) if 0 <= f < nframes})
     d2h = FRAMES_PER_STEP * fs
 
     if rank == 0:

@@ -241,6 +241,15 @@ int tw_select(const tw_time_params* p, int32_t n, int32_t width, int32_t height,
 int tw_retime_frame(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection* sel, const void* wire_a,
                     const void* wire_b, int32_t width, int32_t height, int32_t fmt, void* wire_out);
 
+/* The same over a clip in HOST memory (page-locked memory makes the copies asynchronous):
+ * `frames` holds nframes wire frames back to back, output frame k goes to out + k * frame_bytes.
+ * Each source frame a selection references is uploaded once into a device frame cache (the
+ * reference's device backend keeps resident frames the same way, device/exec/backend.rs:190-208),
+ * several output frames are in flight at once, and uploads, kernels and downloads overlap on
+ * separate streams. Returns after every output frame is in `out`. */
+int tw_retime_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
+                   const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out);
+
 /* The same over a clip resident in device memory: `frames` holds nframes wire frames back to
  * back, `sels` nout selections; output frame k goes to out + k * frame_bytes. Source frames
  * outside the clip are blank. All pointers are device pointers; the call enqueues on the

@@ -239,3 +239,31 @@ def test_unsupported_settings_fail_loudly(dev):
         dev.solve_pair(a, b, w, h, 0, tw.FlowSettings(prep_contrast_edge=True))
     with pytest.raises(tw.BadParam):
         dev.solve_pair(a, b, w, h, 0, tw.FlowSettings(quality=0))
+
+
+@pytest.mark.parametrize("speed,n,nout,size", [(50.0, 48, 95, (160, 96)), (150.0, 8, 12, (64, 48)),
+                                               (33.3333, 12, 30, (97, 61)), (-50.0, 6, 8, (48, 32))])
+def test_retime_clip_host_buffers(dev, speed, n, nout, size):
+    """tw_retime_clip: the clip in host memory, a device frame cache with eviction, frames past the
+    clip's ends blank, three output frames in flight; every output byte equals the oracle's."""
+    w, h = size
+    frames = synth.moving_clip(w, h, n, depth=8, seed=int(speed * 10) & 0xffff)
+    tp = tw.TimeParams(speed_percent=speed)
+    sels = [tw.select(tp, k, w, h) for k in range(nout)]
+    out = dev.retime_clip(tw.RetimeSettings(), frames, n, sels, w, h, 0)
+    want = O.retime_clip(frames, n, w, h, 0, O.retime_params(speed=speed), nout)
+    assert same(out, want)
+
+
+def test_retime_clip_device_matches_host_clip(dev):
+    import torch
+    w, h, n = 160, 96, 10
+    frames = synth.moving_clip(w, h, n, depth=8, seed=5)
+    tp = tw.TimeParams(speed_percent=40.0)
+    sels = [tw.select(tp, k, w, h) for k in range(20)]
+    host = dev.retime_clip(tw.RetimeSettings(), frames, n, sels, w, h, 0)
+    d_in = torch.from_numpy(frames).cuda()
+    d_out = torch.zeros(len(sels) * w * h * 4, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    dev.retime_clip_device(tw.RetimeSettings(), d_in.data_ptr(), n, sels, w, h, 0, d_out.data_ptr())
+    assert same(d_out.cpu().numpy(), host)

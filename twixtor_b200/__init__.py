@@ -248,6 +248,8 @@ def library():
     L.tw_select.argtypes = [ctypes.POINTER(_TimeParams), i32, i32, i32, ctypes.POINTER(_Selection)]
     L.tw_retime_frame.argtypes = [P, ctypes.POINTER(_RetimeSettings), ctypes.POINTER(_Selection), P, P, i32, i32,
                                   i32, P]
+    L.tw_retime_clip.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, ctypes.POINTER(_Selection), i32, i32,
+                                 i32, i32, P]
     L.tw_retime_clip_device.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, ctypes.POINTER(_Selection), i32,
                                         i32, i32, i32, P]
     _lib = L
@@ -452,6 +454,18 @@ class Device:
             out = np.zeros(width * height * 4, DTYPES[fmt])
         self._check(self._L.tw_retime_frame(self._h, ctypes.byref(settings._c()), ctypes.byref(sel._c()),
                                             _ptr(wire_a), _ptr(wire_b), width, height, fmt, _ptr(out)))
+        return out
+
+    def retime_clip(self, settings: RetimeSettings, frames, nframes: int, sels, width, height, fmt, out=None):
+        """Output frames ``sels`` of a clip in host memory (wire frames back to back in ``frames``;
+        page-locked memory makes the copies asynchronous). Returns the output frames back to back."""
+        frames = np.ascontiguousarray(frames)
+        fs = width * height * 4
+        if out is None:
+            out = np.zeros(len(sels) * fs, DTYPES[fmt])
+        arr = (_Selection * len(sels))(*[s._c() for s in sels])
+        self._check(self._L.tw_retime_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes, arr, len(sels),
+                                           width, height, fmt, _ptr(out)))
         return out
 
     def retime_clip_device(self, settings: RetimeSettings, frames_ptr: int, nframes: int, sels, width, height, fmt,

@@ -180,6 +180,13 @@ struct tw_ctx {
     cudaStream_t cur = nullptr;  // the stream every launch goes to
     Lane lanes[MAX_LANES];
     cudaEvent_t ev_start = nullptr;
+    // tw_retime_clip: a device cache of source frames, and the copy streams
+    static constexpr int CACHE_SLOTS = 10;
+    DevBuf cache[CACHE_SLOTS], outbuf[MAX_LANES];
+    int cache_frame[CACHE_SLOTS];
+    cudaEvent_t cache_ready[CACHE_SLOTS] = {}, out_free[MAX_LANES] = {};
+    cudaEvent_t cache_free[CACHE_SLOTS][MAX_LANES] = {};  // per slot, the end of each lane's last read
+    cudaStream_t up = nullptr, down = nullptr;
     cudaStream_t stream = nullptr;
     cudaStream_t own = nullptr;  // the stream the context created
     bool own_stream = true;
@@ -587,6 +594,18 @@ void tw_close(tw_ctx* ctx) {
         if (L.ev_done) cudaEventDestroy(L.ev_done);
     }
     if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+    for (int i = 0; i < tw_ctx::CACHE_SLOTS; i++) {
+        ctx->cache[i].release(&ctx->held);
+        if (ctx->cache_ready[i]) cudaEventDestroy(ctx->cache_ready[i]);
+        for (int j = 0; j < MAX_LANES; j++)
+            if (ctx->cache_free[i][j]) cudaEventDestroy(ctx->cache_free[i][j]);
+    }
+    for (int i = 0; i < MAX_LANES; i++) {
+        ctx->outbuf[i].release(&ctx->held);
+        if (ctx->out_free[i]) cudaEventDestroy(ctx->out_free[i]);
+    }
+    if (ctx->up) cudaStreamDestroy(ctx->up);
+    if (ctx->down) cudaStreamDestroy(ctx->down);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     for (auto e : ctx->prof.ev) cudaEventDestroy(e);
     delete ctx;
@@ -1116,6 +1135,95 @@ int tw_retime_frame(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection
     if (rc) return rc;
     if (rc2) return rc2;
     CHECK(ctx->cuda(cudaMemcpyAsync(wire_out, ctx->wire[2].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    return ctx->cuda(cudaStreamSynchronize(ctx->stream), "download");
+}
+
+// tw_retime_clip: output frame k runs on lane k % nl. Its two source frames come from the device
+// frame cache (uploaded on the `up` stream once, in order of first use; a slot is reused only after
+// the frames that read it are done); the frame is composed into the lane's output buffer and copied
+// down on the `down` stream, which the lane's next frame waits for before it writes that buffer.
+int tw_retime_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
+                   const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!s || !sels || !frames || !out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
+        return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
+    const int nl = std::min(MAX_LANES, 3);
+    const int NS = tw_ctx::CACHE_SLOTS;
+    if (!ctx->up) {
+        CHECK(ctx->cuda(cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking), "copy stream"));
+        CHECK(ctx->cuda(cudaStreamCreateWithFlags(&ctx->down, cudaStreamNonBlocking), "copy stream"));
+        for (int i = 0; i < NS; i++) {
+            CHECK(ctx->cuda(cudaEventCreateWithFlags(&ctx->cache_ready[i], cudaEventDisableTiming), "event"));
+            for (int j = 0; j < MAX_LANES; j++)
+                CHECK(ctx->cuda(cudaEventCreateWithFlags(&ctx->cache_free[i][j], cudaEventDisableTiming), "event"));
+        }
+        for (int i = 0; i < MAX_LANES; i++)
+            CHECK(ctx->cuda(cudaEventCreateWithFlags(&ctx->out_free[i], cudaEventDisableTiming), "event"));
+    }
+    for (int i = 0; i < NS; i++) {
+        CHECK(ctx->ensure(ctx->cache[i], bytes, "frame cache"));
+        ctx->cache_frame[i] = -1;
+    }
+    for (int i = 0; i < nl; i++) CHECK(ctx->ensure(ctx->outbuf[i], bytes, "output buffer"));
+    CHECK(lanes_begin(ctx, nl));
+    CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->up, ctx->ev_start, 0), "event"));
+    CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->down, ctx->ev_start, 0), "event"));
+    std::vector<int> last_use(NS, -1);   // the last output frame that reads each slot
+    std::vector<unsigned> readers(NS, 0);  // lanes that read each slot since its upload
+    std::vector<bool> out_used(nl, false);
+    auto frame_slot = [&](int f, int k, int keep) -> int {  // the slot holding source frame f (uploaded if absent)
+        for (int i = 0; i < NS; i++)
+            if (ctx->cache_frame[i] == f) { last_use[i] = k; return i; }
+        int best = -1;
+        for (int i = 0; i < NS; i++) {  // the least recently used slot that the current frame does not hold
+            if (i == keep) continue;
+            if (best < 0 || last_use[i] < last_use[best]) best = i;
+        }
+        for (int j = 0; j < nl; j++)  // every frame that read the old contents has finished
+            if (readers[best] & (1u << j)) cudaStreamWaitEvent(ctx->up, ctx->cache_free[best][j], 0);
+        readers[best] = 0;
+        cudaMemcpyAsync(ctx->cache[best].p, (const uint8_t*)frames + (size_t)f * bytes, bytes, cudaMemcpyHostToDevice, ctx->up);
+        cudaEventRecord(ctx->cache_ready[best], ctx->up);
+        ctx->cache_frame[best] = f;
+        last_use[best] = k;
+        return best;
+    };
+    int rc = TW_OK;
+    for (int k = 0; k < nout && rc == TW_OK; k++) {
+        const tw_selection& sel = sels[k];
+        int li = k % nl;
+        Lane& L = ctx->lanes[li];
+        int sa = (sel.a >= 0 && sel.a < nframes) ? frame_slot(sel.a, k, -1) : -1;
+        int sb = (sel.b >= 0 && sel.b < nframes) ? frame_slot(sel.b, k, sa) : -1;
+        for (int st = 0; st < 2; st++) {
+            if (sa >= 0) cudaStreamWaitEvent(L.s[st], ctx->cache_ready[sa], 0);
+            if (sb >= 0) cudaStreamWaitEvent(L.s[st], ctx->cache_ready[sb], 0);
+        }
+        if (out_used[li]) cudaStreamWaitEvent(L.s[0], ctx->out_free[li], 0);
+        rc = retime_frame_lane(ctx, L, *s, sel, sa >= 0 ? ctx->cache[sa].p : nullptr, sb >= 0 ? ctx->cache[sb].p : nullptr,
+                               width, height, fmt, ctx->outbuf[li].p);
+        if (rc) break;
+        // the frame's reads of its slots end with the lane's frame (both streams joined at ev_done)
+        if (sa >= 0) { cudaEventRecord(ctx->cache_free[sa][li], L.s[0]); readers[sa] |= 1u << li; }
+        if (sb >= 0) { cudaEventRecord(ctx->cache_free[sb][li], L.s[0]); readers[sb] |= 1u << li; }
+        cudaStreamWaitEvent(ctx->down, L.ev_done, 0);
+        cudaMemcpyAsync((uint8_t*)out + (size_t)k * bytes, ctx->outbuf[li].p, bytes, cudaMemcpyDeviceToHost, ctx->down);
+        cudaEventRecord(ctx->out_free[li], ctx->down);
+        out_used[li] = true;
+    }
+    // the caller's stream waits for the uploads and downloads too
+    cudaEvent_t e_up = ctx->cache_ready[0];
+    CHECK(ctx->cuda(cudaEventRecord(e_up, ctx->up), "event"));
+    CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, e_up, 0), "event"));
+    cudaEvent_t e_down = ctx->out_free[0];
+    CHECK(ctx->cuda(cudaEventRecord(e_down, ctx->down), "event"));
+    CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, e_down, 0), "event"));
+    int rc2 = lanes_end(ctx, nl);
+    if (rc) return rc;
+    if (rc2) return rc2;
     return ctx->cuda(cudaStreamSynchronize(ctx->stream), "download");
 }
 
