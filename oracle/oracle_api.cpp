@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "oracle_core.h"
+#include "oracle_smart.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -148,6 +149,7 @@ struct or_retime_params {
     // flow/conv.rs:598-615); 0, 0 reproduces parity/retime-flow/results/base.grid.tsv.
     int rows_reversed;         // motion path on bottom-up rows
     int taps_above_first;      // vertical border rows of the solver's filters
+    int video_360;             // "360 Video": video range luma, binary alpha Smart Blend
 };
 
 const char* or_last_error(void) { return g_err.c_str(); }
@@ -313,6 +315,51 @@ int or_compose_vectors(const void* a_eng, const void* b_eng, int w, int h, int f
     return 0;
 }
 
+// smartblend.rs:268-298 on engine images (binary != 0: the binary alpha variant)
+int or_smart_blend(void* out_eng, const void* p1_eng, const void* p2_eng, int w, int h, int fmt, float wt, int binary) {
+    Image p1(w, h, (Fmt)fmt), p2(w, h, (Fmt)fmt), out;
+    std::memcpy(p1.data(), p1_eng, p1.bytes());
+    std::memcpy(p2.data(), p2_eng, p2.bytes());
+    smart_blend(out, p1, p2, wt, binary != 0);
+    std::memcpy(out_eng, out.data(), out.bytes());
+    return 0;
+}
+
+// holefill.rs:452-491 in place on an engine image; mask_kind 1 u8, 2 u16, 3 f32
+int or_fill_holes(void* eng, int w, int h, int fmt, const void* mask, int mask_kind, int above_first) {
+    Image img(w, h, (Fmt)fmt);
+    std::memcpy(img.data(), eng, img.bytes());
+    std::string e;
+    int rc = fill_holes(img, mask, mask_kind, above_first != 0, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(eng, img.data(), img.bytes());
+    return 0;
+}
+
+// compose::compose_vectors with a warping code (0 inverse, 1 Smart Blend) and the binary alpha flag
+int or_compose_vectors2(const void* a_eng, const void* b_eng, int w, int h, int fmt, const float* f_ab, const float* f_ba,
+                        int fw, int fh, float wa, int interp, int warp_mode, int video_360, int taps_above_first,
+                        void* out_eng) {
+    Image a(w, h, (Fmt)fmt), b(w, h, (Fmt)fmt), out;
+    std::memcpy(a.data(), a_eng, a.bytes());
+    std::memcpy(b.data(), b_eng, b.bytes());
+    FlowField fab(fw, fh), fba(fw, fh);
+    if (f_ab) std::memcpy(fab.d.data(), f_ab, fab.d.size() * 4);
+    if (f_ba) std::memcpy(fba.d.data(), f_ba, fba.d.size() * 4);
+    ComposeSettings cs;
+    cs.warp_mode = warp_mode;
+    cs.video_360 = video_360 != 0;
+    cs.taps_above_first = taps_above_first != 0;
+    Selection sel;
+    sel.wa = wa;
+    sel.interp = interp;
+    std::string e;
+    int rc = compose_vectors(cs, sel, a, b, f_ab ? &fab : nullptr, f_ba ? &fba : nullptr, &out, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(out_eng, out.data(), out.bytes());
+    return 0;
+}
+
 // ---- the whole effect ---------------------------------------------------------------------------
 
 // One output frame's selection (timeline.rs:451-469) for output frame index n of a clip.
@@ -355,7 +402,6 @@ int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const 
     size_t frame_bytes = (size_t)w * h * 4 * es;
     bool integer = p->fps_den == 1;
     int time_step = integer ? 100 : p->fps_den;
-    if (p->smart_blend) return fail(2, "smart blend is not restated in the clip runner");
     float sensitivity = fixed_reader(float_to_fixed(p->sensitivity), 1.0f) / 100.0f;
     float s0, s1, wa;
     int a, exact, vq, interp;
@@ -383,11 +429,11 @@ int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const 
         fs.hiq = p->quality_high != 0;
         fs.sensitivity = sensitivity;
         fs.taps_above_first = p->taps_above_first != 0;
+        fs.video_range_luma = p->video_360 != 0;  // compose/vector.rs:72-82 (flow_settings)
         FlowField fab, fba;
         bool have_ab = false, have_ba = false;
         if (interp == 0) {
-            ComposeSettings cs0;
-            if (nearest_uses_f_ab(wa, cs0.warp_mode)) {
+            if (nearest_uses_f_ab(wa, p->smart_blend ? 1 : 0)) {
                 if (!solve(ar, br, fs, &fab, &e)) return fail(1, e);
                 have_ab = true;
             } else {
@@ -401,6 +447,9 @@ int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const 
         ComposeSettings cs;
         cs.quality_high = fs.hiq;
         cs.blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
+        cs.warp_mode = p->smart_blend ? 1 : 0;  // plugins/retime frontend: warp_mode = i32::from(smart_blend)
+        cs.video_360 = p->video_360 != 0;
+        cs.taps_above_first = p->taps_above_first != 0;
         Image o;
         int rc = compose_vectors(cs, sel, ar, br, have_ab ? &fab : nullptr, have_ba ? &fba : nullptr, &o, &e);
         if (rc) return fail(rc, e);

@@ -1,6 +1,7 @@
 // CPU oracle, core functions. TEST INFRASTRUCTURE ONLY (see oracle_core.h). Each function cites
 // the reference file:line (crate plugins/retime-engine/src/) whose arithmetic it restates.
 #include "oracle_core.h"
+#include "oracle_smart.h"
 
 #include <algorithm>
 #include <cstdio>
@@ -1071,8 +1072,9 @@ bool nearest_uses_f_ab(float wa, int code) {  // compose/vector.rs:61-64
 
 int compose_vectors(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b,
                     const FlowField* f_ab, const FlowField* f_ba, Image* out, std::string* err) {
-    if (cs.warp_mode != 0) { *err = "compose: only warping code 0 is restated here"; return 2; }
     if (cs.blur > 0.005f && std::fabs(sel.s0 - sel.s1) > 1e-6f) { *err = "blur compensation is not restated"; return 2; }
+    if (cs.warp_mode == 1) return compose_smart(cs, sel, a, b, f_ab, f_ba, cs.taps_above_first, out, err);
+    if (cs.warp_mode != 0) { *err = "compose: warping codes 2 and 3 are not restated here"; return 2; }
     float wa = sel.wa;
     float frac = 1.0f - wa;
     WarpOpts o;

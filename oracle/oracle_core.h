@@ -215,6 +215,7 @@ struct ComposeSettings {
     bool video_360 = false;   // binary alpha Smart Blend / video range luma
     bool quality_high = true;
     float blur = 0.0f;        // blur compensation slider
+    bool taps_above_first = true;  // Stages::vertical_taps() of the hole fill (stages.rs:66-70)
 };
 
 bool nearest_uses_f_ab(float wa, int code);

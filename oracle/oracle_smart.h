@@ -1,0 +1,27 @@
+// CPU oracle: Smart Blend and the hole fill (warping code 1). TEST INFRASTRUCTURE ONLY.
+#pragma once
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "oracle_core.h"
+
+namespace orc {
+
+struct FillGeometry {  // holefill.rs:133-171
+    std::vector<std::pair<int, int>> dims;
+    int top = 0;
+};
+FillGeometry fill_geometry(int w, int h);
+
+// smartblend.rs:268-298: smart_blend (binary false) / smart_blend_binary (binary true)
+void smart_blend(Image& out, const Image& p1, const Image& p2, float w, bool binary);
+
+// holefill.rs:452-491 with the plain passes; mask_kind 1 u8, 2 u16, 3 f32 (w*h entries)
+int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, std::string* err);
+
+// warping code 1 compositions (smartblend.rs:350-393): Nearest and Blend
+int compose_smart(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b, const FlowField* f_ab,
+                  const FlowField* f_ba, bool taps_above_first, Image* out, std::string* err);
+
+}  // namespace orc

@@ -7,13 +7,16 @@ Run in a container that has the reference mounted (default /root/reference):
 Writes, next to this script:
 
 * ``retime_flow_grid.npz`` - the cases of the reference's parity grid
-  ``parity/retime-flow`` that the hot path serves (warping code 0, Nearest or Blend, no prep, no
-  360 video, no smart blend, no blur compensation), their raw input clips as
+  ``parity/retime-flow`` that the hot path serves (warping codes 0 and 1, Nearest or Blend, no
+  prep, no blur compensation), their raw input clips as
   ``parity/retime-flow/gen.py`` regenerates them (numpy, fixed seeds), and the sha256 of the
   output clip that ``parity/retime-flow/results/base.grid.tsv`` records for each. That table was
   recorded by the reference revision whose motion path ran on top-down rows with the vertical
   border taps below first; the tests run the oracle and the CUDA path in that variant
   (``rows_reversed=False, taps_above_first=False``) for these cases.
+* ``f1_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/f1_cases.hex``
+  (the reference's bit-exact numpy models of Smart Blend and the hole fill; format in its
+  ``f1_gen.py``).
 * ``warp_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/warp_cases.hex``
   (the reference's bit-exact numpy model of the inverse warp; format in its ``gen_warp.py``).
 
@@ -33,7 +36,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
-SERVED = {"vectors", "frame_interp", "sensitivity", "blur_compensation", "smart_blend"}
+SERVED = {"vectors", "frame_interp", "sensitivity", "blur_compensation", "smart_blend", "video_360"}
 
 
 def load_gen(ref):
@@ -48,8 +51,6 @@ def served(case):
     params = dict(p.split("=", 1) for p in case["params"])
     params.pop("speed_percent")
     if any(k not in SERVED for k in params):
-        return False
-    if params.get("smart_blend", "0") != "0":
         return False
     if params.get("frame_interp", "2") not in ("1", "2"):
         # Weighted Blend (3) is served on the fast path only, which the case's own frames decide;
@@ -93,6 +94,12 @@ def main():
         arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), np.uint8)
         np.savez_compressed(os.path.join(HERE, "retime_flow_grid.npz"), **arrays)
         print(f"retime_flow_grid.npz: {len(cases)} cases, {len(keys)} input clips")
+
+    txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "f1_cases.hex")).read()
+    blob = bytes.fromhex("".join(txt.split()))
+    with gzip.open(os.path.join(HERE, "f1_cases.bin.gz"), "wb") as f:
+        f.write(blob)
+    print(f"f1_cases.bin.gz: {len(blob)} bytes, sha256 {hashlib.sha256(blob).hexdigest()}")
 
     txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "warp_cases.hex")).read()
     blob = bytes.fromhex("".join(txt.split()))

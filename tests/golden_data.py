@@ -35,7 +35,44 @@ def case_params(case):
     fpsp = tuple(int(x) for x in fps.split("/")) if "/" in fps else (int(fps), 1)
     return dict(fps=fpsp, speed=speed, keys=keys, vectors=int(params.get("vectors", 5)),
                 frame_interp=int(params.get("frame_interp", 2)), sensitivity=float(params.get("sensitivity", 70)),
-                blur=float(params.get("blur_compensation", 0)), rows_reversed=False, taps_above_first=False)
+                blur=float(params.get("blur_compensation", 0)), smart_blend=int(params.get("smart_blend", 0)),
+                video_360=params.get("video_360", "0") == "1", rows_reversed=False, taps_above_first=False)
+
+
+def f1_cases():
+    """The reference's Smart Blend and hole fill model fixtures (f1_cases.hex; format in its f1_gen.py)."""
+    blob = gzip.open(os.path.join(GOLDEN, "f1_cases.bin.gz")).read()
+    assert blob[:4] == b"F1C1"
+    n = struct.unpack_from("<I", blob, 4)[0]
+    p = 8
+    out = []
+    for _ in range(n):
+        kind, depth, w, h = struct.unpack_from("<IIII", blob, p)
+        weight = np.float32(struct.unpack_from("<f", blob, p + 16)[0])
+        mask_kind = struct.unpack_from("<I", blob, p + 20)[0]
+        p += 24
+        dt = DT[depth]
+        cnt = w * h * 4 * np.dtype(dt).itemsize
+
+        def img():
+            nonlocal p
+            v = np.frombuffer(blob[p:p + cnt], dt).copy()
+            p += cnt
+            return v
+
+        p1 = img()
+        p2 = mask = None
+        if kind == 3:
+            msz = {1: 1, 2: 2}.get(mask_kind, 4)
+            mask = np.frombuffer(blob[p:p + w * h * msz], {1: np.uint8, 2: np.uint16}.get(mask_kind, np.float32)).copy()
+            p += w * h * msz
+        else:
+            p2 = img()
+        exp = img()
+        out.append(dict(kind=kind, fmt=depth, w=w, h=h, weight=weight, mask_kind=mask_kind, p1=p1, p2=p2, mask=mask,
+                        out=exp))
+    assert p == len(blob)
+    return out
 
 
 def warp_cases():

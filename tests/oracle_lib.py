@@ -35,6 +35,7 @@ class RetimeParams(ctypes.Structure):
         ("blur_compensation", ctypes.c_double),
         ("rows_reversed", ctypes.c_int),
         ("taps_above_first", ctypes.c_int),
+        ("video_360", ctypes.c_int),
     ]
 
 
@@ -79,6 +80,9 @@ def lib():
         L.or_retime_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_retime_one.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_set_threads.argtypes = [i]
+        L.or_smart_blend.argtypes = [P, P, P, i, i, i, f, i]
+        L.or_fill_holes.argtypes = [P, i, i, i, P, i, i]
+        L.or_compose_vectors2.argtypes = [P, P, i, i, i, P, P, i, i, f, i, i, i, i, P]
         _lib = L
     return _lib
 
@@ -156,11 +160,12 @@ def compose_vectors(a, b, w, h, fmt, f_ab, f_ba, fw, fh, wa, interp=1):
 
 
 def retime_params(fps=(24, 1), quality_high=True, speed=100.0, keys=None, vectors=5, frame_interp=2, smart_blend=0,
-                  sensitivity=70.0, blur=0.0, rows_reversed=True, taps_above_first=True):
+                  sensitivity=70.0, blur=0.0, rows_reversed=True, taps_above_first=True, video_360=False):
     """The `retime` parameters of one render. rows_reversed / taps_above_first at their defaults
     are the reference's current code; both False is the revision the parity grid records."""
     p = RetimeParams()
     p.rows_reversed, p.taps_above_first = int(rows_reversed), int(taps_above_first)
+    p.video_360 = int(video_360)
     p.fps_num, p.fps_den = fps
     p.quality_high = int(quality_high)
     p.speed_percent = speed

@@ -165,3 +165,22 @@ def test_retime_flow_grid_sha256(case):
     p = O.retime_params(**golden_data.case_params(case))
     out = O.retime_clip(raw, case["frames"], case["width"], case["height"], fmt, p, case["frames"])
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
+
+
+F1 = golden_data.f1_cases()
+
+
+@pytest.mark.parametrize("i", range(len(F1)))
+def test_smart_blend_and_hole_fill_model_fixtures(i):
+    """The reference's numpy models of Smart Blend (kind 1), its binary alpha variant (kind 2) and the
+    hole fill (kind 3, engine tap order: below first) reproduced bit for bit."""
+    c = F1[i]
+    if c["kind"] in (1, 2):
+        out = np.zeros_like(c["p1"])
+        O.lib().or_smart_blend(O.ptr(out), O.ptr(c["p1"]), O.ptr(c["p2"]), c["w"], c["h"], c["fmt"], c["weight"],
+                               int(c["kind"] == 2))
+    else:
+        out = c["p1"].copy()
+        rc = O.lib().or_fill_holes(O.ptr(out), c["w"], c["h"], c["fmt"], O.ptr(c["mask"]), c["mask_kind"], 0)
+        assert rc == 0, O.err()
+    assert out.view(np.uint8).tobytes() == c["out"].view(np.uint8).tobytes()
