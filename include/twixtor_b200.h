@@ -204,6 +204,17 @@ int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_fl
 /* blend::blend (blend.rs:55-114). */
 int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* b, float w);
 
+/* smartblend::smart_blend / smart_blend_binary (smartblend.rs:305-315): p1 over p2 and p2 over p1
+ * blended at w, or (binary != 0) the binary alpha composite. */
+int tw_smart_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* p1, const tw_image* p2, float w, int32_t binary);
+
+/* holefill::fill_holes_masked_with (holefill.rs:452-491) with is360 off: the pull-push fill of
+ * `img` in place. `mask` holds width*height values of kind 1 (u8), 2 (u16) or 3 (f32); a pixel is
+ * a hole when !(eps > m) (holefill.rs:124-133). taps_above_first: the vertical border tap order
+ * (0: below first, the engine's order the unit tests use). A hole in an image with a side of 1
+ * pixel is TW_ERR_UNSUPPORTED, as in the reference. */
+int tw_fill_holes(tw_ctx* ctx, tw_image_mut* img, const void* mask, int32_t mask_kind, int32_t taps_above_first);
+
 /* image::Image::from_frame / to_frame (image.rs:178-245): wire frame <-> engine image. */
 int tw_from_frame(tw_ctx* ctx, const void* wire, int32_t width, int32_t height, int32_t fmt, void* engine_out);
 int tw_to_frame(tw_ctx* ctx, const void* engine, int32_t width, int32_t height, int32_t fmt, void* wire_out);

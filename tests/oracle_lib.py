@@ -159,6 +159,26 @@ def compose_vectors(a, b, w, h, fmt, f_ab, f_ba, fw, fh, wa, interp=1):
     return out
 
 
+def compose_vectors2(a, b, w, h, fmt, f_ab, f_ba, fw, fh, wa, interp, warp_mode, video_360=False,
+                     taps_above_first=True):
+    """compose_vectors with a warping code (1: Smart Blend with the hole fill) and the binary alpha flag."""
+    out = np.zeros_like(a)
+    rc = lib().or_compose_vectors2(ptr(a), ptr(b), w, h, fmt, ptr(f_ab) if f_ab is not None else None,
+                                   ptr(f_ba) if f_ba is not None else None, fw, fh, wa, interp, warp_mode,
+                                   int(video_360), int(taps_above_first), ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out
+
+
+def fill_holes(img, w, h, fmt, mask, mask_kind, above_first=True):
+    out = np.array(img, copy=True)
+    rc = lib().or_fill_holes(ptr(out), w, h, fmt, ptr(mask), mask_kind, int(above_first))
+    if rc:
+        raise ValueError(err())
+    return out
+
+
 def retime_params(fps=(24, 1), quality_high=True, speed=100.0, keys=None, vectors=5, frame_interp=2, smart_blend=0,
                   sensitivity=70.0, blur=0.0, rows_reversed=True, taps_above_first=True, video_360=False):
     """The `retime` parameters of one render. rows_reversed / taps_above_first at their defaults

@@ -177,6 +177,89 @@ def test_compose_vectors(dev, fmt, wa, interp):
     assert same(got, want)
 
 
+# ---- Smart Blend and the hole fill --------------------------------------------------------------------
+
+F1 = golden_data.f1_cases()
+
+
+@pytest.mark.parametrize("i", range(len(F1)))
+def test_smart_blend_and_hole_fill_model_fixtures(dev, i):
+    """The reference's numpy models of Smart Blend (kind 1), its binary alpha variant (kind 2) and
+    the hole fill (kind 3, below first taps), on the device."""
+    c = F1[i]
+    w, h, fmt = c["w"], c["h"], c["fmt"]
+    if c["kind"] in (1, 2):
+        out = dev.smart_blend(c["p1"], c["p2"], w, h, fmt, c["weight"], binary=c["kind"] == 2)
+    else:
+        out = dev.fill_holes(c["p1"], w, h, fmt, c["mask"], taps_above_first=False)
+    assert same(out, c["out"])
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("size", [(37, 23), (96, 64), (250, 131)])
+@pytest.mark.parametrize("above_first", [False, True])
+@pytest.mark.parametrize("kind", [1, 2, 3])
+def test_hole_fill_random_masks(dev, fmt, size, above_first, kind):
+    """Random images and masks of each kind (sparse holes, a large hole, NaN mask values)."""
+    w, h = size
+    rng = np.random.RandomState(w * 7 + h + kind * 131 + fmt)
+    img, _ = rand_engine(rng, w, h, fmt)
+    n = w * h
+    if kind == 1:
+        mask = (rng.random_sample(n) < 0.3).astype(np.uint8) * rng.randint(1, 256, n).astype(np.uint8)
+    elif kind == 2:
+        mask = np.where(rng.random_sample(n) < 0.3, rng.randint(1, 65536, n), 0).astype(np.uint16)
+    else:
+        mask = np.where(rng.random_sample(n) < 0.3, rng.random_sample(n), 0.0).astype(np.float32)
+        mask[rng.randint(0, n, 5)] = np.nan
+        mask[rng.randint(0, n, 5)] = 3.0e-5  # just below the threshold: not a hole
+    m2 = mask.reshape(h, w)
+    m2[h // 4:h // 2, w // 3:w // 2] = {1: 255, 2: 65535, 3: 1.0}[kind]
+    got = dev.fill_holes(img, w, h, fmt, mask, taps_above_first=above_first)
+    want = O.fill_holes(img, w, h, fmt, mask, kind, above_first)
+    assert same(got, want)
+
+
+def test_hole_fill_nan_samples_and_identity(dev):
+    """NaN float samples next to holes take the NaN rule's bits; a mask without a hole leaves the
+    image unchanged, NaN payloads included."""
+    w, h = 64, 40
+    rng = np.random.RandomState(5)
+    img, _ = rand_engine(rng, w, h, 2)
+    img[rng.randint(0, img.size, 40)] = np.float32(np.nan)
+    img.view(np.uint32)[rng.randint(0, img.size, 10)] = 0xffc01234
+    mask = (rng.random_sample(w * h) < 0.2).astype(np.uint8)
+    assert same(dev.fill_holes(img, w, h, 2, mask), O.fill_holes(img, w, h, 2, mask, 1))
+    none = np.zeros(w * h, np.uint8)
+    assert same(dev.fill_holes(img, w, h, 2, none), img)
+
+
+def test_hole_fill_side_of_one_pixel(dev):
+    img = np.zeros(1 * 9 * 4, np.uint8)
+    with pytest.raises(tw.Unsupported):
+        dev.fill_holes(img, 1, 9, 0, np.ones(9, np.uint8))
+    assert same(dev.fill_holes(img, 1, 9, 0, np.zeros(9, np.uint8)), img)
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("wa,interp", [(0.5, 1), (0.75, 1), (0.2, 1), (0.0, 1), (0.6, 0), (0.3, 0), (0.5, 0)])
+@pytest.mark.parametrize("binary", [False, True])
+@pytest.mark.parametrize("above_first", [False, True])
+def test_compose_smart_blend(dev, fmt, wa, interp, binary, above_first):
+    """Warping code 1 through compose_vectors: the warps without hold, Smart Blend and the fill of
+    the uncovered pixels. The flows are the solved ones scaled up so that the borders uncover."""
+    w, h = 96, 64
+    a, b, _, _ = clip_pair(w, h, fmt, seed=21)
+    o_ab, o_ba, (fw, fh) = O.solve_pair(a, b, w, h, fmt)
+    o_ab = (o_ab * np.float32(6.0) + np.float32(3.5)).astype(np.float32)
+    o_ba = (o_ba * np.float32(6.0) - np.float32(2.25)).astype(np.float32)
+    sel = tw.Selection(wa=np.float32(wa), interp=interp)
+    cs = tw.EngineSettings(warp_mode=1, video_360=binary, taps_above_first=above_first)
+    got = dev.compose_vectors(cs, sel, a, b, w, h, fmt, o_ab, o_ba, (fw, fh))
+    want = O.compose_vectors2(a, b, w, h, fmt, o_ab, o_ba, fw, fh, np.float32(wa), interp, 1, binary, above_first)
+    assert same(got, want)
+
+
 # ---- whole output frames -----------------------------------------------------------------------------
 
 CASES, INPUTS = golden_data.grid()
@@ -192,8 +275,9 @@ def test_retime_flow_grid_sha256(dev, case):
                        frame_interp=kw["frame_interp"], blur_compensation=kw["blur"])
     settings = tw.RetimeSettings(
         flow=tw.FlowSettings(hiq=True, sensitivity=np.float32(np.float32(kw["sensitivity"]) / np.float32(100.0)),
-                             taps_above_first=False),
-        compose=tw.EngineSettings(taps_above_first=False), motion_rows_reversed=False)
+                             taps_above_first=False, video_range_luma=kw["video_360"]),
+        compose=tw.EngineSettings(warp_mode=kw["smart_blend"], video_360=kw["video_360"], taps_above_first=False),
+        motion_rows_reversed=False)
     out = tw.retime_clip(dev, raw, case["frames"], case["width"], case["height"], fmt, tp, case["frames"], settings)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
 

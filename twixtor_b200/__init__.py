@@ -243,6 +243,8 @@ def library():
     L.tw_inv_warp.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, P]
     L.tw_block_match.argtypes = [P, P, P, P, i32, i32]
     L.tw_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float]
+    L.tw_smart_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float, i32]
+    L.tw_fill_holes.argtypes = [P, pimg, P, i32, i32]
     L.tw_from_frame.argtypes = [P, P, i32, i32, i32, P]
     L.tw_to_frame.argtypes = [P, P, i32, i32, i32, P]
     L.tw_select.argtypes = [ctypes.POINTER(_TimeParams), i32, i32, i32, ctypes.POINTER(_Selection)]
@@ -432,6 +434,28 @@ class Device:
         bi, ba = _img(b, width, height, fmt)
         oi = _Image(width, height, fmt, out.ctypes.data)
         self._check(self._L.tw_blend(self._h, ctypes.byref(oi), ctypes.byref(ai), ctypes.byref(bi), np.float32(w)))
+        return out
+
+    def smart_blend(self, p1, p2, width, height, fmt, w, binary=False):
+        """``smartblend::smart_blend`` (or ``smart_blend_binary``) of two engine images."""
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        ai, aa = _img(p1, width, height, fmt)
+        bi, ba = _img(p2, width, height, fmt)
+        oi = _Image(width, height, fmt, out.ctypes.data)
+        self._check(self._L.tw_smart_blend(self._h, ctypes.byref(oi), ctypes.byref(ai), ctypes.byref(bi), np.float32(w),
+                                           int(binary)))
+        return out
+
+    def fill_holes(self, img, width, height, fmt, mask, taps_above_first=True):
+        """``holefill::fill_holes_masked_with`` (is360 off): the filled copy of an engine image. The
+        mask's dtype picks its kind: uint8, uint16 or float32 (one value per pixel)."""
+        kind = {np.dtype(np.uint8): 1, np.dtype(np.uint16): 2, np.dtype(np.float32): 3}[np.asarray(mask).dtype]
+        mask = np.ascontiguousarray(mask)
+        if mask.size != width * height:
+            raise Mismatch(ERR_MISMATCH, f"hole fill: mask has {mask.size} entries for an image of {width}x{height}")
+        out = np.array(img, DTYPES[fmt], copy=True).reshape(-1)
+        oi = _Image(width, height, fmt, out.ctypes.data)
+        self._check(self._L.tw_fill_holes(self._h, ctypes.byref(oi), _ptr(mask), kind, int(taps_above_first)))
         return out
 
     def from_frame(self, wire, width, height, fmt):

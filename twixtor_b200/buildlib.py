@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtwixtor_b200.so")
-SOURCES = ["solver.cu", "fused.cu", "image.cu", "runtime.cu", "noalloc.cu"]
+SOURCES = ["solver.cu", "fused.cu", "image.cu", "smart.cu", "runtime.cu", "noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FLAGS = [

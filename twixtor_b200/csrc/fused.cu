@@ -6,6 +6,7 @@
 // (flow/conv.rs for the separable passes, flow.rs for the solver steps), so the results are bit
 // identical to the unfused kernels and to the reference CPU path.
 #include "kernels.cuh"
+#include "luma.cuh"
 
 namespace tw {
 
@@ -95,23 +96,9 @@ __device__ __forceinline__ void vpass(const float* src, int RW, int gx0, int gy0
 // ---- pyramid: blur5 + band (flow.rs:261-268) and the first reduction step --------------------------
 
 // tmp = blur5(orig) and band = orig - tmp over one tile; orig is a plane, or (luma_src != nullptr)
-// the luma of an engine image computed on the fly (prep.rs:168-235).
-__device__ __forceinline__ float luma_of(const void* eng, int fmt, long i) {
-    if (fmt == 0) {
-        uchar4 p = reinterpret_cast<const uchar4*>(eng)[i];
-        return ((float)p.y * 0.3f + (float)p.z * 0.59f) + (float)p.w * 0.11f;
-    } else if (fmt == 1) {
-        ushort4 p = reinterpret_cast<const ushort4*>(eng)[i];
-        double sum = ((double)p.z * 0.59 + (double)p.y * 0.3) + (double)p.w * 0.11;
-        return (float)(sum / 257.0);
-    }
-    float4 p = reinterpret_cast<const float4*>(eng)[i];
-    double sum = ((double)p.z * 0.59 + (double)p.y * 0.3) + (double)p.w * 0.11;
-    return (float)(sum * 255.0);
-}
-
+// the luma of an engine image computed on the fly (prep.rs:168-235; luma_mode: the LUMA_* bits).
 __global__ void __launch_bounds__(FT_THREADS) k_blur5_band(const float* __restrict__ orig, const void* __restrict__ luma_src,
-                                                           int fmt, int w, int h, bool above_first,
+                                                           int fmt, int luma_mode, int w, int h, bool above_first,
                                                            float* __restrict__ tmp_out, float* __restrict__ band_out,
                                                            float* __restrict__ band_t_out) {
     constexpr int N = 3, HALO = N - 1;
@@ -128,7 +115,7 @@ __global__ void __launch_bounds__(FT_THREADS) k_blur5_band(const float* __restri
         float v = 0.0f;
         if (X >= 0 && X < w && Y >= 0 && Y < h) {
             long i = (long)Y * w + X;
-            v = luma_src ? luma_of(luma_src, fmt, i) : orig[i];
+            v = luma_src ? luma_px(luma_src, fmt, i, luma_mode) : orig[i];
         }
         s_in[e] = v;
     }

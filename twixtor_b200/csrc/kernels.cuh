@@ -108,8 +108,8 @@ __global__ void k_compose_blend(WarpParams pa, WarpParams pb, int fmt, float wbl
 
 // ---- fused, shared-memory tiled kernels (fused.cu) -----------------------------------------------------
 constexpr int FUSED_TILE_X = 32, FUSED_TILE_Y = 32, FUSED_THREADS = 256;
-__global__ void k_blur5_band(const float* __restrict__ orig, const void* __restrict__ luma_src, int fmt, int w, int h,
-                             bool above_first, float* __restrict__ tmp_out, float* __restrict__ band_out,
+__global__ void k_blur5_band(const float* __restrict__ orig, const void* __restrict__ luma_src, int fmt, int luma_mode,
+                             int w, int h, bool above_first, float* __restrict__ tmp_out, float* __restrict__ band_out,
                              float* __restrict__ band_t_out);
 __global__ void k_level_init(const float* __restrict__ img, int w, int h, Taps g7, bool above_first,
                              float* __restrict__ gxo, float* __restrict__ gyo, float* __restrict__ a0o,
@@ -127,5 +127,30 @@ __global__ void k_apply_upsample(const float* __restrict__ su, const float* __re
 __global__ void k_apply_negate(const float* __restrict__ fu, const float* __restrict__ fv, long n,
                                const int* __restrict__ any, int start, bool damp_now, float damp,
                                float* __restrict__ out, int* __restrict__ nan_flag);
+
+// ---- warping code 1: Smart Blend and the hole fill (smart.cu) -----------------------------------------
+// mode 0: Nearest (the warp pa only), 1: Blend (pa = A, pb = B, w = frac); binary: the binary alpha
+// composite. Writes the engine image, the u8 holes mask and sets *any_hole when a pixel is a hole.
+__global__ void k_compose_smart(WarpParams pa, WarpParams pb, int fmt, int mode, float w, bool binary,
+                                void* __restrict__ out, uint8_t* __restrict__ holes, int W, int H,
+                                int* __restrict__ any_hole, int* __restrict__ bad);
+__global__ void k_smart_blend(const void* __restrict__ p1, const void* __restrict__ p2, int fmt, float w, bool binary,
+                              void* __restrict__ out, long n);
+__global__ void k_mask_holes(const void* __restrict__ mask, int kind, uint8_t* __restrict__ holes, long n,
+                             int* __restrict__ any_hole);
+__global__ void k_fill_load(const void* __restrict__ img, int fmt, const uint8_t* __restrict__ holes,
+                            float* __restrict__ stack, long n, const int* __restrict__ any_hole);
+// n: 3 (blur5) or 6 (Gaussian r5) taps; dir: 0 horizontal, 1 vertical below first, 2 vertical above
+// first; rule: the NaN rule arithmetic (float images)
+__global__ void k_stack_pass(const float* __restrict__ src, float* __restrict__ dst, int w, int h, long pstride, Taps t,
+                             int n, int dir, int rule, const int* __restrict__ any_hole);
+__global__ void k_stack_resample(const float* __restrict__ src, int sw, int sh, long sstride, float* __restrict__ dst,
+                                 int dw, int dh, long dstride, int rule, const int* __restrict__ any_hole);
+__global__ void k_fill_combine(float* __restrict__ sol, const float* __restrict__ vals, long n, int rule,
+                               const int* __restrict__ any_hole);
+__global__ void k_fill_store(void* __restrict__ img, int fmt, const float* __restrict__ sol, long n,
+                             const int* __restrict__ any_hole);
+__global__ void k_stack_zero(float* __restrict__ p, long n, const int* __restrict__ any_hole);
+__global__ void k_hole_side1(const int* __restrict__ any_hole, int* __restrict__ flag);
 
 }  // namespace tw

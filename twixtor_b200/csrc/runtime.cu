@@ -18,6 +18,7 @@
 
 #include "../../include/twixtor_b200.h"
 #include "kernels.cuh"
+#include "luma.cuh"
 
 using namespace tw;
 
@@ -171,6 +172,7 @@ struct Lane {
     cudaEvent_t ev_done = nullptr;               // the frame's composition done (stream 0)
     bool used = false;
     DevBuf eng[2], pyr[2], work[2], flow[2], scratch[2][3], flags;
+    DevBuf comp, holes, fill;  // warping code 1: the composite, its holes mask, the fill's planes
 };
 constexpr int MAX_LANES = 4;
 
@@ -196,7 +198,7 @@ struct tw_ctx {
     size_t held = 0;
     Taps g7{}, g5{}, b5{};
     // engine images, wire staging, pyramids, solve work, flows
-    DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags;
+    DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags, holes, fill;
     DevBuf host_stage;  // unused placeholder for pinned staging
 
     int fail(int code, const char* fmt, ...) {
@@ -254,7 +256,7 @@ void prof_mark(tw_ctx* ctx) {
 constexpr int TB = 256;
 // device flags (ints): [0..31] per-level range flags of solve 0, [32..63] of solve 1, [64] NaN in a
 // flow, [65] a warp refused a sample coordinate
-constexpr int FL_ANY0 = 0, FL_ANY1 = 32, FL_NAN = 64, FL_BAD = 65;
+constexpr int FL_ANY0 = 0, FL_ANY1 = 32, FL_NAN = 64, FL_BAD = 65, FL_HOLE = 66, FL_SIDE1 = 67;
 constexpr size_t FLAGS_BYTES = 128 * sizeof(int);
 
 dim3 grid2(int w, int h) { return dim3((unsigned)((w + TB - 1) / TB), (unsigned)h); }
@@ -285,8 +287,7 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
         return ctx->fail(TW_ERR_UNSUPPORTED, "image prep (Contrast/Edge Enhance, Delinearize) is not on the device");
     if (s.video_range_luma && s.track_alpha)
         return ctx->fail(TW_ERR_UNSUPPORTED, "optical flow luma: video range conversion together with Track RGB+A is not supported");
-    if (s.video_range_luma || s.track_alpha)
-        return ctx->fail(TW_ERR_UNSUPPORTED, "video range luma and Track RGB+A are not on the device");
+    int lmode = (s.track_alpha ? LUMA_TRACK_ALPHA : 0) | (s.video_range_luma ? LUMA_VIDEO_RANGE : 0);
     size_t full = (size_t)W * H * sizeof(float);
     for (int i = 0; i < 3; i++) CHECK(ctx->ensure(scratch[i], full, "pyramid scratch"));
     float* cur = scratch[0].as<float>();
@@ -296,11 +297,11 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
     int cw = W, ch = H;
     if (g.reduction == 0) {
         long n = (long)W * H;
-        LAUNCH(ctx, k_luma, grid1(n), TB, 0, eng_dev, fmt, cur, W, H, false, false);
+        LAUNCH(ctx, k_luma, grid1(n), TB, 0, eng_dev, fmt, cur, W, H, s.track_alpha != 0, s.video_range_luma != 0);
     }
     for (int r = 0; r < g.reduction; r++) {  // prep.rs:252-259; the first step reads the luma on the fly
         LAUNCHB(ctx, (r == 0 ? 4.0 * sample_bytes(fmt) : 4.0) * cw * ch + 4.0 * cw * ch, k_blur5_band, tiles(cw, ch),
-                FUSED_THREADS, 0, r == 0 ? (const float*)nullptr : cur, r == 0 ? eng_dev : nullptr, fmt, cw, ch, af, tmp,
+                FUSED_THREADS, 0, r == 0 ? (const float*)nullptr : cur, r == 0 ? eng_dev : nullptr, fmt, lmode, cw, ch, af, tmp,
                 (float*)nullptr, (float*)nullptr);
         int nw = cw / 2, nh = ch / 2;
         LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, tmp, cw, ch, nxt, nw, nh);
@@ -312,8 +313,8 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
     size_t pf = pyramid_floats(g);
     for (int i = 0; i < g.levels; i++) {
         int lw = g.sizes[i][0], lh = g.sizes[i][1];
-        LAUNCHB(ctx, 16.0 * lw * lh, k_blur5_band, tiles(lw, lh), FUSED_THREADS, 0, cur, (const void*)nullptr, fmt, lw, lh,
-                af, tmp, out + off, out_t ? out_t + off : (float*)nullptr);
+        LAUNCHB(ctx, 16.0 * lw * lh, k_blur5_band, tiles(lw, lh), FUSED_THREADS, 0, cur, (const void*)nullptr, fmt, 0, lw,
+                lh, af, tmp, out + off, out_t ? out_t + off : (float*)nullptr);
         if (i + 1 < g.levels) {
             int nw = g.sizes[i + 1][0], nh = g.sizes[i + 1][1];
             LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, tmp, lw, lh, cur, nw, nh);
@@ -450,13 +451,116 @@ WarpParams warp_params(const void* src, const float* flow_interleaved, int fw, i
     return p;
 }
 
+// ---- the hole fill (holefill.rs) ------------------------------------------------------------------------
+struct FillGeo {
+    int dims[40][2];
+    int top = 0;
+};
+
+FillGeo fill_geometry(int w, int h) {  // holefill.rs:140-171
+    FillGeo g;
+    long a = w, b = h;
+    int count = 1;
+    for (;;) {
+        a /= 2;
+        b /= 2;
+        if (a < 2) a = 2;
+        if (b < 2) b = 2;
+        count += 1;
+        if (!(a > 1 && b > 1 && (a != 2 || b != 2))) break;
+    }
+    int cw = w, ch = h;
+    for (int k = 0; k <= count && k < 40; k++) {
+        g.dims[k][0] = cw;
+        g.dims[k][1] = ch;
+        cw = std::max(cw / 2, 2);
+        ch = std::max(ch / 2, 2);
+    }
+    g.top = count - 1;
+    return g;
+}
+
+// one blur of a stack of planes: the horizontal pass into tmp, the vertical one back
+void fill_passes(tw_ctx* ctx, float* src_dst, float* tmp, int w, int h, long stride, int planes, const Taps& t, int n,
+                 bool above_first, int rule, const int* any) {
+    dim3 g((unsigned)((w + TB - 1) / TB), (unsigned)h, (unsigned)planes);
+    LAUNCH(ctx, k_stack_pass, g, TB, 0, src_dst, tmp, w, h, stride, t, n, 0, rule, any);
+    LAUNCH(ctx, k_stack_pass, g, TB, 0, tmp, src_dst, w, h, stride, t, n, above_first ? 2 : 1, rule, any);
+}
+
+void fill_resample(tw_ctx* ctx, const float* src, int sw, int sh, float* dst, int dw, int dh, int planes, int rule,
+                   const int* any) {
+    dim3 g((unsigned)((dw + TB - 1) / TB), (unsigned)dh, (unsigned)planes);
+    LAUNCH(ctx, k_stack_resample, g, TB, 0, src, sw, sh, (long)sw * sh, dst, dw, dh, (long)dw * dh, rule, any);
+}
+
+// The pull-push fill of an engine image in place (holefill.rs:260-350, :452-491) with the u8
+// holes mask; every kernel returns at once when *any (no hole) is 0. Per level a stack of five
+// planes: the four channels' values and the weights. Float images run the NaN rule arithmetic
+// (for numbers the plain arithmetic bit for bit, and where a NaN reaches the result the bits of
+// the reference's repeat with the rule).
+int fill_dev(tw_ctx* ctx, void* img, int W, int H, int fmt, const uint8_t* holes, const int* any, bool above_first,
+             DevBuf& fb) {
+    int rule = fmt == TW_F32;
+    FillGeo g = fill_geometry(W, H);
+    long n0 = (long)W * H;
+    size_t offs[40];
+    size_t tot = 0;
+    for (int k = 0; k <= g.top; k++) { offs[k] = tot; tot += 5 * (size_t)g.dims[k][0] * g.dims[k][1]; }
+    size_t o_ta = tot, o_sa = tot + 5 * n0, o_sb = o_sa + 4 * n0;
+    tot = o_sb + 4 * n0;
+    CHECK(ctx->ensure(fb, tot * sizeof(float), "hole fill planes"));
+    float* base = fb.as<float>();
+    float* ta = base + o_ta;
+    LAUNCH(ctx, k_fill_load, grid1(n0), TB, 0, img, fmt, holes, base + offs[0], n0, any);
+    for (int k = 1; k <= g.top; k++) {  // pull: blur5 and the resample of the values and the weights
+        int pw = g.dims[k - 1][0], ph = g.dims[k - 1][1], cw = g.dims[k][0], chh = g.dims[k][1];
+        long pn = (long)pw * ph;
+        // the level k - 1 planes stay for the push: blur a copy
+        CHECK(ctx->cuda(cudaMemcpyAsync(ta, base + offs[k - 1], 5 * pn * sizeof(float), cudaMemcpyDeviceToDevice, ctx->cur),
+                        "fill copy"));
+        fill_passes(ctx, ta, base + o_sa, pw, ph, pn, 5, ctx->b5, 3, above_first, rule, any);
+        fill_resample(ctx, ta, pw, ph, base + offs[k], cw, chh, 5, rule, any);
+    }
+    float* sol = base + o_sa;
+    float* nxt = base + o_sb;
+    {
+        long tn = (long)g.dims[g.top][0] * g.dims[g.top][1];
+        LAUNCH(ctx, k_stack_zero, grid1(4 * tn), TB, 0, sol, 4 * tn, any);
+    }
+    for (int lv = g.top; lv >= 0; lv--) {  // push
+        int lw = g.dims[lv][0], lh = g.dims[lv][1];
+        long ln = (long)lw * lh;
+        LAUNCH(ctx, k_fill_combine, grid1(ln), TB, 0, sol, base + offs[lv], ln, rule, any);
+        fill_passes(ctx, sol, ta, lw, lh, ln, 4, ctx->g5, 6, above_first, rule, any);
+        if (lv == 0) {
+            LAUNCH(ctx, k_fill_combine, grid1(ln), TB, 0, sol, base + offs[0], ln, rule, any);
+        } else {
+            fill_resample(ctx, sol, lw, lh, nxt, g.dims[lv - 1][0], g.dims[lv - 1][1], 4, rule, any);
+            std::swap(sol, nxt);
+        }
+    }
+    LAUNCH(ctx, k_fill_store, grid1(n0), TB, 0, img, fmt, sol, n0, any);
+    return TW_OK;
+}
+
+// Scratch of the warping code 1 composition: the composite (engine image), its holes mask, the
+// fill's planes, and the device flag "some pixel is a hole".
+struct SmartScratch {
+    DevBuf* comp;
+    DevBuf* holes;
+    DevBuf* fill;
+    int* any_hole;  // set by the composition when a pixel is a hole
+    int* side1;     // set when an image with a side of 1 pixel has a hole (the fill refuses it)
+};
+
 // compose_vectors for warping code 0 (compose/vector.rs:209-284) plus the fast path blends
 // (compose.rs:218-231), all as one fused kernel launch. eng_a/eng_b/f_ab/f_ba are device pointers.
 int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& sel, const void* eng_a,
                 const void* eng_b, const float* f_ab, const float* f_ba, int fw, int fh, int W, int H, int fmt,
-                void* out, bool to_wire, bool flip_out, int* bad) {
-    if (cs.warp_mode != 0)
-        return ctx->fail(TW_ERR_UNSUPPORTED, "warping code %d (Smart Blend / forward warp) is not on the device yet", cs.warp_mode);
+                void* out, bool to_wire, bool flip_out, int* bad, const SmartScratch* ss) {
+    if (cs.warp_mode != 0 && cs.warp_mode != 1)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "warping code %d (forward warp) is not on the device yet", cs.warp_mode);
     if (cs.wrap_360) return ctx->fail(TW_ERR_UNSUPPORTED, "the 360 inverse warp is not on the device");
     if (W < 2 || H < 2 || fw < 2 || fh < 2)
         return ctx->fail(TW_ERR_MISMATCH, "inverse warp needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W, H, fw, fh);
@@ -469,6 +573,48 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
     WarpParams pa{}, pb{};
     float wb = 0.0f;
     int mode;
+    if (cs.warp_mode == 1) {  // Smart Blend (smartblend.rs:350-393): warps without hold, coverage, fill
+        if (!ss) return ctx->fail(TW_ERR_UNSUPPORTED, "Smart Blend needs its scratch");
+        int smode;
+        if (sel.interp == 0) {
+            bool use_ab = (wa < 0.5f && 1u < 2) || (0.5f <= wa && 1u > 1);
+            const float* flow = use_ab ? f_ab : f_ba;
+            if (!flow) return ctx->fail(TW_ERR_MISMATCH, "the composition needs the flow %s but it was not computed", use_ab ? "F_AB" : "F_BA");
+            // the A branch unless 0.5 > wa (a NaN weight takes A)
+            if (!(0.5f > wa)) pa = warp_params(eng_a, flow, fw, fh, 1.0f - wa, W, false);
+            else pa = warp_params(eng_b, flow, fw, fh, wa, W, false);
+            pb = pa;
+            smode = 0;
+        } else if (sel.interp == 1) {
+            if (!f_ab || !f_ba) return ctx->fail(TW_ERR_MISMATCH, "the composition needs both flows");
+            pa = warp_params(eng_a, f_ba, fw, fh, frac, W, false);
+            pb = warp_params(eng_b, f_ab, fw, fh, wa, W, false);
+            smode = 1;
+        } else if (sel.interp == 2) {
+            return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend with Smart Blend is not on the device yet");
+        } else {
+            return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
+        }
+        size_t px = (size_t)W * H;
+        void* comp = out;
+        if (to_wire) {
+            CHECK(ctx->ensure(*ss->comp, px * 4 * sample_bytes(fmt), "composite"));
+            comp = ss->comp->p;
+        }
+        CHECK(ctx->ensure(*ss->holes, px, "holes mask"));
+        CHECK(ctx->cuda(cudaMemsetAsync(ss->any_hole, 0, sizeof(int), ctx->cur), "holes flag"));
+        LAUNCH(ctx, k_compose_smart, grid2(W, H), TB, 0, pa, pb, fmt, smode, frac, cs.video_360 != 0, comp,
+               ss->holes->as<uint8_t>(), W, H, ss->any_hole, bad);
+        if (W < 2 || H < 2) LAUNCH(ctx, k_hole_side1, 1, 1, 0, ss->any_hole, ss->side1);
+        else CHECK(fill_dev(ctx, comp, W, H, fmt, ss->holes->as<uint8_t>(), ss->any_hole, cs.taps_above_first != 0, *ss->fill));
+        if (to_wire) {
+            long n = (long)px;
+            if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)comp, (uint8_t*)out, W, H, flip_out);
+            else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)comp, (uint16_t*)out, W, H, flip_out);
+            else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)comp, (float*)out, W, H, flip_out);
+        }
+        return TW_OK;
+    }
     if (sel.interp == 0) {
         bool use_ab = (wa < 0.5f && (unsigned)cs.warp_mode < 2) || (0.5f <= wa && (unsigned)cs.warp_mode > 1);
         const float* flow = use_ab ? f_ab : f_ba;
@@ -576,7 +722,7 @@ int tw_open(int device, tw_ctx** out) {
 void tw_close(tw_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    for (auto* b : {&ctx->flags, &ctx->host_stage})
+    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill})
         b->release(&ctx->held);
     for (int i = 0; i < 3; i++) { ctx->eng[i].release(&ctx->held); ctx->wire[i].release(&ctx->held); }
     for (int i = 0; i < 2; i++) { ctx->pyr[i].release(&ctx->held); ctx->work[i].release(&ctx->held); ctx->flow[i].release(&ctx->held); }
@@ -586,6 +732,7 @@ void tw_close(tw_ctx* ctx) {
             L.eng[i].release(&ctx->held); L.pyr[i].release(&ctx->held); L.work[i].release(&ctx->held);
             L.flow[i].release(&ctx->held);
             for (int j = 0; j < 3; j++) L.scratch[i][j].release(&ctx->held);
+            if (i == 0) { L.comp.release(&ctx->held); L.holes.release(&ctx->held); L.fill.release(&ctx->held); }
             if (L.s[i]) cudaStreamDestroy(L.s[i]);
             if (L.ev_pyr[i]) cudaEventDestroy(L.ev_pyr[i]);
         }
@@ -845,13 +992,17 @@ int tw_compose_vectors(tw_ctx* ctx, const tw_engine_settings* settings, const tw
     CHECK(ctx->ensure(ctx->eng[2], ob, "compose output"));
     int* flags = ctx->flags.as<int>();
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
+    SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1};
     CHECK(compose_dev(ctx, *settings, *sel, ctx->eng[0].p, ctx->eng[1].p, f_ab ? ctx->flow[0].as<float>() : nullptr,
                       f_ba ? ctx->flow[1].as<float>() : nullptr, fw, fh, a->width, a->height, a->fmt, ctx->eng[2].p,
-                      false, false, flags + FL_BAD));
+                      false, false, flags + FL_BAD, &ss));
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
-    int hf[2];
-    CHECK(finish(ctx, hf, 2));
+    int hf[4];
+    CHECK(finish(ctx, hf, 4));
     if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    if (hf[3])
+        return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of a %dx%d image: the pyramid resample divides by zero for a side of 1",
+                         a->width, a->height);
     return TW_OK;
 }
 
@@ -937,6 +1088,59 @@ int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* 
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     int hf[1];
     return finish(ctx, hf, 1);
+}
+
+int tw_smart_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* p1, const tw_image* p2, float w, int32_t binary) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    CHECK(check_image(ctx, p1, "smart blend"));
+    CHECK(check_image(ctx, p2, "smart blend"));
+    if (!out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    if (!same_shape(p1, p2) || out->width != p1->width || out->height != p1->height || out->fmt != p1->fmt)
+        return ctx->fail(TW_ERR_MISMATCH, "smart blend: images of %dx%d and %dx%d", p1->width, p1->height, p2->width,
+                         p2->height);
+    long n = (long)p1->width * p1->height;
+    CHECK(upload_image(ctx, ctx->eng[0], p1));
+    CHECK(upload_image(ctx, ctx->eng[1], p2));
+    size_t ob = (size_t)n * 4 * sample_bytes(p1->fmt);
+    CHECK(ctx->ensure(ctx->eng[2], ob, "smart blend output"));
+    LAUNCH(ctx, k_smart_blend, grid1(n), TB, 0, ctx->eng[0].p, ctx->eng[1].p, p1->fmt, w, binary != 0, ctx->eng[2].p, n);
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[1];
+    return finish(ctx, hf, 1);
+}
+
+int tw_fill_holes(tw_ctx* ctx, tw_image_mut* img, const void* mask, int32_t mask_kind, int32_t taps_above_first) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!img || !img->data || !mask) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    if (img->fmt < 0 || img->fmt > 2 || img->width <= 0 || img->height <= 0)
+        return ctx->fail(TW_ERR_BAD_PARAM, "hole fill: bad image");
+    if (mask_kind < 1 || mask_kind > 3)
+        return ctx->fail(TW_ERR_BAD_PARAM, "hole fill: mask kind %d is not 1 (u8), 2 (u16) or 3 (f32)", mask_kind);
+    int W = img->width, H = img->height;
+    long n = (long)W * H;
+    size_t ib = (size_t)n * 4 * sample_bytes(img->fmt);
+    size_t mb = (size_t)n * (mask_kind == 1 ? 1 : mask_kind == 2 ? 2 : 4);
+    CHECK(ctx->ensure(ctx->eng[0], ib, "hole fill image"));
+    CHECK(ctx->ensure(ctx->eng[1], mb, "hole fill mask"));
+    CHECK(ctx->ensure(ctx->holes, (size_t)n, "holes mask"));
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->eng[0].p, img->data, ib, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->eng[1].p, mask, mb, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    LAUNCH(ctx, k_mask_holes, grid1(n), TB, 0, ctx->eng[1].p, mask_kind, ctx->holes.as<uint8_t>(), n, flags + FL_HOLE);
+    if (W < 2 || H < 2) LAUNCH(ctx, k_hole_side1, 1, 1, 0, flags + FL_HOLE, flags + FL_SIDE1);
+    else CHECK(fill_dev(ctx, ctx->eng[0].p, W, H, img->fmt, ctx->holes.as<uint8_t>(), flags + FL_HOLE, taps_above_first != 0, ctx->fill));
+    CHECK(ctx->cuda(cudaMemcpyAsync(img->data, ctx->eng[0].p, ib, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[4];
+    CHECK(finish(ctx, hf, 4));
+    if (hf[3])
+        return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of a %dx%d image: the pyramid resample divides by zero for a side of 1",
+                         W, H);
+    return TW_OK;
 }
 
 int tw_from_frame(tw_ctx* ctx, const void* wire, int32_t width, int32_t height, int32_t fmt, void* engine_out) {
@@ -1068,9 +1272,10 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
     CHECK(ctx->cuda(cudaEventRecord(L.ev_solve1, L.s[1]), "event"));
     CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_solve1, 0), "event"));
     ctx->cur = L.s[0];
+    SmartScratch ss{&L.comp, &L.holes, &L.fill, flags + FL_HOLE, flags + FL_SIDE1};
     CHECK(compose_dev(ctx, s.compose, sel, L.eng[0].p, L.eng[1].p, need_ab ? L.flow[0].as<float>() : nullptr,
                       need_ba ? L.flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, out_wire, true, flip,
-                      flags + FL_BAD));
+                      flags + FL_BAD, &ss));
     CHECK(ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event"));
     return TW_OK;
 }
@@ -1098,20 +1303,20 @@ static int lanes_end(tw_ctx* ctx, int nl) {
         CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, L.ev_done, 0), "event"));
     }
     ctx->cur = ctx->stream;
-    int hf[2] = {0, 0};
+    int hf[4] = {0, 0, 0, 0};
     for (int i = 0; i < nl; i++) {
         Lane& L = ctx->lanes[i];
         if (!L.used) continue;
-        int f[2];
+        int f[4];
         CHECK(ctx->cuda(cudaMemcpyAsync(f, (int*)L.flags.p + FL_NAN, sizeof f, cudaMemcpyDeviceToHost, ctx->stream), "flags"));
         CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution"));
-        hf[0] |= f[0];
-        hf[1] |= f[1];
+        for (int k = 0; k < 4; k++) hf[k] |= f[k];
         L.used = false;
     }
     CHECK(ctx->cuda(cudaGetLastError(), "kernel execution"));
     if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
     if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    if (hf[3]) return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of an image with a side of 1 pixel that has a hole");
     return TW_OK;
 }
 
