@@ -15,6 +15,7 @@
 
 #include "oracle_core.h"
 #include "oracle_smart.h"
+#include "oracle_forward.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -334,6 +335,54 @@ int or_fill_holes(void* eng, int w, int h, int fmt, const void* mask, int mask_k
     if (rc) return fail(rc, e);
     std::memcpy(eng, img.data(), img.bytes());
     return 0;
+}
+
+// forward.rs:229-320 (pyramid != 0: textured) / :327-373 (Gouraud); cov may be null
+int or_forward_warp(void* out_eng, const void* src_eng, int w, int h, int fmt, const float* flow, int fw, int fh,
+                    float amount, int pyramid, uint8_t* cov) {
+    Image src(w, h, (Fmt)fmt), out(w, h, (Fmt)fmt);
+    std::memcpy(src.data(), src_eng, src.bytes());
+    FlowField f(fw, fh);
+    std::memcpy(f.d.data(), flow, f.d.size() * 4);
+    Coverage c;
+    std::string e;
+    int rc = forward_warp(out, src, f, amount, pyramid != 0, cov ? &c : nullptr, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(out_eng, out.data(), out.bytes());
+    if (cov) std::memcpy(cov, c.d.data(), c.d.size());
+    return 0;
+}
+
+// forward/mesh.rs:63-91 and forward/pyramid.rs:20-36
+float or_fw_mip_level(int w, int h, const float* flow, int fw, int fh, float amount, int c, int r) {
+    FlowField f(fw, fh);
+    std::memcpy(f.d.data(), flow, f.d.size() * 4);
+    return fw_mip_level(w, h, f, amount, c, r);
+}
+int or_fw_level_count(int w, int h) { return fw_level_count(w, h); }
+
+// forward/raster.rs:158-300 on one triangle (5 floats x, y, u, v, d per vertex); writes up to cap
+// hits (x, y, u, v, d as floats) and returns their count, or -1 when the degenerate pass would
+// write outside the image
+int or_fw_triangle(const float* v, int w1, int h1, float* hits, int cap) {
+    FwVtx t[3];
+    for (int i = 0; i < 3; i++) t[i] = FwVtx{v[i * 5], v[i * 5 + 1], v[i * 5 + 2], v[i * 5 + 3], v[i * 5 + 4]};
+    FwHits s;
+    fw_triangle(t, w1, h1, &s);
+    int n = 0;
+    for (const FwHit& hh : s.hits) {
+        if (n < cap) {
+            float* o = hits + (size_t)n * 5;
+            o[0] = (float)hh.x; o[1] = (float)hh.y; o[2] = hh.u; o[3] = hh.v; o[4] = hh.d;
+        }
+        n++;
+    }
+    return s.outside ? -1 : n;
+}
+
+// glibc's logf over an array (the mip level's libm call), for the device's logf check
+void or_logf(const float* x, float* out, long n) {
+    for (long i = 0; i < n; i++) out[i] = logf(x[i]);
 }
 
 // compose::compose_vectors with a warping code (0 inverse, 1 Smart Blend) and the binary alpha flag

@@ -967,6 +967,13 @@ int inv_warp(Image& out, const Image& src, const FlowField& flow, float amount, 
 // =============================================================================================
 // blend (blend.rs)
 
+void bilerp4_image(const Image& img, float x, float y, float out[4]) {
+    int w1 = img.w - 1, h1 = img.h - 1;
+    if (img.fmt == U8) bilerp4(img.u8.data(), img.w, w1, h1, x, y, out);
+    else if (img.fmt == U16) bilerp4(img.u16.data(), img.w, w1, h1, x, y, out);
+    else bilerp4(img.f32.data(), img.w, w1, h1, x, y, out);
+}
+
 void copy_image(Image& out, const Image& src) {  // blend.rs:117-125
     std::memcpy(out.data(), src.data(), src.bytes());
 }

@@ -17,6 +17,8 @@ Writes, next to this script:
 * ``f1_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/f1_cases.hex``
   (the reference's bit-exact numpy models of Smart Blend and the hole fill; format in its
   ``f1_gen.py``).
+* ``f2_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/f2_cases.hex``
+  (the reference's numpy model of the textured forward warp; format in its ``f2_gen.py``).
 * ``warp_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/warp_cases.hex``
   (the reference's bit-exact numpy model of the inverse warp; format in its ``gen_warp.py``).
 
@@ -100,6 +102,12 @@ def main():
     with gzip.open(os.path.join(HERE, "f1_cases.bin.gz"), "wb") as f:
         f.write(blob)
     print(f"f1_cases.bin.gz: {len(blob)} bytes, sha256 {hashlib.sha256(blob).hexdigest()}")
+
+    txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "f2_cases.hex")).read()
+    blob = bytes.fromhex("".join(txt.split()))
+    with gzip.open(os.path.join(HERE, "f2_cases.bin.gz"), "wb") as f:
+        f.write(blob)
+    print(f"f2_cases.bin.gz: {len(blob)} bytes, sha256 {hashlib.sha256(blob).hexdigest()}")
 
     txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "warp_cases.hex")).read()
     blob = bytes.fromhex("".join(txt.split()))

@@ -39,6 +39,32 @@ def case_params(case):
                 video_360=params.get("video_360", "0") == "1", rows_reversed=False, taps_above_first=False)
 
 
+def f2_cases():
+    """The reference's numpy model of the textured forward warp (f2_cases.hex; format in its f2_gen.py)."""
+    blob = gzip.open(os.path.join(GOLDEN, "f2_cases.bin.gz")).read()
+    assert blob[:4] == b"F2C1"
+    n = struct.unpack_from("<I", blob, 4)[0]
+    p = 8
+    out = []
+    for _ in range(n):
+        fmt, w, h, fw, fh = struct.unpack_from("<5I", blob, p)
+        amount = np.float32(struct.unpack_from("<f", blob, p + 20)[0])
+        p += 28
+        dt = {0: np.uint8, 1: np.uint16, 2: np.float32}[fmt]
+        cnt = w * h * 4 * np.dtype(dt).itemsize
+        src = np.frombuffer(blob[p:p + cnt], dt).copy()
+        p += cnt
+        flow = np.frombuffer(blob[p:p + fw * fh * 8], np.float32).copy()
+        p += fw * fh * 8
+        want = np.frombuffer(blob[p:p + cnt], dt).copy()
+        p += cnt
+        cov = np.frombuffer(blob[p:p + w * h], np.uint8).copy()
+        p += w * h
+        out.append(dict(fmt=fmt, w=w, h=h, fw=fw, fh=fh, amount=amount, src=src, flow=flow, out=want, cov=cov))
+    assert p == len(blob)
+    return out
+
+
 def f1_cases():
     """The reference's Smart Blend and hole fill model fixtures (f1_cases.hex; format in its f1_gen.py)."""
     blob = gzip.open(os.path.join(GOLDEN, "f1_cases.bin.gz")).read()

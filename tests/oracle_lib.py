@@ -83,6 +83,12 @@ def lib():
         L.or_smart_blend.argtypes = [P, P, P, i, i, i, f, i]
         L.or_fill_holes.argtypes = [P, i, i, i, P, i, i]
         L.or_compose_vectors2.argtypes = [P, P, i, i, i, P, P, i, i, f, i, i, i, i, P]
+        L.or_forward_warp.argtypes = [P, P, i, i, i, P, i, i, f, i, P]
+        L.or_fw_mip_level.argtypes = [i, i, P, i, i, f, i, i]
+        L.or_fw_mip_level.restype = f
+        L.or_fw_level_count.argtypes = [i, i]
+        L.or_fw_triangle.argtypes = [P, i, i, P, i]
+        L.or_logf.argtypes = [P, P, ctypes.c_long]
         _lib = L
     return _lib
 
@@ -177,6 +183,25 @@ def fill_holes(img, w, h, fmt, mask, mask_kind, above_first=True):
     if rc:
         raise ValueError(err())
     return out
+
+
+def forward_warp(src, w, h, fmt, flow, fw, fh, amount, pyramid=True, coverage=False):
+    """forward.rs forward_warp_with: (out, cov) with coverage, else out."""
+    out = np.zeros_like(src)
+    cov = np.zeros(w * h, np.uint8) if coverage else None
+    rc = lib().or_forward_warp(ptr(out), ptr(src), w, h, fmt, ptr(np.ascontiguousarray(flow, np.float32)), fw, fh,
+                               np.float32(amount), int(pyramid), ptr(cov))
+    if rc:
+        raise ValueError(err())
+    return (out, cov) if coverage else out
+
+
+def fw_triangle(verts, w1, h1, cap=4096):
+    """forward/raster.rs triangle: the hits (x, y, u, v, d) in order, or None for an outside write."""
+    v = np.asarray(verts, np.float32).reshape(-1)
+    hits = np.zeros(cap * 5, np.float32)
+    n = lib().or_fw_triangle(ptr(v), w1, h1, ptr(hits), cap)
+    return None if n < 0 else hits[:n * 5].reshape(n, 5)
 
 
 def retime_params(fps=(24, 1), quality_high=True, speed=100.0, keys=None, vectors=5, frame_interp=2, smart_blend=0,
