@@ -208,6 +208,20 @@ int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* 
  * blended at w, or (binary != 0) the binary alpha composite. */
 int tw_smart_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* p1, const tw_image* p2, float w, int32_t binary);
 
+/* forward::forward_warp_with (forward.rs:229-320) with the coverage image when cov != NULL (w*h
+ * bytes, 255 where a triangle covered the pixel): the displaced triangle mesh of the flow
+ * rasterised into a running mean, textured from the source's mip pyramid (pyramid != 0, the
+ * compositor's default) or with the vertex colours interpolated (pyramid == 0, the Gouraud variant
+ * `stages::GouraudForward` selects). The flow may have any size of at least 2x2. Replaces
+ * Stages::forward_warp_with (stages.rs:33-71). TW_ERR_UNSUPPORTED where the reference refuses (the
+ * degenerate last-row pass would write outside the image). */
+int tw_forward_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_flow* flow, float amount,
+                    int32_t pyramid, uint8_t* cov);
+
+/* Self check of the device's logf of the forward warp's mip level (forward/mesh.rs:89-90), which
+ * must equal the host C library's logf bit for bit: out[i] = logf(x[i]) computed on the device. */
+int tw_check_logf(tw_ctx* ctx, const float* x, float* out, int64_t n);
+
 /* holefill::fill_holes_masked_with (holefill.rs:452-491) with is360 off: the pull-push fill of
  * `img` in place. `mask` holds width*height values of kind 1 (u8), 2 (u16) or 3 (f32); a pixel is
  * a hole when !(eps > m) (holefill.rs:124-133). taps_above_first: the vertical border tap order

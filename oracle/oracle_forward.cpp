@@ -165,9 +165,22 @@ struct FwPyramid {  // pyramid.rs:39-70
     }
 };
 
+// A texture coordinate whose cell leaves the level: the reference indexes outside its slice there
+// (a panic); here it is recorded and reads zeros, and the warp reports an error.
+static bool g_tap_bad = false;
+
 static void tap(const Image& img, float u, float v, float out[4]) {  // pyramid.rs:98-108
     int w1 = img.w - 1, h1 = img.h - 1;
-    bilerp4_image(img, (float)w1 * u, (float)h1 * v, out);
+    float x = (float)w1 * u, y = (float)h1 * v;
+    int ix = cvtt32(x), iy = cvtt32(y);
+    if (ix >= w1) ix = w1 - 1;
+    if (iy >= h1) iy = h1 - 1;
+    if (ix < 0 || iy < 0) {
+        g_tap_bad = true;
+        for (int k = 0; k < 4; k++) out[k] = 0.0f;
+        return;
+    }
+    bilerp4_image(img, x, y, out);
 }
 
 static void sample(const FwPyramid& p, const Image& src, float u, float v, float d, float out[4]) {  // :72-95
@@ -492,6 +505,7 @@ int forward_warp(Image& out, const Image& src, const FlowField& flow, float amou
     }
     std::vector<float> pos;
     fw_positions(w, h, flow, amount, &pos);
+    g_tap_bad = false;
     std::vector<float> acc((size_t)w * h * 4, 0.0f);
     std::vector<uint8_t> cnt((size_t)w * h, 0);
     int w1 = w - 1, h1 = h - 1;
@@ -572,6 +586,10 @@ int forward_warp(Image& out, const Image& src, const FlowField& flow, float amou
     }
     if (outside) {
         *err = "forward warp: the degenerate last row pass of the rasteriser would write outside the image";
+        return 2;
+    }
+    if (g_tap_bad) {
+        *err = "forward warp: a texture coordinate outside the image";
         return 2;
     }
     convert(out, acc);

@@ -244,6 +244,8 @@ def library():
     L.tw_block_match.argtypes = [P, P, P, P, i32, i32]
     L.tw_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float]
     L.tw_smart_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float, i32]
+    L.tw_forward_warp.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, P]
+    L.tw_check_logf.argtypes = [P, P, P, ctypes.c_int64]
     L.tw_fill_holes.argtypes = [P, pimg, P, i32, i32]
     L.tw_from_frame.argtypes = [P, P, i32, i32, i32, P]
     L.tw_to_frame.argtypes = [P, P, i32, i32, i32, P]
@@ -434,6 +436,27 @@ class Device:
         bi, ba = _img(b, width, height, fmt)
         oi = _Image(width, height, fmt, out.ctypes.data)
         self._check(self._L.tw_blend(self._h, ctypes.byref(oi), ctypes.byref(ai), ctypes.byref(bi), np.float32(w)))
+        return out
+
+    def forward_warp(self, src, width, height, fmt, flow, flow_size, amount, pyramid=True, coverage=False):
+        """``forward::forward_warp_with``: the engine image (and the coverage bytes with coverage=True).
+        pyramid=False is the Gouraud variant."""
+        fw, fh = flow_size
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        si, sa = _img(src, width, height, fmt)
+        oi = _Image(width, height, fmt, out.ctypes.data)
+        flow = np.ascontiguousarray(flow, np.float32)
+        fl = _Flow(fw, fh, flow.ctypes.data)
+        cov = np.zeros(width * height, np.uint8) if coverage else None
+        self._check(self._L.tw_forward_warp(self._h, ctypes.byref(oi), ctypes.byref(si), ctypes.byref(fl), np.float32(amount),
+                                            int(pyramid), _ptr(cov)))
+        return (out, cov) if coverage else out
+
+    def check_logf(self, x):
+        """The device's logf of the forward warp's mip level (equal to the host C library's)."""
+        x = np.ascontiguousarray(x, np.float32)
+        out = np.zeros_like(x)
+        self._check(self._L.tw_check_logf(self._h, _ptr(x), _ptr(out), x.size))
         return out
 
     def smart_blend(self, p1, p2, width, height, fmt, w, binary=False):

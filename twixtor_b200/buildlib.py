@@ -2,6 +2,11 @@
 
 Strict mode flags: no FMA contraction (-fmad=false), IEEE division and square root, denormals
 kept (-ftz=false). The library is plain C ABI + CUDA runtime; it links no PyTorch.
+
+One generated input: the table of inputs where glibc's logf differs from the library's own
+double precision log (csrc/twlog.h), made by running csrc/gen_logf_table.c (it calls this
+machine's glibc logf on every positive finite float, a few seconds on all cores) into
+_build/logf_table.bin and embedded through csrc/logf_table.S.
 """
 import os
 import subprocess
@@ -10,7 +15,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtwixtor_b200.so")
-SOURCES = ["solver.cu", "fused.cu", "image.cu", "smart.cu", "runtime.cu", "noalloc.cu"]
+SOURCES = ["solver.cu", "fused.cu", "image.cu", "smart.cu", "forward.cu", "runtime.cu", "noalloc.cu"]
+BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FLAGS = [
@@ -31,10 +37,33 @@ def stale():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def logf_table_object(verbose=False):
+    """_build/logf_table.o: the glibc logf exception table, regenerated when its generator changes."""
+    os.makedirs(BUILD, exist_ok=True)
+    gen_src = os.path.join(CSRC, "gen_logf_table.c")
+    deps = [gen_src, os.path.join(CSRC, "twlog.h")]
+    table = os.path.join(BUILD, "logf_table.bin")
+    obj = os.path.join(BUILD, "logf_table.o")
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    if not os.path.exists(table) or any(os.path.getmtime(d) > os.path.getmtime(table) for d in deps):
+        gen = os.path.join(BUILD, "gen_logf_table")
+        subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fopenmp", "-I", CSRC, "-o", gen, gen_src, "-lm"],
+                       check=True, env=env)
+        r = subprocess.run([gen, table], check=True, capture_output=True, text=True)
+        if verbose:
+            print("logf table:", r.stdout.strip(), "entries")
+    asm = os.path.join(CSRC, "logf_table.S")
+    if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(table), os.path.getmtime(asm)):
+        subprocess.run(["gcc", "-c", "-fPIC", "-Wa,-I," + BUILD, "-o", obj, asm], check=True, env=env)
+    return obj
+
+
 def build(force=False, verbose=False):
     if not force and not stale():
         return LIB
-    cmd = [NVCC] + FLAGS + ["-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES]
+    obj = logf_table_object(verbose)
+    cmd = [NVCC] + FLAGS + ["-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES] + [obj]
     if verbose:
         print(" ".join(cmd))
     env = dict(os.environ)

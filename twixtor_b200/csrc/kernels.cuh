@@ -153,4 +153,50 @@ __global__ void k_fill_store(void* __restrict__ img, int fmt, const float* __res
 __global__ void k_stack_zero(float* __restrict__ p, long n, const int* __restrict__ any_hole);
 __global__ void k_hole_side1(const int* __restrict__ any_hole, int* __restrict__ flag);
 
+// ---- the forward warp (forward.cu) ---------------------------------------------------------------------
+struct FwGrid {  // forward/mesh.rs:11-26
+    int w, h;
+    float rx, ry, sx, sy;
+};
+constexpr int FW_MAX_LEVELS = 16;
+struct FwLevels {  // level 0 is the source
+    const void* p[FW_MAX_LEVELS];
+    int w[FW_MAX_LEVELS], h[FW_MAX_LEVELS];
+    int count;
+};
+struct FwRaster {
+    int w, h, fmt;
+    bool pyramid;                     // textured (true) or Gouraud
+    const float *vx, *vy, *vd;        // vertex positions, mip levels (null: all 0)
+    FwLevels levels;
+    uint32_t *cnt, *off, *fill;       // per pixel: hit count, segment start, hits written
+    uint32_t* keys;                   // per hit: triangle index
+    float4* cols;                     // per hit: colour
+    void* out;
+    uint8_t* cov;                     // may be null
+    int *outside, *bad;
+    uint32_t *nlong, *longq;          // the queue of pixels with long hit lists
+    uint2* scratch;                   // 2 * total pairs for lists above the shared memory sort
+    uint32_t total;
+};
+__global__ void k_logf_glibc(const float* __restrict__ x, float* __restrict__ out, long n, const uint2* __restrict__ tab,
+                             int ntab);
+__global__ void k_fw_flow_nonzero(const float* __restrict__ flow, long n, int* __restrict__ flag);
+__global__ void k_fw_vertices(const float* __restrict__ flow, int fw, int fh, FwGrid g, float* __restrict__ vx,
+                              float* __restrict__ vy, float* __restrict__ vd, float inv_ln2,
+                              const uint2* __restrict__ tab, int ntab);
+__global__ void k_fwp_blur(const void* __restrict__ in, void* __restrict__ out, int w, int h, int vertical, int fmt);
+__global__ void k_fwp_resample(const void* __restrict__ src, int sw, int sh, void* __restrict__ dst, int dw, int dh,
+                               int fmt);
+__global__ void k_fw_count(FwRaster R);
+__global__ void k_fw_emit(FwRaster R);
+constexpr int FW_SCAN_BLOCK = 2048;
+__global__ void k_scan_block(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long n,
+                             uint32_t* __restrict__ sums, uint32_t* __restrict__ maxc);
+__global__ void k_scan_sums(uint32_t* __restrict__ sums, int nb, unsigned long long* __restrict__ total);
+__global__ void k_scan_add(uint32_t* __restrict__ out, long n, const uint32_t* __restrict__ sums);
+__global__ void k_fw_resolve(FwRaster R);
+constexpr int FW_LONG_SMEM_BYTES = 4096 * 8;
+__global__ void k_fw_resolve_long(FwRaster R);
+
 }  // namespace tw

@@ -200,6 +200,9 @@ struct tw_ctx {
     // engine images, wire staging, pyramids, solve work, flows
     DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags, holes, fill;
     DevBuf host_stage;  // unused placeholder for pinned staging
+    // the forward warp: vertices, mip pyramid, per pixel counts / offsets, hit lists, flags
+    DevBuf logf_tab, fw_vx, fw_vy, fw_vd, fw_pyr, fw_tmp[2], fw_cnt, fw_off, fw_fill, fw_sums, fw_keys, fw_cols,
+        fw_scratch, fw_longq, fw_flags, fw_out, fw_cov;
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];
@@ -722,7 +725,10 @@ int tw_open(int device, tw_ctx** out) {
 void tw_close(tw_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill})
+    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
+                    &ctx->fw_vd, &ctx->fw_pyr, &ctx->fw_tmp[0], &ctx->fw_tmp[1], &ctx->fw_cnt, &ctx->fw_off,
+                    &ctx->fw_fill, &ctx->fw_sums, &ctx->fw_keys, &ctx->fw_cols, &ctx->fw_scratch, &ctx->fw_longq,
+                    &ctx->fw_flags, &ctx->fw_out, &ctx->fw_cov})
         b->release(&ctx->held);
     for (int i = 0; i < 3; i++) { ctx->eng[i].release(&ctx->held); ctx->wire[i].release(&ctx->held); }
     for (int i = 0; i < 2; i++) { ctx->pyr[i].release(&ctx->held); ctx->work[i].release(&ctx->held); ctx->flow[i].release(&ctx->held); }
@@ -1141,6 +1147,215 @@ int tw_fill_holes(tw_ctx* ctx, tw_image_mut* img, const void* mask, int32_t mask
         return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of a %dx%d image: the pyramid resample divides by zero for a side of 1",
                          W, H);
     return TW_OK;
+}
+
+// ---- the forward warp (forward.rs:229-373) -----------------------------------------------------------
+
+// The glibc logf exception table embedded by the build (csrc/logf_table.S), uploaded once.
+extern "C" const uint32_t tw_logf_table[];
+extern "C" const uint32_t tw_logf_table_end[];
+
+static int logf_table(tw_ctx* ctx, const uint2** tab, int* n) {
+    size_t bytes = (size_t)((const char*)tw_logf_table_end - (const char*)tw_logf_table);
+    *n = (int)(bytes / sizeof(uint2));
+    if (!ctx->logf_tab.p) {
+        CHECK(ctx->ensure(ctx->logf_tab, bytes, "logf table"));
+        CHECK(ctx->cuda(cudaMemcpy(ctx->logf_tab.p, tw_logf_table, bytes, cudaMemcpyHostToDevice), "logf table upload"));
+    }
+    *tab = ctx->logf_tab.as<uint2>();
+    return TW_OK;
+}
+
+static int fw_level_count(int w, int h) {  // forward/pyramid.rs:20-36
+    int n = 1, a = std::max(w, 2), b = std::max(h, 2);
+    for (;;) {
+        a /= 2;
+        if (a < 2) break;
+        b /= 2;
+        if (b < 2) break;
+        n++;
+    }
+    return n;
+}
+
+// fw_flags ints: [0] outside, [1] bad texture coordinate, [2] flow not zero, [3] long lists,
+// [4] longest list, [6..7] the total number of hits (64 bit)
+enum { FW_OUTSIDE = 0, FW_BAD = 1, FW_NONZERO = 2, FW_NLONG = 3, FW_MAXC = 4, FW_TOTAL = 6 };
+
+int tw_forward_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_flow* flow, float amount,
+                    int32_t pyramid, uint8_t* cov) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    CHECK(check_image(ctx, src, "forward warp"));
+    if (!out || !out->data || !flow || !flow->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    if (out->width != src->width || out->height != src->height || out->fmt != src->fmt)
+        return ctx->fail(TW_ERR_MISMATCH, "forward warp: destination %dx%d fmt %d against source %dx%d fmt %d", out->width,
+                         out->height, out->fmt, src->width, src->height, src->fmt);
+    int W = src->width, H = src->height, fmt = src->fmt;
+    if (W < 2 || H < 2 || flow->width < 2 || flow->height < 2)
+        return ctx->fail(TW_ERR_MISMATCH, "forward warp needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W, H,
+                         flow->width, flow->height);
+    long n = (long)W * H;
+    size_t px = 4 * sample_bytes(fmt);
+    CHECK(upload_image(ctx, ctx->eng[0], src));
+    CHECK(ctx->ensure(ctx->fw_flags, 64, "forward warp flags"));
+    CHECK(ctx->ensure(ctx->fw_cov, (size_t)n, "coverage"));
+    int* ff = ctx->fw_flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(ff, 0, 64, ctx->stream), "flags"));
+    // early outs (forward.rs:252-257): |amount| below 1e-5 as a double, or a flow of zeros
+    float a = 0.0f > amount ? -amount : amount;
+    bool early = 1e-05 > (double)a;
+    long nf = (long)flow->width * flow->height * 2;
+    if (!early) {
+        CHECK(ctx->ensure(ctx->flow[0], nf * sizeof(float), "flow"));
+        CHECK(ctx->cuda(cudaMemcpyAsync(ctx->flow[0].p, flow->data, nf * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
+                        "flow upload"));
+        LAUNCH(ctx, k_fw_flow_nonzero, grid1(nf), TB, 0, ctx->flow[0].as<float>(), nf, ff + FW_NONZERO);
+        int nz = 0;
+        CHECK(ctx->cuda(cudaMemcpyAsync(&nz, ff + FW_NONZERO, sizeof nz, cudaMemcpyDeviceToHost, ctx->stream), "flags"));
+        CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution"));
+        early = nz == 0;
+    }
+    if (early) {  // blend::copy and a full coverage
+        CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[0].p, (size_t)n * px, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+        if (cov) std::memset(cov, 0xff, (size_t)n);
+        return ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution");
+    }
+    // 1. the vertex grid and the mip levels (forward/mesh.rs)
+    FwGrid g;
+    g.w = W;
+    g.h = H;
+    g.rx = (float)(flow->width - 1) / (float)(W - 1);
+    g.ry = (float)(flow->height - 1) / (float)(H - 1);
+    g.sx = amount / g.rx;
+    g.sy = amount / g.ry;
+    int levels = fw_level_count(W, H);
+    bool mips = pyramid && levels > 1;
+    if (levels > FW_MAX_LEVELS) return ctx->fail(TW_ERR_TOO_LARGE, "forward warp: %d pyramid levels", levels);
+    CHECK(ctx->ensure(ctx->fw_vx, n * sizeof(float), "vertices"));
+    CHECK(ctx->ensure(ctx->fw_vy, n * sizeof(float), "vertices"));
+    if (mips) CHECK(ctx->ensure(ctx->fw_vd, n * sizeof(float), "mip levels"));
+    const uint2* tab = nullptr;
+    int ntab = 0;
+    if (mips) CHECK(logf_table(ctx, &tab, &ntab));
+    float inv_ln2 = 1.0f / logf(2.0f);  // mesh.rs:89, the host libm like the reference's
+    LAUNCH(ctx, k_fw_vertices, grid1(n), TB, 0, ctx->flow[0].as<float>(), flow->width, flow->height, g,
+           ctx->fw_vx.as<float>(), ctx->fw_vy.as<float>(), mips ? ctx->fw_vd.as<float>() : (float*)nullptr, inv_ln2, tab,
+           ntab);
+    // 2. the mip pyramid (forward/pyramid.rs:39-70); level 0 is the source
+    FwLevels L{};
+    L.p[0] = ctx->eng[0].p;
+    L.w[0] = W;
+    L.h[0] = H;
+    L.count = pyramid ? levels : 1;
+    if (pyramid && levels > 1) {
+        size_t tot = 0;
+        int cw = W, chh = H;
+        size_t offs[FW_MAX_LEVELS];
+        for (int i = 1; i < levels; i++) {
+            cw = std::max(cw / 2, 2);
+            chh = std::max(chh / 2, 2);
+            offs[i] = tot;
+            tot += (size_t)cw * chh * px;
+            L.w[i] = cw;
+            L.h[i] = chh;
+        }
+        CHECK(ctx->ensure(ctx->fw_pyr, tot, "mip pyramid"));
+        CHECK(ctx->ensure(ctx->fw_tmp[0], (size_t)n * px, "mip blur"));
+        CHECK(ctx->ensure(ctx->fw_tmp[1], (size_t)n * px, "mip blur"));
+        for (int i = 1; i < levels; i++) {
+            L.p[i] = (char*)ctx->fw_pyr.p + offs[i];
+            int pw = L.w[i - 1], ph = L.h[i - 1];
+            dim3 gb((unsigned)((pw + 127) / 128), (unsigned)ph);
+            LAUNCH(ctx, k_fwp_blur, gb, 128, 0, L.p[i - 1], ctx->fw_tmp[0].p, pw, ph, 0, fmt);
+            LAUNCH(ctx, k_fwp_blur, gb, 128, 0, ctx->fw_tmp[0].p, ctx->fw_tmp[1].p, pw, ph, 1, fmt);
+            dim3 gr((unsigned)((L.w[i] + 127) / 128), (unsigned)L.h[i]);
+            LAUNCH(ctx, k_fwp_resample, gr, 128, 0, ctx->fw_tmp[1].p, pw, ph, (void*)L.p[i], L.w[i], L.h[i], fmt);
+        }
+    }
+    // 3. count the hits of every pixel, then their offsets
+    CHECK(ctx->ensure(ctx->fw_cnt, n * sizeof(uint32_t), "hit counts"));
+    CHECK(ctx->ensure(ctx->fw_off, n * sizeof(uint32_t), "hit offsets"));
+    CHECK(ctx->ensure(ctx->fw_fill, n * sizeof(uint32_t), "hit fill"));
+    int nb = (int)((n + FW_SCAN_BLOCK - 1) / FW_SCAN_BLOCK);
+    CHECK(ctx->ensure(ctx->fw_sums, (size_t)nb * sizeof(uint32_t), "scan sums"));
+    CHECK(ctx->ensure(ctx->fw_longq, n * sizeof(uint32_t), "long lists"));
+    CHECK(ctx->ensure(ctx->fw_out, (size_t)n * px, "forward warp output"));
+    CHECK(ctx->cuda(cudaMemsetAsync(ctx->fw_cnt.p, 0, n * sizeof(uint32_t), ctx->stream), "counts"));
+    CHECK(ctx->cuda(cudaMemsetAsync(ctx->fw_fill.p, 0, n * sizeof(uint32_t), ctx->stream), "fill"));
+    FwRaster R{};
+    R.w = W;
+    R.h = H;
+    R.fmt = fmt;
+    R.pyramid = pyramid != 0;
+    R.vx = ctx->fw_vx.as<float>();
+    R.vy = ctx->fw_vy.as<float>();
+    R.vd = mips ? ctx->fw_vd.as<float>() : nullptr;
+    R.levels = L;
+    R.cnt = ctx->fw_cnt.as<uint32_t>();
+    R.off = ctx->fw_off.as<uint32_t>();
+    R.fill = ctx->fw_fill.as<uint32_t>();
+    R.out = ctx->fw_out.p;
+    R.cov = ctx->fw_cov.as<uint8_t>();
+    R.outside = ff + FW_OUTSIDE;
+    R.bad = ff + FW_BAD;
+    R.nlong = (uint32_t*)(ff + FW_NLONG);
+    R.longq = ctx->fw_longq.as<uint32_t>();
+    long tris = 2L * (W - 1) * (H - 1);
+    unsigned gt = (unsigned)((tris + 127) / 128);
+    LAUNCH(ctx, k_fw_count, gt, 128, 0, R);
+    LAUNCH(ctx, k_scan_block, (unsigned)nb, 256, 0, R.cnt, R.off, n, ctx->fw_sums.as<uint32_t>(), (uint32_t*)(ff + FW_MAXC));
+    LAUNCH(ctx, k_scan_sums, 1, 1024, 0, ctx->fw_sums.as<uint32_t>(), nb, (unsigned long long*)(ff + FW_TOTAL));
+    LAUNCH(ctx, k_scan_add, grid1(n), TB, 0, R.off, n, ctx->fw_sums.as<uint32_t>());
+    int hf[8];
+    CHECK(ctx->cuda(cudaMemcpyAsync(hf, ff, sizeof hf, cudaMemcpyDeviceToHost, ctx->stream), "flags"));
+    CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution"));
+    if (hf[FW_OUTSIDE])
+        return ctx->fail(TW_ERR_UNSUPPORTED, "forward warp: the degenerate last row pass of the rasteriser would write outside "
+                                             "the image, which is not supported");
+    unsigned long long total;
+    std::memcpy(&total, hf + FW_TOTAL, sizeof total);
+    uint32_t maxc = (uint32_t)hf[FW_MAXC];
+    if (total >= (1ull << 31)) return ctx->fail(TW_ERR_TOO_LARGE, "forward warp: %llu covered pixel hits", total);
+    // 4. the hit lists
+    size_t nt = total ? (size_t)total : 1;
+    CHECK(ctx->ensure(ctx->fw_keys, nt * sizeof(uint32_t), "hit keys"));
+    CHECK(ctx->ensure(ctx->fw_cols, nt * sizeof(float4), "hit colours"));
+    if (maxc > 4096) CHECK(ctx->ensure(ctx->fw_scratch, 2 * nt * sizeof(uint2), "long list scratch"));
+    R.keys = ctx->fw_keys.as<uint32_t>();
+    R.cols = ctx->fw_cols.as<float4>();
+    R.scratch = maxc > 4096 ? ctx->fw_scratch.as<uint2>() : nullptr;
+    R.total = (uint32_t)total;
+    LAUNCH(ctx, k_fw_emit, gt, 128, 0, R);
+    // 5. the running mean of every pixel in triangle order, the depth conversion, the coverage
+    LAUNCH(ctx, k_fw_resolve, grid1(n), TB, 0, R);
+    LAUNCH(ctx, k_fw_resolve_long, 296, 512, FW_LONG_SMEM_BYTES, R);
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->fw_out.p, (size_t)n * px, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    if (cov) CHECK(ctx->cuda(cudaMemcpyAsync(cov, ctx->fw_cov.p, (size_t)n, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(hf, ff, sizeof hf, cudaMemcpyDeviceToHost, ctx->stream), "flags"));
+    CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution"));
+    CHECK(ctx->cuda(cudaGetLastError(), "kernel execution"));
+    if (hf[FW_BAD]) return ctx->fail(TW_ERR_UNSUPPORTED, "forward warp: a texture coordinate outside the image");
+    return TW_OK;
+}
+
+int tw_check_logf(tw_ctx* ctx, const float* x, float* out, int64_t n) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!x || !out || n < 0) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    if (n == 0) return TW_OK;
+    const uint2* tab;
+    int ntab;
+    CHECK(logf_table(ctx, &tab, &ntab));
+    CHECK(ctx->ensure(ctx->fw_vx, (size_t)n * sizeof(float), "logf input"));
+    CHECK(ctx->ensure(ctx->fw_vy, (size_t)n * sizeof(float), "logf output"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->fw_vx.p, x, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    LAUNCH(ctx, k_logf_glibc, grid1((long)n), TB, 0, ctx->fw_vx.as<float>(), ctx->fw_vy.as<float>(), (long)n, tab, ntab);
+    CHECK(ctx->cuda(cudaMemcpyAsync(out, ctx->fw_vy.p, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution"));
+    return ctx->cuda(cudaGetLastError(), "kernel execution");
 }
 
 int tw_from_frame(tw_ctx* ctx, const void* wire, int32_t width, int32_t height, int32_t fmt, void* engine_out) {

@@ -70,6 +70,23 @@ __device__ __forceinline__ float mul(float a, float b) { return fix(a * b, a, b)
 __device__ __forceinline__ float div(float a, float b) { return fix(a / b, a, b); }
 }  // namespace nr
 
+// The x86 SSE results of the plain single precision operations, NaNs included: a NaN operand
+// propagates quieted (the first one when both are NaN), an invalid operation on numbers gives the
+// default NaN 0xffc00000. The device's own NaN is canonical, so where a plain operation of the
+// reference can carry a NaN into an output these give its bits; numbers are unchanged.
+namespace x86 {
+__device__ __forceinline__ float fix(float r, float a, float b) {
+    if (!isnan(r)) return r;
+    if (isnan(a)) return nr::quiet(a);
+    if (isnan(b)) return nr::quiet(b);
+    return __uint_as_float(0xffc00000u);
+}
+__device__ __forceinline__ float add(float a, float b) { return fix(a + b, a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return fix(a - b, a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return fix(a * b, a, b); }
+__device__ __forceinline__ float div(float a, float b) { return fix(a / b, a, b); }
+}  // namespace x86
+
 // sample.rs:31-41: index and fraction of one coordinate, clamped into 0..=len-2
 __device__ __forceinline__ void cell(float x, int len, int& io, float& fo) {
     int i = cvtt32(x);
