@@ -197,6 +197,22 @@ def run_reference(args):
     return 0
 
 
+def ncu_case():
+    """One step of the workload (10 output frames of the 1080p clip, 2 exact and 8 in-between), for
+    an ncu capture: a few hundred kernel launches, 0.1 GB on the device."""
+    import twixtor_b200 as tw
+    nframes = source_frames_needed(FRAMES_PER_STEP)
+    frames_np = make_clip(nframes)
+    dev = tw.Device(0)
+    tp = tw.TimeParams(speed_percent=SPEED)
+    sels = [tw.select(tp, n, W, H) for n in range(FRAMES_PER_STEP)]
+    out = np.zeros(FRAMES_PER_STEP * W * H * 4, np.uint8)
+    dev.retime_clip(tw.RetimeSettings(), frames_np, nframes, sels, W, H, 0, out=out)
+    print(json.dumps({"ncu_case": "ok", "frames": FRAMES_PER_STEP, "launches": dev.stats()["kernel_launches"]}))
+    dev.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -204,6 +220,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="profiling driver, no timing: renders the first 10 output frames of the 1080p workload once "
+                         "(device resident clip) and exits; the command the committed ncu summaries name")
     ap.add_argument("--breakdown", action="store_true",
                     help="after the timed region, time one more step with every kernel bracketed by events and "
                          "print the per-kernel table to stderr (not part of the reported numbers)")
@@ -212,6 +231,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.ncu_case:
+        return ncu_case()
 
     import torch
     import twixtor_b200 as tw

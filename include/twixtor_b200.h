@@ -117,6 +117,16 @@ typedef struct tw_retime_settings {
     int32_t motion_rows_reversed;
 } tw_retime_settings;
 
+/* The Create Vectors pass of one layer (create_vectors.rs:97-135): the solver settings (quality 4
+ * Normal (half res) or 5 Full res, hiq, sensitivity, track_alpha for Track RGB+A, the tap order;
+ * video_range_luma, skip_refine and wrap are off), Max Displace in pixels of the output, and the
+ * row order the engine sees (plugin 02 turns the frames upside down, glue.rs:28-37). */
+typedef struct tw_vectors_settings {
+    tw_flow_settings flow;
+    float max_displace;
+    int32_t rows_reversed;
+} tw_vectors_settings;
+
 /* ---- context ------------------------------------------------------------------------------ */
 
 /* Opens device `device` (the reference's `--device gpu=N` open, device/exec/open.rs:72-116).
@@ -221,6 +231,29 @@ int tw_forward_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const t
 /* Self check of the device's logf of the forward warp's mip level (forward/mesh.rs:89-90), which
  * must equal the host C library's logf bit for bit: out[i] = logf(x[i]) computed on the device. */
 int tw_check_logf(tw_ctx* ctx, const float* x, float* out, int64_t n);
+
+/* vectors::encode_vectors (vectors.rs:57-130): the flow (any size of at least 2x2) encoded into
+ * `out` (engine image, its size and format): R dx and G dy centred and scaled by `scale` (Max
+ * Displace), B 0, A white. */
+int tw_encode_vectors(tw_ctx* ctx, tw_image_mut* out, const tw_flow* flow, float scale);
+
+/* create_vectors::create_vectors_on (create_vectors.rs:162-183) for one layer: solve(x, y) on the
+ * device and the encode of the flow, engine images in and out (s->rows_reversed is ignored: the
+ * caller hands the images in the engine's row order). A side of 1 gives the zero vector image. */
+int tw_create_vectors(tw_ctx* ctx, const tw_vectors_settings* s, const tw_image* x, const tw_image* y,
+                      tw_image_mut* out);
+
+/* The clip frames of output frame n of Create Vectors (create_vectors.rs:59-97, glue.rs:488-524):
+ * a = n, b = n - 1 (track_frame 1, Previous) or n + 1 (2, Next); a frame outside the clip is
+ * blank. time_step: ticks per frame (integer rates: 100). */
+int tw_vectors_pair(int32_t n, int32_t time_step, int32_t track_frame, int32_t* a, int32_t* b);
+
+/* The Create Vectors effect over a clip in HOST memory (wire frames back to back): output frame k
+ * encodes the flow from clip frame pairs[2k] to pairs[2k + 1] (a frame index outside 0..nframes-1
+ * is a blank frame), with the device frame cache, the lanes and the copy streams of
+ * tw_retime_clip. The output wire frames go to out + k * frame_bytes. */
+int tw_create_vectors_clip(tw_ctx* ctx, const tw_vectors_settings* s, const void* frames, int32_t nframes,
+                           const int32_t* pairs, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out);
 
 /* holefill::fill_holes_masked_with (holefill.rs:452-491) with is360 off: the pull-push fill of
  * `img` in place. `mask` holds width*height values of kind 1 (u8), 2 (u16) or 3 (f32); a pixel is

@@ -16,6 +16,7 @@
 #include "oracle_core.h"
 #include "oracle_smart.h"
 #include "oracle_forward.h"
+#include "oracle_vectors.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -519,6 +520,94 @@ int or_retime_clip(const void* frames, int nframes, int w, int h, int fmt, const
     size_t frame_bytes = (size_t)w * h * 4 * es;
     for (int n = 0; n < nout; n++) {
         int rc = or_retime_one(frames, nframes, w, h, fmt, p, n, (uint8_t*)out + (size_t)n * frame_bytes);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+// ---- Create Vectors (plugins/create-vectors/src/glue.rs:488-569, one layer, Display Motion Vectors)
+
+struct or_cv_params {
+    int fps_num, fps_den;
+    int quality_high;
+    int vector_resolution;  // popup: 1 Normal (half res), 2 Full res
+    double max_displace;    // Max Displace (16.16 reader)
+    int track_frame;        // popup: 1 Previous, 2 Next
+    double sensitivity;     // Main_BG: Sensitivity, 0..100 (16.16 reader)
+    int track_rgb_a;
+    int rows_reversed;      // the plugin turns the frames upside down for the engine (glue.rs:28-37)
+    int taps_above_first;   // the solver's vertical border tap order
+};
+
+// vectors.rs:57-130 on a flow field; dst_fmt 0/1/2
+int or_encode_vectors(void* out_eng, int w, int h, int fmt, const float* flow, int fw, int fh, float scale) {
+    Image out(w, h, (Fmt)fmt);
+    FlowField f(fw, fh);
+    std::memcpy(f.d.data(), flow, f.d.size() * 4);
+    std::string e;
+    int rc = encode_vectors(out, f, scale, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(out_eng, out.data(), out.bytes());
+    return 0;
+}
+
+// Output frame n of the Create Vectors effect over a raw clip (wire frames back to back).
+int or_create_vectors_one(const void* frames, int nframes, int w, int h, int fmt, const or_cv_params* p, int n,
+                          void* out) {
+    Fmt f = (Fmt)fmt;
+    size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
+    size_t frame_bytes = (size_t)w * h * 4 * es;
+    int ts = p->fps_den == 1 ? 100 : p->fps_den;
+    int ct = n * ts;
+    // create_vectors.rs:59-62, :71-89, :92-97
+    uint32_t frame = (uint32_t)cvtt64f((float)ct / (float)ts + 0.5f);
+    float nf = (float)(int32_t)frame;
+    float fa = nf, fb = nf;
+    if (p->track_frame == 1) fb = nf - 1.0f;
+    else if (p->track_frame == 2) fb = nf + 1.0f;
+    int a = cvtt32(fa), b = cvtt32(fb);
+    auto frame_time = [&](int k) {
+        float tsf = (float)ts, x = (float)k;
+        float t = x < 0.0f ? -((-x) * tsf + 0.5f) : tsf * x + 0.5f;
+        return cvtt32(t);
+    };
+    auto fetch = [&](int t) -> Image {  // glue.rs:399-421: a tick outside the clip is transparent
+        long long idx = t >= 0 ? t / ts : -(((long long)-t + ts - 1) / ts);
+        if (idx < 0 || idx >= nframes) return Image(w, h, f);
+        return from_frame((const uint8_t*)frames + (size_t)idx * frame_bytes, w, h, f);
+    };
+    Image x = fetch(frame_time(a)), y = fetch(frame_time(b));
+    if (!(w >= 2 && h >= 2)) {  // glue.rs:537-540
+        to_frame(zero_vectors_image(w, h, f), out);
+        return 0;
+    }
+    if (p->rows_reversed) {
+        x = rows_reversed(x);
+        y = rows_reversed(y);
+    }
+    CreateVectorsSettings cs;
+    cs.quality = p->vector_resolution == 2 ? 5 : 4;
+    cs.hiq = p->quality_high != 0;
+    cs.sensitivity = fixed_reader(float_to_fixed(p->sensitivity), 1.0f) / 100.0f;
+    cs.track_rgb_a = p->track_rgb_a != 0;
+    cs.max_displace = (1.0f / 1.0f) * fixed_reader(float_to_fixed(p->max_displace), 1.0f);
+    cs.taps_above_first = p->taps_above_first != 0;
+    Image enc;
+    std::string e;
+    int rc = create_vectors(x, y, cs, &enc, &e);
+    if (rc) return fail(rc, e);
+    if (p->rows_reversed) enc = rows_reversed(enc);
+    to_frame(enc, out);
+    return 0;
+}
+
+int or_create_vectors_clip(const void* frames, int nframes, int w, int h, int fmt, const or_cv_params* p, int nout,
+                           void* out) {
+    Fmt f = (Fmt)fmt;
+    size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
+    size_t frame_bytes = (size_t)w * h * 4 * es;
+    for (int n = 0; n < nout; n++) {
+        int rc = or_create_vectors_one(frames, nframes, w, h, fmt, p, n, (uint8_t*)out + (size_t)n * frame_bytes);
         if (rc) return rc;
     }
     return 0;

@@ -967,6 +967,10 @@ int inv_warp(Image& out, const Image& src, const FlowField& flow, float amount, 
 // =============================================================================================
 // blend (blend.rs)
 
+void warp_flow_bilerp(const FlowField& f, float x, float y, float out[2]) {
+    flow_bilerp(f.d.data(), f.w, f.w - 1, f.h - 1, x, y, out);
+}
+
 void bilerp4_image(const Image& img, float x, float y, float out[4]) {
     int w1 = img.w - 1, h1 = img.h - 1;
     if (img.fmt == U8) bilerp4(img.u8.data(), img.w, w1, h1, x, y, out);

@@ -195,6 +195,8 @@ bool clip_to_rect(float x, float y, float* ix, float* iy, float w1, float h1);
 int inv_warp(Image& out, const Image& src, const FlowField& flow, float amount, WarpOpts o, Coverage* cov,
              std::string* err);
 void copy_image(Image& out, const Image& src);
+// warp.rs:415-442 Flow::bilerp (the warps' two channel flow sampler)
+void warp_flow_bilerp(const FlowField& f, float x, float y, float out[2]);
 // warp.rs:308-331 bilerp4 (with mix4's NaN rule repeat) over an image, w1 = w - 1, h1 = h - 1
 void bilerp4_image(const Image& img, float x, float y, float out[4]);
 void blend(Image& out, const Image& a, const Image& b, float w);

@@ -14,6 +14,14 @@ Writes, next to this script:
   recorded by the reference revision whose motion path ran on top-down rows with the vertical
   border taps below first; the tests run the oracle and the CUDA path in that variant
   (``rows_reversed=False, taps_above_first=False``) for these cases.
+* ``create_vectors_grid.npz`` - the cases of the reference's parity grid ``parity/create-vectors``
+  that the single layer Create Vectors pass serves (Display Motion Vectors, no FG matte or Alt
+  Motion Src layer, no tracking points, no prep, no keyed parameter, integer frame rates), their
+  raw input clips as ``parity/create-vectors/gen_grid.py`` renders them, and the sha256 of the
+  output clip that ``parity/create-vectors/results/base_outputs.tsv`` records. That table was
+  recorded, like the retime one, by the revision whose engine saw the frames top row first and
+  whose vertical border taps came below first: the tests run those cases with
+  ``rows_reversed=False, taps_above_first=False``.
 * ``f1_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/f1_cases.hex``
   (the reference's bit-exact numpy models of Smart Blend and the hole fill; format in its
   ``f1_gen.py``).
@@ -63,6 +71,53 @@ def served(case):
     return True
 
 
+CV_SERVED = {"max_displace", "main_bg_sensitivity", "track_frame", "vector_resolution", "track_rgb_a", "display",
+             "layers_output", "main_bg_track"}
+
+
+def cv_served(case):
+    params = dict(p.split("=", 1) for p in case["params"])
+    if case.get("layers"):
+        return False
+    if any(k not in CV_SERVED for k in params) or any("@" in v for v in params.values()):
+        return False
+    if params.get("display", "2") != "2" or params.get("main_bg_track", "1") != "1":
+        return False
+    if params.get("layers_output", "1") not in ("1", "5"):
+        return False
+    return "/" not in case["fps"] and "." not in case["fps"]
+
+
+def create_vectors_grid(ref):
+    path = os.path.join(ref, "parity", "create-vectors", "gen_grid.py")
+    spec = importlib.util.spec_from_file_location("cv_gen", path)
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    g = gen.Grid()
+    gen.build(g)
+    table = {}
+    for line in open(os.path.join(ref, "parity", "create-vectors", "results", "base_outputs.tsv")):
+        parts = line.rstrip("\n").split("\t")
+        if parts[0] != "id":
+            table[parts[0]] = (parts[1], parts[3])
+    cases, inputs = [], {}
+    for c in g.cases:
+        if not cv_served(c) or table[c["id"]][0] != "0":
+            continue
+        key = c["input"]
+        if key not in inputs:
+            info = g.inputs[key]
+            inputs[key] = np.frombuffer(gen.render_clip(info["source"], info["width"], info["height"], info["depth"],
+                                                        info["frames"]), np.uint8)
+        cases.append(dict(id=c["id"], params=c["params"], depth=c["depth"], width=c["width"], height=c["height"],
+                          frames=c["frames"], fps=c["fps"], input=key, sha256=table[c["id"]][1]))
+    keys = sorted(inputs)
+    arrays = {f"input_{i}": inputs[k] for i, k in enumerate(keys)}
+    arrays["meta"] = np.frombuffer(json.dumps(dict(inputs=keys, cases=cases)).encode(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "create_vectors_grid.npz"), **arrays)
+    print(f"create_vectors_grid.npz: {len(cases)} cases, {len(keys)} input clips")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -96,6 +151,8 @@ def main():
         arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), np.uint8)
         np.savez_compressed(os.path.join(HERE, "retime_flow_grid.npz"), **arrays)
         print(f"retime_flow_grid.npz: {len(cases)} cases, {len(keys)} input clips")
+
+    create_vectors_grid(ref)
 
     txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "f1_cases.hex")).read()
     blob = bytes.fromhex("".join(txt.split()))

@@ -19,6 +19,23 @@ def grid():
     return meta["cases"], inputs
 
 
+def cv_grid():
+    """The served cases of the create-vectors parity grid: (meta cases, {input name: raw bytes})."""
+    z = np.load(os.path.join(GOLDEN, "create_vectors_grid.npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    inputs = {name: z[f"input_{i}"] for i, name in enumerate(meta["inputs"])}
+    return meta["cases"], inputs
+
+
+def cv_case_params(case):
+    """The parameter values of a create-vectors grid case (plugin defaults where the case sets none)."""
+    p = dict(x.split("=", 1) for x in case["params"])
+    return dict(fps=(int(case["fps"]), 1), vector_resolution=int(p.get("vector_resolution", 1)),
+                max_displace=float(p.get("max_displace", 2048)), track_frame=int(p.get("track_frame", 1)),
+                sensitivity=float(p.get("main_bg_sensitivity", 70)),
+                track_rgb_a=p.get("track_rgb_a", "0") in ("1", "true", "True"))
+
+
 def case_params(case):
     """Keyword arguments of oracle_lib.retime_params for a grid case (grid variant of the orders)."""
     params = dict(p.split("=", 1) for p in case["params"])

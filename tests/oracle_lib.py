@@ -89,6 +89,8 @@ def lib():
         L.or_fw_level_count.argtypes = [i, i]
         L.or_fw_triangle.argtypes = [P, i, i, P, i]
         L.or_logf.argtypes = [P, P, ctypes.c_long]
+        L.or_create_vectors_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(CvParams), i, P]
+        L.or_encode_vectors.argtypes = [P, i, i, i, P, i, i, f]
         _lib = L
     return _lib
 
@@ -180,6 +182,35 @@ def compose_vectors2(a, b, w, h, fmt, f_ab, f_ba, fw, fh, wa, interp, warp_mode,
 def fill_holes(img, w, h, fmt, mask, mask_kind, above_first=True):
     out = np.array(img, copy=True)
     rc = lib().or_fill_holes(ptr(out), w, h, fmt, ptr(mask), mask_kind, int(above_first))
+    if rc:
+        raise ValueError(err())
+    return out
+
+
+class CvParams(ctypes.Structure):
+    _fields_ = [("fps_num", ctypes.c_int), ("fps_den", ctypes.c_int), ("quality_high", ctypes.c_int),
+                ("vector_resolution", ctypes.c_int), ("max_displace", ctypes.c_double), ("track_frame", ctypes.c_int),
+                ("sensitivity", ctypes.c_double), ("track_rgb_a", ctypes.c_int), ("rows_reversed", ctypes.c_int),
+                ("taps_above_first", ctypes.c_int)]
+
+
+def create_vectors_clip(frames, nframes, w, h, fmt, nout, fps=(24, 1), vector_resolution=1, max_displace=2048.0,
+                        track_frame=1, sensitivity=70.0, track_rgb_a=False, rows_reversed=True, taps_above_first=True):
+    """Output frames 0..nout-1 of the Create Vectors effect (plugin 02, one layer) over a raw clip."""
+    p = CvParams(fps[0], fps[1], 1, vector_resolution, max_displace, track_frame, sensitivity, int(track_rgb_a),
+                 int(rows_reversed), int(taps_above_first))
+    out = np.zeros(nout * w * h * 4, DTYPE[fmt])
+    rc = lib().or_create_vectors_clip(ptr(np.ascontiguousarray(frames)), nframes, w, h, fmt, ctypes.byref(p), nout,
+                                      ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out
+
+
+def encode_vectors(flow, fw, fh, w, h, fmt, scale):
+    out = np.zeros(w * h * 4, DTYPE[fmt])
+    rc = lib().or_encode_vectors(ptr(out), w, h, fmt, ptr(np.ascontiguousarray(flow, np.float32)), fw, fh,
+                                 np.float32(scale))
     if rc:
         raise ValueError(err())
     return out

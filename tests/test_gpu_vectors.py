@@ -1,0 +1,104 @@
+"""Parity of the CUDA Create Vectors pass (tw_create_vectors, tw_create_vectors_clip,
+tw_encode_vectors) with the reference's recorded outputs and with the oracle, bit for bit."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import golden_data
+import oracle_lib as O
+import twixtor_b200 as tw
+from twixtor_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    tw.build()
+    d = tw.Device(0)
+    yield d
+    d.close()
+
+
+def same(a, b):
+    return np.asarray(a).view(np.uint8).tobytes() == np.asarray(b).view(np.uint8).tobytes()
+
+
+CV_CASES, CV_INPUTS = golden_data.cv_grid()
+
+
+@pytest.mark.parametrize("case", CV_CASES, ids=[c["id"] for c in CV_CASES])
+def test_create_vectors_grid_sha256(dev, case):
+    """The reference's recorded output clips of the served create-vectors grid cases."""
+    fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
+    raw = CV_INPUTS[case["input"]].view(tw.DTYPES[fmt])
+    kw = golden_data.cv_case_params(case)
+    s = tw.vectors_settings(vector_resolution=kw["vector_resolution"], max_displace=kw["max_displace"],
+                            sensitivity=kw["sensitivity"], track_rgb_a=kw["track_rgb_a"], rows_reversed=False,
+                            taps_above_first=False)
+    pairs = [tw.vectors_pair(n, kw["track_frame"], kw["fps"]) for n in range(case["frames"])]
+    out = dev.create_vectors_clip(s, raw, case["frames"], pairs, case["width"], case["height"], fmt)
+    assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("track_frame", [1, 2])
+@pytest.mark.parametrize("rows_reversed", [True, False])
+def test_clip_matches_oracle(dev, fmt, track_frame, rows_reversed):
+    """The reference's current orders (rows reversed, taps above first) and the grid's."""
+    w, h, n = 160, 96, 6
+    depth = {0: 8, 1: 16, 2: 32}[fmt]
+    frames = synth.moving_clip(w, h, n, depth=depth, seed=0x74570002)
+    s = tw.vectors_settings(max_displace=24.0, rows_reversed=rows_reversed, taps_above_first=rows_reversed)
+    pairs = [tw.vectors_pair(k, track_frame) for k in range(n)]
+    got = dev.create_vectors_clip(s, frames, n, pairs, w, h, fmt)
+    want = O.create_vectors_clip(frames, n, w, h, fmt, n, max_displace=24.0, track_frame=track_frame,
+                                 rows_reversed=rows_reversed, taps_above_first=rows_reversed)
+    assert same(got, want)
+
+
+def test_1080p_u16_pair_matches_oracle(dev):
+    """One frame pair of the 1920x1080 16 bpc workload (solve at 960x540, 8 levels)."""
+    w, h = 1920, 1080
+    frames = synth.moving_clip(w, h, 2, depth=16, seed=0x74570002, bg_velocity=(6.0, -3.0), square=240,
+                               square_start=(600.0, 400.0), square_velocity=(9.0, 4.0))
+    s = tw.vectors_settings()
+    got = dev.create_vectors_clip(s, frames, 2, [(1, 0)], w, h, 1)
+    want = O.create_vectors_clip(frames, 2, w, h, 1, 2)[w * h * 4:]
+    assert same(got, want)
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+def test_engine_entry_matches_oracle(dev, fmt):
+    w, h = 97, 61
+    depth = {0: 8, 1: 16, 2: 32}[fmt]
+    frames = synth.moving_clip(w, h, 2, depth=depth, seed=5)
+    n = w * h * 4
+    x, y = O.from_frame(frames[:n], w, h, fmt), O.from_frame(frames[n:], w, h, fmt)
+    s = tw.vectors_settings(max_displace=10.0)
+    got = dev.create_vectors(s, y, x, w, h, fmt)
+    flow_b, _, (fw, fh) = O.solve_pair(y, x, w, h, fmt)
+    want = O.encode_vectors(flow_b, fw, fh, w, h, fmt, np.float32(10.0))
+    assert same(got, want)
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+def test_encode_special_values(dev, fmt):
+    """Clamps, NaN and infinite vectors, a flow of another size than the image."""
+    rng = np.random.RandomState(2)
+    fw, fh, w, h = 13, 9, 40, 30
+    flow = rng.uniform(-30, 30, fw * fh * 2).astype(np.float32)
+    flow[rng.randint(0, flow.size, 6)] = np.nan
+    flow[rng.randint(0, flow.size, 4)] = np.inf
+    flow[rng.randint(0, flow.size, 4)] = -np.inf
+    got = dev.encode_vectors(flow, (fw, fh), w, h, fmt, 7.5)
+    want = O.encode_vectors(flow, fw, fh, w, h, fmt, 7.5)
+    assert same(got, want)
+
+
+def test_tiny_frames_are_zero_vectors(dev):
+    frames = np.arange(1 * 7 * 4 * 3, dtype=np.uint8)
+    out = dev.create_vectors_clip(tw.vectors_settings(), frames, 3, [(1, 0), (2, 1)], 1, 7, 0)
+    want = O.create_vectors_clip(frames, 3, 1, 7, 0, 3)[7 * 4:]
+    assert same(out, want)

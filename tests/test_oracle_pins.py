@@ -184,3 +184,18 @@ def test_smart_blend_and_hole_fill_model_fixtures(i):
         rc = O.lib().or_fill_holes(O.ptr(out), c["w"], c["h"], c["fmt"], O.ptr(c["mask"]), c["mask_kind"], 0)
         assert rc == 0, O.err()
     assert out.view(np.uint8).tobytes() == c["out"].view(np.uint8).tobytes()
+
+
+CV_CASES, CV_INPUTS = golden_data.cv_grid()
+
+
+@pytest.mark.parametrize("case", CV_CASES, ids=[c["id"] for c in CV_CASES])
+def test_create_vectors_grid_sha256(case):
+    """The reference's recorded output clips of the served create-vectors grid cases (solve + encode,
+    frame pairs, blank neighbours outside the clip, tiny frames)."""
+    fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
+    raw = CV_INPUTS[case["input"]].view(O.DTYPE[fmt])
+    kw = golden_data.cv_case_params(case)
+    out = O.create_vectors_clip(raw, case["frames"], case["width"], case["height"], fmt, case["frames"],
+                                rows_reversed=False, taps_above_first=False, **kw)
+    assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]

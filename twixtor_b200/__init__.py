@@ -91,6 +91,10 @@ class _RetimeSettings(ctypes.Structure):
     _fields_ = [("flow", _FlowSettings), ("compose", _EngineSettings), ("motion_rows_reversed", ctypes.c_int32)]
 
 
+class _VectorsSettings(ctypes.Structure):
+    _fields_ = [("flow", _FlowSettings), ("max_displace", ctypes.c_float), ("rows_reversed", ctypes.c_int32)]
+
+
 class _TimeParams(ctypes.Structure):
     _fields_ = [("fps_num", ctypes.c_int32), ("fps_den", ctypes.c_int32), ("speed_percent", ctypes.c_double),
                 ("nkeys", ctypes.c_int32), ("key_frames", ctypes.POINTER(ctypes.c_double)),
@@ -171,6 +175,36 @@ class RetimeSettings:
 
 
 @dataclass
+class VectorsSettings:
+    """The Create Vectors pass of one layer (create_vectors.rs:97-135): the solver settings (quality 4
+    Normal (half res) / 5 Full res, ``track_alpha`` for Track RGB+A), Max Displace in output pixels,
+    and whether the engine sees the frames upside down (plugin 02's glue)."""
+    flow: FlowSettings = field(default_factory=FlowSettings)
+    max_displace: float = 2048.0
+    rows_reversed: bool = True
+
+    def _c(self):
+        return _VectorsSettings(self.flow._c(), np.float32(self.max_displace), int(self.rows_reversed))
+
+
+def vectors_settings(vector_resolution=1, max_displace=2048.0, sensitivity=70.0, track_rgb_a=False, hiq=True,
+                     rows_reversed=True, taps_above_first=True) -> VectorsSettings:
+    """The settings of plugin 02 (create-vectors) from its parameter values (glue.rs:133-146): the
+    popup Vector Resolution, the 16.16 readers of Max Displace and Sensitivity (percent)."""
+    def fixed(v):
+        f = v * 65536.0 + (-0.5 if v < 0 else 0.5)
+        return int(np.clip(np.trunc(f), -2 ** 31, 2 ** 31 - 1))
+
+    def reader(v):
+        return np.float32(np.float64(fixed(v)) * (1.0 / 65536.0))
+
+    sens = np.float32(reader(sensitivity) / np.float32(100.0))
+    fs = FlowSettings(quality=5 if vector_resolution == 2 else 4, hiq=hiq, sensitivity=sens, track_alpha=track_rgb_a,
+                      taps_above_first=taps_above_first)
+    return VectorsSettings(flow=fs, max_displace=float(np.float32(1.0) * reader(max_displace)), rows_reversed=rows_reversed)
+
+
+@dataclass
 class TimeParams:
     """The parameters the Speed time map reads (plugins/retime/src/lib.rs:59-99). Popups carry
     their 1-based values; ``keys`` is a list of (frame, value, ease) of a keyed Speed %."""
@@ -245,6 +279,10 @@ def library():
     L.tw_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float]
     L.tw_smart_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float, i32]
     L.tw_forward_warp.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, P]
+    L.tw_encode_vectors.argtypes = [P, pimg, pflow, ctypes.c_float]
+    L.tw_create_vectors.argtypes = [P, ctypes.POINTER(_VectorsSettings), pimg, pimg, pimg]
+    L.tw_vectors_pair.argtypes = [i32, i32, i32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+    L.tw_create_vectors_clip.argtypes = [P, ctypes.POINTER(_VectorsSettings), P, i32, P, i32, i32, i32, i32, P]
     L.tw_check_logf.argtypes = [P, P, P, ctypes.c_int64]
     L.tw_fill_holes.argtypes = [P, pimg, P, i32, i32]
     L.tw_from_frame.argtypes = [P, P, i32, i32, i32, P]
@@ -268,6 +306,16 @@ def _img(a, w, h, fmt):
     a = np.ascontiguousarray(a)
     assert a.dtype == DTYPES[fmt] and a.size == w * h * 4, "engine image of the wrong size or depth"
     return _Image(w, h, fmt, a.ctypes.data), a
+
+
+def vectors_pair(n: int, track_frame: int = 1, fps: Tuple[int, int] = (24, 1)) -> Tuple[int, int]:
+    """The clip frames (X, Y) of output frame ``n`` of Create Vectors (create_vectors.rs:59-97)."""
+    ts = 100 if fps[1] == 1 else fps[1]
+    a, b = ctypes.c_int32(), ctypes.c_int32()
+    rc = library().tw_vectors_pair(n, ts, track_frame, ctypes.byref(a), ctypes.byref(b))
+    if rc:
+        raise BadParam(rc, "bad argument")
+    return a.value, b.value
 
 
 def select(params: TimeParams, n: int, width: int, height: int) -> Selection:
@@ -451,6 +499,39 @@ class Device:
         self._check(self._L.tw_forward_warp(self._h, ctypes.byref(oi), ctypes.byref(si), ctypes.byref(fl), np.float32(amount),
                                             int(pyramid), _ptr(cov)))
         return (out, cov) if coverage else out
+
+    def encode_vectors(self, flow, flow_size, width, height, fmt, scale):
+        """``vectors::encode_vectors``: the encoded vector image (engine samples) of a flow."""
+        fw, fh = flow_size
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        oi = _Image(width, height, fmt, out.ctypes.data)
+        flow = np.ascontiguousarray(flow, np.float32)
+        fl = _Flow(fw, fh, flow.ctypes.data)
+        self._check(self._L.tw_encode_vectors(self._h, ctypes.byref(oi), ctypes.byref(fl), np.float32(scale)))
+        return out
+
+    def create_vectors(self, settings: VectorsSettings, x, y, width, height, fmt):
+        """``create_vectors::create_vectors_on`` for one layer: engine images in, the encoded engine image out."""
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        xi, xa = _img(x, width, height, fmt)
+        yi, ya = _img(y, width, height, fmt)
+        oi = _Image(width, height, fmt, out.ctypes.data)
+        self._check(self._L.tw_create_vectors(self._h, ctypes.byref(settings._c()), ctypes.byref(xi), ctypes.byref(yi),
+                                              ctypes.byref(oi)))
+        return out
+
+    def create_vectors_clip(self, settings: VectorsSettings, frames, nframes, pairs, width, height, fmt, out=None):
+        """Create Vectors over a clip in host memory: output frame k encodes the flow from clip frame
+        pairs[k][0] to pairs[k][1]. Returns the output wire frames back to back."""
+        frames = np.ascontiguousarray(frames)
+        fs = width * height * 4
+        pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1)
+        nout = pairs.size // 2
+        if out is None:
+            out = np.zeros(nout * fs, DTYPES[fmt])
+        self._check(self._L.tw_create_vectors_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes, _ptr(pairs),
+                                                   nout, width, height, fmt, _ptr(out)))
+        return out
 
     def check_logf(self, x):
         """The device's logf of the forward warp's mip level (equal to the host C library's)."""

@@ -153,6 +153,9 @@ __global__ void k_fill_store(void* __restrict__ img, int fmt, const float* __res
 __global__ void k_stack_zero(float* __restrict__ p, long n, const int* __restrict__ any_hole);
 __global__ void k_hole_side1(const int* __restrict__ any_hole, int* __restrict__ flag);
 
+__global__ void k_encode_vectors(const float* __restrict__ flow, int fw, int fh, void* __restrict__ out, int W, int H,
+                                 int fmt, float sx, float sy, float kx, float ky, int zero);
+
 // ---- the forward warp (forward.cu) ---------------------------------------------------------------------
 struct FwGrid {  // forward/mesh.rs:11-26
     int w, h;

@@ -1495,6 +1495,65 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
     return TW_OK;
 }
 
+// The Create Vectors pass on lane L (create_vectors.rs:162-183): the engine images X and Y are in
+// L.eng[0] (ready on stream 0) and L.eng[1] (ready on stream 1), in the engine's row order. The
+// pyramids run on both streams, the solve X -> Y and the encode on stream 0; `out` receives the
+// engine image, or with to_wire the wire frame (rows turned back when flip). The frame's end is
+// L.ev_done on stream 0.
+static int vectors_lane(tw_ctx* ctx, Lane& L, const tw_vectors_settings& s, int W, int H, int fmt, void* out,
+                        bool to_wire, bool flip) {
+    int* flags = L.flags.as<int>();
+    size_t bytes = (size_t)W * H * 4 * sample_bytes(fmt);
+    void* eng_out = out;
+    if (to_wire) {
+        CHECK(ctx->ensure(L.comp, bytes, "encoded vectors"));
+        eng_out = L.comp.p;
+    }
+    bool searchable = W >= 2 && H >= 2;  // prep.rs:100-102
+    tw_flow_settings fs = s.flow;
+    fs.video_range_luma = 0;
+    fs.skip_refine = 0;
+    if (fs.wrap) return ctx->fail(TW_ERR_UNSUPPORTED, "the wrap-around (360) solve is not on the device");
+    if (!searchable) {
+        CHECK(ctx->cuda(cudaEventRecord(L.ev_pyr[1], L.s[1]), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_pyr[1], 0), "event"));
+        ctx->cur = L.s[0];
+        LAUNCH(ctx, k_encode_vectors, grid2(W, H), TB, 0, (const float*)nullptr, 0, 0, eng_out, W, H, fmt, 0.0f, 0.0f, 0.0f,
+               0.0f, 1);
+    } else {
+        Geo g;
+        CHECK(geometry(fs, W, H, &g, &ctx->err));
+        size_t pf = pyramid_floats(g);
+        CHECK(ctx->ensure(L.pyr[0], 2 * pf * 4, "pyramid"));
+        CHECK(ctx->ensure(L.pyr[1], 2 * pf * 4, "pyramid"));
+        CHECK(ctx->ensure(L.flow[0], (size_t)g.w * g.h * 2 * sizeof(float), "flow"));
+        float* px_ = L.pyr[0].as<float>();
+        float* py_ = L.pyr[1].as<float>();
+        ctx->cur = L.s[0];
+        CHECK(build_pyramid_dev(ctx, L.eng[0].p, W, H, fmt, fs, g, px_, px_ + pf, L.scratch[0]));
+        ctx->cur = L.s[1];
+        CHECK(build_pyramid_dev(ctx, L.eng[1].p, W, H, fmt, fs, g, py_, py_ + pf, L.scratch[1]));
+        CHECK(ctx->cuda(cudaEventRecord(L.ev_pyr[1], L.s[1]), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_pyr[1], 0), "event"));
+        ctx->cur = L.s[0];
+        CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, fs, L.work[0], L.flow[0].as<float>(), flags + FL_ANY0,
+                                 flags + FL_NAN));
+        // vectors.rs:78-83, host scalars in single precision
+        float dw1 = (float)(W - 1), dh1 = (float)(H - 1), fw1 = (float)(g.w - 1), fh1 = (float)(g.h - 1);
+        float sx = fw1 / dw1, sy = fh1 / dh1;
+        float kx = (dw1 / fw1) / s.max_displace, ky = (dh1 / fh1) / s.max_displace;
+        LAUNCH(ctx, k_encode_vectors, grid2(W, H), TB, 0, L.flow[0].as<float>(), g.w, g.h, eng_out, W, H, fmt, sx, sy, kx, ky, 0);
+    }
+    if (to_wire) {
+        long n = (long)W * H;
+        if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)eng_out, (uint8_t*)out, W, H, flip);
+        else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)eng_out, (uint16_t*)out, W, H, flip);
+        else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)eng_out, (float*)out, W, H, flip);
+    }
+    CHECK(ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event"));
+    return TW_OK;
+}
+
 // Orders the first `nl` lanes' streams after the caller's work on ctx->stream (flags cleared first).
 static int lanes_begin(tw_ctx* ctx, int nl) {
     for (int i = 0; i < nl; i++) {
@@ -1562,14 +1621,15 @@ int tw_retime_frame(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection
 // frame cache (uploaded on the `up` stream once, in order of first use; a slot is reused only after
 // the frames that read it are done); the frame is composed into the lane's output buffer and copied
 // down on the `down` stream, which the lane's next frame waits for before it writes that buffer.
-int tw_retime_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
-                   const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out) {
-    if (!ctx) return TW_ERR_BAD_PARAM;
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    ctx->cur = ctx->stream;
-    if (!s || !sels || !frames || !out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
-        return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
-    size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
+// The host-buffer clip driver shared by tw_retime_clip and tw_create_vectors_clip: output frame k
+// reads clip frames src(k) = (a, b) (an index outside the clip is a blank frame) through the device
+// frame cache (uploaded once on the copy stream), runs frame_fn(k, lane, device A or null, device B
+// or null, device output) on lane k % nl, and copies the output back on the other copy stream.
+extern "C++" {
+template <typename Src, typename FrameFn>
+static int clip_host(tw_ctx* ctx, const void* frames, int nframes, int nout, int W, int H, int fmt, void* out, Src src,
+                     FrameFn frame_fn) {
+    size_t bytes = (size_t)W * H * 4 * sample_bytes(fmt);
     const int nl = std::min(MAX_LANES, 3);
     const int NS = tw_ctx::CACHE_SLOTS;
     if (!ctx->up) {
@@ -1613,18 +1673,18 @@ int tw_retime_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames,
     };
     int rc = TW_OK;
     for (int k = 0; k < nout && rc == TW_OK; k++) {
-        const tw_selection& sel = sels[k];
+        int fa, fb;
+        src(k, &fa, &fb);
         int li = k % nl;
         Lane& L = ctx->lanes[li];
-        int sa = (sel.a >= 0 && sel.a < nframes) ? frame_slot(sel.a, k, -1) : -1;
-        int sb = (sel.b >= 0 && sel.b < nframes) ? frame_slot(sel.b, k, sa) : -1;
+        int sa = (fa >= 0 && fa < nframes) ? frame_slot(fa, k, -1) : -1;
+        int sb = (fb >= 0 && fb < nframes) ? (fb == fa ? sa : frame_slot(fb, k, sa)) : -1;
         for (int st = 0; st < 2; st++) {
             if (sa >= 0) cudaStreamWaitEvent(L.s[st], ctx->cache_ready[sa], 0);
             if (sb >= 0) cudaStreamWaitEvent(L.s[st], ctx->cache_ready[sb], 0);
         }
         if (out_used[li]) cudaStreamWaitEvent(L.s[0], ctx->out_free[li], 0);
-        rc = retime_frame_lane(ctx, L, *s, sel, sa >= 0 ? ctx->cache[sa].p : nullptr, sb >= 0 ? ctx->cache[sb].p : nullptr,
-                               width, height, fmt, ctx->outbuf[li].p);
+        rc = frame_fn(k, L, sa >= 0 ? ctx->cache[sa].p : nullptr, sb >= 0 ? ctx->cache[sb].p : nullptr, ctx->outbuf[li].p);
         if (rc) break;
         // the frame's reads of its slots end with the lane's frame (both streams joined at ev_done)
         if (sa >= 0) { cudaEventRecord(ctx->cache_free[sa][li], L.s[0]); readers[sa] |= 1u << li; }
@@ -1645,6 +1705,135 @@ int tw_retime_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames,
     if (rc) return rc;
     if (rc2) return rc2;
     return ctx->cuda(cudaStreamSynchronize(ctx->stream), "download");
+}
+}  // extern "C++"
+
+int tw_retime_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
+                   const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!s || !sels || !frames || !out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
+        return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    return clip_host(
+        ctx, frames, nframes, nout, width, height, fmt, out,
+        [&](int k, int* a, int* b) {
+            *a = sels[k].a;
+            *b = sels[k].b;
+        },
+        [&](int k, Lane& L, const void* wa, const void* wb, void* ow) {
+            return retime_frame_lane(ctx, L, *s, sels[k], wa, wb, width, height, fmt, ow);
+        });
+}
+
+// ---- Create Vectors ----------------------------------------------------------------------------------
+
+int tw_encode_vectors(tw_ctx* ctx, tw_image_mut* out, const tw_flow* flow, float scale) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!out || !out->data || !flow || !flow->data || out->fmt < 0 || out->fmt > 2)
+        return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    int W = out->width, H = out->height;
+    if (W < 2 || H < 2 || flow->width < 2 || flow->height < 2)
+        return ctx->fail(TW_ERR_MISMATCH, "vector encode needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W,
+                         H, flow->width, flow->height);
+    size_t fb = (size_t)flow->width * flow->height * 2 * sizeof(float);
+    size_t ob = (size_t)W * H * 4 * sample_bytes(out->fmt);
+    CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
+    CHECK(ctx->ensure(ctx->eng[2], ob, "encoded vectors"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->flow[0].p, flow->data, fb, cudaMemcpyHostToDevice, ctx->stream), "flow upload"));
+    float dw1 = (float)(W - 1), dh1 = (float)(H - 1), fw1 = (float)(flow->width - 1), fh1 = (float)(flow->height - 1);
+    float sx = fw1 / dw1, sy = fh1 / dh1, kx = (dw1 / fw1) / scale, ky = (dh1 / fh1) / scale;
+    LAUNCH(ctx, k_encode_vectors, grid2(W, H), TB, 0, ctx->flow[0].as<float>(), flow->width, flow->height, ctx->eng[2].p, W,
+           H, out->fmt, sx, sy, kx, ky, 0);
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[1];
+    return finish(ctx, hf, 1);
+}
+
+int tw_create_vectors(tw_ctx* ctx, const tw_vectors_settings* s, const tw_image* x, const tw_image* y,
+                      tw_image_mut* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!s || !out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_image(ctx, x, "create vectors"));
+    CHECK(check_image(ctx, y, "create vectors"));
+    if (!same_shape(x, y) || out->width != x->width || out->height != x->height || out->fmt != x->fmt)
+        return ctx->fail(TW_ERR_MISMATCH, "create vectors: incompatible inputs (%dx%d fmt %d against %dx%d fmt %d)", x->width,
+                         x->height, x->fmt, y->width, y->height, y->fmt);
+    int W = x->width, H = x->height, fmt = x->fmt;
+    size_t bytes = (size_t)W * H * 4 * sample_bytes(fmt);
+    Lane& L = ctx->lanes[0];
+    CHECK(lanes_begin(ctx, 1));
+    CHECK(ctx->ensure(L.eng[0], bytes, "engine X"));
+    CHECK(ctx->ensure(L.eng[1], bytes, "engine Y"));
+    CHECK(ctx->ensure(ctx->eng[2], bytes, "encoded vectors"));
+    L.used = true;
+    CHECK(ctx->cuda(cudaMemcpyAsync(L.eng[0].p, x->data, bytes, cudaMemcpyHostToDevice, L.s[0]), "upload"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(L.eng[1].p, y->data, bytes, cudaMemcpyHostToDevice, L.s[1]), "upload"));
+    int rc = vectors_lane(ctx, L, *s, W, H, fmt, ctx->eng[2].p, false, false);
+    int rc2 = lanes_end(ctx, 1);
+    if (rc) return rc;
+    if (rc2) return rc2;
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    return ctx->cuda(cudaStreamSynchronize(ctx->stream), "download");
+}
+
+int tw_vectors_pair(int32_t n, int32_t time_step, int32_t track_frame, int32_t* a, int32_t* b) {
+    if (!a || !b || time_step <= 0) return TW_ERR_BAD_PARAM;
+    int64_t ct = (int64_t)n * time_step;
+    if (ct > INT32_MAX || ct < INT32_MIN) return TW_ERR_BAD_PARAM;
+    // create_vectors.rs:59-62: the frame number of the current time
+    float q = (float)(int32_t)ct / (float)time_step + 0.5f;
+    uint32_t frame = (uint32_t)(int64_t)q;
+    // :71-89: the pair (Display Motion Vectors)
+    float nf = (float)(int32_t)frame, fa = nf, fb = nf;
+    if (track_frame == 1) fb = nf - 1.0f;
+    else if (track_frame == 2) fb = nf + 1.0f;
+    auto cvtt = [](float v) { return (v > -2147483904.0f && v < 2147483648.0f) ? (int32_t)v : INT32_MIN; };
+    // :92-97 and the clip frame of that tick (a layer time divided by the frame length, rounded down)
+    auto clip_index = [&](int32_t k) {
+        float tsf = (float)time_step, x = (float)k;
+        float t = x < 0.0f ? -((-x) * tsf + 0.5f) : tsf * x + 0.5f;
+        int64_t ticks = cvtt(t);
+        int64_t idx = ticks >= 0 ? ticks / time_step : -((-ticks + time_step - 1) / time_step);
+        return (int32_t)std::max<int64_t>(std::min<int64_t>(idx, INT32_MAX), INT32_MIN);
+    };
+    *a = clip_index(cvtt(fa));
+    *b = clip_index(cvtt(fb));
+    return TW_OK;
+}
+
+int tw_create_vectors_clip(tw_ctx* ctx, const tw_vectors_settings* s, const void* frames, int32_t nframes,
+                           const int32_t* pairs, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!s || !pairs || !frames || !out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
+        return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
+    bool flip = s->rows_reversed != 0 && width >= 2 && height >= 2;
+    return clip_host(
+        ctx, frames, nframes, nout, width, height, fmt, out,
+        [&](int k, int* a, int* b) {
+            *a = pairs[2 * k];
+            *b = pairs[2 * k + 1];
+        },
+        [&](int k, Lane& L, const void* wa, const void* wb, void* ow) {
+            CHECK(ctx->ensure(L.eng[0], bytes, "engine X"));
+            CHECK(ctx->ensure(L.eng[1], bytes, "engine Y"));
+            if (L.used) CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[1], L.ev_done, 0), "lane order"));
+            L.used = true;
+            ctx->cur = L.s[0];
+            if (wa) from_frame_dev(ctx, wa, L.eng[0].p, width, height, fmt, flip);
+            else CHECK(ctx->cuda(cudaMemsetAsync(L.eng[0].p, 0, bytes, ctx->cur), "blank"));
+            ctx->cur = L.s[1];
+            if (wb) from_frame_dev(ctx, wb, L.eng[1].p, width, height, fmt, flip);
+            else CHECK(ctx->cuda(cudaMemsetAsync(L.eng[1].p, 0, bytes, ctx->cur), "blank"));
+            return vectors_lane(ctx, L, *s, width, height, fmt, ow, true, flip);
+        });
 }
 
 int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
