@@ -138,6 +138,11 @@ size_t tw_last_error(const tw_ctx* ctx, char* buf, size_t cap);
 /* Per-stage counters: launches of the library's kernels since open, and device bytes held. */
 int tw_stats(const tw_ctx* ctx, uint64_t* kernel_launches, uint64_t* device_bytes);
 
+/* The number of output frames the clip calls keep in flight (1..8; default 4): each has its own
+ * buffers and two streams, so their solves overlap on the GPU. A tuning knob only: the output
+ * bytes do not depend on it. */
+int tw_set_lanes(tw_ctx* ctx, int32_t lanes);
+
 /* Makes the context enqueue on `stream` (a cudaStream_t; NULL is the legacy default stream)
  * instead of its own, so a caller can order the library's work with its own and time it with its
  * own events. */

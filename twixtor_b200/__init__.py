@@ -278,6 +278,7 @@ def library():
     L.tw_block_match.argtypes = [P, P, P, P, i32, i32]
     L.tw_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float]
     L.tw_smart_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float, i32]
+    L.tw_set_lanes.argtypes = [P, i32]
     L.tw_forward_warp.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, P]
     L.tw_encode_vectors.argtypes = [P, pimg, pflow, ctypes.c_float]
     L.tw_create_vectors.argtypes = [P, ctypes.POINTER(_VectorsSettings), pimg, pimg, pimg]
@@ -532,6 +533,10 @@ class Device:
         self._check(self._L.tw_create_vectors_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes, _ptr(pairs),
                                                    nout, width, height, fmt, _ptr(out)))
         return out
+
+    def set_lanes(self, lanes):
+        """Output frames in flight in the clip calls (1..8)."""
+        self._check(self._L.tw_set_lanes(self._h, int(lanes)))
 
     def check_logf(self, x):
         """The device's logf of the forward warp's mip level (equal to the host C library's)."""

@@ -12,7 +12,7 @@ namespace tw {
 
 constexpr int FT_X = 32;  // tile width (outputs)
 constexpr int FT_Y = 32;  // tile height
-constexpr int FT_THREADS = 256;
+constexpr int FT_THREADS = 1024;  // the launch bound; each launch picks 256 to 1024 threads
 
 // ---- separable pass elements ---------------------------------------------------------------------
 

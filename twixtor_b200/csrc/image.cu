@@ -364,16 +364,18 @@ __global__ void k_encode_vectors(const float* __restrict__ flow, int fw, int fh,
         if (ix >= fw1) { ix = fw1 - 1; fx = 1.0f; }
         if (iy >= fh1) { iy = fh1 - 1; fy = 1.0f; }
         long i00 = ((long)iy * fw + ix) * 2, i01 = i00 + (long)fw * 2;
+        // x86 arithmetic: a NaN vector (a NaN or infinite flow) keeps the reference's bits in the
+        // float depth's output
         float o[2];
 #pragma unroll
         for (int k = 0; k < 2; k++) {
             float p00 = flow[i00 + k], p10 = flow[i00 + 2 + k], p01 = flow[i01 + k], p11 = flow[i01 + 2 + k];
-            float top = (p10 - p00) * fx + p00;
-            float bot = (p11 - p01) * fx + p01;
-            o[k] = (bot - top) * fy + top;
+            float top = x86::add(x86::mul(x86::sub(p10, p00), fx), p00);
+            float bot = x86::add(x86::mul(x86::sub(p11, p01), fx), p01);
+            o[k] = x86::add(x86::mul(x86::sub(bot, top), fy), top);
         }
-        a = o[0] * kx;
-        b = o[1] * ky;
+        a = x86::mul(o[0], kx);
+        b = x86::mul(o[1], ky);
     }
     long i = ((long)y * W + x) * 4;
     if (fmt == 2) {

@@ -174,16 +174,17 @@ struct Lane {
     DevBuf eng[2], pyr[2], work[2], flow[2], scratch[2][3], flags;
     DevBuf comp, holes, fill;  // warping code 1: the composite, its holes mask, the fill's planes
 };
-constexpr int MAX_LANES = 4;
+constexpr int MAX_LANES = 8;
 
 struct tw_ctx {
     int device = 0;
     KernelProfile prof;
     cudaStream_t cur = nullptr;  // the stream every launch goes to
     Lane lanes[MAX_LANES];
+    int nlanes = 4;  // output frames in flight in the clip calls (tw_set_lanes)
     cudaEvent_t ev_start = nullptr;
     // tw_retime_clip: a device cache of source frames, and the copy streams
-    static constexpr int CACHE_SLOTS = 10;
+    static constexpr int CACHE_SLOTS = 20;
     DevBuf cache[CACHE_SLOTS], outbuf[MAX_LANES];
     int cache_frame[CACHE_SLOTS];
     cudaEvent_t cache_ready[CACHE_SLOTS] = {}, out_free[MAX_LANES] = {};
@@ -284,6 +285,14 @@ dim3 tiles(int w, int h) { return dim3((unsigned)((w + FUSED_TILE_X - 1) / FUSED
 
 size_t pyramid_floats(const Geo& g);
 
+// Threads per CTA of the tiled level kernels: a level of few tiles is latency bound (every CTA
+// walks its stages one after the other), so its CTAs get more threads and each thread fewer
+// elements per stage; a level with tiles enough to fill the GPU keeps 256.
+static int level_threads(int w, int h) {
+    long tiles_n = (long)((w + 31) / 32) * ((h + 31) / 32);
+    return tiles_n <= 148 ? 1024 : tiles_n <= 296 ? 512 : 256;
+}
+
 int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, const tw_flow_settings& s, const Geo& g,
                       float* out, float* out_t, DevBuf* scratch) {
     if (s.prep_contrast_edge || s.prep_delinearize)
@@ -316,7 +325,7 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
     size_t pf = pyramid_floats(g);
     for (int i = 0; i < g.levels; i++) {
         int lw = g.sizes[i][0], lh = g.sizes[i][1];
-        LAUNCHB(ctx, 16.0 * lw * lh, k_blur5_band, tiles(lw, lh), FUSED_THREADS, 0, cur, (const void*)nullptr, fmt, 0, lw,
+        LAUNCHB(ctx, 16.0 * lw * lh, k_blur5_band, tiles(lw, lh), level_threads(lw, lh), 0, cur, (const void*)nullptr, fmt, 0, lw,
                 lh, af, tmp, out + off, out_t ? out_t + off : (float*)nullptr);
         if (i + 1 < g.levels) {
             int nw = g.sizes[i + 1][0], nh = g.sizes[i + 1][1];
@@ -386,12 +395,12 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
         const float* AT = xt + offs[l];
         const float* BT = yt + offs[l];
         double px = (double)w * h;
-        LAUNCHB(ctx, 24.0 * px, k_level_init, tiles(w, h), FUSED_THREADS, level_init_smem(), A, w, h, ctx->g7, af, gx, gy,
-                a0, a1, a2);
+        int lt = level_threads(w, h);
+        LAUNCHB(ctx, 24.0 * px, k_level_init, tiles(w, h), lt, level_init_smem(), A, w, h, ctx->g7, af, gx, gy, a0, a1, a2);
         for (int it = 0; it < 3; it++) {
             // I1, I0 (gather), grad, tensor, flow in; flow out
-            LAUNCHB(ctx, 4.0 * px * 12, k_level_iter, tiles(w, h), FUSED_THREADS, level_iter_smem(), A, B, gx, gy, a0, a1,
-                    a2, fu, fv, w, h, ctx->g7, ctx->g5, af, nu, nv);
+            LAUNCHB(ctx, 4.0 * px * 12, k_level_iter, tiles(w, h), lt, level_iter_smem(), A, B, gx, gy, a0, a1, a2, fu, fv,
+                    w, h, ctx->g7, ctx->g5, af, nu, nv);
             std::swap(fu, nu);
             std::swap(fv, nv);
             if (it == 1 && l == 0 && !s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h);
@@ -848,6 +857,14 @@ size_t tw_profile_report(tw_ctx* ctx, char* buf, size_t cap) {
         buf[m] = 0;
     }
     return out.size();
+}
+
+int tw_set_lanes(tw_ctx* ctx, int32_t lanes) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (lanes < 1 || lanes > MAX_LANES) return ctx->fail(TW_ERR_BAD_PARAM, "lanes %d is not in 1..%d", lanes, MAX_LANES);
+    ctx->nlanes = lanes;
+    return TW_OK;
 }
 
 int tw_set_stream(tw_ctx* ctx, void* stream) {
@@ -1630,7 +1647,7 @@ template <typename Src, typename FrameFn>
 static int clip_host(tw_ctx* ctx, const void* frames, int nframes, int nout, int W, int H, int fmt, void* out, Src src,
                      FrameFn frame_fn) {
     size_t bytes = (size_t)W * H * 4 * sample_bytes(fmt);
-    const int nl = std::min(MAX_LANES, 3);
+    const int nl = std::min(MAX_LANES, std::max(1, ctx->nlanes));
     const int NS = tw_ctx::CACHE_SLOTS;
     if (!ctx->up) {
         CHECK(ctx->cuda(cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking), "copy stream"));
@@ -1844,7 +1861,7 @@ int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* 
     if (!s || !sels || !frames || !out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
         return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
     size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
-    const int nl = std::min(MAX_LANES, 3);
+    const int nl = std::min(MAX_LANES, std::max(1, ctx->nlanes));
     CHECK(lanes_begin(ctx, nl));
     int rc = TW_OK;
     for (int k = 0; k < nout && rc == TW_OK; k++) {
