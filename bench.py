@@ -40,7 +40,7 @@ SPEED = 40.0
 FRAMES_PER_STEP = 10
 METRIC = "1080p retime output frames/s (strict byte-exact GPU vs CPU)"
 WORKLOAD = "retime 1920x1080 8bpc RGBA, speed 40%, defaults (vectors Best, Blend, sensitivity 70)"
-ROOFLINE_KERNEL = os.environ.get("TW_ROOFLINE_KERNEL", "k_level_iter")
+ROOFLINE_KERNEL = os.environ.get("TW_ROOFLINE_KERNEL", "k_bm_rows")
 CLIP_KW = dict(seed=0x74570002, bg_velocity=(6.0, -3.0), square=240, square_start=(600.0, 400.0),
                square_velocity=(9.0, 4.0))
 

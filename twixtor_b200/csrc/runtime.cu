@@ -154,6 +154,7 @@ struct DevBuf {
 // the context's stream, with the algorithmic bytes each launch moves.
 struct KernelProfile {
     bool on = false;
+    size_t pooled = 0;            // events of the context's pool in use by this session
     std::string name;             // one kernel, or "*" for every kernel
     std::vector<cudaEvent_t> ev;  // start, stop pairs
     std::vector<std::string> who; // the kernel of each pair
@@ -201,6 +202,7 @@ struct tw_ctx {
     // engine images, wire staging, pyramids, solve work, flows
     DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags, holes, fill;
     DevBuf host_stage;  // unused placeholder for pinned staging
+    std::vector<cudaEvent_t> ev_pool;  // the profiler's events (KernelProfile)
     // the forward warp: vertices, mip pyramid, per pixel counts / offsets, hit lists, flags
     DevBuf logf_tab, fw_vx, fw_vy, fw_vd, fw_pyr, fw_tmp[2], fw_cnt, fw_off, fw_fill, fw_sums, fw_keys, fw_cols,
         fw_scratch, fw_longq, fw_flags, fw_out, fw_cov;
@@ -228,9 +230,15 @@ namespace {
 bool prof_match(tw_ctx* ctx, const char* kernel) {
     return ctx->prof.on && (ctx->prof.name == kernel || ctx->prof.name == "*");
 }
+// Events come from a pool that the context keeps (created before a profiled region, reused by
+// every session), so a profiled launch costs two event records, no event creation.
 void prof_mark(tw_ctx* ctx) {
-    cudaEvent_t e;
-    cudaEventCreate(&e);
+    if (ctx->prof.pooled == ctx->ev_pool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        ctx->ev_pool.push_back(e);
+    }
+    cudaEvent_t e = ctx->ev_pool[ctx->prof.pooled++];
     cudaEventRecord(e, ctx->cur);
     ctx->prof.ev.push_back(e);
 }
@@ -769,7 +777,7 @@ void tw_close(tw_ctx* ctx) {
     if (ctx->up) cudaStreamDestroy(ctx->up);
     if (ctx->down) cudaStreamDestroy(ctx->down);
     if (ctx->own) cudaStreamDestroy(ctx->own);
-    for (auto e : ctx->prof.ev) cudaEventDestroy(e);
+    for (auto e : ctx->ev_pool) cudaEventDestroy(e);
     delete ctx;
 }
 
@@ -795,10 +803,14 @@ int tw_profile_begin(tw_ctx* ctx, const char* kernel) {
     if (!ctx || !kernel) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cur = ctx->stream;
-    for (auto e : ctx->prof.ev) cudaEventDestroy(e);
     ctx->prof = KernelProfile();
     ctx->prof.on = true;
     ctx->prof.name = kernel;
+    while (ctx->ev_pool.size() < 8192) {  // enough for a timed region of a few thousand launches
+        cudaEvent_t e;
+        CHECK(ctx->cuda(cudaEventCreate(&e), "profile events"));
+        ctx->ev_pool.push_back(e);
+    }
     return TW_OK;
 }
 
@@ -816,7 +828,6 @@ int tw_profile_end(tw_ctx* ctx, double* total_ms, uint64_t* launches, double* by
     if (total_ms) *total_ms = ms;
     if (launches) *launches = ctx->prof.launches;
     if (bytes) *bytes = ctx->prof.bytes;
-    for (auto e : ctx->prof.ev) cudaEventDestroy(e);
     ctx->prof = KernelProfile();
     return TW_OK;
 }
