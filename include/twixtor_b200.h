@@ -171,6 +171,15 @@ int tw_flow_geometry(const tw_flow_settings* s, int32_t width, int32_t height, i
  * Backend::solve (device/exec/backend.rs:29). */
 int tw_solve(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_flow_settings* s, tw_flow* out);
 
+/* flow::extras::solve_pyramids_with (flow/extras.rs:244-265) with the mask pyramids of a layer
+ * (MaskPyramid::build_ungated, extras.rs:130-134, the masks the layered effects build): X(p) ~
+ * Y(p + out(p)) with X's gradient masked by X's binary level mask and the B step gated by the
+ * warped level mask of Y (flow.rs:737-845). matte_x, matte_y: width*height values 0..1 (the layer's
+ * effective matte at X and at Y), both NULL for the plain solve. Replaces
+ * Backend::solve_pyramids_with (device/exec/backend.rs:33) for the layers without tracking points. */
+int tw_solve_masked(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_flow_settings* s, const float* matte_x,
+                    const float* matte_y, tw_flow* out);
+
 /* flow::solve_pair (flow.rs:1347-1353): f_ab = solve(A, B), f_ba = solve(B, A), the pyramids built
  * once. Replaces Backend::solve_pair (device/exec/backend.rs:31). */
 int tw_solve_pair(tw_ctx* ctx, const tw_image* a, const tw_image* b, const tw_flow_settings* s, tw_flow* f_ab,

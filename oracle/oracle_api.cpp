@@ -525,6 +525,62 @@ int or_retime_clip(const void* frames, int nframes, int w, int h, int fmt, const
     return 0;
 }
 
+// ---- the masked solve of the layered paths (flow/extras.rs) -----------------------------------------
+
+int or_mask_pyramid(const float* matte, int w, int h, int quality, int hiq, int above_first, float* out, int* sizes,
+                    int cap_levels) {
+    FlowSettings s;
+    s.quality = quality;
+    s.hiq = hiq != 0;
+    s.taps_above_first = above_first != 0;
+    std::vector<Plane> lv;
+    std::string e;
+    if (!mask_pyramid(matte, w, h, s, &lv, &e)) return -fail(1, e);
+    size_t off = 0;
+    for (size_t i = 0; i < lv.size() && (int)i < cap_levels; i++) {
+        sizes[2 * i] = lv[i].w;
+        sizes[2 * i + 1] = lv[i].h;
+        std::memcpy(out + off, lv[i].d.data(), lv[i].d.size() * 4);
+        off += lv[i].d.size();
+    }
+    return (int)lv.size();
+}
+
+void or_mask_gradient(float* grad, const float* mask, int w, int h) { mask_gradient(grad, mask, w, h); }
+
+void or_calc_b_masked(const float* i1, const float* i0, const float* grad, const float* flow, int w, int h,
+                      const float* mask_y, float* out) {
+    std::vector<float> b = calc_b_masked(i1, i0, grad, flow, w, h, mask_y);
+    std::memcpy(out, b.data(), b.size() * 4);
+}
+
+void or_block_match_gated(const float* a, const float* b, float* flow, int w, int h, const float* gate) {
+    block_match_gated(a, b, flow, w, h, gate);
+}
+
+// flow/extras.rs:244-265 with the mask pyramids of two mattes (0..1 at the image size, either may
+// be null: no masks) and the block matching gate on or off; out: the flow at the working size
+int or_solve_masked(const void* x_eng, const void* y_eng, int w, int h, int fmt, int quality, int hiq, float sensitivity,
+                    int above_first, const float* matte_x, const float* matte_y, int gate, float* out) {
+    Image x(w, h, (Fmt)fmt), y(w, h, (Fmt)fmt);
+    std::memcpy(x.data(), x_eng, x.bytes());
+    std::memcpy(y.data(), y_eng, y.bytes());
+    FlowSettings s;
+    s.quality = quality;
+    s.hiq = hiq != 0;
+    s.sensitivity = sensitivity;
+    s.taps_above_first = above_first != 0;
+    Pyramid px, py;
+    std::string e;
+    if (!build_pyramid(x, s, &px, &e) || !build_pyramid(y, s, &py, &e)) return fail(1, e);
+    std::vector<Plane> mx, my;
+    bool masks = matte_x && matte_y;
+    if (masks && (!mask_pyramid(matte_x, w, h, s, &mx, &e) || !mask_pyramid(matte_y, w, h, s, &my, &e))) return fail(1, e);
+    FlowField f = solve_pyramids_masked(px, py, s, masks ? &mx : nullptr, masks ? &my : nullptr, gate != 0);
+    std::memcpy(out, f.d.data(), f.d.size() * 4);
+    return 0;
+}
+
 // ---- Create Vectors (plugins/create-vectors/src/glue.rs:488-569, one layer, Display Motion Vectors)
 
 struct or_cv_params {

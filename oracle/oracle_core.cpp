@@ -653,7 +653,16 @@ static inline bool bm_step(const float* a, const float* b, int w, int h, int x, 
 }
 
 void block_match(const float* a, const float* b, float* flow, int w, int h) {  // flow.rs:551-622
+    block_match_gated(a, b, flow, w, h, nullptr);
+}
+
+// flow.rs:1225-1245 without wrap: a pixel whose gate value is below 0.95 keeps its vector
+void block_match_gated(const float* a, const float* b, float* flow, int w, int h, const float* gate) {
     if (w < 3 || h < 3) return;
+    auto bm_step = [&](const float* A, const float* B, int W, int H, int x, int y, const float* cur, float* nb) {
+        if (gate && gate[(long)y * W + x] < 0.95f) return false;
+        return ::orc::bm_step(A, B, W, H, x, y, cur, nb);
+    };
     OMP_FOR
     for (int y = 1; y <= h - 2; y++) {
         float* row = flow + (long)y * w * 2;
@@ -695,8 +704,85 @@ void block_match(const float* a, const float* b, float* flow, int w, int h) {  /
     }
 }
 
+// flow.rs:743-761 (wrap off): the gradient is zero where the level mask is below 0.95 at the pixel
+// or at one of its four neighbours that exist
+void mask_gradient(float* grad, const float* mask, int w, int h) {
+    OMP_FOR
+    for (int y = 0; y < h; y++) {
+        auto off = [&](int xx, int yy) { return mask[(long)yy * w + xx] < 0.95f; };
+        for (int x = 0; x < w; x++) {
+            bool out = off(x, y) || (y >= 1 && off(x, y - 1)) || (y + 1 < h && off(x, y + 1)) || (x >= 1 && off(x - 1, y)) ||
+                       (x + 1 < w && off(x + 1, y));
+            if (out) { grad[((long)y * w + x) * 2] = 0.0f; grad[((long)y * w + x) * 2 + 1] = 0.0f; }
+        }
+    }
+}
+
+// flow.rs:777-845 (wrap off): calc_b with the warped mask of Y at least 0.999 at the target
+std::vector<float> calc_b_masked(const float* i1, const float* i0, const float* grad, const float* flow, int w, int h,
+                                 const float* mask_y) {
+    std::vector<float> b((size_t)w * h * 2, 0.0f);
+    float fw = (float)w, fh = (float)h;
+    OMP_FOR
+    for (int y = 0; y < h; y++) {
+        float fy = (float)y;
+        for (int x = 0; x < w; x++) {
+            float fx = (float)x;
+            long i = (long)y * w + x;
+            float sx = fx - flow[i * 2], sy = fy - flow[i * 2 + 1];
+            bool inside = !(sx < 0.0f || fw - 1.0f < sx || sy < 0.0f || fh - 1.0f < sy);
+            bool pass = inside && (!mask_y || bilinear1(mask_y, w, h, sx, sy) >= 0.999f);
+            if (pass) {
+                float r = bilinear1(i0, w, h, sx, sy) - i1[i];
+                b[i * 2] = r * grad[i * 2];
+                b[i * 2 + 1] = r * grad[i * 2 + 1];
+            }
+        }
+    }
+    return b;
+}
+
+static void binarize(Plane& p) {  // flow/extras.rs:64-72 (a NaN gives 0)
+    for (auto& v : p.d) v = v >= 0.95f ? 1.0f : 0.0f;
+}
+
+// flow/extras.rs:76-123: the binary mask pyramid of a matte (values 0..1, the output size)
+bool mask_pyramid(const float* matte, int w, int h, const FlowSettings& s, std::vector<Plane>* levels, std::string* err) {
+    Geometry g;
+    if (!geometry(s, w, h, &g, err)) return false;
+    Plane cur(w, h);
+    std::memcpy(cur.d.data(), matte, sizeof(float) * (size_t)w * h);
+    binarize(cur);
+    auto step = [&](const Plane& p, int nw, int nh) {
+        Plane t = p;
+        blur5(t.d.data(), t.w, t.h, s.taps_above_first);
+        Plane r = resample1(t, nw, nh);
+        binarize(r);
+        return r;
+    };
+    for (int i = 0; i < g.reduction; i++) cur = step(cur, cur.w / 2, cur.h / 2);
+    levels->clear();
+    for (int i = 0; i < g.levels; i++) {
+        Plane next;
+        bool has_next = i + 1 < g.levels;
+        if (has_next) next = step(cur, g.sizes[i + 1].first, g.sizes[i + 1].second);
+        levels->push_back(std::move(cur));
+        if (!has_next) break;
+        cur = std::move(next);
+    }
+    return true;
+}
+
 // flow.rs:1258-1307
 FlowField solve_pyramids(const Pyramid& x, const Pyramid& y, const FlowSettings& s) {
+    return solve_pyramids_masked(x, y, s, nullptr, nullptr, false);
+}
+
+// flow/extras.rs:244-430 without user displacement and wrap: the plain driver with the gradient
+// masked by X's level mask, the B step gated by Y's warped level mask, and (gate) the block
+// matching sweeps gated by X's mask. With no masks it is the plain driver.
+FlowField solve_pyramids_masked(const Pyramid& x, const Pyramid& y, const FlowSettings& s, const std::vector<Plane>* mx,
+                                const std::vector<Plane>* my, bool gate) {
     const Geometry& geo = x.geo;
     int levels = geo.levels;
     int start; float damp;
@@ -708,17 +794,22 @@ FlowField solve_pyramids(const Pyramid& x, const Pyramid& y, const FlowSettings&
         int w = geo.sizes[l].first, h = geo.sizes[l].second;
         const float* img_a = x.levels[l].d.data();
         const float* img_b = y.levels[l].d.data();
+        const float* mask_x = mx ? (*mx)[l].d.data() : nullptr;
+        const float* mask_y = my ? (*my)[l].d.data() : nullptr;
+        const float* g8 = gate ? mask_x : nullptr;
         std::vector<float> grad = calc_grad(img_a, w, h);
+        if (mask_x) mask_gradient(grad.data(), mask_x, w, h);
         std::vector<float> a = calc_a(grad, w, h);
         blur_gaussian(a.data(), w, h, 3, 7.0f, s.taps_above_first);
         for (int it = 0; it < 3; it++) {
-            std::vector<float> b = calc_b(img_a, img_b, grad.data(), flow.data(), w, h);
+            std::vector<float> b = mask_y ? calc_b_masked(img_a, img_b, grad.data(), flow.data(), w, h, mask_y)
+                                          : calc_b(img_a, img_b, grad.data(), flow.data(), w, h);
             blur_gaussian(b.data(), w, h, 2, 7.0f, s.taps_above_first);
             new_disp(flow.data(), a.data(), b.data(), (size_t)w * h);
             blur_gaussian(flow.data(), w, h, 2, 5.0f, s.taps_above_first);
-            if (it == 1 && l == 0 && !s.skip_refine) block_match(img_a, img_b, flow.data(), w, h);
+            if (it == 1 && l == 0 && !s.skip_refine) block_match_gated(img_a, img_b, flow.data(), w, h, g8);
         }
-        if (l != 0 && !s.skip_refine) block_match(img_a, img_b, flow.data(), w, h);
+        if (l != 0 && !s.skip_refine) block_match_gated(img_a, img_b, flow.data(), w, h, g8);
         if (check) {
             if (all_flow_out_of_range(flow.data(), w, h)) std::fill(flow.begin(), flow.end(), 0.0f);
             else check = false;

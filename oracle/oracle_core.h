@@ -175,7 +175,14 @@ void scale_values(float* d, size_t n, float f);
 bool all_flow_out_of_range(const float* flow, int w, int h);
 float block_cost(const float* a, const float* b, int w, int h, const float p[9], float x2, float y2, bool* some);
 void block_match(const float* a, const float* b, float* flow, int w, int h);
+void block_match_gated(const float* a, const float* b, float* flow, int w, int h, const float* gate);
+void mask_gradient(float* grad, const float* mask, int w, int h);
+std::vector<float> calc_b_masked(const float* i1, const float* i0, const float* grad, const float* flow, int w, int h,
+                                 const float* mask_y);
+bool mask_pyramid(const float* matte, int w, int h, const FlowSettings& s, std::vector<Plane>* levels, std::string* err);
 FlowField solve_pyramids(const Pyramid& x, const Pyramid& y, const FlowSettings& s);
+FlowField solve_pyramids_masked(const Pyramid& x, const Pyramid& y, const FlowSettings& s, const std::vector<Plane>* mx,
+                                const std::vector<Plane>* my, bool gate);
 bool solve(const Image& x, const Image& y, const FlowSettings& s, FlowField* out, std::string* err);
 bool solve_pair(const Image& a, const Image& b, const FlowSettings& s, FlowField* f_ab, FlowField* f_ba,
                 std::string* err);

@@ -27,6 +27,10 @@ Writes, next to this script:
   ``f1_gen.py``).
 * ``f2_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/f2_cases.hex``
   (the reference's numpy model of the textured forward warp; format in its ``f2_gen.py``).
+* ``mask_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/mask_cases.hex``
+  (the reference's numpy models of the solver hooks of the layered solve: mask pyramid, gradient
+  masking, the B step with the warped mask test, the gated block matching; format in its
+  ``gen_mask.py``).
 * ``warp_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/warp_cases.hex``
   (the reference's bit-exact numpy model of the inverse warp; format in its ``gen_warp.py``).
 
@@ -165,6 +169,12 @@ def main():
     with gzip.open(os.path.join(HERE, "f2_cases.bin.gz"), "wb") as f:
         f.write(blob)
     print(f"f2_cases.bin.gz: {len(blob)} bytes, sha256 {hashlib.sha256(blob).hexdigest()}")
+
+    txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "mask_cases.hex")).read()
+    blob = bytes.fromhex("".join(txt.split()))
+    with gzip.open(os.path.join(HERE, "mask_cases.bin.gz"), "wb") as f:
+        f.write(blob)
+    print(f"mask_cases.bin.gz: {len(blob)} bytes, sha256 {hashlib.sha256(blob).hexdigest()}")
 
     txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "warp_cases.hex")).read()
     blob = bytes.fromhex("".join(txt.split()))

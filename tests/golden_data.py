@@ -82,6 +82,59 @@ def f2_cases():
     return out
 
 
+def mask_cases():
+    """The reference's models of the layered solve's hooks (mask_cases.hex; format in its gen_mask.py):
+    dicts with kind 1 (mask pyramid), 2 (gradient masking), 3 (B step), 4 (block matching)."""
+    blob = gzip.open(os.path.join(GOLDEN, "mask_cases.bin.gz")).read()
+    assert blob[:4] == b"MSK1"
+    p = 8
+    n = struct.unpack_from("<I", blob, 4)[0]
+
+    def u32():
+        nonlocal p
+        v = struct.unpack_from("<I", blob, p)[0]
+        p += 4
+        return v
+
+    def f32s(k):
+        nonlocal p
+        v = np.frombuffer(blob[p:p + 4 * k], np.float32).copy()
+        p += 4 * k
+        return v
+
+    out = []
+    for _ in range(n):
+        kind = u32()
+        if kind == 1:
+            w, h, q, hiq = u32(), u32(), u32(), u32()
+            matte = f32s(w * h)
+            levels = []
+            for _ in range(u32()):
+                lw, lh = u32(), u32()
+                levels.append((lw, lh, f32s(lw * lh)))
+            out.append(dict(kind=1, w=w, h=h, quality=q, hiq=hiq, matte=matte, levels=levels))
+        elif kind == 2:
+            w, h, wrap, has = u32(), u32(), u32(), u32()
+            img = f32s(w * h)
+            mask = f32s(w * h) if has else None
+            out.append(dict(kind=2, w=w, h=h, wrap=wrap, img=img, mask=mask, want=f32s(w * h * 2)))
+        elif kind == 3:
+            w, h, wrap, has = u32(), u32(), u32(), u32()
+            i1, i0, grad, flow = f32s(w * h), f32s(w * h), f32s(w * h * 2), f32s(w * h * 2)
+            mask = f32s(w * h) if has else None
+            out.append(dict(kind=3, w=w, h=h, wrap=wrap, i1=i1, i0=i0, grad=grad, flow=flow, mask=mask,
+                            want=f32s(w * h * 2)))
+        elif kind == 4:
+            w, h, wrap, has = u32(), u32(), u32(), u32()
+            a, b, flow = f32s(w * h), f32s(w * h), f32s(w * h * 2)
+            gate = f32s(w * h) if has else None
+            out.append(dict(kind=4, w=w, h=h, wrap=wrap, a=a, b=b, flow=flow, gate=gate, want=f32s(w * h * 2)))
+        else:
+            raise ValueError(kind)
+    assert p == len(blob)
+    return out
+
+
 def f1_cases():
     """The reference's Smart Blend and hole fill model fixtures (f1_cases.hex; format in its f1_gen.py)."""
     blob = gzip.open(os.path.join(GOLDEN, "f1_cases.bin.gz")).read()

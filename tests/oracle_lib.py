@@ -89,6 +89,11 @@ def lib():
         L.or_fw_level_count.argtypes = [i, i]
         L.or_fw_triangle.argtypes = [P, i, i, P, i]
         L.or_logf.argtypes = [P, P, ctypes.c_long]
+        L.or_mask_pyramid.argtypes = [P, i, i, i, i, i, P, P, i]
+        L.or_mask_gradient.argtypes = [P, P, i, i]
+        L.or_calc_b_masked.argtypes = [P, P, P, P, i, i, P, P]
+        L.or_block_match_gated.argtypes = [P, P, P, i, i, P]
+        L.or_solve_masked.argtypes = [P, P, i, i, i, i, i, f, i, P, P, i, P]
         L.or_create_vectors_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(CvParams), i, P]
         L.or_encode_vectors.argtypes = [P, i, i, i, P, i, i, f]
         _lib = L
@@ -214,6 +219,37 @@ def encode_vectors(flow, fw, fh, w, h, fmt, scale):
     if rc:
         raise ValueError(err())
     return out
+
+
+def mask_pyramid(matte, w, h, quality=4, hiq=True, above_first=True):
+    """flow/extras.rs MaskPyramid::build: the binary mask levels (finest first) as (w, h, values)."""
+    out = np.zeros(2 * w * h + 64, np.float32)
+    sizes = np.zeros(64, np.int32)
+    n = lib().or_mask_pyramid(ptr(np.ascontiguousarray(matte, np.float32)), w, h, quality, int(hiq), int(above_first),
+                              ptr(out), ptr(sizes), 32)
+    if n < 0:
+        raise ValueError(err())
+    levels, off = [], 0
+    for i in range(n):
+        lw, lh = int(sizes[2 * i]), int(sizes[2 * i + 1])
+        levels.append((lw, lh, out[off:off + lw * lh].copy()))
+        off += lw * lh
+    return levels
+
+
+def solve_masked(x, y, w, h, fmt, matte_x=None, matte_y=None, quality=4, hiq=True, sensitivity=0.7, above_first=True,
+                 gate=False):
+    """flow::extras::solve_pyramids_with with the mask pyramids of two mattes: the flow of X -> Y."""
+    _, sizes = geometry(quality, hiq, w, h)
+    fw, fh = sizes[0]
+    out = np.zeros(fw * fh * 2, np.float32)
+    mx = None if matte_x is None else np.ascontiguousarray(matte_x, np.float32)
+    my = None if matte_y is None else np.ascontiguousarray(matte_y, np.float32)
+    rc = lib().or_solve_masked(ptr(x), ptr(y), w, h, fmt, quality, int(hiq), np.float32(sensitivity), int(above_first),
+                               ptr(mx), ptr(my), int(gate), ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out, (fw, fh)
 
 
 def forward_warp(src, w, h, fmt, flow, fw, fh, amount, pyramid=True, coverage=False):

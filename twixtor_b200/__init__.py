@@ -279,6 +279,7 @@ def library():
     L.tw_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float]
     L.tw_smart_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float, i32]
     L.tw_set_lanes.argtypes = [P, i32]
+    L.tw_solve_masked.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), P, P, pflow]
     L.tw_forward_warp.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, P]
     L.tw_encode_vectors.argtypes = [P, pimg, pflow, ctypes.c_float]
     L.tw_create_vectors.argtypes = [P, ctypes.POINTER(_VectorsSettings), pimg, pimg, pimg]
@@ -532,6 +533,21 @@ class Device:
             out = np.zeros(nout * fs, DTYPES[fmt])
         self._check(self._L.tw_create_vectors_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes, _ptr(pairs),
                                                    nout, width, height, fmt, _ptr(out)))
+        return out
+
+    def solve_masked(self, x, y, width, height, fmt, settings: FlowSettings, matte_x=None, matte_y=None):
+        """``flow::extras::solve_pyramids_with`` with the (ungated) mask pyramids of a layer's mattes
+        (``width * height`` values 0..1 at X and at Y): the flow X -> Y at the working size."""
+        _, _, sizes = flow_geometry(settings, width, height)
+        fw, fh = sizes[0]
+        out = np.zeros(fw * fh * 2, np.float32)
+        xi, xa = _img(x, width, height, fmt)
+        yi, ya = _img(y, width, height, fmt)
+        fl = _Flow(fw, fh, out.ctypes.data)
+        mx = None if matte_x is None else np.ascontiguousarray(matte_x, np.float32)
+        my = None if matte_y is None else np.ascontiguousarray(matte_y, np.float32)
+        self._check(self._L.tw_solve_masked(self._h, ctypes.byref(xi), ctypes.byref(yi), ctypes.byref(settings._c()),
+                                            _ptr(mx), _ptr(my), ctypes.byref(fl)))
         return out
 
     def set_lanes(self, lanes):

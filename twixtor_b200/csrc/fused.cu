@@ -149,10 +149,13 @@ __global__ void __launch_bounds__(FT_THREADS) k_blur5_band(const float* __restri
 
 // ---- one solver level: gradient, tensor and its blur (flow.rs:1275-1277) ---------------------------
 
+// mask (may be null): the level mask of X of a layered solve; the gradient is zero where the mask
+// is below 0.95 at the pixel or at one of its four neighbours that exist (flow.rs:743-761)
 __global__ void __launch_bounds__(FT_THREADS) k_level_init(const float* __restrict__ img, int w, int h, Taps g7,
                                                            bool above_first, float* __restrict__ gxo,
                                                            float* __restrict__ gyo, float* __restrict__ a0o,
-                                                           float* __restrict__ a1o, float* __restrict__ a2o) {
+                                                           float* __restrict__ a1o, float* __restrict__ a2o,
+                                                           const float* __restrict__ mask) {
     constexpr int N = 8, HALO = N - 1;
     constexpr int RW = FT_X + 2 * HALO, RH = FT_Y + 2 * HALO;
     extern __shared__ float sm[];
@@ -173,6 +176,14 @@ __global__ void __launch_bounds__(FT_THREADS) k_level_init(const float* __restri
             if (x + 1 <= w - 1) { nx = nx + (__ldg(img + i + 1) - cc); dx = dx + 1.0f; }
             if (y + 1 <= h - 1) { ny = ny + (__ldg(img + i + w) - cc); dy = dy + 1.0f; }
             float gx = nx / dx, gy = ny / dy;
+            if (mask) {
+                auto off = [&](long j) { return __ldg(mask + j) < 0.95f; };
+                if (off(i) || (y >= 1 && off(i - w)) || (y + 1 < h && off(i + w)) || (x >= 1 && off(i - 1)) ||
+                    (x + 1 < w && off(i + 1))) {
+                    gx = 0.0f;
+                    gy = 0.0f;
+                }
+            }
             t0 = gx * gx;  // flow.rs:319-328
             t1 = gx * gy;
             t2 = gy * gy;
@@ -210,6 +221,7 @@ size_t level_init_smem() {
 }
 
 // ---- one solver iteration (flow.rs:1278-1282): calc_b, blur7 of B, new_disp, blur5 of the flow -----
+// mask_y (may be null): the level mask of Y of a layered solve
 
 // Halos: the flow's blur5 needs new_disp on the tile + 5; new_disp needs blurred B there, which
 // needs B on the tile + 12.
@@ -232,7 +244,8 @@ __global__ void __launch_bounds__(FT_THREADS) k_level_iter(const float* __restri
                                                            const float* __restrict__ a2, const float* __restrict__ fu,
                                                            const float* __restrict__ fv, int w, int h, Taps g7, Taps g5,
                                                            bool above_first, float* __restrict__ fu_out,
-                                                           float* __restrict__ fv_out) {
+                                                           float* __restrict__ fv_out,
+                                                           const float* __restrict__ mask_y) {
     extern __shared__ float sm[];
     float* s_b = sm;                                  // 2 x IT_BH x IT_BW
     float* s_h = s_b + 2 * IT_BH * IT_BW;             // 2 x IT_BH x IT_DW
@@ -251,7 +264,9 @@ __global__ void __launch_bounds__(FT_THREADS) k_level_iter(const float* __restri
             long i = (long)y * w + x;
             float sx = (float)x - __ldg(fu + i);
             float sy = (float)y - __ldg(fv + i);
-            if (!(sx < 0.0f || fw - 1.0f < sx || sy < 0.0f || fh - 1.0f < sy)) {
+            // flow.rs:777-845: in a layered solve the warped mask of Y must be at least 0.999
+            if (!(sx < 0.0f || fw - 1.0f < sx || sy < 0.0f || fh - 1.0f < sy) &&
+                (!mask_y || bilinear1(mask_y, w, h, sx, sy) >= 0.999f)) {
                 float s = bilinear1(i0, w, h, sx, sy);
                 float rr = s - __ldg(i1 + i);
                 b0 = rr * __ldg(gx + i);
@@ -379,4 +394,12 @@ __global__ void k_apply_negate(const float* __restrict__ fu, const float* __rest
     if (isnan(u) || isnan(v)) atomicOr(nan_flag, 1);
 }
 
+}  // namespace tw
+
+namespace tw {
+// flow/extras.rs:64-72: v >= 0.95 gives 1, else 0 (a NaN gives 0), in place
+__global__ void k_binarize(float* __restrict__ p, long n) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = p[i] >= 0.95f ? 1.0f : 0.0f;
+}
 }  // namespace tw

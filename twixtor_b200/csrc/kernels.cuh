@@ -113,13 +113,14 @@ __global__ void k_blur5_band(const float* __restrict__ orig, const void* __restr
                              float* __restrict__ band_t_out);
 __global__ void k_level_init(const float* __restrict__ img, int w, int h, Taps g7, bool above_first,
                              float* __restrict__ gxo, float* __restrict__ gyo, float* __restrict__ a0o,
-                             float* __restrict__ a1o, float* __restrict__ a2o);
+                             float* __restrict__ a1o, float* __restrict__ a2o, const float* __restrict__ mask);
+__global__ void k_binarize(float* __restrict__ p, long n);
 size_t level_init_smem();
 __global__ void k_level_iter(const float* __restrict__ i1, const float* __restrict__ i0, const float* __restrict__ gx,
                              const float* __restrict__ gy, const float* __restrict__ a0, const float* __restrict__ a1,
                              const float* __restrict__ a2, const float* __restrict__ fu, const float* __restrict__ fv,
                              int w, int h, Taps g7, Taps g5, bool above_first, float* __restrict__ fu_out,
-                             float* __restrict__ fv_out);
+                             float* __restrict__ fv_out, const float* __restrict__ mask_y);
 size_t level_iter_smem();
 __global__ void k_apply_upsample(const float* __restrict__ su, const float* __restrict__ sv, int sw, int sh,
                                  const int* __restrict__ any, int l, int start, bool damp_now, float damp,

@@ -200,7 +200,7 @@ struct tw_ctx {
     size_t held = 0;
     Taps g7{}, g5{}, b5{};
     // engine images, wire staging, pyramids, solve work, flows
-    DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags, holes, fill;
+    DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags, holes, fill, masks;
     DevBuf host_stage;  // unused placeholder for pinned staging
     std::vector<cudaEvent_t> ev_pool;  // the profiler's events (KernelProfile)
     // the forward warp: vertices, mip pyramid, per pixel counts / offsets, hit lists, flags
@@ -268,7 +268,7 @@ void prof_mark(tw_ctx* ctx) {
 constexpr int TB = 256;
 // device flags (ints): [0..31] per-level range flags of solve 0, [32..63] of solve 1, [64] NaN in a
 // flow, [65] a warp refused a sample coordinate
-constexpr int FL_ANY0 = 0, FL_ANY1 = 32, FL_NAN = 64, FL_BAD = 65, FL_HOLE = 66, FL_SIDE1 = 67;
+constexpr int FL_ANY0 = 0, FL_ANY1 = 32, FL_NAN = 64, FL_BAD = 65, FL_HOLE = 66, FL_SIDE1 = 67, FL_ONE = 68;
 constexpr size_t FLAGS_BYTES = 128 * sizeof(int);
 
 dim3 grid2(int w, int h) { return dim3((unsigned)((w + TB - 1) / TB), (unsigned)h); }
@@ -374,8 +374,13 @@ void block_match(tw_ctx* ctx, const float* A, const float* B, const float* AT, c
 // result holds a NaN. Per level: one tiled kernel for the gradient and the blurred tensor, one per
 // iteration (calc_b, blur7, new_disp, blur5 in shared memory, the flow ping-ponged), the block
 // matching sweeps, the range check, and the reset / damping fused into the upsample.
+// mx, my (may be null): the binary mask pyramids of a layered solve (flow/extras.rs:386-430), laid
+// out like the band pyramids; the gradient is masked by X's level mask and the B step gated by Y's.
+// The block matching is not gated (the effects build ungated masks, create_vectors.rs:360,
+// layers/plates.rs:360).
 int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float* xt, const float* yt, const Geo& g,
-                       const tw_flow_settings& s, DevBuf& work, float* out, int* any, int* nan_flag) {
+                       const tw_flow_settings& s, DevBuf& work, float* out, int* any, int* nan_flag,
+                       const float* mx = nullptr, const float* my = nullptr) {
     size_t np0 = (size_t)g.w * g.h;
     // planes: gx gy a0 a1 a2 u0 v0 u1 v1 uT vT
     const int NP = 11;
@@ -404,11 +409,14 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
         const float* BT = yt + offs[l];
         double px = (double)w * h;
         int lt = level_threads(w, h);
-        LAUNCHB(ctx, 24.0 * px, k_level_init, tiles(w, h), lt, level_init_smem(), A, w, h, ctx->g7, af, gx, gy, a0, a1, a2);
+        const float* mask_x = mx ? mx + offs[l] : nullptr;
+        const float* mask_y = my ? my + offs[l] : nullptr;
+        LAUNCHB(ctx, 24.0 * px, k_level_init, tiles(w, h), lt, level_init_smem(), A, w, h, ctx->g7, af, gx, gy, a0, a1, a2,
+                mask_x);
         for (int it = 0; it < 3; it++) {
             // I1, I0 (gather), grad, tensor, flow in; flow out
             LAUNCHB(ctx, 4.0 * px * 12, k_level_iter, tiles(w, h), lt, level_iter_smem(), A, B, gx, gy, a0, a1, a2, fu, fv,
-                    w, h, ctx->g7, ctx->g5, af, nu, nv);
+                    w, h, ctx->g7, ctx->g5, af, nu, nv, mask_y);
             std::swap(fu, nu);
             std::swap(fv, nv);
             if (it == 1 && l == 0 && !s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h);
@@ -423,6 +431,52 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
             std::swap(fv, nv);
         } else {
             LAUNCH(ctx, k_apply_negate, grid1((long)np0), TB, 0, fu, fv, (long)np0, any, start, damp_now, damp, out, nan_flag);
+        }
+    }
+    return TW_OK;
+}
+
+// The binary mask pyramid of a matte (flow/extras.rs:76-123): binarize at 0.95, then per reduction
+// step and per level the blur5 (the pyramid's tap order), the corner aligned resample, binarize.
+// matte: w*h values 0..1 on the device (consumed); out: pyramid_floats(g) values, laid out like
+// the band pyramid; scratch: two planes of w*h. `one` points at a nonzero device int (the stack
+// passes run unconditionally).
+int build_mask_pyramid_dev(tw_ctx* ctx, float* matte, int W, int H, const tw_flow_settings& s, const Geo& g, float* out,
+                           float* scratch0, float* scratch1, const int* one) {
+    float* cur = matte;
+    float* tmp = scratch0;
+    float* nxt = scratch1;
+    int dir = s.taps_above_first ? 2 : 1;
+    auto blur5 = [&](float* p, int w, int h) {  // prep::blur5 on one plane: rows into tmp, columns back
+        dim3 gp((unsigned)((w + TB - 1) / TB), (unsigned)h, 1);
+        LAUNCH(ctx, k_stack_pass, gp, TB, 0, p, tmp, w, h, (long)w * h, ctx->b5, 3, 0, 0, one);
+        LAUNCH(ctx, k_stack_pass, gp, TB, 0, tmp, p, w, h, (long)w * h, ctx->b5, 3, dir, 0, one);
+    };
+    auto resample = [&](const float* src, int sw, int sh, float* dst, int dw, int dh) {
+        dim3 gp((unsigned)((dw + TB - 1) / TB), (unsigned)dh, 1);
+        LAUNCH(ctx, k_stack_resample, gp, TB, 0, src, sw, sh, (long)sw * sh, dst, dw, dh, (long)dw * dh, 0, one);
+        LAUNCH(ctx, k_binarize, grid1((long)dw * dh), TB, 0, dst, (long)dw * dh);
+    };
+    int cw = W, ch = H;
+    LAUNCH(ctx, k_binarize, grid1((long)W * H), TB, 0, cur, (long)W * H);
+    for (int r = 0; r < g.reduction; r++) {
+        int nw = cw / 2, nh = ch / 2;
+        blur5(cur, cw, ch);
+        resample(cur, cw, ch, nxt, nw, nh);
+        std::swap(cur, nxt);
+        cw = nw;
+        ch = nh;
+    }
+    size_t off = 0;
+    for (int i = 0; i < g.levels; i++) {
+        int lw = g.sizes[i][0], lh = g.sizes[i][1];
+        CHECK(ctx->cuda(cudaMemcpyAsync(out + off, cur, (size_t)lw * lh * sizeof(float), cudaMemcpyDeviceToDevice, ctx->cur),
+                        "mask level"));
+        off += (size_t)lw * lh;
+        if (i + 1 < g.levels) {
+            blur5(cur, lw, lh);
+            resample(cur, lw, lh, nxt, g.sizes[i + 1][0], g.sizes[i + 1][1]);
+            std::swap(cur, nxt);
         }
     }
     return TW_OK;
@@ -742,7 +796,7 @@ int tw_open(int device, tw_ctx** out) {
 void tw_close(tw_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
+    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->masks, &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
                     &ctx->fw_vd, &ctx->fw_pyr, &ctx->fw_tmp[0], &ctx->fw_tmp[1], &ctx->fw_cnt, &ctx->fw_off,
                     &ctx->fw_fill, &ctx->fw_sums, &ctx->fw_keys, &ctx->fw_cols, &ctx->fw_scratch, &ctx->fw_longq,
                     &ctx->fw_flags, &ctx->fw_out, &ctx->fw_cov})
@@ -955,6 +1009,60 @@ static int solve_common(tw_ctx* ctx, const tw_image* a, const tw_image* b, const
                                  flags + FL_ANY1, flags + FL_NAN));
     if (f_ab) CHECK(ctx->cuda(cudaMemcpyAsync(f_ab->data, ctx->flow[0].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
     if (pair && f_ba) CHECK(ctx->cuda(cudaMemcpyAsync(f_ba->data, ctx->flow[1].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
+    int hf[2];
+    CHECK(finish(ctx, hf, 2));
+    if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "the solved flow holds a NaN");
+    return TW_OK;
+}
+
+int tw_solve_masked(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_flow_settings* s, const float* matte_x,
+                    const float* matte_y, tw_flow* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!out || !out->data || !s) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    if (!matte_x != !matte_y) return ctx->fail(TW_ERR_BAD_PARAM, "a masked solve needs the mattes of both images");
+    CHECK(check_image(ctx, x, "solve"));
+    CHECK(check_image(ctx, y, "solve"));
+    if (!same_shape(x, y))
+        return ctx->fail(TW_ERR_MISMATCH, "optical flow: incompatible inputs (%dx%d fmt %d against %dx%d fmt %d)", x->width,
+                         x->height, x->fmt, y->width, y->height, y->fmt);
+    if (s->wrap) return ctx->fail(TW_ERR_UNSUPPORTED, "the wrap-around (360) solve is not on the device");
+    Geo g;
+    CHECK(geometry(*s, x->width, x->height, &g, &ctx->err));
+    if (out->width != g.w || out->height != g.h) return ctx->fail(TW_ERR_MISMATCH, "flow buffer is not %dx%d", g.w, g.h);
+    int W = x->width, H = x->height;
+    size_t n = (size_t)W * H;
+    CHECK(upload_image(ctx, ctx->eng[0], x));
+    CHECK(upload_image(ctx, ctx->eng[1], y));
+    size_t pf = pyramid_floats(g);
+    CHECK(ctx->ensure(ctx->pyr[0], 2 * pf * 4, "pyramid"));
+    CHECK(ctx->ensure(ctx->pyr[1], 2 * pf * 4, "pyramid"));
+    float* px_ = ctx->pyr[0].as<float>();
+    float* py_ = ctx->pyr[1].as<float>();
+    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, W, H, x->fmt, *s, g, px_, px_ + pf, ctx->plane));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, W, H, y->fmt, *s, g, py_, py_ + pf, ctx->plane));
+    float *mx = nullptr, *my = nullptr;
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
+    if (matte_x) {
+        CHECK(ctx->ensure(ctx->masks, 2 * pf * sizeof(float), "mask pyramids"));
+        CHECK(ctx->ensure(ctx->holes, 4 * n * sizeof(float), "mattes"));
+        float* mt = ctx->holes.as<float>();
+        CHECK(ctx->cuda(cudaMemcpyAsync(mt, matte_x, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), "matte upload"));
+        CHECK(ctx->cuda(cudaMemcpyAsync(mt + n, matte_y, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), "matte upload"));
+        // a nonzero int for the stack passes' "run" flag
+        CHECK(ctx->cuda(cudaMemsetAsync(flags + FL_ONE, 0x01, sizeof(int), ctx->stream), "flags"));
+        mx = ctx->masks.as<float>();
+        my = mx + pf;
+        CHECK(build_mask_pyramid_dev(ctx, mt, W, H, *s, g, mx, mt + 2 * n, mt + 3 * n, flags + FL_ONE));
+        CHECK(build_mask_pyramid_dev(ctx, mt + n, W, H, *s, g, my, mt + 2 * n, mt + 3 * n, flags + FL_ONE));
+    }
+    size_t fb = (size_t)g.w * g.h * 2 * sizeof(float);
+    CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
+    CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, *s, ctx->work[0], ctx->flow[0].as<float>(), flags + FL_ANY0,
+                             flags + FL_NAN, mx, my));
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->flow[0].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
     int hf[2];
     CHECK(finish(ctx, hf, 2));
     if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "the solved flow holds a NaN");
