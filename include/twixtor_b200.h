@@ -232,6 +232,20 @@ int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* 
  * blended at w, or (binary != 0) the binary alpha composite. */
 int tw_smart_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* p1, const tw_image* p2, float w, int32_t binary);
 
+/* The layered composition with plates (layers/plates.rs:330-412, solve_and_compose_plates) of one
+ * in-between frame of the FG matte effects: every layer (FG1 .. FG nfg, then Main_BG) solved on its
+ * own layer images with its solver masks (tw_solve_masked), its plates (its layer image OVER the
+ * other frame's warped to its time) refilled, the single layer composition of the warping code
+ * (codes 0 and 1, Nearest or Blend), and the layers composed OVER from the bottom up. a, b: the
+ * engine images (also the tracking frames); mattes_a / mattes_b: nfg raw mattes of width*height
+ * floats each at A and at B, FG1 first (0..1; a float matte as it is); sensitivity: nfg + 1 values
+ * (0..1), Main_BG last. nfg <= 3. The inverse matte shrink is 0 and no tracking point is in use;
+ * the caller hands the images in the motion path's row order. Replaces the CPU
+ * compose::retime_layers vector path for those settings. */
+int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection* sel, const tw_image* a,
+                      const tw_image* b, int32_t nfg, const float* mattes_a, const float* mattes_b,
+                      const float* sensitivity, tw_image_mut* out);
+
 /* forward::forward_warp_with (forward.rs:229-320) with the coverage image when cov != NULL (w*h
  * bytes, 255 where a triangle covered the pixel): the displaced triangle mesh of the flow
  * rasterised into a running mean, textured from the source's mip pyramid (pyramid != 0, the

@@ -17,6 +17,7 @@
 #include "oracle_smart.h"
 #include "oracle_forward.h"
 #include "oracle_vectors.h"
+#include "oracle_layers.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -578,6 +579,42 @@ int or_solve_masked(const void* x_eng, const void* y_eng, int w, int h, int fmt,
     if (masks && (!mask_pyramid(matte_x, w, h, s, &mx, &e) || !mask_pyramid(matte_y, w, h, s, &my, &e))) return fail(1, e);
     FlowField f = solve_pyramids_masked(px, py, s, masks ? &mx : nullptr, masks ? &my : nullptr, gate != 0);
     std::memcpy(out, f.d.data(), f.d.size() * 4);
+    return 0;
+}
+
+// ---- the layered composition with plates (layers/plates.rs) ------------------------------------------
+
+// One layered output frame: engine images A and B, nfg FG mattes at A and at B (nfg * w * h floats
+// each, FG1 first), nfg + 1 sensitivities (0..1), the selection weight / interpolation and the
+// settings; out: the engine image
+int or_compose_layers(const void* a_eng, const void* b_eng, int w, int h, int fmt, int nfg, const float* mattes_a,
+                      const float* mattes_b, const float* sens, int quality, int hiq, int above_first, int warp_mode,
+                      int video_360, float wa, int interp, void* out_eng) {
+    Image a(w, h, (Fmt)fmt), b(w, h, (Fmt)fmt), out;
+    std::memcpy(a.data(), a_eng, a.bytes());
+    std::memcpy(b.data(), b_eng, b.bytes());
+    LayerJob job;
+    size_t n = (size_t)w * h;
+    for (int j = 0; j < nfg; j++) {
+        job.mattes_a.emplace_back(mattes_a + j * n, mattes_a + (j + 1) * n);
+        job.mattes_b.emplace_back(mattes_b + j * n, mattes_b + (j + 1) * n);
+    }
+    job.sensitivity.assign(sens, sens + nfg + 1);
+    job.fs.quality = quality;
+    job.fs.hiq = hiq != 0;
+    job.fs.video_range_luma = video_360 != 0;
+    job.fs.taps_above_first = above_first != 0;
+    job.cs.warp_mode = warp_mode;
+    job.cs.video_360 = video_360 != 0;
+    job.cs.taps_above_first = above_first != 0;
+    job.sel.wa = wa;
+    job.sel.interp = interp;
+    job.sel.exact = false;
+    job.sel.vectors_quality = quality;
+    std::string e;
+    int rc = compose_layers_plates(job, a, b, &out, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(out_eng, out.data(), out.bytes());
     return 0;
 }
 

@@ -30,7 +30,7 @@ static inline uint16_t q15_to_u16(uint16_t v) {
 }
 
 // image.rs:276-280
-static inline void premultiply_u8(const uint8_t p[4], uint8_t o[4]) {
+void premultiply_u8(const uint8_t p[4], uint8_t o[4]) {
     float a = (float)p[0] * INV_255;
     o[0] = p[0];
     for (int c = 1; c < 4; c++) o[c] = (uint8_t)q((float)p[c] * a);
@@ -42,7 +42,7 @@ static inline void premultiply_u16(const uint16_t p[4], uint16_t o[4]) {
     for (int c = 1; c < 4; c++) o[c] = (uint16_t)q((float)p[c] * a);
 }
 // image.rs:294-303
-static inline void premultiply_f32(const float p[4], float o[4]) {
+void premultiply_f32(const float p[4], float o[4]) {
     float r[4] = {p[0], p[0] * p[1], p[0] * p[2], p[0] * p[3]};
     if (std::isnan(r[1]) || std::isnan(r[2]) || std::isnan(r[3]) || std::isnan(r[0])) {
         r[1] = nr::mul(p[0], p[1]);
@@ -52,7 +52,7 @@ static inline void premultiply_f32(const float p[4], float o[4]) {
     for (int c = 0; c < 4; c++) o[c] = r[c];
 }
 // image.rs:306-320
-static inline void unpremultiply_u8(const uint8_t p[4], uint8_t o[4]) {
+void unpremultiply_u8(const uint8_t p[4], uint8_t o[4]) {
     if (p[0] == 0) { for (int c = 0; c < 4; c++) o[c] = p[c]; return; }
     float s = 255.0f / (float)p[0];
     o[0] = p[0];

@@ -108,6 +108,10 @@ struct Coverage {  // warp.rs:57-97
 
 // wire frames (crates/fx-core/src/frame.rs:79-141): u8 RGBA interleaved, u16 LE RGBA interleaved,
 // f32 planar in the plane order G, B, R, A.
+// image.rs:276-320: the per pixel premultiply / unpremultiply of the boundary
+void premultiply_u8(const uint8_t p[4], uint8_t o[4]);
+void premultiply_f32(const float p[4], float o[4]);
+void unpremultiply_u8(const uint8_t p[4], uint8_t o[4]);
 Image from_frame(const void* wire, int w, int h, Fmt fmt);                  // image.rs:178-206
 void to_frame(const Image& img, void* wire);                                 // image.rs:213-245
 Image rows_reversed(const Image& img);                                       // image.rs:96-114

@@ -1,0 +1,305 @@
+// CPU oracle of the layered composition with plates (plugins/retime-engine/src/layers/plates.rs,
+// matte.rs) for the FG matte layers of retime-fgbg. TEST INFRASTRUCTURE ONLY (see oracle_core.h).
+//
+// Restated scope: warping codes 0 and 1, Nearest and Blend, zero inverse matte shrink (the choke
+// of the cut is then the clamp of the plane), no tracking points, no wrap-around.
+#include "oracle_layers.h"
+
+#include <algorithm>
+#include <cmath>
+
+#include "oracle_smart.h"
+
+namespace orc {
+
+static const float PL_K8 = bits_f(0x3b808081u);   // matte.rs:921
+static const float PL_K16 = bits_f(0x37800080u);  // matte.rs:922
+
+static float white_of(Fmt f) { return f == U8 ? 255.0f : f == U16 ? 65535.0f : 1.0f; }
+
+// Rust's saturating float -> i64 cast (`as i64`: NaN gives 0)
+static int64_t as_i64(float x) {
+    if (std::isnan(x)) return 0;
+    if (x >= 9223372036854775808.0f) return INT64_MAX;
+    if (x < -9223372036854775808.0f) return INT64_MIN;
+    return (int64_t)x;
+}
+
+LPlane raw_plane(const float* m, size_t n, Fmt fmt) {  // plates.rs:50-57
+    LPlane p;
+    p.white = white_of(fmt);
+    p.v.assign(m, m + n);
+    if (fmt == F32) return p;
+    bool in = true;  // matte.rs:106-112 (in_range): the clamp only when a value leaves 0..1
+    for (float x : p.v) in = in && x >= 0.0f && x <= 1.0f;
+    for (float& x : p.v) {
+        float c = x;
+        if (!in) c = x > 1.0f ? 1.0f : (x >= 0.0f ? x : 0.0f);  // matte.rs:94-102
+        x = (float)as_i64(c * p.white + 0.5f);
+    }
+    return p;
+}
+
+static float cut(float c, float v, float white, bool isf) {  // plates.rs:63-78
+    float x = (float)((1.0 - (double)v) * (double)c);
+    if (0.0f > x) x = 0.0f;
+    else if (x > white) x = white;
+    if (isf) return x + 0.0f;
+    return (float)as_i64(x + 0.5f);
+}
+
+static float clamp_pl(float v) {  // matte.rs:350-359
+    if (0.0f > v) return 0.0f;
+    if (v >= 1.0f) return 1.0f;
+    return v;
+}
+
+LPlane comp_plane(const std::vector<LPlane>& raws, int k, Fmt fmt, size_t n) {  // plates.rs:86-97
+    float white = white_of(fmt);
+    bool isf = fmt == F32;
+    LPlane c;
+    c.white = white;
+    if (k == (int)raws.size()) c.v.assign(n, white);
+    else c = raws[k];
+    for (int j = k - 1; j >= 0; j--) {
+        float kk = 1.0f / raws[j].white;  // plates.rs:80-85, the zero shrink: the choke is the clamp
+        for (size_t i = 0; i < n; i++) c.v[i] = cut(c.v[i], clamp_pl(raws[j].v[i] * kk), white, isf);
+    }
+    return c;
+}
+
+Image layer_times(const Image& src, const LPlane& p) {  // plates.rs:128-156
+    Image out(src.w, src.h, src.fmt);
+    size_t n = (size_t)src.w * src.h;
+    for (size_t i = 0; i < n; i++) {
+        for (int c = 0; c < 4; c++) {
+            size_t j = i * 4 + c;
+            if (src.fmt == U8) out.u8[j] = (uint8_t)as_i64((float)src.u8[j] * (p.v[i] * PL_K8) + 0.5f);
+            else if (src.fmt == U16) out.u16[j] = (uint16_t)as_i64((float)src.u16[j] * (p.v[i] * PL_K16) + 0.5f);
+            else out.f32[j] = nr::mul(p.v[i], src.f32[j]);
+        }
+    }
+    return out;
+}
+
+// plates.rs:296-309: 1 where no layer above covers layer k; empty when it is 1 everywhere
+bool solver_mask(const std::vector<LPlane>& raws, const LPlane& comp, int k, size_t n, std::vector<float>* out) {
+    float white = comp.white;
+    out->resize(n);
+    bool all_one = true;
+    for (size_t i = 0; i < n; i++) {
+        float r = k == (int)raws.size() ? white : raws[k].v[i];
+        float v = (white - (r - comp.v[i])) / white;
+        (*out)[i] = v;
+        all_one = all_one && v == 1.0f;
+    }
+    return !all_one;
+}
+
+static void unpremultiply_pl(Image& img) {  // plates.rs:160-187
+    size_t n = (size_t)img.w * img.h;
+    for (size_t i = 0; i < n; i++) {
+        if (img.fmt == U8) {
+            uint8_t o[4];
+            unpremultiply_u8(&img.u8[i * 4], o);
+            for (int c = 0; c < 4; c++) img.u8[i * 4 + c] = o[c];
+        } else if (img.fmt == U16) {
+            uint16_t* p = &img.u16[i * 4];
+            if (p[0] == 0) continue;
+            float inv = 65535.0f / (float)p[0];
+            for (int c = 1; c < 4; c++) {
+                float v = (float)p[c] * inv;
+                if (65535.0f < v) v = 65535.0f;
+                p[c] = (uint16_t)q(v);
+            }
+        } else {
+            float* p = &img.f32[i * 4];
+            if (1e-7 > (double)p[0]) continue;
+            float inv = 1.0f / p[0];
+            for (int c = 1; c < 4; c++) p[c] = nr::mul(inv, p[c]);
+        }
+    }
+}
+
+static void premultiply_pl(Image& img) {  // plates.rs:191-208
+    size_t n = (size_t)img.w * img.h;
+    for (size_t i = 0; i < n; i++) {
+        if (img.fmt == U8) {
+            uint8_t o[4];
+            premultiply_u8(&img.u8[i * 4], o);
+            for (int c = 0; c < 4; c++) img.u8[i * 4 + c] = o[c];
+        } else if (img.fmt == U16) {
+            uint16_t* p = &img.u16[i * 4];
+            float f = (float)p[0] * PL_K16;
+            for (int c = 1; c < 4; c++) p[c] = (uint16_t)q((float)p[c] * f);
+        } else {
+            float o[4];
+            premultiply_f32(&img.f32[i * 4], o);
+            for (int c = 0; c < 4; c++) img.f32[i * 4 + c] = o[c];
+        }
+    }
+}
+
+// plates.rs:245-256: unpremultiply, fill the colour where the plate is not opaque (holes:
+// white - alpha), the alpha replaced by the layer's raw matte plane or (frame != null) the frame's
+// alpha, premultiply
+static int refill(Image& img, const LPlane* plane, const Image* frame, bool above_first, std::string* err) {
+    unpremultiply_pl(img);
+    size_t n = (size_t)img.w * img.h;
+    int rc;
+    if (img.fmt == U8) {
+        std::vector<uint8_t> m(n);
+        for (size_t i = 0; i < n; i++) m[i] = (uint8_t)(0xffu - img.u8[i * 4]);
+        rc = fill_holes(img, m.data(), 1, above_first, err);
+    } else if (img.fmt == U16) {
+        std::vector<uint16_t> m(n);
+        for (size_t i = 0; i < n; i++) m[i] = (uint16_t)(0xffffu - img.u16[i * 4]);
+        rc = fill_holes(img, m.data(), 2, above_first, err);
+    } else {
+        std::vector<float> m(n);
+        for (size_t i = 0; i < n; i++) m[i] = 1.0f - img.f32[i * 4];
+        rc = fill_holes(img, m.data(), 3, above_first, err);
+    }
+    if (rc) return rc;
+    for (size_t i = 0; i < n; i++) {  // plates.rs:211-239 (set_alpha)
+        if (frame) {
+            if (img.fmt == U8) img.u8[i * 4] = frame->u8[i * 4];
+            else if (img.fmt == U16) img.u16[i * 4] = frame->u16[i * 4];
+            else img.f32[i * 4] = frame->f32[i * 4];
+        } else {
+            float v = plane->v[i];
+            if (img.fmt == U8) img.u8[i * 4] = (uint8_t)std::min<int64_t>(std::max<int64_t>(as_i64(v), 0), 255);
+            else if (img.fmt == U16) img.u16[i * 4] = (uint16_t)std::min<int64_t>(std::max<int64_t>(as_i64(v), 0), 65535);
+            else img.f32[i * 4] = v;
+        }
+    }
+    premultiply_pl(img);
+    return 0;
+}
+
+void over_pl(Image& d, const Image& s) {  // matte.rs:923-1030
+    size_t n = (size_t)d.w * d.h;
+    for (size_t i = 0; i < n; i++) {
+        if (d.fmt == U8) {
+            uint8_t* dp = &d.u8[i * 4];
+            const uint8_t* sp = &s.u8[i * 4];
+            uint8_t sa = sp[0];
+            if (sa == 0) continue;
+            if (sa == 255) { for (int c = 0; c < 4; c++) dp[c] = sp[c]; continue; }
+            float saf = (float)sa, f = 1.0f - saf * PL_K8;
+            uint8_t da = dp[0];
+            for (int c = 1; c < 4; c++) dp[c] = (uint8_t)as_i64((float)dp[c] * f + (float)sp[c] + 0.5f);
+            dp[0] = (uint8_t)as_i64((float)(255 - da) * saf * PL_K8 + (float)da + 0.5f);
+        } else if (d.fmt == U16) {
+            uint16_t* dp = &d.u16[i * 4];
+            const uint16_t* sp = &s.u16[i * 4];
+            uint16_t sa = sp[0];
+            if (sa == 0) continue;
+            if (sa == 65535) { for (int c = 0; c < 4; c++) dp[c] = sp[c]; continue; }
+            float saf = (float)sa, f = 1.0f - saf * PL_K16;
+            uint16_t da = dp[0];
+            for (int c = 1; c < 4; c++) dp[c] = (uint16_t)as_i64((float)dp[c] * f + (float)sp[c] + 0.5f);
+            dp[0] = (uint16_t)as_i64((float)(65535 - (int32_t)da) * saf * PL_K16 + (float)da + 0.5f);
+        } else {
+            float* dp = &d.f32[i * 4];
+            const float* sp = &s.f32[i * 4];
+            float sa = sp[0];
+            if (sa == 0.0f) continue;
+            if (sa == 1.0f) { for (int c = 0; c < 4; c++) dp[c] = sp[c]; continue; }
+            float f = nr::sub(1.0f, sa);
+            float da = dp[0];
+            for (int c = 1; c < 4; c++) dp[c] = nr::add(nr::add(nr::mul(f, dp[c]), sp[c]), 0.0f);
+            dp[0] = nr::add(nr::add(nr::mul(nr::sub(1.0f, da), sa), da), 0.0f);
+        }
+    }
+}
+
+static bool nearest_takes_a(int code, float wa) {  // layers.rs:697-703
+    if (code == 0) return 0.5f <= wa;
+    return !(0.5f > wa);
+}
+
+int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, Image* out, std::string* err) {
+    int w = a.w, h = a.h;
+    size_t n = (size_t)w * h;
+    Fmt fmt = a.fmt;
+    int nfg = (int)job.mattes_a.size();
+    std::vector<LPlane> raws_a, raws_b;
+    for (int j = 0; j < nfg; j++) {
+        raws_a.push_back(raw_plane(job.mattes_a[j].data(), n, fmt));
+        raws_b.push_back(raw_plane(job.mattes_b[j].data(), n, fmt));
+    }
+    const Selection& sel = job.sel;
+    int code = job.cs.warp_mode;
+    if (code != 0 && code != 1) { *err = "plates: warping codes 2 and 3 are not restated"; return 2; }
+    if (sel.interp != 0 && sel.interp != 1) { *err = "plates: Weighted Blend is not restated"; return 2; }
+    // plates.rs:330-370: the solves, one layer after the other
+    std::vector<FlowField> f_ab(nfg + 1), f_ba(nfg + 1);
+    std::vector<bool> has_ab(nfg + 1, false), has_ba(nfg + 1, false);
+    for (int k = 0; k <= nfg; k++) {
+        FlowSettings fs = job.fs;
+        fs.track_alpha = false;
+        fs.sensitivity = job.sensitivity[k];
+        LPlane ca = comp_plane(raws_a, k, fmt, n), cb = comp_plane(raws_b, k, fmt, n);
+        Pyramid pa, pb;
+        if (!build_pyramid(layer_times(a, ca), fs, &pa, err) || !build_pyramid(layer_times(b, cb), fs, &pb, err)) return 1;
+        std::vector<float> ma, mb;
+        bool hm_a = solver_mask(raws_a, ca, k, n, &ma), hm_b = solver_mask(raws_b, cb, k, n, &mb);
+        std::vector<Plane> mpa, mpb;
+        bool masks = hm_a || hm_b;
+        if (masks) {
+            if (!hm_a) ma.assign(n, 1.0f);
+            if (!hm_b) mb.assign(n, 1.0f);
+            if (!mask_pyramid(ma.data(), w, h, fs, &mpa, err) || !mask_pyramid(mb.data(), w, h, fs, &mpb, err)) return 1;
+        }
+        bool need_ab = true, need_ba = true;
+        if (sel.interp == 0) {
+            need_ab = nearest_uses_f_ab(sel.wa, code);
+            need_ba = !need_ab;
+        }
+        if (need_ab) { f_ab[k] = solve_pyramids_masked(pa, pb, fs, masks ? &mpa : nullptr, masks ? &mpb : nullptr, false); has_ab[k] = true; }
+        if (need_ba) { f_ba[k] = solve_pyramids_masked(pb, pa, fs, masks ? &mpb : nullptr, masks ? &mpa : nullptr, false); has_ba[k] = true; }
+    }
+    // plates.rs:373-412: the composition, bottom layer first
+    Image res(w, h, fmt);
+    for (int k = nfg; k >= 0; k--) {
+        const FlowField* fab = has_ab[k] ? &f_ab[k] : nullptr;
+        const FlowField* fba = has_ba[k] ? &f_ba[k] : nullptr;
+        const LPlane* pl_a = k == nfg ? nullptr : &raws_a[k];
+        const LPlane* pl_b = k == nfg ? nullptr : &raws_b[k];
+        const Image* fr_a = k == nfg ? &a : nullptr;
+        const Image* fr_b = k == nfg ? &b : nullptr;
+        Image la = layer_times(a, comp_plane(raws_a, k, fmt, n));
+        Image lb = layer_times(b, comp_plane(raws_b, k, fmt, n));
+        Image r;
+        if (sel.interp == 0) {
+            bool takes_a = nearest_takes_a(code, sel.wa);
+            Image p = takes_a ? la : lb;
+            int rc = refill(p, takes_a ? pl_a : pl_b, takes_a ? fr_a : fr_b, job.cs.taps_above_first, err);
+            if (rc) return rc;
+            rc = compose_vectors(job.cs, sel, p, p, fab, fba, &r, err);
+            if (rc) return rc;
+        } else {
+            WarpOpts o;  // hold edges, amount 1 (plates.rs:260-268)
+            Image pa(w, h, fmt), pb(w, h, fmt);
+            int rc = inv_warp(pa, lb, *fab, 1.0f, o, nullptr, err);
+            if (rc) return rc;
+            over_pl(pa, la);
+            rc = inv_warp(pb, la, *fba, 1.0f, o, nullptr, err);
+            if (rc) return rc;
+            over_pl(pb, lb);
+            rc = refill(pa, pl_a, fr_a, job.cs.taps_above_first, err);
+            if (rc) return rc;
+            rc = refill(pb, pl_b, fr_b, job.cs.taps_above_first, err);
+            if (rc) return rc;
+            rc = compose_vectors(job.cs, sel, pa, pb, fab, fba, &r, err);
+            if (rc) return rc;
+        }
+        if (k == nfg) res = std::move(r);
+        else over_pl(res, r);
+    }
+    *out = std::move(res);
+    return 0;
+}
+
+}  // namespace orc

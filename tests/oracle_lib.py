@@ -89,6 +89,7 @@ def lib():
         L.or_fw_level_count.argtypes = [i, i]
         L.or_fw_triangle.argtypes = [P, i, i, P, i]
         L.or_logf.argtypes = [P, P, ctypes.c_long]
+        L.or_compose_layers.argtypes = [P, P, i, i, i, i, P, P, P, i, i, i, i, i, f, i, P]
         L.or_mask_pyramid.argtypes = [P, i, i, i, i, i, P, P, i]
         L.or_mask_gradient.argtypes = [P, P, i, i]
         L.or_calc_b_masked.argtypes = [P, P, P, P, i, i, P, P]
@@ -250,6 +251,21 @@ def solve_masked(x, y, w, h, fmt, matte_x=None, matte_y=None, quality=4, hiq=Tru
     if rc:
         raise ValueError(err())
     return out, (fw, fh)
+
+
+def compose_layers(a, b, w, h, fmt, mattes_a, mattes_b, sensitivity, wa, interp=1, quality=4, hiq=True,
+                   above_first=True, warp_mode=0, video_360=False):
+    """layers/plates.rs solve_and_compose_plates of one in-between frame (engine images in and out)."""
+    nfg = len(mattes_a)
+    ma = np.ascontiguousarray(np.concatenate(mattes_a) if nfg else np.zeros(1), np.float32)
+    mb = np.ascontiguousarray(np.concatenate(mattes_b) if nfg else np.zeros(1), np.float32)
+    sens = np.ascontiguousarray(sensitivity, np.float32)
+    out = np.zeros_like(a)
+    rc = lib().or_compose_layers(ptr(a), ptr(b), w, h, fmt, nfg, ptr(ma), ptr(mb), ptr(sens), quality, int(hiq),
+                                 int(above_first), warp_mode, int(video_360), np.float32(wa), interp, ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out
 
 
 def forward_warp(src, w, h, fmt, flow, fw, fh, amount, pyramid=True, coverage=False):

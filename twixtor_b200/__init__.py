@@ -279,6 +279,8 @@ def library():
     L.tw_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float]
     L.tw_smart_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float, i32]
     L.tw_set_lanes.argtypes = [P, i32]
+    L.tw_compose_layers.argtypes = [P, ctypes.POINTER(_RetimeSettings), ctypes.POINTER(_Selection), pimg, pimg, i32, P, P, P,
+                                    pimg]
     L.tw_solve_masked.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), P, P, pflow]
     L.tw_forward_warp.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, P]
     L.tw_encode_vectors.argtypes = [P, pimg, pflow, ctypes.c_float]
@@ -548,6 +550,23 @@ class Device:
         my = None if matte_y is None else np.ascontiguousarray(matte_y, np.float32)
         self._check(self._L.tw_solve_masked(self._h, ctypes.byref(xi), ctypes.byref(yi), ctypes.byref(settings._c()),
                                             _ptr(mx), _ptr(my), ctypes.byref(fl)))
+        return out
+
+    def compose_layers(self, settings: RetimeSettings, sel: Selection, a, b, width, height, fmt, mattes_a, mattes_b,
+                       sensitivity):
+        """The layered composition with plates of one in-between frame (layers/plates.rs): ``mattes_a`` /
+        ``mattes_b`` the FG raw mattes at A and B (FG1 first, ``width * height`` floats each),
+        ``sensitivity`` one value per layer, Main_BG last. Returns the engine image."""
+        nfg = len(mattes_a)
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        ai, aa = _img(a, width, height, fmt)
+        bi, ba = _img(b, width, height, fmt)
+        oi = _Image(width, height, fmt, out.ctypes.data)
+        ma = np.ascontiguousarray(np.concatenate(mattes_a) if nfg else np.zeros(1), np.float32)
+        mb = np.ascontiguousarray(np.concatenate(mattes_b) if nfg else np.zeros(1), np.float32)
+        sens = np.ascontiguousarray(sensitivity, np.float32)
+        self._check(self._L.tw_compose_layers(self._h, ctypes.byref(settings._c()), ctypes.byref(sel._c()), ctypes.byref(ai),
+                                              ctypes.byref(bi), nfg, _ptr(ma), _ptr(mb), _ptr(sens), ctypes.byref(oi)))
         return out
 
     def set_lanes(self, lanes):

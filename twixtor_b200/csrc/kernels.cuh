@@ -157,6 +157,21 @@ __global__ void k_hole_side1(const int* __restrict__ any_hole, int* __restrict__
 __global__ void k_encode_vectors(const float* __restrict__ flow, int fw, int fh, void* __restrict__ out, int W, int H,
                                  int fmt, float sx, float sy, float kx, float ky, int zero);
 
+// ---- the layered composition with plates (layers.cu) -----------------------------------------------
+__global__ void k_matte_out_of_range(const float* __restrict__ m, long n, int* __restrict__ flag);
+__global__ void k_raw_plane(const float* __restrict__ m, long n, int fmt, const int* __restrict__ clamp,
+                            float* __restrict__ out);
+__global__ void k_comp_plane(const float* __restrict__ raws, int nfg, int k, long n, int fmt, float* __restrict__ out);
+__global__ void k_solver_mask(const float* __restrict__ raws, int nfg, int k, const float* __restrict__ comp, long n,
+                              int fmt, float* __restrict__ out);
+__global__ void k_layer_times(const void* __restrict__ src, const float* __restrict__ p, void* __restrict__ out, int fmt,
+                              long n);
+__global__ void k_over_pl(void* __restrict__ dest, const void* __restrict__ src, int fmt, long n);
+__global__ void k_refill_pre(void* __restrict__ img, int fmt, long n, uint8_t* __restrict__ holes,
+                             int* __restrict__ any_hole);
+__global__ void k_refill_post(void* __restrict__ img, int fmt, long n, const float* __restrict__ plane,
+                              const void* __restrict__ frame);
+
 // ---- the forward warp (forward.cu) ---------------------------------------------------------------------
 struct FwGrid {  // forward/mesh.rs:11-26
     int w, h;

@@ -1,0 +1,232 @@
+// The layered composition with plates of the FG matte effects (layers/plates.rs, matte.rs): the
+// per pixel kernels of the matte planes, the layer images, the plate OVER and the refill around
+// the hole fill. The solves, warps, fills and single layer compositions are the library's own
+// stages; runtime.cu (tw_compose_layers) strings them together.
+//
+// Matte planes hold the units of the depth (whole numbers 0..255 / 0..65535 as floats, or the float
+// value itself). NaN handling follows the reference's x86 arithmetic where a NaN of a float matte
+// can reach an output (the cut, in double precision there), and its NaN rule where it uses it.
+#include "kernels.cuh"
+
+namespace tw {
+
+__device__ __forceinline__ float white_of(int fmt) { return fmt == 0 ? 255.0f : fmt == 1 ? 65535.0f : 1.0f; }
+
+// Rust's saturating float -> i64 cast (`as i64`: NaN gives 0)
+__device__ __forceinline__ int64_t as_i64(float x) {
+    if (isnan(x)) return 0;
+    if (x >= 9223372036854775808.0f) return INT64_MAX;
+    if (x < -9223372036854775808.0f) return INT64_MIN;
+    return __float2ll_rz(x);
+}
+
+// matte.rs:106-112: whether some value of a matte lies outside 0..1 (the clamp then applies to all)
+__global__ void k_matte_out_of_range(const float* __restrict__ m, long n, int* __restrict__ flag) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool out = false;
+    if (i < n) {
+        float v = m[i];
+        out = !(v >= 0.0f && v <= 1.0f);
+    }
+    if (__syncthreads_or(out) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+// plates.rs:50-57: the raw matte in the units of the depth (clamped first when `*clamp`)
+__global__ void k_raw_plane(const float* __restrict__ m, long n, int fmt, const int* __restrict__ clamp,
+                            float* __restrict__ out) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float x = m[i];
+    if (fmt == 2) {
+        out[i] = x;
+        return;
+    }
+    if (*clamp) x = x > 1.0f ? 1.0f : (x >= 0.0f ? x : 0.0f);  // matte.rs:94-102
+    out[i] = (float)as_i64(x * white_of(fmt) + 0.5f);
+}
+
+// plates.rs:63-78, the cut of c by the matte v of a layer above, with the x86 results for NaNs: the
+// double product takes v's NaN first, then c's
+__device__ __forceinline__ float cut(float c, float v, float white, bool isf) {
+    float x;
+    if (isnan(v)) x = nr::quiet(v);
+    else if (isnan(c)) x = nr::quiet(c);
+    else {
+        double d = (1.0 - (double)v) * (double)c;
+        x = isnan(d) ? __uint_as_float(0xffc00000u) : (float)d;  // an invalid product: the default NaN
+    }
+    if (0.0f > x) x = 0.0f;
+    else if (x > white) x = white;
+    if (isf) return x86::add(x, 0.0f);
+    return (float)as_i64(x + 0.5f);
+}
+
+// plates.rs:86-97 with a zero inverse matte shrink (the choke of the cut is then the clamp of
+// matte.rs:350-359): layer k's composition plane; raws: nfg planes of n values, FG1 first
+__global__ void k_comp_plane(const float* __restrict__ raws, int nfg, int k, long n, int fmt, float* __restrict__ out) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float white = white_of(fmt);
+    bool isf = fmt == 2;
+    float c = k == nfg ? white : raws[(long)k * n + i];
+    float kk = 1.0f / white;
+    for (int j = k - 1; j >= 0; j--) {
+        float v = x86::mul(raws[(long)j * n + i], kk);
+        if (0.0f > v) v = 0.0f;
+        else if (v >= 1.0f) v = 1.0f;
+        c = cut(c, v, white, isf);
+    }
+    out[i] = c;
+}
+
+// plates.rs:296-309: the solver mask of layer k, (white - (raw - comp)) / white. A mask of ones is
+// the plain solve (the binary pyramid is 1 everywhere and gates nothing), so it is always built.
+__global__ void k_solver_mask(const float* __restrict__ raws, int nfg, int k, const float* __restrict__ comp, long n,
+                              int fmt, float* __restrict__ out) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float white = white_of(fmt);
+    float r = k == nfg ? white : raws[(long)k * n + i];
+    out[i] = (white - (r - comp[i])) / white;
+}
+
+// plates.rs:128-156: every channel times the plane (units)
+__global__ void k_layer_times(const void* __restrict__ src, const float* __restrict__ p, void* __restrict__ out, int fmt,
+                              long n) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float K8 = __uint_as_float(0x3b808081u), K16 = __uint_as_float(0x37800080u);  // matte.rs:921-922
+    float pv = p[i];
+    for (int c = 0; c < 4; c++) {
+        long j = i * 4 + c;
+        if (fmt == 0) ((uint8_t*)out)[j] = (uint8_t)as_i64((float)((const uint8_t*)src)[j] * (pv * K8) + 0.5f);
+        else if (fmt == 1) ((uint16_t*)out)[j] = (uint16_t)as_i64((float)((const uint16_t*)src)[j] * (pv * K16) + 0.5f);
+        else ((float*)out)[j] = nr::mul(pv, ((const float*)src)[j]);
+    }
+}
+
+// matte.rs:923-1030: src OVER dest with the plugin's kernels
+__global__ void k_over_pl(void* __restrict__ dest, const void* __restrict__ src, int fmt, long n) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float K8 = __uint_as_float(0x3b808081u), K16 = __uint_as_float(0x37800080u);
+    if (fmt == 0) {
+        uint8_t* d = (uint8_t*)dest + i * 4;
+        const uint8_t* s = (const uint8_t*)src + i * 4;
+        uint8_t sa = s[0];
+        if (sa == 0) return;
+        if (sa == 255) { for (int c = 0; c < 4; c++) d[c] = s[c]; return; }
+        float saf = (float)sa, f = 1.0f - saf * K8;
+        uint8_t da = d[0];
+        for (int c = 1; c < 4; c++) d[c] = (uint8_t)as_i64((float)d[c] * f + (float)s[c] + 0.5f);
+        d[0] = (uint8_t)as_i64((float)(255 - da) * saf * K8 + (float)da + 0.5f);
+    } else if (fmt == 1) {
+        uint16_t* d = (uint16_t*)dest + i * 4;
+        const uint16_t* s = (const uint16_t*)src + i * 4;
+        uint16_t sa = s[0];
+        if (sa == 0) return;
+        if (sa == 65535) { for (int c = 0; c < 4; c++) d[c] = s[c]; return; }
+        float saf = (float)sa, f = 1.0f - saf * K16;
+        uint16_t da = d[0];
+        for (int c = 1; c < 4; c++) d[c] = (uint16_t)as_i64((float)d[c] * f + (float)s[c] + 0.5f);
+        d[0] = (uint16_t)as_i64((float)(65535 - (int32_t)da) * saf * K16 + (float)da + 0.5f);
+    } else {
+        float* d = (float*)dest + i * 4;
+        const float* s = (const float*)src + i * 4;
+        float sa = s[0];
+        if (sa == 0.0f) return;
+        if (sa == 1.0f) { for (int c = 0; c < 4; c++) d[c] = s[c]; return; }
+        float f = nr::sub(1.0f, sa);
+        float da = d[0];
+        for (int c = 1; c < 4; c++) d[c] = nr::add(nr::add(nr::mul(f, d[c]), s[c]), 0.0f);
+        d[0] = nr::add(nr::add(nr::mul(nr::sub(1.0f, da), sa), da), 0.0f);
+    }
+}
+
+// plates.rs:245-256, first half: the unpremultiply of the plate (plates.rs:160-187) and its holes,
+// white - alpha through the hole rule of the mask's type (holefill.rs:124-133): u8 / u16 any non
+// zero value, f32 !(3.1e-5 > m) in double (a NaN alpha is a hole)
+__global__ void k_refill_pre(void* __restrict__ img, int fmt, long n, uint8_t* __restrict__ holes,
+                             int* __restrict__ any_hole) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool hole = false;
+    if (i < n) {
+        if (fmt == 0) {
+            uint8_t* p = (uint8_t*)img + i * 4;
+            if (p[0] != 0) {
+                float s = 255.0f / (float)p[0];  // image.rs:306-320
+                for (int c = 1; c < 4; c++) {
+                    float v = (float)p[c] * s;
+                    if (v > 255.0f) v = 255.0f;
+                    p[c] = (uint8_t)qround(v);
+                }
+            }
+            hole = (uint8_t)(0xffu - p[0]) != 0;
+        } else if (fmt == 1) {
+            uint16_t* p = (uint16_t*)img + i * 4;
+            if (p[0] != 0) {
+                float inv = 65535.0f / (float)p[0];
+                for (int c = 1; c < 4; c++) {
+                    float v = (float)p[c] * inv;
+                    if (65535.0f < v) v = 65535.0f;
+                    p[c] = (uint16_t)qround(v);
+                }
+            }
+            hole = (uint16_t)(0xffffu - p[0]) != 0;
+        } else {
+            float* p = (float*)img + i * 4;
+            if (!(1e-7 > (double)p[0])) {
+                float inv = 1.0f / p[0];
+                for (int c = 1; c < 4; c++) p[c] = nr::mul(inv, p[c]);
+            }
+            float m = 1.0f - p[0];
+            hole = !(__longlong_as_double(0x3f0040bfe3b03e21ll) > (double)m);
+        }
+        holes[i] = hole ? 1 : 0;
+    }
+    if (__syncthreads_or(hole) && threadIdx.x == 0) atomicOr(any_hole, 1);
+}
+
+// plates.rs:245-256, second half: the alpha replaced by the plane (units; plane != null) or by the
+// frame's alpha, then the premultiply of the plugin's kernel (plates.rs:191-208)
+__global__ void k_refill_post(void* __restrict__ img, int fmt, long n, const float* __restrict__ plane,
+                              const void* __restrict__ frame) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float K16 = __uint_as_float(0x37800080u);
+    if (fmt == 0) {
+        uint8_t* p = (uint8_t*)img + i * 4;
+        if (plane) {
+            int64_t v = as_i64(plane[i]);
+            p[0] = (uint8_t)(v < 0 ? 0 : v > 255 ? 255 : v);
+        } else {
+            p[0] = ((const uint8_t*)frame)[i * 4];
+        }
+        float a = (float)p[0] * __uint_as_float(0x3b808081u);  // image.rs:276-280
+        for (int c = 1; c < 4; c++) p[c] = (uint8_t)qround((float)p[c] * a);
+    } else if (fmt == 1) {
+        uint16_t* p = (uint16_t*)img + i * 4;
+        if (plane) {
+            int64_t v = as_i64(plane[i]);
+            p[0] = (uint16_t)(v < 0 ? 0 : v > 65535 ? 65535 : v);
+        } else {
+            p[0] = ((const uint16_t*)frame)[i * 4];
+        }
+        float f = (float)p[0] * K16;
+        for (int c = 1; c < 4; c++) p[c] = (uint16_t)qround((float)p[c] * f);
+    } else {
+        float* p = (float*)img + i * 4;
+        p[0] = plane ? plane[i] : ((const float*)frame)[i * 4];
+        float r1 = p[0] * p[1], r2 = p[0] * p[2], r3 = p[0] * p[3];  // image.rs:294-303
+        if (isnan(r1) || isnan(r2) || isnan(r3) || isnan(p[0])) {
+            r1 = nr::mul(p[0], p[1]);
+            r2 = nr::mul(p[0], p[2]);
+            r3 = nr::mul(p[0], p[3]);
+        }
+        p[1] = r1;
+        p[2] = r2;
+        p[3] = r3;
+    }
+}
+
+}  // namespace tw

@@ -201,6 +201,7 @@ struct tw_ctx {
     Taps g7{}, g5{}, b5{};
     // engine images, wire staging, pyramids, solve work, flows
     DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags, holes, fill, masks;
+    DevBuf lay_mem;  // tw_compose_layers: mattes, planes, layer images, plates, flows
     DevBuf host_stage;  // unused placeholder for pinned staging
     std::vector<cudaEvent_t> ev_pool;  // the profiler's events (KernelProfile)
     // the forward warp: vertices, mip pyramid, per pixel counts / offsets, hit lists, flags
@@ -796,7 +797,7 @@ int tw_open(int device, tw_ctx** out) {
 void tw_close(tw_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->masks, &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
+    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->masks, &ctx->lay_mem, &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
                     &ctx->fw_vd, &ctx->fw_pyr, &ctx->fw_tmp[0], &ctx->fw_tmp[1], &ctx->fw_cnt, &ctx->fw_off,
                     &ctx->fw_fill, &ctx->fw_sums, &ctx->fw_keys, &ctx->fw_cols, &ctx->fw_scratch, &ctx->fw_longq,
                     &ctx->fw_flags, &ctx->fw_out, &ctx->fw_cov})
@@ -1282,6 +1283,162 @@ int tw_fill_holes(tw_ctx* ctx, tw_image_mut* img, const void* mask, int32_t mask
     if (hf[3])
         return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of a %dx%d image: the pyramid resample divides by zero for a side of 1",
                          W, H);
+    return TW_OK;
+}
+
+// ---- the layered composition with plates (layers/plates.rs:330-412) ---------------------------------
+
+int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection* sel, const tw_image* a,
+                      const tw_image* b, int32_t nfg, const float* mattes_a, const float* mattes_b,
+                      const float* sensitivity, tw_image_mut* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!s || !sel || !sensitivity || !out || !out->data || nfg < 0 || nfg > 3 || (nfg > 0 && (!mattes_a || !mattes_b)))
+        return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    CHECK(check_image(ctx, a, "layers"));
+    CHECK(check_image(ctx, b, "layers"));
+    if (!same_shape(a, b) || out->width != a->width || out->height != a->height || out->fmt != a->fmt)
+        return ctx->fail(TW_ERR_MISMATCH, "layers: images of different shapes");
+    const tw_engine_settings& cs = s->compose;
+    if (cs.warp_mode != 0 && cs.warp_mode != 1)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "layers: warping codes 2 and 3 are not on the device yet");
+    if (sel->interp != 0 && sel->interp != 1)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "layers: Weighted Blend is not on the device yet");
+    if (cs.wrap_360 || s->flow.wrap || s->flow.track_alpha)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "layers: the wrap-around (360) filters are not on the device");
+    int W = a->width, H = a->height, fmt = a->fmt;
+    long n = (long)W * H;
+    size_t px = 4 * sample_bytes(fmt), ib = (size_t)n * px;
+    tw_flow_settings fs0 = s->flow;
+    fs0.quality = sel->vectors_quality;
+    fs0.track_alpha = 0;  // plates.rs:323-327: the layered solves add no alpha to the luma
+    Geo g;
+    CHECK(geometry(fs0, W, H, &g, &ctx->err));
+    size_t pf = pyramid_floats(g);
+    size_t fb = (size_t)g.w * g.h * 2;
+    int L = nfg + 1;
+    // one block: mattes and raw planes (2 sides x nfg), comp planes and solver mattes (2 x L), layer
+    // images (2 x L), two plates, the result, the flows (2 x L), pyramids and mask pyramids (2 each)
+    size_t fl = 0;
+    auto take = [&](size_t floats) { size_t o = fl; fl += (floats + 63) & ~(size_t)63; return o; };
+    size_t o_mat = take(2 * (size_t)nfg * n), o_raw = take(2 * (size_t)nfg * n), o_comp = take(2 * (size_t)L * n);
+    size_t o_smat = take(2 * (size_t)n), o_img = take(2 * (size_t)L * ib / 4 + 1), o_plate = take(2 * ib / 4 + 1);
+    size_t o_res = take(ib / 4 + 1), o_flow = take(2 * (size_t)L * fb), o_pyr = take(4 * pf), o_mpyr = take(2 * pf);
+    size_t o_scr = take(2 * (size_t)n);
+    CHECK(ctx->ensure(ctx->lay_mem, fl * sizeof(float), "layer buffers"));
+    CHECK(ctx->ensure(ctx->holes, (size_t)n, "holes mask"));
+    float* M = ctx->lay_mem.as<float>();
+    float* mat = M + o_mat;
+    float* raw = M + o_raw;
+    float* comp = M + o_comp;
+    float* smat = M + o_smat;
+    auto img = [&](int side, int k) { return (void*)((char*)(M + o_img) + ((size_t)side * L + k) * ib); };
+    void* plate[2] = {(void*)(M + o_plate), (void*)((char*)(M + o_plate) + ib)};
+    void* res = (void*)(M + o_res);
+    auto flow = [&](int dir, int k) { return M + o_flow + ((size_t)dir * L + k) * fb; };  // dir 0: F_AB, 1: F_BA
+    float* pyr[2] = {M + o_pyr, M + o_pyr + 2 * pf};
+    float* mpyr[2] = {M + o_mpyr, M + o_mpyr + pf};
+    float* scr = M + o_scr;
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
+    CHECK(ctx->cuda(cudaMemsetAsync(flags + FL_ONE, 0x01, sizeof(int), ctx->stream), "flags"));
+    CHECK(upload_image(ctx, ctx->eng[0], a));
+    CHECK(upload_image(ctx, ctx->eng[1], b));
+    const void* frame[2] = {ctx->eng[0].p, ctx->eng[1].p};
+    if (nfg > 0) {
+        CHECK(ctx->cuda(cudaMemcpyAsync(mat, mattes_a, (size_t)nfg * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
+                        "matte upload"));
+        CHECK(ctx->cuda(cudaMemcpyAsync(mat + (size_t)nfg * n, mattes_b, (size_t)nfg * n * sizeof(float),
+                                        cudaMemcpyHostToDevice, ctx->stream), "matte upload"));
+    }
+    // plates.rs:50-57: the raw planes (each matte clamped when one of its values leaves 0..1)
+    for (int side = 0; side < 2; side++)
+        for (int j = 0; j < nfg; j++) {
+            const float* m = mat + ((size_t)side * nfg + j) * n;
+            int* fl_ = flags + FL_ANY0 + side * 4 + j;  // the per-level range flags are not in use yet
+            LAUNCH(ctx, k_matte_out_of_range, grid1(n), TB, 0, m, n, fl_);
+            LAUNCH(ctx, k_raw_plane, grid1(n), TB, 0, m, n, fmt, fl_, raw + ((size_t)side * nfg + j) * n);
+        }
+    // the composition planes and the layer images of every layer at both sides
+    for (int side = 0; side < 2; side++)
+        for (int k = 0; k < L; k++) {
+            float* c = comp + ((size_t)side * L + k) * n;
+            LAUNCH(ctx, k_comp_plane, grid1(n), TB, 0, raw + (size_t)side * nfg * n, nfg, k, n, fmt, c);
+            LAUNCH(ctx, k_layer_times, grid1(n), TB, 0, frame[side], c, img(side, k), fmt, n);
+        }
+    // the solves (plates.rs:340-369): each layer's own layer images, masked by its solver masks
+    bool need_ab = true, need_ba = true;
+    if (sel->interp == 0) {
+        bool use_ab = (sel->wa < 0.5f && (unsigned)cs.warp_mode < 2) || (0.5f <= sel->wa && (unsigned)cs.warp_mode > 1);
+        need_ab = use_ab;
+        need_ba = !use_ab;
+    }
+    for (int k = 0; k < L; k++) {
+        tw_flow_settings fs = fs0;
+        fs.sensitivity = sensitivity[k];
+        Geo gk;
+        CHECK(geometry(fs, W, H, &gk, &ctx->err));
+        for (int side = 0; side < 2; side++) {
+            CHECK(build_pyramid_dev(ctx, img(side, k), W, H, fmt, fs, gk, pyr[side], pyr[side] + pf, ctx->plane));
+            LAUNCH(ctx, k_solver_mask, grid1(n), TB, 0, raw + (size_t)side * nfg * n, nfg, k,
+                   comp + ((size_t)side * L + k) * n, n, fmt, smat);
+            CHECK(build_mask_pyramid_dev(ctx, smat, W, H, fs, gk, mpyr[side], scr, scr + n, flags + FL_ONE));
+        }
+        if (need_ab)
+            CHECK(solve_pyramids_dev(ctx, pyr[0], pyr[1], pyr[0] + pf, pyr[1] + pf, gk, fs, ctx->work[0], flow(0, k),
+                                     flags + FL_ANY0, flags + FL_NAN, mpyr[0], mpyr[1]));
+        if (need_ba)
+            CHECK(solve_pyramids_dev(ctx, pyr[1], pyr[0], pyr[1] + pf, pyr[0] + pf, gk, fs, ctx->work[0], flow(1, k),
+                                     flags + FL_ANY1, flags + FL_NAN, mpyr[1], mpyr[0]));
+    }
+    // the composition, bottom layer first (plates.rs:373-412)
+    SmartScratch ss{nullptr, &ctx->fill, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1};
+    DevBuf& fillbuf = ctx->work[1];
+    ss.holes = &ctx->masks;  // the composition's own holes mask (the refill uses ctx->holes)
+    auto refill = [&](void* p, int side, int k) -> int {
+        CHECK(ctx->cuda(cudaMemsetAsync(flags + FL_HOLE, 0, sizeof(int), ctx->cur), "holes flag"));
+        LAUNCH(ctx, k_refill_pre, grid1(n), TB, 0, p, fmt, n, ctx->holes.as<uint8_t>(), flags + FL_HOLE);
+        if (W < 2 || H < 2) LAUNCH(ctx, k_hole_side1, 1, 1, 0, flags + FL_HOLE, flags + FL_SIDE1);
+        else CHECK(fill_dev(ctx, p, W, H, fmt, ctx->holes.as<uint8_t>(), flags + FL_HOLE, cs.taps_above_first != 0, fillbuf));
+        const float* plane = k == nfg ? nullptr : raw + ((size_t)side * nfg + k) * n;
+        LAUNCH(ctx, k_refill_post, grid1(n), TB, 0, p, fmt, n, plane, frame[side]);
+        return TW_OK;
+    };
+    for (int k = nfg; k >= 0; k--) {
+        const float* fab = need_ab ? flow(0, k) : nullptr;
+        const float* fba = need_ba ? flow(1, k) : nullptr;
+        void* dst = k == nfg ? res : ctx->eng[2].p;
+        CHECK(ctx->ensure(ctx->eng[2], ib, "layer result"));
+        if (k != nfg) dst = ctx->eng[2].p;
+        if (sel->interp == 0) {
+            bool takes_a = cs.warp_mode == 0 ? 0.5f <= sel->wa : !(0.5f > sel->wa);  // layers.rs:697-703
+            int side = takes_a ? 0 : 1;
+            CHECK(ctx->cuda(cudaMemcpyAsync(plate[0], img(side, k), ib, cudaMemcpyDeviceToDevice, ctx->cur), "plate"));
+            CHECK(refill(plate[0], side, k));
+            CHECK(compose_dev(ctx, cs, *sel, plate[0], plate[0], fab, fba, g.w, g.h, W, H, fmt, dst, false, false,
+                              flags + FL_BAD, &ss));
+        } else {
+            // PA = LA OVER warp(LB, F_AB, 1), PB = LB OVER warp(LA, F_BA, 1): hold edges (plates.rs:260-268)
+            WarpParams pa_ = warp_params(img(1, k), fab, g.w, g.h, 1.0f, W, true);
+            WarpParams pb_ = warp_params(img(0, k), fba, g.w, g.h, 1.0f, W, true);
+            LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pa_, fmt, plate[0], (uint8_t*)nullptr, W, H, flags + FL_BAD);
+            LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, plate[0], img(0, k), fmt, n);
+            LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pb_, fmt, plate[1], (uint8_t*)nullptr, W, H, flags + FL_BAD);
+            LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, plate[1], img(1, k), fmt, n);
+            CHECK(refill(plate[0], 0, k));
+            CHECK(refill(plate[1], 1, k));
+            CHECK(compose_dev(ctx, cs, *sel, plate[0], plate[1], fab, fba, g.w, g.h, W, H, fmt, dst, false, false,
+                              flags + FL_BAD, &ss));
+        }
+        if (k != nfg) LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, res, dst, fmt, n);
+    }
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, res, ib, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[4];
+    CHECK(finish(ctx, hf, 4));
+    if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
+    if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    if (hf[3]) return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of an image with a side of 1 pixel that has a hole");
     return TW_OK;
 }
 
