@@ -344,6 +344,21 @@ int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* 
                           const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt,
                           void* out);
 
+/* retime-fgbg with FG matte layers over a clip in HOST memory (plugins/retime-fgbg/src/glue.rs:
+ * 275, render_temporal, with compose.rs:149-170 and layers.rs:530-567): output frame k of the
+ * selections `sels`; footage in `frames` (nframes wire frames back to back), the FG matte layers
+ * FG1 .. FG nfg in matte_clips[j] (wire frames of the footage's size and format, matte_nframes[j]
+ * of them, or nframes when matte_nframes is NULL), each read through its channel matte_chan[j]
+ * (the popup: 1 R, 2 G, 3 B, else alpha); sensitivity: nfg + 1 values 0..1, Main_BG last. The
+ * in-between frames run tw_compose_layers in the motion path's row order (rows reversed when
+ * s->motion_rows_reversed), the exact frames the interpolation without flows. A frame outside a
+ * clip is blank. The inverse matte shrink is 0, no tracking point is in use and the output is
+ * Display Twixtored Output. nfg 0 is tw_retime_clip. */
+int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes, int32_t nfg,
+                          const void* const* matte_clips, const int32_t* matte_nframes, const int32_t* matte_chan,
+                          const float* sensitivity, const tw_selection* sels, int32_t nout, int32_t width,
+                          int32_t height, int32_t fmt, void* out);
+
 #ifdef __cplusplus
 }
 #endif

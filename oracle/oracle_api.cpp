@@ -513,6 +513,91 @@ int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const 
     return 0;
 }
 
+// ---- retime-fgbg with FG matte layers (plugins/retime-fgbg/src/glue.rs, compose.rs:149-170,
+// layers.rs:530-567) --------------------------------------------------------------------------------
+
+// matte.rs:141-188 (extract_raw): the channel (1 R, 2 G, 3 B, else alpha) of an engine image as a
+// matte; 8 and 16 bpc v / white then clamped to 0..1, float the sample itself
+static std::vector<float> extract_raw(const Image& img, int chan) {
+    int c = chan == 1 ? 1 : chan == 2 ? 2 : chan == 3 ? 3 : 0;
+    size_t n = (size_t)img.w * img.h;
+    std::vector<float> m(n);
+    for (size_t i = 0; i < n; i++) {
+        float v;
+        if (img.fmt == U8) v = (float)img.u8[i * 4 + c] / 255.0f;
+        else if (img.fmt == U16) v = (float)img.u16[i * 4 + c] / 65535.0f;
+        else { m[i] = img.f32[i * 4 + c] * 1.0f; continue; }
+        m[i] = v > 1.0f ? 1.0f : v > 0.0f ? v : 0.0f;  // matte.rs:79-87 (clamp01)
+    }
+    return m;
+}
+
+static std::vector<float> flip_matte(const std::vector<float>& m, int w, int h) {
+    std::vector<float> o(m.size());
+    for (int y = 0; y < h; y++) std::memcpy(&o[(size_t)y * w], &m[(size_t)(h - 1 - y) * w], sizeof(float) * w);
+    return o;
+}
+
+// Output frame n of retime-fgbg with `nfg` FG matte clips (wire frames back to back, the size and
+// format of the footage): fg_chan / fg_sens per layer (popup 1..4, sensitivity 0..100). The
+// selection is the retime time map of p (plugin 03's without the source time offset: the same at
+// equal rates); p->smart_blend carries the warping code (0 or 1). Display Twixtored Output, no
+// inverse matte shrink, no tracking points.
+int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte_clips, int nfg, const int* fg_chan,
+                       const double* fg_sens, int w, int h, int fmt, const or_retime_params* p, int n, void* out) {
+    if (nfg == 0) return or_retime_one(frames, nframes, w, h, fmt, p, n, out);
+    Fmt f = (Fmt)fmt;
+    size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
+    size_t frame_bytes = (size_t)w * h * 4 * es;
+    bool integer = p->fps_den == 1;
+    int time_step = integer ? 100 : p->fps_den;
+    float s0, s1, wa;
+    int a, exact, vq, interp;
+    or_select(p, n, w, h, &s0, &s1, &a, &wa, &exact, &vq, &interp);
+    auto fetch = [&](const void* clip, int pos) -> Image {
+        double d = (double)(float)pos;
+        int time = cvtt_i32_d(d * (double)time_step + 0.5);
+        long long idx = time >= 0 ? time / time_step : -(((long long)-time + time_step - 1) / time_step);
+        if (idx < 0 || idx >= nframes) return Image(w, h, f);
+        return from_frame((const uint8_t*)clip + (size_t)idx * frame_bytes, w, h, f);
+    };
+    Image A = fetch(frames, a), B = fetch(frames, a + 1), result;
+    Selection sel;
+    sel.s0 = s0; sel.s1 = s1; sel.a = a; sel.b = a + 1; sel.wa = wa; sel.exact = exact != 0;
+    sel.vectors_quality = vq; sel.interp = interp;
+    std::string e;
+    if (vq != 0 && !exact) {  // compose.rs:155-158: the layered vector path
+        if (interp < 0 || interp > 1) return fail(2, "weighted blend on the vector path is not restated");
+        LayerJob job;
+        for (int k = 0; k < nfg; k++) {
+            std::vector<float> ma = extract_raw(fetch(matte_clips[k], a), fg_chan[k]);
+            std::vector<float> mb = extract_raw(fetch(matte_clips[k], a + 1), fg_chan[k]);
+            if (p->rows_reversed) { ma = flip_matte(ma, w, h); mb = flip_matte(mb, w, h); }
+            job.mattes_a.push_back(std::move(ma));
+            job.mattes_b.push_back(std::move(mb));
+            job.sensitivity.push_back(fixed_reader(float_to_fixed(fg_sens[k]), 1.0f) / 100.0f);
+        }
+        job.sensitivity.push_back(fixed_reader(float_to_fixed(p->sensitivity), 1.0f) / 100.0f);
+        job.fs.quality = vq;
+        job.fs.hiq = p->quality_high != 0;
+        job.fs.taps_above_first = p->taps_above_first != 0;
+        job.cs.quality_high = p->quality_high != 0;
+        job.cs.warp_mode = p->smart_blend ? 1 : 0;
+        job.cs.taps_above_first = p->taps_above_first != 0;
+        job.sel = sel;
+        Image ar = p->rows_reversed ? rows_reversed(A) : A, br = p->rows_reversed ? rows_reversed(B) : B;
+        Image o;
+        int rc = compose_layers_plates(job, ar, br, &o, &e);
+        if (rc) return fail(rc, e);
+        result = p->rows_reversed ? rows_reversed(o) : o;
+    } else {  // compose.rs:166-169 with the full group fast path (layers.rs:177-179): the plain one
+        int rc = interpolate(sel, A, B, &result, &e);
+        if (rc) return fail(rc, e);
+    }
+    to_frame(result, out);
+    return 0;
+}
+
 // Renders `nout` output frames of the `retime` effect over a raw clip of `nframes` wire frames.
 int or_retime_clip(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int nout,
                    void* out) {

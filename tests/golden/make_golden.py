@@ -22,6 +22,12 @@ Writes, next to this script:
   recorded, like the retime one, by the revision whose engine saw the frames top row first and
   whose vertical border taps came below first: the tests run those cases with
   ``rows_reversed=False, taps_above_first=False``.
+* ``fgbg_layers_grid.npz`` - the cases of the reference's parity grid ``parity/fgbg-layers`` that
+  the layered path with plates serves (FG matte layers FG1.. consecutive, warping Inverse or
+  Inverse w/ Smart Blend, Nearest or Blend, no inverse matte shrink, no tracking points, Display
+  Twixtored Output, integer frame rates), their footage and matte clips as its ``gen_grid.py``
+  renders them, and the sha256 of the output clip ``results/base.tsv`` records (the reference's
+  current revision: rows reversed, taps above first).
 * ``f1_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/f1_cases.hex``
   (the reference's bit-exact numpy models of Smart Blend and the hole fill; format in its
   ``f1_gen.py``).
@@ -122,6 +128,62 @@ def create_vectors_grid(ref):
     print(f"create_vectors_grid.npz: {len(cases)} cases, {len(keys)} input clips")
 
 
+FG_SERVED = {"speed_percent", "warping", "frame_interp", "fg1_matte_chan", "fg2_matte_chan", "fg3_matte_chan",
+             "fg1_sensitivity", "fg2_sensitivity", "fg3_sensitivity", "main_bg_sensitivity", "vectors"}
+
+
+def fgbg_layers_grid(ref):
+    root = os.path.join(ref, "parity", "fgbg-layers")
+    spec = importlib.util.spec_from_file_location("fg_gen", os.path.join(root, "gen_grid.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    g = gen.build_grid()
+    table = {}
+    for line in open(os.path.join(root, "results", "base.tsv")):
+        parts = line.rstrip("\n").split("\t")
+        if parts[0] != "id":
+            table[parts[0]] = (parts[1], parts[3])
+    ids = ["fg1_matte", "fg2_matte", "fg3_matte"]
+    cases, inputs = [], {}
+
+    def clip(rel):
+        if rel not in inputs:
+            spec_ = g.files[rel]
+            if spec_[0] == "scene":
+                _, src, w, h, d, n = spec_
+                fn = gen.SOURCES[src]
+            else:
+                _, kind, box, fast, w, h, d, n = spec_
+                mfn = gen.matte(kind, box, fast, d)
+                fn = (lambda mm: (lambda x, y, f, w_, h_, depth: mm(x, y, f, w_, h_)))(mfn)
+            inputs[rel] = np.frombuffer(gen.render_clip(fn, w, h, d, n), np.uint8)
+        return rel
+
+    for c in g.cases:
+        params = dict(p.split("=", 1) for p in c["params"])
+        if any(k not in FG_SERVED for k in params) or any("@" in v for v in params.values()):
+            continue
+        if params.get("warping", "1") not in ("1", "2") or params.get("frame_interp", "2") not in ("1", "2"):
+            continue
+        if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
+            continue
+        lay = c.get("layers", {})
+        nfg = 0
+        while nfg < 3 and ids[nfg] in lay:
+            nfg += 1
+        if any(k in lay for k in ids[nfg:]) or set(lay) - set(ids):
+            continue
+        mattes = [clip(lay[ids[k]]) for k in range(nfg)]
+        cases.append(dict(id=c["id"], params=c["params"], depth=c["depth"], width=c["width"], height=c["height"],
+                          frames=c["frames"], fps=c["fps"], input=clip(c["input"]), mattes=mattes,
+                          sha256=table[c["id"]][1]))
+    keys = sorted(inputs)
+    arrays = {f"input_{i}": inputs[k] for i, k in enumerate(keys)}
+    arrays["meta"] = np.frombuffer(json.dumps(dict(inputs=keys, cases=cases)).encode(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "fgbg_layers_grid.npz"), **arrays)
+    print(f"fgbg_layers_grid.npz: {len(cases)} cases, {len(keys)} clips")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -157,6 +219,7 @@ def main():
         print(f"retime_flow_grid.npz: {len(cases)} cases, {len(keys)} input clips")
 
     create_vectors_grid(ref)
+    fgbg_layers_grid(ref)
 
     txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "f1_cases.hex")).read()
     blob = bytes.fromhex("".join(txt.split()))

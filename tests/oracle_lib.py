@@ -79,6 +79,7 @@ def lib():
         L.or_select.argtypes = [ctypes.POINTER(RetimeParams), i, i, i, P, P, P, P, P, P, P]
         L.or_retime_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_retime_one.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
+        L.or_retime_fgbg_one.argtypes = [P, i, P, i, P, P, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_set_threads.argtypes = [i]
         L.or_smart_blend.argtypes = [P, P, P, i, i, i, f, i]
         L.or_fill_holes.argtypes = [P, i, i, i, P, i, i]
@@ -327,6 +328,25 @@ def retime_one(frames, nframes, w, h, fmt, params, n):
     rc = lib().or_retime_one(ptr(frames), nframes, w, h, fmt, ctypes.byref(params), n, ptr(out))
     if rc:
         raise ValueError(err())
+    return out
+
+
+def retime_fgbg_clip(frames, nframes, mattes, chans, sens, w, h, fmt, params, nout):
+    """retime-fgbg with FG matte layers (FG1 first): ``mattes`` the matte clips (nframes wire frames
+    each), ``chans`` their channel popups, ``sens`` their sensitivities 0..100; Main_BG's is
+    params.sensitivity. Output frames 0..nout-1 back to back."""
+    nfg = len(mattes)
+    mattes = [np.ascontiguousarray(m) for m in mattes]
+    arr = (ctypes.c_void_p * max(nfg, 1))(*[m.ctypes.data for m in mattes])
+    ch = (ctypes.c_int * 3)(*(list(chans) + [1] * (3 - nfg)))
+    se = (ctypes.c_double * 3)(*(list(sens) + [70.0] * (3 - nfg)))
+    fb = w * h * 4
+    out = np.zeros(nout * fb, DTYPE[fmt])
+    for n in range(nout):
+        rc = lib().or_retime_fgbg_one(ptr(frames), nframes, arr, nfg, ch, se, w, h, fmt, ctypes.byref(params), n,
+                                      ptr(out[n * fb:]))
+        if rc:
+            raise ValueError(err())
     return out
 
 

@@ -1,9 +1,13 @@
 """Parity of the CUDA layered composition with plates (tw_compose_layers) with the oracle, bit for
 bit: one to three FG matte layers moving over a background, Nearest and Blend, warping codes 0 and
-1, the three depths, soft mattes and float mattes outside 0..1."""
+1, the three depths, soft mattes and float mattes outside 0..1; and retime-fgbg over whole clips
+(tw_retime_layers_clip) against the sha256 the reference's fgbg-layers parity grid records."""
+import hashlib
+
 import numpy as np
 import pytest
 
+import golden_data
 import oracle_lib as O
 import twixtor_b200 as tw
 from twixtor_b200 import synth
@@ -101,3 +105,52 @@ def test_video_360_binary_alpha(dev):
     w, h = 96, 64
     a, b, ma, mb = scene(w, h, 1, 1, seed=4)
     run(dev, a, b, w, h, 1, ma, mb, [0.7, 0.7], 0.4, 1, 1, video_360=True)
+
+
+FG_CASES, FG_INPUTS = golden_data.fgbg_grid()
+
+
+def fgbg_clip(dev, case, rows_reversed=True, taps_above_first=True):
+    fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
+    w, h, n = case["width"], case["height"], case["frames"]
+    kw = golden_data.fgbg_case_params(case)
+    tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], vectors=kw["vectors"], frame_interp=kw["frame_interp"])
+    sels = [tw.select(tp, k, w, h) for k in range(n)]
+    s = tw.RetimeSettings(flow=tw.FlowSettings(hiq=True, taps_above_first=taps_above_first),
+                          compose=tw.EngineSettings(warp_mode=kw["smart_blend"], taps_above_first=taps_above_first),
+                          motion_rows_reversed=rows_reversed)
+    sens = [tw.percent_param(v) for v in kw["fg_sens"]] + [tw.percent_param(kw["sensitivity"])]
+    mattes = [FG_INPUTS[m].view(tw.DTYPES[fmt]) for m in case["mattes"]]
+    return dev.retime_layers_clip(s, FG_INPUTS[case["input"]].view(tw.DTYPES[fmt]), n, mattes, kw["chans"], sens, sels,
+                                  w, h, fmt)
+
+
+@pytest.mark.parametrize("case", FG_CASES, ids=[c["id"] for c in FG_CASES])
+def test_fgbg_layers_grid_sha256(dev, case):
+    """Every served case of the reference's retime-fgbg grid, rendered by the CUDA path."""
+    out = fgbg_clip(dev, case)
+    assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
+
+
+def test_fgbg_clip_matches_oracle_at_larger_size(dev):
+    """A 160x96 clip of 6 frames at 40 %, two FG layers on the G and alpha channels, 16 bpc."""
+    w, h, n, fmt = 160, 96, 6, 1
+    frames = synth.moving_clip(w, h, n, depth=16, seed=0x5eed)
+    rng = np.random.RandomState(11)
+    mattes = []
+    for j in range(2):
+        m = synth.moving_clip(w, h, n, depth=16, seed=100 + j).view(np.uint16).reshape(n, h, w, 4).copy()
+        cx, cy, vx = rng.uniform(0.3, 0.7) * w, rng.uniform(0.3, 0.7) * h, rng.uniform(-3, 3)
+        for f in range(n):
+            e = ellipse(w, h, cx + vx * f, cy, 0.2 * w, 0.25 * h, soft=2.0).reshape(h, w)
+            m[f, :, :, 1 if j == 0 else 3] = (e * 65535.0 + 0.5).astype(np.uint16)
+        mattes.append(m.reshape(-1))
+    tp = tw.TimeParams(speed_percent=40.0)
+    nout = 12
+    sels = [tw.select(tp, k, w, h) for k in range(nout)]
+    s = tw.RetimeSettings(flow=tw.FlowSettings(hiq=True), compose=tw.EngineSettings(warp_mode=1))
+    sens = [tw.percent_param(55.0), tw.percent_param(70.0), tw.percent_param(70.0)]
+    got = dev.retime_layers_clip(s, frames, n, mattes, [2, 4], sens, sels, w, h, fmt)
+    p = O.retime_params(speed=40.0, smart_blend=1, sensitivity=70.0)
+    want = O.retime_fgbg_clip(frames, n, mattes, [2, 4], [55.0, 70.0], w, h, fmt, p, nout)
+    assert same(got, want)

@@ -5,7 +5,10 @@
 * the reference's bit-exact numpy model fixtures of the inverse warp (tests/fixtures/warp_cases.hex);
 * end to end: the sha256 of every served case of the reference's parity grid
   parity/retime-flow/results/base.grid.tsv (whole output clips of the `retime` effect: frame
-  selection, pyramids, both solves with block matching, warps, blend, boundary conversions).
+  selection, pyramids, both solves with block matching, warps, blend, boundary conversions);
+* the same for the layered path with plates: every served case of parity/fgbg-layers/results/base.tsv
+  (retime-fgbg with 1 to 3 FG matte layers, recorded at the reference's current revision: rows
+  reversed, taps above first).
 """
 import ctypes
 import hashlib
@@ -198,4 +201,21 @@ def test_create_vectors_grid_sha256(case):
     kw = golden_data.cv_case_params(case)
     out = O.create_vectors_clip(raw, case["frames"], case["width"], case["height"], fmt, case["frames"],
                                 rows_reversed=False, taps_above_first=False, **kw)
+    assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
+
+
+FG_CASES, FG_INPUTS = golden_data.fgbg_grid()
+
+
+@pytest.mark.parametrize("case", FG_CASES, ids=[c["id"] for c in FG_CASES])
+def test_fgbg_layers_grid_sha256(case):
+    """The reference's recorded output clips of the served retime-fgbg grid cases: matte channels,
+    raw and composition planes, layer images, masked solves per layer, plates, refill, OVER."""
+    fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
+    w, h, n = case["width"], case["height"], case["frames"]
+    kw = golden_data.fgbg_case_params(case)
+    chans, sens = kw.pop("chans"), kw.pop("fg_sens")
+    p = O.retime_params(rows_reversed=True, taps_above_first=True, **kw)
+    mattes = [FG_INPUTS[m].view(O.DTYPE[fmt]) for m in case["mattes"]]
+    out = O.retime_fgbg_clip(FG_INPUTS[case["input"]].view(O.DTYPE[fmt]), n, mattes, chans, sens, w, h, fmt, p, n)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]

@@ -187,18 +187,25 @@ class VectorsSettings:
         return _VectorsSettings(self.flow._c(), np.float32(self.max_displace), int(self.rows_reversed))
 
 
+def fixed_param(v) -> np.float32:
+    """A slider value as the plugin reads it: through 16.16 fixed point (crates/fx-core/src/fixed.rs:
+    8-10, rounded half away from zero, saturated) and back (frontend.rs:131-133)."""
+    f = v * 65536.0 + (-0.5 if v < 0 else 0.5)
+    fixed = 0 if np.isnan(f) else int(np.clip(np.trunc(f), -2 ** 31, 2 ** 31 - 1))
+    return np.float32(np.float64(fixed) * (1.0 / 65536.0))
+
+
+def percent_param(v) -> np.float32:
+    """A percent slider (a sensitivity) as the fraction the solver takes."""
+    return np.float32(fixed_param(v) / np.float32(100.0))
+
+
 def vectors_settings(vector_resolution=1, max_displace=2048.0, sensitivity=70.0, track_rgb_a=False, hiq=True,
                      rows_reversed=True, taps_above_first=True) -> VectorsSettings:
     """The settings of plugin 02 (create-vectors) from its parameter values (glue.rs:133-146): the
     popup Vector Resolution, the 16.16 readers of Max Displace and Sensitivity (percent)."""
-    def fixed(v):
-        f = v * 65536.0 + (-0.5 if v < 0 else 0.5)
-        return int(np.clip(np.trunc(f), -2 ** 31, 2 ** 31 - 1))
-
-    def reader(v):
-        return np.float32(np.float64(fixed(v)) * (1.0 / 65536.0))
-
-    sens = np.float32(reader(sensitivity) / np.float32(100.0))
+    reader = fixed_param
+    sens = percent_param(sensitivity)
     fs = FlowSettings(quality=5 if vector_resolution == 2 else 4, hiq=hiq, sensitivity=sens, track_alpha=track_rgb_a,
                       taps_above_first=taps_above_first)
     return VectorsSettings(flow=fs, max_displace=float(np.float32(1.0) * reader(max_displace)), rows_reversed=rows_reversed)
@@ -298,6 +305,8 @@ def library():
                                  i32, i32, P]
     L.tw_retime_clip_device.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, ctypes.POINTER(_Selection), i32,
                                         i32, i32, i32, P]
+    L.tw_retime_layers_clip.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, i32, P, P, P, P,
+                                        ctypes.POINTER(_Selection), i32, i32, i32, i32, P]
     _lib = L
     return L
 
@@ -634,6 +643,28 @@ class Device:
         arr = (_Selection * len(sels))(*[s._c() for s in sels])
         self._check(self._L.tw_retime_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes, arr, len(sels),
                                            width, height, fmt, _ptr(out)))
+        return out
+
+    def retime_layers_clip(self, settings: RetimeSettings, frames, nframes: int, mattes, matte_chan, sensitivity, sels,
+                           width, height, fmt, matte_nframes=None, out=None):
+        """retime-fgbg with FG matte layers over a clip in host memory: ``mattes`` the FG1.. matte
+        clips (wire frames back to back, the footage's size and format), ``matte_chan`` their channel
+        popups (1 R, 2 G, 3 B, else alpha), ``sensitivity`` one value 0..1 per layer, Main_BG last.
+        Returns the output frames ``sels`` back to back."""
+        frames = np.ascontiguousarray(frames)
+        fs = width * height * 4
+        if out is None:
+            out = np.zeros(len(sels) * fs, DTYPES[fmt])
+        nfg = len(mattes)
+        mattes = [np.ascontiguousarray(m) for m in mattes]
+        clips = (ctypes.c_void_p * max(nfg, 1))(*[m.ctypes.data for m in mattes])
+        chans = np.ascontiguousarray(list(matte_chan) + [0], np.int32)
+        counts = None if matte_nframes is None else np.ascontiguousarray(matte_nframes, np.int32)
+        sens = np.ascontiguousarray(sensitivity, np.float32)
+        arr = (_Selection * max(len(sels), 1))(*[x._c() for x in sels])
+        self._check(self._L.tw_retime_layers_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes, nfg, clips,
+                                                  _ptr(counts), _ptr(chans), _ptr(sens),
+                                                  arr, len(sels), width, height, fmt, _ptr(out)))
         return out
 
     def retime_clip_device(self, settings: RetimeSettings, frames_ptr: int, nframes: int, sels, width, height, fmt,

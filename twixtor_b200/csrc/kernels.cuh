@@ -158,6 +158,7 @@ __global__ void k_encode_vectors(const float* __restrict__ flow, int fw, int fh,
                                  int fmt, float sx, float sy, float kx, float ky, int zero);
 
 // ---- the layered composition with plates (layers.cu) -----------------------------------------------
+__global__ void k_matte_extract(const void* __restrict__ eng, int fmt, int chan, long n, float* __restrict__ out);
 __global__ void k_matte_out_of_range(const float* __restrict__ m, long n, int* __restrict__ flag);
 __global__ void k_raw_plane(const float* __restrict__ m, long n, int fmt, const int* __restrict__ clamp,
                             float* __restrict__ out);

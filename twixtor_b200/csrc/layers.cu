@@ -20,6 +20,23 @@ __device__ __forceinline__ int64_t as_i64(float x) {
     return __float2ll_rz(x);
 }
 
+// matte.rs:141-188 (extract_raw): channel `chan` (1 R, 2 G, 3 B, else alpha) of an engine image as
+// a raw matte; 8 and 16 bpc the sample over white clamped to 0..1, float the sample times one (the
+// x86 product: a NaN keeps its payload, quieted)
+__global__ void k_matte_extract(const void* __restrict__ eng, int fmt, int chan, long n, float* __restrict__ out) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = chan == 1 ? 1 : chan == 2 ? 2 : chan == 3 ? 3 : 0;
+    float v;
+    if (fmt == 0) v = (float)((const uint8_t*)eng)[i * 4 + c] / 255.0f;
+    else if (fmt == 1) v = (float)((const uint16_t*)eng)[i * 4 + c] / 65535.0f;
+    else {
+        out[i] = x86::mul(((const float*)eng)[i * 4 + c], 1.0f);
+        return;
+    }
+    out[i] = v > 1.0f ? 1.0f : v > 0.0f ? v : 0.0f;  // matte.rs:79-87
+}
+
 // matte.rs:106-112: whether some value of a matte lies outside 0..1 (the clamp then applies to all)
 __global__ void k_matte_out_of_range(const float* __restrict__ m, long n, int* __restrict__ flag) {
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -201,7 +201,8 @@ struct tw_ctx {
     Taps g7{}, g5{}, b5{};
     // engine images, wire staging, pyramids, solve work, flows
     DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags, holes, fill, masks;
-    DevBuf lay_mem;  // tw_compose_layers: mattes, planes, layer images, plates, flows
+    DevBuf lay_mem;  // the layered path: planes, layer images, plates, flows
+    DevBuf lay_in;   // the layered path: the raw mattes at A and B
     DevBuf host_stage;  // unused placeholder for pinned staging
     std::vector<cudaEvent_t> ev_pool;  // the profiler's events (KernelProfile)
     // the forward warp: vertices, mip pyramid, per pixel counts / offsets, hit lists, flags
@@ -797,7 +798,7 @@ int tw_open(int device, tw_ctx** out) {
 void tw_close(tw_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->masks, &ctx->lay_mem, &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
+    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->masks, &ctx->lay_mem, &ctx->lay_in, &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
                     &ctx->fw_vd, &ctx->fw_pyr, &ctx->fw_tmp[0], &ctx->fw_tmp[1], &ctx->fw_cnt, &ctx->fw_off,
                     &ctx->fw_fill, &ctx->fw_sums, &ctx->fw_keys, &ctx->fw_cols, &ctx->fw_scratch, &ctx->fw_longq,
                     &ctx->fw_flags, &ctx->fw_out, &ctx->fw_cov})
@@ -1288,29 +1289,39 @@ int tw_fill_holes(tw_ctx* ctx, tw_image_mut* img, const void* mask, int32_t mask
 
 // ---- the layered composition with plates (layers/plates.rs:330-412) ---------------------------------
 
-int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection* sel, const tw_image* a,
-                      const tw_image* b, int32_t nfg, const float* mattes_a, const float* mattes_b,
-                      const float* sensitivity, tw_image_mut* out) {
-    if (!ctx) return TW_ERR_BAD_PARAM;
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    ctx->cur = ctx->stream;
-    if (!s || !sel || !sensitivity || !out || !out->data || nfg < 0 || nfg > 3 || (nfg > 0 && (!mattes_a || !mattes_b)))
-        return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
-    CHECK(check_image(ctx, a, "layers"));
-    CHECK(check_image(ctx, b, "layers"));
-    if (!same_shape(a, b) || out->width != a->width || out->height != a->height || out->fmt != a->fmt)
-        return ctx->fail(TW_ERR_MISMATCH, "layers: images of different shapes");
-    const tw_engine_settings& cs = s->compose;
+// The settings the layered path serves (warping codes 0 and 1, Nearest or Blend, no 360 filters).
+static int layers_check(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel) {
+    const tw_engine_settings& cs = s.compose;
     if (cs.warp_mode != 0 && cs.warp_mode != 1)
         return ctx->fail(TW_ERR_UNSUPPORTED, "layers: warping codes 2 and 3 are not on the device yet");
-    if (sel->interp != 0 && sel->interp != 1)
+    if (sel.interp != 0 && sel.interp != 1)
         return ctx->fail(TW_ERR_UNSUPPORTED, "layers: Weighted Blend is not on the device yet");
-    if (cs.wrap_360 || s->flow.wrap || s->flow.track_alpha)
+    if (cs.wrap_360 || s.flow.wrap || s.flow.track_alpha)
         return ctx->fail(TW_ERR_UNSUPPORTED, "layers: the wrap-around (360) filters are not on the device");
-    int W = a->width, H = a->height, fmt = a->fmt;
+    return TW_OK;
+}
+
+// The state a layered frame leaves in the flags, read after the stream is drained.
+static int layers_status(tw_ctx* ctx) {
+    int hf[4];
+    CHECK(finish(ctx, hf, 4));
+    if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
+    if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    if (hf[3]) return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of an image with a side of 1 pixel that has a hole");
+    return TW_OK;
+}
+
+// One layered frame on ctx->stream: the engine images A and B in ctx->eng[0] / ctx->eng[1] (motion
+// row order), `mat` the 2 x nfg raw mattes on the device (A's, then B's; FG1 first), sensitivity
+// nfg + 1 host values. Clears the flags first; *res_out receives the engine result (device).
+static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel_, int nfg, const float* mat,
+                      const float* sensitivity, int W, int H, int fmt, void** res_out) {
+    const tw_selection* sel = &sel_;
+    const tw_engine_settings& cs = s.compose;
+    CHECK(layers_check(ctx, s, sel_));
     long n = (long)W * H;
     size_t px = 4 * sample_bytes(fmt), ib = (size_t)n * px;
-    tw_flow_settings fs0 = s->flow;
+    tw_flow_settings fs0 = s.flow;
     fs0.quality = sel->vectors_quality;
     fs0.track_alpha = 0;  // plates.rs:323-327: the layered solves add no alpha to the luma
     Geo g;
@@ -1318,18 +1329,18 @@ int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selecti
     size_t pf = pyramid_floats(g);
     size_t fb = (size_t)g.w * g.h * 2;
     int L = nfg + 1;
-    // one block: mattes and raw planes (2 sides x nfg), comp planes and solver mattes (2 x L), layer
-    // images (2 x L), two plates, the result, the flows (2 x L), pyramids and mask pyramids (2 each)
+    // one block: raw planes (2 sides x nfg), comp planes (2 x L), a solver matte, layer images
+    // (2 x L), two plates, the result, the flows (2 x L), pyramids and mask pyramids (2 each)
     size_t fl = 0;
     auto take = [&](size_t floats) { size_t o = fl; fl += (floats + 63) & ~(size_t)63; return o; };
-    size_t o_mat = take(2 * (size_t)nfg * n), o_raw = take(2 * (size_t)nfg * n), o_comp = take(2 * (size_t)L * n);
+    size_t o_raw = take(2 * (size_t)nfg * n), o_comp = take(2 * (size_t)L * n);
     size_t o_smat = take(2 * (size_t)n), o_img = take(2 * (size_t)L * ib / 4 + 1), o_plate = take(2 * ib / 4 + 1);
     size_t o_res = take(ib / 4 + 1), o_flow = take(2 * (size_t)L * fb), o_pyr = take(4 * pf), o_mpyr = take(2 * pf);
     size_t o_scr = take(2 * (size_t)n);
     CHECK(ctx->ensure(ctx->lay_mem, fl * sizeof(float), "layer buffers"));
     CHECK(ctx->ensure(ctx->holes, (size_t)n, "holes mask"));
+    CHECK(ctx->ensure(ctx->eng[2], ib, "layer result"));
     float* M = ctx->lay_mem.as<float>();
-    float* mat = M + o_mat;
     float* raw = M + o_raw;
     float* comp = M + o_comp;
     float* smat = M + o_smat;
@@ -1343,15 +1354,7 @@ int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selecti
     int* flags = ctx->flags.as<int>();
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
     CHECK(ctx->cuda(cudaMemsetAsync(flags + FL_ONE, 0x01, sizeof(int), ctx->stream), "flags"));
-    CHECK(upload_image(ctx, ctx->eng[0], a));
-    CHECK(upload_image(ctx, ctx->eng[1], b));
     const void* frame[2] = {ctx->eng[0].p, ctx->eng[1].p};
-    if (nfg > 0) {
-        CHECK(ctx->cuda(cudaMemcpyAsync(mat, mattes_a, (size_t)nfg * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
-                        "matte upload"));
-        CHECK(ctx->cuda(cudaMemcpyAsync(mat + (size_t)nfg * n, mattes_b, (size_t)nfg * n * sizeof(float),
-                                        cudaMemcpyHostToDevice, ctx->stream), "matte upload"));
-    }
     // plates.rs:50-57: the raw planes (each matte clamped when one of its values leaves 0..1)
     for (int side = 0; side < 2; side++)
         for (int j = 0; j < nfg; j++) {
@@ -1409,8 +1412,6 @@ int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selecti
         const float* fab = need_ab ? flow(0, k) : nullptr;
         const float* fba = need_ba ? flow(1, k) : nullptr;
         void* dst = k == nfg ? res : ctx->eng[2].p;
-        CHECK(ctx->ensure(ctx->eng[2], ib, "layer result"));
-        if (k != nfg) dst = ctx->eng[2].p;
         if (sel->interp == 0) {
             bool takes_a = cs.warp_mode == 0 ? 0.5f <= sel->wa : !(0.5f > sel->wa);  // layers.rs:697-703
             int side = takes_a ? 0 : 1;
@@ -1433,13 +1434,39 @@ int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selecti
         }
         if (k != nfg) LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, res, dst, fmt, n);
     }
-    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, res, ib, cudaMemcpyDeviceToHost, ctx->stream), "download"));
-    int hf[4];
-    CHECK(finish(ctx, hf, 4));
-    if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
-    if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
-    if (hf[3]) return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of an image with a side of 1 pixel that has a hole");
+    *res_out = res;
     return TW_OK;
+}
+
+int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection* sel, const tw_image* a,
+                      const tw_image* b, int32_t nfg, const float* mattes_a, const float* mattes_b,
+                      const float* sensitivity, tw_image_mut* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!s || !sel || !sensitivity || !out || !out->data || nfg < 0 || nfg > 3 || (nfg > 0 && (!mattes_a || !mattes_b)))
+        return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    CHECK(check_image(ctx, a, "layers"));
+    CHECK(check_image(ctx, b, "layers"));
+    if (!same_shape(a, b) || out->width != a->width || out->height != a->height || out->fmt != a->fmt)
+        return ctx->fail(TW_ERR_MISMATCH, "layers: images of different shapes");
+    CHECK(layers_check(ctx, *s, *sel));
+    int W = a->width, H = a->height, fmt = a->fmt;
+    size_t n = (size_t)W * H, ib = n * 4 * sample_bytes(fmt);
+    CHECK(ctx->ensure(ctx->lay_in, std::max<size_t>(2 * (size_t)nfg * n, 1) * sizeof(float), "mattes"));
+    float* mat = ctx->lay_in.as<float>();
+    CHECK(upload_image(ctx, ctx->eng[0], a));
+    CHECK(upload_image(ctx, ctx->eng[1], b));
+    if (nfg > 0) {
+        CHECK(ctx->cuda(cudaMemcpyAsync(mat, mattes_a, (size_t)nfg * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
+                        "matte upload"));
+        CHECK(ctx->cuda(cudaMemcpyAsync(mat + (size_t)nfg * n, mattes_b, (size_t)nfg * n * sizeof(float),
+                                        cudaMemcpyHostToDevice, ctx->stream), "matte upload"));
+    }
+    void* res = nullptr;
+    CHECK(layers_dev(ctx, *s, *sel, nfg, mat, sensitivity, W, H, fmt, &res));
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, res, ib, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    return layers_status(ctx);
 }
 
 // ---- the forward warp (forward.rs:229-373) -----------------------------------------------------------
@@ -2017,6 +2044,73 @@ int tw_retime_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames,
         [&](int k, Lane& L, const void* wa, const void* wb, void* ow) {
             return retime_frame_lane(ctx, L, *s, sels[k], wa, wb, width, height, fmt, ow);
         });
+}
+
+// retime-fgbg with FG matte layers over a clip in host memory: per output frame the footage and
+// matte frames are uploaded, the in-between frames run the layered path in the motion path's row
+// order and the exact frames the interpolation without flows (the full group fast path,
+// layers.rs:177-179), each frame on the context's stream.
+int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes, int32_t nfg,
+                          const void* const* matte_clips, const int32_t* matte_nframes, const int32_t* matte_chan,
+                          const float* sensitivity, const tw_selection* sels, int32_t nout, int32_t width,
+                          int32_t height, int32_t fmt, void* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    if (nfg == 0 && sels && s) return tw_retime_clip(ctx, s, frames, nframes, sels, nout, width, height, fmt, out);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!s || !sels || !frames || !out || !sensitivity || !matte_clips || !matte_chan || nfg < 0 || nfg > 3 || fmt < 0 ||
+        fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
+        return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    for (int j = 0; j < nfg; j++)
+        if (!matte_clips[j] || (matte_nframes && matte_nframes[j] < 0)) return ctx->fail(TW_ERR_BAD_PARAM, "bad matte clip");
+    int W = width, H = height;
+    long n = (long)W * H;
+    size_t bytes = (size_t)n * 4 * sample_bytes(fmt);
+    for (int i = 0; i < 3; i++) CHECK(ctx->ensure(ctx->wire[i], bytes, "wire staging"));
+    for (int i = 0; i < 3; i++) CHECK(ctx->ensure(ctx->eng[i], bytes, "engine images"));
+    CHECK(ctx->ensure(ctx->lay_in, 2 * (size_t)nfg * n * sizeof(float), "mattes"));
+    CHECK(ctx->ensure(ctx->flags, FLAGS_BYTES, "flags"));
+    float* mat = ctx->lay_in.as<float>();
+    int* flags = ctx->flags.as<int>();
+    // a frame of a clip in the staging buffer dst, or a blank frame outside the clip (host.rs:338-352)
+    auto upload = [&](const void* clip, int count, int f, void* dst) -> int {
+        if (f >= 0 && f < count)
+            return ctx->cuda(cudaMemcpyAsync(dst, (const uint8_t*)clip + (size_t)f * bytes, bytes, cudaMemcpyHostToDevice,
+                                             ctx->stream), "upload");
+        return ctx->cuda(cudaMemsetAsync(dst, 0, bytes, ctx->stream), "blank");
+    };
+    for (int k = 0; k < nout; k++) {
+        const tw_selection& sel = sels[k];
+        bool vector = sel.vectors_quality != 0 && !sel.exact;
+        bool flip = vector && s->motion_rows_reversed != 0;
+        CHECK(upload(frames, nframes, sel.a, ctx->wire[0].p));
+        CHECK(upload(frames, nframes, sel.b, ctx->wire[1].p));
+        from_frame_dev(ctx, ctx->wire[0].p, ctx->eng[0].p, W, H, fmt, flip);
+        from_frame_dev(ctx, ctx->wire[1].p, ctx->eng[1].p, W, H, fmt, flip);
+        uint8_t* dst = (uint8_t*)out + (size_t)k * bytes;
+        if (!vector) {
+            CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
+            CHECK(interpolate_dev(ctx, sel, ctx->eng[0].p, ctx->eng[1].p, W, H, fmt, ctx->wire[2].p, true, flags + FL_BAD));
+        } else {
+            // matte.rs:141-188: each layer's raw matte at A and at B, in the same row order
+            for (int side = 0; side < 2; side++)
+                for (int j = 0; j < nfg; j++) {
+                    int count = matte_nframes ? matte_nframes[j] : nframes;
+                    CHECK(upload(matte_clips[j], count, side ? sel.b : sel.a, ctx->wire[2].p));
+                    from_frame_dev(ctx, ctx->wire[2].p, ctx->eng[2].p, W, H, fmt, flip);
+                    LAUNCH(ctx, k_matte_extract, grid1(n), TB, 0, ctx->eng[2].p, fmt, matte_chan[j], n,
+                           mat + ((size_t)side * nfg + j) * n);
+                }
+            void* res = nullptr;
+            CHECK(layers_dev(ctx, *s, sel, nfg, mat, sensitivity, W, H, fmt, &res));
+            if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)res, ctx->wire[2].as<uint8_t>(), W, H, flip);
+            else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)res, ctx->wire[2].as<uint16_t>(), W, H, flip);
+            else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)res, ctx->wire[2].as<float>(), W, H, flip);
+        }
+        CHECK(ctx->cuda(cudaMemcpyAsync(dst, ctx->wire[2].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+        CHECK(layers_status(ctx));
+    }
+    return TW_OK;
 }
 
 // ---- Create Vectors ----------------------------------------------------------------------------------
