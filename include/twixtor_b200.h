@@ -106,6 +106,9 @@ typedef struct tw_engine_settings {
     int32_t quality_high;
     float blur;               /* Blur Compensation slider */
     int32_t taps_above_first; /* Stages::vertical_taps() of the stage set (stages.rs:66-70) */
+    int32_t gouraud;          /* forward warps of codes 2/3 as the Gouraud variant: the stage set is
+                                 wrapped in stages::GouraudForward (stages.rs:101-129), as retime-fgbg's
+                                 is (plugins/retime-fgbg/src/glue.rs:142-143); 0 the textured warp */
 } tw_engine_settings;
 
 /* Everything one output frame of the `retime` effect needs beyond its selection: the flow

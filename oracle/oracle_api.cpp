@@ -390,7 +390,7 @@ void or_logf(const float* x, float* out, long n) {
 // compose::compose_vectors with a warping code (0 inverse, 1 Smart Blend) and the binary alpha flag
 int or_compose_vectors2(const void* a_eng, const void* b_eng, int w, int h, int fmt, const float* f_ab, const float* f_ba,
                         int fw, int fh, float wa, int interp, int warp_mode, int video_360, int taps_above_first,
-                        void* out_eng) {
+                        int gouraud, void* out_eng) {
     Image a(w, h, (Fmt)fmt), b(w, h, (Fmt)fmt), out;
     std::memcpy(a.data(), a_eng, a.bytes());
     std::memcpy(b.data(), b_eng, b.bytes());
@@ -401,6 +401,7 @@ int or_compose_vectors2(const void* a_eng, const void* b_eng, int w, int h, int 
     cs.warp_mode = warp_mode;
     cs.video_360 = video_360 != 0;
     cs.taps_above_first = taps_above_first != 0;
+    cs.gouraud = gouraud != 0;
     Selection sel;
     sel.wa = wa;
     sel.interp = interp;
@@ -484,7 +485,7 @@ int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const 
         FlowField fab, fba;
         bool have_ab = false, have_ba = false;
         if (interp == 0) {
-            if (nearest_uses_f_ab(wa, p->smart_blend ? 1 : 0)) {
+            if (nearest_uses_f_ab(wa, p->smart_blend)) {
                 if (!solve(ar, br, fs, &fab, &e)) return fail(1, e);
                 have_ab = true;
             } else {
@@ -498,7 +499,7 @@ int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const 
         ComposeSettings cs;
         cs.quality_high = fs.hiq;
         cs.blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
-        cs.warp_mode = p->smart_blend ? 1 : 0;  // plugins/retime frontend: warp_mode = i32::from(smart_blend)
+        cs.warp_mode = p->smart_blend;  // plugins/retime frontend: warp_mode = i32::from(smart_blend); 2, 3 the Warping popup of plugin 03
         cs.video_360 = p->video_360 != 0;
         cs.taps_above_first = p->taps_above_first != 0;
         Image o;
@@ -541,7 +542,7 @@ static std::vector<float> flip_matte(const std::vector<float>& m, int w, int h) 
 // Output frame n of retime-fgbg with `nfg` FG matte clips (wire frames back to back, the size and
 // format of the footage): fg_chan / fg_sens per layer (popup 1..4, sensitivity 0..100). The
 // selection is the retime time map of p (plugin 03's without the source time offset: the same at
-// equal rates); p->smart_blend carries the warping code (0 or 1). Display Twixtored Output, no
+// equal rates); p->smart_blend carries the warping code (0 to 3). Display Twixtored Output, no
 // inverse matte shrink, no tracking points.
 int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte_clips, int nfg, const int* fg_chan,
                        const double* fg_sens, int w, int h, int fmt, const or_retime_params* p, int n, void* out) {
@@ -554,14 +555,16 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
     float s0, s1, wa;
     int a, exact, vq, interp;
     or_select(p, n, w, h, &s0, &s1, &a, &wa, &exact, &vq, &interp);
-    auto fetch = [&](const void* clip, int pos) -> Image {
+    // the FG matte frames are read straight (plugins/retime-fgbg/src/glue.rs:335, host.rs:311-314)
+    auto fetch = [&](const void* clip, int pos, bool straight) -> Image {
         double d = (double)(float)pos;
         int time = cvtt_i32_d(d * (double)time_step + 0.5);
         long long idx = time >= 0 ? time / time_step : -(((long long)-time + time_step - 1) / time_step);
         if (idx < 0 || idx >= nframes) return Image(w, h, f);
-        return from_frame((const uint8_t*)clip + (size_t)idx * frame_bytes, w, h, f);
+        const uint8_t* fr = (const uint8_t*)clip + (size_t)idx * frame_bytes;
+        return straight ? from_frame_straight(fr, w, h, f) : from_frame(fr, w, h, f);
     };
-    Image A = fetch(frames, a), B = fetch(frames, a + 1), result;
+    Image A = fetch(frames, a, false), B = fetch(frames, a + 1, false), result;
     Selection sel;
     sel.s0 = s0; sel.s1 = s1; sel.a = a; sel.b = a + 1; sel.wa = wa; sel.exact = exact != 0;
     sel.vectors_quality = vq; sel.interp = interp;
@@ -570,8 +573,8 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
         if (interp < 0 || interp > 1) return fail(2, "weighted blend on the vector path is not restated");
         LayerJob job;
         for (int k = 0; k < nfg; k++) {
-            std::vector<float> ma = extract_raw(fetch(matte_clips[k], a), fg_chan[k]);
-            std::vector<float> mb = extract_raw(fetch(matte_clips[k], a + 1), fg_chan[k]);
+            std::vector<float> ma = extract_raw(fetch(matte_clips[k], a, true), fg_chan[k]);
+            std::vector<float> mb = extract_raw(fetch(matte_clips[k], a + 1, true), fg_chan[k]);
             if (p->rows_reversed) { ma = flip_matte(ma, w, h); mb = flip_matte(mb, w, h); }
             job.mattes_a.push_back(std::move(ma));
             job.mattes_b.push_back(std::move(mb));
@@ -582,7 +585,8 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
         job.fs.hiq = p->quality_high != 0;
         job.fs.taps_above_first = p->taps_above_first != 0;
         job.cs.quality_high = p->quality_high != 0;
-        job.cs.warp_mode = p->smart_blend ? 1 : 0;
+        job.cs.warp_mode = p->smart_blend;
+        job.cs.gouraud = true;  // plugins/retime-fgbg/src/glue.rs:142-143: every forward warp is the Gouraud variant
         job.cs.taps_above_first = p->taps_above_first != 0;
         job.sel = sel;
         Image ar = p->rows_reversed ? rows_reversed(A) : A, br = p->rows_reversed ? rows_reversed(B) : B;
@@ -674,7 +678,7 @@ int or_solve_masked(const void* x_eng, const void* y_eng, int w, int h, int fmt,
 // settings; out: the engine image
 int or_compose_layers(const void* a_eng, const void* b_eng, int w, int h, int fmt, int nfg, const float* mattes_a,
                       const float* mattes_b, const float* sens, int quality, int hiq, int above_first, int warp_mode,
-                      int video_360, float wa, int interp, void* out_eng) {
+                      int video_360, int gouraud, float wa, int interp, void* out_eng) {
     Image a(w, h, (Fmt)fmt), b(w, h, (Fmt)fmt), out;
     std::memcpy(a.data(), a_eng, a.bytes());
     std::memcpy(b.data(), b_eng, b.bytes());
@@ -692,6 +696,7 @@ int or_compose_layers(const void* a_eng, const void* b_eng, int w, int h, int fm
     job.cs.warp_mode = warp_mode;
     job.cs.video_360 = video_360 != 0;
     job.cs.taps_above_first = above_first != 0;
+    job.cs.gouraud = gouraud != 0;
     job.sel.wa = wa;
     job.sel.interp = interp;
     job.sel.exact = false;

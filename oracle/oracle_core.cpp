@@ -2,6 +2,7 @@
 // the reference file:line (crate plugins/retime-engine/src/) whose arithmetic it restates.
 #include "oracle_core.h"
 #include "oracle_smart.h"
+#include "oracle_forward.h"
 
 #include <algorithm>
 #include <cstdio>
@@ -81,6 +82,33 @@ static inline void unpremultiply_f32(const float p[4], float o[4]) {
         r[3] = nr::mul(p[3], inv);
     }
     for (int c = 0; c < 4; c++) o[c] = r[c];
+}
+
+// image.rs:142-171 (from_frame_straight): the channels as stored, in the engine order A, R, G, B; 16
+// bpc every channel to 0..32768 and then scaled like the alpha of from_frame
+Image from_frame_straight(const void* wire, int w, int h, Fmt fmt) {
+    Image img(w, h, fmt);
+    size_t n = (size_t)w * h;
+    if (fmt == U8) {
+        const uint8_t* px = (const uint8_t*)wire;
+        for (size_t i = 0; i < n; i++) {
+            uint8_t* o = &img.u8[i * 4];
+            o[0] = px[i * 4 + 3]; o[1] = px[i * 4 + 0]; o[2] = px[i * 4 + 1]; o[3] = px[i * 4 + 2];
+        }
+    } else if (fmt == U16) {
+        const uint16_t* px = (const uint16_t*)wire;
+        static const int order[4] = {3, 0, 1, 2};
+        for (size_t i = 0; i < n; i++)
+            for (int c = 0; c < 4; c++)
+                img.u16[i * 4 + c] = (uint16_t)q((float)u16_to_q15(px[i * 4 + order[c]]) * PREMUL_16_ALPHA);
+    } else {
+        const float* pl = (const float*)wire;  // planes G, B, R, A
+        for (size_t i = 0; i < n; i++) {
+            float* o = &img.f32[i * 4];
+            o[0] = pl[3 * n + i]; o[1] = pl[2 * n + i]; o[2] = pl[0 * n + i]; o[3] = pl[1 * n + i];
+        }
+    }
+    return img;
 }
 
 Image from_frame(const void* wire, int w, int h, Fmt fmt) {
@@ -1176,7 +1204,8 @@ int compose_vectors(const ComposeSettings& cs, const Selection& sel, const Image
                     const FlowField* f_ab, const FlowField* f_ba, Image* out, std::string* err) {
     if (cs.blur > 0.005f && std::fabs(sel.s0 - sel.s1) > 1e-6f) { *err = "blur compensation is not restated"; return 2; }
     if (cs.warp_mode == 1) return compose_smart(cs, sel, a, b, f_ab, f_ba, cs.taps_above_first, out, err);
-    if (cs.warp_mode != 0) { *err = "compose: warping codes 2 and 3 are not restated here"; return 2; }
+    if (cs.warp_mode == 2 || cs.warp_mode == 3) return compose_forward(cs, sel, a, b, f_ab, f_ba, out, err);
+    if (cs.warp_mode != 0) { *err = "compose: warping code not 0 to 3"; return 1; }
     float wa = sel.wa;
     float frac = 1.0f - wa;
     WarpOpts o;

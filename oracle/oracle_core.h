@@ -113,6 +113,7 @@ void premultiply_u8(const uint8_t p[4], uint8_t o[4]);
 void premultiply_f32(const float p[4], float o[4]);
 void unpremultiply_u8(const uint8_t p[4], uint8_t o[4]);
 Image from_frame(const void* wire, int w, int h, Fmt fmt);                  // image.rs:178-206
+Image from_frame_straight(const void* wire, int w, int h, Fmt fmt);         // image.rs:142-171
 void to_frame(const Image& img, void* wire);                                 // image.rs:213-245
 Image rows_reversed(const Image& img);                                       // image.rs:96-114
 
@@ -231,6 +232,7 @@ struct ComposeSettings {
     bool quality_high = true;
     float blur = 0.0f;        // blur compensation slider
     bool taps_above_first = true;  // Stages::vertical_taps() of the hole fill (stages.rs:66-70)
+    bool gouraud = false;     // forward warps of codes 2/3 as the Gouraud variant (stages::GouraudForward)
 };
 
 bool nearest_uses_f_ab(float wa, int code);

@@ -5,6 +5,7 @@
 // forward/pyramid.rs (the mip pyramid and its sampler). The render is sequential in cell order
 // like the reference's, so the running mean of every pixel folds its hits in the same order.
 #include "oracle_forward.h"
+#include "oracle_smart.h"
 
 #include <algorithm>
 #include <cmath>
@@ -600,6 +601,48 @@ int forward_warp(Image& out, const Image& src, const FlowField& flow, float amou
         for (size_t i = 0; i < cov->d.size(); i++) cov->d[i] = cnt[i] != 0 ? 0xff : 0;
     }
     return 0;
+}
+
+// ---- the compositions of the forward warp codes (compose/vector.rs:117-147, forward.rs:384-496) ----
+// The forward warps are the textured variant unless cs.gouraud (the stage set of retime-fgbg,
+// plugins/retime-fgbg/src/glue.rs:142-143, wraps every forward warp as the Gouraud variant).
+
+int compose_forward(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b,
+                    const FlowField* f_ab, const FlowField* f_ba, Image* out, std::string* err) {
+    float wa = sel.wa;
+    bool fill = cs.warp_mode == 2;
+    *out = Image(a.w, a.h, a.fmt);
+    if (sel.interp == 0) {
+        // the pushed frame uses its own flow: F_AB for wa >= 0.5 (nearest_uses_f_ab with code 2 / 3)
+        const FlowField* flow = nearest_uses_f_ab(wa, cs.warp_mode) ? f_ab : f_ba;
+        if (!flow) { *err = "missing flow"; return 1; }
+        Coverage cov;
+        bool take_a = !(0.5f > wa);  // a NaN weight takes A
+        int rc = take_a ? forward_warp(*out, a, *flow, 1.0f - wa, !cs.gouraud, fill ? &cov : nullptr, err)
+                        : forward_warp(*out, b, *flow, wa, !cs.gouraud, fill ? &cov : nullptr, err);
+        if (rc || !fill) return rc;
+        for (auto& v : cov.d) v = 0xff - v;  // warp.rs:76-80
+        return fill_holes(*out, cov.d.data(), 1, cs.taps_above_first, err);
+    }
+    if (sel.interp == 1) {
+        if (!f_ab || !f_ba) { *err = "missing flow"; return 1; }
+        float frac = 1.0f - wa;
+        Image ta(a.w, a.h, a.fmt), tb(b.w, b.h, b.fmt);
+        Coverage c1, c2;
+        int rc = forward_warp(ta, a, *f_ab, frac, !cs.gouraud, fill ? &c1 : nullptr, err);
+        if (rc) return rc;
+        rc = forward_warp(tb, b, *f_ba, wa, !cs.gouraud, fill ? &c2 : nullptr, err);
+        if (rc) return rc;
+        if (!fill) {  // smartblend.rs:458-477 without coverage: the plain blend
+            blend(*out, ta, tb, frac);
+            return 0;
+        }
+        smart_blend(*out, ta, tb, frac, cs.video_360);  // smart_composite, then smart_finish_with
+        for (size_t i = 0; i < c1.d.size(); i++) c1.d[i] = 0xff - std::max(c1.d[i], c2.d[i]);
+        return fill_holes(*out, c1.d.data(), 1, cs.taps_above_first, err);
+    }
+    *err = "weighted blend with the forward warps is not restated";
+    return 2;
 }
 
 }  // namespace orc

@@ -27,5 +27,11 @@ void fw_triangle(const FwVtx tri[3], int w1, int h1, FwHits* sink);             
 // Returns 0, 1 (mismatch) or 2 (unsupported: the degenerate pass would write outside).
 int forward_warp(Image& out, const Image& src, const FlowField& flow, float amount, bool pyramid, Coverage* cov,
                  std::string* err);
+// compose/vector.rs:117-147 (compose_forward) with forward.rs:384-496: warping codes 2 (coverage,
+// Smart Blend or its binary variant, combine, invert, hole fill) and 3 (no coverage), Nearest and
+// Blend; the textured forward warp, or the Gouraud variant with cs.gouraud. Weighted Blend returns
+// 2 (not restated).
+int compose_forward(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b,
+                    const FlowField* f_ab, const FlowField* f_ba, Image* out, std::string* err);
 
 }  // namespace orc

@@ -4,6 +4,7 @@
 // Restated scope: warping codes 0 and 1, Nearest and Blend, zero inverse matte shrink (the choke
 // of the cut is then the clamp of the plane), no tracking points, no wrap-around.
 #include "oracle_layers.h"
+#include "oracle_forward.h"
 
 #include <algorithm>
 #include <cmath>
@@ -231,7 +232,7 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
     }
     const Selection& sel = job.sel;
     int code = job.cs.warp_mode;
-    if (code != 0 && code != 1) { *err = "plates: warping codes 2 and 3 are not restated"; return 2; }
+    if (code < 0 || code > 3) { *err = "plates: warping code not 0 to 3"; return 1; }
     if (sel.interp != 0 && sel.interp != 1) { *err = "plates: Weighted Blend is not restated"; return 2; }
     // plates.rs:330-370: the solves, one layer after the other
     std::vector<FlowField> f_ab(nfg + 1), f_ba(nfg + 1);
@@ -280,12 +281,15 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
             rc = compose_vectors(job.cs, sel, p, p, fab, fba, &r, err);
             if (rc) return rc;
         } else {
-            WarpOpts o;  // hold edges, amount 1 (plates.rs:260-268)
+            // plates.rs:268-288: each side's plate is its own layer image OVER the other side's brought
+            // to its time with amount 1: the inverse warp with hold edges (codes 0 and 1, A's plate reads
+            // F_AB), the forward warp without coverage (codes 2 and 3, each side pushed by its own flow)
+            WarpOpts o;
             Image pa(w, h, fmt), pb(w, h, fmt);
-            int rc = inv_warp(pa, lb, *fab, 1.0f, o, nullptr, err);
+            int rc = code >= 2 ? forward_warp(pa, lb, *fba, 1.0f, !job.cs.gouraud, nullptr, err) : inv_warp(pa, lb, *fab, 1.0f, o, nullptr, err);
             if (rc) return rc;
             over_pl(pa, la);
-            rc = inv_warp(pb, la, *fba, 1.0f, o, nullptr, err);
+            rc = code >= 2 ? forward_warp(pb, la, *fab, 1.0f, !job.cs.gouraud, nullptr, err) : inv_warp(pb, la, *fba, 1.0f, o, nullptr, err);
             if (rc) return rc;
             over_pl(pb, lb);
             rc = refill(pa, pl_a, fr_a, job.cs.taps_above_first, err);

@@ -23,8 +23,8 @@ Writes, next to this script:
   whose vertical border taps came below first: the tests run those cases with
   ``rows_reversed=False, taps_above_first=False``.
 * ``fgbg_layers_grid.npz`` - the cases of the reference's parity grid ``parity/fgbg-layers`` that
-  the layered path with plates serves (FG matte layers FG1.. consecutive, warping Inverse or
-  Inverse w/ Smart Blend, Nearest or Blend, no inverse matte shrink, no tracking points, Display
+  the layered path with plates serves (FG matte layers FG1.. consecutive, the four warping codes,
+  Nearest or Blend, no inverse matte shrink, no tracking points, Display
   Twixtored Output, integer frame rates), their footage and matte clips as its ``gen_grid.py``
   renders them, and the sha256 of the output clip ``results/base.tsv`` records (the reference's
   current revision: rows reversed, taps above first).
@@ -163,7 +163,7 @@ def fgbg_layers_grid(ref):
         params = dict(p.split("=", 1) for p in c["params"])
         if any(k not in FG_SERVED for k in params) or any("@" in v for v in params.values()):
             continue
-        if params.get("warping", "1") not in ("1", "2") or params.get("frame_interp", "2") not in ("1", "2"):
+        if params.get("warping", "1") not in ("1", "2", "3", "4") or params.get("frame_interp", "2") not in ("1", "2"):
             continue
         if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
             continue

@@ -37,11 +37,12 @@ def fgbg_grid():
 
 def fgbg_case_params(case):
     """The parameters of a fgbg-layers grid case (plugin defaults where the case sets none): the
-    retime selection and Main_BG settings, and per FG layer its channel popup and sensitivity."""
+    retime selection and Main_BG settings (``smart_blend`` carries the warping code, the Warping
+    popup minus one, glue.rs:94-100), and per FG layer its channel popup and sensitivity."""
     p = dict(x.split("=", 1) for x in case["params"])
     nfg = len(case["mattes"])
     return dict(fps=(int(case["fps"]), 1), speed=float(p.get("speed_percent", 100)), vectors=int(p.get("vectors", 5)),
-                frame_interp=int(p.get("frame_interp", 2)), smart_blend=int(p.get("warping", "1") == "2"),
+                frame_interp=int(p.get("frame_interp", 2)), smart_blend=int(p.get("warping", "1")) - 1,
                 sensitivity=float(p.get("main_bg_sensitivity", 70)),
                 chans=[int(p.get(f"fg{k + 1}_matte_chan", 1)) for k in range(nfg)],
                 fg_sens=[float(p.get(f"fg{k + 1}_sensitivity", 70)) for k in range(nfg)])

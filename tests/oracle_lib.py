@@ -83,14 +83,14 @@ def lib():
         L.or_set_threads.argtypes = [i]
         L.or_smart_blend.argtypes = [P, P, P, i, i, i, f, i]
         L.or_fill_holes.argtypes = [P, i, i, i, P, i, i]
-        L.or_compose_vectors2.argtypes = [P, P, i, i, i, P, P, i, i, f, i, i, i, i, P]
+        L.or_compose_vectors2.argtypes = [P, P, i, i, i, P, P, i, i, f, i, i, i, i, i, P]
         L.or_forward_warp.argtypes = [P, P, i, i, i, P, i, i, f, i, P]
         L.or_fw_mip_level.argtypes = [i, i, P, i, i, f, i, i]
         L.or_fw_mip_level.restype = f
         L.or_fw_level_count.argtypes = [i, i]
         L.or_fw_triangle.argtypes = [P, i, i, P, i]
         L.or_logf.argtypes = [P, P, ctypes.c_long]
-        L.or_compose_layers.argtypes = [P, P, i, i, i, i, P, P, P, i, i, i, i, i, f, i, P]
+        L.or_compose_layers.argtypes = [P, P, i, i, i, i, P, P, P, i, i, i, i, i, i, f, i, P]
         L.or_mask_pyramid.argtypes = [P, i, i, i, i, i, P, P, i]
         L.or_mask_gradient.argtypes = [P, P, i, i]
         L.or_calc_b_masked.argtypes = [P, P, P, P, i, i, P, P]
@@ -175,12 +175,13 @@ def compose_vectors(a, b, w, h, fmt, f_ab, f_ba, fw, fh, wa, interp=1):
 
 
 def compose_vectors2(a, b, w, h, fmt, f_ab, f_ba, fw, fh, wa, interp, warp_mode, video_360=False,
-                     taps_above_first=True):
-    """compose_vectors with a warping code (1: Smart Blend with the hole fill) and the binary alpha flag."""
+                     taps_above_first=True, gouraud=False):
+    """compose_vectors with a warping code (1: Smart Blend with the hole fill, 2 / 3 the forward warps
+    with / without coverage and fill; ``gouraud`` their Gouraud variant) and the binary alpha flag."""
     out = np.zeros_like(a)
     rc = lib().or_compose_vectors2(ptr(a), ptr(b), w, h, fmt, ptr(f_ab) if f_ab is not None else None,
                                    ptr(f_ba) if f_ba is not None else None, fw, fh, wa, interp, warp_mode,
-                                   int(video_360), int(taps_above_first), ptr(out))
+                                   int(video_360), int(taps_above_first), int(gouraud), ptr(out))
     if rc:
         raise ValueError(err())
     return out
@@ -255,7 +256,7 @@ def solve_masked(x, y, w, h, fmt, matte_x=None, matte_y=None, quality=4, hiq=Tru
 
 
 def compose_layers(a, b, w, h, fmt, mattes_a, mattes_b, sensitivity, wa, interp=1, quality=4, hiq=True,
-                   above_first=True, warp_mode=0, video_360=False):
+                   above_first=True, warp_mode=0, video_360=False, gouraud=False):
     """layers/plates.rs solve_and_compose_plates of one in-between frame (engine images in and out)."""
     nfg = len(mattes_a)
     ma = np.ascontiguousarray(np.concatenate(mattes_a) if nfg else np.zeros(1), np.float32)
@@ -263,7 +264,8 @@ def compose_layers(a, b, w, h, fmt, mattes_a, mattes_b, sensitivity, wa, interp=
     sens = np.ascontiguousarray(sensitivity, np.float32)
     out = np.zeros_like(a)
     rc = lib().or_compose_layers(ptr(a), ptr(b), w, h, fmt, nfg, ptr(ma), ptr(mb), ptr(sens), quality, int(hiq),
-                                 int(above_first), warp_mode, int(video_360), np.float32(wa), interp, ptr(out))
+                                 int(above_first), warp_mode, int(video_360), int(gouraud), np.float32(wa), interp,
+                                 ptr(out))
     if rc:
         raise ValueError(err())
     return out

@@ -51,12 +51,13 @@ def scene(w, h, fmt, nfg, seed, soft=0.0):
     return a, b, ma, mb
 
 
-def run(dev, a, b, w, h, fmt, ma, mb, sens, wa, interp, code, video_360=False):
+def run(dev, a, b, w, h, fmt, ma, mb, sens, wa, interp, code, video_360=False, gouraud=False):
     s = tw.RetimeSettings(flow=tw.FlowSettings(video_range_luma=video_360),
-                          compose=tw.EngineSettings(warp_mode=code, video_360=video_360))
+                          compose=tw.EngineSettings(warp_mode=code, video_360=video_360, gouraud=gouraud))
     sel = tw.Selection(wa=np.float32(wa), exact=False, vectors_quality=4, interp=interp)
     got = dev.compose_layers(s, sel, a, b, w, h, fmt, ma, mb, sens)
-    want = O.compose_layers(a, b, w, h, fmt, ma, mb, sens, np.float32(wa), interp, warp_mode=code, video_360=video_360)
+    want = O.compose_layers(a, b, w, h, fmt, ma, mb, sens, np.float32(wa), interp, warp_mode=code, video_360=video_360,
+                            gouraud=gouraud)
     assert same(got, want)
 
 
@@ -69,6 +70,17 @@ def test_layers_match_oracle(dev, fmt, nfg, code, wa, interp):
     a, b, ma, mb = scene(w, h, fmt, nfg, seed=11 + nfg)
     sens = [0.7, 0.5, 0.9][:nfg] + [0.7]
     run(dev, a, b, w, h, fmt, ma, mb, sens, wa, interp, code)
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("code", [2, 3])
+@pytest.mark.parametrize("gouraud", [True, False])
+@pytest.mark.parametrize("wa,interp", [(0.4, 1), (0.6, 0), (0.3, 0)])
+def test_layers_forward_codes(dev, fmt, code, gouraud, wa, interp):
+    """Warping codes 2 and 3: plates pushed by the forward warp, the forward compositions per layer."""
+    w, h = 80, 48
+    a, b, ma, mb = scene(w, h, fmt, 2, seed=21 + code)
+    run(dev, a, b, w, h, fmt, ma, mb, [0.7, 0.5, 0.7], wa, interp, code, gouraud=gouraud)
 
 
 @pytest.mark.parametrize("fmt", [0, 2])
@@ -117,7 +129,8 @@ def fgbg_clip(dev, case, rows_reversed=True, taps_above_first=True):
     tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], vectors=kw["vectors"], frame_interp=kw["frame_interp"])
     sels = [tw.select(tp, k, w, h) for k in range(n)]
     s = tw.RetimeSettings(flow=tw.FlowSettings(hiq=True, taps_above_first=taps_above_first),
-                          compose=tw.EngineSettings(warp_mode=kw["smart_blend"], taps_above_first=taps_above_first),
+                          compose=tw.EngineSettings(warp_mode=kw["smart_blend"], taps_above_first=taps_above_first,
+                                                    gouraud=True),
                           motion_rows_reversed=rows_reversed)
     sens = [tw.percent_param(v) for v in kw["fg_sens"]] + [tw.percent_param(kw["sensitivity"])]
     mattes = [FG_INPUTS[m].view(tw.DTYPES[fmt]) for m in case["mattes"]]
@@ -127,7 +140,8 @@ def fgbg_clip(dev, case, rows_reversed=True, taps_above_first=True):
 
 @pytest.mark.parametrize("case", FG_CASES, ids=[c["id"] for c in FG_CASES])
 def test_fgbg_layers_grid_sha256(dev, case):
-    """Every served case of the reference's retime-fgbg grid, rendered by the CUDA path."""
+    """Every served case of the reference's retime-fgbg grid (all four warping codes; retime-fgbg's
+    forward warps are the Gouraud variant), rendered by the CUDA path."""
     out = fgbg_clip(dev, case)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
 
@@ -153,4 +167,19 @@ def test_fgbg_clip_matches_oracle_at_larger_size(dev):
     got = dev.retime_layers_clip(s, frames, n, mattes, [2, 4], sens, sels, w, h, fmt)
     p = O.retime_params(speed=40.0, smart_blend=1, sensitivity=70.0)
     want = O.retime_fgbg_clip(frames, n, mattes, [2, 4], [55.0, 70.0], w, h, fmt, p, nout)
+    assert same(got, want)
+
+
+@pytest.mark.parametrize("code", [2, 3])
+def test_fgbg_clip_without_layers_forward_codes(dev, code):
+    """No FG layer with a forward warping code: the plain vector path on the context's stream."""
+    w, h, n, fmt = 96, 64, 4, 0
+    frames = synth.moving_clip(w, h, n, depth=8, seed=0x5eed + code)
+    tp = tw.TimeParams(speed_percent=50.0)
+    nout = 7
+    sels = [tw.select(tp, k, w, h) for k in range(nout)]
+    s = tw.RetimeSettings(flow=tw.FlowSettings(hiq=True), compose=tw.EngineSettings(warp_mode=code, gouraud=True))
+    got = dev.retime_layers_clip(s, frames, n, [], [], [tw.percent_param(70.0)], sels, w, h, fmt)
+    p = O.retime_params(speed=50.0, smart_blend=code, sensitivity=70.0)
+    want = O.retime_fgbg_clip(frames, n, [], [], [], w, h, fmt, p, nout)
     assert same(got, want)

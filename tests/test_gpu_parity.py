@@ -260,6 +260,27 @@ def test_compose_smart_blend(dev, fmt, wa, interp, binary, above_first):
     assert same(got, want)
 
 
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("code", [2, 3])
+@pytest.mark.parametrize("gouraud", [False, True])
+@pytest.mark.parametrize("wa,interp", [(0.5, 1), (0.75, 1), (0.2, 1), (0.6, 0), (0.3, 0)])
+@pytest.mark.parametrize("binary", [False, True])
+def test_compose_forward_codes(dev, fmt, code, gouraud, wa, interp, binary):
+    """Warping codes 2 (coverage, Smart Blend, combine, invert, fill) and 3 (the plain blend) through
+    compose_vectors: each frame pushed by its own flow with the textured or the Gouraud forward warp.
+    The flows are the solved ones scaled up so that the borders uncover."""
+    w, h = 96, 64
+    a, b, _, _ = clip_pair(w, h, fmt, seed=23)
+    o_ab, o_ba, (fw, fh) = O.solve_pair(a, b, w, h, fmt)
+    o_ab = (o_ab * np.float32(5.0) + np.float32(2.5)).astype(np.float32)
+    o_ba = (o_ba * np.float32(5.0) - np.float32(1.75)).astype(np.float32)
+    sel = tw.Selection(wa=np.float32(wa), interp=interp)
+    cs = tw.EngineSettings(warp_mode=code, video_360=binary, gouraud=gouraud)
+    got = dev.compose_vectors(cs, sel, a, b, w, h, fmt, o_ab, o_ba, (fw, fh))
+    want = O.compose_vectors2(a, b, w, h, fmt, o_ab, o_ba, fw, fh, np.float32(wa), interp, code, binary, True, gouraud)
+    assert same(got, want)
+
+
 # ---- whole output frames -----------------------------------------------------------------------------
 
 CASES, INPUTS = golden_data.grid()
@@ -323,6 +344,11 @@ def test_unsupported_settings_fail_loudly(dev):
         dev.solve_pair(a, b, w, h, 0, tw.FlowSettings(prep_contrast_edge=True))
     with pytest.raises(tw.BadParam):
         dev.solve_pair(a, b, w, h, 0, tw.FlowSettings(quality=0))
+    # the forward compositions read counts back: not on the lanes of the clip calls
+    frames = synth.moving_clip(w, h, 2, depth=8)
+    sel = tw.select(tw.TimeParams(speed_percent=50.0), 1, w, h)
+    with pytest.raises(tw.Unsupported):
+        dev.retime_clip(tw.RetimeSettings(compose=tw.EngineSettings(warp_mode=2)), frames, 2, [sel], w, h, 0)
 
 
 @pytest.mark.parametrize("speed,n,nout,size", [(50.0, 48, 95, (160, 96)), (150.0, 8, 12, (64, 48)),

@@ -84,7 +84,8 @@ class _Selection(ctypes.Structure):
 
 class _EngineSettings(ctypes.Structure):
     _fields_ = [("warp_mode", ctypes.c_int32), ("video_360", ctypes.c_int32), ("wrap_360", ctypes.c_int32),
-                ("quality_high", ctypes.c_int32), ("blur", ctypes.c_float), ("taps_above_first", ctypes.c_int32)]
+                ("quality_high", ctypes.c_int32), ("blur", ctypes.c_float), ("taps_above_first", ctypes.c_int32),
+                ("gouraud", ctypes.c_int32)]
 
 
 class _RetimeSettings(ctypes.Structure):
@@ -150,17 +151,19 @@ class Selection:
 
 @dataclass
 class EngineSettings:
-    """The fields of ``host::EngineSettings`` (host.rs:20-100) that ``compose_vectors`` reads."""
+    """The fields of ``host::EngineSettings`` (host.rs:20-100) that ``compose_vectors`` reads;
+    ``gouraud``: the forward warps of codes 2 and 3 as the Gouraud variant (retime-fgbg's stage set)."""
     warp_mode: int = 0
     video_360: bool = False
     wrap_360: bool = False
     quality_high: bool = True
     blur: float = 0.0
     taps_above_first: bool = True
+    gouraud: bool = False
 
     def _c(self):
         return _EngineSettings(self.warp_mode, int(self.video_360), int(self.wrap_360), int(self.quality_high),
-                               self.blur, int(self.taps_above_first))
+                               self.blur, int(self.taps_above_first), int(self.gouraud))
 
 
 @dataclass

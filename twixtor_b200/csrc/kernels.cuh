@@ -137,6 +137,8 @@ __global__ void k_compose_smart(WarpParams pa, WarpParams pb, int fmt, int mode,
                                 int* __restrict__ any_hole, int* __restrict__ bad);
 __global__ void k_smart_blend(const void* __restrict__ p1, const void* __restrict__ p2, int fmt, float w, bool binary,
                               void* __restrict__ out, long n);
+__global__ void k_cov_holes(const uint8_t* __restrict__ c1, const uint8_t* __restrict__ c2, uint8_t* __restrict__ holes,
+                            long n, int* __restrict__ any_hole);
 __global__ void k_mask_holes(const void* __restrict__ mask, int kind, uint8_t* __restrict__ holes, long n,
                              int* __restrict__ any_hole);
 __global__ void k_fill_load(const void* __restrict__ img, int fmt, const uint8_t* __restrict__ holes,
@@ -158,7 +160,8 @@ __global__ void k_encode_vectors(const float* __restrict__ flow, int fw, int fh,
                                  int fmt, float sx, float sy, float kx, float ky, int zero);
 
 // ---- the layered composition with plates (layers.cu) -----------------------------------------------
-__global__ void k_matte_extract(const void* __restrict__ eng, int fmt, int chan, long n, float* __restrict__ out);
+__global__ void k_matte_extract(const void* __restrict__ wire, int fmt, int chan, int w, int h, bool flip,
+                                float* __restrict__ out);
 __global__ void k_matte_out_of_range(const float* __restrict__ m, long n, int* __restrict__ flag);
 __global__ void k_raw_plane(const float* __restrict__ m, long n, int fmt, const int* __restrict__ clamp,
                             float* __restrict__ out);

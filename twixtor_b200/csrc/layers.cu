@@ -20,18 +20,28 @@ __device__ __forceinline__ int64_t as_i64(float x) {
     return __float2ll_rz(x);
 }
 
-// matte.rs:141-188 (extract_raw): channel `chan` (1 R, 2 G, 3 B, else alpha) of an engine image as
-// a raw matte; 8 and 16 bpc the sample over white clamped to 0..1, float the sample times one (the
-// x86 product: a NaN keeps its payload, quieted)
-__global__ void k_matte_extract(const void* __restrict__ eng, int fmt, int chan, long n, float* __restrict__ out) {
+// matte.rs:141-188 (extract_raw) of a matte frame read straight (image.rs:142-171: the FG mattes of
+// retime-fgbg, plugins/retime-fgbg/src/glue.rs:335): channel `chan` (1 R, 2 G, 3 B, else alpha) of
+// the wire frame as stored, rows reversed when `flip`; 8 bpc v / 255, 16 bpc the q15 value scaled
+// like from_frame's alpha, over 65535, both clamped to 0..1; float the sample times one (the x86
+// product: a NaN keeps its payload, quieted).
+__global__ void k_matte_extract(const void* __restrict__ wire, int fmt, int chan, int w, int h, bool flip,
+                                float* __restrict__ out) {
+    long n = (long)w * h;
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int c = chan == 1 ? 1 : chan == 2 ? 2 : chan == 3 ? 3 : 0;
+    int y = (int)(i / w), x = (int)(i - (long)y * w);
+    long si = (long)(flip ? h - 1 - y : y) * w + x;
+    int c = chan == 1 ? 0 : chan == 2 ? 1 : chan == 3 ? 2 : 3;  // wire order R, G, B, A
     float v;
-    if (fmt == 0) v = (float)((const uint8_t*)eng)[i * 4 + c] / 255.0f;
-    else if (fmt == 1) v = (float)((const uint16_t*)eng)[i * 4 + c] / 65535.0f;
-    else {
-        out[i] = x86::mul(((const float*)eng)[i * 4 + c], 1.0f);
+    if (fmt == 0) {
+        v = (float)((const uint8_t*)wire)[si * 4 + c] / 255.0f;
+    } else if (fmt == 1) {
+        uint16_t q15 = u16_to_q15(((const uint16_t*)wire)[si * 4 + c]);
+        v = (float)(uint16_t)qround((float)q15 * premul16_alpha()) / 65535.0f;
+    } else {
+        int plane = c == 0 ? 2 : c == 1 ? 0 : c == 2 ? 1 : 3;  // float wire planes G, B, R, A
+        out[i] = x86::mul(((const float*)wire)[plane * n + si], 1.0f);
         return;
     }
     out[i] = v > 1.0f ? 1.0f : v > 0.0f ? v : 0.0f;  // matte.rs:79-87

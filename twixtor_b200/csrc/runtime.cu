@@ -203,11 +203,12 @@ struct tw_ctx {
     DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags, holes, fill, masks;
     DevBuf lay_mem;  // the layered path: planes, layer images, plates, flows
     DevBuf lay_in;   // the layered path: the raw mattes at A and B
+    DevBuf fc_img[2], fc_cov[2];  // the forward compositions: the two pushed frames and their coverage
     DevBuf host_stage;  // unused placeholder for pinned staging
     std::vector<cudaEvent_t> ev_pool;  // the profiler's events (KernelProfile)
     // the forward warp: vertices, mip pyramid, per pixel counts / offsets, hit lists, flags
     DevBuf logf_tab, fw_vx, fw_vy, fw_vd, fw_pyr, fw_tmp[2], fw_cnt, fw_off, fw_fill, fw_sums, fw_keys, fw_cols,
-        fw_scratch, fw_longq, fw_flags, fw_out, fw_cov;
+        fw_scratch, fw_longq, fw_flags, fw_cov;
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];
@@ -224,6 +225,10 @@ struct tw_ctx {
     }
     int ensure(DevBuf& b, size_t n, const char* what) { return cuda(b.ensure(n, &held), what); }
 };
+
+// The glibc logf exception table embedded by the build (csrc/logf_table.S).
+extern "C" const uint32_t tw_logf_table[];
+extern "C" const uint32_t tw_logf_table_end[];
 
 namespace {
 
@@ -620,6 +625,182 @@ int fill_dev(tw_ctx* ctx, void* img, int W, int H, int fmt, const uint8_t* holes
     return TW_OK;
 }
 
+// ---- the forward warp (forward.rs:229-373) -----------------------------------------------------------
+
+// The glibc logf exception table embedded by the build (csrc/logf_table.S), uploaded once.
+int logf_table(tw_ctx* ctx, const uint2** tab, int* n) {
+    size_t bytes = (size_t)((const char*)tw_logf_table_end - (const char*)tw_logf_table);
+    *n = (int)(bytes / sizeof(uint2));
+    if (!ctx->logf_tab.p) {
+        CHECK(ctx->ensure(ctx->logf_tab, bytes, "logf table"));
+        CHECK(ctx->cuda(cudaMemcpy(ctx->logf_tab.p, tw_logf_table, bytes, cudaMemcpyHostToDevice), "logf table upload"));
+    }
+    *tab = ctx->logf_tab.as<uint2>();
+    return TW_OK;
+}
+
+int fw_level_count(int w, int h) {  // forward/pyramid.rs:20-36
+    int n = 1, a = std::max(w, 2), b = std::max(h, 2);
+    for (;;) {
+        a /= 2;
+        if (a < 2) break;
+        b /= 2;
+        if (b < 2) break;
+        n++;
+    }
+    return n;
+}
+
+// fw_flags ints: [0] outside, [1] bad texture coordinate, [2] flow not zero, [3] long lists,
+// [4] longest list, [6..7] the total number of hits (64 bit)
+enum { FW_OUTSIDE = 0, FW_BAD = 1, FW_NONZERO = 2, FW_NLONG = 3, FW_MAXC = 4, FW_TOTAL = 6 };
+
+// forward.rs:229-320 on device buffers, on ctx->cur: src (engine image) pushed by flow (fw x fh,
+// interleaved) times amount into out (engine image, not src) and the coverage bytes into cov
+// (nullptr: none). Textured (pyramid) or the Gouraud variant. The zero-flow early out and the hit
+// total are read back, so the call synchronises ctx->cur.
+int forward_warp_dev(tw_ctx* ctx, const void* src, const float* flow, int fw, int fh, int W, int H, int fmt,
+                     float amount, bool pyramid, void* out, uint8_t* cov) {
+    if (W < 2 || H < 2 || fw < 2 || fh < 2)
+        return ctx->fail(TW_ERR_MISMATCH, "forward warp needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W, H,
+                         fw, fh);
+    long n = (long)W * H;
+    size_t px = 4 * sample_bytes(fmt);
+    CHECK(ctx->ensure(ctx->fw_flags, 64, "forward warp flags"));
+    CHECK(ctx->ensure(ctx->fw_cov, (size_t)n, "coverage"));
+    if (!cov) cov = ctx->fw_cov.as<uint8_t>();
+    int* ff = ctx->fw_flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(ff, 0, 64, ctx->cur), "flags"));
+    // early outs (forward.rs:252-257): |amount| below 1e-5 as a double, or a flow of zeros
+    float a = 0.0f > amount ? -amount : amount;
+    bool early = 1e-05 > (double)a;
+    long nf = (long)fw * fh * 2;
+    if (!early) {
+        LAUNCH(ctx, k_fw_flow_nonzero, grid1(nf), TB, 0, flow, nf, ff + FW_NONZERO);
+        int nz = 0;
+        CHECK(ctx->cuda(cudaMemcpyAsync(&nz, ff + FW_NONZERO, sizeof nz, cudaMemcpyDeviceToHost, ctx->cur), "flags"));
+        CHECK(ctx->cuda(cudaStreamSynchronize(ctx->cur), "kernel execution"));
+        early = nz == 0;
+    }
+    if (early) {  // blend::copy and a full coverage
+        CHECK(ctx->cuda(cudaMemcpyAsync(out, src, (size_t)n * px, cudaMemcpyDeviceToDevice, ctx->cur), "copy"));
+        return ctx->cuda(cudaMemsetAsync(cov, 0xff, (size_t)n, ctx->cur), "coverage");
+    }
+    // 1. the vertex grid and the mip levels (forward/mesh.rs)
+    FwGrid g;
+    g.w = W;
+    g.h = H;
+    g.rx = (float)(fw - 1) / (float)(W - 1);
+    g.ry = (float)(fh - 1) / (float)(H - 1);
+    g.sx = amount / g.rx;
+    g.sy = amount / g.ry;
+    int levels = fw_level_count(W, H);
+    bool mips = pyramid && levels > 1;
+    if (levels > FW_MAX_LEVELS) return ctx->fail(TW_ERR_TOO_LARGE, "forward warp: %d pyramid levels", levels);
+    CHECK(ctx->ensure(ctx->fw_vx, n * sizeof(float), "vertices"));
+    CHECK(ctx->ensure(ctx->fw_vy, n * sizeof(float), "vertices"));
+    if (mips) CHECK(ctx->ensure(ctx->fw_vd, n * sizeof(float), "mip levels"));
+    const uint2* tab = nullptr;
+    int ntab = 0;
+    if (mips) CHECK(logf_table(ctx, &tab, &ntab));
+    float inv_ln2 = 1.0f / logf(2.0f);  // mesh.rs:89, the host libm like the reference's
+    LAUNCH(ctx, k_fw_vertices, grid1(n), TB, 0, flow, fw, fh, g,
+           ctx->fw_vx.as<float>(), ctx->fw_vy.as<float>(), mips ? ctx->fw_vd.as<float>() : (float*)nullptr, inv_ln2, tab,
+           ntab);
+    // 2. the mip pyramid (forward/pyramid.rs:39-70); level 0 is the source
+    FwLevels L{};
+    L.p[0] = src;
+    L.w[0] = W;
+    L.h[0] = H;
+    L.count = pyramid ? levels : 1;
+    if (pyramid && levels > 1) {
+        size_t tot = 0;
+        int cw = W, chh = H;
+        size_t offs[FW_MAX_LEVELS];
+        for (int i = 1; i < levels; i++) {
+            cw = std::max(cw / 2, 2);
+            chh = std::max(chh / 2, 2);
+            offs[i] = tot;
+            tot += (size_t)cw * chh * px;
+            L.w[i] = cw;
+            L.h[i] = chh;
+        }
+        CHECK(ctx->ensure(ctx->fw_pyr, tot, "mip pyramid"));
+        CHECK(ctx->ensure(ctx->fw_tmp[0], (size_t)n * px, "mip blur"));
+        CHECK(ctx->ensure(ctx->fw_tmp[1], (size_t)n * px, "mip blur"));
+        for (int i = 1; i < levels; i++) {
+            L.p[i] = (char*)ctx->fw_pyr.p + offs[i];
+            int pw = L.w[i - 1], ph = L.h[i - 1];
+            dim3 gb((unsigned)((pw + 127) / 128), (unsigned)ph);
+            LAUNCH(ctx, k_fwp_blur, gb, 128, 0, L.p[i - 1], ctx->fw_tmp[0].p, pw, ph, 0, fmt);
+            LAUNCH(ctx, k_fwp_blur, gb, 128, 0, ctx->fw_tmp[0].p, ctx->fw_tmp[1].p, pw, ph, 1, fmt);
+            dim3 gr((unsigned)((L.w[i] + 127) / 128), (unsigned)L.h[i]);
+            LAUNCH(ctx, k_fwp_resample, gr, 128, 0, ctx->fw_tmp[1].p, pw, ph, (void*)L.p[i], L.w[i], L.h[i], fmt);
+        }
+    }
+    // 3. count the hits of every pixel, then their offsets
+    CHECK(ctx->ensure(ctx->fw_cnt, n * sizeof(uint32_t), "hit counts"));
+    CHECK(ctx->ensure(ctx->fw_off, n * sizeof(uint32_t), "hit offsets"));
+    CHECK(ctx->ensure(ctx->fw_fill, n * sizeof(uint32_t), "hit fill"));
+    int nb = (int)((n + FW_SCAN_BLOCK - 1) / FW_SCAN_BLOCK);
+    CHECK(ctx->ensure(ctx->fw_sums, (size_t)nb * sizeof(uint32_t), "scan sums"));
+    CHECK(ctx->ensure(ctx->fw_longq, n * sizeof(uint32_t), "long lists"));
+    CHECK(ctx->cuda(cudaMemsetAsync(ctx->fw_cnt.p, 0, n * sizeof(uint32_t), ctx->cur), "counts"));
+    CHECK(ctx->cuda(cudaMemsetAsync(ctx->fw_fill.p, 0, n * sizeof(uint32_t), ctx->cur), "fill"));
+    FwRaster R{};
+    R.w = W;
+    R.h = H;
+    R.fmt = fmt;
+    R.pyramid = pyramid != 0;
+    R.vx = ctx->fw_vx.as<float>();
+    R.vy = ctx->fw_vy.as<float>();
+    R.vd = mips ? ctx->fw_vd.as<float>() : nullptr;
+    R.levels = L;
+    R.cnt = ctx->fw_cnt.as<uint32_t>();
+    R.off = ctx->fw_off.as<uint32_t>();
+    R.fill = ctx->fw_fill.as<uint32_t>();
+    R.out = out;
+    R.cov = cov;
+    R.outside = ff + FW_OUTSIDE;
+    R.bad = ff + FW_BAD;
+    R.nlong = (uint32_t*)(ff + FW_NLONG);
+    R.longq = ctx->fw_longq.as<uint32_t>();
+    long tris = 2L * (W - 1) * (H - 1);
+    unsigned gt = (unsigned)((tris + 127) / 128);
+    LAUNCH(ctx, k_fw_count, gt, 128, 0, R);
+    LAUNCH(ctx, k_scan_block, (unsigned)nb, 256, 0, R.cnt, R.off, n, ctx->fw_sums.as<uint32_t>(), (uint32_t*)(ff + FW_MAXC));
+    LAUNCH(ctx, k_scan_sums, 1, 1024, 0, ctx->fw_sums.as<uint32_t>(), nb, (unsigned long long*)(ff + FW_TOTAL));
+    LAUNCH(ctx, k_scan_add, grid1(n), TB, 0, R.off, n, ctx->fw_sums.as<uint32_t>());
+    int hf[8];
+    CHECK(ctx->cuda(cudaMemcpyAsync(hf, ff, sizeof hf, cudaMemcpyDeviceToHost, ctx->cur), "flags"));
+    CHECK(ctx->cuda(cudaStreamSynchronize(ctx->cur), "kernel execution"));
+    if (hf[FW_OUTSIDE])
+        return ctx->fail(TW_ERR_UNSUPPORTED, "forward warp: the degenerate last row pass of the rasteriser would write outside "
+                                             "the image, which is not supported");
+    unsigned long long total;
+    std::memcpy(&total, hf + FW_TOTAL, sizeof total);
+    uint32_t maxc = (uint32_t)hf[FW_MAXC];
+    if (total >= (1ull << 31)) return ctx->fail(TW_ERR_TOO_LARGE, "forward warp: %llu covered pixel hits", total);
+    // 4. the hit lists
+    size_t nt = total ? (size_t)total : 1;
+    CHECK(ctx->ensure(ctx->fw_keys, nt * sizeof(uint32_t), "hit keys"));
+    CHECK(ctx->ensure(ctx->fw_cols, nt * sizeof(float4), "hit colours"));
+    if (maxc > 4096) CHECK(ctx->ensure(ctx->fw_scratch, 2 * nt * sizeof(uint2), "long list scratch"));
+    R.keys = ctx->fw_keys.as<uint32_t>();
+    R.cols = ctx->fw_cols.as<float4>();
+    R.scratch = maxc > 4096 ? ctx->fw_scratch.as<uint2>() : nullptr;
+    R.total = (uint32_t)total;
+    LAUNCH(ctx, k_fw_emit, gt, 128, 0, R);
+    // 5. the running mean of every pixel in triangle order, the depth conversion, the coverage
+    LAUNCH(ctx, k_fw_resolve, grid1(n), TB, 0, R);
+    LAUNCH(ctx, k_fw_resolve_long, 296, 512, FW_LONG_SMEM_BYTES, R);
+    CHECK(ctx->cuda(cudaMemcpyAsync(hf, ff, sizeof hf, cudaMemcpyDeviceToHost, ctx->cur), "flags"));
+    CHECK(ctx->cuda(cudaStreamSynchronize(ctx->cur), "kernel execution"));
+    CHECK(ctx->cuda(cudaGetLastError(), "kernel execution"));
+    if (hf[FW_BAD]) return ctx->fail(TW_ERR_UNSUPPORTED, "forward warp: a texture coordinate outside the image");
+    return TW_OK;
+}
+
 // Scratch of the warping code 1 composition: the composite (engine image), its holes mask, the
 // fill's planes, and the device flag "some pixel is a hole".
 struct SmartScratch {
@@ -630,20 +811,81 @@ struct SmartScratch {
     int* side1;     // set when an image with a side of 1 pixel has a hole (the fill refuses it)
 };
 
-// compose_vectors for warping code 0 (compose/vector.rs:209-284) plus the fast path blends
-// (compose.rs:218-231), all as one fused kernel launch. eng_a/eng_b/f_ab/f_ba are device pointers.
+// compose/vector.rs:117-147 (compose_forward) with forward.rs:384-496: warping codes 2 (coverage,
+// the Smart Blend composite or its binary variant, the combined and inverted coverage, the hole
+// fill) and 3 (no coverage, the plain blend), Nearest and Blend, on ctx->cur (the forward warps
+// read their counts back). The pushed frame uses its own flow (A by F_AB); cs.gouraud selects the
+// Gouraud forward warp (stages::GouraudForward). out: an engine image.
+int compose_forward_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& sel, const void* eng_a,
+                        const void* eng_b, const float* f_ab, const float* f_ba, int fw, int fh, int W, int H, int fmt,
+                        void* out, int* bad, const SmartScratch* ss) {
+    if (!ss) return ctx->fail(TW_ERR_UNSUPPORTED, "the forward compositions need their scratch");
+    bool fill = cs.warp_mode == 2;
+    bool pyramid = cs.gouraud == 0;
+    float wa = sel.wa, frac = 1.0f - wa;
+    long n = (long)W * H;
+    size_t ib = (size_t)n * 4 * sample_bytes(fmt);
+    for (int i = 0; i < 2; i++) {
+        CHECK(ctx->ensure(ctx->fc_img[i], ib, "forward composition"));
+        CHECK(ctx->ensure(ctx->fc_cov[i], (size_t)n, "forward coverage"));
+    }
+    uint8_t* c0 = ctx->fc_cov[0].as<uint8_t>();
+    uint8_t* c1 = ctx->fc_cov[1].as<uint8_t>();
+    auto finish_fill = [&](const uint8_t* second) -> int {  // smartblend.rs:335-345 / forward.rs:430-432
+        CHECK(ctx->ensure(*ss->holes, (size_t)n, "holes mask"));
+        CHECK(ctx->cuda(cudaMemsetAsync(ss->any_hole, 0, sizeof(int), ctx->cur), "holes flag"));
+        LAUNCH(ctx, k_cov_holes, grid1(n), TB, 0, c0, second, ss->holes->as<uint8_t>(), n, ss->any_hole);
+        return fill_dev(ctx, out, W, H, fmt, ss->holes->as<uint8_t>(), ss->any_hole, cs.taps_above_first != 0, *ss->fill);
+    };
+    if (sel.interp == 0) {
+        bool use_ab = (wa < 0.5f && (unsigned)cs.warp_mode < 2) || (0.5f <= wa && (unsigned)cs.warp_mode > 1);
+        const float* flow = use_ab ? f_ab : f_ba;
+        if (!flow) return ctx->fail(TW_ERR_MISMATCH, "the composition needs the flow %s but it was not computed", use_ab ? "F_AB" : "F_BA");
+        bool take_a = !(0.5f > wa);  // a NaN weight takes A
+        CHECK(forward_warp_dev(ctx, take_a ? eng_a : eng_b, flow, fw, fh, W, H, fmt, take_a ? 1.0f - wa : wa, pyramid, out,
+                               fill ? c0 : nullptr));
+        return fill ? finish_fill(nullptr) : TW_OK;
+    }
+    if (sel.interp == 1) {
+        if (!f_ab || !f_ba) return ctx->fail(TW_ERR_MISMATCH, "the composition needs both flows");
+        void* ta = ctx->fc_img[0].p;
+        void* tb = ctx->fc_img[1].p;
+        CHECK(forward_warp_dev(ctx, eng_a, f_ab, fw, fh, W, H, fmt, frac, pyramid, ta, fill ? c0 : nullptr));
+        CHECK(forward_warp_dev(ctx, eng_b, f_ba, fw, fh, W, H, fmt, wa, pyramid, tb, fill ? c1 : nullptr));
+        if (!fill) {  // blend_tail without coverage: blend(tA, tB, frac)
+            WarpParams pa = warp_params(ta, nullptr, 0, 0, 0.0f, W, true);
+            WarpParams pb = warp_params(tb, nullptr, 0, 0, 0.0f, W, true);
+            LAUNCH(ctx, k_compose_blend, grid2(W, H), TB, 0, pa, pb, fmt, frac, blend_mode(frac), out, W, H, false, false, bad);
+            return TW_OK;
+        }
+        LAUNCH(ctx, k_smart_blend, grid1(n), TB, 0, ta, tb, fmt, frac, cs.video_360 != 0, out, n);
+        return finish_fill(c1);
+    }
+    if (sel.interp == 2) return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend with the forward warps is not on the device yet");
+    return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
+}
+
+// compose_vectors (compose/vector.rs:209-284): warping code 0 and the fast path blends
+// (compose.rs:218-231) as one fused kernel launch, code 1 as the Smart Blend kernel and the fill,
+// codes 2 and 3 through compose_forward_dev (engine output only). eng_a/eng_b/f_ab/f_ba are device
+// pointers.
 int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& sel, const void* eng_a,
                 const void* eng_b, const float* f_ab, const float* f_ba, int fw, int fh, int W, int H, int fmt,
                 void* out, bool to_wire, bool flip_out, int* bad, const SmartScratch* ss) {
-    if (cs.warp_mode != 0 && cs.warp_mode != 1)
-        return ctx->fail(TW_ERR_UNSUPPORTED, "warping code %d (forward warp) is not on the device yet", cs.warp_mode);
+    if (cs.warp_mode < 0 || cs.warp_mode > 3) return ctx->fail(TW_ERR_BAD_PARAM, "warping code %d is not 0 to 3", cs.warp_mode);
     if (cs.wrap_360) return ctx->fail(TW_ERR_UNSUPPORTED, "the 360 inverse warp is not on the device");
-    if (W < 2 || H < 2 || fw < 2 || fh < 2)
-        return ctx->fail(TW_ERR_MISMATCH, "inverse warp needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W, H, fw, fh);
     // blur compensation (warp/blurcomp.rs:33-40): runs only when |s0 - s1| > 1e-6 and blur > 0.005
     float d = std::fabs(sel.s0 - sel.s1);
     if ((double)d > 1e-6 && (double)cs.blur > 0.005)
         return ctx->fail(TW_ERR_UNSUPPORTED, "blur compensation is not on the device yet");
+    if (cs.warp_mode >= 2) {
+        if (to_wire)
+            return ctx->fail(TW_ERR_UNSUPPORTED, "the forward warps compose on the context's stream only (tw_compose_vectors, "
+                                                 "tw_retime_layers_clip)");
+        return compose_forward_dev(ctx, cs, sel, eng_a, eng_b, f_ab, f_ba, fw, fh, W, H, fmt, out, bad, ss);
+    }
+    if (W < 2 || H < 2 || fw < 2 || fh < 2)
+        return ctx->fail(TW_ERR_MISMATCH, "inverse warp needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W, H, fw, fh);
     float wa = sel.wa;
     float frac = 1.0f - wa;
     WarpParams pa{}, pb{};
@@ -798,10 +1040,10 @@ int tw_open(int device, tw_ctx** out) {
 void tw_close(tw_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->masks, &ctx->lay_mem, &ctx->lay_in, &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
+    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->masks, &ctx->lay_mem, &ctx->lay_in, &ctx->fc_img[0], &ctx->fc_img[1], &ctx->fc_cov[0], &ctx->fc_cov[1], &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
                     &ctx->fw_vd, &ctx->fw_pyr, &ctx->fw_tmp[0], &ctx->fw_tmp[1], &ctx->fw_cnt, &ctx->fw_off,
                     &ctx->fw_fill, &ctx->fw_sums, &ctx->fw_keys, &ctx->fw_cols, &ctx->fw_scratch, &ctx->fw_longq,
-                    &ctx->fw_flags, &ctx->fw_out, &ctx->fw_cov})
+                    &ctx->fw_flags, &ctx->fw_cov})
         b->release(&ctx->held);
     for (int i = 0; i < 3; i++) { ctx->eng[i].release(&ctx->held); ctx->wire[i].release(&ctx->held); }
     for (int i = 0; i < 2; i++) { ctx->pyr[i].release(&ctx->held); ctx->work[i].release(&ctx->held); ctx->flow[i].release(&ctx->held); }
@@ -1292,8 +1534,7 @@ int tw_fill_holes(tw_ctx* ctx, tw_image_mut* img, const void* mask, int32_t mask
 // The settings the layered path serves (warping codes 0 and 1, Nearest or Blend, no 360 filters).
 static int layers_check(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel) {
     const tw_engine_settings& cs = s.compose;
-    if (cs.warp_mode != 0 && cs.warp_mode != 1)
-        return ctx->fail(TW_ERR_UNSUPPORTED, "layers: warping codes 2 and 3 are not on the device yet");
+    if (cs.warp_mode < 0 || cs.warp_mode > 3) return ctx->fail(TW_ERR_BAD_PARAM, "layers: warping code %d is not 0 to 3", cs.warp_mode);
     if (sel.interp != 0 && sel.interp != 1)
         return ctx->fail(TW_ERR_UNSUPPORTED, "layers: Weighted Blend is not on the device yet");
     if (cs.wrap_360 || s.flow.wrap || s.flow.track_alpha)
@@ -1420,12 +1661,19 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
             CHECK(compose_dev(ctx, cs, *sel, plate[0], plate[0], fab, fba, g.w, g.h, W, H, fmt, dst, false, false,
                               flags + FL_BAD, &ss));
         } else {
-            // PA = LA OVER warp(LB, F_AB, 1), PB = LB OVER warp(LA, F_BA, 1): hold edges (plates.rs:260-268)
-            WarpParams pa_ = warp_params(img(1, k), fab, g.w, g.h, 1.0f, W, true);
-            WarpParams pb_ = warp_params(img(0, k), fba, g.w, g.h, 1.0f, W, true);
-            LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pa_, fmt, plate[0], (uint8_t*)nullptr, W, H, flags + FL_BAD);
+            // plates.rs:268-288: PA = LA OVER LB brought to A, PB = LB OVER LA brought to B, amount 1:
+            // the inverse warp with hold edges for codes 0 and 1 (LB read through F_AB), the forward
+            // warp without coverage for codes 2 and 3 (each side pushed by its own flow, LB by F_BA)
+            if (cs.warp_mode >= 2) {
+                CHECK(forward_warp_dev(ctx, img(1, k), fba, g.w, g.h, W, H, fmt, 1.0f, cs.gouraud == 0, plate[0], nullptr));
+                CHECK(forward_warp_dev(ctx, img(0, k), fab, g.w, g.h, W, H, fmt, 1.0f, cs.gouraud == 0, plate[1], nullptr));
+            } else {
+                WarpParams pa_ = warp_params(img(1, k), fab, g.w, g.h, 1.0f, W, true);
+                WarpParams pb_ = warp_params(img(0, k), fba, g.w, g.h, 1.0f, W, true);
+                LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pa_, fmt, plate[0], (uint8_t*)nullptr, W, H, flags + FL_BAD);
+                LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pb_, fmt, plate[1], (uint8_t*)nullptr, W, H, flags + FL_BAD);
+            }
             LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, plate[0], img(0, k), fmt, n);
-            LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pb_, fmt, plate[1], (uint8_t*)nullptr, W, H, flags + FL_BAD);
             LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, plate[1], img(1, k), fmt, n);
             CHECK(refill(plate[0], 0, k));
             CHECK(refill(plate[1], 1, k));
@@ -1471,37 +1719,6 @@ int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selecti
 
 // ---- the forward warp (forward.rs:229-373) -----------------------------------------------------------
 
-// The glibc logf exception table embedded by the build (csrc/logf_table.S), uploaded once.
-extern "C" const uint32_t tw_logf_table[];
-extern "C" const uint32_t tw_logf_table_end[];
-
-static int logf_table(tw_ctx* ctx, const uint2** tab, int* n) {
-    size_t bytes = (size_t)((const char*)tw_logf_table_end - (const char*)tw_logf_table);
-    *n = (int)(bytes / sizeof(uint2));
-    if (!ctx->logf_tab.p) {
-        CHECK(ctx->ensure(ctx->logf_tab, bytes, "logf table"));
-        CHECK(ctx->cuda(cudaMemcpy(ctx->logf_tab.p, tw_logf_table, bytes, cudaMemcpyHostToDevice), "logf table upload"));
-    }
-    *tab = ctx->logf_tab.as<uint2>();
-    return TW_OK;
-}
-
-static int fw_level_count(int w, int h) {  // forward/pyramid.rs:20-36
-    int n = 1, a = std::max(w, 2), b = std::max(h, 2);
-    for (;;) {
-        a /= 2;
-        if (a < 2) break;
-        b /= 2;
-        if (b < 2) break;
-        n++;
-    }
-    return n;
-}
-
-// fw_flags ints: [0] outside, [1] bad texture coordinate, [2] flow not zero, [3] long lists,
-// [4] longest list, [6..7] the total number of hits (64 bit)
-enum { FW_OUTSIDE = 0, FW_BAD = 1, FW_NONZERO = 2, FW_NLONG = 3, FW_MAXC = 4, FW_TOTAL = 6 };
-
 int tw_forward_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_flow* flow, float amount,
                     int32_t pyramid, uint8_t* cov) {
     if (!ctx) return TW_ERR_BAD_PARAM;
@@ -1513,151 +1730,20 @@ int tw_forward_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const t
         return ctx->fail(TW_ERR_MISMATCH, "forward warp: destination %dx%d fmt %d against source %dx%d fmt %d", out->width,
                          out->height, out->fmt, src->width, src->height, src->fmt);
     int W = src->width, H = src->height, fmt = src->fmt;
-    if (W < 2 || H < 2 || flow->width < 2 || flow->height < 2)
-        return ctx->fail(TW_ERR_MISMATCH, "forward warp needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W, H,
-                         flow->width, flow->height);
     long n = (long)W * H;
-    size_t px = 4 * sample_bytes(fmt);
-    CHECK(upload_image(ctx, ctx->eng[0], src));
-    CHECK(ctx->ensure(ctx->fw_flags, 64, "forward warp flags"));
-    CHECK(ctx->ensure(ctx->fw_cov, (size_t)n, "coverage"));
-    int* ff = ctx->fw_flags.as<int>();
-    CHECK(ctx->cuda(cudaMemsetAsync(ff, 0, 64, ctx->stream), "flags"));
-    // early outs (forward.rs:252-257): |amount| below 1e-5 as a double, or a flow of zeros
-    float a = 0.0f > amount ? -amount : amount;
-    bool early = 1e-05 > (double)a;
+    size_t ib = (size_t)n * 4 * sample_bytes(fmt);
     long nf = (long)flow->width * flow->height * 2;
-    if (!early) {
-        CHECK(ctx->ensure(ctx->flow[0], nf * sizeof(float), "flow"));
-        CHECK(ctx->cuda(cudaMemcpyAsync(ctx->flow[0].p, flow->data, nf * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
-                        "flow upload"));
-        LAUNCH(ctx, k_fw_flow_nonzero, grid1(nf), TB, 0, ctx->flow[0].as<float>(), nf, ff + FW_NONZERO);
-        int nz = 0;
-        CHECK(ctx->cuda(cudaMemcpyAsync(&nz, ff + FW_NONZERO, sizeof nz, cudaMemcpyDeviceToHost, ctx->stream), "flags"));
-        CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution"));
-        early = nz == 0;
-    }
-    if (early) {  // blend::copy and a full coverage
-        CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[0].p, (size_t)n * px, cudaMemcpyDeviceToHost, ctx->stream), "download"));
-        if (cov) std::memset(cov, 0xff, (size_t)n);
-        return ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution");
-    }
-    // 1. the vertex grid and the mip levels (forward/mesh.rs)
-    FwGrid g;
-    g.w = W;
-    g.h = H;
-    g.rx = (float)(flow->width - 1) / (float)(W - 1);
-    g.ry = (float)(flow->height - 1) / (float)(H - 1);
-    g.sx = amount / g.rx;
-    g.sy = amount / g.ry;
-    int levels = fw_level_count(W, H);
-    bool mips = pyramid && levels > 1;
-    if (levels > FW_MAX_LEVELS) return ctx->fail(TW_ERR_TOO_LARGE, "forward warp: %d pyramid levels", levels);
-    CHECK(ctx->ensure(ctx->fw_vx, n * sizeof(float), "vertices"));
-    CHECK(ctx->ensure(ctx->fw_vy, n * sizeof(float), "vertices"));
-    if (mips) CHECK(ctx->ensure(ctx->fw_vd, n * sizeof(float), "mip levels"));
-    const uint2* tab = nullptr;
-    int ntab = 0;
-    if (mips) CHECK(logf_table(ctx, &tab, &ntab));
-    float inv_ln2 = 1.0f / logf(2.0f);  // mesh.rs:89, the host libm like the reference's
-    LAUNCH(ctx, k_fw_vertices, grid1(n), TB, 0, ctx->flow[0].as<float>(), flow->width, flow->height, g,
-           ctx->fw_vx.as<float>(), ctx->fw_vy.as<float>(), mips ? ctx->fw_vd.as<float>() : (float*)nullptr, inv_ln2, tab,
-           ntab);
-    // 2. the mip pyramid (forward/pyramid.rs:39-70); level 0 is the source
-    FwLevels L{};
-    L.p[0] = ctx->eng[0].p;
-    L.w[0] = W;
-    L.h[0] = H;
-    L.count = pyramid ? levels : 1;
-    if (pyramid && levels > 1) {
-        size_t tot = 0;
-        int cw = W, chh = H;
-        size_t offs[FW_MAX_LEVELS];
-        for (int i = 1; i < levels; i++) {
-            cw = std::max(cw / 2, 2);
-            chh = std::max(chh / 2, 2);
-            offs[i] = tot;
-            tot += (size_t)cw * chh * px;
-            L.w[i] = cw;
-            L.h[i] = chh;
-        }
-        CHECK(ctx->ensure(ctx->fw_pyr, tot, "mip pyramid"));
-        CHECK(ctx->ensure(ctx->fw_tmp[0], (size_t)n * px, "mip blur"));
-        CHECK(ctx->ensure(ctx->fw_tmp[1], (size_t)n * px, "mip blur"));
-        for (int i = 1; i < levels; i++) {
-            L.p[i] = (char*)ctx->fw_pyr.p + offs[i];
-            int pw = L.w[i - 1], ph = L.h[i - 1];
-            dim3 gb((unsigned)((pw + 127) / 128), (unsigned)ph);
-            LAUNCH(ctx, k_fwp_blur, gb, 128, 0, L.p[i - 1], ctx->fw_tmp[0].p, pw, ph, 0, fmt);
-            LAUNCH(ctx, k_fwp_blur, gb, 128, 0, ctx->fw_tmp[0].p, ctx->fw_tmp[1].p, pw, ph, 1, fmt);
-            dim3 gr((unsigned)((L.w[i] + 127) / 128), (unsigned)L.h[i]);
-            LAUNCH(ctx, k_fwp_resample, gr, 128, 0, ctx->fw_tmp[1].p, pw, ph, (void*)L.p[i], L.w[i], L.h[i], fmt);
-        }
-    }
-    // 3. count the hits of every pixel, then their offsets
-    CHECK(ctx->ensure(ctx->fw_cnt, n * sizeof(uint32_t), "hit counts"));
-    CHECK(ctx->ensure(ctx->fw_off, n * sizeof(uint32_t), "hit offsets"));
-    CHECK(ctx->ensure(ctx->fw_fill, n * sizeof(uint32_t), "hit fill"));
-    int nb = (int)((n + FW_SCAN_BLOCK - 1) / FW_SCAN_BLOCK);
-    CHECK(ctx->ensure(ctx->fw_sums, (size_t)nb * sizeof(uint32_t), "scan sums"));
-    CHECK(ctx->ensure(ctx->fw_longq, n * sizeof(uint32_t), "long lists"));
-    CHECK(ctx->ensure(ctx->fw_out, (size_t)n * px, "forward warp output"));
-    CHECK(ctx->cuda(cudaMemsetAsync(ctx->fw_cnt.p, 0, n * sizeof(uint32_t), ctx->stream), "counts"));
-    CHECK(ctx->cuda(cudaMemsetAsync(ctx->fw_fill.p, 0, n * sizeof(uint32_t), ctx->stream), "fill"));
-    FwRaster R{};
-    R.w = W;
-    R.h = H;
-    R.fmt = fmt;
-    R.pyramid = pyramid != 0;
-    R.vx = ctx->fw_vx.as<float>();
-    R.vy = ctx->fw_vy.as<float>();
-    R.vd = mips ? ctx->fw_vd.as<float>() : nullptr;
-    R.levels = L;
-    R.cnt = ctx->fw_cnt.as<uint32_t>();
-    R.off = ctx->fw_off.as<uint32_t>();
-    R.fill = ctx->fw_fill.as<uint32_t>();
-    R.out = ctx->fw_out.p;
-    R.cov = ctx->fw_cov.as<uint8_t>();
-    R.outside = ff + FW_OUTSIDE;
-    R.bad = ff + FW_BAD;
-    R.nlong = (uint32_t*)(ff + FW_NLONG);
-    R.longq = ctx->fw_longq.as<uint32_t>();
-    long tris = 2L * (W - 1) * (H - 1);
-    unsigned gt = (unsigned)((tris + 127) / 128);
-    LAUNCH(ctx, k_fw_count, gt, 128, 0, R);
-    LAUNCH(ctx, k_scan_block, (unsigned)nb, 256, 0, R.cnt, R.off, n, ctx->fw_sums.as<uint32_t>(), (uint32_t*)(ff + FW_MAXC));
-    LAUNCH(ctx, k_scan_sums, 1, 1024, 0, ctx->fw_sums.as<uint32_t>(), nb, (unsigned long long*)(ff + FW_TOTAL));
-    LAUNCH(ctx, k_scan_add, grid1(n), TB, 0, R.off, n, ctx->fw_sums.as<uint32_t>());
-    int hf[8];
-    CHECK(ctx->cuda(cudaMemcpyAsync(hf, ff, sizeof hf, cudaMemcpyDeviceToHost, ctx->stream), "flags"));
-    CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution"));
-    if (hf[FW_OUTSIDE])
-        return ctx->fail(TW_ERR_UNSUPPORTED, "forward warp: the degenerate last row pass of the rasteriser would write outside "
-                                             "the image, which is not supported");
-    unsigned long long total;
-    std::memcpy(&total, hf + FW_TOTAL, sizeof total);
-    uint32_t maxc = (uint32_t)hf[FW_MAXC];
-    if (total >= (1ull << 31)) return ctx->fail(TW_ERR_TOO_LARGE, "forward warp: %llu covered pixel hits", total);
-    // 4. the hit lists
-    size_t nt = total ? (size_t)total : 1;
-    CHECK(ctx->ensure(ctx->fw_keys, nt * sizeof(uint32_t), "hit keys"));
-    CHECK(ctx->ensure(ctx->fw_cols, nt * sizeof(float4), "hit colours"));
-    if (maxc > 4096) CHECK(ctx->ensure(ctx->fw_scratch, 2 * nt * sizeof(uint2), "long list scratch"));
-    R.keys = ctx->fw_keys.as<uint32_t>();
-    R.cols = ctx->fw_cols.as<float4>();
-    R.scratch = maxc > 4096 ? ctx->fw_scratch.as<uint2>() : nullptr;
-    R.total = (uint32_t)total;
-    LAUNCH(ctx, k_fw_emit, gt, 128, 0, R);
-    // 5. the running mean of every pixel in triangle order, the depth conversion, the coverage
-    LAUNCH(ctx, k_fw_resolve, grid1(n), TB, 0, R);
-    LAUNCH(ctx, k_fw_resolve_long, 296, 512, FW_LONG_SMEM_BYTES, R);
-    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->fw_out.p, (size_t)n * px, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    CHECK(upload_image(ctx, ctx->eng[0], src));
+    CHECK(ctx->ensure(ctx->flow[0], std::max(nf, 1L) * sizeof(float), "flow"));
+    CHECK(ctx->ensure(ctx->eng[1], ib, "forward warp output"));
+    CHECK(ctx->ensure(ctx->fw_cov, (size_t)n, "coverage"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->flow[0].p, flow->data, nf * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
+                    "flow upload"));
+    CHECK(forward_warp_dev(ctx, ctx->eng[0].p, ctx->flow[0].as<float>(), flow->width, flow->height, W, H, fmt, amount,
+                           pyramid != 0, ctx->eng[1].p, ctx->fw_cov.as<uint8_t>()));
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[1].p, ib, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     if (cov) CHECK(ctx->cuda(cudaMemcpyAsync(cov, ctx->fw_cov.p, (size_t)n, cudaMemcpyDeviceToHost, ctx->stream), "download"));
-    CHECK(ctx->cuda(cudaMemcpyAsync(hf, ff, sizeof hf, cudaMemcpyDeviceToHost, ctx->stream), "flags"));
-    CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution"));
-    CHECK(ctx->cuda(cudaGetLastError(), "kernel execution"));
-    if (hf[FW_BAD]) return ctx->fail(TW_ERR_UNSUPPORTED, "forward warp: a texture coordinate outside the image");
-    return TW_OK;
+    return ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution");
 }
 
 int tw_check_logf(tw_ctx* ctx, const float* x, float* out, int64_t n) {
@@ -2046,6 +2132,47 @@ int tw_retime_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames,
         });
 }
 
+// One frame of the plain vector path (compose/vector.rs:289-321) on ctx->stream: the engine images in
+// ctx->eng[0] / ctx->eng[1] (motion row order), the solves the interpolation needs, compose_vectors
+// into `res` (an engine image). The serial form of retime_frame_lane, for the compositions that
+// read counts back (the forward warps).
+static int vector_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel, int W, int H, int fmt,
+                            void* res) {
+    tw_flow_settings fs = s.flow;
+    fs.quality = sel.vectors_quality;
+    if (fs.wrap) return ctx->fail(TW_ERR_UNSUPPORTED, "the wrap-around (360) solve is not on the device");
+    Geo g;
+    CHECK(geometry(fs, W, H, &g, &ctx->err));
+    size_t pf = pyramid_floats(g);
+    CHECK(ctx->ensure(ctx->pyr[0], 2 * pf * 4, "pyramid"));
+    CHECK(ctx->ensure(ctx->pyr[1], 2 * pf * 4, "pyramid"));
+    float* px_ = ctx->pyr[0].as<float>();
+    float* py_ = ctx->pyr[1].as<float>();
+    CHECK(build_pyramid_dev(ctx, ctx->eng[0].p, W, H, fmt, fs, g, px_, px_ + pf, ctx->plane));
+    CHECK(build_pyramid_dev(ctx, ctx->eng[1].p, W, H, fmt, fs, g, py_, py_ + pf, ctx->plane));
+    size_t fb = (size_t)g.w * g.h * 2 * sizeof(float);
+    CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
+    CHECK(ctx->ensure(ctx->flow[1], fb, "flow"));
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
+    bool need_ab = true, need_ba = true;
+    if (sel.interp == 0) {
+        bool use_ab = (sel.wa < 0.5f && (unsigned)s.compose.warp_mode < 2) || (0.5f <= sel.wa && (unsigned)s.compose.warp_mode > 1);
+        need_ab = use_ab;
+        need_ba = !use_ab;
+    }
+    if (need_ab)
+        CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, fs, ctx->work[0], ctx->flow[0].as<float>(),
+                                 flags + FL_ANY0, flags + FL_NAN));
+    if (need_ba)
+        CHECK(solve_pyramids_dev(ctx, py_, px_, py_ + pf, px_ + pf, g, fs, ctx->work[1], ctx->flow[1].as<float>(),
+                                 flags + FL_ANY1, flags + FL_NAN));
+    SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1};
+    return compose_dev(ctx, s.compose, sel, ctx->eng[0].p, ctx->eng[1].p, need_ab ? ctx->flow[0].as<float>() : nullptr,
+                       need_ba ? ctx->flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, res, false, false, flags + FL_BAD,
+                       &ss);
+}
+
 // retime-fgbg with FG matte layers over a clip in host memory: per output frame the footage and
 // matte frames are uploaded, the in-between frames run the layered path in the motion path's row
 // order and the exact frames the interpolation without flows (the full group fast path,
@@ -2055,7 +2182,8 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
                           const float* sensitivity, const tw_selection* sels, int32_t nout, int32_t width,
                           int32_t height, int32_t fmt, void* out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
-    if (nfg == 0 && sels && s) return tw_retime_clip(ctx, s, frames, nframes, sels, nout, width, height, fmt, out);
+    if (nfg == 0 && sels && s && s->compose.warp_mode < 2)
+        return tw_retime_clip(ctx, s, frames, nframes, sels, nout, width, height, fmt, out);
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cur = ctx->stream;
     if (!s || !sels || !frames || !out || !sensitivity || !matte_clips || !matte_chan || nfg < 0 || nfg > 3 || fmt < 0 ||
@@ -2092,17 +2220,17 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
             CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
             CHECK(interpolate_dev(ctx, sel, ctx->eng[0].p, ctx->eng[1].p, W, H, fmt, ctx->wire[2].p, true, flags + FL_BAD));
         } else {
-            // matte.rs:141-188: each layer's raw matte at A and at B, in the same row order
+            // matte.rs:141-188: each layer's raw matte at A and at B read straight, in the same row order
             for (int side = 0; side < 2; side++)
                 for (int j = 0; j < nfg; j++) {
                     int count = matte_nframes ? matte_nframes[j] : nframes;
                     CHECK(upload(matte_clips[j], count, side ? sel.b : sel.a, ctx->wire[2].p));
-                    from_frame_dev(ctx, ctx->wire[2].p, ctx->eng[2].p, W, H, fmt, flip);
-                    LAUNCH(ctx, k_matte_extract, grid1(n), TB, 0, ctx->eng[2].p, fmt, matte_chan[j], n,
+                    LAUNCH(ctx, k_matte_extract, grid1(n), TB, 0, ctx->wire[2].p, fmt, matte_chan[j], W, H, flip,
                            mat + ((size_t)side * nfg + j) * n);
                 }
-            void* res = nullptr;
-            CHECK(layers_dev(ctx, *s, sel, nfg, mat, sensitivity, W, H, fmt, &res));
+            void* res = ctx->eng[2].p;
+            if (nfg > 0) CHECK(layers_dev(ctx, *s, sel, nfg, mat, sensitivity, W, H, fmt, &res));
+            else CHECK(vector_frame_dev(ctx, *s, sel, W, H, fmt, res));  // compose.rs:155-161 without layers
             if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)res, ctx->wire[2].as<uint8_t>(), W, H, flip);
             else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)res, ctx->wire[2].as<uint16_t>(), W, H, flip);
             else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)res, ctx->wire[2].as<float>(), W, H, flip);

@@ -202,6 +202,21 @@ __global__ void k_mask_holes(const void* __restrict__ mask, int kind, uint8_t* _
     if (__syncthreads_or(hole) && threadIdx.x == 0) atomicOr(any_hole, 1);
 }
 
+// warp.rs:76-95 then the u8 hole rule (holefill.rs:126-133): the holes of a coverage image, or of the
+// per byte maximum of two (Coverage::combine_max), inverted: a hole where 255 - coverage is not 0
+__global__ void k_cov_holes(const uint8_t* __restrict__ c1, const uint8_t* __restrict__ c2, uint8_t* __restrict__ holes,
+                            long n, int* __restrict__ any_hole) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool hole = false;
+    if (i < n) {
+        uint8_t c = c1[i];
+        if (c2 && c2[i] > c) c = c2[i];
+        hole = (uint8_t)(0xffu - c) != 0;
+        holes[i] = hole ? 1 : 0;
+    }
+    if (__syncthreads_or(hole) && threadIdx.x == 0) atomicOr(any_hole, 1);
+}
+
 // ---- the hole fill on plane stacks (holefill.rs) ------------------------------------------------------
 
 // holefill.rs:300-313 + :452-491: level 0 of the value planes (the four channels, holes zeroed)

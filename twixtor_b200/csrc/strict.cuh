@@ -112,4 +112,17 @@ __device__ __forceinline__ float bilinear1(const float* __restrict__ img, int w,
     return (bot - top) * fy + top;
 }
 
+// the constants and the 16 bpc wire conversion of the image boundary (image.rs:261-267,
+// crates/fx-core/src/frame.rs:131-142)
+__device__ __forceinline__ float inv_255() { return __uint_as_float(0x3b808081u); }            // image.rs:261
+__device__ __forceinline__ float premul16_color() { return __uint_as_float(0x387fff00u); }     // image.rs:263
+__device__ __forceinline__ float premul16_alpha() { return __uint_as_float(0x3fffff00u); }     // image.rs:265
+__device__ __forceinline__ float unpremul16_alpha() { return __uint_as_float(0x3f000080u); }   // image.rs:267
+
+__device__ __forceinline__ uint16_t u16_to_q15(uint16_t v) { return (uint16_t)(((uint32_t)v * 32768u + 32767u) / 65535u); }
+__device__ __forceinline__ uint16_t q15_to_u16(uint16_t v) {
+    uint32_t m = v < 32768 ? v : 32768;
+    return (uint16_t)((m * 65535u + 16384u) / 32768u);
+}
+
 }  // namespace tw
