@@ -356,7 +356,9 @@ int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* 
  * in-between frames run tw_compose_layers in the motion path's row order (rows reversed when
  * s->motion_rows_reversed), the exact frames the interpolation without flows. A frame outside a
  * clip is blank. The inverse matte shrink is 0, no tracking point is in use and the output is
- * Display Twixtored Output. nfg 0 is tw_retime_clip. */
+ * Display Twixtored Output. s->compose.gouraud should be 1 (retime-fgbg's forward warps are the
+ * Gouraud variant). nfg 0 with warping codes 0/1 is tw_retime_clip; codes 2/3 run the plain vector
+ * path frame by frame on the context's stream. */
 int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes, int32_t nfg,
                           const void* const* matte_clips, const int32_t* matte_nframes, const int32_t* matte_chan,
                           const float* sensitivity, const tw_selection* sels, int32_t nout, int32_t width,

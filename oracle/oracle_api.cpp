@@ -448,7 +448,10 @@ int or_select(const or_retime_params* p, int n, int w, int h, float* s0, float* 
 // Renders output frame n of the `retime` effect over a raw clip of `nframes` wire frames into
 // `out` (one wire frame). Returns 0, or a nonzero status with or_last_error() naming what is not
 // restated.
-int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int n, void* out) {
+// One output frame of the plain vector path; `gouraud`: the forward warps of codes 2/3 as the
+// Gouraud variant (the stage set of retime-fgbg, plugins/retime-fgbg/src/glue.rs:142-143).
+static int retime_one(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int n, void* out,
+                      bool gouraud) {
     Fmt f = (Fmt)fmt;
     size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
     size_t frame_bytes = (size_t)w * h * 4 * es;
@@ -502,6 +505,7 @@ int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const 
         cs.warp_mode = p->smart_blend;  // plugins/retime frontend: warp_mode = i32::from(smart_blend); 2, 3 the Warping popup of plugin 03
         cs.video_360 = p->video_360 != 0;
         cs.taps_above_first = p->taps_above_first != 0;
+        cs.gouraud = gouraud;
         Image o;
         int rc = compose_vectors(cs, sel, ar, br, have_ab ? &fab : nullptr, have_ba ? &fba : nullptr, &o, &e);
         if (rc) return fail(rc, e);
@@ -512,6 +516,10 @@ int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const 
     }
     to_frame(result, out);
     return 0;
+}
+
+int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int n, void* out) {
+    return retime_one(frames, nframes, w, h, fmt, p, n, out, false);
 }
 
 // ---- retime-fgbg with FG matte layers (plugins/retime-fgbg/src/glue.rs, compose.rs:149-170,
@@ -546,7 +554,9 @@ static std::vector<float> flip_matte(const std::vector<float>& m, int w, int h) 
 // inverse matte shrink, no tracking points.
 int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte_clips, int nfg, const int* fg_chan,
                        const double* fg_sens, int w, int h, int fmt, const or_retime_params* p, int n, void* out) {
-    if (nfg == 0) return or_retime_one(frames, nframes, w, h, fmt, p, n, out);
+    // compose.rs:155-161: without FG layers (and tracking points) the plain vector path, with the
+    // stage set of the effect (the Gouraud forward warps)
+    if (nfg == 0) return retime_one(frames, nframes, w, h, fmt, p, n, out, true);
     Fmt f = (Fmt)fmt;
     size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
     size_t frame_bytes = (size_t)w * h * 4 * es;
