@@ -475,7 +475,7 @@ static int retime_one(const void* frames, int nframes, int w, int h, int fmt, co
     sel.vectors_quality = vq; sel.interp = interp;
     std::string e;
     if (vq != 0 && !exact) {
-        if (interp < 0 || interp > 1) return fail(2, "weighted blend on the vector path is not restated");
+        if (interp < 0 || interp > 2) return fail(1, "bad interpolation mode");
         // plugin 01 runs the motion path on bottom-up rows (plugins/retime/src/glue.rs:39-40,
         // compose/vector.rs:303-314)
         Image ar = p->rows_reversed ? rows_reversed(A) : A, br = p->rows_reversed ? rows_reversed(B) : B;
@@ -580,7 +580,7 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
     sel.vectors_quality = vq; sel.interp = interp;
     std::string e;
     if (vq != 0 && !exact) {  // compose.rs:155-158: the layered vector path
-        if (interp < 0 || interp > 1) return fail(2, "weighted blend on the vector path is not restated");
+        if (interp < 0 || interp > 2) return fail(1, "bad interpolation mode");
         LayerJob job;
         for (int k = 0; k < nfg; k++) {
             std::vector<float> ma = extract_raw(fetch(matte_clips[k], a, true), fg_chan[k]);

@@ -3,6 +3,7 @@
 #include "oracle_core.h"
 #include "oracle_smart.h"
 #include "oracle_forward.h"
+#include "oracle_filters.h"
 
 #include <algorithm>
 #include <cstdio>
@@ -1216,18 +1217,22 @@ int compose_vectors(const ComposeSettings& cs, const Selection& sel, const Image
         if (0.5f <= wa) return inv_warp(*out, a, *flow, frac, o, nullptr, err);
         return inv_warp(*out, b, *flow, wa, o, nullptr, err);
     }
-    if (sel.interp == 1) {
+    if (sel.interp == 1 || sel.interp == 2) {
         if (!f_ab || !f_ba) { *err = "missing flow"; return 1; }
         Image ta(a.w, a.h, a.fmt), tb(b.w, b.h, b.fmt);
         int rc = inv_warp(ta, a, *f_ba, frac, o, nullptr, err);
         if (rc) return rc;
         rc = inv_warp(tb, b, *f_ab, wa, o, nullptr, err);
         if (rc) return rc;
+        if (sel.interp == 2) {  // compose/vector.rs:264-269: the sharpening of each warped frame
+            sharpen_step(ta, a, frac, cs.taps_above_first);
+            sharpen_step(tb, b, wa, cs.taps_above_first);
+        }
         blend(*out, ta, tb, frac);
         return 0;
     }
-    *err = "compose: interpolation mode not restated";
-    return 2;
+    *err = "bad interpolation mode";
+    return 1;
 }
 
 int interpolate(const Selection& sel, const Image& a, const Image& b, Image* out, std::string* err) {
@@ -1238,8 +1243,17 @@ int interpolate(const Selection& sel, const Image& a, const Image& b, Image* out
         // blend.rs:281-302: Weighted Blend without flows equals the plain Blend with weight 1 - wa
         // for 8 and 16 bpc, and for float data whose samples are finite and at most 1e30
         if (a.fmt == F32) {
-            for (float v : a.f32) if (!(std::fabs(v) <= 1.0e30f)) { *err = "weighted blend of unsound floats"; return 2; }
-            for (float v : b.f32) if (!(std::fabs(v) <= 1.0e30f)) { *err = "weighted blend of unsound floats"; return 2; }
+            bool sound = true;
+            for (float v : a.f32) sound = sound && std::fabs(v) <= 1.0e30f;
+            for (float v : b.f32) sound = sound && std::fabs(v) <= 1.0e30f;
+            if (!sound) {  // blend.rs:316-324 (weighted_blend_noflow_reference): every filter, engine taps
+                float t = 1.0f - sel.wa;
+                Image a1 = a, b1 = b;
+                sharpen_step(a1, a, t, false);
+                sharpen_step(b1, b, sel.wa, false);
+                blend(*out, a1, b1, t);
+                return 0;
+            }
             Image a1 = a, b1 = b;
             for (auto& v : a1.f32) v = v + 0.0f;
             for (auto& v : b1.f32) v = v + 0.0f;

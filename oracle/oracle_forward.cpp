@@ -641,8 +641,19 @@ int compose_forward(const ComposeSettings& cs, const Selection& sel, const Image
         for (size_t i = 0; i < c1.d.size(); i++) c1.d[i] = 0xff - std::max(c1.d[i], c2.d[i]);
         return fill_holes(*out, c1.d.data(), 1, cs.taps_above_first, err);
     }
-    *err = "weighted blend with the forward warps is not restated";
-    return 2;
+    if (sel.interp == 2) {  // forward.rs:498-572 (weighted_forward, weighted_forward_fill)
+        if (!f_ab || !f_ba) { *err = "missing flow"; return 1; }
+        float frac = 1.0f - wa;
+        Image ta(a.w, a.h, a.fmt), tb(b.w, b.h, b.fmt);
+        Coverage c1, c2;
+        int rc = forward_warp(ta, a, *f_ab, frac, !cs.gouraud, fill ? &c1 : nullptr, err);
+        if (rc) return rc;
+        rc = forward_warp(tb, b, *f_ba, wa, !cs.gouraud, fill ? &c2 : nullptr, err);
+        if (rc) return rc;
+        return weighted_tail(*out, ta, a, tb, b, wa, fill ? &c1 : nullptr, fill ? &c2 : nullptr, cs.taps_above_first, err);
+    }
+    *err = "bad interpolation mode";
+    return 1;
 }
 
 }  // namespace orc

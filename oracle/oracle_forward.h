@@ -29,8 +29,7 @@ int forward_warp(Image& out, const Image& src, const FlowField& flow, float amou
                  std::string* err);
 // compose/vector.rs:117-147 (compose_forward) with forward.rs:384-496: warping codes 2 (coverage,
 // Smart Blend or its binary variant, combine, invert, hole fill) and 3 (no coverage), Nearest and
-// Blend; the textured forward warp, or the Gouraud variant with cs.gouraud. Weighted Blend returns
-// 2 (not restated).
+// Blend and Weighted Blend; the textured forward warp, or the Gouraud variant with cs.gouraud.
 int compose_forward(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b,
                     const FlowField* f_ab, const FlowField* f_ba, Image* out, std::string* err);
 

@@ -233,7 +233,7 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
     const Selection& sel = job.sel;
     int code = job.cs.warp_mode;
     if (code < 0 || code > 3) { *err = "plates: warping code not 0 to 3"; return 1; }
-    if (sel.interp != 0 && sel.interp != 1) { *err = "plates: Weighted Blend is not restated"; return 2; }
+    if (sel.interp < 0 || sel.interp > 2) { *err = "plates: bad interpolation mode"; return 1; }
     // plates.rs:330-370: the solves, one layer after the other
     std::vector<FlowField> f_ab(nfg + 1), f_ba(nfg + 1);
     std::vector<bool> has_ab(nfg + 1, false), has_ba(nfg + 1, false);

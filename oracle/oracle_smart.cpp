@@ -9,6 +9,7 @@
 
 #include "oracle_core.h"
 #include "oracle_smart.h"
+#include "oracle_filters.h"
 
 namespace orc {
 
@@ -361,8 +362,34 @@ int compose_smart(const ComposeSettings& cs, const Selection& sel, const Image& 
         for (size_t i = 0; i < c1.d.size(); i++) c1.d[i] = 0xff - std::max(c1.d[i], c2.d[i]);
         return fill_holes(*out, c1.d.data(), 1, taps_above_first, err);
     }
-    *err = "weighted blend with smart blend is not restated";
-    return 2;
+    if (sel.interp == 2) {  // smartblend.rs:400-420 (weighted_blend_smart) and :427-456 (weighted_tail)
+        if (!f_ab || !f_ba) { *err = "missing flow"; return 1; }
+        float frac = 1.0f - wa;
+        Image ta(a.w, a.h, a.fmt), tb(b.w, b.h, b.fmt);
+        Coverage c1, c2;
+        int rc = inv_warp(ta, a, *f_ba, frac, o, &c1, err);
+        if (rc) return rc;
+        rc = inv_warp(tb, b, *f_ab, wa, o, &c2, err);
+        if (rc) return rc;
+        return weighted_tail(*out, ta, a, tb, b, wa, &c1, &c2, taps_above_first, err);
+    }
+    *err = "bad interpolation mode";
+    return 1;
+}
+
+int weighted_tail(Image& out, Image& ta, const Image& a, Image& tb, const Image& b, float wa, Coverage* c1,
+                  const Coverage* c2, bool taps_above_first, std::string* err) {
+    float frac = 1.0f - wa;
+    sharpen_step(ta, a, frac, taps_above_first);
+    sharpen_step(tb, b, wa, taps_above_first);
+    out = Image(a.w, a.h, a.fmt);
+    if (!c1) {
+        blend(out, ta, tb, frac);
+        return 0;
+    }
+    smart_blend(out, ta, tb, frac, false);  // always the plain Smart Blend kernel, the fill without wrap
+    for (size_t i = 0; i < c1->d.size(); i++) c1->d[i] = 0xff - std::max(c1->d[i], c2->d[i]);
+    return fill_holes(out, c1->d.data(), 1, taps_above_first, err);
 }
 
 }  // namespace orc

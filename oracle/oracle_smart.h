@@ -24,4 +24,10 @@ int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, st
 int compose_smart(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b, const FlowField* f_ab,
                   const FlowField* f_ba, bool taps_above_first, Image* out, std::string* err);
 
+// smartblend.rs:427-456 (weighted_tail): the sharpening of both warped frames against the unwarped
+// ones, then with coverage (c1 != null) Smart Blend, the combined and inverted coverage and the
+// fill, else the plain blend. c1 is left holding the holes.
+int weighted_tail(Image& out, Image& ta, const Image& a, Image& tb, const Image& b, float wa, Coverage* c1,
+                  const Coverage* c2, bool taps_above_first, std::string* err);
+
 }  // namespace orc

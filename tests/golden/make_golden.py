@@ -24,7 +24,7 @@ Writes, next to this script:
   ``rows_reversed=False, taps_above_first=False``.
 * ``fgbg_layers_grid.npz`` - the cases of the reference's parity grid ``parity/fgbg-layers`` that
   the layered path with plates serves (FG matte layers FG1.. consecutive, the four warping codes,
-  Nearest or Blend, no inverse matte shrink, no tracking points, Display
+  Nearest, Blend or Weighted Blend, no inverse matte shrink, no tracking points, Display
   Twixtored Output, integer frame rates), their footage and matte clips as its ``gen_grid.py``
   renders them, and the sha256 of the output clip ``results/base.tsv`` records (the reference's
   current revision: rows reversed, taps above first).
@@ -72,10 +72,7 @@ def served(case):
     params.pop("speed_percent")
     if any(k not in SERVED for k in params):
         return False
-    if params.get("frame_interp", "2") not in ("1", "2"):
-        # Weighted Blend (3) is served on the fast path only, which the case's own frames decide;
-        # keep those cases out of the fixture set
-        return False
+
     if float(params.get("blur_compensation", "0")) > 0.005:
         return False
     return True
@@ -163,7 +160,7 @@ def fgbg_layers_grid(ref):
         params = dict(p.split("=", 1) for p in c["params"])
         if any(k not in FG_SERVED for k in params) or any("@" in v for v in params.values()):
             continue
-        if params.get("warping", "1") not in ("1", "2", "3", "4") or params.get("frame_interp", "2") not in ("1", "2"):
+        if params.get("warping", "1") not in ("1", "2", "3", "4"):
             continue
         if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
             continue

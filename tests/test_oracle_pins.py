@@ -161,7 +161,7 @@ def test_inverse_warp_model_fixtures(i):
 CASES, INPUTS = golden_data.grid()
 
 
-@pytest.mark.parametrize("case", CASES, ids=[c["id"] for c in CASES])
+@pytest.mark.parametrize("case", golden_data.grid_params(CASES))
 def test_retime_flow_grid_sha256(case):
     fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
     raw = INPUTS[case["input"]].view(O.DTYPE[fmt])

@@ -222,4 +222,29 @@ __global__ void k_fw_resolve(FwRaster R);
 constexpr int FW_LONG_SMEM_BYTES = 4096 * 8;
 __global__ void k_fw_resolve_long(FwRaster R);
 
+// ---- the Weighted Blend filters (filters.cu, filters.rs) ----
+struct WbTaps {  // the half kernel of the sharpening blur (filters.rs:75-93), w[0] the centre
+    float w[8];
+    int count;
+};
+__global__ void k_wb_blur(const void* __restrict__ src, void* __restrict__ dst, int fmt, int w, int h, WbTaps T, bool cols,
+                          bool above_first, const int* __restrict__ gate);
+__global__ void k_wb_diff_mask(const void* __restrict__ a, const void* __restrict__ b, int fmt, long n, float limit,
+                               uint8_t* __restrict__ mask, const int* __restrict__ gate);
+__global__ void k_mask_prune(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int w, int h, int limit,
+                             const int* __restrict__ gate);
+__global__ void k_mask_dilate(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int w, int h,
+                              const int* __restrict__ gate);
+__global__ void k_mask_fill_border(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int w, int h, int limit,
+                                   int value, const int* __restrict__ gate);
+__global__ void k_mask_clean_small(uint8_t* __restrict__ m, uint8_t* __restrict__ scratch, int w, int h,
+                                   const int* __restrict__ gate);
+__global__ void k_wb_finish(void* __restrict__ frame, const void* __restrict__ blurred, const uint8_t* __restrict__ mask,
+                            int fmt, long n, float c, const int* __restrict__ gate);
+__global__ void k_f32_unsound(const float* __restrict__ a, long n, int* __restrict__ flag);
+__global__ void k_copy_gated(const uint4* __restrict__ src, uint4* __restrict__ dst, long n, const int* __restrict__ gate);
+__global__ void k_wb_noflow_f32(const float* __restrict__ a, const float* __restrict__ b, const float* __restrict__ a1,
+                                const float* __restrict__ b1, const int* __restrict__ unsound, float w, float wl, int mode,
+                                float* __restrict__ out, long n);
+
 }  // namespace tw

@@ -174,6 +174,7 @@ struct Lane {
     bool used = false;
     DevBuf eng[2], pyr[2], work[2], flow[2], scratch[2][3], flags;
     DevBuf comp, holes, fill;  // warping code 1: the composite, its holes mask, the fill's planes
+    DevBuf wb_wt[2], wb_tmp[2], wb_mask[2], wb_cov[2];  // Weighted Blend: warped frames, blur planes, masks, coverage
 };
 constexpr int MAX_LANES = 8;
 
@@ -204,6 +205,7 @@ struct tw_ctx {
     DevBuf lay_mem;  // the layered path: planes, layer images, plates, flows
     DevBuf lay_in;   // the layered path: the raw mattes at A and B
     DevBuf fc_img[2], fc_cov[2];  // the forward compositions: the two pushed frames and their coverage
+    DevBuf wb_wt[2], wb_tmp[2], wb_mask[2], wb_cov[2];  // Weighted Blend (the calls on the context's stream)
     DevBuf host_stage;  // unused placeholder for pinned staging
     std::vector<cudaEvent_t> ev_pool;  // the profiler's events (KernelProfile)
     // the forward warp: vertices, mip pyramid, per pixel counts / offsets, hit lists, flags
@@ -275,7 +277,7 @@ void prof_mark(tw_ctx* ctx) {
 constexpr int TB = 256;
 // device flags (ints): [0..31] per-level range flags of solve 0, [32..63] of solve 1, [64] NaN in a
 // flow, [65] a warp refused a sample coordinate
-constexpr int FL_ANY0 = 0, FL_ANY1 = 32, FL_NAN = 64, FL_BAD = 65, FL_HOLE = 66, FL_SIDE1 = 67, FL_ONE = 68;
+constexpr int FL_ANY0 = 0, FL_ANY1 = 32, FL_NAN = 64, FL_BAD = 65, FL_HOLE = 66, FL_SIDE1 = 67, FL_ONE = 68, FL_WB = 69;
 constexpr size_t FLAGS_BYTES = 128 * sizeof(int);
 
 dim3 grid2(int w, int h) { return dim3((unsigned)((w + TB - 1) / TB), (unsigned)h); }
@@ -803,13 +805,115 @@ int forward_warp_dev(tw_ctx* ctx, const void* src, const float* flow, int fw, in
 
 // Scratch of the warping code 1 composition: the composite (engine image), its holes mask, the
 // fill's planes, and the device flag "some pixel is a hole".
+struct WbScratch {  // Weighted Blend: the two warped frames, the blur planes, the masks, the coverage
+    DevBuf* wt[2];
+    DevBuf* tmp[2];
+    DevBuf* mask[2];
+    DevBuf* cov[2];
+};
+
 struct SmartScratch {
     DevBuf* comp;
     DevBuf* holes;
     DevBuf* fill;
     int* any_hole;  // set by the composition when a pixel is a hole
     int* side1;     // set when an image with a side of 1 pixel has a hole (the fill refuses it)
+    const WbScratch* wb = nullptr;  // Weighted Blend scratch (nullptr: Weighted Blend refused)
+    int* wb_gate = nullptr;         // the unsound float flag of the Weighted Blend without flows
 };
+
+WbScratch wb_scratch(DevBuf* wt, DevBuf* tmp, DevBuf* mask, DevBuf* cov) {
+    return WbScratch{{&wt[0], &wt[1]}, {&tmp[0], &tmp[1]}, {&mask[0], &mask[1]}, {&cov[0], &cov[1]}};
+}
+
+// filters.rs:627-631 (sharpen_weight), in double precision as the reference computes it
+float sharpen_weight(float t) {
+    double x = 1.0 - std::fabs(0.5 - (double)t) * 2.0;
+    float neg = -(float)x;
+    return (float)((double)neg * 0.5);
+}
+
+// filters.rs:649-657 (sharpen_step_with): frame (an engine image, in place) against the unwarped
+// orig, on ctx->cur. gate: see filters.cu (nullptr: always).
+int sharpen_dev(tw_ctx* ctx, void* frame, const void* orig, int W, int H, int fmt, float t, bool above_first,
+                const WbScratch& ws, const int* gate) {
+    long n = (long)W * H;
+    size_t ib = (size_t)n * 4 * sample_bytes(fmt);
+    for (int i = 0; i < 2; i++) {
+        CHECK(ctx->ensure(*ws.tmp[i], ib, "sharpening planes"));
+        CHECK(ctx->ensure(*ws.mask[i], (size_t)n, "sharpening mask"));
+    }
+    uint8_t* cur = ws.mask[0]->as<uint8_t>();
+    uint8_t* nxt = ws.mask[1]->as<uint8_t>();
+    float white = fmt == TW_U8 ? 255.0f : fmt == TW_U16 ? 65535.0f : 1.0f;
+    float limit = 0.4f * white * 0.4f * 0.4f * 3.0f;  // filters.rs:293-295, MASK_THRESHOLD 0.4
+    LAUNCH(ctx, k_wb_diff_mask, grid1(n), TB, 0, frame, orig, fmt, n, limit, cur, gate);
+    // filters.rs:507-520: prune 254 and 509, dilate, fill 254 -> 255 twice, 254 -> 128, 127 -> 64
+    if (W >= 3 && H >= 3) {
+        auto step = [&]() { std::swap(cur, nxt); };
+        if (H >= 5) {
+            LAUNCH(ctx, k_mask_prune, grid1(n), TB, 0, cur, nxt, W, H, 254, gate);
+            step();
+            LAUNCH(ctx, k_mask_prune, grid1(n), TB, 0, cur, nxt, W, H, 509, gate);
+            step();
+        }
+        LAUNCH(ctx, k_mask_dilate, grid1(n), TB, 0, cur, nxt, W, H, gate);
+        step();
+        const int fills[4][2] = {{254, 255}, {254, 255}, {254, 128}, {127, 64}};
+        for (auto& f : fills) {
+            LAUNCH(ctx, k_mask_fill_border, grid1(n), TB, 0, cur, nxt, W, H, f[0], f[1], gate);
+            step();
+        }
+    } else {
+        LAUNCH(ctx, k_mask_clean_small, 1, 1, 0, cur, nxt, W, H, gate);
+    }
+    // the blur (radius 3.0, filters.rs:75-93: taps 1, 1/2, 1/16, 1/512 over their sum, from powf)
+    WbTaps T{};
+    {
+        float sum = 0.0f, wv[4];
+        for (int i = 0; i < 4; i++) {
+            float fi = (float)i;
+            float x = -((fi * fi) / 1.0f);
+            wv[i] = powf(2.0f, x);
+            sum += wv[i];
+        }
+        float denom = sum * 2.0f - wv[0];
+        for (int i = 0; i < 4; i++) T.w[i] = wv[i] / denom;
+        T.count = 4;
+    }
+    void* t0 = ws.tmp[0]->p;
+    void* t1 = ws.tmp[1]->p;
+    LAUNCH(ctx, k_wb_blur, grid1(n), TB, 0, frame, t0, fmt, W, H, T, false, false, gate);
+    LAUNCH(ctx, k_wb_blur, grid1(n), TB, 0, t0, t1, fmt, W, H, T, true, above_first, gate);
+    LAUNCH(ctx, k_wb_finish, grid1(n), TB, 0, frame, t1, cur, fmt, n, sharpen_weight(t), gate);
+    return TW_OK;
+}
+
+// smartblend.rs:427-456 (weighted_tail) on ctx->cur: ta / tb sharpened against a / b, then with
+// coverage (c0 != nullptr) the plain Smart Blend into out, the combined inverted coverage and the
+// fill; without coverage the blend. out: an engine image.
+int weighted_tail_dev(tw_ctx* ctx, void* out, void* ta, const void* a, void* tb, const void* b, float wa, int W, int H,
+                      int fmt, const uint8_t* c0, const uint8_t* c1, bool above_first, const SmartScratch& ss, int* bad) {
+    long n = (long)W * H;
+    float frac = 1.0f - wa;
+    CHECK(sharpen_dev(ctx, ta, a, W, H, fmt, frac, above_first, *ss.wb, nullptr));
+    CHECK(sharpen_dev(ctx, tb, b, W, H, fmt, wa, above_first, *ss.wb, nullptr));
+    if (!c0) {
+        WarpParams pa = warp_params(ta, nullptr, 0, 0, 0.0f, W, true);
+        WarpParams pb = warp_params(tb, nullptr, 0, 0, 0.0f, W, true);
+        LAUNCH(ctx, k_compose_blend, grid2(W, H), TB, 0, pa, pb, fmt, frac, blend_mode(frac), out, W, H, false, false, bad);
+        return TW_OK;
+    }
+    LAUNCH(ctx, k_smart_blend, grid1(n), TB, 0, ta, tb, fmt, frac, false, out, n);
+    CHECK(ctx->ensure(*ss.holes, (size_t)n, "holes mask"));
+    CHECK(ctx->cuda(cudaMemsetAsync(ss.any_hole, 0, sizeof(int), ctx->cur), "holes flag"));
+    LAUNCH(ctx, k_cov_holes, grid1(n), TB, 0, c0, c1, ss.holes->as<uint8_t>(), n, ss.any_hole);
+    if (W < 2 || H < 2) {
+        LAUNCH(ctx, k_hole_side1, 1, 1, 0, ss.any_hole, ss.side1);
+        return TW_OK;
+    }
+    return fill_dev(ctx, out, W, H, fmt, ss.holes->as<uint8_t>(), ss.any_hole, above_first, *ss.fill);
+}
 
 // compose/vector.rs:117-147 (compose_forward) with forward.rs:384-496: warping codes 2 (coverage,
 // the Smart Blend composite or its binary variant, the combined and inverted coverage, the hole
@@ -861,7 +965,16 @@ int compose_forward_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_sele
         LAUNCH(ctx, k_smart_blend, grid1(n), TB, 0, ta, tb, fmt, frac, cs.video_360 != 0, out, n);
         return finish_fill(c1);
     }
-    if (sel.interp == 2) return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend with the forward warps is not on the device yet");
+    if (sel.interp == 2) {  // forward.rs:498-572: the two pushes, then weighted_tail
+        if (!ss->wb) return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend needs its scratch");
+        if (!f_ab || !f_ba) return ctx->fail(TW_ERR_MISMATCH, "the composition needs both flows");
+        void* ta = ctx->fc_img[0].p;
+        void* tb = ctx->fc_img[1].p;
+        CHECK(forward_warp_dev(ctx, eng_a, f_ab, fw, fh, W, H, fmt, frac, pyramid, ta, fill ? c0 : nullptr));
+        CHECK(forward_warp_dev(ctx, eng_b, f_ba, fw, fh, W, H, fmt, wa, pyramid, tb, fill ? c1 : nullptr));
+        return weighted_tail_dev(ctx, out, ta, eng_a, tb, eng_b, wa, W, H, fmt, fill ? c0 : nullptr, fill ? c1 : nullptr,
+                                 cs.taps_above_first != 0, *ss, bad);
+    }
     return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
 }
 
@@ -909,7 +1022,34 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
             pb = warp_params(eng_b, f_ab, fw, fh, wa, W, false);
             smode = 1;
         } else if (sel.interp == 2) {
-            return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend with Smart Blend is not on the device yet");
+            // smartblend.rs:400-420 (weighted_blend_smart): the warps without hold and with coverage,
+            // then weighted_tail (sharpening, the plain Smart Blend, the fill)
+            if (!ss->wb) return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend needs its scratch");
+            if (!f_ab || !f_ba) return ctx->fail(TW_ERR_MISMATCH, "the composition needs both flows");
+            const WbScratch& ws = *ss->wb;
+            size_t px = (size_t)W * H, ib = px * 4 * sample_bytes(fmt);
+            for (int i = 0; i < 2; i++) {
+                CHECK(ctx->ensure(*ws.wt[i], ib, "warped frame"));
+                CHECK(ctx->ensure(*ws.cov[i], px, "coverage"));
+            }
+            pa = warp_params(eng_a, f_ba, fw, fh, frac, W, false);
+            pb = warp_params(eng_b, f_ab, fw, fh, wa, W, false);
+            LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pa, fmt, ws.wt[0]->p, ws.cov[0]->as<uint8_t>(), W, H, bad);
+            LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pb, fmt, ws.wt[1]->p, ws.cov[1]->as<uint8_t>(), W, H, bad);
+            void* comp = out;
+            if (to_wire) {
+                CHECK(ctx->ensure(*ss->comp, ib, "composite"));
+                comp = ss->comp->p;
+            }
+            CHECK(weighted_tail_dev(ctx, comp, ws.wt[0]->p, eng_a, ws.wt[1]->p, eng_b, wa, W, H, fmt, ws.cov[0]->as<uint8_t>(),
+                                    ws.cov[1]->as<uint8_t>(), cs.taps_above_first != 0, *ss, bad));
+            if (to_wire) {
+                long n = (long)px;
+                if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)comp, (uint8_t*)out, W, H, flip_out);
+                else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)comp, (uint16_t*)out, W, H, flip_out);
+                else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)comp, (float*)out, W, H, flip_out);
+            }
+            return TW_OK;
         } else {
             return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
         }
@@ -948,7 +1088,22 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
         wb = frac;
         mode = blend_mode(frac);
     } else if (sel.interp == 2) {
-        return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend on the vector path is not on the device yet");
+        // compose/vector.rs:255-272: the two warps with hold, each sharpened against its frame, blend
+        if (!ss || !ss->wb) return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend needs its scratch");
+        if (!f_ab || !f_ba) return ctx->fail(TW_ERR_MISMATCH, "the composition needs both flows");
+        const WbScratch& ws = *ss->wb;
+        size_t ib = (size_t)W * H * 4 * sample_bytes(fmt);
+        for (int i = 0; i < 2; i++) CHECK(ctx->ensure(*ws.wt[i], ib, "warped frame"));
+        WarpParams qa = warp_params(eng_a, f_ba, fw, fh, frac, W, true);
+        WarpParams qb = warp_params(eng_b, f_ab, fw, fh, wa, W, true);
+        LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, qa, fmt, ws.wt[0]->p, (uint8_t*)nullptr, W, H, bad);
+        LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, qb, fmt, ws.wt[1]->p, (uint8_t*)nullptr, W, H, bad);
+        CHECK(sharpen_dev(ctx, ws.wt[0]->p, eng_a, W, H, fmt, frac, cs.taps_above_first != 0, ws, nullptr));
+        CHECK(sharpen_dev(ctx, ws.wt[1]->p, eng_b, W, H, fmt, wa, cs.taps_above_first != 0, ws, nullptr));
+        pa = warp_params(ws.wt[0]->p, nullptr, 0, 0, 0.0f, W, true);
+        pb = warp_params(ws.wt[1]->p, nullptr, 0, 0, 0.0f, W, true);
+        wb = frac;
+        mode = blend_mode(frac);
     } else {
         return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
     }
@@ -961,7 +1116,7 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
 
 // compose.rs:218-231 (interpolate): the fast path without flows
 int interpolate_dev(tw_ctx* ctx, const tw_selection& sel, const void* eng_a, const void* eng_b, int W, int H, int fmt,
-                    void* out, bool to_wire, int* bad) {
+                    void* out, bool to_wire, int* bad, const SmartScratch* ss) {
     WarpParams pa = warp_params(eng_a, nullptr, 0, 0, 0.0f, W, true);
     WarpParams pb = warp_params(eng_b, nullptr, 0, 0, 0.0f, W, true);
     int mode;
@@ -972,11 +1127,38 @@ int interpolate_dev(tw_ctx* ctx, const tw_selection& sel, const void* eng_a, con
         wb = (float)(1.0 - (double)sel.wa);
         mode = blend_mode(wb);
     } else if (sel.interp == 2) {
-        // blend.rs:281-302: equals blend(a, b, 1 - wa) for 8 and 16 bpc
-        if (fmt == TW_F32)
-            return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend without flows of float frames is not on the device yet");
+        // blend.rs:276-296: equals blend(a, b, 1 - wa) for 8 and 16 bpc
         wb = 1.0f - sel.wa;
         mode = blend_mode(wb);
+        if (fmt == TW_F32) {
+            // float frames: blend(a + 0, b + 0, 1 - wa), unless a sample is NaN or above 1e30 in
+            // magnitude; then the full sequence with every filter (weighted_blend_noflow_reference:
+            // sharpen_step, the engine's tap order). The device decides: the sharpening kernels are
+            // gated by the unsound flag.
+            if (!ss || !ss->wb || !ss->wb_gate || (to_wire && !ss->comp))
+                return ctx->fail(TW_ERR_UNSUPPORTED, "Weighted Blend without flows needs its scratch");
+            const WbScratch& ws = *ss->wb;
+            long n = (long)W * H;
+            size_t ib = (size_t)n * 16;
+            for (int i = 0; i < 2; i++) CHECK(ctx->ensure(*ws.wt[i], ib, "sharpened frame"));
+            int* gate = ss->wb_gate;
+            CHECK(ctx->cuda(cudaMemsetAsync(gate, 0, sizeof(int), ctx->cur), "flag"));
+            LAUNCH(ctx, k_f32_unsound, grid1(4 * n), TB, 0, (const float*)eng_a, 4 * n, gate);
+            LAUNCH(ctx, k_f32_unsound, grid1(4 * n), TB, 0, (const float*)eng_b, 4 * n, gate);
+            LAUNCH(ctx, k_copy_gated, grid1(n), TB, 0, (const uint4*)eng_a, (uint4*)ws.wt[0]->p, n, gate);
+            LAUNCH(ctx, k_copy_gated, grid1(n), TB, 0, (const uint4*)eng_b, (uint4*)ws.wt[1]->p, n, gate);
+            CHECK(sharpen_dev(ctx, ws.wt[0]->p, eng_a, W, H, fmt, wb, false, ws, gate));
+            CHECK(sharpen_dev(ctx, ws.wt[1]->p, eng_b, W, H, fmt, sel.wa, false, ws, gate));
+            void* eo = out;
+            if (to_wire) {
+                CHECK(ctx->ensure(*ss->comp, ib, "composite"));
+                eo = ss->comp->p;
+            }
+            LAUNCH(ctx, k_wb_noflow_f32, grid1(n), TB, 0, (const float*)eng_a, (const float*)eng_b, ws.wt[0]->as<float>(),
+                   ws.wt[1]->as<float>(), gate, wb, (float)(1.0 - (double)wb), mode, (float*)eo, n);
+            if (to_wire) LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)eo, (float*)out, W, H, false);
+            return TW_OK;
+        }
     } else {
         return ctx->fail(TW_ERR_BAD_PARAM, "interpolation mode %d is not 0 (Nearest), 1 (Blend) or 2 (Weighted Blend)", sel.interp);
     }
@@ -1040,7 +1222,8 @@ int tw_open(int device, tw_ctx** out) {
 void tw_close(tw_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->masks, &ctx->lay_mem, &ctx->lay_in, &ctx->fc_img[0], &ctx->fc_img[1], &ctx->fc_cov[0], &ctx->fc_cov[1], &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
+    for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->masks, &ctx->lay_mem, &ctx->lay_in, &ctx->fc_img[0], &ctx->fc_img[1], &ctx->fc_cov[0], &ctx->fc_cov[1], &ctx->wb_wt[0], &ctx->wb_wt[1],
+                    &ctx->wb_tmp[0], &ctx->wb_tmp[1], &ctx->wb_mask[0], &ctx->wb_mask[1], &ctx->wb_cov[0], &ctx->wb_cov[1], &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
                     &ctx->fw_vd, &ctx->fw_pyr, &ctx->fw_tmp[0], &ctx->fw_tmp[1], &ctx->fw_cnt, &ctx->fw_off,
                     &ctx->fw_fill, &ctx->fw_sums, &ctx->fw_keys, &ctx->fw_cols, &ctx->fw_scratch, &ctx->fw_longq,
                     &ctx->fw_flags, &ctx->fw_cov})
@@ -1054,6 +1237,7 @@ void tw_close(tw_ctx* ctx) {
             L.flow[i].release(&ctx->held);
             for (int j = 0; j < 3; j++) L.scratch[i][j].release(&ctx->held);
             if (i == 0) { L.comp.release(&ctx->held); L.holes.release(&ctx->held); L.fill.release(&ctx->held); }
+            for (DevBuf* b : {&L.wb_wt[i], &L.wb_tmp[i], &L.wb_mask[i], &L.wb_cov[i]}) b->release(&ctx->held);
             if (L.s[i]) cudaStreamDestroy(L.s[i]);
             if (L.ev_pyr[i]) cudaEventDestroy(L.ev_pyr[i]);
         }
@@ -1378,7 +1562,8 @@ int tw_compose_vectors(tw_ctx* ctx, const tw_engine_settings* settings, const tw
     CHECK(ctx->ensure(ctx->eng[2], ob, "compose output"));
     int* flags = ctx->flags.as<int>();
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
-    SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1};
+    WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
+    SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
     CHECK(compose_dev(ctx, *settings, *sel, ctx->eng[0].p, ctx->eng[1].p, f_ab ? ctx->flow[0].as<float>() : nullptr,
                       f_ba ? ctx->flow[1].as<float>() : nullptr, fw, fh, a->width, a->height, a->fmt, ctx->eng[2].p,
                       false, false, flags + FL_BAD, &ss));
@@ -1637,7 +1822,8 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
                                      flags + FL_ANY1, flags + FL_NAN, mpyr[1], mpyr[0]));
     }
     // the composition, bottom layer first (plates.rs:373-412)
-    SmartScratch ss{nullptr, &ctx->fill, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1};
+    WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
+    SmartScratch ss{nullptr, &ctx->fill, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
     DevBuf& fillbuf = ctx->work[1];
     ss.holes = &ctx->masks;  // the composition's own holes mask (the refill uses ctx->holes)
     auto refill = [&](void* p, int side, int k) -> int {
@@ -1846,7 +2032,9 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
         CHECK(ctx->cuda(cudaEventRecord(L.ev_pyr[1], L.s[1]), "event"));
         CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_pyr[1], 0), "event"));
         ctx->cur = L.s[0];
-        CHECK(interpolate_dev(ctx, sel, L.eng[0].p, L.eng[1].p, W, H, fmt, out_wire, true, flags + FL_BAD));
+        WbScratch wbs = wb_scratch(L.wb_wt, L.wb_tmp, L.wb_mask, L.wb_cov);
+        SmartScratch ss{&L.comp, &L.holes, &L.fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
+        CHECK(interpolate_dev(ctx, sel, L.eng[0].p, L.eng[1].p, W, H, fmt, out_wire, true, flags + FL_BAD, &ss));
         CHECK(ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event"));
         return TW_OK;
     }
@@ -1893,7 +2081,8 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
     CHECK(ctx->cuda(cudaEventRecord(L.ev_solve1, L.s[1]), "event"));
     CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_solve1, 0), "event"));
     ctx->cur = L.s[0];
-    SmartScratch ss{&L.comp, &L.holes, &L.fill, flags + FL_HOLE, flags + FL_SIDE1};
+    WbScratch wbs = wb_scratch(L.wb_wt, L.wb_tmp, L.wb_mask, L.wb_cov);
+    SmartScratch ss{&L.comp, &L.holes, &L.fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
     CHECK(compose_dev(ctx, s.compose, sel, L.eng[0].p, L.eng[1].p, need_ab ? L.flow[0].as<float>() : nullptr,
                       need_ba ? L.flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, out_wire, true, flip,
                       flags + FL_BAD, &ss));
@@ -2167,7 +2356,8 @@ static int vector_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_s
     if (need_ba)
         CHECK(solve_pyramids_dev(ctx, py_, px_, py_ + pf, px_ + pf, g, fs, ctx->work[1], ctx->flow[1].as<float>(),
                                  flags + FL_ANY1, flags + FL_NAN));
-    SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1};
+    WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
+    SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
     return compose_dev(ctx, s.compose, sel, ctx->eng[0].p, ctx->eng[1].p, need_ab ? ctx->flow[0].as<float>() : nullptr,
                        need_ba ? ctx->flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, res, false, false, flags + FL_BAD,
                        &ss);
@@ -2218,7 +2408,9 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
         uint8_t* dst = (uint8_t*)out + (size_t)k * bytes;
         if (!vector) {
             CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
-            CHECK(interpolate_dev(ctx, sel, ctx->eng[0].p, ctx->eng[1].p, W, H, fmt, ctx->wire[2].p, true, flags + FL_BAD));
+            WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
+            SmartScratch ss{&ctx->eng[2], &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
+            CHECK(interpolate_dev(ctx, sel, ctx->eng[0].p, ctx->eng[1].p, W, H, fmt, ctx->wire[2].p, true, flags + FL_BAD, &ss));
         } else {
             // matte.rs:141-188: each layer's raw matte at A and at B read straight, in the same row order
             for (int side = 0; side < 2; side++)
