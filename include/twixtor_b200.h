@@ -239,7 +239,7 @@ int tw_smart_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* p1, const tw_
  * in-between frame of the FG matte effects: every layer (FG1 .. FG nfg, then Main_BG) solved on its
  * own layer images with its solver masks (tw_solve_masked), its plates (its layer image OVER the
  * other frame's warped to its time) refilled, the single layer composition of the warping code
- * (codes 0 and 1, Nearest or Blend), and the layers composed OVER from the bottom up. a, b: the
+ * (codes 0 to 3; Nearest, Blend or Weighted Blend), and the layers composed OVER from the bottom up. a, b: the
  * engine images (also the tracking frames); mattes_a / mattes_b: nfg raw mattes of width*height
  * floats each at A and at B, FG1 first (0..1; a float matte as it is); sensitivity: nfg + 1 values
  * (0..1), Main_BG last. nfg <= 3. The inverse matte shrink is 0 and no tracking point is in use;

@@ -1716,12 +1716,13 @@ int tw_fill_holes(tw_ctx* ctx, tw_image_mut* img, const void* mask, int32_t mask
 
 // ---- the layered composition with plates (layers/plates.rs:330-412) ---------------------------------
 
-// The settings the layered path serves (warping codes 0 and 1, Nearest or Blend, no 360 filters).
+// The settings the layered path serves (warping codes 0 to 3, Nearest, Blend or Weighted Blend, no
+// 360 filters).
 static int layers_check(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel) {
     const tw_engine_settings& cs = s.compose;
     if (cs.warp_mode < 0 || cs.warp_mode > 3) return ctx->fail(TW_ERR_BAD_PARAM, "layers: warping code %d is not 0 to 3", cs.warp_mode);
-    if (sel.interp != 0 && sel.interp != 1)
-        return ctx->fail(TW_ERR_UNSUPPORTED, "layers: Weighted Blend is not on the device yet");
+    if (sel.interp < 0 || sel.interp > 2)
+        return ctx->fail(TW_ERR_BAD_PARAM, "layers: interpolation mode %d is not 0 to 2", sel.interp);
     if (cs.wrap_360 || s.flow.wrap || s.flow.track_alpha)
         return ctx->fail(TW_ERR_UNSUPPORTED, "layers: the wrap-around (360) filters are not on the device");
     return TW_OK;
