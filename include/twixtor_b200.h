@@ -259,6 +259,19 @@ int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selecti
 int tw_forward_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_flow* flow, float amount,
                     int32_t pyramid, uint8_t* cov);
 
+/* warp::blurcomp::motion_blur (warp/blurcomp.rs:176-559, is360 off): the flow directed motion blur
+ * of Blur Compensation, the bilinear taps (hiq != 0) or the nearest ones, the shutter offset of
+ * the centre. The compositions run it themselves after the composite (with the clear or the lerp
+ * of compensate); this is the primitive alone. */
+int tw_motion_blur(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_flow* flow, float amount,
+                   int32_t hiq, float shutter);
+
+/* The powf of the plugin's C runtime that the Delinearize prep calls (crt_powf.rs:229-268), over
+ * n argument pairs: a check hook for the runtime's traced values, as tw_check_logf is for logf.
+ * Bit exact on the prep's arguments (a base >= 0 or NaN, the exponent 1 / 2.2); a negative base
+ * with an integer exponent and results that over- or underflow float are not the runtime's. */
+int tw_check_powf(tw_ctx* ctx, const float* x, const float* y, float* out, int64_t n);
+
 /* Self check of the device's logf of the forward warp's mip level (forward/mesh.rs:89-90), which
  * must equal the host C library's logf bit for bit: out[i] = logf(x[i]) computed on the device. */
 int tw_check_logf(tw_ctx* ctx, const float* x, float* out, int64_t n);

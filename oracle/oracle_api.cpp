@@ -18,6 +18,7 @@
 #include "oracle_forward.h"
 #include "oracle_vectors.h"
 #include "oracle_layers.h"
+#include "oracle_filters.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -153,6 +154,7 @@ struct or_retime_params {
     int rows_reversed;         // motion path on bottom-up rows
     int taps_above_first;      // vertical border rows of the solver's filters
     int video_360;             // "360 Video": video range luma, binary alpha Smart Blend
+    int prep;                  // Image Prep popup: 1 None, 2 Contrast/Edge Enhance, 3 Delinearize
 };
 
 const char* or_last_error(void) { return g_err.c_str(); }
@@ -234,10 +236,12 @@ int or_geometry(int quality, int hiq, int w, int h, int* reduction, int* sizes, 
 
 // The band pass levels of one engine image, concatenated finest first.
 int or_build_pyramid(const void* engine, int w, int h, int fmt, int quality, int hiq, float sensitivity, int above_first,
-                     float* levels_out) {
+                     int prep, float* levels_out) {
     Image img(w, h, (Fmt)fmt);
     std::memcpy(img.data(), engine, img.bytes());
     FlowSettings s;
+    s.prep_contrast_edge = prep == 2;
+    s.prep_delinearize = prep == 3;
     s.taps_above_first = above_first != 0;
     s.quality = quality;
     s.hiq = hiq != 0;
@@ -412,6 +416,55 @@ int or_compose_vectors2(const void* a_eng, const void* b_eng, int w, int h, int 
     return 0;
 }
 
+// warp/blurcomp.rs:176-559 (motion_blur, is360 off) on engine images
+int or_motion_blur(void* out_eng, const void* src_eng, int w, int h, int fmt, const float* flow, int fw, int fh,
+                   float amount, int hiq, float shutter) {
+    Image src(w, h, (Fmt)fmt), out(w, h, (Fmt)fmt);
+    std::memcpy(src.data(), src_eng, src.bytes());
+    FlowField f(fw, fh);
+    std::memcpy(f.d.data(), flow, f.d.size() * 4);
+    std::string e;
+    int rc = motion_blur(out, src, f, amount, hiq != 0, shutter, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(out_eng, out.data(), out.bytes());
+    return 0;
+}
+
+// crt_powf.rs:229-268 over arrays (the Delinearize powf)
+void or_crt_powf(const float* x, const float* y, float* out, int n) {
+    for (int i = 0; i < n; i++) out[i] = crt_powf(x[i], y[i]);
+}
+
+// compose_vectors with the whole selection and compose settings (the Blur Compensation tail reads
+// s0, s1, the slider and the render quality)
+int or_compose_vectors3(const void* a_eng, const void* b_eng, int w, int h, int fmt, const float* f_ab, const float* f_ba,
+                        int fw, int fh, float s0, float s1, float wa, int interp, int warp_mode, int video_360,
+                        int taps_above_first, int gouraud, float blur, int quality_high, void* out_eng) {
+    Image a(w, h, (Fmt)fmt), b(w, h, (Fmt)fmt), out;
+    std::memcpy(a.data(), a_eng, a.bytes());
+    std::memcpy(b.data(), b_eng, b.bytes());
+    FlowField fab(fw, fh), fba(fw, fh);
+    if (f_ab) std::memcpy(fab.d.data(), f_ab, fab.d.size() * 4);
+    if (f_ba) std::memcpy(fba.d.data(), f_ba, fba.d.size() * 4);
+    ComposeSettings cs;
+    cs.warp_mode = warp_mode;
+    cs.video_360 = video_360 != 0;
+    cs.taps_above_first = taps_above_first != 0;
+    cs.gouraud = gouraud != 0;
+    cs.blur = blur;
+    cs.quality_high = quality_high != 0;
+    Selection sel;
+    sel.s0 = s0;
+    sel.s1 = s1;
+    sel.wa = wa;
+    sel.interp = interp;
+    std::string e;
+    int rc = compose_vectors(cs, sel, a, b, f_ab ? &fab : nullptr, f_ba ? &fba : nullptr, &out, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(out_eng, out.data(), out.bytes());
+    return 0;
+}
+
 // ---- the whole effect ---------------------------------------------------------------------------
 
 // One output frame's selection (timeline.rs:451-469) for output frame index n of a clip.
@@ -485,6 +538,8 @@ static int retime_one(const void* frames, int nframes, int w, int h, int fmt, co
         fs.sensitivity = sensitivity;
         fs.taps_above_first = p->taps_above_first != 0;
         fs.video_range_luma = p->video_360 != 0;  // compose/vector.rs:72-82 (flow_settings)
+        fs.prep_contrast_edge = p->prep == 2;     // frontend.rs:224-225
+        fs.prep_delinearize = p->prep == 3;
         FlowField fab, fba;
         bool have_ab = false, have_ba = false;
         if (interp == 0) {
@@ -595,6 +650,7 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
         job.fs.hiq = p->quality_high != 0;
         job.fs.taps_above_first = p->taps_above_first != 0;
         job.cs.quality_high = p->quality_high != 0;
+        job.cs.blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
         job.cs.warp_mode = p->smart_blend;
         job.cs.gouraud = true;  // plugins/retime-fgbg/src/glue.rs:142-143: every forward warp is the Gouraud variant
         job.cs.taps_above_first = p->taps_above_first != 0;

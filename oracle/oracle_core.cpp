@@ -4,6 +4,8 @@
 #include "oracle_smart.h"
 #include "oracle_forward.h"
 #include "oracle_filters.h"
+#include "pow_tables.h"
+#include <cstring>
 
 #include <algorithm>
 #include <cstdio>
@@ -483,6 +485,77 @@ Plane luma(const Image& img, bool track_alpha, bool video_range) {
     return out;
 }
 
+// crt_powf.rs:229-268: the plugin runtime's single precision powf for a positive finite base (a
+// logarithm and an exponential in double precision from tables, narrowed once), the rounded double
+// precision pow elsewhere. The tables are the closed forms of the generator beside the library's
+// sources (1/c, ln 2c, 2^(j/64)).
+float crt_powf(float x, float y) {
+    static const uint64_t RCP[257] = TW_POW_RCP_INIT;
+    static const uint64_t LOG[257] = TW_POW_LOG_INIT;
+    static const uint64_t EXP2[64] = TW_POW_EXP2_INIT;
+    auto d = [](uint64_t b) { double v; std::memcpy(&v, &b, 8); return v; };
+    auto u = [](double v) { uint64_t b; std::memcpy(&b, &v, 8); return b; };
+    if (!(x > 0.0f) || !std::isfinite(x) || !std::isfinite(y) || y == 0.0f || y == 1.0f)
+        return (float)std::pow((double)x, (double)y);
+    double xd = x, yd = y;
+    double t = xd - 1.0;
+    double l;
+    if (x < 1.0625f && std::fabs(t) < 0.0625) {
+        double sv = t / (t + 2.0);
+        double st = sv * t;
+        double uu = sv + sv;
+        double z = uu * uu;
+        double t0 = z * d(TW_POW_C0), t1 = z * d(TW_POW_C1);
+        double uz = uu * z;
+        double u0 = t0 + d(TW_POW_A0), u1 = t1 + d(TW_POW_A1);
+        double uz3 = (z * z) * uz;
+        double sum = uz * u0 + uz3 * u1;
+        l = t + (sum - st);
+    } else {
+        uint64_t mant = u(xd) & 0x000fffffffffffffull;
+        size_t idx = (size_t)((mant >> 44) + ((mant >> 43) & 1));
+        double c = d(((uint64_t)idx | 0x3fe00ull) << 44);
+        double m = d(mant | 0x3fe0000000000000ull);
+        int64_t e = (int64_t)((u(xd) & 0x7ff0000000000000ull) >> 52) - 1023;
+        double r = (c - m) * d(RCP[idx]);
+        double q = r + (r * r) * (r * d(TW_POW_THIRD) + 0.5);
+        double el = (double)e * d(TW_POW_LN2);
+        l = (el + d(LOG[idx])) - q;
+    }
+    double w = yd * l;
+    if (w > d(TW_POW_LIM_HI) || w <= d(TW_POW_LIM_LO)) return (float)std::pow(xd, yd);
+    int32_t n = (int32_t)std::nearbyint(w * d(TW_POW_K64));
+    double r = w - (double)n * d(TW_POW_LN2_64);
+    double p = (r * r) * (r * d(TW_POW_SIXTH) + 0.5) + r;
+    double tj = d(EXP2[n & 63]);
+    double v = p * tj + tj;
+    uint64_t k = (uint64_t)(uint32_t)(n >> 6);
+    return (float)d(u(v) + (k << 52));
+}
+
+// prep.rs:296-307 (delinearize): p = powf(max(p, 0) / 255, 1 / 2.2) * 255; -0.0 stays
+void delinearize(Plane& p) {
+    const float inv = 1.0f / 2.2f;
+    for (auto& v : p.d) {
+        if (v <= 0.0f && v != 0.0f) v = 0.0f;
+        float base = v / 255.0f;
+        v = crt_powf(base, inv) * 255.0f;
+    }
+}
+
+// prep.rs:326-340 (edge_enhance): the Gaussian of radius 2.0, the solver's gradient, then per pixel
+// m = sqrt(gx^2 + gy^2), f = m <= 20 ? m * 0.05 : 1, p = (f * 255 + p) * 0.5
+void edge_enhance(Plane& p, bool above_first) {
+    blur_gaussian(p.d.data(), p.w, p.h, 1, 2.0f, above_first);
+    std::vector<float> g = calc_grad(p.d.data(), p.w, p.h);
+    for (size_t i = 0; i < p.d.size(); i++) {
+        float gx = g[i * 2], gy = g[i * 2 + 1];
+        float m = std::sqrt(gx * gx + gy * gy);
+        float f = m <= 20.0f ? m * 0.05f : 1.0f;
+        p.d[i] = (f * 255.0f + p.d[i]) * 0.5f;
+    }
+}
+
 Plane reduce(Plane t, int r, bool above_first) {  // prep.rs:252-259
     for (int i = 0; i < r; i++) {
         blur5(t.d.data(), t.w, t.h, above_first);
@@ -495,8 +568,9 @@ Plane reduce(Plane t, int r, bool above_first) {  // prep.rs:252-259
 bool build_pyramid(const Image& img, const FlowSettings& s, Pyramid* out, std::string* err) {
     if (!geometry(s, img.w, img.h, &out->geo, err)) return false;
     if (s.video_range_luma && s.track_alpha) { *err = "video range luma with track alpha"; return false; }
-    if (s.prep_delinearize || s.prep_contrast_edge) { *err = "prep transforms are not restated"; return false; }
     Plane orig = reduce(luma(img, s.track_alpha, s.video_range_luma), out->geo.reduction, s.taps_above_first);
+    if (s.prep_delinearize) delinearize(orig);  // flow.rs:248-253: Delinearize, then Contrast/Edge
+    if (s.prep_contrast_edge) edge_enhance(orig, s.taps_above_first);
     int n = out->geo.levels;
     out->levels.clear();
     for (int i = 0; i < n; i++) {
@@ -1201,9 +1275,8 @@ bool nearest_uses_f_ab(float wa, int code) {  // compose/vector.rs:61-64
     return (wa < 0.5f && c < 2) || (0.5f <= wa && c > 1);
 }
 
-int compose_vectors(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b,
-                    const FlowField* f_ab, const FlowField* f_ba, Image* out, std::string* err) {
-    if (cs.blur > 0.005f && std::fabs(sel.s0 - sel.s1) > 1e-6f) { *err = "blur compensation is not restated"; return 2; }
+static int compose_body(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b,
+                        const FlowField* f_ab, const FlowField* f_ba, Image* out, std::string* err) {
     if (cs.warp_mode == 1) return compose_smart(cs, sel, a, b, f_ab, f_ba, cs.taps_above_first, out, err);
     if (cs.warp_mode == 2 || cs.warp_mode == 3) return compose_forward(cs, sel, a, b, f_ab, f_ba, out, err);
     if (cs.warp_mode != 0) { *err = "compose: warping code not 0 to 3"; return 1; }
@@ -1233,6 +1306,16 @@ int compose_vectors(const ComposeSettings& cs, const Selection& sel, const Image
     }
     *err = "bad interpolation mode";
     return 1;
+}
+
+int compose_vectors(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b,
+                    const FlowField* f_ab, const FlowField* f_ba, Image* out, std::string* err) {
+    int rc = compose_body(cs, sel, a, b, f_ab, f_ba, out, err);
+    if (rc) return rc;
+    // compose/vector.rs:276-281: the Blur Compensation tail with F_AB, else the single flow
+    const FlowField* flow = f_ab ? f_ab : f_ba;
+    if (!flow) return 0;
+    return blur_compensation(*out, *flow, sel.s0, sel.s1, cs.blur, cs.quality_high, err);
 }
 
 int interpolate(const Selection& sel, const Image& a, const Image& b, Image* out, std::string* err) {

@@ -172,6 +172,9 @@ bool build_pyramid(const Image& img, const FlowSettings& s, Pyramid* out, std::s
 // solver (flow.rs:277-1353)
 
 std::vector<float> calc_grad(const float* img, int w, int h);
+void edge_enhance(Plane& p, bool above_first);  // prep.rs:326-340
+void delinearize(Plane& p);                      // prep.rs:296-307
+float crt_powf(float x, float y);                // crt_powf.rs:229-268
 std::vector<float> calc_a(const std::vector<float>& grad, int w, int h);
 std::vector<float> calc_b(const float* i1, const float* i0, const float* grad, const float* flow, int w, int h);
 void new_disp(float* flow, const float* a, const float* b, size_t npx);

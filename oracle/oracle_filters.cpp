@@ -1,6 +1,7 @@
-// Test infrastructure: the CPU oracle's restatement of the Weighted Blend filters
-// (plugins/retime-engine/src/filters.rs). Plain single-threaded C++, compiled without FP
-// contraction; each function names the reference lines it follows.
+// Test infrastructure: the CPU oracle's restatement of the compositor's tails, the Weighted Blend
+// filters (plugins/retime-engine/src/filters.rs) and Blur Compensation (warp/blurcomp.rs). Plain
+// single-threaded C++, compiled without FP contraction; each function names the reference lines it
+// follows.
 #include "oracle_filters.h"
 #include <algorithm>
 #include <cmath>
@@ -300,6 +301,146 @@ void sharpen_step(Image& frame, const Image& original, float t, bool above_first
     lerp(sharp, base, sharpen_weight(t));
     for (auto& v : mask.d) v = 255 - v;
     composite_masked(frame, sharp, mask);
+}
+
+// ---- Blur Compensation (warp/blurcomp.rs) --------------------------------------------------------------
+
+namespace {
+
+const int TAP_LIMIT = 1 << 16;
+
+float store_blur_int(float v, float white) {  // warp.rs:272-274 / :292-294
+    float f = (float)cvtt32(v + 0.5f);
+    f = std::max(f, 0.0f);
+    return std::min(f, white);
+}
+
+}  // namespace
+
+int motion_blur(Image& dest, const Image& src, const FlowField& flow, float amount, bool hiq, float shutter,
+                std::string* err) {
+    if (dest.w != src.w || dest.h != src.h || dest.fmt != src.fmt) { *err = "motion blur: shapes"; return 1; }
+    if (src.w < 2 || src.h < 2 || flow.w < 2 || flow.h < 2) { *err = "motion blur needs at least 2x2"; return 1; }
+    int w = src.w, h = src.h;
+    int w1i = w - 1, h1i = h - 1;
+    float rx = (float)(flow.w - 1) / (float)w1i;
+    float ry = (float)(flow.h - 1) / (float)h1i;
+    float kx = (0.5f / rx) * amount;
+    float ky = (0.5f / ry) * amount;
+    bool shifted = shutter != 0.5f;
+    float k = shutter * 2.0f - 1.0f;
+    float wf = (float)w, hf = (float)h;
+    const float TINY = bits_f(0x358637bdu);
+    bool bad = false;
+    auto sample = [&](size_t i, int c) -> float {
+        return src.fmt == U8 ? (float)src.u8[i * 4 + c] : src.fmt == U16 ? (float)src.u16[i * 4 + c] : src.f32[i * 4 + c];
+    };
+    auto store = [&](size_t i, int c, float v) {
+        if (dest.fmt == U8) dest.u8[i * 4 + c] = (uint8_t)store_blur_int(v, 255.0f);
+        else if (dest.fmt == U16) dest.u16[i * 4 + c] = (uint16_t)store_blur_int(v, 65535.0f);
+        else dest.f32[i * 4 + c] = v;
+    };
+    for (int y = 0; y < h; y++) {
+        float yf = (float)y, fy = yf * ry;
+        for (int x = 0; x < w; x++) {
+            size_t i = (size_t)y * w + x;
+            float xf = (float)x;
+            float d[2];
+            warp_flow_bilerp(flow, xf * rx, fy, d);
+            float vx = d[0] * kx, vy = d[1] * ky;
+            float d2 = vy * vy + vx * vx;
+            if (hiq && TINY > d2) {  // the source pixel, copied
+                if (dest.fmt == U8) for (int c = 0; c < 4; c++) dest.u8[i * 4 + c] = src.u8[i * 4 + c];
+                else if (dest.fmt == U16) for (int c = 0; c < 4; c++) dest.u16[i * 4 + c] = src.u16[i * 4 + c];
+                else for (int c = 0; c < 4; c++) dest.f32[i * 4 + c] = src.f32[i * 4 + c];
+                continue;
+            }
+            float dist = std::sqrt(d2);
+            float cx = shifted ? vx * k + xf : xf, cy = shifted ? vy * k + yf : yf;
+            if (!hiq) { cx = cx + 0.5f; cy = cy + 0.5f; }
+            int n = cvtt32(dist + 1.0f);
+            float sx, sy;
+            if (n < 2) { n = 2; sx = vx; sy = vy; }
+            else { float dd = (float)(n - 1); sx = vx / dd; sy = vy / dd; }
+            if (n > TAP_LIMIT) {
+                bad = true;
+                for (int c = 0; c < 4; c++) store(i, c, 0.0f);
+                continue;
+            }
+            float sum[4] = {0, 0, 0, 0};
+            int cnt = 0;
+            if (hiq) {  // blurcomp.rs:398-455
+                auto tap = [&](float qx, float qy) {
+                    if (std::isnan(qx) || std::isnan(qy)) { bad = true; return; }
+                    if (0.0f <= qx && qx < wf && 0.0f <= qy && qy < hf) {
+                        cnt++;
+                        float t[4];
+                        bilerp4_image(src, qx, qy, t);
+                        for (int c = 0; c < 4; c++) sum[c] += t[c];
+                    }
+                };
+                float qx = cx, qy = cy;
+                for (int j = 0; j < n; j++) { tap(qx, qy); qx += sx; qy += sy; }
+                float nsx = -sx, nsy = -sy;
+                qx = cx - sx; qy = cy - sy;
+                for (int j = 1; j < n; j++) { tap(qx, qy); qx += nsx; qy += nsy; }
+            } else {  // blurcomp.rs:459-559: the backward taps always count
+                int wi = w, hi = (int)hf;
+                float qx = cx, qy = cy;
+                for (int j = 0; j < n; j++) {
+                    int ix = cvtt32(qx), iy = cvtt32(qy);
+                    if (ix >= 0 && ix < wi && iy >= 0 && iy < hi) {
+                        cnt++;
+                        for (int c = 0; c < 4; c++) sum[c] += sample((size_t)iy * w + ix, c);
+                    }
+                    qx += sx; qy += sy;
+                }
+                float nsx = -sx, nsy = -sy;
+                qx = cx - sx; qy = cy - sy;
+                for (int j = 1; j < n; j++) {
+                    int ix = cvtt32(qx), iy = cvtt32(qy);
+                    if (ix >= 0 && ix < wi && iy >= 0 && iy < hi)
+                        for (int c = 0; c < 4; c++) sum[c] += sample((size_t)iy * w + ix, c);
+                    cnt++;
+                    qx += nsx; qy += nsy;
+                }
+            }
+            float inv = 1.0f / (float)cnt;
+            for (int c = 0; c < 4; c++) store(i, c, inv * sum[c]);
+        }
+    }
+    if (bad) { *err = "motion blur: a tap coordinate is NaN or a vector needs more than 65536 taps"; return 2; }
+    return 0;
+}
+
+int blur_compensation(Image& img, const FlowField& flow, float s0, float s1, float blur, bool hiq, std::string* err) {
+    float a = std::fabs(s0 - s1);  // blurcomp.rs:42-48 (blur_amount)
+    if (!((double)a > 1e-6) || !((double)blur > 0.005)) return 0;
+    float amount = (a - 1.0f) * blur;
+    if (20.0f < amount) amount = 20.0f;  // blurcomp.rs:105-128 (compensate)
+    else if (amount < -10.0f) amount = -10.0f;
+    if ((double)std::fabs(amount) < 1e-6) return 0;
+    Image tmp(img.w, img.h, img.fmt);
+    if (0.0f < amount) {
+        int rc = motion_blur(tmp, img, flow, amount, hiq, 0.5f, err);
+        if (rc) return rc;
+        size_t n = (size_t)img.w * img.h;  // blurcomp.rs:134-149 (clear_rgb_where_transparent)
+        for (size_t i = 0; i < n; i++) {
+            bool clear = tmp.fmt == U8 ? tmp.u8[i * 4] == 0 : tmp.fmt == U16 ? tmp.u16[i * 4] == 0 : tmp.f32[i * 4] == 0.0f;
+            if (!clear) continue;
+            for (int c = 1; c < 4; c++) {
+                if (tmp.fmt == U8) tmp.u8[i * 4 + c] = 0;
+                else if (tmp.fmt == U16) tmp.u16[i * 4 + c] = 0;
+                else tmp.f32[i * 4 + c] = 0.0f;
+            }
+        }
+    } else {
+        int rc = motion_blur(tmp, img, flow, 0.5f, hiq, 0.5f, err);
+        if (rc) return rc;
+        lerp(tmp, img, amount);
+    }
+    copy_image(img, tmp);
+    return 0;
 }
 
 }  // namespace orc

@@ -1,7 +1,8 @@
-// Test infrastructure: the CPU oracle's restatement of the Weighted Blend filters of the reference
-// (plugins/retime-engine/src/filters.rs): the separable blur of the sharpening step, the
-// difference mask and its clean-up, the masked composite, and one half of Weighted Blend
-// (sharpen_step_with). Only the tests, the smoke check and the benchmark's CPU legs load it.
+// Test infrastructure: the CPU oracle's restatement of the compositor's tails in the reference: the
+// Weighted Blend filters (plugins/retime-engine/src/filters.rs: the separable blur of the
+// sharpening step, the difference mask and its clean-up, the masked composite, one half of Weighted
+// Blend) and Blur Compensation (warp/blurcomp.rs: the flow directed motion blur and its amount).
+// Only the tests, the smoke check and the benchmark's CPU legs load it.
 #pragma once
 #include "oracle_core.h"
 
@@ -27,5 +28,12 @@ Mask change_mask(const Image& warped, const Image& original);                   
 void composite_masked(Image& dest, const Image& src, const Mask& m);             // filters.rs:543-603
 float sharpen_weight(float t);                                                   // filters.rs:627-631
 void sharpen_step(Image& frame, const Image& original, float t, bool above_first);  // filters.rs:649-657
+
+// warp/blurcomp.rs:176-559 (motion_blur, is360 off): returns 0, 1 (mismatch) or 2 (a NaN tap or a
+// vector of more than 65536 taps)
+int motion_blur(Image& dest, const Image& src, const FlowField& flow, float amount, bool hiq, float shutter,
+                std::string* err);
+// warp/blurcomp.rs:42-130 (blur_compensation with is360 off): in place on the composed image
+int blur_compensation(Image& img, const FlowField& flow, float s0, float s1, float blur, bool hiq, std::string* err);
 
 }  // namespace orc

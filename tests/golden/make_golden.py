@@ -28,6 +28,8 @@ Writes, next to this script:
   Twixtored Output, integer frame rates), their footage and matte clips as its ``gen_grid.py``
   renders them, and the sha256 of the output clip ``results/base.tsv`` records (the reference's
   current revision: rows reversed, taps above first).
+* ``crt_powf_traced.json`` - the 72 (x, y, powf(x, y)) bit patterns the reference traced from the
+  plugin's C runtime (plugins/retime-engine/src/crt_powf.rs tests), read as text.
 * ``f1_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/f1_cases.hex``
   (the reference's bit-exact numpy models of Smart Blend and the hole fill; format in its
   ``f1_gen.py``).
@@ -37,6 +39,9 @@ Writes, next to this script:
   (the reference's numpy models of the solver hooks of the layered solve: mask pyramid, gradient
   masking, the B step with the warped mask test, the gated block matching; format in its
   ``gen_mask.py``).
+* ``blur_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/blur_cases.hex``
+  (the reference's numpy model of the motion blur of Blur Compensation; format in its
+  ``gen_blur.py``).
 * ``warp_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/warp_cases.hex``
   (the reference's bit-exact numpy model of the inverse warp; format in its ``gen_warp.py``).
 
@@ -49,6 +54,7 @@ import importlib.util
 import io
 import json
 import os
+import re
 import sys
 import tempfile
 
@@ -56,7 +62,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
-SERVED = {"vectors", "frame_interp", "sensitivity", "blur_compensation", "smart_blend", "video_360"}
+SERVED = {"vectors", "frame_interp", "sensitivity", "blur_compensation", "smart_blend", "video_360", "prep"}
 
 
 def load_gen(ref):
@@ -73,8 +79,6 @@ def served(case):
     if any(k not in SERVED for k in params):
         return False
 
-    if float(params.get("blur_compensation", "0")) > 0.005:
-        return False
     return True
 
 
@@ -125,7 +129,7 @@ def create_vectors_grid(ref):
     print(f"create_vectors_grid.npz: {len(cases)} cases, {len(keys)} input clips")
 
 
-FG_SERVED = {"speed_percent", "warping", "frame_interp", "fg1_matte_chan", "fg2_matte_chan", "fg3_matte_chan",
+FG_SERVED = {"speed_percent", "warping", "frame_interp", "blur_compensation", "fg1_matte_chan", "fg2_matte_chan", "fg3_matte_chan",
              "fg1_sensitivity", "fg2_sensitivity", "fg3_sensitivity", "main_bg_sensitivity", "vectors"}
 
 
@@ -181,6 +185,16 @@ def fgbg_layers_grid(ref):
     print(f"fgbg_layers_grid.npz: {len(cases)} cases, {len(keys)} clips")
 
 
+def crt_powf_traced(ref):
+    src = open(os.path.join(ref, "plugins", "retime-engine", "src", "crt_powf.rs")).read()
+    m = re.search(r"const TRACED: \[\(u32, u32, u32\); \d+\] = \[(.*?)\];", src, re.S)
+    triples = [[int(a, 16), int(b, 16), int(c, 16)]
+               for a, b, c in re.findall(r"\((0x[0-9a-f]+), (0x[0-9a-f]+), (0x[0-9a-f]+)\)", m.group(1))]
+    with open(os.path.join(HERE, "crt_powf_traced.json"), "w") as f:
+        json.dump(triples, f)
+    print(f"crt_powf_traced.json: {len(triples)} vectors")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -217,6 +231,7 @@ def main():
 
     create_vectors_grid(ref)
     fgbg_layers_grid(ref)
+    crt_powf_traced(ref)
 
     txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "f1_cases.hex")).read()
     blob = bytes.fromhex("".join(txt.split()))
@@ -235,6 +250,12 @@ def main():
     with gzip.open(os.path.join(HERE, "mask_cases.bin.gz"), "wb") as f:
         f.write(blob)
     print(f"mask_cases.bin.gz: {len(blob)} bytes, sha256 {hashlib.sha256(blob).hexdigest()}")
+
+    txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "blur_cases.hex")).read()
+    blob = bytes.fromhex("".join(txt.split()))
+    with gzip.open(os.path.join(HERE, "blur_cases.bin.gz"), "wb") as f:
+        f.write(blob)
+    print(f"blur_cases.bin.gz: {len(blob)} bytes, sha256 {hashlib.sha256(blob).hexdigest()}")
 
     txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "warp_cases.hex")).read()
     blob = bytes.fromhex("".join(txt.split()))

@@ -42,6 +42,12 @@ def cv_grid():
     return meta["cases"], inputs
 
 
+def crt_powf_traced():
+    """(x, y, powf(x, y)) bit patterns traced from the plugin's C runtime."""
+    with open(os.path.join(GOLDEN, "crt_powf_traced.json")) as f:
+        return json.load(f)
+
+
 def fgbg_grid():
     """The served cases of the fgbg-layers parity grid: (meta cases, {clip name: raw bytes})."""
     z = np.load(os.path.join(GOLDEN, "fgbg_layers_grid.npz"))
@@ -58,6 +64,7 @@ def fgbg_case_params(case):
     nfg = len(case["mattes"])
     return dict(fps=(int(case["fps"]), 1), speed=float(p.get("speed_percent", 100)), vectors=int(p.get("vectors", 5)),
                 frame_interp=int(p.get("frame_interp", 2)), smart_blend=int(p.get("warping", "1")) - 1,
+                blur=float(p.get("blur_compensation", 0)),
                 sensitivity=float(p.get("main_bg_sensitivity", 70)),
                 chans=[int(p.get(f"fg{k + 1}_matte_chan", 1)) for k in range(nfg)],
                 fg_sens=[float(p.get(f"fg{k + 1}_sensitivity", 70)) for k in range(nfg)])
@@ -89,7 +96,8 @@ def case_params(case):
     return dict(fps=fpsp, speed=speed, keys=keys, vectors=int(params.get("vectors", 5)),
                 frame_interp=int(params.get("frame_interp", 2)), sensitivity=float(params.get("sensitivity", 70)),
                 blur=float(params.get("blur_compensation", 0)), smart_blend=int(params.get("smart_blend", 0)),
-                video_360=params.get("video_360", "0") == "1", rows_reversed=False, taps_above_first=False)
+                video_360=params.get("video_360", "0") == "1", rows_reversed=False, taps_above_first=False,
+                prep=int(params.get("prep", 1)))
 
 
 def f2_cases():
@@ -203,6 +211,33 @@ def f1_cases():
         exp = img()
         out.append(dict(kind=kind, fmt=depth, w=w, h=h, weight=weight, mask_kind=mask_kind, p1=p1, p2=p2, mask=mask,
                         out=exp))
+    assert p == len(blob)
+    return out
+
+
+def blur_cases():
+    """The reference's motion blur model fixtures (blur_cases.hex; format in its gen_blur.py): dicts of
+    depth, size, flow, amount, shutter, hiq, source and expected output."""
+    blob = gzip.open(os.path.join(GOLDEN, "blur_cases.bin.gz")).read()
+    assert blob[:4] == b"BLR1"
+    n = struct.unpack_from("<I", blob, 4)[0]
+    p = 8
+    out = []
+    for _ in range(n):
+        depth, w, h, fw, fh = struct.unpack_from("<IIIII", blob, p)
+        amount, shutter = (np.float32(v) for v in struct.unpack_from("<ff", blob, p + 20))
+        hiq = struct.unpack_from("<I", blob, p + 28)[0] != 0
+        p += 32
+        dt = DT[depth]
+        cnt = w * h * 4 * np.dtype(dt).itemsize
+        src = np.frombuffer(blob[p:p + cnt], dt).copy()
+        p += cnt
+        flow = np.frombuffer(blob[p:p + fw * fh * 8], np.float32).copy()
+        p += fw * fh * 8
+        want = np.frombuffer(blob[p:p + cnt], dt).copy()
+        p += cnt
+        out.append(dict(fmt=depth, w=w, h=h, fw=fw, fh=fh, amount=amount, shutter=shutter, hiq=hiq, src=src, flow=flow,
+                        out=want))
     assert p == len(blob)
     return out
 

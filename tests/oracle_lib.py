@@ -36,6 +36,7 @@ class RetimeParams(ctypes.Structure):
         ("rows_reversed", ctypes.c_int),
         ("taps_above_first", ctypes.c_int),
         ("video_360", ctypes.c_int),
+        ("prep", ctypes.c_int),
     ]
 
 
@@ -69,7 +70,8 @@ def lib():
         L.or_block_match.argtypes = [P, P, P, i, i]
         L.or_all_out_of_range.argtypes = [P, i, i]
         L.or_geometry.argtypes = [i, i, i, i, P, P, i]
-        L.or_build_pyramid.argtypes = [P, i, i, i, i, i, f, i, P]
+        L.or_build_pyramid.argtypes = [P, i, i, i, i, i, f, i, i, P]
+        L.or_compose_vectors3.argtypes = [P, P, i, i, i, P, P, i, i, f, f, f, i, i, i, i, i, f, i, P]
         L.or_solve_pair.argtypes = [P, P, i, i, i, i, i, f, i, i, P, P]
         L.or_inv_warp.argtypes = [P, P, i, i, i, P, i, i, f, i, P]
         L.or_blend.argtypes = [P, P, P, i, i, i, f]
@@ -79,6 +81,8 @@ def lib():
         L.or_select.argtypes = [ctypes.POINTER(RetimeParams), i, i, i, P, P, P, P, P, P, P]
         L.or_retime_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_retime_one.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
+        L.or_crt_powf.argtypes = [P, P, P, i]
+        L.or_motion_blur.argtypes = [P, P, i, i, i, P, i, i, f, i, f]
         L.or_retime_fgbg_one.argtypes = [P, i, P, i, P, P, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_set_threads.argtypes = [i]
         L.or_smart_blend.argtypes = [P, P, P, i, i, i, f, i]
@@ -131,11 +135,12 @@ def to_frame(engine, w, h, fmt):
     return out
 
 
-def build_pyramid(engine, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, above_first=True):
+def build_pyramid(engine, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, above_first=True, prep=1):
     _, sizes = geometry(quality, hiq, w, h)
     total = sum(a * b for a, b in sizes)
     out = np.zeros(total, np.float32)
-    n = lib().or_build_pyramid(ptr(engine), w, h, fmt, quality, int(hiq), sensitivity, int(above_first), ptr(out))
+    n = lib().or_build_pyramid(ptr(engine), w, h, fmt, quality, int(hiq), sensitivity, int(above_first), int(prep),
+                               ptr(out))
     if n < 0:
         raise ValueError(err())
     levels, off = [], 0
@@ -169,6 +174,20 @@ def inv_warp(src, w, h, fmt, flow, fw, fh, amount, hold=True, coverage=False, ou
 def compose_vectors(a, b, w, h, fmt, f_ab, f_ba, fw, fh, wa, interp=1):
     out = np.zeros_like(a)
     rc = lib().or_compose_vectors(ptr(a), ptr(b), w, h, fmt, ptr(f_ab), ptr(f_ba), fw, fh, wa, interp, ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out
+
+
+def compose_vectors3(a, b, w, h, fmt, f_ab, f_ba, fw, fh, sel, cs):
+    """compose_vectors with the selection and compose settings of the library (tw.Selection,
+    tw.EngineSettings): the Blur Compensation tail included."""
+    out = np.zeros_like(a)
+    rc = lib().or_compose_vectors3(ptr(a), ptr(b), w, h, fmt, ptr(f_ab) if f_ab is not None else None,
+                                   ptr(f_ba) if f_ba is not None else None, fw, fh, np.float32(sel.s0), np.float32(sel.s1),
+                                   np.float32(sel.wa), sel.interp, cs.warp_mode, int(cs.video_360),
+                                   int(cs.taps_above_first), int(cs.gouraud), np.float32(cs.blur), int(cs.quality_high),
+                                   ptr(out))
     if rc:
         raise ValueError(err())
     return out
@@ -291,12 +310,13 @@ def fw_triangle(verts, w1, h1, cap=4096):
 
 
 def retime_params(fps=(24, 1), quality_high=True, speed=100.0, keys=None, vectors=5, frame_interp=2, smart_blend=0,
-                  sensitivity=70.0, blur=0.0, rows_reversed=True, taps_above_first=True, video_360=False):
+                  sensitivity=70.0, blur=0.0, rows_reversed=True, taps_above_first=True, video_360=False, prep=1):
     """The `retime` parameters of one render. rows_reversed / taps_above_first at their defaults
     are the reference's current code; both False is the revision the parity grid records."""
     p = RetimeParams()
     p.rows_reversed, p.taps_above_first = int(rows_reversed), int(taps_above_first)
     p.video_360 = int(video_360)
+    p.prep = int(prep)
     p.fps_num, p.fps_den = fps
     p.quality_high = int(quality_high)
     p.speed_percent = speed
@@ -355,6 +375,25 @@ def retime_fgbg_clip(frames, nframes, mattes, chans, sens, w, h, fmt, params, no
 def retime_clip(frames, nframes, w, h, fmt, params, nout):
     out = np.zeros(nout * w * h * 4, DTYPE[fmt])
     rc = lib().or_retime_clip(ptr(frames), nframes, w, h, fmt, ctypes.byref(params), nout, ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out
+
+
+def crt_powf(x, y):
+    """The Delinearize powf of the plugin's runtime (crt_powf.rs) over float32 arrays."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(np.broadcast_to(np.asarray(y, np.float32), x.shape), np.float32)
+    out = np.zeros_like(x)
+    lib().or_crt_powf(ptr(x), ptr(y), ptr(out), x.size)
+    return out
+
+
+def motion_blur(src, w, h, fmt, flow, fw, fh, amount, hiq, shutter):
+    """warp::blurcomp::motion_blur (is360 off) of an engine image."""
+    out = np.zeros_like(src)
+    rc = lib().or_motion_blur(ptr(out), ptr(src), w, h, fmt, ptr(np.ascontiguousarray(flow, np.float32)), fw, fh,
+                              np.float32(amount), int(hiq), np.float32(shutter))
     if rc:
         raise ValueError(err())
     return out

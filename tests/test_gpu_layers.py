@@ -126,11 +126,12 @@ def fgbg_clip(dev, case, rows_reversed=True, taps_above_first=True):
     fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
     w, h, n = case["width"], case["height"], case["frames"]
     kw = golden_data.fgbg_case_params(case)
-    tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], vectors=kw["vectors"], frame_interp=kw["frame_interp"])
+    tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], vectors=kw["vectors"], frame_interp=kw["frame_interp"],
+                       blur_compensation=kw["blur"])
     sels = [tw.select(tp, k, w, h) for k in range(n)]
     s = tw.RetimeSettings(flow=tw.FlowSettings(hiq=True, taps_above_first=taps_above_first),
                           compose=tw.EngineSettings(warp_mode=kw["smart_blend"], taps_above_first=taps_above_first,
-                                                    gouraud=True),
+                                                    gouraud=True, blur=float(tw.fixed_param(kw["blur"]))),
                           motion_rows_reversed=rows_reversed)
     sens = [tw.percent_param(v) for v in kw["fg_sens"]] + [tw.percent_param(kw["sensitivity"])]
     mattes = [FG_INPUTS[m].view(tw.DTYPES[fmt]) for m in case["mattes"]]

@@ -42,6 +42,17 @@ def rand_engine(rng, w, h, fmt):
 
 CASES_ALL, INPUTS_ALL = golden_data.grid()
 
+
+def grid_settings(kw):
+    """The settings of a retime grid case (the grid's revision: rows top down, taps below first)."""
+    return tw.RetimeSettings(
+        flow=tw.FlowSettings(hiq=True, sensitivity=np.float32(np.float32(kw["sensitivity"]) / np.float32(100.0)),
+                             taps_above_first=False, video_range_luma=kw["video_360"],
+                             prep_contrast_edge=kw["prep"] == 2, prep_delinearize=kw["prep"] == 3),
+        compose=tw.EngineSettings(warp_mode=kw["smart_blend"], video_360=kw["video_360"], taps_above_first=False,
+                                  blur=float(tw.fixed_param(kw["blur"]))),
+        motion_rows_reversed=False)
+
 # ---- image boundary ------------------------------------------------------------------------------
 
 @pytest.mark.parametrize("fmt", [0, 1, 2])
@@ -338,14 +349,66 @@ def test_known_gap_cases_equal_the_oracle(dev, case):
     kw = golden_data.case_params(case)
     tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], keys=kw["keys"], vectors=kw["vectors"],
                        frame_interp=kw["frame_interp"], blur_compensation=kw["blur"])
-    settings = tw.RetimeSettings(
-        flow=tw.FlowSettings(hiq=True, sensitivity=np.float32(np.float32(kw["sensitivity"]) / np.float32(100.0)),
-                             taps_above_first=False, video_range_luma=kw["video_360"]),
-        compose=tw.EngineSettings(warp_mode=kw["smart_blend"], video_360=kw["video_360"], taps_above_first=False),
-        motion_rows_reversed=False)
+    settings = grid_settings(kw)
     out = tw.retime_clip(dev, raw, case["frames"], case["width"], case["height"], fmt, tp, case["frames"], settings)
     want = O.retime_clip(raw, case["frames"], case["width"], case["height"], fmt, O.retime_params(**kw), case["frames"])
     assert same(out, want)
+
+
+BLUR = golden_data.blur_cases()
+
+
+@pytest.mark.parametrize("i", range(len(BLUR)))
+def test_motion_blur_model_fixtures(dev, i):
+    """Blur Compensation's motion blur (warp/blurcomp.rs) against the reference's model fixtures."""
+    c = BLUR[i]
+    got = dev.motion_blur(c["src"], c["w"], c["h"], c["fmt"], c["flow"], (c["fw"], c["fh"]), c["amount"], c["hiq"],
+                          c["shutter"])
+    assert same(got, c["out"])
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("code", [0, 1, 2, 3])
+@pytest.mark.parametrize("s0,s1,blur", [(3.0, 0.5, 1.0), (1.2, 1.0, 2.0), (0.0, 3.5, 0.25), (1.0, 1.2, 0.004)])
+@pytest.mark.parametrize("hiq", [True, False])
+def test_compose_blur_compensation(dev, fmt, code, s0, s1, blur, hiq):
+    """The Blur Compensation tail of compose_vectors: the motion blur along F_AB of the composite, with
+    the clear of a positive amount and the lerp of a negative one; below the slider's threshold none."""
+    w, h = 64, 40
+    rng = np.random.RandomState(fmt * 7 + code)
+    a, b, _, _ = clip_pair(w, h, fmt, seed=31)
+    fw, fh = 32, 20
+    f_ab = rng.uniform(-4.0, 4.0, fw * fh * 2).astype(np.float32)
+    f_ba = rng.uniform(-4.0, 4.0, fw * fh * 2).astype(np.float32)
+    sel = tw.Selection(s0=np.float32(s0), s1=np.float32(s1), wa=np.float32(0.6), interp=1)
+    cs = tw.EngineSettings(warp_mode=code, blur=blur, quality_high=hiq, gouraud=code == 3)
+    got = dev.compose_vectors(cs, sel, a, b, w, h, fmt, f_ab, f_ba, (fw, fh))
+    want = O.compose_vectors3(a, b, w, h, fmt, f_ab, f_ba, fw, fh, sel, cs)
+    assert same(got, want)
+
+
+def test_device_powf_traced_vectors(dev):
+    """The Delinearize powf on the device equals the plugin runtime's traced values."""
+    v = np.array(golden_data.crt_powf_traced(), np.uint32)
+    got = dev.check_powf(v[:, 0].view(np.float32), v[:, 1].view(np.float32))
+    assert (got.view(np.uint32) == v[:, 2]).all()
+    rng = np.random.RandomState(5)
+    x = np.concatenate([rng.uniform(0, 4, 200000), rng.uniform(0.93, 1.07, 200000), [0.0, -0.0, np.inf, np.nan, 1e-40,
+                                                                                      3e38 / 255]]).astype(np.float32)
+    y = np.float32(1.0) / np.float32(2.2)
+    assert (dev.check_powf(x, y).view(np.uint32) == O.crt_powf(x, y).view(np.uint32)).all()
+
+
+@pytest.mark.parametrize("prep", [2, 3])
+@pytest.mark.parametrize("fmt", [0, 2])
+def test_prep_pyramids(dev, prep, fmt):
+    """Image prep on level 0 of the pyramid: Delinearize and Contrast / Edge Enhance at 320x180."""
+    w, h = 320, 180
+    a, b, _, _ = clip_pair(w, h, fmt, seed=37)
+    fs = tw.FlowSettings(prep_contrast_edge=prep == 2, prep_delinearize=prep == 3)
+    got = dev.build_pyramid(a, w, h, fmt, fs)
+    want = O.build_pyramid(a, w, h, fmt, prep=prep)
+    assert len(got) == len(want) and all(same(g, x) for g, x in zip(got, want))
 
 
 # ---- whole output frames -----------------------------------------------------------------------------
@@ -361,11 +424,7 @@ def test_retime_flow_grid_sha256(dev, case):
     kw = golden_data.case_params(case)
     tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], keys=kw["keys"], vectors=kw["vectors"],
                        frame_interp=kw["frame_interp"], blur_compensation=kw["blur"])
-    settings = tw.RetimeSettings(
-        flow=tw.FlowSettings(hiq=True, sensitivity=np.float32(np.float32(kw["sensitivity"]) / np.float32(100.0)),
-                             taps_above_first=False, video_range_luma=kw["video_360"]),
-        compose=tw.EngineSettings(warp_mode=kw["smart_blend"], video_360=kw["video_360"], taps_above_first=False),
-        motion_rows_reversed=False)
+    settings = grid_settings(kw)
     out = tw.retime_clip(dev, raw, case["frames"], case["width"], case["height"], fmt, tp, case["frames"], settings)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
 

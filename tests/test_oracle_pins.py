@@ -6,6 +6,10 @@
 * end to end: the sha256 of every served case of the reference's parity grid
   parity/retime-flow/results/base.grid.tsv (whole output clips of the `retime` effect: frame
   selection, pyramids, both solves with block matching, warps, blend, boundary conversions);
+* the motion blur of Blur Compensation against the reference's numpy model fixtures
+  (tests/fixtures/blur_cases.hex), bit for bit;
+* the Delinearize powf against the 72 arguments the reference traced from the plugin's C runtime
+  (crt_powf.rs tests) and its fall back cases;
 * the same for the layered path with plates: every served case of parity/fgbg-layers/results/base.tsv
   (retime-fgbg with 1 to 3 FG matte layers, recorded at the reference's current revision: rows
   reversed, taps above first).
@@ -219,3 +223,35 @@ def test_fgbg_layers_grid_sha256(case):
     mattes = [FG_INPUTS[m].view(O.DTYPE[fmt]) for m in case["mattes"]]
     out = O.retime_fgbg_clip(FG_INPUTS[case["input"]].view(O.DTYPE[fmt]), n, mattes, chans, sens, w, h, fmt, p, n)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
+
+
+def test_crt_powf_traced_vectors():
+    """The plugin runtime's powf of the Delinearize step, bit for bit on every traced argument."""
+    v = np.array(golden_data.crt_powf_traced(), np.uint32)
+    got = O.crt_powf(v[:, 0].view(np.float32), v[:, 1].view(np.float32))
+    assert (got.view(np.uint32) == v[:, 2]).all()
+
+
+def test_crt_powf_fall_back_cases():
+    """crt_powf.rs:229-232: outside the table path, the double precision pow narrowed to float."""
+    f = lambda x, y: float(O.crt_powf([x], [y])[0])  # noqa: E731
+    assert f(0.0, 0.5) == 0.0 and f(1.0, 0.45454544) == 1.0 and f(0.25, 1.0) == 0.25 and f(0.5, 0.0) == 1.0
+    assert np.isnan(f(-1.0, 0.5)) and np.isnan(f(np.nan, 2.0))
+    assert f(np.inf, 2.0) == np.inf and f(2.0, 200.0) == np.inf
+    y = np.float32(1.0) / np.float32(2.2)
+    x = (np.arange(1, 2000, dtype=np.float32) / np.float32(997.0)).astype(np.float32)
+    got = O.crt_powf(x, y).astype(np.float64)
+    want = np.power(x.astype(np.float64), np.float64(y))
+    assert (np.abs((got - want) / want) < 2.0e-7).all()
+
+
+BLUR = golden_data.blur_cases()
+
+
+@pytest.mark.parametrize("i", range(len(BLUR)))
+def test_motion_blur_model_fixtures(i):
+    """warp/blurcomp.rs motion_blur: bilinear and nearest taps, shutter offsets, every depth."""
+    c = BLUR[i]
+    out = O.motion_blur(c["src"], c["w"], c["h"], c["fmt"], c["flow"], c["fw"], c["fh"], c["amount"], c["hiq"],
+                        c["shutter"])
+    assert out.view(np.uint8).tobytes() == c["out"].view(np.uint8).tobytes()

@@ -298,6 +298,8 @@ def library():
     L.tw_vectors_pair.argtypes = [i32, i32, i32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     L.tw_create_vectors_clip.argtypes = [P, ctypes.POINTER(_VectorsSettings), P, i32, P, i32, i32, i32, i32, P]
     L.tw_check_logf.argtypes = [P, P, P, ctypes.c_int64]
+    L.tw_check_powf.argtypes = [P, P, P, P, ctypes.c_int64]
+    L.tw_motion_blur.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, ctypes.c_float]
     L.tw_fill_holes.argtypes = [P, pimg, P, i32, i32]
     L.tw_from_frame.argtypes = [P, P, i32, i32, i32, P]
     L.tw_to_frame.argtypes = [P, P, i32, i32, i32, P]
@@ -590,6 +592,25 @@ class Device:
         x = np.ascontiguousarray(x, np.float32)
         out = np.zeros_like(x)
         self._check(self._L.tw_check_logf(self._h, _ptr(x), _ptr(out), x.size))
+        return out
+
+    def motion_blur(self, src, width, height, fmt, flow, flow_size, amount, hiq, shutter):
+        """``warp::blurcomp::motion_blur`` of an engine image (the Blur Compensation primitive)."""
+        fw, fh = flow_size
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        si, sa = _img(src, width, height, fmt)
+        oi = _Image(width, height, fmt, out.ctypes.data)
+        fl = np.ascontiguousarray(flow, np.float32)
+        self._check(self._L.tw_motion_blur(self._h, ctypes.byref(oi), ctypes.byref(si), ctypes.byref(_Flow(fw, fh, fl.ctypes.data)),
+                                           np.float32(amount), int(hiq), np.float32(shutter)))
+        return out
+
+    def check_powf(self, x, y):
+        """The device's powf of the Delinearize prep (the plugin runtime's, crt_powf.rs)."""
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(np.broadcast_to(np.asarray(y, np.float32), x.shape), np.float32)
+        out = np.zeros_like(x)
+        self._check(self._L.tw_check_powf(self._h, _ptr(x), _ptr(y), _ptr(out), x.size))
         return out
 
     def smart_blend(self, p1, p2, width, height, fmt, w, binary=False):

@@ -247,4 +247,24 @@ __global__ void k_wb_noflow_f32(const float* __restrict__ a, const float* __rest
                                 const float* __restrict__ b1, const int* __restrict__ unsound, float w, float wl, int mode,
                                 float* __restrict__ out, long n);
 
+// ---- the image prep (prep.cu, prep.rs) ----
+__device__ float crt_powf(float x, float y);
+__global__ void k_delinearize(float* __restrict__ p, long n);
+__global__ void k_edge_map(const float* __restrict__ src, float* __restrict__ dst, int w, int h);
+__global__ void k_check_powf(const float* __restrict__ x, const float* __restrict__ y, float* __restrict__ out, long n);
+
+// ---- Blur Compensation (filters.cu, warp/blurcomp.rs) ----
+struct MotionBlur {
+    const void* src;
+    void* dst;
+    WarpParams flow;  // the flow field of the blur (fu, fv, fstride, fw, fh)
+    int fmt, w, h;
+    float rx, ry, kx, ky, k;
+    bool shifted, bilinear;
+    int post;        // 0 none, 1 clear the colour of transparent pixels, 2 lerp(dst, src, lerp_w)
+    float lerp_w;
+    int* bad;        // bit 2: a NaN tap or a vector of more than 65536 taps
+};
+__global__ void k_motion_blur(MotionBlur B);
+
 }  // namespace tw

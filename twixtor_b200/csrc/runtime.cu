@@ -175,6 +175,7 @@ struct Lane {
     DevBuf eng[2], pyr[2], work[2], flow[2], scratch[2][3], flags;
     DevBuf comp, holes, fill;  // warping code 1: the composite, its holes mask, the fill's planes
     DevBuf wb_wt[2], wb_tmp[2], wb_mask[2], wb_cov[2];  // Weighted Blend: warped frames, blur planes, masks, coverage
+    DevBuf pre_blur;  // Blur Compensation: the composite before the motion blur
 };
 constexpr int MAX_LANES = 8;
 
@@ -199,13 +200,14 @@ struct tw_ctx {
     std::string err;
     uint64_t launches = 0;
     size_t held = 0;
-    Taps g7{}, g5{}, b5{};
+    Taps g7{}, g5{}, b5{}, g2{};
     // engine images, wire staging, pyramids, solve work, flows
     DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags, holes, fill, masks;
     DevBuf lay_mem;  // the layered path: planes, layer images, plates, flows
     DevBuf lay_in;   // the layered path: the raw mattes at A and B
     DevBuf fc_img[2], fc_cov[2];  // the forward compositions: the two pushed frames and their coverage
     DevBuf wb_wt[2], wb_tmp[2], wb_mask[2], wb_cov[2];  // Weighted Blend (the calls on the context's stream)
+    DevBuf pre_blur, comp_e;  // Blur Compensation: the composite before the blur, the engine result
     DevBuf host_stage;  // unused placeholder for pinned staging
     std::vector<cudaEvent_t> ev_pool;  // the profiler's events (KernelProfile)
     // the forward warp: vertices, mip pyramid, per pixel counts / offsets, hit lists, flags
@@ -312,8 +314,6 @@ static int level_threads(int w, int h) {
 
 int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, const tw_flow_settings& s, const Geo& g,
                       float* out, float* out_t, DevBuf* scratch) {
-    if (s.prep_contrast_edge || s.prep_delinearize)
-        return ctx->fail(TW_ERR_UNSUPPORTED, "image prep (Contrast/Edge Enhance, Delinearize) is not on the device");
     if (s.video_range_luma && s.track_alpha)
         return ctx->fail(TW_ERR_UNSUPPORTED, "optical flow luma: video range conversion together with Track RGB+A is not supported");
     int lmode = (s.track_alpha ? LUMA_TRACK_ALPHA : 0) | (s.video_range_luma ? LUMA_VIDEO_RANGE : 0);
@@ -337,6 +337,13 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
         std::swap(cur, nxt);
         cw = nw;
         ch = nh;
+    }
+    // flow.rs:248-253: the image prep of level 0, Delinearize then Contrast / Edge Enhance
+    if (s.prep_delinearize) LAUNCH(ctx, k_delinearize, grid1((long)cw * ch), TB, 0, cur, (long)cw * ch);
+    if (s.prep_contrast_edge) {
+        conv_planes(ctx, &cur, 1, cw, ch, ctx->g2, af, tmp);  // prep.rs:329, the Gaussian of radius 2.0
+        LAUNCH(ctx, k_edge_map, grid1((long)cw * ch), TB, 0, cur, nxt, cw, ch);
+        std::swap(cur, nxt);
     }
     size_t off = 0;
     size_t pf = pyramid_floats(g);
@@ -820,7 +827,53 @@ struct SmartScratch {
     int* side1;     // set when an image with a side of 1 pixel has a hole (the fill refuses it)
     const WbScratch* wb = nullptr;  // Weighted Blend scratch (nullptr: Weighted Blend refused)
     int* wb_gate = nullptr;         // the unsound float flag of the Weighted Blend without flows
+    DevBuf* blur = nullptr;         // Blur Compensation: the composite before the blur (nullptr: refused)
 };
+
+// warp/blurcomp.rs:42-130 (blur_compensation with is360 off): the amount from the two source
+// positions and the slider, clamped; the motion blur of img (engine image) into dst with the post
+// step of its sign. Returns TW_OK with *ran false when the compensation does nothing (dst untouched).
+int blur_comp_dev(tw_ctx* ctx, const void* img, void* dst, const float* flow, int fw, int fh, float s0, float s1,
+                  float blur, bool hiq, int W, int H, int fmt, int* bad, bool* ran) {
+    *ran = false;
+    float a = std::fabs(s0 - s1);
+    if (!((double)a > 1e-6) || !((double)blur > 0.005)) return TW_OK;
+    float amount = (a - 1.0f) * blur;
+    if (20.0f < amount) amount = 20.0f;
+    else if (amount < -10.0f) amount = -10.0f;
+    if ((double)std::fabs(amount) < 1e-6) return TW_OK;
+    if (W < 2 || H < 2 || fw < 2 || fh < 2)
+        return ctx->fail(TW_ERR_MISMATCH, "motion blur needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W, H, fw, fh);
+    MotionBlur B{};
+    B.src = img;
+    B.dst = dst;
+    B.flow = warp_params(img, flow, fw, fh, 0.0f, W, true);
+    B.fmt = fmt;
+    B.w = W;
+    B.h = H;
+    B.rx = (float)(fw - 1) / (float)(W - 1);
+    B.ry = (float)(fh - 1) / (float)(H - 1);
+    float eff = 0.0f < amount ? amount : 0.5f;  // a negative amount blurs by 0.5 and lerps
+    B.kx = (0.5f / B.rx) * eff;
+    B.ky = (0.5f / B.ry) * eff;
+    B.shifted = false;  // shutter 0.5
+    B.k = 0.5f * 2.0f - 1.0f;
+    B.bilinear = hiq;
+    B.post = 0.0f < amount ? 1 : 2;
+    B.lerp_w = amount;
+    B.bad = bad;
+    LAUNCH(ctx, k_motion_blur, grid1((long)W * H), TB, 0, B);
+    *ran = true;
+    return TW_OK;
+}
+
+// The refusal a composition's bad flag carries: bit 2 the motion blur, else the inverse warp.
+int bad_fail(tw_ctx* ctx, int v) {
+    if (v & 2)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "motion blur: a tap coordinate is NaN or a vector needs more than 65536 taps, "
+                                             "which is not supported");
+    return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+}
 
 WbScratch wb_scratch(DevBuf* wt, DevBuf* tmp, DevBuf* mask, DevBuf* cov) {
     return WbScratch{{&wt[0], &wt[1]}, {&tmp[0], &tmp[1]}, {&mask[0], &mask[1]}, {&cov[0], &cov[1]}};
@@ -987,10 +1040,38 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
                 void* out, bool to_wire, bool flip_out, int* bad, const SmartScratch* ss) {
     if (cs.warp_mode < 0 || cs.warp_mode > 3) return ctx->fail(TW_ERR_BAD_PARAM, "warping code %d is not 0 to 3", cs.warp_mode);
     if (cs.wrap_360) return ctx->fail(TW_ERR_UNSUPPORTED, "the 360 inverse warp is not on the device");
-    // blur compensation (warp/blurcomp.rs:33-40): runs only when |s0 - s1| > 1e-6 and blur > 0.005
+    // the Blur Compensation tail (compose/vector.rs:276-281, warp/blurcomp.rs:42-48): when
+    // |s0 - s1| > 1e-6 and the slider > 0.005, the composition goes to an engine image first and
+    // the motion blur along F_AB (else the single flow) writes the output
     float d = std::fabs(sel.s0 - sel.s1);
-    if ((double)d > 1e-6 && (double)cs.blur > 0.005)
-        return ctx->fail(TW_ERR_UNSUPPORTED, "blur compensation is not on the device yet");
+    const float* bflow = f_ab ? f_ab : f_ba;
+    if ((double)d > 1e-6 && (double)cs.blur > 0.005 && bflow) {
+        if (!ss || !ss->blur || (to_wire && !ss->comp))
+            return ctx->fail(TW_ERR_UNSUPPORTED, "Blur Compensation needs its scratch");
+        size_t ib = (size_t)W * H * 4 * sample_bytes(fmt);
+        CHECK(ctx->ensure(*ss->blur, ib, "composite before the blur"));
+        tw_engine_settings c2 = cs;
+        c2.blur = 0.0f;
+        void* pre = ss->blur->p;
+        CHECK(compose_dev(ctx, c2, sel, eng_a, eng_b, f_ab, f_ba, fw, fh, W, H, fmt, pre, false, false, bad, ss));
+        void* post = out;
+        if (to_wire) {
+            CHECK(ctx->ensure(*ss->comp, ib, "composite"));
+            post = ss->comp->p;
+        }
+        bool ran = false;
+        CHECK(blur_comp_dev(ctx, pre, post, bflow, fw, fh, sel.s0, sel.s1, cs.blur, cs.quality_high != 0, W, H, fmt, bad, &ran));
+        const void* res = ran ? post : pre;
+        long n = (long)W * H;
+        if (to_wire) {
+            if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)res, (uint8_t*)out, W, H, flip_out);
+            else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)res, (uint16_t*)out, W, H, flip_out);
+            else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)res, (float*)out, W, H, flip_out);
+        } else if (!ran) {
+            CHECK(ctx->cuda(cudaMemcpyAsync(out, pre, ib, cudaMemcpyDeviceToDevice, ctx->cur), "copy"));
+        }
+        return TW_OK;
+    }
     if (cs.warp_mode >= 2) {
         if (to_wire)
             return ctx->fail(TW_ERR_UNSUPPORTED, "the forward warps compose on the context's stream only (tw_compose_vectors, "
@@ -1198,6 +1279,7 @@ int tw_open(int device, tw_ctx** out) {
     if (cudaEventCreateWithFlags(&ctx->ev_start, cudaEventDisableTiming) != cudaSuccess) { tw_close(ctx); return TW_ERR_CUDA; }
     ctx->g7 = gaussian_taps(7.0f);
     ctx->g5 = gaussian_taps(5.0f);
+    ctx->g2 = gaussian_taps(2.0f);
     ctx->b5 = binomial5();
     // block matching keeps one line of the field in shared memory (up to BM_MAX_LINE elements)
     e = cudaFuncSetAttribute(k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(BM_MAX_LINE));
@@ -1223,7 +1305,7 @@ void tw_close(tw_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     for (auto* b : {&ctx->flags, &ctx->host_stage, &ctx->holes, &ctx->fill, &ctx->masks, &ctx->lay_mem, &ctx->lay_in, &ctx->fc_img[0], &ctx->fc_img[1], &ctx->fc_cov[0], &ctx->fc_cov[1], &ctx->wb_wt[0], &ctx->wb_wt[1],
-                    &ctx->wb_tmp[0], &ctx->wb_tmp[1], &ctx->wb_mask[0], &ctx->wb_mask[1], &ctx->wb_cov[0], &ctx->wb_cov[1], &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
+                    &ctx->wb_tmp[0], &ctx->wb_tmp[1], &ctx->wb_mask[0], &ctx->wb_mask[1], &ctx->wb_cov[0], &ctx->wb_cov[1], &ctx->pre_blur, &ctx->comp_e, &ctx->logf_tab, &ctx->fw_vx, &ctx->fw_vy,
                     &ctx->fw_vd, &ctx->fw_pyr, &ctx->fw_tmp[0], &ctx->fw_tmp[1], &ctx->fw_cnt, &ctx->fw_off,
                     &ctx->fw_fill, &ctx->fw_sums, &ctx->fw_keys, &ctx->fw_cols, &ctx->fw_scratch, &ctx->fw_longq,
                     &ctx->fw_flags, &ctx->fw_cov})
@@ -1238,6 +1320,7 @@ void tw_close(tw_ctx* ctx) {
             for (int j = 0; j < 3; j++) L.scratch[i][j].release(&ctx->held);
             if (i == 0) { L.comp.release(&ctx->held); L.holes.release(&ctx->held); L.fill.release(&ctx->held); }
             for (DevBuf* b : {&L.wb_wt[i], &L.wb_tmp[i], &L.wb_mask[i], &L.wb_cov[i]}) b->release(&ctx->held);
+            if (i == 0) L.pre_blur.release(&ctx->held);
             if (L.s[i]) cudaStreamDestroy(L.s[i]);
             if (L.ev_pyr[i]) cudaEventDestroy(L.ev_pyr[i]);
         }
@@ -1563,14 +1646,14 @@ int tw_compose_vectors(tw_ctx* ctx, const tw_engine_settings* settings, const tw
     int* flags = ctx->flags.as<int>();
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
     WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
-    SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
+    SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB, &ctx->pre_blur};
     CHECK(compose_dev(ctx, *settings, *sel, ctx->eng[0].p, ctx->eng[1].p, f_ab ? ctx->flow[0].as<float>() : nullptr,
                       f_ba ? ctx->flow[1].as<float>() : nullptr, fw, fh, a->width, a->height, a->fmt, ctx->eng[2].p,
                       false, false, flags + FL_BAD, &ss));
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     int hf[4];
     CHECK(finish(ctx, hf, 4));
-    if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    if (hf[1]) return bad_fail(ctx, hf[1]);
     if (hf[3])
         return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of a %dx%d image: the pyramid resample divides by zero for a side of 1",
                          a->width, a->height);
@@ -1633,7 +1716,7 @@ int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_fl
     if (cov) CHECK(ctx->cuda(cudaMemcpyAsync(cov, dcov, (size_t)W * H, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     int hf[2];
     CHECK(finish(ctx, hf, 2));
-    if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    if (hf[1]) return bad_fail(ctx, hf[1]);
     return TW_OK;
 }
 
@@ -1733,7 +1816,7 @@ static int layers_status(tw_ctx* ctx) {
     int hf[4];
     CHECK(finish(ctx, hf, 4));
     if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
-    if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    if (hf[1]) return bad_fail(ctx, hf[1]);
     if (hf[3]) return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of an image with a side of 1 pixel that has a hole");
     return TW_OK;
 }
@@ -1824,7 +1907,7 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     }
     // the composition, bottom layer first (plates.rs:373-412)
     WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
-    SmartScratch ss{nullptr, &ctx->fill, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
+    SmartScratch ss{nullptr, &ctx->fill, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB, &ctx->pre_blur};
     DevBuf& fillbuf = ctx->work[1];
     ss.holes = &ctx->masks;  // the composition's own holes mask (the refill uses ctx->holes)
     auto refill = [&](void* p, int side, int k) -> int {
@@ -1930,6 +2013,67 @@ int tw_forward_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const t
                            pyramid != 0, ctx->eng[1].p, ctx->fw_cov.as<uint8_t>()));
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[1].p, ib, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     if (cov) CHECK(ctx->cuda(cudaMemcpyAsync(cov, ctx->fw_cov.p, (size_t)n, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    return ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution");
+}
+
+int tw_motion_blur(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_flow* flow, float amount,
+                   int32_t hiq, float shutter) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    CHECK(check_image(ctx, src, "motion blur"));
+    if (!out || !out->data || !flow || !flow->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    if (out->width != src->width || out->height != src->height || out->fmt != src->fmt)
+        return ctx->fail(TW_ERR_MISMATCH, "motion blur: destination and source differ in shape");
+    int W = src->width, H = src->height, fmt = src->fmt;
+    if (W < 2 || H < 2 || flow->width < 2 || flow->height < 2)
+        return ctx->fail(TW_ERR_MISMATCH, "motion blur needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W, H,
+                         flow->width, flow->height);
+    size_t ib = (size_t)W * H * 4 * sample_bytes(fmt), fb = (size_t)flow->width * flow->height * 2 * sizeof(float);
+    CHECK(upload_image(ctx, ctx->eng[0], src));
+    CHECK(ctx->ensure(ctx->eng[1], ib, "motion blur output"));
+    CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->flow[0].p, flow->data, fb, cudaMemcpyHostToDevice, ctx->stream), "flow upload"));
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
+    MotionBlur B{};
+    B.src = ctx->eng[0].p;
+    B.dst = ctx->eng[1].p;
+    B.flow = warp_params(ctx->eng[0].p, ctx->flow[0].as<float>(), flow->width, flow->height, 0.0f, W, true);
+    B.fmt = fmt;
+    B.w = W;
+    B.h = H;
+    B.rx = (float)(flow->width - 1) / (float)(W - 1);
+    B.ry = (float)(flow->height - 1) / (float)(H - 1);
+    B.kx = (0.5f / B.rx) * amount;
+    B.ky = (0.5f / B.ry) * amount;
+    B.shifted = shutter != 0.5f;
+    B.k = shutter * 2.0f - 1.0f;
+    B.bilinear = hiq != 0;
+    B.bad = flags + FL_BAD;
+    LAUNCH(ctx, k_motion_blur, grid1((long)W * H), TB, 0, B);
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[1].p, ib, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    int hf[2];
+    CHECK(finish(ctx, hf, 2));
+    if (hf[1]) return bad_fail(ctx, hf[1]);
+    return TW_OK;
+}
+
+int tw_check_powf(tw_ctx* ctx, const float* x, const float* y, float* out, int64_t n) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!x || !y || !out || n < 0) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    if (n == 0) return TW_OK;
+    size_t b = (size_t)n * sizeof(float);
+    CHECK(ctx->ensure(ctx->plane[0], b, "powf input"));
+    CHECK(ctx->ensure(ctx->plane[1], b, "powf input"));
+    CHECK(ctx->ensure(ctx->plane[2], b, "powf output"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->plane[0].p, x, b, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->plane[1].p, y, b, cudaMemcpyHostToDevice, ctx->stream), "upload"));
+    LAUNCH(ctx, k_check_powf, grid1(n), TB, 0, ctx->plane[0].as<float>(), ctx->plane[1].as<float>(), ctx->plane[2].as<float>(),
+           (long)n);
+    CHECK(ctx->cuda(cudaMemcpyAsync(out, ctx->plane[2].p, b, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     return ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution");
 }
 
@@ -2083,7 +2227,7 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
     CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_solve1, 0), "event"));
     ctx->cur = L.s[0];
     WbScratch wbs = wb_scratch(L.wb_wt, L.wb_tmp, L.wb_mask, L.wb_cov);
-    SmartScratch ss{&L.comp, &L.holes, &L.fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
+    SmartScratch ss{&L.comp, &L.holes, &L.fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB, &L.pre_blur};
     CHECK(compose_dev(ctx, s.compose, sel, L.eng[0].p, L.eng[1].p, need_ab ? L.flow[0].as<float>() : nullptr,
                       need_ba ? L.flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, out_wire, true, flip,
                       flags + FL_BAD, &ss));
@@ -2185,7 +2329,7 @@ static int lanes_end(tw_ctx* ctx, int nl) {
     }
     CHECK(ctx->cuda(cudaGetLastError(), "kernel execution"));
     if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
-    if (hf[1]) return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
+    if (hf[1]) return bad_fail(ctx, hf[1]);
     if (hf[3]) return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of an image with a side of 1 pixel that has a hole");
     return TW_OK;
 }
@@ -2358,7 +2502,7 @@ static int vector_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_s
         CHECK(solve_pyramids_dev(ctx, py_, px_, py_ + pf, px_ + pf, g, fs, ctx->work[1], ctx->flow[1].as<float>(),
                                  flags + FL_ANY1, flags + FL_NAN));
     WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
-    SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
+    SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB, &ctx->pre_blur};
     return compose_dev(ctx, s.compose, sel, ctx->eng[0].p, ctx->eng[1].p, need_ab ? ctx->flow[0].as<float>() : nullptr,
                        need_ba ? ctx->flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, res, false, false, flags + FL_BAD,
                        &ss);
