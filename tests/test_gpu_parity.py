@@ -467,7 +467,7 @@ def test_unsupported_settings_fail_loudly(dev):
     w, h = 32, 24
     a, b, _, _ = clip_pair(w, h, 0, seed=1)
     with pytest.raises(tw.Unsupported):
-        dev.solve_pair(a, b, w, h, 0, tw.FlowSettings(prep_contrast_edge=True))
+        dev.solve_pair(a, b, w, h, 0, tw.FlowSettings(wrap=True))  # the wrap-around (360) solve
     with pytest.raises(tw.BadParam):
         dev.solve_pair(a, b, w, h, 0, tw.FlowSettings(quality=0))
     # the forward compositions read counts back: not on the lanes of the clip calls
