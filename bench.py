@@ -16,6 +16,11 @@ the reference CPU path.
 * ``cpu_baseline``: the CPU oracle (the reference CPU path restated in C++, OpenMP over all host
   cores) on a bounded sample of the same workload.
 
+``--workload create-vectors`` and ``--workload fgbg`` measure the other two single-GPU
+configurations the same way through their host-buffer C ABI calls (tw_create_vectors_clip on a
+1920x1080 16 bpc clip under random affine motion; tw_retime_layers_clip on a 1920x1080 8 bpc clip
+with three FG matte layers at speed 40 %), with the oracle beside them on a small sample.
+
 ``--impl reference`` times the reference's CPU path the same way (the oracle port: the reference
 is Rust and no Rust toolchain exists on these machines). Under torchrun every rank renders its own
 clip (weak scaling, no collective on the data path).
@@ -213,6 +218,95 @@ def ncu_case():
     return 0
 
 
+def _timed(stream, fn, k, flush):
+    import torch
+    flush.fill_(k & 0xff)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn(k)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_workload(args):
+    """The create-vectors (1080p 16 bpc, frame pairs n -> n - 1) and retime-fgbg (1080p 8 bpc, three
+    FG layers, speed 40 %) configurations through their host-buffer clip calls, one GPU."""
+    import torch
+    import twixtor_b200 as tw
+    from twixtor_b200 import synth
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    dev = tw.Device(0)
+    dev.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda:0")
+    steps, warmup = args.steps, args.warmup
+    if args.workload == "create-vectors":
+        per, nsrc, fmt = 8, 24, 1
+        frames = synth.affine_clip(W, H, nsrc, depth=16)
+        pinned = torch.from_numpy(frames).pin_memory().numpy()
+        vs = tw.vectors_settings()
+        pairs = [(1 + (n % (nsrc - 1)), n % (nsrc - 1)) for n in range((warmup + steps) * per)]
+        out = torch.empty(per * W * H * 4, dtype=torch.int16).pin_memory().numpy().view(np.uint16)
+
+        def step(k):
+            dev.create_vectors_clip(vs, pinned, nsrc, pairs[k * per:(k + 1) * per], W, H, fmt, out=out)
+        metric = "1080p create-vectors output frames/s (strict byte-exact GPU vs CPU)"
+        workload = "create-vectors 1920x1080 16bpc RGBA, pairs n -> n-1 under random affine motion, defaults (half res)"
+        h2d = per * 2 * W * H * 8
+    else:
+        per, fmt, nfg = 5, 0, 3
+        nsrc = int(math.ceil(SPEED / 100.0 * (warmup + steps) * per)) + 2
+        frames, mattes = synth.layered_clip(W, H, nsrc, nfg=nfg)
+        pin = [torch.from_numpy(x).pin_memory().numpy() for x in [frames] + mattes]
+        tp = tw.TimeParams(speed_percent=SPEED)
+        sels = [tw.select(tp, n, W, H) for n in range((warmup + steps) * per)]
+        settings = tw.RetimeSettings(compose=tw.EngineSettings(gouraud=True))
+        sens = [tw.percent_param(70.0)] * (nfg + 1)
+        out = torch.empty(per * W * H * 4, dtype=torch.uint8).pin_memory().numpy()
+
+        def step(k):
+            dev.retime_layers_clip(settings, pin[0], nsrc, pin[1:], [1] * nfg, sens, sels[k * per:(k + 1) * per], W, H,
+                                   fmt, out=out)
+        metric = "1080p retime-fgbg output frames/s, 3 FG layers (strict byte-exact GPU vs CPU)"
+        workload = "retime-fgbg 1920x1080 8bpc RGBA, 3 FG matte layers (binary ellipses, red channel), speed 40%"
+        h2d = per * 2 * (nfg + 1) * W * H * 4
+    for k in range(warmup):
+        step(k)
+    torch.cuda.synchronize()
+    with Clocks(0) as clk:
+        times = [_timed(stream, step, k, flush) for k in range(warmup, warmup + steps)]
+    total_ms = sum(times)
+    value = steps * per / (total_ms / 1e3)
+    line = {"metric": metric, "value": value, "unit": "frames/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
+            "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload, "output_frames_per_step": per,
+                       "timing": "host buffers through the C ABI clip call (uploads and downloads inside)",
+                       "l2": "flushed between steps (256 MiB write)"},
+            "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": per * W * H * 4 * (2 if fmt == 1 else 1)},
+            "gpu_launches": dev.stats()["kernel_launches"], "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        import oracle_lib as O
+        threads = os.cpu_count() or 1
+        O.lib().or_set_threads(threads)
+        t = time.perf_counter()
+        if args.workload == "create-vectors":
+            O.create_vectors_clip(frames, 3, W, H, fmt, 2)
+            n = 2
+        else:
+            O.retime_fgbg_clip(frames, nsrc, mattes, [1] * nfg, [70.0] * nfg, W, H, fmt, O.retime_params(speed=SPEED), 2)
+            n = 2
+        dt = time.perf_counter() - t
+        line["cpu_baseline"] = {"value": n / dt, "unit": "frames/s", "cores": threads, "kind": "port",
+                                "sample": f"{n} output frame(s) of the same clip, {dt:.2f} s on {threads} OpenMP threads"}
+    emit(line)
+    dev.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -226,11 +320,15 @@ def main():
     ap.add_argument("--breakdown", action="store_true",
                     help="after the timed region, time one more step with every kernel bracketed by events and "
                          "print the per-kernel table to stderr (not part of the reported numbers)")
+    ap.add_argument("--workload", default="retime", choices=["retime", "create-vectors", "fgbg"],
+                    help="retime (the headline, default), create-vectors (1080p 16 bpc) or fgbg (1080p, 3 FG layers)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "retime":
+        return run_workload(args)
     if args.ncu_case:
         return ncu_case()
 

@@ -184,3 +184,17 @@ def test_fgbg_clip_without_layers_forward_codes(dev, code):
     p = O.retime_params(speed=50.0, smart_blend=code, sensitivity=70.0)
     want = O.retime_fgbg_clip(frames, n, [], [], [], w, h, fmt, p, nout)
     assert same(got, want)
+
+
+def test_fgbg_1080p_frame_matches_oracle(dev):
+    """One in-between frame of the 1080p retime-fgbg workload (three FG matte layers, speed 40 %)."""
+    w, h, n = 1920, 1080, 3
+    frames, mattes = synth.layered_clip(w, h, n, nfg=3)
+    tp = tw.TimeParams(speed_percent=40.0)
+    sels = [tw.select(tp, k, w, h) for k in range(2)]
+    assert not sels[1].exact
+    s = tw.RetimeSettings(compose=tw.EngineSettings(gouraud=True))
+    sens = [tw.percent_param(70.0)] * 4
+    got = dev.retime_layers_clip(s, frames, n, mattes, [1, 1, 1], sens, sels, w, h, 0)
+    want = O.retime_fgbg_clip(frames, n, mattes, [1, 1, 1], [70.0] * 3, w, h, 0, O.retime_params(speed=40.0), 2)
+    assert same(got, want)

@@ -106,3 +106,82 @@ def moving_clip(width, height, frames, depth=8, seed=0x74570001, bg_velocity=(1.
         a = np.ones((height, width)) if alpha is None else alpha(X, Y, t)
         out.append(_to_wire(rgb, a, depth))
     return np.concatenate(out)
+
+
+def _bilinear(img, X, Y):
+    """Bilinear sample of a 2D array at float coordinates, clamped at the edges."""
+    h, w = img.shape
+    X = np.clip(X, 0.0, w - 1.001)
+    Y = np.clip(Y, 0.0, h - 1.001)
+    ix, iy = np.floor(X).astype(np.int64), np.floor(Y).astype(np.int64)
+    fx, fy = X - ix, Y - iy
+    a = img[iy, ix] * (1 - fx) + img[iy, ix + 1] * fx
+    b = img[iy + 1, ix] * (1 - fx) + img[iy + 1, ix + 1] * fx
+    return a * (1 - fy) + b * fy
+
+
+def affine_clip(width, height, frames, depth=16, seed=0x74570002):
+    """The Create Vectors workload: a seeded value noise texture (uniform octave amplitudes) under a
+    random affine motion from each frame to the next (translation U[-16, 16] px, rotation U[-3, 3]
+    degrees, scale U[0.97, 1.03] about the centre), opaque, as wire frames back to back."""
+    rng = np.random.RandomState(seed)
+    pad = 96
+    tw_, th_ = width + 2 * pad, height + 2 * pad
+    tex = 0.0
+    for cell in (32, 12, 5):
+        lat, c = _lattice_noise(rng, tw_, th_, cell)
+        X, Y = np.meshgrid(np.arange(tw_, dtype=np.float64), np.arange(th_, dtype=np.float64))
+        tex = tex + _sample(lat, c, X, Y)
+    tex = 128.0 + 40.0 * (tex - tex.mean()) / (tex.std() or 1.0)
+    X, Y = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64))
+    cx, cy = width / 2.0, height / 2.0
+    m = np.eye(3)  # the cumulative map from frame coordinates to texture coordinates
+    out = []
+    for t in range(frames):
+        if t:
+            ang = np.deg2rad(rng.uniform(-3.0, 3.0))
+            s = rng.uniform(0.97, 1.03)
+            tx, ty = rng.uniform(-16.0, 16.0, 2)
+            c, sn = np.cos(ang) * s, np.sin(ang) * s
+            step = np.array([[c, -sn, cx - c * cx + sn * cy + tx], [sn, c, cy - sn * cx - c * cy + ty], [0, 0, 1]])
+            m = m @ step
+        U = m[0, 0] * X + m[0, 1] * Y + m[0, 2] + pad
+        V = m[1, 0] * X + m[1, 1] * Y + m[1, 2] + pad
+        g = _bilinear(tex, U, V)
+        rgb = np.stack([g, 0.9 * g + 12.0, 1.05 * g - 6.0], -1)
+        out.append(_to_wire(rgb, np.ones((height, width)), depth))
+    return np.concatenate(out)
+
+
+def layered_clip(width, height, frames, nfg=3, depth=8, seed=0x74570004, bg_velocity=(3.0, 0.0)):
+    """The retime-fgbg workload: a noise background translating by ``bg_velocity`` px/frame and ``nfg``
+    textured ellipses (semi-axes 80 to 300 px) each moving on its own at up to 12 px/frame, FG1 on
+    top. Returns (footage, [matte clips]): each matte clip holds its layer's binary ellipse in the
+    red channel (the FG matte channel popup's default), white elsewhere in alpha."""
+    rng = np.random.RandomState(seed)
+    base = moving_clip(width, height, frames, depth=8, seed=seed, bg_velocity=bg_velocity, square=0)
+    base = base.reshape(frames, height, width, 4).astype(np.float64)
+    X, Y = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64))
+    layers = []
+    for k in range(nfg):
+        ax, ay = rng.uniform(80.0, 300.0, 2) * min(1.0, width / 1920.0)
+        cx, cy = rng.uniform(0.25, 0.75) * width, rng.uniform(0.25, 0.75) * height
+        speed, ang = rng.uniform(4.0, 12.0), rng.uniform(0, 2 * np.pi)
+        vx, vy = speed * np.cos(ang), speed * np.sin(ang)
+        tex = NoiseField(seed + 17 * (k + 1), width, height)
+        layers.append((ax, ay, cx, cy, vx, vy, tex, 60.0 + 50.0 * k))
+    foot, mattes = [], [[] for _ in range(nfg)]
+    for t in range(frames):
+        rgb = base[t, ..., :3].copy()
+        for k in reversed(range(nfg)):  # bottom layer first, FG1 last (on top)
+            ax, ay, cx, cy, vx, vy, tex, tint = layers[k]
+            px, py = cx + vx * t, cy + vy * t
+            inside = ((X - px) / ax) ** 2 + ((Y - py) / ay) ** 2 <= 1.0
+            g = tex.at(X - vx * t, Y - vy * t)
+            fg = np.stack([g, 0.5 * g + tint, 0.8 * g + 30.0], -1)
+            rgb = np.where(inside[..., None], fg, rgb)
+            m = np.zeros((height, width, 3))
+            m[..., 0] = inside * 255.0
+            mattes[k].append(_to_wire(m, np.ones((height, width)), depth))
+        foot.append(_to_wire(rgb, np.ones((height, width)), depth))
+    return np.concatenate(foot), [np.concatenate(m) for m in mattes]
