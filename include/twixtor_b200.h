@@ -266,6 +266,22 @@ int tw_forward_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const t
 int tw_motion_blur(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_flow* flow, float amount,
                    int32_t hiq, float shutter);
 
+/* The adjoint of warp + blend (no reference counterpart: the differentiable twin of compose_vectors'
+ * Blend with warping code 0, for photometric flow refinement). Forward: out = ta + (tb - ta) * w,
+ * w = 1 - wa, ta = warp(a, f_ba, 1 - wa), tb = warp(b, f_ab, wa), warp(S, F, s)(p) = S sampled
+ * bilinearly at p + F(p r) s / r (F sampled bilinearly at p r, r = (flow size - 1) / (image size -
+ * 1) per axis, as warp.rs:693-786), the position clamped to the image. Backward: from grad_out
+ * (d loss / d out), or with target != NULL from the L1 loss sum |out - target| (its sum per batch
+ * item added to loss[i]); the gradients are ADDED into da, db (w x h x 4), df_ab, df_ba (flow_w x
+ * flow_h x 2), each NULL when not wanted; the forward output goes to out (NULL: not written).
+ * All pointers are DEVICE pointers to float RGBA frames and interleaved flows, batch items back
+ * to back. The work is enqueued on the context's stream and the call returns without waiting;
+ * nothing of the forward pass is stored (the backward recomputes the samples). */
+int tw_warp_blend_adjoint(tw_ctx* ctx, const float* a, const float* b, const float* f_ab, const float* f_ba,
+                          int32_t width, int32_t height, int32_t flow_w, int32_t flow_h, int32_t batch, float wa,
+                          const float* target, const float* grad_out, float* out, float* loss, float* da, float* db,
+                          float* df_ab, float* df_ba);
+
 /* The powf of the plugin's C runtime that the Delinearize prep calls (crt_powf.rs:229-268), over
  * n argument pairs: a check hook for the runtime's traced values, as tw_check_logf is for logf.
  * Bit exact on the prep's arguments (a base >= 0 or NaN, the exponent 1 / 2.2); a negative base

@@ -300,6 +300,7 @@ def library():
     L.tw_check_logf.argtypes = [P, P, P, ctypes.c_int64]
     L.tw_check_powf.argtypes = [P, P, P, P, ctypes.c_int64]
     L.tw_motion_blur.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, ctypes.c_float]
+    L.tw_warp_blend_adjoint.argtypes = [P, P, P, P, P, i32, i32, i32, i32, i32, ctypes.c_float, P, P, P, P, P, P, P, P]
     L.tw_fill_holes.argtypes = [P, pimg, P, i32, i32]
     L.tw_from_frame.argtypes = [P, P, i32, i32, i32, P]
     L.tw_to_frame.argtypes = [P, P, i32, i32, i32, P]
@@ -604,6 +605,17 @@ class Device:
         self._check(self._L.tw_motion_blur(self._h, ctypes.byref(oi), ctypes.byref(si), ctypes.byref(_Flow(fw, fh, fl.ctypes.data)),
                                            np.float32(amount), int(hiq), np.float32(shutter)))
         return out
+
+    def warp_blend_adjoint(self, a, b, f_ab, f_ba, width, height, flow_w, flow_h, batch, wa, target=0, grad_out=0,
+                           out=0, loss=0, da=0, db=0, df_ab=0, df_ba=0):
+        """tw_warp_blend_adjoint on DEVICE pointers (ints, e.g. tensor.data_ptr(); 0 for none): the
+        forward of warp + blend and, from the L1 loss against ``target`` or from ``grad_out``, the
+        gradients added into ``da``, ``db``, ``df_ab``, ``df_ba``. Enqueued on the device's stream."""
+        vp = ctypes.c_void_p
+        self._check(self._L.tw_warp_blend_adjoint(self._h, vp(a), vp(b), vp(f_ab), vp(f_ba), width, height, flow_w, flow_h,
+                                                  batch, np.float32(wa), vp(target or None), vp(grad_out or None),
+                                                  vp(out or None), vp(loss or None), vp(da or None), vp(db or None),
+                                                  vp(df_ab or None), vp(df_ba or None)))
 
     def check_powf(self, x, y):
         """The device's powf of the Delinearize prep (the plugin runtime's, crt_powf.rs)."""

@@ -267,4 +267,24 @@ struct MotionBlur {
 };
 __global__ void k_motion_blur(MotionBlur B);
 
+// ---- the adjoint of warp + blend (adjoint.cu) ----
+struct AdjParams {
+    const float* a;         // batch x (w x h x 4)
+    const float* b;
+    const float* f_ab;      // batch x (fw x fh x 2), interleaved
+    const float* f_ba;
+    const float* target;    // the L1 loss against it (nullptr: grad_out drives the backward)
+    const float* grad_out;  // d loss / d out (nullptr with target == nullptr: forward only)
+    float* out;             // the forward output (nullptr: not written)
+    float* loss;            // batch sums of |out - target| (accumulated)
+    float* da;              // the gradients (accumulated; nullptr: not computed)
+    float* db;
+    float* df_ab;
+    float* df_ba;
+    int w, h, fw, fh;
+    float rx, ry, wa;
+    bool tiled;             // rx <= 1 and ry <= 1: the flow gradients gather in shared memory first
+};
+__global__ void k_warp_blend_adjoint(AdjParams P);
+
 }  // namespace tw

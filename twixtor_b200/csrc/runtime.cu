@@ -2059,6 +2059,51 @@ int tw_motion_blur(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw
     return TW_OK;
 }
 
+int tw_warp_blend_adjoint(tw_ctx* ctx, const float* a, const float* b, const float* f_ab, const float* f_ba,
+                          int32_t width, int32_t height, int32_t flow_w, int32_t flow_h, int32_t batch, float wa,
+                          const float* target, const float* grad_out, float* out, float* loss, float* da, float* db,
+                          float* df_ab, float* df_ba) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!a || !b || !f_ab || !f_ba || batch < 0) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    if (width < 2 || height < 2 || flow_w < 2 || flow_h < 2)
+        return ctx->fail(TW_ERR_MISMATCH, "warp + blend needs images and flows of at least 2x2 (image %dx%d, flow %dx%d)",
+                         width, height, flow_w, flow_h);
+    if (batch > 65535) return ctx->fail(TW_ERR_TOO_LARGE, "warp + blend: a batch of %d", batch);
+    if (loss && !target) return ctx->fail(TW_ERR_BAD_PARAM, "warp + blend: a loss needs its target");
+    if (batch == 0) return TW_OK;
+    AdjParams P{};
+    P.a = a;
+    P.b = b;
+    P.f_ab = f_ab;
+    P.f_ba = f_ba;
+    P.target = target;
+    P.grad_out = grad_out;
+    P.out = out;
+    P.loss = loss;
+    P.da = da;
+    P.db = db;
+    P.df_ab = df_ab;
+    P.df_ba = df_ba;
+    P.w = width;
+    P.h = height;
+    P.fw = flow_w;
+    P.fh = flow_h;
+    P.rx = (float)(flow_w - 1) / (float)(width - 1);
+    P.ry = (float)(flow_h - 1) / (float)(height - 1);
+    P.wa = wa;
+    P.tiled = P.rx <= 1.0f && P.ry <= 1.0f;
+    dim3 grid((unsigned)((width + 31) / 32), (unsigned)((height + 7) / 8), (unsigned)batch);
+    // algorithmic bytes: A, B and the target or output gradient read, the output and the four
+    // gradients written once, the flows read once
+    double img = 16.0 * width * height * batch, fl = 8.0 * flow_w * flow_h * batch;
+    double bytes = img * (2 + (target || grad_out ? 1 : 0) + (out ? 1 : 0) + (da ? 1 : 0) + (db ? 1 : 0)) +
+                   fl * (2 + (df_ab ? 1 : 0) + (df_ba ? 1 : 0));
+    LAUNCHB(ctx, bytes, k_warp_blend_adjoint, grid, 256, 0, P);
+    return ctx->cuda(cudaGetLastError(), "launch");
+}
+
 int tw_check_powf(tw_ctx* ctx, const float* x, const float* y, float* out, int64_t n) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);

@@ -185,3 +185,37 @@ def layered_clip(width, height, frames, nfg=3, depth=8, seed=0x74570004, bg_velo
             mattes[k].append(_to_wire(m, np.ones((height, width)), depth))
         foot.append(_to_wire(rgb, np.ones((height, width)), depth))
     return np.concatenate(foot), [np.concatenate(m) for m in mattes]
+
+
+def adjoint_triples(width, height, batch, seed=0x74570005, peak=10.0):
+    """The warp + blend adjoint workload: per batch item a seeded value noise texture T (float RGBA
+    in [0, 1], alpha 1) and a smooth ground truth displacement D, the sum of four random Gaussian
+    bumps with a peak of ``peak`` px; the middle frame is T, A samples T at p - D(p) / 2 and B at
+    p + D(p) / 2. Returns (A, B, M, D) as float32 arrays (batch, height, width, 4) and
+    (batch, height, width, 2)."""
+    rng = np.random.RandomState(seed)
+    Y, X = np.mgrid[0:height, 0:width].astype(np.float64)
+    As, Bs, Ms, Ds = [], [], [], []
+    for _ in range(batch):
+        pad = int(peak) + 4
+        tex = NoiseField(int(rng.randint(1 << 30)), width + 2 * pad, height + 2 * pad)
+        D = np.zeros((height, width, 2))
+        for _ in range(4):
+            cx, cy = rng.uniform(0, width), rng.uniform(0, height)
+            sg = rng.uniform(0.12, 0.3) * min(width, height)
+            amp = rng.uniform(-1.0, 1.0, 2)
+            g = np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * sg * sg))
+            D += g[..., None] * amp
+        D *= peak / max(np.abs(D).max(), 1e-9)
+
+        def frame(dx, dy):
+            g = tex.at(X + dx + pad, Y + dy + pad) / 255.0
+            rgb = np.stack([g, 0.8 * g + 0.1, 1.0 - 0.7 * g], -1)
+            return np.concatenate([rgb, np.ones((height, width, 1))], -1).clip(0, 1)
+
+        Ms.append(frame(0.0, 0.0))
+        As.append(frame(-0.5 * D[..., 0], -0.5 * D[..., 1]))
+        Bs.append(frame(0.5 * D[..., 0], 0.5 * D[..., 1]))
+        Ds.append(D)
+    f = lambda v: np.ascontiguousarray(np.stack(v), np.float32)  # noqa: E731
+    return f(As), f(Bs), f(Ms), f(Ds)
