@@ -307,6 +307,70 @@ def run_workload(args):
     return 0
 
 
+def run_adjoint(args):
+    """The adjoint of warp + blend: per step the L1 loss against the middle frame and its gradients
+    w.r.t. both frames and both flows for a batch of 64 triples of 1280x720 float RGBA (flows at
+    640x360), the gradient buffers zeroed first; triples/s with everything resident in HBM."""
+    import torch
+    import twixtor_b200 as tw
+    from twixtor_b200 import adjoint, synth
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    dev = tw.Device(0)
+    dev.set_stream(stream.cuda_stream)
+    w, h, fw, fh, batch, distinct = 1280, 720, 640, 360, 64, 4
+    A_, B_, M_, D_ = synth.adjoint_triples(w, h, distinct)
+    rep = lambda x: torch.from_numpy(x).cuda().repeat((batch // distinct,) + (1,) * (x.ndim - 1)).contiguous()  # noqa
+    a, b, m = rep(A_), rep(B_), rep(M_)
+    d_half = np.ascontiguousarray(D_[:, ::2, ::2, :] * np.float32(0.5))  # flow grid units (r ~ 0.5)
+    fab, fba = rep(d_half), rep(-d_half)
+    loss = torch.zeros(batch, device="cuda:0")
+    da, db = torch.zeros_like(a), torch.zeros_like(b)
+    dfab, dfba = torch.zeros_like(fab), torch.zeros_like(fba)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda:0")
+
+    def step(k):
+        for t in (loss, da, db, dfab, dfba):
+            t.zero_()
+        dev.warp_blend_adjoint(a.data_ptr(), b.data_ptr(), fab.data_ptr(), fba.data_ptr(), w, h, fw, fh, batch, 0.5,
+                               target=m.data_ptr(), loss=loss.data_ptr(), da=da.data_ptr(), db=db.data_ptr(),
+                               df_ab=dfab.data_ptr(), df_ba=dfba.data_ptr())
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    dev.profile_begin("k_warp_blend_adjoint")
+    with Clocks(0) as clk:
+        times = [_timed(stream, step, k, flush) for k in range(args.warmup, args.warmup + args.steps)]
+    kms, klaunch, kbytes = dev.profile_end()
+    total_ms = sum(times)
+    value = args.steps * batch / (total_ms / 1e3)
+    # the torch harness (l1_loss_and_grads allocates its zeroed gradients per call)
+    for k in range(args.warmup):
+        adjoint.l1_loss_and_grads(dev, a, b, fab, fba, m, 0.5)
+    torch.cuda.synchronize()
+    etimes = [_timed(stream, lambda k: adjoint.l1_loss_and_grads(dev, a, b, fab, fba, m, 0.5), k, flush)
+              for k in range(args.steps)]
+    peak, which = peaks()
+    achieved = (kbytes / (kms / 1e3)) / 1e9 if kms > 0 else None
+    emit({"metric": "adjoint of warp + blend, triples/s (L1 loss, gradients for both frames and both flows)",
+          "value": value, "unit": "triples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+          "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+          "dtype": "f32", "data": "synthetic",
+          "config": {"workload": "64 triples of 1280x720 float RGBA, flows 640x360, wa 0.5, L1 against the middle frame",
+                     "batch": batch, "l2": "flushed between steps (256 MiB write); inputs 2.8 GB > L2"},
+          "e2e": {"value": args.steps * batch / (sum(etimes) / 1e3), "unit": "triples/s", "h2d_bytes_per_step": 0,
+                  "d2h_bytes_per_step": 0, "note": "through the torch harness (device tensors)"},
+          "gpu_launches": dev.stats()["kernel_launches"],
+          "roofline": {"bound": "hbm", "kernel": "k_warp_blend_adjoint", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                       "frac": (achieved / peak) if achieved else None, "traffic": None, "peak_source": which,
+                       "algorithmic_bytes_per_launch": kbytes / max(klaunch, 1),
+                       "avg_launch_us": 1e3 * kms / max(klaunch, 1)},
+          "clocks": clk.summary()})
+    dev.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -320,13 +384,16 @@ def main():
     ap.add_argument("--breakdown", action="store_true",
                     help="after the timed region, time one more step with every kernel bracketed by events and "
                          "print the per-kernel table to stderr (not part of the reported numbers)")
-    ap.add_argument("--workload", default="retime", choices=["retime", "create-vectors", "fgbg"],
-                    help="retime (the headline, default), create-vectors (1080p 16 bpc) or fgbg (1080p, 3 FG layers)")
+    ap.add_argument("--workload", default="retime", choices=["retime", "create-vectors", "fgbg", "adjoint"],
+                    help="retime (the headline, default), create-vectors (1080p 16 bpc), fgbg (1080p, 3 FG layers) or "
+                         "adjoint (warp + blend gradients, 64 triples of 1280x720)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     if args.workload != "retime":
         return run_workload(args)
     if args.ncu_case:
