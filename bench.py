@@ -319,6 +319,8 @@ def run_adjoint(args):
     dev = tw.Device(0)
     dev.set_stream(stream.cuda_stream)
     w, h, fw, fh, batch, distinct = 1280, 720, 640, 360, 64, 4
+    if args.ncu_case:  # the profiling driver: one launch on 8 triples (0.7 GB on the device)
+        batch = 8
     A_, B_, M_, D_ = synth.adjoint_triples(w, h, distinct)
     rep = lambda x: torch.from_numpy(x).cuda().repeat((batch // distinct,) + (1,) * (x.ndim - 1)).contiguous()  # noqa
     a, b, m = rep(A_), rep(B_), rep(M_)
@@ -336,6 +338,12 @@ def run_adjoint(args):
                                target=m.data_ptr(), loss=loss.data_ptr(), da=da.data_ptr(), db=db.data_ptr(),
                                df_ab=dfab.data_ptr(), df_ba=dfba.data_ptr())
 
+    if args.ncu_case:
+        step(0)
+        torch.cuda.synchronize()
+        print(json.dumps({"ncu_case": "ok", "workload": "adjoint", "batch": batch}))
+        dev.close()
+        return 0
     for k in range(args.warmup):
         step(k)
     torch.cuda.synchronize()
@@ -396,7 +404,7 @@ def main():
         return run_adjoint(args)
     if args.workload != "retime":
         return run_workload(args)
-    if args.ncu_case:
+    if args.ncu_case and args.workload == "retime":
         return ncu_case()
 
     import torch

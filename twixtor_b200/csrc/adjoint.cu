@@ -5,19 +5,21 @@
 // to the image rectangle. One fused kernel per pixel recomputes the forward sample (nothing of the
 // forward pass is stored), takes the output gradient (given, or the sign of out - target for the
 // photometric L1 loss) and scatters:
-//   dA, dB     the bilinear weights times (1 - w) g and w g (vector atomics, 16 bytes per corner);
+//   dA, dB     the bilinear weights times (1 - w) g and w g, accumulated per CTA in a shared tile
+//              of the box the CTA's samples reach, then added to global memory once per pixel
+//              (vector atomics; straight to global memory when the box does not fit);
 //   dF_BA, dF_AB  the image gradient at the sample point times s / r, through the flow's bilinear
 //              weights: accumulated per CTA in shared memory (a tile of flow texels), then added
 //              to global memory once per texel.
 // Frames are float RGBA (4 channels, any premultiplication), batch items back to back.
 #include "kernels.cuh"
+#include <climits>
 
 namespace tw {
 
 namespace {
 
-constexpr int AT_X = 32, AT_Y = 8;               // pixels per CTA
-constexpr int FT_X = AT_X + 2, FT_Y = AT_Y + 2;  // the flow texel tile when r <= 1 per axis
+constexpr int FT_X = ADJ_TX + 2, FT_Y = ADJ_TY + 2;  // the flow texel tile when r <= 1 per axis
 
 __device__ __forceinline__ float4 ld4(const float* p, long i) { return reinterpret_cast<const float4*>(p)[i]; }
 
@@ -60,7 +62,7 @@ __device__ __forceinline__ float4 scale4(float4 a, float s) { return make_float4
 // One side: the sample of S (and its four corners) at p + F(p r) s / r
 struct Side {
     Sample smp;
-    float4 c00, c10, c01, c11, val;
+    float4 val;
     int fix, fiy;    // the flow footprint
     float ffx, ffy;
 };
@@ -77,116 +79,245 @@ __device__ __forceinline__ Side side_at(const float* S, const float* F, const Ad
     float px = (float)x + u * amount / P.rx, py = (float)y + v * amount / P.ry;
     d.smp = sample_at(px, py, P.w, P.h);
     long i00 = (long)d.smp.iy * P.w + d.smp.ix, i01 = i00 + P.w;
-    d.c00 = ld4(S, i00);
-    d.c10 = ld4(S, i00 + 1);
-    d.c01 = ld4(S, i01);
-    d.c11 = ld4(S, i01 + 1);
-    d.val = lerp4(lerp4(d.c00, d.c10, d.smp.fx), lerp4(d.c01, d.c11, d.smp.fx), d.smp.fy);
+    d.val = lerp4(lerp4(ld4(S, i00), ld4(S, i00 + 1), d.smp.fx), lerp4(ld4(S, i01), ld4(S, i01 + 1), d.smp.fx), d.smp.fy);
     return d;
 }
 
-// the gradient of one side: dS at the four corners (vector atomics), the positional gradient into
-// the flow tile (shared) or straight to global memory
-__device__ __forceinline__ void side_back(const Side& d, float4 g, const AdjParams& P, float* dS, float* sflow, int tx0,
-                                          int ty0, bool tiled, float* dF, float amount) {
-    const Sample& s = d.smp;
-    long i00 = (long)s.iy * P.w + s.ix, i01 = i00 + P.w;
-    float w00 = (1.0f - s.fx) * (1.0f - s.fy), w10 = s.fx * (1.0f - s.fy), w01 = (1.0f - s.fx) * s.fy, w11 = s.fx * s.fy;
-    if (dS) {
-        atomicAdd(reinterpret_cast<float4*>(dS) + i00, scale4(g, w00));
-        atomicAdd(reinterpret_cast<float4*>(dS) + i00 + 1, scale4(g, w10));
-        atomicAdd(reinterpret_cast<float4*>(dS) + i01, scale4(g, w01));
-        atomicAdd(reinterpret_cast<float4*>(dS) + i01 + 1, scale4(g, w11));
+// the top left cell of one side's sample (pass 1 of the kernel)
+__device__ __forceinline__ void side_cell(const float* F, const AdjParams& P, int x, int y, float amount, int& cx, int& cy) {
+    int fix, fiy;
+    float ffx, ffy;
+    footprint((float)x * P.rx, (float)y * P.ry, P.fw, P.fh, fix, fiy, ffx, ffy);
+    long f00 = ((long)fiy * P.fw + fix) * 2, f01 = f00 + (long)P.fw * 2;
+    float2 a = *reinterpret_cast<const float2*>(F + f00), b = *reinterpret_cast<const float2*>(F + f00 + 2);
+    float2 c = *reinterpret_cast<const float2*>(F + f01), e = *reinterpret_cast<const float2*>(F + f01 + 2);
+    float u = (a.x + (b.x - a.x) * ffx) * (1.0f - ffy) + (c.x + (e.x - c.x) * ffx) * ffy;
+    float v = (a.y + (b.y - a.y) * ffx) * (1.0f - ffy) + (c.y + (e.y - c.y) * ffx) * ffy;
+    Sample s = sample_at((float)x + u * amount / P.rx, (float)y + v * amount / P.ry, P.w, P.h);
+    cx = s.ix;
+    cy = s.iy;
+}
+
+// where a side's image gradient goes: a shared tile of the CTA's box (tile != nullptr) or the
+// global gradient (vector atomics)
+struct Acc {
+    float* tile;     // four planes of ADJ_BOX_PX floats (a warp's adjacent pixels on adjacent banks)
+    int bx, by, bw;
+    float* global;
+};
+
+__device__ __forceinline__ void acc_add(const Acc& c, const AdjParams& P, int px, int py, float4 v) {
+    if (c.tile) {
+        float* t = c.tile + ((py - c.by) * c.bw + (px - c.bx));
+        atomicAdd(t, v.x);
+        atomicAdd(t + ADJ_BOX_PX, v.y);
+        atomicAdd(t + 2 * ADJ_BOX_PX, v.z);
+        atomicAdd(t + 3 * ADJ_BOX_PX, v.w);
+    } else if (c.global) {
+        atomicAdd(reinterpret_cast<float4*>(c.global) + ((long)py * P.w + px), v);
     }
+}
+
+// the gradient of one side: dS at the four corners, the positional gradient into the flow tile
+// (shared) or straight to global memory
+__device__ __forceinline__ void side_back(const float* S, const Side& d, float4 g, const AdjParams& P, const Acc& acc,
+                                          float* sflow, int tx0, int ty0, bool tiled, float* dF, float amount) {
+    const Sample& s = d.smp;
+    float w00 = (1.0f - s.fx) * (1.0f - s.fy), w10 = s.fx * (1.0f - s.fy), w01 = (1.0f - s.fx) * s.fy, w11 = s.fx * s.fy;
+    acc_add(acc, P, s.ix, s.iy, scale4(g, w00));
+    acc_add(acc, P, s.ix + 1, s.iy, scale4(g, w10));
+    acc_add(acc, P, s.ix, s.iy + 1, scale4(g, w01));
+    acc_add(acc, P, s.ix + 1, s.iy + 1, scale4(g, w11));
     if (!dF) return;
-    // d val / d px and d val / d py of the bilinear sample, per channel
-    float4 dx = lerp4(make_float4(d.c10.x - d.c00.x, d.c10.y - d.c00.y, d.c10.z - d.c00.z, d.c10.w - d.c00.w),
-                      make_float4(d.c11.x - d.c01.x, d.c11.y - d.c01.y, d.c11.z - d.c01.z, d.c11.w - d.c01.w), s.fy);
-    float4 dy = lerp4(make_float4(d.c01.x - d.c00.x, d.c01.y - d.c00.y, d.c01.z - d.c00.z, d.c01.w - d.c00.w),
-                      make_float4(d.c11.x - d.c10.x, d.c11.y - d.c10.y, d.c11.z - d.c10.z, d.c11.w - d.c10.w), s.fx);
+    // d val / d px and d val / d py of the bilinear sample, per channel (the corners read again: the
+    // forward kept only the value)
+    long i00 = (long)s.iy * P.w + s.ix, i01 = i00 + P.w;
+    float4 c00 = ld4(S, i00), c10 = ld4(S, i00 + 1), c01 = ld4(S, i01), c11 = ld4(S, i01 + 1);
+    float4 dx = lerp4(make_float4(c10.x - c00.x, c10.y - c00.y, c10.z - c00.z, c10.w - c00.w),
+                      make_float4(c11.x - c01.x, c11.y - c01.y, c11.z - c01.z, c11.w - c01.w), s.fy);
+    float4 dy = lerp4(make_float4(c01.x - c00.x, c01.y - c00.y, c01.z - c00.z, c01.w - c00.w),
+                      make_float4(c11.x - c10.x, c11.y - c10.y, c11.z - c10.z, c11.w - c10.w), s.fx);
     float gu = s.cx ? 0.0f : dot4(g, dx) * amount / P.rx;
     float gv = s.cy ? 0.0f : dot4(g, dy) * amount / P.ry;
-    if (gu == 0.0f && gv == 0.0f) return;
     float fw00 = (1.0f - d.ffx) * (1.0f - d.ffy), fw10 = d.ffx * (1.0f - d.ffy), fw01 = (1.0f - d.ffx) * d.ffy,
           fw11 = d.ffx * d.ffy;
     const int cx[4] = {0, 1, 0, 1}, cy[4] = {0, 0, 1, 1};
     const float wt[4] = {fw00, fw10, fw01, fw11};
+    if (tiled) {
+        // adjacent lanes whose samples share the flow cell (a flow at half the image size pairs
+        // them) add their contributions first: one shared atomic for the pair
+        // (lanes past the image's right edge are inactive: only the active ones exchange)
+        int lane = threadIdx.x & 31;
+        unsigned mask = __activemask();
+        int key = d.fiy * P.fw + d.fix;
+        int okey = __shfl_xor_sync(mask, key, 1);
+        bool pair = (mask >> (lane ^ 1) & 1u) && okey == key;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            float u = gu * wt[k], v = gv * wt[k];
+            float ou = __shfl_xor_sync(mask, u, 1), ov = __shfl_xor_sync(mask, v, 1);
+            if (pair) {
+                if (lane & 1) continue;
+                u += ou;
+                v += ov;
+            }
+            if (u == 0.0f && v == 0.0f) continue;
+            int lx = d.fix + cx[k] - tx0, ly = d.fiy + cy[k] - ty0;
+            atomicAdd(sflow + (ly * FT_X + lx) * 2, u);
+            atomicAdd(sflow + (ly * FT_X + lx) * 2 + 1, v);
+        }
+        return;
+    }
+    if (gu == 0.0f && gv == 0.0f) return;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         int fx = d.fix + cx[k], fy = d.fiy + cy[k];
-        if (tiled) {
-            int lx = fx - tx0, ly = fy - ty0;
-            atomicAdd(sflow + (ly * FT_X + lx) * 2, gu * wt[k]);
-            atomicAdd(sflow + (ly * FT_X + lx) * 2 + 1, gv * wt[k]);
-        } else {
-            atomicAdd(reinterpret_cast<float2*>(dF) + ((long)fy * P.fw + fx), make_float2(gu * wt[k], gv * wt[k]));
-        }
+        atomicAdd(reinterpret_cast<float2*>(dF) + ((long)fy * P.fw + fx), make_float2(gu * wt[k], gv * wt[k]));
     }
 }
 
 }  // namespace
 
-// grid: (ceil(w / 32), ceil(h / 8), batch), 256 threads
-__global__ void __launch_bounds__(AT_X * AT_Y) k_warp_blend_adjoint(AdjParams P) {
-    __shared__ float sflow[2][FT_X * FT_Y * 2];
+// One CTA per 32 x 32 output tile of a batch item, 256 threads, 4 pixels a thread (the columns of a
+// warp adjacent). Three passes: (1) the sample cells of both sides, reduced to their bounding boxes;
+// (2) the forward recomputed, the loss and the backward, the image gradients added into a shared
+// tile of each box (when it fits, else straight to global memory with vector atomics) and the flow
+// gradients into the shared flow tile; (3) the shared tiles added to global memory, one coalesced
+// vector atomic per touched pixel. Smooth flows shift a tile nearly rigidly, so a box holds about
+// one tile: the global atomics drop from 8 to about 2.5 per output pixel.
+__global__ void __launch_bounds__(ADJ_THREADS, 3) k_warp_blend_adjoint(AdjParams P) {
+    extern __shared__ float4 adj_smem[];
+    float* sacc0 = reinterpret_cast<float*>(adj_smem);  // four planes of ADJ_BOX_PX floats per side
+    float* sacc1 = sacc0 + 4 * ADJ_BOX_PX;
+    float* sflow0 = sacc1 + 4 * ADJ_BOX_PX;
+    float* sflow1 = sflow0 + FT_X * FT_Y * 2;
+    __shared__ int box[2][4];                       // min x, min y, max x, max y of the cells
     int b = blockIdx.z;
     long img = (long)P.w * P.h * 4 * b, flo = (long)P.fw * P.fh * 2 * b;
-    int x0 = blockIdx.x * AT_X, y0 = blockIdx.y * AT_Y;
-    int x = x0 + (int)(threadIdx.x % AT_X), y = y0 + (int)(threadIdx.x / AT_X);
-    // the flow texels this tile's footprints reach, when they fit the shared tile
-    int tx0 = (int)floorf((float)x0 * P.rx), ty0 = (int)floorf((float)y0 * P.ry);
-    tx0 = min(tx0, max(P.fw - 2, 0));
-    ty0 = min(ty0, max(P.fh - 2, 0));
+    const float* A = P.a + img;
+    const float* B = P.b + img;
+    const float* Fba = P.f_ba + flo;
+    const float* Fab = P.f_ab + flo;
+    float frac = 1.0f - P.wa;
+    int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TY;
+    int x = x0 + (int)(threadIdx.x % ADJ_TX);
+    int yb = y0 + (int)(threadIdx.x / ADJ_TX);
+    const int ROWS = ADJ_THREADS / ADJ_TX;  // 8 rows a pass
+    int tx0 = min((int)floorf((float)x0 * P.rx), max(P.fw - 2, 0));
+    int ty0 = min((int)floorf((float)y0 * P.ry), max(P.fh - 2, 0));
     bool tiled = P.tiled;
-    if (tiled) {
-        for (int i = threadIdx.x; i < FT_X * FT_Y * 2; i += blockDim.x) {
-            sflow[0][i] = 0.0f;
-            sflow[1][i] = 0.0f;
-        }
-        __syncthreads();
+    bool backward = P.grad_out || P.target;
+    if (threadIdx.x < 2) {
+        box[threadIdx.x][0] = INT_MAX;
+        box[threadIdx.x][1] = INT_MAX;
+        box[threadIdx.x][2] = INT_MIN;
+        box[threadIdx.x][3] = INT_MIN;
     }
-    bool live = x < P.w && y < P.h;
+    if (tiled)
+        for (int i = threadIdx.x; i < FT_X * FT_Y * 2; i += blockDim.x) sflow0[i] = sflow1[i] = 0.0f;
+    __syncthreads();
+    // pass 1: the cells
+    if (backward) {
+        int mn[2][2] = {{INT_MAX, INT_MAX}, {INT_MAX, INT_MAX}}, mx[2][2] = {{INT_MIN, INT_MIN}, {INT_MIN, INT_MIN}};
+        for (int j = 0; j < ADJ_TY / ROWS; j++) {
+            int y = yb + j * ROWS;
+            if (x >= P.w || y >= P.h) continue;
+            int cx, cy;
+            side_cell(Fba, P, x, y, frac, cx, cy);
+            mn[0][0] = min(mn[0][0], cx); mn[0][1] = min(mn[0][1], cy);
+            mx[0][0] = max(mx[0][0], cx); mx[0][1] = max(mx[0][1], cy);
+            side_cell(Fab, P, x, y, P.wa, cx, cy);
+            mn[1][0] = min(mn[1][0], cx); mn[1][1] = min(mn[1][1], cy);
+            mx[1][0] = max(mx[1][0], cx); mx[1][1] = max(mx[1][1], cy);
+        }
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                mn[s][0] = min(mn[s][0], __shfl_xor_sync(0xffffffffu, mn[s][0], o));
+                mn[s][1] = min(mn[s][1], __shfl_xor_sync(0xffffffffu, mn[s][1], o));
+                mx[s][0] = max(mx[s][0], __shfl_xor_sync(0xffffffffu, mx[s][0], o));
+                mx[s][1] = max(mx[s][1], __shfl_xor_sync(0xffffffffu, mx[s][1], o));
+            }
+            if ((threadIdx.x & 31) == 0) {
+                atomicMin(&box[s][0], mn[s][0]);
+                atomicMin(&box[s][1], mn[s][1]);
+                atomicMax(&box[s][2], mx[s][0]);
+                atomicMax(&box[s][3], mx[s][1]);
+            }
+        }
+    }
+    __syncthreads();
+    int bw[2], bh[2];
+    bool shared_box[2];
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+        bw[s] = box[s][2] - box[s][0] + 2;
+        bh[s] = box[s][3] - box[s][1] + 2;
+        shared_box[s] = backward && box[s][2] >= box[s][0] && (long)bw[s] * bh[s] <= ADJ_BOX_PX;
+    }
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+        if (!shared_box[s]) continue;
+        float* t = s == 0 ? sacc0 : sacc1;
+        for (int i = threadIdx.x; i < bw[s] * bh[s]; i += blockDim.x)
+            t[i] = t[i + ADJ_BOX_PX] = t[i + 2 * ADJ_BOX_PX] = t[i + 3 * ADJ_BOX_PX] = 0.0f;
+    }
+    __syncthreads();
+    // pass 2: forward, loss, backward
     float loss = 0.0f;
-    if (live) {
-        const float* A = P.a + img;
-        const float* B = P.b + img;
-        float frac = 1.0f - P.wa;
-        Side sa = side_at(A, P.f_ba + flo, P, x, y, frac);
-        Side sb = side_at(B, P.f_ab + flo, P, x, y, P.wa);
+    for (int j = 0; j < ADJ_TY / ROWS; j++) {
+        int y = yb + j * ROWS;
+        if (x >= P.w || y >= P.h) continue;
+        Side sa = side_at(A, Fba, P, x, y, frac);
+        Side sb = side_at(B, Fab, P, x, y, P.wa);
         float4 out = lerp4(sa.val, sb.val, frac);
         long i = (long)y * P.w + x;
         if (P.out) reinterpret_cast<float4*>(P.out + img)[i] = out;
+        if (!backward) continue;
         float4 g;
         if (P.target) {  // the photometric L1 loss: d|out - t| / d out = sign(out - t)
             float4 t = ld4(P.target + img, i);
             float4 r = make_float4(out.x - t.x, out.y - t.y, out.z - t.z, out.w - t.w);
-            loss = fabsf(r.x) + fabsf(r.y) + fabsf(r.z) + fabsf(r.w);
+            loss += fabsf(r.x) + fabsf(r.y) + fabsf(r.z) + fabsf(r.w);
             g = make_float4((r.x > 0.0f) - (r.x < 0.0f), (r.y > 0.0f) - (r.y < 0.0f), (r.z > 0.0f) - (r.z < 0.0f),
                             (r.w > 0.0f) - (r.w < 0.0f));
         } else {
-            g = P.grad_out ? ld4(P.grad_out + img, i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            g = ld4(P.grad_out + img, i);
         }
-        if (P.grad_out || P.target) {
-            side_back(sa, scale4(g, 1.0f - frac), P, P.da ? P.da + img : nullptr, sflow[0], tx0, ty0, tiled,
-                      P.df_ba ? P.df_ba + flo : nullptr, frac);
-            side_back(sb, scale4(g, frac), P, P.db ? P.db + img : nullptr, sflow[1], tx0, ty0, tiled,
-                      P.df_ab ? P.df_ab + flo : nullptr, P.wa);
-        }
+        Acc ca{shared_box[0] ? sacc0 : nullptr, box[0][0], box[0][1], bw[0], P.da ? P.da + img : nullptr};
+        Acc cb{shared_box[1] ? sacc1 : nullptr, box[1][0], box[1][1], bw[1], P.db ? P.db + img : nullptr};
+        side_back(A, sa, scale4(g, 1.0f - frac), P, ca, sflow0, tx0, ty0, tiled, P.df_ba ? P.df_ba + flo : nullptr, frac);
+        side_back(B, sb, scale4(g, frac), P, cb, sflow1, tx0, ty0, tiled, P.df_ab ? P.df_ab + flo : nullptr, P.wa);
     }
     if (P.loss) {  // the loss of the batch item: a warp shuffle sum, one atomic per warp
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
         if ((threadIdx.x & 31) == 0 && loss != 0.0f) atomicAdd(P.loss + b, loss);
     }
+    __syncthreads();
+    // pass 3: the shared tiles into global memory
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+        float* dS = s == 0 ? P.da : P.db;
+        if (!shared_box[s] || !dS) continue;
+        float* acc = s == 0 ? sacc0 : sacc1;
+        float4* g4 = reinterpret_cast<float4*>(dS + img);
+        for (int i = threadIdx.x; i < bw[s] * bh[s]; i += blockDim.x) {
+            float4 v = make_float4(acc[i], acc[i + ADJ_BOX_PX], acc[i + 2 * ADJ_BOX_PX], acc[i + 3 * ADJ_BOX_PX]);
+            if (v.x == 0.0f && v.y == 0.0f && v.z == 0.0f && v.w == 0.0f) continue;
+            int px = box[s][0] + i % bw[s], py = box[s][1] + i / bw[s];
+            if (px < P.w && py < P.h) atomicAdd(g4 + ((long)py * P.w + px), v);
+        }
+    }
     if (tiled) {
-        __syncthreads();
         for (int i = threadIdx.x; i < FT_X * FT_Y; i += blockDim.x) {
             int lx = i % FT_X, ly = i / FT_X;
             int fx = tx0 + lx, fy = ty0 + ly;
             if (fx >= P.fw || fy >= P.fh) continue;
             long k = (long)fy * P.fw + fx;
-            float2 ga = make_float2(sflow[0][i * 2], sflow[0][i * 2 + 1]);
-            float2 gb = make_float2(sflow[1][i * 2], sflow[1][i * 2 + 1]);
+            float2 ga = make_float2(sflow0[i * 2], sflow0[i * 2 + 1]);
+            float2 gb = make_float2(sflow1[i * 2], sflow1[i * 2 + 1]);
             if (P.df_ba && (ga.x != 0.0f || ga.y != 0.0f)) atomicAdd(reinterpret_cast<float2*>(P.df_ba + flo) + k, ga);
             if (P.df_ab && (gb.x != 0.0f || gb.y != 0.0f)) atomicAdd(reinterpret_cast<float2*>(P.df_ab + flo) + k, gb);
         }

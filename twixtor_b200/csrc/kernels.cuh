@@ -285,6 +285,10 @@ struct AdjParams {
     float rx, ry, wa;
     bool tiled;             // rx <= 1 and ry <= 1: the flow gradients gather in shared memory first
 };
+constexpr int ADJ_TX = 32, ADJ_TY = 32, ADJ_THREADS = 256;  // the output tile of a CTA
+constexpr int ADJ_BOX_PX = 1536;                            // the shared image gradient tile, per side
+// dynamic shared memory: two image tiles (float4) and two flow tiles ((TX + 2) x (TY + 2) x 2 floats)
+constexpr int ADJ_SMEM = 2 * ADJ_BOX_PX * 16 + 2 * (ADJ_TX + 2) * (ADJ_TY + 2) * 2 * 4;
 __global__ void k_warp_blend_adjoint(AdjParams P);
 
 }  // namespace tw

@@ -208,6 +208,7 @@ struct tw_ctx {
     DevBuf fc_img[2], fc_cov[2];  // the forward compositions: the two pushed frames and their coverage
     DevBuf wb_wt[2], wb_tmp[2], wb_mask[2], wb_cov[2];  // Weighted Blend (the calls on the context's stream)
     DevBuf pre_blur, comp_e;  // Blur Compensation: the composite before the blur, the engine result
+    bool adj_smem_set = false;  // the adjoint kernel's dynamic shared memory limit is raised
     DevBuf host_stage;  // unused placeholder for pinned staging
     std::vector<cudaEvent_t> ev_pool;  // the profiler's events (KernelProfile)
     // the forward warp: vertices, mip pyramid, per pixel counts / offsets, hit lists, flags
@@ -2094,13 +2095,18 @@ int tw_warp_blend_adjoint(tw_ctx* ctx, const float* a, const float* b, const flo
     P.ry = (float)(flow_h - 1) / (float)(height - 1);
     P.wa = wa;
     P.tiled = P.rx <= 1.0f && P.ry <= 1.0f;
-    dim3 grid((unsigned)((width + 31) / 32), (unsigned)((height + 7) / 8), (unsigned)batch);
+    if (!ctx->adj_smem_set) {
+        CHECK(ctx->cuda(cudaFuncSetAttribute(k_warp_blend_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, ADJ_SMEM),
+                        "adjoint shared memory"));
+        ctx->adj_smem_set = true;
+    }
+    dim3 grid((unsigned)((width + ADJ_TX - 1) / ADJ_TX), (unsigned)((height + ADJ_TY - 1) / ADJ_TY), (unsigned)batch);
     // algorithmic bytes: A, B and the target or output gradient read, the output and the four
     // gradients written once, the flows read once
     double img = 16.0 * width * height * batch, fl = 8.0 * flow_w * flow_h * batch;
     double bytes = img * (2 + (target || grad_out ? 1 : 0) + (out ? 1 : 0) + (da ? 1 : 0) + (db ? 1 : 0)) +
                    fl * (2 + (df_ab ? 1 : 0) + (df_ba ? 1 : 0));
-    LAUNCHB(ctx, bytes, k_warp_blend_adjoint, grid, 256, 0, P);
+    LAUNCHB(ctx, bytes, k_warp_blend_adjoint, grid, ADJ_THREADS, ADJ_SMEM, P);
     return ctx->cuda(cudaGetLastError(), "launch");
 }
 
