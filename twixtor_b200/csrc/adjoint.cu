@@ -83,32 +83,18 @@ __device__ __forceinline__ Side side_at(const float* S, const float* F, const Ad
     return d;
 }
 
-// the top left cell of one side's sample (pass 1 of the kernel)
-__device__ __forceinline__ void side_cell(const float* F, const AdjParams& P, int x, int y, float amount, int& cx, int& cy) {
-    int fix, fiy;
-    float ffx, ffy;
-    footprint((float)x * P.rx, (float)y * P.ry, P.fw, P.fh, fix, fiy, ffx, ffy);
-    long f00 = ((long)fiy * P.fw + fix) * 2, f01 = f00 + (long)P.fw * 2;
-    float2 a = *reinterpret_cast<const float2*>(F + f00), b = *reinterpret_cast<const float2*>(F + f00 + 2);
-    float2 c = *reinterpret_cast<const float2*>(F + f01), e = *reinterpret_cast<const float2*>(F + f01 + 2);
-    float u = (a.x + (b.x - a.x) * ffx) * (1.0f - ffy) + (c.x + (e.x - c.x) * ffx) * ffy;
-    float v = (a.y + (b.y - a.y) * ffx) * (1.0f - ffy) + (c.y + (e.y - c.y) * ffx) * ffy;
-    Sample s = sample_at((float)x + u * amount / P.rx, (float)y + v * amount / P.ry, P.w, P.h);
-    cx = s.ix;
-    cy = s.iy;
-}
-
 // where a side's image gradient goes: a shared tile of the CTA's box (tile != nullptr) or the
 // global gradient (vector atomics)
 struct Acc {
     float* tile;     // four planes of ADJ_BOX_PX floats (a warp's adjacent pixels on adjacent banks)
-    int bx, by, bw;
-    float* global;
+    int bx, by, bw, bh;
+    float* global;   // a cell outside the box (a NaN flow) goes here too
 };
 
 __device__ __forceinline__ void acc_add(const Acc& c, const AdjParams& P, int px, int py, float4 v) {
-    if (c.tile) {
-        float* t = c.tile + ((py - c.by) * c.bw + (px - c.bx));
+    int lx = px - c.bx, ly = py - c.by;
+    if (c.tile && lx >= 0 && lx < c.bw && ly >= 0 && ly < c.bh) {
+        float* t = c.tile + (ly * c.bw + lx);
         atomicAdd(t, v.x);
         atomicAdd(t + ADJ_BOX_PX, v.y);
         atomicAdd(t + 2 * ADJ_BOX_PX, v.z);
@@ -179,7 +165,8 @@ __device__ __forceinline__ void side_back(const float* S, const Side& d, float4 
 }  // namespace
 
 // One CTA per 32 x 32 output tile of a batch item, 256 threads, 4 pixels a thread (the columns of a
-// warp adjacent). Three passes: (1) the sample cells of both sides, reduced to their bounding boxes;
+// warp adjacent). Three passes: (1) the bounding box of each side's sample cells, from the extremes
+// of the flow texels the tile reads;
 // (2) the forward recomputed, the loss and the backward, the image gradients added into a shared
 // tile of each box (when it fits, else straight to global memory with vector atomics) and the flow
 // gradients into the shared flow tile; (3) the shared tiles added to global memory, one coalesced
@@ -216,35 +203,64 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_warp_blend_adjoint(AdjParams
     if (tiled)
         for (int i = threadIdx.x; i < FT_X * FT_Y * 2; i += blockDim.x) sflow0[i] = sflow1[i] = 0.0f;
     __syncthreads();
-    // pass 1: the cells
+    // pass 1: the boxes the samples reach, from the flow texels the tile's pixels read: the flow at
+    // a pixel is a convex combination of its footprint's texels, and every step from the flow to
+    // the sample cell is monotone, so the extremes of the texels bound the cells
+    __shared__ float ext[ADJ_THREADS / 32][2][4];  // per warp and side: min u, max u, min v, max v
     if (backward) {
-        int mn[2][2] = {{INT_MAX, INT_MAX}, {INT_MAX, INT_MAX}}, mx[2][2] = {{INT_MIN, INT_MIN}, {INT_MIN, INT_MIN}};
-        for (int j = 0; j < ADJ_TY / ROWS; j++) {
-            int y = yb + j * ROWS;
-            if (x >= P.w || y >= P.h) continue;
-            int cx, cy;
-            side_cell(Fba, P, x, y, frac, cx, cy);
-            mn[0][0] = min(mn[0][0], cx); mn[0][1] = min(mn[0][1], cy);
-            mx[0][0] = max(mx[0][0], cx); mx[0][1] = max(mx[0][1], cy);
-            side_cell(Fab, P, x, y, P.wa, cx, cy);
-            mn[1][0] = min(mn[1][0], cx); mn[1][1] = min(mn[1][1], cy);
-            mx[1][0] = max(mx[1][0], cx); mx[1][1] = max(mx[1][1], cy);
+        int xe = min(x0 + ADJ_TX - 1, P.w - 1), ye = min(y0 + ADJ_TY - 1, P.h - 1);
+        int fx0, fy0, fx1, fy1;
+        float t0, t1;
+        footprint((float)x0 * P.rx, (float)y0 * P.ry, P.fw, P.fh, fx0, fy0, t0, t1);
+        footprint((float)xe * P.rx, (float)ye * P.ry, P.fw, P.fh, fx1, fy1, t0, t1);
+        int tw = fx1 + 2 - fx0, th = fy1 + 2 - fy0;
+        float e[2][4];
+#pragma unroll
+        for (int s = 0; s < 2; s++) e[s][0] = e[s][2] = INFINITY, e[s][1] = e[s][3] = -INFINITY;
+        for (int i = threadIdx.x; i < tw * th; i += blockDim.x) {
+            long k = ((long)(fy0 + i / tw) * P.fw + fx0 + i % tw) * 2;
+            float2 f0 = *reinterpret_cast<const float2*>(Fba + k), f1 = *reinterpret_cast<const float2*>(Fab + k);
+            e[0][0] = fminf(e[0][0], f0.x); e[0][1] = fmaxf(e[0][1], f0.x);
+            e[0][2] = fminf(e[0][2], f0.y); e[0][3] = fmaxf(e[0][3], f0.y);
+            e[1][0] = fminf(e[1][0], f1.x); e[1][1] = fmaxf(e[1][1], f1.x);
+            e[1][2] = fminf(e[1][2], f1.y); e[1][3] = fmaxf(e[1][3], f1.y);
         }
 #pragma unroll
-        for (int s = 0; s < 2; s++) {
+        for (int s = 0; s < 2; s++)
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
-                mn[s][0] = min(mn[s][0], __shfl_xor_sync(0xffffffffu, mn[s][0], o));
-                mn[s][1] = min(mn[s][1], __shfl_xor_sync(0xffffffffu, mn[s][1], o));
-                mx[s][0] = max(mx[s][0], __shfl_xor_sync(0xffffffffu, mx[s][0], o));
-                mx[s][1] = max(mx[s][1], __shfl_xor_sync(0xffffffffu, mx[s][1], o));
+                e[s][0] = fminf(e[s][0], __shfl_xor_sync(0xffffffffu, e[s][0], o));
+                e[s][1] = fmaxf(e[s][1], __shfl_xor_sync(0xffffffffu, e[s][1], o));
+                e[s][2] = fminf(e[s][2], __shfl_xor_sync(0xffffffffu, e[s][2], o));
+                e[s][3] = fmaxf(e[s][3], __shfl_xor_sync(0xffffffffu, e[s][3], o));
             }
-            if ((threadIdx.x & 31) == 0) {
-                atomicMin(&box[s][0], mn[s][0]);
-                atomicMin(&box[s][1], mn[s][1]);
-                atomicMax(&box[s][2], mx[s][0]);
-                atomicMax(&box[s][3], mx[s][1]);
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+            for (int s = 0; s < 2; s++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) ext[threadIdx.x >> 5][s][k] = e[s][k];
+        __syncthreads();
+        if (threadIdx.x < 2) {
+            int s = threadIdx.x;
+            float m[4] = {INFINITY, -INFINITY, INFINITY, -INFINITY};
+            for (int wi = 0; wi < ADJ_THREADS / 32; wi++) {
+                m[0] = fminf(m[0], ext[wi][s][0]);
+                m[1] = fmaxf(m[1], ext[wi][s][1]);
+                m[2] = fminf(m[2], ext[wi][s][2]);
+                m[3] = fmaxf(m[3], ext[wi][s][3]);
             }
+            float amount = s == 0 ? frac : P.wa;
+            // the extremes of (u * amount) / r and of (v * amount) / r, as side_at forms them
+            float ua = (m[0] * amount) / P.rx, ub = (m[1] * amount) / P.rx;
+            float va = (m[2] * amount) / P.ry, vb = (m[3] * amount) / P.ry;
+            float lo_x = (float)x0 + fminf(ua, ub), hi_x = (float)xe + fmaxf(ua, ub);
+            float lo_y = (float)y0 + fminf(va, vb), hi_y = (float)ye + fmaxf(va, vb);
+            Sample a = sample_at(lo_x, lo_y, P.w, P.h), c = sample_at(hi_x, hi_y, P.w, P.h);
+            bool finite = m[0] <= m[1] && m[2] <= m[3];
+            box[s][0] = a.ix;
+            box[s][1] = a.iy;
+            box[s][2] = finite ? c.ix : a.ix - 1;  // no finite texel: an empty box, the global path
+            box[s][3] = c.iy;
         }
     }
     __syncthreads();
@@ -285,8 +301,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_warp_blend_adjoint(AdjParams
         } else {
             g = ld4(P.grad_out + img, i);
         }
-        Acc ca{shared_box[0] ? sacc0 : nullptr, box[0][0], box[0][1], bw[0], P.da ? P.da + img : nullptr};
-        Acc cb{shared_box[1] ? sacc1 : nullptr, box[1][0], box[1][1], bw[1], P.db ? P.db + img : nullptr};
+        Acc ca{shared_box[0] ? sacc0 : nullptr, box[0][0], box[0][1], bw[0], bh[0], P.da ? P.da + img : nullptr};
+        Acc cb{shared_box[1] ? sacc1 : nullptr, box[1][0], box[1][1], bw[1], bh[1], P.db ? P.db + img : nullptr};
         side_back(A, sa, scale4(g, 1.0f - frac), P, ca, sflow0, tx0, ty0, tiled, P.df_ba ? P.df_ba + flo : nullptr, frac);
         side_back(B, sb, scale4(g, frac), P, cb, sflow1, tx0, ty0, tiled, P.df_ab ? P.df_ab + flo : nullptr, P.wa);
     }
