@@ -379,6 +379,80 @@ def run_adjoint(args):
     return 0
 
 
+BATCH_SIZES = [(1280, 720), (1440, 1080), (1920, 1080), (3840, 2160)]
+BATCH_KEYS = [(0.0, 100.0, True), (48.0, 25.0, True), (96.0, 100.0, True)]
+
+
+def run_batch(args):
+    """Four clips of uneven size (1280x720, 1440x1080, 1920x1080, 3840x2160; float RGBA), the keyed
+    speed ramp 100@0e;25@48e;100@96e, in one batched call per step (tw_retime_batch_device): every
+    step renders the next 8 output frames of every clip, frames of different clips in flight
+    together. Clips generated and resident on the device."""
+    import torch
+    import twixtor_b200 as tw
+    from twixtor_b200 import synth
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    dev = tw.Device(0)
+    dev.set_stream(stream.cuda_stream)
+    per = 8
+    total = (args.warmup + args.steps) * per
+    tp = tw.TimeParams(keys=BATCH_KEYS)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda:0")
+    jobs, keep = [], []
+    for i, (w, h) in enumerate(BATCH_SIZES):
+        sels = [tw.select(tp, n, w, h) for n in range(total)]
+        nsrc = max(max(s.a, s.b) for s in sels) + 1
+        frames = synth.batch_clip_gpu(w, h, nsrc, seed=0x74570030 + i)
+        out = torch.empty(per * w * h * 4, dtype=torch.float32, device="cuda:0")
+        keep += [frames, out]
+        jobs.append(dict(settings=tw.RetimeSettings(), frames=frames.data_ptr(), nframes=nsrc, sels=sels, width=w,
+                         height=h, fmt=2, out=out.data_ptr()))
+
+    def step(k):
+        dev.retime_batch_device([dict(j, sels=j["sels"][k * per:(k + 1) * per]) for j in jobs])
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    l0 = dev.stats()["kernel_launches"]
+    with Clocks(0) as clk:
+        times = [_timed(stream, step, k, flush) for k in range(args.warmup, args.warmup + args.steps)]
+    launches = dev.stats()["kernel_launches"] - l0
+    total_ms = sum(times)
+    nframes = args.steps * per * len(jobs)
+    mpx = args.steps * per * sum(w * h for w, h in BATCH_SIZES) / 1e6
+    line = {"metric": "batched retime output frames/s, 4 clips of uneven size (strict byte-exact GPU vs CPU)",
+            "value": nframes / (total_ms / 1e3), "unit": "frames/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "retime of 1280x720, 1440x1080, 1920x1080 and 3840x2160 float RGBA clips, keyed speed "
+                                   "100@0e;25@48e;100@96e, 8 output frames of each clip per step in one batched call",
+                       "megapixels_per_s": mpx / (total_ms / 1e3), "output_frames_per_step": per * len(jobs),
+                       "l2": "flushed between steps (256 MiB write); clips resident in HBM"},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as O
+        threads = os.cpu_count() or 1
+        O.lib().or_set_threads(threads)
+        p = O.retime_params(keys=BATCH_KEYS)
+        t = time.perf_counter()
+        px = 0
+        for (w, h), j, fr in zip(BATCH_SIZES, jobs, keep[0::2]):
+            k = next(n for n, s in enumerate(j["sels"]) if not s.exact)
+            need = j["sels"][k].a + 2  # only the frames up to the pair go to the host
+            O.retime_one(fr[:need * w * h * 4].cpu().numpy(), need, w, h, 2, p, k)
+            px += w * h
+        dt = time.perf_counter() - t
+        line["cpu_baseline"] = {"value": 4 / dt, "unit": "frames/s", "cores": threads, "kind": "port",
+                                "sample": f"one in-between frame of each clip ({px / 1e6:.1f} Mpx), {dt:.2f} s on "
+                                          f"{threads} OpenMP threads", "megapixels_per_s": px / 1e6 / dt}
+    emit(line)
+    dev.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -392,9 +466,9 @@ def main():
     ap.add_argument("--breakdown", action="store_true",
                     help="after the timed region, time one more step with every kernel bracketed by events and "
                          "print the per-kernel table to stderr (not part of the reported numbers)")
-    ap.add_argument("--workload", default="retime", choices=["retime", "create-vectors", "fgbg", "adjoint"],
+    ap.add_argument("--workload", default="retime", choices=["retime", "create-vectors", "fgbg", "adjoint", "batch"],
                     help="retime (the headline, default), create-vectors (1080p 16 bpc), fgbg (1080p, 3 FG layers) or "
-                         "adjoint (warp + blend gradients, 64 triples of 1280x720)")
+                         "adjoint (warp + blend gradients, 64 triples of 1280x720) or batch (4 clips of uneven size)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -402,6 +476,8 @@ def main():
         return run_reference(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "batch":
+        return run_batch(args)
     if args.workload != "retime":
         return run_workload(args)
     if args.ncu_case and args.workload == "retime":

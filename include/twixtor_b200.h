@@ -393,6 +393,23 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
                           const float* sensitivity, const tw_selection* sels, int32_t nout, int32_t width,
                           int32_t height, int32_t fmt, void* out);
 
+/* One clip of a batch: its settings, its source frames (nframes wire frames back to back, DEVICE
+ * memory), its selections and its output (nout wire frames, DEVICE memory). */
+typedef struct tw_clip_job {
+    const tw_retime_settings* settings;
+    const void* frames;
+    int32_t nframes;
+    const tw_selection* sels;
+    int32_t nout;
+    int32_t width, height, fmt;
+    void* out;
+} tw_clip_job;
+
+/* Several clips of any sizes and depths in one call (the batched retime): the output frames of all
+ * jobs are dealt round robin over the clips onto the lanes, so frames of different clips are in
+ * flight together; each equals tw_retime_clip_device of its own clip. Returns when all are done. */
+int tw_retime_batch_device(tw_ctx* ctx, const tw_clip_job* jobs, int32_t njobs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -503,3 +503,26 @@ def test_retime_clip_device_matches_host_clip(dev):
     torch.cuda.synchronize()
     dev.retime_clip_device(tw.RetimeSettings(), d_in.data_ptr(), n, sels, w, h, 0, d_out.data_ptr())
     assert same(d_out.cpu().numpy(), host)
+
+
+def test_batch_of_uneven_clips_equals_each_clip(dev):
+    """tw_retime_batch_device: three clips of different sizes and depths in one call, frames of the
+    clips in flight together, each output equal to its own clip call."""
+    import torch
+    specs = [(96, 64, 0, 50.0), (160, 96, 2, 40.0), (64, 48, 1, 75.0)]
+    jobs, keep, want = [], [], []
+    for i, (w, h, fmt, speed) in enumerate(specs):
+        n = 8
+        frames = synth.moving_clip(w, h, n, depth={0: 8, 1: 16, 2: 32}[fmt], seed=40 + i)
+        tp = tw.TimeParams(speed_percent=speed)
+        sels = [tw.select(tp, k, w, h) for k in range(10)]
+        want.append(tw.retime_clip(dev, frames, n, w, h, fmt, tp, 10))
+        t = torch.from_numpy(frames).cuda()
+        out = torch.zeros(10 * w * h * 4, dtype=t.dtype, device="cuda")
+        keep += [t, out]
+        jobs.append(dict(settings=tw.RetimeSettings(), frames=t.data_ptr(), nframes=n, sels=sels, width=w, height=h,
+                         fmt=fmt, out=out.data_ptr()))
+    dev.set_lanes(4)
+    dev.retime_batch_device(jobs)
+    for (w, h, fmt, _), out, wnt in zip(specs, keep[1::2], want):
+        assert same(out.cpu().numpy(), wnt)

@@ -92,6 +92,12 @@ class _RetimeSettings(ctypes.Structure):
     _fields_ = [("flow", _FlowSettings), ("compose", _EngineSettings), ("motion_rows_reversed", ctypes.c_int32)]
 
 
+class _ClipJob(ctypes.Structure):
+    _fields_ = [("settings", ctypes.POINTER(_RetimeSettings)), ("frames", ctypes.c_void_p), ("nframes", ctypes.c_int32),
+                ("sels", ctypes.POINTER(_Selection)), ("nout", ctypes.c_int32), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32), ("fmt", ctypes.c_int32), ("out", ctypes.c_void_p)]
+
+
 class _VectorsSettings(ctypes.Structure):
     _fields_ = [("flow", _FlowSettings), ("max_displace", ctypes.c_float), ("rows_reversed", ctypes.c_int32)]
 
@@ -300,6 +306,7 @@ def library():
     L.tw_check_logf.argtypes = [P, P, P, ctypes.c_int64]
     L.tw_check_powf.argtypes = [P, P, P, P, ctypes.c_int64]
     L.tw_motion_blur.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, ctypes.c_float]
+    L.tw_retime_batch_device.argtypes = [P, ctypes.POINTER(_ClipJob), i32]
     L.tw_warp_blend_adjoint.argtypes = [P, P, P, P, P, i32, i32, i32, i32, i32, ctypes.c_float, P, P, P, P, P, P, P, P]
     L.tw_fill_holes.argtypes = [P, pimg, P, i32, i32]
     L.tw_from_frame.argtypes = [P, P, i32, i32, i32, P]
@@ -702,6 +709,20 @@ class Device:
                                                   _ptr(counts), _ptr(chans), _ptr(sens),
                                                   arr, len(sels), width, height, fmt, _ptr(out)))
         return out
+
+    def retime_batch_device(self, jobs):
+        """Several clips in one call (tw_retime_batch_device): ``jobs`` is a list of dicts with
+        settings (RetimeSettings), frames (device pointer), nframes, sels, width, height, fmt and out
+        (device pointer, len(sels) output frames)."""
+        keep = []
+        arr = (_ClipJob * max(len(jobs), 1))()
+        for i, j in enumerate(jobs):
+            st = j["settings"]._c()
+            sl = (_Selection * max(len(j["sels"]), 1))(*[x._c() for x in j["sels"]])
+            keep += [st, sl]
+            arr[i] = _ClipJob(ctypes.pointer(st), ctypes.c_void_p(j["frames"]), j["nframes"], sl, len(j["sels"]),
+                              j["width"], j["height"], j["fmt"], ctypes.c_void_p(j["out"]))
+        self._check(self._L.tw_retime_batch_device(self._h, arr, len(jobs)))
 
     def retime_clip_device(self, settings: RetimeSettings, frames_ptr: int, nframes: int, sels, width, height, fmt,
                            out_ptr: int):

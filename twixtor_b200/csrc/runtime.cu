@@ -2761,6 +2761,47 @@ int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* 
     return rc ? rc : rc2;
 }
 
+int tw_retime_batch_device(tw_ctx* ctx, const tw_clip_job* jobs, int32_t njobs) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!jobs || njobs < 0) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    for (int j = 0; j < njobs; j++) {
+        const tw_clip_job& J = jobs[j];
+        if (!J.settings || !J.sels || !J.frames || !J.out || J.fmt < 0 || J.fmt > 2 || J.width <= 0 || J.height <= 0 ||
+            J.nout < 0 || J.nframes < 0)
+            return ctx->fail(TW_ERR_BAD_PARAM, "batch job %d: bad argument", j);
+    }
+    // the deal: round k takes output frame k of every clip that has one, the largest frames first
+    std::vector<int> order(njobs);
+    for (int j = 0; j < njobs; j++) order[j] = j;
+    std::sort(order.begin(), order.end(), [&](int x, int y) {
+        return (long)jobs[x].width * jobs[x].height * sample_bytes(jobs[x].fmt) >
+               (long)jobs[y].width * jobs[y].height * sample_bytes(jobs[y].fmt);
+    });
+    int rounds = 0;
+    for (int j = 0; j < njobs; j++) rounds = std::max(rounds, jobs[j].nout);
+    const int nl = std::min(MAX_LANES, std::max(1, ctx->nlanes));
+    CHECK(lanes_begin(ctx, nl));
+    int rc = TW_OK;
+    long slot = 0;
+    for (int k = 0; k < rounds && rc == TW_OK; k++)
+        for (int j : order) {
+            const tw_clip_job& J = jobs[j];
+            if (k >= J.nout) continue;
+            size_t bytes = (size_t)J.width * J.height * 4 * sample_bytes(J.fmt);
+            const tw_selection& sel = J.sels[k];
+            const uint8_t* base = (const uint8_t*)J.frames;
+            const void* fa = (sel.a >= 0 && sel.a < J.nframes) ? base + (size_t)sel.a * bytes : nullptr;
+            const void* fb = (sel.b >= 0 && sel.b < J.nframes) ? base + (size_t)sel.b * bytes : nullptr;
+            rc = retime_frame_lane(ctx, ctx->lanes[slot++ % nl], *J.settings, sel, fa, fb, J.width, J.height, J.fmt,
+                                   (uint8_t*)J.out + (size_t)k * bytes);
+            if (rc) break;
+        }
+    int rc2 = lanes_end(ctx, nl);
+    return rc ? rc : rc2;
+}
+
 }  // extern "C"
 
 // =======================================================================================================

@@ -219,3 +219,43 @@ def adjoint_triples(width, height, batch, seed=0x74570005, peak=10.0):
         Ds.append(D)
     f = lambda v: np.ascontiguousarray(np.stack(v), np.float32)  # noqa: E731
     return f(As), f(Bs), f(Ms), f(Ds)
+
+
+def batch_clip_gpu(width, height, frames, seed, device="cuda:0"):
+    """The batched retime workload, generated on the GPU with torch: float RGBA in [0, 1] as wire
+    frames (planes G, B, R, A), a seeded value noise background moving at a random velocity and 3
+    to 8 textured ellipses, each moving at up to 24 px/frame (the textures wrap around). Returns a
+    flat float32 tensor of ``frames`` wire frames back to back."""
+    import torch
+    import torch.nn.functional as F
+    g = torch.Generator(device="cpu").manual_seed(seed)
+
+    def noise(cell):
+        lat = torch.rand((1, 1, height // cell + 4, width // cell + 4), generator=g)
+        return F.interpolate(lat.to(device), size=(height, width), mode="bicubic", align_corners=False)[0, 0]
+
+    bg = 0.6 * noise(48) + 0.4 * noise(12)
+    bg = ((bg - bg.mean()) / bg.std() * 0.18 + 0.5).clamp(0, 1)
+    vb = (torch.rand(2, generator=g) * 2 - 1) * 6.0
+    n_ell = int(torch.randint(3, 9, (1,), generator=g))
+    ells = []
+    for _ in range(n_ell):
+        ax, ay = (torch.rand(2, generator=g) * 0.2 + 0.06) * min(width, height)
+        cx, cy = torch.rand(1, generator=g) * width, torch.rand(1, generator=g) * height
+        ang = torch.rand(1, generator=g) * 6.2832
+        sp = torch.rand(1, generator=g) * 24.0
+        ells.append((float(ax), float(ay), float(cx), float(cy), float(sp * torch.cos(ang)), float(sp * torch.sin(ang)),
+                     noise(8).clamp(0, 1)))
+    Y, X = torch.meshgrid(torch.arange(height, device=device, dtype=torch.float32),
+                          torch.arange(width, device=device, dtype=torch.float32), indexing="ij")
+    out = torch.empty((frames, 4, height, width), device=device, dtype=torch.float32)
+    for t in range(frames):
+        lum = torch.roll(bg, shifts=(int(round(float(vb[1]) * t)), int(round(float(vb[0]) * t))), dims=(0, 1))
+        r, gg, b = lum, 0.85 * lum + 0.08, (1.0 - 0.6 * lum)
+        for ax, ay, cx, cy, vx, vy, tex in ells:
+            px, py = cx + vx * t, cy + vy * t
+            m = ((X - px) / ax) ** 2 + ((Y - py) / ay) ** 2 <= 1.0
+            tl = torch.roll(tex, shifts=(int(round(vy * t)), int(round(vx * t))), dims=(0, 1))
+            r, gg, b = torch.where(m, tl, r), torch.where(m, 0.5 * tl + 0.3, gg), torch.where(m, 1.0 - tl, b)
+        out[t, 0], out[t, 1], out[t, 2], out[t, 3] = gg, b, r, 1.0  # wire planes G, B, R, A
+    return out.reshape(-1)
