@@ -68,10 +68,12 @@ __global__ void k_interleave(const float* __restrict__ fu, const float* __restri
 
 // block matching (flow.rs:447-622): the four in-place sweeps; one CTA per row or column. The column
 // sweeps take the transposes of A, B and the field (element (x, y) at [x * h + y]).
+// both sweeps of every row (left to right, then right to left) / of every column of the transposed
+// planes (top to bottom, then bottom to top), one CTA per line, bm_smem_bytes(line) shared
 __global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
-                          float* __restrict__ fv, int w, int h, bool reverse);
+                          float* __restrict__ fv, int w, int h);
 __global__ void k_bm_cols(const float* __restrict__ AT, const float* __restrict__ BT, float* __restrict__ fuT,
-                          float* __restrict__ fvT, int w, int h, bool reverse);
+                          float* __restrict__ fvT, int w, int h);
 // two w x h planes into their h x w transposes; block (32, 8), grid (ceil(w/32), ceil(h/32))
 __global__ void k_transpose2(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ at,
                              float* __restrict__ bt, int w, int h);

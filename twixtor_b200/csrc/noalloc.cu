@@ -71,12 +71,10 @@ extern "C" int tw_block_match_noalloc(const float* a, const float* b, float* flo
     // contents never reach the result
     tw::k_deinterleave<<<g1, tb, 0, s>>>(flow, n, fu, fv);
     if (width >= 3 && height >= 3) {
-        tw::k_bm_rows<<<height - 2, tb, tw::bm_smem_bytes(width), s>>>(a, b, fu, fv, width, height, false);
-        tw::k_bm_rows<<<height - 2, tb, tw::bm_smem_bytes(width), s>>>(a, b, fu, fv, width, height, true);
+        tw::k_bm_rows<<<height - 2, tb, tw::bm_smem_bytes(width), s>>>(a, b, fu, fv, width, height);
         tw::k_transpose2<<<ga, tt, 0, s>>>(a, b, at, bt, width, height);
         tw::k_transpose2<<<ga, tt, 0, s>>>(fu, fv, ut, vt, width, height);
-        tw::k_bm_cols<<<width - 2, tb, tw::bm_smem_bytes(height), s>>>(at, bt, ut, vt, width, height, false);
-        tw::k_bm_cols<<<width - 2, tb, tw::bm_smem_bytes(height), s>>>(at, bt, ut, vt, width, height, true);
+        tw::k_bm_cols<<<width - 2, tb, tw::bm_smem_bytes(height), s>>>(at, bt, ut, vt, width, height);
         tw::k_transpose2<<<gb, tt, 0, s>>>(ut, vt, fu, fv, height, width);
     }
     tw::k_interleave<<<g1, tb, 0, s>>>(fu, fv, n, flow);

@@ -375,13 +375,11 @@ size_t pyramid_floats(const Geo& g) {
 void block_match(tw_ctx* ctx, const float* A, const float* B, const float* AT, const float* BT, float* fu, float* fv,
                  float* uT, float* vT, int w, int h) {
     if (w < 3 || h < 3) return;  // callers refuse lines above BM_MAX_LINE before any launch
-    double b = 24.0 * w * h;  // per sweep: the field read and written (8 + 8), A and B read once (4 + 4)
-    LAUNCHB(ctx, b, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, false);
-    LAUNCHB(ctx, b, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h, true);
+    double b = 24.0 * w * h;  // per launch (both sweeps): the field read and written (8 + 8), A and B read once (4 + 4)
+    LAUNCHB(ctx, b, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h);
     dim3 tb(32, 8);
     LAUNCHB(ctx, 16.0 * w * h, k_transpose2, dim3((w + 31) / 32, (h + 31) / 32), tb, 0, fu, fv, uT, vT, w, h);
-    LAUNCHB(ctx, b, k_bm_cols, w - 2, TB, bm_smem_bytes(h), AT, BT, uT, vT, w, h, false);
-    LAUNCHB(ctx, b, k_bm_cols, w - 2, TB, bm_smem_bytes(h), AT, BT, uT, vT, w, h, true);
+    LAUNCHB(ctx, b, k_bm_cols, w - 2, TB, bm_smem_bytes(h), AT, BT, uT, vT, w, h);
     LAUNCHB(ctx, 16.0 * w * h, k_transpose2, dim3((h + 31) / 32, (w + 31) / 32), tb, 0, uT, vT, fu, fv, h, w);
 }
 

@@ -341,41 +341,18 @@ __device__ __forceinline__ bool bm_accept(const float* s_a, int len, const float
     return c1 < ci;
 }
 
-// One sweep over a line. The line is the row y (COLS false: pixel (i, y)) or the column x
-// (COLS true: pixel (x, i)); len is its length. Forward sweeps run i = 1..len-2 with the
-// neighbour i - 1, reverse sweeps i = len-2..1 with the neighbour i + 1. In "sweep order"
-// position q (q = i forward, q = len-1-i reverse) both are the same forward recurrence.
-// Column sweeps take TRANSPOSED planes (A, B and the field stored column by column, element
-// (x, y) at [x * h + y]) so that a warp's lanes, which walk down one column, read contiguous memory;
-// the reference transposes its field for the same sweeps (flow.rs:583-621).
+// One sweep over a line held in shared memory (su, sv: the field along the line, updated in place;
+// s_a: the three lines of A across it). The line is the row y (COLS false: pixel (i, y)) or the
+// column x (COLS true: pixel (x, i)); len is its length. Forward sweeps run i = 1..len-2 with the
+// neighbour i - 1, reverse sweeps i = len-2..1 with the neighbour i + 1. In "sweep order" position
+// q (q = i forward, q = len-1-i reverse) both are the same forward recurrence. The in place update
+// is safe: step 4 reads only run starts, which keep their own vectors and are never written.
 template <bool COLS>
-__device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
-                        float* __restrict__ fv, int w, int h, int fixed, bool reverse) {
-    extern __shared__ float sm[];
-    const int len = COLS ? h : w;
-    float* su = sm;
-    float* sv = su + len;
-    float* c0 = sv + len;
-    float* s_a = c0 + len;        // 3 * len
-    int* jmp = (int*)(s_a + 3 * len);  // next^(2^r), ping-ponged with jmp2
-    int* jmp2 = jmp + len;
-    int* on = jmp2 + len;
-    int* wscan = on + len;        // one int per warp
+__device__ void bm_sweep(float* su, float* sv, float* c0, const float* s_a, int* jmp, int* jmp2, int* on, int* wscan,
+                         const float* __restrict__ B, int w, int h, int fixed, int len, bool reverse) {
     const float w1 = (float)(w - 1), h1 = (float)(h - 1);
-    // both layouts keep the line contiguous: row y of a row-major plane, column x of a transposed one
-    auto gidx = [&](int i) -> long { return (long)fixed * len + i; };
     auto line_of = [&](int q) -> int { return reverse ? len - 1 - q : q; };  // sweep position -> line index
-
-    for (int i = threadIdx.x; i < len; i += blockDim.x) {
-        long g = gidx(i);
-        su[i] = fu[g];
-        sv[i] = fv[g];
-        on[i] = 0;
-#pragma unroll
-        for (int o = 0; o < 3; o++)  // A at offset o-1 across the line: rows y-1..y+1, or columns x-1..x+1
-            s_a[o * len + i] = __ldg(A + (long)(fixed - 1 + o) * len + i);
-    }
-    __syncthreads();
+    for (int i = threadIdx.x; i < len; i += blockDim.x) on[i] = 0;
     // 1. c0: the cost of the current vector at every interior position, NaN where no step can happen
     for (int i = threadIdx.x; i < len; i += blockDim.x) {
         float c = __int_as_float(0x7fc00000);
@@ -433,7 +410,7 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
         jmp2 = t;
     }
     // 4. owner of each position: the last marked start at or before it (a block-wide max scan over
-    //    contiguous chunks), then the scatter of v[owner]
+    //    contiguous chunks), then v[owner] into the line
     int nt = blockDim.x;
     int chunk = (len + nt - 1) / nt;
     int lo = threadIdx.x * chunk, hi = min(lo + chunk, len);
@@ -460,9 +437,49 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
         int i = line_of(q);
         if (i >= 1 && i <= len - 2 && cur >= 0 && cur != q) {
             int o = line_of(cur);
-            fu[gidx(i)] = su[o];
-            fv[gidx(i)] = sv[o];
+            su[i] = su[o];
+            sv[i] = sv[o];
         }
+    }
+    __syncthreads();
+}
+
+// The two sweeps of a line (flow.rs:551-622: left to right then right to left, or top to bottom
+// then bottom to top), with the field, A's three lines and the chain in shared memory; the field
+// goes to global memory once, after both. Column sweeps take TRANSPOSED planes (A, B and the field
+// stored column by column, element (x, y) at [x * h + y]) so that a warp's lanes, which walk down
+// one column, read contiguous memory; the reference transposes its field for the same sweeps
+// (flow.rs:583-621).
+template <bool COLS>
+__device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
+                        float* __restrict__ fv, int w, int h, int fixed) {
+    extern __shared__ float sm[];
+    const int len = COLS ? h : w;
+    float* su = sm;
+    float* sv = su + len;
+    float* c0 = sv + len;
+    float* s_a = c0 + len;        // 3 * len
+    int* jmp = (int*)(s_a + 3 * len);  // next^(2^r), ping-ponged with jmp2
+    int* jmp2 = jmp + len;
+    int* on = jmp2 + len;
+    int* wscan = on + len;        // one int per warp
+    // both layouts keep the line contiguous: row y of a row-major plane, column x of a transposed one
+    auto gidx = [&](int i) -> long { return (long)fixed * len + i; };
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        long g = gidx(i);
+        su[i] = fu[g];
+        sv[i] = fv[g];
+#pragma unroll
+        for (int o = 0; o < 3; o++)  // A at offset o-1 across the line: rows y-1..y+1, or columns x-1..x+1
+            s_a[o * len + i] = __ldg(A + (long)(fixed - 1 + o) * len + i);
+    }
+    __syncthreads();
+    bm_sweep<COLS>(su, sv, c0, s_a, jmp, jmp2, on, wscan, B, w, h, fixed, len, false);
+    bm_sweep<COLS>(su, sv, c0, s_a, jmp, jmp2, on, wscan, B, w, h, fixed, len, true);
+    for (int i = threadIdx.x + 1; i <= len - 2; i += blockDim.x) {
+        long g = gidx(i);
+        fu[g] = su[i];
+        fv[g] = sv[i];
     }
 }
 
@@ -489,17 +506,17 @@ __global__ void k_transpose2(const float* __restrict__ a, const float* __restric
 }
 
 __global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
-                          float* __restrict__ fv, int w, int h, bool reverse) {
+                          float* __restrict__ fv, int w, int h) {
     int y = blockIdx.x + 1;  // rows 1..h-2
     if (y > h - 2) return;
-    bm_line<false>(A, B, fu, fv, w, h, y, reverse);
+    bm_line<false>(A, B, fu, fv, w, h, y);
 }
 
 __global__ void k_bm_cols(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
-                          float* __restrict__ fv, int w, int h, bool reverse) {
+                          float* __restrict__ fv, int w, int h) {
     int x = blockIdx.x + 1;  // columns 1..w-2
     if (x > w - 2) return;
-    bm_line<true>(A, B, fu, fv, w, h, x, reverse);
+    bm_line<true>(A, B, fu, fv, w, h, x);
 }
 
 }  // namespace tw
