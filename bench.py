@@ -45,7 +45,7 @@ SPEED = 40.0
 FRAMES_PER_STEP = 10
 METRIC = "1080p retime output frames/s (strict byte-exact GPU vs CPU)"
 WORKLOAD = "retime 1920x1080 8bpc RGBA, speed 40%, defaults (vectors Best, Blend, sensitivity 70)"
-ROOFLINE_KERNEL = os.environ.get("TW_ROOFLINE_KERNEL", "k_bm_rows")
+ROOFLINE_KERNEL = os.environ.get("TW_ROOFLINE_KERNEL", "k_level_iter")
 CLIP_KW = dict(seed=0x74570002, bg_velocity=(6.0, -3.0), square=240, square_start=(600.0, 400.0),
                square_velocity=(9.0, 4.0))
 
@@ -361,6 +361,9 @@ def run_adjoint(args):
               for k in range(args.steps)]
     peak, which = peaks()
     achieved = (kbytes / (kms / 1e3)) / 1e9 if kms > 0 else None
+    tr = traffic_of("k_warp_blend_adjoint")
+    if isinstance(tr, dict):
+        tr = tr["dram_bytes"] / tr["algorithmic_bytes"] * (kbytes / max(klaunch, 1))
     emit({"metric": "adjoint of warp + blend, triples/s (L1 loss, gradients for both frames and both flows)",
           "value": value, "unit": "triples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
           "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -371,7 +374,7 @@ def run_adjoint(args):
                   "d2h_bytes_per_step": 0, "note": "through the torch harness (device tensors)"},
           "gpu_launches": dev.stats()["kernel_launches"],
           "roofline": {"bound": "hbm", "kernel": "k_warp_blend_adjoint", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                       "frac": (achieved / peak) if achieved else None, "traffic": None, "peak_source": which,
+                       "frac": (achieved / peak) if achieved else None, "traffic": tr, "peak_source": which,
                        "algorithmic_bytes_per_launch": kbytes / max(klaunch, 1),
                        "avg_launch_us": 1e3 * kms / max(klaunch, 1)},
           "clocks": clk.summary()})
