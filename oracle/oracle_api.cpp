@@ -605,10 +605,11 @@ static std::vector<float> flip_matte(const std::vector<float>& m, int w, int h) 
 // Output frame n of retime-fgbg with `nfg` FG matte clips (wire frames back to back, the size and
 // format of the footage): fg_chan / fg_sens per layer (popup 1..4, sensitivity 0..100). The
 // selection is the retime time map of p (plugin 03's without the source time offset: the same at
-// equal rates); p->smart_blend carries the warping code (0 to 3). Display Twixtored Output, no
-// inverse matte shrink, no tracking points.
+// equal rates); p->smart_blend carries the warping code (0 to 3); fg_shrink the inverse matte shrink of
+// every layer (16.16 reader); display the Display popup (1, 3 to 6). No tracking points.
 int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte_clips, int nfg, const int* fg_chan,
-                       const double* fg_sens, int w, int h, int fmt, const or_retime_params* p, int n, void* out) {
+                       const double* fg_sens, const double* fg_shrink, int display, int w, int h, int fmt,
+                       const or_retime_params* p, int n, void* out) {
     // compose.rs:155-161: without FG layers (and tracking points) the plain vector path, with the
     // stage set of the effect (the Gouraud forward warps)
     if (nfg == 0) return retime_one(frames, nframes, w, h, fmt, p, n, out, true);
@@ -634,9 +635,22 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
     sel.s0 = s0; sel.s1 = s1; sel.a = a; sel.b = a + 1; sel.wa = wa; sel.exact = exact != 0;
     sel.vectors_quality = vq; sel.interp = interp;
     std::string e;
-    if (vq != 0 && !exact) {  // compose.rs:155-158: the layered vector path
+    if (display == 2) return fail(1, "the Source display composes no layer");
+    int first, last;
+    display_group(display, nfg, &first, &last);  // plugins/retime-fgbg/src/glue.rs:180
+    std::vector<float> shrink;
+    bool any_shrink = false;
+    for (int k = 0; k < nfg; k++) {
+        shrink.push_back(fixed_reader(float_to_fixed(fg_shrink[k]), 1.0f));
+        any_shrink = any_shrink || shrink.back() != 0.0f;
+    }
+    // compose.rs (layered_exact): an FG layer with a shrink clears the exactness of the position
+    if (vq != 0 && !(exact && !any_shrink)) {  // compose.rs:155-158: the layered vector path
         if (interp < 0 || interp > 2) return fail(1, "bad interpolation mode");
         LayerJob job;
+        job.shrink = shrink;
+        job.first = first;
+        job.last = last;
         for (int k = 0; k < nfg; k++) {
             std::vector<float> ma = extract_raw(fetch(matte_clips[k], a, true), fg_chan[k]);
             std::vector<float> mb = extract_raw(fetch(matte_clips[k], a + 1, true), fg_chan[k]);
@@ -660,9 +674,25 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
         int rc = compose_layers_plates(job, ar, br, &o, &e);
         if (rc) return fail(rc, e);
         result = p->rows_reversed ? rows_reversed(o) : o;
-    } else {  // compose.rs:166-169 with the full group fast path (layers.rs:177-179): the plain one
+    } else if (first == 0 && last == nfg && !any_shrink) {
+        // compose.rs:166-169 with the full group fast path (layers.rs:177-179): the plain one
         int rc = interpolate(sel, A, B, &result, &e);
         if (rc) return fail(rc, e);
+    } else if (first == last) {
+        // layers.rs:414-436: a single group display rebuilds the group's plate of each frame
+        std::vector<std::vector<float>> ma, mb;
+        for (int k = 0; k < nfg; k++) {
+            ma.push_back(extract_raw(fetch(matte_clips[k], a, true), fg_chan[k]));
+            mb.push_back(extract_raw(fetch(matte_clips[k], a + 1, true), fg_chan[k]));
+        }
+        Image ra, rb;
+        bool rev = p->rows_reversed != 0, above = p->taps_above_first != 0;
+        int rc = rebuilt_plate(A, ma, shrink, first, rev, above, &ra, &e);
+        if (!rc) rc = rebuilt_plate(B, mb, shrink, first, rev, above, &rb, &e);
+        if (!rc) rc = interpolate(sel, ra, rb, &result, &e);
+        if (rc) return fail(rc, e);
+    } else {
+        return fail(1, "the full group of an unwarped frame with an inverse matte shrink is not restated");
     }
     to_frame(result, out);
     return 0;
@@ -743,8 +773,9 @@ int or_solve_masked(const void* x_eng, const void* y_eng, int w, int h, int fmt,
 // each, FG1 first), nfg + 1 sensitivities (0..1), the selection weight / interpolation and the
 // settings; out: the engine image
 int or_compose_layers(const void* a_eng, const void* b_eng, int w, int h, int fmt, int nfg, const float* mattes_a,
-                      const float* mattes_b, const float* sens, int quality, int hiq, int above_first, int warp_mode,
-                      int video_360, int gouraud, float wa, int interp, void* out_eng) {
+                      const float* mattes_b, const float* sens, const float* shrink, int first, int last, int quality,
+                      int hiq, int above_first, int warp_mode, int video_360, int gouraud, float wa, int interp,
+                      void* out_eng) {
     Image a(w, h, (Fmt)fmt), b(w, h, (Fmt)fmt), out;
     std::memcpy(a.data(), a_eng, a.bytes());
     std::memcpy(b.data(), b_eng, b.bytes());
@@ -755,6 +786,9 @@ int or_compose_layers(const void* a_eng, const void* b_eng, int w, int h, int fm
         job.mattes_b.emplace_back(mattes_b + j * n, mattes_b + (j + 1) * n);
     }
     job.sensitivity.assign(sens, sens + nfg + 1);
+    if (shrink) job.shrink.assign(shrink, shrink + nfg);
+    job.first = first;
+    job.last = last;
     job.fs.quality = quality;
     job.fs.hiq = hiq != 0;
     job.fs.video_range_luma = video_360 != 0;

@@ -1,13 +1,15 @@
 // CPU oracle of the layered composition with plates (plugins/retime-engine/src/layers/plates.rs,
 // matte.rs) for the FG matte layers of retime-fgbg. TEST INFRASTRUCTURE ONLY (see oracle_core.h).
 //
-// Restated scope: warping codes 0 and 1, Nearest and Blend, zero inverse matte shrink (the choke
-// of the cut is then the clamp of the plane), no tracking points, no wrap-around.
+// Restated scope: warping codes 0 to 3, Nearest, Blend and Weighted Blend, the display groups and the
+// inverse matte shrink (the plugin's choke of the cut), no tracking points, no wrap-around.
 #include "oracle_layers.h"
 #include "oracle_forward.h"
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 
 #include "oracle_smart.h"
 
@@ -55,16 +57,125 @@ static float clamp_pl(float v) {  // matte.rs:350-359
     return v;
 }
 
-LPlane comp_plane(const std::vector<LPlane>& raws, int k, Fmt fmt, size_t n) {  // plates.rs:86-97
+void display_group(int display, int nfg, int* first, int* last) {  // layers.rs:120-129
+    if (display >= 3 && display <= 5) *first = *last = std::min(display - 3, nfg);
+    else if (display == 6) *first = *last = nfg;
+    else { *first = 0; *last = nfg; }
+}
+
+// matte.rs:337-341 (invert_pl_value)
+static float invert_pl_value(float v) {
+    float x = (float)(1.0 - (double)v);
+    return x > 0.999f ? 1.0f : x;
+}
+
+// matte.rs:366-385 (blur_pl): the Gaussian of radius r with the runtime's powf taps, column pass above first
+static void blur_pl(std::vector<float>& d, int w, int h, float r) {
+    if ((double)r < 0.001 || d.empty()) return;  // conv.rs:52 (BLUR_RADIUS_EPS)
+    int n = std::max((int)r + 1, 0);
+    float s3 = r / 3.0f, dd = s3 * s3, sum = 0.0f;
+    std::vector<float> k(n);
+    for (int i = 0; i < n; i++) {
+        float fi = (float)i;
+        k[i] = crt_powf(2.0f, -((fi * fi) / dd));
+        sum += k[i];
+    }
+    float den = sum * 2.0f - k[0];
+    for (float& v : k) v /= den;
+    convolve(d.data(), w, h, 1, k.data(), n, true);
+}
+
+// matte.rs:418-430 (choke_geometry): the half width r and the weight of the shrink step by a > 0
+static void choke_geometry(float a, float* r_out, float* wgt) {
+    float r = std::ceil(a + 1.0f);
+    float fr = (float)((double)r - ((double)a + 1.0));
+    if (fr < 0.01f) {
+        a = a + 0.01f;
+        r = std::ceil(a + 1.0f);
+        fr = (float)((double)r - ((double)a + 1.0));
+    }
+    *r_out = r;
+    *wgt = (float)(1.0 - (double)fr);
+}
+
+// matte.rs:441-484 (shrink_pl): one shrink step by the whole number of pixels a
+static void shrink_pl(std::vector<float>& d, int w, int h, float a) {
+    if (!(a > 0.0f) || d.empty()) return;
+    float r, wgt;
+    choke_geometry(a, &r, &wgt);
+    blur_pl(d, w, h, wgt + r);
+    long long n = (long long)r;
+    float sigma = (float)((double)r / 3.0), s2 = sigma * sigma;
+    size_t size = (size_t)(2 * n + 1);
+    std::vector<float> k(size);
+    float sum = 0.0f;
+    for (size_t j = 0; j < size; j++) {
+        float x = (float)std::llabs((long long)j - n);
+        k[j] = crt_powf(2.0f, -((x * x) / s2));
+        sum += k[j];
+    }
+    for (float& v : k) v /= sum;
+    auto tail = [&](size_t from) {
+        float acc = 0.0f;
+        for (size_t j = from; j < size; j++) acc += k[j];
+        return acc;
+    };
+    float s2sum = tail(2), s3sum = tail(3);
+    float t = (s2sum - s3sum) * wgt + s3sum;
+    double den = 1.0 - (double)t;
+    for (float& v : d) {
+        if (t > v) { v = 0.0f; continue; }
+        float o = (float)((double)(v - t) / den);
+        v = std::fabs((double)o - 1.0) < 1e-4 ? 1.0f : o;
+    }
+}
+
+void choke_pl(std::vector<float>& m, int w, int h, float amount) {  // matte.rs:280-310
+    if (!std::isfinite(amount)) return;
+    bool grow = amount < 0.0f;
+    float a = grow ? -amount : amount;
+    if (a > 65536.0f) a = 65536.0f;  // matte.rs:190 (CHOKE_MAX)
+    if (grow) for (float& v : m) v = invert_pl_value(v);
+    float lo = std::floor(a), hi = std::ceil(a);
+    if (lo == hi) {
+        shrink_pl(m, w, h, lo);
+    } else {
+        std::vector<float> c = m;
+        shrink_pl(m, w, h, lo);
+        shrink_pl(c, w, h, hi);
+        float t = a - lo;
+        for (size_t i = 0; i < m.size(); i++) {  // matte.rs:326-345 (mix_pl)
+            float x = (c[i] - m[i]) * t + m[i];
+            if (x >= 1.0f) x = 1.0f;
+            else if (0.0f > x) x = 0.0f;
+            m[i] = x;
+        }
+    }
+    if (grow) for (float& v : m) v = invert_pl_value(v);
+    for (float& v : m) v = clamp_pl(v);
+}
+
+// plates.rs:80-90 (cut_matte): the FG matte as the cut reads it, choked by minus its inverse matte shrink
+static std::vector<float> cut_matte(const LPlane& raw, float shrink, int w, int h) {
+    float kk = 1.0f / raw.white;
+    std::vector<float> v(raw.v.size());
+    for (size_t i = 0; i < v.size(); i++) v[i] = raw.v[i] * kk;
+    choke_pl(v, w, h, -shrink);
+    return v;
+}
+
+LPlane comp_plane(const std::vector<LPlane>& raws, const std::vector<float>& shrink, int k, Fmt fmt, int w,
+                  int h) {  // plates.rs:95-107
     float white = white_of(fmt);
     bool isf = fmt == F32;
+    size_t n = (size_t)w * h;
     LPlane c;
     c.white = white;
     if (k == (int)raws.size()) c.v.assign(n, white);
     else c = raws[k];
     for (int j = k - 1; j >= 0; j--) {
-        float kk = 1.0f / raws[j].white;  // plates.rs:80-85, the zero shrink: the choke is the clamp
-        for (size_t i = 0; i < n; i++) c.v[i] = cut(c.v[i], clamp_pl(raws[j].v[i] * kk), white, isf);
+        std::vector<float> v = cut_matte(raws[j], shrink.empty() ? 0.0f : shrink[j], w, h);
+        for (size_t i = 0; i < n; i++) c.v[i] = cut(c.v[i], v[i], white, isf);
     }
     return c;
 }
@@ -234,14 +345,16 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
     int code = job.cs.warp_mode;
     if (code < 0 || code > 3) { *err = "plates: warping code not 0 to 3"; return 1; }
     if (sel.interp < 0 || sel.interp > 2) { *err = "plates: bad interpolation mode"; return 1; }
-    // plates.rs:330-370: the solves, one layer after the other
+    int first = job.first, last = job.last < 0 ? nfg : job.last;
+    if (first < 0 || first > last || last > nfg) { *err = "plates: bad layer group"; return 1; }
+    // plates.rs:330-370: the solves of the group's layers, one after the other
     std::vector<FlowField> f_ab(nfg + 1), f_ba(nfg + 1);
     std::vector<bool> has_ab(nfg + 1, false), has_ba(nfg + 1, false);
-    for (int k = 0; k <= nfg; k++) {
+    for (int k = first; k <= last; k++) {
         FlowSettings fs = job.fs;
         fs.track_alpha = false;
         fs.sensitivity = job.sensitivity[k];
-        LPlane ca = comp_plane(raws_a, k, fmt, n), cb = comp_plane(raws_b, k, fmt, n);
+        LPlane ca = comp_plane(raws_a, job.shrink, k, fmt, w, h), cb = comp_plane(raws_b, job.shrink, k, fmt, w, h);
         Pyramid pa, pb;
         if (!build_pyramid(layer_times(a, ca), fs, &pa, err) || !build_pyramid(layer_times(b, cb), fs, &pb, err)) return 1;
         std::vector<float> ma, mb;
@@ -261,17 +374,17 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
         if (need_ab) { f_ab[k] = solve_pyramids_masked(pa, pb, fs, masks ? &mpa : nullptr, masks ? &mpb : nullptr, false); has_ab[k] = true; }
         if (need_ba) { f_ba[k] = solve_pyramids_masked(pb, pa, fs, masks ? &mpb : nullptr, masks ? &mpa : nullptr, false); has_ba[k] = true; }
     }
-    // plates.rs:373-412: the composition, bottom layer first
+    // plates.rs:373-412: the composition of the group, bottom layer first, over an empty image
     Image res(w, h, fmt);
-    for (int k = nfg; k >= 0; k--) {
+    for (int k = last; k >= first; k--) {
         const FlowField* fab = has_ab[k] ? &f_ab[k] : nullptr;
         const FlowField* fba = has_ba[k] ? &f_ba[k] : nullptr;
         const LPlane* pl_a = k == nfg ? nullptr : &raws_a[k];
         const LPlane* pl_b = k == nfg ? nullptr : &raws_b[k];
         const Image* fr_a = k == nfg ? &a : nullptr;
         const Image* fr_b = k == nfg ? &b : nullptr;
-        Image la = layer_times(a, comp_plane(raws_a, k, fmt, n));
-        Image lb = layer_times(b, comp_plane(raws_b, k, fmt, n));
+        Image la = layer_times(a, comp_plane(raws_a, job.shrink, k, fmt, w, h));
+        Image lb = layer_times(b, comp_plane(raws_b, job.shrink, k, fmt, w, h));
         Image r;
         if (sel.interp == 0) {
             bool takes_a = nearest_takes_a(code, sel.wa);
@@ -303,6 +416,39 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
         else over_pl(res, r);
     }
     *out = std::move(res);
+    return 0;
+}
+
+int rebuilt_plate(const Image& frame, const std::vector<std::vector<float>>& mattes, const std::vector<float>& shrink,
+                  int k, bool reversed, bool above_first, Image* out, std::string* err) {
+    int w = frame.w, h = frame.h, nfg = (int)mattes.size();
+    size_t n = (size_t)w * h;
+    std::vector<LPlane> raws;
+    for (const auto& m : mattes) raws.push_back(raw_plane(m.data(), n, frame.fmt));
+    Image l = layer_times(frame, comp_plane(raws, shrink, k, frame.fmt, w, h));
+    Image p = l;
+    over_pl(p, l);  // the degenerate plate of an exact frame: the layer image OVER itself
+    Image q = reversed ? rows_reversed(p) : p;
+    int rc;
+    if (k == nfg) {
+        Image fa = reversed ? rows_reversed(frame) : frame;
+        rc = refill(q, nullptr, &fa, above_first, err);
+    } else {
+        LPlane rp = raws[k];
+        if (reversed)
+            for (int y = 0; y < h; y++)
+                std::memcpy(&rp.v[(size_t)y * w], &raws[k].v[(size_t)(h - 1 - y) * w], sizeof(float) * w);
+        rc = refill(q, &rp, nullptr, above_first, err);
+    }
+    if (rc) return rc;
+    p = reversed ? rows_reversed(q) : q;
+    if (k == nfg) {
+        *out = std::move(p);
+        return 0;
+    }
+    Image o(w, h, frame.fmt);
+    over_pl(o, p);
+    *out = std::move(o);
     return 0;
 }
 

@@ -18,10 +18,21 @@ struct LayerJob {
     Selection sel;
     std::vector<std::vector<float>> mattes_a, mattes_b;
     std::vector<float> sensitivity;
+    std::vector<float> shrink;  // the inverse matte shrink of every FG layer (empty: all zero)
+    int first = 0, last = -1;   // the displayed group first..=last (last -1: the full group 0..=nfg)
 };
 
+// layers.rs:120-129 (LayerJob::display_group): the group of the Display popup
+void display_group(int display, int nfg, int* first, int* last);
+// matte.rs:280-310 (choke_pl), the plugin's matte choke of a w x h float plane
+void choke_pl(std::vector<float>& m, int w, int h, float amount);
+// layers.rs:497-528 (rebuilt_plate): the single group display of an unwarped frame; mattes raw (0..1)
+// in host rows; the fill runs on bottom-up rows when `reversed`
+int rebuilt_plate(const Image& frame, const std::vector<std::vector<float>>& mattes, const std::vector<float>& shrink,
+                  int k, bool reversed, bool above_first, Image* out, std::string* err);
+
 LPlane raw_plane(const float* m, size_t n, Fmt fmt);
-LPlane comp_plane(const std::vector<LPlane>& raws, int k, Fmt fmt, size_t n);
+LPlane comp_plane(const std::vector<LPlane>& raws, const std::vector<float>& shrink, int k, Fmt fmt, int w, int h);
 Image layer_times(const Image& src, const LPlane& p);
 bool solver_mask(const std::vector<LPlane>& raws, const LPlane& comp, int k, size_t n, std::vector<float>* out);
 void over_pl(Image& dest, const Image& src);

@@ -130,7 +130,8 @@ def create_vectors_grid(ref):
 
 
 FG_SERVED = {"speed_percent", "warping", "frame_interp", "blur_compensation", "fg1_matte_chan", "fg2_matte_chan", "fg3_matte_chan",
-             "fg1_sensitivity", "fg2_sensitivity", "fg3_sensitivity", "main_bg_sensitivity", "vectors"}
+             "fg1_sensitivity", "fg2_sensitivity", "fg3_sensitivity", "main_bg_sensitivity", "vectors", "display",
+             "fg1_inv_matte_shrink", "fg2_inv_matte_shrink", "fg3_inv_matte_shrink"}
 
 
 def fgbg_layers_grid(ref):
@@ -165,6 +166,8 @@ def fgbg_layers_grid(ref):
         if any(k not in FG_SERVED for k in params) or any("@" in v for v in params.values()):
             continue
         if params.get("warping", "1") not in ("1", "2", "3", "4"):
+            continue
+        if params.get("display", "1") == "2":  # the Source display composes no layer
             continue
         if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
             continue

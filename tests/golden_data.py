@@ -59,7 +59,8 @@ def fgbg_grid():
 def fgbg_case_params(case):
     """The parameters of a fgbg-layers grid case (plugin defaults where the case sets none): the
     retime selection and Main_BG settings (``smart_blend`` carries the warping code, the Warping
-    popup minus one, glue.rs:94-100), and per FG layer its channel popup and sensitivity."""
+    popup minus one, glue.rs:94-100), the Display popup, and per FG layer its channel popup,
+    sensitivity and inverse matte shrink."""
     p = dict(x.split("=", 1) for x in case["params"])
     nfg = len(case["mattes"])
     return dict(fps=(int(case["fps"]), 1), speed=float(p.get("speed_percent", 100)), vectors=int(p.get("vectors", 5)),
@@ -67,7 +68,9 @@ def fgbg_case_params(case):
                 blur=float(p.get("blur_compensation", 0)),
                 sensitivity=float(p.get("main_bg_sensitivity", 70)),
                 chans=[int(p.get(f"fg{k + 1}_matte_chan", 1)) for k in range(nfg)],
-                fg_sens=[float(p.get(f"fg{k + 1}_sensitivity", 70)) for k in range(nfg)])
+                fg_sens=[float(p.get(f"fg{k + 1}_sensitivity", 70)) for k in range(nfg)],
+                shrinks=[float(p.get(f"fg{k + 1}_inv_matte_shrink", 0)) for k in range(nfg)],
+                display=int(p.get("display", 1)))
 
 
 def cv_case_params(case):

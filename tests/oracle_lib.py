@@ -83,7 +83,7 @@ def lib():
         L.or_retime_one.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_crt_powf.argtypes = [P, P, P, i]
         L.or_motion_blur.argtypes = [P, P, i, i, i, P, i, i, f, i, f]
-        L.or_retime_fgbg_one.argtypes = [P, i, P, i, P, P, i, i, i, ctypes.POINTER(RetimeParams), i, P]
+        L.or_retime_fgbg_one.argtypes = [P, i, P, i, P, P, P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_set_threads.argtypes = [i]
         L.or_smart_blend.argtypes = [P, P, P, i, i, i, f, i]
         L.or_fill_holes.argtypes = [P, i, i, i, P, i, i]
@@ -94,7 +94,7 @@ def lib():
         L.or_fw_level_count.argtypes = [i, i]
         L.or_fw_triangle.argtypes = [P, i, i, P, i]
         L.or_logf.argtypes = [P, P, ctypes.c_long]
-        L.or_compose_layers.argtypes = [P, P, i, i, i, i, P, P, P, i, i, i, i, i, i, f, i, P]
+        L.or_compose_layers.argtypes = [P, P, i, i, i, i, P, P, P, P, i, i, i, i, i, i, i, i, f, i, P]
         L.or_mask_pyramid.argtypes = [P, i, i, i, i, i, P, P, i]
         L.or_mask_gradient.argtypes = [P, P, i, i]
         L.or_calc_b_masked.argtypes = [P, P, P, P, i, i, P, P]
@@ -275,16 +275,19 @@ def solve_masked(x, y, w, h, fmt, matte_x=None, matte_y=None, quality=4, hiq=Tru
 
 
 def compose_layers(a, b, w, h, fmt, mattes_a, mattes_b, sensitivity, wa, interp=1, quality=4, hiq=True,
-                   above_first=True, warp_mode=0, video_360=False, gouraud=False):
-    """layers/plates.rs solve_and_compose_plates of one in-between frame (engine images in and out)."""
+                   above_first=True, warp_mode=0, video_360=False, gouraud=False, shrink=None, group=None):
+    """layers/plates.rs solve_and_compose_plates of one in-between frame (engine images in and out);
+    ``shrink`` the inverse matte shrink per FG layer, ``group`` the displayed (first, last)."""
     nfg = len(mattes_a)
     ma = np.ascontiguousarray(np.concatenate(mattes_a) if nfg else np.zeros(1), np.float32)
     mb = np.ascontiguousarray(np.concatenate(mattes_b) if nfg else np.zeros(1), np.float32)
     sens = np.ascontiguousarray(sensitivity, np.float32)
+    sh = np.ascontiguousarray(list(shrink) if shrink is not None else [0.0] * max(nfg, 1), np.float32)
+    first, last = group if group is not None else (0, -1)
     out = np.zeros_like(a)
-    rc = lib().or_compose_layers(ptr(a), ptr(b), w, h, fmt, nfg, ptr(ma), ptr(mb), ptr(sens), quality, int(hiq),
-                                 int(above_first), warp_mode, int(video_360), int(gouraud), np.float32(wa), interp,
-                                 ptr(out))
+    rc = lib().or_compose_layers(ptr(a), ptr(b), w, h, fmt, nfg, ptr(ma), ptr(mb), ptr(sens), ptr(sh), first, last,
+                                 quality, int(hiq), int(above_first), warp_mode, int(video_360), int(gouraud),
+                                 np.float32(wa), interp, ptr(out))
     if rc:
         raise ValueError(err())
     return out
@@ -353,20 +356,23 @@ def retime_one(frames, nframes, w, h, fmt, params, n):
     return out
 
 
-def retime_fgbg_clip(frames, nframes, mattes, chans, sens, w, h, fmt, params, nout):
+def retime_fgbg_clip(frames, nframes, mattes, chans, sens, w, h, fmt, params, nout, shrinks=None, display=1):
     """retime-fgbg with FG matte layers (FG1 first): ``mattes`` the matte clips (nframes wire frames
-    each), ``chans`` their channel popups, ``sens`` their sensitivities 0..100; Main_BG's is
-    params.sensitivity. Output frames 0..nout-1 back to back."""
+    each), ``chans`` their channel popups, ``sens`` their sensitivities 0..100, ``shrinks`` their
+    inverse matte shrinks; Main_BG's sensitivity is params.sensitivity; ``display`` the Display
+    popup. Output frames 0..nout-1 back to back."""
     nfg = len(mattes)
     mattes = [np.ascontiguousarray(m) for m in mattes]
     arr = (ctypes.c_void_p * max(nfg, 1))(*[m.ctypes.data for m in mattes])
     ch = (ctypes.c_int * 3)(*(list(chans) + [1] * (3 - nfg)))
     se = (ctypes.c_double * 3)(*(list(sens) + [70.0] * (3 - nfg)))
+    shr = list(shrinks) if shrinks is not None else [0.0] * nfg
+    sh = (ctypes.c_double * 3)(*(shr + [0.0] * (3 - nfg)))
     fb = w * h * 4
     out = np.zeros(nout * fb, DTYPE[fmt])
     for n in range(nout):
-        rc = lib().or_retime_fgbg_one(ptr(frames), nframes, arr, nfg, ch, se, w, h, fmt, ctypes.byref(params), n,
-                                      ptr(out[n * fb:]))
+        rc = lib().or_retime_fgbg_one(ptr(frames), nframes, arr, nfg, ch, se, sh, display, w, h, fmt,
+                                      ctypes.byref(params), n, ptr(out[n * fb:]))
         if rc:
             raise ValueError(err())
     return out

@@ -214,14 +214,17 @@ FG_CASES, FG_INPUTS = golden_data.fgbg_grid()
 @pytest.mark.parametrize("case", FG_CASES, ids=[c["id"] for c in FG_CASES])
 def test_fgbg_layers_grid_sha256(case):
     """The reference's recorded output clips of the served retime-fgbg grid cases: matte channels,
-    raw and composition planes, layer images, masked solves per layer, plates, refill, OVER."""
+    raw and composition planes (with the inverse matte shrink), layer images, masked solves per
+    layer, plates, refill, OVER, the single group displays."""
     fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
     w, h, n = case["width"], case["height"], case["frames"]
     kw = golden_data.fgbg_case_params(case)
     chans, sens = kw.pop("chans"), kw.pop("fg_sens")
+    shrinks, display = kw.pop("shrinks"), kw.pop("display")
     p = O.retime_params(rows_reversed=True, taps_above_first=True, **kw)
     mattes = [FG_INPUTS[m].view(O.DTYPE[fmt]) for m in case["mattes"]]
-    out = O.retime_fgbg_clip(FG_INPUTS[case["input"]].view(O.DTYPE[fmt]), n, mattes, chans, sens, w, h, fmt, p, n)
+    out = O.retime_fgbg_clip(FG_INPUTS[case["input"]].view(O.DTYPE[fmt]), n, mattes, chans, sens, w, h, fmt, p, n,
+                             shrinks=shrinks, display=display)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
 
 
