@@ -235,19 +235,32 @@ int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* 
  * blended at w, or (binary != 0) the binary alpha composite. */
 int tw_smart_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* p1, const tw_image* p2, float w, int32_t binary);
 
+/* The FG matte layers of a layered render (layers.rs:71-129, LayerParams and LayerJob, as
+ * plugins/retime-fgbg/src/glue.rs:160-193 reads them): FG1 .. FG nfg and Main_BG. */
+typedef struct tw_layer_job {
+    int32_t nfg;            /* FG matte layers, 0 to 3 */
+    int32_t matte_chan[3];  /* fgN_matte_chan: 1 R, 2 G, 3 B, else alpha (read by tw_retime_layers_clip) */
+    float sensitivity[4];   /* 0..1 per layer, FG1 first, Main_BG at index nfg */
+    float shrink[3];        /* fgN_inv_matte_shrink in pixels (the 16.16 reader's value), at most 13 */
+    int32_t display;        /* the Display popup: 1 all layers, 3 to 5 FG1 to FG3 alone, 6 Main_BG alone
+                               (layers.rs:120-129); 2 (Source) composes no layer and is refused */
+} tw_layer_job;
+
 /* The layered composition with plates (layers/plates.rs:330-412, solve_and_compose_plates) of one
- * in-between frame of the FG matte effects: every layer (FG1 .. FG nfg, then Main_BG) solved on its
- * own layer images with its solver masks (tw_solve_masked), its plates (its layer image OVER the
- * other frame's warped to its time) refilled, the single layer composition of the warping code
- * (codes 0 to 3; Nearest, Blend or Weighted Blend), and the layers composed OVER from the bottom up. a, b: the
- * engine images (also the tracking frames); mattes_a / mattes_b: nfg raw mattes of width*height
- * floats each at A and at B, FG1 first (0..1; a float matte as it is); sensitivity: nfg + 1 values
- * (0..1), Main_BG last. nfg <= 3. The inverse matte shrink is 0 and no tracking point is in use;
- * the caller hands the images in the motion path's row order. Replaces the CPU
- * compose::retime_layers vector path for those settings. */
+ * in-between frame of the FG matte effects: every layer of the job's display group (FG1 .. FG nfg,
+ * then Main_BG) solved on its own layer images with its solver masks (tw_solve_masked), its plates
+ * (its layer image OVER the other frame's warped to its time) refilled, the single layer
+ * composition of the warping code (codes 0 to 3; Nearest, Blend or Weighted Blend), and the layers
+ * composed OVER from the bottom up, over an empty image when Main_BG is not in the group. The
+ * composition planes cut each layer by the layers above it, each choked by minus its inverse matte
+ * shrink (plates.rs:80-107, matte.rs:280-484). a, b: the engine images (also the tracking
+ * frames); mattes_a / mattes_b: nfg raw mattes of width*height floats each at A and at B, FG1
+ * first (0..1; a float matte as it is). No tracking point is in use; the caller hands the images
+ * in the motion path's row order. Replaces the CPU compose::retime_layers vector path for those
+ * settings. */
 int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection* sel, const tw_image* a,
-                      const tw_image* b, int32_t nfg, const float* mattes_a, const float* mattes_b,
-                      const float* sensitivity, tw_image_mut* out);
+                      const tw_image* b, const tw_layer_job* job, const float* mattes_a, const float* mattes_b,
+                      tw_image_mut* out);
 
 /* forward::forward_warp_with (forward.rs:229-320) with the coverage image when cov != NULL (w*h
  * bytes, 255 where a triangle covered the pixel): the displaced triangle mesh of the flow
@@ -377,21 +390,23 @@ int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* 
                           void* out);
 
 /* retime-fgbg with FG matte layers over a clip in HOST memory (plugins/retime-fgbg/src/glue.rs:
- * 275, render_temporal, with compose.rs:149-170 and layers.rs:530-567): output frame k of the
+ * 275, render_temporal, with compose.rs:149-223 and layers.rs:410-567): output frame k of the
  * selections `sels`; footage in `frames` (nframes wire frames back to back), the FG matte layers
- * FG1 .. FG nfg in matte_clips[j] (wire frames of the footage's size and format, matte_nframes[j]
- * of them, or nframes when matte_nframes is NULL), each read through its channel matte_chan[j]
- * (the popup: 1 R, 2 G, 3 B, else alpha); sensitivity: nfg + 1 values 0..1, Main_BG last. The
- * in-between frames run tw_compose_layers in the motion path's row order (rows reversed when
- * s->motion_rows_reversed), the exact frames the interpolation without flows. A frame outside a
- * clip is blank. The inverse matte shrink is 0, no tracking point is in use and the output is
- * Display Twixtored Output. s->compose.gouraud should be 1 (retime-fgbg's forward warps are the
- * Gouraud variant). nfg 0 with warping codes 0/1 is tw_retime_clip; codes 2/3 run the plain vector
- * path frame by frame on the context's stream. */
-int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes, int32_t nfg,
-                          const void* const* matte_clips, const int32_t* matte_nframes, const int32_t* matte_chan,
-                          const float* sensitivity, const tw_selection* sels, int32_t nout, int32_t width,
-                          int32_t height, int32_t fmt, void* out);
+ * FG1 .. FG job->nfg in matte_clips[j] (wire frames of the footage's size and format,
+ * matte_nframes[j] of them, or nframes when matte_nframes is NULL), each read through its channel
+ * job->matte_chan[j]. The in-between frames run tw_compose_layers in the motion path's row order
+ * (rows reversed when s->motion_rows_reversed); an FG layer with an inverse matte shrink makes
+ * every position an in-between one (compose.rs:209-211). The unwarped frames take the
+ * interpolation without flows, of the frames themselves for the full group, of the group's rebuilt
+ * plates for a single layer display (layers.rs:414-528). A frame outside a clip is blank. No
+ * tracking point is in use. s->compose.gouraud should be 1 (retime-fgbg's forward warps are the
+ * Gouraud variant). nfg 0 with warping codes 0/1 is tw_retime_clip; codes 2/3 run the plain
+ * vector path frame by frame on the context's stream. The full group of an unwarped frame with a
+ * shrink (Vectors off) is TW_ERR_UNSUPPORTED. */
+int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
+                          const tw_layer_job* job, const void* const* matte_clips, const int32_t* matte_nframes,
+                          const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt,
+                          void* out);
 
 /* One clip of a batch: its settings, its source frames (nframes wire frames back to back, DEVICE
  * memory), its selections and its output (nout wire frames, DEVICE memory). */

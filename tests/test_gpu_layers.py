@@ -51,14 +51,36 @@ def scene(w, h, fmt, nfg, seed, soft=0.0):
     return a, b, ma, mb
 
 
-def run(dev, a, b, w, h, fmt, ma, mb, sens, wa, interp, code, video_360=False, gouraud=False):
+def display_group(display, nfg):
+    """layers.rs:120-129: the layers (first, last) the Display popup composes."""
+    if 3 <= display <= 5:
+        g = min(display - 3, nfg)
+        return g, g
+    if display == 6:
+        return nfg, nfg
+    return 0, nfg
+
+
+def run(dev, a, b, w, h, fmt, ma, mb, sens, wa, interp, code, video_360=False, gouraud=False, shrink=None, display=1):
     s = tw.RetimeSettings(flow=tw.FlowSettings(video_range_luma=video_360),
                           compose=tw.EngineSettings(warp_mode=code, video_360=video_360, gouraud=gouraud))
     sel = tw.Selection(wa=np.float32(wa), exact=False, vectors_quality=4, interp=interp)
-    got = dev.compose_layers(s, sel, a, b, w, h, fmt, ma, mb, sens)
+    got = dev.compose_layers(s, sel, a, b, w, h, fmt, ma, mb, sens, shrink=shrink, display=display)
     want = O.compose_layers(a, b, w, h, fmt, ma, mb, sens, np.float32(wa), interp, warp_mode=code, video_360=video_360,
-                            gouraud=gouraud)
+                            gouraud=gouraud, shrink=shrink, group=display_group(display, len(ma)))
     assert same(got, want)
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("display", [1, 3, 4, 6])
+@pytest.mark.parametrize("shrink", [(0.0, 0.0), (2.5, 0.0), (1.0, 4.0), (-1.5, 0.5), (10.0, 0.0)])
+def test_layers_display_group_and_shrink_match_oracle(dev, fmt, display, shrink):
+    """The display groups (one layer alone over an empty image, or Main_BG alone) and the inverse
+    matte shrink of the cut planes (the plugin's choke: grow, shrink, fractional mixes), soft and
+    hard mattes."""
+    w, h = 96, 64
+    a, b, ma, mb = scene(w, h, fmt, 2, seed=21 + display, soft=3.0 if fmt == 2 else 0.0)
+    run(dev, a, b, w, h, fmt, ma, mb, [0.7, 0.6, 0.7], 0.4, 1, 1, shrink=list(shrink), display=display)
 
 
 @pytest.mark.parametrize("fmt", [0, 1, 2])
@@ -135,14 +157,16 @@ def fgbg_clip(dev, case, rows_reversed=True, taps_above_first=True):
                           motion_rows_reversed=rows_reversed)
     sens = [tw.percent_param(v) for v in kw["fg_sens"]] + [tw.percent_param(kw["sensitivity"])]
     mattes = [FG_INPUTS[m].view(tw.DTYPES[fmt]) for m in case["mattes"]]
+    shrink = [float(tw.fixed_param(v)) for v in kw["shrinks"]]
     return dev.retime_layers_clip(s, FG_INPUTS[case["input"]].view(tw.DTYPES[fmt]), n, mattes, kw["chans"], sens, sels,
-                                  w, h, fmt)
+                                  w, h, fmt, shrink=shrink, display=kw["display"])
 
 
 @pytest.mark.parametrize("case", FG_CASES, ids=[c["id"] for c in FG_CASES])
 def test_fgbg_layers_grid_sha256(dev, case):
     """Every served case of the reference's retime-fgbg grid (all four warping codes; retime-fgbg's
-    forward warps are the Gouraud variant), rendered by the CUDA path."""
+    forward warps are the Gouraud variant; the display groups and the inverse matte shrink),
+    rendered by the CUDA path."""
     out = fgbg_clip(dev, case)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
 

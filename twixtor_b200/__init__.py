@@ -98,6 +98,26 @@ class _ClipJob(ctypes.Structure):
                 ("height", ctypes.c_int32), ("fmt", ctypes.c_int32), ("out", ctypes.c_void_p)]
 
 
+class _LayerJob(ctypes.Structure):
+    _fields_ = [("nfg", ctypes.c_int32), ("matte_chan", ctypes.c_int32 * 3), ("sensitivity", ctypes.c_float * 4),
+                ("shrink", ctypes.c_float * 3), ("display", ctypes.c_int32)]
+
+
+def _layer_job(nfg, sensitivity, matte_chan=None, shrink=None, display=1):
+    """The tw_layer_job of ``nfg`` FG layers: ``sensitivity`` nfg + 1 values (Main_BG last),
+    ``matte_chan`` and ``shrink`` one value per FG layer."""
+    j = _LayerJob()
+    j.nfg = nfg
+    for k, v in enumerate(matte_chan or []):
+        j.matte_chan[k] = int(v)
+    for k, v in enumerate(sensitivity):
+        j.sensitivity[k] = float(v)
+    for k, v in enumerate(shrink or []):
+        j.shrink[k] = float(v)
+    j.display = int(display)
+    return j
+
+
 class _VectorsSettings(ctypes.Structure):
     _fields_ = [("flow", _FlowSettings), ("max_displace", ctypes.c_float), ("rows_reversed", ctypes.c_int32)]
 
@@ -295,8 +315,8 @@ def library():
     L.tw_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float]
     L.tw_smart_blend.argtypes = [P, pimg, pimg, pimg, ctypes.c_float, i32]
     L.tw_set_lanes.argtypes = [P, i32]
-    L.tw_compose_layers.argtypes = [P, ctypes.POINTER(_RetimeSettings), ctypes.POINTER(_Selection), pimg, pimg, i32, P, P, P,
-                                    pimg]
+    L.tw_compose_layers.argtypes = [P, ctypes.POINTER(_RetimeSettings), ctypes.POINTER(_Selection), pimg, pimg,
+                                    ctypes.POINTER(_LayerJob), P, P, pimg]
     L.tw_solve_masked.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), P, P, pflow]
     L.tw_forward_warp.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, P]
     L.tw_encode_vectors.argtypes = [P, pimg, pflow, ctypes.c_float]
@@ -318,7 +338,7 @@ def library():
                                  i32, i32, P]
     L.tw_retime_clip_device.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, ctypes.POINTER(_Selection), i32,
                                         i32, i32, i32, P]
-    L.tw_retime_layers_clip.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, i32, P, P, P, P,
+    L.tw_retime_layers_clip.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, ctypes.POINTER(_LayerJob), P, P,
                                         ctypes.POINTER(_Selection), i32, i32, i32, i32, P]
     _lib = L
     return L
@@ -575,20 +595,21 @@ class Device:
         return out
 
     def compose_layers(self, settings: RetimeSettings, sel: Selection, a, b, width, height, fmt, mattes_a, mattes_b,
-                       sensitivity):
+                       sensitivity, shrink=None, display=1):
         """The layered composition with plates of one in-between frame (layers/plates.rs): ``mattes_a`` /
         ``mattes_b`` the FG raw mattes at A and B (FG1 first, ``width * height`` floats each),
-        ``sensitivity`` one value per layer, Main_BG last. Returns the engine image."""
+        ``sensitivity`` one value per layer, Main_BG last, ``shrink`` the inverse matte shrink per FG
+        layer, ``display`` the Display popup (the group composed). Returns the engine image."""
         nfg = len(mattes_a)
+        job = _layer_job(nfg, sensitivity, shrink=shrink, display=display)
         out = np.zeros(width * height * 4, DTYPES[fmt])
         ai, aa = _img(a, width, height, fmt)
         bi, ba = _img(b, width, height, fmt)
         oi = _Image(width, height, fmt, out.ctypes.data)
         ma = np.ascontiguousarray(np.concatenate(mattes_a) if nfg else np.zeros(1), np.float32)
         mb = np.ascontiguousarray(np.concatenate(mattes_b) if nfg else np.zeros(1), np.float32)
-        sens = np.ascontiguousarray(sensitivity, np.float32)
         self._check(self._L.tw_compose_layers(self._h, ctypes.byref(settings._c()), ctypes.byref(sel._c()), ctypes.byref(ai),
-                                              ctypes.byref(bi), nfg, _ptr(ma), _ptr(mb), _ptr(sens), ctypes.byref(oi)))
+                                              ctypes.byref(bi), ctypes.byref(job), _ptr(ma), _ptr(mb), ctypes.byref(oi)))
         return out
 
     def set_lanes(self, lanes):
@@ -689,10 +710,11 @@ class Device:
         return out
 
     def retime_layers_clip(self, settings: RetimeSettings, frames, nframes: int, mattes, matte_chan, sensitivity, sels,
-                           width, height, fmt, matte_nframes=None, out=None):
+                           width, height, fmt, matte_nframes=None, out=None, shrink=None, display=1):
         """retime-fgbg with FG matte layers over a clip in host memory: ``mattes`` the FG1.. matte
         clips (wire frames back to back, the footage's size and format), ``matte_chan`` their channel
-        popups (1 R, 2 G, 3 B, else alpha), ``sensitivity`` one value 0..1 per layer, Main_BG last.
+        popups (1 R, 2 G, 3 B, else alpha), ``sensitivity`` one value 0..1 per layer, Main_BG last,
+        ``shrink`` the inverse matte shrink per FG layer (pixels), ``display`` the Display popup.
         Returns the output frames ``sels`` back to back."""
         frames = np.ascontiguousarray(frames)
         fs = width * height * 4
@@ -701,12 +723,11 @@ class Device:
         nfg = len(mattes)
         mattes = [np.ascontiguousarray(m) for m in mattes]
         clips = (ctypes.c_void_p * max(nfg, 1))(*[m.ctypes.data for m in mattes])
-        chans = np.ascontiguousarray(list(matte_chan) + [0], np.int32)
+        job = _layer_job(nfg, sensitivity, matte_chan=matte_chan, shrink=shrink, display=display)
         counts = None if matte_nframes is None else np.ascontiguousarray(matte_nframes, np.int32)
-        sens = np.ascontiguousarray(sensitivity, np.float32)
         arr = (_Selection * max(len(sels), 1))(*[x._c() for x in sels])
-        self._check(self._L.tw_retime_layers_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes, nfg, clips,
-                                                  _ptr(counts), _ptr(chans), _ptr(sens),
+        self._check(self._L.tw_retime_layers_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes,
+                                                  ctypes.byref(job), clips, _ptr(counts),
                                                   arr, len(sels), width, height, fmt, _ptr(out)))
         return out
 

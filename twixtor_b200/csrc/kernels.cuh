@@ -18,6 +18,13 @@ struct Taps {
     float k[MAX_TAPS];
     int n;
 };
+// the half kernels of the matte choke's blur (matte.rs:366-385: radius a + 2.01 for a shrink of a
+// pixels, n = a + 3 taps for a whole a); shrinks up to 13 pixels
+constexpr int MAX_WIDE_TAPS = 16;
+struct WideTaps {
+    float k[MAX_WIDE_TAPS];
+    int n;
+};
 
 // ---- image boundary and luma (image.rs, prep.rs) -------------------------------------------------
 // wire -> engine, optionally reading the wire rows bottom up (the motion path's row order)
@@ -36,6 +43,9 @@ __global__ void k_conv_h(const float* __restrict__ src, float* __restrict__ dst,
 // vertical pass; when band != nullptr it also writes band = orig - result (flow.rs:266-267)
 __global__ void k_conv_v(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t, bool multi,
                          bool above_first, const float* __restrict__ orig, float* __restrict__ band);
+__global__ void k_conv_h_wide(const float* __restrict__ src, float* __restrict__ dst, int w, int h, WideTaps t);
+__global__ void k_conv_v_wide(const float* __restrict__ src, float* __restrict__ dst, int w, int h, WideTaps t,
+                              bool above_first);
 __global__ void k_resample(const float* __restrict__ src, int sw, int sh, float* __restrict__ dst, int dw, int dh);
 
 // ---- solver (flow.rs:277-442) ------------------------------------------------------------------------
@@ -167,7 +177,18 @@ __global__ void k_matte_extract(const void* __restrict__ wire, int fmt, int chan
 __global__ void k_matte_out_of_range(const float* __restrict__ m, long n, int* __restrict__ flag);
 __global__ void k_raw_plane(const float* __restrict__ m, long n, int fmt, const int* __restrict__ clamp,
                             float* __restrict__ out);
-__global__ void k_comp_plane(const float* __restrict__ raws, int nfg, int k, long n, int fmt, float* __restrict__ out);
+__global__ void k_comp_plane(const float* __restrict__ raws, const float* __restrict__ cuts, int nfg, int k, long n,
+                             int fmt, float* __restrict__ out);
+// one choke of the cut (matte.rs:280-310): host scalars of its shrink steps
+struct ChokeStep {
+    bool grow, lo_blur, hi_blur, mix;
+    float t_lo, t_hi, t;     // the thresholds of the steps by lo and hi; the mix weight a - lo
+    double den_lo, den_hi;   // 1 - (double)threshold
+};
+__global__ void k_choke_base(const float* __restrict__ raw, long n, float kk, bool grow, float* __restrict__ out);
+__global__ void k_choke_finish(const float* __restrict__ base, const float* __restrict__ b_lo,
+                               const float* __restrict__ b_hi, ChokeStep st, long n, float* __restrict__ out);
+__global__ void k_flip_rows(const void* __restrict__ src, void* __restrict__ dst, int w, int h, int px);
 __global__ void k_solver_mask(const float* __restrict__ raws, int nfg, int k, const float* __restrict__ comp, long n,
                               int fmt, float* __restrict__ out);
 __global__ void k_layer_times(const void* __restrict__ src, const float* __restrict__ p, void* __restrict__ out, int fmt,
@@ -251,6 +272,8 @@ __global__ void k_wb_noflow_f32(const float* __restrict__ a, const float* __rest
 
 // ---- the image prep (prep.cu, prep.rs) ----
 __device__ float crt_powf(float x, float y);
+// the same powf on the host (the matte choke's Gaussian taps)
+float crt_powf_host(float x, float y);
 __global__ void k_delinearize(float* __restrict__ p, long n);
 __global__ void k_edge_map(const float* __restrict__ src, float* __restrict__ dst, int w, int h);
 __global__ void k_check_powf(const float* __restrict__ x, const float* __restrict__ y, float* __restrict__ out, long n);

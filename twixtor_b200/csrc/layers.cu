@@ -90,7 +90,8 @@ __device__ __forceinline__ float cut(float c, float v, float white, bool isf) {
 
 // plates.rs:86-97 with a zero inverse matte shrink (the choke of the cut is then the clamp of
 // matte.rs:350-359): layer k's composition plane; raws: nfg planes of n values, FG1 first
-__global__ void k_comp_plane(const float* __restrict__ raws, int nfg, int k, long n, int fmt, float* __restrict__ out) {
+__global__ void k_comp_plane(const float* __restrict__ raws, const float* __restrict__ cuts, int nfg, int k, long n,
+                             int fmt, float* __restrict__ out) {
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float white = white_of(fmt);
@@ -98,12 +99,75 @@ __global__ void k_comp_plane(const float* __restrict__ raws, int nfg, int k, lon
     float c = k == nfg ? white : raws[(long)k * n + i];
     float kk = 1.0f / white;
     for (int j = k - 1; j >= 0; j--) {
-        float v = x86::mul(raws[(long)j * n + i], kk);
-        if (0.0f > v) v = 0.0f;
-        else if (v >= 1.0f) v = 1.0f;
+        float v;
+        if (cuts) {
+            v = cuts[(long)j * n + i];  // the choked matte of FG j (k_choke_finish)
+        } else {  // no shrink: the choke is the clamp of the plane
+            v = x86::mul(raws[(long)j * n + i], kk);
+            if (0.0f > v) v = 0.0f;
+            else if (v >= 1.0f) v = 1.0f;
+        }
         c = cut(c, v, white, isf);
     }
     out[i] = c;
+}
+
+// ---- the plugin's matte choke of the cut (plates.rs:80-90 cut_matte, matte.rs:280-484 choke_pl) ------
+
+// matte.rs:337-341 (invert_pl_value): (f32)(1.0 - (double)v), above 0.999 1.0; a NaN stays (quieted)
+__device__ __forceinline__ float invert_pl(float v) {
+    if (isnan(v)) return nr::quiet(v);
+    float x = (float)(1.0 - (double)v);
+    return x > 0.999f ? 1.0f : x;
+}
+
+// The matte FG j as the cut reads it before the shrink steps: raw * (1 / white), inverted for a grow
+// (the cut enters the choke with minus the shrink, so a positive shrink grows the inverse).
+__global__ void k_choke_base(const float* __restrict__ raw, long n, float kk, bool grow, float* __restrict__ out) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float v = x86::mul(raw[i], kk);
+    out[i] = grow ? invert_pl(v) : v;
+}
+
+// matte.rs:471-484: the threshold map of a shrink step after its blur
+__device__ __forceinline__ float choke_threshold(float v, float t, double den) {
+    if (isnan(v)) return nr::quiet(v);
+    if (t > v) return 0.0f;
+    float o = (float)((double)(v - t) / den);
+    return fabs((double)o - 1.0) < 1e-4 ? 1.0f : o;
+}
+
+// matte.rs:280-310 after the blurs: the step by lo (blurred into b_lo, or the base itself when lo
+// shrinks nothing), the mix with the step by hi (matte.rs:326-345) when the amount is fractional,
+// the inversion back after a grow, the final clamp (matte.rs:350-359)
+__global__ void k_choke_finish(const float* __restrict__ base, const float* __restrict__ b_lo,
+                               const float* __restrict__ b_hi, ChokeStep st, long n, float* __restrict__ out) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float m = st.lo_blur ? choke_threshold(b_lo[i], st.t_lo, st.den_lo) : base[i];
+    if (st.mix) {
+        float c = st.hi_blur ? choke_threshold(b_hi[i], st.t_hi, st.den_hi) : base[i];
+        float x = x86::add(x86::mul(x86::sub(c, m), st.t), m);
+        if (x >= 1.0f) x = 1.0f;
+        else if (0.0f > x) x = 0.0f;
+        m = x;
+    }
+    if (st.grow) m = invert_pl(m);
+    if (0.0f > m) m = 0.0f;
+    else if (m >= 1.0f) m = 1.0f;
+    out[i] = m;
+}
+
+// a row flip of a w x h image of `px` bytes per pixel (px a multiple of 4), into another buffer
+__global__ void k_flip_rows(const void* __restrict__ src, void* __restrict__ dst, int w, int h, int px) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int words = px / 4;
+    long total = (long)w * h * words;
+    if (i >= total) return;
+    long row_words = (long)w * words;
+    long y = i / row_words, r = i - y * row_words;
+    ((uint32_t*)dst)[(h - 1 - y) * row_words + r] = ((const uint32_t*)src)[i];
 }
 
 // plates.rs:296-309: the solver mask of layer k, (white - (raw - comp)) / white. A mask of ones is

@@ -1810,6 +1810,25 @@ static int layers_check(tw_ctx* ctx, const tw_retime_settings& s, const tw_selec
     return TW_OK;
 }
 
+static int layer_job_check(tw_ctx* ctx, const tw_layer_job* job) {
+    if (!job || job->nfg < 0 || job->nfg > 3) return ctx->fail(TW_ERR_BAD_PARAM, "layers: a job of 0 to 3 FG layers");
+    if (job->display == 2) return ctx->fail(TW_ERR_BAD_PARAM, "layers: the Source display composes no layer");
+    return TW_OK;
+}
+
+// layers.rs:120-129 (LayerJob::display_group): the group first..=last the Display popup shows
+static void display_group(int display, int nfg, int* first, int* last) {
+    if (display >= 3 && display <= 5) *first = *last = std::min(display - 3, nfg);
+    else if (display == 6) *first = *last = nfg;
+    else { *first = 0; *last = nfg; }
+}
+
+static bool any_shrink(const tw_layer_job& job) {
+    for (int j = 0; j < job.nfg; j++)
+        if (job.shrink[j] != 0.0f) return true;
+    return false;
+}
+
 // The state a layered frame leaves in the flags, read after the stream is drained.
 static int layers_status(tw_ctx* ctx) {
     int hf[4];
@@ -1820,14 +1839,159 @@ static int layers_status(tw_ctx* ctx) {
     return TW_OK;
 }
 
+// matte.rs:418-430 (choke_geometry): the half width r and the weight of the shrink step by a > 0
+static void choke_geometry(float a, float* r_out, float* wgt) {
+    float r = std::ceil(a + 1.0f);
+    float fr = (float)((double)r - ((double)a + 1.0));
+    if (fr < 0.01f) {
+        a = a + 0.01f;
+        r = std::ceil(a + 1.0f);
+        fr = (float)((double)r - ((double)a + 1.0));
+    }
+    *r_out = r;
+    *wgt = (float)(1.0 - (double)fr);
+}
+
+// The host scalars of one shrink step by the whole number of pixels a (matte.rs:366-385 blur_pl and
+// 441-484 shrink_pl): the half kernel of its blur and its threshold, both from the runtime's powf.
+struct ShrinkStep {
+    bool blur = false;
+    WideTaps taps{};
+    float t = 0.0f;
+    double den = 1.0;
+};
+
+static int shrink_step(tw_ctx* ctx, float a, ShrinkStep* st) {
+    if (!(a > 0.0f)) return TW_OK;  // a step by 0 is the identity
+    float r, wgt;
+    choke_geometry(a, &r, &wgt);
+    float radius = wgt + r;  // at least 2: the blur always runs
+    int n = std::max((int)radius + 1, 0);
+    if (n > MAX_WIDE_TAPS)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "layers: an inverse matte shrink of %g pixels (at most 13 on the device)",
+                         (double)a);
+    float s3 = radius / 3.0f, d = s3 * s3, sum = 0.0f;
+    for (int i = 0; i < n; i++) {
+        float fi = (float)i;
+        st->taps.k[i] = crt_powf_host(2.0f, -((fi * fi) / d));
+        sum += st->taps.k[i];
+    }
+    float den = sum * 2.0f - st->taps.k[0];
+    for (int i = 0; i < n; i++) st->taps.k[i] /= den;
+    st->taps.n = n;
+    long long hn = (long long)r;
+    float sigma = (float)((double)r / 3.0), s2 = sigma * sigma;
+    std::vector<float> k((size_t)(2 * hn + 1));
+    float ksum = 0.0f;
+    for (size_t j = 0; j < k.size(); j++) {
+        float x = (float)std::llabs((long long)j - hn);
+        k[j] = crt_powf_host(2.0f, -((x * x) / s2));
+        ksum += k[j];
+    }
+    for (float& v : k) v /= ksum;
+    auto tail = [&](size_t from) {
+        float acc = 0.0f;
+        for (size_t j = from; j < k.size(); j++) acc += k[j];
+        return acc;
+    };
+    float s2sum = tail(2), s3sum = tail(3);
+    st->t = (s2sum - s3sum) * wgt + s3sum;
+    st->den = 1.0 - (double)st->t;
+    st->blur = true;
+    return TW_OK;
+}
+
+// plates.rs:80-90 (cut_matte): FG j's raw plane `raw` (units of the depth) as the cut reads it, the
+// plugin's choke by minus its inverse matte shrink (matte.rs:280-310) in the row order given, into
+// `out`; scr: 4 planes of scratch.
+static int choke_dev(tw_ctx* ctx, const float* raw, int W, int H, int fmt, float shrink, float* out, float* scr) {
+    long n = (long)W * H;
+    float white = fmt == TW_U8 ? 255.0f : fmt == TW_U16 ? 65535.0f : 1.0f;
+    float kk = 1.0f / white;
+    float amount = -shrink;
+    float* base = scr;
+    float* tmp = scr + n;
+    float* b_lo = scr + 2 * n;
+    float* b_hi = scr + 3 * n;
+    if (!std::isfinite(amount)) {  // matte.rs:282-284: the plane as it is, not even clamped
+        LAUNCH(ctx, k_choke_base, grid1(n), TB, 0, raw, n, kk, false, out);
+        return TW_OK;
+    }
+    ChokeStep st{};
+    st.grow = amount < 0.0f;
+    float a = st.grow ? -amount : amount;
+    if (a > 65536.0f) a = 65536.0f;  // matte.rs:190 (CHOKE_MAX)
+    float lo = std::floor(a), hi = std::ceil(a);
+    ShrinkStep s_lo, s_hi;
+    CHECK(shrink_step(ctx, lo, &s_lo));
+    st.mix = lo != hi;
+    if (st.mix) CHECK(shrink_step(ctx, hi, &s_hi));
+    st.lo_blur = s_lo.blur;
+    st.hi_blur = st.mix && s_hi.blur;
+    st.t_lo = s_lo.t;
+    st.den_lo = s_lo.den;
+    st.t_hi = s_hi.t;
+    st.den_hi = s_hi.den;
+    st.t = a - lo;
+    LAUNCH(ctx, k_choke_base, grid1(n), TB, 0, raw, n, kk, st.grow, base);
+    // blur_pl: the separable Gaussian with the column pass above first (conv.rs:598-615)
+    if (st.lo_blur) {
+        LAUNCH(ctx, k_conv_h_wide, grid2(W, H), TB, 0, (const float*)base, tmp, W, H, s_lo.taps);
+        LAUNCH(ctx, k_conv_v_wide, grid2(W, H), TB, 0, (const float*)tmp, b_lo, W, H, s_lo.taps, true);
+    }
+    if (st.hi_blur) {
+        LAUNCH(ctx, k_conv_h_wide, grid2(W, H), TB, 0, (const float*)base, tmp, W, H, s_hi.taps);
+        LAUNCH(ctx, k_conv_v_wide, grid2(W, H), TB, 0, (const float*)tmp, b_hi, W, H, s_hi.taps, true);
+    }
+    LAUNCH(ctx, k_choke_finish, grid1(n), TB, 0, (const float*)base, (const float*)b_lo, (const float*)b_hi, st, n, out);
+    return TW_OK;
+}
+
+// plates.rs:50-57: the raw planes of one side (each matte clamped when one of its values leaves
+// 0..1) and, when a layer has an inverse matte shrink, the choked cut planes of every FG layer
+static int raw_and_cut_planes(tw_ctx* ctx, const tw_layer_job& job, const float* mat, int side, int W, int H, int fmt,
+                              float* raw, float* cuts, float* scr, int* range_flags) {
+    long n = (long)W * H;
+    int nfg = job.nfg;
+    for (int j = 0; j < nfg; j++) {
+        const float* m = mat + ((size_t)side * nfg + j) * n;
+        int* fl_ = range_flags + side * 4 + j;
+        LAUNCH(ctx, k_matte_out_of_range, grid1(n), TB, 0, m, n, fl_);
+        LAUNCH(ctx, k_raw_plane, grid1(n), TB, 0, m, n, fmt, fl_, raw + (size_t)j * n);
+    }
+    if (cuts)
+        for (int j = 0; j < nfg; j++) CHECK(choke_dev(ctx, raw + (size_t)j * n, W, H, fmt, job.shrink[j], cuts + (size_t)j * n, scr));
+    return TW_OK;
+}
+
+// plates.rs:245-256 (refill) of the plate p of layer k at one side: unpremultiply, the pull-push fill
+// where the plate is not opaque, the alpha replaced by the layer's raw plane (plane) or the frame's
+// alpha (frame), premultiply
+static int refill_dev(tw_ctx* ctx, void* p, int W, int H, int fmt, const float* plane, const void* frame,
+                      bool above_first, int* flags, DevBuf& fillbuf) {
+    long n = (long)W * H;
+    CHECK(ctx->cuda(cudaMemsetAsync(flags + FL_HOLE, 0, sizeof(int), ctx->cur), "holes flag"));
+    LAUNCH(ctx, k_refill_pre, grid1(n), TB, 0, p, fmt, n, ctx->holes.as<uint8_t>(), flags + FL_HOLE);
+    if (W < 2 || H < 2) LAUNCH(ctx, k_hole_side1, 1, 1, 0, flags + FL_HOLE, flags + FL_SIDE1);
+    else CHECK(fill_dev(ctx, p, W, H, fmt, ctx->holes.as<uint8_t>(), flags + FL_HOLE, above_first, fillbuf));
+    LAUNCH(ctx, k_refill_post, grid1(n), TB, 0, p, fmt, n, plane, frame);
+    return TW_OK;
+}
+
 // One layered frame on ctx->stream: the engine images A and B in ctx->eng[0] / ctx->eng[1] (motion
-// row order), `mat` the 2 x nfg raw mattes on the device (A's, then B's; FG1 first), sensitivity
-// nfg + 1 host values. Clears the flags first; *res_out receives the engine result (device).
-static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel_, int nfg, const float* mat,
-                      const float* sensitivity, int W, int H, int fmt, void** res_out) {
+// row order), `mat` the 2 x nfg raw mattes on the device (A's, then B's; FG1 first). The layers of
+// the job's display group are solved and composed. Clears the flags first; *res_out receives the
+// engine result (device).
+static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel_, const tw_layer_job& job,
+                      const float* mat, int W, int H, int fmt, void** res_out) {
     const tw_selection* sel = &sel_;
     const tw_engine_settings& cs = s.compose;
     CHECK(layers_check(ctx, s, sel_));
+    CHECK(layer_job_check(ctx, &job));
+    int nfg = job.nfg;
+    int first, last;
+    display_group(job.display, nfg, &first, &last);
+    bool shrink = any_shrink(job);
     long n = (long)W * H;
     size_t px = 4 * sample_bytes(fmt), ib = (size_t)n * px;
     tw_flow_settings fs0 = s.flow;
@@ -1838,19 +2002,21 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     size_t pf = pyramid_floats(g);
     size_t fb = (size_t)g.w * g.h * 2;
     int L = nfg + 1;
-    // one block: raw planes (2 sides x nfg), comp planes (2 x L), a solver matte, layer images
-    // (2 x L), two plates, the result, the flows (2 x L), pyramids and mask pyramids (2 each)
+    // one block: raw and cut planes (2 sides x nfg), comp planes (2 x L), a solver matte, layer
+    // images (2 x L), two plates, the result, the flows (2 x L), pyramids and mask pyramids (2
+    // each), scratch
     size_t fl = 0;
     auto take = [&](size_t floats) { size_t o = fl; fl += (floats + 63) & ~(size_t)63; return o; };
-    size_t o_raw = take(2 * (size_t)nfg * n), o_comp = take(2 * (size_t)L * n);
+    size_t o_raw = take(2 * (size_t)nfg * n), o_cut = take(shrink ? 2 * (size_t)nfg * n : 0), o_comp = take(2 * (size_t)L * n);
     size_t o_smat = take(2 * (size_t)n), o_img = take(2 * (size_t)L * ib / 4 + 1), o_plate = take(2 * ib / 4 + 1);
     size_t o_res = take(ib / 4 + 1), o_flow = take(2 * (size_t)L * fb), o_pyr = take(4 * pf), o_mpyr = take(2 * pf);
-    size_t o_scr = take(2 * (size_t)n);
+    size_t o_scr = take(4 * (size_t)n);
     CHECK(ctx->ensure(ctx->lay_mem, fl * sizeof(float), "layer buffers"));
     CHECK(ctx->ensure(ctx->holes, (size_t)n, "holes mask"));
     CHECK(ctx->ensure(ctx->eng[2], ib, "layer result"));
     float* M = ctx->lay_mem.as<float>();
     float* raw = M + o_raw;
+    float* cuts = shrink ? M + o_cut : nullptr;
     float* comp = M + o_comp;
     float* smat = M + o_smat;
     auto img = [&](int side, int k) { return (void*)((char*)(M + o_img) + ((size_t)side * L + k) * ib); };
@@ -1864,19 +2030,17 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
     CHECK(ctx->cuda(cudaMemsetAsync(flags + FL_ONE, 0x01, sizeof(int), ctx->stream), "flags"));
     const void* frame[2] = {ctx->eng[0].p, ctx->eng[1].p};
-    // plates.rs:50-57: the raw planes (each matte clamped when one of its values leaves 0..1)
+    // the raw planes, the cut planes of a shrink (in the motion path's rows, as the plates run), the
+    // per-level range flags are not in use yet
     for (int side = 0; side < 2; side++)
-        for (int j = 0; j < nfg; j++) {
-            const float* m = mat + ((size_t)side * nfg + j) * n;
-            int* fl_ = flags + FL_ANY0 + side * 4 + j;  // the per-level range flags are not in use yet
-            LAUNCH(ctx, k_matte_out_of_range, grid1(n), TB, 0, m, n, fl_);
-            LAUNCH(ctx, k_raw_plane, grid1(n), TB, 0, m, n, fmt, fl_, raw + ((size_t)side * nfg + j) * n);
-        }
-    // the composition planes and the layer images of every layer at both sides
+        CHECK(raw_and_cut_planes(ctx, job, mat, side, W, H, fmt, raw + (size_t)side * nfg * n,
+                                 cuts ? cuts + (size_t)side * nfg * n : nullptr, scr, flags + FL_ANY0));
+    // the composition planes and the layer images of the group's layers at both sides
     for (int side = 0; side < 2; side++)
-        for (int k = 0; k < L; k++) {
+        for (int k = first; k <= last; k++) {
             float* c = comp + ((size_t)side * L + k) * n;
-            LAUNCH(ctx, k_comp_plane, grid1(n), TB, 0, raw + (size_t)side * nfg * n, nfg, k, n, fmt, c);
+            LAUNCH(ctx, k_comp_plane, grid1(n), TB, 0, raw + (size_t)side * nfg * n,
+                   cuts ? (const float*)(cuts + (size_t)side * nfg * n) : (const float*)nullptr, nfg, k, n, fmt, c);
             LAUNCH(ctx, k_layer_times, grid1(n), TB, 0, frame[side], c, img(side, k), fmt, n);
         }
     // the solves (plates.rs:340-369): each layer's own layer images, masked by its solver masks
@@ -1886,9 +2050,9 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
         need_ab = use_ab;
         need_ba = !use_ab;
     }
-    for (int k = 0; k < L; k++) {
+    for (int k = first; k <= last; k++) {
         tw_flow_settings fs = fs0;
-        fs.sensitivity = sensitivity[k];
+        fs.sensitivity = job.sensitivity[k];
         Geo gk;
         CHECK(geometry(fs, W, H, &gk, &ctx->err));
         for (int side = 0; side < 2; side++) {
@@ -1904,21 +2068,17 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
             CHECK(solve_pyramids_dev(ctx, pyr[1], pyr[0], pyr[1] + pf, pyr[0] + pf, gk, fs, ctx->work[0], flow(1, k),
                                      flags + FL_ANY1, flags + FL_NAN, mpyr[1], mpyr[0]));
     }
-    // the composition, bottom layer first (plates.rs:373-412)
+    // the composition of the group, bottom layer first, over an empty image (plates.rs:373-412)
     WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
     SmartScratch ss{nullptr, &ctx->fill, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB, &ctx->pre_blur};
     DevBuf& fillbuf = ctx->work[1];
     ss.holes = &ctx->masks;  // the composition's own holes mask (the refill uses ctx->holes)
     auto refill = [&](void* p, int side, int k) -> int {
-        CHECK(ctx->cuda(cudaMemsetAsync(flags + FL_HOLE, 0, sizeof(int), ctx->cur), "holes flag"));
-        LAUNCH(ctx, k_refill_pre, grid1(n), TB, 0, p, fmt, n, ctx->holes.as<uint8_t>(), flags + FL_HOLE);
-        if (W < 2 || H < 2) LAUNCH(ctx, k_hole_side1, 1, 1, 0, flags + FL_HOLE, flags + FL_SIDE1);
-        else CHECK(fill_dev(ctx, p, W, H, fmt, ctx->holes.as<uint8_t>(), flags + FL_HOLE, cs.taps_above_first != 0, fillbuf));
         const float* plane = k == nfg ? nullptr : raw + ((size_t)side * nfg + k) * n;
-        LAUNCH(ctx, k_refill_post, grid1(n), TB, 0, p, fmt, n, plane, frame[side]);
-        return TW_OK;
+        return refill_dev(ctx, p, W, H, fmt, plane, frame[side], cs.taps_above_first != 0, flags, fillbuf);
     };
-    for (int k = nfg; k >= 0; k--) {
+    if (last != nfg) CHECK(ctx->cuda(cudaMemsetAsync(res, 0, ib, ctx->stream), "empty result"));
+    for (int k = last; k >= first; k--) {
         const float* fab = need_ab ? flow(0, k) : nullptr;
         const float* fba = need_ba ? flow(1, k) : nullptr;
         void* dst = k == nfg ? res : ctx->eng[2].p;
@@ -1955,14 +2115,86 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     return TW_OK;
 }
 
+// layers.rs:414-436 and 497-528 (rebuilt_plate): a single group display of an unwarped frame. For
+// each side the group's layer image (host rows: the frames in ctx->eng[0] / [1] and the raw mattes
+// `mat` as the host delivers them) OVER itself, refilled in the rows of the motion path (`reversed`)
+// and, for an FG layer, laid OVER an empty image; then the interpolation without flows into the wire
+// frame `out`. Clears the flags first.
+static int rebuilt_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel, const tw_layer_job& job,
+                             const float* mat, int W, int H, int fmt, void* out) {
+    CHECK(layer_job_check(ctx, &job));
+    int nfg = job.nfg, k, last;
+    display_group(job.display, nfg, &k, &last);
+    if (k != last) return ctx->fail(TW_ERR_UNSUPPORTED, "layers: the full group of an unwarped frame with a shrink");
+    bool shrink = any_shrink(job), reversed = s.motion_rows_reversed != 0;
+    long n = (long)W * H;
+    size_t px = 4 * sample_bytes(fmt), ib = (size_t)n * px;
+    size_t fl = 0;
+    auto take = [&](size_t floats) { size_t o = fl; fl += (floats + 63) & ~(size_t)63; return o; };
+    size_t o_raw = take((size_t)nfg * n), o_cut = take(shrink ? (size_t)nfg * n : 0), o_comp = take((size_t)n);
+    size_t o_l = take(ib / 4 + 1), o_p = take(ib / 4 + 1), o_q = take(ib / 4 + 1), o_alpha = take(ib / 4 + 1);
+    size_t o_r = take(2 * (ib / 4 + 1)), o_scr = take(4 * (size_t)n);
+    CHECK(ctx->ensure(ctx->lay_mem, fl * sizeof(float), "layer buffers"));
+    CHECK(ctx->ensure(ctx->holes, (size_t)n, "holes mask"));
+    float* M = ctx->lay_mem.as<float>();
+    float* raw = M + o_raw;
+    float* cuts = shrink ? M + o_cut : nullptr;
+    float* comp = M + o_comp;
+    void* l = M + o_l;
+    void* p = M + o_p;
+    void* q = M + o_q;
+    void* alpha = M + o_alpha;
+    void* r[2] = {(void*)(M + o_r), (void*)(M + o_r + (ib / 4 + 1))};
+    float* scr = M + o_scr;
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
+    const void* frame[2] = {ctx->eng[0].p, ctx->eng[1].p};
+    for (int side = 0; side < 2; side++) {
+        CHECK(raw_and_cut_planes(ctx, job, mat, side, W, H, fmt, raw, cuts, scr, flags + FL_ANY0));
+        LAUNCH(ctx, k_comp_plane, grid1(n), TB, 0, raw, (const float*)cuts, nfg, k, n, fmt, comp);
+        LAUNCH(ctx, k_layer_times, grid1(n), TB, 0, frame[side], comp, l, fmt, n);
+        CHECK(ctx->cuda(cudaMemcpyAsync(p, l, ib, cudaMemcpyDeviceToDevice, ctx->stream), "plate"));
+        LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, p, l, fmt, n);  // the degenerate plate: LA OVER LA
+        void* fillme = p;
+        const float* plane = k == nfg ? nullptr : raw + (size_t)k * n;
+        const void* fa = frame[side];
+        if (reversed) {
+            LAUNCH(ctx, k_flip_rows, grid1(n * (long)(px / 4)), TB, 0, (const void*)p, q, W, H, (int)px);
+            if (k == nfg) {
+                LAUNCH(ctx, k_flip_rows, grid1(n * (long)(px / 4)), TB, 0, frame[side], alpha, W, H, (int)px);
+                fa = alpha;
+            } else {
+                LAUNCH(ctx, k_flip_rows, grid1(n), TB, 0, (const void*)plane, alpha, W, H, 4);
+                plane = (const float*)alpha;
+            }
+            fillme = q;
+        }
+        CHECK(refill_dev(ctx, fillme, W, H, fmt, k == nfg ? nullptr : plane, k == nfg ? fa : nullptr,
+                         s.compose.taps_above_first != 0, flags, ctx->work[1]));
+        if (reversed) LAUNCH(ctx, k_flip_rows, grid1(n * (long)(px / 4)), TB, 0, (const void*)q, p, W, H, (int)px);
+        if (k == nfg) {
+            CHECK(ctx->cuda(cudaMemcpyAsync(r[side], p, ib, cudaMemcpyDeviceToDevice, ctx->stream), "plate"));
+        } else {
+            CHECK(ctx->cuda(cudaMemsetAsync(r[side], 0, ib, ctx->stream), "empty layer"));
+            LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, r[side], p, fmt, n);
+        }
+    }
+    WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
+    SmartScratch ss{&ctx->eng[2], &ctx->masks, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
+    return interpolate_dev(ctx, sel, r[0], r[1], W, H, fmt, out, true, flags + FL_BAD, &ss);
+}
+
 int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection* sel, const tw_image* a,
-                      const tw_image* b, int32_t nfg, const float* mattes_a, const float* mattes_b,
-                      const float* sensitivity, tw_image_mut* out) {
+                      const tw_image* b, const tw_layer_job* job, const float* mattes_a, const float* mattes_b,
+                      tw_image_mut* out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cur = ctx->stream;
-    if (!s || !sel || !sensitivity || !out || !out->data || nfg < 0 || nfg > 3 || (nfg > 0 && (!mattes_a || !mattes_b)))
+    if (!s || !sel || !job || !out || !out->data)
         return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    CHECK(layer_job_check(ctx, job));
+    int nfg = job->nfg;
+    if (nfg > 0 && (!mattes_a || !mattes_b)) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument: no mattes");
     CHECK(check_image(ctx, a, "layers"));
     CHECK(check_image(ctx, b, "layers"));
     if (!same_shape(a, b) || out->width != a->width || out->height != a->height || out->fmt != a->fmt)
@@ -1981,7 +2213,7 @@ int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selecti
                                         cudaMemcpyHostToDevice, ctx->stream), "matte upload"));
     }
     void* res = nullptr;
-    CHECK(layers_dev(ctx, *s, *sel, nfg, mat, sensitivity, W, H, fmt, &res));
+    CHECK(layers_dev(ctx, *s, *sel, *job, mat, W, H, fmt, &res));
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, res, ib, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     return layers_status(ctx);
 }
@@ -2561,18 +2793,23 @@ static int vector_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_s
 // matte frames are uploaded, the in-between frames run the layered path in the motion path's row
 // order and the exact frames the interpolation without flows (the full group fast path,
 // layers.rs:177-179), each frame on the context's stream.
-int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes, int32_t nfg,
-                          const void* const* matte_clips, const int32_t* matte_nframes, const int32_t* matte_chan,
-                          const float* sensitivity, const tw_selection* sels, int32_t nout, int32_t width,
-                          int32_t height, int32_t fmt, void* out) {
+int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
+                          const tw_layer_job* job, const void* const* matte_clips, const int32_t* matte_nframes,
+                          const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
-    if (nfg == 0 && sels && s && s->compose.warp_mode < 2)
+    if (job && job->nfg == 0 && job->display != 2 && sels && s && s->compose.warp_mode < 2)
         return tw_retime_clip(ctx, s, frames, nframes, sels, nout, width, height, fmt, out);
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cur = ctx->stream;
-    if (!s || !sels || !frames || !out || !sensitivity || !matte_clips || !matte_chan || nfg < 0 || nfg > 3 || fmt < 0 ||
-        fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
+    if (!s || !sels || !frames || !out || !job || (job->nfg > 0 && !matte_clips) || fmt < 0 || fmt > 2 || width <= 0 ||
+        height <= 0 || nout < 0 || nframes < 0)
         return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    CHECK(layer_job_check(ctx, job));
+    int nfg = job->nfg;
+    const int32_t* matte_chan = job->matte_chan;
+    int first, last;
+    display_group(job->display, nfg, &first, &last);
+    bool shrink = any_shrink(*job);
     for (int j = 0; j < nfg; j++)
         if (!matte_clips[j] || (matte_nframes && matte_nframes[j] < 0)) return ctx->fail(TW_ERR_BAD_PARAM, "bad matte clip");
     int W = width, H = height;
@@ -2591,31 +2828,41 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
                                              ctx->stream), "upload");
         return ctx->cuda(cudaMemsetAsync(dst, 0, bytes, ctx->stream), "blank");
     };
+    // a frame's FG mattes at A and at B, read straight (matte.rs:141-188) in the row order given
+    auto mattes = [&](const tw_selection& sel, bool flip) -> int {
+        for (int side = 0; side < 2; side++)
+            for (int j = 0; j < nfg; j++) {
+                int count = matte_nframes ? matte_nframes[j] : nframes;
+                CHECK(upload(matte_clips[j], count, side ? sel.b : sel.a, ctx->wire[2].p));
+                LAUNCH(ctx, k_matte_extract, grid1(n), TB, 0, ctx->wire[2].p, fmt, matte_chan[j], W, H, flip,
+                       mat + ((size_t)side * nfg + j) * n);
+            }
+        return TW_OK;
+    };
     for (int k = 0; k < nout; k++) {
         const tw_selection& sel = sels[k];
-        bool vector = sel.vectors_quality != 0 && !sel.exact;
+        // compose.rs:209-211 (layered_exact): with FG layers, a shrink clears the exactness of a position
+        bool exact = sel.exact && !(nfg > 0 && shrink);
+        bool vector = sel.vectors_quality != 0 && !exact;
         bool flip = vector && s->motion_rows_reversed != 0;
         CHECK(upload(frames, nframes, sel.a, ctx->wire[0].p));
         CHECK(upload(frames, nframes, sel.b, ctx->wire[1].p));
         from_frame_dev(ctx, ctx->wire[0].p, ctx->eng[0].p, W, H, fmt, flip);
         from_frame_dev(ctx, ctx->wire[1].p, ctx->eng[1].p, W, H, fmt, flip);
         uint8_t* dst = (uint8_t*)out + (size_t)k * bytes;
-        if (!vector) {
+        if (!vector && nfg > 0 && !(first == 0 && last == nfg && !shrink)) {
+            // layers.rs:414-436: a single group display of an unwarped frame rebuilds its plates
+            CHECK(mattes(sel, false));
+            CHECK(rebuilt_frame_dev(ctx, *s, sel, *job, mat, W, H, fmt, ctx->wire[2].p));
+        } else if (!vector) {
             CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
             WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
             SmartScratch ss{&ctx->eng[2], &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
             CHECK(interpolate_dev(ctx, sel, ctx->eng[0].p, ctx->eng[1].p, W, H, fmt, ctx->wire[2].p, true, flags + FL_BAD, &ss));
         } else {
-            // matte.rs:141-188: each layer's raw matte at A and at B read straight, in the same row order
-            for (int side = 0; side < 2; side++)
-                for (int j = 0; j < nfg; j++) {
-                    int count = matte_nframes ? matte_nframes[j] : nframes;
-                    CHECK(upload(matte_clips[j], count, side ? sel.b : sel.a, ctx->wire[2].p));
-                    LAUNCH(ctx, k_matte_extract, grid1(n), TB, 0, ctx->wire[2].p, fmt, matte_chan[j], W, H, flip,
-                           mat + ((size_t)side * nfg + j) * n);
-                }
+            CHECK(mattes(sel, flip));
             void* res = ctx->eng[2].p;
-            if (nfg > 0) CHECK(layers_dev(ctx, *s, sel, nfg, mat, sensitivity, W, H, fmt, &res));
+            if (nfg > 0) CHECK(layers_dev(ctx, *s, sel, *job, mat, W, H, fmt, &res));
             else CHECK(vector_frame_dev(ctx, *s, sel, W, H, fmt, res));  // compose.rs:155-161 without layers
             if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)res, ctx->wire[2].as<uint8_t>(), W, H, flip);
             else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)res, ctx->wire[2].as<uint16_t>(), W, H, flip);

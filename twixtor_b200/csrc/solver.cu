@@ -8,9 +8,9 @@ namespace tw {
 // line[t * stride]. `multi` selects the 2- and 3-channel rule (the -1.0 sentinel decides whether a
 // tap exists, so a real sample of exactly -1.0 is dropped too); LEFT_FIRST adds the tap at i - j
 // before the tap at i + j.
-template <bool LEFT_FIRST>
+template <bool LEFT_FIRST, class T>
 __device__ __forceinline__ float border_value(const float* __restrict__ line, long stride, int len, int i,
-                                              const Taps& t, bool multi) {
+                                              const T& t, bool multi) {
     float centre = (i >= 0 && i < len) ? line[(long)i * stride] : 0.0f;
     float num = t.k[0] * centre;
     float den = t.k[0];
@@ -40,7 +40,9 @@ __device__ __forceinline__ float border_value(const float* __restrict__ line, lo
 }
 
 // conv.rs:141-190 (hrow + interior_run), one output sample per thread
-__global__ void k_conv_h(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t, bool multi) {
+template <class T>
+__device__ __forceinline__ void conv_h_px(const float* __restrict__ src, float* __restrict__ dst, int w, int h,
+                                          const T& t, bool multi) {
     int x = blockIdx.x * blockDim.x + threadIdx.x;
     int y = blockIdx.y;
     if (x >= w || y >= h) return;
@@ -60,8 +62,10 @@ __global__ void k_conv_h(const float* __restrict__ src, float* __restrict__ dst,
 }
 
 // conv.rs:268-301 (vrow_ordered); the optional band output is flow.rs:266-267 (band = orig - blur)
-__global__ void k_conv_v(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t, bool multi,
-                         bool above_first, const float* __restrict__ orig, float* __restrict__ band) {
+template <class T>
+__device__ __forceinline__ void conv_v_px(const float* __restrict__ src, float* __restrict__ dst, int w, int h,
+                                          const T& t, bool multi, bool above_first, const float* __restrict__ orig,
+                                          float* __restrict__ band) {
     int x = blockIdx.x * blockDim.x + threadIdx.x;
     int y = blockIdx.y;
     if (x >= w || y >= h) return;
@@ -81,6 +85,25 @@ __global__ void k_conv_v(const float* __restrict__ src, float* __restrict__ dst,
     long i = (long)y * w + x;
     dst[i] = r;
     if (band) band[i] = orig[i] - r;
+}
+
+__global__ void k_conv_h(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t, bool multi) {
+    conv_h_px(src, dst, w, h, t, multi);
+}
+
+__global__ void k_conv_v(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t, bool multi,
+                         bool above_first, const float* __restrict__ orig, float* __restrict__ band) {
+    conv_v_px(src, dst, w, h, t, multi, above_first, orig, band);
+}
+
+// the same passes with the wide half kernels of the matte choke (one channel)
+__global__ void k_conv_h_wide(const float* __restrict__ src, float* __restrict__ dst, int w, int h, WideTaps t) {
+    conv_h_px(src, dst, w, h, t, false);
+}
+
+__global__ void k_conv_v_wide(const float* __restrict__ src, float* __restrict__ dst, int w, int h, WideTaps t,
+                              bool above_first) {
+    conv_v_px(src, dst, w, h, t, false, above_first, (const float*)nullptr, (float*)nullptr);
 }
 
 // flow/sample.rs:91-112 (resample1): corner aligned bilinear
