@@ -155,6 +155,7 @@ struct or_retime_params {
     int taps_above_first;      // vertical border rows of the solver's filters
     int video_360;             // "360 Video": video range luma, binary alpha Smart Blend
     int prep;                  // Image Prep popup: 1 None, 2 Contrast/Edge Enhance, 3 Delinearize
+    int track_rgb_a;           // retime-fgbg's Track RGB+A (alpha in the luma; the layered pyramids' 360 filters)
 };
 
 const char* or_last_error(void) { return g_err.c_str(); }
@@ -538,6 +539,7 @@ static int retime_one(const void* frames, int nframes, int w, int h, int fmt, co
         fs.sensitivity = sensitivity;
         fs.taps_above_first = p->taps_above_first != 0;
         fs.video_range_luma = p->video_360 != 0;  // compose/vector.rs:72-82 (flow_settings)
+        fs.track_alpha = p->track_rgb_a != 0;     // plugins/retime-fgbg/src/glue.rs:34-38
         fs.prep_contrast_edge = p->prep == 2;     // frontend.rs:224-225
         fs.prep_delinearize = p->prep == 3;
         FlowField fab, fba;
@@ -663,6 +665,7 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
         job.fs.quality = vq;
         job.fs.hiq = p->quality_high != 0;
         job.fs.taps_above_first = p->taps_above_first != 0;
+        job.fs.track_alpha = p->track_rgb_a != 0;
         job.cs.quality_high = p->quality_high != 0;
         job.cs.blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
         job.cs.warp_mode = p->smart_blend;

@@ -556,6 +556,101 @@ void edge_enhance(Plane& p, bool above_first) {
     }
 }
 
+// conv.rs:192-244 (hrow_wrapx): every sample s = x[i] k0, then s = s + (x[(i+j) mod w] + x[(i-j) mod w]) k[j]
+// for j = n-1 down to 1 (the interior run is the same chain without a wrap)
+static void hpass_wrapx(const float* src, float* dst, int w, int h, const float* k, int n) {
+    OMP_FOR
+    for (int y = 0; y < h; y++) {
+        const float* x = src + (long)y * w;
+        for (int i = 0; i < w; i++) {
+            float sum = x[i] * k[0];
+            for (int j = n - 1; j >= 1; j--) {
+                int r = (i + j) % w;
+                int l = ((i - j) % w + w) % w;
+                sum = sum + (x[r] + x[l]) * k[j];
+            }
+            dst[(long)y * w + i] = sum;
+        }
+    }
+}
+
+// conv.rs:326-400 (vpass_sphere): each column padded by n - 1 elements at both ends with the
+// equirectangular walk (reflect at the edge row, move half a turn in x), then the plain chain
+static void vpass_sphere(const float* src, float* dst, int w, int h, const float* k, int n) {
+    int half = w / 2, pad = n - 1;
+    OMP_FOR
+    for (int x = 0; x < w; x++) {
+        std::vector<float> g((size_t)h + 2 * pad);
+        auto walk = [&](int start, int dir, int steps, std::vector<std::pair<int, int>>& out) {
+            int c = x, r = start, d = dir;
+            for (int m = 0; m < steps; m++) {
+                r += d;
+                if (r < 0) { r = 0; d = -d; c = (half + c) % w; }
+                else if (r >= h) { r = h - 1; d = -d; c = (half + c) % w; }
+                out.push_back({c, r});
+            }
+        };
+        std::vector<std::pair<int, int>> up, down;
+        walk(0, -1, pad, up);
+        walk(h - 1, 1, pad, down);
+        for (int m = 0; m < pad; m++) g[pad - 1 - m] = src[(long)up[m].second * w + up[m].first];
+        for (int r = 0; r < h; r++) g[pad + r] = src[(long)r * w + x];
+        for (int m = 0; m < pad; m++) g[pad + h + m] = src[(long)down[m].second * w + down[m].first];
+        for (int y = 0; y < h; y++) {
+            int e = pad + y;
+            float sum = g[e] * k[0];
+            for (int j = n - 1; j >= 1; j--) sum = sum + (g[e + j] + g[e - j]) * k[j];
+            dst[(long)y * w + x] = sum;
+        }
+    }
+}
+
+void convolve_wrapx_sphere(float* data, int w, int h, const float* k, int n) {
+    if (w == 0 || h == 0 || n == 0) return;
+    std::vector<float> tmp((size_t)w * h);
+    hpass_wrapx(data, tmp.data(), w, h, k, n);
+    vpass_sphere(tmp.data(), data, w, h, k, n);
+}
+
+// sample.rs:255-286 (bilinear1_sphere)
+static float bilinear1_sphere(const float* img, int w, int h, float x, float y) {
+    int w1 = w - 1, h1 = h - 1;
+    int tx = cvtt32(x), ty = cvtt32(y);
+    int ix = std::min(std::max(tx, 0), w1), iy = std::min(std::max(ty, 0), h1);
+    float fx = x - (float)tx, fy = y - (float)ty;
+    int x1 = ix + 1 > w1 ? 0 : ix + 1;
+    int xc = ix, xd = x1, yc = iy + 1;
+    if (iy + 1 > h1) {
+        int half = w / 2;
+        xc = (half + ix) % w;
+        xd = (half + x1) % w;
+        yc = h1;
+    }
+    float p00 = img[(long)iy * w + ix], p10 = img[(long)iy * w + x1];
+    float p01 = img[(long)yc * w + xc], p11 = img[(long)yc * w + xd];
+    float top = (p10 - p00) * fx + p00;
+    float bot = (p11 - p01) * fx + p01;
+    return (bot - top) * fy + top;
+}
+
+Plane resample1_wrapx(const Plane& src, int dw, int dh) {
+    Plane d;
+    d.w = dw;
+    d.h = dh;
+    d.d.assign((size_t)dw * dh, 0.0f);
+    if (dw == 0 || dh == 0) return d;
+    float sx = (float)src.w / (float)dw, sy = (float)src.h / (float)dh;
+    OMP_FOR
+    for (int y = 0; y < dh; y++) {
+        float fy = (float)y * sy;
+        for (int x = 0; x < dw; x++) d.d[(long)y * dw + x] = bilinear1_sphere(src.d.data(), src.w, src.h, (float)x * sx, fy);
+    }
+    return d;
+}
+
+// prep.rs:261-299 with wrap: blur5_wrapx_above_first (conv.rs:662) and resample1_wrapx
+static void blur5_wrap(Plane& p) { convolve_wrapx_sphere(p.d.data(), p.w, p.h, BINOMIAL5, 3); }
+
 Plane reduce(Plane t, int r, bool above_first) {  // prep.rs:252-259
     for (int i = 0; i < r; i++) {
         blur5(t.d.data(), t.w, t.h, above_first);
@@ -568,17 +663,30 @@ Plane reduce(Plane t, int r, bool above_first) {  // prep.rs:252-259
 bool build_pyramid(const Image& img, const FlowSettings& s, Pyramid* out, std::string* err) {
     if (!geometry(s, img.w, img.h, &out->geo, err)) return false;
     if (s.video_range_luma && s.track_alpha) { *err = "video range luma with track alpha"; return false; }
-    Plane orig = reduce(luma(img, s.track_alpha, s.video_range_luma), out->geo.reduction, s.taps_above_first);
+    if (s.wrap && s.prep_contrast_edge) { *err = "the 360 mode Contrast / Edge Enhance is not restated"; return false; }
+    Plane orig = luma(img, s.track_alpha, s.video_range_luma);
+    if (s.wrap) {  // prep.rs:288-299 (reduce_with)
+        for (int r = 0; r < out->geo.reduction; r++) {
+            blur5_wrap(orig);
+            orig = resample1_wrapx(orig, orig.w / 2, orig.h / 2);
+        }
+    } else {
+        orig = reduce(std::move(orig), out->geo.reduction, s.taps_above_first);
+    }
     if (s.prep_delinearize) delinearize(orig);  // flow.rs:248-253: Delinearize, then Contrast/Edge
     if (s.prep_contrast_edge) edge_enhance(orig, s.taps_above_first);
     int n = out->geo.levels;
     out->levels.clear();
     for (int i = 0; i < n; i++) {
         Plane tmp = orig;
-        blur5(tmp.d.data(), tmp.w, tmp.h, s.taps_above_first);
+        if (s.wrap) blur5_wrap(tmp);
+        else blur5(tmp.d.data(), tmp.w, tmp.h, s.taps_above_first);
         Plane next;
         bool has_next = i + 1 < n;
-        if (has_next) next = resample1(tmp, out->geo.sizes[i + 1].first, out->geo.sizes[i + 1].second);
+        if (has_next) {
+            int nw = out->geo.sizes[i + 1].first, nh = out->geo.sizes[i + 1].second;
+            next = s.wrap ? resample1_wrapx(tmp, nw, nh) : resample1(tmp, nw, nh);
+        }
         Plane band = orig;
         for (size_t k = 0; k < band.d.size(); k++) band.d[k] = band.d[k] - tmp.d[k];
         out->levels.push_back(std::move(band));

@@ -134,6 +134,9 @@ struct FlowSettings {
     // first, the order of the reference revision whose outputs the parity grid
     // parity/retime-flow/results/base.grid.tsv records.
     bool taps_above_first = true;
+    // The wrap-around (360) mode of the pyramid's filters (flow.rs:236-275 with prep.rs:261-299):
+    // the circular horizontal pass, the equirectangular vertical pass and resample.
+    bool wrap = false;
 };
 
 struct Geometry {
@@ -156,6 +159,10 @@ void blur5(float* data, int w, int h, bool above_first);
 float bilinear1(const float* img, int w, int h, float x, float y);
 void bilinear2(const float* img, int w, int h, float x, float y, float out[2]);
 Plane resample1(const Plane& src, int dw, int dh);
+// conv.rs:643-650 (convolve_wrapx_above_first, 1 channel): hpass_wrapx then vpass_sphere
+void convolve_wrapx_sphere(float* data, int w, int h, const float* k, int n);
+// sample.rs:205-230 (resample1_wrapx): bilinear1_sphere at (x sw / dw, y sh / dh)
+Plane resample1_wrapx(const Plane& src, int dw, int dh);
 
 // ---------------------------------------------------------------------------------------------
 // prep and pyramid (prep.rs, flow.rs:199-275)

@@ -356,7 +356,11 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
         fs.sensitivity = job.sensitivity[k];
         LPlane ca = comp_plane(raws_a, job.shrink, k, fmt, w, h), cb = comp_plane(raws_b, job.shrink, k, fmt, w, h);
         Pyramid pa, pb;
-        if (!build_pyramid(layer_times(a, ca), fs, &pa, err) || !build_pyramid(layer_times(b, cb), fs, &pb, err)) return 1;
+        // plates.rs:319-323 (layer_solve_settings): Track RGB+A puts the luma pyramids (only) in the 360
+        // mode of the filters; the luma itself gets no alpha
+        FlowSettings fp = fs;
+        fp.wrap = job.fs.wrap || job.fs.track_alpha;
+        if (!build_pyramid(layer_times(a, ca), fp, &pa, err) || !build_pyramid(layer_times(b, cb), fp, &pb, err)) return 1;
         std::vector<float> ma, mb;
         bool hm_a = solver_mask(raws_a, ca, k, n, &ma), hm_b = solver_mask(raws_b, cb, k, n, &mb);
         std::vector<Plane> mpa, mpb;

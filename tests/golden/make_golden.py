@@ -131,7 +131,7 @@ def create_vectors_grid(ref):
 
 FG_SERVED = {"speed_percent", "warping", "frame_interp", "blur_compensation", "fg1_matte_chan", "fg2_matte_chan", "fg3_matte_chan",
              "fg1_sensitivity", "fg2_sensitivity", "fg3_sensitivity", "main_bg_sensitivity", "vectors", "display",
-             "fg1_inv_matte_shrink", "fg2_inv_matte_shrink", "fg3_inv_matte_shrink"}
+             "fg1_inv_matte_shrink", "fg2_inv_matte_shrink", "fg3_inv_matte_shrink", "track_rgb_a"}
 
 
 def fgbg_layers_grid(ref):

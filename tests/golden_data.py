@@ -70,7 +70,7 @@ def fgbg_case_params(case):
                 chans=[int(p.get(f"fg{k + 1}_matte_chan", 1)) for k in range(nfg)],
                 fg_sens=[float(p.get(f"fg{k + 1}_sensitivity", 70)) for k in range(nfg)],
                 shrinks=[float(p.get(f"fg{k + 1}_inv_matte_shrink", 0)) for k in range(nfg)],
-                display=int(p.get("display", 1)))
+                display=int(p.get("display", 1)), track_rgb_a=p.get("track_rgb_a", "0") == "1")
 
 
 def cv_case_params(case):

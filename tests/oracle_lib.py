@@ -37,6 +37,7 @@ class RetimeParams(ctypes.Structure):
         ("taps_above_first", ctypes.c_int),
         ("video_360", ctypes.c_int),
         ("prep", ctypes.c_int),
+        ("track_rgb_a", ctypes.c_int),
     ]
 
 
@@ -313,13 +314,15 @@ def fw_triangle(verts, w1, h1, cap=4096):
 
 
 def retime_params(fps=(24, 1), quality_high=True, speed=100.0, keys=None, vectors=5, frame_interp=2, smart_blend=0,
-                  sensitivity=70.0, blur=0.0, rows_reversed=True, taps_above_first=True, video_360=False, prep=1):
+                  sensitivity=70.0, blur=0.0, rows_reversed=True, taps_above_first=True, video_360=False, prep=1,
+                  track_rgb_a=False):
     """The `retime` parameters of one render. rows_reversed / taps_above_first at their defaults
     are the reference's current code; both False is the revision the parity grid records."""
     p = RetimeParams()
     p.rows_reversed, p.taps_above_first = int(rows_reversed), int(taps_above_first)
     p.video_360 = int(video_360)
     p.prep = int(prep)
+    p.track_rgb_a = int(track_rgb_a)
     p.fps_num, p.fps_den = fps
     p.quality_high = int(quality_high)
     p.speed_percent = speed
