@@ -237,10 +237,12 @@ int or_geometry(int quality, int hiq, int w, int h, int* reduction, int* sizes, 
 
 // The band pass levels of one engine image, concatenated finest first.
 int or_build_pyramid(const void* engine, int w, int h, int fmt, int quality, int hiq, float sensitivity, int above_first,
-                     int prep, float* levels_out) {
+                     int prep, int wrap, int track_alpha, float* levels_out) {
     Image img(w, h, (Fmt)fmt);
     std::memcpy(img.data(), engine, img.bytes());
     FlowSettings s;
+    s.wrap = wrap != 0;
+    s.track_alpha = track_alpha != 0;
     s.prep_contrast_edge = prep == 2;
     s.prep_delinearize = prep == 3;
     s.taps_above_first = above_first != 0;

@@ -71,7 +71,7 @@ def lib():
         L.or_block_match.argtypes = [P, P, P, i, i]
         L.or_all_out_of_range.argtypes = [P, i, i]
         L.or_geometry.argtypes = [i, i, i, i, P, P, i]
-        L.or_build_pyramid.argtypes = [P, i, i, i, i, i, f, i, i, P]
+        L.or_build_pyramid.argtypes = [P, i, i, i, i, i, f, i, i, i, i, P]
         L.or_compose_vectors3.argtypes = [P, P, i, i, i, P, P, i, i, f, f, f, i, i, i, i, i, f, i, P]
         L.or_solve_pair.argtypes = [P, P, i, i, i, i, i, f, i, i, P, P]
         L.or_inv_warp.argtypes = [P, P, i, i, i, P, i, i, f, i, P]
@@ -136,12 +136,13 @@ def to_frame(engine, w, h, fmt):
     return out
 
 
-def build_pyramid(engine, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, above_first=True, prep=1):
+def build_pyramid(engine, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, above_first=True, prep=1, wrap=False,
+                  track_alpha=False):
     _, sizes = geometry(quality, hiq, w, h)
     total = sum(a * b for a, b in sizes)
     out = np.zeros(total, np.float32)
     n = lib().or_build_pyramid(ptr(engine), w, h, fmt, quality, int(hiq), sensitivity, int(above_first), int(prep),
-                               ptr(out))
+                               int(wrap), int(track_alpha), ptr(out))
     if n < 0:
         raise ValueError(err())
     levels, off = [], 0

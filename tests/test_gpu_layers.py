@@ -151,7 +151,8 @@ def fgbg_clip(dev, case, rows_reversed=True, taps_above_first=True):
     tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], vectors=kw["vectors"], frame_interp=kw["frame_interp"],
                        blur_compensation=kw["blur"])
     sels = [tw.select(tp, k, w, h) for k in range(n)]
-    s = tw.RetimeSettings(flow=tw.FlowSettings(hiq=True, taps_above_first=taps_above_first),
+    s = tw.RetimeSettings(flow=tw.FlowSettings(hiq=True, taps_above_first=taps_above_first,
+                                               track_alpha=kw["track_rgb_a"]),
                           compose=tw.EngineSettings(warp_mode=kw["smart_blend"], taps_above_first=taps_above_first,
                                                     gouraud=True, blur=float(tw.fixed_param(kw["blur"]))),
                           motion_rows_reversed=rows_reversed)

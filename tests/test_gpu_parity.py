@@ -463,6 +463,23 @@ def test_frames_outside_the_clip_are_blank(dev):
     assert same(out, want)
 
 
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("w,h", [(24, 16), (97, 61), (320, 180), (12, 8)])
+@pytest.mark.parametrize("track_alpha", [False, True])
+def test_pyramid_360_mode_matches_oracle(dev, fmt, w, h, track_alpha):
+    """The 360 mode of the pyramid's filters (the luma pyramids of retime-fgbg's layered solves with
+    Track RGB+A): circular rows, equirectangular columns and resample, odd widths included."""
+    depth = {0: 8, 1: 16, 2: 32}[fmt]
+    wire = synth.moving_clip(w, h, 1, depth=depth, seed=w + h)
+    eng = O.from_frame(wire, w, h, fmt)
+    for q, hiq in [(4, True), (3, False)]:
+        s = tw.FlowSettings(quality=q, hiq=hiq, wrap=True, track_alpha=track_alpha)
+        got = dev.build_pyramid(eng, w, h, fmt, s)
+        want = O.build_pyramid(eng, w, h, fmt, quality=q, hiq=hiq, wrap=True, track_alpha=track_alpha)
+        for lv, (g, x) in enumerate(zip(got, want)):
+            assert g.tobytes() == x.tobytes(), f"level {lv}"
+
+
 def test_unsupported_settings_fail_loudly(dev):
     w, h = 32, 24
     a, b, _, _ = clip_pair(w, h, 0, seed=1)

@@ -47,6 +47,11 @@ __global__ void k_conv_h_wide(const float* __restrict__ src, float* __restrict__
 __global__ void k_conv_v_wide(const float* __restrict__ src, float* __restrict__ dst, int w, int h, WideTaps t,
                               bool above_first);
 __global__ void k_resample(const float* __restrict__ src, int sw, int sh, float* __restrict__ dst, int dw, int dh);
+// the 360 mode of the pyramid's filters: circular rows, equirectangular columns and resample
+__global__ void k_conv_h_wrap(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t);
+__global__ void k_conv_v_sphere(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t,
+                                const float* __restrict__ orig, float* __restrict__ band, float* __restrict__ band_t);
+__global__ void k_resample_sphere(const float* __restrict__ src, int sw, int sh, float* __restrict__ dst, int dw, int dh);
 
 // ---- solver (flow.rs:277-442) ------------------------------------------------------------------------
 // gradient (2 planes) and structure tensor (3 planes)

@@ -325,6 +325,37 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
     float* nxt = scratch[2].as<float>();
     bool af = s.taps_above_first != 0;
     int cw = W, ch = H;
+    if (s.wrap) {
+        // flow.rs:236-275 in the 360 mode of the filters (prep.rs:261-299): the luma, the reduction and
+        // every level with the circular row pass, the equirectangular column pass and resample
+        if (s.prep_contrast_edge)
+            return ctx->fail(TW_ERR_UNSUPPORTED, "the 360 mode Contrast / Edge Enhance is not on the device");
+        long n = (long)W * H;
+        LAUNCH(ctx, k_luma, grid1(n), TB, 0, eng_dev, fmt, cur, W, H, s.track_alpha != 0, s.video_range_luma != 0);
+        for (int r = 0; r < g.reduction; r++) {
+            LAUNCH(ctx, k_conv_h_wrap, grid2(cw, ch), TB, 0, (const float*)cur, tmp, cw, ch, ctx->b5);
+            LAUNCH(ctx, k_conv_v_sphere, grid2(cw, ch), TB, 0, (const float*)tmp, nxt, cw, ch, ctx->b5,
+                   (const float*)nullptr, (float*)nullptr, (float*)nullptr);
+            int nw = cw / 2, nh = ch / 2;
+            LAUNCH(ctx, k_resample_sphere, grid2(nw, nh), TB, 0, (const float*)nxt, cw, ch, cur, nw, nh);
+            cw = nw;
+            ch = nh;
+        }
+        if (s.prep_delinearize) LAUNCH(ctx, k_delinearize, grid1((long)cw * ch), TB, 0, cur, (long)cw * ch);
+        size_t off = 0;
+        for (int i = 0; i < g.levels; i++) {
+            int lw = g.sizes[i][0], lh = g.sizes[i][1];
+            LAUNCH(ctx, k_conv_h_wrap, grid2(lw, lh), TB, 0, (const float*)cur, nxt, lw, lh, ctx->b5);
+            LAUNCH(ctx, k_conv_v_sphere, grid2(lw, lh), TB, 0, (const float*)nxt, tmp, lw, lh, ctx->b5, (const float*)cur,
+                   out + off, out_t ? out_t + off : (float*)nullptr);
+            if (i + 1 < g.levels) {
+                int nw = g.sizes[i + 1][0], nh = g.sizes[i + 1][1];
+                LAUNCH(ctx, k_resample_sphere, grid2(nw, nh), TB, 0, (const float*)tmp, lw, lh, cur, nw, nh);
+            }
+            off += (size_t)lw * lh;
+        }
+        return TW_OK;
+    }
     if (g.reduction == 0) {
         long n = (long)W * H;
         LAUNCH(ctx, k_luma, grid1(n), TB, 0, eng_dev, fmt, cur, W, H, s.track_alpha != 0, s.video_range_luma != 0);
@@ -1805,8 +1836,8 @@ static int layers_check(tw_ctx* ctx, const tw_retime_settings& s, const tw_selec
     if (cs.warp_mode < 0 || cs.warp_mode > 3) return ctx->fail(TW_ERR_BAD_PARAM, "layers: warping code %d is not 0 to 3", cs.warp_mode);
     if (sel.interp < 0 || sel.interp > 2)
         return ctx->fail(TW_ERR_BAD_PARAM, "layers: interpolation mode %d is not 0 to 2", sel.interp);
-    if (cs.wrap_360 || s.flow.wrap || s.flow.track_alpha)
-        return ctx->fail(TW_ERR_UNSUPPORTED, "layers: the wrap-around (360) filters are not on the device");
+    if (cs.wrap_360 || s.flow.wrap)
+        return ctx->fail(TW_ERR_UNSUPPORTED, "layers: the wrap-around (360) solve is not on the device");
     return TW_OK;
 }
 
@@ -1996,7 +2027,9 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     size_t px = 4 * sample_bytes(fmt), ib = (size_t)n * px;
     tw_flow_settings fs0 = s.flow;
     fs0.quality = sel->vectors_quality;
-    fs0.track_alpha = 0;  // plates.rs:323-327: the layered solves add no alpha to the luma
+    fs0.track_alpha = 0;  // plates.rs:319-323: the layered solves add no alpha to the luma,
+    // Track RGB+A puts their luma pyramids (only) in the 360 mode of the filters
+    bool pyramid_wrap = s.flow.wrap || s.flow.track_alpha;
     Geo g;
     CHECK(geometry(fs0, W, H, &g, &ctx->err));
     size_t pf = pyramid_floats(g);
@@ -2055,8 +2088,10 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
         fs.sensitivity = job.sensitivity[k];
         Geo gk;
         CHECK(geometry(fs, W, H, &gk, &ctx->err));
+        tw_flow_settings fp = fs;
+        fp.wrap = pyramid_wrap ? 1 : 0;
         for (int side = 0; side < 2; side++) {
-            CHECK(build_pyramid_dev(ctx, img(side, k), W, H, fmt, fs, gk, pyr[side], pyr[side] + pf, ctx->plane));
+            CHECK(build_pyramid_dev(ctx, img(side, k), W, H, fmt, fp, gk, pyr[side], pyr[side] + pf, ctx->plane));
             LAUNCH(ctx, k_solver_mask, grid1(n), TB, 0, raw + (size_t)side * nfg * n, nfg, k,
                    comp + ((size_t)side * L + k) * n, n, fmt, smat);
             CHECK(build_mask_pyramid_dev(ctx, smat, W, H, fs, gk, mpyr[side], scr, scr + n, flags + FL_ONE));

@@ -106,6 +106,91 @@ __global__ void k_conv_v_wide(const float* __restrict__ src, float* __restrict__
     conv_v_px(src, dst, w, h, t, false, above_first, (const float*)nullptr, (float*)nullptr);
 }
 
+// ---- the 360 mode of the pyramid's filters (prep.rs:261-299, conv.rs:192-400, sample.rs:196-286) ------
+
+// conv.rs:192-244 (hrow_wrapx): s = x[i] k0, then s = s + (x[(i+j) mod w] + x[(i-j) mod w]) k[j] for
+// j = n-1 down to 1; the interior run is the same chain without a wrap
+__global__ void k_conv_h_wrap(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const float* row = src + (long)y * w;
+    float r = row[x] * t.k[0];
+#pragma unroll 1
+    for (int j = t.n - 1; j >= 1; j--) {
+        int rr = (x + j) % w;
+        int l = ((x - j) % w + w) % w;
+        r = r + (row[rr] + row[l]) * t.k[j];
+    }
+    dst[(long)y * w + x] = r;
+}
+
+// conv.rs:326-400 (vpass_sphere): the element of column x at row yy, outside 0..h-1 found by the
+// equirectangular walk from the edge row (reflect, and half a turn in x at every reflection)
+__device__ __forceinline__ float sphere_at(const float* __restrict__ src, int w, int h, int x, int yy) {
+    if (yy >= 0 && yy < h) return src[(long)yy * w + x];
+    int half = w / 2;
+    int c = x, r, d, steps;
+    if (yy < 0) { r = 0; d = -1; steps = -yy; }
+    else { r = h - 1; d = 1; steps = yy - h + 1; }
+#pragma unroll 1
+    for (int m = 0; m < steps; m++) {
+        r += d;
+        if (r < 0) { r = 0; d = -d; c = (half + c) % w; }
+        else if (r >= h) { r = h - 1; d = -d; c = (half + c) % w; }
+    }
+    return src[(long)r * w + c];
+}
+
+// the column pass of the 360 mode: s = g[y] k0, s = s + (g[y+j] + g[y-j]) k[j]; with `band`, the band
+// orig - s and its transpose (element (x, y) at [x * h + y]) for the column sweeps (flow.rs:264-267)
+__global__ void k_conv_v_sphere(const float* __restrict__ src, float* __restrict__ dst, int w, int h, Taps t,
+                                const float* __restrict__ orig, float* __restrict__ band, float* __restrict__ band_t) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    float r = src[(long)y * w + x] * t.k[0];
+#pragma unroll 1
+    for (int j = t.n - 1; j >= 1; j--) r = r + (sphere_at(src, w, h, x, y + j) + sphere_at(src, w, h, x, y - j)) * t.k[j];
+    long i = (long)y * w + x;
+    dst[i] = r;
+    if (band) {
+        float b = orig[i] - r;
+        band[i] = b;
+        if (band_t) band_t[(long)x * h + y] = b;
+    }
+}
+
+// sample.rs:255-286 (bilinear1_sphere)
+__device__ __forceinline__ float bilinear1_sphere(const float* __restrict__ img, int w, int h, float x, float y) {
+    int w1 = w - 1, h1 = h - 1;
+    int tx = cvtt32(x), ty = cvtt32(y);
+    int ix = min(max(tx, 0), w1), iy = min(max(ty, 0), h1);
+    float fx = x - (float)tx, fy = y - (float)ty;
+    int x1 = ix + 1 > w1 ? 0 : ix + 1;
+    int xc = ix, xd = x1, yc = iy + 1;
+    if (iy + 1 > h1) {
+        int half = w / 2;
+        xc = (half + ix) % w;
+        xd = (half + x1) % w;
+        yc = h1;
+    }
+    float p00 = img[(long)iy * w + ix], p10 = img[(long)iy * w + x1];
+    float p01 = img[(long)yc * w + xc], p11 = img[(long)yc * w + xd];
+    float top = (p10 - p00) * fx + p00;
+    float bot = (p11 - p01) * fx + p01;
+    return (bot - top) * fy + top;
+}
+
+// sample.rs:205-230 (resample1_wrapx): the steps sw / dw and sh / dh, the equirectangular sampler
+__global__ void k_resample_sphere(const float* __restrict__ src, int sw, int sh, float* __restrict__ dst, int dw, int dh) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= dw || y >= dh) return;
+    float sx = (float)sw / (float)dw, sy = (float)sh / (float)dh;
+    dst[(long)y * dw + x] = bilinear1_sphere(src, sw, sh, (float)x * sx, (float)y * sy);
+}
+
 // flow/sample.rs:91-112 (resample1): corner aligned bilinear
 __global__ void k_resample(const float* __restrict__ src, int sw, int sh, float* __restrict__ dst, int dw, int dh) {
     int x = blockIdx.x * blockDim.x + threadIdx.x;
