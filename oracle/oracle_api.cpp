@@ -507,7 +507,7 @@ int or_select(const or_retime_params* p, int n, int w, int h, float* s0, float* 
 // One output frame of the plain vector path; `gouraud`: the forward warps of codes 2/3 as the
 // Gouraud variant (the stage set of retime-fgbg, plugins/retime-fgbg/src/glue.rs:142-143).
 static int retime_one(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int n, void* out,
-                      bool gouraud) {
+                      bool gouraud, const std::vector<std::array<float, 4>>* pts = nullptr) {
     Fmt f = (Fmt)fmt;
     size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
     size_t frame_bytes = (size_t)w * h * 4 * es;
@@ -546,7 +546,23 @@ static int retime_one(const void* frames, int nframes, int w, int h, int fmt, co
         fs.prep_delinearize = p->prep == 3;
         FlowField fab, fba;
         bool have_ab = false, have_ba = false;
-        if (interp == 0) {
+        if (pts && !pts->empty()) {
+            // layers.rs:310-336 (single_layer_with_points): the solves take the points' user
+            // displacement (points on the motion path's rows: y -> (H - 1) - y)
+            std::vector<std::array<float, 4>> fwd, bwd;
+            float last_row = (float)h - 1.0f;
+            for (const auto& q : *pts) {
+                float ay = p->rows_reversed ? last_row - q[1] : q[1], by = p->rows_reversed ? last_row - q[3] : q[3];
+                fwd.push_back({q[0], ay, q[2], by});
+                bwd.push_back({q[2], by, q[0], ay});
+            }
+            Pyramid pa, pb;
+            if (!build_pyramid(ar, fs, &pa, &e) || !build_pyramid(br, fs, &pb, &e)) return fail(1, e);
+            std::vector<UserLevel> uab = user_displacement(fwd, pa.geo, w, h), uba = user_displacement(bwd, pa.geo, w, h);
+            bool one = interp == 0, ab = nearest_uses_f_ab(wa, p->smart_blend);
+            if (!one || ab) { fab = solve_pyramids_masked(pa, pb, fs, nullptr, nullptr, false, &uab); have_ab = true; }
+            if (!one || !ab) { fba = solve_pyramids_masked(pb, pa, fs, nullptr, nullptr, false, &uba); have_ba = true; }
+        } else if (interp == 0) {
             if (nearest_uses_f_ab(wa, p->smart_blend)) {
                 if (!solve(ar, br, fs, &fab, &e)) return fail(1, e);
                 have_ab = true;
@@ -612,11 +628,15 @@ static std::vector<float> flip_matte(const std::vector<float>& m, int w, int h) 
 // equal rates); p->smart_blend carries the warping code (0 to 3); fg_shrink the inverse matte shrink of
 // every layer (16.16 reader); display the Display popup (1, 3 to 6). No tracking points.
 int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte_clips, int nfg, const int* fg_chan,
-                       const double* fg_sens, const double* fg_shrink, int display, int w, int h, int fmt,
-                       const or_retime_params* p, int n, void* out) {
-    // compose.rs:155-161: without FG layers (and tracking points) the plain vector path, with the
-    // stage set of the effect (the Gouraud forward warps)
-    if (nfg == 0) return retime_one(frames, nframes, w, h, fmt, p, n, out, true);
+                       const double* fg_sens, const double* fg_shrink, int display, const float* pts, const int* npts,
+                       int w, int h, int fmt, const or_retime_params* p, int n, void* out) {
+    // the tracking points of every layer at this frame (x, y at A, x, y at B; host rows), Main_BG last
+    std::vector<std::vector<std::array<float, 4>>> points(nfg + 1);
+    for (int k = 0, o = 0; pts && npts && k <= nfg; k++)
+        for (int i = 0; i < npts[k]; i++, o++) points[k].push_back({pts[4 * o], pts[4 * o + 1], pts[4 * o + 2], pts[4 * o + 3]});
+    // compose.rs:155-161: without FG layers the plain vector path (with points the single layer one),
+    // with the stage set of the effect (the Gouraud forward warps)
+    if (nfg == 0) return retime_one(frames, nframes, w, h, fmt, p, n, out, true, &points[0]);
     Fmt f = (Fmt)fmt;
     size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
     size_t frame_bytes = (size_t)w * h * 4 * es;
@@ -655,6 +675,13 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
         job.shrink = shrink;
         job.first = first;
         job.last = last;
+        // layers.rs:571-590 (vector_path): the points on the motion path's rows, y -> (H - 1) - y
+        float last_row = (float)h - 1.0f;
+        for (auto& lp : points) {
+            if (p->rows_reversed)
+                for (auto& q : lp) { q[1] = last_row - q[1]; q[3] = last_row - q[3]; }
+            job.points.push_back(lp);
+        }
         for (int k = 0; k < nfg; k++) {
             std::vector<float> ma = extract_raw(fetch(matte_clips[k], a, true), fg_chan[k]);
             std::vector<float> mb = extract_raw(fetch(matte_clips[k], a + 1, true), fg_chan[k]);

@@ -992,8 +992,79 @@ FlowField solve_pyramids(const Pyramid& x, const Pyramid& y, const FlowSettings&
 // flow/extras.rs:244-430 without user displacement and wrap: the plain driver with the gradient
 // masked by X's level mask, the B step gated by Y's warped level mask, and (gate) the block
 // matching sweeps gated by X's mask. With no masks it is the plain driver.
+// points.rs:94-101 (cvtt_f64): truncation of a double to i32, NaN and out of range give INT_MIN
+static int32_t cvtt_f64_i32(double v) {
+    if (std::isnan(v) || v >= 2147483648.0 || v <= -2147483649.0) return INT32_MIN;
+    return (int32_t)v;
+}
+
+std::vector<UserLevel> user_displacement(const std::vector<std::array<float, 4>>& pairs, const Geometry& geo, int W,
+                                         int H) {
+    std::vector<UserLevel> levels;
+    for (int l = 0; l < geo.levels; l++) {
+        int wl = geo.sizes[l].first, hl = geo.sizes[l].second;
+        UserLevel lv;
+        lv.d.assign((size_t)wl * hl * 2, 0.0f);
+        lv.w.assign((size_t)wl * hl, 0.0f);
+        if (l == 0) {  // points.rs:112-144 (finest_level)
+            if (W >= 2 && H >= 2 && wl > 0 && hl > 0) {
+                float kx = (float)(wl - 1) / (float)(W - 1), ky = (float)(hl - 1) / (float)(H - 1);
+                for (const auto& pr : pairs) {
+                    float x = pr[0] * kx, y = pr[1] * ky;
+                    int ix = cvtt_f64_i32((double)x + 0.5), iy = cvtt_f64_i32((double)y + 0.5);
+                    if (ix < 0 || iy < 0 || ix >= wl || iy >= hl) continue;
+                    size_t i = (size_t)iy * wl + ix;
+                    lv.d[2 * i] = (pr[2] * kx - x) + lv.d[2 * i];
+                    lv.d[2 * i + 1] = (pr[3] * ky - y) + lv.d[2 * i + 1];
+                    lv.w[i] = lv.w[i] + 1.0f;
+                }
+                for (size_t i = 0; i < lv.w.size(); i++)
+                    if (0.0f < lv.w[i]) {
+                        lv.d[2 * i] = lv.d[2 * i] / lv.w[i];
+                        lv.d[2 * i + 1] = lv.d[2 * i + 1] / lv.w[i];
+                        lv.w[i] = 1.0f;
+                    }
+            }
+            for (float& v : lv.d) v = -1.0f * v;  // points.rs:103-108 (scale_xy by -1)
+        } else {  // points.rs:147-171 (coarser_level)
+            const UserLevel& pv = levels[l - 1];
+            int pw = geo.sizes[l - 1].first, ph = geo.sizes[l - 1].second;
+            std::vector<float> t = pv.d;
+            convolve(t.data(), pw, ph, 2, BINOMIAL5, 3, true);
+            Plane c0, c1, u;
+            c0.w = c1.w = u.w = pw;
+            c0.h = c1.h = u.h = ph;
+            c0.d.resize((size_t)pw * ph);
+            c1.d.resize((size_t)pw * ph);
+            for (size_t i = 0; i < c0.d.size(); i++) { c0.d[i] = t[2 * i]; c1.d[i] = t[2 * i + 1]; }
+            u.d = pv.w;
+            convolve(u.d.data(), pw, ph, 1, BINOMIAL5, 3, true);
+            Plane rx = resample1(c0, wl, hl), ry = resample1(c1, wl, hl), rw = resample1(u, wl, hl);
+            float sx = (float)(wl - 1) / (float)(pw - 1), sy = (float)(hl - 1) / (float)(ph - 1);
+            for (size_t i = 0; i < rx.d.size(); i++) {
+                lv.d[2 * i] = sx * rx.d[i];
+                lv.d[2 * i + 1] = sy * ry.d[i];
+            }
+            lv.w = rw.d;
+        }
+        levels.push_back(std::move(lv));
+    }
+    return levels;
+}
+
+// flow/extras.rs:181-194 (apply_user): flow = d / w where w != 0
+static void apply_user(std::vector<float>& flow, const UserLevel& u) {
+    for (size_t i = 0; i < u.w.size(); i++) {
+        float k = u.w[i];
+        if (k != 0.0f) {
+            flow[2 * i] = u.d[2 * i] / k;
+            flow[2 * i + 1] = u.d[2 * i + 1] / k;
+        }
+    }
+}
+
 FlowField solve_pyramids_masked(const Pyramid& x, const Pyramid& y, const FlowSettings& s, const std::vector<Plane>* mx,
-                                const std::vector<Plane>* my, bool gate) {
+                                const std::vector<Plane>* my, bool gate, const std::vector<UserLevel>* user) {
     const Geometry& geo = x.geo;
     int levels = geo.levels;
     int start; float damp;
@@ -1008,6 +1079,10 @@ FlowField solve_pyramids_masked(const Pyramid& x, const Pyramid& y, const FlowSe
         const float* mask_x = mx ? (*mx)[l].d.data() : nullptr;
         const float* mask_y = my ? (*my)[l].d.data() : nullptr;
         const float* g8 = gate ? mask_x : nullptr;
+        // flow/extras.rs:198-215 (solve_extended's hooks): the user displacement after the start or
+        // the upsample, after the finest level's block matching and at the end of every level
+        const UserLevel* u = user ? &(*user)[l] : nullptr;
+        if (u) apply_user(flow, *u);
         std::vector<float> grad = calc_grad(img_a, w, h);
         if (mask_x) mask_gradient(grad.data(), mask_x, w, h);
         std::vector<float> a = calc_a(grad, w, h);
@@ -1018,9 +1093,13 @@ FlowField solve_pyramids_masked(const Pyramid& x, const Pyramid& y, const FlowSe
             blur_gaussian(b.data(), w, h, 2, 7.0f, s.taps_above_first);
             new_disp(flow.data(), a.data(), b.data(), (size_t)w * h);
             blur_gaussian(flow.data(), w, h, 2, 5.0f, s.taps_above_first);
-            if (it == 1 && l == 0 && !s.skip_refine) block_match_gated(img_a, img_b, flow.data(), w, h, g8);
+            if (it == 1 && l == 0) {
+                if (!s.skip_refine) block_match_gated(img_a, img_b, flow.data(), w, h, g8);
+                if (u) apply_user(flow, *u);
+            }
         }
         if (l != 0 && !s.skip_refine) block_match_gated(img_a, img_b, flow.data(), w, h, g8);
+        if (u) apply_user(flow, *u);
         if (check) {
             if (all_flow_out_of_range(flow.data(), w, h)) std::fill(flow.begin(), flow.end(), 0.0f);
             else check = false;

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <array>
 #include <vector>
 #include <string>
 
@@ -196,8 +197,18 @@ std::vector<float> calc_b_masked(const float* i1, const float* i0, const float* 
                                  const float* mask_y);
 bool mask_pyramid(const float* matte, int w, int h, const FlowSettings& s, std::vector<Plane>* levels, std::string* err);
 FlowField solve_pyramids(const Pyramid& x, const Pyramid& y, const FlowSettings& s);
+// flow/extras.rs:151-158 (UserLevel): the user displacement of one level, d interleaved (dx, dy)
+// and the weight w, in the solver's internal sign
+struct UserLevel {
+    std::vector<float> d, w;
+};
+// points.rs:201-240 (user_displacement_with, no wrap): pairs (from x, from y, to x, to y) in output
+// pixels of W x H, one level per level of geo, finest first
+std::vector<UserLevel> user_displacement(const std::vector<std::array<float, 4>>& pairs, const Geometry& geo, int W,
+                                         int H);
 FlowField solve_pyramids_masked(const Pyramid& x, const Pyramid& y, const FlowSettings& s, const std::vector<Plane>* mx,
-                                const std::vector<Plane>* my, bool gate);
+                                const std::vector<Plane>* my, bool gate,
+                                const std::vector<UserLevel>* user = nullptr);
 bool solve(const Image& x, const Image& y, const FlowSettings& s, FlowField* out, std::string* err);
 bool solve_pair(const Image& a, const Image& b, const FlowSettings& s, FlowField* f_ab, FlowField* f_ba,
                 std::string* err);

@@ -375,8 +375,23 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
             need_ab = nearest_uses_f_ab(sel.wa, code);
             need_ba = !need_ab;
         }
-        if (need_ab) { f_ab[k] = solve_pyramids_masked(pa, pb, fs, masks ? &mpa : nullptr, masks ? &mpb : nullptr, false); has_ab[k] = true; }
-        if (need_ba) { f_ba[k] = solve_pyramids_masked(pb, pa, fs, masks ? &mpb : nullptr, masks ? &mpa : nullptr, false); has_ba[k] = true; }
+        // layers.rs:247-280 (solve_layer): the solve with X = A takes the pairs (at A, at B), the other
+        // (at B, at A), as their user displacement
+        const std::vector<std::array<float, 4>>* pts = (int)job.points.size() > k ? &job.points[k] : nullptr;
+        std::vector<UserLevel> u_ab, u_ba;
+        if (pts && !pts->empty()) {
+            std::vector<std::array<float, 4>> fwd, bwd;
+            for (const auto& p : *pts) {
+                fwd.push_back({p[0], p[1], p[2], p[3]});
+                bwd.push_back({p[2], p[3], p[0], p[1]});
+            }
+            u_ab = user_displacement(fwd, pa.geo, w, h);
+            u_ba = user_displacement(bwd, pa.geo, w, h);
+        }
+        const std::vector<UserLevel>* uab = u_ab.empty() ? nullptr : &u_ab;
+        const std::vector<UserLevel>* uba = u_ba.empty() ? nullptr : &u_ba;
+        if (need_ab) { f_ab[k] = solve_pyramids_masked(pa, pb, fs, masks ? &mpa : nullptr, masks ? &mpb : nullptr, false, uab); has_ab[k] = true; }
+        if (need_ba) { f_ba[k] = solve_pyramids_masked(pb, pa, fs, masks ? &mpb : nullptr, masks ? &mpa : nullptr, false, uba); has_ba[k] = true; }
     }
     // plates.rs:373-412: the composition of the group, bottom layer first, over an empty image
     Image res(w, h, fmt);

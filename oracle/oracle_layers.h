@@ -20,6 +20,9 @@ struct LayerJob {
     std::vector<float> sensitivity;
     std::vector<float> shrink;  // the inverse matte shrink of every FG layer (empty: all zero)
     int first = 0, last = -1;   // the displayed group first..=last (last -1: the full group 0..=nfg)
+    // the tracking points of every layer (nfg + 1 lists, Main_BG last; empty: none): (x, y at A, x, y
+    // at B) in output pixels, in the row order of the images
+    std::vector<std::vector<std::array<float, 4>>> points;
 };
 
 // layers.rs:120-129 (LayerJob::display_group): the group of the Display popup

@@ -163,7 +163,10 @@ def fgbg_layers_grid(ref):
 
     for c in g.cases:
         params = dict(p.split("=", 1) for p in c["params"])
-        if any(k not in FG_SERVED for k in params) or any("@" in v for v in params.values()):
+        pt = [k for k in params if k.startswith("pt")]
+        if any(k not in FG_SERVED and k not in pt and k != "draw_geom" for k in params):
+            continue
+        if any("@" in v for k, v in params.items() if k not in pt):
             continue
         if params.get("warping", "1") not in ("1", "2", "3", "4"):
             continue

@@ -56,6 +56,76 @@ def fgbg_grid():
     return meta["cases"], inputs
 
 
+def _fixed_reader(v):
+    """A value through 16.16 fixed point and back (crates/fx-core/src/fixed.rs, frontend.rs:131-133)."""
+    f = v * 65536.0 + (-0.5 if v < 0 else 0.5)
+    fixed = 0 if np.isnan(f) else int(np.clip(np.trunc(f), -2 ** 31, 2 ** 31 - 1))
+    return np.float32(np.float64(fixed) * (1.0 / 65536.0))
+
+
+def _eased(u, ease_start, ease_end):
+    """crates/fx-core/src/curves.rs:537-544 (eased_progress)."""
+    if ease_start and ease_end:
+        return u * u * (3.0 - 2.0 * u)
+    if ease_start:
+        return u * u * (2.0 - u)
+    if ease_end:
+        return u * (1.0 + u * (1.0 - u))
+    return u
+
+
+def param_at(text, ticks, kind, default, ticks_per_frame=100):
+    """A keyed CLI value ``V@F[h|e];...`` at ``ticks`` (crates/fx-core/src/curves.rs:79-110 and
+    348-375): before the first key its value, after the last its value, between two keys the
+    first one's value for a hold key or a popup, else the linear (or eased) mix in f64; a point
+    moves on the straight line. Keys without handles only. ``kind``: "int" or "point"."""
+    def parse(v):
+        return int(v) if kind == "int" else [float(x) for x in v.split(",")]
+    if text is None:
+        return default
+    if "@" not in text:
+        return parse(text)
+    keys = []
+    for piece in text.split(";"):
+        v, f = piece.rsplit("@", 1)
+        hold, ease = f.endswith("h"), f.endswith("e")
+        f = f[:-1] if hold or ease else f
+        keys.append((int(round(float(f) * ticks_per_frame)), parse(v), hold, ease))
+    if ticks <= keys[0][0]:
+        return keys[0][1]
+    if ticks >= keys[-1][0]:
+        return keys[-1][1]
+    i = max(j for j, k in enumerate(keys) if k[0] <= ticks)
+    a, b = keys[i], keys[i + 1]
+    if a[2] or kind == "int":
+        return a[1]
+    u = _eased((ticks - a[0]) / (b[0] - a[0]), a[3], b[3])
+    return [x + (y - x) * u for x, y in zip(a[1], b[1])]
+
+
+def fgbg_points(case, a, b, nfg, npoints=12):
+    """The tracking points of a retime-fgbg grid case for the pair of source frames a, b
+    (plugins/retime-fgbg/src/glue.rs:196-211 user_points, 124-133 points_in_use): every point whose
+    Use popup is not Don't Use at the layer time T(a) and equal at T(b) (T(f) = trunc(100 f + 0.5),
+    integer frame rates) goes to the layer points.rs:64-70 (point_layer) names, its position read
+    at both times through the 16.16 reader (points.rs:77-80). One list per layer, Main_BG last, of
+    (x, y at A, x, y at B) in output pixels (host rows)."""
+    p = dict(x.split("=", 1) for x in case["params"])
+    ta, tb = int(100.0 * float(np.float32(a)) + 0.5), int(100.0 * float(np.float32(b)) + 0.5)
+    out = [[] for _ in range(nfg + 1)]
+    for n in range(1, npoints + 1):
+        use = p.get(f"pt{n}_use")
+        v1 = param_at(use, ta, "int", 1)
+        if v1 == 1 or param_at(use, tb, "int", 1) != v1 or v1 < 2:
+            continue
+        k = min(v1 - 2, nfg)
+        pos = p.get(f"pt{n}_pos")
+        pa, pb = param_at(pos, ta, "point", [-5.0, -5.0]), param_at(pos, tb, "point", [-5.0, -5.0])
+        out[k].append((float(_fixed_reader(pa[0])), float(_fixed_reader(pa[1])), float(_fixed_reader(pb[0])),
+                       float(_fixed_reader(pb[1]))))
+    return out
+
+
 def fgbg_case_params(case):
     """The parameters of a fgbg-layers grid case (plugin defaults where the case sets none): the
     retime selection and Main_BG settings (``smart_blend`` carries the warping code, the Warping

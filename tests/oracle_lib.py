@@ -84,7 +84,7 @@ def lib():
         L.or_retime_one.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_crt_powf.argtypes = [P, P, P, i]
         L.or_motion_blur.argtypes = [P, P, i, i, i, P, i, i, f, i, f]
-        L.or_retime_fgbg_one.argtypes = [P, i, P, i, P, P, P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
+        L.or_retime_fgbg_one.argtypes = [P, i, P, i, P, P, P, i, P, P, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_set_threads.argtypes = [i]
         L.or_smart_blend.argtypes = [P, P, P, i, i, i, f, i]
         L.or_fill_holes.argtypes = [P, i, i, i, P, i, i]
@@ -360,11 +360,13 @@ def retime_one(frames, nframes, w, h, fmt, params, n):
     return out
 
 
-def retime_fgbg_clip(frames, nframes, mattes, chans, sens, w, h, fmt, params, nout, shrinks=None, display=1):
+def retime_fgbg_clip(frames, nframes, mattes, chans, sens, w, h, fmt, params, nout, shrinks=None, display=1,
+                     points=None):
     """retime-fgbg with FG matte layers (FG1 first): ``mattes`` the matte clips (nframes wire frames
     each), ``chans`` their channel popups, ``sens`` their sensitivities 0..100, ``shrinks`` their
     inverse matte shrinks; Main_BG's sensitivity is params.sensitivity; ``display`` the Display
-    popup. Output frames 0..nout-1 back to back."""
+    popup; ``points(n)`` the tracking points of output frame n, one list per layer (Main_BG last)
+    of (x, y at A, x, y at B) in host rows. Output frames 0..nout-1 back to back."""
     nfg = len(mattes)
     mattes = [np.ascontiguousarray(m) for m in mattes]
     arr = (ctypes.c_void_p * max(nfg, 1))(*[m.ctypes.data for m in mattes])
@@ -375,8 +377,11 @@ def retime_fgbg_clip(frames, nframes, mattes, chans, sens, w, h, fmt, params, no
     fb = w * h * 4
     out = np.zeros(nout * fb, DTYPE[fmt])
     for n in range(nout):
-        rc = lib().or_retime_fgbg_one(ptr(frames), nframes, arr, nfg, ch, se, sh, display, w, h, fmt,
-                                      ctypes.byref(params), n, ptr(out[n * fb:]))
+        lists = points(n) if points else [[] for _ in range(nfg + 1)]
+        npts = np.array([len(x) for x in lists], np.int32)
+        pts = np.array([q for x in lists for q in x] or [[0, 0, 0, 0]], np.float32).reshape(-1)
+        rc = lib().or_retime_fgbg_one(ptr(frames), nframes, arr, nfg, ch, se, sh, display, ptr(pts), ptr(npts), w, h,
+                                      fmt, ctypes.byref(params), n, ptr(out[n * fb:]))
         if rc:
             raise ValueError(err())
     return out

@@ -223,8 +223,13 @@ def test_fgbg_layers_grid_sha256(case):
     shrinks, display = kw.pop("shrinks"), kw.pop("display")
     p = O.retime_params(rows_reversed=True, taps_above_first=True, **kw)
     mattes = [FG_INPUTS[m].view(O.DTYPE[fmt]) for m in case["mattes"]]
+    nfg = len(mattes)
+
+    def points(k):
+        a = O.select(p, k, w, h)["a"]
+        return golden_data.fgbg_points(case, a, a + 1, nfg)
     out = O.retime_fgbg_clip(FG_INPUTS[case["input"]].view(O.DTYPE[fmt]), n, mattes, chans, sens, w, h, fmt, p, n,
-                             shrinks=shrinks, display=display)
+                             shrinks=shrinks, display=display, points=points)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
 
 
