@@ -235,6 +235,13 @@ int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* 
  * blended at w, or (binary != 0) the binary alpha composite. */
 int tw_smart_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* p1, const tw_image* p2, float w, int32_t binary);
 
+/* One tracking point in use (points.rs:36-55, UserPoint): its position at the layer times of frame
+ * A and of frame B, in output pixels (pixel centres at whole numbers). */
+typedef struct tw_user_point {
+    float at_a[2];
+    float at_b[2];
+} tw_user_point;
+
 /* The FG matte layers of a layered render (layers.rs:71-129, LayerParams and LayerJob, as
  * plugins/retime-fgbg/src/glue.rs:160-193 reads them): FG1 .. FG nfg and Main_BG. */
 typedef struct tw_layer_job {
@@ -244,6 +251,14 @@ typedef struct tw_layer_job {
     float shrink[3];        /* fgN_inv_matte_shrink in pixels (the 16.16 reader's value), at most 13 */
     int32_t display;        /* the Display popup: 1 all layers, 3 to 5 FG1 to FG3 alone, 6 Main_BG alone
                                (layers.rs:120-129); 2 (Source) composes no layer and is refused */
+    /* The tracking points in use (plugins/retime-fgbg/src/glue.rs:196-211, user_points), as the host
+     * evaluates its Track Points at the layer times of the pair: npoints[k] points of layer k (Main_BG
+     * last), back to back in `points`, at most 12 per layer. tw_compose_layers: nfg + 1 counts, the
+     * points in the rows of its images; tw_retime_layers_clip: nout * (nfg + 1) counts, output frame by
+     * output frame, in host rows. NULL: no point. Each solve of a layer with points takes their user
+     * displacement (points.rs:201-240, flow/extras.rs:181-215). */
+    const tw_user_point* points;
+    const int32_t* npoints;
 } tw_layer_job;
 
 /* The layered composition with plates (layers/plates.rs:330-412, solve_and_compose_plates) of one

@@ -805,9 +805,9 @@ int or_solve_masked(const void* x_eng, const void* y_eng, int w, int h, int fmt,
 // each, FG1 first), nfg + 1 sensitivities (0..1), the selection weight / interpolation and the
 // settings; out: the engine image
 int or_compose_layers(const void* a_eng, const void* b_eng, int w, int h, int fmt, int nfg, const float* mattes_a,
-                      const float* mattes_b, const float* sens, const float* shrink, int first, int last, int quality,
-                      int hiq, int above_first, int warp_mode, int video_360, int gouraud, float wa, int interp,
-                      void* out_eng) {
+                      const float* mattes_b, const float* sens, const float* shrink, int first, int last,
+                      const float* pts, const int* npts, int quality, int hiq, int above_first, int warp_mode,
+                      int video_360, int gouraud, float wa, int interp, void* out_eng) {
     Image a(w, h, (Fmt)fmt), b(w, h, (Fmt)fmt), out;
     std::memcpy(a.data(), a_eng, a.bytes());
     std::memcpy(b.data(), b_eng, b.bytes());
@@ -821,6 +821,9 @@ int or_compose_layers(const void* a_eng, const void* b_eng, int w, int h, int fm
     if (shrink) job.shrink.assign(shrink, shrink + nfg);
     job.first = first;
     job.last = last;
+    job.points.resize(nfg + 1);
+    for (int k = 0, o = 0; pts && npts && k <= nfg; k++)
+        for (int i = 0; i < npts[k]; i++, o++) job.points[k].push_back({pts[4 * o], pts[4 * o + 1], pts[4 * o + 2], pts[4 * o + 3]});
     job.fs.quality = quality;
     job.fs.hiq = hiq != 0;
     job.fs.video_range_luma = video_360 != 0;

@@ -95,7 +95,7 @@ def lib():
         L.or_fw_level_count.argtypes = [i, i]
         L.or_fw_triangle.argtypes = [P, i, i, P, i]
         L.or_logf.argtypes = [P, P, ctypes.c_long]
-        L.or_compose_layers.argtypes = [P, P, i, i, i, i, P, P, P, P, i, i, i, i, i, i, i, i, f, i, P]
+        L.or_compose_layers.argtypes = [P, P, i, i, i, i, P, P, P, P, i, i, P, P, i, i, i, i, i, i, f, i, P]
         L.or_mask_pyramid.argtypes = [P, i, i, i, i, i, P, P, i]
         L.or_mask_gradient.argtypes = [P, P, i, i]
         L.or_calc_b_masked.argtypes = [P, P, P, P, i, i, P, P]
@@ -277,7 +277,7 @@ def solve_masked(x, y, w, h, fmt, matte_x=None, matte_y=None, quality=4, hiq=Tru
 
 
 def compose_layers(a, b, w, h, fmt, mattes_a, mattes_b, sensitivity, wa, interp=1, quality=4, hiq=True,
-                   above_first=True, warp_mode=0, video_360=False, gouraud=False, shrink=None, group=None):
+                   above_first=True, warp_mode=0, video_360=False, gouraud=False, shrink=None, group=None, points=None):
     """layers/plates.rs solve_and_compose_plates of one in-between frame (engine images in and out);
     ``shrink`` the inverse matte shrink per FG layer, ``group`` the displayed (first, last)."""
     nfg = len(mattes_a)
@@ -286,9 +286,12 @@ def compose_layers(a, b, w, h, fmt, mattes_a, mattes_b, sensitivity, wa, interp=
     sens = np.ascontiguousarray(sensitivity, np.float32)
     sh = np.ascontiguousarray(list(shrink) if shrink is not None else [0.0] * max(nfg, 1), np.float32)
     first, last = group if group is not None else (0, -1)
+    lists = points if points is not None else [[] for _ in range(nfg + 1)]
+    npts = np.array([len(x) for x in lists], np.int32)
+    pts = np.array([q for x in lists for q in x] or [[0, 0, 0, 0]], np.float32).reshape(-1)
     out = np.zeros_like(a)
     rc = lib().or_compose_layers(ptr(a), ptr(b), w, h, fmt, nfg, ptr(ma), ptr(mb), ptr(sens), ptr(sh), first, last,
-                                 quality, int(hiq), int(above_first), warp_mode, int(video_360), int(gouraud),
+                                 ptr(pts), ptr(npts), quality, int(hiq), int(above_first), warp_mode, int(video_360), int(gouraud),
                                  np.float32(wa), interp, ptr(out))
     if rc:
         raise ValueError(err())

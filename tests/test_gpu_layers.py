@@ -61,14 +61,30 @@ def display_group(display, nfg):
     return 0, nfg
 
 
-def run(dev, a, b, w, h, fmt, ma, mb, sens, wa, interp, code, video_360=False, gouraud=False, shrink=None, display=1):
+def run(dev, a, b, w, h, fmt, ma, mb, sens, wa, interp, code, video_360=False, gouraud=False, shrink=None, display=1,
+        points=None):
     s = tw.RetimeSettings(flow=tw.FlowSettings(video_range_luma=video_360),
                           compose=tw.EngineSettings(warp_mode=code, video_360=video_360, gouraud=gouraud))
     sel = tw.Selection(wa=np.float32(wa), exact=False, vectors_quality=4, interp=interp)
-    got = dev.compose_layers(s, sel, a, b, w, h, fmt, ma, mb, sens, shrink=shrink, display=display)
+    got = dev.compose_layers(s, sel, a, b, w, h, fmt, ma, mb, sens, shrink=shrink, display=display, points=points)
     want = O.compose_layers(a, b, w, h, fmt, ma, mb, sens, np.float32(wa), interp, warp_mode=code, video_360=video_360,
-                            gouraud=gouraud, shrink=shrink, group=display_group(display, len(ma)))
+                            gouraud=gouraud, shrink=shrink, group=display_group(display, len(ma)), points=points)
     assert same(got, want)
+
+
+@pytest.mark.parametrize("fmt", [0, 2])
+@pytest.mark.parametrize("wa,interp", [(0.4, 1), (0.6, 0), (0.3, 0)])
+@pytest.mark.parametrize("display", [1, 3])
+def test_layers_tracking_points_match_oracle(dev, fmt, wa, interp, display):
+    """Tracking points on FG1 and Main_BG: the user displacement pyramid (splat, normalise, blur,
+    resample, scale) and its three hooks in every level of the masked solves; points that share a
+    pixel, points outside the frame, a large motion."""
+    w, h = 96, 64
+    a, b, ma, mb = scene(w, h, fmt, 2, seed=41 + display)
+    points = [[(20.0, 12.5, 24.0, 14.0), (20.2, 12.6, 26.0, 10.0), (-3.0, 5.0, 2.0, 5.0)],
+              [],
+              [(70.0, 40.0, 66.5, 43.25), (10.0, 60.0, 80.0, 2.0), (95.4, 63.4, 90.0, 60.0)]]
+    run(dev, a, b, w, h, fmt, ma, mb, [0.7, 0.7, 0.7], wa, interp, 1, points=points, display=display)
 
 
 @pytest.mark.parametrize("fmt", [0, 1, 2])
@@ -159,8 +175,9 @@ def fgbg_clip(dev, case, rows_reversed=True, taps_above_first=True):
     sens = [tw.percent_param(v) for v in kw["fg_sens"]] + [tw.percent_param(kw["sensitivity"])]
     mattes = [FG_INPUTS[m].view(tw.DTYPES[fmt]) for m in case["mattes"]]
     shrink = [float(tw.fixed_param(v)) for v in kw["shrinks"]]
+    points = [golden_data.fgbg_points(case, x.a, x.a + 1, len(mattes)) for x in sels]
     return dev.retime_layers_clip(s, FG_INPUTS[case["input"]].view(tw.DTYPES[fmt]), n, mattes, kw["chans"], sens, sels,
-                                  w, h, fmt, shrink=shrink, display=kw["display"])
+                                  w, h, fmt, shrink=shrink, display=kw["display"], points=points)
 
 
 @pytest.mark.parametrize("case", FG_CASES, ids=[c["id"] for c in FG_CASES])

@@ -100,13 +100,22 @@ class _ClipJob(ctypes.Structure):
 
 class _LayerJob(ctypes.Structure):
     _fields_ = [("nfg", ctypes.c_int32), ("matte_chan", ctypes.c_int32 * 3), ("sensitivity", ctypes.c_float * 4),
-                ("shrink", ctypes.c_float * 3), ("display", ctypes.c_int32)]
+                ("shrink", ctypes.c_float * 3), ("display", ctypes.c_int32), ("points", ctypes.c_void_p),
+                ("npoints", ctypes.c_void_p)]
 
 
-def _layer_job(nfg, sensitivity, matte_chan=None, shrink=None, display=1):
+def _layer_job(nfg, sensitivity, matte_chan=None, shrink=None, display=1, points=None, per_frame=False):
     """The tw_layer_job of ``nfg`` FG layers: ``sensitivity`` nfg + 1 values (Main_BG last),
-    ``matte_chan`` and ``shrink`` one value per FG layer."""
+    ``matte_chan`` and ``shrink`` one value per FG layer; ``points`` a list of per-layer lists
+    (Main_BG last) of tracking points (x, y at A, x, y at B), or with ``per_frame`` one such list
+    per output frame (the clip call)."""
     j = _LayerJob()
+    if points is not None:
+        frames = points if per_frame else [points]
+        counts = np.array([len(layer) for f in frames for layer in f], np.int32)
+        flat = np.array([q for f in frames for layer in f for q in layer] or [[0, 0, 0, 0]], np.float32).reshape(-1)
+        j.points, j.npoints = flat.ctypes.data, counts.ctypes.data
+        j._keep = (flat, counts)
     j.nfg = nfg
     for k, v in enumerate(matte_chan or []):
         j.matte_chan[k] = int(v)
@@ -595,13 +604,14 @@ class Device:
         return out
 
     def compose_layers(self, settings: RetimeSettings, sel: Selection, a, b, width, height, fmt, mattes_a, mattes_b,
-                       sensitivity, shrink=None, display=1):
+                       sensitivity, shrink=None, display=1, points=None):
         """The layered composition with plates of one in-between frame (layers/plates.rs): ``mattes_a`` /
         ``mattes_b`` the FG raw mattes at A and B (FG1 first, ``width * height`` floats each),
         ``sensitivity`` one value per layer, Main_BG last, ``shrink`` the inverse matte shrink per FG
-        layer, ``display`` the Display popup (the group composed). Returns the engine image."""
+        layer, ``display`` the Display popup (the group composed), ``points`` the tracking points per
+        layer (x, y at A, x, y at B in the images' rows). Returns the engine image."""
         nfg = len(mattes_a)
-        job = _layer_job(nfg, sensitivity, shrink=shrink, display=display)
+        job = _layer_job(nfg, sensitivity, shrink=shrink, display=display, points=points)
         out = np.zeros(width * height * 4, DTYPES[fmt])
         ai, aa = _img(a, width, height, fmt)
         bi, ba = _img(b, width, height, fmt)
@@ -710,12 +720,13 @@ class Device:
         return out
 
     def retime_layers_clip(self, settings: RetimeSettings, frames, nframes: int, mattes, matte_chan, sensitivity, sels,
-                           width, height, fmt, matte_nframes=None, out=None, shrink=None, display=1):
+                           width, height, fmt, matte_nframes=None, out=None, shrink=None, display=1, points=None):
         """retime-fgbg with FG matte layers over a clip in host memory: ``mattes`` the FG1.. matte
         clips (wire frames back to back, the footage's size and format), ``matte_chan`` their channel
         popups (1 R, 2 G, 3 B, else alpha), ``sensitivity`` one value 0..1 per layer, Main_BG last,
-        ``shrink`` the inverse matte shrink per FG layer (pixels), ``display`` the Display popup.
-        Returns the output frames ``sels`` back to back."""
+        ``shrink`` the inverse matte shrink per FG layer (pixels), ``display`` the Display popup,
+        ``points`` per output frame the tracking points of every layer (x, y at A, x, y at B, host
+        rows). Returns the output frames ``sels`` back to back."""
         frames = np.ascontiguousarray(frames)
         fs = width * height * 4
         if out is None:
@@ -723,7 +734,8 @@ class Device:
         nfg = len(mattes)
         mattes = [np.ascontiguousarray(m) for m in mattes]
         clips = (ctypes.c_void_p * max(nfg, 1))(*[m.ctypes.data for m in mattes])
-        job = _layer_job(nfg, sensitivity, matte_chan=matte_chan, shrink=shrink, display=display)
+        job = _layer_job(nfg, sensitivity, matte_chan=matte_chan, shrink=shrink, display=display, points=points,
+                         per_frame=True)
         counts = None if matte_nframes is None else np.ascontiguousarray(matte_nframes, np.int32)
         arr = (_Selection * max(len(sels), 1))(*[x._c() for x in sels])
         self._check(self._L.tw_retime_layers_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes,

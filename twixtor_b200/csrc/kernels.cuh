@@ -194,6 +194,18 @@ __global__ void k_choke_base(const float* __restrict__ raw, long n, float kk, bo
 __global__ void k_choke_finish(const float* __restrict__ base, const float* __restrict__ b_lo,
                                const float* __restrict__ b_hi, ChokeStep st, long n, float* __restrict__ out);
 __global__ void k_flip_rows(const void* __restrict__ src, void* __restrict__ dst, int w, int h, int px);
+// ---- tracking points (points.rs:112-240, flow/extras.rs:181-215) -----------------------------------
+constexpr int MAX_USER_PAIRS = 12;  // the twelve Track Points of the effects
+struct UserPairs {
+    int n;
+    float p[MAX_USER_PAIRS][4];  // (from x, from y, to x, to y) in output pixels, point order
+};
+__global__ void k_user_splat(UserPairs pairs, int w0, int h0, int W, int H, float* __restrict__ du,
+                             float* __restrict__ dv, float* __restrict__ uw);
+__global__ void k_user_finest(float* __restrict__ du, float* __restrict__ dv, float* __restrict__ uw, long n);
+__global__ void k_user_scale(float* __restrict__ du, float* __restrict__ dv, long n, float sx, float sy);
+__global__ void k_apply_user(float* __restrict__ fu, float* __restrict__ fv, const float* __restrict__ du,
+                             const float* __restrict__ dv, const float* __restrict__ uw, long n);
 __global__ void k_solver_mask(const float* __restrict__ raws, int nfg, int k, const float* __restrict__ comp, long n,
                               int fmt, float* __restrict__ out);
 __global__ void k_layer_times(const void* __restrict__ src, const float* __restrict__ p, void* __restrict__ out, int fmt,

@@ -8,6 +8,8 @@
 // can reach an output (the cut, in double precision there), and its NaN rule where it uses it.
 #include "kernels.cuh"
 
+#include <climits>
+
 namespace tw {
 
 __device__ __forceinline__ float white_of(int fmt) { return fmt == 0 ? 255.0f : fmt == 1 ? 65535.0f : 1.0f; }
@@ -317,6 +319,66 @@ __global__ void k_refill_post(void* __restrict__ img, int fmt, long n, const flo
         p[1] = r1;
         p[2] = r2;
         p[3] = r3;
+    }
+}
+
+// ---- tracking points: the user displacement of a solve (points.rs:112-240) ---------------------------
+
+// points.rs:94-101 (cvtt_f64): truncation to i32, NaN and out of range give INT_MIN
+__device__ __forceinline__ int cvtt_f64_i32(double v) {
+    if (isnan(v) || v >= 2147483648.0 || v <= -2147483649.0) return INT_MIN;
+    return (int)v;
+}
+
+// points.rs:112-133: the pairs splatted into level 0 (w0 x h0) of an output of W x H, in point order
+// (one thread: a pixel's sums follow the order of the points)
+__global__ void k_user_splat(UserPairs pairs, int w0, int h0, int W, int H, float* __restrict__ du,
+                             float* __restrict__ dv, float* __restrict__ uw) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    if (W < 2 || H < 2 || w0 == 0 || h0 == 0) return;
+    float kx = (float)(w0 - 1) / (float)(W - 1), ky = (float)(h0 - 1) / (float)(H - 1);
+    for (int k = 0; k < pairs.n && k < MAX_USER_PAIRS; k++) {
+        float x = pairs.p[k][0] * kx, y = pairs.p[k][1] * ky;
+        int ix = cvtt_f64_i32((double)x + 0.5), iy = cvtt_f64_i32((double)y + 0.5);
+        if (ix < 0 || iy < 0 || ix >= w0 || iy >= h0) continue;
+        long i = (long)iy * w0 + ix;
+        du[i] = (pairs.p[k][2] * kx - x) + du[i];
+        dv[i] = (pairs.p[k][3] * ky - y) + dv[i];
+        uw[i] = uw[i] + 1.0f;
+    }
+}
+
+// points.rs:134-143: the mean of the pairs on a pixel (w becomes 1), then d = -1 d everywhere
+__global__ void k_user_finest(float* __restrict__ du, float* __restrict__ dv, float* __restrict__ uw, long n) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float u = du[i], v = dv[i], w = uw[i];
+    if (0.0f < w) {
+        u = u / w;
+        v = v / w;
+        uw[i] = 1.0f;
+    }
+    du[i] = -1.0f * u;
+    dv[i] = -1.0f * v;
+}
+
+// points.rs:103-108 (scale_xy)
+__global__ void k_user_scale(float* __restrict__ du, float* __restrict__ dv, long n, float sx, float sy) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    du[i] = sx * du[i];
+    dv[i] = sy * dv[i];
+}
+
+// flow/extras.rs:181-194 (apply_user): flow = d / w where w != 0
+__global__ void k_apply_user(float* __restrict__ fu, float* __restrict__ fv, const float* __restrict__ du,
+                             const float* __restrict__ dv, const float* __restrict__ uw, long n) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float k = uw[i];
+    if (k != 0.0f) {
+        fu[i] = du[i] / k;
+        fv[i] = dv[i] / k;
     }
 }
 

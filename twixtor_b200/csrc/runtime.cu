@@ -399,6 +399,60 @@ size_t pyramid_floats(const Geo& g) {
     return n;
 }
 
+// The pairs of a solve from a layer's tracking points (layers.rs:254, UserPoint::pair): (at A, at B)
+// for the solve with X = A, (at B, at A) for the other; `flip`: on the motion path's bottom-up rows,
+// y -> (H - 1) - y (layers.rs:348-351). More than twelve points is refused.
+static int user_pairs(tw_ctx* ctx, const tw_user_point* pts, int n, bool x_is_a, bool flip, int H, UserPairs* out) {
+    if (n > MAX_USER_PAIRS) return ctx->fail(TW_ERR_UNSUPPORTED, "%d tracking points on one layer (at most 12)", n);
+    out->n = n;
+    float last_row = (float)H - 1.0f;
+    for (int i = 0; i < n; i++) {
+        float ax = pts[i].at_a[0], ay = pts[i].at_a[1], bx = pts[i].at_b[0], by = pts[i].at_b[1];
+        if (flip) {
+            ay = last_row - ay;
+            by = last_row - by;
+        }
+        out->p[i][0] = x_is_a ? ax : bx;
+        out->p[i][1] = x_is_a ? ay : by;
+        out->p[i][2] = x_is_a ? bx : ax;
+        out->p[i][3] = x_is_a ? by : ay;
+    }
+    return TW_OK;
+}
+
+// points.rs:201-240 (user_displacement_with, no wrap): the user displacement of a solve, planes du,
+// dv, uw laid out like the band pyramid; level 0 the splat of the pairs, normalised and negated,
+// every coarser level the binomial blur of the level above (the two channels with the multi channel
+// border rule, the column pass above first), the corner aligned resample and the scale of d by the
+// ratio of the level sizes. scr: 4 planes of level 0's size.
+static int build_user_dev(tw_ctx* ctx, const UserPairs& pr, const Geo& g, int W, int H, float* du, float* dv, float* uw,
+                          float* scr) {
+    size_t pf = pyramid_floats(g);
+    for (float* p : {du, dv, uw}) CHECK(ctx->cuda(cudaMemsetAsync(p, 0, pf * sizeof(float), ctx->cur), "user displacement"));
+    int w0 = g.sizes[0][0], h0 = g.sizes[0][1];
+    LAUNCH(ctx, k_user_splat, 1, 32, 0, pr, w0, h0, W, H, du, dv, uw);
+    LAUNCH(ctx, k_user_finest, grid1((long)w0 * h0), TB, 0, du, dv, uw, (long)w0 * h0);
+    size_t off = 0;
+    for (int l = 1; l < g.levels; l++) {
+        int pw = g.sizes[l - 1][0], ph = g.sizes[l - 1][1], nw = g.sizes[l][0], nh = g.sizes[l][1];
+        size_t pn = (size_t)pw * ph, noff = off + pn;
+        float* c[3] = {scr, scr + pn, scr + 2 * pn};
+        float* tmp = scr + 3 * pn;
+        CHECK(ctx->cuda(cudaMemcpyAsync(c[0], du + off, pn * sizeof(float), cudaMemcpyDeviceToDevice, ctx->cur), "user"));
+        CHECK(ctx->cuda(cudaMemcpyAsync(c[1], dv + off, pn * sizeof(float), cudaMemcpyDeviceToDevice, ctx->cur), "user"));
+        CHECK(ctx->cuda(cudaMemcpyAsync(c[2], uw + off, pn * sizeof(float), cudaMemcpyDeviceToDevice, ctx->cur), "user"));
+        conv_planes(ctx, c, 2, pw, ph, ctx->b5, true, tmp);
+        conv_planes(ctx, c + 2, 1, pw, ph, ctx->b5, true, tmp);
+        LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, c[0], pw, ph, du + noff, nw, nh);
+        LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, c[1], pw, ph, dv + noff, nw, nh);
+        LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, c[2], pw, ph, uw + noff, nw, nh);
+        float sx = (float)(nw - 1) / (float)(pw - 1), sy = (float)(nh - 1) / (float)(ph - 1);
+        LAUNCH(ctx, k_user_scale, grid1((long)nw * nh), TB, 0, du + noff, dv + noff, (long)nw * nh, sx, sy);
+        off = noff;
+    }
+    return TW_OK;
+}
+
 // ---- block matching (flow.rs:551-622) -----------------------------------------------------------------
 // Rows on the row-major planes; then the field is transposed, the column sweeps run on the
 // transposed planes (AT, BT: the level's bands stored column by column), and the field goes back.
@@ -426,7 +480,8 @@ void block_match(tw_ctx* ctx, const float* A, const float* B, const float* AT, c
 // layers/plates.rs:360).
 int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float* xt, const float* yt, const Geo& g,
                        const tw_flow_settings& s, DevBuf& work, float* out, int* any, int* nan_flag,
-                       const float* mx = nullptr, const float* my = nullptr) {
+                       const float* mx = nullptr, const float* my = nullptr, const float* udu = nullptr,
+                       const float* udv = nullptr, const float* uww = nullptr) {
     size_t np0 = (size_t)g.w * g.h;
     // planes: gx gy a0 a1 a2 u0 v0 u1 v1 uT vT
     const int NP = 11;
@@ -457,6 +512,13 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
         int lt = level_threads(w, h);
         const float* mask_x = mx ? mx + offs[l] : nullptr;
         const float* mask_y = my ? my + offs[l] : nullptr;
+        // flow/extras.rs:198-215: the user displacement of the tracking points, flow = d / w, after the
+        // start or the upsample, after the finest level's block matching and at the end of the level
+        auto user = [&]() {
+            if (udu) LAUNCH(ctx, k_apply_user, grid1((long)w * h), TB, 0, fu, fv, udu + offs[l], udv + offs[l], uww + offs[l],
+                            (long)w * h);
+        };
+        user();
         LAUNCHB(ctx, 24.0 * px, k_level_init, tiles(w, h), lt, level_init_smem(), A, w, h, ctx->g7, af, gx, gy, a0, a1, a2,
                 mask_x);
         for (int it = 0; it < 3; it++) {
@@ -465,9 +527,13 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
                     w, h, ctx->g7, ctx->g5, af, nu, nv, mask_y);
             std::swap(fu, nu);
             std::swap(fv, nv);
-            if (it == 1 && l == 0 && !s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h);
+            if (it == 1 && l == 0) {
+                if (!s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h);
+                user();
+            }
         }
         if (l != 0 && !s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h);
+        user();
         LAUNCH(ctx, k_range_any, grid2(w, h), TB, 0, fu, fv, w, h, any + l);
         bool damp_now = l == start && damp_any;
         if (l > 0) {
@@ -2014,7 +2080,8 @@ static int refill_dev(tw_ctx* ctx, void* p, int W, int H, int fmt, const float* 
 // the job's display group are solved and composed. Clears the flags first; *res_out receives the
 // engine result (device).
 static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel_, const tw_layer_job& job,
-                      const float* mat, int W, int H, int fmt, void** res_out) {
+                      const float* mat, int W, int H, int fmt, void** res_out, const tw_user_point* pts = nullptr,
+                      const int32_t* npts = nullptr, bool flip_points = false) {
     const tw_selection* sel = &sel_;
     const tw_engine_settings& cs = s.compose;
     CHECK(layers_check(ctx, s, sel_));
@@ -2044,10 +2111,14 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     size_t o_smat = take(2 * (size_t)n), o_img = take(2 * (size_t)L * ib / 4 + 1), o_plate = take(2 * ib / 4 + 1);
     size_t o_res = take(ib / 4 + 1), o_flow = take(2 * (size_t)L * fb), o_pyr = take(4 * pf), o_mpyr = take(2 * pf);
     size_t o_scr = take(4 * (size_t)n);
+    bool any_points = false;
+    for (int k = 0; pts && npts && k <= nfg; k++) any_points = any_points || npts[k] > 0;
+    size_t o_user = take(any_points ? 6 * pf : 0);
     CHECK(ctx->ensure(ctx->lay_mem, fl * sizeof(float), "layer buffers"));
     CHECK(ctx->ensure(ctx->holes, (size_t)n, "holes mask"));
     CHECK(ctx->ensure(ctx->eng[2], ib, "layer result"));
     float* M = ctx->lay_mem.as<float>();
+    float* user = any_points ? M + o_user : nullptr;  // du, dv, uw of F_AB's solve, then of F_BA's
     float* raw = M + o_raw;
     float* cuts = shrink ? M + o_cut : nullptr;
     float* comp = M + o_comp;
@@ -2083,11 +2154,30 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
         need_ab = use_ab;
         need_ba = !use_ab;
     }
+    int pt_first[4] = {0, 0, 0, 0};
+    for (int k = 1; pts && npts && k <= nfg; k++) pt_first[k] = pt_first[k - 1] + npts[k - 1];
     for (int k = first; k <= last; k++) {
         tw_flow_settings fs = fs0;
         fs.sensitivity = job.sensitivity[k];
         Geo gk;
         CHECK(geometry(fs, W, H, &gk, &ctx->err));
+        // layers.rs:257-270 (solve_layer): a layer with points solves with their user displacement
+        int np_k = pts && npts ? npts[k] : 0;
+        const float *uab[3] = {nullptr, nullptr, nullptr}, *uba[3] = {nullptr, nullptr, nullptr};
+        if (np_k > 0) {
+            UserPairs pr;
+            float* u = user;
+            if (need_ab) {
+                CHECK(user_pairs(ctx, pts + pt_first[k], np_k, true, flip_points, H, &pr));
+                CHECK(build_user_dev(ctx, pr, gk, W, H, u, u + pf, u + 2 * pf, scr));
+                uab[0] = u; uab[1] = u + pf; uab[2] = u + 2 * pf;
+            }
+            if (need_ba) {
+                CHECK(user_pairs(ctx, pts + pt_first[k], np_k, false, flip_points, H, &pr));
+                CHECK(build_user_dev(ctx, pr, gk, W, H, u + 3 * pf, u + 4 * pf, u + 5 * pf, scr));
+                uba[0] = u + 3 * pf; uba[1] = u + 4 * pf; uba[2] = u + 5 * pf;
+            }
+        }
         tw_flow_settings fp = fs;
         fp.wrap = pyramid_wrap ? 1 : 0;
         for (int side = 0; side < 2; side++) {
@@ -2098,10 +2188,10 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
         }
         if (need_ab)
             CHECK(solve_pyramids_dev(ctx, pyr[0], pyr[1], pyr[0] + pf, pyr[1] + pf, gk, fs, ctx->work[0], flow(0, k),
-                                     flags + FL_ANY0, flags + FL_NAN, mpyr[0], mpyr[1]));
+                                     flags + FL_ANY0, flags + FL_NAN, mpyr[0], mpyr[1], uab[0], uab[1], uab[2]));
         if (need_ba)
             CHECK(solve_pyramids_dev(ctx, pyr[1], pyr[0], pyr[1] + pf, pyr[0] + pf, gk, fs, ctx->work[0], flow(1, k),
-                                     flags + FL_ANY1, flags + FL_NAN, mpyr[1], mpyr[0]));
+                                     flags + FL_ANY1, flags + FL_NAN, mpyr[1], mpyr[0], uba[0], uba[1], uba[2]));
     }
     // the composition of the group, bottom layer first, over an empty image (plates.rs:373-412)
     WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
@@ -2248,7 +2338,7 @@ int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selecti
                                         cudaMemcpyHostToDevice, ctx->stream), "matte upload"));
     }
     void* res = nullptr;
-    CHECK(layers_dev(ctx, *s, *sel, *job, mat, W, H, fmt, &res));
+    CHECK(layers_dev(ctx, *s, *sel, *job, mat, W, H, fmt, &res, job->points, job->npoints, false));
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, res, ib, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     return layers_status(ctx);
 }
@@ -2787,7 +2877,7 @@ int tw_retime_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames,
 // into `res` (an engine image). The serial form of retime_frame_lane, for the compositions that
 // read counts back (the forward warps).
 static int vector_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel, int W, int H, int fmt,
-                            void* res) {
+                            void* res, const tw_user_point* pts = nullptr, int npts = 0, bool flip_points = false) {
     tw_flow_settings fs = s.flow;
     fs.quality = sel.vectors_quality;
     if (fs.wrap) return ctx->fail(TW_ERR_UNSUPPORTED, "the wrap-around (360) solve is not on the device");
@@ -2811,12 +2901,32 @@ static int vector_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_s
         need_ab = use_ab;
         need_ba = !use_ab;
     }
+    // layers.rs:310-336 (single_layer_with_points): with tracking points the solves take their user
+    // displacement
+    const float *uab[3] = {nullptr, nullptr, nullptr}, *uba[3] = {nullptr, nullptr, nullptr};
+    if (pts && npts > 0) {
+        size_t np0 = (size_t)g.w * g.h;
+        CHECK(ctx->ensure(ctx->lay_mem, (6 * pf + 4 * np0) * sizeof(float), "user displacement"));
+        float* u = ctx->lay_mem.as<float>();
+        float* scr = u + 6 * pf;
+        UserPairs pr;
+        if (need_ab) {
+            CHECK(user_pairs(ctx, pts, npts, true, flip_points, H, &pr));
+            CHECK(build_user_dev(ctx, pr, g, W, H, u, u + pf, u + 2 * pf, scr));
+            uab[0] = u; uab[1] = u + pf; uab[2] = u + 2 * pf;
+        }
+        if (need_ba) {
+            CHECK(user_pairs(ctx, pts, npts, false, flip_points, H, &pr));
+            CHECK(build_user_dev(ctx, pr, g, W, H, u + 3 * pf, u + 4 * pf, u + 5 * pf, scr));
+            uba[0] = u + 3 * pf; uba[1] = u + 4 * pf; uba[2] = u + 5 * pf;
+        }
+    }
     if (need_ab)
         CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, fs, ctx->work[0], ctx->flow[0].as<float>(),
-                                 flags + FL_ANY0, flags + FL_NAN));
+                                 flags + FL_ANY0, flags + FL_NAN, nullptr, nullptr, uab[0], uab[1], uab[2]));
     if (need_ba)
         CHECK(solve_pyramids_dev(ctx, py_, px_, py_ + pf, px_ + pf, g, fs, ctx->work[1], ctx->flow[1].as<float>(),
-                                 flags + FL_ANY1, flags + FL_NAN));
+                                 flags + FL_ANY1, flags + FL_NAN, nullptr, nullptr, uba[0], uba[1], uba[2]));
     WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
     SmartScratch ss{nullptr, &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB, &ctx->pre_blur};
     return compose_dev(ctx, s.compose, sel, ctx->eng[0].p, ctx->eng[1].p, need_ab ? ctx->flow[0].as<float>() : nullptr,
@@ -2832,7 +2942,11 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
                           const tw_layer_job* job, const void* const* matte_clips, const int32_t* matte_nframes,
                           const tw_selection* sels, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
-    if (job && job->nfg == 0 && job->display != 2 && sels && s && s->compose.warp_mode < 2)
+    bool no_points = true;
+    if (job && job->nfg >= 0 && job->nfg <= 3 && job->points && job->npoints && nout > 0)
+        for (long i = 0; i < (long)nout * (job->nfg + 1); i++)
+            if (job->npoints[i] != 0) no_points = false;
+    if (job && job->nfg == 0 && job->display != 2 && sels && s && s->compose.warp_mode < 2 && no_points)
         return tw_retime_clip(ctx, s, frames, nframes, sels, nout, width, height, fmt, out);
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cur = ctx->stream;
@@ -2874,8 +2988,15 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
             }
         return TW_OK;
     };
+    long pt_off = 0;  // the first point of output frame k in job->points
     for (int k = 0; k < nout; k++) {
         const tw_selection& sel = sels[k];
+        const int32_t* npts = job->points && job->npoints ? job->npoints + (size_t)k * (nfg + 1) : nullptr;
+        const tw_user_point* pts = npts ? job->points + pt_off : nullptr;
+        for (int j = 0; npts && j <= nfg; j++) {
+            if (npts[j] < 0) return ctx->fail(TW_ERR_BAD_PARAM, "a negative point count");
+            pt_off += npts[j];
+        }
         // compose.rs:209-211 (layered_exact): with FG layers, a shrink clears the exactness of a position
         bool exact = sel.exact && !(nfg > 0 && shrink);
         bool vector = sel.vectors_quality != 0 && !exact;
@@ -2897,8 +3018,9 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
         } else {
             CHECK(mattes(sel, flip));
             void* res = ctx->eng[2].p;
-            if (nfg > 0) CHECK(layers_dev(ctx, *s, sel, *job, mat, W, H, fmt, &res));
-            else CHECK(vector_frame_dev(ctx, *s, sel, W, H, fmt, res));  // compose.rs:155-161 without layers
+            bool fp = s->motion_rows_reversed != 0;  // layers.rs:348-351: points on the motion path's rows
+            if (nfg > 0) CHECK(layers_dev(ctx, *s, sel, *job, mat, W, H, fmt, &res, pts, npts, fp));
+            else CHECK(vector_frame_dev(ctx, *s, sel, W, H, fmt, res, pts, npts ? npts[0] : 0, fp));  // compose.rs:155-164
             if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)res, ctx->wire[2].as<uint8_t>(), W, H, flip);
             else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)res, ctx->wire[2].as<uint16_t>(), W, H, flip);
             else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)res, ctx->wire[2].as<float>(), W, H, flip);
