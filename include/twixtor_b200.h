@@ -339,9 +339,14 @@ int tw_vectors_pair(int32_t n, int32_t time_step, int32_t track_frame, int32_t* 
 /* The Create Vectors effect over a clip in HOST memory (wire frames back to back): output frame k
  * encodes the flow from clip frame pairs[2k] to pairs[2k + 1] (a frame index outside 0..nframes-1
  * is a blank frame), with the device frame cache, the lanes and the copy streams of
- * tw_retime_clip. The output wire frames go to out + k * frame_bytes. */
+ * tw_retime_clip. The output wire frames go to out + k * frame_bytes. points / npoints: the
+ * tracking points in use of each output frame (plugins/create-vectors/src/glue.rs:278-291,
+ * layer_points, as the host evaluates them at the layer times of the pair; host rows), npoints[k]
+ * of them for frame k, at most 12, back to back; they give the solve its user displacement
+ * (create_vectors.rs:336-351). NULL: no point. */
 int tw_create_vectors_clip(tw_ctx* ctx, const tw_vectors_settings* s, const void* frames, int32_t nframes,
-                           const int32_t* pairs, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out);
+                           const int32_t* pairs, int32_t nout, const tw_user_point* points, const int32_t* npoints,
+                           int32_t width, int32_t height, int32_t fmt, void* out);
 
 /* holefill::fill_holes_masked_with (holefill.rs:452-491) with is360 off: the pull-push fill of
  * `img` in place. `mask` holds width*height values of kind 1 (u8), 2 (u16) or 3 (f32); a pixel is

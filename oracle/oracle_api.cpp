@@ -855,6 +855,7 @@ struct or_cv_params {
     int track_rgb_a;
     int rows_reversed;      // the plugin turns the frames upside down for the engine (glue.rs:28-37)
     int taps_above_first;   // the solver's vertical border tap order
+    int prep;               // Image Prep popup: 1 None, 2 Contrast/Edge Enhance, 3 Delinearize
 };
 
 // vectors.rs:57-130 on a flow field; dst_fmt 0/1/2
@@ -871,7 +872,7 @@ int or_encode_vectors(void* out_eng, int w, int h, int fmt, const float* flow, i
 
 // Output frame n of the Create Vectors effect over a raw clip (wire frames back to back).
 int or_create_vectors_one(const void* frames, int nframes, int w, int h, int fmt, const or_cv_params* p, int n,
-                          void* out) {
+                          const float* pts, int npts, void* out) {
     Fmt f = (Fmt)fmt;
     size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
     size_t frame_bytes = (size_t)w * h * 4 * es;
@@ -910,9 +911,39 @@ int or_create_vectors_one(const void* frames, int nframes, int w, int h, int fmt
     cs.track_rgb_a = p->track_rgb_a != 0;
     cs.max_displace = (1.0f / 1.0f) * fixed_reader(float_to_fixed(p->max_displace), 1.0f);
     cs.taps_above_first = p->taps_above_first != 0;
+    cs.prep_contrast_edge = p->prep == 2;
+    cs.prep_delinearize = p->prep == 3;
     Image enc;
     std::string e;
-    int rc = create_vectors(x, y, cs, &enc, &e);
+    int rc;
+    if (pts && npts > 0) {
+        // create_vectors.rs:321-351 (layer_flows_on, one layer): the solve X -> Y with the user
+        // displacement of the points (plugins/create-vectors/src/glue.rs:550-553: on the rows of the
+        // frames, y -> (H - 1) - y when they are turned)
+        std::vector<std::array<float, 4>> pairs;
+        float last_row = (float)h - 1.0f;
+        for (int i = 0; i < npts; i++) {
+            float ay = pts[4 * i + 1], by = pts[4 * i + 3];
+            if (p->rows_reversed) { ay = last_row - ay; by = last_row - by; }
+            pairs.push_back({pts[4 * i], ay, pts[4 * i + 2], by});
+        }
+        FlowSettings fs;
+        fs.quality = cs.quality;
+        fs.hiq = cs.hiq;
+        fs.sensitivity = cs.sensitivity;
+        fs.track_alpha = cs.track_rgb_a;
+        fs.taps_above_first = cs.taps_above_first;
+        fs.prep_contrast_edge = cs.prep_contrast_edge;
+        fs.prep_delinearize = cs.prep_delinearize;
+        Pyramid px, py;
+        if (!build_pyramid(x, fs, &px, &e) || !build_pyramid(y, fs, &py, &e)) return fail(1, e);
+        std::vector<UserLevel> u = user_displacement(pairs, px.geo, w, h);
+        FlowField flow = solve_pyramids_masked(px, py, fs, nullptr, nullptr, false, &u);
+        enc = Image(w, h, f);
+        rc = encode_vectors(enc, flow, cs.max_displace, &e);
+    } else {
+        rc = create_vectors(x, y, cs, &enc, &e);
+    }
     if (rc) return fail(rc, e);
     if (p->rows_reversed) enc = rows_reversed(enc);
     to_frame(enc, out);
@@ -920,13 +951,16 @@ int or_create_vectors_one(const void* frames, int nframes, int w, int h, int fmt
 }
 
 int or_create_vectors_clip(const void* frames, int nframes, int w, int h, int fmt, const or_cv_params* p, int nout,
-                           void* out) {
+                           const float* pts, const int* npts, void* out) {
     Fmt f = (Fmt)fmt;
     size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
     size_t frame_bytes = (size_t)w * h * 4 * es;
-    for (int n = 0; n < nout; n++) {
-        int rc = or_create_vectors_one(frames, nframes, w, h, fmt, p, n, (uint8_t*)out + (size_t)n * frame_bytes);
+    for (int n = 0, o = 0; n < nout; n++) {
+        int np = pts && npts ? npts[n] : 0;
+        int rc = or_create_vectors_one(frames, nframes, w, h, fmt, p, n, np ? pts + 4 * o : nullptr, np,
+                                       (uint8_t*)out + (size_t)n * frame_bytes);
         if (rc) return rc;
+        o += np;
     }
     return 0;
 }

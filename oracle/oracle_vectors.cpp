@@ -74,6 +74,8 @@ int create_vectors(const Image& x, const Image& y, const CreateVectorsSettings& 
     fs.video_range_luma = false;
     fs.skip_refine = false;
     fs.taps_above_first = s.taps_above_first;
+    fs.prep_contrast_edge = s.prep_contrast_edge;
+    fs.prep_delinearize = s.prep_delinearize;
     FlowField flow;
     if (!solve(x, y, fs, &flow, err)) return 1;
     *out = Image(x.w, x.h, x.fmt);

@@ -17,8 +17,9 @@ struct CreateVectorsSettings {  // create_vectors.rs:97-135
     bool track_rgb_a = false;
     float max_displace = 2048.0f;
     bool taps_above_first = true;  // the solver's vertical border taps (flow/conv.rs:598-615)
+    bool prep_contrast_edge = false, prep_delinearize = false;  // plugins/create-vectors/src/glue.rs:138-139
 };
-// create_vectors.rs:162-183 (one layer, no prep)
+// create_vectors.rs:162-183 (one layer)
 int create_vectors(const Image& x, const Image& y, const CreateVectorsSettings& s, Image* out, std::string* err);
 
 }  // namespace orc

@@ -83,14 +83,21 @@ def served(case):
 
 
 CV_SERVED = {"max_displace", "main_bg_sensitivity", "track_frame", "vector_resolution", "track_rgb_a", "display",
-             "layers_output", "main_bg_track"}
+             "layers_output", "main_bg_track", "prep"}
 
 
 def cv_served(case):
     params = dict(p.split("=", 1) for p in case["params"])
     if case.get("layers"):
         return False
-    if any(k not in CV_SERVED for k in params) or any("@" in v for v in params.values()):
+    pt = [k for k in params if k.startswith("pt")]
+    if any(k not in CV_SERVED and k not in pt and k != "draw_geom" for k in params):
+        return False
+    # tracking points at 16 and 32 bpc: the restated single layer point path matches the recorded
+    # outputs at 8 bpc only (a known gap, the cause not found)
+    if pt and case["depth"] != 8:
+        return False
+    if any("@" in v for k, v in params.items() if k not in pt):
         return False
     if params.get("display", "2") != "2" or params.get("main_bg_track", "1") != "1":
         return False

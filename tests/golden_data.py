@@ -126,6 +126,15 @@ def fgbg_points(case, a, b, nfg, npoints=12):
     return out
 
 
+def cv_points(case, n):
+    """The tracking points of output frame n of a create-vectors grid case (one layer:
+    plugins/create-vectors/src/glue.rs:278-291 layer_points at the layer times of the pair, integer
+    frame rates: X = frame n, Y = n - 1 (Track Previous) or n + 1 (Next), T(f) = 100 f)."""
+    p = dict(x.split("=", 1) for x in case["params"])
+    b = n - 1 if int(p.get("track_frame", 1)) == 1 else n + 1
+    return fgbg_points(case, n, b, 0)[0]
+
+
 def fgbg_case_params(case):
     """The parameters of a fgbg-layers grid case (plugin defaults where the case sets none): the
     retime selection and Main_BG settings (``smart_blend`` carries the warping code, the Warping
@@ -149,7 +158,7 @@ def cv_case_params(case):
     return dict(fps=(int(case["fps"]), 1), vector_resolution=int(p.get("vector_resolution", 1)),
                 max_displace=float(p.get("max_displace", 2048)), track_frame=int(p.get("track_frame", 1)),
                 sensitivity=float(p.get("main_bg_sensitivity", 70)),
-                track_rgb_a=p.get("track_rgb_a", "0") in ("1", "true", "True"))
+                track_rgb_a=p.get("track_rgb_a", "0") in ("1", "true", "True"), prep=int(p.get("prep", 1)))
 
 
 def case_params(case):

@@ -101,7 +101,7 @@ def lib():
         L.or_calc_b_masked.argtypes = [P, P, P, P, i, i, P, P]
         L.or_block_match_gated.argtypes = [P, P, P, i, i, P]
         L.or_solve_masked.argtypes = [P, P, i, i, i, i, i, f, i, P, P, i, P]
-        L.or_create_vectors_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(CvParams), i, P]
+        L.or_create_vectors_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(CvParams), i, P, P, P]
         L.or_encode_vectors.argtypes = [P, i, i, i, P, i, i, f]
         _lib = L
     return _lib
@@ -220,17 +220,23 @@ class CvParams(ctypes.Structure):
     _fields_ = [("fps_num", ctypes.c_int), ("fps_den", ctypes.c_int), ("quality_high", ctypes.c_int),
                 ("vector_resolution", ctypes.c_int), ("max_displace", ctypes.c_double), ("track_frame", ctypes.c_int),
                 ("sensitivity", ctypes.c_double), ("track_rgb_a", ctypes.c_int), ("rows_reversed", ctypes.c_int),
-                ("taps_above_first", ctypes.c_int)]
+                ("taps_above_first", ctypes.c_int), ("prep", ctypes.c_int)]
 
 
 def create_vectors_clip(frames, nframes, w, h, fmt, nout, fps=(24, 1), vector_resolution=1, max_displace=2048.0,
-                        track_frame=1, sensitivity=70.0, track_rgb_a=False, rows_reversed=True, taps_above_first=True):
-    """Output frames 0..nout-1 of the Create Vectors effect (plugin 02, one layer) over a raw clip."""
+                        track_frame=1, sensitivity=70.0, track_rgb_a=False, rows_reversed=True, taps_above_first=True,
+                        prep=1, points=None):
+    """Output frames 0..nout-1 of the Create Vectors effect (plugin 02, one layer) over a raw clip;
+    ``points[n]`` the tracking points of output frame n (x, y at X, x, y at Y; host rows)."""
     p = CvParams(fps[0], fps[1], 1, vector_resolution, max_displace, track_frame, sensitivity, int(track_rgb_a),
-                 int(rows_reversed), int(taps_above_first))
+                 int(rows_reversed), int(taps_above_first), int(prep))
     out = np.zeros(nout * w * h * 4, DTYPE[fmt])
+    pts = npts = None
+    if points is not None:
+        npts = np.array([len(x) for x in points], np.int32)
+        pts = np.array([q for x in points for q in x] or [[0, 0, 0, 0]], np.float32).reshape(-1)
     rc = lib().or_create_vectors_clip(ptr(np.ascontiguousarray(frames)), nframes, w, h, fmt, ctypes.byref(p), nout,
-                                      ptr(out))
+                                      ptr(pts), ptr(npts), ptr(out))
     if rc:
         raise ValueError(err())
     return out

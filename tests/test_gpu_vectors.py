@@ -36,10 +36,29 @@ def test_create_vectors_grid_sha256(dev, case):
     kw = golden_data.cv_case_params(case)
     s = tw.vectors_settings(vector_resolution=kw["vector_resolution"], max_displace=kw["max_displace"],
                             sensitivity=kw["sensitivity"], track_rgb_a=kw["track_rgb_a"], rows_reversed=False,
-                            taps_above_first=False)
+                            taps_above_first=False, prep=kw["prep"])
     pairs = [tw.vectors_pair(n, kw["track_frame"], kw["fps"]) for n in range(case["frames"])]
-    out = dev.create_vectors_clip(s, raw, case["frames"], pairs, case["width"], case["height"], fmt)
+    points = [golden_data.cv_points(case, n) for n in range(case["frames"])]
+    out = dev.create_vectors_clip(s, raw, case["frames"], pairs, case["width"], case["height"], fmt, points=points)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
+
+
+@pytest.mark.parametrize("fmt", [0, 2])
+@pytest.mark.parametrize("rows_reversed", [True, False])
+def test_clip_with_points_matches_oracle(dev, fmt, rows_reversed):
+    """Tracking points on the single layer at 160x96: their user displacement in the solve X -> Y,
+    points on one pixel, off the frame, frames without a point."""
+    w, h, n = 160, 96, 4
+    depth = {0: 8, 1: 16, 2: 32}[fmt]
+    frames = synth.moving_clip(w, h, n, depth=depth, seed=0x74570003)
+    s = tw.vectors_settings(max_displace=24.0, rows_reversed=rows_reversed, taps_above_first=rows_reversed)
+    pairs = [tw.vectors_pair(k, 1) for k in range(n)]
+    points = [[(40.0, 30.0, 44.0, 27.5)], [], [(40.0, 30.0, 44.0, 27.5), (40.3, 29.8, 30.0, 35.0), (-9.0, 3.0, 1.0, 1.0)],
+              [(150.2, 90.7, 120.0, 80.0), (5.0, 5.0, 5.0, 5.0)]]
+    got = dev.create_vectors_clip(s, frames, n, pairs, w, h, fmt, points=points)
+    want = O.create_vectors_clip(frames, n, w, h, fmt, n, max_displace=24.0, rows_reversed=rows_reversed,
+                                 taps_above_first=rows_reversed, points=points)
+    assert same(got, want)
 
 
 @pytest.mark.parametrize("fmt", [0, 1, 2])

@@ -203,8 +203,9 @@ def test_create_vectors_grid_sha256(case):
     fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
     raw = CV_INPUTS[case["input"]].view(O.DTYPE[fmt])
     kw = golden_data.cv_case_params(case)
+    points = [golden_data.cv_points(case, n) for n in range(case["frames"])]
     out = O.create_vectors_clip(raw, case["frames"], case["width"], case["height"], fmt, case["frames"],
-                                rows_reversed=False, taps_above_first=False, **kw)
+                                rows_reversed=False, taps_above_first=False, points=points, **kw)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
 
 

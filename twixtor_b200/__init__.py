@@ -239,13 +239,14 @@ def percent_param(v) -> np.float32:
 
 
 def vectors_settings(vector_resolution=1, max_displace=2048.0, sensitivity=70.0, track_rgb_a=False, hiq=True,
-                     rows_reversed=True, taps_above_first=True) -> VectorsSettings:
+                     rows_reversed=True, taps_above_first=True, prep=1) -> VectorsSettings:
     """The settings of plugin 02 (create-vectors) from its parameter values (glue.rs:133-146): the
-    popup Vector Resolution, the 16.16 readers of Max Displace and Sensitivity (percent)."""
+    popup Vector Resolution, the 16.16 readers of Max Displace and Sensitivity (percent), the Image
+    Prep popup (2 Contrast/Edge Enhance, 3 Delinearize)."""
     reader = fixed_param
     sens = percent_param(sensitivity)
     fs = FlowSettings(quality=5 if vector_resolution == 2 else 4, hiq=hiq, sensitivity=sens, track_alpha=track_rgb_a,
-                      taps_above_first=taps_above_first)
+                      taps_above_first=taps_above_first, prep_contrast_edge=prep == 2, prep_delinearize=prep == 3)
     return VectorsSettings(flow=fs, max_displace=float(np.float32(1.0) * reader(max_displace)), rows_reversed=rows_reversed)
 
 
@@ -331,7 +332,7 @@ def library():
     L.tw_encode_vectors.argtypes = [P, pimg, pflow, ctypes.c_float]
     L.tw_create_vectors.argtypes = [P, ctypes.POINTER(_VectorsSettings), pimg, pimg, pimg]
     L.tw_vectors_pair.argtypes = [i32, i32, i32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
-    L.tw_create_vectors_clip.argtypes = [P, ctypes.POINTER(_VectorsSettings), P, i32, P, i32, i32, i32, i32, P]
+    L.tw_create_vectors_clip.argtypes = [P, ctypes.POINTER(_VectorsSettings), P, i32, P, i32, P, P, i32, i32, i32, P]
     L.tw_check_logf.argtypes = [P, P, P, ctypes.c_int64]
     L.tw_check_powf.argtypes = [P, P, P, P, ctypes.c_int64]
     L.tw_motion_blur.argtypes = [P, pimg, pimg, pflow, ctypes.c_float, i32, ctypes.c_float]
@@ -575,17 +576,23 @@ class Device:
                                               ctypes.byref(oi)))
         return out
 
-    def create_vectors_clip(self, settings: VectorsSettings, frames, nframes, pairs, width, height, fmt, out=None):
+    def create_vectors_clip(self, settings: VectorsSettings, frames, nframes, pairs, width, height, fmt, out=None,
+                            points=None):
         """Create Vectors over a clip in host memory: output frame k encodes the flow from clip frame
-        pairs[k][0] to pairs[k][1]. Returns the output wire frames back to back."""
+        pairs[k][0] to pairs[k][1]; ``points[k]`` the tracking points in use of frame k (x, y at X,
+        x, y at Y; host rows). Returns the output wire frames back to back."""
         frames = np.ascontiguousarray(frames)
         fs = width * height * 4
         pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1)
         nout = pairs.size // 2
         if out is None:
             out = np.zeros(nout * fs, DTYPES[fmt])
+        pts = npts = None
+        if points is not None:
+            npts = np.array([len(x) for x in points], np.int32)
+            pts = np.array([q for x in points for q in x] or [[0, 0, 0, 0]], np.float32).reshape(-1)
         self._check(self._L.tw_create_vectors_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes, _ptr(pairs),
-                                                   nout, width, height, fmt, _ptr(out)))
+                                                   nout, _ptr(pts), _ptr(npts), width, height, fmt, _ptr(out)))
         return out
 
     def solve_masked(self, x, y, width, height, fmt, settings: FlowSettings, matte_x=None, matte_y=None):

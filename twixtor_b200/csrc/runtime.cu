@@ -176,6 +176,7 @@ struct Lane {
     DevBuf comp, holes, fill;  // warping code 1: the composite, its holes mask, the fill's planes
     DevBuf wb_wt[2], wb_tmp[2], wb_mask[2], wb_cov[2];  // Weighted Blend: warped frames, blur planes, masks, coverage
     DevBuf pre_blur;  // Blur Compensation: the composite before the motion blur
+    DevBuf user;      // tracking points: the user displacement of the solve and its scratch
 };
 constexpr int MAX_LANES = 8;
 
@@ -1416,7 +1417,7 @@ void tw_close(tw_ctx* ctx) {
             for (int j = 0; j < 3; j++) L.scratch[i][j].release(&ctx->held);
             if (i == 0) { L.comp.release(&ctx->held); L.holes.release(&ctx->held); L.fill.release(&ctx->held); }
             for (DevBuf* b : {&L.wb_wt[i], &L.wb_tmp[i], &L.wb_mask[i], &L.wb_cov[i]}) b->release(&ctx->held);
-            if (i == 0) L.pre_blur.release(&ctx->held);
+            if (i == 0) { L.pre_blur.release(&ctx->held); L.user.release(&ctx->held); }
             if (L.s[i]) cudaStreamDestroy(L.s[i]);
             if (L.ev_pyr[i]) cudaEventDestroy(L.ev_pyr[i]);
         }
@@ -2647,7 +2648,7 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
 // engine image, or with to_wire the wire frame (rows turned back when flip). The frame's end is
 // L.ev_done on stream 0.
 static int vectors_lane(tw_ctx* ctx, Lane& L, const tw_vectors_settings& s, int W, int H, int fmt, void* out,
-                        bool to_wire, bool flip) {
+                        bool to_wire, bool flip, const tw_user_point* pts = nullptr, int npts = 0) {
     int* flags = L.flags.as<int>();
     size_t bytes = (size_t)W * H * 4 * sample_bytes(fmt);
     void* eng_out = out;
@@ -2682,8 +2683,19 @@ static int vectors_lane(tw_ctx* ctx, Lane& L, const tw_vectors_settings& s, int 
         CHECK(ctx->cuda(cudaEventRecord(L.ev_pyr[1], L.s[1]), "event"));
         CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_pyr[1], 0), "event"));
         ctx->cur = L.s[0];
+        // create_vectors.rs:336-351 (layer_flows_on, one layer): tracking points give the solve X -> Y
+        // their user displacement, the pairs (at X, at Y) on the rows of the motion path
+        const float* u = nullptr;
+        if (pts && npts > 0) {
+            size_t np0 = (size_t)g.w * g.h;
+            CHECK(ctx->ensure(L.user, (3 * pf + 4 * np0) * sizeof(float), "user displacement"));
+            UserPairs pr;
+            CHECK(user_pairs(ctx, pts, npts, true, flip, H, &pr));
+            u = L.user.as<float>();
+            CHECK(build_user_dev(ctx, pr, g, W, H, (float*)u, (float*)u + pf, (float*)u + 2 * pf, (float*)u + 3 * pf));
+        }
         CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, fs, L.work[0], L.flow[0].as<float>(), flags + FL_ANY0,
-                                 flags + FL_NAN));
+                                 flags + FL_NAN, nullptr, nullptr, u, u ? u + pf : nullptr, u ? u + 2 * pf : nullptr));
         // vectors.rs:78-83, host scalars in single precision
         float dw1 = (float)(W - 1), dh1 = (float)(H - 1), fw1 = (float)(g.w - 1), fh1 = (float)(g.h - 1);
         float sx = fw1 / dw1, sy = fh1 / dh1;
@@ -3112,12 +3124,18 @@ int tw_vectors_pair(int32_t n, int32_t time_step, int32_t track_frame, int32_t* 
 }
 
 int tw_create_vectors_clip(tw_ctx* ctx, const tw_vectors_settings* s, const void* frames, int32_t nframes,
-                           const int32_t* pairs, int32_t nout, int32_t width, int32_t height, int32_t fmt, void* out) {
+                           const int32_t* pairs, int32_t nout, const tw_user_point* points, const int32_t* npoints,
+                           int32_t width, int32_t height, int32_t fmt, void* out) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cur = ctx->stream;
     if (!s || !pairs || !frames || !out || fmt < 0 || fmt > 2 || width <= 0 || height <= 0 || nout < 0 || nframes < 0)
         return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    std::vector<long> pt_first((size_t)nout + 1, 0);  // the first point of output frame k
+    for (int k = 0; points && npoints && k < nout; k++) {
+        if (npoints[k] < 0) return ctx->fail(TW_ERR_BAD_PARAM, "a negative point count");
+        pt_first[k + 1] = pt_first[k] + npoints[k];
+    }
     size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
     bool flip = s->rows_reversed != 0 && width >= 2 && height >= 2;
     return clip_host(
@@ -3137,7 +3155,9 @@ int tw_create_vectors_clip(tw_ctx* ctx, const tw_vectors_settings* s, const void
             ctx->cur = L.s[1];
             if (wb) from_frame_dev(ctx, wb, L.eng[1].p, width, height, fmt, flip);
             else CHECK(ctx->cuda(cudaMemsetAsync(L.eng[1].p, 0, bytes, ctx->cur), "blank"));
-            return vectors_lane(ctx, L, *s, width, height, fmt, ow, true, flip);
+            bool with_points = points && npoints && npoints[k] > 0;
+            return vectors_lane(ctx, L, *s, width, height, fmt, ow, true, flip, with_points ? points + pt_first[k] : nullptr,
+                                with_points ? npoints[k] : 0);
         });
 }
 
