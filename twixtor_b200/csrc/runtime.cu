@@ -2080,6 +2080,8 @@ static int refill_dev(tw_ctx* ctx, void* p, int W, int H, int fmt, const float* 
 // row order), `mat` the 2 x nfg raw mattes on the device (A's, then B's; FG1 first). The layers of
 // the job's display group are solved and composed. Clears the flags first; *res_out receives the
 // engine result (device).
+static int lane_ready(tw_ctx* ctx, Lane& L);
+
 static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selection& sel_, const tw_layer_job& job,
                       const float* mat, int W, int H, int fmt, void** res_out, const tw_user_point* pts = nullptr,
                       const int32_t* npts = nullptr, bool flip_points = false) {
@@ -2111,7 +2113,7 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     size_t o_raw = take(2 * (size_t)nfg * n), o_cut = take(shrink ? 2 * (size_t)nfg * n : 0), o_comp = take(2 * (size_t)L * n);
     size_t o_smat = take(2 * (size_t)n), o_img = take(2 * (size_t)L * ib / 4 + 1), o_plate = take(2 * ib / 4 + 1);
     size_t o_res = take(ib / 4 + 1), o_flow = take(2 * (size_t)L * fb), o_pyr = take(4 * pf), o_mpyr = take(2 * pf);
-    size_t o_scr = take(4 * (size_t)n);
+    size_t o_scr = take(4 * (size_t)n), o_side1 = take(5 * (size_t)n);
     bool any_points = false;
     for (int k = 0; pts && npts && k <= nfg; k++) any_points = any_points || npts[k] > 0;
     size_t o_user = take(any_points ? 6 * pf : 0);
@@ -2131,6 +2133,8 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     float* pyr[2] = {M + o_pyr, M + o_pyr + 2 * pf};
     float* mpyr[2] = {M + o_mpyr, M + o_mpyr + pf};
     float* scr = M + o_scr;
+    float* smat_b = M + o_side1;   // side B's solver matte and scratch (its pyramids run on a second stream)
+    float* scr_b = smat_b + n;
     int* flags = ctx->flags.as<int>();
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
     CHECK(ctx->cuda(cudaMemsetAsync(flags + FL_ONE, 0x01, sizeof(int), ctx->stream), "flags"));
@@ -2157,43 +2161,61 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     }
     int pt_first[4] = {0, 0, 0, 0};
     for (int k = 1; pts && npts && k <= nfg; k++) pt_first[k] = pt_first[k - 1] + npts[k - 1];
+    // The two sides of a layer are independent until its solves, and its two solves of each other:
+    // side A's pyramids and F_AB run on the context's stream, side B's and F_BA on a second stream,
+    // each with its own scratch; the streams join before the solves and after them.
+    Lane& L2 = ctx->lanes[0];
+    CHECK(lane_ready(ctx, L2));
+    cudaStream_t st[2] = {ctx->stream, L2.s[1]};
+    auto join = [&]() -> int {  // each stream waits for the other's work so far
+        CHECK(ctx->cuda(cudaEventRecord(L2.ev_pyr[0], st[0]), "event"));
+        CHECK(ctx->cuda(cudaEventRecord(L2.ev_pyr[1], st[1]), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(st[1], L2.ev_pyr[0], 0), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(st[0], L2.ev_pyr[1], 0), "event"));
+        return TW_OK;
+    };
     for (int k = first; k <= last; k++) {
         tw_flow_settings fs = fs0;
         fs.sensitivity = job.sensitivity[k];
         Geo gk;
         CHECK(geometry(fs, W, H, &gk, &ctx->err));
-        // layers.rs:257-270 (solve_layer): a layer with points solves with their user displacement
-        int np_k = pts && npts ? npts[k] : 0;
-        const float *uab[3] = {nullptr, nullptr, nullptr}, *uba[3] = {nullptr, nullptr, nullptr};
-        if (np_k > 0) {
-            UserPairs pr;
-            float* u = user;
-            if (need_ab) {
-                CHECK(user_pairs(ctx, pts + pt_first[k], np_k, true, flip_points, H, &pr));
-                CHECK(build_user_dev(ctx, pr, gk, W, H, u, u + pf, u + 2 * pf, scr));
-                uab[0] = u; uab[1] = u + pf; uab[2] = u + 2 * pf;
-            }
-            if (need_ba) {
-                CHECK(user_pairs(ctx, pts + pt_first[k], np_k, false, flip_points, H, &pr));
-                CHECK(build_user_dev(ctx, pr, gk, W, H, u + 3 * pf, u + 4 * pf, u + 5 * pf, scr));
-                uba[0] = u + 3 * pf; uba[1] = u + 4 * pf; uba[2] = u + 5 * pf;
-            }
-        }
         tw_flow_settings fp = fs;
         fp.wrap = pyramid_wrap ? 1 : 0;
+        // layers.rs:257-270 (solve_layer): a layer with points solves with their user displacement
+        int np_k = pts && npts ? npts[k] : 0;
+        const float* ud[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};  // F_AB's, F_BA's
+        CHECK(join());
         for (int side = 0; side < 2; side++) {
-            CHECK(build_pyramid_dev(ctx, img(side, k), W, H, fmt, fp, gk, pyr[side], pyr[side] + pf, ctx->plane));
+            ctx->cur = st[side];
+            float* sm = side ? smat_b : smat;
+            float* sc = side ? scr_b : scr;
+            CHECK(build_pyramid_dev(ctx, img(side, k), W, H, fmt, fp, gk, pyr[side], pyr[side] + pf,
+                                    side ? L2.scratch[1] : ctx->plane));
             LAUNCH(ctx, k_solver_mask, grid1(n), TB, 0, raw + (size_t)side * nfg * n, nfg, k,
-                   comp + ((size_t)side * L + k) * n, n, fmt, smat);
-            CHECK(build_mask_pyramid_dev(ctx, smat, W, H, fs, gk, mpyr[side], scr, scr + n, flags + FL_ONE));
+                   comp + ((size_t)side * L + k) * n, n, fmt, sm);
+            CHECK(build_mask_pyramid_dev(ctx, sm, W, H, fs, gk, mpyr[side], sc, sc + n, flags + FL_ONE));
+            if (np_k > 0 && (side == 0 ? need_ab : need_ba)) {
+                UserPairs pr;
+                float* u = user + (size_t)side * 3 * pf;
+                CHECK(user_pairs(ctx, pts + pt_first[k], np_k, side == 0, flip_points, H, &pr));
+                CHECK(build_user_dev(ctx, pr, gk, W, H, u, u + pf, u + 2 * pf, sc));
+                ud[side][0] = u; ud[side][1] = u + pf; ud[side][2] = u + 2 * pf;
+            }
         }
-        if (need_ab)
+        CHECK(join());
+        if (need_ab) {
+            ctx->cur = st[0];
             CHECK(solve_pyramids_dev(ctx, pyr[0], pyr[1], pyr[0] + pf, pyr[1] + pf, gk, fs, ctx->work[0], flow(0, k),
-                                     flags + FL_ANY0, flags + FL_NAN, mpyr[0], mpyr[1], uab[0], uab[1], uab[2]));
-        if (need_ba)
-            CHECK(solve_pyramids_dev(ctx, pyr[1], pyr[0], pyr[1] + pf, pyr[0] + pf, gk, fs, ctx->work[0], flow(1, k),
-                                     flags + FL_ANY1, flags + FL_NAN, mpyr[1], mpyr[0], uba[0], uba[1], uba[2]));
+                                     flags + FL_ANY0, flags + FL_NAN, mpyr[0], mpyr[1], ud[0][0], ud[0][1], ud[0][2]));
+        }
+        if (need_ba) {
+            ctx->cur = st[1];
+            CHECK(solve_pyramids_dev(ctx, pyr[1], pyr[0], pyr[1] + pf, pyr[0] + pf, gk, fs, ctx->work[1], flow(1, k),
+                                     flags + FL_ANY1, flags + FL_NAN, mpyr[1], mpyr[0], ud[1][0], ud[1][1], ud[1][2]));
+        }
     }
+    CHECK(join());
+    ctx->cur = ctx->stream;
     // the composition of the group, bottom layer first, over an empty image (plates.rs:373-412)
     WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
     SmartScratch ss{nullptr, &ctx->fill, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB, &ctx->pre_blur};
