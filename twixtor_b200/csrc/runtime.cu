@@ -2105,18 +2105,19 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     size_t pf = pyramid_floats(g);
     size_t fb = (size_t)g.w * g.h * 2;
     int L = nfg + 1;
-    // one block: raw and cut planes (2 sides x nfg), comp planes (2 x L), a solver matte, layer
-    // images (2 x L), two plates, the result, the flows (2 x L), pyramids and mask pyramids (2
-    // each), scratch
+    // one block: raw and cut planes (2 sides x nfg), comp planes (2 x L), layer images (2 x L), two
+    // plates, the result, the flows (2 x L), per solved layer and side its pyramids, mask pyramid,
+    // solver matte and scratch, and the user displacements
     size_t fl = 0;
     auto take = [&](size_t floats) { size_t o = fl; fl += (floats + 63) & ~(size_t)63; return o; };
     size_t o_raw = take(2 * (size_t)nfg * n), o_cut = take(shrink ? 2 * (size_t)nfg * n : 0), o_comp = take(2 * (size_t)L * n);
-    size_t o_smat = take(2 * (size_t)n), o_img = take(2 * (size_t)L * ib / 4 + 1), o_plate = take(2 * ib / 4 + 1);
-    size_t o_res = take(ib / 4 + 1), o_flow = take(2 * (size_t)L * fb), o_pyr = take(4 * pf), o_mpyr = take(2 * pf);
-    size_t o_scr = take(4 * (size_t)n), o_side1 = take(5 * (size_t)n);
+    size_t o_img = take(2 * (size_t)L * ib / 4 + 1), o_plate = take(2 * ib / 4 + 1);
+    int G = last - first + 1;  // the layers solved, each on its own pair of streams with its own buffers
+    size_t o_res = take(ib / 4 + 1), o_flow = take(2 * (size_t)L * fb), o_pyr = take(4 * pf * G), o_mpyr = take(2 * pf * G);
+    size_t o_scr = take(4 * (size_t)n), o_sides = take(10 * (size_t)n * G);
     bool any_points = false;
     for (int k = 0; pts && npts && k <= nfg; k++) any_points = any_points || npts[k] > 0;
-    size_t o_user = take(any_points ? 6 * pf : 0);
+    size_t o_user = take(any_points ? 6 * pf * G : 0);
     CHECK(ctx->ensure(ctx->lay_mem, fl * sizeof(float), "layer buffers"));
     CHECK(ctx->ensure(ctx->holes, (size_t)n, "holes mask"));
     CHECK(ctx->ensure(ctx->eng[2], ib, "layer result"));
@@ -2125,16 +2126,16 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     float* raw = M + o_raw;
     float* cuts = shrink ? M + o_cut : nullptr;
     float* comp = M + o_comp;
-    float* smat = M + o_smat;
     auto img = [&](int side, int k) { return (void*)((char*)(M + o_img) + ((size_t)side * L + k) * ib); };
     void* plate[2] = {(void*)(M + o_plate), (void*)((char*)(M + o_plate) + ib)};
     void* res = (void*)(M + o_res);
     auto flow = [&](int dir, int k) { return M + o_flow + ((size_t)dir * L + k) * fb; };  // dir 0: F_AB, 1: F_BA
-    float* pyr[2] = {M + o_pyr, M + o_pyr + 2 * pf};
-    float* mpyr[2] = {M + o_mpyr, M + o_mpyr + pf};
+    // layer g of the group (g = k - first), side 0 (A) or 1 (B): its band pyramid (with the transposed
+    // copy), its mask pyramid, its solver matte plus four planes of scratch, its user displacement
+    auto pyr = [&](int g, int side) { return M + o_pyr + ((size_t)g * 2 + side) * 2 * pf; };
+    auto mpyr = [&](int g, int side) { return M + o_mpyr + ((size_t)g * 2 + side) * pf; };
+    auto sides = [&](int g, int side) { return M + o_sides + ((size_t)g * 2 + side) * 5 * (size_t)n; };
     float* scr = M + o_scr;
-    float* smat_b = M + o_side1;   // side B's solver matte and scratch (its pyramids run on a second stream)
-    float* scr_b = smat_b + n;
     int* flags = ctx->flags.as<int>();
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
     CHECK(ctx->cuda(cudaMemsetAsync(flags + FL_ONE, 0x01, sizeof(int), ctx->stream), "flags"));
@@ -2161,20 +2162,17 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     }
     int pt_first[4] = {0, 0, 0, 0};
     for (int k = 1; pts && npts && k <= nfg; k++) pt_first[k] = pt_first[k - 1] + npts[k - 1];
-    // The two sides of a layer are independent until its solves, and its two solves of each other:
-    // side A's pyramids and F_AB run on the context's stream, side B's and F_BA on a second stream,
-    // each with its own scratch; the streams join before the solves and after them.
-    Lane& L2 = ctx->lanes[0];
-    CHECK(lane_ready(ctx, L2));
-    cudaStream_t st[2] = {ctx->stream, L2.s[1]};
-    auto join = [&]() -> int {  // each stream waits for the other's work so far
-        CHECK(ctx->cuda(cudaEventRecord(L2.ev_pyr[0], st[0]), "event"));
-        CHECK(ctx->cuda(cudaEventRecord(L2.ev_pyr[1], st[1]), "event"));
-        CHECK(ctx->cuda(cudaStreamWaitEvent(st[1], L2.ev_pyr[0], 0), "event"));
-        CHECK(ctx->cuda(cudaStreamWaitEvent(st[0], L2.ev_pyr[1], 0), "event"));
-        return TW_OK;
-    };
+    // The layers of the group are independent until the composition, a layer's two sides until its
+    // solves, and its two solves of each other: layer g runs on the two streams of lane g (side A's
+    // pyramids and F_AB on the first, side B's and F_BA on the second) with its own buffers and range
+    // flags; the lanes fork from the context's stream here and join it before the composition.
+    CHECK(ctx->cuda(cudaEventRecord(ctx->ev_start, ctx->stream), "event"));
     for (int k = first; k <= last; k++) {
+        int g = k - first;
+        Lane& LL = ctx->lanes[g];
+        CHECK(lane_ready(ctx, LL));
+        cudaStream_t st[2] = {LL.s[0], LL.s[1]};
+        for (int i = 0; i < 2; i++) CHECK(ctx->cuda(cudaStreamWaitEvent(st[i], ctx->ev_start, 0), "event"));
         tw_flow_settings fs = fs0;
         fs.sensitivity = job.sensitivity[k];
         Geo gk;
@@ -2184,37 +2182,45 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
         // layers.rs:257-270 (solve_layer): a layer with points solves with their user displacement
         int np_k = pts && npts ? npts[k] : 0;
         const float* ud[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};  // F_AB's, F_BA's
-        CHECK(join());
         for (int side = 0; side < 2; side++) {
             ctx->cur = st[side];
-            float* sm = side ? smat_b : smat;
-            float* sc = side ? scr_b : scr;
-            CHECK(build_pyramid_dev(ctx, img(side, k), W, H, fmt, fp, gk, pyr[side], pyr[side] + pf,
-                                    side ? L2.scratch[1] : ctx->plane));
+            float* sm = sides(g, side);
+            float* sc = sm + n;
+            CHECK(build_pyramid_dev(ctx, img(side, k), W, H, fmt, fp, gk, pyr(g, side), pyr(g, side) + pf, LL.scratch[side]));
             LAUNCH(ctx, k_solver_mask, grid1(n), TB, 0, raw + (size_t)side * nfg * n, nfg, k,
                    comp + ((size_t)side * L + k) * n, n, fmt, sm);
-            CHECK(build_mask_pyramid_dev(ctx, sm, W, H, fs, gk, mpyr[side], sc, sc + n, flags + FL_ONE));
+            CHECK(build_mask_pyramid_dev(ctx, sm, W, H, fs, gk, mpyr(g, side), sc, sc + n, flags + FL_ONE));
             if (np_k > 0 && (side == 0 ? need_ab : need_ba)) {
                 UserPairs pr;
-                float* u = user + (size_t)side * 3 * pf;
+                float* u = user + ((size_t)g * 2 + side) * 3 * pf;
                 CHECK(user_pairs(ctx, pts + pt_first[k], np_k, side == 0, flip_points, H, &pr));
                 CHECK(build_user_dev(ctx, pr, gk, W, H, u, u + pf, u + 2 * pf, sc));
                 ud[side][0] = u; ud[side][1] = u + pf; ud[side][2] = u + 2 * pf;
             }
         }
-        CHECK(join());
+        // both sides' pyramids before either solve
+        CHECK(ctx->cuda(cudaEventRecord(LL.ev_pyr[0], st[0]), "event"));
+        CHECK(ctx->cuda(cudaEventRecord(LL.ev_pyr[1], st[1]), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(st[1], LL.ev_pyr[0], 0), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(st[0], LL.ev_pyr[1], 0), "event"));
+        int* lf = LL.flags.as<int>();
         if (need_ab) {
             ctx->cur = st[0];
-            CHECK(solve_pyramids_dev(ctx, pyr[0], pyr[1], pyr[0] + pf, pyr[1] + pf, gk, fs, ctx->work[0], flow(0, k),
-                                     flags + FL_ANY0, flags + FL_NAN, mpyr[0], mpyr[1], ud[0][0], ud[0][1], ud[0][2]));
+            CHECK(solve_pyramids_dev(ctx, pyr(g, 0), pyr(g, 1), pyr(g, 0) + pf, pyr(g, 1) + pf, gk, fs, LL.work[0],
+                                     flow(0, k), lf + FL_ANY0, flags + FL_NAN, mpyr(g, 0), mpyr(g, 1), ud[0][0], ud[0][1],
+                                     ud[0][2]));
         }
         if (need_ba) {
             ctx->cur = st[1];
-            CHECK(solve_pyramids_dev(ctx, pyr[1], pyr[0], pyr[1] + pf, pyr[0] + pf, gk, fs, ctx->work[1], flow(1, k),
-                                     flags + FL_ANY1, flags + FL_NAN, mpyr[1], mpyr[0], ud[1][0], ud[1][1], ud[1][2]));
+            CHECK(solve_pyramids_dev(ctx, pyr(g, 1), pyr(g, 0), pyr(g, 1) + pf, pyr(g, 0) + pf, gk, fs, LL.work[1],
+                                     flow(1, k), lf + FL_ANY1, flags + FL_NAN, mpyr(g, 1), mpyr(g, 0), ud[1][0], ud[1][1],
+                                     ud[1][2]));
         }
+        CHECK(ctx->cuda(cudaEventRecord(LL.ev_done, st[0]), "event"));
+        CHECK(ctx->cuda(cudaEventRecord(LL.ev_solve1, st[1]), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, LL.ev_done, 0), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, LL.ev_solve1, 0), "event"));
     }
-    CHECK(join());
     ctx->cur = ctx->stream;
     // the composition of the group, bottom layer first, over an empty image (plates.rs:373-412)
     WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
