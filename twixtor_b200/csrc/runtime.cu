@@ -2065,13 +2065,15 @@ static int raw_and_cut_planes(tw_ctx* ctx, const tw_layer_job& job, const float*
 // plates.rs:245-256 (refill) of the plate p of layer k at one side: unpremultiply, the pull-push fill
 // where the plate is not opaque, the alpha replaced by the layer's raw plane (plane) or the frame's
 // alpha (frame), premultiply
+// holes: w*h bytes of scratch for the hole mask; hole_flag / side1_flag: the "some hole" flag of this
+// fill and the refused fill of an image with a side of 1
 static int refill_dev(tw_ctx* ctx, void* p, int W, int H, int fmt, const float* plane, const void* frame,
-                      bool above_first, int* flags, DevBuf& fillbuf) {
+                      bool above_first, uint8_t* holes, int* hole_flag, int* side1_flag, DevBuf& fillbuf) {
     long n = (long)W * H;
-    CHECK(ctx->cuda(cudaMemsetAsync(flags + FL_HOLE, 0, sizeof(int), ctx->cur), "holes flag"));
-    LAUNCH(ctx, k_refill_pre, grid1(n), TB, 0, p, fmt, n, ctx->holes.as<uint8_t>(), flags + FL_HOLE);
-    if (W < 2 || H < 2) LAUNCH(ctx, k_hole_side1, 1, 1, 0, flags + FL_HOLE, flags + FL_SIDE1);
-    else CHECK(fill_dev(ctx, p, W, H, fmt, ctx->holes.as<uint8_t>(), flags + FL_HOLE, above_first, fillbuf));
+    CHECK(ctx->cuda(cudaMemsetAsync(hole_flag, 0, sizeof(int), ctx->cur), "holes flag"));
+    LAUNCH(ctx, k_refill_pre, grid1(n), TB, 0, p, fmt, n, holes, hole_flag);
+    if (W < 2 || H < 2) LAUNCH(ctx, k_hole_side1, 1, 1, 0, hole_flag, side1_flag);
+    else CHECK(fill_dev(ctx, p, W, H, fmt, holes, hole_flag, above_first, fillbuf));
     LAUNCH(ctx, k_refill_post, grid1(n), TB, 0, p, fmt, n, plane, frame);
     return TW_OK;
 }
@@ -2114,7 +2116,8 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     size_t o_img = take(2 * (size_t)L * ib / 4 + 1), o_plate = take(2 * ib / 4 + 1);
     int G = last - first + 1;  // the layers solved, each on its own pair of streams with its own buffers
     size_t o_res = take(ib / 4 + 1), o_flow = take(2 * (size_t)L * fb), o_pyr = take(4 * pf * G), o_mpyr = take(2 * pf * G);
-    size_t o_scr = take(4 * (size_t)n), o_sides = take(10 * (size_t)n * G);
+    size_t lres_floats = (ib + 255) / 256 * 64;  // one layer's composition, 256-byte aligned (8 and 16 B pixels)
+    size_t o_scr = take(4 * (size_t)n), o_sides = take(10 * (size_t)n * G), o_lres = take(G * lres_floats);
     bool any_points = false;
     for (int k = 0; pts && npts && k <= nfg; k++) any_points = any_points || npts[k] > 0;
     size_t o_user = take(any_points ? 6 * pf * G : 0);
@@ -2166,6 +2169,9 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
     // solves, and its two solves of each other: layer g runs on the two streams of lane g (side A's
     // pyramids and F_AB on the first, side B's and F_BA on the second) with its own buffers and range
     // flags; the lanes fork from the context's stream here and join it before the composition.
+    // warping codes 0 and 1 compose every layer on its lane too (codes 2 and 3 read the forward warp's
+    // hit counts back and compose on the context's stream)
+    bool lane_compose = cs.warp_mode < 2;
     CHECK(ctx->cuda(cudaEventRecord(ctx->ev_start, ctx->stream), "event"));
     for (int k = first; k <= last; k++) {
         int g = k - first;
@@ -2216,54 +2222,86 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
                                      flow(1, k), lf + FL_ANY1, flags + FL_NAN, mpyr(g, 1), mpyr(g, 0), ud[1][0], ud[1][1],
                                      ud[1][2]));
         }
-        CHECK(ctx->cuda(cudaEventRecord(LL.ev_done, st[0]), "event"));
         CHECK(ctx->cuda(cudaEventRecord(LL.ev_solve1, st[1]), "event"));
-        CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, LL.ev_done, 0), "event"));
-        CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, LL.ev_solve1, 0), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(st[0], LL.ev_solve1, 0), "event"));  // lane stream 0 after both solves
+        if (!lane_compose) {
+            CHECK(ctx->cuda(cudaEventRecord(LL.ev_done, st[0]), "event"));
+            CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, LL.ev_done, 0), "event"));
+        }
     }
     ctx->cur = ctx->stream;
-    // the composition of the group, bottom layer first, over an empty image (plates.rs:373-412)
-    WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
-    SmartScratch ss{nullptr, &ctx->fill, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB, &ctx->pre_blur};
-    DevBuf& fillbuf = ctx->work[1];
-    ss.holes = &ctx->masks;  // the composition's own holes mask (the refill uses ctx->holes)
-    auto refill = [&](void* p, int side, int k) -> int {
-        const float* plane = k == nfg ? nullptr : raw + ((size_t)side * nfg + k) * n;
-        return refill_dev(ctx, p, W, H, fmt, plane, frame[side], cs.taps_above_first != 0, flags, fillbuf);
-    };
-    if (last != nfg) CHECK(ctx->cuda(cudaMemsetAsync(res, 0, ib, ctx->stream), "empty result"));
-    for (int k = last; k >= first; k--) {
+    // the composition of the group, bottom layer first, over an empty image (plates.rs:373-412): each
+    // layer's own composition, then OVER
+    auto layer_res = [&](int k) { return (void*)(M + o_lres + (size_t)(k - first) * lres_floats); };
+    // one layer's composition into dst on ctx->cur, with the scratch given
+    auto compose_layer = [&](int k, void* const* plate, void* dst, const SmartScratch& sc, uint8_t* holes,
+                             int* hole_flag, DevBuf& fillbuf) -> int {
         const float* fab = need_ab ? flow(0, k) : nullptr;
         const float* fba = need_ba ? flow(1, k) : nullptr;
-        void* dst = k == nfg ? res : ctx->eng[2].p;
+        auto refill = [&](void* p, int side) -> int {
+            const float* plane = k == nfg ? nullptr : raw + ((size_t)side * nfg + k) * n;
+            return refill_dev(ctx, p, W, H, fmt, plane, frame[side], cs.taps_above_first != 0, holes, hole_flag,
+                              flags + FL_SIDE1, fillbuf);
+        };
         if (sel->interp == 0) {
             bool takes_a = cs.warp_mode == 0 ? 0.5f <= sel->wa : !(0.5f > sel->wa);  // layers.rs:697-703
             int side = takes_a ? 0 : 1;
             CHECK(ctx->cuda(cudaMemcpyAsync(plate[0], img(side, k), ib, cudaMemcpyDeviceToDevice, ctx->cur), "plate"));
-            CHECK(refill(plate[0], side, k));
-            CHECK(compose_dev(ctx, cs, *sel, plate[0], plate[0], fab, fba, g.w, g.h, W, H, fmt, dst, false, false,
-                              flags + FL_BAD, &ss));
-        } else {
-            // plates.rs:268-288: PA = LA OVER LB brought to A, PB = LB OVER LA brought to B, amount 1:
-            // the inverse warp with hold edges for codes 0 and 1 (LB read through F_AB), the forward
-            // warp without coverage for codes 2 and 3 (each side pushed by its own flow, LB by F_BA)
-            if (cs.warp_mode >= 2) {
-                CHECK(forward_warp_dev(ctx, img(1, k), fba, g.w, g.h, W, H, fmt, 1.0f, cs.gouraud == 0, plate[0], nullptr));
-                CHECK(forward_warp_dev(ctx, img(0, k), fab, g.w, g.h, W, H, fmt, 1.0f, cs.gouraud == 0, plate[1], nullptr));
-            } else {
-                WarpParams pa_ = warp_params(img(1, k), fab, g.w, g.h, 1.0f, W, true);
-                WarpParams pb_ = warp_params(img(0, k), fba, g.w, g.h, 1.0f, W, true);
-                LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pa_, fmt, plate[0], (uint8_t*)nullptr, W, H, flags + FL_BAD);
-                LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pb_, fmt, plate[1], (uint8_t*)nullptr, W, H, flags + FL_BAD);
-            }
-            LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, plate[0], img(0, k), fmt, n);
-            LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, plate[1], img(1, k), fmt, n);
-            CHECK(refill(plate[0], 0, k));
-            CHECK(refill(plate[1], 1, k));
-            CHECK(compose_dev(ctx, cs, *sel, plate[0], plate[1], fab, fba, g.w, g.h, W, H, fmt, dst, false, false,
-                              flags + FL_BAD, &ss));
+            CHECK(refill(plate[0], side));
+            return compose_dev(ctx, cs, *sel, plate[0], plate[0], fab, fba, g.w, g.h, W, H, fmt, dst, false, false,
+                               flags + FL_BAD, &sc);
         }
-        if (k != nfg) LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, res, dst, fmt, n);
+        // plates.rs:268-288: PA = LA OVER LB brought to A, PB = LB OVER LA brought to B, amount 1: the
+        // inverse warp with hold edges for codes 0 and 1 (LB read through F_AB), the forward warp without
+        // coverage for codes 2 and 3 (each side pushed by its own flow, LB by F_BA)
+        if (cs.warp_mode >= 2) {
+            CHECK(forward_warp_dev(ctx, img(1, k), fba, g.w, g.h, W, H, fmt, 1.0f, cs.gouraud == 0, plate[0], nullptr));
+            CHECK(forward_warp_dev(ctx, img(0, k), fab, g.w, g.h, W, H, fmt, 1.0f, cs.gouraud == 0, plate[1], nullptr));
+        } else {
+            WarpParams pa_ = warp_params(img(1, k), fab, g.w, g.h, 1.0f, W, true);
+            WarpParams pb_ = warp_params(img(0, k), fba, g.w, g.h, 1.0f, W, true);
+            LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pa_, fmt, plate[0], (uint8_t*)nullptr, W, H, flags + FL_BAD);
+            LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pb_, fmt, plate[1], (uint8_t*)nullptr, W, H, flags + FL_BAD);
+        }
+        LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, plate[0], img(0, k), fmt, n);
+        LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, plate[1], img(1, k), fmt, n);
+        CHECK(refill(plate[0], 0));
+        CHECK(refill(plate[1], 1));
+        return compose_dev(ctx, cs, *sel, plate[0], plate[1], fab, fba, g.w, g.h, W, H, fmt, dst, false, false,
+                           flags + FL_BAD, &sc);
+    };
+    if (lane_compose) {
+        for (int k = first; k <= last; k++) {
+            Lane& LL = ctx->lanes[k - first];
+            ctx->cur = LL.s[0];
+            for (int i = 0; i < 2; i++) CHECK(ctx->ensure(LL.eng[i], ib, "layer plates"));
+            CHECK(ctx->ensure(LL.comp, (size_t)n, "refill holes"));
+            int* lf = LL.flags.as<int>();
+            WbScratch wl = wb_scratch(LL.wb_wt, LL.wb_tmp, LL.wb_mask, LL.wb_cov);
+            SmartScratch sl{nullptr, &LL.holes, &LL.fill, lf + FL_HOLE, flags + FL_SIDE1, &wl, lf + FL_WB, &LL.pre_blur};
+            void* plates_l[2] = {LL.eng[0].p, LL.eng[1].p};
+            CHECK(compose_layer(k, plates_l, layer_res(k), sl, LL.comp.as<uint8_t>(), lf + FL_HOLE, LL.work[0]));
+            CHECK(ctx->cuda(cudaEventRecord(LL.ev_done, LL.s[0]), "event"));
+            CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, LL.ev_done, 0), "event"));
+        }
+        ctx->cur = ctx->stream;
+        if (last == nfg) {
+            res = layer_res(last);  // Main_BG's composition is the bottom of the stack
+        } else {
+            CHECK(ctx->cuda(cudaMemsetAsync(res, 0, ib, ctx->stream), "empty result"));
+            LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, res, layer_res(last), fmt, n);
+        }
+        for (int k = last - 1; k >= first; k--) LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, res, layer_res(k), fmt, n);
+    } else {
+        WbScratch wbs = wb_scratch(ctx->wb_wt, ctx->wb_tmp, ctx->wb_mask, ctx->wb_cov);
+        SmartScratch ss{nullptr, &ctx->masks, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB,
+                        &ctx->pre_blur};
+        if (last != nfg) CHECK(ctx->cuda(cudaMemsetAsync(res, 0, ib, ctx->stream), "empty result"));
+        for (int k = last; k >= first; k--) {
+            void* dst = k == nfg ? res : ctx->eng[2].p;
+            CHECK(compose_layer(k, plate, dst, ss, ctx->holes.as<uint8_t>(), flags + FL_HOLE, ctx->work[1]));
+            if (k != nfg) LAUNCH(ctx, k_over_pl, grid1(n), TB, 0, res, dst, fmt, n);
+        }
     }
     *res_out = res;
     return TW_OK;
@@ -2287,7 +2325,8 @@ static int rebuilt_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_
     auto take = [&](size_t floats) { size_t o = fl; fl += (floats + 63) & ~(size_t)63; return o; };
     size_t o_raw = take((size_t)nfg * n), o_cut = take(shrink ? (size_t)nfg * n : 0), o_comp = take((size_t)n);
     size_t o_l = take(ib / 4 + 1), o_p = take(ib / 4 + 1), o_q = take(ib / 4 + 1), o_alpha = take(ib / 4 + 1);
-    size_t o_r = take(2 * (ib / 4 + 1)), o_scr = take(4 * (size_t)n);
+    size_t img_floats = (ib + 255) / 256 * 64;  // an engine image, 256-byte aligned (8 and 16 B pixels)
+    size_t o_r = take(2 * img_floats), o_scr = take(4 * (size_t)n);
     CHECK(ctx->ensure(ctx->lay_mem, fl * sizeof(float), "layer buffers"));
     CHECK(ctx->ensure(ctx->holes, (size_t)n, "holes mask"));
     float* M = ctx->lay_mem.as<float>();
@@ -2298,7 +2337,7 @@ static int rebuilt_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_
     void* p = M + o_p;
     void* q = M + o_q;
     void* alpha = M + o_alpha;
-    void* r[2] = {(void*)(M + o_r), (void*)(M + o_r + (ib / 4 + 1))};
+    void* r[2] = {(void*)(M + o_r), (void*)(M + o_r + img_floats)};
     float* scr = M + o_scr;
     int* flags = ctx->flags.as<int>();
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
@@ -2324,7 +2363,8 @@ static int rebuilt_frame_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_
             fillme = q;
         }
         CHECK(refill_dev(ctx, fillme, W, H, fmt, k == nfg ? nullptr : plane, k == nfg ? fa : nullptr,
-                         s.compose.taps_above_first != 0, flags, ctx->work[1]));
+                         s.compose.taps_above_first != 0, ctx->holes.as<uint8_t>(), flags + FL_HOLE, flags + FL_SIDE1,
+                         ctx->work[1]));
         if (reversed) LAUNCH(ctx, k_flip_rows, grid1(n * (long)(px / 4)), TB, 0, (const void*)q, p, W, H, (int)px);
         if (k == nfg) {
             CHECK(ctx->cuda(cudaMemcpyAsync(r[side], p, ib, cudaMemcpyDeviceToDevice, ctx->stream), "plate"));
