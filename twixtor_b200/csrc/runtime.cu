@@ -206,6 +206,10 @@ struct tw_ctx {
     DevBuf eng[3], wire[3], pyr[2], plane[4], work[2], flow[2], flags, holes, fill, masks;
     DevBuf lay_mem;  // the layered path: planes, layer images, plates, flows
     DevBuf lay_in;   // the layered path: the raw mattes at A and B
+    // tw_retime_layers_clip: two staging slots (the footage pair and the matte frames of a frame),
+    // filled on the copy stream one frame ahead; uploaded / last read events per slot
+    DevBuf lay_stage[2][8];
+    cudaEvent_t lay_up[2] = {nullptr, nullptr}, lay_free[2] = {nullptr, nullptr};
     DevBuf fc_img[2], fc_cov[2];  // the forward compositions: the two pushed frames and their coverage
     DevBuf wb_wt[2], wb_tmp[2], wb_mask[2], wb_cov[2];  // Weighted Blend (the calls on the context's stream)
     DevBuf pre_blur, comp_e;  // Blur Compensation: the composite before the blur, the engine result
@@ -1435,6 +1439,11 @@ void tw_close(tw_ctx* ctx) {
     for (int i = 0; i < MAX_LANES; i++) {
         ctx->outbuf[i].release(&ctx->held);
         if (ctx->out_free[i]) cudaEventDestroy(ctx->out_free[i]);
+    }
+    for (int i = 0; i < 2; i++) {
+        for (auto& b : ctx->lay_stage[i]) b.release(&ctx->held);
+        if (ctx->lay_up[i]) cudaEventDestroy(ctx->lay_up[i]);
+        if (ctx->lay_free[i]) cudaEventDestroy(ctx->lay_free[i]);
     }
     if (ctx->up) cudaStreamDestroy(ctx->up);
     if (ctx->down) cudaStreamDestroy(ctx->down);
@@ -3050,24 +3059,56 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
     CHECK(ctx->ensure(ctx->flags, FLAGS_BYTES, "flags"));
     float* mat = ctx->lay_in.as<float>();
     int* flags = ctx->flags.as<int>();
-    // a frame of a clip in the staging buffer dst, or a blank frame outside the clip (host.rs:338-352)
+    if (!ctx->up) CHECK(ctx->cuda(cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking), "copy stream"));
+    for (int i = 0; i < 2; i++) {
+        if (!ctx->lay_up[i]) CHECK(ctx->cuda(cudaEventCreateWithFlags(&ctx->lay_up[i], cudaEventDisableTiming), "event"));
+        if (!ctx->lay_free[i]) CHECK(ctx->cuda(cudaEventCreateWithFlags(&ctx->lay_free[i], cudaEventDisableTiming), "event"));
+        for (int j = 0; j < 2 + 2 * nfg; j++) CHECK(ctx->ensure(ctx->lay_stage[i][j], bytes, "staging"));
+    }
+    // how output frame k is rendered: the vector path, the rebuilt plates of a single layer display or
+    // the interpolation of the two frames (compose.rs:209-211: with FG layers a shrink clears the
+    // exactness of a position)
+    auto is_vector = [&](const tw_selection& sel) {
+        bool exact = sel.exact && !(nfg > 0 && shrink);
+        return sel.vectors_quality != 0 && !exact;
+    };
+    auto is_rebuilt = [&](const tw_selection& sel) {
+        return !is_vector(sel) && nfg > 0 && !(first == 0 && last == nfg && !shrink);
+    };
+    // a frame of a clip into a staging buffer on the copy stream, or a blank frame outside the clip
+    // (host.rs:338-352)
     auto upload = [&](const void* clip, int count, int f, void* dst) -> int {
         if (f >= 0 && f < count)
             return ctx->cuda(cudaMemcpyAsync(dst, (const uint8_t*)clip + (size_t)f * bytes, bytes, cudaMemcpyHostToDevice,
-                                             ctx->stream), "upload");
-        return ctx->cuda(cudaMemsetAsync(dst, 0, bytes, ctx->stream), "blank");
+                                             ctx->up), "upload");
+        return ctx->cuda(cudaMemsetAsync(dst, 0, bytes, ctx->up), "blank");
     };
-    // a frame's FG mattes at A and at B, read straight (matte.rs:141-188) in the row order given
-    auto mattes = [&](const tw_selection& sel, bool flip) -> int {
+    // the uploads of output frame k into staging slot k % 2, once the frame before the last is done
+    // reading that slot: the footage pair, and each FG layer's matte frames at A and at B
+    auto stage = [&](int k) -> int {
+        const tw_selection& sel = sels[k];
+        int slot = k & 1;
+        CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->up, ctx->lay_free[slot], 0), "event"));
+        CHECK(upload(frames, nframes, sel.a, ctx->lay_stage[slot][0].p));
+        CHECK(upload(frames, nframes, sel.b, ctx->lay_stage[slot][1].p));
+        if (is_vector(sel) || is_rebuilt(sel))
+            for (int side = 0; side < 2; side++)
+                for (int j = 0; j < nfg; j++) {
+                    int count = matte_nframes ? matte_nframes[j] : nframes;
+                    CHECK(upload(matte_clips[j], count, side ? sel.b : sel.a, ctx->lay_stage[slot][2 + side * nfg + j].p));
+                }
+        return ctx->cuda(cudaEventRecord(ctx->lay_up[slot], ctx->up), "event");
+    };
+    // a frame's FG mattes at A and at B from its staging slot, read straight (matte.rs:141-188) in the
+    // row order given
+    auto mattes = [&](int slot, bool flip) -> int {
         for (int side = 0; side < 2; side++)
-            for (int j = 0; j < nfg; j++) {
-                int count = matte_nframes ? matte_nframes[j] : nframes;
-                CHECK(upload(matte_clips[j], count, side ? sel.b : sel.a, ctx->wire[2].p));
-                LAUNCH(ctx, k_matte_extract, grid1(n), TB, 0, ctx->wire[2].p, fmt, matte_chan[j], W, H, flip,
-                       mat + ((size_t)side * nfg + j) * n);
-            }
+            for (int j = 0; j < nfg; j++)
+                LAUNCH(ctx, k_matte_extract, grid1(n), TB, 0, ctx->lay_stage[slot][2 + side * nfg + j].p, fmt, matte_chan[j],
+                       W, H, flip, mat + ((size_t)side * nfg + j) * n);
         return TW_OK;
     };
+    if (nout > 0) CHECK(stage(0));
     long pt_off = 0;  // the first point of output frame k in job->points
     for (int k = 0; k < nout; k++) {
         const tw_selection& sel = sels[k];
@@ -3077,18 +3118,19 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
             if (npts[j] < 0) return ctx->fail(TW_ERR_BAD_PARAM, "a negative point count");
             pt_off += npts[j];
         }
-        // compose.rs:209-211 (layered_exact): with FG layers, a shrink clears the exactness of a position
-        bool exact = sel.exact && !(nfg > 0 && shrink);
-        bool vector = sel.vectors_quality != 0 && !exact;
+        if (k + 1 < nout) CHECK(stage(k + 1));  // the next frame's uploads overlap this frame's work
+        int slot = k & 1;
+        bool vector = is_vector(sel);
         bool flip = vector && s->motion_rows_reversed != 0;
-        CHECK(upload(frames, nframes, sel.a, ctx->wire[0].p));
-        CHECK(upload(frames, nframes, sel.b, ctx->wire[1].p));
-        from_frame_dev(ctx, ctx->wire[0].p, ctx->eng[0].p, W, H, fmt, flip);
-        from_frame_dev(ctx, ctx->wire[1].p, ctx->eng[1].p, W, H, fmt, flip);
+        CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, ctx->lay_up[slot], 0), "event"));
+        from_frame_dev(ctx, ctx->lay_stage[slot][0].p, ctx->eng[0].p, W, H, fmt, flip);
+        from_frame_dev(ctx, ctx->lay_stage[slot][1].p, ctx->eng[1].p, W, H, fmt, flip);
+        bool rebuilt = is_rebuilt(sel);
+        if (vector || rebuilt) CHECK(mattes(slot, flip));
+        CHECK(ctx->cuda(cudaEventRecord(ctx->lay_free[slot], ctx->stream), "event"));  // the slot is read
         uint8_t* dst = (uint8_t*)out + (size_t)k * bytes;
-        if (!vector && nfg > 0 && !(first == 0 && last == nfg && !shrink)) {
+        if (rebuilt) {
             // layers.rs:414-436: a single group display of an unwarped frame rebuilds its plates
-            CHECK(mattes(sel, false));
             CHECK(rebuilt_frame_dev(ctx, *s, sel, *job, mat, W, H, fmt, ctx->wire[2].p));
         } else if (!vector) {
             CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
@@ -3096,7 +3138,6 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
             SmartScratch ss{&ctx->eng[2], &ctx->holes, &ctx->fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
             CHECK(interpolate_dev(ctx, sel, ctx->eng[0].p, ctx->eng[1].p, W, H, fmt, ctx->wire[2].p, true, flags + FL_BAD, &ss));
         } else {
-            CHECK(mattes(sel, flip));
             void* res = ctx->eng[2].p;
             bool fp = s->motion_rows_reversed != 0;  // layers.rs:348-351: points on the motion path's rows
             if (nfg > 0) CHECK(layers_dev(ctx, *s, sel, *job, mat, W, H, fmt, &res, pts, npts, fp));
