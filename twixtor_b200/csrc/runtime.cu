@@ -563,11 +563,11 @@ int build_mask_pyramid_dev(tw_ctx* ctx, float* matte, int W, int H, const tw_flo
     float* cur = matte;
     float* tmp = scratch0;
     float* nxt = scratch1;
-    int dir = s.taps_above_first ? 2 : 1;
-    auto blur5 = [&](float* p, int w, int h) {  // prep::blur5 on one plane: rows into tmp, columns back
-        dim3 gp((unsigned)((w + TB - 1) / TB), (unsigned)h, 1);
-        LAUNCH(ctx, k_stack_pass, gp, TB, 0, p, tmp, w, h, (long)w * h, ctx->b5, 3, 0, 0, one);
-        LAUNCH(ctx, k_stack_pass, gp, TB, 0, tmp, p, w, h, (long)w * h, ctx->b5, 3, dir, 0, one);
+    bool af = s.taps_above_first != 0;
+    // prep::blur5 of one plane into tmp: the band pyramid's tiled kernel (both passes in one launch)
+    auto blur5 = [&](const float* p, int w, int h) {
+        LAUNCHB(ctx, 8.0 * w * h, k_blur5_band, tiles(w, h), level_threads(w, h), 0, p, (const void*)nullptr, 0, 0, w, h,
+                af, tmp, (float*)nullptr, (float*)nullptr);
     };
     auto resample = [&](const float* src, int sw, int sh, float* dst, int dw, int dh) {
         dim3 gp((unsigned)((dw + TB - 1) / TB), (unsigned)dh, 1);
@@ -579,7 +579,7 @@ int build_mask_pyramid_dev(tw_ctx* ctx, float* matte, int W, int H, const tw_flo
     for (int r = 0; r < g.reduction; r++) {
         int nw = cw / 2, nh = ch / 2;
         blur5(cur, cw, ch);
-        resample(cur, cw, ch, nxt, nw, nh);
+        resample(tmp, cw, ch, nxt, nw, nh);
         std::swap(cur, nxt);
         cw = nw;
         ch = nh;
@@ -592,7 +592,7 @@ int build_mask_pyramid_dev(tw_ctx* ctx, float* matte, int W, int H, const tw_flo
         off += (size_t)lw * lh;
         if (i + 1 < g.levels) {
             blur5(cur, lw, lh);
-            resample(cur, lw, lh, nxt, g.sizes[i + 1][0], g.sizes[i + 1][1]);
+            resample(tmp, lw, lh, nxt, g.sizes[i + 1][0], g.sizes[i + 1][1]);
             std::swap(cur, nxt);
         }
     }
