@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtwixtor_b200.so")
-SOURCES = ["solver.cu", "fused.cu", "image.cu", "smart.cu", "forward.cu", "layers.cu", "filters.cu", "prep.cu", "adjoint.cu", "runtime.cu", "noalloc.cu"]
+SOURCES = ["solver.cu", "fused.cu", "image.cu", "smart.cu", "forward.cu", "layers.cu", "filters.cu", "prep.cu", "adjoint.cu", "host_context.cu", "host_solve.cu", "host_compose.cu", "host_layers.cu", "host_clips.cu", "host_time.cu", "noalloc.cu"]
 BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
@@ -59,15 +59,44 @@ def logf_table_object(verbose=False):
     return obj
 
 
+def _objects_stale(src, obj):
+    """An object is rebuilt when its source or any header of csrc/ (or the C ABI header) is newer."""
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    heads = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    heads.append(os.path.join(os.path.dirname(HERE), "include", "twixtor_b200.h"))
+    return os.path.getmtime(src) > t or any(os.path.getmtime(h) > t for h in heads)
+
+
 def build(force=False, verbose=False):
+    """Compiles every translation unit to an object in _build/ (in parallel), then links the library."""
     if not force and not stale():
         return LIB
-    obj = logf_table_object(verbose)
-    cmd = [NVCC] + FLAGS + ["-o", LIB] + [os.path.join(CSRC, s) for s in SOURCES] + [obj]
-    if verbose:
-        print(" ".join(cmd))
+    from concurrent.futures import ThreadPoolExecutor
+    table_obj = logf_table_object(verbose)
     env = dict(os.environ)
     env.pop("CXX", None)  # host compiler: the system g++ (ccbin default)
+    compile_flags = [f for f in FLAGS if f not in ("-shared", "-cudart", "shared")]
+
+    def compile_one(name):
+        src = os.path.join(CSRC, name)
+        obj = os.path.join(BUILD, name[:-3] + ".o")
+        if force or _objects_stale(src, obj):
+            cmd = [NVCC] + compile_flags + ["-c", "-o", obj, src]
+            if verbose:
+                print(" ".join(cmd))
+            r = subprocess.run(cmd, env=env, cwd=CSRC, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed on {name}:\n{r.stdout}{r.stderr}")
+        return obj
+
+    os.makedirs(BUILD, exist_ok=True)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as pool:
+        objs = list(pool.map(compile_one, SOURCES))
+    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-cudart", "shared", "-o", LIB] + objs + [table_obj]
+    if verbose:
+        print(" ".join(cmd))
     subprocess.run(cmd, check=True, env=env, cwd=CSRC)
     return LIB
 
