@@ -12,9 +12,14 @@ the reference CPU path.
 * ``e2e``: the same frames through the C ABI's host-buffer clip call (tw_retime_clip): every
   source frame the step references is uploaded from pinned host memory and every output frame is
   read back into pinned host memory inside the timed region.
-* ``roofline``: the dominant kernel's algorithmic bytes / its event-timed device time.
-* ``cpu_baseline``: the CPU oracle (the reference CPU path restated in C++, OpenMP over all host
-  cores) on a bounded sample of the same workload.
+* ``roofline``: after the timed region the last step runs once more in the library's serial mode
+  (every kernel alone on the stream, CUDA events around each launch): the dominant kernel's
+  algorithmic bytes per launch over its average launch time, against the measured HBM bandwidth,
+  with the next kernels of that table.
+* ``parity``: the last timed step's output frames (device resident, serial and e2e) compared byte
+  for byte with the oracle's render of the same frames; any difference fails the run (exit 3).
+* ``cpu_baseline``: the time of that oracle render (the reference CPU path restated in C++, OpenMP
+  over all host cores): a bounded sample of the same workload.
 
 ``--workload create-vectors`` and ``--workload fgbg`` measure the other two single-GPU
 configurations the same way through their host-buffer C ABI calls (tw_create_vectors_clip on a
@@ -22,10 +27,13 @@ configurations the same way through their host-buffer C ABI calls (tw_create_vec
 with three FG matte layers at speed 40 %), with the oracle beside them on a small sample.
 
 ``--impl reference`` times the reference's CPU path the same way (the oracle port: the reference
-is Rust and no Rust toolchain exists on these machines). Under torchrun every rank renders its own
-clip (weak scaling, no collective on the data path).
+is Rust and no Rust toolchain exists on these machines). Under torchrun the output frames of ONE
+clip are split into contiguous ranges, one per rank (tw_shard), each rank holding only the clip
+frames its range reads (tw_source_window): weak scaling, no collective on the data path (NCCL only
+for the barrier and the max over ranks of the timings).
 """
 import argparse
+import hashlib
 import json
 import math
 import os
@@ -45,7 +53,6 @@ SPEED = 40.0
 FRAMES_PER_STEP = 10
 METRIC = "1080p retime output frames/s (strict byte-exact GPU vs CPU)"
 WORKLOAD = "retime 1920x1080 8bpc RGBA, speed 40%, defaults (vectors Best, Blend, sensitivity 70)"
-ROOFLINE_KERNEL = os.environ.get("TW_ROOFLINE_KERNEL", "k_level_iter")
 CLIP_KW = dict(seed=0x74570002, bg_velocity=(6.0, -3.0), square=240, square_start=(600.0, 400.0),
                square_velocity=(9.0, 4.0))
 
@@ -63,11 +70,10 @@ def source_frames_needed(nout):
     return int(math.ceil(SPEED / 100.0 * nout)) + 2
 
 
-def make_clip(nframes, seed_offset=0):
+def make_clip(nframes, window=None):
+    """The 1080p clip of nframes frames, or only its frames window = (first, last)."""
     from twixtor_b200 import synth
-    kw = dict(CLIP_KW)
-    kw["seed"] = kw["seed"] + seed_offset
-    return synth.moving_clip(W, H, nframes, depth=8, **kw)
+    return synth.moving_clip(W, H, nframes, depth=8, window=window, **CLIP_KW)
 
 
 def peaks():
@@ -147,30 +153,13 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_sample(frames_np, nframes):
-    """The oracle (reference CPU path restated in C++) on the first FRAMES_PER_STEP output frames."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib as O
-    O.lib()
-    threads = os.cpu_count() or 1
-    O.lib().or_set_threads(threads)
-    p = O.retime_params(speed=SPEED)
-    t = time.perf_counter()
-    for n in range(FRAMES_PER_STEP):
-        O.retime_one(frames_np, nframes, W, H, 0, p, n)
-    dt = time.perf_counter() - t
-    return {"value": FRAMES_PER_STEP / dt, "unit": "frames/s", "cores": threads, "kind": "port",
-            "sample": f"{FRAMES_PER_STEP} output frames (2 exact, 8 in-between) of the same 1080p clip, "
-                      f"{dt:.2f} s on {threads} OpenMP threads"}
-
-
 def run_reference(args):
-    """The reference CPU path (restated in C++, all host threads) on the same workload: a step is one
-    period of the 40 % cadence, 5 output frames (1 exact, 4 in-between)."""
+    """The reference CPU path (restated in C++, all host threads) on the same workload and step as
+    the CUDA arm: 10 consecutive output frames of the 1080p clip (2 exact, 8 in-between)."""
     rank, ws, _ = dist_env()
     if rank != 0:
         return 0
-    nout = 5
+    nout = FRAMES_PER_STEP
     total = (args.warmup + args.steps) * nout
     nframes = source_frames_needed(total)
     frames = make_clip(nframes)
@@ -196,7 +185,7 @@ def run_reference(args):
           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
           "config": {"workload": WORKLOAD, "output_frames_per_step": nout},
           "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads, "kind": "port",
-                           "sample": f"{args.steps} steps of {nout} output frames (1 exact, 4 in-between) "
+                           "sample": f"{args.steps} steps of {nout} output frames (2 exact, 8 in-between) "
                                      f"of the 1080p clip on {threads} OpenMP threads"},
           "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     return 0
@@ -282,10 +271,14 @@ def run_workload(args):
     for k in range(warmup):
         step(k)
     torch.cuda.synchronize()
+    l0 = dev.stats()["kernel_launches"]
     with Clocks(0) as clk:
         times = [_timed(stream, step, k, flush) for k in range(warmup, warmup + steps)]
+    launches = dev.stats()["kernel_launches"] - l0
     total_ms = sum(times)
     value = steps * per / (total_ms / 1e3)
+    kernels, serial_ms = roofline_pass(dev, stream, flush, lambda: step(warmup + steps - 1))
+    peak, which = peaks()
     line = {"metric": metric, "value": value, "unit": "frames/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
             "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
@@ -294,7 +287,9 @@ def run_workload(args):
                        "l2": "flushed between steps (256 MiB write)"},
             "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": per * W * H * 4 * (2 if fmt == 1 else 1)},
-            "gpu_launches": dev.stats()["kernel_launches"], "clocks": clk.summary()}
+            "gpu_launches": launches,
+            "roofline": roofline_entry(kernels, serial_ms, launches / steps, total_ms / steps, peak, which),
+            "clocks": clk.summary()}
     if not args.no_cpu_baseline:
         import oracle_lib as O
         threads = os.cpu_count() or 1
@@ -431,6 +426,8 @@ def run_batch(args):
     launches = dev.stats()["kernel_launches"] - l0
     total_ms = sum(times)
     nframes = args.steps * per * len(jobs)
+    kernels, serial_ms = roofline_pass(dev, stream, flush, lambda: step(args.warmup + args.steps - 1))
+    peak, which = peaks()
     mpx = args.steps * per * sum(w * h for w, h in BATCH_SIZES) / 1e6
     line = {"metric": "batched retime output frames/s, 4 clips of uneven size (strict byte-exact GPU vs CPU)",
             "value": nframes / (total_ms / 1e3), "unit": "frames/s", "n_gpus": 1, "steps": args.steps,
@@ -440,7 +437,9 @@ def run_batch(args):
                                    "100@0e;25@48e;100@96e, 8 output frames of each clip per step in one batched call",
                        "megapixels_per_s": mpx / (total_ms / 1e3), "output_frames_per_step": per * len(jobs),
                        "l2": "flushed between steps (256 MiB write); clips resident in HBM"},
-            "gpu_launches": launches, "clocks": clk.summary()}
+            "gpu_launches": launches,
+            "roofline": roofline_entry(kernels, serial_ms, launches / args.steps, total_ms / args.steps, peak, which),
+            "clocks": clk.summary()}
     if not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib as O
@@ -503,15 +502,22 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
 
-    total_out = (args.warmup + args.steps) * FRAMES_PER_STEP
-    nframes = source_frames_needed(total_out)
-    frames_np = make_clip(nframes, seed_offset=rank)
+    # One clip; under torchrun its output frames are split into contiguous ranges, one per rank
+    # (tw_shard), and each rank holds only the clip frames its range reads (tw_source_window).
+    per_rank = (args.warmup + args.steps) * FRAMES_PER_STEP
+    total_out = ws * per_rank
+    nclip = source_frames_needed(total_out)
+    tp = tw.TimeParams(speed_percent=SPEED)
+    all_sels = [tw.select(tp, n, W, H) for n in range(total_out)]
+    lo, hi = tw.shard(total_out, ws, rank)
+    first, last = tw.source_window(all_sels[lo:hi], nclip)
+    nframes = last - first + 1
+    frames_np = make_clip(nclip, window=(first, last))
+    sels = tw.rebase(all_sels[lo:hi], first, nclip)  # frame indices into this rank's window
     fs = W * H * 4
     stream = torch.cuda.current_stream()
     dev = tw.Device(local)
     dev.set_stream(stream.cuda_stream)
-    tp = tw.TimeParams(speed_percent=SPEED)
-    sels = [tw.select(tp, n, W, H) for n in range(total_out)]
     settings = tw.RetimeSettings()
 
     clip = torch.from_numpy(frames_np).to(f"cuda:{local}")
@@ -539,7 +545,6 @@ def main():
         step_device(k)
     barrier()
     l0 = dev.stats()["kernel_launches"]
-    dev.profile_begin(ROOFLINE_KERNEL)
     times = []
     with Clocks(local) as clk:
         for k in range(args.warmup, args.warmup + args.steps):
@@ -550,17 +555,17 @@ def main():
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
-    kms, klaunch, kbytes = dev.profile_end()
     launches = dev.stats()["kernel_launches"] - l0
-    if args.breakdown:
-        dev.profile_begin("*")
-        step_device(args.warmup)
-        print(dev.profile_report(), file=sys.stderr)
-        dev.profile_end()
+    last_k = args.warmup + args.steps - 1
+    dev_out = out.cpu().numpy()  # the last timed step's output frames
     barrier()
     total_ms = max_over_ranks(sum(times))
     clocks = clk.summary()
     value = ws * args.steps * FRAMES_PER_STEP / (total_ms / 1e3)
+
+    # ---- roofline: the same step once more in serial mode (every kernel alone on the stream) -------
+    kernels, serial_ms = roofline_pass(dev, stream, flush, lambda: step_device(last_k))
+    serial_out = out.cpu().numpy()
 
     # ---- e2e: host buffers through the C ABI ------------------------------------------------
     pinned = torch.from_numpy(frames_np).pin_memory()
@@ -588,42 +593,121 @@ def main():
     barrier()
     e2e_ms = max_over_ranks(sum(etimes))
     e2e_value = ws * args.steps * FRAMES_PER_STEP / (e2e_ms / 1e3)
-    h2d = fs * len({f for s in sels[:FRAMES_PER_STEP] for f in (s.a, s.b) if 0 <= f < nframes})
+    step_sels = sels[:FRAMES_PER_STEP]
+    h2d = fs * len({f for s in step_sels for f in (s.a, s.b) if 0 <= f < nframes})
     d2h = FRAMES_PER_STEP * fs
+
+    # ---- parity: the last timed step, device resident, serial and e2e, against the oracle --------
+    threads = max(1, (os.cpu_count() or 1) // ws)
+    glob = [lo + last_k * FRAMES_PER_STEP + j for j in range(FRAMES_PER_STEP)]
+    want, cpu_dt = oracle_frames(frames_np, first, nframes, nclip, glob, threads)
+    equal = {"device": dev_out.tobytes() == want.tobytes(), "serial": serial_out.tobytes() == want.tobytes(),
+             "e2e": out_host.tobytes() == want.tobytes()}
+    ok = all(equal.values())
+    if ws > 1:
+        t = torch.tensor([0 if ok else 1], dtype=torch.int32, device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ok_all = int(t.item()) == 0
+    else:
+        ok_all = ok
+    parity = {"frames": FRAMES_PER_STEP * ws, "equal": ok_all, "paths": equal,
+              "sha256_rank0": hashlib.sha256(dev_out.tobytes()).hexdigest(),
+              "checked": "the last timed step's output frames of every rank, byte for byte against the oracle"}
 
     if rank == 0:
         peak, which = peaks()
-        achieved = (kbytes / (kms / 1e3)) / 1e9 if kms > 0 else None
-        tr = traffic_of(ROOFLINE_KERNEL)
-        if isinstance(tr, dict):
-            # DRAM bytes of the captured launch scaled to the average launch of the timed region by
-            # the algorithmic bytes each moves (traffic grows in proportion to the units processed)
-            tr = tr["dram_bytes"] / tr["algorithmic_bytes"] * (kbytes / max(klaunch, 1))
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "output_frames_per_step": FRAMES_PER_STEP,
-                       "in_between_frames_per_step": sum(1 for s in sels[:FRAMES_PER_STEP] if not s.exact),
+            "config": {"workload": WORKLOAD, "output_frames_per_step": FRAMES_PER_STEP * ws,
+                       "in_between_frames_per_step": sum(1 for s in step_sels if not s.exact),
                        "source_frames_resident": nframes, "frame_bytes": fs,
                        "l2": "flushed between steps (256 MiB write), inputs resident 0.5 GB > L2",
-                       "parallelism": f"{ws} independent clips (one per GPU)"},
+                       "parallelism": (f"one clip of {total_out} output frames split into {ws} contiguous ranges "
+                                       f"of {per_rank} (one per GPU, each holding only its source window); "
+                                       "no collective on the data path") if ws > 1 else "1 GPU"},
             "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": ROOFLINE_KERNEL, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": tr, "peak_source": which, "launches_timed": klaunch,
-                         "algorithmic_bytes_per_launch": kbytes / max(klaunch, 1),
-                         "avg_launch_us": 1e3 * kms / max(klaunch, 1)},
+            "roofline": roofline_entry(kernels, serial_ms, launches / args.steps, total_ms / args.steps, peak,
+                                       which),
+            "parity": parity,
             "clocks": clocks,
         }
         if not args.no_cpu_baseline and ws == 1:
-            line["cpu_baseline"] = cpu_sample(frames_np, nframes)
+            line["cpu_baseline"] = {"value": FRAMES_PER_STEP / cpu_dt, "unit": "frames/s", "cores": threads,
+                                    "kind": "port",
+                                    "sample": f"the parity render: the {FRAMES_PER_STEP} output frames of the last timed "
+                                              f"step ({sum(1 for s in step_sels if not s.exact)} in-between) of the "
+                                              f"same 1080p clip, {cpu_dt:.2f} s on {threads} OpenMP threads"}
         emit(line)
     if ws > 1:
         torch.distributed.destroy_process_group()
     dev.close()
-    return 0
+    return 0 if ok_all else 3
+
+
+def oracle_frames(window, first, count, nclip, outputs, threads):
+    """The oracle's render of the given output frames from the clip window a rank holds (test
+    infrastructure, after the timed regions): the parity reference and the CPU baseline's sample."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    O.lib().or_set_threads(threads)
+    p = O.retime_params(speed=SPEED)
+    t = time.perf_counter()
+    res = [O.retime_window(window, first, count, nclip, W, H, 0, p, n) for n in outputs]
+    return np.concatenate(res), time.perf_counter() - t
+
+
+def roofline_pass(dev, stream, flush, run):
+    """One more step in the library's serial mode (tw_set_lanes(0): every kernel in issue order on the
+    stream, nothing overlapping), with every launch bracketed by CUDA events on that stream: per
+    kernel its launches, device time and algorithmic bytes. Outside the timed region."""
+    import torch
+    dev.set_lanes(0)
+    flush.fill_(7)
+    torch.cuda.synchronize()
+    dev.profile_begin("*")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run()
+    e1.record(stream)
+    e1.synchronize()
+    table = dev.profile_report()
+    dev.profile_end()
+    dev.set_lanes(4)
+    kernels = []
+    for row in table.splitlines()[1:]:
+        p = row.split()
+        if len(p) >= 6:
+            kernels.append({"kernel": p[0], "launches": int(p[1]), "ms": float(p[2]), "us_per_launch": float(p[3]),
+                            "share": float(p[4].rstrip("%")) / 100.0, "alg_gbs": float(p[5])})
+    return kernels, e0.elapsed_time(e1)
+
+
+def roofline_entry(kernels, serial_ms, launches_per_step, ms_per_step, peak, which):
+    """The dominant kernel by serial device time: its algorithmic bytes per launch over its average
+    launch duration (measured alone), as a fraction of the measured HBM copy bandwidth; with the
+    next kernels of the table beside it."""
+    top = kernels[0]
+    achieved = top["alg_gbs"]
+    bytes_per_launch = achieved * 1e9 * top["us_per_launch"] * 1e-6
+    tr = traffic_of(top["kernel"])
+    if isinstance(tr, dict):
+        # DRAM bytes of the captured launch scaled to the average launch by the algorithmic bytes
+        # each moves (traffic grows in proportion to the units processed)
+        tr = tr["dram_bytes"] / tr["algorithmic_bytes"] * bytes_per_launch
+    return {"bound": "hbm", "kernel": top["kernel"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if peak else None, "traffic": tr, "peak_source": which,
+            "launches_per_step": top["launches"], "avg_launch_us": top["us_per_launch"],
+            "algorithmic_bytes_per_launch": bytes_per_launch,
+            "timing": "one step in serial mode (each kernel alone on the stream, CUDA events per launch), "
+                      "after the timed region",
+            "serial_step_ms": serial_ms, "kernel_ms_per_step": top["ms"],
+            "kernel_ms_fits_step": top["ms"] <= serial_ms,
+            "timed_ms_per_step": ms_per_step, "timed_launches_per_step": launches_per_step,
+            "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} | 
+                        {"frac": round(r["alg_gbs"] / peak, 4) if peak else None} for r in kernels[:8]]}
 
 
 if __name__ == "__main__":

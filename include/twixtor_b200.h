@@ -55,15 +55,20 @@ typedef enum tw_fmt { TW_U8 = 0, TW_U16 = 1, TW_F32 = 2 } tw_fmt;
 
 typedef struct tw_ctx tw_ctx;
 
-/* An engine image (image.rs:66-71). `data` holds width * height * 4 samples of `fmt`. */
+/* An engine image (image.rs:66-71). `data` holds width * height * 4 samples of `fmt`; `bytes` is the
+ * size of the caller's buffer behind `data`. A buffer shorter than the image needs is refused with
+ * TW_ERR_BAD_PARAM before anything is read or written (the reference's slices carry their length;
+ * a C pointer does not). */
 typedef struct tw_image {
     int32_t width, height, fmt;
     const void* data;
+    size_t bytes;
 } tw_image;
 
 typedef struct tw_image_mut {
     int32_t width, height, fmt;
     void* data;
+    size_t bytes;
 } tw_image_mut;
 
 /* flow::FlowField (flow.rs:37-76). */
@@ -142,9 +147,22 @@ size_t tw_last_error(const tw_ctx* ctx, char* buf, size_t cap);
 int tw_stats(const tw_ctx* ctx, uint64_t* kernel_launches, uint64_t* device_bytes);
 
 /* The number of output frames the clip calls keep in flight (1..8; default 4): each has its own
- * buffers and two streams, so their solves overlap on the GPU. A tuning knob only: the output
- * bytes do not depend on it. */
+ * buffers and two streams, so their solves overlap on the GPU. 0 is the serial mode: one frame at a
+ * time with all its work on the context's stream in issue order (nothing overlaps, so the profiler's
+ * events time each kernel alone). A tuning knob only: the output bytes do not depend on it. */
 int tw_set_lanes(tw_ctx* ctx, int32_t lanes);
+
+/* Failure injection, for tests of the error paths (the reference's device tests fake failing
+ * backends the same way, device/exec/tests.rs). Nothing faults, traps or hangs the GPU: with
+ * TW_INJECT_ALLOC the n-th device allocation from now (a buffer that has to grow) fails as a
+ * cudaMalloc out of memory would, leaving the buffer as it was, and the call returns TW_ERR_CUDA;
+ * with TW_INJECT_STATUS a small kernel sets the device status word of the n-th output frame from
+ * now, as a kernel whose bounded loop ran out sets it, and the clip or frame call that reads it
+ * returns TW_ERR_DEVICE_BOUND. The context stays usable after either. TW_INJECT_NONE disarms. */
+#define TW_INJECT_NONE 0
+#define TW_INJECT_ALLOC 1
+#define TW_INJECT_STATUS 2
+int tw_debug_inject(tw_ctx* ctx, int32_t kind, int32_t n);
 
 /* Makes the context enqueue on `stream` (a cudaStream_t; NULL is the legacy default stream)
  * instead of its own, so a caller can order the library's work with its own and time it with its
@@ -215,11 +233,17 @@ int tw_block_match(tw_ctx* ctx, const float* a, const float* b, float* flow, int
  * floats (12 MiB), which every GPU that loads the library holds until the process exits; frames
  * above TW_NOALLOC_MAX_PIXELS pixels (e.g. anything above a 960 x 540 working size plus a
  * little), or a side above 6144, return TW_ERR_TOO_LARGE. The work runs on `stream` (a
- * cudaStream_t, NULL for the default stream) of the current device and the call returns when it
- * is done. The first call on a device looks up the array's device address and sets the kernels'
- * shared memory limit (no allocation either), so make that first call before any stream capture.
- * All calls share the one array: calls that overlap on the GPU (from several host threads or
- * streams at once) race on it and must be serialised by the caller. */
+ * cudaStream_t, NULL for the default stream) in the CUDA context current on the calling thread,
+ * and the call returns when it is done. Every call looks the array's address up in that context
+ * and sets the sweep kernels' shared memory limit there (neither allocates), so a host may bind its
+ * own context or reset the device between calls. The first call in a process or context may still
+ * load the library's device code (lazy module loading, the CUDA default), which is when the array
+ * and the kernels take their device memory: make one warm-up call off the real-time thread and
+ * before any stream capture. All calls share the one array, which keeps the last call's contents
+ * (each call writes every element it reads first): calls that overlap on the GPU (from several
+ * host threads or streams at once) race on it and must be serialised by the caller. The status
+ * covers this call's own launches and the completion of `stream`; an error that earlier launches
+ * of the host left pending is neither reported as this call's nor cleared. */
 #define TW_NOALLOC_MAX_PIXELS (1L << 19)
 int tw_block_match_noalloc(const float* a, const float* b, float* flow, int32_t width, int32_t height, void* stream);
 
@@ -381,6 +405,21 @@ typedef struct tw_time_params {
 /* The selection of output frame n of a clip of width x height (timeline::select, timeline.rs:
  * 451-469, with RemapTimeMap::src_pos :266-331 and the tiny-frame rule prep.rs:111-117). */
 int tw_select(const tw_time_params* p, int32_t n, int32_t width, int32_t height, tw_selection* out);
+
+/* ---- one clip over several GPUs ------------------------------------------------------------ */
+
+/* The output frames [lo, hi) of a clip of nout output frames that rank `rank` of `nranks` renders:
+ * contiguous ranges in rank order whose sizes differ by at most one. No counterpart in the reference,
+ * whose renderer walks the output frames in order on one device (crates/fx-cli/src/temporal.rs:
+ * 206-249); an output frame needs nothing from any other (timeline.rs:447-469), so the ranks
+ * exchange nothing and the outputs concatenate in rank order. */
+int tw_shard(int32_t nout, int32_t nranks, int32_t rank, int32_t* lo, int32_t* hi);
+
+/* The clip frames [first, last] that selections sels[0 .. n) read inside a clip of nframes frames
+ * (frames a and b of every selection; first > last when none lies inside the clip): the source
+ * window one rank uploads. A frame at the boundary of two ranks' ranges lies in both windows, and
+ * each rank builds its pyramid itself, which costs one frame per boundary and needs no exchange. */
+int tw_source_window(const tw_selection* sels, int32_t n, int32_t nframes, int32_t* first, int32_t* last);
 
 /* ---- whole output frames ------------------------------------------------------------------ */
 

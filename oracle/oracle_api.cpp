@@ -506,8 +506,11 @@ int or_select(const or_retime_params* p, int n, int w, int h, float* s0, float* 
 // restated.
 // One output frame of the plain vector path; `gouraud`: the forward warps of codes 2/3 as the
 // Gouraud variant (the stage set of retime-fgbg, plugins/retime-fgbg/src/glue.rs:142-143).
+// `frames` holds the clip frames [first, first + count) of a clip of nframes frames (the whole clip:
+// first 0, count nframes); a frame the selection needs outside that window is an error (-2).
 static int retime_one(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int n, void* out,
-                      bool gouraud, const std::vector<std::array<float, 4>>* pts = nullptr) {
+                      bool gouraud, const std::vector<std::array<float, 4>>* pts = nullptr, int first = 0, int count = -1) {
+    if (count < 0) count = nframes;
     Fmt f = (Fmt)fmt;
     size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
     size_t frame_bytes = (size_t)w * h * 4 * es;
@@ -517,15 +520,18 @@ static int retime_one(const void* frames, int nframes, int w, int h, int fmt, co
     float s0, s1, wa;
     int a, exact, vq, interp;
     or_select(p, n, w, h, &s0, &s1, &a, &wa, &exact, &vq, &interp);
+    bool outside_window = false;
     auto fetch = [&](int pos) -> Image {
         // main_frame(position): frame_time (dur == lts, equal rates), then the clip frame of that tick
         double d = (double)(float)pos;
         int time = cvtt_i32_d(d * (double)time_step + 0.5);
         long long idx = time >= 0 ? time / time_step : -(((long long)-time + time_step - 1) / time_step);
         if (idx < 0 || idx >= nframes) return Image(w, h, f);
-        return from_frame((const uint8_t*)frames + (size_t)idx * frame_bytes, w, h, f);
+        if (idx < first || idx >= (long long)first + count) { outside_window = true; return Image(w, h, f); }
+        return from_frame((const uint8_t*)frames + (size_t)(idx - first) * frame_bytes, w, h, f);
     };
     Image A = fetch(a), B = fetch(a + 1), result;
+    if (outside_window) return fail(2, "output frame needs a source frame outside the window it was given");
     Selection sel;
     sel.s0 = s0; sel.s1 = s1; sel.a = a; sel.b = a + 1; sel.wa = wa; sel.exact = exact != 0;
     sel.vectors_quality = vq; sel.interp = interp;
@@ -595,6 +601,13 @@ static int retime_one(const void* frames, int nframes, int w, int h, int fmt, co
 
 int or_retime_one(const void* frames, int nframes, int w, int h, int fmt, const or_retime_params* p, int n, void* out) {
     return retime_one(frames, nframes, w, h, fmt, p, n, out, false);
+}
+
+// Output frame n of a clip of nframes frames from the window of clip frames [first, first + count)
+// alone (the frames one rank of a sharded render holds); -2 when the frame needs one outside it.
+int or_retime_window(const void* frames, int first, int count, int nframes, int w, int h, int fmt,
+                     const or_retime_params* p, int n, void* out) {
+    return retime_one(frames, nframes, w, h, fmt, p, n, out, false, nullptr, first, count);
 }
 
 // ---- retime-fgbg with FG matte layers (plugins/retime-fgbg/src/glue.rs, compose.rs:149-170,

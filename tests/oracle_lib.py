@@ -82,6 +82,7 @@ def lib():
         L.or_select.argtypes = [ctypes.POINTER(RetimeParams), i, i, i, P, P, P, P, P, P, P]
         L.or_retime_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_retime_one.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
+        L.or_retime_window.argtypes = [P, i, i, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_crt_powf.argtypes = [P, P, P, i]
         L.or_motion_blur.argtypes = [P, P, i, i, i, P, i, i, f, i, f]
         L.or_retime_fgbg_one.argtypes = [P, i, P, i, P, P, P, i, P, P, i, i, i, ctypes.POINTER(RetimeParams), i, P]
@@ -366,6 +367,16 @@ def retime_one(frames, nframes, w, h, fmt, params, n):
     rc = lib().or_retime_one(ptr(frames), nframes, w, h, fmt, ctypes.byref(params), n, ptr(out))
     if rc:
         raise ValueError(err())
+    return out
+
+
+def retime_window(frames, first, count, nframes, w, h, fmt, params, n):
+    """Output frame n of a clip of nframes frames from the clip frames [first, first + count) alone;
+    raises when the frame needs one outside that window."""
+    out = np.zeros(w * h * 4, DTYPE[fmt])
+    rc = lib().or_retime_window(ptr(frames), first, count, nframes, w, h, fmt, ctypes.byref(params), n, ptr(out))
+    if rc:
+        raise RuntimeError(f"or_retime_window: {rc} {err()}")
     return out
 
 

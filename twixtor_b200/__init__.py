@@ -54,6 +54,8 @@ class BadParam(StageError):
     pass
 
 
+INJECT_NONE, INJECT_ALLOC, INJECT_STATUS = 0, 1, 2
+
 _ERRORS = {ERR_UNSUPPORTED: Unsupported, ERR_NAN_OUTPUT: NanOutput, ERR_MISMATCH: Mismatch, ERR_BAD_PARAM: BadParam,
            ERR_DEVICE_BOUND: Unsupported}
 
@@ -62,7 +64,7 @@ _ERRORS = {ERR_UNSUPPORTED: Unsupported, ERR_NAN_OUTPUT: NanOutput, ERR_MISMATCH
 
 class _Image(ctypes.Structure):
     _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("fmt", ctypes.c_int32),
-                ("data", ctypes.c_void_p)]
+                ("data", ctypes.c_void_p), ("bytes", ctypes.c_size_t)]
 
 
 class _Flow(ctypes.Structure):
@@ -309,6 +311,7 @@ def library():
     L.tw_last_error.restype = ctypes.c_size_t
     L.tw_stats.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.tw_set_stream.argtypes = [P, P]
+    L.tw_debug_inject.argtypes = [P, i32, i32]
     L.tw_profile_begin.argtypes = [P, ctypes.c_char_p]
     L.tw_profile_end.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64),
                                  ctypes.POINTER(ctypes.c_double)]
@@ -342,6 +345,9 @@ def library():
     L.tw_from_frame.argtypes = [P, P, i32, i32, i32, P]
     L.tw_to_frame.argtypes = [P, P, i32, i32, i32, P]
     L.tw_select.argtypes = [ctypes.POINTER(_TimeParams), i32, i32, i32, ctypes.POINTER(_Selection)]
+    L.tw_shard.argtypes = [i32, i32, i32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+    L.tw_source_window.argtypes = [ctypes.POINTER(_Selection), i32, i32, ctypes.POINTER(ctypes.c_int32),
+                                   ctypes.POINTER(ctypes.c_int32)]
     L.tw_retime_frame.argtypes = [P, ctypes.POINTER(_RetimeSettings), ctypes.POINTER(_Selection), P, P, i32, i32,
                                   i32, P]
     L.tw_retime_clip.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, ctypes.POINTER(_Selection), i32, i32,
@@ -361,7 +367,7 @@ def _ptr(a):
 def _img(a, w, h, fmt):
     a = np.ascontiguousarray(a)
     assert a.dtype == DTYPES[fmt] and a.size == w * h * 4, "engine image of the wrong size or depth"
-    return _Image(w, h, fmt, a.ctypes.data), a
+    return _Image(w, h, fmt, a.ctypes.data, a.nbytes), a
 
 
 def vectors_pair(n: int, track_frame: int = 1, fps: Tuple[int, int] = (24, 1)) -> Tuple[int, int]:
@@ -381,6 +387,37 @@ def select(params: TimeParams, n: int, width: int, height: int) -> Selection:
     if rc:
         raise BadParam(rc, "tw_select")
     return Selection._from_c(out)
+
+
+def shard(nout: int, nranks: int, rank: int) -> Tuple[int, int]:
+    """The output frames [lo, hi) rank ``rank`` of ``nranks`` renders (tw_shard)."""
+    lo, hi = ctypes.c_int32(), ctypes.c_int32()
+    rc = library().tw_shard(nout, nranks, rank, ctypes.byref(lo), ctypes.byref(hi))
+    if rc:
+        raise BadParam(rc, "tw_shard")
+    return lo.value, hi.value
+
+
+def source_window(sels, nframes: int) -> Tuple[int, int]:
+    """The clip frames [first, last] the selections read (tw_source_window); first > last: none."""
+    arr = (_Selection * max(len(sels), 1))(*[s._c() for s in sels])
+    first, last = ctypes.c_int32(), ctypes.c_int32()
+    rc = library().tw_source_window(arr, len(sels), nframes, ctypes.byref(first), ctypes.byref(last))
+    if rc:
+        raise BadParam(rc, "tw_source_window")
+    return first.value, last.value
+
+
+def rebase(sels, first: int, nframes: int):
+    """The selections with their frames counted from the window's first frame (a frame outside the
+    clip stays outside: -1), for a rank that holds only frames [first, ...] of the clip."""
+    out = []
+    for s in sels:
+        c = Selection._from_c(s._c())
+        c.a = c.a - first if 0 <= c.a < nframes else -1
+        c.b = c.b - first if 0 <= c.b < nframes else -1
+        out.append(c)
+    return out
 
 
 def flow_geometry(settings: FlowSettings, width: int, height: int):
@@ -434,6 +471,11 @@ class Device:
             buf = ctypes.create_string_buffer(n + 1)
             self._L.tw_last_error(self._h, buf, n + 1)
             raise (_ERRORS.get(rc, StageError))(rc, buf.value.decode())
+
+    def debug_inject(self, kind: int, n: int = 1):
+        """Arms a host-injected failure (tw_debug_inject): INJECT_ALLOC fails the n-th device
+        allocation, INJECT_STATUS sets the device status word of the n-th output frame."""
+        self._check(self._L.tw_debug_inject(self._h, int(kind), int(n)))
 
     def set_stream(self, stream_handle: int):
         """Enqueue on a caller's CUDA stream (e.g. ``torch.cuda.current_stream().cuda_stream``)."""
@@ -492,7 +534,7 @@ class Device:
         out = np.zeros(width * height * 4, DTYPES[fmt])
         ai, aa = _img(a, width, height, fmt)
         bi, ba = _img(b, width, height, fmt)
-        oi = _Image(width, height, fmt, out.ctypes.data)
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         fab = _Flow(fw, fh, f_ab.ctypes.data) if f_ab is not None else None
         fba = _Flow(fw, fh, f_ba.ctypes.data) if f_ba is not None else None
         self._check(self._L.tw_compose_vectors(self._h, ctypes.byref(settings._c()), ctypes.byref(sel._c()),
@@ -526,7 +568,7 @@ class Device:
         fw, fh = flow_size
         out = np.zeros(width * height * 4, DTYPES[fmt])
         si, sa = _img(src, width, height, fmt)
-        oi = _Image(width, height, fmt, out.ctypes.data)
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         flow = np.ascontiguousarray(flow, np.float32)
         fl = _Flow(fw, fh, flow.ctypes.data)
         cov = np.zeros(width * height, np.uint8) if coverage else None
@@ -538,7 +580,7 @@ class Device:
         out = np.zeros(width * height * 4, DTYPES[fmt])
         ai, aa = _img(a, width, height, fmt)
         bi, ba = _img(b, width, height, fmt)
-        oi = _Image(width, height, fmt, out.ctypes.data)
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         self._check(self._L.tw_blend(self._h, ctypes.byref(oi), ctypes.byref(ai), ctypes.byref(bi), np.float32(w)))
         return out
 
@@ -548,7 +590,7 @@ class Device:
         fw, fh = flow_size
         out = np.zeros(width * height * 4, DTYPES[fmt])
         si, sa = _img(src, width, height, fmt)
-        oi = _Image(width, height, fmt, out.ctypes.data)
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         flow = np.ascontiguousarray(flow, np.float32)
         fl = _Flow(fw, fh, flow.ctypes.data)
         cov = np.zeros(width * height, np.uint8) if coverage else None
@@ -560,7 +602,7 @@ class Device:
         """``vectors::encode_vectors``: the encoded vector image (engine samples) of a flow."""
         fw, fh = flow_size
         out = np.zeros(width * height * 4, DTYPES[fmt])
-        oi = _Image(width, height, fmt, out.ctypes.data)
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         flow = np.ascontiguousarray(flow, np.float32)
         fl = _Flow(fw, fh, flow.ctypes.data)
         self._check(self._L.tw_encode_vectors(self._h, ctypes.byref(oi), ctypes.byref(fl), np.float32(scale)))
@@ -571,7 +613,7 @@ class Device:
         out = np.zeros(width * height * 4, DTYPES[fmt])
         xi, xa = _img(x, width, height, fmt)
         yi, ya = _img(y, width, height, fmt)
-        oi = _Image(width, height, fmt, out.ctypes.data)
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         self._check(self._L.tw_create_vectors(self._h, ctypes.byref(settings._c()), ctypes.byref(xi), ctypes.byref(yi),
                                               ctypes.byref(oi)))
         return out
@@ -622,7 +664,7 @@ class Device:
         out = np.zeros(width * height * 4, DTYPES[fmt])
         ai, aa = _img(a, width, height, fmt)
         bi, ba = _img(b, width, height, fmt)
-        oi = _Image(width, height, fmt, out.ctypes.data)
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         ma = np.ascontiguousarray(np.concatenate(mattes_a) if nfg else np.zeros(1), np.float32)
         mb = np.ascontiguousarray(np.concatenate(mattes_b) if nfg else np.zeros(1), np.float32)
         self._check(self._L.tw_compose_layers(self._h, ctypes.byref(settings._c()), ctypes.byref(sel._c()), ctypes.byref(ai),
@@ -645,7 +687,7 @@ class Device:
         fw, fh = flow_size
         out = np.zeros(width * height * 4, DTYPES[fmt])
         si, sa = _img(src, width, height, fmt)
-        oi = _Image(width, height, fmt, out.ctypes.data)
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         fl = np.ascontiguousarray(flow, np.float32)
         self._check(self._L.tw_motion_blur(self._h, ctypes.byref(oi), ctypes.byref(si), ctypes.byref(_Flow(fw, fh, fl.ctypes.data)),
                                            np.float32(amount), int(hiq), np.float32(shutter)))
@@ -675,7 +717,7 @@ class Device:
         out = np.zeros(width * height * 4, DTYPES[fmt])
         ai, aa = _img(p1, width, height, fmt)
         bi, ba = _img(p2, width, height, fmt)
-        oi = _Image(width, height, fmt, out.ctypes.data)
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         self._check(self._L.tw_smart_blend(self._h, ctypes.byref(oi), ctypes.byref(ai), ctypes.byref(bi), np.float32(w),
                                            int(binary)))
         return out
@@ -688,7 +730,7 @@ class Device:
         if mask.size != width * height:
             raise Mismatch(ERR_MISMATCH, f"hole fill: mask has {mask.size} entries for an image of {width}x{height}")
         out = np.array(img, DTYPES[fmt], copy=True).reshape(-1)
-        oi = _Image(width, height, fmt, out.ctypes.data)
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         self._check(self._L.tw_fill_holes(self._h, ctypes.byref(oi), _ptr(mask), kind, int(taps_above_first)))
         return out
 

@@ -39,6 +39,7 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
         WbScratch wbs = wb_scratch(L.wb_wt, L.wb_tmp, L.wb_mask, L.wb_cov);
         SmartScratch ss{&L.comp, &L.holes, &L.fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB};
         CHECK(interpolate_dev(ctx, sel, L.eng[0].p, L.eng[1].p, W, H, fmt, out_wire, true, flags + FL_BAD, &ss));
+        if (ctx->inject_now(TW_INJECT_STATUS)) LAUNCH(ctx, k_set_flag, 1, 1, 0, flags, FL_BOUND);
         CHECK(ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event"));
         return TW_OK;
     }
@@ -90,6 +91,7 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
     CHECK(compose_dev(ctx, s.compose, sel, L.eng[0].p, L.eng[1].p, need_ab ? L.flow[0].as<float>() : nullptr,
                       need_ba ? L.flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, out_wire, true, flip,
                       flags + FL_BAD, &ss));
+    if (ctx->inject_now(TW_INJECT_STATUS)) LAUNCH(ctx, k_set_flag, 1, 1, 0, flags, FL_BOUND);
     CHECK(ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event"));
     return TW_OK;
 }
@@ -308,6 +310,7 @@ int tw_encode_vectors(tw_ctx* ctx, tw_image_mut* out, const tw_flow* flow, float
     ctx->cur = ctx->stream;
     if (!out || !out->data || !flow || !flow->data || out->fmt < 0 || out->fmt > 2)
         return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_out(ctx, out, "encode_vectors output"));
     int W = out->width, H = out->height;
     if (W < 2 || H < 2 || flow->width < 2 || flow->height < 2)
         return ctx->fail(TW_ERR_MISMATCH, "vector encode needs images and a flow of at least 2x2 (image %dx%d, flow %dx%d)", W,
@@ -332,6 +335,7 @@ int tw_create_vectors(tw_ctx* ctx, const tw_vectors_settings* s, const tw_image*
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cur = ctx->stream;
     if (!s || !out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_out(ctx, out, "create_vectors output"));
     CHECK(check_image(ctx, x, "create vectors"));
     CHECK(check_image(ctx, y, "create vectors"));
     if (!same_shape(x, y) || out->width != x->width || out->height != x->height || out->fmt != x->fmt)

@@ -725,6 +725,7 @@ int tw_compose_vectors(tw_ctx* ctx, const tw_engine_settings* settings, const tw
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cur = ctx->stream;
     if (!settings || !sel || !out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_out(ctx, out, "compose_vectors output"));
     CHECK(check_image(ctx, a, "compose"));
     CHECK(check_image(ctx, b, "compose"));
     if (!same_shape(a, b) || out->width != a->width || out->height != a->height || out->fmt != a->fmt)
@@ -771,6 +772,7 @@ int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_fl
     ctx->cur = ctx->stream;
     CHECK(check_image(ctx, src, "inv_warp"));
     if (!out || !out->data || !flow || !flow->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_out(ctx, out, "inv_warp output"));
     if (out->width != src->width || out->height != src->height || out->fmt != src->fmt)
         return ctx->fail(TW_ERR_MISMATCH, "inverse warp: destination and source differ");
     int W = src->width, H = src->height;
@@ -804,6 +806,7 @@ int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* 
     CHECK(check_image(ctx, a, "blend"));
     CHECK(check_image(ctx, b, "blend"));
     if (!out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_out(ctx, out, "blend output"));
     if (!same_shape(a, b) || out->width != a->width || out->height != a->height || out->fmt != a->fmt)
         return ctx->fail(TW_ERR_MISMATCH, "image primitives need equal size and format");
     int W = a->width, H = a->height;
@@ -828,6 +831,7 @@ int tw_smart_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* p1, const tw_
     CHECK(check_image(ctx, p1, "smart blend"));
     CHECK(check_image(ctx, p2, "smart blend"));
     if (!out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_out(ctx, out, "smart_blend output"));
     if (!same_shape(p1, p2) || out->width != p1->width || out->height != p1->height || out->fmt != p1->fmt)
         return ctx->fail(TW_ERR_MISMATCH, "smart blend: images of %dx%d and %dx%d", p1->width, p1->height, p2->width,
                          p2->height);
@@ -849,6 +853,7 @@ int tw_fill_holes(tw_ctx* ctx, tw_image_mut* img, const void* mask, int32_t mask
     if (!img || !img->data || !mask) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
     if (img->fmt < 0 || img->fmt > 2 || img->width <= 0 || img->height <= 0)
         return ctx->fail(TW_ERR_BAD_PARAM, "hole fill: bad image");
+    CHECK(check_out(ctx, img, "fill_holes image"));
     if (mask_kind < 1 || mask_kind > 3)
         return ctx->fail(TW_ERR_BAD_PARAM, "hole fill: mask kind %d is not 1 (u8), 2 (u16) or 3 (f32)", mask_kind);
     int W = img->width, H = img->height;
@@ -883,6 +888,7 @@ int tw_forward_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const t
     ctx->cur = ctx->stream;
     CHECK(check_image(ctx, src, "forward warp"));
     if (!out || !out->data || !flow || !flow->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_out(ctx, out, "forward_warp output"));
     if (out->width != src->width || out->height != src->height || out->fmt != src->fmt)
         return ctx->fail(TW_ERR_MISMATCH, "forward warp: destination %dx%d fmt %d against source %dx%d fmt %d", out->width,
                          out->height, out->fmt, src->width, src->height, src->fmt);
@@ -910,6 +916,7 @@ int tw_motion_blur(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw
     ctx->cur = ctx->stream;
     CHECK(check_image(ctx, src, "motion blur"));
     if (!out || !out->data || !flow || !flow->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_out(ctx, out, "motion_blur output"));
     if (out->width != src->width || out->height != src->height || out->fmt != src->fmt)
         return ctx->fail(TW_ERR_MISMATCH, "motion blur: destination and source differ in shape");
     int W = src->width, H = src->height, fmt = src->fmt;

@@ -23,6 +23,8 @@ void prof_mark(tw_ctx* ctx) {
 }
 
 
+__global__ void k_set_flag(int* flags, int idx) { flags[idx] = 1; }
+
 __global__ void k_selfcheck(int* out) {
     // the x86 truncation rules the strict kernels rely on
     float vals[6] = {-2.5f, 2.5f, 2147483648.0f, -2147483904.0f, __int_as_float(0x7fc00000), -0.0f};
@@ -55,7 +57,18 @@ int check_image(tw_ctx* ctx, const tw_image* im, const char* what) {
     if (!im || !im->data) return ctx->fail(TW_ERR_MISMATCH, "%s: no image", what);
     if (im->fmt < 0 || im->fmt > 2) return ctx->fail(TW_ERR_BAD_PARAM, "%s: format %d is not 0..2", what, im->fmt);
     if (im->width <= 0 || im->height <= 0) return ctx->fail(TW_ERR_MISMATCH, "%s: empty image", what);
+    size_t need = image_bytes(im->width, im->height, im->fmt);
+    if (im->bytes < need)
+        return ctx->fail(TW_ERR_BAD_PARAM, "%s: the buffer holds %zu bytes, a %dx%d image needs %zu", what, im->bytes,
+                         im->width, im->height, need);
     return TW_OK;
+}
+
+// An output image: the checks of an input image on the caller's writable buffer.
+int check_out(tw_ctx* ctx, const tw_image_mut* im, const char* what) {
+    if (!im) return ctx->fail(TW_ERR_BAD_PARAM, "%s: no output image", what);
+    tw_image c{im->width, im->height, im->fmt, im->data, im->bytes};
+    return check_image(ctx, &c, what);
 }
 
 
@@ -67,15 +80,20 @@ int bad_fail(tw_ctx* ctx, int v) {
     return ctx->fail(TW_ERR_UNSUPPORTED, "inverse warp: a sample coordinate is NaN or never converges, which is not supported");
 }
 
+// Creates the lane's streams and events once; every call then points the lane's working streams at
+// its own pair, or in serial mode at the context's stream (every kernel in issue order, so that each
+// launch's events time that kernel alone).
 int lane_ready(tw_ctx* ctx, Lane& L) {
-    if (L.s[0]) return TW_OK;
-    for (int i = 0; i < 2; i++) {
-        CHECK(ctx->cuda(cudaStreamCreateWithFlags(&L.s[i], cudaStreamNonBlocking), "lane stream"));
-        CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_pyr[i], cudaEventDisableTiming), "lane event"));
+    if (!L.own[0]) {
+        for (int i = 0; i < 2; i++) {
+            CHECK(ctx->cuda(cudaStreamCreateWithFlags(&L.own[i], cudaStreamNonBlocking), "lane stream"));
+            CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_pyr[i], cudaEventDisableTiming), "lane event"));
+        }
+        CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_solve1, cudaEventDisableTiming), "lane event"));
+        CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming), "lane event"));
+        CHECK(ctx->ensure(L.flags, FLAGS_BYTES, "lane flags"));
     }
-    CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_solve1, cudaEventDisableTiming), "lane event"));
-    CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming), "lane event"));
-    CHECK(ctx->ensure(L.flags, FLAGS_BYTES, "lane flags"));
+    for (int i = 0; i < 2; i++) L.s[i] = ctx->serial ? ctx->stream : L.own[i];
     return TW_OK;
 }
 
@@ -102,20 +120,21 @@ int lanes_end(tw_ctx* ctx, int nl) {
         CHECK(ctx->cuda(cudaStreamWaitEvent(ctx->stream, L.ev_done, 0), "event"));
     }
     ctx->cur = ctx->stream;
-    int hf[4] = {0, 0, 0, 0};
+    int hf[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int i = 0; i < nl; i++) {
         Lane& L = ctx->lanes[i];
         if (!L.used) continue;
-        int f[4];
+        int f[8];
         CHECK(ctx->cuda(cudaMemcpyAsync(f, (int*)L.flags.p + FL_NAN, sizeof f, cudaMemcpyDeviceToHost, ctx->stream), "flags"));
         CHECK(ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution"));
-        for (int k = 0; k < 4; k++) hf[k] |= f[k];
+        for (int k = 0; k < 8; k++) hf[k] |= f[k];
         L.used = false;
     }
     CHECK(ctx->cuda(cudaGetLastError(), "kernel execution"));
     if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "a solved flow holds a NaN");
     if (hf[1]) return bad_fail(ctx, hf[1]);
     if (hf[3]) return ctx->fail(TW_ERR_UNSUPPORTED, "hole fill of an image with a side of 1 pixel that has a hole");
+    if (hf[FL_BOUND - FL_NAN]) return ctx->fail(TW_ERR_DEVICE_BOUND, "a device loop reached its bound");
     return TW_OK;
 }
 
@@ -179,7 +198,7 @@ void tw_close(tw_ctx* ctx) {
             if (i == 0) { L.comp.release(&ctx->held); L.holes.release(&ctx->held); L.fill.release(&ctx->held); }
             for (DevBuf* b : {&L.wb_wt[i], &L.wb_tmp[i], &L.wb_mask[i], &L.wb_cov[i]}) b->release(&ctx->held);
             if (i == 0) { L.pre_blur.release(&ctx->held); L.user.release(&ctx->held); }
-            if (L.s[i]) cudaStreamDestroy(L.s[i]);
+            if (L.own[i]) cudaStreamDestroy(L.own[i]);
             if (L.ev_pyr[i]) cudaEventDestroy(L.ev_pyr[i]);
         }
         L.flags.release(&ctx->held);
@@ -301,8 +320,19 @@ size_t tw_profile_report(tw_ctx* ctx, char* buf, size_t cap) {
 int tw_set_lanes(tw_ctx* ctx, int32_t lanes) {
     if (!ctx) return TW_ERR_BAD_PARAM;
     std::lock_guard<std::mutex> lk(ctx->mu);
-    if (lanes < 1 || lanes > MAX_LANES) return ctx->fail(TW_ERR_BAD_PARAM, "lanes %d is not in 1..%d", lanes, MAX_LANES);
-    ctx->nlanes = lanes;
+    if (lanes < 0 || lanes > MAX_LANES) return ctx->fail(TW_ERR_BAD_PARAM, "lanes %d is not in 0..%d", lanes, MAX_LANES);
+    ctx->serial = lanes == 0;
+    ctx->nlanes = lanes == 0 ? 1 : lanes;
+    return TW_OK;
+}
+
+int tw_debug_inject(tw_ctx* ctx, int32_t kind, int32_t n) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (kind < TW_INJECT_NONE || kind > TW_INJECT_STATUS || (kind != TW_INJECT_NONE && n < 1))
+        return ctx->fail(TW_ERR_BAD_PARAM, "failure injection: kind %d with count %d", kind, n);
+    ctx->inject_kind = kind;
+    ctx->inject_n = kind == TW_INJECT_NONE ? 0 : n;
     return TW_OK;
 }
 

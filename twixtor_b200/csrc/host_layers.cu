@@ -562,6 +562,7 @@ int tw_compose_layers(tw_ctx* ctx, const tw_retime_settings* s, const tw_selecti
     ctx->cur = ctx->stream;
     if (!s || !sel || !job || !out || !out->data)
         return ctx->fail(TW_ERR_BAD_PARAM, "bad argument");
+    CHECK(check_out(ctx, out, "compose_layers output"));
     CHECK(layer_job_check(ctx, job));
     int nfg = job->nfg;
     if (nfg > 0 && (!mattes_a || !mattes_b)) return ctx->fail(TW_ERR_BAD_PARAM, "bad argument: no mattes");

@@ -97,3 +97,34 @@ extern "C" int tw_select(const tw_time_params* p, int32_t n, int32_t width, int3
     out->interp = p->frame_interp - 1;
     return TW_OK;
 }
+
+// ---- one clip over several GPUs ------------------------------------------------------------------
+
+extern "C" int tw_shard(int32_t nout, int32_t nranks, int32_t rank, int32_t* lo, int32_t* hi) {
+    if (!lo || !hi || nout < 0 || nranks < 1 || rank < 0 || rank >= nranks) return TW_ERR_BAD_PARAM;
+    // contiguous ranges in rank order; the first nout % nranks ranks take one frame more
+    int64_t base = nout / nranks, extra = nout % nranks;
+    int64_t l = rank * base + std::min<int64_t>(rank, extra);
+    *lo = (int32_t)l;
+    *hi = (int32_t)(l + base + (rank < extra ? 1 : 0));
+    return TW_OK;
+}
+
+extern "C" int tw_source_window(const tw_selection* sels, int32_t n, int32_t nframes, int32_t* first, int32_t* last) {
+    if (!first || !last || n < 0 || nframes < 0 || (n > 0 && !sels)) return TW_ERR_BAD_PARAM;
+    int64_t f = INT64_MAX, l = INT64_MIN;
+    for (int32_t k = 0; k < n; k++)
+        for (int32_t idx : {sels[k].a, sels[k].b})  // both frames of the pair are read, exact frames included
+            if (idx >= 0 && idx < nframes) {
+                f = std::min<int64_t>(f, idx);
+                l = std::max<int64_t>(l, idx);
+            }
+    if (f > l) {  // nothing inside the clip
+        *first = 0;
+        *last = -1;
+    } else {
+        *first = (int32_t)f;
+        *last = (int32_t)l;
+    }
+    return TW_OK;
+}

@@ -10,8 +10,6 @@
 // library holds until the process exits.
 #include <cuda_runtime.h>
 
-#include <mutex>
-
 #include "../../include/twixtor_b200.h"
 #include "kernels.cuh"
 
@@ -22,29 +20,29 @@ namespace {
 constexpr long NOALLOC_MAX_PIXELS = TW_NOALLOC_MAX_PIXELS;
 static __device__ __align__(256) float g_noalloc_planes[6 * NOALLOC_MAX_PIXELS];
 
-constexpr int MAX_DEVICES = 64;
-std::mutex g_setup_mu;
-float* g_planes_addr[MAX_DEVICES] = {};  // device address of g_noalloc_planes, per device
-
-// Once per device, with that device current: the device address of the scratch array (the host
-// side name g_noalloc_planes is only a stand-in, not a device pointer) and the shared memory limit
-// of the sweep kernels. Neither allocates.
-int setup(int device, float** planes) {
-    std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (device < 0 || device >= MAX_DEVICES) return TW_ERR_UNSUPPORTED;
-    if (!g_planes_addr[device]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_planes) != cudaSuccess || !p) return TW_ERR_CUDA;
-        if (cudaFuncSetAttribute(tw::k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tw::bm_smem_bytes(tw::BM_MAX_LINE)) != cudaSuccess)
-            return TW_ERR_CUDA;
-        if (cudaFuncSetAttribute(tw::k_bm_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tw::bm_smem_bytes(tw::BM_MAX_LINE)) != cudaSuccess)
-            return TW_ERR_CUDA;
-        g_planes_addr[device] = (float*)p;
-    }
-    *planes = g_planes_addr[device];
+// The set-up of every call, in the CUDA context current on the calling thread: the device address of
+// the scratch array there (the host side name g_noalloc_planes is only a stand-in, not a device
+// pointer) and the shared memory limit of the sweep kernels. Both belong to the context, not to the
+// device ordinal (a host may bind its own driver context, or reset the device between calls), so
+// nothing is cached across calls; neither allocates.
+int setup(float** planes) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_planes) != cudaSuccess || !p) return TW_ERR_CUDA;
+    int smem = (int)tw::bm_smem_bytes(tw::BM_MAX_LINE);
+    if (cudaFuncSetAttribute(tw::k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return TW_ERR_CUDA;
+    if (cudaFuncSetAttribute(tw::k_bm_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return TW_ERR_CUDA;
+    *planes = (float*)p;
     return TW_OK;
+}
+
+// One launch through cudaLaunchKernel, whose return code is this launch's own: an error that the
+// host's earlier launches left pending is neither reported as this call's nor cleared.
+template <typename... Args>
+cudaError_t launch(void (*kernel)(Args...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    void* argv[] = {(void*)&args...};
+    return cudaLaunchKernel((const void*)kernel, grid, block, argv, smem, s);
 }
 
 }  // namespace
@@ -54,10 +52,8 @@ extern "C" int tw_block_match_noalloc(const float* a, const float* b, float* flo
     if (!a || !b || !flow || width <= 0 || height <= 0) return TW_ERR_BAD_PARAM;
     if ((long)width * height > NOALLOC_MAX_PIXELS || width > tw::BM_MAX_LINE || height > tw::BM_MAX_LINE)
         return TW_ERR_TOO_LARGE;
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess) return TW_ERR_CUDA;
     float* planes = nullptr;
-    int rc = setup(device, &planes);
+    int rc = setup(&planes);
     if (rc != TW_OK) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     long n = (long)width * height;
@@ -65,20 +61,27 @@ extern "C" int tw_block_match_noalloc(const float* a, const float* b, float* flo
     float* fv = fu + n;
     float *at = fv + n, *bt = at + n, *ut = bt + n, *vt = ut + n;
     const int tb = 256;
-    unsigned g1 = (unsigned)((n + tb - 1) / tb);
+    dim3 g1((unsigned)((n + tb - 1) / tb));
     dim3 tt(32, 8), ga((width + 31) / 32, (height + 31) / 32), gb((height + 31) / 32, (width + 31) / 32);
+    const float* cfu = fu;
+    const float* cfv = fv;
+    const float* cut = ut;
+    const float* cvt = vt;
     // every element of the planes this call reads is written first, so the previous call's
     // contents never reach the result
-    tw::k_deinterleave<<<g1, tb, 0, s>>>(flow, n, fu, fv);
-    if (width >= 3 && height >= 3) {
-        tw::k_bm_rows<<<height - 2, tb, tw::bm_smem_bytes(width), s>>>(a, b, fu, fv, width, height);
-        tw::k_transpose2<<<ga, tt, 0, s>>>(a, b, at, bt, width, height);
-        tw::k_transpose2<<<ga, tt, 0, s>>>(fu, fv, ut, vt, width, height);
-        tw::k_bm_cols<<<width - 2, tb, tw::bm_smem_bytes(height), s>>>(at, bt, ut, vt, width, height);
-        tw::k_transpose2<<<gb, tt, 0, s>>>(ut, vt, fu, fv, height, width);
+    cudaError_t e = launch(tw::k_deinterleave, g1, dim3(tb), 0, s, (const float*)flow, n, fu, fv);
+    if (e == cudaSuccess && width >= 3 && height >= 3) {
+        e = launch(tw::k_bm_rows, dim3(height - 2), dim3(tb), tw::bm_smem_bytes(width), s, a, b, fu, fv, (int)width,
+                   (int)height);
+        if (e == cudaSuccess) e = launch(tw::k_transpose2, ga, tt, 0, s, a, b, at, bt, (int)width, (int)height);
+        if (e == cudaSuccess) e = launch(tw::k_transpose2, ga, tt, 0, s, cfu, cfv, ut, vt, (int)width, (int)height);
+        if (e == cudaSuccess)
+            e = launch(tw::k_bm_cols, dim3(width - 2), dim3(tb), tw::bm_smem_bytes(height), s, (const float*)at,
+                       (const float*)bt, ut, vt, (int)width, (int)height);
+        if (e == cudaSuccess) e = launch(tw::k_transpose2, gb, tt, 0, s, cut, cvt, fu, fv, (int)height, (int)width);
     }
-    tw::k_interleave<<<g1, tb, 0, s>>>(fu, fv, n, flow);
-    if (cudaGetLastError() != cudaSuccess) return TW_ERR_CUDA;
+    if (e == cudaSuccess) e = launch(tw::k_interleave, g1, dim3(tb), 0, s, cfu, cfv, n, flow);
+    if (e != cudaSuccess) return TW_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return TW_ERR_CUDA;
     return TW_OK;
 }

@@ -31,6 +31,7 @@ void start_level(float sensitivity, int levels, int* start, float* damp);
 Taps gaussian_taps(float r);
 Taps binomial5();
 inline size_t sample_bytes(int fmt) { return fmt == TW_U8 ? 1 : fmt == TW_U16 ? 2 : 4; }
+inline size_t image_bytes(int w, int h, int fmt) { return (size_t)w * h * 4 * sample_bytes(fmt); }
 
 // ---- device buffers --------------------------------------------------------------------------------
 
@@ -74,7 +75,8 @@ struct KernelProfile {
 // two solves of a pair run concurrently (stream 0: A's pyramid, solve(A, B), the composition;
 // stream 1: B's pyramid, solve(B, A)). Several lanes keep several output frames in flight.
 struct Lane {
-    cudaStream_t s[2] = {nullptr, nullptr};
+    cudaStream_t s[2] = {nullptr, nullptr};    // the streams this call uses: own[] or, serial, the context's
+    cudaStream_t own[2] = {nullptr, nullptr};  // the lane's own streams
     cudaEvent_t ev_pyr[2] = {nullptr, nullptr};  // pyramid of A / B done
     cudaEvent_t ev_solve1 = nullptr;             // solve on stream 1 done
     cudaEvent_t ev_done = nullptr;               // the frame's composition done (stream 0)
@@ -93,6 +95,7 @@ struct tw_ctx {
     cudaStream_t cur = nullptr;  // the stream every launch goes to
     Lane lanes[MAX_LANES];
     int nlanes = 4;  // output frames in flight in the clip calls (tw_set_lanes)
+    bool serial = false;  // tw_set_lanes(ctx, 0): one lane whose work all runs on the context's stream
     cudaEvent_t ev_start = nullptr;
     // tw_retime_clip: a device cache of source frames, and the copy streams
     static constexpr int CACHE_SLOTS = 20;
@@ -140,7 +143,19 @@ struct tw_ctx {
         if (e == cudaSuccess) return TW_OK;
         return fail(TW_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
     }
-    int ensure(DevBuf& b, size_t n, const char* what) { return cuda(b.ensure(n, &held), what); }
+    // tw_debug_inject: the kind of failure armed and the count of events before it fires
+    int inject_kind = 0, inject_n = 0;
+    bool inject_now(int kind) {  // true once, at the n-th event of the armed kind
+        if (inject_kind != kind || inject_n <= 0) return false;
+        if (--inject_n > 0) return false;
+        inject_kind = 0;
+        return true;
+    }
+    int ensure(DevBuf& b, size_t n, const char* what) {
+        if (n > b.cap && inject_now(TW_INJECT_ALLOC))  // the buffer is left as it was, as a failed cudaMalloc leaves it
+            return fail(TW_ERR_CUDA, "%s: out of memory (injected allocation failure)", what);
+        return cuda(b.ensure(n, &held), what);
+    }
 };
 
 // The glibc logf exception table embedded by the build (csrc/logf_table.S).
@@ -179,7 +194,8 @@ void prof_mark(tw_ctx* ctx);
 constexpr int TB = 256;
 // device flags (ints): [0..31] per-level range flags of solve 0, [32..63] of solve 1, [64] NaN in a
 // flow, [65] a warp refused a sample coordinate
-constexpr int FL_ANY0 = 0, FL_ANY1 = 32, FL_NAN = 64, FL_BAD = 65, FL_HOLE = 66, FL_SIDE1 = 67, FL_ONE = 68, FL_WB = 69;
+constexpr int FL_ANY0 = 0, FL_ANY1 = 32, FL_NAN = 64, FL_BAD = 65, FL_HOLE = 66, FL_SIDE1 = 67, FL_ONE = 68, FL_WB = 69,
+              FL_BOUND = 70;  // [70] a device loop reached its bound
 constexpr size_t FLAGS_BYTES = 128 * sizeof(int);
 
 inline dim3 grid2(int w, int h) { return dim3((unsigned)((w + TB - 1) / TB), (unsigned)h); }
@@ -213,10 +229,12 @@ int upload_image(tw_ctx* ctx, DevBuf& b, const tw_image* im);
 int finish(tw_ctx* ctx, int* flags_host, int n);
 bool same_shape(const tw_image* a, const tw_image* b);
 int check_image(tw_ctx* ctx, const tw_image* im, const char* what);
+int check_out(tw_ctx* ctx, const tw_image_mut* im, const char* what);
 int lane_ready(tw_ctx* ctx, Lane& L);
 int lanes_begin(tw_ctx* ctx, int nl);
 int lanes_end(tw_ctx* ctx, int nl);
 int bad_fail(tw_ctx* ctx, int v);
+__global__ void k_set_flag(int* flags, int idx);  // flags[idx] = 1 (the injected device status)
 
 // host_solve.cu
 size_t pyramid_floats(const Geo& g);

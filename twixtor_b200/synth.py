@@ -68,11 +68,12 @@ def _to_wire(rgb, alpha, depth):
 
 
 def moving_clip(width, height, frames, depth=8, seed=0x74570001, bg_velocity=(1.5, -0.75), square=32,
-                square_start=(20.0, 30.0), square_velocity=(2.0, 1.0), alpha=None):
+                square_start=(20.0, 30.0), square_velocity=(2.0, 1.0), alpha=None, window=None):
     """A clip of ``frames`` wire frames back to back (one flat array): the noise background
     translated by ``bg_velocity`` px/frame and a ``square`` x ``square`` checker (8 px cells,
     values 40 / 215) moving by ``square_velocity``. ``alpha`` (optional callable (X, Y, t) -> [0,1])
-    makes a straight alpha channel; opaque by default.
+    makes a straight alpha channel; opaque by default. ``window`` = (first, last): only the frames
+    first..last of the clip (the same samples as in the whole clip), for a rank of a sharded render.
 
     The background is evaluated once over the area every frame's translation covers and each
     frame resamples it bilinearly at its sub-pixel offset."""
@@ -87,7 +88,8 @@ def moving_clip(width, height, frames, depth=8, seed=0x74570001, bg_velocity=(1.
     base = noise.at(BX, BY)
     X, Y = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64))
     out = []
-    for t in range(frames):
+    t_first, t_last = (0, frames - 1) if window is None else window
+    for t in range(t_first, t_last + 1):
         # background value at (X - vx t, Y - vy t): position inside the base grid
         px, py = -vx * t - ox, -vy * t - oy
         ix, iy = int(np.floor(px)), int(np.floor(py))
