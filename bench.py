@@ -191,13 +191,16 @@ def run_reference(args):
     return 0
 
 
-def ncu_case():
+def ncu_case(tune_cache=None):
     """One step of the workload (10 output frames of the 1080p clip, 2 exact and 8 in-between), for
-    an ncu capture: a few hundred kernel launches, 0.1 GB on the device."""
+    an ncu capture: a few hundred kernel launches, 0.1 GB on the device. The autotuner's table comes
+    from `tune_cache` when given (a run without ncu writes it; under ncu it is only read, so the
+    launch list holds the step alone)."""
     import twixtor_b200 as tw
     nframes = source_frames_needed(FRAMES_PER_STEP)
     frames_np = make_clip(nframes)
     dev = tw.Device(0)
+    dev.autotune(tw.FlowSettings(quality=4), W, H, path=tune_cache)
     tp = tw.TimeParams(speed_percent=SPEED)
     sels = [tw.select(tp, n, W, H) for n in range(FRAMES_PER_STEP)]
     out = np.zeros(FRAMES_PER_STEP * W * H * 4, np.uint8)
@@ -261,6 +264,7 @@ def run_workload(args):
         metric = "1080p retime-fgbg output frames/s, 3 FG layers (strict byte-exact GPU vs CPU)"
         workload = "retime-fgbg 1920x1080 8bpc RGBA, 3 FG matte layers (binary ellipses, red channel), speed 40%"
         h2d = per * 2 * (nfg + 1) * W * H * 4
+    dev.autotune(tw.FlowSettings(quality=4), W, H)
     if args.ncu_case:  # the profiling driver: one step (5 output frames), no timing
         step(0)
         torch.cuda.synchronize()
@@ -414,6 +418,9 @@ def run_batch(args):
         jobs.append(dict(settings=tw.RetimeSettings(), frames=frames.data_ptr(), nframes=nsrc, sels=sels, width=w,
                          height=h, fmt=2, out=out.data_ptr()))
 
+    for w, h in BATCH_SIZES:
+        dev.autotune(tw.FlowSettings(quality=4), w, h)
+
     def step(k):
         dev.retime_batch_device([dict(j, sels=j["sels"][k * per:(k + 1) * per]) for j in jobs])
 
@@ -472,9 +479,8 @@ def main():
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling driver, no timing: renders the first 10 output frames of the 1080p workload once "
                          "(device resident clip) and exits; the command the committed ncu summaries name")
-    ap.add_argument("--breakdown", action="store_true",
-                    help="after the timed region, time one more step with every kernel bracketed by events and "
-                         "print the per-kernel table to stderr (not part of the reported numbers)")
+    ap.add_argument("--tune-cache", default=None,
+                    help="--ncu-case: the autotuner's JSON table, read when present, written otherwise")
     ap.add_argument("--workload", default="retime", choices=["retime", "create-vectors", "fgbg", "adjoint", "batch"],
                     help="retime (the headline, default), create-vectors (1080p 16 bpc), fgbg (1080p, 3 FG layers) or "
                          "adjoint (warp + blend gradients, 64 triples of 1280x720) or batch (4 clips of uneven size)")
@@ -490,7 +496,7 @@ def main():
     if args.workload != "retime":
         return run_workload(args)
     if args.ncu_case and args.workload == "retime":
-        return ncu_case()
+        return ncu_case(args.tune_cache)
 
     import torch
     import twixtor_b200 as tw
@@ -520,6 +526,9 @@ def main():
     dev.set_stream(stream.cuda_stream)
     settings = tw.RetimeSettings()
 
+    # the autotuner's launch shapes for every level of the 1080p solve (measured once, before the
+    # warm-up; the table only changes the time, never the bytes)
+    tuned = dev.autotune(tw.FlowSettings(quality=sels[0].vectors_quality or 4), W, H)
     clip = torch.from_numpy(frames_np).to(f"cuda:{local}")
     out = torch.empty(FRAMES_PER_STEP * fs, dtype=torch.uint8, device=f"cuda:{local}")
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
@@ -626,7 +635,8 @@ def main():
                        "l2": "flushed between steps (256 MiB write), inputs resident 0.5 GB > L2",
                        "parallelism": (f"one clip of {total_out} output frames split into {ws} contiguous ranges "
                                        f"of {per_rank} (one per GPU, each holding only its source window); "
-                                       "no collective on the data path") if ws > 1 else "1 GPU"},
+                                       "no collective on the data path") if ws > 1 else "1 GPU",
+                       "autotuned_levels": tuned, "tuning": json.loads(dev.tuning_table())["levels"]},
             "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": roofline_entry(kernels, serial_ms, launches / args.steps, total_ms / args.steps, peak,

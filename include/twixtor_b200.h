@@ -164,6 +164,26 @@ int tw_set_lanes(tw_ctx* ctx, int32_t lanes);
 #define TW_INJECT_STATUS 2
 int tw_debug_inject(tw_ctx* ctx, int32_t kind, int32_t n);
 
+/* The autotuner (no counterpart in the reference, whose OpenCL kernels launch one shape): for every
+ * level size of a solve of a width x height frame under settings s, it times on the device the
+ * tile shapes (32x32, 64x32, 64x64) and block sizes (256, 512) of the solver iteration and the
+ * block sizes (128, 256, 512 threads per line) of the row and the column block matching, on
+ * stand-in planes of that size, and keeps the fastest of each in the context's table, which every
+ * later solve on the context uses. With path != NULL the table is first read from that JSON file
+ * (entries written by this library for a device of the same name; sizes found there are not
+ * measured again) and then written back: the persistent cache of the tuned shapes. `measured`
+ * (may be NULL) receives the number of level sizes timed. Every shape computes the same bytes. */
+int tw_autotune(tw_ctx* ctx, const tw_flow_settings* s, int32_t width, int32_t height, const char* path,
+                int32_t* measured);
+/* The context's table as the JSON text tw_autotune writes (NUL terminated); returns its full length. */
+size_t tw_tuning_table(tw_ctx* ctx, char* buf, size_t cap);
+/* Sets the table entry of one level size by hand (iter_tile 0 32x32, 1 64x32, 2 64x64; block sizes
+ * multiples of 32, at most 512 for the iteration and 1024 for block matching), or clears the
+ * table (sizes without an entry take the defaults). */
+int tw_tuning_set(tw_ctx* ctx, int32_t width, int32_t height, int32_t iter_tile, int32_t iter_threads,
+                  int32_t bm_rows_threads, int32_t bm_cols_threads);
+int tw_tuning_clear(tw_ctx* ctx);
+
 /* Makes the context enqueue on `stream` (a cudaStream_t; NULL is the legacy default stream)
  * instead of its own, so a caller can order the library's work with its own and time it with its
  * own events. */

@@ -312,6 +312,11 @@ def library():
     L.tw_stats.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.tw_set_stream.argtypes = [P, P]
     L.tw_debug_inject.argtypes = [P, i32, i32]
+    L.tw_autotune.argtypes = [P, ctypes.POINTER(_FlowSettings), i32, i32, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32)]
+    L.tw_tuning_table.argtypes = [P, ctypes.c_char_p, ctypes.c_size_t]
+    L.tw_tuning_table.restype = ctypes.c_size_t
+    L.tw_tuning_set.argtypes = [P, i32, i32, i32, i32, i32, i32]
+    L.tw_tuning_clear.argtypes = [P]
     L.tw_profile_begin.argtypes = [P, ctypes.c_char_p]
     L.tw_profile_end.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64),
                                  ctypes.POINTER(ctypes.c_double)]
@@ -471,6 +476,28 @@ class Device:
             buf = ctypes.create_string_buffer(n + 1)
             self._L.tw_last_error(self._h, buf, n + 1)
             raise (_ERRORS.get(rc, StageError))(rc, buf.value.decode())
+
+    def autotune(self, settings: FlowSettings, width: int, height: int, path: Optional[str] = None) -> int:
+        """Times the launch shapes of every level size of a width x height solve and keeps the
+        fastest (tw_autotune); ``path``: the JSON cache read first and written after. Returns the
+        number of level sizes measured."""
+        n = ctypes.c_int32()
+        self._check(self._L.tw_autotune(self._h, ctypes.byref(settings._c()), width, height,
+                                        None if path is None else path.encode(), ctypes.byref(n)))
+        return n.value
+
+    def tuning_table(self) -> str:
+        n = self._L.tw_tuning_table(self._h, None, 0)
+        buf = ctypes.create_string_buffer(n + 1)
+        self._L.tw_tuning_table(self._h, buf, n + 1)
+        return buf.value.decode()
+
+    def tuning_set(self, width, height, iter_tile, iter_threads, bm_rows_threads, bm_cols_threads):
+        self._check(self._L.tw_tuning_set(self._h, width, height, iter_tile, iter_threads, bm_rows_threads,
+                                          bm_cols_threads))
+
+    def tuning_clear(self):
+        self._check(self._L.tw_tuning_clear(self._h))
 
     def debug_inject(self, kind: int, n: int = 1):
         """Arms a host-injected failure (tw_debug_inject): INJECT_ALLOC fails the n-th device

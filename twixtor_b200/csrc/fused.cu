@@ -222,104 +222,228 @@ size_t level_init_smem() {
 
 // ---- one solver iteration (flow.rs:1278-1282): calc_b, blur7 of B, new_disp, blur5 of the flow -----
 // mask_y (may be null): the level mask of Y of a layered solve
-
+//
 // Halos: the flow's blur5 needs new_disp on the tile + 5; new_disp needs blurred B there, which
-// needs B on the tile + 12.
-constexpr int IT_HB = 12;                 // B region halo
-constexpr int IT_HD = 5;                  // new_disp region halo
-constexpr int IT_BW = FT_X + 2 * IT_HB;   // 56
-constexpr int IT_BH = FT_Y + 2 * IT_HB;
-constexpr int IT_DW = FT_X + 2 * IT_HD;   // 42
-constexpr int IT_DH = FT_Y + 2 * IT_HD;
+// needs B on the tile + 12. The tile is TX x TY outputs (a template: the host picks the shape per
+// level size from its tuning table). The separable passes are register blocked: a thread computes R
+// consecutive outputs along the pass from R + 2N - 2 inputs held in registers (each input read once
+// from shared memory instead of once per tap), each output with the reference's interior chain;
+// outputs near the image border, or at the ragged end of a region, take the element rule (interior
+// chain or border renormalisation) one by one. Horizontal passes give each lane of a warp its own
+// row (row strides are odd, so the lanes hit distinct banks), vertical passes its own column.
 
-size_t level_iter_smem() {
-    // buffer 1: B (2 planes IT_BH x IT_BW), later the blurred B / new flow (2 x IT_DH x IT_DW)
-    // buffer 2: horizontal pass of B (2 x IT_BH x IT_DW), later of the flow (2 x IT_DH x FT_X)
-    return sizeof(float) * (2 * IT_BH * IT_BW + 2 * IT_BH * IT_DW);
+template <int TX, int TY>
+struct IterGeom {
+    static constexpr int HB = 12, HD = 5;
+    static constexpr int BW = TX + 2 * HB, BH = TY + 2 * HB;  // B region
+    static constexpr int DW = TX + 2 * HD, DH = TY + 2 * HD;  // new_disp region
+    static constexpr int BS = BW | 1;                          // row strides (odd)
+    static constexpr int HS = DW | 1;
+    static constexpr int DS = DW | 1;
+    static constexpr int FS = TX | 1;
+    // buffer 1: B (2 planes BH x BS), later the blurred B / new flow (2 planes DH x DS)
+    // buffer 2: the horizontal pass of B (2 planes BH x HS), later of the flow (2 planes DH x FS)
+    static constexpr int BUF1 = 2 * BH * BS;
+    static constexpr int BUF2 = 2 * BH * HS;
+    static constexpr size_t SMEM = sizeof(float) * (BUF1 + BUF2);
+    static_assert(2 * DH * DS <= BUF1 && 2 * DH * FS <= BUF2, "the reused buffers must fit");
+};
+
+// R outputs of a pass along one line at line indices i0 .. i0 + R - 1 (global), written to
+// out[r * ostride] for r < nvalid where the index lies in [0, len). The line's element t (global
+// index) is line[(t - origin) * stride]; the region holds indices [origin, origin + rlen). The
+// register path runs only when every output is interior and every input lies in the region.
+template <int N, int R, bool MULTI, bool LEFT_FIRST>
+__device__ __forceinline__ void pass_run(const float* line, int origin, int rlen, int stride, int len, int i0,
+                                         const float* k, float* out, int ostride, int nvalid) {
+    constexpr int NV = R + 2 * N - 2;
+    bool interior = nvalid == R && len >= 2 * N && i0 >= N && i0 + R - 1 < len - N && i0 - (N - 1) >= origin &&
+                    i0 + R - 1 + (N - 1) < origin + rlen;
+    if (interior) {
+        float v[NV];
+        const float* base = line + (i0 - (N - 1) - origin) * stride;
+#pragma unroll
+        for (int j = 0; j < NV; j++) v[j] = base[j * stride];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            float s = v[r + N - 1] * k[0];
+#pragma unroll
+            for (int j = N - 1; j >= 1; j--) s = s + (v[r + N - 1 + j] + v[r + N - 1 - j]) * k[j];
+            out[r * ostride] = s;
+        }
+    } else {
+        for (int r = 0; r < nvalid; r++) {
+            int i = i0 + r;
+            if (i < 0 || i >= len) continue;
+            out[r * ostride] = pass_elem<N, MULTI, LEFT_FIRST>(line, origin, stride, len, i, k);
+        }
+    }
 }
 
-__global__ void __launch_bounds__(FT_THREADS) k_level_iter(const float* __restrict__ i1, const float* __restrict__ i0,
-                                                           const float* __restrict__ gx, const float* __restrict__ gy,
-                                                           const float* __restrict__ a0, const float* __restrict__ a1,
-                                                           const float* __restrict__ a2, const float* __restrict__ fu,
-                                                           const float* __restrict__ fv, int w, int h, Taps g7, Taps g5,
-                                                           bool above_first, float* __restrict__ fu_out,
-                                                           float* __restrict__ fv_out,
-                                                           const float* __restrict__ mask_y) {
+template <int TX, int TY>
+__device__ __forceinline__ void level_iter_body(const float* __restrict__ i1, const float* __restrict__ i0,
+                                                const float* __restrict__ gx, const float* __restrict__ gy,
+                                                const float* __restrict__ a0, const float* __restrict__ a1,
+                                                const float* __restrict__ a2, const float* __restrict__ fu,
+                                                const float* __restrict__ fv, int w, int h, const Taps& g7,
+                                                const Taps& g5, bool above_first, float* __restrict__ fu_out,
+                                                float* __restrict__ fv_out, const float* __restrict__ mask_y) {
+    using G = IterGeom<TX, TY>;
+    constexpr int R7 = 6, R5 = 8;  // outputs per thread of the blur7 and blur5 passes
     extern __shared__ float sm[];
-    float* s_b = sm;                                  // 2 x IT_BH x IT_BW
-    float* s_h = s_b + 2 * IT_BH * IT_BW;             // 2 x IT_BH x IT_DW
-    float* s_d = s_b;                                 // reuse: 2 x IT_DH x IT_DW (blurred B -> new flow)
-    float* s_f = s_h;                                 // reuse: 2 x IT_DH x FT_X
-    int X0 = blockIdx.x * FT_X, Y0 = blockIdx.y * FT_Y;
-    int bx0 = X0 - IT_HB, by0 = Y0 - IT_HB;
-    int dx0 = X0 - IT_HD, dy0 = Y0 - IT_HD;
+    float* s_b = sm;            // 2 x BH x BS
+    float* s_h = sm + G::BUF1;  // 2 x BH x HS
+    float* s_d = s_b;           // reuse: 2 x DH x DS (blurred B -> new flow)
+    float* s_f = s_h;           // reuse: 2 x DH x FS
+    const int X0 = blockIdx.x * TX, Y0 = blockIdx.y * TY;
+    const int bx0 = X0 - G::HB, by0 = Y0 - G::HB;
+    const int dx0 = X0 - G::HD, dy0 = Y0 - G::HD;
     const float fw = (float)w, fh = (float)h;
-    // 1. B = calc_b over the B region (flow.rs:334-357)
-    for (int e = threadIdx.x; e < IT_BW * IT_BH; e += blockDim.x) {
-        int r = e / IT_BW, c = e - r * IT_BW;
-        int x = bx0 + c, y = by0 + r;
-        float b0 = 0.0f, b1 = 0.0f;
-        if (x >= 0 && x < w && y >= 0 && y < h) {
-            long i = (long)y * w + x;
-            float sx = (float)x - __ldg(fu + i);
-            float sy = (float)y - __ldg(fv + i);
-            // flow.rs:777-845: in a layered solve the warped mask of Y must be at least 0.999
-            if (!(sx < 0.0f || fw - 1.0f < sx || sy < 0.0f || fh - 1.0f < sy) &&
-                (!mask_y || bilinear1(mask_y, w, h, sx, sy) >= 0.999f)) {
-                float s = bilinear1(i0, w, h, sx, sy);
-                float rr = s - __ldg(i1 + i);
-                b0 = rr * __ldg(gx + i);
-                b1 = rr * __ldg(gy + i);
+    const int nt = blockDim.x;
+    // 1. B = calc_b over the B region (flow.rs:334-357), two elements per thread and round so that
+    //    the loads of both are in flight together
+    constexpr int NB = G::BW * G::BH;
+    for (int e0 = threadIdx.x; e0 < NB; e0 += 2 * nt) {
+        float sx[2], sy[2], i1v[2], gxv[2], gyv[2];
+        bool in[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            int e = e0 + k * nt;
+            int r = e / G::BW, c = e - r * G::BW;
+            int x = bx0 + c, y = by0 + r;
+            in[k] = e < NB && x >= 0 && x < w && y >= 0 && y < h;
+            sx[k] = sy[k] = i1v[k] = gxv[k] = gyv[k] = 0.0f;
+            if (in[k]) {
+                int i = y * w + x;
+                sx[k] = (float)x - __ldg(fu + i);
+                sy[k] = (float)y - __ldg(fv + i);
+                i1v[k] = __ldg(i1 + i);
+                gxv[k] = __ldg(gx + i);
+                gyv[k] = __ldg(gy + i);
             }
         }
-        s_b[e] = b0;
-        s_b[IT_BH * IT_BW + e] = b1;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            int e = e0 + k * nt;
+            if (e >= NB) break;
+            float b0 = 0.0f, b1 = 0.0f;
+            // flow.rs:777-845: in a layered solve the warped mask of Y must be at least 0.999
+            if (in[k] && !(sx[k] < 0.0f || fw - 1.0f < sx[k] || sy[k] < 0.0f || fh - 1.0f < sy[k]) &&
+                (!mask_y || bilinear1(mask_y, w, h, sx[k], sy[k]) >= 0.999f)) {
+                float sv = bilinear1(i0, w, h, sx[k], sy[k]);
+                float rr = sv - i1v[k];
+                b0 = rr * gxv[k];
+                b1 = rr * gyv[k];
+            }
+            int r = e / G::BW, c = e - r * G::BW;
+            s_b[r * G::BS + c] = b0;
+            s_b[G::BH * G::BS + r * G::BS + c] = b1;
+        }
     }
     __syncthreads();
-    // 2. blur7 of B (2 channels): horizontal over the B rows, at the new_disp columns
-    for (int ch = 0; ch < 2; ch++)
-        region_pass<8, true, false, false>(s_b + ch * IT_BH * IT_BW, IT_BW, bx0, by0, s_h + ch * IT_BH * IT_DW, IT_DW,
-                                           IT_BH, dx0, by0, w, h, g7.k);
+    // 2. blur7 of B (2 channels): horizontal along the B rows, outputs at the new_disp columns
+    {
+        constexpr int NSEG = (G::DW + R7 - 1) / R7;
+        for (int e = threadIdx.x; e < 2 * G::BH * NSEG; e += nt) {
+            int r = e % G::BH, rest = e / G::BH;
+            int seg = rest % NSEG, ch = rest / NSEG;
+            int Y = by0 + r;
+            if (Y < 0 || Y >= h) continue;
+            int c0 = seg * R7;
+            const float* line = s_b + ch * G::BH * G::BS + r * G::BS;
+            pass_run<8, R7, true, false>(line, bx0, G::BW, 1, w, dx0 + c0, g7.k,
+                                         s_h + ch * G::BH * G::HS + r * G::HS + c0, 1, min(R7, G::DW - c0));
+        }
+    }
     __syncthreads();
-    //    vertical, at the new_disp rows (into buffer 1, whose B is no longer needed)
-    for (int ch = 0; ch < 2; ch++)
-        vpass<8, true>(s_h + ch * IT_BH * IT_DW, IT_DW, dx0, by0, s_d + ch * IT_DH * IT_DW, IT_DW, IT_DH, dx0, dy0, w, h,
-                       g7.k, above_first);
+    //    vertical, outputs at the new_disp rows (into buffer 1, whose B is no longer needed)
+    {
+        constexpr int NSEG = (G::DH + R7 - 1) / R7;
+        for (int e = threadIdx.x; e < 2 * G::DW * NSEG; e += nt) {
+            int c = e % G::DW, rest = e / G::DW;
+            int seg = rest % NSEG, ch = rest / NSEG;
+            int X = dx0 + c;
+            if (X < 0 || X >= w) continue;
+            int r0 = seg * R7;
+            const float* line = s_h + ch * G::BH * G::HS + c;
+            float* o = s_d + ch * G::DH * G::DS + r0 * G::DS + c;
+            int nv = min(R7, G::DH - r0);
+            if (above_first) pass_run<8, R7, true, true>(line, by0, G::BH, G::HS, h, dy0 + r0, g7.k, o, G::DS, nv);
+            else pass_run<8, R7, true, false>(line, by0, G::BH, G::HS, h, dy0 + r0, g7.k, o, G::DS, nv);
+        }
+    }
     __syncthreads();
     // 3. new_disp over the new_disp region (flow.rs:361-371), in place on the blurred B
-    for (int e = threadIdx.x; e < IT_DW * IT_DH; e += blockDim.x) {
-        int r = e / IT_DW, c = e - r * IT_DW;
+    for (int e = threadIdx.x; e < G::DW * G::DH; e += nt) {
+        int r = e / G::DW, c = e - r * G::DW;
         int x = dx0 + c, y = dy0 + r;
         if (x < 0 || x >= w || y < 0 || y >= h) continue;
-        long i = (long)y * w + x;
+        int i = y * w + x;
         float aa = __ldg(a0 + i), ab = __ldg(a1 + i), ad = __ldg(a2 + i);
-        float b0 = s_d[e], b1 = s_d[IT_DH * IT_DW + e];
+        int si = r * G::DS + c;
+        float b0 = s_d[si], b1 = s_d[G::DH * G::DS + si];
         float u = __ldg(fu + i), v = __ldg(fv + i);
         float t = ab * ab - ad * aa;
         if (fabsf(t) > 40.0f) {
             u = (ab * b1 - ad * b0) / t + u;
             v = (ab * b0 - aa * b1) / t + v;
         }
-        s_d[e] = u;
-        s_d[IT_DH * IT_DW + e] = v;
+        s_d[si] = u;
+        s_d[G::DH * G::DS + si] = v;
     }
     __syncthreads();
     // 4. blur5 of the flow: horizontal at the tile columns, then vertical at the tile rows
-    for (int ch = 0; ch < 2; ch++)
-        region_pass<6, true, false, false>(s_d + ch * IT_DH * IT_DW, IT_DW, dx0, dy0, s_f + ch * IT_DH * FT_X, FT_X,
-                                           IT_DH, X0, dy0, w, h, g5.k);
+    {
+        constexpr int NSEG = (TX + R5 - 1) / R5;
+        for (int e = threadIdx.x; e < 2 * G::DH * NSEG; e += nt) {
+            int r = e % G::DH, rest = e / G::DH;
+            int seg = rest % NSEG, ch = rest / NSEG;
+            int Y = dy0 + r;
+            if (Y < 0 || Y >= h) continue;
+            int c0 = seg * R5;
+            const float* line = s_d + ch * G::DH * G::DS + r * G::DS;
+            pass_run<6, R5, true, false>(line, dx0, G::DW, 1, w, X0 + c0, g5.k,
+                                         s_f + ch * G::DH * G::FS + r * G::FS + c0, 1, min(R5, TX - c0));
+        }
+    }
     __syncthreads();
-    for (int e = threadIdx.x; e < 2 * FT_X * FT_Y; e += blockDim.x) {
-        int ch = e / (FT_X * FT_Y);
-        int q = e - ch * FT_X * FT_Y;
-        int r = q / FT_X, c = q - r * FT_X;
-        int X = X0 + c, Y = Y0 + r;
-        if (X >= w || Y >= h) continue;
-        const float* line = s_f + ch * IT_DH * FT_X + c;
-        float v = above_first ? pass_elem<6, true, true>(line, dy0, FT_X, h, Y, g5.k)
-                              : pass_elem<6, true, false>(line, dy0, FT_X, h, Y, g5.k);
-        (ch == 0 ? fu_out : fv_out)[(long)Y * w + X] = v;
+    {
+        constexpr int NSEG = (TY + R5 - 1) / R5;
+        for (int e = threadIdx.x; e < 2 * TX * NSEG; e += nt) {
+            int c = e % TX, rest = e / TX;
+            int seg = rest % NSEG, ch = rest / NSEG;
+            int X = X0 + c;
+            if (X >= w) continue;
+            int r0 = seg * R5;
+            const float* line = s_f + ch * G::DH * G::FS + c;
+            int nv = min(R5, TY - r0);
+            float* dst = (ch == 0 ? fu_out : fv_out) + (Y0 + r0) * w + X;  // rows past h are never written
+            if (above_first) pass_run<6, R5, true, true>(line, dy0, G::DH, G::FS, h, Y0 + r0, g5.k, dst, w, nv);
+            else pass_run<6, R5, true, false>(line, dy0, G::DH, G::FS, h, Y0 + r0, g5.k, dst, w, nv);
+        }
+    }
+}
+
+#define TW_LEVEL_ITER(TX, TY)                                                                                         \
+    __global__ void __launch_bounds__(LEVEL_ITER_MAX_THREADS) k_level_iter_##TX##x##TY(                              \
+        const float* __restrict__ i1, const float* __restrict__ i0, const float* __restrict__ gx,                    \
+        const float* __restrict__ gy, const float* __restrict__ a0, const float* __restrict__ a1,                    \
+        const float* __restrict__ a2, const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,      \
+        Taps g7, Taps g5, bool above_first, float* __restrict__ fu_out, float* __restrict__ fv_out,                 \
+        const float* __restrict__ mask_y) {                                                                          \
+        level_iter_body<TX, TY>(i1, i0, gx, gy, a0, a1, a2, fu, fv, w, h, g7, g5, above_first, fu_out, fv_out,     \
+                                mask_y);                                                                             \
+    }
+TW_LEVEL_ITER(32, 32)
+TW_LEVEL_ITER(64, 32)
+TW_LEVEL_ITER(64, 64)
+#undef TW_LEVEL_ITER
+
+size_t level_iter_smem(int tile) {
+    switch (tile) {
+        case LEVEL_TILE_64x32: return IterGeom<64, 32>::SMEM;
+        case LEVEL_TILE_64x64: return IterGeom<64, 64>::SMEM;
+        default: return IterGeom<32, 32>::SMEM;
     }
 }
 

@@ -118,6 +118,42 @@ size_t pyramid_floats(const Geo& g);
 // Threads per CTA of the tiled level kernels: a level of few tiles is latency bound (every CTA
 // walks its stages one after the other), so its CTAs get more threads and each thread fewer
 // elements per stage; a level with tiles enough to fill the GPU keeps 256.
+// One solver iteration (k_level_iter_*) with the tile shape and block size of the level's choice.
+// Algorithmic bytes per pixel: I1, the I0 gather, the gradient (2), the tensor (3) and the flow (2)
+// read, the flow (2) written.
+void level_iter(tw_ctx* ctx, LevelTune ic, const float* A, const float* B, const float* gx, const float* gy,
+                const float* a0, const float* a1, const float* a2, const float* fu, const float* fv, int w, int h, bool af,
+                float* nu, float* nv, const float* mask_y) {
+    double b = 48.0 * w * h;
+    size_t smem = level_iter_smem(ic.iter_tile);
+    if (ic.iter_tile == LEVEL_TILE_64x64) {
+        dim3 g((unsigned)((w + 63) / 64), (unsigned)((h + 63) / 64));
+        LAUNCHB(ctx, b, k_level_iter_64x64, g, ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7, ctx->g5, af,
+                nu, nv, mask_y);
+    } else if (ic.iter_tile == LEVEL_TILE_64x32) {
+        dim3 g((unsigned)((w + 63) / 64), (unsigned)((h + 31) / 32));
+        LAUNCHB(ctx, b, k_level_iter_64x32, g, ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7, ctx->g5, af,
+                nu, nv, mask_y);
+    } else {
+        LAUNCHB(ctx, b, k_level_iter_32x32, tiles(w, h), ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7,
+                ctx->g5, af, nu, nv, mask_y);
+    }
+}
+
+// The launch shapes at a level of w x h: the tuning table's entry when the autotuner measured this
+// size, else the defaults: 32 x 32 iteration tiles with 512 threads for levels of few tiles
+// (latency bound: fewer elements per thread per stage) and 256 otherwise; 256 threads per line of
+// block matching.
+LevelTune default_tune(int w, int h) {
+    long tiles_n = (long)((w + 31) / 32) * ((h + 31) / 32);
+    return LevelTune{LEVEL_TILE_32x32, tiles_n <= 296 ? 512 : 256, TB, TB};
+}
+
+LevelTune level_tune(tw_ctx* ctx, int w, int h) {
+    auto it = ctx->tune_table.find(((uint64_t)(uint32_t)w << 32) | (uint32_t)h);
+    return it != ctx->tune_table.end() ? it->second : default_tune(w, h);
+}
+
 static int level_threads(int w, int h) {
     long tiles_n = (long)((w + 31) / 32) * ((h + 31) / 32);
     return tiles_n <= 148 ? 1024 : tiles_n <= 296 ? 512 : 256;
@@ -271,10 +307,11 @@ void block_match(tw_ctx* ctx, const float* A, const float* B, const float* AT, c
                  float* uT, float* vT, int w, int h) {
     if (w < 3 || h < 3) return;  // callers refuse lines above BM_MAX_LINE before any launch
     double b = 24.0 * w * h;  // per launch (both sweeps): the field read and written (8 + 8), A and B read once (4 + 4)
-    LAUNCHB(ctx, b, k_bm_rows, h - 2, TB, bm_smem_bytes(w), A, B, fu, fv, w, h);
+    LevelTune t = level_tune(ctx, w, h);
+    LAUNCHB(ctx, b, k_bm_rows, h - 2, t.bm_rows_threads, bm_smem_bytes(w), A, B, fu, fv, w, h);
     dim3 tb(32, 8);
     LAUNCHB(ctx, 16.0 * w * h, k_transpose2, dim3((w + 31) / 32, (h + 31) / 32), tb, 0, fu, fv, uT, vT, w, h);
-    LAUNCHB(ctx, b, k_bm_cols, w - 2, TB, bm_smem_bytes(h), AT, BT, uT, vT, w, h);
+    LAUNCHB(ctx, b, k_bm_cols, w - 2, t.bm_cols_threads, bm_smem_bytes(h), AT, BT, uT, vT, w, h);
     LAUNCHB(ctx, 16.0 * w * h, k_transpose2, dim3((h + 31) / 32, (w + 31) / 32), tb, 0, uT, vT, fu, fv, h, w);
 }
 
@@ -329,12 +366,12 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
                             (long)w * h);
         };
         user();
+        LevelTune ic = level_tune(ctx, w, h);
         LAUNCHB(ctx, 24.0 * px, k_level_init, tiles(w, h), lt, level_init_smem(), A, w, h, ctx->g7, af, gx, gy, a0, a1, a2,
                 mask_x);
         for (int it = 0; it < 3; it++) {
             // I1, I0 (gather), grad, tensor, flow in; flow out
-            LAUNCHB(ctx, 4.0 * px * 12, k_level_iter, tiles(w, h), lt, level_iter_smem(), A, B, gx, gy, a0, a1, a2, fu, fv,
-                    w, h, ctx->g7, ctx->g5, af, nu, nv, mask_y);
+            level_iter(ctx, ic, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, af, nu, nv, mask_y);
             std::swap(fu, nu);
             std::swap(fv, nv);
             if (it == 1 && l == 0) {

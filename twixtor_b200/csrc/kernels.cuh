@@ -133,12 +133,22 @@ __global__ void k_level_init(const float* __restrict__ img, int w, int h, Taps g
                              float* __restrict__ a1o, float* __restrict__ a2o, const float* __restrict__ mask);
 __global__ void k_binarize(float* __restrict__ p, long n);
 size_t level_init_smem();
-__global__ void k_level_iter(const float* __restrict__ i1, const float* __restrict__ i0, const float* __restrict__ gx,
-                             const float* __restrict__ gy, const float* __restrict__ a0, const float* __restrict__ a1,
-                             const float* __restrict__ a2, const float* __restrict__ fu, const float* __restrict__ fv,
-                             int w, int h, Taps g7, Taps g5, bool above_first, float* __restrict__ fu_out,
-                             float* __restrict__ fv_out, const float* __restrict__ mask_y);
-size_t level_iter_smem();
+// One solver iteration (calc_b, blur7 of B, new_disp, blur5 of the flow) over TX x TY tiles: one
+// kernel per tile shape; the host picks the shape per level size (its tuning table).
+enum { LEVEL_TILE_32x32 = 0, LEVEL_TILE_64x32 = 1, LEVEL_TILE_64x64 = 2, LEVEL_TILE_COUNT = 3 };
+constexpr int LEVEL_ITER_MAX_THREADS = 512;
+#define TW_DECLARE_LEVEL_ITER(TX, TY)                                                                                 \
+    __global__ void k_level_iter_##TX##x##TY(                                                                       \
+        const float* __restrict__ i1, const float* __restrict__ i0, const float* __restrict__ gx,                    \
+        const float* __restrict__ gy, const float* __restrict__ a0, const float* __restrict__ a1,                    \
+        const float* __restrict__ a2, const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,      \
+        Taps g7, Taps g5, bool above_first, float* __restrict__ fu_out, float* __restrict__ fv_out,                 \
+        const float* __restrict__ mask_y);
+TW_DECLARE_LEVEL_ITER(32, 32)
+TW_DECLARE_LEVEL_ITER(64, 32)
+TW_DECLARE_LEVEL_ITER(64, 64)
+#undef TW_DECLARE_LEVEL_ITER
+size_t level_iter_smem(int tile);
 __global__ void k_apply_upsample(const float* __restrict__ su, const float* __restrict__ sv, int sw, int sh,
                                  const int* __restrict__ any, int l, int start, bool damp_now, float damp,
                                  float* __restrict__ du, float* __restrict__ dv, int dw, int dh);

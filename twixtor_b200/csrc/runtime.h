@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -60,6 +61,15 @@ using namespace tw;
 
 // Live per-kernel timing for the benchmark: CUDA events around every launch of one named kernel on
 // the context's stream, with the algorithmic bytes each launch moves.
+// The launch shapes at one level size (the autotuner's table entries): the solver iteration's tile
+// shape and block size, and the block size of each block matching kernel (one block per line).
+struct LevelTune {
+    int iter_tile;        // LEVEL_TILE_*
+    int iter_threads;     // a multiple of 32 up to LEVEL_ITER_MAX_THREADS
+    int bm_rows_threads;  // a multiple of 32 up to 1024
+    int bm_cols_threads;
+};
+
 struct KernelProfile {
     bool on = false;
     size_t pooled = 0;            // events of the context's pool in use by this session
@@ -95,6 +105,7 @@ struct tw_ctx {
     cudaStream_t cur = nullptr;  // the stream every launch goes to
     Lane lanes[MAX_LANES];
     int nlanes = 4;  // output frames in flight in the clip calls (tw_set_lanes)
+    std::map<uint64_t, LevelTune> tune_table;  // (w << 32 | h) -> the measured launch shapes of that level size
     bool serial = false;  // tw_set_lanes(ctx, 0): one lane whose work all runs on the context's stream
     cudaEvent_t ev_start = nullptr;
     // tw_retime_clip: a device cache of source frames, and the copy streams
@@ -237,6 +248,13 @@ int bad_fail(tw_ctx* ctx, int v);
 __global__ void k_set_flag(int* flags, int idx);  // flags[idx] = 1 (the injected device status)
 
 // host_solve.cu
+LevelTune level_tune(tw_ctx* ctx, int w, int h);
+LevelTune default_tune(int w, int h);
+void block_match(tw_ctx* ctx, const float* A, const float* B, const float* AT, const float* BT, float* fu, float* fv,
+                 float* uT, float* vT, int w, int h);
+void level_iter(tw_ctx* ctx, LevelTune ic, const float* A, const float* B, const float* gx, const float* gy,
+                const float* a0, const float* a1, const float* a2, const float* fu, const float* fv, int w, int h, bool af,
+                float* nu, float* nv, const float* mask_y);
 size_t pyramid_floats(const Geo& g);
 int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, const tw_flow_settings& s, const Geo& g,
                       float* out, float* out_t, DevBuf* scratch);

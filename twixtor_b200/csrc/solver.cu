@@ -383,10 +383,12 @@ __global__ void k_fill(float* __restrict__ p, long n, float v) {
 //   4. v'[x] = v[start of x's run].
 // Each cost evaluation is Block::cost bit for bit, so the result equals the sequential sweep.
 
-// flow.rs:474-523 (Block::cost). B(X, Y) is read at B[X * xs + Y * ys]: (1, w) for a row-major
-// plane, (h, 1) for its transpose; the arithmetic does not depend on the layout.
-__device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int h, long xs, long ys, const float p[9],
-                                        float x2, float y2, float& out) {
+// flow.rs:474-523 (Block::cost). B(X, Y) is B[Y * w + X] for a row-major plane (COLS false) and
+// B[X * h + Y] for its transpose (COLS true); the arithmetic does not depend on the layout. Indices
+// are 32-bit (a level plane holds at most 6144 x 6144 elements).
+template <bool COLS>
+__device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int h, const float p[9], float x2, float y2,
+                                        float& out) {
     float wm2 = (float)(w - 2), hm2 = (float)(h - 2);
     if (x2 > wm2 || y2 > hm2) return false;
     int ix, iy;
@@ -400,12 +402,20 @@ __device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int 
     float w10 = fx - w11;
     float w01 = fy - w11;
     float w00 = ((1.0f - fx) - fy) + w11;
-    const float* base = B + (long)(iy - 1) * ys + (long)(ix - 1) * xs;
     float t[4][4];
+    if (!COLS) {
+        const float* base = B + (iy - 1) * w + (ix - 1);
 #pragma unroll
-    for (int r = 0; r < 4; r++)
+        for (int r = 0; r < 4; r++)
 #pragma unroll
-        for (int c = 0; c < 4; c++) t[r][c] = __ldg(base + (long)r * ys + (long)c * xs);
+            for (int c = 0; c < 4; c++) t[r][c] = __ldg(base + r * w + c);
+    } else {
+        const float* base = B + (ix - 1) * h + (iy - 1);
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) t[r][c] = __ldg(base + c * h + r);
+    }
     float sq[9];
 #pragma unroll
     for (int b = 0; b < 3; b++) {
@@ -424,13 +434,22 @@ __device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int 
 }
 
 // Shared memory of one line of length len: u, v, c0 (floats), the three rows of A along the line
-// (floats), next / jump / on (ints), plus one int per warp for the block scan.
+// (floats), next / jump / on (ints), plus 64 ints for the block scan and the queue counter.
 size_t bm_smem_bytes(int len) { return (size_t)len * 4 * (3 + 3 + 3) + 64 * 4; }
 
-constexpr int BM_WINDOW = 4;  // accept tests a candidate run start evaluates at once (independent loads)
+constexpr int BM_WINDOW = 4;  // accept tests a long candidate run evaluates at once (independent loads)
 
-// accept(i, n) of the sweep at line position i (Block::step, flow.rs:529-546): the patch of A
-// around the pixel comes from shared memory (three rows of A along the line), c0 is the cost of
+// The 3x3 patch of A around line position i (flow.rs:454-469) from the three lines of A in shared
+// memory (rows y-1..y+1 for a row sweep, columns x-1..x+1 for a column sweep).
+template <bool COLS>
+__device__ __forceinline__ void bm_patch(const float* s_a, int len, int i, float p[9]) {
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) p[r * 3 + c] = COLS ? s_a[c * len + (i - 1 + r)] : s_a[r * len + (i - 1 + c)];
+}
+
+// accept(i, n) of the sweep at line position i (Block::step, flow.rs:529-546): c0 is the cost of
 // the current vector (NaN when the step cannot happen at i: no target or no cost).
 template <bool COLS>
 __device__ __forceinline__ bool bm_accept(const float* s_a, int len, const float* __restrict__ B, int w, int h,
@@ -438,14 +457,9 @@ __device__ __forceinline__ bool bm_accept(const float* s_a, int len, const float
     if (isnan(ci)) return false;  // None, or a NaN cost that nothing compares below
     int x = COLS ? fixed : i, y = COLS ? i : fixed;
     float p[9];
-    // s_a holds A at offsets -1, 0, +1 across the line (rows y-1..y+1 for a row sweep, columns
-    // x-1..x+1 for a column sweep), each a line of len values
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) p[r * 3 + c] = COLS ? s_a[c * len + (i - 1 + r)] : s_a[r * len + (i - 1 + c)];
+    bm_patch<COLS>(s_a, len, i, p);
     float c1;
-    if (!bm_cost(B, w, h, COLS ? (long)h : 1L, COLS ? 1L : (long)w, p, (float)x - nu, (float)y - nv, c1)) return false;
+    if (!bm_cost<COLS>(B, w, h, p, (float)x - nu, (float)y - nv, c1)) return false;
     return c1 < ci;
 }
 
@@ -453,16 +467,30 @@ __device__ __forceinline__ bool bm_accept(const float* s_a, int len, const float
 // s_a: the three lines of A across it). The line is the row y (COLS false: pixel (i, y)) or the
 // column x (COLS true: pixel (x, i)); len is its length. Forward sweeps run i = 1..len-2 with the
 // neighbour i - 1, reverse sweeps i = len-2..1 with the neighbour i + 1. In "sweep order" position
-// q (q = i forward, q = len-1-i reverse) both are the same forward recurrence. The in place update
-// is safe: step 4 reads only run starts, which keep their own vectors and are never written.
+// q (q = i forward, q = len-1-i reverse) both are the same forward recurrence
+// v'[q] = accept(q, v'[q-1]) ? v'[q-1] : v[q], so every v'[q] is the vector of its run's start and
+// a run started at j continues while accept(q, v[j]) holds:
+//   1. c0[i], the cost of the current vector, at every interior position (the reverse sweep keeps
+//      the forward sweep's value where that sweep left the vector as it was: chg[i] == 0);
+//   2. end[q] for every candidate start q: one accept test of the next position; the candidates
+//      whose run goes on (about a third at the finest level) are compacted into a queue;
+//   3. the queued candidates scan on, BM_WINDOW tests at a time, to the first refusal;
+//   4. the run starts 0, end[0], end[end[0]], ... marked by pointer jumping, the owner of each
+//      position by a block max-scan, then v[owner] into the line (the forward sweep records in
+//      chg which positions took another vector).
+// The in place update is safe: step 4 reads only run starts, which keep their own vectors.
 template <bool COLS>
 __device__ void bm_sweep(float* su, float* sv, float* c0, const float* s_a, int* jmp, int* jmp2, int* on, int* wscan,
-                         const float* __restrict__ B, int w, int h, int fixed, int len, bool reverse) {
+                         int* chg, const float* __restrict__ B, int w, int h, int fixed, int len, bool reverse) {
     const float w1 = (float)(w - 1), h1 = (float)(h - 1);
+    const int tid = threadIdx.x, nt = blockDim.x;
     auto line_of = [&](int q) -> int { return reverse ? len - 1 - q : q; };  // sweep position -> line index
-    for (int i = threadIdx.x; i < len; i += blockDim.x) on[i] = 0;
-    // 1. c0: the cost of the current vector at every interior position, NaN where no step can happen
-    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+    int* queue = jmp2;  // steps 2-3; jmp2 is free until the pointer jumping
+    int* qn = wscan + 32;
+    // 1. c0 (NaN where no step can happen); the reverse sweep computes it only where the forward
+    //    sweep changed the vector, those positions first compacted into jmp (free until step 2) so
+    //    that every lane of a warp evaluates one
+    auto c0_at = [&](int i) {
         float c = __int_as_float(0x7fc00000);
         if (i >= 1 && i <= len - 2) {
             int x = COLS ? fixed : i, y = COLS ? i : fixed;
@@ -470,25 +498,76 @@ __device__ void bm_sweep(float* su, float* sv, float* c0, const float* s_a, int*
             float ty = (float)y - sv[i];
             if (0.0f <= tx && tx <= w1 && 0.0f <= ty && ty <= h1) {
                 float p[9];
-#pragma unroll
-                for (int r = 0; r < 3; r++)
-#pragma unroll
-                    for (int cc = 0; cc < 3; cc++) p[r * 3 + cc] = COLS ? s_a[cc * len + (i - 1 + r)] : s_a[r * len + (i - 1 + cc)];
+                bm_patch<COLS>(s_a, len, i, p);
                 float cost;
-                if (bm_cost(B, w, h, COLS ? (long)h : 1L, COLS ? 1L : (long)w, p, tx, ty, cost)) c = cost;
+                if (bm_cost<COLS>(B, w, h, p, tx, ty, cost)) c = cost;
             }
         }
         c0[i] = c;
+    };
+    if (!reverse) {
+        for (int i = tid; i < len; i += nt) {
+            on[i] = 0;
+            c0_at(i);
+        }
+    } else {
+        int* list = jmp;
+        int* ln = wscan + 33;
+        if (tid == 0) *ln = 0;
+        __syncthreads();
+        for (int ib = 0; ib < len; ib += nt) {
+            int i = ib + tid;
+            bool want = false;
+            if (i < len) {
+                on[i] = 0;
+                want = chg[i] != 0;
+            }
+            unsigned m = __ballot_sync(0xffffffffu, want);
+            if (m) {
+                int lane = tid & 31, lead = __ffs(m) - 1;
+                int base = 0;
+                if (lane == lead) base = atomicAdd(ln, __popc(m));
+                base = __shfl_sync(0xffffffffu, base, lead);
+                if (want) list[base + __popc(m & ((1u << lane) - 1u))] = i;
+            }
+        }
+        __syncthreads();
+        const int n = *ln;
+        for (int k = tid; k < n; k += nt) c0_at(list[k]);
+    }
+    if (tid == 0) *qn = 0;
+    __syncthreads();
+    // 2. end[q] = q + 1 where the next position refuses v[q]; the others go to the queue
+    for (int qb = 0; qb < len; qb += nt) {
+        int q = qb + tid;
+        bool pend = false;
+        if (q < len) {
+            int e = len - 1;
+            if (q + 1 <= len - 2) {
+                int j = line_of(q), i1 = line_of(q + 1);
+                if (bm_accept<COLS>(s_a, len, B, w, h, fixed, i1, su[j], sv[j], c0[i1])) pend = true;
+                else e = q + 1;
+            }
+            if (!pend) jmp[q] = e;
+        }
+        unsigned m = __ballot_sync(0xffffffffu, pend);
+        if (m) {
+            int lane = tid & 31, lead = __ffs(m) - 1;
+            int base = 0;
+            if (lane == lead) base = atomicAdd(qn, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, lead);
+            if (pend) queue[base + __popc(m & ((1u << lane) - 1u))] = q;
+        }
     }
     __syncthreads();
-    // 2. next[q]: the sweep position where the run started at q ends (the first q' > q whose
-    //    accept of v[q] fails; len - 1 when the run reaches the end). BM_WINDOW tests at once;
-    //    longer runs continue one window at a time (bounded by the line).
-    for (int q = threadIdx.x; q < len; q += blockDim.x) {
+    // 3. the queued candidates: the first refusal from q + 2 on (len - 1 when the run reaches the end)
+    const int nq = *qn;
+    for (int k = tid; k < nq; k += nt) {
+        int q = queue[k];
         int j = line_of(q);
         float nu = su[j], nv = sv[j];
         int e = len - 1;
-        for (int q0 = q + 1; q0 <= len - 2; q0 += BM_WINDOW) {
+        for (int q0 = q + 2; q0 <= len - 2; q0 += BM_WINDOW) {
             bool acc[BM_WINDOW];
 #pragma unroll
             for (int d = 0; d < BM_WINDOW; d++) {
@@ -504,29 +583,27 @@ __device__ void bm_sweep(float* su, float* sv, float* c0, const float* s_a, int*
         jmp[q] = e;
     }
     __syncthreads();
-    // 3. the chain of run starts from sweep position 0, by pointer jumping: after round r every
+    // 4. the chain of run starts from sweep position 0, by pointer jumping: after round r every
     //    start within 2^(r+1) hops of position 0 is marked (jmp holds next^(2^r))
-    if (threadIdx.x == 0) on[0] = 1;
+    if (tid == 0) on[0] = 1;
     __syncthreads();
     for (int span = 1; span < 2 * len; span *= 2) {
-        for (int q = threadIdx.x; q < len; q += blockDim.x)
+        for (int q = tid; q < len; q += nt)
             if (on[q] && jmp[q] < len - 1) on[jmp[q]] = 1;
-        for (int q = threadIdx.x; q < len; q += blockDim.x) jmp2[q] = jmp[q] < len - 1 ? jmp[jmp[q]] : jmp[q];
+        for (int q = tid; q < len; q += nt) jmp2[q] = jmp[q] < len - 1 ? jmp[jmp[q]] : jmp[q];
         __syncthreads();
         int* t = jmp;
         jmp = jmp2;
         jmp2 = t;
     }
-    // 4. owner of each position: the last marked start at or before it (a block-wide max scan over
+    //    owner of each position: the last marked start at or before it (a block-wide max scan over
     //    contiguous chunks), then v[owner] into the line
-    int nt = blockDim.x;
     int chunk = (len + nt - 1) / nt;
-    int lo = threadIdx.x * chunk, hi = min(lo + chunk, len);
+    int lo = tid * chunk, hi = min(lo + chunk, len);
     int mark = -1;
     for (int q = lo; q < hi; q++)
         if (on[q]) mark = q;
-    // inclusive max scan of `mark` over the threads
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int lane = tid & 31, warp = tid >> 5;
     int v = mark;
 #pragma unroll
     for (int o = 1; o < 32; o *= 2) {
@@ -543,11 +620,13 @@ __device__ void bm_sweep(float* su, float* sv, float* c0, const float* s_a, int*
     for (int q = lo; q < hi; q++) {
         if (on[q]) cur = q;
         int i = line_of(q);
-        if (i >= 1 && i <= len - 2 && cur >= 0 && cur != q) {
+        bool moved = i >= 1 && i <= len - 2 && cur >= 0 && cur != q;
+        if (moved) {
             int o = line_of(cur);
             su[i] = su[o];
             sv[i] = sv[o];
         }
+        if (!reverse) chg[i] = moved ? 1 : 0;
     }
     __syncthreads();
 }
@@ -566,11 +645,11 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
     float* su = sm;
     float* sv = su + len;
     float* c0 = sv + len;
-    float* s_a = c0 + len;        // 3 * len
+    float* s_a = c0 + len;             // 3 * len
     int* jmp = (int*)(s_a + 3 * len);  // next^(2^r), ping-ponged with jmp2
     int* jmp2 = jmp + len;
     int* on = jmp2 + len;
-    int* wscan = on + len;        // one int per warp
+    int* wscan = on + len;  // one int per warp, then the queue counter
     // both layouts keep the line contiguous: row y of a row-major plane, column x of a transposed one
     auto gidx = [&](int i) -> long { return (long)fixed * len + i; };
     for (int i = threadIdx.x; i < len; i += blockDim.x) {
@@ -582,8 +661,10 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
             s_a[o * len + i] = __ldg(A + (long)(fixed - 1 + o) * len + i);
     }
     __syncthreads();
-    bm_sweep<COLS>(su, sv, c0, s_a, jmp, jmp2, on, wscan, B, w, h, fixed, len, false);
-    bm_sweep<COLS>(su, sv, c0, s_a, jmp, jmp2, on, wscan, B, w, h, fixed, len, true);
+    // chg (which positions the forward sweep replaced) lives in jmp2 between the two sweeps: the
+    // reverse sweep reads it in its step 1, before its step 2 reuses jmp2 as the queue
+    bm_sweep<COLS>(su, sv, c0, s_a, jmp, jmp2, on, wscan, jmp2, B, w, h, fixed, len, false);
+    bm_sweep<COLS>(su, sv, c0, s_a, jmp, jmp2, on, wscan, jmp2, B, w, h, fixed, len, true);
     for (int i = threadIdx.x + 1; i <= len - 2; i += blockDim.x) {
         long g = gidx(i);
         fu[g] = su[i];
