@@ -692,6 +692,26 @@ def roofline_pass(dev, stream, flush, run):
         if len(p) >= 6:
             kernels.append({"kernel": p[0], "launches": int(p[1]), "ms": float(p[2]), "us_per_launch": float(p[3]),
                             "share": float(p[4].rstrip("%")) / 100.0, "alg_gbs": float(p[5])})
+    # the tile shapes of one kernel (k_level_iter_32x32, _64x32, ...) count as that kernel
+    fam = {}
+    for k in kernels:
+        name = k["kernel"].rsplit("_", 1)[0] if k["kernel"].startswith("k_level_iter_") else k["kernel"]
+        f = fam.setdefault(name, {"kernel": name, "launches": 0, "ms": 0.0, "bytes": 0.0, "share": 0.0,
+                                  "shapes": []})
+        f["launches"] += k["launches"]
+        f["ms"] += k["ms"]
+        f["bytes"] += k["alg_gbs"] * 1e9 * k["ms"] * 1e-3
+        f["share"] += k["share"]
+        if name != k["kernel"]:
+            f["shapes"].append({x: k[x] for x in ("kernel", "launches", "us_per_launch", "alg_gbs")})
+    kernels = []
+    for f in sorted(fam.values(), key=lambda f: -f["ms"]):
+        row = {"kernel": f["kernel"], "launches": f["launches"], "ms": f["ms"],
+               "us_per_launch": 1e3 * f["ms"] / max(f["launches"], 1), "share": f["share"],
+               "alg_gbs": f["bytes"] / (f["ms"] * 1e-3) / 1e9 if f["ms"] > 0 else 0.0}
+        if f["shapes"]:
+            row["shapes"] = f["shapes"]
+        kernels.append(row)
     return kernels, e0.elapsed_time(e1)
 
 
@@ -716,7 +736,7 @@ def roofline_entry(kernels, serial_ms, launches_per_step, ms_per_step, peak, whi
             "serial_step_ms": serial_ms, "kernel_ms_per_step": top["ms"],
             "kernel_ms_fits_step": top["ms"] <= serial_ms,
             "timed_ms_per_step": ms_per_step, "timed_launches_per_step": launches_per_step,
-            "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} | 
+            "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()} |
                         {"frac": round(r["alg_gbs"] / peak, 4) if peak else None} for r in kernels[:8]]}
 
 
