@@ -6,6 +6,7 @@
 // (flow/conv.rs for the separable passes, flow.rs for the solver steps), so the results are bit
 // identical to the unfused kernels and to the reference CPU path.
 #include "kernels.cuh"
+#include "level.cuh"
 #include "luma.cuh"
 
 namespace tw {
@@ -13,54 +14,6 @@ namespace tw {
 constexpr int FT_X = 32;  // tile width (outputs)
 constexpr int FT_Y = 32;  // tile height
 constexpr int FT_THREADS = 1024;  // the launch bound; each launch picks 256 to 1024 threads
-
-// ---- separable pass elements ---------------------------------------------------------------------
-
-// flow/conv.rs:101-137 on a line held in shared memory: element t of the line (global index, inside
-// [0, len)) lives at line[(t - origin) * stride].
-template <int N, bool MULTI, bool LEFT_FIRST>
-__device__ __forceinline__ float border_sm(const float* line, int origin, int stride, int len, int i, const float* k) {
-    float centre = line[(i - origin) * stride];
-    float num = k[0] * centre;
-    float den = k[0];
-#pragma unroll
-    for (int j = N - 1; j >= 1; j--) {
-        float kj = k[j];
-#pragma unroll
-        for (int side = 0; side < 2; side++) {
-            bool right = (side == 0) != LEFT_FIRST;
-            int t = right ? i + j : i - j;
-            bool inside = t >= 0 && t < len;
-            float xv, wv;
-            if (!MULTI) {
-                xv = inside ? line[(t - origin) * stride] : 0.0f;
-                wv = inside ? kj : 0.0f;
-            } else {
-                float v = inside ? line[(t - origin) * stride] : -1.0f;
-                float mask = (v != -1.0f) ? 1.0f : 0.0f;
-                xv = v;
-                wv = mask * kj;
-            }
-            den = den + wv;
-            num = num + xv * wv;
-        }
-    }
-    return num / den;
-}
-
-// One output of a pass along a line (conv.rs:141-190 horizontally, :268-301 vertically): the
-// interior chain for elements whose taps all lie inside [n, len - n), the border rule otherwise.
-template <int N, bool MULTI, bool LEFT_FIRST>
-__device__ __forceinline__ float pass_elem(const float* line, int origin, int stride, int len, int i, const float* k) {
-    if (len >= 2 * N && i >= N && i < len - N) {
-        const float* c = line + (i - origin) * stride;
-        float s = c[0] * k[0];
-#pragma unroll
-        for (int j = N - 1; j >= 1; j--) s = s + (c[j * stride] + c[-j * stride]) * k[j];
-        return s;
-    }
-    return border_sm<N, MULTI, LEFT_FIRST>(line, origin, stride, len, i, k);
-}
 
 // A separable pass over a shared-memory region, both directions:
 //   src: RH x RW region whose (0,0) is global (gx0, gy0); dst: OH x OW region at global (ox0, oy0).
@@ -449,14 +402,6 @@ size_t level_iter_smem(int tile) {
 
 // ---- the end of a level (flow.rs:1292-1303): range reset, damping, then the upsample ---------------
 
-// any[k] (k = level) is set when some pixel of level k is in range after its refinement.
-// check at level l = no level processed before (start .. l+1) had a pixel in range.
-__device__ __forceinline__ bool zero_at_level(const int* any, int l, int start) {
-    bool check = true;
-    for (int k = start; k > l; k--) check = check && any[k] == 0;
-    return check && any[l] == 0;
-}
-
 // The coarse field (with the reset and damping of its level applied on the fly) upsampled to the
 // next finer level (flow.rs:376-391, bilinear2 of sample.rs:69-86). Applying the elementwise reset
 // and damping to the four gathered samples is the same as applying them to the whole field first.
@@ -466,35 +411,11 @@ __global__ void k_apply_upsample(const float* __restrict__ su, const float* __re
     int x = blockIdx.x * blockDim.x + threadIdx.x;
     int y = blockIdx.y;
     if (x >= dw || y >= dh) return;
-    bool zero = zero_at_level(any, l, start);
-    float sx = ((float)dw - 1.0f) / (float)(sw - 1);
-    float sy = ((float)dh - 1.0f) / (float)(sh - 1);
-    float rx = (float)(1.0 / (double)sx);
-    float ry = (float)(1.0 / (double)sy);
-    int ix, iy;
-    float fx, fy;
-    cell((float)x * rx, sw, ix, fx);
-    cell((float)y * ry, sh, iy, fy);
-    long i = (long)iy * sw + ix;
-    const float* planes[2] = {su, sv};
-    float r[2];
-#pragma unroll
-    for (int c = 0; c < 2; c++) {
-        const float* p = planes[c];
-        float q[4] = {p[i], p[i + 1], p[i + sw], p[i + sw + 1]};
-#pragma unroll
-        for (int m = 0; m < 4; m++) {
-            float v = zero ? 0.0f : q[m];
-            if (damp_now) v = damp * v;
-            q[m] = v;
-        }
-        float top = (q[1] - q[0]) * fx + q[0];
-        float bot = (q[3] - q[2]) * fx + q[2];
-        r[c] = (bot - top) * fy + top;
-    }
+    float u, v;
+    upsample_at(su, sv, sw, sh, zero_at_level(any, l, start), damp_now, damp, x, y, dw, dh, &u, &v);
     long o = (long)y * dw + x;
-    du[o] = r[0] * sx;
-    dv[o] = r[1] * sy;
+    du[o] = u;
+    dv[o] = v;
 }
 
 // The finest level: reset and damping, then the final negation (flow.rs:1305) into the

@@ -173,6 +173,8 @@ int tw_open(int device, tw_ctx** out) {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_level_iter_64x64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)level_iter_smem(LEVEL_TILE_64x64));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_solve_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem_bytes());
     if (e != cudaSuccess) { tw_close(ctx); return TW_ERR_CUDA; }
     if (ctx->ensure(ctx->flags, FLAGS_BYTES, "flags") != TW_OK) { tw_close(ctx); return TW_ERR_CUDA; }
     k_selfcheck<<<1, 1, 0, ctx->stream>>>(ctx->flags.as<int>());

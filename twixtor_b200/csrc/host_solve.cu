@@ -349,7 +349,43 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
     CHECK(ctx->cuda(cudaMemsetAsync(any, 0, 32 * sizeof(int), ctx->cur), "range flags"));
     bool af = s.taps_above_first != 0;
     bool damp_any = std::fabs((double)damp - 1.0) >= 1e-6;
-    for (int l = start; l >= 0; l--) {
+    // The coarse levels whose planes fit one block's shared memory run in one launch (coarse.cu),
+    // for the plain solve; the masked and the tracked solves keep the kernel by kernel path.
+    int first = start;
+    if (!mx && !my && !udu) {
+        int last = -1;
+        for (int l = start; l >= 1; l--) {
+            int w = g.sizes[l][0], h = g.sizes[l][1];
+            if (w * h > COARSE_MAX_PIXELS || w > COARSE_MAX_LINE || h > COARSE_MAX_LINE) break;
+            last = l;
+        }
+        if (last >= 1) {
+            CoarseJob J{};
+            J.x = x;
+            J.y = y;
+            for (int i = 0; i < g.levels; i++) {
+                J.sizes[i][0] = g.sizes[i][0];
+                J.sizes[i][1] = g.sizes[i][1];
+                J.offs[i] = (int)offs[i];
+            }
+            J.start = start;
+            J.last = last;
+            J.damp_any = damp_any;
+            J.damp = damp;
+            J.refine = !s.skip_refine;
+            J.af = af;
+            J.g7 = ctx->g7;
+            J.g5 = ctx->g5;
+            J.any = any;
+            J.fu_out = fu;
+            J.fv_out = fv;
+            double px = 0.0;
+            for (int l = start; l >= last; l--) px += (double)g.sizes[l][0] * g.sizes[l][1];
+            LAUNCHB(ctx, 8.0 * px, k_solve_coarse, 1, COARSE_THREADS, coarse_smem_bytes(), J);
+            first = last - 1;
+        }
+    }
+    for (int l = first; l >= 0; l--) {
         int w = g.sizes[l][0], h = g.sizes[l][1];
         const float* A = x + offs[l];
         const float* B = y + offs[l];

@@ -149,6 +149,30 @@ TW_DECLARE_LEVEL_ITER(64, 32)
 TW_DECLARE_LEVEL_ITER(64, 64)
 #undef TW_DECLARE_LEVEL_ITER
 size_t level_iter_smem(int tile);
+
+// The persistent coarse-level solve (coarse.cu): one block walks the levels start .. last of a solve
+// whose planes fit its shared memory (at most COARSE_MAX_PIXELS pixels and COARSE_MAX_LINE per side;
+// last >= 1), and writes the upsampled flow of level last - 1 (planar) for the tiled kernels.
+constexpr int COARSE_THREADS = 1024;
+constexpr int COARSE_MAX_PIXELS = 2048;
+constexpr int COARSE_MAX_LINE = 256;
+struct CoarseJob {
+    const float* x;  // the band pyramids of X and Y, levels concatenated finest first
+    const float* y;
+    int sizes[32][2];
+    int offs[32];  // the first element of each level
+    int start, last;
+    bool damp_any;  // the start level's damping differs from 1
+    float damp;
+    bool refine;  // block matching (not skip_refine)
+    bool af;      // the vertical tap above first
+    Taps g7, g5;
+    int* any;  // the per level range flags (32 ints, zeroed before)
+    float* fu_out;
+    float* fv_out;
+};
+__global__ void k_solve_coarse(CoarseJob job);
+size_t coarse_smem_bytes();
 __global__ void k_apply_upsample(const float* __restrict__ su, const float* __restrict__ sv, int sw, int sh,
                                  const int* __restrict__ any, int l, int start, bool damp_now, float damp,
                                  float* __restrict__ du, float* __restrict__ dv, int dw, int dh);

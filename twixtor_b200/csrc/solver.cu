@@ -1,6 +1,7 @@
 // Pyramid filters and the optical flow solver, strict mode. Each kernel cites the reference
 // function (plugins/retime-engine/src/...) whose per-element arithmetic it repeats.
 #include "kernels.cuh"
+#include "level.cuh"
 
 namespace tw {
 
@@ -382,56 +383,6 @@ __global__ void k_fill(float* __restrict__ p, long n, float v) {
 //   3. the run starts: 0, end[0], end[end[0]], ... (a chain walked in shared memory);
 //   4. v'[x] = v[start of x's run].
 // Each cost evaluation is Block::cost bit for bit, so the result equals the sequential sweep.
-
-// flow.rs:474-523 (Block::cost). B(X, Y) is B[Y * w + X] for a row-major plane (COLS false) and
-// B[X * h + Y] for its transpose (COLS true); the arithmetic does not depend on the layout. Indices
-// are 32-bit (a level plane holds at most 6144 x 6144 elements).
-template <bool COLS>
-__device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int h, const float p[9], float x2, float y2,
-                                        float& out) {
-    float wm2 = (float)(w - 2), hm2 = (float)(h - 2);
-    if (x2 > wm2 || y2 > hm2) return false;
-    int ix, iy;
-    float fx, fy;
-    if (x2 == wm2) { ix = cvtt32(wm2 - 1.0f); fx = 1.0f; }
-    else { ix = cvtt32(x2); fx = x2 - (float)ix; }
-    if (y2 == hm2) { iy = cvtt32(hm2 - 1.0f); fy = 1.0f; }
-    else { iy = cvtt32(y2); fy = y2 - (float)iy; }
-    if (ix < 1 || iy < 1) return false;
-    float w11 = fy * fx;
-    float w10 = fx - w11;
-    float w01 = fy - w11;
-    float w00 = ((1.0f - fx) - fy) + w11;
-    float t[4][4];
-    if (!COLS) {
-        const float* base = B + (iy - 1) * w + (ix - 1);
-#pragma unroll
-        for (int r = 0; r < 4; r++)
-#pragma unroll
-            for (int c = 0; c < 4; c++) t[r][c] = __ldg(base + r * w + c);
-    } else {
-        const float* base = B + (ix - 1) * h + (iy - 1);
-#pragma unroll
-        for (int c = 0; c < 4; c++)
-#pragma unroll
-            for (int r = 0; r < 4; r++) t[r][c] = __ldg(base + c * h + r);
-    }
-    float sq[9];
-#pragma unroll
-    for (int b = 0; b < 3; b++) {
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            float q = ((w00 * t[b][a] + w10 * t[b][a + 1]) + w01 * t[b + 1][a]) + w11 * t[b + 1][a + 1];
-            float d = p[b * 3 + a] - q;
-            sq[b * 3 + a] = d * d;
-        }
-    }
-    float s = sq[0] + sq[1];
-#pragma unroll
-    for (int k = 2; k < 8; k++) s = s + sq[k];
-    out = sq[8] + s;
-    return true;
-}
 
 // Shared memory of one line of length len: u, v, c0 (floats), the three rows of A along the line
 // (floats), next / jump / on (ints), plus 64 ints for the block scan and the queue counter.
