@@ -10,11 +10,12 @@
 // writes the flow of the first level the tiled kernels take over. Every element follows the same
 // rules as those kernels (level.cuh), so the flow is bit identical. No block waits on another.
 //
-// Block matching here gives each line to one warp: the sweep's recurrence
-// v'[q] = accept(q, v'[q-1]) ? v'[q-1] : v[q] is walked run by run. S[q] = accept(q, v[q-1]) (the
-// test when q-1 kept its own vector) is evaluated for every position up front; a stretch of
-// positions that start their own runs is skipped with one ballot over S, and a run that goes on
-// tests its vector at the next 32 positions at once (one lane each), the first refusal ending it.
+// Block matching here gives each line to a group of 8 lanes (4 lines per warp, 128 in flight): the
+// sweep's recurrence v'[q] = accept(q, v'[q-1]) ? v'[q-1] : v[q] is walked run by run.
+// S[q] = accept(q, v[q-1]) (the test when q-1 kept its own vector) is evaluated for every position
+// up front; a stretch of positions that start their own runs is skipped with ballots over S, and a
+// run that goes on tests its vector at the next 8 positions at once (one lane each), the first
+// refusal ending it (most runs end within a few positions).
 #include "kernels.cuh"
 #include "level.cuh"
 
@@ -23,7 +24,8 @@ namespace tw {
 namespace {
 
 constexpr int NT = COARSE_THREADS;
-constexpr int NW = NT / 32;
+constexpr int GL = 8;        // lanes per line of block matching
+constexpr int NG = NT / GL;  // lines in flight
 
 // sample.rs:47-64 on a plane in shared memory (bilinear1 reads global memory through __ldg)
 __device__ __forceinline__ float bilinear_s(const float* img, int w, int h, float x, float y) {
@@ -68,12 +70,12 @@ __device__ __forceinline__ bool accept_at(const float* A, const float* B, int w,
     return c1 < c0;
 }
 
-// One sweep of one line by one warp, in place on the field (fu, fv row-major w x h): the row y
-// (COLS false) or the column x; reverse: from the far end. c0w / sw: the warp's scratch.
+// One sweep of one line by one group of GL lanes (the group's lanes call it together; gmask names
+// them), in place on the field (fu, fv row-major w x h): the row y (COLS false) or the column x;
+// reverse: from the far end. c0w / sw: the group's scratch.
 template <bool COLS>
 __device__ void sweep_line(const float* A, const float* B, float* fu, float* fv, int w, int h, int fixed, bool reverse,
-                           float* c0w, unsigned char* sw) {
-    const int lane = threadIdx.x & 31;
+                           float* c0w, unsigned char* sw, int gl, unsigned gmask, int gshift) {
     const int len = COLS ? h : w;
     const float w1 = (float)(w - 1), h1 = (float)(h - 1);
     auto line_of = [&](int q) { return reverse ? len - 1 - q : q; };
@@ -82,8 +84,9 @@ __device__ void sweep_line(const float* A, const float* B, float* fu, float* fv,
         *x = COLS ? fixed : i;
         *y = COLS ? i : fixed;
     };
+    auto group_ballot = [&](bool p) { return (__ballot_sync(gmask, p) >> gshift) & ((1u << GL) - 1u); };
     // c0 of every interior position, then S
-    for (int q = 1 + lane; q <= len - 2; q += 32) {
+    for (int q = 1 + gl; q <= len - 2; q += GL) {
         int i = line_of(q), e = elem(i), x, y;
         xy(i, &x, &y);
         float c = __int_as_float(0x7fc00000);
@@ -100,31 +103,31 @@ __device__ void sweep_line(const float* A, const float* B, float* fu, float* fv,
         }
         c0w[q] = c;
     }
-    __syncwarp();
-    for (int q = 1 + lane; q <= len - 2; q += 32) {
+    __syncwarp(gmask);
+    for (int q = 1 + gl; q <= len - 2; q += GL) {
         int i = line_of(q), x, y;
         xy(i, &x, &y);
         int ep = elem(line_of(q - 1));
         sw[q] = accept_at(A, B, w, h, x, y, fu[ep], fv[ep], c0w[q]) ? 1 : 0;
     }
-    __syncwarp();
-    float ou = 0.0f, ov = 0.0f;  // the vector of the run in progress (warp uniform)
+    __syncwarp(gmask);
+    float ou = 0.0f, ov = 0.0f;  // the vector of the run in progress (uniform over the group)
     bool own = true;             // position q - 1 kept its own vector
     int q = 1;
     while (q <= len - 2) {
         if (own) {
             // the first r >= q that takes the vector of r - 1: positions q .. r - 1 start runs
             int r = -1;
-            for (int qb = q; qb <= len - 2 && r < 0; qb += 32) {
-                int qq = qb + lane;
-                unsigned m = __ballot_sync(0xffffffffu, qq <= len - 2 && sw[qq]);
+            for (int qb = q; qb <= len - 2 && r < 0; qb += GL) {
+                int qq = qb + gl;
+                unsigned m = group_ballot(qq <= len - 2 && sw[qq]);
                 if (m) r = qb + __ffs(m) - 1;
             }
             if (r < 0) break;
             int ep = elem(line_of(r - 1));
             ou = fu[ep];
             ov = fv[ep];
-            if (lane == 0) {
+            if (gl == 0) {
                 int e = elem(line_of(r));
                 fu[e] = ou;
                 fv[e] = ov;
@@ -133,7 +136,7 @@ __device__ void sweep_line(const float* A, const float* B, float* fu, float* fv,
             own = false;
         } else {
             // the run of (ou, ov) goes on while the next positions accept it
-            int qq = q + lane;
+            int qq = q + gl;
             bool valid = qq <= len - 2;
             bool acc = false;
             if (valid) {
@@ -141,11 +144,11 @@ __device__ void sweep_line(const float* A, const float* B, float* fu, float* fv,
                 xy(line_of(qq), &x, &y);
                 acc = accept_at(A, B, w, h, x, y, ou, ov, c0w[qq]);
             }
-            unsigned va = __ballot_sync(0xffffffffu, valid);
-            unsigned am = __ballot_sync(0xffffffffu, acc);
+            unsigned va = group_ballot(valid);
+            unsigned am = group_ballot(acc);
             unsigned fails = va & ~am;
             int f = fails ? __ffs(fails) - 1 : __popc(va);
-            if (valid && lane < f) {
+            if (valid && gl < f) {
                 int e = elem(line_of(qq));
                 fu[e] = ou;
                 fv[e] = ov;
@@ -158,7 +161,7 @@ __device__ void sweep_line(const float* A, const float* B, float* fu, float* fv,
             }
         }
     }
-    __syncwarp();
+    __syncwarp(gmask);
 }
 
 }  // namespace
@@ -171,12 +174,14 @@ __global__ void __launch_bounds__(COARSE_THREADS) k_solve_coarse(CoarseJob J) {
     float *gx = B + M, *gy = gx + M, *a0 = gy + M, *a1 = a0 + M, *a2 = a1 + M;
     float *fu = a2 + M, *fv = fu + M, *nu = fv + M, *nv = nu + M;
     float *t0 = nv + M, *t1 = t0 + M, *t2 = t1 + M, *t3 = t2 + M;
-    float* c0_all = t3 + M;                                   // NW x COARSE_MAX_LINE
-    unsigned char* s_all = (unsigned char*)(c0_all + NW * COARSE_MAX_LINE);
+    float* c0_all = t3 + M;                                   // NG x COARSE_MAX_LINE
+    unsigned char* s_all = (unsigned char*)(c0_all + NG * COARSE_MAX_LINE);
     __shared__ int s_any[32];
-    const int tid = threadIdx.x, warp = tid >> 5;
-    float* c0w = c0_all + warp * COARSE_MAX_LINE;
-    unsigned char* sw = s_all + warp * COARSE_MAX_LINE;
+    const int tid = threadIdx.x;
+    const int grp = tid / GL, gl = tid % GL, gshift = (tid & 31) & ~(GL - 1);
+    const unsigned gmask = ((1u << GL) - 1u) << gshift;
+    float* c0w = c0_all + grp * COARSE_MAX_LINE;
+    unsigned char* sw = s_all + grp * COARSE_MAX_LINE;
     if (tid < 32) s_any[tid] = 0;
     for (int l = J.start; l >= J.last; l--) {
         const int w = J.sizes[l][0], h = J.sizes[l][1], n = w * h;
@@ -257,14 +262,14 @@ __global__ void __launch_bounds__(COARSE_THREADS) k_solve_coarse(CoarseJob J) {
         }
         // block matching (flow.rs:551-622): the row sweeps, then the column sweeps
         if (J.refine && w >= 3 && h >= 3) {
-            for (int y = 1 + warp; y <= h - 2; y += NW) {
-                sweep_line<false>(A, B, fu, fv, w, h, y, false, c0w, sw);
-                sweep_line<false>(A, B, fu, fv, w, h, y, true, c0w, sw);
+            for (int y = 1 + grp; y <= h - 2; y += NG) {
+                sweep_line<false>(A, B, fu, fv, w, h, y, false, c0w, sw, gl, gmask, gshift);
+                sweep_line<false>(A, B, fu, fv, w, h, y, true, c0w, sw, gl, gmask, gshift);
             }
             __syncthreads();
-            for (int x = 1 + warp; x <= w - 2; x += NW) {
-                sweep_line<true>(A, B, fu, fv, w, h, x, false, c0w, sw);
-                sweep_line<true>(A, B, fu, fv, w, h, x, true, c0w, sw);
+            for (int x = 1 + grp; x <= w - 2; x += NG) {
+                sweep_line<true>(A, B, fu, fv, w, h, x, false, c0w, sw, gl, gmask, gshift);
+                sweep_line<true>(A, B, fu, fv, w, h, x, true, c0w, sw, gl, gmask, gshift);
             }
             __syncthreads();
         }
@@ -304,7 +309,7 @@ __global__ void __launch_bounds__(COARSE_THREADS) k_solve_coarse(CoarseJob J) {
 }
 
 size_t coarse_smem_bytes() {
-    return sizeof(float) * (15 * (size_t)COARSE_MAX_PIXELS + (size_t)NW * COARSE_MAX_LINE) + (size_t)NW * COARSE_MAX_LINE;
+    return sizeof(float) * (15 * (size_t)COARSE_MAX_PIXELS + (size_t)NG * COARSE_MAX_LINE) + (size_t)NG * COARSE_MAX_LINE;
 }
 
 }  // namespace tw

@@ -155,7 +155,7 @@ size_t level_iter_smem(int tile);
 // last >= 1), and writes the upsampled flow of level last - 1 (planar) for the tiled kernels.
 constexpr int COARSE_THREADS = 1024;
 constexpr int COARSE_MAX_PIXELS = 2048;
-constexpr int COARSE_MAX_LINE = 256;
+constexpr int COARSE_MAX_LINE = 128;
 struct CoarseJob {
     const float* x;  // the band pyramids of X and Y, levels concatenated finest first
     const float* y;
