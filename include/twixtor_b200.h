@@ -91,6 +91,10 @@ typedef struct tw_flow_settings {
     int32_t skip_refine;
     int32_t wrap;             /* 360 solve: TW_ERR_UNSUPPORTED */
     int32_t taps_above_first;
+    int32_t fast_mode;        /* 0: strict (bit identical to the CPU path); 1: the solver's kernels (pyramid,
+                                 iterations, block matching) as built with FMA contraction, approximate division
+                                 and flushed denormals: not bit identical; the library's tests state its flow
+                                 error in pixels and frame PSNR against a double precision CPU restatement */
 } tw_flow_settings;
 
 /* timeline::Selection (timeline.rs:391-414). */

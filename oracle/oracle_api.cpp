@@ -212,12 +212,12 @@ void or_convolve(float* data, int w, int h, int c, const float* k, int n, int ab
 }
 void or_calc_grad(const float* img, int w, int h, float* g) {
     auto v = calc_grad(img, w, h);
-    std::memcpy(g, v.data(), v.size() * 4);
+    std::memcpy(g, v.data(), v.size() * sizeof(float));
 }
 void or_new_disp(float* flow, const float* a, const float* b, long npx) { new_disp(flow, a, b, (size_t)npx); }
 void or_upsample_flow(const float* src, int sw, int sh, int dw, int dh, float* dst) {
     auto v = upsample_flow(src, sw, sh, dw, dh);
-    std::memcpy(dst, v.data(), v.size() * 4);
+    std::memcpy(dst, v.data(), v.size() * sizeof(float));
 }
 void or_block_match(const float* a, const float* b, float* flow, int w, int h) { block_match(a, b, flow, w, h); }
 int or_all_out_of_range(const float* flow, int w, int h) { return all_flow_out_of_range(flow, w, h) ? 1 : 0; }
@@ -253,7 +253,7 @@ int or_build_pyramid(const void* engine, int w, int h, int fmt, int quality, int
     std::string e;
     if (!build_pyramid(img, s, &p, &e)) return fail(-1, e);
     size_t off = 0;
-    for (auto& l : p.levels) { std::memcpy(levels_out + off, l.d.data(), l.d.size() * 4); off += l.d.size(); }
+    for (auto& l : p.levels) { std::memcpy(levels_out + off, l.d.data(), l.d.size() * sizeof(float)); off += l.d.size(); }
     return p.geo.levels;
 }
 
@@ -272,8 +272,30 @@ int or_solve_pair(const void* a_eng, const void* b_eng, int w, int h, int fmt, i
     FlowField fab, fba;
     std::string e;
     if (!solve_pair(a, b, s, &fab, &fba, &e)) return fail(-1, e);
-    std::memcpy(f_ab, fab.d.data(), fab.d.size() * 4);
-    std::memcpy(f_ba, fba.d.data(), fba.d.size() * 4);
+    std::memcpy(f_ab, fab.d.data(), fab.d.size() * sizeof(float));
+    std::memcpy(f_ba, fba.d.data(), fba.d.size() * sizeof(float));
+    return 0;
+}
+
+// flow::solve (flow.rs:1328-1332) X -> Y with the image prep (0 none, 2 Contrast/Edge Enhance,
+// 3 Delinearize, as FlowSettings reads it): `out` receives the working size field.
+int or_solve(const void* x_eng, const void* y_eng, int w, int h, int fmt, int quality, int hiq, float sensitivity,
+             int skip_refine, int above_first, int prep, float* out) {
+    Image x(w, h, (Fmt)fmt), y(w, h, (Fmt)fmt);
+    std::memcpy(x.data(), x_eng, x.bytes());
+    std::memcpy(y.data(), y_eng, y.bytes());
+    FlowSettings s;
+    s.quality = quality;
+    s.hiq = hiq != 0;
+    s.sensitivity = sensitivity;
+    s.skip_refine = skip_refine != 0;
+    s.taps_above_first = above_first != 0;
+    s.prep_contrast_edge = prep == 2;
+    s.prep_delinearize = prep == 3;
+    FlowField f;
+    std::string e;
+    if (!solve(x, y, s, &f, &e)) return fail(-1, e);
+    std::memcpy(out, f.d.data(), f.d.size() * sizeof(float));
     return 0;
 }
 
@@ -284,7 +306,7 @@ int or_inv_warp(void* out_eng, const void* src_eng, int w, int h, int fmt, const
     std::memcpy(src.data(), src_eng, src.bytes());
     std::memcpy(out.data(), out_eng, out.bytes());
     FlowField f(fw, fh);
-    std::memcpy(f.d.data(), flow, f.d.size() * 4);
+    std::memcpy(f.d.data(), flow, f.d.size() * sizeof(float));
     WarpOpts o;
     o.hold = hold != 0;
     Coverage c;
@@ -312,8 +334,8 @@ int or_compose_vectors(const void* a_eng, const void* b_eng, int w, int h, int f
     std::memcpy(a.data(), a_eng, a.bytes());
     std::memcpy(b.data(), b_eng, b.bytes());
     FlowField fab(fw, fh), fba(fw, fh);
-    if (f_ab) std::memcpy(fab.d.data(), f_ab, fab.d.size() * 4);
-    if (f_ba) std::memcpy(fba.d.data(), f_ba, fba.d.size() * 4);
+    if (f_ab) std::memcpy(fab.d.data(), f_ab, fab.d.size() * sizeof(float));
+    if (f_ba) std::memcpy(fba.d.data(), f_ba, fba.d.size() * sizeof(float));
     ComposeSettings cs;
     Selection sel;
     sel.wa = wa;
@@ -352,7 +374,7 @@ int or_forward_warp(void* out_eng, const void* src_eng, int w, int h, int fmt, c
     Image src(w, h, (Fmt)fmt), out(w, h, (Fmt)fmt);
     std::memcpy(src.data(), src_eng, src.bytes());
     FlowField f(fw, fh);
-    std::memcpy(f.d.data(), flow, f.d.size() * 4);
+    std::memcpy(f.d.data(), flow, f.d.size() * sizeof(float));
     Coverage c;
     std::string e;
     int rc = forward_warp(out, src, f, amount, pyramid != 0, cov ? &c : nullptr, &e);
@@ -365,7 +387,7 @@ int or_forward_warp(void* out_eng, const void* src_eng, int w, int h, int fmt, c
 // forward/mesh.rs:63-91 and forward/pyramid.rs:20-36
 float or_fw_mip_level(int w, int h, const float* flow, int fw, int fh, float amount, int c, int r) {
     FlowField f(fw, fh);
-    std::memcpy(f.d.data(), flow, f.d.size() * 4);
+    std::memcpy(f.d.data(), flow, f.d.size() * sizeof(float));
     return fw_mip_level(w, h, f, amount, c, r);
 }
 int or_fw_level_count(int w, int h) { return fw_level_count(w, h); }
@@ -402,8 +424,8 @@ int or_compose_vectors2(const void* a_eng, const void* b_eng, int w, int h, int 
     std::memcpy(a.data(), a_eng, a.bytes());
     std::memcpy(b.data(), b_eng, b.bytes());
     FlowField fab(fw, fh), fba(fw, fh);
-    if (f_ab) std::memcpy(fab.d.data(), f_ab, fab.d.size() * 4);
-    if (f_ba) std::memcpy(fba.d.data(), f_ba, fba.d.size() * 4);
+    if (f_ab) std::memcpy(fab.d.data(), f_ab, fab.d.size() * sizeof(float));
+    if (f_ba) std::memcpy(fba.d.data(), f_ba, fba.d.size() * sizeof(float));
     ComposeSettings cs;
     cs.warp_mode = warp_mode;
     cs.video_360 = video_360 != 0;
@@ -425,7 +447,7 @@ int or_motion_blur(void* out_eng, const void* src_eng, int w, int h, int fmt, co
     Image src(w, h, (Fmt)fmt), out(w, h, (Fmt)fmt);
     std::memcpy(src.data(), src_eng, src.bytes());
     FlowField f(fw, fh);
-    std::memcpy(f.d.data(), flow, f.d.size() * 4);
+    std::memcpy(f.d.data(), flow, f.d.size() * sizeof(float));
     std::string e;
     int rc = motion_blur(out, src, f, amount, hiq != 0, shutter, &e);
     if (rc) return fail(rc, e);
@@ -447,8 +469,8 @@ int or_compose_vectors3(const void* a_eng, const void* b_eng, int w, int h, int 
     std::memcpy(a.data(), a_eng, a.bytes());
     std::memcpy(b.data(), b_eng, b.bytes());
     FlowField fab(fw, fh), fba(fw, fh);
-    if (f_ab) std::memcpy(fab.d.data(), f_ab, fab.d.size() * 4);
-    if (f_ba) std::memcpy(fba.d.data(), f_ba, fba.d.size() * 4);
+    if (f_ab) std::memcpy(fab.d.data(), f_ab, fab.d.size() * sizeof(float));
+    if (f_ba) std::memcpy(fba.d.data(), f_ba, fba.d.size() * sizeof(float));
     ComposeSettings cs;
     cs.warp_mode = warp_mode;
     cs.video_360 = video_360 != 0;
@@ -771,7 +793,7 @@ int or_mask_pyramid(const float* matte, int w, int h, int quality, int hiq, int 
     for (size_t i = 0; i < lv.size() && (int)i < cap_levels; i++) {
         sizes[2 * i] = lv[i].w;
         sizes[2 * i + 1] = lv[i].h;
-        std::memcpy(out + off, lv[i].d.data(), lv[i].d.size() * 4);
+        std::memcpy(out + off, lv[i].d.data(), lv[i].d.size() * sizeof(float));
         off += lv[i].d.size();
     }
     return (int)lv.size();
@@ -782,7 +804,7 @@ void or_mask_gradient(float* grad, const float* mask, int w, int h) { mask_gradi
 void or_calc_b_masked(const float* i1, const float* i0, const float* grad, const float* flow, int w, int h,
                       const float* mask_y, float* out) {
     std::vector<float> b = calc_b_masked(i1, i0, grad, flow, w, h, mask_y);
-    std::memcpy(out, b.data(), b.size() * 4);
+    std::memcpy(out, b.data(), b.size() * sizeof(float));
 }
 
 void or_block_match_gated(const float* a, const float* b, float* flow, int w, int h, const float* gate) {
@@ -808,7 +830,7 @@ int or_solve_masked(const void* x_eng, const void* y_eng, int w, int h, int fmt,
     bool masks = matte_x && matte_y;
     if (masks && (!mask_pyramid(matte_x, w, h, s, &mx, &e) || !mask_pyramid(matte_y, w, h, s, &my, &e))) return fail(1, e);
     FlowField f = solve_pyramids_masked(px, py, s, masks ? &mx : nullptr, masks ? &my : nullptr, gate != 0);
-    std::memcpy(out, f.d.data(), f.d.size() * 4);
+    std::memcpy(out, f.d.data(), f.d.size() * sizeof(float));
     return 0;
 }
 
@@ -875,7 +897,7 @@ struct or_cv_params {
 int or_encode_vectors(void* out_eng, int w, int h, int fmt, const float* flow, int fw, int fh, float scale) {
     Image out(w, h, (Fmt)fmt);
     FlowField f(fw, fh);
-    std::memcpy(f.d.data(), flow, f.d.size() * 4);
+    std::memcpy(f.d.data(), flow, f.d.size() * sizeof(float));
     std::string e;
     int rc = encode_vectors(out, f, scale, &e);
     if (rc) return fail(rc, e);

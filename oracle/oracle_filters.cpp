@@ -311,7 +311,7 @@ const int TAP_LIMIT = 1 << 16;
 
 float store_blur_int(float v, float white) {  // warp.rs:272-274 / :292-294
     float f = (float)cvtt32(v + 0.5f);
-    f = std::max(f, 0.0f);
+    f = std::max(f, (float)0.0f);
     return std::min(f, white);
 }
 

@@ -1,8 +1,8 @@
 """Builds the committed golden fixtures of the parity tests from the reference tree.
 
-Run in a container that has the reference mounted (default /root/reference):
+Run in a container that has the reference tree (its path is required):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference tree> [--only flow_models]
 
 Writes, next to this script:
 
@@ -44,6 +44,11 @@ Writes, next to this script:
   ``gen_blur.py``).
 * ``warp_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/warp_cases.hex``
   (the reference's bit-exact numpy model of the inverse warp; format in its ``gen_warp.py``).
+
+* ``flow_models.bin.gz`` - the six differential fixtures ``plugins/retime-engine/tests/fixtures/
+  flow_{a..f}.hex`` (the reference's float32 numpy model of the solver without block matching,
+  ``flow_ref.py``; not bit exact: the reference's own test accepts 1e-4, 1e-3 with prep), each
+  blob prefixed by its length as a little endian u32, in the order a to f.
 
 Nothing under ``tests/`` reads the reference tree at test time; only this script does.
 """
@@ -208,11 +213,27 @@ def crt_powf_traced(ref):
     print(f"crt_powf_traced.json: {len(triples)} vectors")
 
 
+def flow_models(ref):
+    out = b""
+    for name in "abcdef":
+        txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", f"flow_{name}.hex")).read()
+        blob = bytes.fromhex("".join(txt.split()))
+        out += len(blob).to_bytes(4, "little") + blob
+    with gzip.open(os.path.join(HERE, "flow_models.bin.gz"), "wb") as f:
+        f.write(out)
+    print(f"flow_models.bin.gz: {len(out)} bytes, sha256 {hashlib.sha256(out).hexdigest()}")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="the reference tree (baairon/twixtor)")
+    ap.add_argument("--only", choices=["flow_models"], default=None, help="write one fixture only")
     args = ap.parse_args()
     ref = args.reference
+    if args.only == "flow_models":
+        flow_models(ref)
+        return
+    flow_models(ref)
     gen = load_gen(ref)
     with tempfile.TemporaryDirectory() as tmp:
         builder = gen.Builder()

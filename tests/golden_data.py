@@ -364,3 +364,29 @@ def warp_cases():
                         is360=bool(flags & 2), want_cov=bool(flags & 4), src=src, flow=flow, out=exp, cov=cov))
     assert p == len(blob)
     return out
+
+
+FLOW_MODEL_TOL = {"a": 1e-4, "b": 1e-4, "c": 1e-4, "d": 1e-4, "e": 1e-3, "f": 1e-3}  # flow_d.rs:231-236
+
+
+def flow_models():
+    """The reference's differential fixtures of the solver (flow_{a..f}.hex, its float32 numpy model
+    without block matching, flow_ref.py): list of dicts with the engine images x and y (8 bit A, R,
+    G, B), the settings and the model's flow; the reference accepts FLOW_MODEL_TOL."""
+    blob = gzip.open(os.path.join(GOLDEN, "flow_models.bin.gz")).read()
+    p, out = 0, []
+    for name in "abcdef":
+        n = struct.unpack_from("<I", blob, p)[0]
+        b = blob[p + 4:p + 4 + n]
+        p += 4 + n
+        magic, w, h, sens, quality, prep = struct.unpack_from("<IIIfII", b, 0)
+        assert magic == 0x32444C46
+        o = 24
+        x = np.frombuffer(b, np.uint8, w * h * 4, o).copy()
+        y = np.frombuffer(b, np.uint8, w * h * 4, o + w * h * 4).copy()
+        r = 1 if quality == 4 else 0
+        fw, fh = w >> r, h >> r
+        flow = np.frombuffer(b, "<f4", fw * fh * 2, o + 2 * w * h * 4).astype(np.float32)
+        out.append(dict(name=name, w=w, h=h, sens=np.float32(sens), quality=quality, prep=prep, x=x, y=y,
+                        flow=flow, tol=FLOW_MODEL_TOL[name]))
+    return out

@@ -74,6 +74,7 @@ def lib():
         L.or_build_pyramid.argtypes = [P, i, i, i, i, i, f, i, i, i, i, P]
         L.or_compose_vectors3.argtypes = [P, P, i, i, i, P, P, i, i, f, f, f, i, i, i, i, i, f, i, P]
         L.or_solve_pair.argtypes = [P, P, i, i, i, i, i, f, i, i, P, P]
+        L.or_solve.argtypes = [P, P, i, i, i, i, i, f, i, i, i, P]
         L.or_inv_warp.argtypes = [P, P, i, i, i, P, i, i, f, i, P]
         L.or_blend.argtypes = [P, P, P, i, i, i, f]
         L.or_compose_vectors.argtypes = [P, P, i, i, i, P, P, i, i, f, i, P]
@@ -106,6 +107,51 @@ def lib():
         L.or_encode_vectors.argtypes = [P, i, i, i, P, i, i, f]
         _lib = L
     return _lib
+
+
+_lib64 = None
+
+
+def lib64():
+    """The oracle in double precision (oracle/liboracle64.so, the fast mode's FP64 yardstick)."""
+    global _lib64
+    if _lib64 is None:
+        path = os.path.join(ORACLE_DIR, "liboracle64.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        P, i = ctypes.c_void_p, ctypes.c_int
+        L.or_solve_pair.argtypes = [P, P, i, i, i, i, i, ctypes.c_double, i, i, P, P]
+        L.or_solve.argtypes = [P, P, i, i, i, i, i, ctypes.c_double, i, i, i, P]
+        L.or_last_error.restype = ctypes.c_char_p
+        L.or_set_threads.argtypes = [i]
+        _lib64 = L
+    return _lib64
+
+
+def solve_pair64(a, b, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, skip_refine=False, above_first=True):
+    """solve_pair evaluated in double precision: (f_ab, f_ba) as float64 arrays."""
+    _, sizes = geometry(quality, hiq, w, h)
+    fw, fh = sizes[0]
+    f_ab = np.zeros(fw * fh * 2, np.float64)
+    f_ba = np.zeros(fw * fh * 2, np.float64)
+    rc = lib64().or_solve_pair(ptr(a), ptr(b), w, h, fmt, quality, int(hiq), float(np.float32(sensitivity)),
+                               int(skip_refine), int(above_first), ptr(f_ab), ptr(f_ba))
+    if rc:
+        raise ValueError(lib64().or_last_error().decode())
+    return f_ab, f_ba, (fw, fh)
+
+
+def solve64(x, y, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, skip_refine=False, above_first=True, prep=1):
+    """flow::solve X -> Y evaluated in double precision (float64 field)."""
+    _, sizes = geometry(quality, hiq, w, h)
+    fw, fh = sizes[0]
+    out = np.zeros(fw * fh * 2, np.float64)
+    rc = lib64().or_solve(ptr(x), ptr(y), w, h, fmt, quality, int(hiq), float(np.float32(sensitivity)),
+                          int(skip_refine), int(above_first), prep, ptr(out))
+    if rc:
+        raise ValueError(lib64().or_last_error().decode())
+    return out, (fw, fh)
 
 
 def ptr(a):
@@ -163,6 +209,18 @@ def solve_pair(a, b, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, skip_refin
     if rc:
         raise ValueError(err())
     return f_ab, f_ba, (fw, fh)
+
+
+def solve(x, y, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, skip_refine=False, above_first=True, prep=1):
+    """flow::solve X -> Y (prep: 1 none, 2 Contrast/Edge Enhance, 3 Delinearize)."""
+    _, sizes = geometry(quality, hiq, w, h)
+    fw, fh = sizes[0]
+    out = np.zeros(fw * fh * 2, np.float32)
+    rc = lib().or_solve(ptr(x), ptr(y), w, h, fmt, quality, int(hiq), np.float32(sensitivity), int(skip_refine),
+                        int(above_first), prep, ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out, (fw, fh)
 
 
 def inv_warp(src, w, h, fmt, flow, fw, fh, amount, hold=True, coverage=False, out=None):

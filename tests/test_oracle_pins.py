@@ -264,3 +264,16 @@ def test_motion_blur_model_fixtures(i):
     out = O.motion_blur(c["src"], c["w"], c["h"], c["fmt"], c["flow"], c["fw"], c["fh"], c["amount"], c["hiq"],
                         c["shutter"])
     assert out.view(np.uint8).tobytes() == c["out"].view(np.uint8).tobytes()
+
+
+@pytest.mark.parametrize("c", golden_data.flow_models(), ids=lambda c: c["name"])
+def test_oracle_solve_matches_the_reference_solver_models(c):
+    """The reference's differential fixtures of the solver (its float32 numpy model, no block
+    matching; tests/flow_d.rs:224-242): the oracle's solve X -> Y within the reference's own
+    tolerances, and the double precision build of the oracle within them too."""
+    prep = {0: 1, 1: 2, 2: 3}[c["prep"]]
+    kw = dict(quality=c["quality"], hiq=True, sensitivity=c["sens"], skip_refine=True, prep=prep)
+    f, _ = O.solve(c["x"], c["y"], c["w"], c["h"], 0, **kw)
+    f64, _ = O.solve64(c["x"], c["y"], c["w"], c["h"], 0, **kw)
+    assert np.abs(f.astype(np.float64) - c["flow"]).max() < c["tol"]
+    assert np.abs(f64 - c["flow"]).max() < c["tol"]

@@ -75,7 +75,8 @@ class _FlowSettings(ctypes.Structure):
     _fields_ = [("quality", ctypes.c_int32), ("hiq", ctypes.c_int32), ("sensitivity", ctypes.c_float),
                 ("prep_contrast_edge", ctypes.c_int32), ("prep_delinearize", ctypes.c_int32),
                 ("track_alpha", ctypes.c_int32), ("video_range_luma", ctypes.c_int32),
-                ("skip_refine", ctypes.c_int32), ("wrap", ctypes.c_int32), ("taps_above_first", ctypes.c_int32)]
+                ("skip_refine", ctypes.c_int32), ("wrap", ctypes.c_int32), ("taps_above_first", ctypes.c_int32),
+                ("fast_mode", ctypes.c_int32)]
 
 
 class _Selection(ctypes.Structure):
@@ -158,11 +159,12 @@ class FlowSettings:
     skip_refine: bool = False
     wrap: bool = False
     taps_above_first: bool = True
+    fast_mode: bool = False
 
     def _c(self):
         return _FlowSettings(self.quality, int(self.hiq), np.float32(self.sensitivity), int(self.prep_contrast_edge),
                              int(self.prep_delinearize), int(self.track_alpha), int(self.video_range_luma),
-                             int(self.skip_refine), int(self.wrap), int(self.taps_above_first))
+                             int(self.skip_refine), int(self.wrap), int(self.taps_above_first), int(self.fast_mode))
 
 
 @dataclass

@@ -1,7 +1,7 @@
 """Builds the library twixtor_b200/libtwixtor_b200.so with nvcc for sm_100a (in tree).
 
 Strict mode flags: no FMA contraction (-fmad=false), IEEE division and square root, denormals
-kept (-ftz=false). The library is plain C ABI + CUDA runtime; it links no PyTorch.
+kept (-ftz=false). The solver's translation units are built a second time for the fast mode. The library is plain C ABI + CUDA runtime; it links no PyTorch.
 
 One generated input: the table of inputs where glibc's logf differs from the library's own
 double precision log (csrc/twlog.h), made by running csrc/gen_logf_table.c (it calls this
@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtwixtor_b200.so")
 SOURCES = ["solver.cu", "fused.cu", "coarse.cu", "image.cu", "smart.cu", "forward.cu", "layers.cu", "filters.cu", "prep.cu", "adjoint.cu", "host_context.cu", "host_solve.cu", "host_compose.cu", "host_layers.cu", "host_clips.cu", "host_time.cu", "host_tune.cu", "noalloc.cu"]
+FAST_SOURCES = ["fused.cu", "solver.cu", "coarse.cu"]  # built a second time for the fast mode
 BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
@@ -78,12 +79,18 @@ def build(force=False, verbose=False):
     env = dict(os.environ)
     env.pop("CXX", None)  # host compiler: the system g++ (ccbin default)
     compile_flags = [f for f in FLAGS if f not in ("-shared", "-cudart", "shared")]
+    # the fast mode's build of the solver's translation units: FMA contraction, approximate division
+    # and square root, denormals flushed; its kernels in namespace tw::fast (TW_FAST_VARIANT)
+    fast_flags = [{"-fmad=false": "-fmad=true", "-prec-div=true": "-prec-div=false",
+                   "-prec-sqrt=true": "-prec-sqrt=false", "-ftz=false": "-ftz=true"}.get(f, f)
+                  for f in compile_flags] + ["-DTW_FAST_VARIANT"]
 
-    def compile_one(name):
+    def compile_one(unit):
+        name, fast = unit
         src = os.path.join(CSRC, name)
-        obj = os.path.join(BUILD, name[:-3] + ".o")
+        obj = os.path.join(BUILD, name[:-3] + ("_fast.o" if fast else ".o"))
         if force or _objects_stale(src, obj):
-            cmd = [NVCC] + compile_flags + ["-c", "-o", obj, src]
+            cmd = [NVCC] + (fast_flags if fast else compile_flags) + ["-c", "-o", obj, src]
             if verbose:
                 print(" ".join(cmd))
             r = subprocess.run(cmd, env=env, cwd=CSRC, capture_output=True, text=True)
@@ -93,7 +100,7 @@ def build(force=False, verbose=False):
 
     os.makedirs(BUILD, exist_ok=True)
     with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as pool:
-        objs = list(pool.map(compile_one, SOURCES))
+        objs = list(pool.map(compile_one, [(n, False) for n in SOURCES] + [(n, True) for n in FAST_SOURCES]))
     cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-cudart", "shared", "-o", LIB] + objs + [table_obj]
     if verbose:
         print(" ".join(cmd))

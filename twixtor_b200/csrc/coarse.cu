@@ -20,6 +20,7 @@
 #include "level.cuh"
 
 namespace tw {
+TW_VARIANT_BEGIN
 
 namespace {
 
@@ -312,4 +313,5 @@ size_t coarse_smem_bytes() {
     return sizeof(float) * (15 * (size_t)COARSE_MAX_PIXELS + (size_t)NG * COARSE_MAX_LINE) + (size_t)NG * COARSE_MAX_LINE;
 }
 
+TW_VARIANT_END
 }  // namespace tw

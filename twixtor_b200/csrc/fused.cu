@@ -10,6 +10,7 @@
 #include "luma.cuh"
 
 namespace tw {
+TW_VARIANT_BEGIN
 
 constexpr int FT_X = 32;  // tile width (outputs)
 constexpr int FT_Y = 32;  // tile height
@@ -439,12 +440,15 @@ __global__ void k_apply_negate(const float* __restrict__ fu, const float* __rest
     if (isnan(u) || isnan(v)) atomicOr(nan_flag, 1);
 }
 
+TW_VARIANT_END
 }  // namespace tw
 
 namespace tw {
+TW_VARIANT_BEGIN
 // flow/extras.rs:64-72: v >= 0.95 gives 1, else 0 (a NaN gives 0), in place
 __global__ void k_binarize(float* __restrict__ p, long n) {
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = p[i] >= 0.95f ? 1.0f : 0.0f;
 }
+TW_VARIANT_END
 }  // namespace tw

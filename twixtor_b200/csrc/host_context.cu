@@ -175,6 +175,24 @@ int tw_open(int device, tw_ctx** out) {
                                  (int)level_iter_smem(LEVEL_TILE_64x64));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_solve_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem_bytes());
+    // the fast mode's builds of the same kernels
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fast::k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(BM_MAX_LINE));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fast::k_bm_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(BM_MAX_LINE));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fast::k_level_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)level_init_smem());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fast::k_level_iter_32x32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)level_iter_smem(LEVEL_TILE_32x32));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fast::k_level_iter_64x32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)level_iter_smem(LEVEL_TILE_64x32));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fast::k_level_iter_64x64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)level_iter_smem(LEVEL_TILE_64x64));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fast::k_solve_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem_bytes());
     if (e != cudaSuccess) { tw_close(ctx); return TW_ERR_CUDA; }
     if (ctx->ensure(ctx->flags, FLAGS_BYTES, "flags") != TW_OK) { tw_close(ctx); return TW_ERR_CUDA; }
     k_selfcheck<<<1, 1, 0, ctx->stream>>>(ctx->flags.as<int>());

@@ -123,19 +123,19 @@ size_t pyramid_floats(const Geo& g);
 // read, the flow (2) written.
 void level_iter(tw_ctx* ctx, LevelTune ic, const float* A, const float* B, const float* gx, const float* gy,
                 const float* a0, const float* a1, const float* a2, const float* fu, const float* fv, int w, int h, bool af,
-                float* nu, float* nv, const float* mask_y) {
+                float* nu, float* nv, const float* mask_y, bool fast) {
     double b = 48.0 * w * h;
     size_t smem = level_iter_smem(ic.iter_tile);
     if (ic.iter_tile == LEVEL_TILE_64x64) {
         dim3 g((unsigned)((w + 63) / 64), (unsigned)((h + 63) / 64));
-        LAUNCHB(ctx, b, k_level_iter_64x64, g, ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7, ctx->g5, af,
+        LAUNCHV(ctx, fast, b, k_level_iter_64x64, g, ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7, ctx->g5, af,
                 nu, nv, mask_y);
     } else if (ic.iter_tile == LEVEL_TILE_64x32) {
         dim3 g((unsigned)((w + 63) / 64), (unsigned)((h + 31) / 32));
-        LAUNCHB(ctx, b, k_level_iter_64x32, g, ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7, ctx->g5, af,
+        LAUNCHV(ctx, fast, b, k_level_iter_64x32, g, ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7, ctx->g5, af,
                 nu, nv, mask_y);
     } else {
-        LAUNCHB(ctx, b, k_level_iter_32x32, tiles(w, h), ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7,
+        LAUNCHV(ctx, fast, b, k_level_iter_32x32, tiles(w, h), ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7,
                 ctx->g5, af, nu, nv, mask_y);
     }
 }
@@ -164,6 +164,7 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
     if (s.video_range_luma && s.track_alpha)
         return ctx->fail(TW_ERR_UNSUPPORTED, "optical flow luma: video range conversion together with Track RGB+A is not supported");
     int lmode = (s.track_alpha ? LUMA_TRACK_ALPHA : 0) | (s.video_range_luma ? LUMA_VIDEO_RANGE : 0);
+    const bool fast = s.fast_mode != 0;  // the fast mode's build of the band pyramid's kernels
     size_t full = (size_t)W * H * sizeof(float);
     for (int i = 0; i < 3; i++) CHECK(ctx->ensure(scratch[i], full, "pyramid scratch"));
     float* cur = scratch[0].as<float>();
@@ -207,11 +208,11 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
         LAUNCH(ctx, k_luma, grid1(n), TB, 0, eng_dev, fmt, cur, W, H, s.track_alpha != 0, s.video_range_luma != 0);
     }
     for (int r = 0; r < g.reduction; r++) {  // prep.rs:252-259; the first step reads the luma on the fly
-        LAUNCHB(ctx, (r == 0 ? 4.0 * sample_bytes(fmt) : 4.0) * cw * ch + 4.0 * cw * ch, k_blur5_band, tiles(cw, ch),
+        LAUNCHV(ctx, fast, (r == 0 ? 4.0 * sample_bytes(fmt) : 4.0) * cw * ch + 4.0 * cw * ch, k_blur5_band, tiles(cw, ch),
                 FUSED_THREADS, 0, r == 0 ? (const float*)nullptr : cur, r == 0 ? eng_dev : nullptr, fmt, lmode, cw, ch, af, tmp,
                 (float*)nullptr, (float*)nullptr);
         int nw = cw / 2, nh = ch / 2;
-        LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, tmp, cw, ch, nxt, nw, nh);
+        LAUNCHV(ctx, fast, 0, k_resample, grid2(nw, nh), TB, 0, tmp, cw, ch, nxt, nw, nh);
         std::swap(cur, nxt);
         cw = nw;
         ch = nh;
@@ -227,11 +228,11 @@ int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, c
     size_t pf = pyramid_floats(g);
     for (int i = 0; i < g.levels; i++) {
         int lw = g.sizes[i][0], lh = g.sizes[i][1];
-        LAUNCHB(ctx, 16.0 * lw * lh, k_blur5_band, tiles(lw, lh), level_threads(lw, lh), 0, cur, (const void*)nullptr, fmt, 0, lw,
+        LAUNCHV(ctx, fast, 16.0 * lw * lh, k_blur5_band, tiles(lw, lh), level_threads(lw, lh), 0, cur, (const void*)nullptr, fmt, 0, lw,
                 lh, af, tmp, out + off, out_t ? out_t + off : (float*)nullptr);
         if (i + 1 < g.levels) {
             int nw = g.sizes[i + 1][0], nh = g.sizes[i + 1][1];
-            LAUNCH(ctx, k_resample, grid2(nw, nh), TB, 0, tmp, lw, lh, cur, nw, nh);
+            LAUNCHV(ctx, fast, 0, k_resample, grid2(nw, nh), TB, 0, tmp, lw, lh, cur, nw, nh);
         }
         off += (size_t)lw * lh;
     }
@@ -304,15 +305,15 @@ int build_user_dev(tw_ctx* ctx, const UserPairs& pr, const Geo& g, int W, int H,
 // transposed planes (AT, BT: the level's bands stored column by column), and the field goes back.
 // uT, vT: scratch for the transposed field (w * h floats each).
 void block_match(tw_ctx* ctx, const float* A, const float* B, const float* AT, const float* BT, float* fu, float* fv,
-                 float* uT, float* vT, int w, int h) {
+                 float* uT, float* vT, int w, int h, bool fast) {
     if (w < 3 || h < 3) return;  // callers refuse lines above BM_MAX_LINE before any launch
     double b = 24.0 * w * h;  // per launch (both sweeps): the field read and written (8 + 8), A and B read once (4 + 4)
     LevelTune t = level_tune(ctx, w, h);
-    LAUNCHB(ctx, b, k_bm_rows, h - 2, t.bm_rows_threads, bm_smem_bytes(w), A, B, fu, fv, w, h);
+    LAUNCHV(ctx, fast, b, k_bm_rows, h - 2, t.bm_rows_threads, bm_smem_bytes(w), A, B, fu, fv, w, h);
     dim3 tb(32, 8);
-    LAUNCHB(ctx, 16.0 * w * h, k_transpose2, dim3((w + 31) / 32, (h + 31) / 32), tb, 0, fu, fv, uT, vT, w, h);
-    LAUNCHB(ctx, b, k_bm_cols, w - 2, t.bm_cols_threads, bm_smem_bytes(h), AT, BT, uT, vT, w, h);
-    LAUNCHB(ctx, 16.0 * w * h, k_transpose2, dim3((h + 31) / 32, (w + 31) / 32), tb, 0, uT, vT, fu, fv, h, w);
+    LAUNCHV(ctx, fast, 16.0 * w * h, k_transpose2, dim3((w + 31) / 32, (h + 31) / 32), tb, 0, fu, fv, uT, vT, w, h);
+    LAUNCHV(ctx, fast, b, k_bm_cols, w - 2, t.bm_cols_threads, bm_smem_bytes(h), AT, BT, uT, vT, w, h);
+    LAUNCHV(ctx, fast, 16.0 * w * h, k_transpose2, dim3((h + 31) / 32, (w + 31) / 32), tb, 0, uT, vT, fu, fv, h, w);
 }
 
 // ---- one solve over two resident pyramids (flow.rs:1258-1307) ------------------------------------------
@@ -349,6 +350,7 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
     CHECK(ctx->cuda(cudaMemsetAsync(any, 0, 32 * sizeof(int), ctx->cur), "range flags"));
     bool af = s.taps_above_first != 0;
     bool damp_any = std::fabs((double)damp - 1.0) >= 1e-6;
+    const bool fast = s.fast_mode != 0;
     // The coarse levels whose planes fit one block's shared memory run in one launch (coarse.cu),
     // for the plain solve; the masked and the tracked solves keep the kernel by kernel path.
     int first = start;
@@ -381,7 +383,7 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
             J.fv_out = fv;
             double px = 0.0;
             for (int l = start; l >= last; l--) px += (double)g.sizes[l][0] * g.sizes[l][1];
-            LAUNCHB(ctx, 8.0 * px, k_solve_coarse, 1, COARSE_THREADS, coarse_smem_bytes(), J);
+            LAUNCHV(ctx, fast, 8.0 * px, k_solve_coarse, 1, COARSE_THREADS, coarse_smem_bytes(), J);
             first = last - 1;
         }
     }
@@ -403,29 +405,29 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
         };
         user();
         LevelTune ic = level_tune(ctx, w, h);
-        LAUNCHB(ctx, 24.0 * px, k_level_init, tiles(w, h), lt, level_init_smem(), A, w, h, ctx->g7, af, gx, gy, a0, a1, a2,
+        LAUNCHV(ctx, fast, 24.0 * px, k_level_init, tiles(w, h), lt, level_init_smem(), A, w, h, ctx->g7, af, gx, gy, a0, a1, a2,
                 mask_x);
         for (int it = 0; it < 3; it++) {
             // I1, I0 (gather), grad, tensor, flow in; flow out
-            level_iter(ctx, ic, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, af, nu, nv, mask_y);
+            level_iter(ctx, ic, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, af, nu, nv, mask_y, fast);
             std::swap(fu, nu);
             std::swap(fv, nv);
             if (it == 1 && l == 0) {
-                if (!s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h);
+                if (!s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h, fast);
                 user();
             }
         }
-        if (l != 0 && !s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h);
+        if (l != 0 && !s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h, fast);
         user();
-        LAUNCH(ctx, k_range_any, grid2(w, h), TB, 0, fu, fv, w, h, any + l);
+        LAUNCHV(ctx, fast, 0, k_range_any, grid2(w, h), TB, 0, fu, fv, w, h, any + l);
         bool damp_now = l == start && damp_any;
         if (l > 0) {
             int dw = g.sizes[l - 1][0], dh = g.sizes[l - 1][1];
-            LAUNCH(ctx, k_apply_upsample, grid2(dw, dh), TB, 0, fu, fv, w, h, any, l, start, damp_now, damp, nu, nv, dw, dh);
+            LAUNCHV(ctx, fast, 0, k_apply_upsample, grid2(dw, dh), TB, 0, fu, fv, w, h, any, l, start, damp_now, damp, nu, nv, dw, dh);
             std::swap(fu, nu);
             std::swap(fv, nv);
         } else {
-            LAUNCH(ctx, k_apply_negate, grid1((long)np0), TB, 0, fu, fv, (long)np0, any, start, damp_now, damp, out, nan_flag);
+            LAUNCHV(ctx, fast, 0, k_apply_negate, grid1((long)np0), TB, 0, fu, fv, (long)np0, any, start, damp_now, damp, out, nan_flag);
         }
     }
     return TW_OK;

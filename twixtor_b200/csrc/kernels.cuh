@@ -10,6 +10,17 @@
 
 #include "strict.cuh"
 
+// The solver's translation units (fused.cu, solver.cu, coarse.cu) are compiled twice: in strict mode,
+// and for the fast mode (TW_FAST_VARIANT: FMA contraction, approximate division and square root,
+// denormals flushed), whose kernels land in namespace tw::fast (declared in kernels_fast.cuh).
+#ifdef TW_FAST_VARIANT
+#define TW_VARIANT_BEGIN namespace fast {
+#define TW_VARIANT_END }
+#else
+#define TW_VARIANT_BEGIN
+#define TW_VARIANT_END
+#endif
+
 namespace tw {
 
 constexpr int MAX_TAPS = 8;  // Gaussian r=7 has 8 half taps (flow/conv.rs:64-86)

@@ -16,6 +16,7 @@
 
 #include "../../include/twixtor_b200.h"
 #include "kernels.cuh"
+#include "kernels_fast.cuh"
 #include "luma.cuh"
 
 namespace tw {
@@ -195,6 +196,12 @@ void prof_mark(tw_ctx* ctx);
         }                                                                          \
     } while (0)
 #define LAUNCH(ctx, kernel, grid, block, smem, ...) LAUNCHB(ctx, 0, kernel, grid, block, smem, __VA_ARGS__)
+// The strict kernel, or with `fastv` its fast mode build (tw::fast, kernels_fast.cuh).
+#define LAUNCHV(ctx, fastv, nbytes_, kernel, grid, block, smem, ...)                         \
+    do {                                                                                   \
+        if (fastv) LAUNCHB(ctx, nbytes_, fast::kernel, grid, block, smem, __VA_ARGS__);    \
+        else LAUNCHB(ctx, nbytes_, kernel, grid, block, smem, __VA_ARGS__);                \
+    } while (0)
 
 #define CHECK(expr)                 \
     do {                            \
@@ -251,10 +258,10 @@ __global__ void k_set_flag(int* flags, int idx);  // flags[idx] = 1 (the injecte
 LevelTune level_tune(tw_ctx* ctx, int w, int h);
 LevelTune default_tune(int w, int h);
 void block_match(tw_ctx* ctx, const float* A, const float* B, const float* AT, const float* BT, float* fu, float* fv,
-                 float* uT, float* vT, int w, int h);
+                 float* uT, float* vT, int w, int h, bool fast = false);
 void level_iter(tw_ctx* ctx, LevelTune ic, const float* A, const float* B, const float* gx, const float* gy,
                 const float* a0, const float* a1, const float* a2, const float* fu, const float* fv, int w, int h, bool af,
-                float* nu, float* nv, const float* mask_y);
+                float* nu, float* nv, const float* mask_y, bool fast = false);
 size_t pyramid_floats(const Geo& g);
 int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, const tw_flow_settings& s, const Geo& g,
                       float* out, float* out_t, DevBuf* scratch);

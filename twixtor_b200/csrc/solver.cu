@@ -4,6 +4,7 @@
 #include "level.cuh"
 
 namespace tw {
+TW_VARIANT_BEGIN
 
 // flow/conv.rs:101-137 (border_value_ordered): one border element of a line whose element t is
 // line[t * stride]. `multi` selects the 2- and 3-channel rule (the -1.0 sentinel decides whether a
@@ -659,4 +660,5 @@ __global__ void k_bm_cols(const float* __restrict__ A, const float* __restrict__
     bm_line<true>(A, B, fu, fv, w, h, x);
 }
 
+TW_VARIANT_END
 }  // namespace tw
