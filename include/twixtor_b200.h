@@ -225,6 +225,19 @@ int tw_solve(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_flow_se
 int tw_solve_masked(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_flow_settings* s, const float* matte_x,
                     const float* matte_y, tw_flow* out);
 
+/* flow::extras::solve_pyramids_with (flow/extras.rs:244-265) on the caller's pyramids: X(p) ~ Y(p +
+ * out(p)) from the band pyramids of X and Y (x_levels, y_levels: the levels of the geometry of s for
+ * a width x height frame concatenated finest first, as tw_build_pyramid returns them) with a
+ * layer's SolveExtras (extras.rs:173-179): the mask pyramids of X and Y (laid out like the bands;
+ * both NULL: none; the sweeps are not gated, as MaskPyramid::build_ungated, the masks the effects
+ * build) and the user displacement of its tracking points (UserDisplacement, points.rs:201-240:
+ * user_d the levels' (dx, dy) interleaved, user_w their weights, both laid out like the bands; both
+ * NULL: none). All host buffers. Replaces Backend::solve_pyramids_with (device/exec/backend.rs:33)
+ * one to one. */
+int tw_solve_pyramids(tw_ctx* ctx, const tw_flow_settings* s, int32_t width, int32_t height, const float* x_levels,
+                      const float* y_levels, const float* mask_x, const float* mask_y, const float* user_d,
+                      const float* user_w, tw_flow* out);
+
 /* flow::solve_pair (flow.rs:1347-1353): f_ab = solve(A, B), f_ba = solve(B, A), the pyramids built
  * once. Replaces Backend::solve_pair (device/exec/backend.rs:31). */
 int tw_solve_pair(tw_ctx* ctx, const tw_image* a, const tw_image* b, const tw_flow_settings* s, tw_flow* f_ab,

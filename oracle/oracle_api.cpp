@@ -299,6 +299,61 @@ int or_solve(const void* x_eng, const void* y_eng, int w, int h, int fmt, int qu
     return 0;
 }
 
+// flow::extras::solve_pyramids_with (flow/extras.rs:244-265) for the test of the device entry that
+// takes the caller's pyramids: the band pyramids of X and Y, the mask pyramids of two mattes (both
+// null: none; ungated, as the effects build them) and the user displacement of the point pairs
+// (from x, from y, to x, to y, npts of them; 0: none) built here and returned beside the flow
+// (user_d: the levels' (dx, dy) interleaved, user_w: their weights, levels concatenated).
+int or_solve_pyramids_with(const void* x_eng, const void* y_eng, int w, int h, int fmt, int quality, int hiq,
+                           float sensitivity, int above_first, const float* matte_x, const float* matte_y,
+                           const float* pts, int npts, float* x_levels, float* y_levels, float* mask_x, float* mask_y,
+                           float* user_d, float* user_w, float* out) {
+    Image x(w, h, (Fmt)fmt), y(w, h, (Fmt)fmt);
+    std::memcpy(x.data(), x_eng, x.bytes());
+    std::memcpy(y.data(), y_eng, y.bytes());
+    FlowSettings s;
+    s.quality = quality;
+    s.hiq = hiq != 0;
+    s.sensitivity = sensitivity;
+    s.taps_above_first = above_first != 0;
+    Pyramid px, py;
+    std::string e;
+    if (!build_pyramid(x, s, &px, &e) || !build_pyramid(y, s, &py, &e)) return fail(-1, e);
+    size_t off = 0;
+    for (size_t l = 0; l < px.levels.size(); l++) {
+        std::memcpy(x_levels + off, px.levels[l].d.data(), px.levels[l].d.size() * sizeof(float));
+        std::memcpy(y_levels + off, py.levels[l].d.data(), py.levels[l].d.size() * sizeof(float));
+        off += px.levels[l].d.size();
+    }
+    std::vector<Plane> mx, my;
+    if (matte_x) {
+        if (!mask_pyramid(matte_x, w, h, s, &mx, &e) || !mask_pyramid(matte_y, w, h, s, &my, &e)) return fail(-1, e);
+        size_t o = 0;
+        for (size_t l = 0; l < mx.size(); l++) {
+            std::memcpy(mask_x + o, mx[l].d.data(), mx[l].d.size() * sizeof(float));
+            std::memcpy(mask_y + o, my[l].d.data(), my[l].d.size() * sizeof(float));
+            o += mx[l].d.size();
+        }
+    }
+    std::vector<UserLevel> u;
+    if (npts > 0) {
+        std::vector<std::array<float, 4>> pairs;
+        for (int i = 0; i < npts; i++) pairs.push_back({pts[4 * i], pts[4 * i + 1], pts[4 * i + 2], pts[4 * i + 3]});
+        u = user_displacement(pairs, px.geo, w, h);
+        size_t od = 0, ow = 0;
+        for (auto& lv : u) {
+            std::memcpy(user_d + od, lv.d.data(), lv.d.size() * sizeof(float));
+            std::memcpy(user_w + ow, lv.w.data(), lv.w.size() * sizeof(float));
+            od += lv.d.size();
+            ow += lv.w.size();
+        }
+    }
+    FlowField f = solve_pyramids_masked(px, py, s, matte_x ? &mx : nullptr, matte_x ? &my : nullptr, false,
+                                        npts > 0 ? &u : nullptr);
+    std::memcpy(out, f.d.data(), f.d.size() * sizeof(float));
+    return 0;
+}
+
 // warp::inv_warp / inv_warp_coverage on engine images (hold, mode 1, no 360). cov may be null.
 int or_inv_warp(void* out_eng, const void* src_eng, int w, int h, int fmt, const float* flow, int fw, int fh, float amount,
                 int hold, uint8_t* cov) {

@@ -75,6 +75,7 @@ def lib():
         L.or_compose_vectors3.argtypes = [P, P, i, i, i, P, P, i, i, f, f, f, i, i, i, i, i, f, i, P]
         L.or_solve_pair.argtypes = [P, P, i, i, i, i, i, f, i, i, P, P]
         L.or_solve.argtypes = [P, P, i, i, i, i, i, f, i, i, i, P]
+        L.or_solve_pyramids_with.argtypes = [P, P, i, i, i, i, i, f, i, P, P, P, i, P, P, P, P, P, P, P]
         L.or_inv_warp.argtypes = [P, P, i, i, i, P, i, i, f, i, P]
         L.or_blend.argtypes = [P, P, P, i, i, i, f]
         L.or_compose_vectors.argtypes = [P, P, i, i, i, P, P, i, i, f, i, P]
@@ -221,6 +222,30 @@ def solve(x, y, w, h, fmt, quality=4, hiq=True, sensitivity=0.7, skip_refine=Fal
     if rc:
         raise ValueError(err())
     return out, (fw, fh)
+
+
+def solve_pyramids_with(x, y, w, h, fmt, matte_x=None, matte_y=None, pairs=None, quality=4, hiq=True, sensitivity=0.7,
+                        above_first=True):
+    """flow::extras::solve_pyramids_with: returns (flow, x_levels, y_levels, mask_x, mask_y, user_d,
+    user_w), the pyramids concatenated finest first; the masks / user displacement None when absent."""
+    _, sizes = geometry(quality, hiq, w, h)
+    fw, fh = sizes[0]
+    pf = sum(a * b for a, b in sizes)
+    out = np.zeros(fw * fh * 2, np.float32)
+    xl, yl = np.zeros(pf, np.float32), np.zeros(pf, np.float32)
+    mxl, myl = np.zeros(pf, np.float32), np.zeros(pf, np.float32)
+    ud, uw = np.zeros(2 * pf, np.float32), np.zeros(pf, np.float32)
+    pts = np.ascontiguousarray(pairs if pairs is not None else np.zeros((1, 4)), np.float32)
+    npts = 0 if pairs is None else len(pairs)
+    mx = None if matte_x is None else np.ascontiguousarray(matte_x, np.float32)
+    my = None if matte_y is None else np.ascontiguousarray(matte_y, np.float32)
+    rc = lib().or_solve_pyramids_with(ptr(x), ptr(y), w, h, fmt, quality, int(hiq), np.float32(sensitivity),
+                                      int(above_first), ptr(mx), ptr(my), ptr(pts), npts, ptr(xl), ptr(yl), ptr(mxl),
+                                      ptr(myl), ptr(ud), ptr(uw), ptr(out))
+    if rc:
+        raise ValueError(err())
+    return (out, xl, yl, mxl if mx is not None else None, myl if mx is not None else None,
+            ud if npts else None, uw if npts else None)
 
 
 def inv_warp(src, w, h, fmt, flow, fw, fh, amount, hold=True, coverage=False, out=None):

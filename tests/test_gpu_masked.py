@@ -86,3 +86,24 @@ def test_empty_matte_gives_the_zero_flow(dev):
     want, _ = O.solve_masked(x, y, w, h, 1, z, z)
     assert same(got, want)
     assert (got.view(np.uint32) == 0x80000000).all()
+
+
+@pytest.mark.parametrize("extras", ["none", "masks", "points", "both"])
+def test_solve_pyramids_with_extras_matches_oracle(dev, extras):
+    """tw_solve_pyramids (Backend::solve_pyramids_with) on the oracle's pyramids with its mask
+    pyramids and user displacement: the flow bit for bit."""
+    w, h = 97, 61
+    rng = np.random.RandomState(3)
+    frames = synth.moving_clip(w, h, 2, depth=8, seed=21)
+    n = w * h * 4
+    x, y = O.from_frame(frames[:n], w, h, 0), O.from_frame(frames[n:], w, h, 0)
+    mx = my = pairs = None
+    if extras in ("masks", "both"):
+        yy, xx = np.mgrid[0:h, 0:w]
+        mx = (((xx - 40) / 30.0) ** 2 + ((yy - 30) / 20.0) ** 2 <= 1).astype(np.float32).ravel()
+        my = (((xx - 43) / 30.0) ** 2 + ((yy - 31) / 20.0) ** 2 <= 1).astype(np.float32).ravel()
+    if extras in ("points", "both"):
+        pairs = rng.uniform([5, 5, 5, 5], [w - 5, h - 5, w - 5, h - 5], (3, 4)).astype(np.float32)
+    want, xl, yl, mxl, myl, ud, uw = O.solve_pyramids_with(x, y, w, h, 0, mx, my, pairs)
+    got, _ = dev.solve_pyramids(tw.FlowSettings(), w, h, xl, yl, mxl, myl, ud, uw)
+    assert got.tobytes() == want.tobytes()

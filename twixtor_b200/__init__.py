@@ -327,6 +327,7 @@ def library():
     L.tw_flow_geometry.argtypes = [ctypes.POINTER(_FlowSettings), i32, i32, P, P, P, P, i32]
     L.tw_solve.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), pflow]
     L.tw_solve_pair.argtypes = [P, pimg, pimg, ctypes.POINTER(_FlowSettings), pflow, pflow]
+    L.tw_solve_pyramids.argtypes = [P, ctypes.POINTER(_FlowSettings), i32, i32, P, P, P, P, P, P, pflow]
     L.tw_compose_vectors.argtypes = [P, ctypes.POINTER(_EngineSettings), ctypes.POINTER(_Selection), pimg, pimg,
                                      pflow, pflow, pimg]
     L.tw_build_pyramid.argtypes = [P, pimg, ctypes.POINTER(_FlowSettings), P]
@@ -542,6 +543,19 @@ class Device:
         fo = _Flow(fw, fh, out.ctypes.data)
         self._check(self._L.tw_solve(self._h, ctypes.byref(xi), ctypes.byref(yi), ctypes.byref(settings._c()),
                                      ctypes.byref(fo)))
+        return out, (fw, fh)
+
+    def solve_pyramids(self, settings: FlowSettings, width, height, x_levels, y_levels, mask_x=None, mask_y=None,
+                       user_d=None, user_w=None):
+        """``flow::extras::solve_pyramids_with`` on given band pyramids (levels concatenated finest
+        first) with the optional mask pyramids and user displacement: the flow and its size."""
+        fw, fh, _ = flow_geometry(settings, width, height)
+        out = np.zeros(fw * fh * 2, np.float32)
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32)
+                for a in (x_levels, y_levels, mask_x, mask_y, user_d, user_w)]
+        fo = _Flow(fw, fh, out.ctypes.data)
+        self._check(self._L.tw_solve_pyramids(self._h, ctypes.byref(settings._c()), width, height,
+                                              *[_ptr(a) for a in arrs], ctypes.byref(fo)))
         return out, (fw, fh)
 
     def solve_pair(self, a, b, width, height, fmt, settings: FlowSettings):

@@ -110,14 +110,6 @@ void conv_planes(tw_ctx* ctx, float* const* planes, int c, int w, int h, const T
     }
 }
 
-// ---- the pyramid of one engine image (flow.rs:242-275) ----------------------------------------------
-// Builds the band pass levels into `out` (levels concatenated, finest first). Scratch: plane[0..2].
-// Luma, the reduction steps (prep.rs:252-259) and each level's blur5 + band run as tiled kernels
-
-size_t pyramid_floats(const Geo& g);
-// Threads per CTA of the tiled level kernels: a level of few tiles is latency bound (every CTA
-// walks its stages one after the other), so its CTAs get more threads and each thread fewer
-// elements per stage; a level with tiles enough to fill the GPU keeps 256.
 // One solver iteration (k_level_iter_*) with the tile shape and block size of the level's choice.
 // Algorithmic bytes per pixel: I1, the I0 gather, the gradient (2), the tensor (3) and the flow (2)
 // read, the flow (2) written.
@@ -154,11 +146,18 @@ LevelTune level_tune(tw_ctx* ctx, int w, int h) {
     return it != ctx->tune_table.end() ? it->second : default_tune(w, h);
 }
 
+// Threads per CTA of the tiled pyramid and tensor kernels: a level of few tiles is latency bound
+// (every CTA walks its stages one after the other), so its CTAs get more threads and each thread
+// fewer elements per stage; a level with tiles enough to fill the GPU keeps 256.
 static int level_threads(int w, int h) {
     long tiles_n = (long)((w + 31) / 32) * ((h + 31) / 32);
     return tiles_n <= 148 ? 1024 : tiles_n <= 296 ? 512 : 256;
 }
 
+// ---- the pyramid of one engine image (flow.rs:242-275) ----------------------------------------------
+// Builds the band pass levels into `out` (levels concatenated, finest first) and their transposes
+// into out_t. Luma, the reduction steps (prep.rs:252-259) and each level's blur5 + band run as
+// tiled kernels (k_blur5_band), each followed by the corner aligned resample to the next size.
 int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, const tw_flow_settings& s, const Geo& g,
                       float* out, float* out_t, DevBuf* scratch) {
     if (s.video_range_luma && s.track_alpha)
@@ -590,6 +589,67 @@ int tw_solve_masked(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_
     CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
     CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, *s, ctx->work[0], ctx->flow[0].as<float>(), flags + FL_ANY0,
                              flags + FL_NAN, mx, my));
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->flow[0].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
+    int hf[2];
+    CHECK(finish(ctx, hf, 2));
+    if (hf[0]) return ctx->fail(TW_ERR_NAN_OUTPUT, "the solved flow holds a NaN");
+    return TW_OK;
+}
+
+int tw_solve_pyramids(tw_ctx* ctx, const tw_flow_settings* s, int32_t width, int32_t height, const float* x_levels,
+                      const float* y_levels, const float* mask_x, const float* mask_y, const float* user_d,
+                      const float* user_w, tw_flow* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    if (!s || !x_levels || !y_levels || !out || !out->data || width <= 0 || height <= 0)
+        return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    if (!mask_x != !mask_y) return ctx->fail(TW_ERR_BAD_PARAM, "solve_pyramids: the mask pyramids of both images, or none");
+    if (!user_d != !user_w) return ctx->fail(TW_ERR_BAD_PARAM, "solve_pyramids: the user displacement and its weights, or none");
+    if (s->wrap) return ctx->fail(TW_ERR_UNSUPPORTED, "the wrap-around (360) solve is not on the device");
+    Geo g;
+    CHECK(geometry(*s, width, height, &g, &ctx->err));
+    if (out->width != g.w || out->height != g.h) return ctx->fail(TW_ERR_MISMATCH, "flow buffer is not %dx%d", g.w, g.h);
+    size_t pf = pyramid_floats(g);
+    CHECK(ctx->ensure(ctx->pyr[0], 2 * pf * 4, "pyramid"));
+    CHECK(ctx->ensure(ctx->pyr[1], 2 * pf * 4, "pyramid"));
+    float* px_ = ctx->pyr[0].as<float>();
+    float* py_ = ctx->pyr[1].as<float>();
+    CHECK(ctx->cuda(cudaMemcpyAsync(px_, x_levels, pf * 4, cudaMemcpyHostToDevice, ctx->stream), "pyramid upload"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(py_, y_levels, pf * 4, cudaMemcpyHostToDevice, ctx->stream), "pyramid upload"));
+    // the transposed levels of the column sweeps, as build_pyramid_dev writes them beside the bands
+    size_t off = 0;
+    for (int i = 0; i < g.levels; i++) {
+        int lw = g.sizes[i][0], lh = g.sizes[i][1];
+        LAUNCHB(ctx, 16.0 * lw * lh, k_transpose2, dim3((lw + 31) / 32, (lh + 31) / 32), dim3(32, 8), 0, px_ + off, py_ + off,
+                px_ + pf + off, py_ + pf + off, lw, lh);
+        off += (size_t)lw * lh;
+    }
+    const float *mx = nullptr, *my = nullptr, *udu = nullptr, *udv = nullptr, *uww = nullptr;
+    if (mask_x) {
+        CHECK(ctx->ensure(ctx->masks, 2 * pf * sizeof(float), "mask pyramids"));
+        float* m = ctx->masks.as<float>();
+        CHECK(ctx->cuda(cudaMemcpyAsync(m, mask_x, pf * 4, cudaMemcpyHostToDevice, ctx->stream), "mask upload"));
+        CHECK(ctx->cuda(cudaMemcpyAsync(m + pf, mask_y, pf * 4, cudaMemcpyHostToDevice, ctx->stream), "mask upload"));
+        mx = m;
+        my = m + pf;
+    }
+    if (user_d) {  // UserLevel::d interleaved (dx, dy) and ::w per level -> the planes du, dv, w
+        CHECK(ctx->ensure(ctx->lay_in, 5 * pf * sizeof(float), "user displacement"));
+        float* u = ctx->lay_in.as<float>();
+        CHECK(ctx->cuda(cudaMemcpyAsync(u + 3 * pf, user_d, 2 * pf * 4, cudaMemcpyHostToDevice, ctx->stream), "user upload"));
+        CHECK(ctx->cuda(cudaMemcpyAsync(u + 2 * pf, user_w, pf * 4, cudaMemcpyHostToDevice, ctx->stream), "user upload"));
+        LAUNCH(ctx, k_deinterleave, grid1((long)pf), TB, 0, (const float*)(u + 3 * pf), (long)pf, u, u + pf);
+        udu = u;
+        udv = u + pf;
+        uww = u + 2 * pf;
+    }
+    int* flags = ctx->flags.as<int>();
+    CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
+    size_t fb = (size_t)g.w * g.h * 2 * sizeof(float);
+    CHECK(ctx->ensure(ctx->flow[0], fb, "flow"));
+    CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, *s, ctx->work[0], ctx->flow[0].as<float>(), flags + FL_ANY0,
+                             flags + FL_NAN, mx, my, udu, udv, uww));
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->flow[0].p, fb, cudaMemcpyDeviceToHost, ctx->stream), "flow download"));
     int hf[2];
     CHECK(finish(ctx, hf, 2));
