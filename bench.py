@@ -52,6 +52,7 @@ W, H = 1920, 1080
 SPEED = 40.0
 FRAMES_PER_STEP = 10
 METRIC = "1080p retime output frames/s (strict byte-exact GPU vs CPU)"
+METRIC_FAST = "1080p retime output frames/s (fast mode: FMA contraction, approximate division; PSNR vs CPU)"
 WORKLOAD = "retime 1920x1080 8bpc RGBA, speed 40%, defaults (vectors Best, Blend, sensitivity 70)"
 CLIP_KW = dict(seed=0x74570002, bg_velocity=(6.0, -3.0), square=240, square_start=(600.0, 400.0),
                square_velocity=(9.0, 4.0))
@@ -479,6 +480,8 @@ def main():
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling driver, no timing: renders the first 10 output frames of the 1080p workload once "
                          "(device resident clip) and exits; the command the committed ncu summaries name")
+    ap.add_argument("--fast", action="store_true",
+                    help="retime: the fast mode (tw_flow_settings.fast_mode); parity becomes PSNR against the strict render")
     ap.add_argument("--tune-cache", default=None,
                     help="--ncu-case: the autotuner's JSON table, read when present, written otherwise")
     ap.add_argument("--workload", default="retime", choices=["retime", "create-vectors", "fgbg", "adjoint", "batch"],
@@ -524,7 +527,7 @@ def main():
     stream = torch.cuda.current_stream()
     dev = tw.Device(local)
     dev.set_stream(stream.cuda_stream)
-    settings = tw.RetimeSettings()
+    settings = tw.RetimeSettings(flow=tw.FlowSettings(fast_mode=args.fast))
 
     # the autotuner's launch shapes for every level of the 1080p solve (measured once, before the
     # warm-up; the table only changes the time, never the bytes)
@@ -610,9 +613,12 @@ def main():
     threads = max(1, (os.cpu_count() or 1) // ws)
     glob = [lo + last_k * FRAMES_PER_STEP + j for j in range(FRAMES_PER_STEP)]
     want, cpu_dt = oracle_frames(frames_np, first, nframes, nclip, glob, threads)
-    equal = {"device": dev_out.tobytes() == want.tobytes(), "serial": serial_out.tobytes() == want.tobytes(),
-             "e2e": out_host.tobytes() == want.tobytes()}
-    ok = all(equal.values())
+    if not args.fast:
+        equal = {"device": dev_out.tobytes() == want.tobytes(), "serial": serial_out.tobytes() == want.tobytes(),
+                 "e2e": out_host.tobytes() == want.tobytes()}
+    else:  # the fast mode is not byte identical: its PSNR against the strict render, at least 45 dB
+        equal = {k: psnr(v, want) for k, v in (("device", dev_out), ("serial", serial_out), ("e2e", out_host))}
+    ok = all(equal.values()) if not args.fast else min(equal.values()) > 45.0
     if ws > 1:
         t = torch.tensor([0 if ok else 1], dtype=torch.int32, device=f"cuda:{local}")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -621,15 +627,19 @@ def main():
         ok_all = ok
     parity = {"frames": FRAMES_PER_STEP * ws, "equal": ok_all, "paths": equal,
               "sha256_rank0": hashlib.sha256(dev_out.tobytes()).hexdigest(),
-              "checked": "the last timed step's output frames of every rank, byte for byte against the oracle"}
+              "checked": "the last timed step's output frames of every rank, byte for byte against the oracle"
+                         if not args.fast else
+                         "fast mode: PSNR (dB) of the last timed step's output frames against the oracle's strict "
+                         "render, every path above 45 dB"}
 
     if rank == 0:
         peak, which = peaks()
         line = {
-            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "metric": METRIC if not args.fast else METRIC_FAST, "value": value, "unit": "frames/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "output_frames_per_step": FRAMES_PER_STEP * ws,
+            "config": {"workload": WORKLOAD + (", fast mode" if args.fast else ""),
+                       "output_frames_per_step": FRAMES_PER_STEP * ws,
                        "in_between_frames_per_step": sum(1 for s in step_sels if not s.exact),
                        "source_frames_resident": nframes, "frame_bytes": fs,
                        "l2": "flushed between steps (256 MiB write), inputs resident 0.5 GB > L2",
@@ -655,6 +665,12 @@ def main():
         torch.distributed.destroy_process_group()
     dev.close()
     return 0 if ok_all else 3
+
+
+def psnr(a, b):
+    d = a.astype(np.float64) - b.astype(np.float64)
+    mse = float(np.mean(d * d))
+    return 1e9 if mse == 0 else round(10.0 * math.log10(255.0 ** 2 / mse), 2)
 
 
 def oracle_frames(window, first, count, nclip, outputs, threads):
