@@ -6,9 +6,9 @@ namespace tw {
 
 void from_frame_dev(tw_ctx* ctx, const void* wire, void* eng, int W, int H, int fmt, bool flip) {
     long n = (long)W * H;
-    if (fmt == TW_U8) LAUNCH(ctx, k_from_frame_u8, grid1(n), TB, 0, (const uint8_t*)wire, (uint8_t*)eng, W, H, flip);
-    else if (fmt == TW_U16) LAUNCH(ctx, k_from_frame_u16, grid1(n), TB, 0, (const uint16_t*)wire, (uint16_t*)eng, W, H, flip);
-    else LAUNCH(ctx, k_from_frame_f32, grid1(n), TB, 0, (const float*)wire, (float*)eng, W, H, flip);
+    if (fmt == TW_U8) LAUNCHB(ctx, 2.0 * 4 * n, k_from_frame_u8, grid1(n), TB, 0, (const uint8_t*)wire, (uint8_t*)eng, W, H, flip);
+    else if (fmt == TW_U16) LAUNCHB(ctx, 2.0 * 8 * n, k_from_frame_u16, grid1(n), TB, 0, (const uint16_t*)wire, (uint16_t*)eng, W, H, flip);
+    else LAUNCHB(ctx, 2.0 * 16 * n, k_from_frame_f32, grid1(n), TB, 0, (const float*)wire, (float*)eng, W, H, flip);
 }
 
 // One output frame on lane L from two device-resident wire frames (nullptr = a blank frame outside
@@ -158,9 +158,9 @@ static int vectors_lane(tw_ctx* ctx, Lane& L, const tw_vectors_settings& s, int 
     }
     if (to_wire) {
         long n = (long)W * H;
-        if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)eng_out, (uint8_t*)out, W, H, flip);
-        else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)eng_out, (uint16_t*)out, W, H, flip);
-        else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)eng_out, (float*)out, W, H, flip);
+        if (fmt == TW_U8) LAUNCHB(ctx, 2.0 * 4 * n, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)eng_out, (uint8_t*)out, W, H, flip);
+        else if (fmt == TW_U16) LAUNCHB(ctx, 2.0 * 8 * n, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)eng_out, (uint16_t*)out, W, H, flip);
+        else LAUNCHB(ctx, 2.0 * 16 * n, k_to_frame_f32, grid1(n), TB, 0, (const float*)eng_out, (float*)out, W, H, flip);
     }
     CHECK(ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event"));
     return TW_OK;

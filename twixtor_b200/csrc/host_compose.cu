@@ -69,14 +69,16 @@ FillGeo fill_geometry(int w, int h) {  // holefill.rs:140-171
 void fill_passes(tw_ctx* ctx, float* src_dst, float* tmp, int w, int h, long stride, int planes, const Taps& t, int n,
                  bool above_first, int rule, const int* any) {
     dim3 g((unsigned)((w + TB - 1) / TB), (unsigned)h, (unsigned)planes);
-    LAUNCH(ctx, k_stack_pass, g, TB, 0, src_dst, tmp, w, h, stride, t, n, 0, rule, any);
-    LAUNCH(ctx, k_stack_pass, g, TB, 0, tmp, src_dst, w, h, stride, t, n, above_first ? 2 : 1, rule, any);
+    double pb = 8.0 * w * h * planes;  // every plane read once and written once
+    LAUNCHB(ctx, pb, k_stack_pass, g, TB, 0, src_dst, tmp, w, h, stride, t, n, 0, rule, any);
+    LAUNCHB(ctx, pb, k_stack_pass, g, TB, 0, tmp, src_dst, w, h, stride, t, n, above_first ? 2 : 1, rule, any);
 }
 
 void fill_resample(tw_ctx* ctx, const float* src, int sw, int sh, float* dst, int dw, int dh, int planes, int rule,
                    const int* any) {
     dim3 g((unsigned)((dw + TB - 1) / TB), (unsigned)dh, (unsigned)planes);
-    LAUNCH(ctx, k_stack_resample, g, TB, 0, src, sw, sh, (long)sw * sh, dst, dw, dh, (long)dw * dh, rule, any);
+    LAUNCHB(ctx, 4.0 * planes * ((double)sw * sh + (double)dw * dh), k_stack_resample, g, TB, 0, src, sw, sh, (long)sw * sh, dst,
+            dw, dh, (long)dw * dh, rule, any);
 }
 
 // The pull-push fill of an engine image in place (holefill.rs:260-350, :452-491) with the u8
@@ -532,9 +534,9 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
         const void* res = ran ? post : pre;
         long n = (long)W * H;
         if (to_wire) {
-            if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)res, (uint8_t*)out, W, H, flip_out);
-            else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)res, (uint16_t*)out, W, H, flip_out);
-            else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)res, (float*)out, W, H, flip_out);
+            if (fmt == TW_U8) LAUNCHB(ctx, 2.0 * 4 * n, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)res, (uint8_t*)out, W, H, flip_out);
+            else if (fmt == TW_U16) LAUNCHB(ctx, 2.0 * 8 * n, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)res, (uint16_t*)out, W, H, flip_out);
+            else LAUNCHB(ctx, 2.0 * 16 * n, k_to_frame_f32, grid1(n), TB, 0, (const float*)res, (float*)out, W, H, flip_out);
         } else if (!ran) {
             CHECK(ctx->cuda(cudaMemcpyAsync(out, pre, ib, cudaMemcpyDeviceToDevice, ctx->cur), "copy"));
         }
@@ -594,9 +596,9 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
                                     ws.cov[1]->as<uint8_t>(), cs.taps_above_first != 0, *ss, bad));
             if (to_wire) {
                 long n = (long)px;
-                if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)comp, (uint8_t*)out, W, H, flip_out);
-                else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)comp, (uint16_t*)out, W, H, flip_out);
-                else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)comp, (float*)out, W, H, flip_out);
+                if (fmt == TW_U8) LAUNCHB(ctx, 2.0 * 4 * n, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)comp, (uint8_t*)out, W, H, flip_out);
+                else if (fmt == TW_U16) LAUNCHB(ctx, 2.0 * 8 * n, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)comp, (uint16_t*)out, W, H, flip_out);
+                else LAUNCHB(ctx, 2.0 * 16 * n, k_to_frame_f32, grid1(n), TB, 0, (const float*)comp, (float*)out, W, H, flip_out);
             }
             return TW_OK;
         } else {
@@ -616,9 +618,9 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
         else CHECK(fill_dev(ctx, comp, W, H, fmt, ss->holes->as<uint8_t>(), ss->any_hole, cs.taps_above_first != 0, *ss->fill));
         if (to_wire) {
             long n = (long)px;
-            if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)comp, (uint8_t*)out, W, H, flip_out);
-            else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)comp, (uint16_t*)out, W, H, flip_out);
-            else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)comp, (float*)out, W, H, flip_out);
+            if (fmt == TW_U8) LAUNCHB(ctx, 2.0 * 4 * n, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)comp, (uint8_t*)out, W, H, flip_out);
+            else if (fmt == TW_U16) LAUNCHB(ctx, 2.0 * 8 * n, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)comp, (uint16_t*)out, W, H, flip_out);
+            else LAUNCHB(ctx, 2.0 * 16 * n, k_to_frame_f32, grid1(n), TB, 0, (const float*)comp, (float*)out, W, H, flip_out);
         }
         return TW_OK;
     }
@@ -705,7 +707,7 @@ int interpolate_dev(tw_ctx* ctx, const tw_selection& sel, const void* eng_a, con
             }
             LAUNCH(ctx, k_wb_noflow_f32, grid1(n), TB, 0, (const float*)eng_a, (const float*)eng_b, ws.wt[0]->as<float>(),
                    ws.wt[1]->as<float>(), gate, wb, (float)(1.0 - (double)wb), mode, (float*)eo, n);
-            if (to_wire) LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)eo, (float*)out, W, H, false);
+            if (to_wire) LAUNCHB(ctx, 2.0 * 16 * n, k_to_frame_f32, grid1(n), TB, 0, (const float*)eo, (float*)out, W, H, false);
             return TW_OK;
         }
     } else {
@@ -1049,9 +1051,9 @@ int tw_from_frame(tw_ctx* ctx, const void* wire, int32_t width, int32_t height, 
     CHECK(ctx->ensure(ctx->eng[0], bytes, "engine"));
     CHECK(ctx->cuda(cudaMemcpyAsync(ctx->wire[0].p, wire, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload"));
     long n = (long)width * height;
-    if (fmt == TW_U8) LAUNCH(ctx, k_from_frame_u8, grid1(n), TB, 0, ctx->wire[0].as<uint8_t>(), ctx->eng[0].as<uint8_t>(), width, height, false);
-    else if (fmt == TW_U16) LAUNCH(ctx, k_from_frame_u16, grid1(n), TB, 0, ctx->wire[0].as<uint16_t>(), ctx->eng[0].as<uint16_t>(), width, height, false);
-    else LAUNCH(ctx, k_from_frame_f32, grid1(n), TB, 0, ctx->wire[0].as<float>(), ctx->eng[0].as<float>(), width, height, false);
+    if (fmt == TW_U8) LAUNCHB(ctx, 2.0 * 4 * n, k_from_frame_u8, grid1(n), TB, 0, ctx->wire[0].as<uint8_t>(), ctx->eng[0].as<uint8_t>(), width, height, false);
+    else if (fmt == TW_U16) LAUNCHB(ctx, 2.0 * 8 * n, k_from_frame_u16, grid1(n), TB, 0, ctx->wire[0].as<uint16_t>(), ctx->eng[0].as<uint16_t>(), width, height, false);
+    else LAUNCHB(ctx, 2.0 * 16 * n, k_from_frame_f32, grid1(n), TB, 0, ctx->wire[0].as<float>(), ctx->eng[0].as<float>(), width, height, false);
     CHECK(ctx->cuda(cudaMemcpyAsync(engine_out, ctx->eng[0].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     int hf[1];
     return finish(ctx, hf, 1);
@@ -1067,9 +1069,9 @@ int tw_to_frame(tw_ctx* ctx, const void* engine, int32_t width, int32_t height, 
     CHECK(ctx->ensure(ctx->eng[0], bytes, "engine"));
     CHECK(ctx->cuda(cudaMemcpyAsync(ctx->eng[0].p, engine, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload"));
     long n = (long)width * height;
-    if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, ctx->eng[0].as<uint8_t>(), ctx->wire[0].as<uint8_t>(), width, height, false);
-    else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, ctx->eng[0].as<uint16_t>(), ctx->wire[0].as<uint16_t>(), width, height, false);
-    else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, ctx->eng[0].as<float>(), ctx->wire[0].as<float>(), width, height, false);
+    if (fmt == TW_U8) LAUNCHB(ctx, 2.0 * 4 * n, k_to_frame_u8, grid1(n), TB, 0, ctx->eng[0].as<uint8_t>(), ctx->wire[0].as<uint8_t>(), width, height, false);
+    else if (fmt == TW_U16) LAUNCHB(ctx, 2.0 * 8 * n, k_to_frame_u16, grid1(n), TB, 0, ctx->eng[0].as<uint16_t>(), ctx->wire[0].as<uint16_t>(), width, height, false);
+    else LAUNCHB(ctx, 2.0 * 16 * n, k_to_frame_f32, grid1(n), TB, 0, ctx->eng[0].as<float>(), ctx->wire[0].as<float>(), width, height, false);
     CHECK(ctx->cuda(cudaMemcpyAsync(wire_out, ctx->wire[0].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
     int hf[1];
     return finish(ctx, hf, 1);

@@ -708,9 +708,9 @@ int tw_retime_layers_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* 
             bool fp = s->motion_rows_reversed != 0;  // layers.rs:348-351: points on the motion path's rows
             if (nfg > 0) CHECK(layers_dev(ctx, *s, sel, *job, mat, W, H, fmt, &res, pts, npts, fp));
             else CHECK(vector_frame_dev(ctx, *s, sel, W, H, fmt, res, pts, npts ? npts[0] : 0, fp));  // compose.rs:155-164
-            if (fmt == TW_U8) LAUNCH(ctx, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)res, ctx->wire[2].as<uint8_t>(), W, H, flip);
-            else if (fmt == TW_U16) LAUNCH(ctx, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)res, ctx->wire[2].as<uint16_t>(), W, H, flip);
-            else LAUNCH(ctx, k_to_frame_f32, grid1(n), TB, 0, (const float*)res, ctx->wire[2].as<float>(), W, H, flip);
+            if (fmt == TW_U8) LAUNCHB(ctx, 2.0 * 4 * n, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)res, ctx->wire[2].as<uint8_t>(), W, H, flip);
+            else if (fmt == TW_U16) LAUNCHB(ctx, 2.0 * 8 * n, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)res, ctx->wire[2].as<uint16_t>(), W, H, flip);
+            else LAUNCHB(ctx, 2.0 * 16 * n, k_to_frame_f32, grid1(n), TB, 0, (const float*)res, ctx->wire[2].as<float>(), W, H, flip);
         }
         CHECK(ctx->cuda(cudaMemcpyAsync(dst, ctx->wire[2].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
         CHECK(layers_status(ctx));
