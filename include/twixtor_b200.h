@@ -188,6 +188,13 @@ int tw_tuning_set(tw_ctx* ctx, int32_t width, int32_t height, int32_t iter_tile,
                   int32_t bm_rows_threads, int32_t bm_cols_threads);
 int tw_tuning_clear(tw_ctx* ctx);
 
+/* CUDA graphs of the per-frame pipeline of the clip calls (on by default): a lane captures the
+ * pipeline of an in-between frame (warping code 0 with Nearest or Blend, both source frames in the
+ * clip, no Blur Compensation) the second time it renders a frame of that shape, then replays the
+ * graph for every later one, updating only the kernel arguments that changed (the source and output
+ * frames, the blend weights). The bytes do not depend on it. 0 turns it off and drops the graphs. */
+int tw_set_graphs(tw_ctx* ctx, int32_t on);
+
 /* Makes the context enqueue on `stream` (a cudaStream_t; NULL is the legacy default stream)
  * instead of its own, so a caller can order the library's work with its own and time it with its
  * own events. */

@@ -126,3 +126,32 @@ def test_fgbg_clip_1080p_five_frames_matches_oracle(dev):
     got = dev.retime_layers_clip(s, frames, nframes, mattes, [1, 1, 1], sens, sels, W, H, 0)
     want = O.retime_fgbg_clip(frames, nframes, mattes, [1, 1, 1], [70.0] * 3, W, H, 0, O.retime_params(speed=SPEED), 5)
     assert same(got, want)
+
+
+@pytest.mark.parametrize("lanes,size,nout", [(1, (160, 96), 24), (2, (320, 180), 20), (4, (1920, 1080), 16)])
+def test_graph_replay_matches_direct_launches(dev, lanes, size, nout):
+    """The clip call with CUDA graphs (captured at a lane's second frame of a shape, replayed with
+    updated arguments after) against the same call with graphs off and against the oracle."""
+    import torch
+    w, h = size
+    nframes = int(np.ceil(0.4 * nout)) + 2
+    kw = CLIP_KW if w == 1920 else dict(seed=w + h)
+    frames = synth.moving_clip(w, h, nframes, depth=8, **kw)
+    tp = tw.TimeParams(speed_percent=SPEED)
+    sels = [tw.select(tp, n, w, h) for n in range(nout)]
+    d_in = torch.from_numpy(frames).cuda()
+    outs = []
+    dev.set_lanes(lanes)
+    try:
+        for graphs in (True, False, True):
+            dev.set_graphs(graphs)
+            d_out = torch.zeros(nout * w * h * 4, dtype=torch.uint8, device="cuda")
+            torch.cuda.synchronize()
+            dev.retime_clip_device(tw.RetimeSettings(), d_in.data_ptr(), nframes, sels, w, h, 0, d_out.data_ptr())
+            outs.append(d_out.cpu().numpy())
+    finally:
+        dev.set_lanes(4)
+        dev.set_graphs(True)
+    want = O.retime_clip(frames, nframes, w, h, 0, O.retime_params(speed=SPEED), nout)
+    for o in outs:
+        assert same(o, want)

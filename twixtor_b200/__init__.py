@@ -314,6 +314,7 @@ def library():
     L.tw_stats.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.tw_set_stream.argtypes = [P, P]
     L.tw_debug_inject.argtypes = [P, i32, i32]
+    L.tw_set_graphs.argtypes = [P, i32]
     L.tw_autotune.argtypes = [P, ctypes.POINTER(_FlowSettings), i32, i32, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32)]
     L.tw_tuning_table.argtypes = [P, ctypes.c_char_p, ctypes.c_size_t]
     L.tw_tuning_table.restype = ctypes.c_size_t
@@ -501,6 +502,10 @@ class Device:
 
     def tuning_clear(self):
         self._check(self._L.tw_tuning_clear(self._h))
+
+    def set_graphs(self, on: bool):
+        """CUDA graphs of the clip calls' per-frame pipeline (tw_set_graphs; on by default)."""
+        self._check(self._L.tw_set_graphs(self._h, int(bool(on))))
 
     def debug_inject(self, kind: int, n: int = 1):
         """Arms a host-injected failure (tw_debug_inject): INJECT_ALLOC fails the n-th device

@@ -14,7 +14,7 @@ void from_frame_dev(tw_ctx* ctx, const void* wire, void* eng, int W, int H, int 
 // One output frame on lane L from two device-resident wire frames (nullptr = a blank frame outside
 // the clip); writes the output wire frame to out_wire (device). Both lane streams must already be
 // ordered after the caller's work (ctx->ev_start); the frame's end is L.ev_done on stream 0.
-static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, const tw_selection& sel, const void* wa,
+static int retime_frame_body(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, const tw_selection& sel, const void* wa,
                              const void* wb, int W, int H, int fmt, void* out_wire) {
     size_t bytes = (size_t)W * H * 4 * sample_bytes(fmt);
     int* flags = L.flags.as<int>();
@@ -22,8 +22,14 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
     CHECK(ctx->ensure(L.eng[1], bytes, "engine B"));
     bool vector = sel.vectors_quality != 0 && !sel.exact;
     bool flip = vector && s.motion_rows_reversed != 0;
-    // stream 1 reuses this lane's buffers: it waits for the lane's previous frame
-    if (L.used) CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[1], L.ev_done, 0), "lane order"));
+    // stream 1 reuses this lane's buffers: it waits for the lane's previous frame (a captured frame
+    // forks stream 1 from stream 0 instead: the graph runs after the lane's previous work on stream 0)
+    if (ctx->gmode == GRAPH_CAPTURE) {
+        CHECK(ctx->cuda(cudaEventRecord(L.ev_fork, L.s[0]), "event"));
+        CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[1], L.ev_fork, 0), "event"));
+    } else if (ctx->gmode == GRAPH_OFF && L.used) {
+        CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[1], L.ev_done, 0), "lane order"));
+    }
     L.used = true;
     // a frame outside the clip is blank (host.rs:338-352); blank images are all zero in every depth
     ctx->cur = L.s[0];
@@ -59,12 +65,12 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
     CHECK(ctx->ensure(L.flow[1], fb, "flow"));
     ctx->cur = L.s[0];
     CHECK(build_pyramid_dev(ctx, L.eng[0].p, W, H, fmt, fs, g, px_, px_ + pf, L.scratch[0]));
-    CHECK(ctx->cuda(cudaEventRecord(L.ev_pyr[0], L.s[0]), "event"));
+    CHECK(GOP(ctx, ctx->cuda(cudaEventRecord(L.ev_pyr[0], L.s[0]), "event")));
     ctx->cur = L.s[1];
     CHECK(build_pyramid_dev(ctx, L.eng[1].p, W, H, fmt, fs, g, py_, py_ + pf, L.scratch[1]));
-    CHECK(ctx->cuda(cudaEventRecord(L.ev_pyr[1], L.s[1]), "event"));
-    CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_pyr[1], 0), "event"));
-    CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[1], L.ev_pyr[0], 0), "event"));
+    CHECK(GOP(ctx, ctx->cuda(cudaEventRecord(L.ev_pyr[1], L.s[1]), "event")));
+    CHECK(GOP(ctx, ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_pyr[1], 0), "event")));
+    CHECK(GOP(ctx, ctx->cuda(cudaStreamWaitEvent(L.s[1], L.ev_pyr[0], 0), "event")));
     bool need_ab = true, need_ba = true;
     if (sel.interp == 0) {
         bool use_ab = (sel.wa < 0.5f && (unsigned)s.compose.warp_mode < 2) || (0.5f <= sel.wa && (unsigned)s.compose.warp_mode > 1);
@@ -83,8 +89,8 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
         CHECK(solve_pyramids_dev(ctx, py_, px_, py_ + pf, px_ + pf, g, fs, L.work[1], L.flow[1].as<float>(),
                                  flags + FL_ANY1, flags + FL_NAN));
     }
-    CHECK(ctx->cuda(cudaEventRecord(L.ev_solve1, L.s[1]), "event"));
-    CHECK(ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_solve1, 0), "event"));
+    CHECK(GOP(ctx, ctx->cuda(cudaEventRecord(L.ev_solve1, L.s[1]), "event")));
+    CHECK(GOP(ctx, ctx->cuda(cudaStreamWaitEvent(L.s[0], L.ev_solve1, 0), "event")));
     ctx->cur = L.s[0];
     WbScratch wbs = wb_scratch(L.wb_wt, L.wb_tmp, L.wb_mask, L.wb_cov);
     SmartScratch ss{&L.comp, &L.holes, &L.fill, flags + FL_HOLE, flags + FL_SIDE1, &wbs, flags + FL_WB, &L.pre_blur};
@@ -92,8 +98,87 @@ static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, 
                       need_ba ? L.flow[1].as<float>() : nullptr, g.w, g.h, W, H, fmt, out_wire, true, flip,
                       flags + FL_BAD, &ss));
     if (ctx->inject_now(TW_INJECT_STATUS)) LAUNCH(ctx, k_set_flag, 1, 1, 0, flags, FL_BOUND);
-    CHECK(ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event"));
+    if (ctx->gmode == GRAPH_OFF) CHECK(ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event"));
     return TW_OK;
+}
+
+// The shape of a frame that decides every launch and stream operation of its pipeline: the frame
+// size and depth, the settings, and the selection's vector quality, interpolation and flow choice.
+static std::string frame_key(const tw_retime_settings& s, const tw_selection& sel, int W, int H, int fmt) {
+    int v[6] = {W, H, fmt, sel.vectors_quality, sel.interp, sel.interp == 0 ? (sel.wa < 0.5f ? 1 : 2) : 0};
+    std::string k((const char*)v, sizeof v);
+    k.append((const char*)&s, sizeof s);
+    return k;
+}
+
+// One output frame on lane L (retime_frame_body), as a CUDA graph where the frame allows it: the
+// vector path of warping code 0 with Nearest or Blend, both source frames in the clip, no Blur
+// Compensation. The first frame of a shape runs as it is (its buffers come to exist), the second is
+// captured into the lane's graph of that shape, and every later one re-issues the same host code
+// in replay mode, which launches nothing and updates the kernel nodes whose arguments changed (the
+// source and output frames, the blend weights), then launches the graph on the lane's first stream.
+static int retime_frame_lane(tw_ctx* ctx, Lane& L, const tw_retime_settings& s, const tw_selection& sel, const void* wa,
+                             const void* wb, int W, int H, int fmt, void* out_wire) {
+    bool vector = sel.vectors_quality != 0 && !sel.exact;
+    bool eligible = ctx->graphs_on && !ctx->serial && !ctx->prof.on && ctx->inject_kind == 0 && vector && wa && wb &&
+                    s.compose.warp_mode == 0 && (sel.interp == 0 || sel.interp == 1) && !((double)s.compose.blur > 0.005) &&
+                    !s.flow.wrap && !s.compose.wrap_360;
+    if (!eligible) return retime_frame_body(ctx, L, s, sel, wa, wb, W, H, fmt, out_wire);
+    FrameGraph& G = L.graphs[frame_key(s, sel, W, H, fmt)];
+    if (G.exec && G.alloc_gen != ctx->alloc_gen) {  // a buffer moved since the capture
+        drop_graph(G);
+        G.seen = true;
+    }
+    if (!G.seen) {
+        G.seen = true;
+        return retime_frame_body(ctx, L, s, sel, wa, wb, W, H, fmt, out_wire);
+    }
+    if (!G.exec) {  // capture
+        ctx->gmode = GRAPH_CAPTURE;
+        ctx->gcur = &G;
+        ctx->gfail = false;
+        cudaError_t e = cudaStreamBeginCapture(L.s[0], cudaStreamCaptureModeRelaxed);
+        int rc = e == cudaSuccess ? retime_frame_body(ctx, L, s, sel, wa, wb, W, H, fmt, out_wire) : TW_OK;
+        cudaGraph_t g = nullptr;
+        cudaError_t e2 = e == cudaSuccess ? cudaStreamEndCapture(L.s[0], &g) : e;
+        bool failed = ctx->gfail || e != cudaSuccess || e2 != cudaSuccess || !g;
+        ctx->gmode = GRAPH_OFF;
+        ctx->gcur = nullptr;
+        ctx->gfail = false;
+        if (!failed) {
+            G.graph = g;
+            failed = cudaGraphInstantiate(&G.exec, g, 0) != cudaSuccess;
+        } else if (g) {
+            cudaGraphDestroy(g);
+        }
+        if (rc || failed) {  // nothing of the frame ran: drop the graph for good, issue it directly
+            cudaGetLastError();
+            drop_graph(G);
+            G.seen = true;
+            ctx->graphs_on = rc ? ctx->graphs_on : false;
+            if (rc) return rc;
+            return retime_frame_body(ctx, L, s, sel, wa, wb, W, H, fmt, out_wire);
+        }
+        G.alloc_gen = ctx->alloc_gen;
+    } else {  // replay
+        ctx->gmode = GRAPH_REPLAY;
+        ctx->gcur = &G;
+        ctx->gi = 0;
+        ctx->gfail = false;
+        int rc = retime_frame_body(ctx, L, s, sel, wa, wb, W, H, fmt, out_wire);
+        bool ok = !ctx->gfail && ctx->gi == G.nodes.size() && G.alloc_gen == ctx->alloc_gen;
+        ctx->gmode = GRAPH_OFF;
+        ctx->gcur = nullptr;
+        ctx->gfail = false;
+        if (rc) return rc;
+        if (!ok) {
+            drop_graph(G);
+            G.seen = true;
+            return retime_frame_body(ctx, L, s, sel, wa, wb, W, H, fmt, out_wire);
+        }
+    }
+    CHECK(ctx->cuda(cudaGraphLaunch(G.exec, L.s[0]), "graph launch"));
+    return ctx->cuda(cudaEventRecord(L.ev_done, L.s[0]), "event");
 }
 
 // The Create Vectors pass on lane L (create_vectors.rs:162-183): the engine images X and Y are in

@@ -25,6 +25,58 @@ void prof_mark(tw_ctx* ctx) {
 
 __global__ void k_set_flag(int* flags, int idx) { flags[idx] = 1; }
 
+// A kernel launch while a lane captures its frame graph (launched into the capture; its node and
+// arguments recorded) or replays it (nothing launched: the node's arguments are updated in the
+// executable graph when they differ from the last ones). A launch that does not line up with the
+// captured graph marks the replay as failed, and the frame is issued again without the graph.
+void graph_kernel(tw_ctx* ctx, const void* func, dim3 grid, dim3 block, size_t smem, void** argv, std::string&& packed) {
+    FrameGraph* G = ctx->gcur;
+    if (ctx->gfail || !G) return;
+    if (ctx->gmode == GRAPH_CAPTURE) {
+        if (cudaLaunchKernel(func, grid, block, argv, smem, ctx->cur) != cudaSuccess) {
+            ctx->gfail = true;
+            return;
+        }
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        if (cudaStreamGetCaptureInfo(ctx->cur, &st, nullptr, nullptr, &deps, &nd) != cudaSuccess || nd != 1 ||
+            st != cudaStreamCaptureStatusActive) {
+            ctx->gfail = true;
+            return;
+        }
+        G->nodes.push_back(deps[0]);
+        G->funcs.push_back(func);
+        G->args.push_back(std::move(packed));
+        return;
+    }
+    size_t i = ctx->gi++;
+    if (i >= G->nodes.size() || G->funcs[i] != func) {
+        ctx->gfail = true;
+        return;
+    }
+    if (G->args[i] != packed) {
+        cudaKernelNodeParams kp{};
+        kp.func = (void*)func;
+        kp.gridDim = grid;
+        kp.blockDim = block;
+        kp.sharedMemBytes = (unsigned)smem;
+        kp.kernelParams = argv;
+        kp.extra = nullptr;
+        if (cudaGraphExecKernelNodeSetParams(G->exec, G->nodes[i], &kp) != cudaSuccess) {
+            ctx->gfail = true;
+            return;
+        }
+        G->args[i] = std::move(packed);
+    }
+}
+
+void drop_graph(FrameGraph& G) {
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    if (G.graph) cudaGraphDestroy(G.graph);
+    G = FrameGraph();
+}
+
 __global__ void k_selfcheck(int* out) {
     // the x86 truncation rules the strict kernels rely on
     float vals[6] = {-2.5f, 2.5f, 2147483648.0f, -2147483904.0f, __int_as_float(0x7fc00000), -0.0f};
@@ -91,6 +143,7 @@ int lane_ready(tw_ctx* ctx, Lane& L) {
         }
         CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_solve1, cudaEventDisableTiming), "lane event"));
         CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming), "lane event"));
+        CHECK(ctx->cuda(cudaEventCreateWithFlags(&L.ev_fork, cudaEventDisableTiming), "lane event"));
         CHECK(ctx->ensure(L.flags, FLAGS_BYTES, "lane flags"));
     }
     for (int i = 0; i < 2; i++) L.s[i] = ctx->serial ? ctx->stream : L.own[i];
@@ -218,6 +271,8 @@ void tw_close(tw_ctx* ctx) {
     for (int i = 0; i < 2; i++) { ctx->pyr[i].release(&ctx->held); ctx->work[i].release(&ctx->held); ctx->flow[i].release(&ctx->held); }
     for (int i = 0; i < 4; i++) ctx->plane[i].release(&ctx->held);
     for (auto& L : ctx->lanes) {
+        for (auto& kv : L.graphs) drop_graph(kv.second);
+        if (L.ev_fork) cudaEventDestroy(L.ev_fork);
         for (int i = 0; i < 2; i++) {
             L.eng[i].release(&ctx->held); L.pyr[i].release(&ctx->held); L.work[i].release(&ctx->held);
             L.flow[i].release(&ctx->held);
@@ -360,6 +415,16 @@ int tw_debug_inject(tw_ctx* ctx, int32_t kind, int32_t n) {
         return ctx->fail(TW_ERR_BAD_PARAM, "failure injection: kind %d with count %d", kind, n);
     ctx->inject_kind = kind;
     ctx->inject_n = kind == TW_INJECT_NONE ? 0 : n;
+    return TW_OK;
+}
+
+int tw_set_graphs(tw_ctx* ctx, int32_t on) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->graphs_on = on != 0;
+    if (!ctx->graphs_on)
+        for (auto& L : ctx->lanes)
+            for (auto& kv : L.graphs) drop_graph(kv.second);
     return TW_OK;
 }
 

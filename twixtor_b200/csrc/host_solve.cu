@@ -344,9 +344,9 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
     size_t off = 0;
     for (int i = 0; i < g.levels; i++) { offs[i] = off; off += (size_t)g.sizes[i][0] * g.sizes[i][1]; }
     long ns = (long)g.sizes[start][0] * g.sizes[start][1];
-    CHECK(ctx->cuda(cudaMemsetAsync(fu, 0, ns * sizeof(float), ctx->cur), "flow init"));
-    CHECK(ctx->cuda(cudaMemsetAsync(fv, 0, ns * sizeof(float), ctx->cur), "flow init"));
-    CHECK(ctx->cuda(cudaMemsetAsync(any, 0, 32 * sizeof(int), ctx->cur), "range flags"));
+    CHECK(GOP(ctx, ctx->cuda(cudaMemsetAsync(fu, 0, ns * sizeof(float), ctx->cur), "flow init")));
+    CHECK(GOP(ctx, ctx->cuda(cudaMemsetAsync(fv, 0, ns * sizeof(float), ctx->cur), "flow init")));
+    CHECK(GOP(ctx, ctx->cuda(cudaMemsetAsync(any, 0, 32 * sizeof(int), ctx->cur), "range flags")));
     bool af = s.taps_above_first != 0;
     bool damp_any = std::fabs((double)damp - 1.0) >= 1e-6;
     const bool fast = s.fast_mode != 0;

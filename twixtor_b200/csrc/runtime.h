@@ -12,6 +12,8 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
+#include <utility>
 #include <vector>
 
 #include "../../include/twixtor_b200.h"
@@ -85,7 +87,23 @@ struct KernelProfile {
 // One set of buffers for one output frame in flight, with two streams: the two pyramids and the
 // two solves of a pair run concurrently (stream 0: A's pyramid, solve(A, B), the composition;
 // stream 1: B's pyramid, solve(B, A)). Several lanes keep several output frames in flight.
+// A captured per-frame pipeline of one lane (CUDA graph): its executable graph, the captured graph
+// that owns the nodes, and each kernel node in launch order with its function and arguments (the last
+// ones set), so that a later frame of the same shape updates only the nodes whose arguments changed.
+struct FrameGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaGraphNode_t> nodes;
+    std::vector<const void*> funcs;
+    std::vector<std::string> args;
+    uint64_t alloc_gen = 0;  // the context's allocation generation at capture (buffers moved since: stale)
+    bool seen = false;       // a frame of this shape ran once without a graph (its buffers exist)
+};
+enum { GRAPH_OFF = 0, GRAPH_CAPTURE = 1, GRAPH_REPLAY = 2 };
+
 struct Lane {
+    std::map<std::string, FrameGraph> graphs;  // by frame shape
+    cudaEvent_t ev_fork = nullptr;             // the second stream's entry into a capture
     cudaStream_t s[2] = {nullptr, nullptr};    // the streams this call uses: own[] or, serial, the context's
     cudaStream_t own[2] = {nullptr, nullptr};  // the lane's own streams
     cudaEvent_t ev_pyr[2] = {nullptr, nullptr};  // pyramid of A / B done
@@ -107,6 +125,14 @@ struct tw_ctx {
     Lane lanes[MAX_LANES];
     int nlanes = 4;  // output frames in flight in the clip calls (tw_set_lanes)
     std::map<uint64_t, LevelTune> tune_table;  // (w << 32 | h) -> the measured launch shapes of that level size
+    // CUDA graphs of the per-frame pipeline (tw_set_graphs): the mode of the launches being issued,
+    // the graph they go to, the next kernel node of a replay, and a failure seen on the way
+    bool graphs_on = true;
+    int gmode = GRAPH_OFF;
+    FrameGraph* gcur = nullptr;
+    size_t gi = 0;
+    bool gfail = false;
+    uint64_t alloc_gen = 0;  // counts the device (re)allocations of the context's buffers
     bool serial = false;  // tw_set_lanes(ctx, 0): one lane whose work all runs on the context's stream
     cudaEvent_t ev_start = nullptr;
     // tw_retime_clip: a device cache of source frames, and the copy streams
@@ -166,6 +192,7 @@ struct tw_ctx {
     int ensure(DevBuf& b, size_t n, const char* what) {
         if (n > b.cap && inject_now(TW_INJECT_ALLOC))  // the buffer is left as it was, as a failed cudaMalloc leaves it
             return fail(TW_ERR_CUDA, "%s: out of memory (injected allocation failure)", what);
+        if (n > b.cap) alloc_gen++;  // a buffer moves: captured graphs that name it are stale
         return cuda(b.ensure(n, &held), what);
     }
 };
@@ -181,11 +208,39 @@ namespace tw {
 bool prof_match(tw_ctx* ctx, const char* kernel);
 void prof_mark(tw_ctx* ctx);
 
+// A kernel launch while a lane captures or replays its frame graph (host_context.cu).
+void graph_kernel(tw_ctx* ctx, const void* func, dim3 grid, dim3 block, size_t smem, void** argv, std::string&& packed);
+void drop_graph(FrameGraph& G);
+
+template <typename T, size_t... I>
+void launch_tuple(tw_ctx* ctx, const void* k, dim3 grid, dim3 block, size_t smem, T& t, std::index_sequence<I...>) {
+    void* argv[] = {(void*)&std::get<I>(t)..., nullptr};
+    if (ctx->gmode == GRAPH_OFF) {
+        cudaLaunchKernel(k, grid, block, argv, smem, ctx->cur);
+        return;
+    }
+    std::string packed;
+    (packed.append((const char*)&std::get<I>(t), sizeof(std::get<I>(t))), ...);
+    graph_kernel(ctx, k, grid, block, smem, argv, std::move(packed));
+}
+
+// One kernel launch: the arguments converted to the kernel's own parameter types, then launched on
+// ctx->cur, or recorded into / updated in the lane's frame graph.
+template <typename... P, typename... A>
+void launch_kernel(tw_ctx* ctx, void (*k)(P...), dim3 grid, dim3 block, size_t smem, A&&... a) {
+    std::tuple<P...> t(static_cast<P>(std::forward<A>(a))...);
+    launch_tuple(ctx, (const void*)k, grid, block, smem, t, std::index_sequence_for<P...>{});
+}
+
+// A stream operation of the per-frame pipeline other than a kernel (a memset, an event): issued
+// normally and while capturing (it becomes a node of the graph), skipped while replaying.
+#define GOP(ctx, expr) ((ctx)->gmode == GRAPH_REPLAY ? (int)TW_OK : (expr))
+
 #define LAUNCHB(ctx, nbytes_, kernel, grid, block, smem, ...)                        \
     do {                                                                           \
         bool _p = prof_match((ctx), #kernel);                                      \
         if (_p) prof_mark(ctx);                                                    \
-        kernel<<<(grid), (block), (smem), (ctx)->cur>>>(__VA_ARGS__);              \
+        launch_kernel((ctx), kernel, dim3(grid), dim3(block), (size_t)(smem), __VA_ARGS__); \
         (ctx)->launches++;                                                         \
         if (_p) {                                                                  \
             prof_mark(ctx);                                                        \
