@@ -1056,3 +1056,206 @@ int or_create_vectors_clip(const void* frames, int nframes, int w, int h, int fm
 }
 
 }  // extern "C"
+
+// ---- Vectors In (plugins/vectors-in: glue.rs:440-495, vectorin.rs, timemap.rs) ----------------------
+
+extern "C" {
+
+// Parameters of one `vectors-in` render (plugins/vectors-in/src/lib.rs), popups 1-based. In FPS is
+// Out FPS is on (the input rate 30, the output rate the composition's: timemap.rs, glue.rs:204-215).
+struct or_vecin_params {
+    int fps_num, fps_den;      // composition rate (--fps)
+    int quality_high;
+    double speed_percent;      // constant Speed %
+    int nkeys;                 // keyed Speed % (0: constant)
+    const double* key_frames;
+    const double* key_values;
+    const int* key_ease;
+    int frame_interp;          // popup 1..3
+    int warping;               // popup: 1 Inverse, 2 Forward (glue.rs:94-100)
+    double blur_compensation;
+    double max_displace;       // Vectors: Max Displace
+    double vec_scale_x, vec_scale_y;
+    // the orders of the plugin's render (glue.rs:44-63): bottom-up rows, the tap above first in the
+    // vertical passes of the fills, the Gouraud forward warp
+    int rows_reversed;
+    int taps_above_first;
+    int gouraud;
+    // the presence of a vector layer: 0 a set layer is present at every time (vectorin.rs:41-58,
+    // the reference's current code); 1 present only where its clip has a frame at the output
+    // frame's time, the error fill when neither is (the revision the parity grid records)
+    int probe_current_time;
+};
+
+// compose/vector.rs:329-345 (flow_from_vector_image_with) over an engine image, for the tests
+int or_flow_from_vectors(const void* vec_eng, int w, int h, int fmt, float max_displace, float sx, float sy,
+                         int above_first, float* flow_out) {
+    Image v(w, h, (Fmt)fmt);
+    std::memcpy(v.data(), vec_eng, v.bytes());
+    FlowField f;
+    std::string e;
+    int rc = flow_from_vector_image(v, max_displace, sx, sy, above_first != 0, &f, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(flow_out, f.d.data(), f.d.size() * sizeof(float));
+    return 0;
+}
+
+// vectors.rs:474-522 alone
+int or_decode_vectors(const void* vec_eng, int w, int h, int fmt, float max_displace, float* flow_out) {
+    Image v(w, h, (Fmt)fmt);
+    std::memcpy(v.data(), vec_eng, v.bytes());
+    FlowField f = decode_vectors(v, max_displace);
+    std::memcpy(flow_out, f.d.data(), f.d.size() * sizeof(float));
+    return 0;
+}
+
+// holefill.rs:497-518 on an interleaved flow in place
+int or_fill_flow_holes(float* flow, int w, int h, const void* mask, int mask_kind, int above_first) {
+    FlowField f(w, h);
+    std::memcpy(f.d.data(), flow, f.d.size() * sizeof(float));
+    std::string e;
+    int rc = fill_flow_holes(f, mask, mask_kind, above_first != 0, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(flow, f.d.data(), f.d.size() * sizeof(float));
+    return 0;
+}
+
+// compose/vector.rs:370-397
+int or_invert_flow(const float* flow, int w, int h, int pyramid, int above_first, float* out) {
+    FlowField f(w, h), o;
+    std::memcpy(f.d.data(), flow, f.d.size() * sizeof(float));
+    std::string e;
+    int rc = invert_flow(f, pyramid != 0, above_first != 0, &o, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(out, o.d.data(), o.d.size() * sizeof(float));
+    return 0;
+}
+
+// vectorin.rs:125-155 on an engine image in place
+void or_matte_step(void* eng, int w, int h, int fmt, const float* matte) {
+    Image v(w, h, (Fmt)fmt);
+    std::memcpy(v.data(), eng, v.bytes());
+    matte_step(v, std::vector<float>(matte, matte + (size_t)w * h));
+    std::memcpy(eng, v.data(), v.bytes());
+}
+
+// Output frame n of the single layer `vectors-in` render (glue.rs:386-495 with nfg 0, Display not
+// Source): the footage clip `frames` (nframes wire frames), the vector layers `Vectors: Next` and
+// `Vectors: Prev` as wire clips of n_next / n_prev frames (NULL: the layer is not set; a frame past
+// a set layer's end is transparent, vectorin.rs:41-58). F_AB is Next at T(A), F_BA Prev at T(B)
+// (vectorin.rs:203-227); a missing one is the other's inversion when the composition reads it
+// (compose/vector.rs:422-447). No vector layer: the plugin's size mismatch error fill.
+int or_vectors_in_one(const void* frames, int nframes, const void* vec_next, int n_next, const void* vec_prev, int n_prev,
+                      int w, int h, int fmt, const or_vecin_params* p, int n, void* out) {
+    Fmt f = (Fmt)fmt;
+    size_t es = f == U8 ? 1 : f == U16 ? 2 : 4;
+    size_t frame_bytes = (size_t)w * h * 4 * es;
+    if (p->probe_current_time) {  // the layer's clip at the output frame's time (clip index n)
+        if (vec_next && (n < 0 || n >= n_next)) vec_next = nullptr;
+        if (vec_prev && (n < 0 || n >= n_prev)) vec_prev = nullptr;
+    }
+    if (!vec_next && !vec_prev) {
+        // the size mismatch error fill (image.rs:388-425), straight to the wire: red, alpha half
+        size_t np = (size_t)w * h;
+        if (f == U8) {
+            uint8_t* o = (uint8_t*)out;
+            for (size_t i = 0; i < np; i++) { o[i * 4] = 0xff; o[i * 4 + 1] = 0; o[i * 4 + 2] = 0; o[i * 4 + 3] = 0x80; }
+        } else if (f == U16) {
+            uint16_t* o = (uint16_t*)out;  // q15_to_u16 of 0x8000 and 0x4000 (crates/fx-core/src/frame.rs:139-141)
+            for (size_t i = 0; i < np; i++) { o[i * 4] = 65535; o[i * 4 + 1] = 0; o[i * 4 + 2] = 0; o[i * 4 + 3] = 32768; }
+        } else {
+            float* o = (float*)out;  // planes G, B, R, A
+            for (size_t i = 0; i < np; i++) { o[i] = 0.0f; o[np + i] = 0.0f; o[2 * np + i] = 1.0f; o[3 * np + i] = 0.5f; }
+        }
+        return 0;
+    }
+    // the time model: plugin 01's Speed map with the plugin's rates (in 30, out the composition's)
+    bool integer = p->fps_den == 1;
+    int time_step = integer ? 100 : p->fps_den;
+    double comp = (double)p->fps_num / (double)p->fps_den;
+    TimeMap map;
+    map.lts = time_step;
+    map.in_fps = 30.0;
+    map.out_fps = comp;
+    map.dur = (float)(((double)time_step * comp) / 30.0);
+    map.speed.constant = p->speed_percent;
+    for (int i = 0; i < p->nkeys; i++) {
+        long long t = (long long)std::llround(p->key_frames[i] * (double)time_step);
+        map.speed.keys.push_back({t, p->key_values[i], p->key_ease && p->key_ease[i] != 0});
+    }
+    int cur = n * time_step;
+    float t0 = (float)cur / (float)time_step;
+    float t1 = ((float)time_step + (float)cur) / (float)time_step;
+    Selection sel;
+    sel.s0 = map.src_pos(t0);
+    sel.s1 = map.src_pos(t1);
+    float blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
+    sel.a = cvtt_i32_f(sel.s0);
+    sel.b = sel.a + 1;
+    sel.wa = 1.0f - (sel.s0 - (float)sel.a);
+    sel.exact = exact_position(sel.s0, sel.s1, blur);
+    sel.vectors_quality = (w >= 2 && h >= 2) ? 4 : 0;
+    sel.interp = p->frame_interp - 1;
+    // T(k) = trunc(dur * k + 0.5) (timemap.rs:45-50), then the clip frame of that tick
+    auto clip_index = [&](int pos) -> long long {
+        int time = cvtt_i32_d((double)map.dur * (double)(float)pos + 0.5);
+        return time >= 0 ? time / time_step : -(((long long)-time + time_step - 1) / time_step);
+    };
+    auto fetch = [&](const void* clip, int count, int pos) -> Image {
+        long long idx = clip_index(pos);
+        if (idx < 0 || idx >= count) return Image(w, h, f);
+        Image img = from_frame((const uint8_t*)clip + (size_t)idx * frame_bytes, w, h, f);
+        return p->rows_reversed ? rows_reversed(img) : img;
+    };
+    Image A = fetch(frames, nframes, sel.a), B = fetch(frames, nframes, sel.b), result;
+    std::string e;
+    if (sel.vectors_quality != 0 && !sel.exact) {
+        if (sel.interp < 0 || sel.interp > 2) return fail(1, "bad interpolation mode");
+        float md = fixed_reader(float_to_fixed(p->max_displace), 1.0f);
+        float sx = fixed_reader(float_to_fixed(p->vec_scale_x), 1.0f), sy = fixed_reader(float_to_fixed(p->vec_scale_y), 1.0f);
+        FlowField fab, fba;
+        bool have_ab = false, have_ba = false;
+        if (vec_next) {
+            if (int rc = flow_from_vector_image(fetch(vec_next, n_next, sel.a), md, sx, sy, p->taps_above_first != 0, &fab, &e)) return fail(rc, e);
+            have_ab = true;
+        }
+        if (vec_prev) {
+            if (int rc = flow_from_vector_image(fetch(vec_prev, n_prev, sel.b), md, sx, sy, p->taps_above_first != 0, &fba, &e)) return fail(rc, e);
+            have_ba = true;
+        }
+        ComposeSettings cs;
+        cs.quality_high = p->quality_high != 0;
+        cs.blur = blur;
+        cs.warp_mode = p->warping == 2 ? 2 : 0;
+        cs.video_360 = false;
+        cs.taps_above_first = p->taps_above_first != 0;
+        cs.gouraud = p->gouraud != 0;
+        // complete_flows: the derived flow only where the composition (or the blur tail, F_AB) reads it
+        bool tail = (double)std::fabs(sel.s0 - sel.s1) > 1e-6 && (double)blur > 0.005;
+        bool need_ab = true, need_ba = true;
+        if (sel.interp == 0) {
+            bool ab = nearest_uses_f_ab(sel.wa, cs.warp_mode);
+            need_ab = ab || tail;
+            need_ba = !ab;
+        }
+        if (!have_ab && need_ab) {
+            if (int rc = invert_flow(fba, !cs.gouraud, cs.taps_above_first, &fab, &e)) return fail(rc, e);
+            have_ab = true;
+        } else if (!have_ba && need_ba) {
+            if (int rc = invert_flow(fab, !cs.gouraud, cs.taps_above_first, &fba, &e)) return fail(rc, e);
+            have_ba = true;
+        }
+        Image o;
+        int rc = compose_vectors(cs, sel, A, B, have_ab ? &fab : nullptr, have_ba ? &fba : nullptr, &o, &e);
+        if (rc) return fail(rc, e);
+        result = p->rows_reversed ? rows_reversed(o) : o;
+    } else {
+        int rc = interpolate(sel, A, B, &result, &e);
+        if (rc) return fail(rc, e);
+        if (p->rows_reversed) result = rows_reversed(result);
+    }
+    to_frame(result, out);
+    return 0;
+}
+
+}  // extern "C"

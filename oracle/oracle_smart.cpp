@@ -281,13 +281,33 @@ static std::vector<float> fill_solve(const FillGeometry& geo, const std::vector<
     return sol;
 }
 
-// holefill.rs:452-491 (fill_holes_masked_with, plain passes): mask_kind 1 u8, 2 u16, 3 f32
-int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, std::string* err) {
-    int w = img.w, h = img.h;
+// holefill.rs:238-345 (Filler): the hole flags and the weight pyramid of a mask, shared by every
+// channel; fill() solves one plane with the processor's arithmetic and again with the NaN rule
+// when that result holds a NaN (holefill.rs:303-309).
+struct PlaneFiller {
+    FillGeometry geo;
+    std::vector<bool> hole;
+    std::vector<std::vector<float>> wts;
+    std::vector<float> g5;
+    bool above_first = false;
+    void fill(std::vector<float>& plane) const {
+        std::vector<float> sol = fill_solve<Plain>(geo, hole, wts, plane, above_first, g5);
+        bool has_nan = false;
+        for (float v : sol) has_nan = has_nan || std::isnan(v);
+        if (has_nan) sol = fill_solve<Rule>(geo, hole, wts, plane, above_first, g5);
+        plane.swap(sol);
+    }
+};
+
+// holefill.rs:251-298 (Filler::new): 0 with *none set when the mask has no hole, 2 for a hole in an
+// image with a side of 1; a pixel is a hole when !(eps > m) (holefill.rs:124-133), mask_kind 1 u8,
+// 2 u16, 3 f32
+static int make_filler(int w, int h, const void* mask, int mask_kind, bool above_first, PlaneFiller* f, bool* none,
+                       std::string* err) {
     long n = (long)w * h;
     const double U8_EPS = [] { uint64_t b = 0x20202020202020fcull; double d; std::memcpy(&d, &b, 8); return d; }();
     const double WIDE_EPS = [] { uint64_t b = 0x3f0040bfe3b03e21ull; double d; std::memcpy(&d, &b, 8); return d; }();
-    std::vector<bool> hole((size_t)n);
+    f->hole.assign((size_t)n, false);
     bool any = false;
     for (long i = 0; i < n; i++) {
         double m;
@@ -295,39 +315,65 @@ int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, st
         else if (mask_kind == 2) m = ((const uint16_t*)mask)[i];
         else m = ((const float*)mask)[i];
         double eps = mask_kind == 1 ? U8_EPS : WIDE_EPS;
-        hole[i] = !(eps > m);
-        any = any || hole[i];
+        f->hole[i] = !(eps > m);
+        any = any || f->hole[i];
     }
+    *none = !any;
     if (!any) return 0;
     if (w < 2 || h < 2) { *err = "hole fill of an image with a side of 1"; return 2; }
-    FillGeometry geo = fill_geometry(w, h);
-    std::vector<std::vector<float>> wts;
-    {
-        std::vector<float> w0((size_t)n);
-        for (long i = 0; i < n; i++) w0[i] = hole[i] ? 0.0f : 1.0f;
-        wts.push_back(w0);
-        for (int k = 1; k <= geo.top; k++) {
-            int pw = geo.dims[k - 1].first, ph = geo.dims[k - 1].second;
-            int cw = geo.dims[k].first, ch = geo.dims[k].second;
-            std::vector<float> tmp = wts[k - 1];
-            convolve1<Plain>(tmp.data(), pw, ph, BIN5, 3, above_first);
-            wts.push_back(resample1_g<Plain>(tmp, pw, ph, cw, ch));
-        }
+    f->geo = fill_geometry(w, h);
+    f->above_first = above_first;
+    f->g5 = gaussian_kernel(5.0f);
+    std::vector<float> w0((size_t)n);
+    for (long i = 0; i < n; i++) w0[i] = f->hole[i] ? 0.0f : 1.0f;
+    f->wts.push_back(w0);
+    for (int k = 1; k <= f->geo.top; k++) {
+        int pw = f->geo.dims[k - 1].first, ph = f->geo.dims[k - 1].second;
+        int cw = f->geo.dims[k].first, ch = f->geo.dims[k].second;
+        std::vector<float> tmp = f->wts[k - 1];
+        convolve1<Plain>(tmp.data(), pw, ph, BIN5, 3, above_first);
+        f->wts.push_back(resample1_g<Plain>(tmp, pw, ph, cw, ch));
     }
-    std::vector<float> g5 = gaussian_kernel(5.0f);
+    return 0;
+}
+
+// holefill.rs:452-491 (fill_holes_masked_with, plain passes): mask_kind 1 u8, 2 u16, 3 f32
+int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, std::string* err) {
+    int w = img.w, h = img.h;
+    long n = (long)w * h;
+    PlaneFiller f;
+    bool none = false;
+    int rc = make_filler(w, h, mask, mask_kind, above_first, &f, &none, err);
+    if (rc || none) return rc;
     std::vector<float> plane((size_t)n);
     for (int c = 0; c < 4; c++) {
+        plane.resize((size_t)n);
         for (long i = 0; i < n; i++)
             plane[i] = img.fmt == U8 ? (float)img.u8[i * 4 + c] : img.fmt == U16 ? (float)img.u16[i * 4 + c] : img.f32[i * 4 + c];
-        std::vector<float> sol = fill_solve<Plain>(geo, hole, wts, plane, above_first, g5);
-        bool has_nan = false;
-        for (float v : sol) has_nan = has_nan || std::isnan(v);
-        if (has_nan) sol = fill_solve<Rule>(geo, hole, wts, plane, above_first, g5);
+        f.fill(plane);
         for (long i = 0; i < n; i++) {
-            if (img.fmt == U8) img.u8[i * 4 + c] = store_plain_int<uint8_t>(sol[i], 255.0f);
-            else if (img.fmt == U16) img.u16[i * 4 + c] = store_plain_int<uint16_t>(sol[i], 65535.0f);
-            else img.f32[i * 4 + c] = sol[i];
+            if (img.fmt == U8) img.u8[i * 4 + c] = store_plain_int<uint8_t>(plane[i], 255.0f);
+            else if (img.fmt == U16) img.u16[i * 4 + c] = store_plain_int<uint16_t>(plane[i], 65535.0f);
+            else img.f32[i * 4 + c] = plane[i];
         }
+    }
+    return 0;
+}
+
+// holefill.rs:497-518 (fill_flow_holes_with, is360 off): both components of a flow filled as
+// planes with the mask of the flow's size
+int fill_flow_holes(FlowField& flow, const void* mask, int mask_kind, bool above_first, std::string* err) {
+    long n = (long)flow.w * flow.h;
+    PlaneFiller f;
+    bool none = false;
+    int rc = make_filler(flow.w, flow.h, mask, mask_kind, above_first, &f, &none, err);
+    if (rc || none) return rc;
+    std::vector<float> plane((size_t)n);
+    for (int c = 0; c < 2; c++) {
+        plane.resize((size_t)n);
+        for (long i = 0; i < n; i++) plane[i] = flow.d[i * 2 + c];
+        f.fill(plane);
+        for (long i = 0; i < n; i++) flow.d[i * 2 + c] = plane[i];
     }
     return 0;
 }

@@ -19,6 +19,8 @@ void smart_blend(Image& out, const Image& p1, const Image& p2, float w, bool bin
 
 // holefill.rs:452-491 with the plain passes; mask_kind 1 u8, 2 u16, 3 f32 (w*h entries)
 int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, std::string* err);
+// holefill.rs:497-518 (fill_flow_holes_with, is360 off): the two components of a flow
+int fill_flow_holes(FlowField& flow, const void* mask, int mask_kind, bool above_first, std::string* err);
 
 // warping code 1 compositions (smartblend.rs:350-393): Nearest and Blend
 int compose_smart(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b, const FlowField* f_ab,

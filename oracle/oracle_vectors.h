@@ -22,4 +22,19 @@ struct CreateVectorsSettings {  // create_vectors.rs:97-135
 // create_vectors.rs:162-183 (one layer)
 int create_vectors(const Image& x, const Image& y, const CreateVectorsSettings& s, Image* out, std::string* err);
 
+// ---- Vectors In (compose/vector.rs:323-397, vectors.rs:474-583) ----
+// vectors.rs:474-522: the encoded image -> the flow of its size (alpha 0 the zero vector)
+FlowField decode_vectors(const Image& vec, float max_displace);
+// vectors.rs:555-561: 255 - A, 65535 - A or 1 - A as raw mask bytes of kind 1, 2 or 3
+void vector_hole_mask(const Image& vec, std::vector<uint8_t>* bytes, int* kind);
+// vectors.rs:573-578
+void apply_vec_scale(FlowField& flow, float sx, float sy);
+// compose/vector.rs:335-345: decode, flow hole fill (the tap order), Vec Scale
+int flow_from_vector_image(const Image& vec, float max_displace, float sx, float sy, bool above_first, FlowField* out,
+                           std::string* err);
+// compose/vector.rs:370-397: the inversion of a flow (textured forward warp, or Gouraud with !pyramid)
+int invert_flow(const FlowField& flow, bool pyramid, bool above_first, FlowField* out, std::string* err);
+// plugins/vectors-in/src/vectorin.rs:125-155: the vector image's alpha capped by a layer matte
+void matte_step(Image& img, const std::vector<float>& m);
+
 }  // namespace orc

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference tree (its path is required):
 
-    python tests/golden/make_golden.py --reference <reference tree> [--only flow_models]
+    python tests/golden/make_golden.py --reference <reference tree> [--only flow_models|vectors_in]
 
 Writes, next to this script:
 
@@ -45,6 +45,14 @@ Writes, next to this script:
 * ``warp_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/warp_cases.hex``
   (the reference's bit-exact numpy model of the inverse warp; format in its ``gen_warp.py``).
 
+* ``vectors_in_grid.npz`` - the cases of the reference's parity grid ``parity/vectors-in`` that the
+  single layer Vectors In render serves (one or both vector layers, no FG matte layer, Display not
+  Source, Speed mode with a constant speed, In FPS is Out FPS, integer frame rates), their footage,
+  Color Source and vector layer clips as its ``gen_grid.py`` writes them, and the sha256 of the
+  output clip ``results/base.grid.tsv`` records.
+* ``vectors_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/
+  vectors_cases.hex`` (the reference's numpy model of the vector encode and decode; format in its
+  ``gen_vectors.py``).
 * ``flow_models.bin.gz`` - the six differential fixtures ``plugins/retime-engine/tests/fixtures/
   flow_{a..f}.hex`` (the reference's float32 numpy model of the solver without block matching,
   ``flow_ref.py``; not bit exact: the reference's own test accepts 1e-4, 1e-3 with prep), each
@@ -203,6 +211,66 @@ def fgbg_layers_grid(ref):
     print(f"fgbg_layers_grid.npz: {len(cases)} cases, {len(keys)} clips")
 
 
+VI_SERVED = {"vectors_max_displace", "speed_percent", "warping", "frame_interp", "blur_compensation", "vec_scale_x",
+             "vec_scale_y", "display"}
+
+
+def vectors_in_grid(ref):
+    root = os.path.join(ref, "parity", "vectors-in")
+    spec = importlib.util.spec_from_file_location("vi_gen", os.path.join(root, "gen_grid.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    table = {}
+    for line in open(os.path.join(root, "results", "base.grid.tsv")):
+        parts = line.rstrip("\n").split("\t")
+        if parts[0] != "id":
+            table[parts[0]] = (parts[1], parts[3])
+    cases, inputs = [], {}
+    with tempfile.TemporaryDirectory() as tmp:
+        g = gen.Grid(tmp)
+        gen.build(g)
+
+        def clip(rel):
+            if rel not in inputs:
+                inputs[rel] = np.fromfile(os.path.join(tmp, rel), np.uint8)
+            return rel
+
+        for c in g.cases:
+            params = dict(p.split("=", 1) for p in c["params"])
+            if any(k not in VI_SERVED for k in params) or any("@" in v for v in params.values()):
+                continue
+            if params.get("display", "1") == "2":
+                continue
+            lay = c.get("layers", {})
+            if set(lay) - {"source", "vectors_prev", "vectors_next"}:
+                continue
+            if "vectors_prev" not in lay and "vectors_next" not in lay:
+                continue
+            if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
+                continue
+            main = lay.get("source", c["input"])
+            frames_of = lambda rel: g.inputs[rel]["frames"]
+            nxt, prv = lay.get("vectors_next"), lay.get("vectors_prev")
+            cases.append(dict(id=c["id"], params=c["params"], depth=c["depth"], width=c["width"], height=c["height"],
+                              frames=c["frames"], fps=c["fps"], main=clip(main), n_main=frames_of(main),
+                              next=clip(nxt) if nxt else None, n_next=frames_of(nxt) if nxt else 0,
+                              prev=clip(prv) if prv else None, n_prev=frames_of(prv) if prv else 0,
+                              sha256=table[c["id"]][1]))
+    keys = sorted(inputs)
+    arrays = {f"input_{i}": inputs[k] for i, k in enumerate(keys)}
+    arrays["meta"] = np.frombuffer(json.dumps(dict(inputs=keys, cases=cases)).encode(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "vectors_in_grid.npz"), **arrays)
+    print(f"vectors_in_grid.npz: {len(cases)} cases, {len(keys)} clips")
+
+
+def vectors_cases(ref):
+    txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "vectors_cases.hex")).read()
+    blob = bytes.fromhex("".join(txt.split()))
+    with gzip.open(os.path.join(HERE, "vectors_cases.bin.gz"), "wb") as f:
+        f.write(blob)
+    print(f"vectors_cases.bin.gz: {len(blob)} bytes, sha256 {hashlib.sha256(blob).hexdigest()}")
+
+
 def crt_powf_traced(ref):
     src = open(os.path.join(ref, "plugins", "retime-engine", "src", "crt_powf.rs")).read()
     m = re.search(r"const TRACED: \[\(u32, u32, u32\); \d+\] = \[(.*?)\];", src, re.S)
@@ -227,12 +295,18 @@ def flow_models(ref):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="the reference tree (baairon/twixtor)")
-    ap.add_argument("--only", choices=["flow_models"], default=None, help="write one fixture only")
+    ap.add_argument("--only", choices=["flow_models", "vectors_in"], default=None, help="write one fixture only")
     args = ap.parse_args()
     ref = args.reference
     if args.only == "flow_models":
         flow_models(ref)
         return
+    if args.only == "vectors_in":
+        vectors_in_grid(ref)
+        vectors_cases(ref)
+        return
+    vectors_in_grid(ref)
+    vectors_cases(ref)
     flow_models(ref)
     gen = load_gen(ref)
     with tempfile.TemporaryDirectory() as tmp:

@@ -390,3 +390,54 @@ def flow_models():
         out.append(dict(name=name, w=w, h=h, sens=np.float32(sens), quality=quality, prep=prep, x=x, y=y,
                         flow=flow, tol=FLOW_MODEL_TOL[name]))
     return out
+
+
+def vi_grid():
+    """The served cases of the vectors-in parity grid: (meta cases, {clip name: raw bytes})."""
+    z = np.load(os.path.join(GOLDEN, "vectors_in_grid.npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    inputs = {name: z[f"input_{i}"] for i, name in enumerate(meta["inputs"])}
+    return meta["cases"], inputs
+
+
+def vi_case_params(case):
+    """Keyword arguments of oracle_lib.vecin_params for a vectors-in grid case (the effect's
+    defaults where the case sets none: Speed 100, Max Displace 2048, Blend, Forward, scale 1)."""
+    p = dict(x.split("=", 1) for x in case["params"])
+    return dict(fps=(int(case["fps"]), 1), speed=float(p.get("speed_percent", 100)),
+                frame_interp=int(p.get("frame_interp", 2)), warping=int(p.get("warping", 2)),
+                blur=float(p.get("blur_compensation", 0)), max_displace=float(p.get("vectors_max_displace", 2048)),
+                vec_scale=(float(p.get("vec_scale_x", 1)), float(p.get("vec_scale_y", 1))))
+
+
+def vectors_cases():
+    """The reference's numpy model of the vector encode and decode (vectors_cases.hex, its
+    gen_vectors.py): b"VEC1", u32 count, then per case u32 kind (0 encode, 1 decode), depth (0 u8,
+    1 u16, 2 f32), W, H,
+    FW, FH, f32 scale; a decode case holds the W x H engine image (A, R, G, B samples of the depth)
+    and the decoded W x H flow; an encode case the FW x FH flow and the encoded W x H image."""
+    blob = gzip.open(os.path.join(GOLDEN, "vectors_cases.bin.gz")).read()
+    assert blob[:4] == b"VEC1"
+    n = struct.unpack_from("<I", blob, 4)[0]
+    p, out = 8, []
+    dt = {0: np.dtype("u1"), 1: np.dtype("<u2"), 2: np.dtype("<f4")}
+    for _ in range(n):
+        kind, depth, w, h, fw, fh = struct.unpack_from("<6I", blob, p)
+        scale = struct.unpack_from("<f", blob, p + 24)[0]
+        p += 28
+        d = dt[depth]
+        if kind == 1:
+            img = np.frombuffer(blob, d, w * h * 4, p).copy()
+            p += w * h * 4 * d.itemsize
+            flow = np.frombuffer(blob, "<f4", w * h * 2, p).astype(np.float32)
+            p += w * h * 8
+            out.append(dict(kind="decode", depth=depth, w=w, h=h, scale=np.float32(scale), image=img, flow=flow))
+        else:
+            flow = np.frombuffer(blob, "<f4", fw * fh * 2, p).astype(np.float32)
+            p += fw * fh * 8
+            img = np.frombuffer(blob, d, w * h * 4, p).copy()
+            p += w * h * 4 * d.itemsize
+            out.append(dict(kind="encode", depth=depth, w=w, h=h, fw=fw, fh=fh, scale=np.float32(scale), flow=flow,
+                            image=img))
+    assert p == len(blob), (p, len(blob))
+    return out

@@ -41,6 +41,29 @@ class RetimeParams(ctypes.Structure):
     ]
 
 
+class VecInParams(ctypes.Structure):
+    _fields_ = [
+        ("fps_num", ctypes.c_int),
+        ("fps_den", ctypes.c_int),
+        ("quality_high", ctypes.c_int),
+        ("speed_percent", ctypes.c_double),
+        ("nkeys", ctypes.c_int),
+        ("key_frames", ctypes.POINTER(ctypes.c_double)),
+        ("key_values", ctypes.POINTER(ctypes.c_double)),
+        ("key_ease", ctypes.POINTER(ctypes.c_int)),
+        ("frame_interp", ctypes.c_int),
+        ("warping", ctypes.c_int),
+        ("blur_compensation", ctypes.c_double),
+        ("max_displace", ctypes.c_double),
+        ("vec_scale_x", ctypes.c_double),
+        ("vec_scale_y", ctypes.c_double),
+        ("rows_reversed", ctypes.c_int),
+        ("taps_above_first", ctypes.c_int),
+        ("gouraud", ctypes.c_int),
+        ("probe_current_time", ctypes.c_int),
+    ]
+
+
 _lib = None
 
 
@@ -106,6 +129,12 @@ def lib():
         L.or_solve_masked.argtypes = [P, P, i, i, i, i, i, f, i, P, P, i, P]
         L.or_create_vectors_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(CvParams), i, P, P, P]
         L.or_encode_vectors.argtypes = [P, i, i, i, P, i, i, f]
+        L.or_flow_from_vectors.argtypes = [P, i, i, i, f, f, f, i, P]
+        L.or_decode_vectors.argtypes = [P, i, i, i, f, P]
+        L.or_fill_flow_holes.argtypes = [P, i, i, P, i, i]
+        L.or_invert_flow.argtypes = [P, i, i, i, i, P]
+        L.or_matte_step.argtypes = [P, i, i, i, P]
+        L.or_vectors_in_one.argtypes = [P, i, P, i, P, i, i, i, i, ctypes.POINTER(VecInParams), i, P]
         _lib = L
     return _lib
 
@@ -514,4 +543,92 @@ def motion_blur(src, w, h, fmt, flow, fw, fh, amount, hiq, shutter):
                               np.float32(amount), int(hiq), np.float32(shutter))
     if rc:
         raise ValueError(err())
+    return out
+
+
+# ---- Vectors In ----------------------------------------------------------------------------------
+
+
+def decode_vectors(vec, w, h, fmt, max_displace):
+    """vectors::decode_vectors of an engine image: the (w, h, 2) float32 flow."""
+    out = np.zeros(w * h * 2, np.float32)
+    lib().or_decode_vectors(ptr(np.ascontiguousarray(vec)), w, h, fmt, np.float32(max_displace), ptr(out))
+    return out
+
+
+def flow_from_vectors(vec, w, h, fmt, max_displace, scale=(1.0, 1.0), above_first=False):
+    """compose::flow_from_vector_image_with: decode, flow hole fill, Vec Scale."""
+    out = np.zeros(w * h * 2, np.float32)
+    rc = lib().or_flow_from_vectors(ptr(np.ascontiguousarray(vec)), w, h, fmt, np.float32(max_displace),
+                                    np.float32(scale[0]), np.float32(scale[1]), int(above_first), ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out
+
+
+def fill_flow_holes(flow, w, h, mask, mask_kind, above_first=False):
+    out = np.array(flow, np.float32, copy=True)
+    rc = lib().or_fill_flow_holes(ptr(out), w, h, ptr(np.ascontiguousarray(mask)), mask_kind, int(above_first))
+    if rc:
+        raise ValueError(err())
+    return out
+
+
+def invert_flow(flow, w, h, pyramid=True, above_first=False):
+    """compose::invert_flow_on: the inversion of a (w, h) flow (textured or Gouraud forward warp)."""
+    out = np.zeros(w * h * 2, np.float32)
+    rc = lib().or_invert_flow(ptr(np.ascontiguousarray(flow, np.float32)), w, h, int(pyramid), int(above_first),
+                              ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out
+
+
+def matte_step(vec, w, h, fmt, matte):
+    out = np.array(vec, copy=True)
+    lib().or_matte_step(ptr(out), w, h, fmt, ptr(np.ascontiguousarray(matte, np.float32)))
+    return out
+
+
+def vecin_params(fps=(30, 1), quality_high=True, speed=100.0, keys=None, frame_interp=2, warping=2, blur=0.0,
+                 max_displace=2048.0, vec_scale=(1.0, 1.0), rows_reversed=True, taps_above_first=True, gouraud=True,
+                 probe_current_time=False):
+    """The `vectors-in` parameters of one render (the effect's defaults; the three orders at the
+    plugin's: bottom-up rows, the tap above first, the Gouraud forward warp; a set vector layer
+    present at every time). All four False is the revision the parity grid records."""
+    p = VecInParams()
+    p.fps_num, p.fps_den = fps
+    p.quality_high = int(quality_high)
+    p.speed_percent = speed
+    p.frame_interp, p.warping = frame_interp, warping
+    p.blur_compensation, p.max_displace = blur, max_displace
+    p.vec_scale_x, p.vec_scale_y = vec_scale
+    p.rows_reversed, p.taps_above_first, p.gouraud = int(rows_reversed), int(taps_above_first), int(gouraud)
+    p.probe_current_time = int(probe_current_time)
+    p.nkeys = 0
+    if keys:
+        fr = (ctypes.c_double * len(keys))(*[k[0] for k in keys])
+        va = (ctypes.c_double * len(keys))(*[k[1] for k in keys])
+        ea = (ctypes.c_int * len(keys))(*[int(k[2]) for k in keys])
+        p.nkeys = len(keys)
+        p.key_frames = ctypes.cast(fr, ctypes.POINTER(ctypes.c_double))
+        p.key_values = ctypes.cast(va, ctypes.POINTER(ctypes.c_double))
+        p.key_ease = ctypes.cast(ea, ctypes.POINTER(ctypes.c_int))
+        p._keep = (fr, va, ea)
+    return p
+
+
+def vectors_in_clip(frames, nframes, vec_next, n_next, vec_prev, n_prev, w, h, fmt, params, nout):
+    """Output frames 0..nout-1 of the single layer `vectors-in` render, back to back. vec_next /
+    vec_prev: wire clips of the vector layers (None: the layer is not set)."""
+    fb = w * h * 4
+    out = np.zeros(nout * fb, DTYPE[fmt])
+    vn = None if vec_next is None else np.ascontiguousarray(vec_next)
+    vp = None if vec_prev is None else np.ascontiguousarray(vec_prev)
+    for n in range(nout):
+        rc = lib().or_vectors_in_one(ptr(frames), nframes, None if vn is None else ptr(vn), n_next,
+                                     None if vp is None else ptr(vp), n_prev, w, h, fmt, ctypes.byref(params), n,
+                                     ptr(out[n * fb:]))
+        if rc:
+            raise ValueError(f"or_vectors_in_one: {rc} {err()}")
     return out
