@@ -450,6 +450,83 @@ typedef struct tw_time_params {
  * 451-469, with RemapTimeMap::src_pos :266-331 and the tiny-frame rule prep.rs:111-117). */
 int tw_select(const tw_time_params* p, int32_t n, int32_t width, int32_t height, tw_selection* out);
 
+/* ---- Vectors In (plugins/vectors-in, compose/vector.rs:323-447) ----------------------------- */
+
+/* One output frame of the Vectors In render beyond its selection (plugins/vectors-in/src/vectorin.rs:
+ * 175-227): the clip frames of the pair (footage A and Vectors: Next at clip frame a, footage B and
+ * Vectors: Prev at clip frame b), which vector layers are present (has_next / has_prev; a present
+ * layer without a frame there is a transparent image, which decodes to the zero flow) and their
+ * Vec Scale X / Y at the fetch times. */
+typedef struct tw_vecin_frame {
+    int32_t a, b;
+    int32_t has_next, has_prev;
+    float next_scale[2];
+    float prev_scale[2];
+} tw_vecin_frame;
+
+/* The selection of output frame n of the Vectors In effect (plugins/vectors-in/src/timemap.rs,
+ * glue.rs:204-215): the Speed map of tw_select with the input rate 30 and the output rate the
+ * composition's (In FPS is Out FPS on), the vectors quality 4 (p->vectors is not read), and in
+ * frame->a / frame->b the clip frames of the pair at T(k) = trunc(dur * k + 0.5) ticks. The
+ * other fields of `frame` are left as they are. */
+int tw_select_vectors_in(const tw_time_params* p, int32_t n, int32_t width, int32_t height, tw_selection* out,
+                         tw_vecin_frame* frame);
+
+/* vectors::decode_vectors (vectors.rs:474-528): the flow of an encoded engine image of the same
+ * size (R dx and G dy, 8 bpc ((c * 2) / 254 - 1) * md and 16 bpc with 65534 in double precision,
+ * float (c * 2 - 1) * md; alpha 0 the zero vector). */
+int tw_decode_vectors(tw_ctx* ctx, const tw_image* vec, float max_displace, tw_flow* out);
+
+/* compose::flow_from_vector_image_with (compose/vector.rs:335-345): the decode, the pull-push fill
+ * of the holes of the inverted alpha (holefill.rs:497-518, is360 off, the tap order
+ * taps_above_first), then Vec Scale (vectors.rs:573-578). A hole in an image with a side of 1
+ * pixel is TW_ERR_UNSUPPORTED, as in the reference. */
+int tw_flow_from_vectors(tw_ctx* ctx, const tw_image* vec, float max_displace, float scale_x, float scale_y,
+                         int32_t taps_above_first, tw_flow* out);
+
+/* holefill::fill_flow_holes_with (holefill.rs:497-518) with is360 off: both components of `flow`
+ * filled in place; the mask as in tw_fill_holes. */
+int tw_fill_flow_holes(tw_ctx* ctx, tw_flow* flow, const void* mask, int32_t mask_kind, int32_t taps_above_first);
+
+/* compose::invert_flow_on (compose/vector.rs:370-397): T = -(1, fx, fy, 1) pushed along the flow
+ * at amount 1 with the forward warp (pyramid != 0 the textured warp, 0 the Gouraud variant), the
+ * coverage inverted, channels 1 and 2 of the pushed image as the flow, the holes filled. `out` has
+ * the flow's size (at least 2x2). */
+int tw_invert_flow(tw_ctx* ctx, const tw_flow* in, int32_t pyramid, int32_t taps_above_first, tw_flow* out);
+
+/* One output frame of the single layer Vectors In render (glue.rs:386-495 with nfg 0, Display not
+ * Source; compose.rs:101-131): wire frames of the footage at A and B (NULL: blank), of Vectors: Next
+ * at A and Vectors: Prev at B (read only for a present layer; NULL: transparent). Neither layer
+ * present: the size mismatch error fill (image.rs:388-425), as the effect writes it. Else the
+ * vector path when sel->vectors_quality != 0 and !sel->exact: each present layer's flow
+ * (tw_flow_from_vectors with Max Displace `max_displace` and the frame's Vec Scale), the missing
+ * one as the inversion of the other where the composition reads it (compose/vector.rs:422-447;
+ * the forward warp Gouraud when s->compose.gouraud), then tw_compose_vectors' composition; else
+ * the fast path. s->motion_rows_reversed turns every input of the vector path, the vector layers
+ * included, upside down and the output back (glue.rs:44-48). The hole fills take
+ * s->compose.taps_above_first. */
+int tw_retime_frame_vectors(tw_ctx* ctx, const tw_retime_settings* s, const tw_selection* sel, const tw_vecin_frame* vf,
+                            float max_displace, const void* wire_a, const void* wire_b, const void* wire_next,
+                            const void* wire_prev, int32_t width, int32_t height, int32_t fmt, void* wire_out);
+
+/* The same over clips in HOST memory: the footage (nframes wire frames back to back), Vectors: Next
+ * (n_next frames; NULL when no frame has it) and Vectors: Prev (n_prev); output frame k from
+ * sels[k] and vfs[k] goes to out + k * frame_bytes. A clip frame outside a clip is blank (footage)
+ * or transparent (vector layer). The clips are uploaded whole; frames run on the lanes, except
+ * that a call whose frames run the forward warp (warping codes 2 and 3, or a flow inversion) runs
+ * them one at a time. */
+int tw_vectors_in_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes, const void* next,
+                       int32_t n_next, const void* prev, int32_t n_prev, const tw_selection* sels,
+                       const tw_vecin_frame* vfs, int32_t nout, float max_displace, int32_t width, int32_t height,
+                       int32_t fmt, void* out);
+
+/* The same with every clip and the output in DEVICE memory; enqueues on the context's stream and
+ * returns after it completes. */
+int tw_vectors_in_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,
+                              const void* next, int32_t n_next, const void* prev, int32_t n_prev,
+                              const tw_selection* sels, const tw_vecin_frame* vfs, int32_t nout, float max_displace,
+                              int32_t width, int32_t height, int32_t fmt, void* out);
+
 /* ---- one clip over several GPUs ------------------------------------------------------------ */
 
 /* The output frames [lo, hi) of a clip of nout output frames that rank `rank` of `nranks` renders:

@@ -1139,6 +1139,53 @@ void or_matte_step(void* eng, int w, int h, int fmt, const float* matte) {
     std::memcpy(eng, v.data(), v.bytes());
 }
 
+// The selection of output frame n of the Vectors In effect: plugin 01's Speed map with the plugin's
+// rates (in 30, out the composition's: timemap.rs, glue.rs:204-215) and the constant quality 4.
+// Returns the ticks per frame.
+static int vecin_select(const or_vecin_params* p, int n, int w, int h, TimeMap* map, Selection* sel) {
+    bool integer = p->fps_den == 1;
+    int time_step = integer ? 100 : p->fps_den;
+    double comp = (double)p->fps_num / (double)p->fps_den;
+    map->lts = time_step;
+    map->in_fps = 30.0;
+    map->out_fps = comp;
+    map->dur = (float)(((double)time_step * comp) / 30.0);
+    map->speed.constant = p->speed_percent;
+    for (int i = 0; i < p->nkeys; i++) {
+        long long t = (long long)std::llround(p->key_frames[i] * (double)time_step);
+        map->speed.keys.push_back({t, p->key_values[i], p->key_ease && p->key_ease[i] != 0});
+    }
+    int cur = n * time_step;
+    float t0 = (float)cur / (float)time_step;
+    float t1 = ((float)time_step + (float)cur) / (float)time_step;
+    sel->s0 = map->src_pos(t0);
+    sel->s1 = map->src_pos(t1);
+    float blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
+    sel->a = cvtt_i32_f(sel->s0);
+    sel->b = sel->a + 1;
+    sel->wa = 1.0f - (sel->s0 - (float)sel->a);
+    sel->exact = exact_position(sel->s0, sel->s1, blur);
+    sel->vectors_quality = (w >= 2 && h >= 2) ? 4 : 0;
+    sel->interp = p->frame_interp - 1;
+    return time_step;
+}
+
+// vecin_select for the tests: s0, s1, wa as floats, then a, exact, vectors quality, interp and the
+// clip frames of A and B at T(A), T(B)
+int or_vecin_select(const or_vecin_params* p, int n, int w, int h, float* f3, int* i6) {
+    TimeMap map;
+    Selection sel;
+    int ts = vecin_select(p, n, w, h, &map, &sel);
+    auto idx = [&](int pos) -> int {
+        int time = cvtt_i32_d((double)map.dur * (double)(float)pos + 0.5);
+        return (int)(time >= 0 ? time / ts : -(((long long)-time + ts - 1) / ts));
+    };
+    f3[0] = sel.s0; f3[1] = sel.s1; f3[2] = sel.wa;
+    i6[0] = sel.a; i6[1] = sel.exact ? 1 : 0; i6[2] = sel.vectors_quality; i6[3] = sel.interp;
+    i6[4] = idx(sel.a); i6[5] = idx(sel.b);
+    return 0;
+}
+
 // Output frame n of the single layer `vectors-in` render (glue.rs:386-495 with nfg 0, Display not
 // Source): the footage clip `frames` (nframes wire frames), the vector layers `Vectors: Next` and
 // `Vectors: Prev` as wire clips of n_next / n_prev frames (NULL: the layer is not set; a frame past
@@ -1169,33 +1216,10 @@ int or_vectors_in_one(const void* frames, int nframes, const void* vec_next, int
         }
         return 0;
     }
-    // the time model: plugin 01's Speed map with the plugin's rates (in 30, out the composition's)
-    bool integer = p->fps_den == 1;
-    int time_step = integer ? 100 : p->fps_den;
-    double comp = (double)p->fps_num / (double)p->fps_den;
     TimeMap map;
-    map.lts = time_step;
-    map.in_fps = 30.0;
-    map.out_fps = comp;
-    map.dur = (float)(((double)time_step * comp) / 30.0);
-    map.speed.constant = p->speed_percent;
-    for (int i = 0; i < p->nkeys; i++) {
-        long long t = (long long)std::llround(p->key_frames[i] * (double)time_step);
-        map.speed.keys.push_back({t, p->key_values[i], p->key_ease && p->key_ease[i] != 0});
-    }
-    int cur = n * time_step;
-    float t0 = (float)cur / (float)time_step;
-    float t1 = ((float)time_step + (float)cur) / (float)time_step;
     Selection sel;
-    sel.s0 = map.src_pos(t0);
-    sel.s1 = map.src_pos(t1);
+    int time_step = vecin_select(p, n, w, h, &map, &sel);
     float blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
-    sel.a = cvtt_i32_f(sel.s0);
-    sel.b = sel.a + 1;
-    sel.wa = 1.0f - (sel.s0 - (float)sel.a);
-    sel.exact = exact_position(sel.s0, sel.s1, blur);
-    sel.vectors_quality = (w >= 2 && h >= 2) ? 4 : 0;
-    sel.interp = p->frame_interp - 1;
     // T(k) = trunc(dur * k + 0.5) (timemap.rs:45-50), then the clip frame of that tick
     auto clip_index = [&](int pos) -> long long {
         int time = cvtt_i32_d((double)map.dur * (double)(float)pos + 0.5);

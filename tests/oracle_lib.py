@@ -135,6 +135,7 @@ def lib():
         L.or_invert_flow.argtypes = [P, i, i, i, i, P]
         L.or_matte_step.argtypes = [P, i, i, i, P]
         L.or_vectors_in_one.argtypes = [P, i, P, i, P, i, i, i, i, ctypes.POINTER(VecInParams), i, P]
+        L.or_vecin_select.argtypes = [ctypes.POINTER(VecInParams), i, i, i, P, P]
         _lib = L
     return _lib
 
@@ -632,3 +633,11 @@ def vectors_in_clip(frames, nframes, vec_next, n_next, vec_prev, n_prev, w, h, f
         if rc:
             raise ValueError(f"or_vectors_in_one: {rc} {err()}")
     return out
+
+
+def vecin_select(params, n, w, h):
+    """The Vectors In effect's selection of output frame n and the clip frames of its pair."""
+    f3, i6 = np.zeros(3, np.float32), np.zeros(6, np.int32)
+    lib().or_vecin_select(ctypes.byref(params), n, w, h, ptr(f3), ptr(i6))
+    return dict(s0=f3[0], s1=f3[1], wa=f3[2], a=int(i6[0]), exact=bool(i6[1]), vq=int(i6[2]), interp=int(i6[3]),
+                clip_a=int(i6[4]), clip_b=int(i6[5]))

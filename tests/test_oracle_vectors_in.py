@@ -111,3 +111,19 @@ def test_matte_step():
     imgf = np.array([0.7, 1, 2, 3, 0.2, 4, 5, 6], np.float32)
     got = O.matte_step(imgf, 2, 1, 2, np.array([np.nan, 0.1], np.float32))
     assert got[0] == np.float32(0.7) and got[4] == np.float32(0.1)
+
+
+@pytest.mark.parametrize("fps", [(30, 1), (24, 1), (25, 1), (12, 1), (60, 1)])
+@pytest.mark.parametrize("speed", [50.0, 100.0, 33.3333, 150.0, -50.0, 0.5])
+def test_selection_of_the_library(fps, speed):
+    """tw_select_vectors_in (the product's host time model of the effect) against the oracle's, for
+    the first 40 output frames: the selection and the clip frames of the pair."""
+    import twixtor_b200 as tw
+    p = O.vecin_params(fps=fps, speed=speed, frame_interp=3, blur=2.5)
+    tp = tw.TimeParams(fps=fps, speed_percent=speed, frame_interp=3, blur_compensation=2.5)
+    for n in range(40):
+        want = O.vecin_select(p, n, 16, 12)
+        sel, vf = tw.select_vectors_in(tp, n, 16, 12)
+        got = dict(s0=np.float32(sel.s0), s1=np.float32(sel.s1), wa=np.float32(sel.wa), a=sel.a, exact=bool(sel.exact),
+                   vq=sel.vectors_quality, interp=sel.interp, clip_a=vf.a, clip_b=vf.b)
+        assert got == want, (n, got, want)

@@ -142,6 +142,11 @@ class _TimeParams(ctypes.Structure):
                 ("blur_compensation", ctypes.c_double)]
 
 
+class _VecInFrame(ctypes.Structure):
+    _fields_ = [("a", ctypes.c_int32), ("b", ctypes.c_int32), ("has_next", ctypes.c_int32), ("has_prev", ctypes.c_int32),
+                ("next_scale", ctypes.c_float * 2), ("prev_scale", ctypes.c_float * 2)]
+
+
 # ---- the Python mirrors of the reference types -----------------------------------------------------
 
 @dataclass
@@ -365,6 +370,17 @@ def library():
                                         i32, i32, i32, P]
     L.tw_retime_layers_clip.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, ctypes.POINTER(_LayerJob), P, P,
                                         ctypes.POINTER(_Selection), i32, i32, i32, i32, P]
+    pvf = ctypes.POINTER(_VecInFrame)
+    L.tw_select_vectors_in.argtypes = [ctypes.POINTER(_TimeParams), i32, i32, i32, ctypes.POINTER(_Selection), pvf]
+    L.tw_decode_vectors.argtypes = [P, pimg, ctypes.c_float, pflow]
+    L.tw_flow_from_vectors.argtypes = [P, pimg, ctypes.c_float, ctypes.c_float, ctypes.c_float, i32, pflow]
+    L.tw_fill_flow_holes.argtypes = [P, pflow, P, i32, i32]
+    L.tw_invert_flow.argtypes = [P, pflow, i32, i32, pflow]
+    L.tw_retime_frame_vectors.argtypes = [P, ctypes.POINTER(_RetimeSettings), ctypes.POINTER(_Selection), pvf,
+                                          ctypes.c_float, P, P, P, P, i32, i32, i32, P]
+    L.tw_vectors_in_clip.argtypes = [P, ctypes.POINTER(_RetimeSettings), P, i32, P, i32, P, i32,
+                                     ctypes.POINTER(_Selection), pvf, i32, ctypes.c_float, i32, i32, i32, P]
+    L.tw_vectors_in_clip_device.argtypes = L.tw_vectors_in_clip.argtypes
     _lib = L
     return L
 
@@ -396,6 +412,46 @@ def select(params: TimeParams, n: int, width: int, height: int) -> Selection:
     if rc:
         raise BadParam(rc, "tw_select")
     return Selection._from_c(out)
+
+
+@dataclass
+class VecInFrame:
+    """One output frame of the Vectors In render beyond its selection (tw_vecin_frame): the clip
+    frames of the pair, which vector layers are present and their Vec Scale at the fetch times."""
+    a: int = 0
+    b: int = 1
+    has_next: bool = True
+    has_prev: bool = True
+    next_scale: Tuple[float, float] = (1.0, 1.0)
+    prev_scale: Tuple[float, float] = (1.0, 1.0)
+
+    def _c(self):
+        return _VecInFrame(self.a, self.b, int(self.has_next), int(self.has_prev),
+                           (ctypes.c_float * 2)(*self.next_scale), (ctypes.c_float * 2)(*self.prev_scale))
+
+
+def select_vectors_in(params: TimeParams, n: int, width: int, height: int, has_next=True, has_prev=True,
+                      next_scale=(1.0, 1.0), prev_scale=(1.0, 1.0)) -> Tuple[Selection, VecInFrame]:
+    """The selection and the clip frames of output frame ``n`` of the Vectors In effect (its time
+    map: the input rate 30, the output rate ``params.fps``; tw_select_vectors_in)."""
+    out, fr = _Selection(), _VecInFrame()
+    rc = library().tw_select_vectors_in(ctypes.byref(params._c()), n, width, height, ctypes.byref(out),
+                                        ctypes.byref(fr))
+    if rc:
+        raise BadParam(rc, "tw_select_vectors_in")
+    return Selection._from_c(out), VecInFrame(fr.a, fr.b, has_next, has_prev, tuple(next_scale), tuple(prev_scale))
+
+
+def vectors_in_settings(warping: int = 2, quality_high=True, blur=0.0, rows_reversed=True, taps_above_first=True,
+                        gouraud=True) -> "RetimeSettings":
+    """The settings of the Vectors In render (plugins/vectors-in/src/glue.rs:204-243): the Warping
+    popup (1 Inverse, 2 Forward) as the warp code, the blur compensation, and its three orders
+    (bottom-up rows, the tap above first in the fills, the Gouraud forward warp); all three False
+    is the revision the reference's parity grid records."""
+    return RetimeSettings(FlowSettings(), EngineSettings(warp_mode=2 if warping == 2 else 0, quality_high=quality_high,
+                                                         blur=float(fixed_param(blur)),
+                                                         taps_above_first=taps_above_first, gouraud=gouraud),
+                          motion_rows_reversed=rows_reversed)
 
 
 def shard(nout: int, nranks: int, rank: int) -> Tuple[int, int]:
@@ -781,6 +837,82 @@ class Device:
         oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
         self._check(self._L.tw_fill_holes(self._h, ctypes.byref(oi), _ptr(mask), kind, int(taps_above_first)))
         return out
+
+    def decode_vectors(self, vec, width, height, fmt, max_displace):
+        """``vectors::decode_vectors`` of an engine image: the interleaved (w x h x 2) flow."""
+        vi, vec = _img(vec, width, height, fmt)
+        out = np.zeros(width * height * 2, np.float32)
+        fo = _Flow(width, height, out.ctypes.data)
+        self._check(self._L.tw_decode_vectors(self._h, ctypes.byref(vi), np.float32(max_displace), ctypes.byref(fo)))
+        return out
+
+    def flow_from_vectors(self, vec, width, height, fmt, max_displace, scale=(1.0, 1.0), taps_above_first=True):
+        """``compose::flow_from_vector_image_with``: decode, flow hole fill, Vec Scale."""
+        vi, vec = _img(vec, width, height, fmt)
+        out = np.zeros(width * height * 2, np.float32)
+        fo = _Flow(width, height, out.ctypes.data)
+        self._check(self._L.tw_flow_from_vectors(self._h, ctypes.byref(vi), np.float32(max_displace),
+                                                 np.float32(scale[0]), np.float32(scale[1]), int(taps_above_first),
+                                                 ctypes.byref(fo)))
+        return out
+
+    def fill_flow_holes(self, flow, width, height, mask, taps_above_first=True):
+        """``holefill::fill_flow_holes_with`` (is360 off): the filled copy of an interleaved flow; the
+        mask's dtype picks its kind as in fill_holes."""
+        kind = {np.dtype(np.uint8): 1, np.dtype(np.uint16): 2, np.dtype(np.float32): 3}[np.asarray(mask).dtype]
+        mask = np.ascontiguousarray(mask)
+        out = np.array(flow, np.float32, copy=True).reshape(-1)
+        fo = _Flow(width, height, out.ctypes.data)
+        self._check(self._L.tw_fill_flow_holes(self._h, ctypes.byref(fo), _ptr(mask), kind, int(taps_above_first)))
+        return out
+
+    def invert_flow(self, flow, width, height, pyramid=True, taps_above_first=True):
+        """``compose::invert_flow_on``: the inversion of a (w x h) interleaved flow."""
+        flow = np.ascontiguousarray(flow, np.float32)
+        out = np.zeros(width * height * 2, np.float32)
+        fi, fo = _Flow(width, height, flow.ctypes.data), _Flow(width, height, out.ctypes.data)
+        self._check(self._L.tw_invert_flow(self._h, ctypes.byref(fi), int(pyramid), int(taps_above_first),
+                                           ctypes.byref(fo)))
+        return out
+
+    def retime_frame_vectors(self, settings: "RetimeSettings", sel: "Selection", vf: VecInFrame, max_displace,
+                             wire_a, wire_b, wire_next, wire_prev, width, height, fmt, out=None):
+        """One output wire frame of the single layer Vectors In render (tw_retime_frame_vectors)."""
+        if out is None:
+            out = np.zeros(width * height * 4, DTYPES[fmt])
+        keep = [None if w is None else np.ascontiguousarray(w) for w in (wire_a, wire_b, wire_next, wire_prev)]
+        self._check(self._L.tw_retime_frame_vectors(self._h, ctypes.byref(settings._c()), ctypes.byref(sel._c()),
+                                                    ctypes.byref(vf._c()), np.float32(max_displace),
+                                                    *[_ptr(k) for k in keep], width, height, fmt, _ptr(out)))
+        return out
+
+    def vectors_in_clip(self, settings: "RetimeSettings", frames, nframes, next_clip, n_next, prev_clip, n_prev, sels,
+                        vfs, max_displace, width, height, fmt, out=None):
+        """Output frames ``sels`` / ``vfs`` of the single layer Vectors In render over clips in host
+        memory (tw_vectors_in_clip); a vector clip None is a layer that is not set."""
+        fs = width * height * 4
+        if out is None:
+            out = np.zeros(len(sels) * fs, DTYPES[fmt])
+        frames = np.ascontiguousarray(frames)
+        nc = None if next_clip is None else np.ascontiguousarray(next_clip)
+        pc = None if prev_clip is None else np.ascontiguousarray(prev_clip)
+        sa = (_Selection * max(len(sels), 1))(*[s._c() for s in sels])
+        va = (_VecInFrame * max(len(vfs), 1))(*[v._c() for v in vfs])
+        self._check(self._L.tw_vectors_in_clip(self._h, ctypes.byref(settings._c()), _ptr(frames), nframes, _ptr(nc),
+                                               n_next if nc is not None else 0, _ptr(pc),
+                                               n_prev if pc is not None else 0, sa, va, len(sels),
+                                               np.float32(max_displace), width, height, fmt, _ptr(out)))
+        return out
+
+    def vectors_in_clip_device(self, settings: "RetimeSettings", frames_ptr, nframes, next_ptr, n_next, prev_ptr,
+                               n_prev, sels, vfs, max_displace, width, height, fmt, out_ptr):
+        """tw_vectors_in_clip_device on device pointers (ints; 0 or None for a layer that is not set)."""
+        sa = (_Selection * max(len(sels), 1))(*[s._c() for s in sels])
+        va = (_VecInFrame * max(len(vfs), 1))(*[v._c() for v in vfs])
+        self._check(self._L.tw_vectors_in_clip_device(self._h, ctypes.byref(settings._c()), frames_ptr, nframes,
+                                                      next_ptr or None, n_next, prev_ptr or None, n_prev, sa, va,
+                                                      len(sels), np.float32(max_displace), width, height, fmt,
+                                                      out_ptr))
 
     def from_frame(self, wire, width, height, fmt):
         wire = np.ascontiguousarray(wire)

@@ -11,6 +11,14 @@ void from_frame_dev(tw_ctx* ctx, const void* wire, void* eng, int W, int H, int 
     else LAUNCHB(ctx, 2.0 * 16 * n, k_from_frame_f32, grid1(n), TB, 0, (const float*)wire, (float*)eng, W, H, flip);
 }
 
+// image.rs:213-245 on ctx->cur: an engine image to a wire frame (upside down with flip)
+void to_frame_dev(tw_ctx* ctx, const void* eng, void* wire, int W, int H, int fmt, bool flip) {
+    long n = (long)W * H;
+    if (fmt == TW_U8) LAUNCHB(ctx, 2.0 * 4 * n, k_to_frame_u8, grid1(n), TB, 0, (const uint8_t*)eng, (uint8_t*)wire, W, H, flip);
+    else if (fmt == TW_U16) LAUNCHB(ctx, 2.0 * 8 * n, k_to_frame_u16, grid1(n), TB, 0, (const uint16_t*)eng, (uint16_t*)wire, W, H, flip);
+    else LAUNCHB(ctx, 2.0 * 16 * n, k_to_frame_f32, grid1(n), TB, 0, (const float*)eng, (float*)wire, W, H, flip);
+}
+
 // One output frame on lane L from two device-resident wire frames (nullptr = a blank frame outside
 // the clip); writes the output wire frame to out_wire (device). Both lane streams must already be
 // ordered after the caller's work (ctx->ev_start); the frame's end is L.ev_done on stream 0.

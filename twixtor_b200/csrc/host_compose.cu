@@ -82,20 +82,23 @@ void fill_resample(tw_ctx* ctx, const float* src, int sw, int sh, float* dst, in
 }
 
 // The pull-push fill of an engine image in place (holefill.rs:260-350, :452-491) with the u8
-// holes mask; every kernel returns at once when *any (no hole) is 0. Per level a stack of five
-// planes: the four channels' values and the weights. Float images run the NaN rule arithmetic
-// (for numbers the plain arithmetic bit for bit, and where a NaN reaches the result the bits of
-// the reference's repeat with the rule).
+// holes mask; every kernel returns at once when *any (no hole) is 0. Per level a stack of the
+// channels' value planes and the weights: five planes for an engine image, three for an
+// interleaved flow (fmt FILL_FLOW, holefill.rs:497-518). Float images and flows run the NaN rule
+// arithmetic (for numbers the plain arithmetic bit for bit, and where a NaN reaches the result the
+// bits of the reference's repeat with the rule).
 int fill_dev(tw_ctx* ctx, void* img, int W, int H, int fmt, const uint8_t* holes, const int* any, bool above_first,
              DevBuf& fb) {
-    int rule = fmt == TW_F32;
+    int rule = fmt == TW_F32 || fmt == FILL_FLOW;
+    int nc = fmt == FILL_FLOW ? 2 : 4;  // value planes; the weights are plane nc
+    int np = nc + 1;
     FillGeo g = fill_geometry(W, H);
     long n0 = (long)W * H;
     size_t offs[40];
     size_t tot = 0;
-    for (int k = 0; k <= g.top; k++) { offs[k] = tot; tot += 5 * (size_t)g.dims[k][0] * g.dims[k][1]; }
-    size_t o_ta = tot, o_sa = tot + 5 * n0, o_sb = o_sa + 4 * n0;
-    tot = o_sb + 4 * n0;
+    for (int k = 0; k <= g.top; k++) { offs[k] = tot; tot += np * (size_t)g.dims[k][0] * g.dims[k][1]; }
+    size_t o_ta = tot, o_sa = tot + np * n0, o_sb = o_sa + nc * n0;
+    tot = o_sb + nc * n0;
     CHECK(ctx->ensure(fb, tot * sizeof(float), "hole fill planes"));
     float* base = fb.as<float>();
     float* ta = base + o_ta;
@@ -104,26 +107,26 @@ int fill_dev(tw_ctx* ctx, void* img, int W, int H, int fmt, const uint8_t* holes
         int pw = g.dims[k - 1][0], ph = g.dims[k - 1][1], cw = g.dims[k][0], chh = g.dims[k][1];
         long pn = (long)pw * ph;
         // the level k - 1 planes stay for the push: blur a copy
-        CHECK(ctx->cuda(cudaMemcpyAsync(ta, base + offs[k - 1], 5 * pn * sizeof(float), cudaMemcpyDeviceToDevice, ctx->cur),
+        CHECK(ctx->cuda(cudaMemcpyAsync(ta, base + offs[k - 1], np * pn * sizeof(float), cudaMemcpyDeviceToDevice, ctx->cur),
                         "fill copy"));
-        fill_passes(ctx, ta, base + o_sa, pw, ph, pn, 5, ctx->b5, 3, above_first, rule, any);
-        fill_resample(ctx, ta, pw, ph, base + offs[k], cw, chh, 5, rule, any);
+        fill_passes(ctx, ta, base + o_sa, pw, ph, pn, np, ctx->b5, 3, above_first, rule, any);
+        fill_resample(ctx, ta, pw, ph, base + offs[k], cw, chh, np, rule, any);
     }
     float* sol = base + o_sa;
     float* nxt = base + o_sb;
     {
         long tn = (long)g.dims[g.top][0] * g.dims[g.top][1];
-        LAUNCH(ctx, k_stack_zero, grid1(4 * tn), TB, 0, sol, 4 * tn, any);
+        LAUNCH(ctx, k_stack_zero, grid1(nc * tn), TB, 0, sol, nc * tn, any);
     }
     for (int lv = g.top; lv >= 0; lv--) {  // push
         int lw = g.dims[lv][0], lh = g.dims[lv][1];
         long ln = (long)lw * lh;
-        LAUNCH(ctx, k_fill_combine, grid1(ln), TB, 0, sol, base + offs[lv], ln, rule, any);
-        fill_passes(ctx, sol, ta, lw, lh, ln, 4, ctx->g5, 6, above_first, rule, any);
+        LAUNCH(ctx, k_fill_combine, grid1(ln), TB, 0, sol, base + offs[lv], ln, nc, rule, any);
+        fill_passes(ctx, sol, ta, lw, lh, ln, nc, ctx->g5, 6, above_first, rule, any);
         if (lv == 0) {
-            LAUNCH(ctx, k_fill_combine, grid1(ln), TB, 0, sol, base + offs[0], ln, rule, any);
+            LAUNCH(ctx, k_fill_combine, grid1(ln), TB, 0, sol, base + offs[0], ln, nc, rule, any);
         } else {
-            fill_resample(ctx, sol, lw, lh, nxt, g.dims[lv - 1][0], g.dims[lv - 1][1], 4, rule, any);
+            fill_resample(ctx, sol, lw, lh, nxt, g.dims[lv - 1][0], g.dims[lv - 1][1], nc, rule, any);
             std::swap(sol, nxt);
         }
     }

@@ -270,6 +270,9 @@ void tw_close(tw_ctx* ctx) {
     for (int i = 0; i < 3; i++) { ctx->eng[i].release(&ctx->held); ctx->wire[i].release(&ctx->held); }
     for (int i = 0; i < 2; i++) { ctx->pyr[i].release(&ctx->held); ctx->work[i].release(&ctx->held); ctx->flow[i].release(&ctx->held); }
     for (int i = 0; i < 4; i++) ctx->plane[i].release(&ctx->held);
+    for (int i = 0; i < 3; i++) ctx->vi_clip[i].release(&ctx->held);
+    for (int i = 0; i < 5; i++) ctx->vi_wire[i].release(&ctx->held);
+    ctx->vi_out.release(&ctx->held);
     for (auto& L : ctx->lanes) {
         for (auto& kv : L.graphs) drop_graph(kv.second);
         if (L.ev_fork) cudaEventDestroy(L.ev_fork);

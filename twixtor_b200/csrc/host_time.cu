@@ -42,8 +42,9 @@ struct SpeedCurve {  // crates/fx-core/src/curves.rs:348-375, :537-544
     }
 };
 
-// timeline.rs:266-331 (Speed mode, Src Time Offset 0, equal rates after "In FPS is Out FPS")
-float src_pos(const SpeedCurve& c, int lts, float t, bool* unsupported) {
+// timeline.rs:266-331 (Speed mode, Src Time Offset 0); `ratio` is in_fps / out_fps (1 for the
+// retime effect with "In FPS is Out FPS")
+float src_pos(const SpeedCurve& c, int lts, float t, bool* unsupported, double ratio = 30.0 / 30.0) {
     float lts_f = (float)lts;
     float out = 0.0f;
     int n2 = cvtt_i32_f(t * 2.0f);
@@ -62,7 +63,7 @@ float src_pos(const SpeedCurve& c, int lts, float t, bool* unsupported) {
         float sp = (float)((double)float_to_fixed(c.at(time, lts)) / 6553600.0);
         out = ((rem * sp) / 2.0f) + out;
     }
-    return (float)((30.0 / 30.0) * (double)out);
+    return (float)(ratio * (double)out);
 }
 
 }  // namespace
@@ -95,6 +96,51 @@ extern "C" int tw_select(const tw_time_params* p, int32_t n, int32_t width, int3
     int vq = p->vectors - 1;
     out->vectors_quality = (width >= 2 && height >= 2) ? vq : 0;
     out->interp = p->frame_interp - 1;
+    return TW_OK;
+}
+
+// plugins/vectors-in/src/timemap.rs and glue.rs:204-215: the Speed map of the retime effect with the
+// rates of the Vectors In effect (In FPS is Out FPS: the input rate 30, the output rate the
+// composition's), the constant vectors quality 4 (prep.rs:111-117 for sides of 1), and the clip
+// frames of the pair at T(k) = trunc(dur * k + 0.5) ticks (timemap.rs:45-50).
+extern "C" int tw_select_vectors_in(const tw_time_params* p, int32_t n, int32_t width, int32_t height,
+                                    tw_selection* out, tw_vecin_frame* frame) {
+    if (!p || !out || !frame || p->fps_num <= 0 || p->fps_den <= 0) return TW_ERR_BAD_PARAM;
+    if (p->nkeys > 0 && (!p->key_frames || !p->key_values)) return TW_ERR_BAD_PARAM;
+    int lts = p->fps_den == 1 ? 100 : p->fps_den;
+    double comp = (double)p->fps_num / (double)p->fps_den;
+    if (0.01 > comp) return TW_ERR_BAD_PARAM;  // timeline.rs:125-127 (the rate check)
+    double ratio = 30.0 / comp;
+    float dur = (float)(((double)lts * comp) / 30.0);  // timeline.rs:128
+    SpeedCurve c{p};
+    int cur = n * lts;
+    float t0 = (float)cur / (float)lts;
+    float t1 = ((float)lts + (float)cur) / (float)lts;
+    bool bad = false;
+    float s0 = src_pos(c, lts, t0, &bad, ratio);
+    float s1 = src_pos(c, lts, t1, &bad, ratio);
+    if (bad) return TW_ERR_UNSUPPORTED;
+    float blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
+    int a = cvtt_i32_f(s0);
+    out->s0 = s0;
+    out->s1 = s1;
+    out->a = a;
+    out->b = (int32_t)((uint32_t)a + 1u);
+    out->wa = 1.0f - (s0 - (float)a);
+    bool exact = true;
+    float fr = s0 - std::floor(s0);
+    if ((double)std::fabs(fr) > 0.005 && (double)std::fabs((float)((double)fr - 1.0)) > 0.005) exact = false;
+    if ((double)std::fabs(s0 - s1) > 1e-6 && (double)blur > 0.005) exact = false;
+    out->exact = exact ? 1 : 0;
+    out->vectors_quality = (width >= 2 && height >= 2) ? 4 : 0;
+    out->interp = p->frame_interp - 1;
+    auto clip_index = [&](int32_t pos) -> int32_t {  // the clip frame shown at T(pos) ticks
+        int32_t time = cvtt_i32_d((double)dur * (double)(float)pos + 0.5);
+        long long idx = time >= 0 ? time / lts : -(((long long)-time + lts - 1) / lts);
+        return (int32_t)std::max<long long>(std::min<long long>(idx, INT32_MAX), INT32_MIN);
+    };
+    frame->a = clip_index(out->a);
+    frame->b = clip_index(out->b);
     return TW_OK;
 }
 

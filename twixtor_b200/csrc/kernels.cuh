@@ -203,6 +203,8 @@ __global__ void k_cov_holes(const uint8_t* __restrict__ c1, const uint8_t* __res
                             long n, int* __restrict__ any_hole);
 __global__ void k_mask_holes(const void* __restrict__ mask, int kind, uint8_t* __restrict__ holes, long n,
                              int* __restrict__ any_hole);
+// The format code of an interleaved 2 channel flow in the hole fill (k_fill_load, k_fill_store, fill_dev)
+constexpr int FILL_FLOW = 3;
 __global__ void k_fill_load(const void* __restrict__ img, int fmt, const uint8_t* __restrict__ holes,
                             float* __restrict__ stack, long n, const int* __restrict__ any_hole);
 // n: 3 (blur5) or 6 (Gaussian r5) taps; dir: 0 horizontal, 1 vertical below first, 2 vertical above
@@ -211,7 +213,7 @@ __global__ void k_stack_pass(const float* __restrict__ src, float* __restrict__ 
                              int n, int dir, int rule, const int* __restrict__ any_hole);
 __global__ void k_stack_resample(const float* __restrict__ src, int sw, int sh, long sstride, float* __restrict__ dst,
                                  int dw, int dh, long dstride, int rule, const int* __restrict__ any_hole);
-__global__ void k_fill_combine(float* __restrict__ sol, const float* __restrict__ vals, long n, int rule,
+__global__ void k_fill_combine(float* __restrict__ sol, const float* __restrict__ vals, long n, int nc, int rule,
                                const int* __restrict__ any_hole);
 __global__ void k_fill_store(void* __restrict__ img, int fmt, const float* __restrict__ sol, long n,
                              const int* __restrict__ any_hole);
@@ -377,5 +379,23 @@ constexpr int ADJ_BOX_PX = 1536;                            // the shared image 
 // dynamic shared memory: two image tiles (float4) and two flow tiles ((TX + 2) x (TY + 2) x 2 floats)
 constexpr int ADJ_SMEM = 2 * ADJ_BOX_PX * 16 + 2 * (ADJ_TX + 2) * (ADJ_TY + 2) * 2 * 4;
 __global__ void k_warp_blend_adjoint(AdjParams P);
+
+// ---- Vectors In (vecin.cu) ----
+// vectors.rs:474-528 + :555-561 with the hole rule of holefill.rs:124-133: the flow of an encoded
+// engine image (interleaved) and its hole flags (the inverted alpha at or above eps), *any_hole set
+// when one is a hole
+__global__ void k_vec_decode(const void* __restrict__ vec, int fmt, float md, float2* __restrict__ flow,
+                             uint8_t* __restrict__ holes, long n, int* __restrict__ any_hole);
+// vectors.rs:573-578: Vec Scale
+__global__ void k_vec_scale(float2* __restrict__ flow, long n, float sx, float sy);
+// compose/vector.rs:376-384: T = (-1 * 1, -1 * fx, -1 * fy, -1 * 1)
+__global__ void k_invert_prep(const float2* __restrict__ flow, float4* __restrict__ t, long n);
+// compose/vector.rs:386-395: channels 1 and 2 of the pushed image as the flow, the inverted coverage
+// as the holes (a hole where 255 - coverage is not 0)
+__global__ void k_invert_take(const float4* __restrict__ pushed, const uint8_t* __restrict__ cov,
+                              float2* __restrict__ flow, uint8_t* __restrict__ holes, long n, int* __restrict__ any_hole);
+// plugins/vectors-in/src/vectorin.rs:125-155: the alpha of an engine image capped by a matte in
+// the units of the depth
+__global__ void k_matte_step(void* __restrict__ img, int fmt, const float* __restrict__ matte, long n);
 
 }  // namespace tw

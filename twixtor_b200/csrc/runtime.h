@@ -161,6 +161,7 @@ struct tw_ctx {
     DevBuf fc_img[2], fc_cov[2];  // the forward compositions: the two pushed frames and their coverage
     DevBuf wb_wt[2], wb_tmp[2], wb_mask[2], wb_cov[2];  // Weighted Blend (the calls on the context's stream)
     DevBuf pre_blur, comp_e;  // Blur Compensation: the composite before the blur, the engine result
+    DevBuf vi_clip[3], vi_out, vi_wire[5];  // Vectors In: the clips on the device, the output clip, one frame's wires
     bool adj_smem_set = false;  // the adjoint kernel's dynamic shared memory limit is raised
     DevBuf host_stage;  // unused placeholder for pinned staging
     std::vector<cudaEvent_t> ev_pool;  // the profiler's events (KernelProfile)
@@ -346,6 +347,13 @@ int interpolate_dev(tw_ctx* ctx, const tw_selection& sel, const void* eng_a, con
 
 // host_clips.cu
 void from_frame_dev(tw_ctx* ctx, const void* wire, void* eng, int W, int H, int fmt, bool flip);
+void to_frame_dev(tw_ctx* ctx, const void* eng, void* wire, int W, int H, int fmt, bool flip);
+
+// host_vecin.cu
+int vec_flow_dev(tw_ctx* ctx, const void* vec, int W, int H, int fmt, float md, float sx, float sy, bool above_first,
+                 float* flow, uint8_t* holes, int* any, DevBuf& fillbuf);
+int invert_flow_dev(tw_ctx* ctx, const float* flow, int W, int H, bool pyramid, bool above_first, float* out,
+                    float* t, float* pushed, uint8_t* holes, int* any, DevBuf& fillbuf);
 
 }  // namespace tw
 

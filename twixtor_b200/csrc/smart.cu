@@ -229,6 +229,15 @@ __device__ __forceinline__ void fill_load_px(const void* img, const uint8_t* hol
     stack[4 * n + i] = hole ? 0.0f : 1.0f;
 }
 
+// holefill.rs:510-517: the two components of an interleaved flow (FILL_FLOW) as value planes
+__device__ __forceinline__ void fill_load_flow(const void* img, const uint8_t* holes, float* stack, long n, long i) {
+    float2 v = ((const float2*)img)[i];
+    bool hole = holes[i] != 0;
+    stack[i] = hole ? 0.0f : v.x;
+    stack[n + i] = hole ? 0.0f : v.y;
+    stack[2 * n + i] = hole ? 0.0f : 1.0f;
+}
+
 __global__ void k_fill_load(const void* __restrict__ img, int fmt, const uint8_t* __restrict__ holes,
                             float* __restrict__ stack, long n, const int* __restrict__ any_hole) {
     if (!*any_hole) return;
@@ -236,6 +245,7 @@ __global__ void k_fill_load(const void* __restrict__ img, int fmt, const uint8_t
     if (i >= n) return;
     if (fmt == 0) fill_load_px<uint8_t>(img, holes, stack, n, i);
     else if (fmt == 1) fill_load_px<uint16_t>(img, holes, stack, n, i);
+    else if (fmt == FILL_FLOW) fill_load_flow(img, holes, stack, n, i);
     else fill_load_px<float>(img, holes, stack, n, i);
 }
 
@@ -341,16 +351,16 @@ __global__ void k_stack_resample(const float* __restrict__ src, int sw, int sh, 
     else stack_resample<false>(src, sw, sh, sstride, dst, dw, dh, dstride);
 }
 
-// holefill.rs:371-377: sol = weight != 0 ? value / weight : sol, for the four channels
-__global__ void k_fill_combine(float* __restrict__ sol, const float* __restrict__ vals, long n, int rule,
+// holefill.rs:371-377: sol = weight != 0 ? value / weight : sol, for the nc channels (4 of an
+// engine image, 2 of a flow); the weights are plane nc of the level's stack
+__global__ void k_fill_combine(float* __restrict__ sol, const float* __restrict__ vals, long n, int nc, int rule,
                                const int* __restrict__ any_hole) {
     if (!*any_hole) return;
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    float wt = vals[4 * n + i];
+    float wt = vals[nc * n + i];
     if (wt != 0.0f) {
-#pragma unroll
-        for (int c = 0; c < 4; c++)
+        for (int c = 0; c < nc; c++)
             sol[c * n + i] = rule ? Ar<true>::div(vals[c * n + i], wt) : Ar<false>::div(vals[c * n + i], wt);
     }
 }
@@ -373,6 +383,7 @@ __global__ void k_fill_store(void* __restrict__ img, int fmt, const float* __res
     if (i >= n) return;
     if (fmt == 0) fill_store_px<uint8_t>(img, sol, n, i);
     else if (fmt == 1) fill_store_px<uint16_t>(img, sol, n, i);
+    else if (fmt == FILL_FLOW) ((float2*)img)[i] = make_float2(sol[i], sol[n + i]);
     else fill_store_px<float>(img, sol, n, i);
 }
 
