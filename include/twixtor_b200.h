@@ -429,25 +429,41 @@ int tw_to_frame(tw_ctx* ctx, const void* engine, int32_t width, int32_t height, 
 
 /* ---- the time model of the `retime` effect (host scalars) ---------------------------------- */
 
-/* The parameters the Speed time map and the frame selection read (plugins/retime/src/lib.rs:59-99
- * as frontend::read_settings reads them, frontend.rs:184-244). Popups carry their raw 1-based
- * values. The speed curve is constant (nkeys == 0) or keyed at frame numbers, linear between keys
- * or eased where a key's ease flag is set (crates/fx-core/src/curves.rs:348-375, :537-544).
- * "In FPS is Out FPS" and Src Time Offset are at their defaults (on, 0). */
+/* The parameters the time map and the frame selection read (plugins/retime/src/lib.rs:59-99 as
+ * frontend::read_settings reads them, frontend.rs:184-244; timeline.rs:106-131, :204-344). Popups
+ * carry their raw 1-based values. A curve is constant (no key) or keyed at frame numbers, linear
+ * between keys, eased at a key whose flag has bit 0, held after a key whose flag has bit 1
+ * (crates/fx-core/src/curves.rs:282-310, :348-375, :537-544). Src Time Offset is 0. A zeroed tail
+ * (remap_mode .. frame_time_bias) is the Speed mode with "In FPS is Out FPS" on. */
 typedef struct tw_time_params {
     int32_t fps_num, fps_den;  /* the host's frame rate; integer rates get 100 ticks a frame */
     double speed_percent;
     int32_t nkeys;
     const double* key_frames;
     const double* key_values;
-    const int32_t* key_ease;
+    const int32_t* key_ease;   /* per key flags: 1 ease, 2 hold */
     int32_t vectors;           /* Motion Vectors popup 1..5 */
     int32_t frame_interp;      /* Frame Interp popup 1..3 */
     double blur_compensation;
+    int32_t remap_mode;        /* Time Remap Mode popup: 1 Speed (0 reads as 1), 2 Frame Number */
+    double frame_num;          /* Frame Num (Frame Number mode), constant when nfn_keys == 0 */
+    int32_t nfn_keys;
+    const double* fn_key_frames;
+    const double* fn_key_values;
+    const int32_t* fn_key_flags;
+    int32_t own_input_rate;    /* "In FPS is Out FPS" off: the input rate input_frame_rate (narrowed to
+                                  float), the output rate fps; both snapped (timeline.rs:69-76) */
+    double input_frame_rate;
+    double frame_time_bias;    /* the bias of the frame time between unequal rates (timeline.rs:25): 0
+                                  reads as 0.05, the reference's value; 0.1 the revision its parity
+                                  grids record */
 } tw_time_params;
 
 /* The selection of output frame n of a clip of width x height (timeline::select, timeline.rs:
- * 451-469, with RemapTimeMap::src_pos :266-331 and the tiny-frame rule prep.rs:111-117). */
+ * 451-469, with RemapTimeMap::src_pos :266-331 and the tiny-frame rule prep.rs:111-117). out->a and
+ * out->b are the CLIP frames of the pair, the frames positions a and a + 1 show at frame_time
+ * (host.rs:155-159, timeline.rs:336-344), which the clip calls read; with equal rates they are the
+ * positions themselves. TW_ERR_BAD_PARAM for a rate at or below 0.01 (timeline.rs:125-127). */
 int tw_select(const tw_time_params* p, int32_t n, int32_t width, int32_t height, tw_selection* out);
 
 /* ---- Vectors In (plugins/vectors-in, compose/vector.rs:323-447) ----------------------------- */
@@ -465,10 +481,10 @@ typedef struct tw_vecin_frame {
 } tw_vecin_frame;
 
 /* The selection of output frame n of the Vectors In effect (plugins/vectors-in/src/timemap.rs,
- * glue.rs:204-215): the Speed map of tw_select with the input rate 30 and the output rate the
- * composition's (In FPS is Out FPS on), the vectors quality 4 (p->vectors is not read), and in
- * frame->a / frame->b the clip frames of the pair at T(k) = trunc(dur * k + 0.5) ticks. The
- * other fields of `frame` are left as they are. */
+ * glue.rs:204-215): the time map of tw_select with the input rate 30 (In FPS is Out FPS on; else
+ * p->input_frame_rate) and the output rate the composition's, the vectors quality 4 (p->vectors is
+ * not read), out->a / out->b the positions, and in frame->a / frame->b the clip frames of the pair
+ * at T(k) = trunc(dur * k + 0.5) ticks. The other fields of `frame` are left as they are. */
 int tw_select_vectors_in(const tw_time_params* p, int32_t n, int32_t width, int32_t height, tw_selection* out,
                          tw_vecin_frame* frame);
 

@@ -39,12 +39,25 @@ struct Key {
     long long time;
     double value;
     bool ease;
+    bool hold;
 };
 
-// crates/fx-core/src/curves.rs:348-375 and :537-544: a float curve (constant when no key)
+// crates/fx-core/src/curves.rs:282-310, :348-375 and :537-544: a float curve (constant when no
+// key), keys sorted by time, a held key keeps its value up to the next
 struct Curve {
     double constant = 0.0;
     std::vector<Key> keys;
+    // keys at frames (ticks: frame * lts rounded half away from zero, time.rs:117-119); flags bit 0
+    // ease, bit 1 hold
+    void set(int n, const double* frames, const double* values, const int* flags, int lts) {
+        keys.clear();
+        for (int i = 0; i < n; i++) {
+            long long t = (long long)std::llround(frames[i] * (double)lts);
+            int f = flags ? flags[i] : 0;
+            keys.push_back({t, values[i], (f & 1) != 0, (f & 2) != 0});
+        }
+        std::stable_sort(keys.begin(), keys.end(), [](const Key& a, const Key& b) { return a.time < b.time; });
+    }
     double at(long long time) const {
         if (keys.empty()) return constant;
         size_t last = keys.size() - 1;
@@ -53,6 +66,7 @@ struct Curve {
         size_t i = 0;
         while (i + 1 < keys.size() && keys[i + 1].time <= time) i++;
         const Key &a = keys[i], &b = keys[i + 1];
+        if (a.hold) return a.value;
         double u = (double)(time - a.time) / (double)(b.time - a.time);
         double f;
         if (!a.ease && !b.ease) f = u;
@@ -84,14 +98,23 @@ int32_t cvtt_i32_f(float x) {  // timeline.rs:52-58
 }
 
 struct TimeMap {
+    double frame_time_k = 0.05;  // FRAME_TIME_K (timeline.rs:25)
     Curve speed;
+    int remap_mode = 1;  // Time Remap Mode: 1 Speed, 2 Frame Number
+    Curve frame_num;
     double in_fps = 30.0, out_fps = 30.0;
     float dur = 100.0f;
     int lts = 100;
     int base = 0;
-    // timeline.rs:266-331 (Speed mode; Src Time Offset 0)
+    // timeline.rs:266-331 (Src Time Offset 0)
     float src_pos(float t) {
         float lts_f = (float)lts;
+        if (remap_mode == 2) {  // Frame Number: the curve at trunc((lts * t) + K), times in / out
+            base = 0;
+            int time = cvtt_i32_d((double)(lts_f * t) + 0.05);
+            float v = (float)frame_num.at(time);
+            return (float)((in_fps / out_fps) * (double)v);
+        }
         float out = 0.0f;
         int time0 = cvtt_i32_d((double)(lts_f * t) + 0.05);
         (void)time0;
@@ -115,8 +138,8 @@ struct TimeMap {
     }
     int frame_time(float f) const {  // timeline.rs:336-344
         float d = f - (float)base;
-        if (std::fabs(in_fps - out_fps) < 0.05) return cvtt_i32_d((double)d * (double)dur + 0.5);
-        return cvtt_i32_d((double)(d * dur) + (double)dur * 0.05);
+        if (std::fabs(in_fps - out_fps) < frame_time_k) return cvtt_i32_d((double)d * (double)dur + 0.5);
+        return cvtt_i32_d((double)(d * dur) + (double)dur * frame_time_k);
     }
 };
 
@@ -142,7 +165,7 @@ struct or_retime_params {
     int nkeys;                 // keyed Speed % (0: constant)
     const double* key_frames;  // frame numbers of the keys
     const double* key_values;
-    const int* key_ease;
+    const int* key_ease;       // per key: bit 0 ease, bit 1 hold
     int vectors;               // popup 1..5 (5 Best)
     int frame_interp;          // popup 1..3 (2 Blend)
     int smart_blend;
@@ -156,7 +179,57 @@ struct or_retime_params {
     int video_360;             // "360 Video": video range luma, binary alpha Smart Blend
     int prep;                  // Image Prep popup: 1 None, 2 Contrast/Edge Enhance, 3 Delinearize
     int track_rgb_a;           // retime-fgbg's Track RGB+A (alpha in the luma; the layered pyramids' 360 filters)
+    // the rest of the time model (timeline.rs:106-131, :266-344): Time Remap Mode (0 or 1 Speed,
+    // 2 Frame Number) with Frame Num constant or keyed, and "In FPS is Out FPS" off (own_input_rate:
+    // the input rate Input: Frame Rate, the output rate the composition's)
+    int remap_mode;
+    double frame_num;
+    int nfn_keys;
+    const double* fn_key_frames;
+    const double* fn_key_values;
+    const int* fn_key_ease;    // per key: bit 0 ease, bit 1 hold
+    int own_input_rate;
+    double input_frame_rate;
+    // the bias of the frame time between unequal rates (timeline.rs:25, :336-344): 0 reads as 0.05,
+    // the reference's current value; 0.1 is the revision the parity grids record
+    double frame_time_bias;
 };
+
+// timeline.rs:69-76: a rate within 2e-5 (an f32 difference) of 29.97, 59.94 or 23.976 becomes it
+static double snap_rate(double rate) {
+    for (double t : {29.97, 59.94, 23.976})
+        if ((double)std::fabs((float)(rate - t)) < 2e-5) rate = t;
+    return rate;
+}
+
+// The time map of the `retime` effect for its parameters (timeline.rs:106-131, the curves of
+// frontend.rs:184-244). Returns the ticks per frame.
+static int retime_map(const or_retime_params* p, TimeMap* map) {
+    bool integer = p->fps_den == 1;
+    int time_step = integer ? 100 : p->fps_den;
+    double in = 30.0, out = 30.0;  // In FPS is Out FPS (default on): both rates 30 (timeline.rs:117-120)
+    if (p->own_input_rate) {
+        in = (double)((float)p->input_frame_rate * 1.0f);
+        out = (double)p->fps_num / (double)p->fps_den;
+    }
+    map->lts = time_step;
+    if (p->frame_time_bias > 0.0) map->frame_time_k = p->frame_time_bias;
+    map->in_fps = snap_rate(in);
+    map->out_fps = snap_rate(out);
+    map->dur = (float)(((double)time_step * map->out_fps) / map->in_fps);
+    map->speed.constant = p->speed_percent;
+    map->speed.set(p->nkeys, p->key_frames, p->key_values, p->key_ease, time_step);
+    map->remap_mode = p->remap_mode == 2 ? 2 : 1;
+    map->frame_num.constant = p->frame_num;
+    map->frame_num.set(p->nfn_keys, p->fn_key_frames, p->fn_key_values, p->fn_key_ease, time_step);
+    return time_step;
+}
+
+// The clip frame a position shows: host.rs:155-159 (frame_time) and the frame of that tick
+static long long clip_frame(const TimeMap& map, int pos) {
+    int time = map.frame_time((float)pos);
+    return time >= 0 ? time / map.lts : -(((long long)-time + map.lts - 1) / map.lts);
+}
 
 const char* or_last_error(void) { return g_err.c_str(); }
 
@@ -550,18 +623,8 @@ int or_compose_vectors3(const void* a_eng, const void* b_eng, int w, int h, int 
 // One output frame's selection (timeline.rs:451-469) for output frame index n of a clip.
 int or_select(const or_retime_params* p, int n, int w, int h, float* s0, float* s1, int* a, float* wa, int* exact,
               int* vq, int* interp) {
-    bool integer = p->fps_den == 1;
-    int time_step = integer ? 100 : p->fps_den;
     TimeMap map;
-    map.lts = time_step;
-    map.in_fps = 30.0;  // In FPS is Out FPS (default on): both rates 30 (timeline.rs:117-120)
-    map.out_fps = 30.0;
-    map.dur = (float)(((double)time_step * 30.0) / 30.0);
-    map.speed.constant = p->speed_percent;
-    for (int i = 0; i < p->nkeys; i++) {
-        long long t = (long long)std::llround(p->key_frames[i] * (double)time_step);
-        map.speed.keys.push_back({t, p->key_values[i], p->key_ease && p->key_ease[i] != 0});
-    }
+    int time_step = retime_map(p, &map);
     int cur = n * time_step;
     float t0 = (float)cur / (float)time_step;
     float t1 = ((float)time_step + (float)cur) / (float)time_step;
@@ -575,6 +638,18 @@ int or_select(const or_retime_params* p, int n, int w, int h, float* s0, float* 
     int vqr = p->vectors - 1;
     *vq = (w >= 2 && h >= 2) ? vqr : 0;  // prep.rs:111-117
     *interp = p->frame_interp - 1;
+    return 0;
+}
+
+// The clip frames output frame n's positions a and a + 1 show (host.rs:155-159)
+int or_clip_frames(const or_retime_params* p, int n, int w, int h, int* clip_a, int* clip_b) {
+    float s0, s1, wa;
+    int a, exact, vq, interp;
+    or_select(p, n, w, h, &s0, &s1, &a, &wa, &exact, &vq, &interp);
+    TimeMap map;
+    retime_map(p, &map);
+    *clip_a = (int)clip_frame(map, a);
+    *clip_b = (int)clip_frame(map, a + 1);
     return 0;
 }
 
@@ -598,11 +673,10 @@ static int retime_one(const void* frames, int nframes, int w, int h, int fmt, co
     int a, exact, vq, interp;
     or_select(p, n, w, h, &s0, &s1, &a, &wa, &exact, &vq, &interp);
     bool outside_window = false;
+    TimeMap map;
+    retime_map(p, &map);
     auto fetch = [&](int pos) -> Image {
-        // main_frame(position): frame_time (dur == lts, equal rates), then the clip frame of that tick
-        double d = (double)(float)pos;
-        int time = cvtt_i32_d(d * (double)time_step + 0.5);
-        long long idx = time >= 0 ? time / time_step : -(((long long)-time + time_step - 1) / time_step);
+        long long idx = clip_frame(map, pos);  // main_frame(position): frame_time, then the clip frame of that tick
         if (idx < 0 || idx >= nframes) return Image(w, h, f);
         if (idx < first || idx >= (long long)first + count) { outside_window = true; return Image(w, h, f); }
         return from_frame((const uint8_t*)frames + (size_t)(idx - first) * frame_bytes, w, h, f);
@@ -736,10 +810,10 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
     int a, exact, vq, interp;
     or_select(p, n, w, h, &s0, &s1, &a, &wa, &exact, &vq, &interp);
     // the FG matte frames are read straight (plugins/retime-fgbg/src/glue.rs:335, host.rs:311-314)
+    TimeMap map;
+    retime_map(p, &map);
     auto fetch = [&](const void* clip, int pos, bool straight) -> Image {
-        double d = (double)(float)pos;
-        int time = cvtt_i32_d(d * (double)time_step + 0.5);
-        long long idx = time >= 0 ? time / time_step : -(((long long)-time + time_step - 1) / time_step);
+        long long idx = clip_frame(map, pos);
         if (idx < 0 || idx >= nframes) return Image(w, h, f);
         const uint8_t* fr = (const uint8_t*)clip + (size_t)idx * frame_bytes;
         return straight ? from_frame_straight(fr, w, h, f) : from_frame(fr, w, h, f);
@@ -1070,7 +1144,7 @@ struct or_vecin_params {
     int nkeys;                 // keyed Speed % (0: constant)
     const double* key_frames;
     const double* key_values;
-    const int* key_ease;
+    const int* key_ease;       // per key: bit 0 ease, bit 1 hold
     int frame_interp;          // popup 1..3
     int warping;               // popup: 1 Inverse, 2 Forward (glue.rs:94-100)
     double blur_compensation;
@@ -1085,6 +1159,15 @@ struct or_vecin_params {
     // the reference's current code); 1 present only where its clip has a frame at the output
     // frame's time, the error fill when neither is (the revision the parity grid records)
     int probe_current_time;
+    // Time Remap Mode (0 or 1 Speed, 2 Frame Number) and Frame Num, constant or keyed
+    int remap_mode;
+    double frame_num;
+    int nfn_keys;
+    const double* fn_key_frames;
+    const double* fn_key_values;
+    const int* fn_key_ease;    // per key: bit 0 ease, bit 1 hold
+    int own_input_rate;        // In FPS is Out FPS off: the input rate Input: Frame Rate
+    double input_frame_rate;
 };
 
 // compose/vector.rs:329-345 (flow_from_vector_image_with) over an engine image, for the tests
@@ -1146,15 +1229,16 @@ static int vecin_select(const or_vecin_params* p, int n, int w, int h, TimeMap* 
     bool integer = p->fps_den == 1;
     int time_step = integer ? 100 : p->fps_den;
     double comp = (double)p->fps_num / (double)p->fps_den;
+    double in = p->own_input_rate ? (double)((float)p->input_frame_rate * 1.0f) : 30.0;
     map->lts = time_step;
-    map->in_fps = 30.0;
-    map->out_fps = comp;
-    map->dur = (float)(((double)time_step * comp) / 30.0);
+    map->in_fps = snap_rate(in);
+    map->out_fps = snap_rate(comp);
+    map->dur = (float)(((double)time_step * map->out_fps) / map->in_fps);
     map->speed.constant = p->speed_percent;
-    for (int i = 0; i < p->nkeys; i++) {
-        long long t = (long long)std::llround(p->key_frames[i] * (double)time_step);
-        map->speed.keys.push_back({t, p->key_values[i], p->key_ease && p->key_ease[i] != 0});
-    }
+    map->speed.set(p->nkeys, p->key_frames, p->key_values, p->key_ease, time_step);
+    map->remap_mode = p->remap_mode == 2 ? 2 : 1;
+    map->frame_num.constant = p->frame_num;
+    map->frame_num.set(p->nfn_keys, p->fn_key_frames, p->fn_key_values, p->fn_key_ease, time_step);
     int cur = n * time_step;
     float t0 = (float)cur / (float)time_step;
     float t1 = ((float)time_step + (float)cur) / (float)time_step;

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference tree (its path is required):
 
-    python tests/golden/make_golden.py --reference <reference tree> [--only flow_models|vectors_in]
+    python tests/golden/make_golden.py --reference <reference tree> [--only flow_models|vectors_in|retime_time]
 
 Writes, next to this script:
 
@@ -45,9 +45,14 @@ Writes, next to this script:
 * ``warp_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/warp_cases.hex``
   (the reference's bit-exact numpy model of the inverse warp; format in its ``gen_warp.py``).
 
+* ``retime_time_grid.npz`` - the cases of the reference's parity grid ``parity/retime-time`` (the
+  time model with No Vectors: Speed and Frame Number modes, constant or keyed without Bezier
+  handles, In FPS is Out FPS and the input rate, Frame Interp; integer composition rates, no Src
+  Mark Segments, no input fields), their input clips as its ``gen_grid.py`` writes them, and the
+  sha256 of the output clip ``results/base.tsv`` records.
 * ``vectors_in_grid.npz`` - the cases of the reference's parity grid ``parity/vectors-in`` that the
   single layer Vectors In render serves (one or both vector layers, no FG matte layer, Display not
-  Source, Speed mode with a constant speed, In FPS is Out FPS, integer frame rates), their footage,
+  Source, Speed or Frame Number mode, keyed or not, the input rate model, integer frame rates), their footage,
   Color Source and vector layer clips as its ``gen_grid.py`` writes them, and the sha256 of the
   output clip ``results/base.grid.tsv`` records.
 * ``vectors_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/
@@ -211,8 +216,46 @@ def fgbg_layers_grid(ref):
     print(f"fgbg_layers_grid.npz: {len(cases)} cases, {len(keys)} clips")
 
 
+RT_SERVED = {"vectors", "speed_percent", "frame_interp", "time_remap_mode", "frame_num", "in_fps_is_out_fps",
+             "input_frame_rate"}
+
+
+def retime_time_grid(ref):
+    root = os.path.join(ref, "parity", "retime-time")
+    spec = importlib.util.spec_from_file_location("rt_gen", os.path.join(root, "gen_grid.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    table = {}
+    for line in open(os.path.join(root, "results", "base.tsv")):
+        parts = line.rstrip("\n").split("\t")
+        if parts[0] != "id":
+            table[parts[0]] = (parts[1], parts[3])
+    g = gen.build()
+    cases, inputs = [], {}
+    for c in g.cases:
+        params = dict(p.split("=", 1) for p in c["params"])
+        if any(k not in RT_SERVED for k in params):
+            continue
+        if any(ch in v for v in params.values() for ch in "io"):  # Bezier handles: not served
+            continue
+        if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
+            continue
+        key = c["input"]
+        if key not in inputs:
+            src, w, h, d, fr = c["source"], c["width"], c["height"], c["depth"], c["frames"]
+            inputs[key] = np.frombuffer(gen.clip_bytes(src, d, w, h, fr, gen.fnv("%s%dx%dd%d" % (src, w, h, d)) & 0xFFFF),
+                                        np.uint8)
+        cases.append(dict(id=c["id"], params=c["params"], depth=c["depth"], width=c["width"], height=c["height"],
+                          frames=c["frames"], fps=c["fps"], input=key, sha256=table[c["id"]][1]))
+    keys = sorted(inputs)
+    arrays = {f"input_{i}": inputs[k] for i, k in enumerate(keys)}
+    arrays["meta"] = np.frombuffer(json.dumps(dict(inputs=keys, cases=cases)).encode(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "retime_time_grid.npz"), **arrays)
+    print(f"retime_time_grid.npz: {len(cases)} cases, {len(keys)} clips")
+
+
 VI_SERVED = {"vectors_max_displace", "speed_percent", "warping", "frame_interp", "blur_compensation", "vec_scale_x",
-             "vec_scale_y", "display"}
+             "vec_scale_y", "display", "time_remap_mode", "frame_num", "in_fps_is_out_fps", "input_frame_rate"}
 
 
 def vectors_in_grid(ref):
@@ -237,7 +280,9 @@ def vectors_in_grid(ref):
 
         for c in g.cases:
             params = dict(p.split("=", 1) for p in c["params"])
-            if any(k not in VI_SERVED for k in params) or any("@" in v for v in params.values()):
+            if any(k not in VI_SERVED for k in params):
+                continue
+            if any("@" in v for k, v in params.items() if k not in ("speed_percent", "frame_num")):
                 continue
             if params.get("display", "1") == "2":
                 continue
@@ -295,7 +340,8 @@ def flow_models(ref):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="the reference tree (baairon/twixtor)")
-    ap.add_argument("--only", choices=["flow_models", "vectors_in"], default=None, help="write one fixture only")
+    ap.add_argument("--only", choices=["flow_models", "vectors_in", "retime_time"], default=None,
+                    help="write one fixture (set) only")
     args = ap.parse_args()
     ref = args.reference
     if args.only == "flow_models":
@@ -305,6 +351,10 @@ def main():
         vectors_in_grid(ref)
         vectors_cases(ref)
         return
+    if args.only == "retime_time":
+        retime_time_grid(ref)
+        return
+    retime_time_grid(ref)
     vectors_in_grid(ref)
     vectors_cases(ref)
     flow_models(ref)

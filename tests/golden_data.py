@@ -404,7 +404,11 @@ def vi_case_params(case):
     """Keyword arguments of oracle_lib.vecin_params for a vectors-in grid case (the effect's
     defaults where the case sets none: Speed 100, Max Displace 2048, Blend, Forward, scale 1)."""
     p = dict(x.split("=", 1) for x in case["params"])
-    return dict(fps=(int(case["fps"]), 1), speed=float(p.get("speed_percent", 100)),
+    keys, speed = parse_keys(p.get("speed_percent", "100"))
+    fn_keys, fnum = parse_keys(p.get("frame_num", "0"))
+    return dict(fps=(int(case["fps"]), 1), speed=speed, keys=keys, remap_mode=int(p.get("time_remap_mode", 1)),
+                frame_num=fnum, fn_keys=fn_keys, own_input_rate=p.get("in_fps_is_out_fps", "1") == "0",
+                input_frame_rate=float(p.get("input_frame_rate", float(np.float32(29.97)))),
                 frame_interp=int(p.get("frame_interp", 2)), warping=int(p.get("warping", 2)),
                 blur=float(p.get("blur_compensation", 0)), max_displace=float(p.get("vectors_max_displace", 2048)),
                 vec_scale=(float(p.get("vec_scale_x", 1)), float(p.get("vec_scale_y", 1))))
@@ -441,3 +445,36 @@ def vectors_cases():
                             image=img))
     assert p == len(blob), (p, len(blob))
     return out
+
+
+def rt_grid():
+    """The served cases of the retime-time parity grid: (meta cases, {clip name: raw bytes})."""
+    z = np.load(os.path.join(GOLDEN, "retime_time_grid.npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    inputs = {name: z[f"input_{i}"] for i, name in enumerate(meta["inputs"])}
+    return meta["cases"], inputs
+
+
+def parse_keys(text):
+    """A keyed CLI value ``V@F[h|e];...`` (crates/fx-core/src/curves.rs:75-115) as (frame, value,
+    flags) triples, flags bit 0 ease, bit 1 hold; a plain value gives None and the value."""
+    if "@" not in text:
+        return None, float(text)
+    keys = []
+    for piece in text.split(";"):
+        v, f = piece.rsplit("@", 1)
+        flags = 2 if f.endswith("h") else 1 if f.endswith("e") else 0
+        keys.append((float(f.rstrip("he")), float(v), flags))
+    return keys, 0.0
+
+
+def rt_case_params(case):
+    """Keyword arguments of oracle_lib.retime_params for a retime-time grid case (the effect's
+    defaults elsewhere; Input: Frame Rate defaults to 29.97 narrowed through f32)."""
+    p = dict(x.split("=", 1) for x in case["params"])
+    keys, speed = parse_keys(p.get("speed_percent", "100"))
+    fn_keys, fnum = parse_keys(p.get("frame_num", "0"))
+    return dict(fps=(int(case["fps"]), 1), speed=speed, keys=keys, vectors=int(p.get("vectors", 5)),
+                frame_interp=int(p.get("frame_interp", 2)), remap_mode=int(p.get("time_remap_mode", 1)),
+                frame_num=fnum, fn_keys=fn_keys, own_input_rate=p.get("in_fps_is_out_fps", "1") == "0",
+                input_frame_rate=float(p.get("input_frame_rate", float(np.float32(29.97)))))

@@ -38,6 +38,15 @@ class RetimeParams(ctypes.Structure):
         ("video_360", ctypes.c_int),
         ("prep", ctypes.c_int),
         ("track_rgb_a", ctypes.c_int),
+        ("remap_mode", ctypes.c_int),
+        ("frame_num", ctypes.c_double),
+        ("nfn_keys", ctypes.c_int),
+        ("fn_key_frames", ctypes.POINTER(ctypes.c_double)),
+        ("fn_key_values", ctypes.POINTER(ctypes.c_double)),
+        ("fn_key_ease", ctypes.POINTER(ctypes.c_int)),
+        ("own_input_rate", ctypes.c_int),
+        ("input_frame_rate", ctypes.c_double),
+        ("frame_time_bias", ctypes.c_double),
     ]
 
 
@@ -61,6 +70,14 @@ class VecInParams(ctypes.Structure):
         ("taps_above_first", ctypes.c_int),
         ("gouraud", ctypes.c_int),
         ("probe_current_time", ctypes.c_int),
+        ("remap_mode", ctypes.c_int),
+        ("frame_num", ctypes.c_double),
+        ("nfn_keys", ctypes.c_int),
+        ("fn_key_frames", ctypes.POINTER(ctypes.c_double)),
+        ("fn_key_values", ctypes.POINTER(ctypes.c_double)),
+        ("fn_key_ease", ctypes.POINTER(ctypes.c_int)),
+        ("own_input_rate", ctypes.c_int),
+        ("input_frame_rate", ctypes.c_double),
     ]
 
 
@@ -107,6 +124,7 @@ def lib():
         L.or_select.argtypes = [ctypes.POINTER(RetimeParams), i, i, i, P, P, P, P, P, P, P]
         L.or_retime_clip.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_retime_one.argtypes = [P, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
+        L.or_clip_frames.argtypes = [ctypes.POINTER(RetimeParams), i, i, i, P, P]
         L.or_retime_window.argtypes = [P, i, i, i, i, i, i, ctypes.POINTER(RetimeParams), i, P]
         L.or_crt_powf.argtypes = [P, P, P, i]
         L.or_motion_blur.argtypes = [P, P, i, i, i, P, i, i, f, i, f]
@@ -437,12 +455,34 @@ def fw_triangle(verts, w1, h1, cap=4096):
     return None if n < 0 else hits[:n * 5].reshape(n, 5)
 
 
+def _keys(p, keys, prefix):
+    """Keyed curve fields of a params struct: (frame, value, ease) triples."""
+    fr = (ctypes.c_double * len(keys))(*[k[0] for k in keys])
+    va = (ctypes.c_double * len(keys))(*[k[1] for k in keys])
+    ea = (ctypes.c_int * len(keys))(*[int(k[2]) for k in keys])
+    setattr(p, "n" + prefix + "keys" if prefix else "nkeys", len(keys))
+    pre = prefix + "key_" if prefix else "key_"
+    setattr(p, pre + "frames", ctypes.cast(fr, ctypes.POINTER(ctypes.c_double)))
+    setattr(p, pre + "values", ctypes.cast(va, ctypes.POINTER(ctypes.c_double)))
+    setattr(p, pre + "ease", ctypes.cast(ea, ctypes.POINTER(ctypes.c_int)))
+    p.__dict__.setdefault("_keep", []).append((fr, va, ea))
+
+
 def retime_params(fps=(24, 1), quality_high=True, speed=100.0, keys=None, vectors=5, frame_interp=2, smart_blend=0,
                   sensitivity=70.0, blur=0.0, rows_reversed=True, taps_above_first=True, video_360=False, prep=1,
-                  track_rgb_a=False):
+                  track_rgb_a=False, remap_mode=1, frame_num=0.0, fn_keys=None, own_input_rate=False,
+                  input_frame_rate=30.0, frame_time_bias=0.05):
     """The `retime` parameters of one render. rows_reversed / taps_above_first at their defaults
-    are the reference's current code; both False is the revision the parity grid records."""
+    are the reference's current code; both False is the revision the parity grid records.
+    remap_mode 2 is Frame Number (frame_num or the keyed fn_keys); own_input_rate turns "In FPS is
+    Out FPS" off (the input rate input_frame_rate, the output rate fps); frame_time_bias 0.1 is the
+    revision the parity grids record (the reference's current value is 0.05)."""
     p = RetimeParams()
+    p.remap_mode, p.frame_num = remap_mode, frame_num
+    p.own_input_rate, p.input_frame_rate = int(own_input_rate), input_frame_rate
+    p.frame_time_bias = frame_time_bias
+    if fn_keys:
+        _keys(p, fn_keys, "fn_")
     p.rows_reversed, p.taps_above_first = int(rows_reversed), int(taps_above_first)
     p.video_360 = int(video_360)
     p.prep = int(prep)
@@ -472,6 +512,13 @@ def select(params, n, w, h):
                     ctypes.byref(wa), ctypes.byref(ex), ctypes.byref(vq), ctypes.byref(it))
     return dict(s0=s0.value, s1=s1.value, a=a.value, wa=wa.value, exact=bool(ex.value), vq=vq.value,
                 interp=it.value)
+
+
+def clip_frames(params, n, w, h):
+    """The clip frames output frame n's pair shows (its positions through frame_time)."""
+    a, b = ctypes.c_int(), ctypes.c_int()
+    lib().or_clip_frames(ctypes.byref(params), n, w, h, ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
 
 
 def retime_one(frames, nframes, w, h, fmt, params, n):
@@ -593,7 +640,8 @@ def matte_step(vec, w, h, fmt, matte):
 
 def vecin_params(fps=(30, 1), quality_high=True, speed=100.0, keys=None, frame_interp=2, warping=2, blur=0.0,
                  max_displace=2048.0, vec_scale=(1.0, 1.0), rows_reversed=True, taps_above_first=True, gouraud=True,
-                 probe_current_time=False):
+                 probe_current_time=False, remap_mode=1, frame_num=0.0, fn_keys=None, own_input_rate=False,
+                 input_frame_rate=30.0):
     """The `vectors-in` parameters of one render (the effect's defaults; the three orders at the
     plugin's: bottom-up rows, the tap above first, the Gouraud forward warp; a set vector layer
     present at every time). All four False is the revision the parity grid records."""
@@ -606,6 +654,10 @@ def vecin_params(fps=(30, 1), quality_high=True, speed=100.0, keys=None, frame_i
     p.vec_scale_x, p.vec_scale_y = vec_scale
     p.rows_reversed, p.taps_above_first, p.gouraud = int(rows_reversed), int(taps_above_first), int(gouraud)
     p.probe_current_time = int(probe_current_time)
+    p.remap_mode, p.frame_num = remap_mode, frame_num
+    p.own_input_rate, p.input_frame_rate = int(own_input_rate), input_frame_rate
+    if fn_keys:
+        _keys(p, fn_keys, "fn_")
     p.nkeys = 0
     if keys:
         fr = (ctypes.c_double * len(keys))(*[k[0] for k in keys])

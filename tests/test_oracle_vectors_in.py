@@ -4,8 +4,9 @@
   vectors_cases.hex, its gen_vectors.py): every decode case (vectors.rs:474-528) and every encode
   case (vectors.rs:57-130) bit for bit;
 * the reference's parity grid of the `vectors-in` effect (parity/vectors-in, results/base.grid.tsv):
-  the sha256 of the whole output clip of every served case. That table was recorded by the
-  revision whose render ran on top-down rows, with the vertical border taps below first, the
+  the sha256 of the whole output clip of every served case (Speed and Frame Number modes, keyed or
+  not, the input rate model). That table was recorded by the revision whose render ran on top-down
+  rows, with the vertical border taps below first, the
   textured forward warp, and a vector layer probed at the output frame's time (absent past its
   clip's end; the error fill when neither is there), so those cases run with the four orders off.
 """
@@ -44,10 +45,10 @@ GRID_ORDERS = dict(rows_reversed=False, taps_above_first=False, gouraud=False, p
 
 
 def test_vectors_in_grid_is_served():
-    assert len(VI_CASES) == 344
+    assert len(VI_CASES) == 390
     groups = {c["id"].split(".")[1].split("-")[0] for c in VI_CASES}
     assert {"size", "warp1", "warp2", "vec", "md16", "scalex2", "prev", "next", "short", "spvecR", "spvecA",
-            "spsrc", "blur1", "foot"} <= groups
+            "spsrc", "blur1", "foot", "fnum", "inrate", "ftime", "key"} <= groups, groups
 
 
 @pytest.mark.parametrize("c", VI_CASES, ids=[c["id"] for c in VI_CASES])

@@ -139,7 +139,11 @@ class _TimeParams(ctypes.Structure):
                 ("nkeys", ctypes.c_int32), ("key_frames", ctypes.POINTER(ctypes.c_double)),
                 ("key_values", ctypes.POINTER(ctypes.c_double)), ("key_ease", ctypes.POINTER(ctypes.c_int32)),
                 ("vectors", ctypes.c_int32), ("frame_interp", ctypes.c_int32),
-                ("blur_compensation", ctypes.c_double)]
+                ("blur_compensation", ctypes.c_double), ("remap_mode", ctypes.c_int32), ("frame_num", ctypes.c_double),
+                ("nfn_keys", ctypes.c_int32), ("fn_key_frames", ctypes.POINTER(ctypes.c_double)),
+                ("fn_key_values", ctypes.POINTER(ctypes.c_double)), ("fn_key_flags", ctypes.POINTER(ctypes.c_int32)),
+                ("own_input_rate", ctypes.c_int32), ("input_frame_rate", ctypes.c_double),
+                ("frame_time_bias", ctypes.c_double)]
 
 
 class _VecInFrame(ctypes.Structure):
@@ -261,14 +265,23 @@ def vectors_settings(vector_resolution=1, max_displace=2048.0, sensitivity=70.0,
 
 @dataclass
 class TimeParams:
-    """The parameters the Speed time map reads (plugins/retime/src/lib.rs:59-99). Popups carry
-    their 1-based values; ``keys`` is a list of (frame, value, ease) of a keyed Speed %."""
+    """The parameters the time map reads (plugins/retime/src/lib.rs:59-99). Popups carry their
+    1-based values; ``keys`` / ``fn_keys`` are lists of (frame, value, flags) of a keyed Speed % /
+    Frame Num (flags: True or 1 ease, 2 hold); ``remap_mode`` 2 is Frame Number; ``own_input_rate``
+    turns "In FPS is Out FPS" off (the input rate ``input_frame_rate``); ``frame_time_bias`` 0.1 is
+    the revision the reference's parity grids record (0 reads as its current 0.05)."""
     fps: Tuple[int, int] = (24, 1)
     speed_percent: float = 100.0
-    keys: Optional[Sequence[Tuple[float, float, bool]]] = None
+    keys: Optional[Sequence[Tuple[float, float, int]]] = None
     vectors: int = 5
     frame_interp: int = 2
     blur_compensation: float = 0.0
+    remap_mode: int = 1
+    frame_num: float = 0.0
+    fn_keys: Optional[Sequence[Tuple[float, float, int]]] = None
+    own_input_rate: bool = False
+    input_frame_rate: float = float(np.float32(29.97))
+    frame_time_bias: float = 0.0
 
     def _c(self):
         p = _TimeParams()
@@ -276,17 +289,25 @@ class TimeParams:
         p.speed_percent = self.speed_percent
         p.vectors, p.frame_interp = self.vectors, self.frame_interp
         p.blur_compensation = self.blur_compensation
-        p.nkeys = 0
-        if self.keys:
-            n = len(self.keys)
-            fr = (ctypes.c_double * n)(*[k[0] for k in self.keys])
-            va = (ctypes.c_double * n)(*[k[1] for k in self.keys])
-            ea = (ctypes.c_int32 * n)(*[int(k[2]) for k in self.keys])
-            p.nkeys = n
-            p.key_frames = ctypes.cast(fr, ctypes.POINTER(ctypes.c_double))
-            p.key_values = ctypes.cast(va, ctypes.POINTER(ctypes.c_double))
-            p.key_ease = ctypes.cast(ea, ctypes.POINTER(ctypes.c_int32))
-            p._keep = (fr, va, ea)
+        p.remap_mode, p.frame_num = self.remap_mode, self.frame_num
+        p.own_input_rate, p.input_frame_rate = int(self.own_input_rate), self.input_frame_rate
+        p.frame_time_bias = self.frame_time_bias
+        keep = []
+        for keys, n_attr, f_attr, v_attr, e_attr in ((self.keys, "nkeys", "key_frames", "key_values", "key_ease"),
+                                                     (self.fn_keys, "nfn_keys", "fn_key_frames", "fn_key_values",
+                                                      "fn_key_flags")):
+            setattr(p, n_attr, 0)
+            if keys:
+                n = len(keys)
+                fr = (ctypes.c_double * n)(*[k[0] for k in keys])
+                va = (ctypes.c_double * n)(*[k[1] for k in keys])
+                ea = (ctypes.c_int32 * n)(*[int(k[2]) for k in keys])
+                setattr(p, n_attr, n)
+                setattr(p, f_attr, ctypes.cast(fr, ctypes.POINTER(ctypes.c_double)))
+                setattr(p, v_attr, ctypes.cast(va, ctypes.POINTER(ctypes.c_double)))
+                setattr(p, e_attr, ctypes.cast(ea, ctypes.POINTER(ctypes.c_int32)))
+                keep.append((fr, va, ea))
+        p._keep = keep
         return p
 
 

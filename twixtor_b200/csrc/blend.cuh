@@ -54,12 +54,13 @@ template <> __device__ __forceinline__ void lerp_px<float>(float f[4], const flo
     bool rule = false;
 #pragma unroll
     for (int i = 0; i < 4; i++) rule = rule || isnan(f[i]) || isnan(s[i]);
-    if (!rule) {
-        float a = (f[0] - s[0]) * w + s[0];
+    if (!rule) {  // the processor's arithmetic: a NaN made of infinities is x86's default NaN
+        auto L = [](float a, float b, float w) { return x86::add(x86::mul(x86::sub(b, a), w), a); };
+        float a = L(s[0], f[0], w);
         if (!(a > 0.0f)) { for (int i = 0; i < 4; i++) f[i] = 0.0f; return; }
-        float r = (f[1] - s[1]) * w + s[1], g = (f[2] - s[2]) * w + s[2], b = (f[3] - s[3]) * w + s[3];
-        if (a > 1.0f) { r = r / a; g = g / a; b = b / a; a = 1.0f; }
-        f[1] = r + 0.0f; f[2] = g + 0.0f; f[3] = b + 0.0f; f[0] = a + 0.0f;
+        float r = L(s[1], f[1], w), g = L(s[2], f[2], w), b = L(s[3], f[3], w);
+        if (a > 1.0f) { r = x86::div(r, a); g = x86::div(g, a); b = x86::div(b, a); a = 1.0f; }
+        f[1] = x86::add(r, 0.0f); f[2] = x86::add(g, 0.0f); f[3] = x86::add(b, 0.0f); f[0] = x86::add(a, 0.0f);
     } else {
         auto L = [](float a, float b, float w) { return nr::add(nr::mul(nr::sub(b, a), w), a); };
         float a = L(s[0], f[0], w);

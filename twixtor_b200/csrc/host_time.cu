@@ -24,69 +24,131 @@ int32_t float_to_fixed(double f) {  // crates/fx-core/src/fixed.rs:8-10 (Rust `a
 }
 float fixed_reader(int32_t fixed, float scale) { return (float)((double)fixed * (1.0 / 65536.0)) * scale; }
 
-struct SpeedCurve {  // crates/fx-core/src/curves.rs:348-375, :537-544
-    const tw_time_params* p;
-    long long key_time(int i, int step) const { return (long long)std::llround(p->key_frames[i] * (double)step); }
-    double at(long long t, int step) const {
-        if (p->nkeys <= 0) return p->speed_percent;
-        int last = p->nkeys - 1;
-        if (t <= key_time(0, step)) return p->key_values[0];
-        if (t >= key_time(last, step)) return p->key_values[last];
-        int i = 0;
-        while (i + 1 < p->nkeys && key_time(i + 1, step) <= t) i++;
-        long long ta = key_time(i, step), tb = key_time(i + 1, step);
-        bool ea = p->key_ease && p->key_ease[i], eb = p->key_ease && p->key_ease[i + 1];
-        double u = (double)(t - ta) / (double)(tb - ta);
+// crates/fx-core/src/curves.rs:282-310, :348-375, :537-544: a float curve, constant when it has no
+// key, else its keys sorted by time (frame * lts rounded half away from zero, time.rs:117-119),
+// linear or eased between keys, held after a hold key (flags bit 0 ease, bit 1 hold)
+struct Curve {
+    struct Key {
+        long long t;
+        double v;
+        int flags;
+    };
+    double constant = 0.0;
+    std::vector<Key> keys;
+    Curve(double c, int n, const double* frames, const double* values, const int32_t* flags, int lts) : constant(c) {
+        for (int i = 0; i < n; i++)
+            keys.push_back({(long long)std::llround(frames[i] * (double)lts), values[i], flags ? flags[i] : 0});
+        std::stable_sort(keys.begin(), keys.end(), [](const Key& a, const Key& b) { return a.t < b.t; });
+    }
+    double at(long long t) const {
+        if (keys.empty()) return constant;
+        size_t last = keys.size() - 1;
+        if (t <= keys[0].t) return keys[0].v;
+        if (t >= keys[last].t) return keys[last].v;
+        size_t i = 0;
+        while (i + 1 < keys.size() && keys[i + 1].t <= t) i++;
+        const Key &a = keys[i], &b = keys[i + 1];
+        if (a.flags & 2) return a.v;
+        double u = (double)(t - a.t) / (double)(b.t - a.t);
+        bool ea = (a.flags & 1) != 0, eb = (b.flags & 1) != 0;
         double f = (!ea && !eb) ? u : (ea && eb) ? u * u * (3.0 - 2.0 * u) : ea ? u * u * (2.0 - u) : u * (1.0 + u * (1.0 - u));
-        return p->key_values[i] + (p->key_values[i + 1] - p->key_values[i]) * f;
+        return a.v + (b.v - a.v) * f;
     }
 };
 
-// timeline.rs:266-331 (Speed mode, Src Time Offset 0); `ratio` is in_fps / out_fps (1 for the
-// retime effect with "In FPS is Out FPS")
-float src_pos(const SpeedCurve& c, int lts, float t, bool* unsupported, double ratio = 30.0 / 30.0) {
-    float lts_f = (float)lts;
-    float out = 0.0f;
-    int n2 = cvtt_i32_f(t * 2.0f);
-    if (n2 >= (1 << 24)) { *unsupported = true; return 0.0f; }
-    float k = 1.0f;
-    while ((float)n2 >= k) {
-        int time = cvtt_i32_d((double)((lts_f * k) / 2.0f) + 0.05);
-        float sp = (float)((double)float_to_fixed(c.at(time, lts)) / 6553600.0);
-        out = (sp / 2.0f) + out;
-        k += 1.0f;
-    }
-    float tt = t * 2.0f;
-    float rem = tt - (k + -1.0f);
-    if ((double)rem > 0.0001) {
-        int time = cvtt_i32_d((double)((tt * lts_f) / 2.0f) + 0.05);
-        float sp = (float)((double)float_to_fixed(c.at(time, lts)) / 6553600.0);
-        out = ((rem * sp) / 2.0f) + out;
-    }
-    return (float)(ratio * (double)out);
+// timeline.rs:69-76: a rate within 2e-5 (an f32 difference) of 29.97, 59.94 or 23.976 becomes it
+double snap_rate(double rate) {
+    for (double t : {29.97, 59.94, 23.976})
+        if ((double)std::fabs((float)(rate - t)) < 2e-5) rate = t;
+    return rate;
 }
+
+// The time map of the retime effect (timeline.rs:106-131, :204-344) for tw_time_params.
+struct RetimeMap {
+    int lts = 100;
+    double in_fps = 30.0, out_fps = 30.0;
+    float dur = 100.0f;
+    double frame_time_k = 0.05;
+    int mode = 1;
+    Curve speed, frame_num;
+    explicit RetimeMap(const tw_time_params* p)
+        : lts(p->fps_den == 1 ? 100 : p->fps_den),  // crates/fx-core/src/time.rs:92-99
+          speed(p->speed_percent, p->nkeys, p->key_frames, p->key_values, p->key_ease, lts),
+          frame_num(p->frame_num, p->nfn_keys, p->fn_key_frames, p->fn_key_values, p->fn_key_flags, lts) {
+        double in = 30.0, out = 30.0;  // "In FPS is Out FPS" on: both 30 (timeline.rs:117-120)
+        if (p->own_input_rate) {
+            in = (double)((float)p->input_frame_rate * 1.0f);
+            out = (double)p->fps_num / (double)p->fps_den;
+        }
+        in_fps = snap_rate(in);
+        out_fps = snap_rate(out);
+        dur = (float)(((double)lts * out_fps) / in_fps);
+        if (p->frame_time_bias > 0.0) frame_time_k = p->frame_time_bias;
+        mode = p->remap_mode == 2 ? 2 : 1;
+    }
+    bool rates_ok() const { return !(0.01 > out_fps || 0.01 >= in_fps); }  // timeline.rs:125-127
+    // timeline.rs:266-331 (Src Time Offset 0)
+    float src_pos(float t, bool* unsupported) const {
+        float lts_f = (float)lts;
+        double ratio = in_fps / out_fps;
+        if (mode == 2) {  // Frame Number: the curve at trunc((lts * t) + K), times in / out
+            int time = cvtt_i32_d((double)(lts_f * t) + 0.05);
+            return (float)(ratio * (double)(float)frame_num.at(time));
+        }
+        float out = 0.0f;
+        int n2 = cvtt_i32_f(t * 2.0f);
+        if (n2 >= (1 << 24)) { *unsupported = true; return 0.0f; }
+        float k = 1.0f;
+        while ((float)n2 >= k) {
+            int time = cvtt_i32_d((double)((lts_f * k) / 2.0f) + 0.05);
+            float sp = (float)((double)float_to_fixed(speed.at(time)) / 6553600.0);
+            out = (sp / 2.0f) + out;
+            k += 1.0f;
+        }
+        float tt = t * 2.0f;
+        float rem = tt - (k + -1.0f);
+        if ((double)rem > 0.0001) {
+            int time = cvtt_i32_d((double)((tt * lts_f) / 2.0f) + 0.05);
+            float sp = (float)((double)float_to_fixed(speed.at(time)) / 6553600.0);
+            out = ((rem * sp) / 2.0f) + out;
+        }
+        return (float)(ratio * (double)out);
+    }
+    // timeline.rs:336-344 (base 0), then the clip frame of that tick
+    int32_t clip_frame(int32_t pos) const {
+        float d = (float)pos;
+        int32_t time = std::fabs(in_fps - out_fps) < frame_time_k ? cvtt_i32_d((double)d * (double)dur + 0.5)
+                                                                   : cvtt_i32_d((double)(d * dur) + (double)dur * frame_time_k);
+        long long idx = time >= 0 ? time / lts : -(((long long)-time + lts - 1) / lts);
+        return (int32_t)std::max<long long>(std::min<long long>(idx, INT32_MAX), INT32_MIN);
+    }
+};
 
 }  // namespace
 
 extern "C" int tw_select(const tw_time_params* p, int32_t n, int32_t width, int32_t height, tw_selection* out) {
     if (!p || !out || p->fps_num <= 0 || p->fps_den <= 0) return TW_ERR_BAD_PARAM;
     if (p->nkeys > 0 && (!p->key_frames || !p->key_values)) return TW_ERR_BAD_PARAM;
-    int lts = p->fps_den == 1 ? 100 : p->fps_den;  // crates/fx-core/src/time.rs:92-99
-    SpeedCurve c{p};
+    if (p->nfn_keys > 0 && (!p->fn_key_frames || !p->fn_key_values)) return TW_ERR_BAD_PARAM;
+    if (p->remap_mode < 0 || p->remap_mode > 2) return TW_ERR_BAD_PARAM;
+    RetimeMap map(p);
+    if (!map.rates_ok()) return TW_ERR_BAD_PARAM;
+    int lts = map.lts;
     int cur = n * lts;
     float t0 = (float)cur / (float)lts;                  // timeline.rs:136-142
     float t1 = ((float)lts + (float)cur) / (float)lts;
     bool bad = false;
-    float s0 = src_pos(c, lts, t0, &bad);
-    float s1 = src_pos(c, lts, t1, &bad);
+    float s0 = map.src_pos(t0, &bad);
+    float s1 = map.src_pos(t1, &bad);
     if (bad) return TW_ERR_UNSUPPORTED;
     float blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
     int a = cvtt_i32_f(s0);
     float frac = s0 - (float)a;
     out->s0 = s0;
     out->s1 = s1;
-    out->a = a;
-    out->b = (int32_t)((uint32_t)a + 1u);
+    // the clip frames of positions a and a + 1 (host.rs:155-159)
+    out->a = map.clip_frame(a);
+    out->b = map.clip_frame((int32_t)((uint32_t)a + 1u));
     out->wa = 1.0f - frac;
     bool exact = true;  // timeline.rs:429-439
     float fr = s0 - std::floor(s0);
@@ -107,18 +169,20 @@ extern "C" int tw_select_vectors_in(const tw_time_params* p, int32_t n, int32_t 
                                     tw_selection* out, tw_vecin_frame* frame) {
     if (!p || !out || !frame || p->fps_num <= 0 || p->fps_den <= 0) return TW_ERR_BAD_PARAM;
     if (p->nkeys > 0 && (!p->key_frames || !p->key_values)) return TW_ERR_BAD_PARAM;
-    int lts = p->fps_den == 1 ? 100 : p->fps_den;
-    double comp = (double)p->fps_num / (double)p->fps_den;
-    if (0.01 > comp) return TW_ERR_BAD_PARAM;  // timeline.rs:125-127 (the rate check)
-    double ratio = 30.0 / comp;
-    float dur = (float)(((double)lts * comp) / 30.0);  // timeline.rs:128
-    SpeedCurve c{p};
+    if (p->nfn_keys > 0 && (!p->fn_key_frames || !p->fn_key_values)) return TW_ERR_BAD_PARAM;
+    if (p->remap_mode < 0 || p->remap_mode > 2) return TW_ERR_BAD_PARAM;
+    tw_time_params q = *p;  // the effect's rates: the input rate (30 with In FPS is Out FPS), the composition's
+    q.own_input_rate = 1;
+    q.input_frame_rate = p->own_input_rate ? p->input_frame_rate : 30.0;
+    RetimeMap map(&q);
+    if (!map.rates_ok()) return TW_ERR_BAD_PARAM;
+    int lts = map.lts;
     int cur = n * lts;
     float t0 = (float)cur / (float)lts;
     float t1 = ((float)lts + (float)cur) / (float)lts;
     bool bad = false;
-    float s0 = src_pos(c, lts, t0, &bad, ratio);
-    float s1 = src_pos(c, lts, t1, &bad, ratio);
+    float s0 = map.src_pos(t0, &bad);
+    float s1 = map.src_pos(t1, &bad);
     if (bad) return TW_ERR_UNSUPPORTED;
     float blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
     int a = cvtt_i32_f(s0);
@@ -134,8 +198,8 @@ extern "C" int tw_select_vectors_in(const tw_time_params* p, int32_t n, int32_t 
     out->exact = exact ? 1 : 0;
     out->vectors_quality = (width >= 2 && height >= 2) ? 4 : 0;
     out->interp = p->frame_interp - 1;
-    auto clip_index = [&](int32_t pos) -> int32_t {  // the clip frame shown at T(pos) ticks
-        int32_t time = cvtt_i32_d((double)dur * (double)(float)pos + 0.5);
+    auto clip_index = [&](int32_t pos) -> int32_t {  // T(k) = trunc(dur * k + 0.5), timemap.rs:45-50
+        int32_t time = cvtt_i32_d((double)map.dur * (double)(float)pos + 0.5);
         long long idx = time >= 0 ? time / lts : -(((long long)-time + lts - 1) / lts);
         return (int32_t)std::max<long long>(std::min<long long>(idx, INT32_MAX), INT32_MIN);
     };
