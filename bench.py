@@ -21,10 +21,11 @@ the reference CPU path.
 * ``cpu_baseline``: the time of that oracle render (the reference CPU path restated in C++, OpenMP
   over all host cores): a bounded sample of the same workload.
 
-``--workload create-vectors`` and ``--workload fgbg`` measure the other two single-GPU
-configurations the same way through their host-buffer C ABI calls (tw_create_vectors_clip on a
-1920x1080 16 bpc clip under random affine motion; tw_retime_layers_clip on a 1920x1080 8 bpc clip
-with three FG matte layers at speed 40 %), with the oracle beside them on a small sample.
+``--workload create-vectors``, ``--workload fgbg`` and ``--workload vectors-in`` measure the other
+single-GPU configurations the same way through their host-buffer C ABI calls (tw_create_vectors_clip
+on a 1920x1080 16 bpc clip under random affine motion; tw_retime_layers_clip on a 1920x1080 8 bpc
+clip with three FG matte layers at speed 40 %; tw_vectors_in_clip on the retime clip with both
+vector layers, holes in them, the effect's defaults), with the oracle beside them on a small sample.
 
 ``--impl reference`` times the reference's CPU path the same way (the oracle port: the reference
 is Rust and no Rust toolchain exists on these machines). Under torchrun the output frames of ONE
@@ -223,8 +224,9 @@ def _timed(stream, fn, k, flush):
 
 
 def run_workload(args):
-    """The create-vectors (1080p 16 bpc, frame pairs n -> n - 1) and retime-fgbg (1080p 8 bpc, three
-    FG layers, speed 40 %) configurations through their host-buffer clip calls, one GPU."""
+    """The create-vectors (1080p 16 bpc, frame pairs n -> n - 1), retime-fgbg (1080p 8 bpc, three FG
+    layers, speed 40 %) and vectors-in (1080p 8 bpc, both vector layers, speed 40 %) configurations
+    through their host-buffer clip calls, one GPU."""
     import torch
     import twixtor_b200 as tw
     from twixtor_b200 import synth
@@ -248,6 +250,33 @@ def run_workload(args):
         metric = "1080p create-vectors output frames/s (strict byte-exact GPU vs CPU)"
         workload = "create-vectors 1920x1080 16bpc RGBA, pairs n -> n-1 under random affine motion, defaults (half res)"
         h2d = per * 2 * W * H * 8
+    elif args.workload == "vectors-in":
+        per, fmt, md = 5, 0, 32.0
+        nsrc = int(math.ceil(SPEED / 100.0 * (warmup + steps) * per)) + 2
+        frames = synth.moving_clip(W, H, nsrc, depth=8, **CLIP_KW)
+        vnext = synth.vector_clip(W, H, nsrc, CLIP_KW["bg_velocity"], max_displace=md)
+        vprev = synth.vector_clip(W, H, nsrc, CLIP_KW["bg_velocity"], max_displace=md, sign=-1.0, seed=0x74570007)
+        fs = W * H * 4
+        tp = tw.TimeParams(fps=(30, 1), speed_percent=SPEED)
+        settings = tw.vectors_in_settings()  # the effect's defaults: Warping Forward, Blend
+        step_args = []
+        for k in range(warmup + steps):  # per step the clip frames its output frames read
+            sv = [tw.select_vectors_in(tp, n, W, H) for n in range(k * per, (k + 1) * per)]
+            lo = min(min(v.a, v.b) for _, v in sv)
+            hi = max(max(v.a, v.b) for _, v in sv)
+            lo, hi = max(lo, 0), min(hi, nsrc - 1)
+            vfs = [tw.VecInFrame(v.a - lo, v.b - lo) for _, v in sv]
+            cut = lambda c: torch.from_numpy(np.ascontiguousarray(c[lo * fs:(hi + 1) * fs])).pin_memory().numpy()
+            step_args.append(([s for s, _ in sv], vfs, cut(frames), cut(vnext), cut(vprev), hi - lo + 1))
+        out = torch.empty(per * W * H * 4, dtype=torch.uint8).pin_memory().numpy()
+
+        def step(k):
+            sels, vfs, f, vn, vp, n = step_args[k]
+            dev.vectors_in_clip(settings, f, n, vn, n, vp, n, sels, vfs, md, W, H, fmt, out=out)
+        metric = "1080p vectors-in output frames/s (strict byte-exact GPU vs CPU)"
+        workload = ("vectors-in 1920x1080 8bpc RGBA, speed 40%, both vector layers (12 alpha-0 holes a frame), "
+                    "defaults (Warping Forward, Blend)")
+        h2d = sum(3 * a[5] * fs for a in step_args[warmup:]) // steps
     else:
         per, fmt, nfg = 5, 0, 3
         nsrc = int(math.ceil(SPEED / 100.0 * (warmup + steps) * per)) + 2
@@ -302,6 +331,10 @@ def run_workload(args):
         t = time.perf_counter()
         if args.workload == "create-vectors":
             O.create_vectors_clip(frames, 3, W, H, fmt, 2)
+            n = 2
+        elif args.workload == "vectors-in":
+            O.vectors_in_clip(frames, nsrc, vnext, nsrc, vprev, nsrc, W, H, fmt, O.vecin_params(speed=SPEED, max_displace=md),
+                              2)
             n = 2
         else:
             O.retime_fgbg_clip(frames, nsrc, mattes, [1] * nfg, [70.0] * nfg, W, H, fmt, O.retime_params(speed=SPEED), 2)
@@ -484,7 +517,8 @@ def main():
                     help="retime: the fast mode (tw_flow_settings.fast_mode); parity becomes PSNR against the strict render")
     ap.add_argument("--tune-cache", default=None,
                     help="--ncu-case: the autotuner's JSON table, read when present, written otherwise")
-    ap.add_argument("--workload", default="retime", choices=["retime", "create-vectors", "fgbg", "adjoint", "batch"],
+    ap.add_argument("--workload", default="retime", choices=["retime", "create-vectors", "fgbg", "vectors-in", "adjoint",
+                                                           "batch"],
                     help="retime (the headline, default), create-vectors (1080p 16 bpc), fgbg (1080p, 3 FG layers) or "
                          "adjoint (warp + blend gradients, 64 triples of 1280x720) or batch (4 clips of uneven size)")
     args = ap.parse_args()

@@ -261,3 +261,36 @@ def batch_clip_gpu(width, height, frames, seed, device="cuda:0"):
             r, gg, b = torch.where(m, tl, r), torch.where(m, 0.5 * tl + 0.3, gg), torch.where(m, 1.0 - tl, b)
         out[t, 0], out[t, 1], out[t, 2], out[t, 3] = gg, b, r, 1.0  # wire planes G, B, R, A
     return out.reshape(-1)
+
+
+def vector_clip(width, height, frames, velocity, depth=8, max_displace=32.0, sign=1.0, seed=0x74570006, holes=12,
+                hole_radius=40.0):
+    """A vector layer of ``frames`` wire frames the way the Vectors In effect reads them: every pixel
+    the displacement ``sign * velocity`` (plus a slow spatial ripple of a tenth of a pixel) encoded
+    against ``max_displace`` (8 bpc R = (u / md + 1) * 127, 16 bpc with 32767, float (u / md + 1) / 2;
+    G likewise; B 0), alpha opaque except ``holes`` discs of alpha 0 per frame (the holes the
+    effect's flow fill closes)."""
+    rng = np.random.RandomState(seed)
+    Y, X = np.mgrid[0:height, 0:width].astype(np.float64)
+    out = []
+    for t in range(frames):
+        u = sign * velocity[0] + 0.1 * np.sin(X / 97.0 + t)
+        v = sign * velocity[1] + 0.1 * np.cos(Y / 61.0 - t)
+        a = np.ones((height, width))
+        for _ in range(holes):
+            cx, cy = rng.uniform(0, width), rng.uniform(0, height)
+            a[(X - cx) ** 2 + (Y - cy) ** 2 < hole_radius ** 2] = 0.0
+        if depth == 8:
+            r = np.clip(np.floor((u / max_displace + 1.0) * 127.0 + 0.5), 0, 254)
+            g = np.clip(np.floor((v / max_displace + 1.0) * 127.0 + 0.5), 0, 254)
+            out.append(np.stack([r, g, np.zeros_like(r), a * 255], -1).astype(np.uint8).reshape(-1))
+        elif depth == 16:
+            r = np.clip(np.floor((u / max_displace + 1.0) * 32767.0 + 0.5), 0, 65534)
+            g = np.clip(np.floor((v / max_displace + 1.0) * 32767.0 + 0.5), 0, 65534)
+            out.append(np.stack([r, g, np.zeros_like(r), a * 65535], -1).astype(np.uint16).reshape(-1))
+        else:
+            r = ((u / max_displace + 1.0) / 2.0).astype(np.float32)
+            g = ((v / max_displace + 1.0) / 2.0).astype(np.float32)
+            out.append(np.concatenate([g.reshape(-1), np.zeros(width * height, np.float32), r.reshape(-1),
+                                       a.astype(np.float32).reshape(-1)]))
+    return np.concatenate(out)
