@@ -434,7 +434,7 @@ int tw_to_frame(tw_ctx* ctx, const void* engine, int32_t width, int32_t height, 
  * carry their raw 1-based values. A curve is constant (no key) or keyed at frame numbers, linear
  * between keys, eased at a key whose flag has bit 0, held after a key whose flag has bit 1
  * (crates/fx-core/src/curves.rs:282-310, :348-375, :537-544). Src Time Offset is 0. A zeroed tail
- * (remap_mode .. frame_time_bias) is the Speed mode with "In FPS is Out FPS" on. */
+ * (remap_mode .. frame_time_plain) is the Speed mode with "In FPS is Out FPS" on. */
 typedef struct tw_time_params {
     int32_t fps_num, fps_den;  /* the host's frame rate; integer rates get 100 ticks a frame */
     double speed_percent;
@@ -457,6 +457,8 @@ typedef struct tw_time_params {
     double frame_time_bias;    /* the bias of the frame time between unequal rates (timeline.rs:25): 0
                                   reads as 0.05, the reference's value; 0.1 the revision its parity
                                   grids record */
+    int32_t frame_time_plain;  /* retime-fgbg's frame time: trunc(dur * k + 0.5) at every rate, no bias
+                                  branch (timeline.rs:204-210) */
 } tw_time_params;
 
 /* The selection of output frame n of a clip of width x height (timeline::select, timeline.rs:

@@ -99,6 +99,7 @@ int32_t cvtt_i32_f(float x) {  // timeline.rs:52-58
 
 struct TimeMap {
     double frame_time_k = 0.05;  // FRAME_TIME_K (timeline.rs:25)
+    bool plain_frame_time = false;  // plugins 03 and 04: trunc(dur * k + 0.5) at every rate
     Curve speed;
     int remap_mode = 1;  // Time Remap Mode: 1 Speed, 2 Frame Number
     Curve frame_num;
@@ -138,7 +139,8 @@ struct TimeMap {
     }
     int frame_time(float f) const {  // timeline.rs:336-344
         float d = f - (float)base;
-        if (std::fabs(in_fps - out_fps) < frame_time_k) return cvtt_i32_d((double)d * (double)dur + 0.5);
+        if (plain_frame_time || std::fabs(in_fps - out_fps) < frame_time_k)
+            return cvtt_i32_d((double)d * (double)dur + 0.5);
         return cvtt_i32_d((double)(d * dur) + (double)dur * frame_time_k);
     }
 };
@@ -177,7 +179,8 @@ struct or_retime_params {
     int rows_reversed;         // motion path on bottom-up rows
     int taps_above_first;      // vertical border rows of the solver's filters
     int video_360;             // "360 Video": video range luma, binary alpha Smart Blend
-    int prep;                  // Image Prep popup: 1 None, 2 Contrast/Edge Enhance, 3 Delinearize
+    int prep;                  // Image Prep popup: 1 None, 2 Contrast/Edge Enhance, 3 Delinearize; 4 both stages
+                               // (retime-fgbg's Contrast/Edge, plugins/retime-fgbg/src/glue.rs:153-154)
     int track_rgb_a;           // retime-fgbg's Track RGB+A (alpha in the luma; the layered pyramids' 360 filters)
     // the rest of the time model (timeline.rs:106-131, :266-344): Time Remap Mode (0 or 1 Speed,
     // 2 Frame Number) with Frame Num constant or keyed, and "In FPS is Out FPS" off (own_input_rate:
@@ -193,6 +196,8 @@ struct or_retime_params {
     // the bias of the frame time between unequal rates (timeline.rs:25, :336-344): 0 reads as 0.05,
     // the reference's current value; 0.1 is the revision the parity grids record
     double frame_time_bias;
+    // retime-fgbg's frame time: trunc(dur * k + 0.5) at every rate (timeline.rs:204-210)
+    int frame_time_plain;
 };
 
 // timeline.rs:69-76: a rate within 2e-5 (an f32 difference) of 29.97, 59.94 or 23.976 becomes it
@@ -214,6 +219,7 @@ static int retime_map(const or_retime_params* p, TimeMap* map) {
     }
     map->lts = time_step;
     if (p->frame_time_bias > 0.0) map->frame_time_k = p->frame_time_bias;
+    map->plain_frame_time = p->frame_time_plain != 0;
     map->in_fps = snap_rate(in);
     map->out_fps = snap_rate(out);
     map->dur = (float)(((double)time_step * map->out_fps) / map->in_fps);
@@ -699,8 +705,8 @@ static int retime_one(const void* frames, int nframes, int w, int h, int fmt, co
         fs.taps_above_first = p->taps_above_first != 0;
         fs.video_range_luma = p->video_360 != 0;  // compose/vector.rs:72-82 (flow_settings)
         fs.track_alpha = p->track_rgb_a != 0;     // plugins/retime-fgbg/src/glue.rs:34-38
-        fs.prep_contrast_edge = p->prep == 2;     // frontend.rs:224-225
-        fs.prep_delinearize = p->prep == 3;
+        fs.prep_contrast_edge = p->prep == 2 || p->prep == 4;  // frontend.rs:224-225; 4: both stages, retime-fgbg's
+        fs.prep_delinearize = p->prep == 3 || p->prep == 4;    // Contrast/Edge (plugins/retime-fgbg/src/glue.rs:153-154)
         FlowField fab, fba;
         bool have_ab = false, have_ba = false;
         if (pts && !pts->empty()) {

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference tree (its path is required):
 
-    python tests/golden/make_golden.py --reference <reference tree> [--only flow_models|vectors_in|retime_time]
+    python tests/golden/make_golden.py --reference <reference tree> [--only flow_models|vectors_in|retime_time|fgbg_core]
 
 Writes, next to this script:
 
@@ -45,6 +45,12 @@ Writes, next to this script:
 * ``warp_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/warp_cases.hex``
   (the reference's bit-exact numpy model of the inverse warp; format in its ``gen_warp.py``).
 
+* ``fgbg_core_grid.npz`` - the cases of the reference's parity grid ``parity/fgbg-core`` (retime-fgbg
+  without FG matte layers: the four warping codes with the Gouraud forward warps, every Motion
+  Vectors quality, Frame Interp, prep, Main_BG sensitivity, Blur Compensation, Track RGB+A, the
+  time model; constant parameters but Speed and Frame Num, integer rates, no 360 Video, no Source
+  display, no input fields or Mark Segments), their input clips as its ``gen_grid.py`` renders
+  them, and the sha256 of the output clip ``results/base.tsv`` records.
 * ``retime_time_grid.npz`` - the cases of the reference's parity grid ``parity/retime-time`` (the
   time model with No Vectors: Speed and Frame Number modes, constant or keyed without Bezier
   handles, In FPS is Out FPS and the input rate, Frame Interp; integer composition rates, no Src
@@ -216,6 +222,45 @@ def fgbg_layers_grid(ref):
     print(f"fgbg_layers_grid.npz: {len(cases)} cases, {len(keys)} clips")
 
 
+FGC_SERVED = {"speed_percent", "warping", "frame_interp", "vectors", "prep", "main_bg_sensitivity", "blur_compensation",
+              "track_rgb_a", "video_360", "display", "time_remap_mode", "frame_num", "in_fps_is_out_fps",
+              "input_frame_rate", "plenty_memory"}
+
+
+def fgbg_core_grid(ref):
+    root = os.path.join(ref, "parity", "fgbg-core")
+    spec = importlib.util.spec_from_file_location("fgc_gen", os.path.join(root, "gen_grid.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    table = {}
+    for line in open(os.path.join(root, "results", "base.tsv")):
+        parts = line.rstrip("\n").split("\t")
+        if parts[0] != "id":
+            table[parts[0]] = (parts[1], parts[3])
+    cases, inputs = [], {}
+    for c in json.load(open(os.path.join(root, "testset", "cases.json")))["cases"]:
+        params = dict(p.split("=", 1) for p in c["params"])
+        if any(k not in FGC_SERVED for k in params):
+            continue
+        if any("@" in v for k, v in params.items() if k not in ("speed_percent", "frame_num")):
+            continue
+        if params.get("video_360", "0") != "0" or params.get("display", "1") == "2":
+            continue
+        if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
+            continue
+        key = c["input"]
+        if key not in inputs:
+            inputs[key] = np.frombuffer(gen.render_clip(c["source"], c["width"], c["height"], c["depth"], c["frames"]),
+                                        np.uint8)
+        cases.append(dict(id=c["id"], params=c["params"], depth=c["depth"], width=c["width"], height=c["height"],
+                          frames=c["frames"], fps=c["fps"], input=key, sha256=table[c["id"]][1]))
+    keys = sorted(inputs)
+    arrays = {f"input_{i}": inputs[k] for i, k in enumerate(keys)}
+    arrays["meta"] = np.frombuffer(json.dumps(dict(inputs=keys, cases=cases)).encode(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "fgbg_core_grid.npz"), **arrays)
+    print(f"fgbg_core_grid.npz: {len(cases)} cases, {len(keys)} clips")
+
+
 RT_SERVED = {"vectors", "speed_percent", "frame_interp", "time_remap_mode", "frame_num", "in_fps_is_out_fps",
              "input_frame_rate"}
 
@@ -340,7 +385,7 @@ def flow_models(ref):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="the reference tree (baairon/twixtor)")
-    ap.add_argument("--only", choices=["flow_models", "vectors_in", "retime_time"], default=None,
+    ap.add_argument("--only", choices=["flow_models", "vectors_in", "retime_time", "fgbg_core"], default=None,
                     help="write one fixture (set) only")
     args = ap.parse_args()
     ref = args.reference
@@ -354,6 +399,10 @@ def main():
     if args.only == "retime_time":
         retime_time_grid(ref)
         return
+    if args.only == "fgbg_core":
+        fgbg_core_grid(ref)
+        return
+    fgbg_core_grid(ref)
     retime_time_grid(ref)
     vectors_in_grid(ref)
     vectors_cases(ref)

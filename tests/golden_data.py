@@ -478,3 +478,28 @@ def rt_case_params(case):
                 frame_interp=int(p.get("frame_interp", 2)), remap_mode=int(p.get("time_remap_mode", 1)),
                 frame_num=fnum, fn_keys=fn_keys, own_input_rate=p.get("in_fps_is_out_fps", "1") == "0",
                 input_frame_rate=float(p.get("input_frame_rate", float(np.float32(29.97)))))
+
+
+def fgc_grid():
+    """The served cases of the fgbg-core parity grid: (meta cases, {clip name: raw bytes})."""
+    z = np.load(os.path.join(GOLDEN, "fgbg_core_grid.npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    inputs = {name: z[f"input_{i}"] for i, name in enumerate(meta["inputs"])}
+    return meta["cases"], inputs
+
+
+def fgc_case_params(case):
+    """Keyword arguments of oracle_lib.retime_params for a fgbg-core grid case (retime-fgbg's
+    defaults elsewhere: Warping 1 Inverse, which is warping code Warping - 1, glue.rs:94-100). Its
+    Image Prep 2 runs both prep stages and 3 none (plugins/retime-fgbg/src/glue.rs:153-154): the
+    oracle's prep code 4 and 1."""
+    p = dict(x.split("=", 1) for x in case["params"])
+    keys, speed = parse_keys(p.get("speed_percent", "100"))
+    fn_keys, fnum = parse_keys(p.get("frame_num", "0"))
+    return dict(fps=(int(case["fps"]), 1), speed=speed, keys=keys, vectors=int(p.get("vectors", 5)),
+                frame_interp=int(p.get("frame_interp", 2)), smart_blend=int(p.get("warping", 1)) - 1,
+                sensitivity=float(p.get("main_bg_sensitivity", 70)), blur=float(p.get("blur_compensation", 0)),
+                prep={1: 1, 2: 4, 3: 1}[int(p.get("prep", 1))], track_rgb_a=p.get("track_rgb_a", "0") == "1",
+                remap_mode=int(p.get("time_remap_mode", 1)), frame_num=fnum, fn_keys=fn_keys,
+                own_input_rate=p.get("in_fps_is_out_fps", "1") == "0",
+                input_frame_rate=float(p.get("input_frame_rate", float(np.float32(29.97)))), frame_time_plain=True)

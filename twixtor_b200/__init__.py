@@ -143,7 +143,7 @@ class _TimeParams(ctypes.Structure):
                 ("nfn_keys", ctypes.c_int32), ("fn_key_frames", ctypes.POINTER(ctypes.c_double)),
                 ("fn_key_values", ctypes.POINTER(ctypes.c_double)), ("fn_key_flags", ctypes.POINTER(ctypes.c_int32)),
                 ("own_input_rate", ctypes.c_int32), ("input_frame_rate", ctypes.c_double),
-                ("frame_time_bias", ctypes.c_double)]
+                ("frame_time_bias", ctypes.c_double), ("frame_time_plain", ctypes.c_int32)]
 
 
 class _VecInFrame(ctypes.Structure):
@@ -269,7 +269,8 @@ class TimeParams:
     1-based values; ``keys`` / ``fn_keys`` are lists of (frame, value, flags) of a keyed Speed % /
     Frame Num (flags: True or 1 ease, 2 hold); ``remap_mode`` 2 is Frame Number; ``own_input_rate``
     turns "In FPS is Out FPS" off (the input rate ``input_frame_rate``); ``frame_time_bias`` 0.1 is
-    the revision the reference's parity grids record (0 reads as its current 0.05)."""
+    the revision the reference's parity grids record (0 reads as its current 0.05);
+    ``frame_time_plain`` is retime-fgbg's frame time (no bias branch)."""
     fps: Tuple[int, int] = (24, 1)
     speed_percent: float = 100.0
     keys: Optional[Sequence[Tuple[float, float, int]]] = None
@@ -282,6 +283,7 @@ class TimeParams:
     own_input_rate: bool = False
     input_frame_rate: float = float(np.float32(29.97))
     frame_time_bias: float = 0.0
+    frame_time_plain: bool = False
 
     def _c(self):
         p = _TimeParams()
@@ -292,6 +294,7 @@ class TimeParams:
         p.remap_mode, p.frame_num = self.remap_mode, self.frame_num
         p.own_input_rate, p.input_frame_rate = int(self.own_input_rate), self.input_frame_rate
         p.frame_time_bias = self.frame_time_bias
+        p.frame_time_plain = int(self.frame_time_plain)
         keep = []
         for keys, n_attr, f_attr, v_attr, e_attr in ((self.keys, "nkeys", "key_frames", "key_values", "key_ease"),
                                                      (self.fn_keys, "nfn_keys", "fn_key_frames", "fn_key_values",

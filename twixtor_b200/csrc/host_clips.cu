@@ -301,9 +301,11 @@ static int clip_host(tw_ctx* ctx, const void* frames, int nframes, int nout, int
     size_t bytes = (size_t)W * H * 4 * sample_bytes(fmt);
     const int nl = std::min(MAX_LANES, std::max(1, ctx->nlanes));
     const int NS = tw_ctx::CACHE_SLOTS;
-    if (!ctx->up) {
-        CHECK(ctx->cuda(cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking), "copy stream"));
-        CHECK(ctx->cuda(cudaStreamCreateWithFlags(&ctx->down, cudaStreamNonBlocking), "copy stream"));
+    // the copy streams and the cache events are made on first use; the layered clip call may have
+    // made the upload stream already, so each is checked on its own
+    if (!ctx->up) CHECK(ctx->cuda(cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking), "copy stream"));
+    if (!ctx->down) CHECK(ctx->cuda(cudaStreamCreateWithFlags(&ctx->down, cudaStreamNonBlocking), "copy stream"));
+    if (!ctx->cache_ready[0]) {
         for (int i = 0; i < NS; i++) {
             CHECK(ctx->cuda(cudaEventCreateWithFlags(&ctx->cache_ready[i], cudaEventDisableTiming), "event"));
             for (int j = 0; j < MAX_LANES; j++)

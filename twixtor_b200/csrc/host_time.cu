@@ -69,6 +69,7 @@ struct RetimeMap {
     double in_fps = 30.0, out_fps = 30.0;
     float dur = 100.0f;
     double frame_time_k = 0.05;
+    bool plain_frame_time = false;  // retime-fgbg's frame time: trunc(dur * k + 0.5) at every rate
     int mode = 1;
     Curve speed, frame_num;
     explicit RetimeMap(const tw_time_params* p)
@@ -84,6 +85,7 @@ struct RetimeMap {
         out_fps = snap_rate(out);
         dur = (float)(((double)lts * out_fps) / in_fps);
         if (p->frame_time_bias > 0.0) frame_time_k = p->frame_time_bias;
+        plain_frame_time = p->frame_time_plain != 0;
         mode = p->remap_mode == 2 ? 2 : 1;
     }
     bool rates_ok() const { return !(0.01 > out_fps || 0.01 >= in_fps); }  // timeline.rs:125-127
@@ -117,7 +119,8 @@ struct RetimeMap {
     // timeline.rs:336-344 (base 0), then the clip frame of that tick
     int32_t clip_frame(int32_t pos) const {
         float d = (float)pos;
-        int32_t time = std::fabs(in_fps - out_fps) < frame_time_k ? cvtt_i32_d((double)d * (double)dur + 0.5)
+        int32_t time = plain_frame_time || std::fabs(in_fps - out_fps) < frame_time_k
+                           ? cvtt_i32_d((double)d * (double)dur + 0.5)
                                                                    : cvtt_i32_d((double)(d * dur) + (double)dur * frame_time_k);
         long long idx = time >= 0 ? time / lts : -(((long long)-time + lts - 1) / lts);
         return (int32_t)std::max<long long>(std::min<long long>(idx, INT32_MAX), INT32_MIN);
