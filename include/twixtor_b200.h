@@ -137,6 +137,11 @@ typedef struct tw_vectors_settings {
     tw_flow_settings flow;
     float max_displace;
     int32_t rows_reversed;
+    int32_t display;           /* Display popup: 2 Motion Vectors (0 reads as 2), 3 Debug (glue.rs:81-118) */
+    int32_t debug_view;        /* the Debug view's engine code (glue.rs:120-130): 0 Blend, 1 Diff, 2 Detail
+                                  Compare, 3 Edge Compare, 4 Warp */
+    int32_t debug_textured;    /* the Debug forward warp textured (the revision the parity grid records);
+                                  0 the Gouraud variant of the reference (glue.rs:39-42, :557-561) */
 } tw_vectors_settings;
 
 /* ---- context ------------------------------------------------------------------------------ */
@@ -398,6 +403,18 @@ int tw_encode_vectors(tw_ctx* ctx, tw_image_mut* out, const tw_flow* flow, float
  * caller hands the images in the engine's row order). A side of 1 gives the zero vector image. */
 int tw_create_vectors(tw_ctx* ctx, const tw_vectors_settings* s, const tw_image* x, const tw_image* y,
                       tw_image_mut* out);
+
+/* debug::debug_view_on (debug.rs:104-171): the view `code` (0 Blend, 1 Diff, 2 Detail Compare, 4 Warp,
+ * any other Edge Compare) of engine images x and y by the flow X(p) ~ Y(p + flow(p)) (any size of at
+ * least 2x2): the forward warp of x at amount 1 (the Gouraud variant with gouraud != 0, else the
+ * textured one), W' = (y OVER a cleared image) with the warp OVER it (matte::over_pl), then the view;
+ * frames with a side of 1 give the zero vector image. */
+int tw_debug_view(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_flow* flow, int32_t code,
+                  int32_t gouraud, tw_image_mut* out);
+
+/* create_vectors::frame_pair (create_vectors.rs:71-89) and the clip frames of the pair: as
+ * tw_vectors_pair, with debug != 0 the Debug display's roles (Previous: a = n + 1, Next: a = n - 1). */
+int tw_vectors_frame_pair(int32_t n, int32_t time_step, int32_t track_frame, int32_t debug, int32_t* a, int32_t* b);
 
 /* The clip frames of output frame n of Create Vectors (create_vectors.rs:59-97, glue.rs:488-524):
  * a = n, b = n - 1 (track_frame 1, Previous) or n + 1 (2, Next); a frame outside the clip is

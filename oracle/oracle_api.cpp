@@ -1026,6 +1026,10 @@ struct or_cv_params {
     int rows_reversed;      // the plugin turns the frames upside down for the engine (glue.rs:28-37)
     int taps_above_first;   // the solver's vertical border tap order
     int prep;               // Image Prep popup: 1 None, 2 Contrast/Edge Enhance, 3 Delinearize
+    int display;            // Display popup: 2 Motion Vectors (0 reads as 2), 3 Debug
+    int debug_view_method;  // Debug View Method: 1 Warp, 2 Blend, 3 Diff, 4 Detail Compare, 5 Edge Compare
+    int debug_textured;     // the Debug warp textured (the revision the parity grid records); 0 the
+                            // Gouraud variant of the reference's current code (glue.rs:39-42)
 };
 
 // vectors.rs:57-130 on a flow field; dst_fmt 0/1/2
@@ -1052,8 +1056,14 @@ int or_create_vectors_one(const void* frames, int nframes, int w, int h, int fmt
     uint32_t frame = (uint32_t)cvtt64f((float)ct / (float)ts + 0.5f);
     float nf = (float)(int32_t)frame;
     float fa = nf, fb = nf;
-    if (p->track_frame == 1) fb = nf - 1.0f;
-    else if (p->track_frame == 2) fb = nf + 1.0f;
+    bool debug = p->display == 3;
+    if (!debug) {
+        if (p->track_frame == 1) fb = nf - 1.0f;
+        else if (p->track_frame == 2) fb = nf + 1.0f;
+    } else {  // create_vectors.rs:71-89: the Debug display swaps the roles
+        if (p->track_frame == 1) fa = nf + 1.0f;
+        else if (p->track_frame == 2) fa = nf - 1.0f;
+    }
     int a = cvtt32(fa), b = cvtt32(fb);
     auto frame_time = [&](int k) {
         float tsf = (float)ts, x = (float)k;
@@ -1086,7 +1096,37 @@ int or_create_vectors_one(const void* frames, int nframes, int w, int h, int fmt
     Image enc;
     std::string e;
     int rc;
-    if (pts && npts > 0) {
+    if (debug) {
+        // plugins/create-vectors/src/glue.rs:557-566: the flow X -> Y of the job (with the points'
+        // user displacement), the view with the Gouraud forward warp (create_vectors.rs:408-416)
+        FlowSettings fs;
+        fs.quality = cs.quality;
+        fs.hiq = cs.hiq;
+        fs.sensitivity = cs.sensitivity;
+        fs.track_alpha = cs.track_rgb_a;
+        fs.taps_above_first = cs.taps_above_first;
+        fs.prep_contrast_edge = cs.prep_contrast_edge;
+        fs.prep_delinearize = cs.prep_delinearize;
+        FlowField flow;
+        if (pts && npts > 0) {
+            std::vector<std::array<float, 4>> pairs;
+            float last_row = (float)h - 1.0f;
+            for (int i = 0; i < npts; i++) {
+                float ay = pts[4 * i + 1], by = pts[4 * i + 3];
+                if (p->rows_reversed) { ay = last_row - ay; by = last_row - by; }
+                pairs.push_back({pts[4 * i], ay, pts[4 * i + 2], by});
+            }
+            Pyramid px, py;
+            if (!build_pyramid(x, fs, &px, &e) || !build_pyramid(y, fs, &py, &e)) return fail(1, e);
+            std::vector<UserLevel> u = user_displacement(pairs, px.geo, w, h);
+            flow = solve_pyramids_masked(px, py, fs, nullptr, nullptr, false, &u);
+        } else if (!solve(x, y, fs, &flow, &e)) {
+            return fail(1, e);
+        }
+        int m = p->debug_view_method;
+        int code = m == 1 ? 4 : m == 2 ? 0 : m == 3 ? 1 : m == 4 ? 2 : 3;  // glue.rs:120-130
+        rc = debug_view(x, y, flow, code, p->debug_textured == 0, &enc, &e);
+    } else if (pts && npts > 0) {
         // create_vectors.rs:321-351 (layer_flows_on, one layer): the solve X -> Y with the user
         // displacement of the points (plugins/create-vectors/src/glue.rs:550-553: on the rows of the
         // frames, y -> (H - 1) - y when they are turned)
@@ -1369,6 +1409,73 @@ int or_vectors_in_one(const void* frames, int nframes, const void* vec_next, int
         if (p->rows_reversed) result = rows_reversed(result);
     }
     to_frame(result, out);
+    return 0;
+}
+
+}  // extern "C"
+
+// ---- the Debug views of Create Vectors (debug.rs), for the tests --------------------------------
+
+namespace orc {
+Image debug_views_of(const Image& wp, const Image& y, int code);
+std::vector<float> debug_luma_plane(const Image& img);
+std::vector<float> debug_detail(const std::vector<float>& l, int w, int h);
+std::vector<float> debug_edge(const std::vector<float>& l, int w, int h);
+void debug_overlay(Image& out, const std::vector<float>& r, const std::vector<float>& g);
+}
+
+extern "C" {
+
+static Image wrap_image(const void* eng, int w, int h, int fmt) {
+    Image im(w, h, (Fmt)fmt);
+    std::memcpy(im.data(), eng, im.bytes());
+    return im;
+}
+
+// debug.rs:285-378 and :399-434: the luma plane, the detail and edge measures, the overlay
+void or_debug_luma(const void* eng, int w, int h, int fmt, float* out) {
+    std::vector<float> l = debug_luma_plane(wrap_image(eng, w, h, fmt));
+    std::memcpy(out, l.data(), l.size() * sizeof(float));
+}
+void or_debug_detail(const float* plane, int w, int h, float* out) {
+    std::vector<float> d = debug_detail(std::vector<float>(plane, plane + (size_t)w * h), w, h);
+    std::memcpy(out, d.data(), d.size() * sizeof(float));
+}
+void or_debug_edge(const float* plane, int w, int h, float* out) {
+    std::vector<float> d = debug_edge(std::vector<float>(plane, plane + (size_t)w * h), w, h);
+    std::memcpy(out, d.data(), d.size() * sizeof(float));
+}
+void or_debug_overlay(const float* r, const float* g, int w, int h, int fmt, void* out) {
+    Image o(w, h, (Fmt)fmt);
+    size_t n = (size_t)w * h;
+    debug_overlay(o, std::vector<float>(r, r + n), std::vector<float>(g, g + n));
+    std::memcpy(out, o.data(), o.bytes());
+}
+
+// debug.rs:155-171: view code 0..3 of W' against Y
+void or_debug_views_of(const void* wp, const void* y, int w, int h, int fmt, int code, void* out) {
+    Image o = debug_views_of(wrap_image(wp, w, h, fmt), wrap_image(y, w, h, fmt), code);
+    std::memcpy(out, o.data(), o.bytes());
+}
+
+// debug.rs:139-143 (compose_over): y OVER a transparent image, then w OVER that
+void or_debug_compose_over(const void* wimg, const void* y, int w, int h, int fmt, void* out) {
+    Image o(w, h, (Fmt)fmt);
+    over_pl(o, wrap_image(y, w, h, fmt));
+    over_pl(o, wrap_image(wimg, w, h, fmt));
+    std::memcpy(out, o.data(), o.bytes());
+}
+
+// debug.rs:104-152: the whole view (code 4 Warp), the forward warp Gouraud or textured
+int or_debug_view(const void* x, const void* y, int w, int h, int fmt, const float* flow, int fw, int fh, int code,
+                  int gouraud, void* out) {
+    FlowField f(fw, fh);
+    std::memcpy(f.d.data(), flow, f.d.size() * sizeof(float));
+    Image o;
+    std::string e;
+    int rc = debug_view(wrap_image(x, w, h, fmt), wrap_image(y, w, h, fmt), f, code, gouraud != 0, &o, &e);
+    if (rc) return fail(rc, e);
+    std::memcpy(out, o.data(), o.bytes());
     return 0;
 }
 

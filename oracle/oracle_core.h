@@ -62,6 +62,32 @@ inline float add(float a, float b) { return fix(a + b, a, b); }
 inline float sub(float a, float b) { return fix(a - b, a, b); }
 inline float mul(float a, float b) { return fix(a * b, a, b); }
 inline float div(float a, float b) { return fix(a / b, a, b); }
+// nanrule.rs:119-161: the double precision add with the rule's NaN choice
+inline double add64(double a, double b) {
+    double r = a + b;
+    if (!std::isnan(r)) return r;
+    uint64_t ba, bb;
+    std::memcpy(&ba, &a, 8);
+    std::memcpy(&bb, &b, 8);
+    const uint64_t Q = 0x0008000000000000ull;
+    uint64_t o;
+    if (std::isnan(a) && std::isnan(b)) {
+        bool sa = (ba & Q) == 0, sb = (bb & Q) == 0;
+        uint64_t fa = ba & 0x000fffffffffffffull, fb = bb & 0x000fffffffffffffull;
+        bool a_larger = fa > fb || (fa == fb && (ba >> 63) < (bb >> 63));
+        bool take_b = sa == sb ? !a_larger : sa;
+        o = (take_b ? bb : ba) | Q;
+    } else if (std::isnan(a)) {
+        o = ba | Q;
+    } else if (std::isnan(b)) {
+        o = bb | Q;
+    } else {
+        o = 0xfff8000000000000ull;
+    }
+    double d;
+    std::memcpy(&d, &o, 8);
+    return d;
+}
 }  // namespace nr
 
 // ---------------------------------------------------------------------------------------------

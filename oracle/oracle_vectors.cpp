@@ -219,3 +219,211 @@ void matte_step(Image& img, const std::vector<float>& m) {
 }
 
 }  // namespace orc
+
+// ---- the Debug views of Create Vectors (debug.rs) ---------------------------------------------
+
+#include "oracle_layers.h"
+
+namespace orc {
+
+namespace {
+
+inline int64_t sat64(double v) {  // Rust's saturating `f64 as i64`
+    if (std::isnan(v)) return 0;
+    if (v >= 9223372036854775807.0) return INT64_MAX;
+    if (v <= -9223372036854775808.0) return INT64_MIN;
+    return (int64_t)v;
+}
+
+const float VIEW_AMOUNT = 0.6f;  // debug.rs:70-78
+float diff_gain() {
+    float amount = (float)(1.0 - (double)VIEW_AMOUNT);
+    return (float)(1.0 / (double)std::fabs(amount));
+}
+float overlay_gain() {  // debug.rs:83-90
+    float amount = 0.001 > (double)VIEW_AMOUNT ? 0.001f : VIEW_AMOUNT;
+    float half = (float)((double)amount * 0.5);
+    float rest = (float)(1.0 - (double)half);
+    return (float)(1.0 / (double)rest);
+}
+
+float diff_luma(double r, double g, double b) { return (float)(((r * 0.29) + (g * 0.59)) + (b * 0.12)); }
+
+// debug.rs:285-310: the luma of the Detail and Edge views
+std::vector<float> debug_luma(const Image& img) {
+    size_t n = (size_t)img.w * img.h;
+    std::vector<float> out(n);
+    for (size_t i = 0; i < n; i++) {
+        if (img.fmt == F32) {
+            const float* p = &img.f32[i * 4];
+            double tr = (double)p[1] * 0.29, tg = (double)p[2] * 0.59, tb = (double)p[3] * 0.12;
+            float v = (float)((tr + tg) + tb);
+            if (std::isnan(v)) v = (float)nr::add64(nr::add64(tr, tg), tb);
+            out[i] = v;
+        } else {
+            double s = img.fmt == U8 ? 255.0 : 65535.0;
+            double r = img.fmt == U8 ? img.u8[i * 4 + 1] : img.u16[i * 4 + 1];
+            double g = img.fmt == U8 ? img.u8[i * 4 + 2] : img.u16[i * 4 + 2];
+            double b = img.fmt == U8 ? img.u8[i * 4 + 3] : img.u16[i * 4 + 3];
+            float v = (float)((((r * 0.29) / s + (g * 0.59) / s)) + (b * 0.12) / s);
+            out[i] = v >= 1.0f ? 1.0f : v;
+        }
+    }
+    return out;
+}
+
+// debug.rs:318-346: the luma on the border, sqrt(S / 8) inside
+std::vector<float> detail(const std::vector<float>& l, int w, int h) {
+    std::vector<float> out((size_t)w * h);
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            float c = l[(size_t)y * w + x];
+            if (x == 0 || y == 0 || x + 1 == w || y + 1 == h) { out[(size_t)y * w + x] = c; continue; }
+            bool first = true;
+            float s = 0.0f;
+            for (int yy = y - 1; yy <= y + 1; yy++)
+                for (int xx = x - 1; xx <= x + 1; xx++) {
+                    if (yy == y && xx == x) continue;
+                    float d = std::fabs(c - l[(size_t)yy * w + xx]);
+                    s = first ? d : s + d;
+                    first = false;
+                }
+            out[(size_t)y * w + x] = std::sqrt(s * 0.125f);
+        }
+    return out;
+}
+
+// debug.rs:355-378: the Sobel magnitude, border repeated, times 2 capped at 255
+std::vector<float> edge(const std::vector<float>& l, int w, int h) {
+    std::vector<float> out((size_t)w * h);
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            auto n = [&](int dx, int dy) {
+                int yy = std::min(std::max(y + dy, 0), h - 1), xx = std::min(std::max(x + dx, 0), w - 1);
+                return l[(size_t)yy * w + xx];
+            };
+            float gx = ((((-n(-1, -1) + n(1, -1)) - 2.0f * n(-1, 0)) + 2.0f * n(1, 0)) - n(-1, 1)) + n(1, 1);
+            float gy = ((((2.0f * n(0, -1) + n(-1, -1)) + n(1, -1)) - n(-1, 1)) - 2.0f * n(0, 1)) - n(1, 1);
+            float e = (float)((double)std::sqrt(gy * gy + gx * gx) * 0.17677669529664);
+            float sc = 2.0f * e;
+            out[(size_t)y * w + x] = sc > 255.0f ? 255.0f : sc;
+        }
+    return out;
+}
+
+float overlay_value(float m, float gain) {  // debug.rs:382-391
+    float v = gain * m;
+    if (v > 1.0f) return 1.0f;
+    if (v < 0.0f) return 0.0f;
+    return v;
+}
+
+// debug.rs:399-434: red the measure r, green and blue the measure g, alpha white
+void overlay(Image& out, const std::vector<float>& r, const std::vector<float>& g) {
+    float gain = overlay_gain();
+    size_t n = (size_t)out.w * out.h;
+    for (size_t i = 0; i < n; i++) {
+        float vr = overlay_value(r[i], gain), vg = overlay_value(g[i], gain);
+        if (out.fmt == U8) {
+            uint8_t* p = &out.u8[i * 4];
+            p[0] = 255;
+            p[1] = (uint8_t)sat64((double)vr * 255.0 + 0.5);
+            p[2] = (uint8_t)sat64((double)vg * 255.0 + 0.5);
+            p[3] = p[2];
+        } else if (out.fmt == U16) {
+            uint16_t* p = &out.u16[i * 4];
+            p[0] = 65535;
+            p[1] = (uint16_t)sat64((double)vr * 65535.0 + 0.5);
+            p[2] = (uint16_t)sat64((double)vg * 65535.0 + 0.5);
+            p[3] = p[2];
+        } else {
+            float* p = &out.f32[i * 4];
+            p[0] = 1.0f;
+            p[1] = vr;
+            p[2] = vg;
+            p[3] = vg;
+        }
+    }
+}
+
+// debug.rs:437-476: the grey Diff, alpha white
+void diff(Image& out, const Image& a, const Image& b) {
+    float gain = diff_gain();
+    size_t n = (size_t)out.w * out.h;
+    for (size_t i = 0; i < n; i++) {
+        auto luma = [&](const Image& im) {
+            if (im.fmt == U8) return diff_luma(im.u8[i * 4 + 1], im.u8[i * 4 + 2], im.u8[i * 4 + 3]);
+            if (im.fmt == U16) return diff_luma(im.u16[i * 4 + 1], im.u16[i * 4 + 2], im.u16[i * 4 + 3]);
+            return diff_luma(im.f32[i * 4 + 1], im.f32[i * 4 + 2], im.f32[i * 4 + 3]);
+        };
+        float v = std::fabs(luma(a) - luma(b)) * gain;
+        if (out.fmt == F32) {
+            float o = v >= 1.0f ? 1.0f : v;
+            float* p = &out.f32[i * 4];
+            p[0] = 1.0f;
+            p[1] = p[2] = p[3] = o;
+        } else {
+            float top = out.fmt == U8 ? 255.0f : 65535.0f;
+            float c = v >= top ? top : v;
+            int64_t q = sat64((double)c + 0.5);
+            if (out.fmt == U8) {
+                uint8_t* p = &out.u8[i * 4];
+                p[0] = 255;
+                p[1] = p[2] = p[3] = (uint8_t)q;
+            } else {
+                uint16_t* p = &out.u16[i * 4];
+                p[0] = 65535;
+                p[1] = p[2] = p[3] = (uint16_t)q;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+// the primitives of the views, for the tests
+std::vector<float> debug_luma_plane(const Image& img) { return debug_luma(img); }
+std::vector<float> debug_detail(const std::vector<float>& l, int w, int h) { return detail(l, w, h); }
+std::vector<float> debug_edge(const std::vector<float>& l, int w, int h) { return edge(l, w, h); }
+void debug_overlay(Image& out, const std::vector<float>& r, const std::vector<float>& g) { overlay(out, r, g); }
+
+// debug.rs:155-171 (views_of)
+Image debug_views_of(const Image& wp, const Image& y, int code) {
+    Image out(wp.w, wp.h, wp.fmt);
+    if (code == 0) {
+        copy_image(out, wp);
+        lerp(out, y, 0.5f);
+    } else if (code == 1) {
+        diff(out, wp, y);
+    } else if (code == 2) {
+        overlay(out, detail(debug_luma(wp), wp.w, wp.h), detail(debug_luma(y), y.w, y.h));
+    } else {
+        overlay(out, edge(debug_luma(wp), wp.w, wp.h), edge(debug_luma(y), y.w, y.h));
+    }
+    return out;
+}
+
+// debug.rs:104-152 (debug_view_on): the forward warp of x by the flow at amount 1 (the Gouraud
+// variant with gouraud, else the textured one), then W' = (y OVER transparent) with W OVER it, then
+// the view; sides of 1: the zero vector image
+int debug_view(const Image& x, const Image& y, const FlowField& flow, int code, bool gouraud, Image* out,
+               std::string* err) {
+    if (!(x.w >= 2 && x.h >= 2)) {
+        *out = zero_vectors_image(x.w, x.h, x.fmt);
+        return 0;
+    }
+    Image warped(x.w, x.h, x.fmt);
+    int rc = forward_warp(warped, x, flow, 1.0f, !gouraud, nullptr, err);
+    if (rc) return rc;
+    if (code == 4) {
+        *out = warped;
+        return 0;
+    }
+    Image wp(y.w, y.h, y.fmt);
+    over_pl(wp, y);
+    over_pl(wp, warped);
+    *out = debug_views_of(wp, y, code);
+    return 0;
+}
+
+}  // namespace orc

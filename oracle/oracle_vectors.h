@@ -37,4 +37,11 @@ int invert_flow(const FlowField& flow, bool pyramid, bool above_first, FlowField
 // plugins/vectors-in/src/vectorin.rs:125-155: the vector image's alpha capped by a layer matte
 void matte_step(Image& img, const std::vector<float>& m);
 
+// ---- the Debug views of Create Vectors (debug.rs) ----
+// debug.rs:155-171: view code 0 Blend, 1 Diff, 2 Detail Compare, else Edge Compare, of W' against y
+Image debug_views_of(const Image& wp, const Image& y, int code);
+// debug.rs:104-152: code 4 is the Warp view
+int debug_view(const Image& x, const Image& y, const FlowField& flow, int code, bool gouraud, Image* out,
+               std::string* err);
+
 }  // namespace orc

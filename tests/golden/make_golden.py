@@ -2,7 +2,7 @@
 
 Run in a container that has the reference tree (its path is required):
 
-    python tests/golden/make_golden.py --reference <reference tree> [--only flow_models|vectors_in|retime_time|fgbg_core]
+    python tests/golden/make_golden.py --reference <reference tree> [--only flow_models|vectors_in|retime_time|fgbg_core|debug]
 
 Writes, next to this script:
 
@@ -15,7 +15,8 @@ Writes, next to this script:
   border taps below first; the tests run the oracle and the CUDA path in that variant
   (``rows_reversed=False, taps_above_first=False``) for these cases.
 * ``create_vectors_grid.npz`` - the cases of the reference's parity grid ``parity/create-vectors``
-  that the single layer Create Vectors pass serves (Display Motion Vectors, no FG matte or Alt
+  that the single layer Create Vectors pass serves (Display Motion Vectors or Debug without the
+  geometry overlay, no FG matte or Alt
   Motion Src layer, no tracking points, no prep, no keyed parameter, integer frame rates), their
   raw input clips as ``parity/create-vectors/gen_grid.py`` renders them, and the sha256 of the
   output clip that ``parity/create-vectors/results/base_outputs.tsv`` records. That table was
@@ -64,6 +65,12 @@ Writes, next to this script:
 * ``vectors_cases.bin.gz`` - the binary blob of ``plugins/retime-engine/tests/fixtures/
   vectors_cases.hex`` (the reference's numpy model of the vector encode and decode; format in its
   ``gen_vectors.py``).
+* ``debug_tables.json`` - the tables of the reference's Debug view tests
+  (``plugins/retime-engine/src/debug/tests.rs``): Diff, luma, Detail, Edge, overlay and Blend values
+  read from the images of the original plugin's view generator, and traced rows of its special
+  value clip (Y, W, W' and the Blend); ``debug_cases.bin.gz`` the blob of ``tests/fixtures/
+  debug_cases.hex`` (the reference's numpy model of the views; its Warp view is the reference's
+  rule, the other views predate the rules read from the original).
 * ``flow_models.bin.gz`` - the six differential fixtures ``plugins/retime-engine/tests/fixtures/
   flow_{a..f}.hex`` (the reference's float32 numpy model of the solver without block matching,
   ``flow_ref.py``; not bit exact: the reference's own test accepts 1e-4, 1e-3 with prep), each
@@ -107,7 +114,7 @@ def served(case):
 
 
 CV_SERVED = {"max_displace", "main_bg_sensitivity", "track_frame", "vector_resolution", "track_rgb_a", "display",
-             "layers_output", "main_bg_track", "prep"}
+             "layers_output", "main_bg_track", "prep", "debug_view_method"}
 
 
 def cv_served(case):
@@ -123,7 +130,9 @@ def cv_served(case):
         return False
     if any("@" in v for k, v in params.items() if k not in pt):
         return False
-    if params.get("display", "2") != "2" or params.get("main_bg_track", "1") != "1":
+    if params.get("display", "2") not in ("2", "3") or params.get("main_bg_track", "1") != "1":
+        return False
+    if params.get("display", "2") == "3" and "draw_geom" in params:  # the Debug display's geometry overlay
         return False
     if params.get("layers_output", "1") not in ("1", "5"):
         return False
@@ -353,6 +362,31 @@ def vectors_in_grid(ref):
     print(f"vectors_in_grid.npz: {len(cases)} cases, {len(keys)} clips")
 
 
+DEBUG_TABLES = ["DIFF8", "DIFF16", "DIFF32", "LUMA8", "LUMA16", "LUMA32", "DETAIL", "EDGE", "OVERLAY8", "OVERLAY16",
+                "OVERLAY32", "BLEND8", "BLEND16", "BLEND32", "SPEC_Y", "SPEC_W", "SPEC_WP", "SPEC_BLEND", "SPEC_WP_LUMA"]
+
+
+def debug_tables(ref):
+    """The tables of the reference's Debug view tests (plugins/retime-engine/src/debug/tests.rs):
+    pixel values read from the images of the original plugin's view generator and traced rows of
+    its special value clip, as JSON (the Rust literals parsed as data)."""
+    import ast
+    src = open(os.path.join(ref, "plugins", "retime-engine", "src", "debug", "tests.rs")).read()
+    out = {}
+    for name in DEBUG_TABLES:
+        m = re.search(r"const %s: [^=]+= (\[.*?\]);\n" % name, src, re.S)
+        body = "\n".join(line.split("//")[0] for line in m.group(1).splitlines())
+        body = re.sub(r"\[(\w+); (\d+)\]", lambda mm: "[" + ", ".join([mm.group(1)] * int(mm.group(2))) + "]", body)
+        out[name] = ast.literal_eval(body.replace("(", "[").replace(")", "]"))
+    with open(os.path.join(HERE, "debug_tables.json"), "w") as f:
+        json.dump(out, f)
+    txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "debug_cases.hex")).read()
+    blob = bytes.fromhex("".join(txt.split()))
+    with gzip.open(os.path.join(HERE, "debug_cases.bin.gz"), "wb") as f:
+        f.write(blob)
+    print(f"debug_tables.json: {len(out)} tables; debug_cases.bin.gz: {len(blob)} bytes")
+
+
 def vectors_cases(ref):
     txt = open(os.path.join(ref, "plugins", "retime-engine", "tests", "fixtures", "vectors_cases.hex")).read()
     blob = bytes.fromhex("".join(txt.split()))
@@ -385,7 +419,7 @@ def flow_models(ref):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="the reference tree (baairon/twixtor)")
-    ap.add_argument("--only", choices=["flow_models", "vectors_in", "retime_time", "fgbg_core"], default=None,
+    ap.add_argument("--only", choices=["flow_models", "vectors_in", "retime_time", "fgbg_core", "debug"], default=None,
                     help="write one fixture (set) only")
     args = ap.parse_args()
     ref = args.reference
@@ -402,7 +436,11 @@ def main():
     if args.only == "fgbg_core":
         fgbg_core_grid(ref)
         return
+    if args.only == "debug":
+        debug_tables(ref)
+        return
     fgbg_core_grid(ref)
+    debug_tables(ref)
     retime_time_grid(ref)
     vectors_in_grid(ref)
     vectors_cases(ref)

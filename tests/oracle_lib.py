@@ -154,6 +154,13 @@ def lib():
         L.or_invert_flow.argtypes = [P, i, i, i, i, P]
         L.or_matte_step.argtypes = [P, i, i, i, P]
         L.or_vectors_in_one.argtypes = [P, i, P, i, P, i, i, i, i, ctypes.POINTER(VecInParams), i, P]
+        L.or_debug_luma.argtypes = [P, i, i, i, P]
+        L.or_debug_detail.argtypes = [P, i, i, P]
+        L.or_debug_edge.argtypes = [P, i, i, P]
+        L.or_debug_overlay.argtypes = [P, P, i, i, i, P]
+        L.or_debug_views_of.argtypes = [P, P, i, i, i, i, P]
+        L.or_debug_compose_over.argtypes = [P, P, i, i, i, P]
+        L.or_debug_view.argtypes = [P, P, i, i, i, P, i, i, i, i, P]
         L.or_vecin_select.argtypes = [ctypes.POINTER(VecInParams), i, i, i, P, P]
         _lib = L
     return _lib
@@ -353,16 +360,20 @@ class CvParams(ctypes.Structure):
     _fields_ = [("fps_num", ctypes.c_int), ("fps_den", ctypes.c_int), ("quality_high", ctypes.c_int),
                 ("vector_resolution", ctypes.c_int), ("max_displace", ctypes.c_double), ("track_frame", ctypes.c_int),
                 ("sensitivity", ctypes.c_double), ("track_rgb_a", ctypes.c_int), ("rows_reversed", ctypes.c_int),
-                ("taps_above_first", ctypes.c_int), ("prep", ctypes.c_int)]
+                ("taps_above_first", ctypes.c_int), ("prep", ctypes.c_int), ("display", ctypes.c_int),
+                ("debug_view_method", ctypes.c_int), ("debug_textured", ctypes.c_int)]
 
 
 def create_vectors_clip(frames, nframes, w, h, fmt, nout, fps=(24, 1), vector_resolution=1, max_displace=2048.0,
                         track_frame=1, sensitivity=70.0, track_rgb_a=False, rows_reversed=True, taps_above_first=True,
-                        prep=1, points=None):
+                        prep=1, points=None, display=2, debug_view_method=1, debug_textured=False):
     """Output frames 0..nout-1 of the Create Vectors effect (plugin 02, one layer) over a raw clip;
-    ``points[n]`` the tracking points of output frame n (x, y at X, x, y at Y; host rows)."""
+    ``points[n]`` the tracking points of output frame n (x, y at X, x, y at Y; host rows); display 3
+    is the Debug display of ``debug_view_method`` (its forward warp the Gouraud variant, or textured
+    with ``debug_textured``: the revision the parity grid records)."""
     p = CvParams(fps[0], fps[1], 1, vector_resolution, max_displace, track_frame, sensitivity, int(track_rgb_a),
-                 int(rows_reversed), int(taps_above_first), int(prep))
+                 int(rows_reversed), int(taps_above_first), int(prep), int(display), int(debug_view_method),
+                 int(debug_textured))
     out = np.zeros(nout * w * h * 4, DTYPE[fmt])
     pts = npts = None
     if points is not None:
@@ -696,3 +707,53 @@ def vecin_select(params, n, w, h):
     lib().or_vecin_select(ctypes.byref(params), n, w, h, ptr(f3), ptr(i6))
     return dict(s0=f3[0], s1=f3[1], wa=f3[2], a=int(i6[0]), exact=bool(i6[1]), vq=int(i6[2]), interp=int(i6[3]),
                 clip_a=int(i6[4]), clip_b=int(i6[5]))
+
+
+# ---- the Debug views of Create Vectors -------------------------------------------------------------
+
+
+def debug_luma(img, w, h, fmt):
+    out = np.zeros(w * h, np.float32)
+    lib().or_debug_luma(ptr(np.ascontiguousarray(img)), w, h, fmt, ptr(out))
+    return out
+
+
+def debug_detail(plane, w, h):
+    out = np.zeros(w * h, np.float32)
+    lib().or_debug_detail(ptr(np.ascontiguousarray(plane, np.float32)), w, h, ptr(out))
+    return out
+
+
+def debug_edge(plane, w, h):
+    out = np.zeros(w * h, np.float32)
+    lib().or_debug_edge(ptr(np.ascontiguousarray(plane, np.float32)), w, h, ptr(out))
+    return out
+
+
+def debug_overlay(r, g, w, h, fmt):
+    out = np.zeros(w * h * 4, DTYPE[fmt])
+    lib().or_debug_overlay(ptr(np.ascontiguousarray(r, np.float32)), ptr(np.ascontiguousarray(g, np.float32)), w, h,
+                           fmt, ptr(out))
+    return out
+
+
+def debug_views_of(wp, y, w, h, fmt, code):
+    out = np.zeros(w * h * 4, DTYPE[fmt])
+    lib().or_debug_views_of(ptr(np.ascontiguousarray(wp)), ptr(np.ascontiguousarray(y)), w, h, fmt, code, ptr(out))
+    return out
+
+
+def debug_compose_over(wimg, y, w, h, fmt):
+    out = np.zeros(w * h * 4, DTYPE[fmt])
+    lib().or_debug_compose_over(ptr(np.ascontiguousarray(wimg)), ptr(np.ascontiguousarray(y)), w, h, fmt, ptr(out))
+    return out
+
+
+def debug_view(x, y, w, h, fmt, flow, fw, fh, code, gouraud=True):
+    """debug::debug_view_on: view code 0 Blend, 1 Diff, 2 Detail, 3 Edge, 4 Warp."""
+    out = np.zeros(w * h * 4, DTYPE[fmt])
+    rc = lib().or_debug_view(ptr(np.ascontiguousarray(x)), ptr(np.ascontiguousarray(y)), w, h, fmt,
+                             ptr(np.ascontiguousarray(flow, np.float32)), fw, fh, code, int(gouraud), ptr(out))
+    if rc:
+        raise ValueError(err())
+    return out

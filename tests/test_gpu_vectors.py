@@ -28,16 +28,18 @@ def same(a, b):
 CV_CASES, CV_INPUTS = golden_data.cv_grid()
 
 
-@pytest.mark.parametrize("case", CV_CASES, ids=[c["id"] for c in CV_CASES])
+@pytest.mark.parametrize("case", golden_data.cv_grid_params(CV_CASES))
 def test_create_vectors_grid_sha256(dev, case):
-    """The reference's recorded output clips of the served create-vectors grid cases."""
+    """The reference's recorded output clips of the served create-vectors grid cases (the Debug
+    display with the textured warp of the recorded revision)."""
     fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
     raw = CV_INPUTS[case["input"]].view(tw.DTYPES[fmt])
     kw = golden_data.cv_case_params(case)
     s = tw.vectors_settings(vector_resolution=kw["vector_resolution"], max_displace=kw["max_displace"],
                             sensitivity=kw["sensitivity"], track_rgb_a=kw["track_rgb_a"], rows_reversed=False,
-                            taps_above_first=False, prep=kw["prep"])
-    pairs = [tw.vectors_pair(n, kw["track_frame"], kw["fps"]) for n in range(case["frames"])]
+                            taps_above_first=False, prep=kw["prep"], display=kw["display"],
+                            debug_view_method=kw["debug_view_method"], debug_textured=True)
+    pairs = [tw.vectors_pair(n, kw["track_frame"], kw["fps"], debug=kw["display"] == 3) for n in range(case["frames"])]
     points = [golden_data.cv_points(case, n) for n in range(case["frames"])]
     out = dev.create_vectors_clip(s, raw, case["frames"], pairs, case["width"], case["height"], fmt, points=points)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
@@ -121,3 +123,57 @@ def test_tiny_frames_are_zero_vectors(dev):
     out = dev.create_vectors_clip(tw.vectors_settings(), frames, 3, [(1, 0), (2, 1)], 1, 7, 0)
     want = O.create_vectors_clip(frames, 3, 1, 7, 0, 3)[7 * 4:]
     assert same(out, want)
+
+
+# ---- the Debug views (debug.rs) -----------------------------------------------------------------------
+
+
+def _debug_pair(w, h, fmt, seed, specials=False):
+    rng = np.random.default_rng(seed)
+    depth = {0: 8, 1: 16, 2: 32}[fmt]
+    frames = synth.moving_clip(w, h, 2, depth=depth, seed=seed, square=max(4, min(w, h) // 3))
+    x, y = O.from_frame(frames[:w * h * 4], w, h, fmt), O.from_frame(frames[w * h * 4:], w, h, fmt)
+    if specials and fmt == 2:
+        bits = np.array([0x7FC00000, 0xFFC00000, 0x7F800000, 0xFF800000, 0x00000001, 0x7F7FFFFF, 0x80000000,
+                         0x7FA00001], np.uint32).view(np.float32)
+        for img in (x, y):
+            idx = rng.integers(0, img.size, img.size // 20)
+            img[idx] = bits[rng.integers(0, bits.size, idx.size)]
+    fw, fh = max(2, w // 2), max(2, h // 2)
+    flow = (rng.standard_normal(fw * fh * 2) * 3.0).astype(np.float32)
+    return x, y, flow, fw, fh
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("code", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("gouraud", [True, False])
+def test_debug_view_matches_oracle(dev, fmt, code, gouraud):
+    w, h = 97, 61
+    x, y, flow, fw, fh = _debug_pair(w, h, fmt, seed=fmt * 10 + code)
+    got = dev.debug_view(x, y, w, h, fmt, flow, (fw, fh), code, gouraud=gouraud)
+    want = O.debug_view(x, y, w, h, fmt, flow, fw, fh, code, gouraud=gouraud)
+    assert same(got, want)
+
+
+@pytest.mark.parametrize("code", [0, 1, 2, 3])
+def test_debug_view_special_floats(dev, code):
+    """Float frames with NaNs of both signs, infinities, denormals and FLT_MAX: the x86 NaN bits of
+    the views (the forward warp's, the OVERs', the luma's rule and the measures')."""
+    w, h = 40, 30
+    x, y, flow, fw, fh = _debug_pair(w, h, 2, seed=77 + code, specials=True)
+    got = dev.debug_view(x, y, w, h, 2, flow, (fw, fh), code)
+    want = O.debug_view(x, y, w, h, 2, flow, fw, fh, code)
+    assert same(got, want)
+
+
+@pytest.mark.parametrize("method", [1, 2, 3, 4, 5])
+def test_debug_display_clip_matches_oracle(dev, method):
+    """The Debug display over a clip (the reference's current orders: bottom-up rows, the taps above
+    first, the Gouraud warp), track Previous, 8 bpc at 160x96."""
+    w, h, n = 160, 96, 5
+    frames = synth.moving_clip(w, h, n, depth=8, seed=0x7457000A)
+    s = tw.vectors_settings(max_displace=24.0, display=3, debug_view_method=method)
+    pairs = [tw.vectors_pair(k, 1, debug=True) for k in range(n)]
+    got = dev.create_vectors_clip(s, frames, n, pairs, w, h, 0)
+    want = O.create_vectors_clip(frames, n, w, h, 0, n, max_displace=24.0, display=3, debug_view_method=method)
+    assert same(got, want)

@@ -196,16 +196,17 @@ def test_smart_blend_and_hole_fill_model_fixtures(i):
 CV_CASES, CV_INPUTS = golden_data.cv_grid()
 
 
-@pytest.mark.parametrize("case", CV_CASES, ids=[c["id"] for c in CV_CASES])
+@pytest.mark.parametrize("case", golden_data.cv_grid_params(CV_CASES))
 def test_create_vectors_grid_sha256(case):
     """The reference's recorded output clips of the served create-vectors grid cases (solve + encode,
-    frame pairs, blank neighbours outside the clip, tiny frames)."""
+    frame pairs, blank neighbours outside the clip, tiny frames, the Debug display with the textured
+    warp of the recorded revision)."""
     fmt = golden_data.FMT_OF_DEPTH[case["depth"]]
     raw = CV_INPUTS[case["input"]].view(O.DTYPE[fmt])
     kw = golden_data.cv_case_params(case)
     points = [golden_data.cv_points(case, n) for n in range(case["frames"])]
     out = O.create_vectors_clip(raw, case["frames"], case["width"], case["height"], fmt, case["frames"],
-                                rows_reversed=False, taps_above_first=False, points=points, **kw)
+                                rows_reversed=False, taps_above_first=False, points=points, debug_textured=True, **kw)
     assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256"]
 
 

@@ -131,7 +131,8 @@ def _layer_job(nfg, sensitivity, matte_chan=None, shrink=None, display=1, points
 
 
 class _VectorsSettings(ctypes.Structure):
-    _fields_ = [("flow", _FlowSettings), ("max_displace", ctypes.c_float), ("rows_reversed", ctypes.c_int32)]
+    _fields_ = [("flow", _FlowSettings), ("max_displace", ctypes.c_float), ("rows_reversed", ctypes.c_int32),
+                ("display", ctypes.c_int32), ("debug_view", ctypes.c_int32), ("debug_textured", ctypes.c_int32)]
 
 
 class _TimeParams(ctypes.Structure):
@@ -229,13 +230,19 @@ class RetimeSettings:
 class VectorsSettings:
     """The Create Vectors pass of one layer (create_vectors.rs:97-135): the solver settings (quality 4
     Normal (half res) / 5 Full res, ``track_alpha`` for Track RGB+A), Max Displace in output pixels,
-    and whether the engine sees the frames upside down (plugin 02's glue)."""
+    and whether the engine sees the frames upside down (plugin 02's glue); ``display`` 3 is the Debug
+    display of the engine view code ``debug_view`` (0 Blend, 1 Diff, 2 Detail, 3 Edge, 4 Warp),
+    its forward warp the Gouraud variant (textured with ``debug_textured``)."""
     flow: FlowSettings = field(default_factory=FlowSettings)
     max_displace: float = 2048.0
     rows_reversed: bool = True
+    display: int = 2
+    debug_view: int = 4
+    debug_textured: bool = False
 
     def _c(self):
-        return _VectorsSettings(self.flow._c(), np.float32(self.max_displace), int(self.rows_reversed))
+        return _VectorsSettings(self.flow._c(), np.float32(self.max_displace), int(self.rows_reversed), self.display,
+                                self.debug_view, int(self.debug_textured))
 
 
 def fixed_param(v) -> np.float32:
@@ -251,16 +258,23 @@ def percent_param(v) -> np.float32:
     return np.float32(fixed_param(v) / np.float32(100.0))
 
 
+DEBUG_VIEW_CODE = {1: 4, 2: 0, 3: 1, 4: 2, 5: 3}  # Debug View Method -> engine view code (glue.rs:120-130)
+
+
 def vectors_settings(vector_resolution=1, max_displace=2048.0, sensitivity=70.0, track_rgb_a=False, hiq=True,
-                     rows_reversed=True, taps_above_first=True, prep=1) -> VectorsSettings:
+                     rows_reversed=True, taps_above_first=True, prep=1, display=2, debug_view_method=1,
+                     debug_textured=False) -> VectorsSettings:
     """The settings of plugin 02 (create-vectors) from its parameter values (glue.rs:133-146): the
     popup Vector Resolution, the 16.16 readers of Max Displace and Sensitivity (percent), the Image
-    Prep popup (2 Contrast/Edge Enhance, 3 Delinearize)."""
+    Prep popup (2 Contrast/Edge Enhance, 3 Delinearize), the Display popup (3 Debug) and the Debug
+    View Method popup."""
     reader = fixed_param
     sens = percent_param(sensitivity)
     fs = FlowSettings(quality=5 if vector_resolution == 2 else 4, hiq=hiq, sensitivity=sens, track_alpha=track_rgb_a,
                       taps_above_first=taps_above_first, prep_contrast_edge=prep == 2, prep_delinearize=prep == 3)
-    return VectorsSettings(flow=fs, max_displace=float(np.float32(1.0) * reader(max_displace)), rows_reversed=rows_reversed)
+    return VectorsSettings(flow=fs, max_displace=float(np.float32(1.0) * reader(max_displace)), rows_reversed=rows_reversed,
+                           display=display, debug_view=DEBUG_VIEW_CODE.get(debug_view_method, 3),
+                           debug_textured=debug_textured)
 
 
 @dataclass
@@ -373,6 +387,8 @@ def library():
     L.tw_encode_vectors.argtypes = [P, pimg, pflow, ctypes.c_float]
     L.tw_create_vectors.argtypes = [P, ctypes.POINTER(_VectorsSettings), pimg, pimg, pimg]
     L.tw_vectors_pair.argtypes = [i32, i32, i32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+    L.tw_vectors_frame_pair.argtypes = [i32, i32, i32, i32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+    L.tw_debug_view.argtypes = [P, pimg, pimg, pflow, i32, i32, pimg]
     L.tw_create_vectors_clip.argtypes = [P, ctypes.POINTER(_VectorsSettings), P, i32, P, i32, P, P, i32, i32, i32, P]
     L.tw_check_logf.argtypes = [P, P, P, ctypes.c_int64]
     L.tw_check_powf.argtypes = [P, P, P, P, ctypes.c_int64]
@@ -419,11 +435,12 @@ def _img(a, w, h, fmt):
     return _Image(w, h, fmt, a.ctypes.data, a.nbytes), a
 
 
-def vectors_pair(n: int, track_frame: int = 1, fps: Tuple[int, int] = (24, 1)) -> Tuple[int, int]:
-    """The clip frames (X, Y) of output frame ``n`` of Create Vectors (create_vectors.rs:59-97)."""
+def vectors_pair(n: int, track_frame: int = 1, fps: Tuple[int, int] = (24, 1), debug: bool = False) -> Tuple[int, int]:
+    """The clip frames (X, Y) of output frame ``n`` of Create Vectors (create_vectors.rs:59-97); with
+    ``debug`` the Debug display's pair."""
     ts = 100 if fps[1] == 1 else fps[1]
     a, b = ctypes.c_int32(), ctypes.c_int32()
-    rc = library().tw_vectors_pair(n, ts, track_frame, ctypes.byref(a), ctypes.byref(b))
+    rc = library().tw_vectors_frame_pair(n, ts, track_frame, int(debug), ctypes.byref(a), ctypes.byref(b))
     if rc:
         raise BadParam(rc, "bad argument")
     return a.value, b.value
@@ -937,6 +954,19 @@ class Device:
                                                       next_ptr or None, n_next, prev_ptr or None, n_prev, sa, va,
                                                       len(sels), np.float32(max_displace), width, height, fmt,
                                                       out_ptr))
+
+    def debug_view(self, x, y, width, height, fmt, flow, flow_size, code, gouraud=True):
+        """``debug::debug_view_on``: view code 0 Blend, 1 Diff, 2 Detail, 3 Edge, 4 Warp of engine
+        images x and y by the interleaved flow of ``flow_size``."""
+        xi, x = _img(x, width, height, fmt)
+        yi, y = _img(y, width, height, fmt)
+        flow = np.ascontiguousarray(flow, np.float32)
+        fi = _Flow(flow_size[0], flow_size[1], flow.ctypes.data)
+        out = np.zeros(width * height * 4, DTYPES[fmt])
+        oi = _Image(width, height, fmt, out.ctypes.data, out.nbytes)
+        self._check(self._L.tw_debug_view(self._h, ctypes.byref(xi), ctypes.byref(yi), ctypes.byref(fi), code,
+                                          int(gouraud), ctypes.byref(oi)))
+        return out
 
     def from_frame(self, wire, width, height, fmt):
         wire = np.ascontiguousarray(wire)

@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtwixtor_b200.so")
-SOURCES = ["solver.cu", "fused.cu", "coarse.cu", "image.cu", "smart.cu", "forward.cu", "layers.cu", "filters.cu", "prep.cu", "adjoint.cu", "host_context.cu", "host_solve.cu", "host_compose.cu", "host_layers.cu", "host_clips.cu", "host_time.cu", "host_tune.cu", "host_vecin.cu", "vecin.cu", "noalloc.cu"]
+SOURCES = ["solver.cu", "fused.cu", "coarse.cu", "image.cu", "smart.cu", "forward.cu", "layers.cu", "filters.cu", "prep.cu", "adjoint.cu", "host_context.cu", "host_solve.cu", "host_compose.cu", "host_layers.cu", "host_clips.cu", "host_time.cu", "host_tune.cu", "host_vecin.cu", "vecin.cu", "debug.cu", "noalloc.cu"]
 FAST_SOURCES = ["fused.cu", "solver.cu", "coarse.cu"]  # built a second time for the fast mode
 BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -243,11 +243,16 @@ static int vectors_lane(tw_ctx* ctx, Lane& L, const tw_vectors_settings& s, int 
         }
         CHECK(solve_pyramids_dev(ctx, px_, py_, px_ + pf, py_ + pf, g, fs, L.work[0], L.flow[0].as<float>(), flags + FL_ANY0,
                                  flags + FL_NAN, nullptr, nullptr, u, u ? u + pf : nullptr, u ? u + 2 * pf : nullptr));
+        if (s.display == 3) {  // glue.rs:557-566: the Debug view of the pair's flow
+            CHECK(debug_view_dev(ctx, L.eng[0].p, L.eng[1].p, L.flow[0].as<float>(), g.w, g.h, W, H, fmt, s.debug_view,
+                                 s.debug_textured == 0, eng_out, L.wb_wt[0], L.wb_wt[1], L.wb_tmp[0]));
+        } else {
         // vectors.rs:78-83, host scalars in single precision
         float dw1 = (float)(W - 1), dh1 = (float)(H - 1), fw1 = (float)(g.w - 1), fh1 = (float)(g.h - 1);
         float sx = fw1 / dw1, sy = fh1 / dh1;
         float kx = (dw1 / fw1) / s.max_displace, ky = (dh1 / fh1) / s.max_displace;
         LAUNCH(ctx, k_encode_vectors, grid2(W, H), TB, 0, L.flow[0].as<float>(), g.w, g.h, eng_out, W, H, fmt, sx, sy, kx, ky, 0);
+        }
     }
     if (to_wire) {
         long n = (long)W * H;
@@ -455,16 +460,25 @@ int tw_create_vectors(tw_ctx* ctx, const tw_vectors_settings* s, const tw_image*
 }
 
 int tw_vectors_pair(int32_t n, int32_t time_step, int32_t track_frame, int32_t* a, int32_t* b) {
+    return tw_vectors_frame_pair(n, time_step, track_frame, 0, a, b);
+}
+
+int tw_vectors_frame_pair(int32_t n, int32_t time_step, int32_t track_frame, int32_t debug, int32_t* a, int32_t* b) {
     if (!a || !b || time_step <= 0) return TW_ERR_BAD_PARAM;
     int64_t ct = (int64_t)n * time_step;
     if (ct > INT32_MAX || ct < INT32_MIN) return TW_ERR_BAD_PARAM;
     // create_vectors.rs:59-62: the frame number of the current time
     float q = (float)(int32_t)ct / (float)time_step + 0.5f;
     uint32_t frame = (uint32_t)(int64_t)q;
-    // :71-89: the pair (Display Motion Vectors)
+    // :71-89: the pair (the Debug display swaps the roles)
     float nf = (float)(int32_t)frame, fa = nf, fb = nf;
-    if (track_frame == 1) fb = nf - 1.0f;
-    else if (track_frame == 2) fb = nf + 1.0f;
+    if (!debug) {
+        if (track_frame == 1) fb = nf - 1.0f;
+        else if (track_frame == 2) fb = nf + 1.0f;
+    } else {
+        if (track_frame == 1) fa = nf + 1.0f;
+        else if (track_frame == 2) fa = nf - 1.0f;
+    }
     auto cvtt = [](float v) { return (v > -2147483904.0f && v < 2147483648.0f) ? (int32_t)v : INT32_MIN; };
     // :92-97 and the clip frame of that tick (a layer time divided by the frame length, rounded down)
     auto clip_index = [&](int32_t k) {
@@ -494,7 +508,10 @@ int tw_create_vectors_clip(tw_ctx* ctx, const tw_vectors_settings* s, const void
     }
     size_t bytes = (size_t)width * height * 4 * sample_bytes(fmt);
     bool flip = s->rows_reversed != 0 && width >= 2 && height >= 2;
-    return clip_host(
+    // the Debug views' forward warp reads its hit total back and uses the context's buffers: one lane
+    int saved_lanes = ctx->nlanes;
+    if (s->display == 3) ctx->nlanes = 1;
+    int rc = clip_host(
         ctx, frames, nframes, nout, width, height, fmt, out,
         [&](int k, int* a, int* b) {
             *a = pairs[2 * k];
@@ -515,6 +532,8 @@ int tw_create_vectors_clip(tw_ctx* ctx, const tw_vectors_settings* s, const void
             return vectors_lane(ctx, L, *s, width, height, fmt, ow, true, flip, with_points ? points + pt_first[k] : nullptr,
                                 with_points ? npoints[k] : 0);
         });
+    ctx->nlanes = saved_lanes;
+    return rc;
 }
 
 int tw_retime_clip_device(tw_ctx* ctx, const tw_retime_settings* s, const void* frames, int32_t nframes,

@@ -394,3 +394,76 @@ int tw_vectors_in_clip(tw_ctx* ctx, const tw_retime_settings* s, const void* fra
 }
 
 }  // extern "C"
+
+// ---- the Debug views of Create Vectors (debug.rs:104-171) ------------------------------------------
+
+namespace tw {
+
+// The view `code` (0 Blend, 1 Diff, 2 Detail Compare, 4 Warp, any other Edge Compare) of engine images
+// x and y by the flow (fw x fh, interleaved) into the engine image `out`, on ctx->cur: the forward warp
+// of x at amount 1 (Gouraud, or textured when !gouraud), then W' = (y OVER cleared) with W OVER it,
+// then the view. Sides of 1: the zero vector image. The forward warp synchronises ctx->cur and uses
+// the context's forward warp buffers.
+int debug_view_dev(tw_ctx* ctx, const void* x, const void* y, const float* flow, int fw, int fh, int W, int H, int fmt,
+                   int code, bool gouraud, void* out, DevBuf& warped, DevBuf& wp, DevBuf& luma) {
+    long n = (long)W * H;
+    size_t bytes = (size_t)n * 4 * sample_bytes(fmt);
+    if (W < 2 || H < 2) {
+        LAUNCH(ctx, k_encode_vectors, grid2(W, H), TB, 0, (const float*)nullptr, 0, 0, out, W, H, fmt, 0.0f, 0.0f, 0.0f,
+               0.0f, 1);
+        return TW_OK;
+    }
+    if (code == 4) return forward_warp_dev(ctx, x, flow, fw, fh, W, H, fmt, 1.0f, !gouraud, out, nullptr);
+    CHECK(ctx->ensure(warped, bytes, "debug warp"));
+    CHECK(ctx->ensure(wp, bytes, "debug composite"));
+    CHECK(forward_warp_dev(ctx, x, flow, fw, fh, W, H, fmt, 1.0f, !gouraud, warped.p, nullptr));
+    CHECK(ctx->cuda(cudaMemsetAsync(wp.p, 0, bytes, ctx->cur), "clear"));
+    double pb = 3.0 * (double)bytes;
+    LAUNCHB(ctx, pb, k_over_pl, grid1(n), TB, 0, wp.p, y, fmt, n);
+    LAUNCHB(ctx, pb, k_over_pl, grid1(n), TB, 0, wp.p, (const void*)warped.p, fmt, n);
+    if (code == 0) {
+        LAUNCHB(ctx, pb, k_debug_blend, grid1(n), TB, 0, (const void*)wp.p, y, fmt, out, n);
+    } else if (code == 1) {
+        LAUNCHB(ctx, pb, k_debug_diff, grid1(n), TB, 0, (const void*)wp.p, y, fmt, out, n);
+    } else {
+        CHECK(ctx->ensure(luma, 2 * (size_t)n * sizeof(float), "debug luma"));
+        float* lw = luma.as<float>();
+        float* ly = lw + n;
+        double lb = (double)bytes + 4.0 * n;
+        LAUNCHB(ctx, lb, k_debug_luma, grid1(n), TB, 0, (const void*)wp.p, fmt, lw, n);
+        LAUNCHB(ctx, lb, k_debug_luma, grid1(n), TB, 0, y, fmt, ly, n);
+        LAUNCHB(ctx, 8.0 * n + (double)bytes, k_debug_overlay, grid2(W, H), TB, 0, (const float*)lw, (const float*)ly, W, H,
+                fmt, code == 2 ? 0 : 1, out);
+    }
+    return TW_OK;
+}
+
+}  // namespace tw
+
+extern "C" int tw_debug_view(tw_ctx* ctx, const tw_image* x, const tw_image* y, const tw_flow* flow, int32_t code,
+                             int32_t gouraud, tw_image_mut* out) {
+    if (!ctx) return TW_ERR_BAD_PARAM;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->cur = ctx->stream;
+    CHECK(check_image(ctx, x, "debug view"));
+    CHECK(check_image(ctx, y, "debug view"));
+    if (!flow || !flow->data || !out || !out->data) return ctx->fail(TW_ERR_BAD_PARAM, "missing argument");
+    CHECK(check_out(ctx, out, "debug view output"));
+    if (!same_shape(x, y) || out->width != x->width || out->height != x->height || out->fmt != x->fmt)
+        return ctx->fail(TW_ERR_MISMATCH, "debug view: incompatible frames");
+    int W = x->width, H = x->height;
+    if ((W >= 2 && H >= 2) && (flow->width < 2 || flow->height < 2))
+        return ctx->fail(TW_ERR_MISMATCH, "debug view: the forward warp needs a flow of at least 2x2");
+    size_t bytes = (size_t)W * H * 4 * sample_bytes(x->fmt);
+    size_t fb = (size_t)std::max(flow->width * flow->height, 1) * 2 * sizeof(float);
+    CHECK(upload_image(ctx, ctx->vi_wire[0], x));
+    CHECK(upload_image(ctx, ctx->vi_wire[1], y));
+    CHECK(ctx->ensure(ctx->vi_wire[2], fb, "flow"));
+    CHECK(ctx->ensure(ctx->vi_wire[3], bytes, "debug output"));
+    CHECK(ctx->cuda(cudaMemcpyAsync(ctx->vi_wire[2].p, flow->data, (size_t)flow->width * flow->height * 2 * sizeof(float),
+                                    cudaMemcpyHostToDevice, ctx->stream), "flow upload"));
+    CHECK(debug_view_dev(ctx, ctx->vi_wire[0].p, ctx->vi_wire[1].p, ctx->vi_wire[2].as<float>(), flow->width, flow->height,
+                         W, H, x->fmt, code, gouraud != 0, ctx->vi_wire[3].p, ctx->eng[0], ctx->eng[1], ctx->plane[0]));
+    CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->vi_wire[3].p, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download"));
+    return ctx->cuda(cudaStreamSynchronize(ctx->stream), "kernel execution");
+}

@@ -398,4 +398,17 @@ __global__ void k_invert_take(const float4* __restrict__ pushed, const uint8_t* 
 // the units of the depth
 __global__ void k_matte_step(void* __restrict__ img, int fmt, const float* __restrict__ matte, long n);
 
+// ---- the Debug views of Create Vectors (debug.cu, debug.rs) ----
+// debug.rs:155-171 Blend: W' lerped towards Y by 0.5 (copy then lerp)
+__global__ void k_debug_blend(const void* __restrict__ wp, const void* __restrict__ y, int fmt, void* __restrict__ out,
+                              long n);
+// debug.rs:437-476: the grey Diff of W' and Y
+__global__ void k_debug_diff(const void* __restrict__ wp, const void* __restrict__ y, int fmt, void* __restrict__ out,
+                             long n);
+// debug.rs:285-310: the luma plane of the Detail and Edge views
+__global__ void k_debug_luma(const void* __restrict__ img, int fmt, float* __restrict__ out, long n);
+// debug.rs:318-434: the Detail (edge == 0) or Edge measure of both luma planes and the overlay
+__global__ void k_debug_overlay(const float* __restrict__ lw, const float* __restrict__ ly, int w, int h, int fmt,
+                                int edge, void* __restrict__ out);
+
 }  // namespace tw

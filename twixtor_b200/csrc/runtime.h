@@ -354,6 +354,8 @@ int vec_flow_dev(tw_ctx* ctx, const void* vec, int W, int H, int fmt, float md, 
                  float* flow, uint8_t* holes, int* any, DevBuf& fillbuf);
 int invert_flow_dev(tw_ctx* ctx, const float* flow, int W, int H, bool pyramid, bool above_first, float* out,
                     float* t, float* pushed, uint8_t* holes, int* any, DevBuf& fillbuf);
+int debug_view_dev(tw_ctx* ctx, const void* x, const void* y, const float* flow, int fw, int fh, int W, int H, int fmt,
+                   int code, bool gouraud, void* out, DevBuf& warped, DevBuf& wp, DevBuf& luma);
 
 }  // namespace tw
 

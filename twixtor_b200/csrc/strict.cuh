@@ -68,6 +68,28 @@ __device__ __forceinline__ float add(float a, float b) { return fix(a + b, a, b)
 __device__ __forceinline__ float sub(float a, float b) { return fix(a - b, a, b); }
 __device__ __forceinline__ float mul(float a, float b) { return fix(a * b, a, b); }
 __device__ __forceinline__ float div(float a, float b) { return fix(a / b, a, b); }
+// nanrule.rs:119-161: the double precision add with the rule's NaN choice
+__device__ __forceinline__ double add64(double a, double b) {
+    double r = __dadd_rn(a, b);
+    if (!isnan(r)) return r;
+    unsigned long long ba = (unsigned long long)__double_as_longlong(a), bb = (unsigned long long)__double_as_longlong(b);
+    const unsigned long long Q = 0x0008000000000000ull;
+    unsigned long long o;
+    if (isnan(a) && isnan(b)) {
+        bool sa = (ba & Q) == 0, sb = (bb & Q) == 0;
+        unsigned long long fa = ba & 0x000fffffffffffffull, fb = bb & 0x000fffffffffffffull;
+        bool a_larger = fa > fb || (fa == fb && (ba >> 63) < (bb >> 63));
+        bool take_b = sa == sb ? !a_larger : sa;
+        o = (take_b ? bb : ba) | Q;
+    } else if (isnan(a)) {
+        o = ba | Q;
+    } else if (isnan(b)) {
+        o = bb | Q;
+    } else {
+        o = 0xfff8000000000000ull;
+    }
+    return __longlong_as_double((long long)o);
+}
 }  // namespace nr
 
 // The x86 SSE results of the plain single precision operations, NaNs included: a NaN operand
@@ -85,6 +107,36 @@ __device__ __forceinline__ float add(float a, float b) { return fix(a + b, a, b)
 __device__ __forceinline__ float sub(float a, float b) { return fix(a - b, a, b); }
 __device__ __forceinline__ float mul(float a, float b) { return fix(a * b, a, b); }
 __device__ __forceinline__ float div(float a, float b) { return fix(a / b, a, b); }
+// sqrtss: a NaN operand quieted, a negative number the default NaN
+__device__ __forceinline__ float sqrt(float a) {
+    if (isnan(a)) return nr::quiet(a);
+    if (a < 0.0f) return __uint_as_float(0xffc00000u);
+    return __fsqrt_rn(a);
+}
+// cvtss2sd / cvtsd2ss: a NaN keeps its sign and the leading bits of its payload, quieted
+__device__ __forceinline__ double widen(float a) {
+    if (!isnan(a)) return (double)a;
+    unsigned long long b = (unsigned long long)__float_as_uint(a);
+    unsigned long long o = ((b >> 31) << 63) | 0x7ff0000000000000ull | ((b & 0x007fffffull) << 29) | 0x0008000000000000ull;
+    return __longlong_as_double((long long)o);
+}
+__device__ __forceinline__ float narrow(double a) {
+    if (!isnan(a)) return __double2float_rn(a);
+    unsigned long long b = (unsigned long long)__double_as_longlong(a);
+    uint32_t o = (uint32_t)((b >> 63) << 31) | 0x7f800000u | (uint32_t)((b >> 29) & 0x007fffffull) | 0x00400000u;
+    return __uint_as_float(o);
+}
+// the double operations: a NaN operand propagates quieted (the first one), an invalid operation on
+// numbers gives the default NaN 0xfff8000000000000
+__device__ __forceinline__ double fixd(double r, double a, double b) {
+    if (!isnan(r)) return r;
+    const unsigned long long Q = 0x0008000000000000ull;
+    if (isnan(a)) return __longlong_as_double(__double_as_longlong(a) | (long long)Q);
+    if (isnan(b)) return __longlong_as_double(__double_as_longlong(b) | (long long)Q);
+    return __longlong_as_double((long long)0xfff8000000000000ull);
+}
+__device__ __forceinline__ double addd(double a, double b) { return fixd(__dadd_rn(a, b), a, b); }
+__device__ __forceinline__ double muld(double a, double b) { return fixd(__dmul_rn(a, b), a, b); }
 }  // namespace x86
 
 // sample.rs:31-41: index and fraction of one coordinate, clamped into 0..=len-2
