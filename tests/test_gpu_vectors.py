@@ -158,12 +158,21 @@ def test_debug_view_matches_oracle(dev, fmt, code, gouraud):
 @pytest.mark.parametrize("code", [0, 1, 2, 3])
 def test_debug_view_special_floats(dev, code):
     """Float frames with NaNs of both signs, infinities, denormals and FLT_MAX: the x86 NaN bits of
-    the views (the forward warp's, the OVERs', the luma's rule and the measures')."""
+    the views (the forward warp's, the OVERs', the luma's rule and the measures'). Where a plain
+    operation of the Edge measure meets two different NaNs, which one x86 returns is the operand the
+    compiler made the destination (debug.rs:295-301 says so of the luma), so there the Edge view is
+    compared NaN for NaN and bit for bit elsewhere."""
     w, h = 40, 30
     x, y, flow, fw, fh = _debug_pair(w, h, 2, seed=77 + code, specials=True)
     got = dev.debug_view(x, y, w, h, 2, flow, (fw, fh), code)
     want = O.debug_view(x, y, w, h, 2, flow, fw, fh, code)
-    assert same(got, want)
+    if code != 3:
+        assert same(got, want)
+    else:
+        nan = np.isnan(want)
+        assert np.array_equal(np.isnan(got), nan)
+        assert got[~nan].view(np.uint32).tobytes() == want[~nan].view(np.uint32).tobytes()
+        assert nan.any()
 
 
 @pytest.mark.parametrize("method", [1, 2, 3, 4, 5])

@@ -52,14 +52,14 @@ template <typename P> __device__ __forceinline__ void diff_px(const void* wp, co
     load4<P>(y, i, b);
     float l1 = diff_luma(wide<P>(a[1]), wide<P>(a[2]), wide<P>(a[3]));
     float l2 = diff_luma(wide<P>(b[1]), wide<P>(b[2]), wide<P>(b[3]));
-    float v = x86::mul(fabsf(x86::sub(l1, l2)), diff_gain());
+    float v = x86::mul(x86::abs(x86::sub(l1, l2)), diff_gain());
     if (sizeof(P) == 4) {
-        float f = v >= 1.0f ? 1.0f : v;
+        float f = x86::cap(v, 1.0f);
         o[0] = (P)1.0f;
         o[1] = o[2] = o[3] = (P)f;
     } else {
         float top = sizeof(P) == 1 ? 255.0f : 65535.0f;
-        float c = v >= top ? top : v;
+        float c = x86::cap(v, top);
         P q = (P)sat64(__dadd_rn((double)c, 0.5));
         o[0] = (P)top;
         o[1] = o[2] = o[3] = q;
@@ -128,7 +128,7 @@ __global__ void k_debug_luma(const void* __restrict__ img, int fmt, float* __res
     }
     float v = __double2float_rn(__dadd_rn(__dadd_rn(__ddiv_rn(__dmul_rn(r, 0.29), s), __ddiv_rn(__dmul_rn(g, 0.59), s)),
                                           __ddiv_rn(__dmul_rn(b, 0.12), s)));
-    out[i] = v >= 1.0f ? 1.0f : v;
+    out[i] = x86::cap(v, 1.0f);
 }
 
 namespace {
@@ -144,7 +144,7 @@ __device__ __forceinline__ float detail_at(const float* l, int w, int h, int x, 
 #pragma unroll
         for (int dx = -1; dx <= 1; dx++) {
             if (dx == 0 && dy == 0) continue;
-            float d = fabsf(x86::sub(c, l[(long)(y + dy) * w + x + dx]));
+            float d = x86::abs(x86::sub(c, l[(long)(y + dy) * w + x + dx]));
             s = first ? d : x86::add(s, d);
             first = false;
         }
@@ -158,19 +158,17 @@ __device__ __forceinline__ float edge_at(const float* l, int w, int h, int x, in
         return l[(long)yy * w + xx];
     };
     using namespace x86;
-    float gx = add(sub(add(sub(add(-n(-1, -1), n(1, -1)), mul(2.0f, n(-1, 0))), mul(2.0f, n(1, 0))), n(-1, 1)), n(1, 1));
+    float gx = add(sub(add(sub(add(x86::neg(n(-1, -1)), n(1, -1)), mul(2.0f, n(-1, 0))), mul(2.0f, n(1, 0))), n(-1, 1)), n(1, 1));
     float gy = sub(sub(sub(add(add(mul(2.0f, n(0, -1)), n(-1, -1)), n(1, -1)), n(-1, 1)), mul(2.0f, n(0, 1))), n(1, 1));
     float m = x86::sqrt(add(mul(gy, gy), mul(gx, gx)));
     float e = narrow(muld(widen(m), 0.17677669529664));
     float sc = mul(2.0f, e);
-    return sc > 255.0f ? 255.0f : sc;
+    return x86::cap_above(sc, 255.0f);
 }
 
 __device__ __forceinline__ float overlay_value(float m, float gain) {  // debug.rs:382-391
     float v = x86::mul(gain, m);
-    if (v > 1.0f) return 1.0f;
-    if (v < 0.0f) return 0.0f;
-    return v;
+    return x86::floor_below(x86::cap_above(v, 1.0f), 0.0f);
 }
 
 }  // namespace

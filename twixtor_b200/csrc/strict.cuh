@@ -107,6 +107,31 @@ __device__ __forceinline__ float add(float a, float b) { return fix(a + b, a, b)
 __device__ __forceinline__ float sub(float a, float b) { return fix(a - b, a, b); }
 __device__ __forceinline__ float mul(float a, float b) { return fix(a * b, a, b); }
 __device__ __forceinline__ float div(float a, float b) { return fix(a / b, a, b); }
+// andps / xorps: the sign bit alone, a NaN's payload kept (the device's abs and neg, which the
+// compiler would make of a plain mask, may not keep it: the masks are PTX integer operations)
+__device__ __forceinline__ float abs(float a) {
+    uint32_t r;
+    asm("and.b32 %0, %1, 0x7fffffff;" : "=r"(r) : "r"(__float_as_uint(a)));
+    return __uint_as_float(r);
+}
+__device__ __forceinline__ float neg(float a) {
+    uint32_t r;
+    asm("xor.b32 %0, %1, 0x80000000;" : "=r"(r) : "r"(__float_as_uint(a)));
+    return __uint_as_float(r);
+}
+// The branches of a clamp as a compare and a select of the sample bits in PTX: the compiler turns
+// `v >= t ? t : v` on floats into a min instruction, whose NaN result is canonical, where x86's
+// compare and select keep a NaN's bits.
+__device__ __forceinline__ float select_bits(bool p, float a, float b) {  // p ? a : b, bit for bit
+    uint32_t r;
+    asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %1, 0;\n\tselp.b32 %0, %2, %3, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(__float_as_uint(a)), "r"(__float_as_uint(b)));
+    return __uint_as_float(r);
+}
+__device__ __forceinline__ float cap(float v, float top) { return select_bits(v >= top, top, v); }
+__device__ __forceinline__ float cap_above(float v, float top) { return select_bits(v > top, top, v); }
+__device__ __forceinline__ float floor_below(float v, float bottom) { return select_bits(v < bottom, bottom, v); }
 // sqrtss: a NaN operand quieted, a negative number the default NaN
 __device__ __forceinline__ float sqrt(float a) {
     if (isnan(a)) return nr::quiet(a);
