@@ -296,8 +296,10 @@ int tw_block_match(tw_ctx* ctx, const float* a, const float* b, float* flow, int
 #define TW_NOALLOC_MAX_PIXELS (1L << 19)
 int tw_block_match_noalloc(const float* a, const float* b, float* flow, int32_t width, int32_t height, void* stream);
 
-/* warp::inv_warp / inv_warp_coverage (warp.rs:693-786) with mode 1 and is360 off; cov may be NULL
- * (no coverage image) or width*height bytes. */
+/* warp::inv_warp / inv_warp_coverage (warp.rs:693-786) with mode 1; `hold` carries WarpOpts: bit 0
+ * hold, bit 1 is360 (the wrap by whole turns, the pole reflection and the 360 sampler, warp.rs:
+ * 563-621; it takes precedence over hold and leaves the coverage at 255). cov may be NULL (no
+ * coverage image) or width*height bytes. */
 int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_flow* flow, float amount, int32_t hold,
                 uint8_t* cov);
 

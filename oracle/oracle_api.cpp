@@ -442,7 +442,8 @@ int or_inv_warp(void* out_eng, const void* src_eng, int w, int h, int fmt, const
     FlowField f(fw, fh);
     std::memcpy(f.d.data(), flow, f.d.size() * sizeof(float));
     WarpOpts o;
-    o.hold = hold != 0;
+    o.hold = (hold & 1) != 0;  // bit 0 hold, bit 1 is360 (warp.rs:29-50)
+    o.is360 = (hold & 2) != 0;
     Coverage c;
     std::string e;
     int rc = inv_warp(out, src, f, amount, o, cov ? &c : nullptr, &e);

@@ -1238,6 +1238,78 @@ static inline void bilerp4(const P* src, int w, int w1, int h1, float x, float y
     }
 }
 
+// warp.rs:339-352 (mix4): the three lerps of four taps, repeated with the NaN rule when NaN
+template <typename P>
+static inline void mix4(const P* a, const P* b, const P* c, const P* d, float fx, float fy, float out[4]) {
+    bool any = false;
+    for (int k = 0; k < 4; k++) {
+        float p00 = PixT<P>::f(a[k]), p10 = PixT<P>::f(b[k]), p01 = PixT<P>::f(c[k]), p11 = PixT<P>::f(d[k]);
+        float top = p00 + (p10 - p00) * fx;
+        float bot = p01 + (p11 - p01) * fx;
+        out[k] = top + (bot - top) * fy;
+        any = any || std::isnan(out[k]);
+    }
+    if (any) {
+        for (int k = 0; k < 4; k++) {
+            float p00 = PixT<P>::f(a[k]), p10 = PixT<P>::f(b[k]), p01 = PixT<P>::f(c[k]), p11 = PixT<P>::f(d[k]);
+            float top = nr::add(p00, nr::mul(nr::sub(p10, p00), fx));
+            float bot = nr::add(p01, nr::mul(nr::sub(p11, p01), fx));
+            out[k] = nr::add(top, nr::mul(nr::sub(bot, top), fy));
+        }
+    }
+}
+
+// warp.rs:362-396 (bilerp360): the right neighbour of the last column is column 0; below the last
+// row the taps come from the last row shifted by half the width
+template <typename P>
+static inline void bilerp360(const P* src, int w, int w1, int h1, float x, float y, float out[4]) {
+    int ix = cvtt32(x), iy = cvtt32(y);
+    float fx = x - (float)ix, fy = y - (float)iy;
+    int x1 = ix + 1 > w1 ? 0 : ix + 1;
+    int xc, xd, yc;
+    if (iy + 1 > h1) {
+        int half = w / 2;
+        xc = (half + ix) % w;
+        xd = (half + x1) % w;
+        yc = h1;
+    } else {
+        xc = ix;
+        xd = x1;
+        yc = iy + 1;
+    }
+    int ya = std::min(iy, h1);
+    xc = std::max(xc, 0);
+    xd = std::max(xd, 0);
+    auto at = [&](int xx, int yy) { return src + ((long)yy * w + xx) * 4; };
+    mix4(at(ix, ya), at(x1, ya), at(xc, yc), at(xd, yc), fx, fy, out);
+}
+
+// warp.rs:563-621 (pixel_360): the point wrapped into the image by whole turns, an odd number of
+// vertical wraps reflected over the pole (half a turn across, H - iy), then the 360 sampler; false
+// when the wrap loops would not end or the point is NaN
+template <typename P>
+static inline bool pixel_360(const P* src, int width, int w1i, int h1i, float wf, float hf, float ix, float iy, P* px) {
+    const uint32_t WRAP_LIMIT = 1u << 16;
+    uint32_t guard = 0, n = 0;
+    while (ix < 0.0f) { ix += wf; if (++guard > WRAP_LIMIT) break; }
+    while (wf <= ix) { ix -= wf; if (++guard > WRAP_LIMIT) break; }
+    while (iy < 0.0f) { iy += hf; n++; if (++guard > WRAP_LIMIT) break; }
+    while (hf <= iy) { iy -= hf; n++; if (++guard > WRAP_LIMIT) break; }
+    if (guard > WRAP_LIMIT || !(ix >= 0.0f && ix < wf) || std::isnan(iy)) {
+        for (int k = 0; k < 4; k++) px[k] = P(0);
+        return false;
+    }
+    if (n & 1) {
+        ix = wf * 0.5f + ix;
+        if (ix >= wf) ix -= wf;
+        if (iy != 0.0f) iy = hf - iy;
+    }
+    float s[4];
+    bilerp360(src, width, w1i, h1i, ix, iy, s);
+    for (int k = 0; k < 4; k++) px[k] = PixT<P>::store(s[k]);
+    return true;
+}
+
 // warp.rs:415-442 (Flow::bilerp)
 static inline void flow_bilerp(const float* d, int fw, int fw1, int fh1, float x, float y, float out[2]) {
     int ix = cvtt32(x), iy = cvtt32(y);
@@ -1277,7 +1349,9 @@ static bool warp_run(P* out, uint8_t* cov, const P* src, const FlowField& flow, 
             float ix = dd[0] * sx + xf;
             float iy = dd[1] * sy + yf;
             P* px = out + ((long)y * width + x) * 4;
-            if (o.hold) {
+            if (o.is360) {
+                if (!pixel_360(src, width, w1i, h1i, wf, hf, ix, iy, px)) bad = true;
+            } else if (o.hold) {
                 if (!clip_to_rect(xf, yf, &ix, &iy, w1, h1) || std::isnan(ix) || std::isnan(iy)) {
                     bad = true;
                     for (int k = 0; k < 4; k++) px[k] = P(0);
@@ -1335,7 +1409,6 @@ int inv_warp(Image& out, const Image& src, const FlowField& flow, float amount, 
     }
     if (copy_only) { copy_image(out, src); return 0; }
     if (o.mode != 1) { *err = "inverse warp: mip map sampling"; return 2; }
-    if (o.is360) { *err = "inverse warp: 360 mode is not restated"; return 2; }
     uint8_t* c = cov ? cov->d.data() : nullptr;
     bool ok;
     if (out.fmt == U8) ok = warp_run<uint8_t>(out.u8.data(), c, src.u8.data(), flow, amount, o, width, height);

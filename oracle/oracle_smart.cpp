@@ -245,10 +245,97 @@ static std::vector<float> resample1_g(const std::vector<float>& src, int sw, int
 
 static const float BIN5[3] = {0.375f, 0.25f, 0.0625f};
 
+// The wrap-around (360) passes of the fill (holefill.rs:174-236, conv.rs:518-536, sample.rs:
+// 204-227) over an arithmetic set: the circular horizontal pass (tap indices modulo the width, no
+// renormalisation), the column walk of the equirectangular frame (reflect at the edge row, half a
+// turn across), and the period keeping resample (steps sw / dw, sh / dh, the sphere sampler)
+template <class A>
+static void convolve1_wrap(float* data, int w, int h, const float* k, int n) {
+    if (w == 0 || h == 0 || n == 0) return;
+    std::vector<float> tmp((size_t)w * h);
+    for (int y = 0; y < h; y++) {
+        const float* x = data + (long)y * w;
+        for (int i = 0; i < w; i++) {
+            float sum = A::mul(x[i], k[0]);
+            for (int j = n - 1; j >= 1; j--) {
+                int r = (i + j) % w;
+                int l = ((i - j) % w + w) % w;
+                sum = A::add(sum, A::mul(A::add(x[r], x[l]), k[j]));
+            }
+            tmp[(size_t)y * w + i] = sum;
+        }
+    }
+    int half = w / 2, pad = n - 1;
+    std::vector<float> g((size_t)h + 2 * pad);
+    for (int x = 0; x < w; x++) {
+        auto walk = [&](int start, int dir, int m_out, float* dst_rev, bool reverse) {
+            int c = x, r = start, d = dir;
+            for (int m = 0; m < m_out; m++) {
+                r += d;
+                if (r < 0) { r = 0; d = -d; c = (half + c) % w; }
+                else if (r >= h) { r = h - 1; d = -d; c = (half + c) % w; }
+                float v = tmp[(size_t)r * w + c];
+                if (reverse) dst_rev[m_out - 1 - m] = v;
+                else dst_rev[m] = v;
+            }
+        };
+        walk(0, -1, pad, g.data(), true);
+        for (int r = 0; r < h; r++) g[pad + r] = tmp[(size_t)r * w + x];
+        walk(h - 1, 1, pad, g.data() + pad + h, false);
+        for (int y = 0; y < h; y++) {
+            int e = pad + y;
+            float sum = A::mul(g[e], k[0]);
+            for (int j = n - 1; j >= 1; j--) sum = A::add(sum, A::mul(A::add(g[e + j], g[e - j]), k[j]));
+            data[(size_t)y * w + x] = sum;
+        }
+    }
+}
+
+template <class A>
+static std::vector<float> resample1_wrap(const std::vector<float>& src, int sw, int sh, int dw, int dh) {
+    std::vector<float> dst((size_t)dw * dh, 0.0f);
+    if (dw == 0 || dh == 0) return dst;
+    float sx = (float)sw / (float)dw, sy = (float)sh / (float)dh;
+    int w1 = sw - 1, h1 = sh - 1;
+    for (int y = 0; y < dh; y++) {
+        float yf = (float)y * sy;
+        for (int x = 0; x < dw; x++) {
+            float xf = (float)x * sx;
+            int tx = cvtt32(xf), ty = cvtt32(yf);
+            int ix = std::min(std::max(tx, 0), w1), iy = std::min(std::max(ty, 0), h1);
+            float fx = xf - (float)tx, fy = yf - (float)ty;
+            int x1 = ix + 1 > w1 ? 0 : ix + 1;
+            int xc = ix, xd = x1, yc = iy + 1;
+            if (iy + 1 > h1) {
+                int half = sw / 2;
+                xc = (half + ix) % sw;
+                xd = (half + x1) % sw;
+                yc = h1;
+            }
+            float p00 = src[(size_t)iy * sw + ix], p10 = src[(size_t)iy * sw + x1];
+            float p01 = src[(size_t)yc * sw + xc], p11 = src[(size_t)yc * sw + xd];
+            float top = lerp_g<A>(p00, p10, fx);
+            float bot = lerp_g<A>(p01, p11, fx);
+            dst[(size_t)y * dw + x] = lerp_g<A>(top, bot, fy);
+        }
+    }
+    return dst;
+}
+
+template <class A>
+static void fill_conv(float* data, int w, int h, const float* k, int n, bool above_first, bool wrap) {
+    if (wrap) convolve1_wrap<A>(data, w, h, k, n);
+    else convolve1<A>(data, w, h, k, n, above_first);
+}
+template <class A>
+static std::vector<float> fill_resample(const std::vector<float>& src, int sw, int sh, int dw, int dh, bool wrap) {
+    return wrap ? resample1_wrap<A>(src, sw, sh, dw, dh) : resample1_g<A>(src, sw, sh, dw, dh);
+}
+
 template <class A>
 static std::vector<float> fill_solve(const FillGeometry& geo, const std::vector<bool>& hole,
                                      const std::vector<std::vector<float>>& wts, const std::vector<float>& plane,
-                                     bool above_first, const std::vector<float>& g5) {
+                                     bool above_first, const std::vector<float>& g5, bool wrap) {
     std::vector<std::vector<float>> vals;
     std::vector<float> v0 = plane;
     for (size_t i = 0; i < v0.size(); i++)
@@ -258,8 +345,8 @@ static std::vector<float> fill_solve(const FillGeometry& geo, const std::vector<
         int pw = geo.dims[k - 1].first, ph = geo.dims[k - 1].second;
         int cw = geo.dims[k].first, ch = geo.dims[k].second;
         std::vector<float> tmp = vals[k - 1];
-        convolve1<A>(tmp.data(), pw, ph, BIN5, 3, above_first);
-        vals.push_back(resample1_g<A>(tmp, pw, ph, cw, ch));
+        fill_conv<A>(tmp.data(), pw, ph, BIN5, 3, above_first, wrap);
+        vals.push_back(fill_resample<A>(tmp, pw, ph, cw, ch, wrap));
     }
     int tw = geo.dims[geo.top].first, th = geo.dims[geo.top].second;
     std::vector<float> sol((size_t)tw * th, 0.0f);
@@ -270,12 +357,12 @@ static std::vector<float> fill_solve(const FillGeometry& geo, const std::vector<
                 if (wt[i] != 0.0f) s[i] = A::div(v[i], wt[i]);
         };
         combine(sol, vals[level], wts[level]);
-        convolve1<A>(sol.data(), lw, lh, g5.data(), (int)g5.size(), above_first);
+        fill_conv<A>(sol.data(), lw, lh, g5.data(), (int)g5.size(), above_first, wrap);
         if (level == 0) {
             combine(sol, vals[0], wts[0]);
         } else {
             int nw = geo.dims[level - 1].first, nh = geo.dims[level - 1].second;
-            sol = resample1_g<A>(sol, lw, lh, nw, nh);
+            sol = fill_resample<A>(sol, lw, lh, nw, nh, wrap);
         }
     }
     return sol;
@@ -290,11 +377,12 @@ struct PlaneFiller {
     std::vector<std::vector<float>> wts;
     std::vector<float> g5;
     bool above_first = false;
+    bool wrap = false;
     void fill(std::vector<float>& plane) const {
-        std::vector<float> sol = fill_solve<Plain>(geo, hole, wts, plane, above_first, g5);
+        std::vector<float> sol = fill_solve<Plain>(geo, hole, wts, plane, above_first, g5, wrap);
         bool has_nan = false;
         for (float v : sol) has_nan = has_nan || std::isnan(v);
-        if (has_nan) sol = fill_solve<Rule>(geo, hole, wts, plane, above_first, g5);
+        if (has_nan) sol = fill_solve<Rule>(geo, hole, wts, plane, above_first, g5, wrap);
         plane.swap(sol);
     }
 };
@@ -303,7 +391,7 @@ struct PlaneFiller {
 // image with a side of 1; a pixel is a hole when !(eps > m) (holefill.rs:124-133), mask_kind 1 u8,
 // 2 u16, 3 f32
 static int make_filler(int w, int h, const void* mask, int mask_kind, bool above_first, PlaneFiller* f, bool* none,
-                       std::string* err) {
+                       std::string* err, bool wrap) {
     long n = (long)w * h;
     const double U8_EPS = [] { uint64_t b = 0x20202020202020fcull; double d; std::memcpy(&d, &b, 8); return d; }();
     const double WIDE_EPS = [] { uint64_t b = 0x3f0040bfe3b03e21ull; double d; std::memcpy(&d, &b, 8); return d; }();
@@ -323,6 +411,7 @@ static int make_filler(int w, int h, const void* mask, int mask_kind, bool above
     if (w < 2 || h < 2) { *err = "hole fill of an image with a side of 1"; return 2; }
     f->geo = fill_geometry(w, h);
     f->above_first = above_first;
+    f->wrap = wrap;
     f->g5 = gaussian_kernel(5.0f);
     std::vector<float> w0((size_t)n);
     for (long i = 0; i < n; i++) w0[i] = f->hole[i] ? 0.0f : 1.0f;
@@ -331,19 +420,19 @@ static int make_filler(int w, int h, const void* mask, int mask_kind, bool above
         int pw = f->geo.dims[k - 1].first, ph = f->geo.dims[k - 1].second;
         int cw = f->geo.dims[k].first, ch = f->geo.dims[k].second;
         std::vector<float> tmp = f->wts[k - 1];
-        convolve1<Plain>(tmp.data(), pw, ph, BIN5, 3, above_first);
-        f->wts.push_back(resample1_g<Plain>(tmp, pw, ph, cw, ch));
+        fill_conv<Plain>(tmp.data(), pw, ph, BIN5, 3, above_first, wrap);
+        f->wts.push_back(fill_resample<Plain>(tmp, pw, ph, cw, ch, wrap));
     }
     return 0;
 }
 
 // holefill.rs:452-491 (fill_holes_masked_with, plain passes): mask_kind 1 u8, 2 u16, 3 f32
-int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, std::string* err) {
+int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, std::string* err, bool wrap) {
     int w = img.w, h = img.h;
     long n = (long)w * h;
     PlaneFiller f;
     bool none = false;
-    int rc = make_filler(w, h, mask, mask_kind, above_first, &f, &none, err);
+    int rc = make_filler(w, h, mask, mask_kind, above_first, &f, &none, err, wrap);
     if (rc || none) return rc;
     std::vector<float> plane((size_t)n);
     for (int c = 0; c < 4; c++) {
@@ -362,11 +451,11 @@ int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, st
 
 // holefill.rs:497-518 (fill_flow_holes_with, is360 off): both components of a flow filled as
 // planes with the mask of the flow's size
-int fill_flow_holes(FlowField& flow, const void* mask, int mask_kind, bool above_first, std::string* err) {
+int fill_flow_holes(FlowField& flow, const void* mask, int mask_kind, bool above_first, std::string* err, bool wrap) {
     long n = (long)flow.w * flow.h;
     PlaneFiller f;
     bool none = false;
-    int rc = make_filler(flow.w, flow.h, mask, mask_kind, above_first, &f, &none, err);
+    int rc = make_filler(flow.w, flow.h, mask, mask_kind, above_first, &f, &none, err, wrap);
     if (rc || none) return rc;
     std::vector<float> plane((size_t)n);
     for (int c = 0; c < 2; c++) {

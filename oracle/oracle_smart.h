@@ -17,10 +17,13 @@ FillGeometry fill_geometry(int w, int h);
 // smartblend.rs:268-298: smart_blend (binary false) / smart_blend_binary (binary true)
 void smart_blend(Image& out, const Image& p1, const Image& p2, float w, bool binary);
 
-// holefill.rs:452-491 with the plain passes; mask_kind 1 u8, 2 u16, 3 f32 (w*h entries)
-int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, std::string* err);
-// holefill.rs:497-518 (fill_flow_holes_with, is360 off): the two components of a flow
-int fill_flow_holes(FlowField& flow, const void* mask, int mask_kind, bool above_first, std::string* err);
+// holefill.rs:452-491; mask_kind 1 u8, 2 u16, 3 f32 (w*h entries); wrap: the is360 passes
+// (holefill.rs:34-40: the circular horizontal pass, the equirectangular column walk, the period
+// keeping resample)
+int fill_holes(Image& img, const void* mask, int mask_kind, bool above_first, std::string* err, bool wrap = false);
+// holefill.rs:497-518 (fill_flow_holes_with): the two components of a flow
+int fill_flow_holes(FlowField& flow, const void* mask, int mask_kind, bool above_first, std::string* err,
+                    bool wrap = false);
 
 // warping code 1 compositions (smartblend.rs:350-393): Nearest and Blend
 int compose_smart(const ComposeSettings& cs, const Selection& sel, const Image& a, const Image& b, const FlowField* f_ab,

@@ -304,10 +304,11 @@ def solve_pyramids_with(x, y, w, h, fmt, matte_x=None, matte_y=None, pairs=None,
             ud if npts else None, uw if npts else None)
 
 
-def inv_warp(src, w, h, fmt, flow, fw, fh, amount, hold=True, coverage=False, out=None):
+def inv_warp(src, w, h, fmt, flow, fw, fh, amount, hold=True, coverage=False, out=None, is360=False):
     o = np.zeros_like(src) if out is None else out.copy()
     cov = np.zeros(w * h, np.uint8) if coverage else None
-    rc = lib().or_inv_warp(ptr(o), ptr(src), w, h, fmt, ptr(flow), fw, fh, amount, int(hold), ptr(cov))
+    rc = lib().or_inv_warp(ptr(o), ptr(src), w, h, fmt, ptr(flow), fw, fh, amount, int(hold) | (2 if is360 else 0),
+                           ptr(cov))
     if rc:
         raise ValueError(err())
     return (o, cov) if coverage else o

@@ -75,11 +75,12 @@ def test_from_and_to_frame(dev, fmt):
 WARP = golden_data.warp_cases()
 
 
-@pytest.mark.parametrize("i", [i for i, c in enumerate(WARP) if not c["is360"]])
+@pytest.mark.parametrize("i", range(len(WARP)))
 def test_inverse_warp_reference_fixtures(dev, i):
+    """Every case of warp_cases.hex, the 360 ones included."""
     c = WARP[i]
     r = dev.inv_warp(c["src"], c["w"], c["h"], c["fmt"], c["flow"], (c["fw"], c["fh"]), c["amount"], hold=c["hold"],
-                     coverage=c["want_cov"])
+                     coverage=c["want_cov"], is360=c["is360"])
     out, cov = r if c["want_cov"] else (r, None)
     assert same(out, c["out"])
     if c["want_cov"]:
@@ -543,3 +544,20 @@ def test_batch_of_uneven_clips_equals_each_clip(dev):
     dev.retime_batch_device(jobs)
     for (w, h, fmt, _), out, wnt in zip(specs, keep[1::2], want):
         assert same(out.cpu().numpy(), wnt)
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("size", [(37, 23), (160, 96), (1920, 1080)])
+def test_inverse_warp_360_matches_oracle(dev, fmt, size):
+    """The 360 inverse warp with flows of several turns in both axes (the pole reflection on odd
+    vertical wraps, the half-width shift below the last row) against the oracle."""
+    w, h = size
+    rng = np.random.RandomState(w + fmt)
+    src, _ = rand_engine(rng, w, h, fmt)
+    fw, fh = max(2, w // 2), max(2, h // 2)
+    flow = (rng.standard_normal(fw * fh * 2) * np.float32(max(w, h) * 0.8)).astype(np.float32)
+    for amount in (1.0, -0.6, 2.5):
+        got, cov = dev.inv_warp(src, w, h, fmt, flow, (fw, fh), amount, coverage=True, is360=True)
+        want, wcov = O.inv_warp(src, w, h, fmt, flow, fw, fh, amount, coverage=True, is360=True)
+        assert same(got, want), amount
+        assert (cov == 255).all() and (wcov == 255).all()

@@ -151,11 +151,12 @@ def test_quality_to_resolution_table():
 WARP = golden_data.warp_cases()
 
 
-@pytest.mark.parametrize("i", [i for i, c in enumerate(WARP) if not c["is360"]])
+@pytest.mark.parametrize("i", range(len(WARP)))
 def test_inverse_warp_model_fixtures(i):
+    """Every case of warp_cases.hex, the 360 ones (wrap, pole reflection, the 360 sampler) included."""
     c = WARP[i]
     r = O.inv_warp(c["src"], c["w"], c["h"], c["fmt"], c["flow"], c["fw"], c["fh"], c["amount"], hold=c["hold"],
-                   coverage=c["want_cov"])
+                   coverage=c["want_cov"], is360=c["is360"])
     out, cov = r if c["want_cov"] else (r, None)
     assert out.view(np.uint8).tobytes() == c["out"].view(np.uint8).tobytes()
     if c["want_cov"]:

@@ -709,7 +709,8 @@ class Device:
         self._check(self._L.tw_block_match(self._h, _ptr(a), _ptr(b), _ptr(f), width, height))
         return f
 
-    def inv_warp(self, src, width, height, fmt, flow, flow_size, amount, hold=True, coverage=False):
+    def inv_warp(self, src, width, height, fmt, flow, flow_size, amount, hold=True, coverage=False, is360=False):
+        """``warp::inv_warp`` (mode 1): hold edges, or the fade with coverage, or the 360 wrap."""
         fw, fh = flow_size
         out = np.zeros(width * height * 4, DTYPES[fmt])
         si, sa = _img(src, width, height, fmt)
@@ -718,7 +719,7 @@ class Device:
         fl = _Flow(fw, fh, flow.ctypes.data)
         cov = np.zeros(width * height, np.uint8) if coverage else None
         self._check(self._L.tw_inv_warp(self._h, ctypes.byref(oi), ctypes.byref(si), ctypes.byref(fl),
-                                        np.float32(amount), int(hold), _ptr(cov)))
+                                        np.float32(amount), int(hold) | (2 if is360 else 0), _ptr(cov)))
         return (out, cov) if coverage else out
 
     def blend(self, a, b, width, height, fmt, w):

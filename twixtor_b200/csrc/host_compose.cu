@@ -793,7 +793,8 @@ int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_fl
     CHECK(ctx->ensure(ctx->plane[3], (size_t)W * H, "coverage"));
     int* flags = ctx->flags.as<int>();
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
-    WarpParams p = warp_params(ctx->eng[0].p, ctx->flow[0].as<float>(), flow->width, flow->height, amount, W, hold != 0);
+    WarpParams p = warp_params(ctx->eng[0].p, ctx->flow[0].as<float>(), flow->width, flow->height, amount, W, (hold & 1) != 0);
+    p.is360 = (hold & 2) != 0;  // warp.rs:29-50: is360 takes precedence over hold
     uint8_t* dcov = cov ? ctx->plane[3].as<uint8_t>() : nullptr;
     LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, p, src->fmt, ctx->eng[2].p, dcov, W, H, flags + FL_BAD);
     CHECK(ctx->cuda(cudaMemcpyAsync(out->data, ctx->eng[2].p, ob, cudaMemcpyDeviceToHost, ctx->stream), "download"));

@@ -117,6 +117,7 @@ struct WarpParams {
     float amount;
     bool copy_only;      // the |amount| early outs of inv_warp (warp.rs:751-764)
     bool hold;
+    bool is360;          // wrap-around: the point wrapped into the image, the pole reflection, the 360 sampler
 };
 // out = inv_warp(src, flow, amount); optional coverage
 __global__ void k_inv_warp(WarpParams p, int fmt, void* __restrict__ out, uint8_t* __restrict__ cov, int w, int h,

@@ -95,6 +95,83 @@ __device__ __forceinline__ void bilerp4(const P* __restrict__ src, int w, int w1
     }
 }
 
+// warp.rs:339-352 (mix4): the three lerps of four taps, repeated with the NaN rule when NaN
+template <typename P>
+__device__ __forceinline__ void mix4(const P* a, const P* b, const P* c, const P* d, float fx, float fy, float o[4]) {
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float p00 = Pix<P>::f(a[k]), p10 = Pix<P>::f(b[k]), p01 = Pix<P>::f(c[k]), p11 = Pix<P>::f(d[k]);
+        float top = p00 + (p10 - p00) * fx;
+        float bot = p01 + (p11 - p01) * fx;
+        o[k] = top + (bot - top) * fy;
+        any = any || isnan(o[k]);
+    }
+    if (any) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            float p00 = Pix<P>::f(a[k]), p10 = Pix<P>::f(b[k]), p01 = Pix<P>::f(c[k]), p11 = Pix<P>::f(d[k]);
+            float top = nr::add(p00, nr::mul(nr::sub(p10, p00), fx));
+            float bot = nr::add(p01, nr::mul(nr::sub(p11, p01), fx));
+            o[k] = nr::add(top, nr::mul(nr::sub(bot, top), fy));
+        }
+    }
+}
+
+// warp.rs:362-396 (bilerp360): the coordinates already in [0, W) x [0, H); the right neighbour of
+// the last column is column 0, below the last row the taps are the last row's shifted by half the
+// width
+template <typename P>
+__device__ __forceinline__ void bilerp360(const P* __restrict__ src, int w, int w1, int h1, float x, float y, float o[4]) {
+    int ix = cvtt32(x), iy = cvtt32(y);
+    float fx = x - (float)ix, fy = y - (float)iy;
+    int x1 = ix + 1 > w1 ? 0 : ix + 1;
+    int xc, xd, yc;
+    if (iy + 1 > h1) {
+        int half = w / 2;
+        xc = (half + ix) % w;
+        xd = (half + x1) % w;
+        yc = h1;
+    } else {
+        xc = ix;
+        xd = x1;
+        yc = iy + 1;
+    }
+    int ya = min(iy, h1);
+    xc = max(xc, 0);
+    xd = max(xd, 0);
+    auto at = [&](int xx, int yy) { return src + ((long)yy * w + xx) * 4; };
+    mix4<P>(at(ix, ya), at(x1, ya), at(xc, yc), at(xd, yc), fx, fy, o);
+}
+
+// warp.rs:563-621 (pixel_360): wrapped by whole turns (at most 2^16 steps, else bad), an odd number
+// of vertical wraps reflected over the pole, then the 360 sampler; the coverage stays 255
+template <typename P>
+__device__ __forceinline__ void pixel_360(const P* src, int w, int h, float ix, float iy, P o[4], bool& bad) {
+    const uint32_t WRAP_LIMIT = 1u << 16;
+    float wf = (float)w, hf = (float)h;
+    uint32_t guard = 0, n = 0;
+    while (ix < 0.0f) { ix += wf; if (++guard > WRAP_LIMIT) break; }
+    while (wf <= ix) { ix -= wf; if (++guard > WRAP_LIMIT) break; }
+    while (iy < 0.0f) { iy += hf; n++; if (++guard > WRAP_LIMIT) break; }
+    while (hf <= iy) { iy -= hf; n++; if (++guard > WRAP_LIMIT) break; }
+    if (guard > WRAP_LIMIT || !(ix >= 0.0f && ix < wf) || isnan(iy)) {
+        bad = true;
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = P(0);
+        return;
+    }
+    if (n & 1) {
+        ix = wf * 0.5f + ix;
+        if (ix >= wf) ix -= wf;
+        if (iy != 0.0f) iy = hf - iy;
+    }
+    float s[4];
+    bilerp360<P>(src, w, w - 1, h - 1, ix, iy, s);
+#pragma unroll
+    for (int k = 0; k < 4; k++) o[k] = Pix<P>::store(s[k]);
+}
+
 // warp.rs:415-442 (Flow::bilerp) on a strided field
 __device__ __forceinline__ void flow_bilerp(const WarpParams& p, float x, float y, float& du, float& dv) {
     int fw1 = p.fw - 1, fh1 = p.fh - 1;
@@ -141,6 +218,10 @@ __device__ __forceinline__ uint8_t warp_pixel(const WarpParams& p, int x, int y,
     float ix = du * sx + xf;
     float iy = dv * sy + yf;
     float s[4];
+    if (p.is360) {
+        pixel_360<P>(src, w, h, ix, iy, o, bad);
+        return 255;
+    }
     if (p.hold) {
         if (!clip_to_rect(xf, yf, ix, iy, w1, h1) || isnan(ix) || isnan(iy)) {
             bad = true;
