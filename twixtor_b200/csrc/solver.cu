@@ -386,10 +386,11 @@ __global__ void k_fill(float* __restrict__ p, long n, float v) {
 // Each cost evaluation is Block::cost bit for bit, so the result equals the sequential sweep.
 
 // Shared memory of one line of length len: u, v, c0 (floats), the three rows of A along the line
-// (floats), next / jump / on (ints), plus 64 ints for the block scan and the queue counter.
-size_t bm_smem_bytes(int len) { return (size_t)len * 4 * (3 + 3 + 3) + 64 * 4; }
+// (floats), end and two queues (ints), then 8 counters and two ints per 32-position chunk.
+size_t bm_smem_bytes(int len) { return (size_t)len * 4 * (3 + 3 + 3) + (size_t)(8 + 2 * ((len + 31) / 32)) * 4; }
 
-constexpr int BM_WINDOW = 4;  // accept tests a long candidate run evaluates at once (independent loads)
+constexpr int BM_STAGES = 3;      // run extension tests made one per queued candidate before groups of 8 lanes
+constexpr int BM_TERM = 1 << 30;  // "past the line" in the chain tables
 
 // The 3x3 patch of A around line position i (flow.rs:454-469) from the three lines of A in shared
 // memory (rows y-1..y+1 for a row sweep, columns x-1..x+1 for a column sweep).
@@ -401,18 +402,53 @@ __device__ __forceinline__ void bm_patch(const float* s_a, int len, int i, float
         for (int c = 0; c < 3; c++) p[r * 3 + c] = COLS ? s_a[c * len + (i - 1 + r)] : s_a[r * len + (i - 1 + c)];
 }
 
-// accept(i, n) of the sweep at line position i (Block::step, flow.rs:529-546): c0 is the cost of
-// the current vector (NaN when the step cannot happen at i: no target or no cost).
+// accept(i, n) of the sweep at line position i with its patch p (Block::step, flow.rs:529-546): ci is
+// the cost of the current vector (NaN when the step cannot happen at i: no target or no cost).
 template <bool COLS>
-__device__ __forceinline__ bool bm_accept(const float* s_a, int len, const float* __restrict__ B, int w, int h,
-                                          int fixed, int i, float nu, float nv, float ci) {
+__device__ __forceinline__ bool bm_accept_p(const float p[9], const float* __restrict__ B, int w, int h, int fixed,
+                                            int i, float nu, float nv, float ci) {
     if (isnan(ci)) return false;  // None, or a NaN cost that nothing compares below
     int x = COLS ? fixed : i, y = COLS ? i : fixed;
-    float p[9];
-    bm_patch<COLS>(s_a, len, i, p);
     float c1;
     if (!bm_cost<COLS>(B, w, h, p, (float)x - nu, (float)y - nv, c1)) return false;
     return c1 < ci;
+}
+
+template <bool COLS>
+__device__ __forceinline__ bool bm_accept(const float* s_a, int len, const float* __restrict__ B, int w, int h,
+                                          int fixed, int i, float nu, float nv, float ci) {
+    float p[9];
+    bm_patch<COLS>(s_a, len, i, p);
+    return bm_accept_p<COLS>(p, B, w, h, fixed, i, nu, nv, ci);
+}
+
+// The cost of the vector (u, v) at line position i (flow.rs:529-536): NaN when its target leaves the
+// level or the block has no cost.
+template <bool COLS>
+__device__ __forceinline__ float bm_own_cost(const float p[9], const float* __restrict__ B, int w, int h, int fixed,
+                                             int i, float u, float v) {
+    float c = __int_as_float(0x7fc00000);
+    int x = COLS ? fixed : i, y = COLS ? i : fixed;
+    float tx = (float)x - u;
+    float ty = (float)y - v;
+    if (0.0f <= tx && tx <= (float)(w - 1) && 0.0f <= ty && ty <= (float)(h - 1)) {
+        float cost;
+        if (bm_cost<COLS>(B, w, h, p, tx, ty, cost)) c = cost;
+    }
+    return c;
+}
+
+// Appends val to q (counter *n) for the lanes of the warp with `want`: one atomic per warp. Every lane
+// of the warp calls it.
+__device__ __forceinline__ void bm_push(int* q, int* n, bool want, int val) {
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (m) {
+        const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
+        int base = 0;
+        if (lane == lead) base = atomicAdd(n, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, lead);
+        if (want) q[base + __popc(m & ((1u << lane) - 1u))] = val;
+    }
 }
 
 // One sweep over a line held in shared memory (su, sv: the field along the line, updated in place;
@@ -420,171 +456,216 @@ __device__ __forceinline__ bool bm_accept(const float* s_a, int len, const float
 // column x (COLS true: pixel (x, i)); len is its length. Forward sweeps run i = 1..len-2 with the
 // neighbour i - 1, reverse sweeps i = len-2..1 with the neighbour i + 1. In "sweep order" position
 // q (q = i forward, q = len-1-i reverse) both are the same forward recurrence
-// v'[q] = accept(q, v'[q-1]) ? v'[q-1] : v[q], so every v'[q] is the vector of its run's start and
-// a run started at j continues while accept(q, v[j]) holds:
-//   1. c0[i], the cost of the current vector, at every interior position (the reverse sweep keeps
-//      the forward sweep's value where that sweep left the vector as it was: chg[i] == 0);
-//   2. end[q] for every candidate start q: one accept test of the next position; the candidates
-//      whose run goes on (about a third at the finest level) are compacted into a queue;
-//   3. the queued candidates scan on, BM_WINDOW tests at a time, to the first refusal;
-//   4. the run starts 0, end[0], end[end[0]], ... marked by pointer jumping, the owner of each
-//      position by a block max-scan, then v[owner] into the line (the forward sweep records in
-//      chg which positions took another vector).
-// The in place update is safe: step 4 reads only run starts, which keep their own vectors.
+// v'[q] = accept(q, v'[q-1]) ? v'[q-1] : v[q], so every v'[q] is the vector of its run's start, and
+// a run started at j ends at end[j], the first position past j that refuses v[j]. The sweep:
+//   1. c0[i], the cost of the current vector (the reverse sweep recomputes it only where the forward
+//      sweep replaced the vector, those positions listed by the forward sweep), and the test of
+//      v[q-1] at every q: end[q-1] = q where it refuses, the others queued;
+//   2. the queued candidates extended one position per stage (BM_STAGES stages, the survivors
+//      compacted after each), then the rest by groups of 8 lanes testing 8 positions at once;
+//   3. the chain of run starts 0, end[0], end[end[0]], ... in 32-position chunks, one warp per
+//      chunk: the successor tables doubled by shuffles give every position's first chain element
+//      past the chunk; one thread walks the chunks from position 0 (their entries and the last start
+//      before each);
+//   4. the owner of every position (the last start at or before it, by binary lifting over the
+//      doubled tables from the chunk's entry), and v[owner] into the line.
+// Every cost is Block::cost bit for bit, so the result equals the sequential sweep. The in place
+// update is safe: step 4 reads only run starts, which keep their own vectors.
 template <bool COLS>
-__device__ void bm_sweep(float* su, float* sv, float* c0, const float* s_a, int* jmp, int* jmp2, int* on, int* wscan,
-                         int* chg, const float* __restrict__ B, int w, int h, int fixed, int len, bool reverse) {
-    const float w1 = (float)(w - 1), h1 = (float)(h - 1);
-    const int tid = threadIdx.x, nt = blockDim.x;
+__device__ void bm_sweep(float* su, float* sv, float* c0, const float* s_a, int* endp, int* qa, int* qb, int* ctl,
+                         int* entry, int* prevl, const float* __restrict__ B, int w, int h, int fixed, int len,
+                         bool reverse) {
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     auto line_of = [&](int q) -> int { return reverse ? len - 1 - q : q; };  // sweep position -> line index
-    int* queue = jmp2;  // steps 2-3; jmp2 is free until the pointer jumping
-    int* qn = wscan + 32;
-    // 1. c0 (NaN where no step can happen); the reverse sweep computes it only where the forward
-    //    sweep changed the vector, those positions first compacted into jmp (free until step 2) so
-    //    that every lane of a warp evaluates one
-    auto c0_at = [&](int i) {
-        float c = __int_as_float(0x7fc00000);
-        if (i >= 1 && i <= len - 2) {
-            int x = COLS ? fixed : i, y = COLS ? i : fixed;
-            float tx = (float)x - su[i];
-            float ty = (float)y - sv[i];
-            if (0.0f <= tx && tx <= w1 && 0.0f <= ty && ty <= h1) {
+    // 1. the reverse sweep's costs of the replaced vectors (qa holds their line indices, ctl[3] their count)
+    if (reverse) {
+        const int n = ctl[3];
+        for (int k = tid; k < n; k += nt) {
+            const int i = qa[k];
+            float p[9];
+            bm_patch<COLS>(s_a, len, i, p);
+            c0[i] = bm_own_cost<COLS>(p, B, w, h, fixed, i, su[i], sv[i]);
+        }
+        __syncthreads();
+    }
+    //    the test of v[q-1] at q (candidate j = q - 1), the forward sweep computing c0 on the way
+    for (int qb0 = 0; qb0 < len; qb0 += nt) {
+        const int q = qb0 + tid, j = q - 1;
+        bool more = false;
+        if (q >= 1 && q < len) {
+            if (q <= len - 2) {
+                const int i = line_of(q), jl = line_of(j);
                 float p[9];
                 bm_patch<COLS>(s_a, len, i, p);
-                float cost;
-                if (bm_cost<COLS>(B, w, h, p, tx, ty, cost)) c = cost;
+                float ci;
+                if (!reverse) {
+                    ci = bm_own_cost<COLS>(p, B, w, h, fixed, i, su[i], sv[i]);
+                    c0[i] = ci;
+                } else {
+                    ci = c0[i];
+                }
+                if (!bm_accept_p<COLS>(p, B, w, h, fixed, i, su[jl], sv[jl], ci)) endp[j] = q;
+                else if (q + 1 <= len - 2) more = true;
+                else endp[j] = len - 1;
+            } else {
+                endp[j] = len - 1;  // j = len - 2: no position left to test
             }
         }
-        c0[i] = c;
-    };
-    if (!reverse) {
-        for (int i = tid; i < len; i += nt) {
-            on[i] = 0;
-            c0_at(i);
-        }
-    } else {
-        int* list = jmp;
-        int* ln = wscan + 33;
-        if (tid == 0) *ln = 0;
-        __syncthreads();
-        for (int ib = 0; ib < len; ib += nt) {
-            int i = ib + tid;
-            bool want = false;
-            if (i < len) {
-                on[i] = 0;
-                want = chg[i] != 0;
-            }
-            unsigned m = __ballot_sync(0xffffffffu, want);
-            if (m) {
-                int lane = tid & 31, lead = __ffs(m) - 1;
-                int base = 0;
-                if (lane == lead) base = atomicAdd(ln, __popc(m));
-                base = __shfl_sync(0xffffffffu, base, lead);
-                if (want) list[base + __popc(m & ((1u << lane) - 1u))] = i;
-            }
-        }
-        __syncthreads();
-        const int n = *ln;
-        for (int k = tid; k < n; k += nt) c0_at(list[k]);
+        bm_push(qa, ctl + 0, more, j);
     }
-    if (tid == 0) *qn = 0;
     __syncthreads();
-    // 2. end[q] = q + 1 where the next position refuses v[q]; the others go to the queue
-    for (int qb = 0; qb < len; qb += nt) {
-        int q = qb + tid;
-        bool pend = false;
+    // 2. stage t tests position j + t + 2 of every queued candidate j (counters rotate over ctl[0..2]:
+    //    stage t reads ctl[t % 3], appends to ctl[(t + 1) % 3] and clears ctl[(t + 2) % 3], whose last
+    //    reader passed the barrier before this stage)
+    int nq = ctl[0];
+    int* cur = qa;
+    int* nxt = qb;
+    int t = 0;
+    for (; t < BM_STAGES && nq > 0; t++) {
+        if (tid == 0) ctl[(t + 2) % 3] = 0;
+        const int step = t + 2;
+        for (int kb = 0; kb < nq; kb += nt) {
+            const int k = kb + tid;
+            bool more = false;
+            int j = 0;
+            if (k < nq) {
+                j = cur[k];
+                const int qq = j + step;  // <= len - 2: a candidate is queued only with a position left
+                const int jl = line_of(j), il = line_of(qq);
+                if (!bm_accept<COLS>(s_a, len, B, w, h, fixed, il, su[jl], sv[jl], c0[il])) endp[j] = qq;
+                else if (qq + 1 > len - 2) endp[j] = len - 1;
+                else more = true;
+            }
+            bm_push(nxt, ctl + (t + 1) % 3, more, j);
+        }
+        __syncthreads();
+        nq = ctl[(t + 1) % 3];
+        int* sw = cur;
+        cur = nxt;
+        nxt = sw;
+    }
+    //    the long runs: a group of 8 lanes per candidate, 8 positions per test round
+    if (nq > 0) {
+        const int g = lane >> 3, sub = lane & 7, step = BM_STAGES + 2;
+        for (int kb = warp * 4; kb < nq; kb += nw * 4) {
+            const int k = kb + g;
+            bool live = k < nq;
+            const int j = live ? cur[k] : 0;
+            const int jl = line_of(j);
+            const float nu = live ? su[jl] : 0.0f, nv = live ? sv[jl] : 0.0f;
+            int pos = j + step;
+            for (int guard = 0; guard <= len && __any_sync(FULL, live); guard += 8) {
+                const int qq = pos + sub;
+                bool refuse = false;
+                if (live && qq <= len - 2) {
+                    const int il = line_of(qq);
+                    refuse = !bm_accept<COLS>(s_a, len, B, w, h, fixed, il, nu, nv, c0[il]);
+                }
+                const unsigned gm = (__ballot_sync(FULL, refuse) >> (g * 8)) & 0xffu;
+                if (live) {
+                    if (gm) {
+                        if (sub == 0) endp[j] = pos + __ffs(gm) - 1;
+                        live = false;
+                    } else if (pos + 8 > len - 2) {
+                        if (sub == 0) endp[j] = len - 1;
+                        live = false;
+                    } else {
+                        pos += 8;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // 3. per chunk: J = the successor (end) doubled five times, L = the last start inside the chunk on
+    //    the way; the queues are free now and take the two tables
+    const int nch = (len + 31) >> 5;
+    int* exitq = qa;
+    int* lastq = qb;
+    for (int c = warp; c < nch; c += nw) {
+        const int base = c << 5, q = base + lane;
+        int J = q <= len - 2 ? endp[q] : BM_TERM;
+        int L = q;
+#pragma unroll
+        for (int r = 0; r < 5; r++) {
+            const int src = J - base;  // > 0: a successor lies past its position
+            const int tJ = __shfl_sync(FULL, J, src & 31);
+            const int tL = __shfl_sync(FULL, L, src & 31);
+            if (src < 32) {
+                J = tJ;
+                L = tL;
+            }
+        }
         if (q < len) {
-            int e = len - 1;
-            if (q + 1 <= len - 2) {
-                int j = line_of(q), i1 = line_of(q + 1);
-                if (bm_accept<COLS>(s_a, len, B, w, h, fixed, i1, su[j], sv[j], c0[i1])) pend = true;
-                else e = q + 1;
+            exitq[q] = J;
+            lastq[q] = L;
+        }
+    }
+    __syncthreads();
+    //    the walk over the chunks from position 0: entry[c] = the first start in chunk c (-1: none),
+    //    prevl[c] = the last start before it
+    if (tid == 0) {
+        int E = 0, Lp = -1, k = 0;
+        for (int guard = 0; guard < len; guard++) {
+            const int kE = E >> 5;
+            for (; k < kE; k++) {
+                entry[k] = -1;
+                prevl[k] = Lp;
             }
-            if (!pend) jmp[q] = e;
+            entry[kE] = E;
+            prevl[kE] = Lp;
+            k = kE + 1;
+            Lp = lastq[E];
+            const int F = exitq[E];
+            if (F >= len - 1) break;  // the line's last position, or past it: no start to follow
+            E = F;
         }
-        unsigned m = __ballot_sync(0xffffffffu, pend);
-        if (m) {
-            int lane = tid & 31, lead = __ffs(m) - 1;
-            int base = 0;
-            if (lane == lead) base = atomicAdd(qn, __popc(m));
-            base = __shfl_sync(0xffffffffu, base, lead);
-            if (pend) queue[base + __popc(m & ((1u << lane) - 1u))] = q;
+        for (; k < nch; k++) {
+            entry[k] = -1;
+            prevl[k] = Lp;
         }
+        ctl[0] = ctl[1] = ctl[2] = ctl[3] = 0;  // the next sweep's counters and the list of replaced positions
     }
     __syncthreads();
-    // 3. the queued candidates: the first refusal from q + 2 on (len - 1 when the run reaches the end)
-    const int nq = *qn;
-    for (int k = tid; k < nq; k += nt) {
-        int q = queue[k];
-        int j = line_of(q);
-        float nu = su[j], nv = sv[j];
-        int e = len - 1;
-        for (int q0 = q + 2; q0 <= len - 2; q0 += BM_WINDOW) {
-            bool acc[BM_WINDOW];
+    // 4. owners by binary lifting from the chunk's entry over the doubled tables Jr[r] (2^r successors,
+    //    saturated at the chunk's end), then the scatter; the forward sweep lists the replaced
+    //    positions for the reverse sweep's costs
+    for (int c = warp; c < nch; c += nw) {
+        const int base = c << 5, q = base + lane;
+        int Jr[5];
+        Jr[0] = q <= len - 2 ? endp[q] : BM_TERM;
 #pragma unroll
-            for (int d = 0; d < BM_WINDOW; d++) {
-                int qq = q0 + d;
-                acc[d] = qq <= len - 2 && bm_accept<COLS>(s_a, len, B, w, h, fixed, line_of(qq), nu, nv, c0[line_of(qq)]);
+        for (int r = 1; r < 5; r++) {
+            const int src = Jr[r - 1] - base;
+            const int tv = __shfl_sync(FULL, Jr[r - 1], src & 31);
+            Jr[r] = src < 32 ? tv : Jr[r - 1];
+        }
+        const int e = entry[c];
+        int own = prevl[c];
+        if (e >= 0) {  // the same for the whole warp
+            int x = e;
+#pragma unroll
+            for (int r = 4; r >= 0; r--) {
+                const int y = __shfl_sync(FULL, Jr[r], (x - base) & 31);
+                if (y <= q) x = y;
             }
-            int stop = -1;
-#pragma unroll
-            for (int d = BM_WINDOW - 1; d >= 0; d--)
-                if (!acc[d] && q0 + d <= len - 2) stop = q0 + d;
-            if (stop >= 0) { e = stop; break; }
+            if (q >= e) own = x;
         }
-        jmp[q] = e;
-    }
-    __syncthreads();
-    // 4. the chain of run starts from sweep position 0, by pointer jumping: after round r every
-    //    start within 2^(r+1) hops of position 0 is marked (jmp holds next^(2^r))
-    if (tid == 0) on[0] = 1;
-    __syncthreads();
-    for (int span = 1; span < 2 * len; span *= 2) {
-        for (int q = tid; q < len; q += nt)
-            if (on[q] && jmp[q] < len - 1) on[jmp[q]] = 1;
-        for (int q = tid; q < len; q += nt) jmp2[q] = jmp[q] < len - 1 ? jmp[jmp[q]] : jmp[q];
-        __syncthreads();
-        int* t = jmp;
-        jmp = jmp2;
-        jmp2 = t;
-    }
-    //    owner of each position: the last marked start at or before it (a block-wide max scan over
-    //    contiguous chunks), then v[owner] into the line
-    int chunk = (len + nt - 1) / nt;
-    int lo = tid * chunk, hi = min(lo + chunk, len);
-    int mark = -1;
-    for (int q = lo; q < hi; q++)
-        if (on[q]) mark = q;
-    int lane = tid & 31, warp = tid >> 5;
-    int v = mark;
-#pragma unroll
-    for (int o = 1; o < 32; o *= 2) {
-        int t = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v = max(v, t);
-    }
-    if (lane == 31) wscan[warp] = v;
-    __syncthreads();
-    int before = -1;  // the max over all previous warps
-    for (int k = 0; k < warp; k++) before = max(before, wscan[k]);
-    int excl = __shfl_up_sync(0xffffffffu, v, 1);
-    if (lane == 0) excl = -1;
-    int cur = max(before, excl);  // the last start before this thread's chunk
-    for (int q = lo; q < hi; q++) {
-        if (on[q]) cur = q;
-        int i = line_of(q);
-        bool moved = i >= 1 && i <= len - 2 && cur >= 0 && cur != q;
+        const bool moved = q >= 1 && q <= len - 2 && own != q;
+        const int i = line_of(q);
         if (moved) {
-            int o = line_of(cur);
+            const int o = line_of(own);
             su[i] = su[o];
             sv[i] = sv[o];
         }
-        if (!reverse) chg[i] = moved ? 1 : 0;
+        if (!reverse) bm_push(qa, ctl + 3, moved, i);
     }
     __syncthreads();
 }
 
 // The two sweeps of a line (flow.rs:551-622: left to right then right to left, or top to bottom
-// then bottom to top), with the field, A's three lines and the chain in shared memory; the field
+// then bottom to top), with the field, A's three lines and the tables in shared memory; the field
 // goes to global memory once, after both. Column sweeps take TRANSPOSED planes (A, B and the field
 // stored column by column, element (x, y) at [x * h + y]) so that a warp's lanes, which walk down
 // one column, read contiguous memory; the reference transposes its field for the same sweeps
@@ -594,14 +675,18 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
                         float* __restrict__ fv, int w, int h, int fixed) {
     extern __shared__ float sm[];
     const int len = COLS ? h : w;
+    if (len < 3) return;  // no interior position
+    const int nch = (len + 31) >> 5;
     float* su = sm;
     float* sv = su + len;
     float* c0 = sv + len;
-    float* s_a = c0 + len;             // 3 * len
-    int* jmp = (int*)(s_a + 3 * len);  // next^(2^r), ping-ponged with jmp2
-    int* jmp2 = jmp + len;
-    int* on = jmp2 + len;
-    int* wscan = on + len;  // one int per warp, then the queue counter
+    float* s_a = c0 + len;  // 3 * len
+    int* endp = (int*)(s_a + 3 * len);
+    int* qa = endp + len;
+    int* qb = qa + len;
+    int* ctl = qb + len;  // 8 counters
+    int* entry = ctl + 8;
+    int* prevl = entry + nch;
     // both layouts keep the line contiguous: row y of a row-major plane, column x of a transposed one
     auto gidx = [&](int i) -> long { return (long)fixed * len + i; };
     for (int i = threadIdx.x; i < len; i += blockDim.x) {
@@ -612,11 +697,10 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
         for (int o = 0; o < 3; o++)  // A at offset o-1 across the line: rows y-1..y+1, or columns x-1..x+1
             s_a[o * len + i] = __ldg(A + (long)(fixed - 1 + o) * len + i);
     }
+    if (threadIdx.x < 8) ctl[threadIdx.x] = 0;
     __syncthreads();
-    // chg (which positions the forward sweep replaced) lives in jmp2 between the two sweeps: the
-    // reverse sweep reads it in its step 1, before its step 2 reuses jmp2 as the queue
-    bm_sweep<COLS>(su, sv, c0, s_a, jmp, jmp2, on, wscan, jmp2, B, w, h, fixed, len, false);
-    bm_sweep<COLS>(su, sv, c0, s_a, jmp, jmp2, on, wscan, jmp2, B, w, h, fixed, len, true);
+    bm_sweep<COLS>(su, sv, c0, s_a, endp, qa, qb, ctl, entry, prevl, B, w, h, fixed, len, false);
+    bm_sweep<COLS>(su, sv, c0, s_a, endp, qa, qb, ctl, entry, prevl, B, w, h, fixed, len, true);
     for (int i = threadIdx.x + 1; i <= len - 2; i += blockDim.x) {
         long g = gidx(i);
         fu[g] = su[i];
