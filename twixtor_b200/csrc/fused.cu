@@ -104,12 +104,18 @@ __global__ void __launch_bounds__(FT_THREADS) k_blur5_band(const float* __restri
 // ---- one solver level: gradient, tensor and its blur (flow.rs:1275-1277) ---------------------------
 
 // mask (may be null): the level mask of X of a layered solve; the gradient is zero where the mask
-// is below 0.95 at the pixel or at one of its four neighbours that exist (flow.rs:743-761)
+// is below 0.95 at the pixel or at one of its four neighbours that exist (flow.rs:743-761).
+// b_out (may be null): calc_b of the first iteration from the level's flow fu, fv, the image i0 and
+// the mask of Y (flow.rs:334-357), into two planes of pitch bp (plane stride bplane).
 __global__ void __launch_bounds__(FT_THREADS) k_level_init(const float* __restrict__ img, int w, int h, Taps g7,
                                                            bool above_first, float* __restrict__ gxo,
                                                            float* __restrict__ gyo, float* __restrict__ a0o,
                                                            float* __restrict__ a1o, float* __restrict__ a2o,
-                                                           const float* __restrict__ mask) {
+                                                           const float* __restrict__ mask,
+                                                           const float* __restrict__ fu, const float* __restrict__ fv,
+                                                           const float* __restrict__ i0,
+                                                           const float* __restrict__ mask_y, float* __restrict__ b_out,
+                                                           int bp, long bplane) {
     constexpr int N = 8, HALO = N - 1;
     constexpr int RW = FT_X + 2 * HALO, RH = FT_Y + 2 * HALO;
     extern __shared__ float sm[];
@@ -144,6 +150,12 @@ __global__ void __launch_bounds__(FT_THREADS) k_level_init(const float* __restri
             if (x >= X0 && x < X0 + FT_X && y >= Y0 && y < Y0 + FT_Y) {
                 gxo[i] = gx;
                 gyo[i] = gy;
+                if (b_out) {  // calc_b of the level's first iteration
+                    float b0, b1;
+                    calc_b_at(i0, mask_y, w, h, x, y, __ldg(fu + i), __ldg(fv + i), cc, gx, gy, b0, b1);
+                    b_out[(long)y * bp + x] = b0;
+                    b_out[bplane + (long)y * bp + x] = b1;
+                }
             }
         }
         s_t[e] = t0;
@@ -177,6 +189,11 @@ size_t level_init_smem() {
 // ---- one solver iteration (flow.rs:1278-1282): calc_b, blur7 of B, new_disp, blur5 of the flow -----
 // mask_y (may be null): the level mask of Y of a layered solve
 //
+// calc_b depends only on the flow at its own pixel, so it is computed once per pixel where the flow
+// is made: k_level_init for the level's first iteration, each iteration's epilogue for the next one
+// (k_calc_b_pitched after the level's block matching). B lives in two planes with a pitch of a
+// multiple of 4 floats, so that an iteration loads its B region with 128-bit loads.
+//
 // Halos: the flow's blur5 needs new_disp on the tile + 5; new_disp needs blurred B there, which
 // needs B on the tile + 12. The tile is TX x TY outputs (a template: the host picks the shape per
 // level size from its tuning table). The separable passes are register blocked: a thread computes R
@@ -195,12 +212,13 @@ struct IterGeom {
     static constexpr int HS = DW | 1;
     static constexpr int DS = DW | 1;
     static constexpr int FS = TX | 1;
-    // buffer 1: B (2 planes BH x BS), later the blurred B / new flow (2 planes DH x DS)
+    // buffer 1: B (2 planes BH x BS), later the blurred B / new flow (2 planes DH x DS), last the
+    // tile's new flow (2 planes TY x TX)
     // buffer 2: the horizontal pass of B (2 planes BH x HS), later of the flow (2 planes DH x FS)
     static constexpr int BUF1 = 2 * BH * BS;
     static constexpr int BUF2 = 2 * BH * HS;
     static constexpr size_t SMEM = sizeof(float) * (BUF1 + BUF2);
-    static_assert(2 * DH * DS <= BUF1 && 2 * DH * FS <= BUF2, "the reused buffers must fit");
+    static_assert(2 * DH * DS <= BUF1 && 2 * DH * FS <= BUF2 && 2 * TX * TY <= BUF1, "the reused buffers must fit");
 };
 
 // R outputs of a pass along one line at line indices i0 .. i0 + R - 1 (global), written to
@@ -235,13 +253,15 @@ __device__ __forceinline__ void pass_run(const float* line, int origin, int rlen
 }
 
 template <int TX, int TY>
-__device__ __forceinline__ void level_iter_body(const float* __restrict__ i1, const float* __restrict__ i0,
+__device__ __forceinline__ void level_iter_body(const float* __restrict__ b_in, int bp, long bplane,
+                                                const float* __restrict__ i1, const float* __restrict__ i0,
                                                 const float* __restrict__ gx, const float* __restrict__ gy,
                                                 const float* __restrict__ a0, const float* __restrict__ a1,
                                                 const float* __restrict__ a2, const float* __restrict__ fu,
                                                 const float* __restrict__ fv, int w, int h, const Taps& g7,
                                                 const Taps& g5, bool above_first, float* __restrict__ fu_out,
-                                                float* __restrict__ fv_out, const float* __restrict__ mask_y) {
+                                                float* __restrict__ fv_out, const float* __restrict__ mask_y,
+                                                float* __restrict__ b_out) {
     using G = IterGeom<TX, TY>;
     constexpr int R7 = 6, R5 = 8;  // outputs per thread of the blur7 and blur5 passes
     extern __shared__ float sm[];
@@ -252,46 +272,43 @@ __device__ __forceinline__ void level_iter_body(const float* __restrict__ i1, co
     const int X0 = blockIdx.x * TX, Y0 = blockIdx.y * TY;
     const int bx0 = X0 - G::HB, by0 = Y0 - G::HB;
     const int dx0 = X0 - G::HD, dy0 = Y0 - G::HD;
-    const float fw = (float)w, fh = (float)h;
     const int nt = blockDim.x;
-    // 1. B = calc_b over the B region (flow.rs:334-357), two elements per thread and round so that
-    //    the loads of both are in flight together
-    constexpr int NB = G::BW * G::BH;
-    for (int e0 = threadIdx.x; e0 < NB; e0 += 2 * nt) {
-        float sx[2], sy[2], i1v[2], gxv[2], gyv[2];
-        bool in[2];
+    // 1. B over the B region, from the planes b_in (calc_b of flow.rs:334-357, computed once per pixel
+    //    by the kernel that produced the flow): 128-bit loads of 4 columns (bx0 and the pitch are
+    //    multiples of 4, the planes 16-byte aligned), zero outside the level as calc_b gives there;
+    //    four loads per thread in flight before their stores
+    {
+        constexpr int Q = G::BW / 4;  // 128-bit groups per region row
+        constexpr int NQ = 2 * G::BH * Q;
+        static_assert(G::BW % 4 == 0 && G::HB % 4 == 0, "the B region must start and end on 4-column groups");
+        for (int e0 = threadIdx.x; e0 < NQ; e0 += 4 * nt) {
+            float4 v[4];
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
-            int e = e0 + k * nt;
-            int r = e / G::BW, c = e - r * G::BW;
-            int x = bx0 + c, y = by0 + r;
-            in[k] = e < NB && x >= 0 && x < w && y >= 0 && y < h;
-            sx[k] = sy[k] = i1v[k] = gxv[k] = gyv[k] = 0.0f;
-            if (in[k]) {
-                int i = y * w + x;
-                sx[k] = (float)x - __ldg(fu + i);
-                sy[k] = (float)y - __ldg(fv + i);
-                i1v[k] = __ldg(i1 + i);
-                gxv[k] = __ldg(gx + i);
-                gyv[k] = __ldg(gy + i);
+            for (int k = 0; k < 4; k++) {
+                const int e = e0 + k * nt;
+                const int q = e % Q, rest = e / Q;
+                const int r = rest % G::BH, ch = rest / G::BH;
+                const int x = bx0 + 4 * q, y = by0 + r;
+                v[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (e < NQ && x >= 0 && x < w && y >= 0 && y < h) {
+                    v[k] = __ldg(reinterpret_cast<const float4*>(b_in + ch * bplane + (long)y * bp + x));
+                    if (x + 1 >= w) v[k].y = 0.0f;  // the pitch's padding columns
+                    if (x + 2 >= w) v[k].z = 0.0f;
+                    if (x + 3 >= w) v[k].w = 0.0f;
+                }
             }
-        }
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
-            int e = e0 + k * nt;
-            if (e >= NB) break;
-            float b0 = 0.0f, b1 = 0.0f;
-            // flow.rs:777-845: in a layered solve the warped mask of Y must be at least 0.999
-            if (in[k] && !(sx[k] < 0.0f || fw - 1.0f < sx[k] || sy[k] < 0.0f || fh - 1.0f < sy[k]) &&
-                (!mask_y || bilinear1(mask_y, w, h, sx[k], sy[k]) >= 0.999f)) {
-                float sv = bilinear1(i0, w, h, sx[k], sy[k]);
-                float rr = sv - i1v[k];
-                b0 = rr * gxv[k];
-                b1 = rr * gyv[k];
+            for (int k = 0; k < 4; k++) {
+                const int e = e0 + k * nt;
+                if (e >= NQ) break;
+                const int q = e % Q, rest = e / Q;
+                const int r = rest % G::BH, ch = rest / G::BH;
+                float* d = s_b + ch * G::BH * G::BS + r * G::BS + 4 * q;
+                d[0] = v[k].x;
+                d[1] = v[k].y;
+                d[2] = v[k].z;
+                d[3] = v[k].w;
             }
-            int r = e / G::BW, c = e - r * G::BW;
-            s_b[r * G::BS + c] = b0;
-            s_b[G::BH * G::BS + r * G::BS + c] = b1;
         }
     }
     __syncthreads();
@@ -327,7 +344,9 @@ __device__ __forceinline__ void level_iter_body(const float* __restrict__ i1, co
         }
     }
     __syncthreads();
-    // 3. new_disp over the new_disp region (flow.rs:361-371), in place on the blurred B
+    // 3. new_disp over the new_disp region (flow.rs:361-371), in place on the blurred B (one element
+    //    per thread and round: batching more raises the registers past three blocks per SM, which
+    //    costs more when several solves share the GPU than the batching gains)
     for (int e = threadIdx.x; e < G::DW * G::DH; e += nt) {
         int r = e / G::DW, c = e - r * G::DW;
         int x = dx0 + c, y = dy0 + r;
@@ -361,6 +380,9 @@ __device__ __forceinline__ void level_iter_body(const float* __restrict__ i1, co
         }
     }
     __syncthreads();
+    //    vertical at the tile rows, into the tile buffer (buffer 1: its new_disp region was read by the
+    //    horizontal pass)
+    float* s_o = s_b;  // 2 x TY x TX
     {
         constexpr int NSEG = (TY + R5 - 1) / R5;
         for (int e = threadIdx.x; e < 2 * TX * NSEG; e += nt) {
@@ -371,22 +393,68 @@ __device__ __forceinline__ void level_iter_body(const float* __restrict__ i1, co
             int r0 = seg * R5;
             const float* line = s_f + ch * G::DH * G::FS + c;
             int nv = min(R5, TY - r0);
-            float* dst = (ch == 0 ? fu_out : fv_out) + (Y0 + r0) * w + X;  // rows past h are never written
-            if (above_first) pass_run<6, R5, true, true>(line, dy0, G::DH, G::FS, h, Y0 + r0, g5.k, dst, w, nv);
-            else pass_run<6, R5, true, false>(line, dy0, G::DH, G::FS, h, Y0 + r0, g5.k, dst, w, nv);
+            float* dst = s_o + ch * TY * TX + r0 * TX + c;  // rows past h are never written
+            if (above_first) pass_run<6, R5, true, true>(line, dy0, G::DH, G::FS, h, Y0 + r0, g5.k, dst, TX, nv);
+            else pass_run<6, R5, true, false>(line, dy0, G::DH, G::FS, h, Y0 + r0, g5.k, dst, TX, nv);
+        }
+    }
+    __syncthreads();
+    // 5. the new flow to the planes; with b_out also calc_b of the next iteration at every pixel of the
+    //    tile (flow.rs:334-357), two pixels per thread and round with their loads in flight together
+    {
+        constexpr int K = 2;
+        for (int e0 = threadIdx.x; e0 < TX * TY; e0 += K * nt) {
+            float u[K], v[K], i1v[K], gxv[K], gyv[K];
+            bool in[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const int e = e0 + k * nt;
+                const int r = e / TX, c = e - r * TX;
+                const int x = X0 + c, y = Y0 + r;
+                in[k] = e < TX * TY && x < w && y < h;
+                u[k] = v[k] = i1v[k] = gxv[k] = gyv[k] = 0.0f;
+                if (in[k]) {
+                    const int i = y * w + x;
+                    u[k] = s_o[e];
+                    v[k] = s_o[TY * TX + e];
+                    fu_out[i] = u[k];
+                    fv_out[i] = v[k];
+                    if (b_out) {
+                        i1v[k] = __ldg(i1 + i);
+                        gxv[k] = __ldg(gx + i);
+                        gyv[k] = __ldg(gy + i);
+                    }
+                }
+            }
+            if (b_out) {
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    if (!in[k]) continue;
+                    const int e = e0 + k * nt;
+                    const int r = e / TX, c = e - r * TX;
+                    const int x = X0 + c, y = Y0 + r;
+                    float b0, b1;
+                    calc_b_at(i0, mask_y, w, h, x, y, u[k], v[k], i1v[k], gxv[k], gyv[k], b0, b1);
+                    b_out[(long)y * bp + x] = b0;
+                    b_out[bplane + (long)y * bp + x] = b1;
+                }
+            }
         }
     }
 }
 
+// The iteration reads B from b_in and, with b_out (same pitch bp and plane stride bplane), writes the
+// next iteration's B; b_in and b_out are different buffers (other tiles still read b_in's halo).
 #define TW_LEVEL_ITER(TX, TY)                                                                                         \
     __global__ void __launch_bounds__(LEVEL_ITER_MAX_THREADS) k_level_iter_##TX##x##TY(                              \
-        const float* __restrict__ i1, const float* __restrict__ i0, const float* __restrict__ gx,                    \
-        const float* __restrict__ gy, const float* __restrict__ a0, const float* __restrict__ a1,                    \
-        const float* __restrict__ a2, const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,      \
-        Taps g7, Taps g5, bool above_first, float* __restrict__ fu_out, float* __restrict__ fv_out,                 \
-        const float* __restrict__ mask_y) {                                                                          \
-        level_iter_body<TX, TY>(i1, i0, gx, gy, a0, a1, a2, fu, fv, w, h, g7, g5, above_first, fu_out, fv_out,     \
-                                mask_y);                                                                             \
+        const float* __restrict__ b_in, int bp, long bplane, const float* __restrict__ i1,                          \
+        const float* __restrict__ i0, const float* __restrict__ gx, const float* __restrict__ gy,                    \
+        const float* __restrict__ a0, const float* __restrict__ a1, const float* __restrict__ a2,                    \
+        const float* __restrict__ fu, const float* __restrict__ fv, int w, int h, Taps g7, Taps g5,                  \
+        bool above_first, float* __restrict__ fu_out, float* __restrict__ fv_out, const float* __restrict__ mask_y,  \
+        float* __restrict__ b_out) {                                                                                 \
+        level_iter_body<TX, TY>(b_in, bp, bplane, i1, i0, gx, gy, a0, a1, a2, fu, fv, w, h, g7, g5, above_first,    \
+                                fu_out, fv_out, mask_y, b_out);                                                      \
     }
 TW_LEVEL_ITER(32, 32)
 TW_LEVEL_ITER(64, 32)
@@ -399,6 +467,22 @@ size_t level_iter_smem(int tile) {
         case LEVEL_TILE_64x64: return IterGeom<64, 64>::SMEM;
         default: return IterGeom<32, 32>::SMEM;
     }
+}
+
+// calc_b (flow.rs:334-357) of the next iteration where the flow changed outside an iteration (after
+// the block matching and the user displacement of the finest level): one thread per pixel, into two
+// planes of pitch bp (plane stride bplane).
+__global__ void k_calc_b_pitched(const float* __restrict__ i1, const float* __restrict__ i0,
+                                 const float* __restrict__ gx, const float* __restrict__ gy,
+                                 const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,
+                                 const float* __restrict__ mask_y, float* __restrict__ b_out, int bp, long bplane) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const int i = y * w + x;
+    float b0, b1;
+    calc_b_at(i0, mask_y, w, h, x, y, __ldg(fu + i), __ldg(fv + i), __ldg(i1 + i), __ldg(gx + i), __ldg(gy + i), b0, b1);
+    b_out[(long)y * bp + x] = b0;
+    b_out[bplane + (long)y * bp + x] = b1;
 }
 
 // ---- the end of a level (flow.rs:1292-1303): range reset, damping, then the upsample ---------------

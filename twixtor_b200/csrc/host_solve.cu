@@ -110,25 +110,27 @@ void conv_planes(tw_ctx* ctx, float* const* planes, int c, int w, int h, const T
     }
 }
 
-// One solver iteration (k_level_iter_*) with the tile shape and block size of the level's choice.
-// Algorithmic bytes per pixel: I1, the I0 gather, the gradient (2), the tensor (3) and the flow (2)
-// read, the flow (2) written.
+// One solver iteration (k_level_iter_*) with the tile shape and block size of the level's choice:
+// B read from b_in; with b_out the next iteration's B written (planes of pitch bp, stride bplane).
+// Algorithmic bytes per pixel: B (2), the tensor (3) and the flow (2) read, the flow (2) written;
+// with b_out also I1, the I0 gather and the gradient (2) read and B (2) written.
 void level_iter(tw_ctx* ctx, LevelTune ic, const float* A, const float* B, const float* gx, const float* gy,
                 const float* a0, const float* a1, const float* a2, const float* fu, const float* fv, int w, int h, bool af,
-                float* nu, float* nv, const float* mask_y, bool fast) {
-    double b = 48.0 * w * h;
+                float* nu, float* nv, const float* mask_y, bool fast, const float* b_in, float* b_out, int bp,
+                long bplane) {
+    double b = (b_out ? 60.0 : 36.0) * w * h;
     size_t smem = level_iter_smem(ic.iter_tile);
     if (ic.iter_tile == LEVEL_TILE_64x64) {
         dim3 g((unsigned)((w + 63) / 64), (unsigned)((h + 63) / 64));
-        LAUNCHV(ctx, fast, b, k_level_iter_64x64, g, ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7, ctx->g5, af,
-                nu, nv, mask_y);
+        LAUNCHV(ctx, fast, b, k_level_iter_64x64, g, ic.iter_threads, smem, b_in, bp, bplane, A, B, gx, gy, a0, a1, a2, fu, fv, w,
+                h, ctx->g7, ctx->g5, af, nu, nv, mask_y, b_out);
     } else if (ic.iter_tile == LEVEL_TILE_64x32) {
         dim3 g((unsigned)((w + 63) / 64), (unsigned)((h + 31) / 32));
-        LAUNCHV(ctx, fast, b, k_level_iter_64x32, g, ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7, ctx->g5, af,
-                nu, nv, mask_y);
+        LAUNCHV(ctx, fast, b, k_level_iter_64x32, g, ic.iter_threads, smem, b_in, bp, bplane, A, B, gx, gy, a0, a1, a2, fu, fv, w,
+                h, ctx->g7, ctx->g5, af, nu, nv, mask_y, b_out);
     } else {
-        LAUNCHV(ctx, fast, b, k_level_iter_32x32, tiles(w, h), ic.iter_threads, smem, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, ctx->g7,
-                ctx->g5, af, nu, nv, mask_y);
+        LAUNCHV(ctx, fast, b, k_level_iter_32x32, tiles(w, h), ic.iter_threads, smem, b_in, bp, bplane, A, B, gx, gy, a0, a1, a2,
+                fu, fv, w, h, ctx->g7, ctx->g5, af, nu, nv, mask_y, b_out);
     }
 }
 
@@ -330,13 +332,17 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
                        const float* mx, const float* my, const float* udu,
                        const float* udv, const float* uww) {
     size_t np0 = (size_t)g.w * g.h;
-    // planes: gx gy a0 a1 a2 u0 v0 u1 v1 uT vT
+    // planes: gx gy a0 a1 a2 u0 v0 u1 v1 uT vT, then two B buffers of two planes each, 16-byte
+    // aligned, of pitch (w + 3) & ~3 at every level (plane stride bplane: the finest level's)
     const int NP = 11;
-    CHECK(ctx->ensure(work, np0 * NP * sizeof(float), "solve scratch"));
+    const size_t boff = (np0 * NP + 3) & ~(size_t)3;
+    const long bplane = (long)((g.w + 3) & ~3) * g.h;
+    CHECK(ctx->ensure(work, (boff + 4 * (size_t)bplane) * sizeof(float), "solve scratch"));
     float* base = work.as<float>();
     float *gx = base, *gy = base + np0, *a0 = base + 2 * np0, *a1 = base + 3 * np0, *a2 = base + 4 * np0;
     float *fu = base + 5 * np0, *fv = base + 6 * np0, *nu = base + 7 * np0, *nv = base + 8 * np0;
     float *ut = base + 9 * np0, *vt = base + 10 * np0;
+    float* bb[2] = {base + boff, base + boff + 2 * bplane};
     int start;
     float damp;
     start_level(s.sensitivity, g.levels, &start, &damp);
@@ -404,16 +410,23 @@ int solve_pyramids_dev(tw_ctx* ctx, const float* x, const float* y, const float*
         };
         user();
         LevelTune ic = level_tune(ctx, w, h);
-        LAUNCHV(ctx, fast, 24.0 * px, k_level_init, tiles(w, h), lt, level_init_smem(), A, w, h, ctx->g7, af, gx, gy, a0, a1, a2,
-                mask_x);
+        const int bp = (w + 3) & ~3;
+        // the image read, the gradient and the tensor written; the flow, I0 (gather) read and B written
+        LAUNCHV(ctx, fast, 44.0 * px, k_level_init, tiles(w, h), lt, level_init_smem(), A, w, h, ctx->g7, af, gx, gy, a0, a1, a2,
+                mask_x, fu, fv, B, mask_y, bb[0], bp, bplane);
         for (int it = 0; it < 3; it++) {
-            // I1, I0 (gather), grad, tensor, flow in; flow out
-            level_iter(ctx, ic, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, af, nu, nv, mask_y, fast);
+            // iteration it reads B from bb[it & 1]; the next one's B comes from its epilogue, or after
+            // the finest level's block matching from the pointwise pass
+            const bool emit = it == 0 || (it == 1 && l != 0);
+            level_iter(ctx, ic, A, B, gx, gy, a0, a1, a2, fu, fv, w, h, af, nu, nv, mask_y, fast, bb[it & 1],
+                       emit ? bb[(it + 1) & 1] : nullptr, bp, bplane);
             std::swap(fu, nu);
             std::swap(fv, nv);
             if (it == 1 && l == 0) {
                 if (!s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h, fast);
                 user();
+                LAUNCHV(ctx, fast, 32.0 * px, k_calc_b_pitched, grid2(w, h), TB, 0, A, B, gx, gy, fu, fv, w, h, mask_y, bb[0], bp,
+                        bplane);
             }
         }
         if (l != 0 && !s.skip_refine) block_match(ctx, A, B, AT, BT, fu, fv, ut, vt, w, h, fast);

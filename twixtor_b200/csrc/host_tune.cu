@@ -101,7 +101,10 @@ int tw_autotune(tw_ctx* ctx, const tw_flow_settings* s, int32_t width, int32_t h
         DevBuf buf;
         size_t held = 0;
         const int NP = 16;
-        cudaError_t e = buf.ensure(NP * n0 * sizeof(float), &held);
+        // and two B buffers (two planes each) of pitch (w + 3) & ~3, 16-byte aligned
+        const size_t boff = (NP * n0 + 3) & ~(size_t)3;
+        const long bplane = (long)((g.w + 3) & ~3) * g.h;
+        cudaError_t e = buf.ensure((boff + 4 * (size_t)bplane) * sizeof(float), &held);
         if (e != cudaSuccess) return ctx->cuda(e, "autotune buffers");
         float* p = buf.as<float>();
         float *A = p, *Bp = p + n0, *gx = p + 2 * n0, *gy = p + 3 * n0, *a0 = p + 4 * n0, *a1 = p + 5 * n0,
@@ -112,6 +115,10 @@ int tw_autotune(tw_ctx* ctx, const tw_flow_settings* s, int32_t width, int32_t h
             k_tune_fill<<<grid1((long)n0), TB, 0, ctx->stream>>>(p + i * n0, (long)n0, 0x9e3779b9u * (i + 1), amps[i]);
             ctx->launches++;
         }
+        float* bin = p + boff;
+        float* bout = bin + 2 * bplane;
+        k_tune_fill<<<grid1(2 * bplane), TB, 0, ctx->stream>>>(bin, 2 * bplane, 0x85ebca6bu, 50.f);
+        ctx->launches++;
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -139,7 +146,8 @@ int tw_autotune(tw_ctx* ctx, const tw_flow_settings* s, int32_t width, int32_t h
                                              {LEVEL_TILE_64x64, 512, 0, 0}};
             float bt = 1e30f;
             for (const LevelTune& c : iter_cands) {
-                float ms = timed([&] { level_iter(ctx, c, A, Bp, gx, gy, a0, a1, a2, fu, fv, w, h, af, nu, nv, nullptr); });
+                float ms = timed([&] { level_iter(ctx, c, A, Bp, gx, gy, a0, a1, a2, fu, fv, w, h, af, nu, nv, nullptr, false, bin, bout,
+                                                  (w + 3) & ~3, bplane); });
                 if (ms < bt) {
                     bt = ms;
                     best.iter_tile = c.iter_tile;

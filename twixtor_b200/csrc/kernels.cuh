@@ -142,20 +142,29 @@ __global__ void k_blur5_band(const float* __restrict__ orig, const void* __restr
                              float* __restrict__ band_t_out);
 __global__ void k_level_init(const float* __restrict__ img, int w, int h, Taps g7, bool above_first,
                              float* __restrict__ gxo, float* __restrict__ gyo, float* __restrict__ a0o,
-                             float* __restrict__ a1o, float* __restrict__ a2o, const float* __restrict__ mask);
+                             float* __restrict__ a1o, float* __restrict__ a2o, const float* __restrict__ mask,
+                             const float* __restrict__ fu, const float* __restrict__ fv, const float* __restrict__ i0,
+                             const float* __restrict__ mask_y, float* __restrict__ b_out, int bp, long bplane);
+__global__ void k_calc_b_pitched(const float* __restrict__ i1, const float* __restrict__ i0,
+                                 const float* __restrict__ gx, const float* __restrict__ gy,
+                                 const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,
+                                 const float* __restrict__ mask_y, float* __restrict__ b_out, int bp, long bplane);
 __global__ void k_binarize(float* __restrict__ p, long n);
 size_t level_init_smem();
-// One solver iteration (calc_b, blur7 of B, new_disp, blur5 of the flow) over TX x TY tiles: one
-// kernel per tile shape; the host picks the shape per level size (its tuning table).
+// One solver iteration (blur7 of B, new_disp, blur5 of the flow, then calc_b of the next iteration
+// at its outputs when b_out is given) over TX x TY tiles: one kernel per tile shape; the host picks
+// the shape per level size (its tuning table). B planes: pitch bp (a multiple of 4 floats), plane
+// stride bplane, 16-byte aligned.
 enum { LEVEL_TILE_32x32 = 0, LEVEL_TILE_64x32 = 1, LEVEL_TILE_64x64 = 2, LEVEL_TILE_COUNT = 3 };
 constexpr int LEVEL_ITER_MAX_THREADS = 512;
 #define TW_DECLARE_LEVEL_ITER(TX, TY)                                                                                 \
     __global__ void k_level_iter_##TX##x##TY(                                                                       \
-        const float* __restrict__ i1, const float* __restrict__ i0, const float* __restrict__ gx,                    \
-        const float* __restrict__ gy, const float* __restrict__ a0, const float* __restrict__ a1,                    \
-        const float* __restrict__ a2, const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,      \
-        Taps g7, Taps g5, bool above_first, float* __restrict__ fu_out, float* __restrict__ fv_out,                 \
-        const float* __restrict__ mask_y);
+        const float* __restrict__ b_in, int bp, long bplane, const float* __restrict__ i1,                          \
+        const float* __restrict__ i0, const float* __restrict__ gx, const float* __restrict__ gy,                    \
+        const float* __restrict__ a0, const float* __restrict__ a1, const float* __restrict__ a2,                    \
+        const float* __restrict__ fu, const float* __restrict__ fv, int w, int h, Taps g7, Taps g5,                  \
+        bool above_first, float* __restrict__ fu_out, float* __restrict__ fv_out, const float* __restrict__ mask_y,  \
+        float* __restrict__ b_out);
 TW_DECLARE_LEVEL_ITER(32, 32)
 TW_DECLARE_LEVEL_ITER(64, 32)
 TW_DECLARE_LEVEL_ITER(64, 64)

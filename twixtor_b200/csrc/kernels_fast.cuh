@@ -21,7 +21,13 @@ __global__ void k_blur5_band(const float* __restrict__ orig, const void* __restr
                              float* __restrict__ band_t_out);
 __global__ void k_level_init(const float* __restrict__ img, int w, int h, Taps g7, bool above_first,
                              float* __restrict__ gxo, float* __restrict__ gyo, float* __restrict__ a0o,
-                             float* __restrict__ a1o, float* __restrict__ a2o, const float* __restrict__ mask);
+                             float* __restrict__ a1o, float* __restrict__ a2o, const float* __restrict__ mask,
+                             const float* __restrict__ fu, const float* __restrict__ fv, const float* __restrict__ i0,
+                             const float* __restrict__ mask_y, float* __restrict__ b_out, int bp, long bplane);
+__global__ void k_calc_b_pitched(const float* __restrict__ i1, const float* __restrict__ i0,
+                                 const float* __restrict__ gx, const float* __restrict__ gy,
+                                 const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,
+                                 const float* __restrict__ mask_y, float* __restrict__ b_out, int bp, long bplane);
 __global__ void k_apply_upsample(const float* __restrict__ su, const float* __restrict__ sv, int sw, int sh,
                                  const int* __restrict__ any, int l, int start, bool damp_now, float damp,
                                  float* __restrict__ du, float* __restrict__ dv, int dw, int dh);
@@ -31,11 +37,12 @@ __global__ void k_apply_negate(const float* __restrict__ fu, const float* __rest
 __global__ void k_solve_coarse(CoarseJob job);
 #define TW_DECLARE_LEVEL_ITER(TX, TY)                                                                                 \
     __global__ void k_level_iter_##TX##x##TY(                                                                       \
-        const float* __restrict__ i1, const float* __restrict__ i0, const float* __restrict__ gx,                    \
-        const float* __restrict__ gy, const float* __restrict__ a0, const float* __restrict__ a1,                    \
-        const float* __restrict__ a2, const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,      \
-        Taps g7, Taps g5, bool above_first, float* __restrict__ fu_out, float* __restrict__ fv_out,                 \
-        const float* __restrict__ mask_y);
+        const float* __restrict__ b_in, int bp, long bplane, const float* __restrict__ i1,                          \
+        const float* __restrict__ i0, const float* __restrict__ gx, const float* __restrict__ gy,                    \
+        const float* __restrict__ a0, const float* __restrict__ a1, const float* __restrict__ a2,                    \
+        const float* __restrict__ fu, const float* __restrict__ fv, int w, int h, Taps g7, Taps g5,                  \
+        bool above_first, float* __restrict__ fu_out, float* __restrict__ fv_out, const float* __restrict__ mask_y,  \
+        float* __restrict__ b_out);
 TW_DECLARE_LEVEL_ITER(32, 32)
 TW_DECLARE_LEVEL_ITER(64, 32)
 TW_DECLARE_LEVEL_ITER(64, 64)

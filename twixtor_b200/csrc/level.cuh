@@ -106,6 +106,23 @@ __device__ __forceinline__ bool bm_cost(const float* __restrict__ B, int w, int 
     return true;
 }
 
+// flow.rs:334-357 (calc_b) at pixel (x, y) whose flow is (u, v): B = (I0(x - u, y - v) - I1) * grad,
+// zero where the source point leaves the level, and in a layered solve (mask_y) where the warped
+// mask of Y is below 0.999 (flow.rs:777-845). i1v, gxv, gyv: I1 and the gradient at the pixel.
+__device__ __forceinline__ void calc_b_at(const float* __restrict__ i0, const float* __restrict__ mask_y, int w, int h,
+                                          int x, int y, float u, float v, float i1v, float gxv, float gyv, float& b0,
+                                          float& b1) {
+    const float sx = (float)x - u, sy = (float)y - v;
+    b0 = 0.0f;
+    b1 = 0.0f;
+    if (!(sx < 0.0f || (float)w - 1.0f < sx || sy < 0.0f || (float)h - 1.0f < sy) &&
+        (!mask_y || bilinear1(mask_y, w, h, sx, sy) >= 0.999f)) {
+        const float rr = bilinear1(i0, w, h, sx, sy) - i1v;
+        b0 = rr * gxv;
+        b1 = rr * gyv;
+    }
+}
+
 // any[k] (k = level) is set when some pixel of level k is in range after its refinement.
 // check at level l = no level processed before (start .. l+1) had a pixel in range.
 __device__ __forceinline__ bool zero_at_level(const int* any, int l, int start) {

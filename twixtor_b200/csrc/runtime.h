@@ -317,7 +317,8 @@ void block_match(tw_ctx* ctx, const float* A, const float* B, const float* AT, c
                  float* uT, float* vT, int w, int h, bool fast = false);
 void level_iter(tw_ctx* ctx, LevelTune ic, const float* A, const float* B, const float* gx, const float* gy,
                 const float* a0, const float* a1, const float* a2, const float* fu, const float* fv, int w, int h, bool af,
-                float* nu, float* nv, const float* mask_y, bool fast = false);
+                float* nu, float* nv, const float* mask_y, bool fast, const float* b_in, float* b_out, int bp,
+                long bplane);
 size_t pyramid_floats(const Geo& g);
 int build_pyramid_dev(tw_ctx* ctx, const void* eng_dev, int W, int H, int fmt, const tw_flow_settings& s, const Geo& g,
                       float* out, float* out_t, DevBuf* scratch);
