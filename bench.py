@@ -358,14 +358,22 @@ def run_adjoint(args):
     stream = torch.cuda.current_stream()
     dev = tw.Device(0)
     dev.set_stream(stream.cuda_stream)
-    w, h, fw, fh, batch, distinct = 1280, 720, 640, 360, 64, 4
+    w, h, fw, fh, batch, base = 1280, 720, 640, 360, 64, 8
     if args.ncu_case:  # the profiling driver: one launch on 8 triples (0.7 GB on the device)
         batch = 8
-    A_, B_, M_, D_ = synth.adjoint_triples(w, h, distinct)
-    rep = lambda x: torch.from_numpy(x).cuda().repeat((batch // distinct,) + (1,) * (x.ndim - 1)).contiguous()  # noqa
-    a, b, m = rep(A_), rep(B_), rep(M_)
+    A_, B_, M_, D_ = synth.adjoint_triples(w, h, base)
     d_half = np.ascontiguousarray(D_[:, ::2, ::2, :] * np.float32(0.5))  # flow grid units (r ~ 0.5)
-    fab, fba = rep(d_half), rep(-d_half)
+    # 64 distinct triples: each generated triple (texture, displacement) and 7 copies rolled by an
+    # even pixel offset (the flows by half of it), the same shift for the three frames and the flows
+    shifts = [(0, 0)] + [(2 * ((97 * k) % (h // 2)), 2 * ((211 * k) % (w // 2))) for k in range(1, batch // base)]
+    def spread(x, flow):  # noqa: E306
+        t = torch.from_numpy(x).cuda()
+        out = [torch.roll(t, (dy // 2, dx // 2) if flow else (dy, dx), dims=(1, 2)) for dy, dx in shifts]
+        return torch.cat(out, 0).contiguous()
+    a, b, m = spread(A_, False), spread(B_, False), spread(M_, False)
+    fab, fba = spread(d_half, True), spread(-d_half, True)
+    wts = (torch.arange(a[0].numel(), device=a.device, dtype=torch.float64) % 1013) + 1.0
+    distinct = len({float((a[i].reshape(-1).double() * wts).sum()) for i in range(batch)})  # position weighted sums
     loss = torch.zeros(batch, device="cuda:0")
     da, db = torch.zeros_like(a), torch.zeros_like(b)
     dfab, dfba = torch.zeros_like(fab), torch.zeros_like(fba)
@@ -409,7 +417,8 @@ def run_adjoint(args):
           "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
           "dtype": "f32", "data": "synthetic",
           "config": {"workload": "64 triples of 1280x720 float RGBA, flows 640x360, wa 0.5, L1 against the middle frame",
-                     "batch": batch, "l2": "flushed between steps (256 MiB write); inputs 2.8 GB > L2"},
+                     "batch": batch, "distinct_triples": distinct,
+                     "l2": "flushed between steps (256 MiB write); inputs 2.8 GB > L2"},
           "e2e": {"value": args.steps * batch / (sum(etimes) / 1e3), "unit": "triples/s", "h2d_bytes_per_step": 0,
                   "d2h_bytes_per_step": 0, "note": "through the torch harness (device tensors)"},
           "gpu_launches": dev.stats()["kernel_launches"],

@@ -372,8 +372,9 @@ int tw_motion_blur(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw
 /* The adjoint of warp + blend (no reference counterpart: the differentiable twin of compose_vectors'
  * Blend with warping code 0, for photometric flow refinement). Forward: out = ta + (tb - ta) * w,
  * w = 1 - wa, ta = warp(a, f_ba, 1 - wa), tb = warp(b, f_ab, wa), warp(S, F, s)(p) = S sampled
- * bilinearly at p + F(p r) s / r (F sampled bilinearly at p r, r = (flow size - 1) / (image size -
- * 1) per axis, as warp.rs:693-786), the position clamped to the image. Backward: from grad_out
+ * bilinearly at p + F(p r) (s / r) (F sampled bilinearly at p r, r = (flow size - 1) / (image size -
+ * 1) per axis, the step s / r formed once as warp.rs:636-651 forms it), the position clamped to the
+ * image. Backward: from grad_out
  * (d loss / d out), or with target != NULL from the L1 loss sum |out - target| (its sum per batch
  * item added to loss[i]); the gradients are ADDED into da, db (w x h x 4), df_ab, df_ba (flow_w x
  * flow_h x 2), each NULL when not wanted; the forward output goes to out (NULL: not written).

@@ -28,7 +28,7 @@ def _footprint(x, n):
 
 def _side(S, F, w, h, fw, fh, amount, pos32=False):
     """S: (h, w, 4), F: (fh, fw, 2) float64; the sample of S and what its gradient needs. With
-    pos32 the sample positions (the flow's bilinear value and p + F s / r) are formed in single
+    pos32 the sample positions (the flow's bilinear value and p + F (s / r)) are formed in single
     precision in the kernel's order, so that a position within rounding of a pixel boundary falls
     in the same bilinear cell as on the device; values and gradients stay double."""
     # the kernel forms r in single precision; keep the same values
@@ -44,8 +44,11 @@ def _side(S, F, w, h, fw, fh, amount, pos32=False):
     fxx, fyy = ffx[..., None].astype(dt), ffy[..., None].astype(dt)
     one = dt(1.0)
     uv = (f00 + (f10 - f00) * fxx) * (one - fyy) + (f01 + (f11 - f01) * fxx) * fyy
-    px = (X + uv[..., 0] * dt(amount) / dt(rx32)).astype(np.float64)
-    py = (Y + uv[..., 1] * dt(amount) / dt(ry32)).astype(np.float64)
+    # the step per flow unit, amount / r, formed once as warp.rs forms sx, sy (single precision)
+    sx = dt(dt(amount) / dt(rx32)) if pos32 else amount / rx
+    sy = dt(dt(amount) / dt(ry32)) if pos32 else amount / ry
+    px = (X + uv[..., 0] * sx).astype(np.float64)
+    py = (Y + uv[..., 1] * sy).astype(np.float64)
     ffx, ffy = ffx.astype(np.float64), ffy.astype(np.float64)
     cx = ~((px >= 0) & (px <= w - 1))
     cy = ~((py >= 0) & (py <= h - 1))

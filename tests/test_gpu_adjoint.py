@@ -134,3 +134,49 @@ def test_refinement_beats_the_solver(dev):
     ref = adjoint.warp_blend(a, b, rab, rba, wa, dev)
     assert hist[-1] < hist[0]
     assert psnr(ref) > psnr(base) + 0.5
+
+
+def test_smooth_flows_match_fp64(dev):
+    """Smooth flows (the refinement workload's displacements): neighbouring samples share their
+    corners, so the scatter sums them in registers (carried down a column, handed to the next lane)
+    before the shared tile; the gradients still match the FP64 reference."""
+    w, h, fw, fh, n, wa = 160, 96, 80, 48, 2, 0.5
+    A_, B_, M_, D_ = synth.adjoint_triples(w, h, n, seed=5, peak=6.0)
+    d_half = np.ascontiguousarray(D_[:, ::2, ::2, :] * np.float32(0.5))
+    cu = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()  # noqa: E731
+    a, b, m, fab, fba = cu(A_), cu(B_), cu(M_), cu(d_half), cu(-d_half)
+    loss, da, db, dfab, dfba = adjoint.l1_loss_and_grads(dev, a, b, fab, fba, m, wa)
+    out = adjoint.warp_blend(a, b, fab, fba, wa, dev)
+    torch.cuda.synchronize()
+    for i in range(n):
+        args = [np.ascontiguousarray(x[i]).reshape(-1) for x in (A_, B_, d_half, -d_half)]
+        tt = M_[i].reshape(-1)
+        o32 = out[i].cpu().numpy().reshape(-1)
+        kw = dict(grad_out=np.sign(o32.astype(np.float64) - tt))
+        _, oref, daref, dbref, dfabref, dfbaref = A.warp_blend_grads(*args, w, h, fw, fh, wa, pos32=True, **kw)
+        assert np.abs(o32.astype(np.float64) - oref.reshape(-1)).max() < 1e-5
+        for got, ref in ((da, daref), (db, dbref), (dfab, dfabref), (dfba, dfbaref)):
+            assert rel(got[i].cpu().numpy(), ref) < 1e-3
+
+
+@pytest.mark.parametrize("wa", [0.25, 0.5, 0.8])
+def test_forward_is_the_library_warp_and_blend(dev, wa):
+    """The adjoint's forward is compose_vectors' Blend with warping code 0 on float frames:
+    blend(inv_warp(A, F_BA, 1 - wa), inv_warp(B, F_AB, wa), 1 - wa) by tw_inv_warp (hold) and
+    tw_blend, wherever no sample leaves the image (there the library slides the point back along
+    its segment, the adjoint clamps it). The positions round differently (u * s / r against
+    u * (s / r)), so the values agree to float rounding, not bit for bit."""
+    w, h, fw, fh = 96, 64, 48, 32
+    rng = np.random.RandomState(int(wa * 100))
+    a = rng.rand(h, w, 4).astype(np.float32)
+    b = rng.rand(h, w, 4).astype(np.float32)
+    fab = rng.uniform(-1.5, 1.5, (fh, fw, 2)).astype(np.float32)
+    fba = rng.uniform(-1.5, 1.5, (fh, fw, 2)).astype(np.float32)
+    cu = lambda x: torch.from_numpy(np.ascontiguousarray(x)[None]).cuda()  # noqa: E731
+    out = adjoint.warp_blend(cu(a), cu(b), cu(fab), cu(fba), wa, dev)[0].cpu().numpy()
+    ta = dev.inv_warp(a.reshape(-1), w, h, 2, fba.reshape(-1), (fw, fh), 1.0 - wa, hold=True)
+    tb = dev.inv_warp(b.reshape(-1), w, h, 2, fab.reshape(-1), (fw, fh), wa, hold=True)
+    ref = dev.blend(ta, tb, w, h, 2, 1.0 - wa).reshape(h, w, 4)
+    # displacements reach 1.5 / r ~ 3 px: the pixels 4 or more from the border never clip
+    inner = (slice(4, h - 4), slice(4, w - 4))
+    assert np.abs(out[inner].astype(np.float64) - ref[inner]).max() < 1e-5

@@ -1,7 +1,8 @@
 // The adjoint of warp + blend (the differentiable twin of compose_vectors' Blend with warping code
 // 0): out = ta + (tb - ta) * w with ta = warp(A, F_BA, 1 - wa), tb = warp(B, F_AB, wa), w = 1 - wa,
-// where warp(S, F, s)(p) samples S bilinearly at p + F(p r) s / r (the flow sampled bilinearly at
-// p r, r = (flow size - 1) / (image size - 1) per axis, as warp.rs:693-786), the position clamped
+// where warp(S, F, s)(p) samples S bilinearly at p + F(p r) (s / r) (the flow sampled bilinearly at
+// p r, r = (flow size - 1) / (image size - 1) per axis, the step s / r formed once per side as
+// warp.rs:636-651 forms sx, sy), the position clamped
 // to the image rectangle. One fused kernel per pixel recomputes the forward sample (nothing of the
 // forward pass is stored), takes the output gradient (given, or the sign of out - target for the
 // photometric L1 loss) and scatters:
@@ -59,7 +60,7 @@ __device__ __forceinline__ float dot4(float4 a, float4 b) { return a.x * b.x + a
 
 __device__ __forceinline__ float4 scale4(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
 
-// One side: the sample of S (and its four corners) at p + F(p r) s / r
+// One side: the sample of S (and its four corners) at p + F(p r) (s / r); sx, sy = s / r
 struct Side {
     Sample smp;
     float4 val;
@@ -67,7 +68,8 @@ struct Side {
     float ffx, ffy;
 };
 
-__device__ __forceinline__ Side side_at(const float* S, const float* F, const AdjParams& P, int x, int y, float amount) {
+__device__ __forceinline__ Side side_at(const float* S, const float* F, const AdjParams& P, int x, int y, float sx,
+                                        float sy) {
     Side d;
     float qx = (float)x * P.rx, qy = (float)y * P.ry;
     footprint(qx, qy, P.fw, P.fh, d.fix, d.fiy, d.ffx, d.ffy);
@@ -76,7 +78,7 @@ __device__ __forceinline__ Side side_at(const float* S, const float* F, const Ad
     float2 c = *reinterpret_cast<const float2*>(F + f01), e = *reinterpret_cast<const float2*>(F + f01 + 2);
     float u = (a.x + (b.x - a.x) * d.ffx) * (1.0f - d.ffy) + (c.x + (e.x - c.x) * d.ffx) * d.ffy;
     float v = (a.y + (b.y - a.y) * d.ffx) * (1.0f - d.ffy) + (c.y + (e.y - c.y) * d.ffx) * d.ffy;
-    float px = (float)x + u * amount / P.rx, py = (float)y + v * amount / P.ry;
+    float px = (float)x + u * sx, py = (float)y + v * sy;
     d.smp = sample_at(px, py, P.w, P.h);
     long i00 = (long)d.smp.iy * P.w + d.smp.ix, i01 = i00 + P.w;
     d.val = lerp4(lerp4(ld4(S, i00), ld4(S, i00 + 1), d.smp.fx), lerp4(ld4(S, i01), ld4(S, i01 + 1), d.smp.fx), d.smp.fy);
@@ -107,7 +109,7 @@ __device__ __forceinline__ void acc_add(const Acc& c, const AdjParams& P, int px
 // the gradient of one side: dS at the four corners, the positional gradient into the flow tile
 // (shared) or straight to global memory
 __device__ __forceinline__ void side_back(const float* S, const Side& d, float4 g, const AdjParams& P, const Acc& acc,
-                                          float* sflow, int tx0, int ty0, bool tiled, float* dF, float amount) {
+                                          float* sflow, int tx0, int ty0, bool tiled, float* dF, float sx, float sy) {
     const Sample& s = d.smp;
     float w00 = (1.0f - s.fx) * (1.0f - s.fy), w10 = s.fx * (1.0f - s.fy), w01 = (1.0f - s.fx) * s.fy, w11 = s.fx * s.fy;
     acc_add(acc, P, s.ix, s.iy, scale4(g, w00));
@@ -123,8 +125,8 @@ __device__ __forceinline__ void side_back(const float* S, const Side& d, float4 
                       make_float4(c11.x - c01.x, c11.y - c01.y, c11.z - c01.z, c11.w - c01.w), s.fy);
     float4 dy = lerp4(make_float4(c01.x - c00.x, c01.y - c00.y, c01.z - c00.z, c01.w - c00.w),
                       make_float4(c11.x - c10.x, c11.y - c10.y, c11.z - c10.z, c11.w - c10.w), s.fx);
-    float gu = s.cx ? 0.0f : dot4(g, dx) * amount / P.rx;
-    float gv = s.cy ? 0.0f : dot4(g, dy) * amount / P.ry;
+    float gu = s.cx ? 0.0f : dot4(g, dx) * sx;
+    float gv = s.cy ? 0.0f : dot4(g, dy) * sy;
     float fw00 = (1.0f - d.ffx) * (1.0f - d.ffy), fw10 = d.ffx * (1.0f - d.ffy), fw01 = (1.0f - d.ffx) * d.ffy,
           fw11 = d.ffx * d.ffy;
     const int cx[4] = {0, 1, 0, 1}, cy[4] = {0, 0, 1, 1};
@@ -186,6 +188,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_warp_blend_adjoint(AdjParams
     const float* Fba = P.f_ba + flo;
     const float* Fab = P.f_ab + flo;
     float frac = 1.0f - P.wa;
+    // the steps per flow unit of the two sides (A by F_BA at 1 - wa, B by F_AB at wa)
+    const float sxa = frac / P.rx, sya = frac / P.ry, sxb = P.wa / P.rx, syb = P.wa / P.ry;
     int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TY;
     int x = x0 + (int)(threadIdx.x % ADJ_TX);
     int yb = y0 + (int)(threadIdx.x / ADJ_TX);
@@ -217,13 +221,15 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_warp_blend_adjoint(AdjParams
         float e[2][4];
 #pragma unroll
         for (int s = 0; s < 2; s++) e[s][0] = e[s][2] = INFINITY, e[s][1] = e[s][3] = -INFINITY;
-        for (int i = threadIdx.x; i < tw * th; i += blockDim.x) {
-            long k = ((long)(fy0 + i / tw) * P.fw + fx0 + i % tw) * 2;
-            float2 f0 = *reinterpret_cast<const float2*>(Fba + k), f1 = *reinterpret_cast<const float2*>(Fab + k);
-            e[0][0] = fminf(e[0][0], f0.x); e[0][1] = fmaxf(e[0][1], f0.x);
-            e[0][2] = fminf(e[0][2], f0.y); e[0][3] = fmaxf(e[0][3], f0.y);
-            e[1][0] = fminf(e[1][0], f1.x); e[1][1] = fmaxf(e[1][1], f1.x);
-            e[1][2] = fminf(e[1][2], f1.y); e[1][3] = fmaxf(e[1][3], f1.y);
+        for (int ty = threadIdx.x >> 5; ty < th; ty += blockDim.x >> 5) {  // a warp per texel row
+            for (int tx = threadIdx.x & 31; tx < tw; tx += 32) {
+                long k = ((long)(fy0 + ty) * P.fw + fx0 + tx) * 2;
+                float2 f0 = *reinterpret_cast<const float2*>(Fba + k), f1 = *reinterpret_cast<const float2*>(Fab + k);
+                e[0][0] = fminf(e[0][0], f0.x); e[0][1] = fmaxf(e[0][1], f0.x);
+                e[0][2] = fminf(e[0][2], f0.y); e[0][3] = fmaxf(e[0][3], f0.y);
+                e[1][0] = fminf(e[1][0], f1.x); e[1][1] = fmaxf(e[1][1], f1.x);
+                e[1][2] = fminf(e[1][2], f1.y); e[1][3] = fmaxf(e[1][3], f1.y);
+            }
         }
 #pragma unroll
         for (int s = 0; s < 2; s++)
@@ -249,10 +255,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_warp_blend_adjoint(AdjParams
                 m[2] = fminf(m[2], ext[wi][s][2]);
                 m[3] = fmaxf(m[3], ext[wi][s][3]);
             }
-            float amount = s == 0 ? frac : P.wa;
-            // the extremes of (u * amount) / r and of (v * amount) / r, as side_at forms them
-            float ua = (m[0] * amount) / P.rx, ub = (m[1] * amount) / P.rx;
-            float va = (m[2] * amount) / P.ry, vb = (m[3] * amount) / P.ry;
+            const float sx = s == 0 ? sxa : sxb, sy = s == 0 ? sya : syb;
+            // the extremes of u * sx and of v * sy, as side_at forms them
+            float ua = m[0] * sx, ub = m[1] * sx;
+            float va = m[2] * sy, vb = m[3] * sy;
             float lo_x = (float)x0 + fminf(ua, ub), hi_x = (float)xe + fmaxf(ua, ub);
             float lo_y = (float)y0 + fminf(va, vb), hi_y = (float)ye + fmaxf(va, vb);
             Sample a = sample_at(lo_x, lo_y, P.w, P.h), c = sample_at(hi_x, hi_y, P.w, P.h);
@@ -285,8 +291,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_warp_blend_adjoint(AdjParams
     for (int j = 0; j < ADJ_TY / ROWS; j++) {
         int y = yb + j * ROWS;
         if (x >= P.w || y >= P.h) continue;
-        Side sa = side_at(A, Fba, P, x, y, frac);
-        Side sb = side_at(B, Fab, P, x, y, P.wa);
+        Side sa = side_at(A, Fba, P, x, y, sxa, sya);
+        Side sb = side_at(B, Fab, P, x, y, sxb, syb);
         float4 out = lerp4(sa.val, sb.val, frac);
         long i = (long)y * P.w + x;
         if (P.out) reinterpret_cast<float4*>(P.out + img)[i] = out;
@@ -303,8 +309,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_warp_blend_adjoint(AdjParams
         }
         Acc ca{shared_box[0] ? sacc0 : nullptr, box[0][0], box[0][1], bw[0], bh[0], P.da ? P.da + img : nullptr};
         Acc cb{shared_box[1] ? sacc1 : nullptr, box[1][0], box[1][1], bw[1], bh[1], P.db ? P.db + img : nullptr};
-        side_back(A, sa, scale4(g, 1.0f - frac), P, ca, sflow0, tx0, ty0, tiled, P.df_ba ? P.df_ba + flo : nullptr, frac);
-        side_back(B, sb, scale4(g, frac), P, cb, sflow1, tx0, ty0, tiled, P.df_ab ? P.df_ab + flo : nullptr, P.wa);
+        side_back(A, sa, scale4(g, 1.0f - frac), P, ca, sflow0, tx0, ty0, tiled, P.df_ba ? P.df_ba + flo : nullptr, sxa, sya);
+        side_back(B, sb, scale4(g, frac), P, cb, sflow1, tx0, ty0, tiled, P.df_ab ? P.df_ab + flo : nullptr, sxb, syb);
     }
     if (P.loss) {  // the loss of the batch item: a warp shuffle sum, one atomic per warp
 #pragma unroll
@@ -319,11 +325,16 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_warp_blend_adjoint(AdjParams
         if (!shared_box[s] || !dS) continue;
         float* acc = s == 0 ? sacc0 : sacc1;
         float4* g4 = reinterpret_cast<float4*>(dS + img);
-        for (int i = threadIdx.x; i < bw[s] * bh[s]; i += blockDim.x) {
-            float4 v = make_float4(acc[i], acc[i + ADJ_BOX_PX], acc[i + 2 * ADJ_BOX_PX], acc[i + 3 * ADJ_BOX_PX]);
-            if (v.x == 0.0f && v.y == 0.0f && v.z == 0.0f && v.w == 0.0f) continue;
-            int px = box[s][0] + i % bw[s], py = box[s][1] + i / bw[s];
-            if (px < P.w && py < P.h) atomicAdd(g4 + ((long)py * P.w + px), v);
+        // a warp per box row, its lanes along the row (no division by the box width)
+        for (int ry = threadIdx.x >> 5; ry < bh[s]; ry += blockDim.x >> 5) {
+            const int py = box[s][1] + ry;
+            for (int rx = threadIdx.x & 31; rx < bw[s]; rx += 32) {
+                const int i = ry * bw[s] + rx;
+                float4 v = make_float4(acc[i], acc[i + ADJ_BOX_PX], acc[i + 2 * ADJ_BOX_PX], acc[i + 3 * ADJ_BOX_PX]);
+                if (v.x == 0.0f && v.y == 0.0f && v.z == 0.0f && v.w == 0.0f) continue;
+                const int px = box[s][0] + rx;
+                if (px < P.w && py < P.h) atomicAdd(g4 + ((long)py * P.w + px), v);
+            }
         }
     }
     if (tiled) {
