@@ -310,11 +310,9 @@ void block_match(tw_ctx* ctx, const float* A, const float* B, const float* AT, c
     if (w < 3 || h < 3) return;  // callers refuse lines above BM_MAX_LINE before any launch
     double b = 24.0 * w * h;  // per launch (both sweeps): the field read and written (8 + 8), A and B read once (4 + 4)
     LevelTune t = level_tune(ctx, w, h);
-    LAUNCHV(ctx, fast, b, k_bm_rows, h - 2, t.bm_rows_threads, bm_smem_bytes(w), A, B, fu, fv, w, h);
-    dim3 tb(32, 8);
-    LAUNCHV(ctx, fast, 16.0 * w * h, k_transpose2, dim3((w + 31) / 32, (h + 31) / 32), tb, 0, fu, fv, uT, vT, w, h);
-    LAUNCHV(ctx, fast, b, k_bm_cols, w - 2, t.bm_cols_threads, bm_smem_bytes(h), AT, BT, uT, vT, w, h);
-    LAUNCHV(ctx, fast, 16.0 * w * h, k_transpose2, dim3((h + 31) / 32, (w + 31) / 32), tb, 0, uT, vT, fu, fv, h, w);
+    // the row sweeps write the transposed field the column sweeps read, and those write it back
+    LAUNCHV(ctx, fast, b, k_bm_rows, h - 2, t.bm_rows_threads, bm_smem_bytes(w), A, B, fu, fv, w, h, uT, vT);
+    LAUNCHV(ctx, fast, b, k_bm_cols, w - 2, t.bm_cols_threads, bm_smem_bytes(h), AT, BT, uT, vT, w, h, fu, fv);
 }
 
 // ---- one solve over two resident pyramids (flow.rs:1258-1307) ------------------------------------------

@@ -154,20 +154,20 @@ int tw_autotune(tw_ctx* ctx, const tw_flow_settings* s, int32_t width, int32_t h
                     best.iter_threads = c.iter_threads;
                 }
             }
-            // block matching: the row and the column kernel, 128 to 512 threads per line (the field
-            // restored before every launch: the sweeps update it in place)
+            // block matching: the row and the column kernel, 128 to 512 threads per line (each one's
+            // input field restored before every launch)
             if (w >= 3 && h >= 3) {
                 cudaMemcpyAsync(fsave, fu, (size_t)w * h * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream);
                 float br = 1e30f, bc = 1e30f;
                 for (int th : {128, 256, 512}) {
                     float ms = timed([&] {
                         cudaMemcpyAsync(fu, fsave, (size_t)w * h * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream);
-                        LAUNCH(ctx, k_bm_rows, h - 2, th, bm_smem_bytes(w), A, Bp, fu, fv, w, h);
+                        LAUNCH(ctx, k_bm_rows, h - 2, th, bm_smem_bytes(w), A, Bp, fu, fv, w, h, uT, vT);
                     });
                     if (ms < br) { br = ms; best.bm_rows_threads = th; }
                     ms = timed([&] {
                         cudaMemcpyAsync(uT, fsave, (size_t)w * h * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream);
-                        LAUNCH(ctx, k_bm_cols, w - 2, th, bm_smem_bytes(h), AT, BT, uT, vT, w, h);
+                        LAUNCH(ctx, k_bm_cols, w - 2, th, bm_smem_bytes(h), AT, BT, uT, vT, w, h, fu, fv);
                     });
                     if (ms < bc) { bc = ms; best.bm_cols_threads = th; }
                 }

@@ -92,14 +92,15 @@ __global__ void k_fill(float* __restrict__ p, long n, float v);
 __global__ void k_deinterleave(const float* __restrict__ in, long n, float* __restrict__ fu, float* __restrict__ fv);
 __global__ void k_interleave(const float* __restrict__ fu, const float* __restrict__ fv, long n, float* __restrict__ out);
 
-// block matching (flow.rs:447-622): the four in-place sweeps; one CTA per row or column. The column
-// sweeps take the transposes of A, B and the field (element (x, y) at [x * h + y]).
-// both sweeps of every row (left to right, then right to left) / of every column of the transposed
-// planes (top to bottom, then bottom to top), one CTA per line, bm_smem_bytes(line) shared
-__global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
-                          float* __restrict__ fv, int w, int h);
-__global__ void k_bm_cols(const float* __restrict__ AT, const float* __restrict__ BT, float* __restrict__ fuT,
-                          float* __restrict__ fvT, int w, int h);
+// block matching (flow.rs:447-622): the four sweeps; one CTA per row or column, bm_smem_bytes(line)
+// shared. k_bm_rows: both sweeps of every row (left to right, then right to left) of (fu, fv), the
+// result written into the transposes (uT, vT; element (x, y) at [x * h + y]); k_bm_cols: both
+// sweeps of every column (top to bottom, then bottom to top) read from (uT, vT), with the
+// transposes of A and B, the result written back into (fu, fv). Lines 0 and last are not swept.
+__global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, const float* __restrict__ fu,
+                          const float* __restrict__ fv, int w, int h, float* __restrict__ uT, float* __restrict__ vT);
+__global__ void k_bm_cols(const float* __restrict__ AT, const float* __restrict__ BT, const float* __restrict__ uT,
+                          const float* __restrict__ vT, int w, int h, float* fu, float* fv);
 // two w x h planes into their h x w transposes; block (32, 8), grid (ceil(w/32), ceil(h/32))
 __global__ void k_transpose2(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ at,
                              float* __restrict__ bt, int w, int h);

@@ -10,10 +10,10 @@ namespace fast {
 __global__ void k_resample(const float* __restrict__ src, int sw, int sh, float* __restrict__ dst, int dw, int dh);
 __global__ void k_range_any(const float* __restrict__ fu, const float* __restrict__ fv, int w, int h,
                             int* __restrict__ any_in_range);
-__global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
-                          float* __restrict__ fv, int w, int h);
-__global__ void k_bm_cols(const float* __restrict__ AT, const float* __restrict__ BT, float* __restrict__ fuT,
-                          float* __restrict__ fvT, int w, int h);
+__global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, const float* __restrict__ fu,
+                          const float* __restrict__ fv, int w, int h, float* __restrict__ uT, float* __restrict__ vT);
+__global__ void k_bm_cols(const float* __restrict__ AT, const float* __restrict__ BT, const float* __restrict__ uT,
+                          const float* __restrict__ vT, int w, int h, float* fu, float* fv);
 __global__ void k_transpose2(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ at,
                              float* __restrict__ bt, int w, int h);
 __global__ void k_blur5_band(const float* __restrict__ orig, const void* __restrict__ luma_src, int fmt, int luma_mode,

@@ -62,7 +62,7 @@ extern "C" int tw_block_match_noalloc(const float* a, const float* b, float* flo
     float *at = fv + n, *bt = at + n, *ut = bt + n, *vt = ut + n;
     const int tb = 256;
     dim3 g1((unsigned)((n + tb - 1) / tb));
-    dim3 tt(32, 8), ga((width + 31) / 32, (height + 31) / 32), gb((height + 31) / 32, (width + 31) / 32);
+    dim3 tt(32, 8), ga((width + 31) / 32, (height + 31) / 32);
     const float* cfu = fu;
     const float* cfv = fv;
     const float* cut = ut;
@@ -71,14 +71,14 @@ extern "C" int tw_block_match_noalloc(const float* a, const float* b, float* flo
     // contents never reach the result
     cudaError_t e = launch(tw::k_deinterleave, g1, dim3(tb), 0, s, (const float*)flow, n, fu, fv);
     if (e == cudaSuccess && width >= 3 && height >= 3) {
-        e = launch(tw::k_bm_rows, dim3(height - 2), dim3(tb), tw::bm_smem_bytes(width), s, a, b, fu, fv, (int)width,
-                   (int)height);
+        // the row sweeps write the transposed field (ut, vt), the column sweeps read it with the
+        // transposes of A and B and write the result back into (fu, fv)
+        e = launch(tw::k_bm_rows, dim3(height - 2), dim3(tb), tw::bm_smem_bytes(width), s, a, b, cfu, cfv, (int)width,
+                   (int)height, ut, vt);
         if (e == cudaSuccess) e = launch(tw::k_transpose2, ga, tt, 0, s, a, b, at, bt, (int)width, (int)height);
-        if (e == cudaSuccess) e = launch(tw::k_transpose2, ga, tt, 0, s, cfu, cfv, ut, vt, (int)width, (int)height);
         if (e == cudaSuccess)
             e = launch(tw::k_bm_cols, dim3(width - 2), dim3(tb), tw::bm_smem_bytes(height), s, (const float*)at,
-                       (const float*)bt, ut, vt, (int)width, (int)height);
-        if (e == cudaSuccess) e = launch(tw::k_transpose2, gb, tt, 0, s, cut, cvt, fu, fv, (int)height, (int)width);
+                       (const float*)bt, cut, cvt, (int)width, (int)height, fu, fv);
     }
     if (e == cudaSuccess) e = launch(tw::k_interleave, g1, dim3(tb), 0, s, cfu, cfv, n, flow);
     if (e != cudaSuccess) return TW_ERR_CUDA;

@@ -665,16 +665,20 @@ __device__ void bm_sweep(float* su, float* sv, float* c0, const float* s_a, int*
 }
 
 // The two sweeps of a line (flow.rs:551-622: left to right then right to left, or top to bottom
-// then bottom to top), with the field, A's three lines and the tables in shared memory; the field
-// goes to global memory once, after both. Column sweeps take TRANSPOSED planes (A, B and the field
-// stored column by column, element (x, y) at [x * h + y]) so that a warp's lanes, which walk down
-// one column, read contiguous memory; the reference transposes its field for the same sweeps
-// (flow.rs:583-621).
+// then bottom to top), with the field, A's three lines and the tables in shared memory. The line is
+// read contiguously from src (row y of the row-major field, or column x of the transposed one; a
+// column's two end elements, which no sweep changes, from the row-major field ends) and its swept
+// interior written across: element i of line `fixed` to dst[i * other + fixed], other = h for a row
+// (into the transposed field the column sweeps read) and w for a column (back into the row-major
+// field). So no transpose of the field runs between the row and the column sweeps; the reference
+// transposes its field for the column sweeps (flow.rs:583-621). A and B of a column sweep are the
+// transposed planes (element (x, y) at [x * h + y]) so that the line's patches stay contiguous.
 template <bool COLS>
-__device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
-                        float* __restrict__ fv, int w, int h, int fixed) {
+__device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B, const float* src_u,
+                        const float* src_v, const float* ends_u, const float* ends_v, float* dst_u, float* dst_v, int w,
+                        int h, int fixed) {
     extern __shared__ float sm[];
-    const int len = COLS ? h : w;
+    const int len = COLS ? h : w, other = COLS ? w : h;
     if (len < 3) return;  // no interior position
     const int nch = (len + 31) >> 5;
     float* su = sm;
@@ -687,12 +691,14 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
     int* ctl = qb + len;  // 8 counters
     int* entry = ctl + 8;
     int* prevl = entry + nch;
-    // both layouts keep the line contiguous: row y of a row-major plane, column x of a transposed one
-    auto gidx = [&](int i) -> long { return (long)fixed * len + i; };
     for (int i = threadIdx.x; i < len; i += blockDim.x) {
-        long g = gidx(i);
-        su[i] = fu[g];
-        sv[i] = fv[g];
+        if (COLS && (i == 0 || i == len - 1)) {
+            su[i] = ends_u[(long)i * w + fixed];
+            sv[i] = ends_v[(long)i * w + fixed];
+        } else {
+            su[i] = src_u[(long)fixed * len + i];
+            sv[i] = src_v[(long)fixed * len + i];
+        }
 #pragma unroll
         for (int o = 0; o < 3; o++)  // A at offset o-1 across the line: rows y-1..y+1, or columns x-1..x+1
             s_a[o * len + i] = __ldg(A + (long)(fixed - 1 + o) * len + i);
@@ -702,9 +708,8 @@ __device__ void bm_line(const float* __restrict__ A, const float* __restrict__ B
     bm_sweep<COLS>(su, sv, c0, s_a, endp, qa, qb, ctl, entry, prevl, B, w, h, fixed, len, false);
     bm_sweep<COLS>(su, sv, c0, s_a, endp, qa, qb, ctl, entry, prevl, B, w, h, fixed, len, true);
     for (int i = threadIdx.x + 1; i <= len - 2; i += blockDim.x) {
-        long g = gidx(i);
-        fu[g] = su[i];
-        fv[g] = sv[i];
+        dst_u[(long)i * other + fixed] = su[i];
+        dst_v[(long)i * other + fixed] = sv[i];
     }
 }
 
@@ -730,18 +735,22 @@ __global__ void k_transpose2(const float* __restrict__ a, const float* __restric
     }
 }
 
-__global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
-                          float* __restrict__ fv, int w, int h) {
+// The row sweeps of rows 1..h-2 of the field (fu, fv), the result into the transposed planes
+// (uT, vT; element (x, y) at [x * h + y]) at the interior of those rows
+__global__ void k_bm_rows(const float* __restrict__ A, const float* __restrict__ B, const float* __restrict__ fu,
+                          const float* __restrict__ fv, int w, int h, float* __restrict__ uT, float* __restrict__ vT) {
     int y = blockIdx.x + 1;  // rows 1..h-2
     if (y > h - 2) return;
-    bm_line<false>(A, B, fu, fv, w, h, y);
+    bm_line<false>(A, B, fu, fv, nullptr, nullptr, uT, vT, w, h, y);
 }
 
-__global__ void k_bm_cols(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ fu,
-                          float* __restrict__ fv, int w, int h) {
+// The column sweeps of columns 1..w-2 from the transposed planes (uT, vT) that k_bm_rows wrote, the
+// end rows 0 and h-1 from (fu, fv); the result into (fu, fv) at rows 1..h-2 of those columns
+__global__ void k_bm_cols(const float* __restrict__ AT, const float* __restrict__ BT, const float* __restrict__ uT,
+                          const float* __restrict__ vT, int w, int h, float* fu, float* fv) {
     int x = blockIdx.x + 1;  // columns 1..w-2
     if (x > w - 2) return;
-    bm_line<true>(A, B, fu, fv, w, h, x);
+    bm_line<true>(AT, BT, uT, vT, fu, fv, fu, fv, w, h, x);
 }
 
 TW_VARIANT_END
