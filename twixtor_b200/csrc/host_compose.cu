@@ -22,7 +22,8 @@ bool warp_copy_only(float amount, int fw, int width) {
     return 0.0001 > (double)q;
 }
 
-WarpParams warp_params(const void* src, const float* flow_interleaved, int fw, int fh, float amount, int width, bool hold) {
+WarpParams warp_params(const void* src, const float* flow_interleaved, int fw, int fh, float amount, int width, int height,
+                       bool hold) {
     WarpParams p{};
     p.src = src;
     p.fu = flow_interleaved;
@@ -31,6 +32,12 @@ WarpParams warp_params(const void* src, const float* flow_interleaved, int fw, i
     p.fw = fw;
     p.fh = fh;
     p.amount = amount;
+    if (flow_interleaved) {
+        p.rx = (float)(fw - 1) / (float)(width - 1);
+        p.ry = (float)(fh - 1) / (float)(height - 1);
+        p.sx = amount / p.rx;
+        p.sy = amount / p.ry;
+    }
     p.hold = hold;
     p.copy_only = flow_interleaved ? warp_copy_only(amount, fw, width) : true;
     return p;
@@ -327,7 +334,7 @@ int blur_comp_dev(tw_ctx* ctx, const void* img, void* dst, const float* flow, in
     MotionBlur B{};
     B.src = img;
     B.dst = dst;
-    B.flow = warp_params(img, flow, fw, fh, 0.0f, W, true);
+    B.flow = warp_params(img, flow, fw, fh, 0.0f, W, H, true);
     B.fmt = fmt;
     B.w = W;
     B.h = H;
@@ -425,8 +432,8 @@ int weighted_tail_dev(tw_ctx* ctx, void* out, void* ta, const void* a, void* tb,
     CHECK(sharpen_dev(ctx, ta, a, W, H, fmt, frac, above_first, *ss.wb, nullptr));
     CHECK(sharpen_dev(ctx, tb, b, W, H, fmt, wa, above_first, *ss.wb, nullptr));
     if (!c0) {
-        WarpParams pa = warp_params(ta, nullptr, 0, 0, 0.0f, W, true);
-        WarpParams pb = warp_params(tb, nullptr, 0, 0, 0.0f, W, true);
+        WarpParams pa = warp_params(ta, nullptr, 0, 0, 0.0f, W, H, true);
+        WarpParams pb = warp_params(tb, nullptr, 0, 0, 0.0f, W, H, true);
         LAUNCH(ctx, k_compose_blend, grid2(W, H), TB, 0, pa, pb, fmt, frac, blend_mode(frac), out, W, H, false, false, bad);
         return TW_OK;
     }
@@ -483,8 +490,8 @@ int compose_forward_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_sele
         CHECK(forward_warp_dev(ctx, eng_a, f_ab, fw, fh, W, H, fmt, frac, pyramid, ta, fill ? c0 : nullptr));
         CHECK(forward_warp_dev(ctx, eng_b, f_ba, fw, fh, W, H, fmt, wa, pyramid, tb, fill ? c1 : nullptr));
         if (!fill) {  // blend_tail without coverage: blend(tA, tB, frac)
-            WarpParams pa = warp_params(ta, nullptr, 0, 0, 0.0f, W, true);
-            WarpParams pb = warp_params(tb, nullptr, 0, 0, 0.0f, W, true);
+            WarpParams pa = warp_params(ta, nullptr, 0, 0, 0.0f, W, H, true);
+            WarpParams pb = warp_params(tb, nullptr, 0, 0, 0.0f, W, H, true);
             LAUNCH(ctx, k_compose_blend, grid2(W, H), TB, 0, pa, pb, fmt, frac, blend_mode(frac), out, W, H, false, false, bad);
             return TW_OK;
         }
@@ -566,14 +573,14 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
             const float* flow = use_ab ? f_ab : f_ba;
             if (!flow) return ctx->fail(TW_ERR_MISMATCH, "the composition needs the flow %s but it was not computed", use_ab ? "F_AB" : "F_BA");
             // the A branch unless 0.5 > wa (a NaN weight takes A)
-            if (!(0.5f > wa)) pa = warp_params(eng_a, flow, fw, fh, 1.0f - wa, W, false);
-            else pa = warp_params(eng_b, flow, fw, fh, wa, W, false);
+            if (!(0.5f > wa)) pa = warp_params(eng_a, flow, fw, fh, 1.0f - wa, W, H, false);
+            else pa = warp_params(eng_b, flow, fw, fh, wa, W, H, false);
             pb = pa;
             smode = 0;
         } else if (sel.interp == 1) {
             if (!f_ab || !f_ba) return ctx->fail(TW_ERR_MISMATCH, "the composition needs both flows");
-            pa = warp_params(eng_a, f_ba, fw, fh, frac, W, false);
-            pb = warp_params(eng_b, f_ab, fw, fh, wa, W, false);
+            pa = warp_params(eng_a, f_ba, fw, fh, frac, W, H, false);
+            pb = warp_params(eng_b, f_ab, fw, fh, wa, W, H, false);
             smode = 1;
         } else if (sel.interp == 2) {
             // smartblend.rs:400-420 (weighted_blend_smart): the warps without hold and with coverage,
@@ -586,8 +593,8 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
                 CHECK(ctx->ensure(*ws.wt[i], ib, "warped frame"));
                 CHECK(ctx->ensure(*ws.cov[i], px, "coverage"));
             }
-            pa = warp_params(eng_a, f_ba, fw, fh, frac, W, false);
-            pb = warp_params(eng_b, f_ab, fw, fh, wa, W, false);
+            pa = warp_params(eng_a, f_ba, fw, fh, frac, W, H, false);
+            pb = warp_params(eng_b, f_ab, fw, fh, wa, W, H, false);
             LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pa, fmt, ws.wt[0]->p, ws.cov[0]->as<uint8_t>(), W, H, bad);
             LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pb, fmt, ws.wt[1]->p, ws.cov[1]->as<uint8_t>(), W, H, bad);
             void* comp = out;
@@ -631,14 +638,14 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
         bool use_ab = (wa < 0.5f && (unsigned)cs.warp_mode < 2) || (0.5f <= wa && (unsigned)cs.warp_mode > 1);
         const float* flow = use_ab ? f_ab : f_ba;
         if (!flow) return ctx->fail(TW_ERR_MISMATCH, "the composition needs the flow %s but it was not computed", use_ab ? "F_AB" : "F_BA");
-        if (0.5f <= wa) pa = warp_params(eng_a, flow, fw, fh, frac, W, true);
-        else pa = warp_params(eng_b, flow, fw, fh, wa, W, true);
+        if (0.5f <= wa) pa = warp_params(eng_a, flow, fw, fh, frac, W, H, true);
+        else pa = warp_params(eng_b, flow, fw, fh, wa, W, H, true);
         pb = pa;
         mode = 1;
     } else if (sel.interp == 1) {
         if (!f_ab || !f_ba) return ctx->fail(TW_ERR_MISMATCH, "the composition needs both flows");
-        pa = warp_params(eng_a, f_ba, fw, fh, frac, W, true);
-        pb = warp_params(eng_b, f_ab, fw, fh, wa, W, true);
+        pa = warp_params(eng_a, f_ba, fw, fh, frac, W, H, true);
+        pb = warp_params(eng_b, f_ab, fw, fh, wa, W, H, true);
         wb = frac;
         mode = blend_mode(frac);
     } else if (sel.interp == 2) {
@@ -648,14 +655,14 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
         const WbScratch& ws = *ss->wb;
         size_t ib = (size_t)W * H * 4 * sample_bytes(fmt);
         for (int i = 0; i < 2; i++) CHECK(ctx->ensure(*ws.wt[i], ib, "warped frame"));
-        WarpParams qa = warp_params(eng_a, f_ba, fw, fh, frac, W, true);
-        WarpParams qb = warp_params(eng_b, f_ab, fw, fh, wa, W, true);
+        WarpParams qa = warp_params(eng_a, f_ba, fw, fh, frac, W, H, true);
+        WarpParams qb = warp_params(eng_b, f_ab, fw, fh, wa, W, H, true);
         LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, qa, fmt, ws.wt[0]->p, (uint8_t*)nullptr, W, H, bad);
         LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, qb, fmt, ws.wt[1]->p, (uint8_t*)nullptr, W, H, bad);
         CHECK(sharpen_dev(ctx, ws.wt[0]->p, eng_a, W, H, fmt, frac, cs.taps_above_first != 0, ws, nullptr));
         CHECK(sharpen_dev(ctx, ws.wt[1]->p, eng_b, W, H, fmt, wa, cs.taps_above_first != 0, ws, nullptr));
-        pa = warp_params(ws.wt[0]->p, nullptr, 0, 0, 0.0f, W, true);
-        pb = warp_params(ws.wt[1]->p, nullptr, 0, 0, 0.0f, W, true);
+        pa = warp_params(ws.wt[0]->p, nullptr, 0, 0, 0.0f, W, H, true);
+        pb = warp_params(ws.wt[1]->p, nullptr, 0, 0, 0.0f, W, H, true);
         wb = frac;
         mode = blend_mode(frac);
     } else {
@@ -671,8 +678,8 @@ int compose_dev(tw_ctx* ctx, const tw_engine_settings& cs, const tw_selection& s
 // compose.rs:218-231 (interpolate): the fast path without flows
 int interpolate_dev(tw_ctx* ctx, const tw_selection& sel, const void* eng_a, const void* eng_b, int W, int H, int fmt,
                     void* out, bool to_wire, int* bad, const SmartScratch* ss) {
-    WarpParams pa = warp_params(eng_a, nullptr, 0, 0, 0.0f, W, true);
-    WarpParams pb = warp_params(eng_b, nullptr, 0, 0, 0.0f, W, true);
+    WarpParams pa = warp_params(eng_a, nullptr, 0, 0, 0.0f, W, H, true);
+    WarpParams pb = warp_params(eng_b, nullptr, 0, 0, 0.0f, W, H, true);
     int mode;
     float wb = 0.0f;
     if (sel.interp == 0) {
@@ -793,7 +800,7 @@ int tw_inv_warp(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw_fl
     CHECK(ctx->ensure(ctx->plane[3], (size_t)W * H, "coverage"));
     int* flags = ctx->flags.as<int>();
     CHECK(ctx->cuda(cudaMemsetAsync(flags, 0, FLAGS_BYTES, ctx->stream), "flags"));
-    WarpParams p = warp_params(ctx->eng[0].p, ctx->flow[0].as<float>(), flow->width, flow->height, amount, W, (hold & 1) != 0);
+    WarpParams p = warp_params(ctx->eng[0].p, ctx->flow[0].as<float>(), flow->width, flow->height, amount, W, H, (hold & 1) != 0);
     p.is360 = (hold & 2) != 0;  // warp.rs:29-50: is360 takes precedence over hold
     uint8_t* dcov = cov ? ctx->plane[3].as<uint8_t>() : nullptr;
     LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, p, src->fmt, ctx->eng[2].p, dcov, W, H, flags + FL_BAD);
@@ -820,8 +827,8 @@ int tw_blend(tw_ctx* ctx, tw_image_mut* out, const tw_image* a, const tw_image* 
     CHECK(upload_image(ctx, ctx->eng[1], b));
     size_t ob = (size_t)W * H * 4 * sample_bytes(a->fmt);
     CHECK(ctx->ensure(ctx->eng[2], ob, "blend output"));
-    WarpParams pa = warp_params(ctx->eng[0].p, nullptr, 0, 0, 0.0f, W, true);
-    WarpParams pb = warp_params(ctx->eng[1].p, nullptr, 0, 0, 0.0f, W, true);
+    WarpParams pa = warp_params(ctx->eng[0].p, nullptr, 0, 0, 0.0f, W, H, true);
+    WarpParams pb = warp_params(ctx->eng[1].p, nullptr, 0, 0, 0.0f, W, H, true);
     int* flags = ctx->flags.as<int>();
     LAUNCH(ctx, k_compose_blend, grid2(W, H), TB, 0, pa, pb, a->fmt, w, blend_mode(w), ctx->eng[2].p, W, H, false, false,
            flags + FL_BAD);
@@ -939,7 +946,7 @@ int tw_motion_blur(tw_ctx* ctx, tw_image_mut* out, const tw_image* src, const tw
     MotionBlur B{};
     B.src = ctx->eng[0].p;
     B.dst = ctx->eng[1].p;
-    B.flow = warp_params(ctx->eng[0].p, ctx->flow[0].as<float>(), flow->width, flow->height, 0.0f, W, true);
+    B.flow = warp_params(ctx->eng[0].p, ctx->flow[0].as<float>(), flow->width, flow->height, 0.0f, W, H, true);
     B.fmt = fmt;
     B.w = W;
     B.h = H;

@@ -367,8 +367,8 @@ static int layers_dev(tw_ctx* ctx, const tw_retime_settings& s, const tw_selecti
             CHECK(forward_warp_dev(ctx, img(1, k), fba, g.w, g.h, W, H, fmt, 1.0f, cs.gouraud == 0, plate[0], nullptr));
             CHECK(forward_warp_dev(ctx, img(0, k), fab, g.w, g.h, W, H, fmt, 1.0f, cs.gouraud == 0, plate[1], nullptr));
         } else {
-            WarpParams pa_ = warp_params(img(1, k), fab, g.w, g.h, 1.0f, W, true);
-            WarpParams pb_ = warp_params(img(0, k), fba, g.w, g.h, 1.0f, W, true);
+            WarpParams pa_ = warp_params(img(1, k), fab, g.w, g.h, 1.0f, W, H, true);
+            WarpParams pb_ = warp_params(img(0, k), fba, g.w, g.h, 1.0f, W, H, true);
             LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pa_, fmt, plate[0], (uint8_t*)nullptr, W, H, flags + FL_BAD);
             LAUNCH(ctx, k_inv_warp, grid2(W, H), TB, 0, pb_, fmt, plate[1], (uint8_t*)nullptr, W, H, flags + FL_BAD);
         }

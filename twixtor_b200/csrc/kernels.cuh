@@ -116,6 +116,10 @@ struct WarpParams {
     int fstride;
     int fw, fh;
     float amount;
+    // warp.rs:636-651: the flow's ratios to the image, rx = (fw - 1) / (w - 1), ry likewise, and the
+    // steps sx = amount / rx, sy = amount / ry, single precision, formed once on the host (the same
+    // IEEE divisions the kernel made per pixel)
+    float rx, ry, sx, sy;
     bool copy_only;      // the |amount| early outs of inv_warp (warp.rs:751-764)
     bool hold;
     bool is360;          // wrap-around: the point wrapped into the image, the pole reflection, the 360 sampler

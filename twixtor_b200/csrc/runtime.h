@@ -334,7 +334,8 @@ int build_mask_pyramid_dev(tw_ctx* ctx, float* matte, int W, int H, const tw_flo
 
 // host_compose.cu
 bool warp_copy_only(float amount, int fw, int width);
-WarpParams warp_params(const void* src, const float* flow_interleaved, int fw, int fh, float amount, int width, bool hold);
+WarpParams warp_params(const void* src, const float* flow_interleaved, int fw, int fh, float amount, int width, int height,
+                       bool hold);
 int fill_dev(tw_ctx* ctx, void* img, int W, int H, int fmt, const uint8_t* holes, const int* any, bool above_first,
              DevBuf& fb);
 int forward_warp_dev(tw_ctx* ctx, const void* src, const float* flow, int fw, int fh, int W, int H, int fmt,

@@ -208,9 +208,7 @@ __device__ __forceinline__ uint8_t warp_pixel(const WarpParams& p, int x, int y,
         return 255;
     }
     int w1i = w - 1, h1i = h - 1;
-    float rx = (float)(p.fw - 1) / (float)w1i;
-    float ry = (float)(p.fh - 1) / (float)h1i;
-    float sx = p.amount / rx, sy = p.amount / ry;
+    const float rx = p.rx, ry = p.ry, sx = p.sx, sy = p.sy;  // formed on the host (warp_params)
     float wf = (float)w, hf = (float)h, w1 = (float)w1i, h1 = (float)h1i;
     float xf = (float)x, yf = (float)y;
     float du, dv;
