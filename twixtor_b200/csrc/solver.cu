@@ -389,7 +389,9 @@ __global__ void k_fill(float* __restrict__ p, long n, float v) {
 // (floats), end and two queues (ints), then 8 counters and two ints per 32-position chunk.
 size_t bm_smem_bytes(int len) { return (size_t)len * 4 * (3 + 3 + 3) + (size_t)(8 + 2 * ((len + 31) / 32)) * 4; }
 
-constexpr int BM_STAGES = 3;      // run extension tests made one per queued candidate before groups of 8 lanes
+constexpr int BM_STAGES = 3;      // run extension tests made one per queued candidate before the lane groups
+constexpr int BM_GROUP = 8;       // lanes per queued candidate after the stages (positions tested per round)
+static_assert(BM_GROUP >= 2 && BM_GROUP < 32 && 32 % BM_GROUP == 0, "groups tile a warp");
 constexpr int BM_TERM = 1 << 30;  // "past the line" in the chain tables
 
 // The 3x3 patch of A around line position i (flow.rs:454-469) from the three lines of A in shared
@@ -462,7 +464,7 @@ __device__ __forceinline__ void bm_push(int* q, int* n, bool want, int val) {
 //      sweep replaced the vector, those positions listed by the forward sweep), and the test of
 //      v[q-1] at every q: end[q-1] = q where it refuses, the others queued;
 //   2. the queued candidates extended one position per stage (BM_STAGES stages, the survivors
-//      compacted after each), then the rest by groups of 8 lanes testing 8 positions at once;
+//      compacted after each), then the rest by groups of BM_GROUP lanes testing as many positions at once;
 //   3. the chain of run starts 0, end[0], end[end[0]], ... in 32-position chunks, one warp per
 //      chunk: the successor tables doubled by shuffles give every position's first chain element
 //      past the chunk; one thread walks the chunks from position 0 (their entries and the last start
@@ -545,33 +547,34 @@ __device__ void bm_sweep(float* su, float* sv, float* c0, const float* s_a, int*
         cur = nxt;
         nxt = sw;
     }
-    //    the long runs: a group of 8 lanes per candidate, 8 positions per test round
+    //    the long runs: a group of BM_GROUP lanes per candidate, BM_GROUP positions per test round
     if (nq > 0) {
-        const int g = lane >> 3, sub = lane & 7, step = BM_STAGES + 2;
-        for (int kb = warp * 4; kb < nq; kb += nw * 4) {
+        constexpr int GPW = 32 / BM_GROUP;  // groups per warp
+        const int g = lane / BM_GROUP, sub = lane % BM_GROUP, step = BM_STAGES + 2;
+        for (int kb = warp * GPW; kb < nq; kb += nw * GPW) {
             const int k = kb + g;
             bool live = k < nq;
             const int j = live ? cur[k] : 0;
             const int jl = line_of(j);
             const float nu = live ? su[jl] : 0.0f, nv = live ? sv[jl] : 0.0f;
             int pos = j + step;
-            for (int guard = 0; guard <= len && __any_sync(FULL, live); guard += 8) {
+            for (int guard = 0; guard <= len && __any_sync(FULL, live); guard += BM_GROUP) {
                 const int qq = pos + sub;
                 bool refuse = false;
                 if (live && qq <= len - 2) {
                     const int il = line_of(qq);
                     refuse = !bm_accept<COLS>(s_a, len, B, w, h, fixed, il, nu, nv, c0[il]);
                 }
-                const unsigned gm = (__ballot_sync(FULL, refuse) >> (g * 8)) & 0xffu;
+                const unsigned gm = (__ballot_sync(FULL, refuse) >> (g * BM_GROUP)) & ((1u << BM_GROUP) - 1u);
                 if (live) {
                     if (gm) {
                         if (sub == 0) endp[j] = pos + __ffs(gm) - 1;
                         live = false;
-                    } else if (pos + 8 > len - 2) {
+                    } else if (pos + BM_GROUP > len - 2) {
                         if (sub == 0) endp[j] = len - 1;
                         live = false;
                     } else {
-                        pos += 8;
+                        pos += BM_GROUP;
                     }
                 }
             }
