@@ -101,6 +101,37 @@ __global__ void __launch_bounds__(FT_THREADS) k_blur5_band(const float* __restri
     }
 }
 
+// R outputs of a pass along one line at line indices i0 .. i0 + R - 1 (global), written to
+// out[r * ostride] for r < nvalid where the index lies in [0, len). The line's element t (global
+// index) is line[(t - origin) * stride]; the region holds indices [origin, origin + rlen). The
+// register path runs only when every output is interior and every input lies in the region.
+template <int N, int R, bool MULTI, bool LEFT_FIRST>
+__device__ __forceinline__ void pass_run(const float* line, int origin, int rlen, int stride, int len, int i0,
+                                         const float* k, float* out, int ostride, int nvalid) {
+    constexpr int NV = R + 2 * N - 2;
+    bool interior = nvalid == R && len >= 2 * N && i0 >= N && i0 + R - 1 < len - N && i0 - (N - 1) >= origin &&
+                    i0 + R - 1 + (N - 1) < origin + rlen;
+    if (interior) {
+        float v[NV];
+        const float* base = line + (i0 - (N - 1) - origin) * stride;
+#pragma unroll
+        for (int j = 0; j < NV; j++) v[j] = base[j * stride];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            float s = v[r + N - 1] * k[0];
+#pragma unroll
+            for (int j = N - 1; j >= 1; j--) s = s + (v[r + N - 1 + j] + v[r + N - 1 - j]) * k[j];
+            out[r * ostride] = s;
+        }
+    } else {
+        for (int r = 0; r < nvalid; r++) {
+            int i = i0 + r;
+            if (i < 0 || i >= len) continue;
+            out[r * ostride] = pass_elem<N, MULTI, LEFT_FIRST>(line, origin, stride, len, i, k);
+        }
+    }
+}
+
 // ---- one solver level: gradient, tensor and its blur (flow.rs:1275-1277) ---------------------------
 
 // mask (may be null): the level mask of X of a layered solve; the gradient is zero where the mask
@@ -118,9 +149,11 @@ __global__ void __launch_bounds__(FT_THREADS) k_level_init(const float* __restri
                                                            int bp, long bplane) {
     constexpr int N = 8, HALO = N - 1;
     constexpr int RW = FT_X + 2 * HALO, RH = FT_Y + 2 * HALO;
+    constexpr int RS = RW | 1, HS = FT_X | 1;  // row strides (odd: a warp's lanes on distinct rows hit distinct banks)
+    constexpr int R = 8;                        // outputs per thread of the register blocked passes
     extern __shared__ float sm[];
-    float* s_t = sm;                  // 3 x RH x RW tensor
-    float* s_h = s_t + 3 * RH * RW;   // 3 x RH x FT_X
+    float* s_t = sm;                  // 3 x RH x RS tensor
+    float* s_h = s_t + 3 * RH * RS;   // 3 x RH x HS
     int X0 = blockIdx.x * FT_X, Y0 = blockIdx.y * FT_Y;
     int gx0 = X0 - HALO, gy0 = Y0 - HALO;
     for (int e = threadIdx.x; e < RW * RH; e += blockDim.x) {
@@ -158,32 +191,49 @@ __global__ void __launch_bounds__(FT_THREADS) k_level_init(const float* __restri
                 }
             }
         }
-        s_t[e] = t0;
-        s_t[RH * RW + e] = t1;
-        s_t[2 * RH * RW + e] = t2;
+        const int se = r * RS + c;
+        s_t[se] = t0;
+        s_t[RH * RS + se] = t1;
+        s_t[2 * RH * RS + se] = t2;
     }
     __syncthreads();
-    for (int ch = 0; ch < 3; ch++)
-        region_pass<N, true, false, false>(s_t + ch * RH * RW, RW, gx0, gy0, s_h + ch * RH * FT_X, FT_X, RH, X0, gy0, w,
-                                           h, g7.k);
+    // blur7 of the tensor, register blocked (pass_run: R outputs from R + 14 inputs held in
+    // registers, each output with the interior chain, or the border rule near the image's edges):
+    // horizontal along the region's rows at the tile's columns, a lane per row
+    {
+        constexpr int NSEG = FT_X / R;
+        for (int e = threadIdx.x; e < 3 * RH * NSEG; e += blockDim.x) {
+            const int r = e % RH, rest = e / RH;
+            const int seg = rest % NSEG, ch = rest / NSEG;
+            const int Y = gy0 + r;
+            if (Y < 0 || Y >= h) continue;
+            const int c0 = seg * R;
+            pass_run<N, R, true, false>(s_t + ch * RH * RS + r * RS, gx0, RW, 1, w, X0 + c0, g7.k,
+                                        s_h + ch * RH * HS + r * HS + c0, 1, R);
+        }
+    }
     __syncthreads();
-    float* outs[3] = {a0o, a1o, a2o};
-    for (int e = threadIdx.x; e < 3 * FT_X * FT_Y; e += blockDim.x) {
-        int ch = e / (FT_X * FT_Y);
-        int q = e - ch * FT_X * FT_Y;
-        int r = q / FT_X, c = q - r * FT_X;
-        int X = X0 + c, Y = Y0 + r;
-        if (X >= w || Y >= h) continue;
-        const float* line = s_h + ch * RH * FT_X + c;
-        float v = above_first ? pass_elem<N, true, true>(line, gy0, FT_X, h, Y, g7.k)
-                              : pass_elem<N, true, false>(line, gy0, FT_X, h, Y, g7.k);
-        outs[ch][(long)Y * w + X] = v;
+    //    vertical at the tile's rows, a lane per column, into the tensor planes
+    {
+        constexpr int NSEG = FT_Y / R;
+        float* outs[3] = {a0o, a1o, a2o};
+        for (int e = threadIdx.x; e < 3 * FT_X * NSEG; e += blockDim.x) {
+            const int c = e % FT_X, rest = e / FT_X;
+            const int seg = rest % NSEG, ch = rest / NSEG;
+            const int X = X0 + c;
+            if (X >= w) continue;
+            const int r0 = seg * R;
+            const float* line = s_h + ch * RH * HS + c;
+            float* dst = (ch == 0 ? outs[0] : ch == 1 ? outs[1] : outs[2]) + (long)(Y0 + r0) * w + X;  // rows past h are never written
+            if (above_first) pass_run<N, R, true, true>(line, gy0, RH, HS, h, Y0 + r0, g7.k, dst, w, R);
+            else pass_run<N, R, true, false>(line, gy0, RH, HS, h, Y0 + r0, g7.k, dst, w, R);
+        }
     }
 }
 
 size_t level_init_smem() {
     constexpr int RW = FT_X + 14, RH = FT_Y + 14;
-    return sizeof(float) * (3 * RH * RW + 3 * RH * FT_X);
+    return sizeof(float) * (3 * RH * (RW | 1) + 3 * RH * (FT_X | 1));
 }
 
 // ---- one solver iteration (flow.rs:1278-1282): calc_b, blur7 of B, new_disp, blur5 of the flow -----
@@ -220,37 +270,6 @@ struct IterGeom {
     static constexpr size_t SMEM = sizeof(float) * (BUF1 + BUF2);
     static_assert(2 * DH * DS <= BUF1 && 2 * DH * FS <= BUF2 && 2 * TX * TY <= BUF1, "the reused buffers must fit");
 };
-
-// R outputs of a pass along one line at line indices i0 .. i0 + R - 1 (global), written to
-// out[r * ostride] for r < nvalid where the index lies in [0, len). The line's element t (global
-// index) is line[(t - origin) * stride]; the region holds indices [origin, origin + rlen). The
-// register path runs only when every output is interior and every input lies in the region.
-template <int N, int R, bool MULTI, bool LEFT_FIRST>
-__device__ __forceinline__ void pass_run(const float* line, int origin, int rlen, int stride, int len, int i0,
-                                         const float* k, float* out, int ostride, int nvalid) {
-    constexpr int NV = R + 2 * N - 2;
-    bool interior = nvalid == R && len >= 2 * N && i0 >= N && i0 + R - 1 < len - N && i0 - (N - 1) >= origin &&
-                    i0 + R - 1 + (N - 1) < origin + rlen;
-    if (interior) {
-        float v[NV];
-        const float* base = line + (i0 - (N - 1) - origin) * stride;
-#pragma unroll
-        for (int j = 0; j < NV; j++) v[j] = base[j * stride];
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-            float s = v[r + N - 1] * k[0];
-#pragma unroll
-            for (int j = N - 1; j >= 1; j--) s = s + (v[r + N - 1 + j] + v[r + N - 1 - j]) * k[j];
-            out[r * ostride] = s;
-        }
-    } else {
-        for (int r = 0; r < nvalid; r++) {
-            int i = i0 + r;
-            if (i < 0 || i >= len) continue;
-            out[r * ostride] = pass_elem<N, MULTI, LEFT_FIRST>(line, origin, stride, len, i, k);
-        }
-    }
-}
 
 template <int TX, int TY>
 __device__ __forceinline__ void level_iter_body(const float* __restrict__ b_in, int bp, long bplane,
