@@ -110,7 +110,14 @@ int fill_dev(tw_ctx* ctx, void* img, int W, int H, int fmt, const uint8_t* holes
     float* base = fb.as<float>();
     float* ta = base + o_ta;
     LAUNCH(ctx, k_fill_load, grid1(n0), TB, 0, img, fmt, holes, base + offs[0], n0, any);
-    for (int k = 1; k <= g.top; k++) {  // pull: blur5 and the resample of the values and the weights
+    // the coarse levels k0 .. top (every stack of them fits one block's shared memory) run in one
+    // launch, k_fill_coarse: the finest such level k0 >= 1 is built by the pull below, the launch
+    // pulls on from it, pushes down to it and leaves the push's level k0 - 1 in the solution planes
+    int k0 = g.top + 1;
+    for (int k = 1; k <= g.top; k++)
+        if (fill_coarse_floats(g.dims, k, g.top, np, nc) <= FILL_COARSE_MAX_FLOATS) { k0 = k; break; }
+    const int pull_to = k0 <= g.top ? k0 : g.top;
+    for (int k = 1; k <= pull_to; k++) {  // pull: blur5 and the resample of the values and the weights
         int pw = g.dims[k - 1][0], ph = g.dims[k - 1][1], cw = g.dims[k][0], chh = g.dims[k][1];
         long pn = (long)pw * ph;
         // the level k - 1 planes stay for the push: blur a copy
@@ -121,11 +128,33 @@ int fill_dev(tw_ctx* ctx, void* img, int W, int H, int fmt, const uint8_t* holes
     }
     float* sol = base + o_sa;
     float* nxt = base + o_sb;
-    {
+    int push_from = g.top;
+    if (k0 <= g.top) {
+        FillCoarseJob J{};
+        J.s_k0 = base + offs[k0];
+        J.out = sol;
+        for (int k = 0; k <= g.top; k++) {
+            J.dims[k][0] = g.dims[k][0];
+            J.dims[k][1] = g.dims[k][1];
+        }
+        J.k0 = k0;
+        J.top = g.top;
+        J.np = np;
+        J.nc = nc;
+        J.rule = rule;
+        J.above_first = above_first;
+        J.b5 = ctx->b5;
+        J.g5 = ctx->g5;
+        J.any = any;
+        // the stack of level k0 read, the push's level k0 - 1 written
+        double b = 4.0 * ((double)np * g.dims[k0][0] * g.dims[k0][1] + (double)nc * g.dims[k0 - 1][0] * g.dims[k0 - 1][1]);
+        LAUNCHB(ctx, b, k_fill_coarse, 1, FILL_COARSE_THREADS, fill_coarse_floats(g.dims, k0, g.top, np, nc) * sizeof(float), J);
+        push_from = k0 - 1;
+    } else {
         long tn = (long)g.dims[g.top][0] * g.dims[g.top][1];
         LAUNCH(ctx, k_stack_zero, grid1(nc * tn), TB, 0, sol, nc * tn, any);
     }
-    for (int lv = g.top; lv >= 0; lv--) {  // push
+    for (int lv = push_from; lv >= 0; lv--) {  // push
         int lw = g.dims[lv][0], lh = g.dims[lv][1];
         long ln = (long)lw * lh;
         LAUNCH(ctx, k_fill_combine, grid1(ln), TB, 0, sol, base + offs[lv], ln, nc, rule, any);

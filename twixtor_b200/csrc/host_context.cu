@@ -228,6 +228,9 @@ int tw_open(int device, tw_ctx** out) {
                                  (int)level_iter_smem(LEVEL_TILE_64x64));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_solve_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem_bytes());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fill_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(FILL_COARSE_MAX_FLOATS * sizeof(float)));
     // the fast mode's builds of the same kernels
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(fast::k_bm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bm_smem_bytes(BM_MAX_LINE));

@@ -234,6 +234,23 @@ __global__ void k_fill_store(void* __restrict__ img, int fmt, const float* __res
                              const int* __restrict__ any_hole);
 __global__ void k_stack_zero(float* __restrict__ p, long n, const int* __restrict__ any_hole);
 __global__ void k_hole_side1(const int* __restrict__ any_hole, int* __restrict__ flag);
+// The coarse levels of the pull-push fill in one block: the pull from level k0 (its stack given,
+// np planes) up to the top level and the push from the top down to level k0, every stack of those
+// levels in shared memory; the push's result resampled to level k0 - 1 goes to out (nc planes of
+// that level). Level sizes as the fill's geometry (holefill.rs:140-171). fill_coarse_floats: the
+// shared memory it needs, in floats.
+constexpr int FILL_COARSE_THREADS = 1024;
+constexpr int FILL_COARSE_MAX_FLOATS = 50 * 1024;  // 200 KB
+struct FillCoarseJob {
+    const float* s_k0;
+    float* out;
+    int dims[40][2];
+    int k0, top, np, nc, rule, above_first;
+    Taps b5, g5;
+    const int* any;
+};
+__global__ void k_fill_coarse(FillCoarseJob J);
+long fill_coarse_floats(const int dims[][2], int k0, int top, int np, int nc);
 
 __global__ void k_encode_vectors(const float* __restrict__ flow, int fw, int fh, void* __restrict__ out, int W, int H,
                                  int fmt, float sx, float sy, float kx, float ky, int zero);

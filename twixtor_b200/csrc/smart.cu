@@ -272,14 +272,10 @@ __device__ __forceinline__ float border1(const float* line, long stride, int len
     return Ar<R>::div(num, den);
 }
 
-// One pass of the 1 channel convolution over a stack of planes (conv.rs:141-190, :268-301).
+// One element (x, y) of one pass of the 1 channel convolution of a plane s into d (conv.rs:141-190,
+// :268-301).
 template <bool R, int N, bool VERT, bool ABOVE_FIRST>
-__device__ __forceinline__ void stack_pass(const float* __restrict__ src, float* __restrict__ dst, int w, int h,
-                                           long pstride, const Taps& t) {
-    int x = blockIdx.x * blockDim.x + threadIdx.x;
-    int y = blockIdx.y;
-    if (x >= w || y >= h) return;
-    const float* s = src + blockIdx.z * pstride;
+__device__ __forceinline__ float stack_pass_px(const float* __restrict__ s, int w, int h, int x, int y, const Taps& t) {
     float r;
     if (!VERT) {
         const float* row = s + (long)y * w;
@@ -301,7 +297,18 @@ __device__ __forceinline__ void stack_pass(const float* __restrict__ src, float*
             r = border1<R, ABOVE_FIRST, N>(col, w, h, y, t.k);
         }
     }
-    dst[blockIdx.z * pstride + (long)y * w + x] = r;
+    return r;
+}
+
+// One pass over a stack of planes, one element per thread (plane blockIdx.z).
+template <bool R, int N, bool VERT, bool ABOVE_FIRST>
+__device__ __forceinline__ void stack_pass(const float* __restrict__ src, float* __restrict__ dst, int w, int h,
+                                           long pstride, const Taps& t) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    dst[blockIdx.z * pstride + (long)y * w + x] =
+        stack_pass_px<R, N, VERT, ABOVE_FIRST>(src + blockIdx.z * pstride, w, h, x, y, t);
 }
 
 template <bool R, int N>
@@ -324,24 +331,30 @@ __global__ void k_stack_pass(const float* __restrict__ src, float* __restrict__ 
     }
 }
 
-// flow/sample.rs:91-112 over a stack (the lerps over the arithmetic set)
+// flow/sample.rs:91-112 at element (x, y) of a dw x dh plane from the sw x sh plane s (the lerps
+// over the arithmetic set)
 template <bool R>
-__device__ __forceinline__ void stack_resample(const float* __restrict__ src, int sw, int sh, long sstride,
-                                               float* __restrict__ dst, int dw, int dh, long dstride) {
-    int x = blockIdx.x * blockDim.x + threadIdx.x;
-    int y = blockIdx.y;
-    if (x >= dw || y >= dh) return;
+__device__ __forceinline__ float stack_resample_px(const float* __restrict__ s, int sw, int sh, int dw, int dh, int x,
+                                                   int y) {
     float sx = ((float)sw - 1.0f) / (float)(dw - 1);
     float sy = ((float)sh - 1.0f) / (float)(dh - 1);
     int ix, iy;
     float fx, fy;
     cell((float)x * sx, sw, ix, fx);
     cell((float)y * sy, sh, iy, fy);
-    const float* s = src + blockIdx.z * sstride;
     long i = (long)iy * sw + ix;
     float top = lerp_r<R>(s[i], s[i + 1], fx);
     float bot = lerp_r<R>(s[i + sw], s[i + sw + 1], fx);
-    dst[blockIdx.z * dstride + (long)y * dw + x] = lerp_r<R>(top, bot, fy);
+    return lerp_r<R>(top, bot, fy);
+}
+
+template <bool R>
+__device__ __forceinline__ void stack_resample(const float* __restrict__ src, int sw, int sh, long sstride,
+                                               float* __restrict__ dst, int dw, int dh, long dstride) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y;
+    if (x >= dw || y >= dh) return;
+    dst[blockIdx.z * dstride + (long)y * dw + x] = stack_resample_px<R>(src + blockIdx.z * sstride, sw, sh, dw, dh, x, y);
 }
 
 __global__ void k_stack_resample(const float* __restrict__ src, int sw, int sh, long sstride, float* __restrict__ dst,
@@ -363,6 +376,102 @@ __global__ void k_fill_combine(float* __restrict__ sol, const float* __restrict_
         for (int c = 0; c < nc; c++)
             sol[c * n + i] = rule ? Ar<true>::div(vals[c * n + i], wt) : Ar<false>::div(vals[c * n + i], wt);
     }
+}
+
+// ---- the coarse levels of the fill in one block ------------------------------------------------------
+
+long fill_coarse_floats(const int dims[][2], int k0, int top, int np, int nc) {
+    long f = 0;
+    for (int k = k0; k <= top; k++) f += (long)np * dims[k][0] * dims[k][1];  // the stacks
+    long n0 = (long)dims[k0][0] * dims[k0][1];
+    return f + 2 * np * n0 + 2 * nc * n0;  // two pass scratches, the solution and the next one
+}
+
+// holefill.rs:260-377 over the levels k0 .. top, the same elements as the stack kernels (the pull's
+// blur5 and resample, the push's combine, Gaussian r5 and resample), block barriers between them.
+// The pull reads level k - 1 directly (the stack kernels blur a copy, which keeps it for the push;
+// here the blur writes scratch planes and the level stays as it is).
+template <bool R>
+__device__ void fill_coarse_body(const FillCoarseJob& J, float* fsm) {
+    const int np = J.np, nc = J.nc, k0 = J.k0, top = J.top;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    auto n_of = [&](int k) { return J.dims[k][0] * J.dims[k][1]; };
+    auto stack_at = [&](int k) {
+        float* p = fsm;
+        for (int j = k0; j < k; j++) p += np * n_of(j);
+        return p;
+    };
+    const int n0 = n_of(k0);
+    float* T = stack_at(top + 1);
+    float* U = T + np * n0;
+    float* sol = U + np * n0;
+    float* nxt = sol + nc * n0;
+    for (int i = tid; i < np * n0; i += nt) fsm[i] = J.s_k0[i];
+    __syncthreads();
+    // pull: blur5 of level k - 1 (horizontal into U, vertical into T), resampled into level k
+    for (int k = k0 + 1; k <= top; k++) {
+        const int pw = J.dims[k - 1][0], ph = J.dims[k - 1][1], cw = J.dims[k][0], chh = J.dims[k][1];
+        const int pn = pw * ph, cn = cw * chh;
+        const float* P = stack_at(k - 1);
+        float* C = stack_at(k);
+        for (int i = tid; i < np * pn; i += nt) {
+            const int pl = i / pn, e = i - pl * pn, y = e / pw, x = e - y * pw;
+            U[i] = stack_pass_px<R, 3, false, false>(P + pl * pn, pw, ph, x, y, J.b5);
+        }
+        __syncthreads();
+        for (int i = tid; i < np * pn; i += nt) {
+            const int pl = i / pn, e = i - pl * pn, y = e / pw, x = e - y * pw;
+            T[i] = J.above_first ? stack_pass_px<R, 3, true, true>(U + pl * pn, pw, ph, x, y, J.b5)
+                                 : stack_pass_px<R, 3, true, false>(U + pl * pn, pw, ph, x, y, J.b5);
+        }
+        __syncthreads();
+        for (int i = tid; i < np * cn; i += nt) {
+            const int pl = i / cn, e = i - pl * cn, y = e / cw, x = e - y * cw;
+            C[i] = stack_resample_px<R>(T + pl * pn, pw, ph, cw, chh, x, y);
+        }
+        __syncthreads();
+    }
+    // push: the solution starts at zero on the top level
+    for (int i = tid; i < nc * n_of(top); i += nt) sol[i] = 0.0f;
+    __syncthreads();
+    for (int lv = top; lv >= k0; lv--) {
+        const int lw = J.dims[lv][0], lh = J.dims[lv][1], ln = lw * lh;
+        const float* V = stack_at(lv);
+        for (int i = tid; i < ln; i += nt) {  // holefill.rs:371-377
+            const float wt = V[nc * ln + i];
+            if (wt != 0.0f)
+                for (int c = 0; c < nc; c++) sol[c * ln + i] = Ar<R>::div(V[c * ln + i], wt);
+        }
+        __syncthreads();
+        for (int i = tid; i < nc * ln; i += nt) {
+            const int pl = i / ln, e = i - pl * ln, y = e / lw, x = e - y * lw;
+            U[i] = stack_pass_px<R, 6, false, false>(sol + pl * ln, lw, lh, x, y, J.g5);
+        }
+        __syncthreads();
+        for (int i = tid; i < nc * ln; i += nt) {
+            const int pl = i / ln, e = i - pl * ln, y = e / lw, x = e - y * lw;
+            sol[i] = J.above_first ? stack_pass_px<R, 6, true, true>(U + pl * ln, lw, lh, x, y, J.g5)
+                                   : stack_pass_px<R, 6, true, false>(U + pl * ln, lw, lh, x, y, J.g5);
+        }
+        __syncthreads();
+        const int dw = J.dims[lv - 1][0], dh = J.dims[lv - 1][1], dn = dw * dh;
+        float* dst = lv > k0 ? nxt : J.out;  // level k0 - 1 is the host's to push further
+        for (int i = tid; i < nc * dn; i += nt) {
+            const int pl = i / dn, e = i - pl * dn, y = e / dw, x = e - y * dw;
+            dst[i] = stack_resample_px<R>(sol + pl * ln, lw, lh, dw, dh, x, y);
+        }
+        __syncthreads();
+        float* t = sol;
+        sol = nxt;
+        nxt = t;
+    }
+}
+
+__global__ void __launch_bounds__(FILL_COARSE_THREADS) k_fill_coarse(FillCoarseJob J) {
+    if (!*J.any) return;
+    extern __shared__ float fsm[];
+    if (J.rule) fill_coarse_body<true>(J, fsm);
+    else fill_coarse_body<false>(J, fsm);
 }
 
 // holefill.rs:379-404 (+ the f32 bit copy): the filled channels back into the engine image
