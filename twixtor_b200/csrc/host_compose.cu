@@ -312,7 +312,11 @@ int forward_warp_dev(tw_ctx* ctx, const void* src, const float* flow, int fw, in
     R.longq = ctx->fw_longq.as<uint32_t>();
     long tris = 2L * (W - 1) * (H - 1);
     unsigned gt = (unsigned)((tris + 127) / 128);
-    LAUNCH(ctx, k_fw_count, gt, 128, 0, R);
+    // algorithmic bytes: the vertices (20 per source pixel) read by the two scan conversions; the hit
+    // list (key and colour, 20 per hit) written by the emit and read by the resolve, which writes the
+    // output pixel and its coverage
+    const double vbytes = 20.0 * W * H;
+    LAUNCHB(ctx, vbytes, k_fw_count, gt, 128, 0, R);
     LAUNCH(ctx, k_scan_block, (unsigned)nb, 256, 0, R.cnt, R.off, n, ctx->fw_sums.as<uint32_t>(), (uint32_t*)(ff + FW_MAXC));
     LAUNCH(ctx, k_scan_sums, 1, 1024, 0, ctx->fw_sums.as<uint32_t>(), nb, (unsigned long long*)(ff + FW_TOTAL));
     LAUNCH(ctx, k_scan_add, grid1(n), TB, 0, R.off, n, ctx->fw_sums.as<uint32_t>());
@@ -335,9 +339,9 @@ int forward_warp_dev(tw_ctx* ctx, const void* src, const float* flow, int fw, in
     R.cols = ctx->fw_cols.as<float4>();
     R.scratch = maxc > 4096 ? ctx->fw_scratch.as<uint2>() : nullptr;
     R.total = (uint32_t)total;
-    LAUNCH(ctx, k_fw_emit, gt, 128, 0, R);
+    LAUNCHB(ctx, vbytes + 20.0 * (double)total, k_fw_emit, gt, 128, 0, R);
     // 5. the running mean of every pixel in triangle order, the depth conversion, the coverage
-    LAUNCH(ctx, k_fw_resolve, grid1(n), TB, 0, R);
+    LAUNCHB(ctx, 20.0 * (double)total + 17.0 * W * H, k_fw_resolve, grid1(n), TB, 0, R);
     LAUNCH(ctx, k_fw_resolve_long, 296, 512, FW_LONG_SMEM_BYTES, R);
     CHECK(ctx->cuda(cudaMemcpyAsync(hf, ff, sizeof hf, cudaMemcpyDeviceToHost, ctx->cur), "flags"));
     CHECK(ctx->cuda(cudaStreamSynchronize(ctx->cur), "kernel execution"));
