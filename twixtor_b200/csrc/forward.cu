@@ -310,9 +310,9 @@ struct Edge {
 // raster.rs:61-86; channels 0..2 run the arithmetic `a`, channel 3 the arithmetic `b`
 __device__ __forceinline__ void edge_init(const Vt& a, const Vt& b, float y, Edge e[2], int& count, Ar aa, Ar ab) {
     if (a.y <= y && y < b.y) {
-        int slot = count != 0 ? 1 : 0;
+        const bool second = count != 0;
         count += 1;
-        Edge& s = e[slot];
+        Edge s;
         float dx = b.x - a.x;
         float inv = 1.0f / (b.y - a.y);
         float t = ((y - 1.0f) - a.y) * inv;
@@ -327,6 +327,10 @@ __device__ __forceinline__ void edge_init(const Vt& a, const Vt& b, float y, Edg
             s.p[q] = A.add(A.mul(dq, t), a.p[q]);
             s.dp[q] = A.mul(dq, inv);
         }
+        // a constant index on both sides: the two edges stay in registers (a runtime index would
+        // put them in local memory)
+        if (second) e[1] = s;
+        else e[0] = s;
     }
 }
 
@@ -372,14 +376,21 @@ __device__ __forceinline__ void sort3(const Vt* v, Vt* o) {  // raster.rs:90-113
         if (y0 < y2) { a = 0; b = 2; c = 1; }
         else { a = 2; b = 0; c = 1; }
     } else { a = 0; b = 1; c = 2; }
-    o[0] = v[a];
-    o[1] = v[b];
-    o[2] = v[c];
+    // copies by constant indices (v[a] with a runtime a would put the vertices in local memory)
+    auto pick = [&](int k, Vt& d) {
+        d.x = k == 0 ? v[0].x : k == 1 ? v[1].x : v[2].x;
+        d.y = k == 0 ? v[0].y : k == 1 ? v[1].y : v[2].y;
+#pragma unroll
+        for (int q = 0; q < 4; q++) d.p[q] = k == 0 ? v[0].p[q] : k == 1 ? v[1].p[q] : v[2].p[q];
+    };
+    pick(a, o[0]);
+    pick(b, o[1]);
+    pick(c, o[2]);
 }
 
 // raster.rs:171-300
 template <typename Sink>
-__device__ void triangle(const Vt* t, int w1, int h1, Ar aa, Ar ab, Sink& sink) {
+__device__ __forceinline__ void triangle(const Vt* t, int w1, int h1, Ar aa, Ar ab, Sink& sink) {
     float w1f = (float)w1, h1f = (float)h1;
     bool ok = (0.0f <= t[0].x || 0.0f <= t[1].x || 0.0f <= t[2].x) && (0.0f <= t[0].y || 0.0f <= t[1].y || 0.0f <= t[2].y) &&
               (t[0].x <= w1f || t[1].x <= w1f || t[2].x <= w1f) && (t[0].y <= h1f || t[1].y <= h1f || t[2].y <= h1f);
@@ -396,7 +407,7 @@ __device__ void triangle(const Vt* t, int w1, int h1, Ar aa, Ar ab, Sink& sink) 
         for (;;) {  // at most h rows: y advances by 1 from >= 0 to <= h1
             if (vi < 3) {
                 for (;;) {
-                    if (y < vs[vi].y) break;
+                    if (y < (vi == 0 ? vs[0].y : vi == 1 ? vs[1].y : vs[2].y)) break;
                     if (count == 1) {
                         if (e[0].ay <= y && e[0].by <= y) count = 0;
                     } else if (count == 2) {
@@ -411,9 +422,18 @@ __device__ void triangle(const Vt* t, int w1, int h1, Ar aa, Ar ab, Sink& sink) 
                             count = 1;
                         }
                     }
-                    const int ia[3] = {0, 1, 2}, ib[3] = {1, 2, 0}, ic[3] = {2, 0, 1};
-                    edge_init(vs[ia[vi]], vs[ib[vi]], y, e, count, aa, ab);
-                    edge_init(vs[ia[vi]], vs[ic[vi]], y, e, count, aa, ab);
+                    // the edges from vertex vi to the next two (vi, vi + 1), (vi, vi + 2) mod 3, with
+                    // constant indices per case
+                    if (vi == 0) {
+                        edge_init(vs[0], vs[1], y, e, count, aa, ab);
+                        edge_init(vs[0], vs[2], y, e, count, aa, ab);
+                    } else if (vi == 1) {
+                        edge_init(vs[1], vs[2], y, e, count, aa, ab);
+                        edge_init(vs[1], vs[0], y, e, count, aa, ab);
+                    } else {
+                        edge_init(vs[2], vs[0], y, e, count, aa, ab);
+                        edge_init(vs[2], vs[1], y, e, count, aa, ab);
+                    }
                     vi += 1;
                     if (vi >= 3) break;
                 }
@@ -428,12 +448,18 @@ __device__ void triangle(const Vt* t, int w1, int h1, Ar aa, Ar ab, Sink& sink) 
                 }
             }
             if (count == 2) {
-                const Edge& l = e[1].x < e[0].x ? e[1] : e[0];
-                const Edge& r = e[1].x < e[0].x ? e[0] : e[1];
-                int x0 = max(cvtt32(ceilf(l.x)), 0);
-                int x1 = min(cvtt32(floorf(r.x)), w1);
-                float wid = r.x - l.x;
-                if (x0 <= x1 && (double)wid > 1e-08) run(x0, x1, l.x, wid, l.p, r.p, cvtt32(y), false, w1, h1, aa, ab, sink);
+                const bool sw = e[1].x < e[0].x;  // the left edge is e[1]
+                const float lx = sw ? e[1].x : e[0].x, rx = sw ? e[0].x : e[1].x;
+                float lp[4], rp[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    lp[q] = sw ? e[1].p[q] : e[0].p[q];
+                    rp[q] = sw ? e[0].p[q] : e[1].p[q];
+                }
+                int x0 = max(cvtt32(ceilf(lx)), 0);
+                int x1 = min(cvtt32(floorf(rx)), w1);
+                float wid = rx - lx;
+                if (x0 <= x1 && (double)wid > 1e-08) run(x0, x1, lx, wid, lp, rp, cvtt32(y), false, w1, h1, aa, ab, sink);
             }
             y += 1.0f;
             if (!(y <= y_end)) break;
@@ -442,15 +468,21 @@ __device__ void triangle(const Vt* t, int w1, int h1, Ar aa, Ar ab, Sink& sink) 
     const Vt& mid = vs[1];
     const Vt& bot = vs[2];
     if (mid.y == h1f && mid.y == bot.y) {
-        const Vt& l = bot.x <= mid.x ? bot : mid;
-        const Vt& r = bot.x <= mid.x ? mid : bot;
-        float yy = l.y;
+        const bool bl = bot.x <= mid.x;  // the left vertex is bot
+        const float lx = bl ? bot.x : mid.x, rx = bl ? mid.x : bot.x;
+        float lp[4], rp[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            lp[q] = bl ? bot.p[q] : mid.p[q];
+            rp[q] = bl ? mid.p[q] : bot.p[q];
+        }
+        float yy = bl ? bot.y : mid.y;
         float yt = (float)cvtt32(yy);
         if (0.0f <= yt && yt <= h1f && !((double)(yy - yt) > 0.01)) {
-            int x0 = max(cvtt32(ceilf(l.x)), 0);
-            int x1 = min(cvtt32(floorf(r.x)), w1);
-            float wid = r.x - l.x;
-            if ((double)wid > 1e-05) run(x0, x1, l.x, wid, l.p, r.p, cvtt32(yt), true, w1, h1, aa, ab, sink);
+            int x0 = max(cvtt32(ceilf(lx)), 0);
+            int x1 = min(cvtt32(floorf(rx)), w1);
+            float wid = rx - lx;
+            if ((double)wid > 1e-05) run(x0, x1, lx, wid, lp, rp, cvtt32(yt), true, w1, h1, aa, ab, sink);
         }
     }
 }
@@ -490,6 +522,33 @@ struct EmitSink {
     __device__ void outside() { atomicOr(R.outside, 1); }
 };
 
+// The Gouraud variant's sink: the hit's interpolated colours; its pointers copied out of the kernel
+// parameters (a reference to them, which the textured sink's mip level table needs, makes every
+// thread copy the whole parameter block to local memory)
+struct EmitSinkG {
+    uint32_t* fill;
+    const uint32_t* cnt;
+    const uint32_t* off;
+    uint32_t* keys;
+    float4* cols;
+    int* bad;
+    int* out_flag;
+    int w;
+    uint32_t tri;
+    __device__ void hit(int x, int y, const float* p) {
+        long px = (long)y * w + x;
+        uint32_t k = atomicAdd(&fill[px], 1u);
+        if (k >= cnt[px]) {  // the count pass saw fewer hits: never expected, never written
+            atomicOr(bad, 2);
+            return;
+        }
+        uint32_t slot = off[px] + k;
+        keys[slot] = tri;
+        cols[slot] = make_float4(p[0], p[1], p[2], p[3]);
+    }
+    __device__ void outside() { atomicOr(out_flag, 1); }
+};
+
 template <typename P>
 __device__ __forceinline__ void load_vertex(const FwRaster& R, int r, int c, Vt& v) {
     long i = (long)r * R.w + c;
@@ -507,7 +566,8 @@ __device__ __forceinline__ void load_vertex(const FwRaster& R, int r, int c, Vt&
     }
 }
 
-template <typename P, bool EMIT>
+// MODE 0: the count pass; 1: the emit of the Gouraud variant; 2: the emit of the textured variant
+template <typename P, int MODE>
 __device__ __forceinline__ void raster_one(const FwRaster& R) {
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     long cells = (long)(R.w - 1) * (R.h - 1);
@@ -533,8 +593,11 @@ __device__ __forceinline__ void raster_one(const FwRaster& R) {
         nb = nb || isnan(v[k].p[3]);
     }
     Ar aa{na}, ab{nb};
-    if (EMIT) {
+    if (MODE == 2) {
         EmitSink<P> s{R, (uint32_t)t};
+        triangle(v, R.w - 1, R.h - 1, aa, ab, s);
+    } else if (MODE == 1) {
+        EmitSinkG s{R.fill, R.cnt, R.off, R.keys, R.cols, R.bad, R.outside, R.w, (uint32_t)t};
         triangle(v, R.w - 1, R.h - 1, aa, ab, s);
     } else {
         CountSink s{R.cnt, R.w, R.outside};
@@ -543,15 +606,23 @@ __device__ __forceinline__ void raster_one(const FwRaster& R) {
 }
 
 __global__ void __launch_bounds__(128) k_fw_count(FwRaster R) {
-    if (R.fmt == 0) raster_one<uint8_t, false>(R);
-    else if (R.fmt == 1) raster_one<uint16_t, false>(R);
-    else raster_one<float, false>(R);
+    if (R.fmt == 0) raster_one<uint8_t, 0>(R);
+    else if (R.fmt == 1) raster_one<uint16_t, 0>(R);
+    else raster_one<float, 0>(R);
 }
 
-__global__ void __launch_bounds__(128) k_fw_emit(FwRaster R) {
-    if (R.fmt == 0) raster_one<uint8_t, true>(R);
-    else if (R.fmt == 1) raster_one<uint16_t, true>(R);
-    else raster_one<float, true>(R);
+// the emit of the Gouraud variant (R.pyramid false)
+__global__ void __launch_bounds__(128, 4) k_fw_emit(FwRaster R) {
+    if (R.fmt == 0) raster_one<uint8_t, 1>(R);
+    else if (R.fmt == 1) raster_one<uint16_t, 1>(R);
+    else raster_one<float, 1>(R);
+}
+
+// the emit of the textured variant (R.pyramid true)
+__global__ void __launch_bounds__(128, 4) k_fw_emit_tex(FwRaster R) {
+    if (R.fmt == 0) raster_one<uint8_t, 2>(R);
+    else if (R.fmt == 1) raster_one<uint16_t, 2>(R);
+    else raster_one<float, 2>(R);
 }
 
 // ---- the exclusive scan of the per pixel counts ---------------------------------------------------------

@@ -339,7 +339,8 @@ int forward_warp_dev(tw_ctx* ctx, const void* src, const float* flow, int fw, in
     R.cols = ctx->fw_cols.as<float4>();
     R.scratch = maxc > 4096 ? ctx->fw_scratch.as<uint2>() : nullptr;
     R.total = (uint32_t)total;
-    LAUNCHB(ctx, vbytes + 20.0 * (double)total, k_fw_emit, gt, 128, 0, R);
+    if (R.pyramid) LAUNCHB(ctx, vbytes + 20.0 * (double)total, k_fw_emit_tex, gt, 128, 0, R);
+    else LAUNCHB(ctx, vbytes + 20.0 * (double)total, k_fw_emit, gt, 128, 0, R);
     // 5. the running mean of every pixel in triangle order, the depth conversion, the coverage
     LAUNCHB(ctx, 20.0 * (double)total + 17.0 * W * H, k_fw_resolve, grid1(n), TB, 0, R);
     LAUNCH(ctx, k_fw_resolve_long, 296, 512, FW_LONG_SMEM_BYTES, R);

@@ -331,7 +331,8 @@ __global__ void k_fwp_blur(const void* __restrict__ in, void* __restrict__ out, 
 __global__ void k_fwp_resample(const void* __restrict__ src, int sw, int sh, void* __restrict__ dst, int dw, int dh,
                                int fmt);
 __global__ void k_fw_count(FwRaster R);
-__global__ void k_fw_emit(FwRaster R);
+__global__ void k_fw_emit(FwRaster R);      // the Gouraud variant
+__global__ void k_fw_emit_tex(FwRaster R);  // the textured variant (R.pyramid)
 constexpr int FW_SCAN_BLOCK = 2048;
 __global__ void k_scan_block(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long n,
                              uint32_t* __restrict__ sums, uint32_t* __restrict__ maxc);
