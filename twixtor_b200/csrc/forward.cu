@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(128) k_fw_count(FwRaster R) {
 }
 
 // the emit of the Gouraud variant (R.pyramid false)
-__global__ void __launch_bounds__(128, 4) k_fw_emit(FwRaster R) {
+__global__ void __launch_bounds__(128, 6) k_fw_emit(FwRaster R) {
     if (R.fmt == 0) raster_one<uint8_t, 1>(R);
     else if (R.fmt == 1) raster_one<uint16_t, 1>(R);
     else raster_one<float, 1>(R);
