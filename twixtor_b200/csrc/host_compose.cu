@@ -72,13 +72,12 @@ FillGeo fill_geometry(int w, int h) {  // holefill.rs:140-171
     return g;
 }
 
-// one blur of a stack of planes: the horizontal pass into tmp, the vertical one back
-void fill_passes(tw_ctx* ctx, float* src_dst, float* tmp, int w, int h, long stride, int planes, const Taps& t, int n,
-                 bool above_first, int rule, const int* any) {
-    dim3 g((unsigned)((w + TB - 1) / TB), (unsigned)h, (unsigned)planes);
+// one blur of a stack of planes, out of place (src stays as it is): both passes in one tiled launch
+void fill_blur(tw_ctx* ctx, const float* src, float* dst, int w, int h, long stride, int planes, const Taps& t, int n,
+               bool above_first, int rule, const int* any) {
+    dim3 g((unsigned)((w + 31) / 32), (unsigned)((h + 31) / 32), (unsigned)planes);
     double pb = 8.0 * w * h * planes;  // every plane read once and written once
-    LAUNCHB(ctx, pb, k_stack_pass, g, TB, 0, src_dst, tmp, w, h, stride, t, n, 0, rule, any);
-    LAUNCHB(ctx, pb, k_stack_pass, g, TB, 0, tmp, src_dst, w, h, stride, t, n, above_first ? 2 : 1, rule, any);
+    LAUNCHB(ctx, pb, k_stack_blur, g, 256, 0, src, dst, w, h, stride, t, n, above_first ? 1 : 0, rule, any);
 }
 
 void fill_resample(tw_ctx* ctx, const float* src, int sw, int sh, float* dst, int dw, int dh, int planes, int rule,
@@ -120,10 +119,8 @@ int fill_dev(tw_ctx* ctx, void* img, int W, int H, int fmt, const uint8_t* holes
     for (int k = 1; k <= pull_to; k++) {  // pull: blur5 and the resample of the values and the weights
         int pw = g.dims[k - 1][0], ph = g.dims[k - 1][1], cw = g.dims[k][0], chh = g.dims[k][1];
         long pn = (long)pw * ph;
-        // the level k - 1 planes stay for the push: blur a copy
-        CHECK(ctx->cuda(cudaMemcpyAsync(ta, base + offs[k - 1], np * pn * sizeof(float), cudaMemcpyDeviceToDevice, ctx->cur),
-                        "fill copy"));
-        fill_passes(ctx, ta, base + o_sa, pw, ph, pn, np, ctx->b5, 3, above_first, rule, any);
+        // the level k - 1 planes stay for the push: the blur writes ta
+        fill_blur(ctx, base + offs[k - 1], ta, pw, ph, pn, np, ctx->b5, 3, above_first, rule, any);
         fill_resample(ctx, ta, pw, ph, base + offs[k], cw, chh, np, rule, any);
     }
     float* sol = base + o_sa;
@@ -158,11 +155,12 @@ int fill_dev(tw_ctx* ctx, void* img, int W, int H, int fmt, const uint8_t* holes
         int lw = g.dims[lv][0], lh = g.dims[lv][1];
         long ln = (long)lw * lh;
         LAUNCH(ctx, k_fill_combine, grid1(ln), TB, 0, sol, base + offs[lv], ln, nc, rule, any);
-        fill_passes(ctx, sol, ta, lw, lh, ln, nc, ctx->g5, 6, above_first, rule, any);
+        fill_blur(ctx, sol, ta, lw, lh, ln, nc, ctx->g5, 6, above_first, rule, any);  // the blurred solution in ta
         if (lv == 0) {
-            LAUNCH(ctx, k_fill_combine, grid1(ln), TB, 0, sol, base + offs[0], ln, nc, rule, any);
+            LAUNCH(ctx, k_fill_combine, grid1(ln), TB, 0, ta, base + offs[0], ln, nc, rule, any);
+            sol = ta;
         } else {
-            fill_resample(ctx, sol, lw, lh, nxt, g.dims[lv - 1][0], g.dims[lv - 1][1], nc, rule, any);
+            fill_resample(ctx, ta, lw, lh, nxt, g.dims[lv - 1][0], g.dims[lv - 1][1], nc, rule, any);
             std::swap(sol, nxt);
         }
     }

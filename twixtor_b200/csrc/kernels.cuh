@@ -226,6 +226,10 @@ __global__ void k_fill_load(const void* __restrict__ img, int fmt, const uint8_t
 // first; rule: the NaN rule arithmetic (float images)
 __global__ void k_stack_pass(const float* __restrict__ src, float* __restrict__ dst, int w, int h, long pstride, Taps t,
                              int n, int dir, int rule, const int* __restrict__ any_hole);
+// both passes of the fill's blur (horizontal, then vertical, the vertical border taps above first
+// with above_first) out of place, 32 x 32 output tiles per block and plane; 256 threads
+__global__ void k_stack_blur(const float* __restrict__ src, float* __restrict__ dst, int w, int h, long pstride, Taps t,
+                             int n, int above_first, int rule, const int* __restrict__ any_hole);
 __global__ void k_stack_resample(const float* __restrict__ src, int sw, int sh, long sstride, float* __restrict__ dst,
                                  int dw, int dh, long dstride, int rule, const int* __restrict__ any_hole);
 __global__ void k_fill_combine(float* __restrict__ sol, const float* __restrict__ vals, long n, int nc, int rule,

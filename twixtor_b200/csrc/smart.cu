@@ -331,6 +331,86 @@ __global__ void k_stack_pass(const float* __restrict__ src, float* __restrict__ 
     }
 }
 
+// ---- both passes of the fill's blur in one launch ---------------------------------------------------
+
+// One element of a pass along a line held in shared memory: element t (global index in [0, len)) of
+// the line at line[(t - origin) * stride]; the interior chain or the 1 channel border rule, the
+// operations of stack_pass_px / border1 in their order.
+template <bool R, int N, bool LEFT_FIRST>
+__device__ __forceinline__ float stack_elem(const float* line, int origin, int stride, int len, int i, const Taps& t) {
+    if (len >= 2 * N && i >= N && i < len - N) {
+        const float* c = line + (i - origin) * stride;
+        float r = Ar<R>::mul(c[0], t.k[0]);
+#pragma unroll
+        for (int j = N - 1; j >= 1; j--) r = Ar<R>::add(r, Ar<R>::mul(Ar<R>::add(c[j * stride], c[-j * stride]), t.k[j]));
+        return r;
+    }
+    float num = Ar<R>::mul(t.k[0], line[(i - origin) * stride]);
+    float den = t.k[0];
+#pragma unroll
+    for (int j = N - 1; j >= 1; j--) {
+        float kj = t.k[j];
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            bool right = (side == 0) != LEFT_FIRST;
+            int tt = right ? i + j : i - j;
+            bool inside = tt >= 0 && tt < len;
+            float xv = inside ? line[(tt - origin) * stride] : 0.0f;
+            float wv = inside ? kj : 0.0f;
+            den = den + wv;
+            num = Ar<R>::add(num, Ar<R>::mul(xv, wv));
+        }
+    }
+    return Ar<R>::div(num, den);
+}
+
+// dst = the separable blur (horizontal, then vertical) of the stack src, out of place: a 32 x 32
+// output tile per block and plane (blockIdx.z), its region with the halo of N - 1 in shared memory
+// (the halo's horizontal pass computed again by the neighbouring tiles).
+constexpr int SB_TX = 32, SB_TY = 32, SB_MAXN = 6;  // the tile and the widest kernel (the push's r5 Gaussian)
+constexpr int SB_IN = (SB_TY + 2 * SB_MAXN - 2) * (SB_TX + 2 * SB_MAXN - 1), SB_H = (SB_TY + 2 * SB_MAXN - 2) * (SB_TX + 1);
+
+template <bool R, int N, bool ABOVE_FIRST>
+__device__ __forceinline__ void stack_blur_tile(const float* __restrict__ src, float* __restrict__ dst, int w, int h,
+                                                long pstride, const Taps& t, float* s_in, float* s_h) {
+    constexpr int TX = SB_TX, TY = SB_TY, HL = N - 1, RW = TX + 2 * HL, RH = TY + 2 * HL, RS = RW + 1, HS = TX + 1;
+    static_assert(N <= SB_MAXN && RH * RS <= SB_IN && RH * HS <= SB_H, "the shared buffers hold the widest region");
+    const float* s = src + blockIdx.z * pstride;
+    const int X0 = blockIdx.x * TX, Y0 = blockIdx.y * TY, gx0 = X0 - HL, gy0 = Y0 - HL;
+    for (int e = threadIdx.x; e < RH * RW; e += blockDim.x) {
+        const int r = e / RW, c = e - r * RW, X = gx0 + c, Y = gy0 + r;
+        s_in[r * RS + c] = (X >= 0 && X < w && Y >= 0 && Y < h) ? s[(long)Y * w + X] : 0.0f;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < RH * TX; e += blockDim.x) {
+        const int r = e / TX, c = e - r * TX, X = X0 + c, Y = gy0 + r;
+        if (X < w && Y >= 0 && Y < h) s_h[r * HS + c] = stack_elem<R, N, false>(s_in + r * RS, gx0, 1, w, X, t);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < TY * TX; e += blockDim.x) {
+        const int r = e / TX, c = e - r * TX, X = X0 + c, Y = Y0 + r;
+        if (X < w && Y < h)
+            dst[blockIdx.z * pstride + (long)Y * w + X] = stack_elem<R, N, ABOVE_FIRST>(s_h + c, gy0, HS, h, Y, t);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_stack_blur(const float* __restrict__ src, float* __restrict__ dst, int w, int h,
+                                                    long pstride, Taps t, int n, int above_first, int rule,
+                                                    const int* __restrict__ any_hole) {
+    if (!*any_hole) return;
+    __shared__ float s_in[SB_IN];
+    __shared__ float s_h[SB_H];
+#define TW_SB(Rr, Nn, Aa) stack_blur_tile<Rr, Nn, Aa>(src, dst, w, h, pstride, t, s_in, s_h)
+    if (rule) {
+        if (n == 3) { if (above_first) TW_SB(true, 3, true); else TW_SB(true, 3, false); }
+        else { if (above_first) TW_SB(true, 6, true); else TW_SB(true, 6, false); }
+    } else {
+        if (n == 3) { if (above_first) TW_SB(false, 3, true); else TW_SB(false, 3, false); }
+        else { if (above_first) TW_SB(false, 6, true); else TW_SB(false, 6, false); }
+    }
+#undef TW_SB
+}
+
 // flow/sample.rs:91-112 at element (x, y) of a dw x dh plane from the sw x sh plane s (the lerps
 // over the arithmetic set)
 template <bool R>
