@@ -222,12 +222,9 @@ __global__ void k_mask_holes(const void* __restrict__ mask, int kind, uint8_t* _
 constexpr int FILL_FLOW = 3;
 __global__ void k_fill_load(const void* __restrict__ img, int fmt, const uint8_t* __restrict__ holes,
                             float* __restrict__ stack, long n, const int* __restrict__ any_hole);
-// n: 3 (blur5) or 6 (Gaussian r5) taps; dir: 0 horizontal, 1 vertical below first, 2 vertical above
-// first; rule: the NaN rule arithmetic (float images)
-__global__ void k_stack_pass(const float* __restrict__ src, float* __restrict__ dst, int w, int h, long pstride, Taps t,
-                             int n, int dir, int rule, const int* __restrict__ any_hole);
 // both passes of the fill's blur (horizontal, then vertical, the vertical border taps above first
-// with above_first) out of place, 32 x 32 output tiles per block and plane; 256 threads
+// with above_first) out of place, 32 x 32 output tiles per block and plane; 256 threads; n: 3
+// (blur5) or 6 (Gaussian r5) taps; rule: the NaN rule arithmetic (float images and flows)
 __global__ void k_stack_blur(const float* __restrict__ src, float* __restrict__ dst, int w, int h, long pstride, Taps t,
                              int n, int above_first, int rule, const int* __restrict__ any_hole);
 __global__ void k_stack_resample(const float* __restrict__ src, int sw, int sh, long sstride, float* __restrict__ dst,

@@ -300,37 +300,6 @@ __device__ __forceinline__ float stack_pass_px(const float* __restrict__ s, int 
     return r;
 }
 
-// One pass over a stack of planes, one element per thread (plane blockIdx.z).
-template <bool R, int N, bool VERT, bool ABOVE_FIRST>
-__device__ __forceinline__ void stack_pass(const float* __restrict__ src, float* __restrict__ dst, int w, int h,
-                                           long pstride, const Taps& t) {
-    int x = blockIdx.x * blockDim.x + threadIdx.x;
-    int y = blockIdx.y;
-    if (x >= w || y >= h) return;
-    dst[blockIdx.z * pstride + (long)y * w + x] =
-        stack_pass_px<R, N, VERT, ABOVE_FIRST>(src + blockIdx.z * pstride, w, h, x, y, t);
-}
-
-template <bool R, int N>
-__device__ __forceinline__ void stack_pass_dir(const float* src, float* dst, int w, int h, long pstride, const Taps& t,
-                                               int dir) {
-    if (dir == 0) stack_pass<R, N, false, false>(src, dst, w, h, pstride, t);
-    else if (dir == 1) stack_pass<R, N, true, false>(src, dst, w, h, pstride, t);
-    else stack_pass<R, N, true, true>(src, dst, w, h, pstride, t);
-}
-
-__global__ void k_stack_pass(const float* __restrict__ src, float* __restrict__ dst, int w, int h, long pstride, Taps t,
-                             int n, int dir, int rule, const int* __restrict__ any_hole) {
-    if (!*any_hole) return;
-    if (rule) {
-        if (n == 3) stack_pass_dir<true, 3>(src, dst, w, h, pstride, t, dir);
-        else stack_pass_dir<true, 6>(src, dst, w, h, pstride, t, dir);
-    } else {
-        if (n == 3) stack_pass_dir<false, 3>(src, dst, w, h, pstride, t, dir);
-        else stack_pass_dir<false, 6>(src, dst, w, h, pstride, t, dir);
-    }
-}
-
 // ---- both passes of the fill's blur in one launch ---------------------------------------------------
 
 // One element of a pass along a line held in shared memory: element t (global index in [0, len)) of
