@@ -198,6 +198,9 @@ struct or_retime_params {
     double frame_time_bias;
     // retime-fgbg's frame time: trunc(dur * k + 0.5) at every rate (timeline.rs:204-210)
     int frame_time_plain;
+    // retime-fgbg's "360 Video": the engine's wrap-around flag (plugins/retime-fgbg/src/glue.rs:146-151),
+    // the wrap solve, the 360 warps, fills and Blur Compensation
+    int wrap_360;
 };
 
 // timeline.rs:69-76: a rate within 2e-5 (an f32 difference) of 29.97, 59.94 or 23.976 becomes it
@@ -706,6 +709,7 @@ static int retime_one(const void* frames, int nframes, int w, int h, int fmt, co
         fs.taps_above_first = p->taps_above_first != 0;
         fs.video_range_luma = p->video_360 != 0;  // compose/vector.rs:72-82 (flow_settings)
         fs.track_alpha = p->track_rgb_a != 0;     // plugins/retime-fgbg/src/glue.rs:34-38
+        fs.wrap = p->wrap_360 != 0;
         fs.prep_contrast_edge = p->prep == 2 || p->prep == 4;  // frontend.rs:224-225; 4: both stages, retime-fgbg's
         fs.prep_delinearize = p->prep == 3 || p->prep == 4;    // Contrast/Edge (plugins/retime-fgbg/src/glue.rs:153-154)
         FlowField fab, fba;
@@ -743,6 +747,7 @@ static int retime_one(const void* frames, int nframes, int w, int h, int fmt, co
         cs.blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
         cs.warp_mode = p->smart_blend;  // plugins/retime frontend: warp_mode = i32::from(smart_blend); 2, 3 the Warping popup of plugin 03
         cs.video_360 = p->video_360 != 0;
+        cs.wrap_360 = p->wrap_360 != 0;
         cs.taps_above_first = p->taps_above_first != 0;
         cs.gouraud = gouraud;
         Image o;
@@ -866,6 +871,8 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
         job.fs.hiq = p->quality_high != 0;
         job.fs.taps_above_first = p->taps_above_first != 0;
         job.fs.track_alpha = p->track_rgb_a != 0;
+        job.fs.wrap = p->wrap_360 != 0;
+        job.cs.wrap_360 = p->wrap_360 != 0;
         job.cs.quality_high = p->quality_high != 0;
         job.cs.blur = fixed_reader(float_to_fixed(p->blur_compensation), 1.0f);
         job.cs.warp_mode = p->smart_blend;
@@ -890,8 +897,9 @@ int or_retime_fgbg_one(const void* frames, int nframes, const void* const* matte
         }
         Image ra, rb;
         bool rev = p->rows_reversed != 0, above = p->taps_above_first != 0;
-        int rc = rebuilt_plate(A, ma, shrink, first, rev, above, &ra, &e);
-        if (!rc) rc = rebuilt_plate(B, mb, shrink, first, rev, above, &rb, &e);
+        bool wrap = p->wrap_360 != 0;
+        int rc = rebuilt_plate(A, ma, shrink, first, rev, above, &ra, &e, wrap);
+        if (!rc) rc = rebuilt_plate(B, mb, shrink, first, rev, above, &rb, &e, wrap);
         if (!rc) rc = interpolate(sel, ra, rb, &result, &e);
         if (rc) return fail(rc, e);
     } else {

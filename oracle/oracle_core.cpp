@@ -556,60 +556,90 @@ void edge_enhance(Plane& p, bool above_first) {
     }
 }
 
+std::vector<float> calc_grad_wrap(const float* img, int w, int h);
+void blur_gaussian_wrap(float* data, int w, int h, int c, float r);
+
+// prep.rs:377-398 (edge_enhance_with, wrap): the 360 Gaussian of radius 2.0 and the 360 gradient,
+// then the plain per pixel step
+static void edge_enhance_wrap(Plane& p) {
+    blur_gaussian_wrap(p.d.data(), p.w, p.h, 1, 2.0f);
+    std::vector<float> g = calc_grad_wrap(p.d.data(), p.w, p.h);
+    for (size_t i = 0; i < p.d.size(); i++) {
+        float gx = g[i * 2], gy = g[i * 2 + 1];
+        float m = std::sqrt(gx * gx + gy * gy);
+        float f = m <= 20.0f ? m * 0.05f : 1.0f;
+        p.d[i] = (f * 255.0f + p.d[i]) * 0.5f;
+    }
+}
+
 // conv.rs:192-244 (hrow_wrapx): every sample s = x[i] k0, then s = s + (x[(i+j) mod w] + x[(i-j) mod w]) k[j]
-// for j = n-1 down to 1 (the interior run is the same chain without a wrap)
-static void hpass_wrapx(const float* src, float* dst, int w, int h, const float* k, int n) {
+// for j = n-1 down to 1 (the interior run is the same chain without a wrap); c interleaved channels
+static void hpass_wrapx(const float* src, float* dst, int w, int h, int c, const float* k, int n) {
     OMP_FOR
     for (int y = 0; y < h; y++) {
-        const float* x = src + (long)y * w;
+        const float* x = src + (long)y * w * c;
         for (int i = 0; i < w; i++) {
-            float sum = x[i] * k[0];
-            for (int j = n - 1; j >= 1; j--) {
-                int r = (i + j) % w;
-                int l = ((i - j) % w + w) % w;
-                sum = sum + (x[r] + x[l]) * k[j];
+            for (int ch = 0; ch < c; ch++) {
+                float sum = x[(long)i * c + ch] * k[0];
+                for (int j = n - 1; j >= 1; j--) {
+                    int r = (i + j) % w;
+                    int l = ((i - j) % w + w) % w;
+                    sum = sum + (x[(long)r * c + ch] + x[(long)l * c + ch]) * k[j];
+                }
+                dst[((long)y * w + i) * c + ch] = sum;
             }
-            dst[(long)y * w + i] = sum;
         }
     }
 }
 
 // conv.rs:326-400 (vpass_sphere): each column padded by n - 1 elements at both ends with the
 // equirectangular walk (reflect at the edge row, move half a turn in x), then the plain chain
-static void vpass_sphere(const float* src, float* dst, int w, int h, const float* k, int n) {
+static void vpass_sphere(const float* src, float* dst, int w, int h, int c, const float* k, int n) {
     int half = w / 2, pad = n - 1;
     OMP_FOR
     for (int x = 0; x < w; x++) {
-        std::vector<float> g((size_t)h + 2 * pad);
         auto walk = [&](int start, int dir, int steps, std::vector<std::pair<int, int>>& out) {
-            int c = x, r = start, d = dir;
+            int cc = x, r = start, d = dir;
             for (int m = 0; m < steps; m++) {
                 r += d;
-                if (r < 0) { r = 0; d = -d; c = (half + c) % w; }
-                else if (r >= h) { r = h - 1; d = -d; c = (half + c) % w; }
-                out.push_back({c, r});
+                if (r < 0) { r = 0; d = -d; cc = (half + cc) % w; }
+                else if (r >= h) { r = h - 1; d = -d; cc = (half + cc) % w; }
+                out.push_back({cc, r});
             }
         };
         std::vector<std::pair<int, int>> up, down;
         walk(0, -1, pad, up);
         walk(h - 1, 1, pad, down);
-        for (int m = 0; m < pad; m++) g[pad - 1 - m] = src[(long)up[m].second * w + up[m].first];
-        for (int r = 0; r < h; r++) g[pad + r] = src[(long)r * w + x];
-        for (int m = 0; m < pad; m++) g[pad + h + m] = src[(long)down[m].second * w + down[m].first];
-        for (int y = 0; y < h; y++) {
-            int e = pad + y;
-            float sum = g[e] * k[0];
-            for (int j = n - 1; j >= 1; j--) sum = sum + (g[e + j] + g[e - j]) * k[j];
-            dst[(long)y * w + x] = sum;
+        std::vector<float> g((size_t)h + 2 * pad);
+        for (int ch = 0; ch < c; ch++) {
+            auto at = [&](int cc, int r) { return src[((long)r * w + cc) * c + ch]; };
+            for (int m = 0; m < pad; m++) g[pad - 1 - m] = at(up[m].first, up[m].second);
+            for (int r = 0; r < h; r++) g[pad + r] = at(x, r);
+            for (int m = 0; m < pad; m++) g[pad + h + m] = at(down[m].first, down[m].second);
+            for (int y = 0; y < h; y++) {
+                int e = pad + y;
+                float sum = g[e] * k[0];
+                for (int j = n - 1; j >= 1; j--) sum = sum + (g[e + j] + g[e - j]) * k[j];
+                dst[((long)y * w + x) * c + ch] = sum;
+            }
         }
     }
 }
 
-void convolve_wrapx_sphere(float* data, int w, int h, const float* k, int n) {
+// conv.rs:646-660 (convolve_wrapx_above_first): the circular horizontal pass, then the column walk
+// over the poles
+void convolve_wrapx_sphere(float* data, int w, int h, const float* k, int n, int c) {
     if (w == 0 || h == 0 || n == 0) return;
-    std::vector<float> tmp((size_t)w * h);
-    hpass_wrapx(data, tmp.data(), w, h, k, n);
-    vpass_sphere(tmp.data(), data, w, h, k, n);
+    std::vector<float> tmp((size_t)w * h * c);
+    hpass_wrapx(data, tmp.data(), w, h, c, k, n);
+    vpass_sphere(tmp.data(), data, w, h, c, k, n);
+}
+
+// conv.rs:662-668 (blur_gaussian_wrapx_above_first)
+void blur_gaussian_wrap(float* data, int w, int h, int c, float r) {
+    if ((double)r < 0.001) return;
+    std::vector<float> k = gaussian_kernel(r);
+    convolve_wrapx_sphere(data, w, h, k.data(), (int)k.size(), c);
 }
 
 // sample.rs:255-286 (bilinear1_sphere)
@@ -663,7 +693,6 @@ Plane reduce(Plane t, int r, bool above_first) {  // prep.rs:252-259
 bool build_pyramid(const Image& img, const FlowSettings& s, Pyramid* out, std::string* err) {
     if (!geometry(s, img.w, img.h, &out->geo, err)) return false;
     if (s.video_range_luma && s.track_alpha) { *err = "video range luma with track alpha"; return false; }
-    if (s.wrap && s.prep_contrast_edge) { *err = "the 360 mode Contrast / Edge Enhance is not restated"; return false; }
     Plane orig = luma(img, s.track_alpha, s.video_range_luma);
     if (s.wrap) {  // prep.rs:288-299 (reduce_with)
         for (int r = 0; r < out->geo.reduction; r++) {
@@ -674,7 +703,10 @@ bool build_pyramid(const Image& img, const FlowSettings& s, Pyramid* out, std::s
         orig = reduce(std::move(orig), out->geo.reduction, s.taps_above_first);
     }
     if (s.prep_delinearize) delinearize(orig);  // flow.rs:248-253: Delinearize, then Contrast/Edge
-    if (s.prep_contrast_edge) edge_enhance(orig, s.taps_above_first);
+    if (s.prep_contrast_edge) {
+        if (s.wrap) edge_enhance_wrap(orig);
+        else edge_enhance(orig, s.taps_above_first);
+    }
     int n = out->geo.levels;
     out->levels.clear();
     for (int i = 0; i < n; i++) {
@@ -953,6 +985,217 @@ std::vector<float> calc_b_masked(const float* i1, const float* i0, const float* 
     return b;
 }
 
+// ---- the wrap-around (360) solve (flow.rs:625-1246 with flow/extras.rs:286-430) ----------------
+
+// flow.rs:661-690 (sphere_target): x into [0, fw) and y into [0, fh) one period at a time; an odd
+// count of vertical periods moves x half a turn and mirrors y (unless it is 0). Non-finite
+// positions are returned as they are. The loops are bounded: a finite position past 2^25 periods
+// would not move (x + fw == x there) and is returned as it is, where the reference's loop would
+// not end.
+static inline void sphere_target(float& x, float& y, float fw, float fh) {
+    if (!(std::isfinite(x) && std::isfinite(y)) || !(fw > 0.0f && fh > 0.0f)) return;
+    const long cap = 1L << 25;
+    float x0 = x, y0 = y;
+    long m = 0;
+    while (x < 0.0f && m < cap) { x = x + fw; m++; }
+    while (fw <= x && m < cap) { x = x - fw; m++; }
+    unsigned n = 0;
+    while (y < 0.0f && m < cap) { y = y + fh; n++; m++; }
+    while (fh <= y && m < cap) { y = y - fh; n++; m++; }
+    if (m >= cap) { x = x0; y = y0; return; }
+    if (n % 2 == 1) {
+        x = fw * 0.5f + x;
+        if (fw <= x) x = x - fw;
+        if (y != 0.0f) y = fh - y;
+    }
+}
+
+// sample.rs:231-252 (bilinear2_sphere): bilinear1_sphere on (dx, dy) pairs
+static void bilinear2_sphere(const float* img, int w, int h, float x, float y, float out[2]) {
+    int w1 = w - 1, h1 = h - 1;
+    int tx = cvtt32(x), ty = cvtt32(y);
+    int ix = std::min(std::max(tx, 0), w1), iy = std::min(std::max(ty, 0), h1);
+    float fx = x - (float)tx, fy = y - (float)ty;
+    int x1 = ix + 1 > w1 ? 0 : ix + 1;
+    int xc = ix, xd = x1, yc = iy + 1;
+    if (iy + 1 > h1) {
+        int half = w / 2;
+        xc = (half + ix) % w;
+        xd = (half + x1) % w;
+        yc = h1;
+    }
+    for (int c = 0; c < 2; c++) {
+        float p00 = img[((long)iy * w + ix) * 2 + c], p10 = img[((long)iy * w + x1) * 2 + c];
+        float p01 = img[((long)yc * w + xc) * 2 + c], p11 = img[((long)yc * w + xd) * 2 + c];
+        float top = (p10 - p00) * fx + p00;
+        float bot = (p11 - p01) * fx + p01;
+        out[c] = (bot - top) * fy + top;
+    }
+}
+
+// flow.rs:716-741 (calc_grad_wrap): central differences times 0.5, the columns modulo the width;
+// above row 0 and below row h - 1 the same edge row half a turn away
+std::vector<float> calc_grad_wrap(const float* img, int w, int h) {
+    std::vector<float> g((size_t)w * h * 2, 0.0f);
+    if (w == 0 || h == 0) return g;
+    OMP_FOR
+    for (int y = 0; y < h; y++) {
+        for (int x = 0; x < w; x++) {
+            float c = img[(long)y * w + x];
+            float left = img[(long)y * w + (x + w - 1) % w];
+            float right = img[(long)y * w + (x + 1) % w];
+            int pole = (w / 2 + x) % w;
+            float up = y >= 1 ? img[(long)(y - 1) * w + x] : img[pole];
+            float down = y + 1 <= h - 1 ? img[(long)(y + 1) * w + x] : img[(long)(h - 1) * w + pole];
+            g[((long)y * w + x) * 2] = ((c - left) + (right - c)) * 0.5f;
+            g[((long)y * w + x) * 2 + 1] = ((c - up) + (down - c)) * 0.5f;
+        }
+    }
+    return g;
+}
+
+// flow.rs:743-761 with wrap: the left and right neighbours of the mask test modulo the width
+static void mask_gradient_wrap(float* grad, const float* mask, int w, int h) {
+    OMP_FOR
+    for (int y = 0; y < h; y++) {
+        auto off = [&](int xx, int yy) { return mask[(long)yy * w + xx] < 0.95f; };
+        for (int x = 0; x < w; x++) {
+            bool out = off(x, y) || (y >= 1 && off(x, y - 1)) || (y + 1 < h && off(x, y + 1)) || off((x + w - 1) % w, y) ||
+                       off((x + 1) % w, y);
+            if (out) { grad[((long)y * w + x) * 2] = 0.0f; grad[((long)y * w + x) * 2 + 1] = 0.0f; }
+        }
+    }
+}
+
+// flow.rs:777-822 (calc_b_with, wrap): a flow of a whole width or height or more gives B = 0; else
+// the target (x - u, y - v) goes onto the sphere and is sampled with the 360 sampler (the warped
+// mask of Y, when given, at least 0.999 there)
+static std::vector<float> calc_b_wrap(const float* i1, const float* i0, const float* grad, const float* flow, int w, int h,
+                                      const float* mask_y) {
+    std::vector<float> b((size_t)w * h * 2, 0.0f);
+    float fw = (float)w, fh = (float)h;
+    OMP_FOR
+    for (int y = 0; y < h; y++) {
+        float fy = (float)y;
+        for (int x = 0; x < w; x++) {
+            long i = (long)y * w + x;
+            float u = flow[i * 2], v = flow[i * 2 + 1];
+            if (fw <= std::fabs(u) || fh <= std::fabs(v)) continue;
+            float sx = (float)x - u, sy = fy - v;
+            sphere_target(sx, sy, fw, fh);
+            if (mask_y && !(bilinear1_sphere(mask_y, w, h, sx, sy) >= 0.999f)) continue;
+            float r = bilinear1_sphere(i0, w, h, sx, sy) - i1[i];
+            b[i * 2] = r * grad[i * 2];
+            b[i * 2 + 1] = r * grad[i * 2 + 1];
+        }
+    }
+    return b;
+}
+
+// flow.rs:862-884 (Block::patch_sphere): the 3x3 patch of A, each column modulo the width, each
+// row brought into [0, 2h) and past the last row mirrored onto the column half a turn away
+static void patch_sphere(const float* a, int w, int h, int x, int y, float p[9]) {
+    int n = 0;
+    for (int dy = -1; dy <= 1; dy++) {
+        for (int dx = -1; dx <= 1; dx++) {
+            int c = ((x + dx) % w + w) % w;
+            int r = ((y + dy) % (2 * h) + 2 * h) % (2 * h);
+            if (r > h - 1) {
+                c += w / 2;
+                if (c >= w) c -= w;
+                r = 2 * h - r - 1;
+            }
+            p[n++] = a[(long)r * w + c];
+        }
+    }
+}
+
+// flow.rs:891-911 (Block::cost_sphere): the target on the sphere, the nine positions around it each
+// on the sphere again, sampled with the 360 sampler; d8^2 + ((d0^2 + d1^2) + ... + d7^2)
+static float cost_sphere(const float* b, int w, int h, const float p[9], float tx, float ty) {
+    float fw = (float)w, fh = (float)h;
+    sphere_target(tx, ty, fw, fh);
+    float xs[3] = {tx - 1.0f, tx, tx + 1.0f}, ys[3] = {ty - 1.0f, ty, ty + 1.0f};
+    float sq[9];
+    int n = 0;
+    for (int j = 0; j < 3; j++) {
+        for (int i = 0; i < 3; i++) {
+            float sx = xs[i], sy = ys[j];
+            sphere_target(sx, sy, fw, fh);
+            float d = p[n] - bilinear1_sphere(b, w, h, sx, sy);
+            sq[n++] = d * d;
+        }
+    }
+    float s = sq[0];
+    for (int k = 1; k < 8; k++) s = s + sq[k];
+    return sq[8] + s;
+}
+
+// flow.rs:916-925 (Block::step_sphere): no range check, the neighbour wins on a smaller cost
+static inline bool bm_step_sphere(const float* a, const float* b, int w, int h, int x, int y, const float cur[2],
+                                  const float nb[2]) {
+    float p[9];
+    patch_sphere(a, w, h, x, y, p);
+    float c0 = cost_sphere(b, w, h, p, (float)x - cur[0], (float)y - cur[1]);
+    float c1 = cost_sphere(b, w, h, p, (float)x - nb[0], (float)y - nb[1]);
+    return c1 < c0;
+}
+
+// flow.rs:1087-1145 (sweeps_sphere) through flow.rs:1225-1245 (block_match_with, wrap): the two row
+// sweeps over every row and every column in place (the left neighbour modulo the width with the
+// columns increasing, then the right one with the columns decreasing) with the 360 step, then the
+// two column sweeps of the plain block matching; a pixel whose gate value is below 0.95 keeps its
+// vector
+void block_match_sphere(const float* a, const float* b, float* flow, int w, int h, const float* gate) {
+    if (w < 3 || h < 3) return;
+    auto gated = [&](int x, int y) { return gate && gate[(long)y * w + x] < 0.95f; };
+    for (int right = 0; right < 2; right++) {
+        OMP_FOR
+        for (int y = 0; y < h; y++) {
+            float* row = flow + (long)y * w * 2;
+            for (int m = 0; m < w; m++) {
+                int x = right ? w - 1 - m : m;
+                int nx = right ? (x + 1) % w : (x + w - 1) % w;
+                float cur[2] = {row[x * 2], row[x * 2 + 1]};
+                float nb[2] = {row[nx * 2], row[nx * 2 + 1]};
+                if (!gated(x, y) && bm_step_sphere(a, b, w, h, x, y, cur, nb)) { row[x * 2] = nb[0]; row[x * 2 + 1] = nb[1]; }
+            }
+        }
+    }
+    for (int below = 0; below < 2; below++) {
+        OMP_FOR
+        for (int x = 1; x <= w - 2; x++) {
+            for (int m = 1; m <= h - 2; m++) {
+                int y = below ? h - 1 - m : m;
+                float* c = flow + ((long)y * w + x) * 2;
+                float* q = flow + ((long)(below ? y + 1 : y - 1) * w + x) * 2;
+                float cur[2] = {c[0], c[1]};
+                float nb[2] = {q[0], q[1]};
+                if (!gated(x, y) && bm_step(a, b, w, h, x, y, cur, nb)) { c[0] = nb[0]; c[1] = nb[1]; }
+            }
+        }
+    }
+}
+
+// flow.rs:401-420 (upsample_flow_wrapx): the scales dw / sw and dh / sh, the steps their double
+// reciprocals narrowed, the 2 channel 360 sampler
+std::vector<float> upsample_flow_wrapx(const float* src, int sw, int sh, int dw, int dh) {
+    float sx = (float)dw / (float)sw, sy = (float)dh / (float)sh;
+    float rx = (float)(1.0 / (double)sx), ry = (float)(1.0 / (double)sy);
+    std::vector<float> dst((size_t)dw * dh * 2, 0.0f);
+    OMP_FOR
+    for (int y = 0; y < dh; y++) {
+        float fy = (float)y * ry;
+        for (int x = 0; x < dw; x++) {
+            float v[2];
+            bilinear2_sphere(src, sw, sh, (float)x * rx, fy, v);
+            dst[((long)y * dw + x) * 2] = v[0] * sx;
+            dst[((long)y * dw + x) * 2 + 1] = v[1] * sy;
+        }
+    }
+    return dst;
+}
+
 static void binarize(Plane& p) {  // flow/extras.rs:64-72 (a NaN gives 0)
     for (auto& v : p.d) v = v >= 0.95f ? 1.0f : 0.0f;
 }
@@ -964,10 +1207,11 @@ bool mask_pyramid(const float* matte, int w, int h, const FlowSettings& s, std::
     Plane cur(w, h);
     std::memcpy(cur.d.data(), matte, sizeof(float) * (size_t)w * h);
     binarize(cur);
-    auto step = [&](const Plane& p, int nw, int nh) {
+    auto step = [&](const Plane& p, int nw, int nh) {  // flow/extras.rs:76-85 (mask_step; wrap: the 360 passes)
         Plane t = p;
-        blur5(t.d.data(), t.w, t.h, s.taps_above_first);
-        Plane r = resample1(t, nw, nh);
+        if (s.wrap) blur5_wrap(t);
+        else blur5(t.d.data(), t.w, t.h, s.taps_above_first);
+        Plane r = s.wrap ? resample1_wrapx(t, nw, nh) : resample1(t, nw, nh);
         binarize(r);
         return r;
     };
@@ -1083,22 +1327,37 @@ FlowField solve_pyramids_masked(const Pyramid& x, const Pyramid& y, const FlowSe
         // the upsample, after the finest level's block matching and at the end of every level
         const UserLevel* u = user ? &(*user)[l] : nullptr;
         if (u) apply_user(flow, *u);
-        std::vector<float> grad = calc_grad(img_a, w, h);
-        if (mask_x) mask_gradient(grad.data(), mask_x, w, h);
+        // flow/extras.rs:337-380 (level_step_gated): with wrap the periodic gradient, the circular
+        // Gaussians, the 360 B step and the 360 block matching
+        const bool wrap = s.wrap;
+        auto blur = [&](std::vector<float>& d, int c, float r) {
+            if (wrap) blur_gaussian_wrap(d.data(), w, h, c, r);
+            else blur_gaussian(d.data(), w, h, c, r, s.taps_above_first);
+        };
+        auto refine = [&]() {
+            if (wrap) block_match_sphere(img_a, img_b, flow.data(), w, h, g8);
+            else block_match_gated(img_a, img_b, flow.data(), w, h, g8);
+        };
+        std::vector<float> grad = wrap ? calc_grad_wrap(img_a, w, h) : calc_grad(img_a, w, h);
+        if (mask_x) {
+            if (wrap) mask_gradient_wrap(grad.data(), mask_x, w, h);
+            else mask_gradient(grad.data(), mask_x, w, h);
+        }
         std::vector<float> a = calc_a(grad, w, h);
-        blur_gaussian(a.data(), w, h, 3, 7.0f, s.taps_above_first);
+        blur(a, 3, 7.0f);
         for (int it = 0; it < 3; it++) {
-            std::vector<float> b = mask_y ? calc_b_masked(img_a, img_b, grad.data(), flow.data(), w, h, mask_y)
-                                          : calc_b(img_a, img_b, grad.data(), flow.data(), w, h);
-            blur_gaussian(b.data(), w, h, 2, 7.0f, s.taps_above_first);
+            std::vector<float> b = wrap     ? calc_b_wrap(img_a, img_b, grad.data(), flow.data(), w, h, mask_y)
+                                   : mask_y ? calc_b_masked(img_a, img_b, grad.data(), flow.data(), w, h, mask_y)
+                                            : calc_b(img_a, img_b, grad.data(), flow.data(), w, h);
+            blur(b, 2, 7.0f);
             new_disp(flow.data(), a.data(), b.data(), (size_t)w * h);
-            blur_gaussian(flow.data(), w, h, 2, 5.0f, s.taps_above_first);
+            blur(flow, 2, 5.0f);
             if (it == 1 && l == 0) {
-                if (!s.skip_refine) block_match_gated(img_a, img_b, flow.data(), w, h, g8);
+                if (!s.skip_refine) refine();
                 if (u) apply_user(flow, *u);
             }
         }
-        if (l != 0 && !s.skip_refine) block_match_gated(img_a, img_b, flow.data(), w, h, g8);
+        if (l != 0 && !s.skip_refine) refine();
         if (u) apply_user(flow, *u);
         if (check) {
             if (all_flow_out_of_range(flow.data(), w, h)) std::fill(flow.begin(), flow.end(), 0.0f);
@@ -1107,7 +1366,7 @@ FlowField solve_pyramids_masked(const Pyramid& x, const Pyramid& y, const FlowSe
         if (l == start && std::fabs((double)damp - 1.0) >= 1e-6) scale_values(flow.data(), flow.size(), damp);
         if (l > 0) {
             int nw = geo.sizes[l - 1].first, nh = geo.sizes[l - 1].second;
-            flow = upsample_flow(flow.data(), w, h, nw, nh);
+            flow = wrap ? upsample_flow_wrapx(flow.data(), w, h, nw, nh) : upsample_flow(flow.data(), w, h, nw, nh);
         }
     }
     scale_values(flow.data(), flow.size(), -1.0f);
@@ -1432,6 +1691,13 @@ void bilerp4_image(const Image& img, float x, float y, float out[4]) {
     else bilerp4(img.f32.data(), img.w, w1, h1, x, y, out);
 }
 
+void bilerp360_image(const Image& img, float x, float y, float out[4]) {
+    int w1 = img.w - 1, h1 = img.h - 1;
+    if (img.fmt == U8) bilerp360(img.u8.data(), img.w, w1, h1, x, y, out);
+    else if (img.fmt == U16) bilerp360(img.u16.data(), img.w, w1, h1, x, y, out);
+    else bilerp360(img.f32.data(), img.w, w1, h1, x, y, out);
+}
+
 void copy_image(Image& out, const Image& src) {  // blend.rs:117-125
     std::memcpy(out.data(), src.data(), src.bytes());
 }
@@ -1543,6 +1809,7 @@ static int compose_body(const ComposeSettings& cs, const Selection& sel, const I
     float wa = sel.wa;
     float frac = 1.0f - wa;
     WarpOpts o;
+    o.is360 = cs.wrap_360;  // compose/vector.rs:214 (every interpolation mode of code 0)
     *out = Image(a.w, a.h, a.fmt);
     if (sel.interp == 0) {
         const FlowField* flow = nearest_uses_f_ab(wa, cs.warp_mode) ? f_ab : f_ba;
@@ -1575,7 +1842,7 @@ int compose_vectors(const ComposeSettings& cs, const Selection& sel, const Image
     // compose/vector.rs:276-281: the Blur Compensation tail with F_AB, else the single flow
     const FlowField* flow = f_ab ? f_ab : f_ba;
     if (!flow) return 0;
-    return blur_compensation(*out, *flow, sel.s0, sel.s1, cs.blur, cs.quality_high, err);
+    return blur_compensation(*out, *flow, sel.s0, sel.s1, cs.blur, cs.quality_high, err, cs.wrap_360);
 }
 
 int interpolate(const Selection& sel, const Image& a, const Image& b, Image* out, std::string* err) {

@@ -186,8 +186,10 @@ void blur5(float* data, int w, int h, bool above_first);
 float bilinear1(const float* img, int w, int h, float x, float y);
 void bilinear2(const float* img, int w, int h, float x, float y, float out[2]);
 Plane resample1(const Plane& src, int dw, int dh);
-// conv.rs:643-650 (convolve_wrapx_above_first, 1 channel): hpass_wrapx then vpass_sphere
-void convolve_wrapx_sphere(float* data, int w, int h, const float* k, int n);
+// conv.rs:643-660 (convolve_wrapx_above_first, c interleaved channels): hpass_wrapx then vpass_sphere
+void convolve_wrapx_sphere(float* data, int w, int h, const float* k, int n, int c = 1);
+// conv.rs:662-668 (blur_gaussian_wrapx_above_first): radii below 0.001 do nothing
+void blur_gaussian_wrap(float* data, int w, int h, int c, float r);
 // sample.rs:205-230 (resample1_wrapx): bilinear1_sphere at (x sw / dw, y sh / dh)
 Plane resample1_wrapx(const Plane& src, int dw, int dh);
 
@@ -258,6 +260,8 @@ void copy_image(Image& out, const Image& src);
 void warp_flow_bilerp(const FlowField& f, float x, float y, float out[2]);
 // warp.rs:308-331 bilerp4 (with mix4's NaN rule repeat) over an image, w1 = w - 1, h1 = h - 1
 void bilerp4_image(const Image& img, float x, float y, float out[4]);
+// warp.rs:362-396 (bilerp360) on an engine image
+void bilerp360_image(const Image& img, float x, float y, float out[4]);
 void blend(Image& out, const Image& a, const Image& b, float w);
 void lerp(Image& first, const Image& second, float w);
 
@@ -276,6 +280,9 @@ struct Selection {  // timeline.rs:391-414
 struct ComposeSettings {
     int warp_mode = 0;        // 0 inverse, 1 Smart Blend (inverse + coverage), 2/3 forward
     bool video_360 = false;   // binary alpha Smart Blend / video range luma
+    // the engine's wrap-around (360) flag (compose/vector.rs:1-13): the inverse warps of code 0, the
+    // warps and fills of Smart Blend (codes 1 and 2), the Blur Compensation tail
+    bool wrap_360 = false;
     bool quality_high = true;
     float blur = 0.0f;        // blur compensation slider
     bool taps_above_first = true;  // Stages::vertical_taps() of the hole fill (stages.rs:66-70)

@@ -317,8 +317,36 @@ float store_blur_int(float v, float white) {  // warp.rs:272-274 / :292-294
 
 }  // namespace
 
+// blurcomp.rs:282-322 (Blur::wrap_x): x into [0, W) by the loops of the 360 inverse warp, false past
+// their bound or when the result is outside (NaN, infinite)
+static bool wrap_x(float qx, float wf, float* out) {
+    float x = qx;
+    unsigned guard = 0;
+    while (x < 0.0f) { x += wf; if (++guard > (unsigned)TAP_LIMIT) return false; }
+    while (wf <= x) { x -= wf; if (++guard > (unsigned)TAP_LIMIT) return false; }
+    *out = x;
+    return x >= 0.0f && x < wf;
+}
+
+// blurcomp.rs:248-280 (sphere_tap): y into [0, H) counting the periods; after an odd count x moves half
+// a turn and a y other than 0 becomes H - y; false past the loops' bound or outside the frame
+static bool sphere_tap(float x, float qy, float wf, float hf, float* ox, float* oy) {
+    float y = qy;
+    unsigned steps = 0;
+    while (y < 0.0f) { y += hf; if (++steps > (unsigned)TAP_LIMIT) return false; }
+    while (hf <= y) { y -= hf; if (++steps > (unsigned)TAP_LIMIT) return false; }
+    if (steps % 2 == 1) {
+        x = wf * 0.5f + x;
+        if (!(x < wf)) x -= wf;
+        if (y != 0.0f) y = hf - y;
+    }
+    *ox = x;
+    *oy = y;
+    return x >= 0.0f && x < wf && y >= 0.0f && y < hf;
+}
+
 int motion_blur(Image& dest, const Image& src, const FlowField& flow, float amount, bool hiq, float shutter,
-                std::string* err) {
+                std::string* err, bool is360) {
     if (dest.w != src.w || dest.h != src.h || dest.fmt != src.fmt) { *err = "motion blur: shapes"; return 1; }
     if (src.w < 2 || src.h < 2 || flow.w < 2 || flow.h < 2) { *err = "motion blur needs at least 2x2"; return 1; }
     int w = src.w, h = src.h;
@@ -372,7 +400,14 @@ int motion_blur(Image& dest, const Image& src, const FlowField& flow, float amou
             if (hiq) {  // blurcomp.rs:398-455
                 auto tap = [&](float qx, float qy) {
                     if (std::isnan(qx) || std::isnan(qy)) { bad = true; return; }
-                    if (0.0f <= qx && qx < wf && 0.0f <= qy && qy < hf) {
+                    if (is360) {  // blurcomp.rs:425-434: every tap counts, on the sphere, the 360 sampler
+                        float wx, sx2, sy2;
+                        if (!wrap_x(qx, wf, &wx) || !sphere_tap(wx, qy, wf, hf, &sx2, &sy2)) { bad = true; return; }
+                        cnt++;
+                        float t[4];
+                        bilerp360_image(src, sx2, sy2, t);
+                        for (int c = 0; c < 4; c++) sum[c] += t[c];
+                    } else if (0.0f <= qx && qx < wf && 0.0f <= qy && qy < hf) {
                         cnt++;
                         float t[4];
                         bilerp4_image(src, qx, qy, t);
@@ -387,9 +422,21 @@ int motion_blur(Image& dest, const Image& src, const FlowField& flow, float amou
             } else {  // blurcomp.rs:459-559: the backward taps always count
                 int wi = w, hi = (int)hf;
                 float qx = cx, qy = cy;
+                // blurcomp.rs:496-512 with is360: a tap whose row is inside reads the column of its wrapped x
+                auto column = [&](float q, int* ix) {
+                    float wx;
+                    if (!wrap_x(q, wf, &wx)) { bad = true; return false; }
+                    *ix = cvtt32(wx);
+                    return true;
+                };
                 for (int j = 0; j < n; j++) {
                     int ix = cvtt32(qx), iy = cvtt32(qy);
-                    if (ix >= 0 && ix < wi && iy >= 0 && iy < hi) {
+                    if (is360) {
+                        if (iy >= 0 && iy < hi && column(qx, &ix)) {
+                            cnt++;
+                            for (int c = 0; c < 4; c++) sum[c] += sample((size_t)iy * w + ix, c);
+                        }
+                    } else if (ix >= 0 && ix < wi && iy >= 0 && iy < hi) {
                         cnt++;
                         for (int c = 0; c < 4; c++) sum[c] += sample((size_t)iy * w + ix, c);
                     }
@@ -399,8 +446,12 @@ int motion_blur(Image& dest, const Image& src, const FlowField& flow, float amou
                 qx = cx - sx; qy = cy - sy;
                 for (int j = 1; j < n; j++) {
                     int ix = cvtt32(qx), iy = cvtt32(qy);
-                    if (ix >= 0 && ix < wi && iy >= 0 && iy < hi)
+                    if (is360) {
+                        if (iy >= 0 && iy < hi && column(qx, &ix))
+                            for (int c = 0; c < 4; c++) sum[c] += sample((size_t)iy * w + ix, c);
+                    } else if (ix >= 0 && ix < wi && iy >= 0 && iy < hi) {
                         for (int c = 0; c < 4; c++) sum[c] += sample((size_t)iy * w + ix, c);
+                    }
                     cnt++;
                     qx += nsx; qy += nsy;
                 }
@@ -413,7 +464,8 @@ int motion_blur(Image& dest, const Image& src, const FlowField& flow, float amou
     return 0;
 }
 
-int blur_compensation(Image& img, const FlowField& flow, float s0, float s1, float blur, bool hiq, std::string* err) {
+int blur_compensation(Image& img, const FlowField& flow, float s0, float s1, float blur, bool hiq, std::string* err,
+                      bool is360) {
     float a = std::fabs(s0 - s1);  // blurcomp.rs:42-48 (blur_amount)
     if (!((double)a > 1e-6) || !((double)blur > 0.005)) return 0;
     float amount = (a - 1.0f) * blur;
@@ -422,7 +474,7 @@ int blur_compensation(Image& img, const FlowField& flow, float s0, float s1, flo
     if ((double)std::fabs(amount) < 1e-6) return 0;
     Image tmp(img.w, img.h, img.fmt);
     if (0.0f < amount) {
-        int rc = motion_blur(tmp, img, flow, amount, hiq, 0.5f, err);
+        int rc = motion_blur(tmp, img, flow, amount, hiq, 0.5f, err, is360);
         if (rc) return rc;
         size_t n = (size_t)img.w * img.h;  // blurcomp.rs:134-149 (clear_rgb_where_transparent)
         for (size_t i = 0; i < n; i++) {
@@ -435,7 +487,7 @@ int blur_compensation(Image& img, const FlowField& flow, float s0, float s1, flo
             }
         }
     } else {
-        int rc = motion_blur(tmp, img, flow, 0.5f, hiq, 0.5f, err);
+        int rc = motion_blur(tmp, img, flow, 0.5f, hiq, 0.5f, err, is360);
         if (rc) return rc;
         lerp(tmp, img, amount);
     }

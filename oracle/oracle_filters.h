@@ -29,11 +29,13 @@ void composite_masked(Image& dest, const Image& src, const Mask& m);            
 float sharpen_weight(float t);                                                   // filters.rs:627-631
 void sharpen_step(Image& frame, const Image& original, float t, bool above_first);  // filters.rs:649-657
 
-// warp/blurcomp.rs:176-559 (motion_blur, is360 off): returns 0, 1 (mismatch) or 2 (a NaN tap or a
-// vector of more than 65536 taps)
+// warp/blurcomp.rs:176-559 (motion_blur): returns 0, 1 (mismatch) or 2 (a NaN tap, a vector of more
+// than 65536 taps, or with is360 a tap that the wrap loops cannot bring into the frame)
 int motion_blur(Image& dest, const Image& src, const FlowField& flow, float amount, bool hiq, float shutter,
-                std::string* err);
-// warp/blurcomp.rs:42-130 (blur_compensation with is360 off): in place on the composed image
-int blur_compensation(Image& img, const FlowField& flow, float s0, float s1, float blur, bool hiq, std::string* err);
+                std::string* err, bool is360 = false);
+// warp/blurcomp.rs:42-130 (blur_compensation; with is360 blur_compensation_wrap, :73-87): in place on
+// the composed image
+int blur_compensation(Image& img, const FlowField& flow, float s0, float s1, float blur, bool hiq, std::string* err,
+                      bool is360 = false);
 
 }  // namespace orc

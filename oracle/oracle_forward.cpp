@@ -622,7 +622,7 @@ int compose_forward(const ComposeSettings& cs, const Selection& sel, const Image
                         : forward_warp(*out, b, *flow, wa, !cs.gouraud, fill ? &cov : nullptr, err);
         if (rc || !fill) return rc;
         for (auto& v : cov.d) v = 0xff - v;  // warp.rs:76-80
-        return fill_holes(*out, cov.d.data(), 1, cs.taps_above_first, err);
+        return fill_holes(*out, cov.d.data(), 1, cs.taps_above_first, err, cs.wrap_360);
     }
     if (sel.interp == 1) {
         if (!f_ab || !f_ba) { *err = "missing flow"; return 1; }
@@ -639,7 +639,7 @@ int compose_forward(const ComposeSettings& cs, const Selection& sel, const Image
         }
         smart_blend(*out, ta, tb, frac, cs.video_360);  // smart_composite, then smart_finish_with
         for (size_t i = 0; i < c1.d.size(); i++) c1.d[i] = 0xff - std::max(c1.d[i], c2.d[i]);
-        return fill_holes(*out, c1.d.data(), 1, cs.taps_above_first, err);
+        return fill_holes(*out, c1.d.data(), 1, cs.taps_above_first, err, cs.wrap_360);
     }
     if (sel.interp == 2) {  // forward.rs:498-572 (weighted_forward, weighted_forward_fill)
         if (!f_ab || !f_ba) { *err = "missing flow"; return 1; }

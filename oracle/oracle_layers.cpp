@@ -255,22 +255,24 @@ static void premultiply_pl(Image& img) {  // plates.rs:191-208
 // plates.rs:245-256: unpremultiply, fill the colour where the plate is not opaque (holes:
 // white - alpha), the alpha replaced by the layer's raw matte plane or (frame != null) the frame's
 // alpha, premultiply
-static int refill(Image& img, const LPlane* plane, const Image* frame, bool above_first, std::string* err) {
+// is360: the 360 passes of the fill (plates.rs:252-263)
+static int refill(Image& img, const LPlane* plane, const Image* frame, bool above_first, std::string* err,
+                  bool is360 = false) {
     unpremultiply_pl(img);
     size_t n = (size_t)img.w * img.h;
     int rc;
     if (img.fmt == U8) {
         std::vector<uint8_t> m(n);
         for (size_t i = 0; i < n; i++) m[i] = (uint8_t)(0xffu - img.u8[i * 4]);
-        rc = fill_holes(img, m.data(), 1, above_first, err);
+        rc = fill_holes(img, m.data(), 1, above_first, err, is360);
     } else if (img.fmt == U16) {
         std::vector<uint16_t> m(n);
         for (size_t i = 0; i < n; i++) m[i] = (uint16_t)(0xffffu - img.u16[i * 4]);
-        rc = fill_holes(img, m.data(), 2, above_first, err);
+        rc = fill_holes(img, m.data(), 2, above_first, err, is360);
     } else {
         std::vector<float> m(n);
         for (size_t i = 0; i < n; i++) m[i] = 1.0f - img.f32[i * 4];
-        rc = fill_holes(img, m.data(), 3, above_first, err);
+        rc = fill_holes(img, m.data(), 3, above_first, err, is360);
     }
     if (rc) return rc;
     for (size_t i = 0; i < n; i++) {  // plates.rs:211-239 (set_alpha)
@@ -408,7 +410,7 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
         if (sel.interp == 0) {
             bool takes_a = nearest_takes_a(code, sel.wa);
             Image p = takes_a ? la : lb;
-            int rc = refill(p, takes_a ? pl_a : pl_b, takes_a ? fr_a : fr_b, job.cs.taps_above_first, err);
+            int rc = refill(p, takes_a ? pl_a : pl_b, takes_a ? fr_a : fr_b, job.cs.taps_above_first, err, job.cs.wrap_360);
             if (rc) return rc;
             rc = compose_vectors(job.cs, sel, p, p, fab, fba, &r, err);
             if (rc) return rc;
@@ -417,6 +419,7 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
             // to its time with amount 1: the inverse warp with hold edges (codes 0 and 1, A's plate reads
             // F_AB), the forward warp without coverage (codes 2 and 3, each side pushed by its own flow)
             WarpOpts o;
+            o.is360 = job.cs.wrap_360;  // plates.rs:268-276 (warp_full)
             Image pa(w, h, fmt), pb(w, h, fmt);
             int rc = code >= 2 ? forward_warp(pa, lb, *fba, 1.0f, !job.cs.gouraud, nullptr, err) : inv_warp(pa, lb, *fab, 1.0f, o, nullptr, err);
             if (rc) return rc;
@@ -424,9 +427,9 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
             rc = code >= 2 ? forward_warp(pb, la, *fab, 1.0f, !job.cs.gouraud, nullptr, err) : inv_warp(pb, la, *fba, 1.0f, o, nullptr, err);
             if (rc) return rc;
             over_pl(pb, lb);
-            rc = refill(pa, pl_a, fr_a, job.cs.taps_above_first, err);
+            rc = refill(pa, pl_a, fr_a, job.cs.taps_above_first, err, job.cs.wrap_360);
             if (rc) return rc;
-            rc = refill(pb, pl_b, fr_b, job.cs.taps_above_first, err);
+            rc = refill(pb, pl_b, fr_b, job.cs.taps_above_first, err, job.cs.wrap_360);
             if (rc) return rc;
             rc = compose_vectors(job.cs, sel, pa, pb, fab, fba, &r, err);
             if (rc) return rc;
@@ -439,7 +442,7 @@ int compose_layers_plates(const LayerJob& job, const Image& a, const Image& b, I
 }
 
 int rebuilt_plate(const Image& frame, const std::vector<std::vector<float>>& mattes, const std::vector<float>& shrink,
-                  int k, bool reversed, bool above_first, Image* out, std::string* err) {
+                  int k, bool reversed, bool above_first, Image* out, std::string* err, bool is360) {
     int w = frame.w, h = frame.h, nfg = (int)mattes.size();
     size_t n = (size_t)w * h;
     std::vector<LPlane> raws;
@@ -451,13 +454,13 @@ int rebuilt_plate(const Image& frame, const std::vector<std::vector<float>>& mat
     int rc;
     if (k == nfg) {
         Image fa = reversed ? rows_reversed(frame) : frame;
-        rc = refill(q, nullptr, &fa, above_first, err);
+        rc = refill(q, nullptr, &fa, above_first, err, is360);
     } else {
         LPlane rp = raws[k];
         if (reversed)
             for (int y = 0; y < h; y++)
                 std::memcpy(&rp.v[(size_t)y * w], &raws[k].v[(size_t)(h - 1 - y) * w], sizeof(float) * w);
-        rc = refill(q, &rp, nullptr, above_first, err);
+        rc = refill(q, &rp, nullptr, above_first, err, is360);
     }
     if (rc) return rc;
     p = reversed ? rows_reversed(q) : q;

@@ -32,7 +32,8 @@ void choke_pl(std::vector<float>& m, int w, int h, float amount);
 // layers.rs:497-528 (rebuilt_plate): the single group display of an unwarped frame; mattes raw (0..1)
 // in host rows; the fill runs on bottom-up rows when `reversed`
 int rebuilt_plate(const Image& frame, const std::vector<std::vector<float>>& mattes, const std::vector<float>& shrink,
-                  int k, bool reversed, bool above_first, Image* out, std::string* err);
+                  int k, bool reversed, bool above_first, Image* out, std::string* err,
+                  bool is360 = false);
 
 LPlane raw_plane(const float* m, size_t n, Fmt fmt);
 LPlane comp_plane(const std::vector<LPlane>& raws, const std::vector<float>& shrink, int k, Fmt fmt, int w, int h);

@@ -473,6 +473,7 @@ int compose_smart(const ComposeSettings& cs, const Selection& sel, const Image& 
     float wa = sel.wa;
     WarpOpts o;
     o.hold = false;
+    o.is360 = sel.interp != 2 && cs.wrap_360;  // the weighted variant keeps the flag off (smartblend.rs:408)
     if (sel.interp == 0) {
         bool use_ab = nearest_uses_f_ab(wa, 1);
         const FlowField* flow = use_ab ? f_ab : f_ba;
@@ -482,7 +483,7 @@ int compose_smart(const ComposeSettings& cs, const Selection& sel, const Image& 
         int rc = !(0.5f > wa) ? inv_warp(*out, a, *flow, 1.0f - wa, o, &cov, err) : inv_warp(*out, b, *flow, wa, o, &cov, err);
         if (rc) return rc;
         for (auto& v : cov.d) v = 0xff - v;
-        return fill_holes(*out, cov.d.data(), 1, taps_above_first, err);
+        return fill_holes(*out, cov.d.data(), 1, taps_above_first, err, cs.wrap_360);
     }
     if (sel.interp == 1) {
         if (!f_ab || !f_ba) { *err = "missing flow"; return 1; }
@@ -495,7 +496,7 @@ int compose_smart(const ComposeSettings& cs, const Selection& sel, const Image& 
         if (rc) return rc;
         smart_blend(*out, ta, tb, frac, cs.video_360);
         for (size_t i = 0; i < c1.d.size(); i++) c1.d[i] = 0xff - std::max(c1.d[i], c2.d[i]);
-        return fill_holes(*out, c1.d.data(), 1, taps_above_first, err);
+        return fill_holes(*out, c1.d.data(), 1, taps_above_first, err, cs.wrap_360);
     }
     if (sel.interp == 2) {  // smartblend.rs:400-420 (weighted_blend_smart) and :427-456 (weighted_tail)
         if (!f_ab || !f_ba) { *err = "missing flow"; return 1; }

@@ -52,6 +52,8 @@ Writes, next to this script:
   time model; constant parameters but Speed and Frame Num, integer rates, no 360 Video, no Source
   display, no input fields or Mark Segments), their input clips as its ``gen_grid.py`` renders
   them, and the sha256 of the output clip ``results/base.tsv`` records.
+* ``fgbg_core_360_grid.npz`` - the cases of the same grid with 360 Video on (the engine's
+  wrap-around flag: the wrap solve, the 360 warps, fills, Blur Compensation and prep), same format.
 * ``retime_time_grid.npz`` - the cases of the reference's parity grid ``parity/retime-time`` (the
   time model with No Vectors: Speed and Frame Number modes, constant or keyed without Bezier
   handles, In FPS is Out FPS and the input rate, Frame Interp; integer composition rates, no Src
@@ -236,7 +238,9 @@ FGC_SERVED = {"speed_percent", "warping", "frame_interp", "vectors", "prep", "ma
               "input_frame_rate", "plenty_memory"}
 
 
-def fgbg_core_grid(ref):
+def fgbg_core_grid(ref, video_360=False):
+    """The served cases without 360 Video (fgbg_core_grid.npz), or with video_360 the cases that set
+    it (fgbg_core_360_grid.npz)."""
     root = os.path.join(ref, "parity", "fgbg-core")
     spec = importlib.util.spec_from_file_location("fgc_gen", os.path.join(root, "gen_grid.py"))
     gen = importlib.util.module_from_spec(spec)
@@ -253,7 +257,7 @@ def fgbg_core_grid(ref):
             continue
         if any("@" in v for k, v in params.items() if k not in ("speed_percent", "frame_num")):
             continue
-        if params.get("video_360", "0") != "0" or params.get("display", "1") == "2":
+        if (params.get("video_360", "0") != "0") != video_360 or params.get("display", "1") == "2":
             continue
         if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
             continue
@@ -266,8 +270,9 @@ def fgbg_core_grid(ref):
     keys = sorted(inputs)
     arrays = {f"input_{i}": inputs[k] for i, k in enumerate(keys)}
     arrays["meta"] = np.frombuffer(json.dumps(dict(inputs=keys, cases=cases)).encode(), np.uint8)
-    np.savez_compressed(os.path.join(HERE, "fgbg_core_grid.npz"), **arrays)
-    print(f"fgbg_core_grid.npz: {len(cases)} cases, {len(keys)} clips")
+    name = "fgbg_core_360_grid.npz" if video_360 else "fgbg_core_grid.npz"
+    np.savez_compressed(os.path.join(HERE, name), **arrays)
+    print(f"{name}: {len(cases)} cases, {len(keys)} clips")
 
 
 RT_SERVED = {"vectors", "speed_percent", "frame_interp", "time_remap_mode", "frame_num", "in_fps_is_out_fps",
@@ -435,11 +440,13 @@ def main():
         return
     if args.only == "fgbg_core":
         fgbg_core_grid(ref)
+        fgbg_core_grid(ref, video_360=True)
         return
     if args.only == "debug":
         debug_tables(ref)
         return
     fgbg_core_grid(ref)
+    fgbg_core_grid(ref, video_360=True)
     debug_tables(ref)
     retime_time_grid(ref)
     vectors_in_grid(ref)

@@ -532,9 +532,10 @@ def rt_case_params(case):
                 input_frame_rate=float(p.get("input_frame_rate", float(np.float32(29.97)))))
 
 
-def fgc_grid():
-    """The served cases of the fgbg-core parity grid: (meta cases, {clip name: raw bytes})."""
-    z = np.load(os.path.join(GOLDEN, "fgbg_core_grid.npz"))
+def fgc_grid(video_360=False):
+    """The served cases of the fgbg-core parity grid: (meta cases, {clip name: raw bytes}); with
+    video_360 the cases with 360 Video on."""
+    z = np.load(os.path.join(GOLDEN, "fgbg_core_360_grid.npz" if video_360 else "fgbg_core_grid.npz"))
     meta = json.loads(bytes(z["meta"]).decode())
     inputs = {name: z[f"input_{i}"] for i, name in enumerate(meta["inputs"])}
     return meta["cases"], inputs
@@ -554,7 +555,8 @@ def fgc_case_params(case):
                 prep={1: 1, 2: 4, 3: 1}[int(p.get("prep", 1))], track_rgb_a=p.get("track_rgb_a", "0") == "1",
                 remap_mode=int(p.get("time_remap_mode", 1)), frame_num=fnum, fn_keys=fn_keys,
                 own_input_rate=p.get("in_fps_is_out_fps", "1") == "0",
-                input_frame_rate=float(p.get("input_frame_rate", float(np.float32(29.97)))), frame_time_plain=True)
+                input_frame_rate=float(p.get("input_frame_rate", float(np.float32(29.97)))), frame_time_plain=True,
+                wrap_360=p.get("video_360", "0") == "1")
 
 
 def debug_tables():

@@ -46,3 +46,26 @@ def test_library_selection_on_the_grid():
             want = O.select(p, n, w, h)
             assert (sel.a, sel.b) == O.clip_frames(p, n, w, h), (c["id"], n)
             assert (sel.exact, sel.vectors_quality, sel.interp) == (want["exact"], want["vq"], want["interp"])
+
+
+FGC360_CASES, FGC360_INPUTS = G.fgc_grid(video_360=True)
+
+
+def test_360_grid_is_served():
+    assert len(FGC360_CASES) == 16
+
+
+@pytest.mark.parametrize("c", FGC360_CASES, ids=[c["id"] for c in FGC360_CASES])
+def test_fgbg_core_360_grid(c):
+    """The grid's cases with 360 Video on, which retime-fgbg turns into the engine's wrap-around flag
+    (plugins/retime-fgbg/src/glue.rs:146-151): the wrap solve (flow/extras.rs:286-430 with the 360
+    gradient, Gaussians, B step, block matching and upsample of flow.rs:625-1246), the 360 inverse
+    warps, the 360 passes of the hole fill and the plate refills, the 360 taps of Blur Compensation
+    and the 360 Contrast/Edge prep."""
+    w, h = c["width"], c["height"]
+    fmt = G.FMT_OF_DEPTH[c["depth"]]
+    kw = G.fgc_case_params(c)
+    assert kw["wrap_360"]
+    p = O.retime_params(rows_reversed=True, taps_above_first=True, **kw)
+    out = O.retime_fgbg_clip(FGC360_INPUTS[c["input"]], c["frames"], [], [], [], w, h, fmt, p, c["frames"])
+    assert hashlib.sha256(out.tobytes()).hexdigest() == c["sha256"]
