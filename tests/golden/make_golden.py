@@ -56,8 +56,8 @@ Writes, next to this script:
   wrap-around flag: the wrap solve, the 360 warps, fills, Blur Compensation and prep), same format.
 * ``retime_time_grid.npz`` - the cases of the reference's parity grid ``parity/retime-time`` (the
   time model with No Vectors: Speed and Frame Number modes, constant or keyed without Bezier
-  handles, In FPS is Out FPS and the input rate, Frame Interp; integer composition rates, no Src
-  Mark Segments, no input fields), their input clips as its ``gen_grid.py`` writes them, and the
+  handles, In FPS is Out FPS and the input rate, Frame Interp; integer, NTSC and decimal
+  composition rates, no Src Mark Segments, no input fields), their input clips as its ``gen_grid.py`` writes them, and the
   sha256 of the output clip ``results/base.tsv`` records.
 * ``vectors_in_grid.npz`` - the cases of the reference's parity grid ``parity/vectors-in`` that the
   single layer Vectors In render serves (one or both vector layers, no FG matte layer, Display not
@@ -297,7 +297,7 @@ def retime_time_grid(ref):
             continue
         if any(ch in v for v in params.values() for ch in "io"):  # Bezier handles: not served
             continue
-        if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
+        if table.get(c["id"], ("1",))[0] != "0":  # NTSC and decimal composition rates included
             continue
         key = c["input"]
         if key not in inputs:

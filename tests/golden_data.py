@@ -1,4 +1,5 @@
 """Readers of the committed golden fixtures (see tests/golden/make_golden.py)."""
+import fractions
 import gzip
 import json
 import os
@@ -522,11 +523,14 @@ def parse_keys(text):
 
 def rt_case_params(case):
     """Keyword arguments of oracle_lib.retime_params for a retime-time grid case (the effect's
-    defaults elsewhere; Input: Frame Rate defaults to 29.97 narrowed through f32)."""
+    defaults elsewhere; Input: Frame Rate defaults to 29.97 narrowed through f32). The composition
+    rate is the grid's exact rate (``24``, ``30000/1001``, ``29.97``) in lowest terms, the time base
+    the reference's CLI gives it (crates/fx-cli/src/cli.rs:247-257, crates/fx-core/src/time.rs:83-98)."""
     p = dict(x.split("=", 1) for x in case["params"])
     keys, speed = parse_keys(p.get("speed_percent", "100"))
     fn_keys, fnum = parse_keys(p.get("frame_num", "0"))
-    return dict(fps=(int(case["fps"]), 1), speed=speed, keys=keys, vectors=int(p.get("vectors", 5)),
+    fps = fractions.Fraction(case["fps"])
+    return dict(fps=(fps.numerator, fps.denominator), speed=speed, keys=keys, vectors=int(p.get("vectors", 5)),
                 frame_interp=int(p.get("frame_interp", 2)), remap_mode=int(p.get("time_remap_mode", 1)),
                 frame_num=fnum, fn_keys=fn_keys, own_input_rate=p.get("in_fps_is_out_fps", "1") == "0",
                 input_frame_rate=float(p.get("input_frame_rate", float(np.float32(29.97)))))

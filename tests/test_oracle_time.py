@@ -38,7 +38,8 @@ def rt_params():
 
 
 def test_grid_is_served():
-    assert len(RT_CASES) == 400
+    assert len(RT_CASES) == 417
+    assert sum("/" in c["fps"] or "." in c["fps"] for c in RT_CASES) == 17
     labels = {c["id"].split(".")[1].split("-")[0] for c in RT_CASES}
     assert {"speed", "framenum", "rate", "keyed", "interp", "special", "extreme", "length"} <= labels, labels
 
