@@ -479,10 +479,19 @@ typedef struct tw_time_params {
                                   grids record */
     int32_t frame_time_plain;  /* retime-fgbg's frame time: trunc(dur * k + 0.5) at every rate, no bias
                                   branch (timeline.rs:204-210) */
+    int32_t input_fields;      /* Input: Fields popup (plugins/retime/src/lib.rs:70): 2 Upper Field First or
+                                  3 Lower Field First double the source rate (timeline.rs:123-125); 0 and
+                                  1 are None */
+    int32_t mark_segs;         /* Src: Mark Segments popup (1 Cut A, 2 Cut B, 3 Cut C, 4 No MV Use Nearest,
+                                  5 No MV Frame Blend), constant when nmark_keys == 0; 0 reads as 1 */
+    int32_t nmark_keys;        /* its keys: a popup holds each key's value up to the next key */
+    const double* mark_key_frames;
+    const double* mark_key_values;
 } tw_time_params;
 
 /* The selection of output frame n of a clip of width x height (timeline::select, timeline.rs:
- * 451-469, with RemapTimeMap::src_pos :266-331 and the tiny-frame rule prep.rs:111-117). out->a and
+ * 451-469, with RemapTimeMap::src_pos :266-331, the segment override of Src: Mark Segments
+ * marker_override :418-441 and the tiny-frame rule prep.rs:111-117). out->a and
  * out->b are the CLIP frames of the pair, the frames positions a and a + 1 show at frame_time
  * (host.rs:155-159, timeline.rs:336-344), which the clip calls read; with equal rates they are the
  * positions themselves. TW_ERR_BAD_PARAM for a rate at or below 0.01 (timeline.rs:125-127). */

@@ -137,6 +137,15 @@ struct TimeMap {
         }
         return (float)((in_fps / out_fps) * (double)out);
     }
+    // timeline.rs:347-354 (marker): Src: Mark Segments at trunc(((f - base) * dur) + 0.5), the popup's
+    // 1..5 as 0..4, anything else 0
+    Curve marks;
+    int marker(float f) const {
+        float d = f - (float)base;
+        int time = cvtt_i32_d((double)(d * dur) + 0.5);
+        long long v = (long long)marks.at(time);
+        return v >= 1 && v <= 5 ? (int)v - 1 : 0;
+    }
     int frame_time(float f) const {  // timeline.rs:336-344
         float d = f - (float)base;
         if (plain_frame_time || std::fabs(in_fps - out_fps) < frame_time_k)
@@ -201,6 +210,15 @@ struct or_retime_params {
     // retime-fgbg's "360 Video": the engine's wrap-around flag (plugins/retime-fgbg/src/glue.rs:146-151),
     // the wrap solve, the 360 warps, fills and Blur Compensation
     int wrap_360;
+    // Input: Fields (plugins/retime/src/lib.rs:70; 1 None, 2 Upper Field First, 3 Lower Field First):
+    // any field order doubles the source rate (timeline.rs:123-125)
+    int input_fields;
+    // Src: Mark Segments (1 Cut A, 2 Cut B, 3 Cut C, 4 No MV Use Nearest, 5 No MV Frame Blend), a
+    // constant or keys (a popup holds its value from one key to the next)
+    int mark_segs;
+    int nmark_keys;
+    const double* mark_key_frames;
+    const double* mark_key_values;
 };
 
 // timeline.rs:69-76: a rate within 2e-5 (an f32 difference) of 29.97, 59.94 or 23.976 becomes it
@@ -225,12 +243,16 @@ static int retime_map(const or_retime_params* p, TimeMap* map) {
     map->plain_frame_time = p->frame_time_plain != 0;
     map->in_fps = snap_rate(in);
     map->out_fps = snap_rate(out);
+    if (p->input_fields == 2 || p->input_fields == 3) map->in_fps *= 2.0;
     map->dur = (float)(((double)time_step * map->out_fps) / map->in_fps);
     map->speed.constant = p->speed_percent;
     map->speed.set(p->nkeys, p->key_frames, p->key_values, p->key_ease, time_step);
     map->remap_mode = p->remap_mode == 2 ? 2 : 1;
     map->frame_num.constant = p->frame_num;
     map->frame_num.set(p->nfn_keys, p->fn_key_frames, p->fn_key_values, p->fn_key_ease, time_step);
+    map->marks.constant = p->mark_segs > 0 ? p->mark_segs : 1;
+    std::vector<int> hold(p->nmark_keys > 0 ? p->nmark_keys : 0, 2);
+    map->marks.set(p->nmark_keys, p->mark_key_frames, p->mark_key_values, hold.data(), time_step);
     return time_step;
 }
 
@@ -648,6 +670,14 @@ int or_select(const or_retime_params* p, int n, int w, int h, float* s0, float* 
     int vqr = p->vectors - 1;
     *vq = (w >= 2 && h >= 2) ? vqr : 0;  // prep.rs:111-117
     *interp = p->frame_interp - 1;
+    // timeline.rs:418-441 (marker_override, the core's g = trunc(s0 + 1.0)): markers that differ
+    // give (No Vectors, Nearest), then "No MV, Use Nearest" (0, Nearest) and "No MV, Frame Blend"
+    // (0, Blend)
+    int g = cvtt_i32_d((double)*s0 + 1.0);
+    int ma = map.marker((float)*a), mb = map.marker((float)g);
+    if (ma != mb) { *vq = 0; *interp = 0; }
+    if (ma == 3) { *vq = 0; *interp = 0; }
+    if (ma == 4) { *vq = 0; *interp = 1; }
     return 0;
 }
 

@@ -56,8 +56,8 @@ Writes, next to this script:
   wrap-around flag: the wrap solve, the 360 warps, fills, Blur Compensation and prep), same format.
 * ``retime_time_grid.npz`` - the cases of the reference's parity grid ``parity/retime-time`` (the
   time model with No Vectors: Speed and Frame Number modes, constant or keyed without Bezier
-  handles, In FPS is Out FPS and the input rate, Frame Interp; integer, NTSC and decimal
-  composition rates, no Src Mark Segments, no input fields), their input clips as its ``gen_grid.py`` writes them, and the
+  handles, In FPS is Out FPS and the input rate, Frame Interp, Input: Fields, Src: Mark Segments
+  constant or keyed; integer, NTSC and decimal composition rates), their input clips as its ``gen_grid.py`` writes them, and the
   sha256 of the output clip ``results/base.tsv`` records.
 * ``vectors_in_grid.npz`` - the cases of the reference's parity grid ``parity/vectors-in`` that the
   single layer Vectors In render serves (one or both vector layers, no FG matte layer, Display not
@@ -276,7 +276,7 @@ def fgbg_core_grid(ref, video_360=False):
 
 
 RT_SERVED = {"vectors", "speed_percent", "frame_interp", "time_remap_mode", "frame_num", "in_fps_is_out_fps",
-             "input_frame_rate"}
+             "input_frame_rate", "input_fields", "src_mark_segments"}
 
 
 def retime_time_grid(ref):

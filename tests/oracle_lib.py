@@ -49,6 +49,11 @@ class RetimeParams(ctypes.Structure):
         ("frame_time_bias", ctypes.c_double),
         ("frame_time_plain", ctypes.c_int),
         ("wrap_360", ctypes.c_int),
+        ("input_fields", ctypes.c_int),
+        ("mark_segs", ctypes.c_int),
+        ("nmark_keys", ctypes.c_int),
+        ("mark_key_frames", ctypes.POINTER(ctypes.c_double)),
+        ("mark_key_values", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -485,20 +490,30 @@ def _keys(p, keys, prefix):
 def retime_params(fps=(24, 1), quality_high=True, speed=100.0, keys=None, vectors=5, frame_interp=2, smart_blend=0,
                   sensitivity=70.0, blur=0.0, rows_reversed=True, taps_above_first=True, video_360=False, prep=1,
                   track_rgb_a=False, remap_mode=1, frame_num=0.0, fn_keys=None, own_input_rate=False,
-                  input_frame_rate=30.0, frame_time_bias=0.05, frame_time_plain=False, wrap_360=False):
+                  input_frame_rate=30.0, frame_time_bias=0.05, frame_time_plain=False, wrap_360=False, input_fields=1,
+                  mark_segs=1, mark_keys=None):
     """The `retime` parameters of one render. rows_reversed / taps_above_first at their defaults
     are the reference's current code; both False is the revision the parity grid records.
     remap_mode 2 is Frame Number (frame_num or the keyed fn_keys); own_input_rate turns "In FPS is
     Out FPS" off (the input rate input_frame_rate, the output rate fps); frame_time_bias 0.1 is the
     revision the parity grids record (the reference's current value is 0.05); frame_time_plain is
     retime-fgbg's frame time (trunc(dur * k + 0.5) at every rate); wrap_360 is retime-fgbg's "360 Video"
-    (the engine's wrap-around flag)."""
+    (the engine's wrap-around flag); input_fields the Input: Fields popup (1 None); mark_segs the Src:
+    Mark Segments popup, or mark_keys its (frame, value) keys."""
     p = RetimeParams()
     p.remap_mode, p.frame_num = remap_mode, frame_num
     p.own_input_rate, p.input_frame_rate = int(own_input_rate), input_frame_rate
     p.frame_time_bias = frame_time_bias
     p.frame_time_plain = int(frame_time_plain)
     p.wrap_360 = int(wrap_360)
+    p.input_fields, p.mark_segs = int(input_fields), int(mark_segs)
+    if mark_keys:
+        fr = (ctypes.c_double * len(mark_keys))(*[k[0] for k in mark_keys])
+        va = (ctypes.c_double * len(mark_keys))(*[k[1] for k in mark_keys])
+        p.nmark_keys = len(mark_keys)
+        p.mark_key_frames = ctypes.cast(fr, ctypes.POINTER(ctypes.c_double))
+        p.mark_key_values = ctypes.cast(va, ctypes.POINTER(ctypes.c_double))
+        p.__dict__.setdefault("_keep", []).append((fr, va))
     if fn_keys:
         _keys(p, fn_keys, "fn_")
     p.rows_reversed, p.taps_above_first = int(rows_reversed), int(taps_above_first)

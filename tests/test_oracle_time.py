@@ -3,8 +3,8 @@ pinned to the reference's retime-time parity grid, and the library's host time m
 against the oracle's. CPU only.
 
 parity/retime-time renders the effect with No Vectors over Speed and Frame Number modes (constant
-or keyed curves, hold and ease keys), "In FPS is Out FPS" and the input rate model, and Frame
-Interp; its results/base.tsv was recorded by the revision whose frame time between unequal rates
+or keyed curves, hold and ease keys), "In FPS is Out FPS" and the input rate model, Frame Interp,
+Input: Fields and Src: Mark Segments, at integer, NTSC and decimal composition rates; its results/base.tsv was recorded by the revision whose frame time between unequal rates
 took the bias 0.1 (the reference now uses 0.05), so those cases run with frame_time_bias=0.1.
 """
 import hashlib
@@ -38,10 +38,13 @@ def rt_params():
 
 
 def test_grid_is_served():
-    assert len(RT_CASES) == 417
+    assert len(RT_CASES) == 460
     assert sum("/" in c["fps"] or "." in c["fps"] for c in RT_CASES) == 17
+    assert sum(any(x.startswith("input_fields=") for x in c["params"]) for c in RT_CASES) == 15
+    assert sum(any(x.startswith("src_mark_segments=") for x in c["params"]) for c in RT_CASES) == 28
     labels = {c["id"].split(".")[1].split("-")[0] for c in RT_CASES}
-    assert {"speed", "framenum", "rate", "keyed", "interp", "special", "extreme", "length"} <= labels, labels
+    assert {"speed", "framenum", "rate", "keyed", "interp", "special", "extreme", "length", "fields", "marks"} <= labels, \
+        labels
 
 
 @pytest.mark.parametrize("c", rt_params())
@@ -57,7 +60,8 @@ def time_params(kw, bias=0.1):
     return tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], keys=kw["keys"], vectors=kw["vectors"],
                          frame_interp=kw["frame_interp"], remap_mode=kw["remap_mode"], frame_num=kw["frame_num"],
                          fn_keys=kw["fn_keys"], own_input_rate=kw["own_input_rate"],
-                         input_frame_rate=kw["input_frame_rate"], frame_time_bias=bias)
+                         input_frame_rate=kw["input_frame_rate"], frame_time_bias=bias,
+                         input_fields=kw["input_fields"], mark_segs=kw["mark_segs"], mark_keys=kw["mark_keys"])
 
 
 @pytest.mark.parametrize("bias", [0.1, 0.05])

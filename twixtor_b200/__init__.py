@@ -144,7 +144,10 @@ class _TimeParams(ctypes.Structure):
                 ("nfn_keys", ctypes.c_int32), ("fn_key_frames", ctypes.POINTER(ctypes.c_double)),
                 ("fn_key_values", ctypes.POINTER(ctypes.c_double)), ("fn_key_flags", ctypes.POINTER(ctypes.c_int32)),
                 ("own_input_rate", ctypes.c_int32), ("input_frame_rate", ctypes.c_double),
-                ("frame_time_bias", ctypes.c_double), ("frame_time_plain", ctypes.c_int32)]
+                ("frame_time_bias", ctypes.c_double), ("frame_time_plain", ctypes.c_int32),
+                ("input_fields", ctypes.c_int32), ("mark_segs", ctypes.c_int32), ("nmark_keys", ctypes.c_int32),
+                ("mark_key_frames", ctypes.POINTER(ctypes.c_double)),
+                ("mark_key_values", ctypes.POINTER(ctypes.c_double))]
 
 
 class _VecInFrame(ctypes.Structure):
@@ -284,7 +287,9 @@ class TimeParams:
     Frame Num (flags: True or 1 ease, 2 hold); ``remap_mode`` 2 is Frame Number; ``own_input_rate``
     turns "In FPS is Out FPS" off (the input rate ``input_frame_rate``); ``frame_time_bias`` 0.1 is
     the revision the reference's parity grids record (0 reads as its current 0.05);
-    ``frame_time_plain`` is retime-fgbg's frame time (no bias branch)."""
+    ``frame_time_plain`` is retime-fgbg's frame time (no bias branch); ``input_fields`` the Input:
+    Fields popup (2 and 3 double the source rate); ``mark_segs`` the Src: Mark Segments popup, or
+    ``mark_keys`` its (frame, value) keys (held from one key to the next)."""
     fps: Tuple[int, int] = (24, 1)
     speed_percent: float = 100.0
     keys: Optional[Sequence[Tuple[float, float, int]]] = None
@@ -298,6 +303,9 @@ class TimeParams:
     input_frame_rate: float = float(np.float32(29.97))
     frame_time_bias: float = 0.0
     frame_time_plain: bool = False
+    input_fields: int = 1
+    mark_segs: int = 1
+    mark_keys: Optional[Sequence[Tuple[float, float]]] = None
 
     def _c(self):
         p = _TimeParams()
@@ -324,6 +332,15 @@ class TimeParams:
                 setattr(p, v_attr, ctypes.cast(va, ctypes.POINTER(ctypes.c_double)))
                 setattr(p, e_attr, ctypes.cast(ea, ctypes.POINTER(ctypes.c_int32)))
                 keep.append((fr, va, ea))
+        p.input_fields, p.mark_segs, p.nmark_keys = self.input_fields, self.mark_segs, 0
+        if self.mark_keys:
+            n = len(self.mark_keys)
+            fr = (ctypes.c_double * n)(*[k[0] for k in self.mark_keys])
+            va = (ctypes.c_double * n)(*[k[1] for k in self.mark_keys])
+            p.nmark_keys = n
+            p.mark_key_frames = ctypes.cast(fr, ctypes.POINTER(ctypes.c_double))
+            p.mark_key_values = ctypes.cast(va, ctypes.POINTER(ctypes.c_double))
+            keep.append((fr, va))
         p._keep = keep
         return p
 

@@ -71,11 +71,14 @@ struct RetimeMap {
     double frame_time_k = 0.05;
     bool plain_frame_time = false;  // retime-fgbg's frame time: trunc(dur * k + 0.5) at every rate
     int mode = 1;
-    Curve speed, frame_num;
-    explicit RetimeMap(const tw_time_params* p)
+    Curve speed, frame_num, marks;
+    // fields: the retime effect's Input: Fields (the Vectors In map has none)
+    RetimeMap(const tw_time_params* p, bool fields)
         : lts(p->fps_den == 1 ? 100 : p->fps_den),  // crates/fx-core/src/time.rs:92-99
           speed(p->speed_percent, p->nkeys, p->key_frames, p->key_values, p->key_ease, lts),
-          frame_num(p->frame_num, p->nfn_keys, p->fn_key_frames, p->fn_key_values, p->fn_key_flags, lts) {
+          frame_num(p->frame_num, p->nfn_keys, p->fn_key_frames, p->fn_key_values, p->fn_key_flags, lts),
+          marks(p->mark_segs > 0 ? p->mark_segs : 1, p->nmark_keys, p->mark_key_frames, p->mark_key_values, nullptr, lts) {
+        for (auto& k : marks.keys) k.flags = 2;  // a popup holds its value between keys (curves.rs:362)
         double in = 30.0, out = 30.0;  // "In FPS is Out FPS" on: both 30 (timeline.rs:117-120)
         if (p->own_input_rate) {
             in = (double)((float)p->input_frame_rate * 1.0f);
@@ -83,6 +86,7 @@ struct RetimeMap {
         }
         in_fps = snap_rate(in);
         out_fps = snap_rate(out);
+        if (fields && (p->input_fields == 2 || p->input_fields == 3)) in_fps *= 2.0;  // timeline.rs:123-125
         dur = (float)(((double)lts * out_fps) / in_fps);
         if (p->frame_time_bias > 0.0) frame_time_k = p->frame_time_bias;
         plain_frame_time = p->frame_time_plain != 0;
@@ -116,6 +120,12 @@ struct RetimeMap {
         }
         return (float)(ratio * (double)out);
     }
+    // timeline.rs:347-354 (base 0): Src: Mark Segments at trunc((f * dur) + 0.5), 1..5 as 0..4, else 0
+    int marker(float f) const {
+        int32_t time = cvtt_i32_d((double)(f * dur) + 0.5);
+        double v = marks.at(time);
+        return v >= 1.0 && v <= 5.0 ? (int)v - 1 : 0;
+    }
     // timeline.rs:336-344 (base 0), then the clip frame of that tick
     int32_t clip_frame(int32_t pos) const {
         float d = (float)pos;
@@ -134,7 +144,8 @@ extern "C" int tw_select(const tw_time_params* p, int32_t n, int32_t width, int3
     if (p->nkeys > 0 && (!p->key_frames || !p->key_values)) return TW_ERR_BAD_PARAM;
     if (p->nfn_keys > 0 && (!p->fn_key_frames || !p->fn_key_values)) return TW_ERR_BAD_PARAM;
     if (p->remap_mode < 0 || p->remap_mode > 2) return TW_ERR_BAD_PARAM;
-    RetimeMap map(p);
+    if (p->nmark_keys > 0 && (!p->mark_key_frames || !p->mark_key_values)) return TW_ERR_BAD_PARAM;
+    RetimeMap map(p, true);
     if (!map.rates_ok()) return TW_ERR_BAD_PARAM;
     int lts = map.lts;
     int cur = n * lts;
@@ -159,8 +170,16 @@ extern "C" int tw_select(const tw_time_params* p, int32_t n, int32_t width, int3
     if ((double)std::fabs(s0 - s1) > 1e-6 && (double)blur > 0.005) exact = false;
     out->exact = exact ? 1 : 0;
     int vq = p->vectors - 1;
-    out->vectors_quality = (width >= 2 && height >= 2) ? vq : 0;
-    out->interp = p->frame_interp - 1;
+    vq = (width >= 2 && height >= 2) ? vq : 0;
+    int ip = p->frame_interp - 1;
+    // timeline.rs:418-441 (marker_override, the core's g = trunc(s0 + 1.0)): markers that differ give
+    // (No Vectors, Nearest), then No MV Use Nearest (0, Nearest) and No MV Frame Blend (0, Blend)
+    int ma = map.marker((float)a), mb = map.marker((float)cvtt_i32_d((double)s0 + 1.0));
+    if (ma != mb) { vq = 0; ip = 0; }
+    if (ma == 3) { vq = 0; ip = 0; }
+    if (ma == 4) { vq = 0; ip = 1; }
+    out->vectors_quality = vq;
+    out->interp = ip;
     return TW_OK;
 }
 
@@ -177,7 +196,8 @@ extern "C" int tw_select_vectors_in(const tw_time_params* p, int32_t n, int32_t 
     tw_time_params q = *p;  // the effect's rates: the input rate (30 with In FPS is Out FPS), the composition's
     q.own_input_rate = 1;
     q.input_frame_rate = p->own_input_rate ? p->input_frame_rate : 30.0;
-    RetimeMap map(&q);
+    q.nmark_keys = 0;  // the Vectors In effect has no Src: Mark Segments
+    RetimeMap map(&q, false);
     if (!map.rates_ok()) return TW_ERR_BAD_PARAM;
     int lts = map.lts;
     int cur = n * lts;
