@@ -49,9 +49,10 @@ Writes, next to this script:
 * ``fgbg_core_grid.npz`` - the cases of the reference's parity grid ``parity/fgbg-core`` (retime-fgbg
   without FG matte layers: the four warping codes with the Gouraud forward warps, every Motion
   Vectors quality, Frame Interp, prep, Main_BG sensitivity, Blur Compensation, Track RGB+A, the
-  time model; constant parameters but Speed and Frame Num, integer rates, no 360 Video, no Source
-  display, no input fields or Mark Segments), their input clips as its ``gen_grid.py`` renders
-  them, and the sha256 of the output clip ``results/base.tsv`` records.
+  time model with Input: Fields and Src: Mark Segments; constant parameters but Speed, Frame Num and
+  Mark Segments, integer, NTSC and decimal rates, no 360 Video, no Source display), their input
+  clips as its ``gen_grid.py`` renders them, and the sha256 of the output clip ``results/base.tsv``
+  records.
 * ``fgbg_core_360_grid.npz`` - the cases of the same grid with 360 Video on (the engine's
   wrap-around flag: the wrap solve, the 360 warps, fills, Blur Compensation and prep), same format.
 * ``retime_time_grid.npz`` - the cases of the reference's parity grid ``parity/retime-time`` (the
@@ -235,7 +236,7 @@ def fgbg_layers_grid(ref):
 
 FGC_SERVED = {"speed_percent", "warping", "frame_interp", "vectors", "prep", "main_bg_sensitivity", "blur_compensation",
               "track_rgb_a", "video_360", "display", "time_remap_mode", "frame_num", "in_fps_is_out_fps",
-              "input_frame_rate", "plenty_memory"}
+              "input_frame_rate", "plenty_memory", "input_fields", "src_mark_segments"}
 
 
 def fgbg_core_grid(ref, video_360=False):
@@ -255,11 +256,11 @@ def fgbg_core_grid(ref, video_360=False):
         params = dict(p.split("=", 1) for p in c["params"])
         if any(k not in FGC_SERVED for k in params):
             continue
-        if any("@" in v for k, v in params.items() if k not in ("speed_percent", "frame_num")):
+        if any("@" in v for k, v in params.items() if k not in ("speed_percent", "frame_num", "src_mark_segments")):
             continue
         if (params.get("video_360", "0") != "0") != video_360 or params.get("display", "1") == "2":
             continue
-        if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
+        if table.get(c["id"], ("1",))[0] != "0":
             continue
         key = c["input"]
         if key not in inputs:

@@ -555,7 +555,11 @@ def fgc_case_params(case):
     p = dict(x.split("=", 1) for x in case["params"])
     keys, speed = parse_keys(p.get("speed_percent", "100"))
     fn_keys, fnum = parse_keys(p.get("frame_num", "0"))
-    return dict(fps=(int(case["fps"]), 1), speed=speed, keys=keys, vectors=int(p.get("vectors", 5)),
+    fps = fractions.Fraction(case["fps"])
+    mark_keys, marks = parse_keys(p.get("src_mark_segments", "1"))
+    return dict(fps=(fps.numerator, fps.denominator), speed=speed, keys=keys, vectors=int(p.get("vectors", 5)),
+                input_fields=int(p.get("input_fields", 1)), mark_segs=1 if mark_keys else int(marks),
+                mark_keys=[(f, v) for f, v, _ in mark_keys] if mark_keys else None,
                 frame_interp=int(p.get("frame_interp", 2)), smart_blend=int(p.get("warping", 1)) - 1,
                 sensitivity=float(p.get("main_bg_sensitivity", 70)), blur=float(p.get("blur_compensation", 0)),
                 prep={1: 1, 2: 4, 3: 1}[int(p.get("prep", 1))], track_rgb_a=p.get("track_rgb_a", "0") == "1",

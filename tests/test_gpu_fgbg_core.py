@@ -27,7 +27,8 @@ def test_fgbg_core_grid_sha256(dev, c):
     tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], keys=kw["keys"], vectors=kw["vectors"],
                        frame_interp=kw["frame_interp"], blur_compensation=kw["blur"], remap_mode=kw["remap_mode"],
                        frame_num=kw["frame_num"], fn_keys=kw["fn_keys"], own_input_rate=kw["own_input_rate"],
-                       input_frame_rate=kw["input_frame_rate"], frame_time_plain=True)
+                       input_frame_rate=kw["input_frame_rate"], frame_time_plain=True,
+                       input_fields=kw["input_fields"], mark_segs=kw["mark_segs"], mark_keys=kw["mark_keys"])
     sels = [tw.select(tp, k, w, h) for k in range(n)]
     sens = tw.percent_param(kw["sensitivity"])
     both = kw["prep"] == 4

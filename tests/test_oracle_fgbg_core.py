@@ -1,9 +1,10 @@
 """retime-fgbg without FG matte layers, pinned to the reference's fgbg-core parity grid (CPU only).
 
-The 360 served cases of parity/fgbg-core (the four warping codes with the effect's Gouraud forward
-warps, every Motion Vectors quality, the three Frame Interp modes, its Image Prep (2 runs both prep
+The 371 served cases of parity/fgbg-core without 360 Video (the four warping codes with the
+effect's Gouraud forward warps, every Motion Vectors quality, the three Frame Interp modes, its Image Prep (2 runs both prep
 stages, 3 none: plugins/retime-fgbg/src/glue.rs:153-154), Main_BG sensitivity, Blur Compensation,
-Track RGB+A, Speed and Frame Number modes, the input rate model with the effect's plain frame time)
+Track RGB+A, Speed and Frame Number modes, the input rate model with the effect's plain frame time,
+Input: Fields, Src: Mark Segments, NTSC and decimal rates)
 against the sha256 of the output clips results/base.tsv records. That table was recorded at the
 reference's current code: the motion path on bottom-up rows, the taps above first.
 """
@@ -19,7 +20,7 @@ FGC_CASES, FGC_INPUTS = G.fgc_grid()
 
 
 def test_grid_is_served():
-    assert len(FGC_CASES) == 360
+    assert len(FGC_CASES) == 371
 
 
 @pytest.mark.parametrize("c", FGC_CASES, ids=[c["id"] for c in FGC_CASES])
@@ -40,7 +41,8 @@ def test_library_selection_on_the_grid():
         tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], keys=kw["keys"], vectors=kw["vectors"],
                            frame_interp=kw["frame_interp"], blur_compensation=kw["blur"], remap_mode=kw["remap_mode"],
                            frame_num=kw["frame_num"], fn_keys=kw["fn_keys"], own_input_rate=kw["own_input_rate"],
-                           input_frame_rate=kw["input_frame_rate"], frame_time_plain=True)
+                           input_frame_rate=kw["input_frame_rate"], frame_time_plain=True,
+                           input_fields=kw["input_fields"], mark_segs=kw["mark_segs"], mark_keys=kw["mark_keys"])
         for n in range(c["frames"]):
             sel = tw.select(tp, n, w, h)
             want = O.select(p, n, w, h)
