@@ -174,7 +174,7 @@ def create_vectors_grid(ref):
 
 FG_SERVED = {"speed_percent", "warping", "frame_interp", "blur_compensation", "fg1_matte_chan", "fg2_matte_chan", "fg3_matte_chan",
              "fg1_sensitivity", "fg2_sensitivity", "fg3_sensitivity", "main_bg_sensitivity", "vectors", "display",
-             "fg1_inv_matte_shrink", "fg2_inv_matte_shrink", "fg3_inv_matte_shrink", "track_rgb_a"}
+             "fg1_inv_matte_shrink", "fg2_inv_matte_shrink", "fg3_inv_matte_shrink", "track_rgb_a", "src_mark_segments"}
 
 
 def fgbg_layers_grid(ref):
@@ -209,7 +209,7 @@ def fgbg_layers_grid(ref):
         pt = [k for k in params if k.startswith("pt")]
         if any(k not in FG_SERVED and k not in pt and k != "draw_geom" for k in params):
             continue
-        if any("@" in v for k, v in params.items() if k not in pt):
+        if any("@" in v for k, v in params.items() if k not in pt and k != "src_mark_segments"):
             continue
         if params.get("warping", "1") not in ("1", "2", "3", "4"):
             continue

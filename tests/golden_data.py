@@ -194,7 +194,9 @@ def fgbg_case_params(case):
     sensitivity and inverse matte shrink."""
     p = dict(x.split("=", 1) for x in case["params"])
     nfg = len(case["mattes"])
+    mark_keys, marks = parse_keys(p.get("src_mark_segments", "1"))
     return dict(fps=(int(case["fps"]), 1), speed=float(p.get("speed_percent", 100)), vectors=int(p.get("vectors", 5)),
+                mark_segs=1 if mark_keys else int(marks), mark_keys=[(f, v) for f, v, _ in mark_keys] if mark_keys else None,
                 frame_interp=int(p.get("frame_interp", 2)), smart_blend=int(p.get("warping", "1")) - 1,
                 blur=float(p.get("blur_compensation", 0)),
                 sensitivity=float(p.get("main_bg_sensitivity", 70)),

@@ -165,7 +165,7 @@ def fgbg_clip(dev, case, rows_reversed=True, taps_above_first=True):
     w, h, n = case["width"], case["height"], case["frames"]
     kw = golden_data.fgbg_case_params(case)
     tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], vectors=kw["vectors"], frame_interp=kw["frame_interp"],
-                       blur_compensation=kw["blur"])
+                       blur_compensation=kw["blur"], mark_segs=kw["mark_segs"], mark_keys=kw["mark_keys"])
     sels = [tw.select(tp, k, w, h) for k in range(n)]
     s = tw.RetimeSettings(flow=tw.FlowSettings(hiq=True, taps_above_first=taps_above_first,
                                                track_alpha=kw["track_rgb_a"]),
