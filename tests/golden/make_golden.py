@@ -351,7 +351,7 @@ def vectors_in_grid(ref):
                 continue
             if "vectors_prev" not in lay and "vectors_next" not in lay:
                 continue
-            if "/" in c["fps"] or "." in c["fps"] or table.get(c["id"], ("1",))[0] != "0":
+            if table.get(c["id"], ("1",))[0] != "0":
                 continue
             main = lay.get("source", c["input"])
             frames_of = lambda rel: g.inputs[rel]["frames"]

@@ -461,7 +461,8 @@ def vi_case_params(case):
     p = dict(x.split("=", 1) for x in case["params"])
     keys, speed = parse_keys(p.get("speed_percent", "100"))
     fn_keys, fnum = parse_keys(p.get("frame_num", "0"))
-    return dict(fps=(int(case["fps"]), 1), speed=speed, keys=keys, remap_mode=int(p.get("time_remap_mode", 1)),
+    fps = fractions.Fraction(case["fps"])
+    return dict(fps=(fps.numerator, fps.denominator), speed=speed, keys=keys, remap_mode=int(p.get("time_remap_mode", 1)),
                 frame_num=fnum, fn_keys=fn_keys, own_input_rate=p.get("in_fps_is_out_fps", "1") == "0",
                 input_frame_rate=float(p.get("input_frame_rate", float(np.float32(29.97)))),
                 frame_interp=int(p.get("frame_interp", 2)), warping=int(p.get("warping", 2)),

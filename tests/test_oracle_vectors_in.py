@@ -45,7 +45,8 @@ GRID_ORDERS = dict(rows_reversed=False, taps_above_first=False, gouraud=False, p
 
 
 def test_vectors_in_grid_is_served():
-    assert len(VI_CASES) == 390
+    assert len(VI_CASES) == 399
+    assert sum("/" in c["fps"] or "." in c["fps"] for c in VI_CASES) == 9
     groups = {c["id"].split(".")[1].split("-")[0] for c in VI_CASES}
     assert {"size", "warp1", "warp2", "vec", "md16", "scalex2", "prev", "next", "short", "spvecR", "spvecA",
             "spsrc", "blur1", "foot", "fnum", "inrate", "ftime", "key"} <= groups, groups
@@ -114,7 +115,7 @@ def test_matte_step():
     assert got[0] == np.float32(0.7) and got[4] == np.float32(0.1)
 
 
-@pytest.mark.parametrize("fps", [(30, 1), (24, 1), (25, 1), (12, 1), (60, 1)])
+@pytest.mark.parametrize("fps", [(30, 1), (24, 1), (25, 1), (12, 1), (60, 1), (30000, 1001), (2997, 100), (24000, 1001)])
 @pytest.mark.parametrize("speed", [50.0, 100.0, 33.3333, 150.0, -50.0, 0.5])
 def test_selection_of_the_library(fps, speed):
     """tw_select_vectors_in (the product's host time model of the effect) against the oracle's, for
