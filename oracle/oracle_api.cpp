@@ -1253,6 +1253,11 @@ struct or_vecin_params {
     const int* fn_key_ease;    // per key: bit 0 ease, bit 1 hold
     int own_input_rate;        // In FPS is Out FPS off: the input rate Input: Frame Rate
     double input_frame_rate;
+    // Src: Mark Segments (plugins/vectors-in/src/lib.rs:93), constant or keys held between keys
+    int mark_segs;
+    int nmark_keys;
+    const double* mark_key_frames;
+    const double* mark_key_values;
 };
 
 // compose/vector.rs:329-345 (flow_from_vector_image_with) over an engine image, for the tests
@@ -1336,6 +1341,20 @@ static int vecin_select(const or_vecin_params* p, int n, int w, int h, TimeMap* 
     sel->exact = exact_position(sel->s0, sel->s1, blur);
     sel->vectors_quality = (w >= 2 && h >= 2) ? 4 : 0;
     sel->interp = p->frame_interp - 1;
+    // timeline.rs:418-441 (marker_override) with the effect's marker, Src: Mark Segments at
+    // T(f) = trunc((f64)dur * (f64)f + 0.5) (plugins/vectors-in/src/timemap.rs:49-70)
+    Curve marks;
+    marks.constant = p->mark_segs > 0 ? p->mark_segs : 1;
+    std::vector<int> hold(p->nmark_keys > 0 ? p->nmark_keys : 0, 2);
+    marks.set(p->nmark_keys, p->mark_key_frames, p->mark_key_values, hold.data(), time_step);
+    auto marker = [&](float f) {
+        long long v = (long long)marks.at(cvtt_i32_d((double)map->dur * (double)f + 0.5));
+        return v >= 1 && v <= 5 ? (int)v - 1 : 0;
+    };
+    int ma = marker((float)sel->a), mb = marker((float)cvtt_i32_d((double)sel->s0 + 1.0));
+    if (ma != mb) { sel->vectors_quality = 0; sel->interp = 0; }
+    if (ma == 3) { sel->vectors_quality = 0; sel->interp = 0; }
+    if (ma == 4) { sel->vectors_quality = 0; sel->interp = 1; }
     return time_step;
 }
 

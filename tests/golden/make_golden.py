@@ -315,7 +315,8 @@ def retime_time_grid(ref):
 
 
 VI_SERVED = {"vectors_max_displace", "speed_percent", "warping", "frame_interp", "blur_compensation", "vec_scale_x",
-             "vec_scale_y", "display", "time_remap_mode", "frame_num", "in_fps_is_out_fps", "input_frame_rate"}
+             "vec_scale_y", "display", "time_remap_mode", "frame_num", "in_fps_is_out_fps", "input_frame_rate",
+             "src_mark_segments"}
 
 
 def vectors_in_grid(ref):
@@ -342,7 +343,7 @@ def vectors_in_grid(ref):
             params = dict(p.split("=", 1) for p in c["params"])
             if any(k not in VI_SERVED for k in params):
                 continue
-            if any("@" in v for k, v in params.items() if k not in ("speed_percent", "frame_num")):
+            if any("@" in v for k, v in params.items() if k not in ("speed_percent", "frame_num", "src_mark_segments")):
                 continue
             if params.get("display", "1") == "2":
                 continue

@@ -462,7 +462,9 @@ def vi_case_params(case):
     keys, speed = parse_keys(p.get("speed_percent", "100"))
     fn_keys, fnum = parse_keys(p.get("frame_num", "0"))
     fps = fractions.Fraction(case["fps"])
+    mark_keys, marks = parse_keys(p.get("src_mark_segments", "1"))
     return dict(fps=(fps.numerator, fps.denominator), speed=speed, keys=keys, remap_mode=int(p.get("time_remap_mode", 1)),
+                mark_segs=1 if mark_keys else int(marks), mark_keys=[(f, v) for f, v, _ in mark_keys] if mark_keys else None,
                 frame_num=fnum, fn_keys=fn_keys, own_input_rate=p.get("in_fps_is_out_fps", "1") == "0",
                 input_frame_rate=float(p.get("input_frame_rate", float(np.float32(29.97)))),
                 frame_interp=int(p.get("frame_interp", 2)), warping=int(p.get("warping", 2)),

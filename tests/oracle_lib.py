@@ -85,6 +85,10 @@ class VecInParams(ctypes.Structure):
         ("fn_key_ease", ctypes.POINTER(ctypes.c_int)),
         ("own_input_rate", ctypes.c_int),
         ("input_frame_rate", ctypes.c_double),
+        ("mark_segs", ctypes.c_int),
+        ("nmark_keys", ctypes.c_int),
+        ("mark_key_frames", ctypes.POINTER(ctypes.c_double)),
+        ("mark_key_values", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -674,7 +678,7 @@ def matte_step(vec, w, h, fmt, matte):
 def vecin_params(fps=(30, 1), quality_high=True, speed=100.0, keys=None, frame_interp=2, warping=2, blur=0.0,
                  max_displace=2048.0, vec_scale=(1.0, 1.0), rows_reversed=True, taps_above_first=True, gouraud=True,
                  probe_current_time=False, remap_mode=1, frame_num=0.0, fn_keys=None, own_input_rate=False,
-                 input_frame_rate=30.0):
+                 input_frame_rate=30.0, mark_segs=1, mark_keys=None):
     """The `vectors-in` parameters of one render (the effect's defaults; the three orders at the
     plugin's: bottom-up rows, the tap above first, the Gouraud forward warp; a set vector layer
     present at every time). All four False is the revision the parity grid records."""
@@ -701,6 +705,14 @@ def vecin_params(fps=(30, 1), quality_high=True, speed=100.0, keys=None, frame_i
         p.key_values = ctypes.cast(va, ctypes.POINTER(ctypes.c_double))
         p.key_ease = ctypes.cast(ea, ctypes.POINTER(ctypes.c_int))
         p._keep = (fr, va, ea)
+    p.mark_segs, p.nmark_keys = int(mark_segs), 0
+    if mark_keys:
+        mf = (ctypes.c_double * len(mark_keys))(*[k[0] for k in mark_keys])
+        mv = (ctypes.c_double * len(mark_keys))(*[k[1] for k in mark_keys])
+        p.nmark_keys = len(mark_keys)
+        p.mark_key_frames = ctypes.cast(mf, ctypes.POINTER(ctypes.c_double))
+        p.mark_key_values = ctypes.cast(mv, ctypes.POINTER(ctypes.c_double))
+        p.__dict__.setdefault("_keep_marks", []).append((mf, mv))
     return p
 
 

@@ -131,7 +131,7 @@ def grid_frames(c):
     tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], keys=kw["keys"], frame_interp=kw["frame_interp"],
                        blur_compensation=kw["blur"], remap_mode=kw["remap_mode"], frame_num=kw["frame_num"],
                        fn_keys=kw["fn_keys"], own_input_rate=kw["own_input_rate"],
-                       input_frame_rate=kw["input_frame_rate"])
+                       input_frame_rate=kw["input_frame_rate"], mark_segs=kw["mark_segs"], mark_keys=kw["mark_keys"])
     sc = tuple(float(tw.fixed_param(v)) for v in kw["vec_scale"])
     sels, vfs = [], []
     for n in range(c["frames"]):

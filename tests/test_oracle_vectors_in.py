@@ -45,7 +45,8 @@ GRID_ORDERS = dict(rows_reversed=False, taps_above_first=False, gouraud=False, p
 
 
 def test_vectors_in_grid_is_served():
-    assert len(VI_CASES) == 399
+    assert len(VI_CASES) == 408
+    assert sum(any(x.startswith("src_mark_segments=") for x in c["params"]) for c in VI_CASES) == 9
     assert sum("/" in c["fps"] or "." in c["fps"] for c in VI_CASES) == 9
     groups = {c["id"].split(".")[1].split("-")[0] for c in VI_CASES}
     assert {"size", "warp1", "warp2", "vec", "md16", "scalex2", "prev", "next", "short", "spvecR", "spvecA",
@@ -129,3 +130,24 @@ def test_selection_of_the_library(fps, speed):
         got = dict(s0=np.float32(sel.s0), s1=np.float32(sel.s1), wa=np.float32(sel.wa), a=sel.a, exact=bool(sel.exact),
                    vq=sel.vectors_quality, interp=sel.interp, clip_a=vf.a, clip_b=vf.b)
         assert got == want, (n, got, want)
+
+
+def test_library_selection_on_the_grid():
+    """tw_select_vectors_in against the oracle's selection on every output frame of every served
+    grid case (Speed and Frame Number modes, keyed curves, the input rate model, Src: Mark Segments
+    constant or keyed, NTSC and decimal rates)."""
+    import twixtor_b200 as tw
+    for c in VI_CASES:
+        w, h = c["width"], c["height"]
+        kw = G.vi_case_params(c)
+        p = O.vecin_params(**kw, **GRID_ORDERS)
+        tp = tw.TimeParams(fps=kw["fps"], speed_percent=kw["speed"], keys=kw["keys"], frame_interp=kw["frame_interp"],
+                           blur_compensation=kw["blur"], remap_mode=kw["remap_mode"], frame_num=kw["frame_num"],
+                           fn_keys=kw["fn_keys"], own_input_rate=kw["own_input_rate"],
+                           input_frame_rate=kw["input_frame_rate"], mark_segs=kw["mark_segs"], mark_keys=kw["mark_keys"])
+        for n in range(c["frames"]):
+            want = O.vecin_select(p, n, w, h)
+            sel, vf = tw.select_vectors_in(tp, n, w, h)
+            got = dict(s0=np.float32(sel.s0), s1=np.float32(sel.s1), wa=np.float32(sel.wa), a=sel.a,
+                       exact=bool(sel.exact), vq=sel.vectors_quality, interp=sel.interp, clip_a=vf.a, clip_b=vf.b)
+            assert got == want, (c["id"], n, got, want)

@@ -193,10 +193,10 @@ extern "C" int tw_select_vectors_in(const tw_time_params* p, int32_t n, int32_t 
     if (p->nkeys > 0 && (!p->key_frames || !p->key_values)) return TW_ERR_BAD_PARAM;
     if (p->nfn_keys > 0 && (!p->fn_key_frames || !p->fn_key_values)) return TW_ERR_BAD_PARAM;
     if (p->remap_mode < 0 || p->remap_mode > 2) return TW_ERR_BAD_PARAM;
+    if (p->nmark_keys > 0 && (!p->mark_key_frames || !p->mark_key_values)) return TW_ERR_BAD_PARAM;
     tw_time_params q = *p;  // the effect's rates: the input rate (30 with In FPS is Out FPS), the composition's
     q.own_input_rate = 1;
     q.input_frame_rate = p->own_input_rate ? p->input_frame_rate : 30.0;
-    q.nmark_keys = 0;  // the Vectors In effect has no Src: Mark Segments
     RetimeMap map(&q, false);
     if (!map.rates_ok()) return TW_ERR_BAD_PARAM;
     int lts = map.lts;
@@ -219,8 +219,19 @@ extern "C" int tw_select_vectors_in(const tw_time_params* p, int32_t n, int32_t 
     if ((double)std::fabs(fr) > 0.005 && (double)std::fabs((float)((double)fr - 1.0)) > 0.005) exact = false;
     if ((double)std::fabs(s0 - s1) > 1e-6 && (double)blur > 0.005) exact = false;
     out->exact = exact ? 1 : 0;
-    out->vectors_quality = (width >= 2 && height >= 2) ? 4 : 0;
-    out->interp = p->frame_interp - 1;
+    int vq = (width >= 2 && height >= 2) ? 4 : 0, ip = p->frame_interp - 1;
+    // timeline.rs:418-441 (marker_override) with the effect's marker: Src: Mark Segments at
+    // T(f) = trunc((f64)dur * (f64)f + 0.5) (plugins/vectors-in/src/timemap.rs:49-70)
+    auto marker = [&](float f) {
+        double v = map.marks.at(cvtt_i32_d((double)map.dur * (double)f + 0.5));
+        return v >= 1.0 && v <= 5.0 ? (int)v - 1 : 0;
+    };
+    int ma = marker((float)a), mb = marker((float)cvtt_i32_d((double)s0 + 1.0));
+    if (ma != mb) { vq = 0; ip = 0; }
+    if (ma == 3) { vq = 0; ip = 0; }
+    if (ma == 4) { vq = 0; ip = 1; }
+    out->vectors_quality = vq;
+    out->interp = ip;
     auto clip_index = [&](int32_t pos) -> int32_t {  // T(k) = trunc(dur * k + 0.5), timemap.rs:45-50
         int32_t time = cvtt_i32_d((double)map.dur * (double)(float)pos + 0.5);
         long long idx = time >= 0 ? time / lts : -(((long long)-time + lts - 1) / lts);
