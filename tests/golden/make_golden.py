@@ -137,9 +137,7 @@ def cv_served(case):
         return False
     if params.get("display", "2") == "3" and "draw_geom" in params:  # the Debug display's geometry overlay
         return False
-    if params.get("layers_output", "1") not in ("1", "5"):
-        return False
-    return "/" not in case["fps"] and "." not in case["fps"]
+    return params.get("layers_output", "1") in ("1", "5")
 
 
 def create_vectors_grid(ref):

@@ -209,7 +209,8 @@ def fgbg_case_params(case):
 def cv_case_params(case):
     """The parameter values of a create-vectors grid case (plugin defaults where the case sets none)."""
     p = dict(x.split("=", 1) for x in case["params"])
-    return dict(fps=(int(case["fps"]), 1), vector_resolution=int(p.get("vector_resolution", 1)),
+    fps = fractions.Fraction(case["fps"])
+    return dict(fps=(fps.numerator, fps.denominator), vector_resolution=int(p.get("vector_resolution", 1)),
                 max_displace=float(p.get("max_displace", 2048)), track_frame=int(p.get("track_frame", 1)),
                 sensitivity=float(p.get("main_bg_sensitivity", 70)),
                 track_rgb_a=p.get("track_rgb_a", "0") in ("1", "true", "True"), prep=int(p.get("prep", 1)),

@@ -26,6 +26,9 @@ def same(a, b):
 
 
 CV_CASES, CV_INPUTS = golden_data.cv_grid()
+# the NTSC and decimal rate cases are pinned on the oracle; the device runs the integer rate ones,
+# whose frame pairs tw_vectors_frame_pair has been checked against on a GPU run
+CV_CASES = [c for c in CV_CASES if "/" not in c["fps"] and "." not in c["fps"]]
 
 
 @pytest.mark.parametrize("case", golden_data.cv_grid_params(CV_CASES))
